@@ -1,0 +1,502 @@
+/*
+ * numi_b200 — B200 (sm_100a) batched articulated-physics microstep behind
+ * numi-lab's task-rollout C ABI.
+ *
+ * Every declaration below that carries a "reference:" note replaces the
+ * numi-lab (MetalRobo) interface at that file:line with the same name,
+ * argument meaning and error behaviour:
+ *   - ints return 0 on success and -1 on error;
+ *   - errors are stored in a thread-local string read by mr_last_error();
+ *   - caller spans are copied before return;
+ *   - returned pointers alias handle-owned memory until the next advance,
+ *     reset or destroy of that handle;
+ *   - a handle is not internally locked: one caller thread per handle.
+ *
+ * Entry points marked "no counterpart in the reference" are additions of
+ * this library (device-pointer advance for zero-copy torch tensors, model
+ * and state export for checking and serving).
+ */
+#ifndef NUMI_B200_H
+#define NUMI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#define MR_API __attribute__((visibility("default")))
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------- */
+/* Capacities and enumerations                                             */
+/* ---------------------------------------------------------------------- */
+
+#define MR_INVALID_INDEX 0xffffffffu
+#define MR_B200_MAX_BODIES 32u     /* bodies per articulated world           */
+#define MR_B200_MAX_DOFS 40u       /* generalized velocities per world       */
+#define MR_B200_MAX_Q 41u          /* generalized coordinates per world      */
+#define MR_B200_MAX_SHAPES 32u     /* colliders per world                    */
+#define MR_B200_MAX_PAIRS 32u      /* compiled eligible collider pairs       */
+#define MR_B200_MAX_CONTACTS 32u   /* solver contacts per environment        */
+#define MR_B200_MANIFOLD_POINTS 4u /* persistent points per manifold         */
+#define MR_B200_MAX_SUBSTEPS 64u   /* physics substeps per control step      */
+
+/* The enumerations below carry the reference's own names and values; a
+ * translation unit that already includes the reference's engine_types.h
+ * defines NUMI_B200_OMIT_SHARED_ENUMS before including this header. */
+#ifndef NUMI_B200_OMIT_SHARED_ENUMS
+/* reference: include/metalrobo/engine_types.h:171-188 (same values). */
+enum MRStepStatusCode {
+    MR_STEP_SUCCESS = 0u,
+    MR_STEP_FIXED_BUDGET_COMPLETE = 1u,
+    MR_STEP_NONFINITE_INPUT = 2u,
+    MR_STEP_NONFINITE_RESULT = 3u,
+    MR_STEP_PAIR_CAPACITY_OVERFLOW = 4u,
+    MR_STEP_CONTACT_CAPACITY_OVERFLOW = 5u,
+    MR_STEP_MANIFOLD_CAPACITY_OVERFLOW = 6u,
+    MR_STEP_CONSTRAINT_CAPACITY_OVERFLOW = 7u,
+    MR_STEP_ISLAND_CAPACITY_OVERFLOW = 8u,
+    MR_STEP_CCD_EVENT_BUDGET_EXHAUSTED = 9u,
+    MR_STEP_FACTORIZATION_FAILED = 10u,
+    MR_STEP_DID_NOT_CONVERGE = 11u,
+    MR_STEP_UNSUPPORTED = 12u,
+    MR_STEP_CCD_CAPACITY_OVERFLOW = 13u
+};
+
+/* reference: include/metalrobo/gpu_types.h:41-49 (same values). */
+enum MRShapeType {
+    MR_SHAPE_SPHERE = 0u,
+    MR_SHAPE_CAPSULE = 1u,
+    MR_SHAPE_BOX = 2u,
+    MR_SHAPE_PLANE = 3u
+};
+
+/* reference: include/metalrobo/engine_types.h:114-134 (same values). */
+enum MRJointTypeExt {
+    MR_JOINT_REVOLUTE = 0u,
+    MR_JOINT_PRISMATIC = 1u,
+    MR_JOINT_CONTINUOUS = 2u,
+    MR_JOINT_FIXED = 5u
+};
+
+enum MRRootType { MR_ROOT_FIXED = 0u, MR_ROOT_FLOATING = 1u };
+enum MRMotionType { MR_MOTION_STATIC = 0u, MR_MOTION_KINEMATIC = 1u, MR_MOTION_DYNAMIC = 2u };
+
+/* reference: include/metalrobo/engine_types.h:262-272 (same bits). */
+enum MRDofFlags {
+    MR_DOF_FLAG_ROOT = 1u << 0u,
+    MR_DOF_FLAG_ACTUATED = 1u << 1u,
+    MR_DOF_FLAG_POSITION_LIMIT = 1u << 2u,
+    MR_DOF_FLAG_VELOCITY_LIMIT = 1u << 3u,
+    MR_DOF_FLAG_EFFORT_LIMIT = 1u << 4u,
+    MR_DOF_FLAG_DRIVE = 1u << 5u
+};
+
+/* reference: include/metalrobo/engine_types.h:149-163 (same values). */
+enum MRCollisionPairClass {
+    MR_COLLISION_PAIR_UNSUPPORTED = 0u,
+    MR_COLLISION_PAIR_SPHERE_PLANE = 2u,
+    MR_COLLISION_PAIR_CAPSULE_PLANE = 3u,
+    MR_COLLISION_PAIR_BOX_PLANE = 4u
+};
+#endif /* NUMI_B200_OMIT_SHARED_ENUMS */
+
+/* Actuation law of a world: efforts are generalized forces, or position
+ * targets of implicit PD drives (reference: MetalWorld.hpp:388-391). */
+enum MRActuationMode { MR_ACTUATION_EFFORT = 0u, MR_ACTUATION_IMPLICIT_POSITION = 1u };
+
+/* ---------------------------------------------------------------------- */
+/* Rollout configuration (reference: include/metalrobo/c_api.h:54-88)     */
+/* ---------------------------------------------------------------------- */
+
+typedef struct MRTaskRolloutHandle MRTaskRolloutHandle;
+
+typedef struct MRTaskRolloutDynamicSphereC {
+    float position[3];
+    float linear_velocity[3];
+    float radius;
+    float mass;
+    uint32_t launch_step;
+} MRTaskRolloutDynamicSphereC;
+
+typedef struct MRTaskRolloutConfigC {
+    uint32_t environment_count;
+    uint32_t physics_substeps;
+    uint32_t velocity_iterations;
+    uint32_t final_velocity_iterations;
+    float control_timestep_seconds;
+    uint64_t seed;
+    const MRTaskRolloutDynamicSphereC* dynamic_spheres;
+    uint32_t dynamic_sphere_count;
+    uint32_t disable_task_terminations;
+    uint32_t interaction_reference_mode;
+    float interaction_student_authority;
+    uint32_t override_interaction_student_authority;
+    float interaction_reset_phase_fraction;
+    uint32_t override_interaction_reset_phase_fraction;
+    uint32_t materialize_articulated_contact_responses;
+    uint32_t override_difficulty_band_range;
+    uint32_t minimum_difficulty_band;
+    uint32_t maximum_difficulty_band;
+    float interaction_reset_phase_probability;
+    uint32_t override_interaction_reset_phase_probability;
+    float interaction_reset_maximum_phase;
+    uint32_t override_interaction_reset_maximum_phase;
+} MRTaskRolloutConfigC;
+
+/* Visual programs are not part of the physics path; the type stays opaque
+ * and a non-null pointer is rejected. */
+typedef struct MRTaskVisualObservationConfigC MRTaskVisualObservationConfigC;
+
+/* reference: include/metalrobo/c_api.h:160-166.  The reference sources
+ * 0..4 load robot assets; this library compiles seeded synthetic worlds. */
+enum MRRunManifestSourceC {
+    MR_RUN_SOURCE_UNITREE_G1 = 0u,
+    MR_RUN_SOURCE_FRANKA_PICK_PLACE = 1u,
+    MR_RUN_SOURCE_IMPORTED_URDF = 2u,
+    MR_RUN_SOURCE_WORLD_PACK = 3u,
+    MR_RUN_SOURCE_PX4_X500 = 4u,
+    /* Fixed-base 7-revolute serial chain, effort actuation, no contact. */
+    MR_RUN_SOURCE_SYNTHETIC_CHAIN7 = 100u,
+    /* Floating 29-DoF humanoid tree (pelvis, 2x6 legs, 3 waist, 2x7 arms),
+     * implicit PD position drives, box feet and 12 sphere proxies on a
+     * ground plane. */
+    MR_RUN_SOURCE_SYNTHETIC_TREE29 = 101u
+};
+
+/* reference: include/metalrobo/c_api.h:171-190 (same shape). */
+typedef struct MRRunManifestC {
+    MRTaskRolloutConfigC profile;
+    uint32_t source;
+    uint32_t surface;
+    uint32_t task;
+    const char* urdf_path;
+    const char* srdf_path;
+    const char* world_pack_path;
+    const char* task_pack_path;
+    const char* robot_actuator_pack_path;
+    const char* sensor_program_pack_path;
+    const char* reality_program_pack_path;
+    const char* teacher_pack_path;
+    const char* teacher_clip_id;
+    const MRTaskVisualObservationConfigC* visual_sensor_program;
+    const MRTaskVisualObservationConfigC* inspection_visual_program;
+    const char* metallib_path;
+} MRRunManifestC;
+
+/* reference: include/metalrobo/c_api.h:128-158 (same shape). */
+typedef struct MRTaskRolloutLayoutC {
+    uint32_t environment_count;
+    uint32_t nq;
+    uint32_t nv;
+    uint32_t action_count;
+    uint32_t actor_observation_count;
+    uint32_t critic_observation_count;
+    uint32_t scene_body_count;
+    uint32_t motion_feature_count;
+    uint32_t maximum_episode_steps;
+    uint64_t world_fingerprint;
+    uint64_t task_fingerprint;
+    uint64_t observation_fingerprint;
+    uint64_t action_fingerprint;
+    uint64_t run_fingerprint;
+    uint64_t robot_fingerprint;
+    uint64_t sensor_fingerprint;
+    uint64_t reality_fingerprint;
+    uint64_t teacher_fingerprint;
+    uint64_t submitted_control_steps;
+    uint64_t completed_environment_steps;
+    uint64_t submission_count;
+    size_t retained_buffer_bytes;
+    size_t immutable_private_bytes;
+    size_t persistent_state_private_bytes;
+    size_t transient_private_bytes;
+    size_t shared_boundary_bytes;
+    size_t peak_aliased_bytes;
+    double total_gpu_milliseconds;
+    double total_submission_milliseconds;
+} MRTaskRolloutLayoutC;
+
+/* reference: include/metalrobo/c_api.h:192-220 (same shape). */
+typedef struct MRTaskRolloutStageHighWaterC {
+    uint32_t candidate_pairs;
+    uint32_t raw_contacts;
+    uint32_t manifolds;
+    uint32_t constraint_blocks;
+    uint32_t constraint_rows;
+    uint32_t islands;
+    uint32_t hard_convex_pairs;
+    uint32_t mesh_triangle_candidates;
+    uint32_t solver_tiles;
+    uint32_t spill_rows;
+    uint32_t ccd_candidates;
+    uint32_t ccd_events;
+    uint32_t endpoint_runtime_records;
+    uint32_t articulation_point_queries;
+    uint32_t rod_candidate_pairs;
+    uint32_t rod_raw_contacts;
+    uint32_t rod_manifolds;
+    uint32_t rod_ccd_events;
+    uint32_t quality_generalized_velocities;
+    uint32_t quality_rows;
+    uint32_t quality_krylov_vectors;
+    uint32_t quality_direct_tiles;
+    uint32_t dynamic_nodes;
+    uint32_t island_node_references;
+    uint32_t island_constraint_references;
+    uint32_t rod_factor_blocks;
+    uint32_t operator_velocity_elements;
+} MRTaskRolloutStageHighWaterC;
+
+/* reference: include/metalrobo/c_api.h:222-235 (same shape). */
+typedef struct MRTaskRolloutAdvanceC {
+    uint32_t control_step_count;
+    uint32_t successful_environment_steps;
+    uint32_t failed_environment_steps;
+    uint32_t first_failing_environment;
+    uint32_t first_failing_control_step;
+    uint32_t first_gpu_status_code;
+    uint32_t host_requested_resets;
+    uint32_t maximum_active_contacts;
+    uint32_t maximum_manifolds;
+    MRTaskRolloutStageHighWaterC high_water;
+    double gpu_milliseconds;
+    double submission_milliseconds;
+} MRTaskRolloutAdvanceC;
+
+/* ---------------------------------------------------------------------- */
+/* Compiled model records (no counterpart in the reference's C ABI; they   */
+/* carry the fields of engine_types.h MRWorldGPU, MRJointDescriptorGPU,    */
+/* MRBodyPropertiesGPU, MRDofPropertiesGPU, MRShapeGPU and MRMaterialGPU   */
+/* that the microstep reads, so a checker can rebuild the same world).     */
+/* ---------------------------------------------------------------------- */
+
+typedef struct MRModelWorldC {
+    uint32_t body_count;
+    uint32_t joint_count;
+    uint32_t nq;
+    uint32_t nv;
+    uint32_t shape_count;
+    uint32_t material_count;
+    uint32_t pair_count;
+    uint32_t root_type;            /* MRRootType                              */
+    uint32_t actuation_mode;       /* MRActuationMode                         */
+    uint32_t action_count;         /* actions per env per control step        */
+    uint32_t contact_capacity;     /* solver contacts per env                 */
+    uint32_t apply_body_damping;
+    float gravity[4];              /* xyz gravity, w unused                   */
+    /* tolerance, minimum compliance, maximum depenetration speed, slop      */
+    float solver_scales[4];
+    /* breaking separation, breaking tangential drift, merge distance,
+     * normal cosine (reference: MetalWorld.hpp:441-444)                     */
+    float manifold_thresholds[4];
+    /* speculative margin scale, speed envelope, reserved, reserved          */
+    float speculative[4];
+} MRModelWorldC;
+
+typedef struct MRModelJointC {
+    uint32_t parent_body;
+    uint32_t child_body;
+    uint32_t joint_type;           /* MRJointTypeExt                          */
+    uint32_t q_index;              /* MR_INVALID_INDEX for fixed joints       */
+    uint32_t v_index;
+    uint32_t reserved[3];
+    float axis[4];                 /* joint-frame axis                        */
+    float parent_anchor[4];        /* relative to parent COM, parent axes     */
+    float child_anchor[4];         /* relative to child COM, child axes       */
+    float parent_rotation[4];      /* joint frame in parent, xyzw             */
+    float child_rotation[4];       /* joint frame in child, xyzw              */
+} MRModelJointC;
+
+typedef struct MRModelBodyC {
+    uint32_t parent_body;          /* MR_INVALID_INDEX for the root / statics */
+    uint32_t inbound_joint;
+    uint32_t motion_type;          /* MRMotionType                            */
+    uint32_t articulated;          /* 1 when part of the articulation         */
+    float mass_inverse_mass[4];
+    float inertia[3][4];           /* symmetric inertia about COM, body axes  */
+    /* linear damping, angular damping, max linear speed, max angular speed  */
+    float damping_speed[4];
+    float static_pose[8];          /* static bodies: position xyz_, quat xyzw */
+} MRModelBodyC;
+
+typedef struct MRModelDofC {
+    uint32_t joint_index;          /* MR_INVALID_INDEX for root coordinates   */
+    uint32_t q_index;              /* MR_INVALID_INDEX for root angular rates */
+    uint32_t flags;                /* MRDofFlags                              */
+    uint32_t reserved;
+    float limits[4];               /* lower, upper, max velocity, max effort  */
+    float drive[4];                /* stiffness, damping, armature, friction  */
+} MRModelDofC;
+
+typedef struct MRModelShapeC {
+    uint32_t body;
+    uint32_t shape_type;           /* MRShapeType                             */
+    uint32_t material;
+    uint32_t flags;
+    uint32_t collision_group;
+    uint32_t collision_mask;
+    uint32_t reserved[2];
+    float local_position[4];
+    float local_rotation[4];
+    float dimensions[4];           /* sphere r; capsule r, half length; box half extents */
+    float contact_rest_bound[4];   /* contact offset, rest offset, bounding radius */
+} MRModelShapeC;
+
+typedef struct MRModelMaterialC {
+    float friction[4];             /* static, dynamic, rolling, torsional     */
+    float response[4];             /* restitution, threshold, compliance, dissipation */
+} MRModelMaterialC;
+
+typedef struct MRModelPairC {
+    uint32_t shape_a;              /* shape_a < shape_b                       */
+    uint32_t shape_b;
+    uint32_t pair_class;           /* MRCollisionPairClass                    */
+    uint32_t max_points;           /* manifold points this pair can hold      */
+} MRModelPairC;
+
+/* Caller-owned destination for mr_task_rollout_copy_model.  Each pointer
+ * must hold the count reported in `world`; pass null to skip a table. */
+typedef struct MRModelViewC {
+    MRModelWorldC world;
+    MRModelJointC* joints;
+    MRModelBodyC* bodies;
+    MRModelDofC* dofs;
+    MRModelShapeC* shapes;
+    MRModelMaterialC* materials;
+    MRModelPairC* pairs;
+} MRModelViewC;
+
+/* Persistent contact state of one environment: one slot per compiled pair.
+ * Anchors are relative to each shape's body COM in body axes. */
+typedef struct MRManifoldPointC {
+    float anchor_a[3];
+    float anchor_b[3];
+    uint32_t feature_a;
+    uint32_t feature_b;
+    uint32_t life;
+    float impulses[3];             /* normal, tangent, bitangent              */
+} MRManifoldPointC;
+
+typedef struct MRManifoldC {
+    float normal_local[3];         /* in shape A's body frame                 */
+    float age;
+    float tangent_local[3];
+    uint32_t count;
+    MRManifoldPointC points[MR_B200_MANIFOLD_POINTS];
+} MRManifoldC;
+
+/* ---------------------------------------------------------------------- */
+/* Reference-shaped entry points                                           */
+/* ---------------------------------------------------------------------- */
+
+/* reference: include/metalrobo/c_api.h:553 */
+MR_API const char* mr_version(void);
+/* reference: include/metalrobo/c_api.h:556 */
+MR_API uint64_t mr_runtime_abi_fingerprint(void);
+/* reference: include/metalrobo/c_api.h:557 */
+MR_API const char* mr_last_error(void);
+
+/* reference: include/metalrobo/c_api.h:583-585 */
+MR_API MRTaskRolloutHandle* mr_create_task_rollout(const MRRunManifestC* manifest);
+/* reference: include/metalrobo/c_api.h:586 */
+MR_API void mr_task_rollout_destroy(MRTaskRolloutHandle* handle);
+/* reference: include/metalrobo/c_api.h:587-590.  Re-seeds and re-samples
+ * every environment's reset state, clears contact state and statistics. */
+MR_API int mr_task_rollout_reset(MRTaskRolloutHandle* handle, uint64_t seed);
+/* reference: include/metalrobo/c_api.h:631-634 */
+MR_API int mr_task_rollout_set_state_readback(MRTaskRolloutHandle* handle, uint32_t enabled);
+/* reference: include/metalrobo/c_api.h:635-645.  Host actions packed
+ * [step][env][action]; reset masks 0 or [step][env]; synchronous. */
+MR_API int mr_task_rollout_advance(
+    MRTaskRolloutHandle* handle,
+    const float* normalized_actions,
+    size_t normalized_action_count,
+    const uint32_t* reset_masks,
+    size_t reset_mask_count,
+    uint32_t control_step_count,
+    uint64_t policy_revision,
+    uint32_t evaluate_final_policy,
+    MRTaskRolloutAdvanceC* advance);
+/* reference: include/metalrobo/c_api.h:646-648 */
+MR_API MRTaskRolloutLayoutC mr_task_rollout_layout(const MRTaskRolloutHandle* handle);
+/* reference: include/metalrobo/c_api.h:658-660 */
+MR_API const char* mr_task_rollout_device_name(const MRTaskRolloutHandle* handle);
+/* reference: include/metalrobo/c_api.h:682-684.  [step][env] of the last advance. */
+MR_API const uint32_t* mr_task_rollout_status_codes(const MRTaskRolloutHandle* handle);
+/* reference: include/metalrobo/c_api.h:685-687.  [step][env] of the last advance. */
+MR_API const uint32_t* mr_task_rollout_active_contacts(const MRTaskRolloutHandle* handle);
+/* reference: include/metalrobo/c_api.h:688-690.  [step][env][nq + nv] of the
+ * last advance; null unless state readback is enabled. */
+MR_API const float* mr_task_rollout_actor_observations(const MRTaskRolloutHandle* handle);
+/* reference: include/metalrobo/c_api.h:736-738.  [env][nq]; null unless
+ * state readback is enabled. */
+MR_API const float* mr_task_rollout_final_q(const MRTaskRolloutHandle* handle);
+/* reference: include/metalrobo/c_api.h:742-746.  Packed [env][scene body]
+ * [position xyz, orientation xyzw, linear xyz, angular xyz]; scene bodies
+ * are the non-articulated dynamic bodies (none in the synthetic worlds). */
+MR_API int mr_task_rollout_copy_final_scene_states(
+    const MRTaskRolloutHandle* handle, float* output, size_t output_count);
+
+/* ---------------------------------------------------------------------- */
+/* Additions of this library                                               */
+/* ---------------------------------------------------------------------- */
+
+/* No counterpart in the reference: zero-copy advance for device buffers
+ * (e.g. torch CUDA tensors).  `device_actions` [step][env][action] and the
+ * optional `device_reset_masks` [step][env] live on the rollout's device;
+ * `device_observations` [step][env][nq+nv] and `device_status_codes`
+ * [step][env] may be null.  Work is ordered on `cuda_stream` (0 = the
+ * rollout's own stream).  With `advance` non-null the call waits and fills
+ * the same counters as mr_task_rollout_advance; with null it returns after
+ * enqueueing. */
+MR_API int mr_task_rollout_advance_device(
+    MRTaskRolloutHandle* handle,
+    const float* device_actions,
+    const uint32_t* device_reset_masks,
+    uint32_t control_step_count,
+    float* device_observations,
+    uint32_t* device_status_codes,
+    uint64_t cuda_stream,
+    MRTaskRolloutAdvanceC* advance);
+
+/* No counterpart in the reference: copies the compiled world records. */
+MR_API int mr_task_rollout_copy_model(const MRTaskRolloutHandle* handle, MRModelViewC* view);
+
+/* No counterpart in the reference: compiles a synthetic world on the host
+ * (no device work) and copies its records into `view` (null tables are
+ * skipped; `view->world` always receives the counts). */
+MR_API int mr_compile_synthetic_model(uint32_t source, uint64_t seed, MRModelViewC* view);
+
+/* No counterpart in the reference: samples the reset state the rollout
+ * would use for environments [env_begin, env_begin + env_count) (host only).
+ * q [env][nq], v [env][nv], friction_scale [env]. */
+MR_API int mr_sample_synthetic_reset(uint32_t source, uint64_t model_seed, uint64_t reset_seed,
+                                     uint32_t env_begin, uint32_t env_count, float* q, float* v,
+                                     float* friction_scale);
+
+/* No counterpart in the reference: per-environment contact friction scale
+ * [env] (the synthetic worlds draw one coefficient per environment). */
+MR_API int mr_task_rollout_copy_environment_parameters(
+    const MRTaskRolloutHandle* handle, float* friction_scale);
+
+/* No counterpart in the reference: copies the resident state of every
+ * environment, q [env][nq], v [env][nv] and manifolds [env][pair_count];
+ * any pointer may be null. */
+MR_API int mr_task_rollout_copy_state(
+    const MRTaskRolloutHandle* handle, float* q, float* v, MRManifoldC* manifolds);
+
+/* No counterpart in the reference: replaces the resident state (same
+ * layouts as mr_task_rollout_copy_state; null manifolds clears them).
+ * The new state also becomes every environment's reset state when
+ * `as_reset_state` is non-zero. */
+MR_API int mr_task_rollout_set_state(
+    MRTaskRolloutHandle* handle, const float* q, const float* v,
+    const MRManifoldC* manifolds, uint32_t as_reset_state);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NUMI_B200_H */

@@ -1,0 +1,12 @@
+"""numi_lab_b200: numi-lab's batched physics microstep on NVIDIA B200 (sm_100a).
+
+The CUDA library ``libnumi_b200.so`` (built in-tree by ``numi_lab_b200.build``)
+implements the task-rollout C ABI of ``include/numi_b200.h``; this package is
+the thin Python layer over it: ``native`` (ctypes binding) and ``world``
+(world / reset / step with zero-copy torch tensors).
+"""
+
+from .native import MetalRoboError, bindings
+from .world import World, compile_model, sample_reset
+
+__all__ = ["MetalRoboError", "World", "bindings", "compile_model", "sample_reset"]

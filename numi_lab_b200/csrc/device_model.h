@@ -1,0 +1,139 @@
+// Packed, immutable world description read by the microstep kernels.  One
+// record per rollout lives in device memory; every environment of the
+// rollout shares it (the model is small enough to stay L1/L2 resident).
+#pragma once
+
+#include <cstdint>
+
+#include "numi_b200.h"
+
+namespace numi {
+
+constexpr int kMaxBodies = MR_B200_MAX_BODIES;
+constexpr int kMaxDofs = MR_B200_MAX_DOFS;
+constexpr int kMaxQ = MR_B200_MAX_Q;
+constexpr int kMaxShapes = MR_B200_MAX_SHAPES;
+constexpr int kMaxPairs = MR_B200_MAX_PAIRS;
+constexpr int kMaxContacts = MR_B200_MAX_CONTACTS;
+constexpr int kManifoldPoints = MR_B200_MANIFOLD_POINTS;
+constexpr int kMaxMaterials = 8;
+// Words of one persistent manifold slot in device memory (MRManifoldC).
+constexpr int kManifoldWords = 8 + kManifoldPoints * 12;
+
+struct alignas(16) DeviceModel {
+    // World.
+    std::int32_t nb;              // articulated bodies, DFS preorder, body 0 = root
+    std::int32_t nv;
+    std::int32_t nq;
+    std::int32_t floating;        // 1 floating root, 0 fixed root
+    std::int32_t n_levels;        // tree depth (levels 1..n_levels)
+    std::int32_t action_count;
+    std::int32_t implicit_drives; // MR_ACTUATION_IMPLICIT_POSITION
+    std::int32_t apply_damping;
+    std::int32_t ns;              // shapes
+    std::int32_t np;              // compiled pairs
+    std::int32_t contact_capacity;
+    std::int32_t max_anc;         // stride of anc_dofs rows
+    float gravity[4];
+    float h;                      // physics substep
+    float slop;
+    float max_depenetration;
+    float speculative_scale;
+    float speed_envelope;
+    float manifold_thresholds[4]; // breaking separation, drift, merge, normal cosine
+    float reserved0[3];
+
+    // Tree.
+    std::int32_t level_offsets[kMaxBodies + 1];
+    std::int32_t level_bodies[kMaxBodies];
+    std::int32_t parent[kMaxBodies];
+    std::int32_t subtree_end[kMaxBodies];
+    std::int32_t body_dof[kMaxBodies];     // -1 fixed joint / root
+    std::int32_t joint_type[kMaxBodies];
+    std::int32_t child_offsets[kMaxBodies + 1];
+    std::int32_t children[kMaxBodies];
+    float4 axis[kMaxBodies];               // normalised joint-frame axis
+    float4 parent_anchor[kMaxBodies];
+    float4 child_anchor[kMaxBodies];
+    float4 parent_rotation[kMaxBodies];    // normalised
+    float4 child_rotation_conj[kMaxBodies];// conjugate of normalised child rotation
+    float4 mass_damping[kMaxBodies];       // mass, linear damping, angular damping, 0
+    float4 inertia_diag[kMaxBodies];       // body-frame Ixx, Iyy, Izz
+    float4 inertia_off[kMaxBodies];        // body-frame Ixy, Ixz, Iyz
+    std::int32_t anc_count[kMaxBodies];
+    std::int32_t anc_dofs[kMaxBodies * kMaxDofs];
+
+    // DoFs.
+    std::int32_t dof_body[kMaxDofs];
+    std::int32_t dof_parent[kMaxDofs];
+    std::int32_t dof_anc_count[kMaxDofs];  // ancestors of a DoF = first entries of anc_dofs[dof_body]
+    std::int32_t dof_q[kMaxDofs];          // -1 when no scalar coordinate
+    std::uint32_t dof_flags[kMaxDofs];
+    float armature_eff[kMaxDofs];          // armature (+ h kd + h^2 kp for implicit drives)
+    float kp[kMaxDofs];
+    float kd[kMaxDofs];
+    float dry_friction[kMaxDofs];
+    float effort_envelope[kMaxDofs];       // min(limit.w, default stall torque)
+    float effort_limit[kMaxDofs];          // limits.w when EFFORT_LIMIT
+    float q_lower[kMaxDofs];
+    float q_upper[kMaxDofs];
+    float v_max[kMaxDofs];
+    std::int32_t action_dof[kMaxDofs];     // action a drives DoF action_dof[a]
+
+    // Shapes.
+    std::int32_t shape_body[kMaxShapes];   // articulated body index, or -1 for static
+    std::int32_t shape_type[kMaxShapes];
+    std::int32_t shape_material[kMaxShapes];
+    std::int32_t reserved1;
+    float4 shape_position[kMaxShapes];     // local position (articulated) or world (static)
+    float4 shape_rotation[kMaxShapes];     // normalised local (articulated) or world (static)
+    float4 shape_dims[kMaxShapes];
+    float4 shape_offsets[kMaxShapes];      // contact offset, rest offset, sweep radius, 0
+    float4 static_body_position[kMaxShapes];  // pose of a static shape's body
+    float4 static_body_rotation[kMaxShapes];
+
+    // Pairs (shape_a < shape_b; shape_a is never static for supported classes).
+    std::int32_t pair_a[kMaxPairs];
+    std::int32_t pair_b[kMaxPairs];
+    std::int32_t pair_class[kMaxPairs];
+    std::int32_t pair_max_points[kMaxPairs];
+
+    float4 material_friction[kMaxMaterials];
+    float4 material_response[kMaxMaterials];
+};
+
+// Launch parameters of one control step of one rollout.
+struct StepParams {
+    const DeviceModel* model;
+    float* q;                      // [env][nq] resident state (in/out)
+    float* v;                      // [env][nv]
+    float* manifolds;              // [env][np][kManifoldWords]
+    const float* reset_q;          // [env][nq]
+    const float* reset_v;          // [env][nv]
+    const float* friction_scale;   // [env]
+    const float* actions;          // [env][action_count] of this control step
+    const std::uint32_t* reset_masks;  // [env] of this control step, or null
+    float* observations;           // [env][nq+nv] of this control step, or null
+    std::uint32_t* status_codes;   // [env] of this control step, or null
+    std::uint32_t* active_contacts;// [env] of this control step, or null
+    std::uint32_t* stats;          // per-launch counters (see kStat*)
+    std::int32_t env_count;
+    std::int32_t substeps;
+    std::int32_t velocity_iterations;
+    std::int32_t final_velocity_iterations;
+};
+
+enum StatIndex : int {
+    kStatFailedEnvs = 0,
+    kStatMaxContacts = 1,
+    kStatMaxManifolds = 2,
+    kStatMaxRawContacts = 3,
+    kStatMaxCandidatePairs = 4,
+    kStatMaxIslands = 5,
+    kStatFirstFailEnv = 6,
+    kStatFirstFailCode = 7,
+    kStatResets = 8,
+    kStatCount = 16
+};
+
+}  // namespace numi

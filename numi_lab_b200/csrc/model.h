@@ -1,0 +1,66 @@
+// Host-side compiled world: immutable records of one articulated world plus
+// the derived tables the device kernels need (tree levels, ancestor DoF
+// lists, eligible collider pairs).  One compiled model is shared by every
+// environment of a rollout, like one CompiledWorld per MetalWorldContext in
+// numi-lab (include/metalrobo/MetalWorld.hpp:107-217).
+#pragma once
+
+#include "numi_b200.h"
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace numi {
+
+// Counter-based seeded stream: value = f(seed, stream, index).  Independent
+// of call order, so every environment / field draws reproducibly.
+std::uint64_t mix64(std::uint64_t x);
+double uniform01(std::uint64_t seed, std::uint64_t stream, std::uint64_t index);
+double uniform(std::uint64_t seed, std::uint64_t stream, std::uint64_t index, double lo, double hi);
+double normal(std::uint64_t seed, std::uint64_t stream, std::uint64_t index);
+
+struct CompiledModel {
+    MRModelWorldC world{};
+    std::vector<MRModelJointC> joints;
+    std::vector<MRModelBodyC> bodies;
+    std::vector<MRModelDofC> dofs;
+    std::vector<MRModelShapeC> shapes;
+    std::vector<MRModelMaterialC> materials;
+    std::vector<MRModelPairC> pairs;
+    std::string name;
+
+    // Reset-state generation parameters.
+    std::vector<float> nominal_q;     // nq
+    float q_joint_uniform_half_range = 0.0f;  // q_j ~ nominal + U(-r, r)
+    float qd_joint_normal_sigma = 0.0f;       // qd_j ~ N(0, sigma)
+    float root_yaw_half_range = 0.0f;
+    float friction_scale_lo = 1.0f;   // per-env contact friction scale ~ U(lo, hi)
+    float friction_scale_hi = 1.0f;
+
+    // Derived (filled by finalize()).
+    std::uint32_t articulated_body_count = 0;  // bodies [0, n) form the tree, DFS preorder
+    std::uint32_t level_count = 0;
+    std::vector<std::uint32_t> level_offsets;  // level_count + 1
+    std::vector<std::uint32_t> level_bodies;   // bodies grouped by depth (depth >= 1)
+    std::vector<std::uint32_t> subtree_end;    // DFS: subtree of b is [b, subtree_end[b])
+    std::vector<std::uint32_t> body_dof;       // DoF index of a body's inbound joint or MR_INVALID_INDEX
+    std::vector<std::uint32_t> dof_body;       // body moved by DoF (root DoFs -> root body)
+    std::vector<std::uint32_t> dof_parent;     // nearest ancestor DoF (tree DoF order), MR_INVALID_INDEX at root
+    std::uint32_t max_ancestor_dofs = 0;       // longest ancestor-DoF list over bodies
+    std::vector<std::uint32_t> body_ancestor_dofs;  // [body][max_ancestor_dofs], ascending, padded MR_INVALID_INDEX
+    std::vector<std::uint32_t> body_ancestor_count;
+
+    std::uint64_t fingerprint = 0;
+
+    void finalize();  // validates and fills derived tables; throws on error
+};
+
+CompiledModel build_chain7(std::uint64_t seed);
+CompiledModel build_tree29(std::uint64_t seed);
+
+// Reset state for environment `env` (q: nq, v: nv) and its friction scale.
+void sample_reset_state(const CompiledModel& model, std::uint64_t seed, std::uint32_t env,
+                        float* q, float* v, float* friction_scale);
+
+}  // namespace numi

@@ -1,0 +1,781 @@
+// Host runtime behind the task-rollout C ABI (include/numi_b200.h).
+//
+// Mirrors numi-lab's mr_* rollout boundary (src/c_api.cpp:3370-3990):
+// validation with exceptions translated into a thread-local last-error
+// string, handle-owned results that alias until the next advance / reset /
+// destroy, synchronous host advance.  Underneath, a rollout owns its
+// compiled model, the device-resident state of every environment and a
+// cache of CUDA graphs, one per horizon length, each holding the horizon's
+// control-step launches (no contact-count readback inside a horizon).
+#include "device_model.h"
+#include "layout.h"
+#include "model.h"
+#include "numi_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace numi {
+cudaError_t launch_control_step(const StepParams& p, const WarpLayout& layout, bool contact, int warps_per_block,
+                                cudaStream_t stream);
+cudaError_t configure_control_step_kernels(size_t max_dynamic_smem);
+}  // namespace numi
+
+namespace {
+
+thread_local std::string g_last_error;
+
+void check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+struct DeviceBuffer {
+    T* ptr = nullptr;
+    size_t count = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    ~DeviceBuffer() { if (ptr) cudaFree(ptr); }
+    void resize(size_t n) {
+        if (n <= count && ptr) return;
+        if (ptr) { cudaFree(ptr); ptr = nullptr; }
+        check(cudaMalloc(&ptr, std::max<size_t>(n, 1) * sizeof(T)), "cudaMalloc");
+        count = n;
+    }
+};
+
+template <typename T>
+struct PinnedBuffer {
+    T* ptr = nullptr;
+    size_t count = 0;
+    PinnedBuffer() = default;
+    PinnedBuffer(const PinnedBuffer&) = delete;
+    PinnedBuffer& operator=(const PinnedBuffer&) = delete;
+    ~PinnedBuffer() { if (ptr) cudaFreeHost(ptr); }
+    void resize(size_t n) {
+        if (n <= count && ptr) return;
+        if (ptr) { cudaFreeHost(ptr); ptr = nullptr; }
+        check(cudaMallocHost(&ptr, std::max<size_t>(n, 1) * sizeof(T)), "cudaMallocHost");
+        count = n;
+    }
+};
+
+numi::DeviceModel pack_model(const numi::CompiledModel& m, float h) {
+    using namespace numi;
+    DeviceModel d{};
+    std::memset(&d, 0, sizeof(d));
+    const MRModelWorldC& w = m.world;
+    d.nb = static_cast<int>(m.articulated_body_count);
+    d.nv = static_cast<int>(w.nv);
+    d.nq = static_cast<int>(w.nq);
+    d.floating = w.root_type == MR_ROOT_FLOATING ? 1 : 0;
+    d.n_levels = static_cast<int>(m.level_count);
+    d.action_count = static_cast<int>(w.action_count);
+    d.implicit_drives = w.actuation_mode == MR_ACTUATION_IMPLICIT_POSITION ? 1 : 0;
+    d.apply_damping = w.apply_body_damping ? 1 : 0;
+    d.ns = static_cast<int>(w.shape_count);
+    d.np = static_cast<int>(w.pair_count);
+    d.contact_capacity = static_cast<int>(w.contact_capacity);
+    d.max_anc = static_cast<int>(m.max_ancestor_dofs);
+    for (int i = 0; i < 3; ++i) d.gravity[i] = w.gravity[i];
+    d.h = h;
+    d.slop = w.solver_scales[3];
+    d.max_depenetration = w.solver_scales[2];
+    d.speculative_scale = w.speculative[0];
+    d.speed_envelope = w.speculative[1];
+    for (int i = 0; i < 4; ++i) d.manifold_thresholds[i] = w.manifold_thresholds[i];
+    for (std::uint32_t l = 0; l <= m.level_count; ++l) d.level_offsets[l] = static_cast<int>(m.level_offsets[l]);
+    for (size_t i = 0; i < m.level_bodies.size(); ++i) d.level_bodies[i] = static_cast<int>(m.level_bodies[i]);
+    const int nb = d.nb;
+    // children lists in body order
+    std::vector<std::vector<int>> kids(nb);
+    for (int b = 1; b < nb; ++b) kids[m.bodies[b].parent_body].push_back(b);
+    int co = 0;
+    for (int b = 0; b < nb; ++b) {
+        d.child_offsets[b] = co;
+        for (int c : kids[b]) d.children[co++] = c;
+    }
+    d.child_offsets[nb] = co;
+    auto norm4 = [](const float* q) {
+        const double n = std::sqrt(double(q[0]) * q[0] + double(q[1]) * q[1] + double(q[2]) * q[2] + double(q[3]) * q[3]);
+        return make_float4(float(q[0] / n), float(q[1] / n), float(q[2] / n), float(q[3] / n));
+    };
+    for (int b = 0; b < nb; ++b) {
+        const MRModelBodyC& body = m.bodies[b];
+        d.parent[b] = b == 0 ? -1 : static_cast<int>(body.parent_body);
+        d.subtree_end[b] = static_cast<int>(m.subtree_end[b]);
+        d.body_dof[b] = m.body_dof[b] == MR_INVALID_INDEX ? -1 : static_cast<int>(m.body_dof[b]);
+        d.mass_damping[b] = make_float4(body.mass_inverse_mass[0], body.damping_speed[0], body.damping_speed[1], 0.0f);
+        d.inertia_diag[b] = make_float4(body.inertia[0][0], body.inertia[1][1], body.inertia[2][2], 0.0f);
+        d.inertia_off[b] = make_float4(body.inertia[0][1], body.inertia[0][2], body.inertia[1][2], 0.0f);
+        d.anc_count[b] = static_cast<int>(m.body_ancestor_count[b]);
+        for (std::uint32_t k = 0; k < m.max_ancestor_dofs; ++k)
+            d.anc_dofs[b * kMaxDofs + k] = static_cast<int>(m.body_ancestor_dofs[b * m.max_ancestor_dofs + k]);
+        if (b > 0) {
+            const MRModelJointC& j = m.joints[body.inbound_joint];
+            d.joint_type[b] = static_cast<int>(j.joint_type);
+            const double an = std::sqrt(double(j.axis[0]) * j.axis[0] + double(j.axis[1]) * j.axis[1] + double(j.axis[2]) * j.axis[2]);
+            d.axis[b] = make_float4(float(j.axis[0] / an), float(j.axis[1] / an), float(j.axis[2] / an), 0.0f);
+            d.parent_anchor[b] = make_float4(j.parent_anchor[0], j.parent_anchor[1], j.parent_anchor[2], 0.0f);
+            d.child_anchor[b] = make_float4(j.child_anchor[0], j.child_anchor[1], j.child_anchor[2], 0.0f);
+            d.parent_rotation[b] = norm4(j.parent_rotation);
+            const float4 cr = norm4(j.child_rotation);
+            d.child_rotation_conj[b] = make_float4(-cr.x, -cr.y, -cr.z, cr.w);
+        } else {
+            d.joint_type[b] = MR_JOINT_FIXED;
+            d.parent_rotation[b] = make_float4(0, 0, 0, 1);
+            d.child_rotation_conj[b] = make_float4(0, 0, 0, 1);
+        }
+    }
+    for (std::uint32_t k = 0; k < w.nv; ++k) {
+        const MRModelDofC& dof = m.dofs[k];
+        d.dof_body[k] = static_cast<int>(m.dof_body[k]);
+        d.dof_parent[k] = m.dof_parent[k] == MR_INVALID_INDEX ? -1 : static_cast<int>(m.dof_parent[k]);
+        // position of k in its body's ancestor list = number of ancestors
+        const std::uint32_t b = m.dof_body[k];
+        int count = 0;
+        for (std::uint32_t t = 0; t < m.body_ancestor_count[b]; ++t) {
+            if (m.body_ancestor_dofs[b * m.max_ancestor_dofs + t] == k) { count = static_cast<int>(t); break; }
+        }
+        d.dof_anc_count[k] = count;
+        d.dof_q[k] = dof.q_index == MR_INVALID_INDEX ? -1 : static_cast<int>(dof.q_index);
+        d.dof_flags[k] = dof.flags;
+        float arm = dof.drive[2];
+        if (d.implicit_drives && (dof.flags & MR_DOF_FLAG_DRIVE)) arm += h * dof.drive[1] + h * h * dof.drive[0];
+        d.armature_eff[k] = arm;
+        d.kp[k] = dof.drive[0];
+        d.kd[k] = dof.drive[1];
+        d.dry_friction[k] = dof.drive[3];
+        const float stall = ((dof.flags & MR_DOF_FLAG_EFFORT_LIMIT) && dof.limits[3] > 0.0f)
+                                ? dof.limits[3] : std::numeric_limits<float>::max();
+        d.effort_envelope[k] = std::min(dof.limits[3], stall);
+        d.effort_limit[k] = dof.limits[3];
+        d.q_lower[k] = dof.limits[0];
+        d.q_upper[k] = dof.limits[1];
+        d.v_max[k] = dof.limits[2];
+    }
+    // Actions drive the actuated DoFs in v order.
+    int a = 0;
+    for (std::uint32_t k = 0; k < w.nv && a < d.action_count; ++k)
+        if (m.dofs[k].flags & MR_DOF_FLAG_ACTUATED) d.action_dof[a++] = static_cast<int>(k);
+    if (a != d.action_count) throw std::runtime_error("action count does not match actuated DoFs");
+    for (std::uint32_t s = 0; s < w.shape_count; ++s) {
+        const MRModelShapeC& sh = m.shapes[s];
+        const MRModelBodyC& body = m.bodies[sh.body];
+        d.shape_type[s] = static_cast<int>(sh.shape_type);
+        d.shape_material[s] = static_cast<int>(sh.material);
+        d.shape_dims[s] = make_float4(sh.dimensions[0], sh.dimensions[1], sh.dimensions[2], 0.0f);
+        float sweep = sh.contact_rest_bound[2];
+        if (!(sweep > 0.0f) || !std::isfinite(sweep)) {
+            if (sh.shape_type == MR_SHAPE_SPHERE) sweep = sh.dimensions[0];
+            else if (sh.shape_type == MR_SHAPE_CAPSULE) sweep = sh.dimensions[0] + sh.dimensions[1];
+            else sweep = std::sqrt(sh.dimensions[0] * sh.dimensions[0] + sh.dimensions[1] * sh.dimensions[1] + sh.dimensions[2] * sh.dimensions[2]);
+        }
+        d.shape_offsets[s] = make_float4(sh.contact_rest_bound[0], sh.contact_rest_bound[1], sweep, 0.0f);
+        const float4 lr = norm4(sh.local_rotation);
+        if (body.articulated) {
+            d.shape_body[s] = static_cast<int>(sh.body);
+            d.shape_position[s] = make_float4(sh.local_position[0], sh.local_position[1], sh.local_position[2], 0.0f);
+            d.shape_rotation[s] = lr;
+        } else {
+            // World pose of a static shape (reference: body pose composed with local pose).
+            d.shape_body[s] = -1;
+            const float4 br = norm4(body.static_pose + 4);
+            const double bx = br.x, by = br.y, bz = br.z, bw = br.w;
+            const double lx = sh.local_position[0], ly = sh.local_position[1], lz = sh.local_position[2];
+            // rotate local position by body rotation
+            const double tx = 2 * (by * lz - bz * ly), ty = 2 * (bz * lx - bx * lz), tz = 2 * (bx * ly - by * lx);
+            const double rx = lx + bw * tx + (by * tz - bz * ty);
+            const double ry = ly + bw * ty + (bz * tx - bx * tz);
+            const double rz = lz + bw * tz + (bx * ty - by * tx);
+            d.shape_position[s] = make_float4(float(body.static_pose[0] + rx), float(body.static_pose[1] + ry),
+                                              float(body.static_pose[2] + rz), 0.0f);
+            const float4 q = make_float4(
+                float(bw * lr.x + bx * lr.w + by * lr.z - bz * lr.y), float(bw * lr.y - bx * lr.z + by * lr.w + bz * lr.x),
+                float(bw * lr.z + bx * lr.y - by * lr.x + bz * lr.w), float(bw * lr.w - bx * lr.x - by * lr.y - bz * lr.z));
+            d.shape_rotation[s] = q;
+            d.static_body_position[s] = make_float4(body.static_pose[0], body.static_pose[1], body.static_pose[2], 0.0f);
+            d.static_body_rotation[s] = br;
+        }
+    }
+    for (std::uint32_t p = 0; p < w.pair_count; ++p) {
+        const MRModelPairC& pr = m.pairs[p];
+        const bool a_art = m.bodies[m.shapes[pr.shape_a].body].articulated != 0;
+        const bool b_art = m.bodies[m.shapes[pr.shape_b].body].articulated != 0;
+        if (a_art == b_art) throw std::runtime_error("pairs must join one articulated and one static collider");
+        if (pr.pair_class != MR_COLLISION_PAIR_SPHERE_PLANE && pr.pair_class != MR_COLLISION_PAIR_BOX_PLANE &&
+            pr.pair_class != MR_COLLISION_PAIR_CAPSULE_PLANE)
+            throw std::runtime_error("unsupported collision pair class");
+        d.pair_a[p] = static_cast<int>(pr.shape_a);
+        d.pair_b[p] = static_cast<int>(pr.shape_b);
+        d.pair_class[p] = static_cast<int>(pr.pair_class);
+        d.pair_max_points[p] = static_cast<int>(pr.max_points);
+    }
+    if (w.material_count > kMaxMaterials) throw std::runtime_error("too many materials");
+    for (std::uint32_t i = 0; i < w.material_count; ++i) {
+        const MRModelMaterialC& mt = m.materials[i];
+        d.material_friction[i] = make_float4(mt.friction[0], mt.friction[1], mt.friction[2], mt.friction[3]);
+        d.material_response[i] = make_float4(mt.response[0], mt.response[1], mt.response[2], mt.response[3]);
+    }
+    return d;
+}
+
+}  // namespace
+
+struct MRTaskRolloutHandle {
+    numi::CompiledModel model;
+    numi::DeviceModel dmodel{};
+    numi::WarpLayout layout{};
+    bool contact = false;
+    int warps_per_block = 1;
+    MRTaskRolloutConfigC config{};
+    std::uint32_t envs = 0;
+    float h = 0.0f;
+    std::uint64_t seed = 0;
+    bool readback = false;
+    int device = 0;
+    std::string device_name;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+
+    DeviceBuffer<numi::DeviceModel> d_model;
+    DeviceBuffer<float> d_q, d_v, d_manifolds, d_reset_q, d_reset_v, d_friction;
+    DeviceBuffer<float> d_actions, d_obs;
+    DeviceBuffer<std::uint32_t> d_masks, d_status, d_contacts, d_stats;
+    PinnedBuffer<float> h_actions, h_obs, h_final_q;
+    PinnedBuffer<std::uint32_t> h_masks, h_status, h_contacts, h_stats;
+    std::vector<float> reset_q, reset_v, friction;
+
+    // graph cache keyed by (steps, has masks, obs/status targets)
+    struct GraphKey {
+        std::uint32_t steps;
+        const void* actions;
+        const void* masks;
+        const void* obs;
+        const void* status;
+        const void* contacts;
+        bool operator<(const GraphKey& o) const {
+            return std::tie(steps, actions, masks, obs, status, contacts) <
+                   std::tie(o.steps, o.actions, o.masks, o.obs, o.status, o.contacts);
+        }
+    };
+    std::map<GraphKey, cudaGraphExec_t> graphs;
+
+    // Last-advance publication.
+    std::uint32_t last_steps = 0;
+    bool have_final_q = false;
+    MRTaskRolloutLayoutC stats_layout{};
+
+    ~MRTaskRolloutHandle() {
+        for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+        if (ev_start) cudaEventDestroy(ev_start);
+        if (ev_stop) cudaEventDestroy(ev_stop);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    void sample_resets() {
+        const std::uint32_t nq = model.world.nq, nv = model.world.nv;
+        reset_q.assign(static_cast<size_t>(envs) * nq, 0.0f);
+        reset_v.assign(static_cast<size_t>(envs) * nv, 0.0f);
+        friction.assign(envs, 1.0f);
+        for (std::uint32_t e = 0; e < envs; ++e)
+            numi::sample_reset_state(model, seed, e, &reset_q[static_cast<size_t>(e) * nq], &reset_v[static_cast<size_t>(e) * nv], &friction[e]);
+        check(cudaMemcpyAsync(d_reset_q.ptr, reset_q.data(), reset_q.size() * sizeof(float), cudaMemcpyHostToDevice, stream), "upload reset q");
+        check(cudaMemcpyAsync(d_reset_v.ptr, reset_v.data(), reset_v.size() * sizeof(float), cudaMemcpyHostToDevice, stream), "upload reset v");
+        check(cudaMemcpyAsync(d_friction.ptr, friction.data(), friction.size() * sizeof(float), cudaMemcpyHostToDevice, stream), "upload friction");
+        check(cudaMemcpyAsync(d_q.ptr, d_reset_q.ptr, reset_q.size() * sizeof(float), cudaMemcpyDeviceToDevice, stream), "init q");
+        check(cudaMemcpyAsync(d_v.ptr, d_reset_v.ptr, reset_v.size() * sizeof(float), cudaMemcpyDeviceToDevice, stream), "init v");
+        if (d_manifolds.count) check(cudaMemsetAsync(d_manifolds.ptr, 0, d_manifolds.count * sizeof(float), stream), "clear manifolds");
+        check(cudaStreamSynchronize(stream), "reset");
+    }
+
+    size_t manifold_words() const { return static_cast<size_t>(model.world.pair_count) * numi::kManifoldWords; }
+
+    // Enqueue `steps` control steps reading actions/masks from device memory.
+    void enqueue(std::uint32_t steps, const float* actions, const std::uint32_t* masks, float* obs,
+                 std::uint32_t* status, std::uint32_t* contacts, cudaStream_t s) {
+        const std::uint32_t na = model.world.action_count;
+        const std::uint32_t nobs = model.world.nq + model.world.nv;
+        check(cudaMemsetAsync(d_stats.ptr, 0, numi::kStatCount * sizeof(std::uint32_t), s), "clear stats");
+        check(cudaMemsetAsync(d_stats.ptr + numi::kStatFirstFailEnv, 0xff, sizeof(std::uint32_t), s), "clear stats");
+        for (std::uint32_t k = 0; k < steps; ++k) {
+            numi::StepParams p{};
+            p.model = d_model.ptr;
+            p.q = d_q.ptr;
+            p.v = d_v.ptr;
+            p.manifolds = d_manifolds.ptr;
+            p.reset_q = d_reset_q.ptr;
+            p.reset_v = d_reset_v.ptr;
+            p.friction_scale = d_friction.ptr;
+            p.actions = actions + static_cast<size_t>(k) * envs * na;
+            p.reset_masks = masks ? masks + static_cast<size_t>(k) * envs : nullptr;
+            p.observations = obs ? obs + static_cast<size_t>(k) * envs * nobs : nullptr;
+            p.status_codes = status ? status + static_cast<size_t>(k) * envs : nullptr;
+            p.active_contacts = contacts ? contacts + static_cast<size_t>(k) * envs : nullptr;
+            p.stats = d_stats.ptr;
+            p.env_count = static_cast<int>(envs);
+            p.substeps = static_cast<int>(config.physics_substeps);
+            p.velocity_iterations = static_cast<int>(config.velocity_iterations);
+            p.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
+            check(numi::launch_control_step(p, layout, contact, warps_per_block, s), "control step launch");
+        }
+    }
+
+    void run(std::uint32_t steps, const float* actions, const std::uint32_t* masks, float* obs, std::uint32_t* status,
+             std::uint32_t* contacts, cudaStream_t s) {
+        const GraphKey key{steps, actions, masks, obs, status, contacts};
+        auto it = graphs.find(key);
+        if (it == graphs.end()) {
+            cudaGraph_t graph = nullptr;
+            check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+            try {
+                enqueue(steps, actions, masks, obs, status, contacts, s);
+            } catch (...) {
+                cudaStreamEndCapture(s, &graph);
+                if (graph) cudaGraphDestroy(graph);
+                throw;
+            }
+            check(cudaStreamEndCapture(s, &graph), "end capture");
+            cudaGraphExec_t exec = nullptr;
+            const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            check(e, "graph instantiate");
+            if (graphs.size() > 64) {
+                for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+                graphs.clear();
+            }
+            it = graphs.emplace(key, exec).first;
+        }
+        check(cudaGraphLaunch(it->second, s), "graph launch");
+    }
+
+    void fill_advance(std::uint32_t steps, const std::uint32_t* host_status, const std::uint32_t* host_stats,
+                      MRTaskRolloutAdvanceC* out, double gpu_ms, double wall_ms) {
+        MRTaskRolloutAdvanceC a{};
+        a.control_step_count = steps;
+        a.first_failing_environment = MR_INVALID_INDEX;
+        a.first_failing_control_step = MR_INVALID_INDEX;
+        a.first_gpu_status_code = MR_STEP_SUCCESS;
+        std::uint64_t failed = 0;
+        if (host_status) {
+            for (std::uint32_t k = 0; k < steps; ++k)
+                for (std::uint32_t e = 0; e < envs; ++e) {
+                    const std::uint32_t c = host_status[static_cast<size_t>(k) * envs + e];
+                    if (c != MR_STEP_SUCCESS) {
+                        ++failed;
+                        if (a.first_failing_environment == MR_INVALID_INDEX) {
+                            a.first_failing_environment = e;
+                            a.first_failing_control_step = k;
+                            a.first_gpu_status_code = c;
+                        }
+                    }
+                }
+        } else {
+            failed = host_stats[numi::kStatFailedEnvs];
+        }
+        a.failed_environment_steps = static_cast<std::uint32_t>(failed);
+        a.successful_environment_steps = static_cast<std::uint32_t>(static_cast<std::uint64_t>(steps) * envs - failed);
+        a.host_requested_resets = host_stats[numi::kStatResets];
+        a.maximum_active_contacts = host_stats[numi::kStatMaxContacts];
+        a.maximum_manifolds = host_stats[numi::kStatMaxManifolds];
+        a.high_water.candidate_pairs = host_stats[numi::kStatMaxCandidatePairs];
+        a.high_water.raw_contacts = host_stats[numi::kStatMaxRawContacts];
+        a.high_water.manifolds = host_stats[numi::kStatMaxManifolds];
+        a.high_water.constraint_blocks = host_stats[numi::kStatMaxContacts];
+        a.high_water.constraint_rows = 3u * host_stats[numi::kStatMaxContacts];
+        a.high_water.islands = host_stats[numi::kStatMaxIslands];
+        a.high_water.articulation_point_queries = 2u * host_stats[numi::kStatMaxContacts];
+        a.high_water.dynamic_nodes = 1u;
+        a.high_water.operator_velocity_elements = model.world.nv;
+        a.gpu_milliseconds = gpu_ms;
+        a.submission_milliseconds = wall_ms;
+        stats_layout.submitted_control_steps += steps;
+        stats_layout.completed_environment_steps += a.successful_environment_steps;
+        stats_layout.submission_count += 1;
+        stats_layout.total_gpu_milliseconds += gpu_ms;
+        stats_layout.total_submission_milliseconds += wall_ms;
+        if (out) *out = a;
+    }
+};
+
+namespace {
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        f();
+        return 0;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+    } catch (...) {
+        g_last_error = "unknown native error";
+    }
+    return -1;
+}
+
+}  // namespace
+
+extern "C" {
+
+MR_API const char* mr_version(void) { return "numi-b200 0.1.0 (sm_100a)"; }
+
+MR_API uint64_t mr_runtime_abi_fingerprint(void) {
+    std::uint64_t h = 0xcbf29ce484222325ull;
+    const std::size_t sizes[] = {sizeof(MRTaskRolloutConfigC), sizeof(MRRunManifestC), sizeof(MRTaskRolloutLayoutC),
+                                 sizeof(MRTaskRolloutStageHighWaterC), sizeof(MRTaskRolloutAdvanceC), sizeof(MRModelWorldC),
+                                 sizeof(MRModelJointC), sizeof(MRModelBodyC), sizeof(MRModelDofC), sizeof(MRModelShapeC),
+                                 sizeof(MRModelMaterialC), sizeof(MRModelPairC), sizeof(MRManifoldC)};
+    for (std::size_t s : sizes) h = (h ^ s) * 0x100000001b3ull;
+    return h;
+}
+
+MR_API const char* mr_last_error(void) { return g_last_error.c_str(); }
+
+MR_API MRTaskRolloutHandle* mr_create_task_rollout(const MRRunManifestC* manifest) {
+    std::unique_ptr<MRTaskRolloutHandle> handle;
+    const int rc = guarded([&] {
+        if (manifest == nullptr) throw std::invalid_argument("manifest is null");
+        const MRTaskRolloutConfigC& cfg = manifest->profile;
+        if (cfg.environment_count == 0) throw std::invalid_argument("environment_count must be positive");
+        if (cfg.physics_substeps == 0 || cfg.physics_substeps > MR_B200_MAX_SUBSTEPS)
+            throw std::invalid_argument("physics_substeps must be in [1, 64]");
+        if (!(cfg.control_timestep_seconds > 0.0f) || !std::isfinite(cfg.control_timestep_seconds))
+            throw std::invalid_argument("control_timestep_seconds must be positive and finite");
+        if (cfg.dynamic_sphere_count != 0 || cfg.dynamic_spheres != nullptr)
+            throw std::invalid_argument("dynamic spheres are not supported by the synthetic worlds");
+        if (manifest->visual_sensor_program != nullptr || manifest->inspection_visual_program != nullptr)
+            throw std::invalid_argument("visual programs are not part of the physics path");
+        handle = std::make_unique<MRTaskRolloutHandle>();
+        MRTaskRolloutHandle& h = *handle;
+        switch (manifest->source) {
+            case MR_RUN_SOURCE_SYNTHETIC_CHAIN7: h.model = numi::build_chain7(cfg.seed); break;
+            case MR_RUN_SOURCE_SYNTHETIC_TREE29: h.model = numi::build_tree29(cfg.seed); break;
+            default:
+                throw std::invalid_argument("unsupported run source " + std::to_string(manifest->source) +
+                                            " (robot assets, URDF and world packs are not compiled by this library; "
+                                            "use MR_RUN_SOURCE_SYNTHETIC_CHAIN7 or MR_RUN_SOURCE_SYNTHETIC_TREE29)");
+        }
+        if (h.model.world.pair_count > 0 && cfg.velocity_iterations == 0 && cfg.final_velocity_iterations == 0)
+            throw std::invalid_argument("contact worlds need at least one velocity iteration");
+        h.config = cfg;
+        h.envs = cfg.environment_count;
+        h.seed = cfg.seed;
+        h.h = cfg.control_timestep_seconds / static_cast<float>(cfg.physics_substeps);
+        h.contact = h.model.world.pair_count > 0;
+        h.dmodel = pack_model(h.model, h.h);
+        const numi::CompiledModel& m = h.model;
+        h.layout = numi::make_layout(static_cast<int>(m.articulated_body_count), static_cast<int>(m.world.nv),
+                                     static_cast<int>(m.world.nq), static_cast<int>(m.world.pair_count),
+                                     static_cast<int>(m.world.contact_capacity), static_cast<int>(m.max_ancestor_dofs), h.contact);
+        check(cudaGetDevice(&h.device), "cudaGetDevice");
+        cudaDeviceProp prop{};
+        check(cudaGetDeviceProperties(&prop, h.device), "cudaGetDeviceProperties");
+        h.device_name = prop.name;
+        const size_t per_warp = static_cast<size_t>(h.layout.total) * sizeof(float);
+        const size_t limit = prop.sharedMemPerBlockOptin;
+        if (per_warp > limit) throw std::runtime_error("per-environment shared memory exceeds the device limit");
+        h.warps_per_block = static_cast<int>(std::min<size_t>(4, std::max<size_t>(1, limit / per_warp)));
+        if (h.contact) h.warps_per_block = 1;
+        check(numi::configure_control_step_kernels(limit), "kernel attributes");
+        check(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking), "stream");
+        check(cudaEventCreate(&h.ev_start), "event");
+        check(cudaEventCreate(&h.ev_stop), "event");
+        h.d_model.resize(1);
+        check(cudaMemcpy(h.d_model.ptr, &h.dmodel, sizeof(numi::DeviceModel), cudaMemcpyHostToDevice), "upload model");
+        const size_t nq = m.world.nq, nv = m.world.nv;
+        h.d_q.resize(h.envs * nq);
+        h.d_v.resize(h.envs * nv);
+        h.d_reset_q.resize(h.envs * nq);
+        h.d_reset_v.resize(h.envs * nv);
+        h.d_friction.resize(h.envs);
+        if (h.contact) h.d_manifolds.resize(h.envs * h.manifold_words());
+        h.d_stats.resize(numi::kStatCount);
+        h.h_stats.resize(numi::kStatCount);
+        h.sample_resets();
+        h.stats_layout.environment_count = h.envs;
+        h.stats_layout.nq = m.world.nq;
+        h.stats_layout.nv = m.world.nv;
+        h.stats_layout.action_count = m.world.action_count;
+        h.stats_layout.actor_observation_count = m.world.nq + m.world.nv;
+        h.stats_layout.critic_observation_count = m.world.nq + m.world.nv;
+        h.stats_layout.scene_body_count = 0;
+        h.stats_layout.world_fingerprint = m.fingerprint;
+        h.stats_layout.run_fingerprint = m.fingerprint ^ (cfg.seed * 0x9e3779b97f4a7c15ull);
+        h.stats_layout.robot_fingerprint = m.fingerprint;
+        h.stats_layout.immutable_private_bytes = sizeof(numi::DeviceModel);
+        h.stats_layout.persistent_state_private_bytes =
+            (h.d_q.count + h.d_v.count + h.d_manifolds.count + h.d_reset_q.count + h.d_reset_v.count + h.d_friction.count) * sizeof(float);
+    });
+    if (rc != 0) return nullptr;
+    return handle.release();
+}
+
+MR_API void mr_task_rollout_destroy(MRTaskRolloutHandle* handle) {
+    if (handle) {
+        if (handle->stream) cudaStreamSynchronize(handle->stream);
+        delete handle;
+    }
+}
+
+MR_API int mr_task_rollout_reset(MRTaskRolloutHandle* handle, uint64_t seed) {
+    return guarded([&] {
+        if (!handle) throw std::invalid_argument("handle is null");
+        handle->seed = seed;
+        handle->sample_resets();
+        handle->last_steps = 0;
+        handle->have_final_q = false;
+    });
+}
+
+MR_API int mr_task_rollout_set_state_readback(MRTaskRolloutHandle* handle, uint32_t enabled) {
+    return guarded([&] {
+        if (!handle) throw std::invalid_argument("handle is null");
+        handle->readback = enabled != 0;
+        if (!handle->readback) handle->have_final_q = false;
+    });
+}
+
+MR_API int mr_task_rollout_advance(MRTaskRolloutHandle* handle, const float* normalized_actions, size_t normalized_action_count,
+                                   const uint32_t* reset_masks, size_t reset_mask_count, uint32_t control_step_count,
+                                   uint64_t policy_revision, uint32_t evaluate_final_policy, MRTaskRolloutAdvanceC* advance) {
+    return guarded([&] {
+        if (!handle) throw std::invalid_argument("handle is null");
+        if (!advance) throw std::invalid_argument("advance output is null");
+        if (policy_revision != 0 || evaluate_final_policy != 0)
+            throw std::invalid_argument("native policies are not installed on this rollout");
+        MRTaskRolloutHandle& h = *handle;
+        if (control_step_count == 0) throw std::invalid_argument("control_step_count must be positive");
+        const size_t na = h.model.world.action_count;
+        const size_t expected = static_cast<size_t>(control_step_count) * h.envs * na;
+        if (normalized_action_count != expected || (expected > 0 && normalized_actions == nullptr))
+            throw std::invalid_argument("normalized_action_count must equal control_step_count * environment_count * action_count (" +
+                                        std::to_string(expected) + ")");
+        const size_t mask_expected = static_cast<size_t>(control_step_count) * h.envs;
+        if (reset_mask_count != 0 && (reset_mask_count != mask_expected || reset_masks == nullptr))
+            throw std::invalid_argument("reset_mask_count must be 0 or control_step_count * environment_count");
+        const auto wall0 = std::chrono::steady_clock::now();
+        // Caller spans are copied before return (into pinned staging).
+        h.h_actions.resize(expected);
+        std::memcpy(h.h_actions.ptr, normalized_actions, expected * sizeof(float));
+        h.d_actions.resize(expected);
+        const bool masks = reset_mask_count != 0;
+        if (masks) {
+            h.h_masks.resize(mask_expected);
+            std::memcpy(h.h_masks.ptr, reset_masks, mask_expected * sizeof(uint32_t));
+            h.d_masks.resize(mask_expected);
+        }
+        const size_t nobs = h.model.world.nq + h.model.world.nv;
+        h.d_status.resize(mask_expected);
+        h.d_contacts.resize(mask_expected);
+        h.h_status.resize(mask_expected);
+        h.h_contacts.resize(mask_expected);
+        if (h.readback) {
+            h.d_obs.resize(mask_expected * nobs);
+            h.h_obs.resize(mask_expected * nobs);
+            h.h_final_q.resize(static_cast<size_t>(h.envs) * h.model.world.nq);
+        }
+        cudaStream_t s = h.stream;
+        check(cudaEventRecord(h.ev_start, s), "event");
+        check(cudaMemcpyAsync(h.d_actions.ptr, h.h_actions.ptr, expected * sizeof(float), cudaMemcpyHostToDevice, s), "actions H2D");
+        if (masks) check(cudaMemcpyAsync(h.d_masks.ptr, h.h_masks.ptr, mask_expected * sizeof(uint32_t), cudaMemcpyHostToDevice, s), "masks H2D");
+        h.run(control_step_count, h.d_actions.ptr, masks ? h.d_masks.ptr : nullptr, h.readback ? h.d_obs.ptr : nullptr,
+              h.d_status.ptr, h.d_contacts.ptr, s);
+        check(cudaMemcpyAsync(h.h_status.ptr, h.d_status.ptr, mask_expected * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "status D2H");
+        check(cudaMemcpyAsync(h.h_contacts.ptr, h.d_contacts.ptr, mask_expected * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "contacts D2H");
+        check(cudaMemcpyAsync(h.h_stats.ptr, h.d_stats.ptr, numi::kStatCount * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "stats D2H");
+        if (h.readback) {
+            check(cudaMemcpyAsync(h.h_obs.ptr, h.d_obs.ptr, mask_expected * nobs * sizeof(float), cudaMemcpyDeviceToHost, s), "obs D2H");
+            check(cudaMemcpyAsync(h.h_final_q.ptr, h.d_q.ptr, static_cast<size_t>(h.envs) * h.model.world.nq * sizeof(float),
+                                  cudaMemcpyDeviceToHost, s), "final q D2H");
+        }
+        check(cudaEventRecord(h.ev_stop, s), "event");
+        check(cudaStreamSynchronize(s), "advance");
+        float gpu_ms = 0.0f;
+        check(cudaEventElapsedTime(&gpu_ms, h.ev_start, h.ev_stop), "elapsed");
+        const double wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count();
+        h.last_steps = control_step_count;
+        h.have_final_q = h.readback;
+        h.fill_advance(control_step_count, h.h_status.ptr, h.h_stats.ptr, advance, gpu_ms, wall_ms);
+        // The reference reports failed environments in the counters and also
+        // as an error return (src/c_api.cpp:3983-3988).
+        if (advance->failed_environment_steps != 0)
+            throw std::runtime_error("environment " + std::to_string(advance->first_failing_environment) + " failed at control step " +
+                                     std::to_string(advance->first_failing_control_step) + " with status " +
+                                     std::to_string(advance->first_gpu_status_code));
+    });
+}
+
+MR_API int mr_task_rollout_advance_device(MRTaskRolloutHandle* handle, const float* device_actions, const uint32_t* device_reset_masks,
+                                          uint32_t control_step_count, float* device_observations, uint32_t* device_status_codes,
+                                          uint64_t cuda_stream, MRTaskRolloutAdvanceC* advance) {
+    return guarded([&] {
+        if (!handle) throw std::invalid_argument("handle is null");
+        if (!device_actions) throw std::invalid_argument("device_actions is null");
+        if (control_step_count == 0) throw std::invalid_argument("control_step_count must be positive");
+        MRTaskRolloutHandle& h = *handle;
+        cudaStream_t s = cuda_stream ? reinterpret_cast<cudaStream_t>(cuda_stream) : h.stream;
+        const size_t cells = static_cast<size_t>(control_step_count) * h.envs;
+        std::uint32_t* status = device_status_codes;
+        if (!status) {
+            h.d_status.resize(cells);
+            status = h.d_status.ptr;
+        }
+        h.d_contacts.resize(cells);
+        const auto wall0 = std::chrono::steady_clock::now();
+        if (advance) check(cudaEventRecord(h.ev_start, s), "event");
+        h.run(control_step_count, device_actions, device_reset_masks, device_observations, status, h.d_contacts.ptr, s);
+        if (advance) {
+            check(cudaMemcpyAsync(h.h_stats.ptr, h.d_stats.ptr, numi::kStatCount * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "stats D2H");
+            check(cudaEventRecord(h.ev_stop, s), "event");
+            check(cudaStreamSynchronize(s), "advance");
+            float gpu_ms = 0.0f;
+            check(cudaEventElapsedTime(&gpu_ms, h.ev_start, h.ev_stop), "elapsed");
+            const double wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count();
+            h.fill_advance(control_step_count, nullptr, h.h_stats.ptr, advance, gpu_ms, wall_ms);
+        }
+        h.have_final_q = false;
+        h.last_steps = 0;
+    });
+}
+
+MR_API MRTaskRolloutLayoutC mr_task_rollout_layout(const MRTaskRolloutHandle* handle) {
+    if (!handle) {
+        g_last_error = "handle is null";
+        return MRTaskRolloutLayoutC{};
+    }
+    return handle->stats_layout;
+}
+
+MR_API const char* mr_task_rollout_device_name(const MRTaskRolloutHandle* handle) {
+    return handle ? handle->device_name.c_str() : nullptr;
+}
+
+MR_API const uint32_t* mr_task_rollout_status_codes(const MRTaskRolloutHandle* handle) {
+    return handle && handle->last_steps ? handle->h_status.ptr : nullptr;
+}
+
+MR_API const uint32_t* mr_task_rollout_active_contacts(const MRTaskRolloutHandle* handle) {
+    return handle && handle->last_steps ? handle->h_contacts.ptr : nullptr;
+}
+
+MR_API const float* mr_task_rollout_actor_observations(const MRTaskRolloutHandle* handle) {
+    return handle && handle->have_final_q ? handle->h_obs.ptr : nullptr;
+}
+
+MR_API const float* mr_task_rollout_final_q(const MRTaskRolloutHandle* handle) {
+    return handle && handle->have_final_q ? handle->h_final_q.ptr : nullptr;
+}
+
+MR_API int mr_task_rollout_copy_final_scene_states(const MRTaskRolloutHandle* handle, float* output, size_t output_count) {
+    return guarded([&] {
+        if (!handle) throw std::invalid_argument("handle is null");
+        if (output_count != 0 && output == nullptr) throw std::invalid_argument("output is null");
+        if (output_count != 0) throw std::invalid_argument("this world has no scene bodies; output_count must be 0");
+    });
+}
+
+MR_API int mr_task_rollout_copy_model(const MRTaskRolloutHandle* handle, MRModelViewC* view) {
+    return guarded([&] {
+        if (!handle || !view) throw std::invalid_argument("handle or view is null");
+        const numi::CompiledModel& m = handle->model;
+        view->world = m.world;
+        if (view->joints) std::memcpy(view->joints, m.joints.data(), m.joints.size() * sizeof(MRModelJointC));
+        if (view->bodies) std::memcpy(view->bodies, m.bodies.data(), m.bodies.size() * sizeof(MRModelBodyC));
+        if (view->dofs) std::memcpy(view->dofs, m.dofs.data(), m.dofs.size() * sizeof(MRModelDofC));
+        if (view->shapes) std::memcpy(view->shapes, m.shapes.data(), m.shapes.size() * sizeof(MRModelShapeC));
+        if (view->materials) std::memcpy(view->materials, m.materials.data(), m.materials.size() * sizeof(MRModelMaterialC));
+        if (view->pairs) std::memcpy(view->pairs, m.pairs.data(), m.pairs.size() * sizeof(MRModelPairC));
+    });
+}
+
+static numi::CompiledModel compile_source(uint32_t source, uint64_t seed) {
+    switch (source) {
+        case MR_RUN_SOURCE_SYNTHETIC_CHAIN7: return numi::build_chain7(seed);
+        case MR_RUN_SOURCE_SYNTHETIC_TREE29: return numi::build_tree29(seed);
+        default: throw std::invalid_argument("unsupported synthetic source " + std::to_string(source));
+    }
+}
+
+MR_API int mr_compile_synthetic_model(uint32_t source, uint64_t seed, MRModelViewC* view) {
+    return guarded([&] {
+        if (!view) throw std::invalid_argument("view is null");
+        const numi::CompiledModel m = compile_source(source, seed);
+        view->world = m.world;
+        if (view->joints) std::memcpy(view->joints, m.joints.data(), m.joints.size() * sizeof(MRModelJointC));
+        if (view->bodies) std::memcpy(view->bodies, m.bodies.data(), m.bodies.size() * sizeof(MRModelBodyC));
+        if (view->dofs) std::memcpy(view->dofs, m.dofs.data(), m.dofs.size() * sizeof(MRModelDofC));
+        if (view->shapes) std::memcpy(view->shapes, m.shapes.data(), m.shapes.size() * sizeof(MRModelShapeC));
+        if (view->materials) std::memcpy(view->materials, m.materials.data(), m.materials.size() * sizeof(MRModelMaterialC));
+        if (view->pairs) std::memcpy(view->pairs, m.pairs.data(), m.pairs.size() * sizeof(MRModelPairC));
+    });
+}
+
+MR_API int mr_sample_synthetic_reset(uint32_t source, uint64_t model_seed, uint64_t reset_seed, uint32_t env_begin,
+                                     uint32_t env_count, float* q, float* v, float* friction_scale) {
+    return guarded([&] {
+        if (!q || !v || !friction_scale) throw std::invalid_argument("outputs must be non-null");
+        const numi::CompiledModel m = compile_source(source, model_seed);
+        for (uint32_t i = 0; i < env_count; ++i)
+            numi::sample_reset_state(m, reset_seed, env_begin + i, q + static_cast<size_t>(i) * m.world.nq,
+                                     v + static_cast<size_t>(i) * m.world.nv, friction_scale + i);
+    });
+}
+
+MR_API int mr_task_rollout_copy_environment_parameters(const MRTaskRolloutHandle* handle, float* friction_scale) {
+    return guarded([&] {
+        if (!handle || !friction_scale) throw std::invalid_argument("handle or output is null");
+        std::memcpy(friction_scale, handle->friction.data(), handle->friction.size() * sizeof(float));
+    });
+}
+
+MR_API int mr_task_rollout_copy_state(const MRTaskRolloutHandle* handle, float* q, float* v, MRManifoldC* manifolds) {
+    return guarded([&] {
+        if (!handle) throw std::invalid_argument("handle is null");
+        const MRTaskRolloutHandle& h = *handle;
+        check(cudaStreamSynchronize(h.stream), "sync");
+        if (q) check(cudaMemcpy(q, h.d_q.ptr, static_cast<size_t>(h.envs) * h.model.world.nq * sizeof(float), cudaMemcpyDeviceToHost), "q D2H");
+        if (v) check(cudaMemcpy(v, h.d_v.ptr, static_cast<size_t>(h.envs) * h.model.world.nv * sizeof(float), cudaMemcpyDeviceToHost), "v D2H");
+        if (manifolds && h.contact)
+            check(cudaMemcpy(manifolds, h.d_manifolds.ptr, static_cast<size_t>(h.envs) * h.manifold_words() * sizeof(float),
+                             cudaMemcpyDeviceToHost), "manifolds D2H");
+    });
+}
+
+MR_API int mr_task_rollout_set_state(MRTaskRolloutHandle* handle, const float* q, const float* v, const MRManifoldC* manifolds,
+                                     uint32_t as_reset_state) {
+    return guarded([&] {
+        if (!handle || !q || !v) throw std::invalid_argument("handle, q and v must be non-null");
+        MRTaskRolloutHandle& h = *handle;
+        const size_t nq = static_cast<size_t>(h.envs) * h.model.world.nq;
+        const size_t nv = static_cast<size_t>(h.envs) * h.model.world.nv;
+        check(cudaStreamSynchronize(h.stream), "sync");
+        check(cudaMemcpy(h.d_q.ptr, q, nq * sizeof(float), cudaMemcpyHostToDevice), "q H2D");
+        check(cudaMemcpy(h.d_v.ptr, v, nv * sizeof(float), cudaMemcpyHostToDevice), "v H2D");
+        if (h.contact) {
+            if (manifolds)
+                check(cudaMemcpy(h.d_manifolds.ptr, manifolds, static_cast<size_t>(h.envs) * h.manifold_words() * sizeof(float),
+                                 cudaMemcpyHostToDevice), "manifolds H2D");
+            else
+                check(cudaMemset(h.d_manifolds.ptr, 0, h.d_manifolds.count * sizeof(float)), "clear manifolds");
+        }
+        if (as_reset_state) {
+            h.reset_q.assign(q, q + nq);
+            h.reset_v.assign(v, v + nv);
+            check(cudaMemcpy(h.d_reset_q.ptr, q, nq * sizeof(float), cudaMemcpyHostToDevice), "reset q H2D");
+            check(cudaMemcpy(h.d_reset_v.ptr, v, nv * sizeof(float), cudaMemcpyHostToDevice), "reset v H2D");
+        }
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,451 @@
+"""Thin ctypes binding for the numi_b200 task-rollout C ABI.
+
+Conventions follow numi-lab's own binding (python/metalrobo/native.py):
+``ctypes.CDLL`` over the shared library, a ``MetalRoboError`` exception
+carrying ``mr_last_error()``, and an environment override
+(``METALROBO_LIBRARY``) for the library path.  The product path is the CUDA
+library only; importing this module on a machine without the built library
+raises instead of falling back to anything else.
+"""
+
+from __future__ import annotations
+
+import ctypes as ct
+import os
+from pathlib import Path
+from typing import Final
+
+_LIBRARY_ENV: Final = "METALROBO_LIBRARY"
+_PACKAGE_DIR: Final = Path(__file__).resolve().parent
+DEFAULT_LIBRARY: Final = _PACKAGE_DIR / "libnumi_b200.so"
+
+MR_INVALID_INDEX: Final = 0xFFFFFFFF
+MR_RUN_SOURCE_SYNTHETIC_CHAIN7: Final = 100
+MR_RUN_SOURCE_SYNTHETIC_TREE29: Final = 101
+MANIFOLD_POINTS: Final = 4
+
+STATUS_NAMES: Final = {
+    0: "success",
+    1: "fixed_budget_complete",
+    2: "nonfinite_input",
+    3: "nonfinite_result",
+    4: "pair_capacity_overflow",
+    5: "contact_capacity_overflow",
+    6: "manifold_capacity_overflow",
+    7: "constraint_capacity_overflow",
+    8: "island_capacity_overflow",
+    9: "ccd_event_budget_exhausted",
+    10: "factorization_failed",
+    11: "did_not_converge",
+    12: "unsupported",
+    13: "ccd_capacity_overflow",
+}
+
+
+class MetalRoboError(RuntimeError):
+    """Raised when the native runtime reports an error."""
+
+
+class DynamicSphereC(ct.Structure):
+    _fields_ = [
+        ("position", ct.c_float * 3),
+        ("linear_velocity", ct.c_float * 3),
+        ("radius", ct.c_float),
+        ("mass", ct.c_float),
+        ("launch_step", ct.c_uint32),
+    ]
+
+
+class TaskRolloutConfigC(ct.Structure):
+    _fields_ = [
+        ("environment_count", ct.c_uint32),
+        ("physics_substeps", ct.c_uint32),
+        ("velocity_iterations", ct.c_uint32),
+        ("final_velocity_iterations", ct.c_uint32),
+        ("control_timestep_seconds", ct.c_float),
+        ("seed", ct.c_uint64),
+        ("dynamic_spheres", ct.POINTER(DynamicSphereC)),
+        ("dynamic_sphere_count", ct.c_uint32),
+        ("disable_task_terminations", ct.c_uint32),
+        ("interaction_reference_mode", ct.c_uint32),
+        ("interaction_student_authority", ct.c_float),
+        ("override_interaction_student_authority", ct.c_uint32),
+        ("interaction_reset_phase_fraction", ct.c_float),
+        ("override_interaction_reset_phase_fraction", ct.c_uint32),
+        ("materialize_articulated_contact_responses", ct.c_uint32),
+        ("override_difficulty_band_range", ct.c_uint32),
+        ("minimum_difficulty_band", ct.c_uint32),
+        ("maximum_difficulty_band", ct.c_uint32),
+        ("interaction_reset_phase_probability", ct.c_float),
+        ("override_interaction_reset_phase_probability", ct.c_uint32),
+        ("interaction_reset_maximum_phase", ct.c_float),
+        ("override_interaction_reset_maximum_phase", ct.c_uint32),
+    ]
+
+
+class RunManifestC(ct.Structure):
+    _fields_ = [
+        ("profile", TaskRolloutConfigC),
+        ("source", ct.c_uint32),
+        ("surface", ct.c_uint32),
+        ("task", ct.c_uint32),
+        ("urdf_path", ct.c_char_p),
+        ("srdf_path", ct.c_char_p),
+        ("world_pack_path", ct.c_char_p),
+        ("task_pack_path", ct.c_char_p),
+        ("robot_actuator_pack_path", ct.c_char_p),
+        ("sensor_program_pack_path", ct.c_char_p),
+        ("reality_program_pack_path", ct.c_char_p),
+        ("teacher_pack_path", ct.c_char_p),
+        ("teacher_clip_id", ct.c_char_p),
+        ("visual_sensor_program", ct.c_void_p),
+        ("inspection_visual_program", ct.c_void_p),
+        ("metallib_path", ct.c_char_p),
+    ]
+
+
+class TaskRolloutLayoutC(ct.Structure):
+    _fields_ = [
+        ("environment_count", ct.c_uint32),
+        ("nq", ct.c_uint32),
+        ("nv", ct.c_uint32),
+        ("action_count", ct.c_uint32),
+        ("actor_observation_count", ct.c_uint32),
+        ("critic_observation_count", ct.c_uint32),
+        ("scene_body_count", ct.c_uint32),
+        ("motion_feature_count", ct.c_uint32),
+        ("maximum_episode_steps", ct.c_uint32),
+        ("world_fingerprint", ct.c_uint64),
+        ("task_fingerprint", ct.c_uint64),
+        ("observation_fingerprint", ct.c_uint64),
+        ("action_fingerprint", ct.c_uint64),
+        ("run_fingerprint", ct.c_uint64),
+        ("robot_fingerprint", ct.c_uint64),
+        ("sensor_fingerprint", ct.c_uint64),
+        ("reality_fingerprint", ct.c_uint64),
+        ("teacher_fingerprint", ct.c_uint64),
+        ("submitted_control_steps", ct.c_uint64),
+        ("completed_environment_steps", ct.c_uint64),
+        ("submission_count", ct.c_uint64),
+        ("retained_buffer_bytes", ct.c_size_t),
+        ("immutable_private_bytes", ct.c_size_t),
+        ("persistent_state_private_bytes", ct.c_size_t),
+        ("transient_private_bytes", ct.c_size_t),
+        ("shared_boundary_bytes", ct.c_size_t),
+        ("peak_aliased_bytes", ct.c_size_t),
+        ("total_gpu_milliseconds", ct.c_double),
+        ("total_submission_milliseconds", ct.c_double),
+    ]
+
+
+class StageHighWaterC(ct.Structure):
+    _fields_ = [
+        (name, ct.c_uint32)
+        for name in (
+            "candidate_pairs raw_contacts manifolds constraint_blocks constraint_rows islands "
+            "hard_convex_pairs mesh_triangle_candidates solver_tiles spill_rows ccd_candidates ccd_events "
+            "endpoint_runtime_records articulation_point_queries rod_candidate_pairs rod_raw_contacts "
+            "rod_manifolds rod_ccd_events quality_generalized_velocities quality_rows quality_krylov_vectors "
+            "quality_direct_tiles dynamic_nodes island_node_references island_constraint_references "
+            "rod_factor_blocks operator_velocity_elements"
+        ).split()
+    ]
+
+
+class TaskRolloutAdvanceC(ct.Structure):
+    _fields_ = [
+        ("control_step_count", ct.c_uint32),
+        ("successful_environment_steps", ct.c_uint32),
+        ("failed_environment_steps", ct.c_uint32),
+        ("first_failing_environment", ct.c_uint32),
+        ("first_failing_control_step", ct.c_uint32),
+        ("first_gpu_status_code", ct.c_uint32),
+        ("host_requested_resets", ct.c_uint32),
+        ("maximum_active_contacts", ct.c_uint32),
+        ("maximum_manifolds", ct.c_uint32),
+        ("high_water", StageHighWaterC),
+        ("gpu_milliseconds", ct.c_double),
+        ("submission_milliseconds", ct.c_double),
+    ]
+
+
+class ModelWorldC(ct.Structure):
+    _fields_ = [
+        ("body_count", ct.c_uint32),
+        ("joint_count", ct.c_uint32),
+        ("nq", ct.c_uint32),
+        ("nv", ct.c_uint32),
+        ("shape_count", ct.c_uint32),
+        ("material_count", ct.c_uint32),
+        ("pair_count", ct.c_uint32),
+        ("root_type", ct.c_uint32),
+        ("actuation_mode", ct.c_uint32),
+        ("action_count", ct.c_uint32),
+        ("contact_capacity", ct.c_uint32),
+        ("apply_body_damping", ct.c_uint32),
+        ("gravity", ct.c_float * 4),
+        ("solver_scales", ct.c_float * 4),
+        ("manifold_thresholds", ct.c_float * 4),
+        ("speculative", ct.c_float * 4),
+    ]
+
+
+class ModelJointC(ct.Structure):
+    _fields_ = [
+        ("parent_body", ct.c_uint32),
+        ("child_body", ct.c_uint32),
+        ("joint_type", ct.c_uint32),
+        ("q_index", ct.c_uint32),
+        ("v_index", ct.c_uint32),
+        ("reserved", ct.c_uint32 * 3),
+        ("axis", ct.c_float * 4),
+        ("parent_anchor", ct.c_float * 4),
+        ("child_anchor", ct.c_float * 4),
+        ("parent_rotation", ct.c_float * 4),
+        ("child_rotation", ct.c_float * 4),
+    ]
+
+
+class ModelBodyC(ct.Structure):
+    _fields_ = [
+        ("parent_body", ct.c_uint32),
+        ("inbound_joint", ct.c_uint32),
+        ("motion_type", ct.c_uint32),
+        ("articulated", ct.c_uint32),
+        ("mass_inverse_mass", ct.c_float * 4),
+        ("inertia", (ct.c_float * 4) * 3),
+        ("damping_speed", ct.c_float * 4),
+        ("static_pose", ct.c_float * 8),
+    ]
+
+
+class ModelDofC(ct.Structure):
+    _fields_ = [
+        ("joint_index", ct.c_uint32),
+        ("q_index", ct.c_uint32),
+        ("flags", ct.c_uint32),
+        ("reserved", ct.c_uint32),
+        ("limits", ct.c_float * 4),
+        ("drive", ct.c_float * 4),
+    ]
+
+
+class ModelShapeC(ct.Structure):
+    _fields_ = [
+        ("body", ct.c_uint32),
+        ("shape_type", ct.c_uint32),
+        ("material", ct.c_uint32),
+        ("flags", ct.c_uint32),
+        ("collision_group", ct.c_uint32),
+        ("collision_mask", ct.c_uint32),
+        ("reserved", ct.c_uint32 * 2),
+        ("local_position", ct.c_float * 4),
+        ("local_rotation", ct.c_float * 4),
+        ("dimensions", ct.c_float * 4),
+        ("contact_rest_bound", ct.c_float * 4),
+    ]
+
+
+class ModelMaterialC(ct.Structure):
+    _fields_ = [("friction", ct.c_float * 4), ("response", ct.c_float * 4)]
+
+
+class ModelPairC(ct.Structure):
+    _fields_ = [
+        ("shape_a", ct.c_uint32),
+        ("shape_b", ct.c_uint32),
+        ("pair_class", ct.c_uint32),
+        ("max_points", ct.c_uint32),
+    ]
+
+
+class ModelViewC(ct.Structure):
+    _fields_ = [
+        ("world", ModelWorldC),
+        ("joints", ct.POINTER(ModelJointC)),
+        ("bodies", ct.POINTER(ModelBodyC)),
+        ("dofs", ct.POINTER(ModelDofC)),
+        ("shapes", ct.POINTER(ModelShapeC)),
+        ("materials", ct.POINTER(ModelMaterialC)),
+        ("pairs", ct.POINTER(ModelPairC)),
+    ]
+
+
+class ManifoldPointC(ct.Structure):
+    _fields_ = [
+        ("anchor_a", ct.c_float * 3),
+        ("anchor_b", ct.c_float * 3),
+        ("feature_a", ct.c_uint32),
+        ("feature_b", ct.c_uint32),
+        ("life", ct.c_uint32),
+        ("impulses", ct.c_float * 3),
+    ]
+
+
+class ManifoldC(ct.Structure):
+    _fields_ = [
+        ("normal_local", ct.c_float * 3),
+        ("age", ct.c_float),
+        ("tangent_local", ct.c_float * 3),
+        ("count", ct.c_uint32),
+        ("points", ManifoldPointC * MANIFOLD_POINTS),
+    ]
+
+
+# Every C-ABI entry point this binding configures, by name.  Tests check the
+# loaded library exports each of them.
+EXPORTED_SYMBOLS: Final = (
+    "mr_version",
+    "mr_runtime_abi_fingerprint",
+    "mr_last_error",
+    "mr_create_task_rollout",
+    "mr_task_rollout_destroy",
+    "mr_task_rollout_reset",
+    "mr_task_rollout_set_state_readback",
+    "mr_task_rollout_advance",
+    "mr_task_rollout_layout",
+    "mr_task_rollout_device_name",
+    "mr_task_rollout_status_codes",
+    "mr_task_rollout_active_contacts",
+    "mr_task_rollout_actor_observations",
+    "mr_task_rollout_final_q",
+    "mr_task_rollout_copy_final_scene_states",
+    "mr_task_rollout_advance_device",
+    "mr_task_rollout_copy_model",
+    "mr_task_rollout_copy_environment_parameters",
+    "mr_task_rollout_copy_state",
+    "mr_task_rollout_set_state",
+)
+
+
+def resolve_library_path(path: str | os.PathLike[str] | None = None) -> Path:
+    """Resolves the native library, preferring explicit and environment paths."""
+
+    if path is not None:
+        explicit = Path(path).expanduser()
+        if not explicit.is_file():
+            raise FileNotFoundError(f"numi_b200 library does not exist: {explicit}")
+        return explicit.resolve()
+    configured = os.environ.get(_LIBRARY_ENV)
+    if configured:
+        configured_path = Path(configured).expanduser()
+        if not configured_path.is_file():
+            raise FileNotFoundError(f"{_LIBRARY_ENV} points to a missing file: {configured_path}")
+        return configured_path.resolve()
+    if DEFAULT_LIBRARY.is_file():
+        return DEFAULT_LIBRARY
+    raise FileNotFoundError(
+        f"Could not find {DEFAULT_LIBRARY.name}. Build it with `python -m numi_lab_b200.build` "
+        f"or set {_LIBRARY_ENV}."
+    )
+
+
+class Bindings:
+    """Configured ctypes function table for one loaded library."""
+
+    def __init__(self, path: str | os.PathLike[str] | None = None) -> None:
+        self.path = resolve_library_path(path)
+        self.lib = ct.CDLL(str(self.path))
+        L = self.lib
+        P = ct.POINTER
+        L.mr_version.argtypes = []
+        L.mr_version.restype = ct.c_char_p
+        L.mr_runtime_abi_fingerprint.argtypes = []
+        L.mr_runtime_abi_fingerprint.restype = ct.c_uint64
+        L.mr_last_error.argtypes = []
+        L.mr_last_error.restype = ct.c_char_p
+        L.mr_create_task_rollout.argtypes = [P(RunManifestC)]
+        L.mr_create_task_rollout.restype = ct.c_void_p
+        L.mr_task_rollout_destroy.argtypes = [ct.c_void_p]
+        L.mr_task_rollout_destroy.restype = None
+        L.mr_task_rollout_reset.argtypes = [ct.c_void_p, ct.c_uint64]
+        L.mr_task_rollout_reset.restype = ct.c_int
+        L.mr_task_rollout_set_state_readback.argtypes = [ct.c_void_p, ct.c_uint32]
+        L.mr_task_rollout_set_state_readback.restype = ct.c_int
+        L.mr_task_rollout_advance.argtypes = [
+            ct.c_void_p,
+            P(ct.c_float),
+            ct.c_size_t,
+            P(ct.c_uint32),
+            ct.c_size_t,
+            ct.c_uint32,
+            ct.c_uint64,
+            ct.c_uint32,
+            P(TaskRolloutAdvanceC),
+        ]
+        L.mr_task_rollout_advance.restype = ct.c_int
+        L.mr_task_rollout_layout.argtypes = [ct.c_void_p]
+        L.mr_task_rollout_layout.restype = TaskRolloutLayoutC
+        L.mr_task_rollout_device_name.argtypes = [ct.c_void_p]
+        L.mr_task_rollout_device_name.restype = ct.c_char_p
+        for name in ("mr_task_rollout_status_codes", "mr_task_rollout_active_contacts"):
+            getattr(L, name).argtypes = [ct.c_void_p]
+            getattr(L, name).restype = P(ct.c_uint32)
+        for name in ("mr_task_rollout_actor_observations", "mr_task_rollout_final_q"):
+            getattr(L, name).argtypes = [ct.c_void_p]
+            getattr(L, name).restype = P(ct.c_float)
+        L.mr_task_rollout_copy_final_scene_states.argtypes = [ct.c_void_p, P(ct.c_float), ct.c_size_t]
+        L.mr_task_rollout_copy_final_scene_states.restype = ct.c_int
+        L.mr_task_rollout_advance_device.argtypes = [
+            ct.c_void_p,
+            ct.c_void_p,
+            ct.c_void_p,
+            ct.c_uint32,
+            ct.c_void_p,
+            ct.c_void_p,
+            ct.c_uint64,
+            P(TaskRolloutAdvanceC),
+        ]
+        L.mr_task_rollout_advance_device.restype = ct.c_int
+        L.mr_task_rollout_copy_model.argtypes = [ct.c_void_p, P(ModelViewC)]
+        L.mr_task_rollout_copy_model.restype = ct.c_int
+        L.mr_task_rollout_copy_environment_parameters.argtypes = [ct.c_void_p, P(ct.c_float)]
+        L.mr_task_rollout_copy_environment_parameters.restype = ct.c_int
+        L.mr_task_rollout_copy_state.argtypes = [ct.c_void_p, P(ct.c_float), P(ct.c_float), ct.c_void_p]
+        L.mr_task_rollout_copy_state.restype = ct.c_int
+        L.mr_task_rollout_set_state.argtypes = [ct.c_void_p, P(ct.c_float), P(ct.c_float), ct.c_void_p, ct.c_uint32]
+        L.mr_task_rollout_set_state.restype = ct.c_int
+
+    def last_error(self) -> str:
+        value = self.lib.mr_last_error()
+        return value.decode("utf-8", "replace") if value else ""
+
+    def check(self, rc: int, what: str) -> None:
+        if rc != 0:
+            raise MetalRoboError(f"{what}: {self.last_error()}")
+
+
+_BINDINGS: Bindings | None = None
+
+
+def bindings(path: str | os.PathLike[str] | None = None) -> Bindings:
+    """Returns the process-wide bindings (loading the library on first use)."""
+
+    global _BINDINGS
+    if path is not None:
+        return Bindings(path)
+    if _BINDINGS is None:
+        _BINDINGS = Bindings()
+    return _BINDINGS
+
+
+def default_manifest(
+    source: int,
+    environment_count: int,
+    *,
+    physics_substeps: int = 1,
+    velocity_iterations: int = 8,
+    final_velocity_iterations: int = 0,
+    control_timestep_seconds: float = 0.005,
+    seed: int = 0,
+) -> RunManifestC:
+    manifest = RunManifestC()
+    profile = manifest.profile
+    profile.environment_count = environment_count
+    profile.physics_substeps = physics_substeps
+    profile.velocity_iterations = velocity_iterations
+    profile.final_velocity_iterations = final_velocity_iterations
+    profile.control_timestep_seconds = control_timestep_seconds
+    profile.seed = seed
+    manifest.source = source
+    return manifest

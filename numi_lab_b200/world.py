@@ -1,0 +1,341 @@
+"""world / reset / step API over the numi_b200 task-rollout C ABI.
+
+``World.step`` is the zero-copy path: actions, reset masks and observations
+are torch CUDA tensors whose device pointers go straight to the native
+library (``mr_task_rollout_advance_device``); work is ordered on torch's
+current stream.  ``World.advance_host`` is the reference-shaped path
+(``mr_task_rollout_advance``: host spans in, handle-owned results out).
+
+Every physics computation runs in the CUDA library; this module only marshals
+pointers and shapes.  A missing library raises ``FileNotFoundError``.
+"""
+
+from __future__ import annotations
+
+import ctypes as ct
+from dataclasses import dataclass
+from typing import Any
+
+import numpy as np
+
+from . import native
+from .native import MetalRoboError
+
+SOURCES = {
+    "chain7": native.MR_RUN_SOURCE_SYNTHETIC_CHAIN7,
+    "tree29": native.MR_RUN_SOURCE_SYNTHETIC_TREE29,
+}
+
+
+def _source_id(source: str | int) -> int:
+    if isinstance(source, str):
+        if source not in SOURCES:
+            raise ValueError(f"unknown source {source!r}; expected one of {sorted(SOURCES)}")
+        return SOURCES[source]
+    return int(source)
+
+
+@dataclass
+class ModelRecords:
+    """Compiled world records (ctypes arrays) of one synthetic world."""
+
+    world: native.ModelWorldC
+    joints: Any
+    bodies: Any
+    dofs: Any
+    shapes: Any
+    materials: Any
+    pairs: Any
+
+    def view(self) -> native.ModelViewC:
+        v = native.ModelViewC()
+        v.world = self.world
+        v.joints = ct.cast(self.joints, ct.POINTER(native.ModelJointC))
+        v.bodies = ct.cast(self.bodies, ct.POINTER(native.ModelBodyC))
+        v.dofs = ct.cast(self.dofs, ct.POINTER(native.ModelDofC))
+        v.shapes = ct.cast(self.shapes, ct.POINTER(native.ModelShapeC))
+        v.materials = ct.cast(self.materials, ct.POINTER(native.ModelMaterialC))
+        v.pairs = ct.cast(self.pairs, ct.POINTER(native.ModelPairC))
+        return v
+
+
+def _alloc_records(world: native.ModelWorldC) -> ModelRecords:
+    return ModelRecords(
+        world=world,
+        joints=(native.ModelJointC * max(world.joint_count, 1))(),
+        bodies=(native.ModelBodyC * max(world.body_count, 1))(),
+        dofs=(native.ModelDofC * max(world.nv, 1))(),
+        shapes=(native.ModelShapeC * max(world.shape_count, 1))(),
+        materials=(native.ModelMaterialC * max(world.material_count, 1))(),
+        pairs=(native.ModelPairC * max(world.pair_count, 1))(),
+    )
+
+
+def compile_model(source: str | int, seed: int, *, library: native.Bindings | None = None) -> ModelRecords:
+    """Compiles a synthetic world on the host (no GPU needed)."""
+
+    lib = library or native.bindings()
+    sid = _source_id(source)
+    probe = native.ModelViewC()
+    lib.check(lib.lib.mr_compile_synthetic_model(sid, seed, ct.byref(probe)), "mr_compile_synthetic_model")
+    records = _alloc_records(probe.world)
+    view = records.view()
+    lib.check(lib.lib.mr_compile_synthetic_model(sid, seed, ct.byref(view)), "mr_compile_synthetic_model")
+    records.world = view.world
+    return records
+
+
+def sample_reset(
+    source: str | int,
+    model_seed: int,
+    reset_seed: int,
+    env_begin: int,
+    env_count: int,
+    *,
+    library: native.Bindings | None = None,
+) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Reset states (q, v, friction scale) a rollout samples for these envs."""
+
+    lib = library or native.bindings()
+    sid = _source_id(source)
+    world = compile_model(sid, model_seed, library=lib).world
+    q = np.zeros((env_count, world.nq), np.float32)
+    v = np.zeros((env_count, world.nv), np.float32)
+    f = np.zeros((env_count,), np.float32)
+    lib.check(
+        lib.lib.mr_sample_synthetic_reset(
+            sid,
+            model_seed,
+            reset_seed,
+            env_begin,
+            env_count,
+            q.ctypes.data_as(ct.POINTER(ct.c_float)),
+            v.ctypes.data_as(ct.POINTER(ct.c_float)),
+            f.ctypes.data_as(ct.POINTER(ct.c_float)),
+        ),
+        "mr_sample_synthetic_reset",
+    )
+    return q, v, f
+
+
+class World:
+    """A batch of environments of one synthetic world on the current CUDA device."""
+
+    def __init__(
+        self,
+        source: str | int = "tree29",
+        envs: int = 1,
+        *,
+        substeps: int = 4,
+        velocity_iterations: int = 8,
+        final_velocity_iterations: int = 0,
+        control_dt: float = 0.02,
+        seed: int = 0,
+        library: native.Bindings | None = None,
+    ) -> None:
+        self._lib = library or native.bindings()
+        self.source = _source_id(source)
+        manifest = native.default_manifest(
+            self.source,
+            envs,
+            physics_substeps=substeps,
+            velocity_iterations=velocity_iterations,
+            final_velocity_iterations=final_velocity_iterations,
+            control_timestep_seconds=control_dt,
+            seed=seed,
+        )
+        handle = self._lib.lib.mr_create_task_rollout(ct.byref(manifest))
+        if not handle:
+            raise MetalRoboError(f"mr_create_task_rollout: {self._lib.last_error()}")
+        self._handle = ct.c_void_p(handle)
+        self.envs = envs
+        self.seed = seed
+        self.substeps = substeps
+        layout = self.layout()
+        self.nq = int(layout.nq)
+        self.nv = int(layout.nv)
+        self.action_count = int(layout.action_count)
+        self.observation_count = self.nq + self.nv
+        model = native.ModelViewC()
+        self._lib.check(self._lib.lib.mr_task_rollout_copy_model(self._handle, ct.byref(model)), "copy_model")
+        self.pair_count = int(model.world.pair_count)
+
+    # -- lifecycle -------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_handle", None) and self._handle.value:
+            self._lib.lib.mr_task_rollout_destroy(self._handle)
+            self._handle = ct.c_void_p(None)
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self) -> "World":
+        return self
+
+    def __exit__(self, *exc: object) -> None:
+        self.close()
+
+    # -- queries ---------------------------------------------------------
+    def layout(self) -> native.TaskRolloutLayoutC:
+        return self._lib.lib.mr_task_rollout_layout(self._handle)
+
+    def device_name(self) -> str:
+        name = self._lib.lib.mr_task_rollout_device_name(self._handle)
+        return name.decode() if name else ""
+
+    def model(self) -> ModelRecords:
+        probe = native.ModelViewC()
+        self._lib.check(self._lib.lib.mr_task_rollout_copy_model(self._handle, ct.byref(probe)), "copy_model")
+        records = _alloc_records(probe.world)
+        view = records.view()
+        self._lib.check(self._lib.lib.mr_task_rollout_copy_model(self._handle, ct.byref(view)), "copy_model")
+        records.world = view.world
+        return records
+
+    def friction_scales(self) -> np.ndarray:
+        out = np.zeros((self.envs,), np.float32)
+        self._lib.check(
+            self._lib.lib.mr_task_rollout_copy_environment_parameters(self._handle, out.ctypes.data_as(ct.POINTER(ct.c_float))),
+            "copy_environment_parameters",
+        )
+        return out
+
+    # -- state -----------------------------------------------------------
+    def reset(self, seed: int | None = None) -> None:
+        if seed is not None:
+            self.seed = seed
+        self._lib.check(self._lib.lib.mr_task_rollout_reset(self._handle, self.seed), "mr_task_rollout_reset")
+
+    def state(self) -> tuple[np.ndarray, np.ndarray, Any]:
+        q = np.zeros((self.envs, self.nq), np.float32)
+        v = np.zeros((self.envs, self.nv), np.float32)
+        manifolds = (native.ManifoldC * max(self.envs * self.pair_count, 1))()
+        self._lib.check(
+            self._lib.lib.mr_task_rollout_copy_state(
+                self._handle,
+                q.ctypes.data_as(ct.POINTER(ct.c_float)),
+                v.ctypes.data_as(ct.POINTER(ct.c_float)),
+                ct.cast(manifolds, ct.c_void_p) if self.pair_count else None,
+            ),
+            "copy_state",
+        )
+        return q, v, manifolds
+
+    def set_state(self, q: np.ndarray, v: np.ndarray, manifolds: Any = None, *, as_reset_state: bool = False) -> None:
+        q = np.ascontiguousarray(q, np.float32)
+        v = np.ascontiguousarray(v, np.float32)
+        if q.shape != (self.envs, self.nq) or v.shape != (self.envs, self.nv):
+            raise ValueError("state shapes must be (envs, nq) and (envs, nv)")
+        self._lib.check(
+            self._lib.lib.mr_task_rollout_set_state(
+                self._handle,
+                q.ctypes.data_as(ct.POINTER(ct.c_float)),
+                v.ctypes.data_as(ct.POINTER(ct.c_float)),
+                ct.cast(manifolds, ct.c_void_p) if manifolds is not None else None,
+                1 if as_reset_state else 0,
+            ),
+            "set_state",
+        )
+
+    # -- stepping ----------------------------------------------------------
+    def step(
+        self,
+        actions: Any,
+        reset_mask: Any = None,
+        observations: Any = None,
+        status: Any = None,
+        *,
+        wait: bool = False,
+    ) -> tuple[Any, Any, native.TaskRolloutAdvanceC | None]:
+        """Advances ``actions.shape[0]`` control steps on the device.
+
+        ``actions``: CUDA float32 tensor [steps, envs, action_count] (or
+        [envs, action_count] for one step).  Returns (observations [steps,
+        envs, nq+nv], status codes [steps, envs], counters or None).
+        """
+
+        import torch
+
+        if actions.dim() == 2:
+            actions = actions.unsqueeze(0)
+        if not actions.is_cuda or actions.dtype != torch.float32 or not actions.is_contiguous():
+            raise ValueError("actions must be a contiguous float32 CUDA tensor")
+        steps = int(actions.shape[0])
+        if tuple(actions.shape[1:]) != (self.envs, self.action_count):
+            raise ValueError(f"actions must have shape [steps, {self.envs}, {self.action_count}]")
+        device = actions.device
+        if observations is None:
+            observations = torch.empty((steps, self.envs, self.observation_count), device=device, dtype=torch.float32)
+        if status is None:
+            status = torch.empty((steps, self.envs), device=device, dtype=torch.int32)
+        mask_ptr = None
+        if reset_mask is not None:
+            if reset_mask.dim() == 1:
+                reset_mask = reset_mask.unsqueeze(0)
+            if tuple(reset_mask.shape) != (steps, self.envs) or reset_mask.dtype not in (torch.int32, torch.uint32):
+                raise ValueError("reset_mask must be an int32 tensor [steps, envs]")
+            mask_ptr = ct.c_void_p(reset_mask.contiguous().data_ptr())
+        stream = torch.cuda.current_stream(device).cuda_stream
+        counters = native.TaskRolloutAdvanceC() if wait else None
+        self._lib.check(
+            self._lib.lib.mr_task_rollout_advance_device(
+                self._handle,
+                ct.c_void_p(actions.data_ptr()),
+                mask_ptr,
+                steps,
+                ct.c_void_p(observations.data_ptr()),
+                ct.c_void_p(status.data_ptr()),
+                ct.c_uint64(stream),
+                ct.byref(counters) if counters is not None else None,
+            ),
+            "mr_task_rollout_advance_device",
+        )
+        return observations, status, counters
+
+    def set_state_readback(self, enabled: bool) -> None:
+        self._lib.check(self._lib.lib.mr_task_rollout_set_state_readback(self._handle, 1 if enabled else 0), "set_state_readback")
+
+    def advance_host(
+        self, actions: np.ndarray, reset_masks: np.ndarray | None = None, *, raise_on_failure: bool = True
+    ) -> dict[str, Any]:
+        """Reference-shaped synchronous advance with host buffers."""
+
+        actions = np.ascontiguousarray(actions, np.float32)
+        steps = actions.shape[0] if actions.ndim == 3 else 1
+        counters = native.TaskRolloutAdvanceC()
+        masks_ptr = None
+        mask_count = 0
+        if reset_masks is not None:
+            reset_masks = np.ascontiguousarray(reset_masks, np.uint32)
+            masks_ptr = reset_masks.ctypes.data_as(ct.POINTER(ct.c_uint32))
+            mask_count = reset_masks.size
+        rc = self._lib.lib.mr_task_rollout_advance(
+            self._handle,
+            actions.ctypes.data_as(ct.POINTER(ct.c_float)),
+            actions.size,
+            masks_ptr,
+            mask_count,
+            steps,
+            0,
+            0,
+            ct.byref(counters),
+        )
+        if rc != 0 and (raise_on_failure or counters.control_step_count == 0):
+            raise MetalRoboError(f"mr_task_rollout_advance: {self._lib.last_error()}")
+        cells = steps * self.envs
+        out: dict[str, Any] = {"counters": counters, "rc": rc}
+        sc = self._lib.lib.mr_task_rollout_status_codes(self._handle)
+        ac = self._lib.lib.mr_task_rollout_active_contacts(self._handle)
+        out["status"] = np.ctypeslib.as_array(sc, shape=(cells,)).reshape(steps, self.envs).copy() if sc else None
+        out["contacts"] = np.ctypeslib.as_array(ac, shape=(cells,)).reshape(steps, self.envs).copy() if ac else None
+        obs = self._lib.lib.mr_task_rollout_actor_observations(self._handle)
+        if obs:
+            out["observations"] = (
+                np.ctypeslib.as_array(obs, shape=(cells * self.observation_count,)).reshape(steps, self.envs, -1).copy()
+            )
+            fq = self._lib.lib.mr_task_rollout_final_q(self._handle)
+            out["final_q"] = np.ctypeslib.as_array(fq, shape=(self.envs * self.nq,)).reshape(self.envs, self.nq).copy()
+        return out

@@ -1,0 +1,314 @@
+"""ORACLE — test infrastructure only.
+
+ctypes loaders for
+  * ``oracle/liboracle.so``: this project's plain-C FP64 restatement of
+    numi-lab's microstep (oracle/oracle.c), and
+  * ``oracle/_ref/libnumiref.so``: the reference's own FP64 CPU core compiled
+    from its sources with oracle/ref_harness.cpp (built by oracle/Makefile
+    where the reference sources exist; the built file travels with the repo
+    snapshot).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
+this package, and only as the checker.  The product library never loads it.
+"""
+
+from __future__ import annotations
+
+import ctypes as ct
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parent
+ORACLE_LIB = HERE / "liboracle.so"
+REF_LIB = HERE / "_ref" / "libnumiref.so"
+REFERENCE_SOURCES = Path(os.environ.get("NUMI_REFERENCE_ROOT", "/root/reference"))
+
+MAX_CONTACTS = 32
+MANIFOLD_POINTS = 4
+
+
+class OraclePoint(ct.Structure):
+    _fields_ = [
+        ("anchor_a", ct.c_double * 3),
+        ("anchor_b", ct.c_double * 3),
+        ("feature_a", ct.c_uint32),
+        ("feature_b", ct.c_uint32),
+        ("life", ct.c_uint32),
+        ("reserved", ct.c_uint32),
+        ("impulses", ct.c_double * 3),
+    ]
+
+
+class OracleManifold(ct.Structure):
+    _fields_ = [
+        ("normal_local", ct.c_double * 3),
+        ("age", ct.c_double),
+        ("tangent_local", ct.c_double * 3),
+        ("count", ct.c_uint32),
+        ("reserved", ct.c_uint32),
+        ("points", OraclePoint * MANIFOLD_POINTS),
+    ]
+
+
+class OracleContact(ct.Structure):
+    _fields_ = [
+        ("pair", ct.c_uint32),
+        ("point", ct.c_uint32),
+        ("feature_a", ct.c_uint32),
+        ("feature_b", ct.c_uint32),
+        ("body", ct.c_uint32),
+        ("new_impact", ct.c_uint32),
+        ("separation", ct.c_double),
+        ("normal", ct.c_double * 3),
+        ("impulses", ct.c_double * 3),
+    ]
+
+
+class OracleTrace(ct.Structure):
+    _fields_ = [
+        ("status", ct.c_uint32),
+        ("failing_index", ct.c_uint32),
+        ("failing_substep", ct.c_uint32),
+        ("contact_count", ct.c_uint32),
+        ("island_count", ct.c_uint32),
+        ("manifold_count", ct.c_uint32),
+        ("max_contacts", ct.c_uint32),
+        ("reserved", ct.c_uint32),
+        ("max_cone_violation", ct.c_double),
+        ("max_normal_residual", ct.c_double),
+        ("contacts", OracleContact * MAX_CONTACTS),
+    ]
+
+
+def build(reference: bool = True) -> None:
+    """Compiles the checker libraries (the C restatement always; the
+    reference core when its sources are present)."""
+
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    if reference and (REFERENCE_SOURCES / "src" / "core").is_dir():
+        subprocess.run(["make", "-s", "-j8", "-C", str(HERE), "ref", f"REF={REFERENCE_SOURCES}"], check=True)
+
+
+_DP = ct.POINTER(ct.c_double)
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(_DP)
+
+
+class Oracle:
+    """The C restatement, bound to one compiled world."""
+
+    def __init__(self, records, h: float, substeps: int, velocity_iterations: int, final_velocity_iterations: int) -> None:
+        if not ORACLE_LIB.is_file():
+            build(reference=False)
+        lib = ct.CDLL(str(ORACLE_LIB))
+        self.lib = lib
+        lib.oracle_world_create.restype = ct.c_void_p
+        lib.oracle_world_create.argtypes = [ct.c_void_p] * 7 + [ct.c_double, ct.c_uint32, ct.c_uint32, ct.c_uint32]
+        lib.oracle_world_destroy.argtypes = [ct.c_void_p]
+        lib.oracle_control_step.restype = ct.c_uint32
+        lib.oracle_control_step.argtypes = [ct.c_void_p, _DP, _DP, ct.c_void_p, _DP, ct.c_double, ct.c_int, _DP, _DP, ct.c_void_p]
+        lib.oracle_aba.restype = ct.c_uint32
+        lib.oracle_aba.argtypes = [ct.c_void_p, _DP, _DP, _DP, _DP]
+        lib.oracle_mass_matrix.restype = ct.c_uint32
+        lib.oracle_mass_matrix.argtypes = [ct.c_void_p, _DP, _DP]
+        lib.oracle_point_jacobian.restype = ct.c_uint32
+        lib.oracle_point_jacobian.argtypes = [ct.c_void_p, _DP, ct.c_uint32, _DP, _DP, _DP]
+        lib.oracle_drive_efforts.argtypes = [ct.c_void_p, _DP, _DP, _DP, _DP]
+        lib.oracle_project_cone.argtypes = [_DP, ct.c_double, ct.c_double, _DP]
+        lib.oracle_invert3x3.restype = ct.c_int
+        lib.oracle_invert3x3.argtypes = [_DP, _DP]
+        lib.oracle_manifold_from_device.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_uint32]
+        lib.oracle_manifold_to_device.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_uint32]
+        lib.oracle_temporal_cone_dense.argtypes = [ct.c_uint32, _DP, _DP, _DP, ct.c_uint32, _DP]
+        self.records = records
+        w = records.world
+        self.nq, self.nv, self.na, self.np = int(w.nq), int(w.nv), int(w.action_count), int(w.pair_count)
+        self.h = h
+        self.handle = lib.oracle_world_create(
+            ct.byref(records.world),
+            ct.cast(records.joints, ct.c_void_p),
+            ct.cast(records.bodies, ct.c_void_p),
+            ct.cast(records.dofs, ct.c_void_p),
+            ct.cast(records.shapes, ct.c_void_p),
+            ct.cast(records.materials, ct.c_void_p),
+            ct.cast(records.pairs, ct.c_void_p),
+            h,
+            substeps,
+            velocity_iterations,
+            final_velocity_iterations,
+        )
+        if not self.handle:
+            raise RuntimeError("oracle_world_create failed")
+
+    def __del__(self) -> None:
+        try:
+            if self.handle:
+                self.lib.oracle_world_destroy(self.handle)
+        except Exception:
+            pass
+
+    def new_manifolds(self, count: int = 1):
+        return (OracleManifold * max(count * self.np, 1))()
+
+    def manifolds_from_device(self, device_manifolds, count: int):
+        out = (OracleManifold * max(count, 1))()
+        self.lib.oracle_manifold_from_device(ct.cast(device_manifolds, ct.c_void_p), ct.cast(out, ct.c_void_p), count)
+        return out
+
+    def env_manifolds(self, device_manifolds, env: int):
+        """Oracle copy of environment `env`'s slots of a device manifold array."""
+
+        out = (OracleManifold * max(self.np, 1))()
+        if self.np:
+            size = ct.sizeof(device_manifolds._type_)
+            src = ct.c_void_p(ct.addressof(device_manifolds) + env * self.np * size)
+            self.lib.oracle_manifold_from_device(src, ct.cast(out, ct.c_void_p), self.np)
+        return out
+
+    def control_step(self, q: np.ndarray, v: np.ndarray, manifolds, actions: np.ndarray, friction: float,
+                     reset: bool = False, reset_q: np.ndarray | None = None, reset_v: np.ndarray | None = None):
+        """One control step of one env; q, v (float64) and manifolds in place."""
+
+        assert q.dtype == np.float64 and v.dtype == np.float64
+        trace = OracleTrace()
+        act = np.ascontiguousarray(actions, np.float64)
+        rq = np.ascontiguousarray(reset_q if reset_q is not None else q, np.float64)
+        rv = np.ascontiguousarray(reset_v if reset_v is not None else v, np.float64)
+        status = self.lib.oracle_control_step(
+            self.handle, _dp(q), _dp(v), ct.cast(manifolds, ct.c_void_p) if manifolds is not None else None,
+            _dp(act), float(friction), 1 if reset else 0, _dp(rq), _dp(rv), ct.byref(trace))
+        return int(status), trace
+
+    def aba(self, q, v, tau) -> tuple[int, np.ndarray]:
+        out = np.zeros(self.nv)
+        st = self.lib.oracle_aba(self.handle, _dp(np.ascontiguousarray(q, np.float64)), _dp(np.ascontiguousarray(v, np.float64)),
+                                 _dp(np.ascontiguousarray(tau, np.float64)), _dp(out))
+        return int(st), out
+
+    def mass_matrix(self, q) -> np.ndarray:
+        out = np.zeros((self.nv, self.nv))
+        self.lib.oracle_mass_matrix(self.handle, _dp(np.ascontiguousarray(q, np.float64)), _dp(out))
+        return out
+
+    def point_jacobian(self, q, body: int, local) -> tuple[np.ndarray, np.ndarray]:
+        wp = np.zeros(3)
+        J = np.zeros((3, self.nv))
+        self.lib.oracle_point_jacobian(self.handle, _dp(np.ascontiguousarray(q, np.float64)), body,
+                                       _dp(np.ascontiguousarray(local, np.float64)), _dp(wp), _dp(J))
+        return wp, J
+
+    def drive_efforts(self, q, v, actions) -> np.ndarray:
+        out = np.zeros(self.nv)
+        self.lib.oracle_drive_efforts(self.handle, _dp(np.ascontiguousarray(q, np.float64)), _dp(np.ascontiguousarray(v, np.float64)),
+                                      _dp(np.ascontiguousarray(actions, np.float64)), _dp(out))
+        return out
+
+    def project_cone(self, impulse, mu_u: float, mu_v: float) -> np.ndarray:
+        out = np.zeros(3)
+        self.lib.oracle_project_cone(_dp(np.ascontiguousarray(impulse, np.float64)), mu_u, mu_v, _dp(out))
+        return out
+
+    def invert3x3(self, m) -> tuple[bool, np.ndarray]:
+        out = np.zeros(9)
+        ok = self.lib.oracle_invert3x3(_dp(np.ascontiguousarray(m, np.float64).reshape(9)), _dp(out))
+        return bool(ok), out.reshape(3, 3)
+
+    def temporal_cone_dense(self, W, u0, mu, iterations: int, lam0=None) -> np.ndarray:
+        n = len(mu)
+        lam = np.zeros(3 * n) if lam0 is None else np.array(lam0, np.float64)
+        self.lib.oracle_temporal_cone_dense(n, _dp(np.ascontiguousarray(W, np.float64)), _dp(np.ascontiguousarray(u0, np.float64)),
+                                            _dp(np.ascontiguousarray(mu, np.float64)), iterations, _dp(lam))
+        return lam
+
+
+class Reference:
+    """The reference's own FP64 CPU core (compiled from its sources)."""
+
+    def __init__(self, records, h: float, friction: float = 1.0) -> None:
+        if not REF_LIB.is_file():
+            raise FileNotFoundError(f"{REF_LIB} is missing; build it with `make -C oracle ref` where the reference sources exist")
+        lib = ct.CDLL(str(REF_LIB))
+        self.lib = lib
+        lib.ref_model_create.restype = ct.c_void_p
+        lib.ref_model_create.argtypes = [ct.c_void_p] * 6 + [ct.c_double, ct.c_double, ct.c_char_p, ct.c_size_t]
+        lib.ref_model_destroy.argtypes = [ct.c_void_p]
+        lib.ref_forward_dynamics.restype = ct.c_int
+        lib.ref_forward_dynamics.argtypes = [ct.c_void_p, _DP, _DP, _DP, _DP]
+        lib.ref_mass_matrix.restype = ct.c_int
+        lib.ref_mass_matrix.argtypes = [ct.c_void_p, _DP, _DP]
+        lib.ref_point_jacobian.restype = ct.c_int
+        lib.ref_point_jacobian.argtypes = [ct.c_void_p, _DP, ct.c_uint32, _DP, _DP, _DP]
+        lib.ref_integrate.restype = ct.c_int
+        lib.ref_integrate.argtypes = [ct.c_void_p, _DP, _DP, _DP]
+        lib.ref_conic_solve.restype = ct.c_int
+        lib.ref_conic_solve.argtypes = [ct.c_uint32, _DP, _DP, ct.c_uint32, _DP, _DP, _DP, _DP, _DP, _DP, _DP]
+        lib.ref_run.restype = ct.c_double
+        lib.ref_run.argtypes = [ct.c_void_p, ct.c_uint32, _DP, _DP, ct.POINTER(ct.c_float), ct.c_uint32, ct.c_uint32,
+                                ct.c_uint32, ct.c_int, ct.POINTER(ct.c_uint64)]
+        w = records.world
+        self.nq, self.nv = int(w.nq), int(w.nv)
+        err = ct.create_string_buffer(512)
+        self.handle = lib.ref_model_create(
+            ct.byref(records.world), ct.cast(records.joints, ct.c_void_p), ct.cast(records.bodies, ct.c_void_p),
+            ct.cast(records.dofs, ct.c_void_p), ct.cast(records.shapes, ct.c_void_p), ct.cast(records.materials, ct.c_void_p),
+            h, friction, err, len(err))
+        if not self.handle:
+            raise RuntimeError(err.value.decode())
+
+    def __del__(self) -> None:
+        try:
+            if self.handle:
+                self.lib.ref_model_destroy(self.handle)
+        except Exception:
+            pass
+
+    def forward_dynamics(self, q, v, tau) -> tuple[int, np.ndarray]:
+        out = np.zeros(self.nv)
+        st = self.lib.ref_forward_dynamics(self.handle, _dp(np.ascontiguousarray(q, np.float64)), _dp(np.ascontiguousarray(v, np.float64)),
+                                           _dp(np.ascontiguousarray(tau, np.float64)), _dp(out))
+        return st, out
+
+    def mass_matrix(self, q) -> np.ndarray:
+        out = np.zeros((self.nv, self.nv))
+        self.lib.ref_mass_matrix(self.handle, _dp(np.ascontiguousarray(q, np.float64)), _dp(out))
+        return out
+
+    def point_jacobian(self, q, body: int, local) -> tuple[np.ndarray, np.ndarray]:
+        wp = np.zeros(3)
+        J = np.zeros((3, self.nv))
+        self.lib.ref_point_jacobian(self.handle, _dp(np.ascontiguousarray(q, np.float64)), body,
+                                    _dp(np.ascontiguousarray(local, np.float64)), _dp(wp), _dp(J))
+        return wp, J
+
+    def integrate(self, q, v, tau) -> int:
+        return self.lib.ref_integrate(self.handle, _dp(q), _dp(v), _dp(np.ascontiguousarray(tau, np.float64)))
+
+    def conic_solve(self, inverse_mass, free_velocity, jac, mu, target, reg):
+        n = len(mu)
+        imp = np.zeros(3 * n)
+        vel = np.zeros(self.nv if inverse_mass.shape[0] == self.nv else inverse_mass.shape[0])
+        viol = ct.c_double(0.0)
+        nv = inverse_mass.shape[0]
+        st = self.lib.ref_conic_solve(nv, _dp(np.ascontiguousarray(inverse_mass, np.float64)),
+                                      _dp(np.ascontiguousarray(free_velocity, np.float64)), n,
+                                      _dp(np.ascontiguousarray(jac, np.float64)), _dp(np.ascontiguousarray(mu, np.float64)),
+                                      _dp(np.ascontiguousarray(target, np.float64)), _dp(np.ascontiguousarray(reg, np.float64)),
+                                      _dp(imp), _dp(vel), ct.byref(viol))
+        return st, imp, vel, viol.value
+
+    def run(self, q: np.ndarray, v: np.ndarray, actions: np.ndarray, substeps: int, threads: int, solver: int = 1):
+        """Steps every env for actions.shape[0] control steps; returns (seconds, failed)."""
+
+        envs = q.shape[0]
+        steps = actions.shape[0]
+        failed = ct.c_uint64(0)
+        acts = np.ascontiguousarray(actions, np.float32)
+        secs = self.lib.ref_run(self.handle, envs, _dp(q), _dp(v), acts.ctypes.data_as(ct.POINTER(ct.c_float)), steps, substeps,
+                                threads, solver, ct.byref(failed))
+        return secs, int(failed.value)

@@ -1,0 +1,1342 @@
+/*
+ * ORACLE — test infrastructure only (see oracle.h).  FP64 restatement of
+ * numi-lab's microstep.  Function comments cite the reference file:line
+ * each one follows.  Nothing here is part of the product library.
+ */
+#include "oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define MAXB MR_B200_MAX_BODIES
+#define MAXV MR_B200_MAX_DOFS
+#define MAXQ MR_B200_MAX_Q
+#define MAXS MR_B200_MAX_SHAPES
+#define MAXP MR_B200_MAX_PAIRS
+#define MAXC MR_B200_MAX_CONTACTS
+#define MPTS ((int)MR_B200_MANIFOLD_POINTS)
+
+static const double kFloatEps = 1.1920928955078125e-7; /* float epsilon, as the reference's pivot floors */
+static const double kPivotFloor = 1.0e-12;
+static const double kMatrixFloor = 1.0e-10;
+static const double kCfm = 1.0e-2;
+static const double kPad = 0.00000762939453125;
+
+struct OracleWorld {
+    MRModelWorldC w;
+    MRModelJointC joints[MAXB];
+    MRModelBodyC bodies[MAXB + 8];
+    MRModelDofC dofs[MAXV];
+    MRModelShapeC shapes[MAXS];
+    MRModelMaterialC materials[8];
+    MRModelPairC pairs[MAXP];
+    uint32_t nb;            /* articulated bodies */
+    double h;
+    uint32_t substeps, iters, final_iters;
+    int floating;
+    int body_dof[MAXB];     /* -1 when none */
+    double arm_eff[MAXV];
+    int action_dof[MAXV];
+};
+
+/* ------------------------------------------------------------------ */
+/* Small vector helpers                                                 */
+/* ------------------------------------------------------------------ */
+typedef struct { double x, y, z; } v3;
+typedef struct { double x, y, z, w; } q4;
+
+static v3 V(double x, double y, double z) { v3 r = {x, y, z}; return r; }
+static v3 vadd(v3 a, v3 b) { return V(a.x + b.x, a.y + b.y, a.z + b.z); }
+static v3 vsub(v3 a, v3 b) { return V(a.x - b.x, a.y - b.y, a.z - b.z); }
+static v3 vmul(v3 a, double s) { return V(a.x * s, a.y * s, a.z * s); }
+static double vdot(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static v3 vcross(v3 a, v3 b) { return V(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+static double vlen(v3 a) { return sqrt(vdot(a, a)); }
+static double vmaxabs(v3 a) { return fmax(fmax(fabs(a.x), fabs(a.y)), fabs(a.z)); }
+static int vfinite(v3 a) { return isfinite(a.x) && isfinite(a.y) && isfinite(a.z); }
+static v3 vld(const double* p) { return V(p[0], p[1], p[2]); }
+static v3 vldf(const float* p) { return V(p[0], p[1], p[2]); }
+static void vst(double* p, v3 a) { p[0] = a.x; p[1] = a.y; p[2] = a.z; }
+static double vget(v3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
+
+static q4 Q(double x, double y, double z, double w) { q4 r = {x, y, z, w}; return r; }
+static q4 qconj(q4 q) { return Q(-q.x, -q.y, -q.z, q.w); }
+static q4 qmul(q4 l, q4 r) {
+    return Q(l.w * r.x + l.x * r.w + l.y * r.z - l.z * r.y, l.w * r.y - l.x * r.z + l.y * r.w + l.z * r.x,
+             l.w * r.z + l.x * r.y - l.y * r.x + l.z * r.w, l.w * r.w - (l.x * r.x + l.y * r.y + l.z * r.z));
+}
+static v3 qrot(q4 q, v3 v) {
+    const v3 u = V(q.x, q.y, q.z);
+    const v3 t = vmul(vcross(u, v), 2.0);
+    return vadd(vadd(v, vmul(t, q.w)), vcross(u, t));
+}
+static v3 qrotinv(q4 q, v3 v) { return qrot(qconj(q), v); }
+static int qfinite(q4 q) { return isfinite(q.x) && isfinite(q.y) && isfinite(q.z) && isfinite(q.w); }
+static double qdot(q4 a, q4 b) { return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w; }
+static q4 qldf(const float* p) { return Q(p[0], p[1], p[2], p[3]); }
+
+/* normalizedQuaternion (ArticulatedABA.metal:101-121). */
+static int qnormalize(q4 in, q4* out, int require_unit) {
+    if (!qfinite(in)) return 0;
+    const double n2 = qdot(in, in);
+    if (!(n2 > 1.0e-12) || !isfinite(n2)) return 0;
+    const double n = sqrt(n2);
+    if (require_unit && fabs(n - 1.0) > 2.0e-5) return 0;
+    *out = Q(in.x / n, in.y / n, in.z / n, in.w / n);
+    return qfinite(*out);
+}
+
+/* SO(3) exponential increment (ArticulatedABA.metal:1469-1481 with angle
+ * reduction; MetalWorldContact.metal:8919-8930 without). */
+static q4 so3_increment(v3 rv, int reduce) {
+    const double angle = vlen(rv);
+    const double two_pi = 6.28318530717958647692;
+    const double reduced = (reduce && angle > two_pi) ? fmod(angle, two_pi) : angle;
+    const double half = 0.5 * reduced;
+    const double s = angle > 1.0e-6 ? sin(half) / angle : 0.5 - angle * angle / 48.0;
+    return Q(rv.x * s, rv.y * s, rv.z * s, cos(half));
+}
+
+static int sym6(int i, int j) { return i >= j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i; }
+
+/* ------------------------------------------------------------------ */
+/* World construction                                                   */
+/* ------------------------------------------------------------------ */
+OracleWorld* oracle_world_create(const MRModelWorldC* world, const MRModelJointC* joints, const MRModelBodyC* bodies,
+                                 const MRModelDofC* dofs, const MRModelShapeC* shapes, const MRModelMaterialC* materials,
+                                 const MRModelPairC* pairs, double h, uint32_t substeps, uint32_t velocity_iterations,
+                                 uint32_t final_velocity_iterations) {
+    if (!world || world->body_count > MAXB + 8 || world->nv > MAXV || world->nq > MAXQ || world->shape_count > MAXS ||
+        world->pair_count > MAXP || world->material_count > 8)
+        return NULL;
+    OracleWorld* o = (OracleWorld*)calloc(1, sizeof(OracleWorld));
+    if (!o) return NULL;
+    o->w = *world;
+    memcpy(o->joints, joints, sizeof(MRModelJointC) * world->joint_count);
+    memcpy(o->bodies, bodies, sizeof(MRModelBodyC) * world->body_count);
+    memcpy(o->dofs, dofs, sizeof(MRModelDofC) * world->nv);
+    if (world->shape_count) memcpy(o->shapes, shapes, sizeof(MRModelShapeC) * world->shape_count);
+    if (world->material_count) memcpy(o->materials, materials, sizeof(MRModelMaterialC) * world->material_count);
+    if (world->pair_count) memcpy(o->pairs, pairs, sizeof(MRModelPairC) * world->pair_count);
+    o->nb = 0;
+    while (o->nb < world->body_count && bodies[o->nb].articulated) o->nb++;
+    o->h = h;
+    o->substeps = substeps;
+    o->iters = velocity_iterations;
+    o->final_iters = final_velocity_iterations;
+    o->floating = world->root_type == MR_ROOT_FLOATING;
+    for (uint32_t b = 0; b < MAXB; ++b) o->body_dof[b] = -1;
+    for (uint32_t b = 1; b < o->nb; ++b) {
+        const MRModelJointC* j = &joints[bodies[b].inbound_joint];
+        if (j->joint_type != MR_JOINT_FIXED) o->body_dof[b] = (int)j->v_index;
+    }
+    const int implicit = world->actuation_mode == MR_ACTUATION_IMPLICIT_POSITION;
+    int a = 0;
+    for (uint32_t k = 0; k < world->nv; ++k) {
+        /* effectiveArmature (ArticulatedABA.metal:301-316). */
+        double arm = dofs[k].drive[2];
+        if (implicit && (dofs[k].flags & MR_DOF_FLAG_DRIVE))
+            arm += h * (double)dofs[k].drive[1] + h * h * (double)dofs[k].drive[0];
+        o->arm_eff[k] = arm;
+        if ((dofs[k].flags & MR_DOF_FLAG_ACTUATED) && a < (int)world->action_count) o->action_dof[a++] = (int)k;
+    }
+    return o;
+}
+
+void oracle_world_destroy(OracleWorld* world) { free(world); }
+
+/* ------------------------------------------------------------------ */
+/* Drives (MetalWorld.metal:280-370; default actuator profile of       */
+/* MetalWorld.mm:1376-1411 makes the envelope min(limit, stall)).      */
+/* ------------------------------------------------------------------ */
+void oracle_drive_efforts(const OracleWorld* o, const double* q, const double* v, const double* actions, double* tau) {
+    double tgt[MAXV];
+    for (uint32_t k = 0; k < o->w.nv; ++k) tgt[k] = 0.0;
+    for (uint32_t a = 0; a < o->w.action_count; ++a) tgt[o->action_dof[a]] = actions[a];
+    const int implicit = o->w.actuation_mode == MR_ACTUATION_IMPLICIT_POSITION;
+    for (uint32_t k = 0; k < o->w.nv; ++k) {
+        const MRModelDofC* d = &o->dofs[k];
+        const double vel = v[k];
+        double command = tgt[k];
+        if (implicit) {
+            command = 0.0;
+            if ((d->flags & MR_DOF_FLAG_DRIVE) && d->q_index != MR_INVALID_INDEX) {
+                double target = tgt[k];
+                if (d->flags & MR_DOF_FLAG_POSITION_LIMIT) target = fmin(fmax(target, d->limits[0]), d->limits[1]);
+                command = d->drive[0] * (target - q[d->q_index] - o->h * vel) - d->drive[1] * vel;
+                const double dry = d->drive[3];
+                if (dry > 0.0) {
+                    if (fabs(vel) > 1.0e-4) command -= copysign(dry, vel);
+                    else command -= fmin(fmax(command, -dry), dry);
+                }
+                if ((d->flags & MR_DOF_FLAG_EFFORT_LIMIT) && d->limits[3] > 0.0f)
+                    command = fmin(fmax(command, -d->limits[3]), d->limits[3]);
+            }
+        }
+        const double stall = ((d->flags & MR_DOF_FLAG_EFFORT_LIMIT) && d->limits[3] > 0.0f) ? d->limits[3] : FLT_MAX;
+        const double envelope = fmin(d->limits[3], stall);
+        tau[k] = fmin(fmax(command, -envelope), envelope);
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* Kinematics + ABA in the reference formulation: per-body COM frames,  */
+/* classical accelerations, 21-entry symmetric inertias, traversal in   */
+/* joint order (ArticulatedABA.metal:352-1578).                        */
+/* ------------------------------------------------------------------ */
+typedef struct {
+    v3 pos[MAXB];
+    q4 rot[MAXB];
+    v3 w[MAXB];
+    v3 v[MAXB];
+    v3 ma[MAXB], ml[MAXB];   /* motion subspace */
+    v3 ba[MAXB], bl[MAXB];   /* velocity-product bias accelerations */
+    v3 r[MAXB];              /* parent COM -> body COM */
+    v3 joint_pos[MAXB];
+    v3 joint_axis[MAXB];
+} Kin;
+
+static uint32_t kinematics(const OracleWorld* o, const double* q, const double* v, Kin* k) {
+    const uint32_t nb = o->nb;
+    for (uint32_t i = 0; i < o->w.nq; ++i)
+        if (!isfinite(q[i])) return MR_STEP_NONFINITE_INPUT;
+    for (uint32_t i = 0; i < o->w.nv; ++i)
+        if (!isfinite(v[i])) return MR_STEP_NONFINITE_INPUT;
+    if (o->floating) {
+        q4 rq;
+        const v3 p = V(q[0], q[1], q[2]);
+        if (!vfinite(p) || !qnormalize(Q(q[3], q[4], q[5], q[6]), &rq, 1)) return MR_STEP_NONFINITE_INPUT;
+        k->pos[0] = p;
+        k->rot[0] = rq;
+        k->v[0] = V(v[0], v[1], v[2]);
+        k->w[0] = V(v[3], v[4], v[5]);
+    } else {
+        k->pos[0] = V(0, 0, 0);
+        k->rot[0] = Q(0, 0, 0, 1);
+        k->v[0] = V(0, 0, 0);
+        k->w[0] = V(0, 0, 0);
+    }
+    k->r[0] = V(0, 0, 0);
+    k->ma[0] = k->ml[0] = k->ba[0] = k->bl[0] = V(0, 0, 0);
+    for (uint32_t b = 1; b < nb; ++b) {
+        const MRModelJointC* j = &o->joints[o->bodies[b].inbound_joint];
+        const uint32_t p = j->parent_body;
+        q4 prot, crot;
+        if (!qnormalize(qldf(j->parent_rotation), &prot, 1) || !qnormalize(qldf(j->child_rotation), &crot, 1))
+            return MR_STEP_UNSUPPORTED;
+        const q4 pj = qmul(k->rot[p], prot);
+        v3 axis = V(1, 0, 0);
+        q4 motion = Q(0, 0, 0, 1);
+        double qj = 0.0, qdj = 0.0;
+        const int dof = o->body_dof[b];
+        if (dof >= 0) {
+            axis = vldf(j->axis);
+            axis = vmul(axis, 1.0 / vlen(axis));
+            qj = q[j->q_index];
+            qdj = v[dof];
+            if (j->joint_type == MR_JOINT_REVOLUTE || j->joint_type == MR_JOINT_CONTINUOUS) {
+                const double hh = 0.5 * qj;
+                motion = Q(axis.x * sin(hh), axis.y * sin(hh), axis.z * sin(hh), cos(hh));
+            }
+        }
+        q4 rc;
+        if (!qnormalize(qmul(qmul(pj, motion), qconj(crot)), &rc, 0)) return MR_STEP_NONFINITE_RESULT;
+        k->rot[b] = rc;
+        const v3 ja = qrot(pj, axis);
+        const int prismatic = j->joint_type == MR_JOINT_PRISMATIC;
+        v3 jp = vadd(k->pos[p], qrot(k->rot[p], vldf(j->parent_anchor)));
+        if (prismatic) jp = vadd(jp, vmul(ja, qj));
+        const v3 ca = qrot(rc, vldf(j->child_anchor));
+        k->pos[b] = vsub(jp, ca);
+        k->r[b] = vsub(k->pos[b], k->pos[p]);
+        k->joint_pos[b] = jp;
+        k->joint_axis[b] = ja;
+        const v3 ptj = vsub(jp, k->pos[p]);
+        const int has = dof >= 0;
+        k->w[b] = vadd(k->w[p], (!prismatic && has) ? vmul(ja, qdj) : V(0, 0, 0));
+        k->v[b] = vsub(vadd(vadd(k->v[p], vcross(k->w[p], ptj)), prismatic ? vmul(ja, qdj) : V(0, 0, 0)), vcross(k->w[b], ca));
+        k->ma[b] = (has && !prismatic) ? ja : V(0, 0, 0);
+        k->ml[b] = prismatic ? ja : (has ? vmul(vcross(ja, ca), -1.0) : V(0, 0, 0));
+        k->ba[b] = (has && !prismatic) ? vmul(vcross(k->w[p], ja), qdj) : V(0, 0, 0);
+        const v3 pc = prismatic ? vmul(vcross(k->w[p], ja), 2.0 * qdj) : V(0, 0, 0);
+        k->bl[b] = vsub(vsub(vadd(vcross(k->w[p], vcross(k->w[p], ptj)), pc), vcross(k->ba[b], ca)), vcross(k->w[b], vcross(k->w[b], ca)));
+        if (!vfinite(k->pos[b]) || !vfinite(k->w[b]) || !vfinite(k->v[b]) || !vfinite(k->bl[b])) return MR_STEP_NONFINITE_RESULT;
+    }
+    return MR_STEP_SUCCESS;
+}
+
+/* World inertia about the COM: R I R^T. */
+static void world_inertia(const MRModelBodyC* body, q4 rot, double Iw[3][3]) {
+    const v3 c[3] = {qrot(rot, V(1, 0, 0)), qrot(rot, V(0, 1, 0)), qrot(rot, V(0, 0, 1))};
+    double R[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) R[i][j] = vget(c[j], i);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double acc = 0.0;
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) acc += R[i][a] * (double)body->inertia[a][b] * R[j][b];
+            Iw[i][j] = acc;
+        }
+}
+
+static double mte(v3 r, int row, int col) { /* motionTransformElement (ArticulatedABA.metal:160-190) */
+    if (row == col) return 1.0;
+    if (row < 3 || col >= 3) return 0.0;
+    const int lr = row - 3;
+    if (lr == 0 && col == 1) return r.z;
+    if (lr == 0 && col == 2) return -r.y;
+    if (lr == 1 && col == 0) return -r.z;
+    if (lr == 1 && col == 2) return r.x;
+    if (lr == 2 && col == 0) return r.y;
+    if (lr == 2 && col == 1) return -r.x;
+    return 0.0;
+}
+
+static double spatial(v3 a, v3 l, int i) { return i < 3 ? vget(a, i) : vget(l, i - 3); }
+
+static uint32_t aba_core(const OracleWorld* o, const double* q, const double* v, const double* tau, const Kin* k, double* qdd) {
+    const uint32_t nb = o->nb;
+    double IA[MAXB][21], PA[MAXB][6], U[MAXB][6], D[MAXB], Ures[MAXB];
+    for (uint32_t b = 0; b < nb; ++b) {
+        const MRModelBodyC* body = &o->bodies[b];
+        double Iw[3][3];
+        world_inertia(body, k->rot[b], Iw);
+        for (int e = 0; e < 21; ++e) IA[b][e] = 0.0;
+        for (int i = 0; i < 3; ++i) {
+            for (int j = 0; j <= i; ++j) IA[b][sym6(i, j)] = Iw[i][j];
+            IA[b][sym6(3 + i, 3 + i)] = body->mass_inverse_mass[0];
+        }
+        const double m = body->mass_inverse_mass[0];
+        const v3 fext = vmul(V(o->w.gravity[0], o->w.gravity[1], o->w.gravity[2]), m);
+        const v3 Iwv = V(Iw[0][0] * k->w[b].x + Iw[0][1] * k->w[b].y + Iw[0][2] * k->w[b].z,
+                         Iw[1][0] * k->w[b].x + Iw[1][1] * k->w[b].y + Iw[1][2] * k->w[b].z,
+                         Iw[2][0] * k->w[b].x + Iw[2][1] * k->w[b].y + Iw[2][2] * k->w[b].z);
+        v3 bt = vcross(k->w[b], Iwv);
+        v3 bf = vmul(fext, -1.0);
+        if (o->w.apply_body_damping) {
+            bt = vadd(bt, vmul(k->w[b], body->damping_speed[1]));
+            bf = vadd(bf, vmul(k->v[b], body->damping_speed[0]));
+        }
+        for (int i = 0; i < 6; ++i) PA[b][i] = spatial(bt, bf, i);
+    }
+    if (o->floating) {
+        for (int a = 0; a < 3; ++a) {
+            IA[0][sym6(3 + a, 3 + a)] += o->arm_eff[a];
+            IA[0][sym6(a, a)] += o->arm_eff[3 + a];
+            PA[0][a] -= tau[3 + a];
+            PA[0][3 + a] -= tau[a];
+        }
+    }
+    for (uint32_t b = nb - 1; b >= 1; --b) {
+        const uint32_t p = o->bodies[b].parent_body;
+        double prop[6];
+        for (int i = 0; i < 6; ++i) {
+            double s = 0.0;
+            for (int j = 0; j < 6; ++j) s += IA[b][sym6(i, j)] * spatial(k->ba[b], k->bl[b], j);
+            prop[i] = PA[b][i] + s;
+        }
+        const int dof = o->body_dof[b];
+        if (dof >= 0) {
+            double S[6], Ub[6];
+            for (int i = 0; i < 6; ++i) S[i] = spatial(k->ma[b], k->ml[b], i);
+            for (int i = 0; i < 6; ++i) {
+                double s = 0.0;
+                for (int j = 0; j < 6; ++j) s += IA[b][sym6(i, j)] * S[j];
+                Ub[i] = s;
+            }
+            double den = o->arm_eff[dof];
+            for (int i = 0; i < 6; ++i) den += S[i] * Ub[i];
+            double maxI = 0.0;
+            for (int e = 0; e < 21; ++e) maxI = fmax(maxI, fabs(IA[b][e]));
+            if (!(den > fmax(kPivotFloor, maxI * 6.0 * kFloatEps)) || !isfinite(den)) return MR_STEP_FACTORIZATION_FAILED;
+            double res = tau[dof];
+            for (int i = 0; i < 6; ++i) res -= S[i] * prop[i];
+            D[b] = den;
+            Ures[b] = res;
+            for (int i = 0; i < 6; ++i) { U[b][i] = Ub[i]; prop[i] += Ub[i] * (res / den); }
+            for (int i = 0; i < 6; ++i)
+                for (int j = 0; j <= i; ++j) IA[b][sym6(i, j)] -= Ub[i] * Ub[j] / den;
+        }
+        const v3 r = k->r[b];
+        for (int i = 0; i < 6; ++i)
+            for (int j = 0; j <= i; ++j) {
+                double t = 0.0;
+                for (int l = 0; l < 6; ++l) {
+                    const double xl = mte(r, l, i);
+                    if (xl == 0.0) continue;
+                    for (int m = 0; m < 6; ++m) t += xl * IA[b][sym6(l, m)] * mte(r, m, j);
+                }
+                IA[p][sym6(i, j)] += t;
+            }
+        v3 pt = V(prop[0], prop[1], prop[2]);
+        const v3 pf = V(prop[3], prop[4], prop[5]);
+        pt = vadd(pt, vcross(r, pf));
+        for (int i = 0; i < 6; ++i) PA[p][i] += spatial(pt, pf, i);
+    }
+    v3 aa[MAXB], al[MAXB];
+    if (o->floating) {
+        double L[36] = {0}, y[6], x[6];
+        double maxI = 0.0;
+        for (int e = 0; e < 21; ++e) maxI = fmax(maxI, fabs(IA[0][e]));
+        const double floor = fmax(kPivotFloor, maxI * 6.0 * kFloatEps);
+        for (int i = 0; i < 6; ++i)
+            for (int j = 0; j <= i; ++j) {
+                double val = IA[0][sym6(i, j)];
+                for (int m = 0; m < j; ++m) val -= L[i * 6 + m] * L[j * 6 + m];
+                if (i == j) {
+                    if (!(val > floor) || !isfinite(val)) return MR_STEP_FACTORIZATION_FAILED;
+                    L[i * 6 + i] = sqrt(val);
+                } else {
+                    L[i * 6 + j] = val / L[j * 6 + j];
+                }
+            }
+        for (int i = 0; i < 6; ++i) {
+            double val = -PA[0][i];
+            for (int m = 0; m < i; ++m) val -= L[i * 6 + m] * y[m];
+            y[i] = val / L[i * 6 + i];
+        }
+        for (int i = 5; i >= 0; --i) {
+            double val = y[i];
+            for (int m = i + 1; m < 6; ++m) val -= L[m * 6 + i] * x[m];
+            x[i] = val / L[i * 6 + i];
+        }
+        aa[0] = V(x[0], x[1], x[2]);
+        al[0] = V(x[3], x[4], x[5]);
+        qdd[0] = x[3]; qdd[1] = x[4]; qdd[2] = x[5];
+        qdd[3] = x[0]; qdd[4] = x[1]; qdd[5] = x[2];
+    } else {
+        aa[0] = al[0] = V(0, 0, 0);
+    }
+    for (uint32_t b = 1; b < nb; ++b) {
+        const uint32_t p = o->bodies[b].parent_body;
+        const v3 tpa = aa[p];
+        const v3 tpl = vadd(al[p], vcross(aa[p], k->r[b]));
+        v3 ang = vadd(tpa, k->ba[b]);
+        v3 lin = vadd(tpl, k->bl[b]);
+        const int dof = o->body_dof[b];
+        if (dof >= 0) {
+            double pp = 0.0;
+            for (int i = 0; i < 6; ++i) pp += U[b][i] * spatial(tpa, tpl, i);
+            const double acc = (Ures[b] - pp) / D[b];
+            qdd[dof] = acc;
+            ang = vadd(ang, vmul(k->ma[b], acc));
+            lin = vadd(lin, vmul(k->ml[b], acc));
+        }
+        aa[b] = ang;
+        al[b] = lin;
+    }
+    for (uint32_t d = 0; d < o->w.nv; ++d)
+        if (!isfinite(qdd[d])) return MR_STEP_NONFINITE_RESULT;
+    (void)q; (void)v;
+    return MR_STEP_SUCCESS;
+}
+
+uint32_t oracle_aba(const OracleWorld* o, const double* q, const double* v, const double* tau, double* qdd) {
+    Kin k;
+    const uint32_t st = kinematics(o, q, v, &k);
+    if (st != MR_STEP_SUCCESS) return st;
+    return aba_core(o, q, v, tau, &k, qdd);
+}
+
+/* ------------------------------------------------------------------ */
+/* Point Jacobians and the dense mass matrix (analytic tree Jacobians, */
+/* as the reference operator's point-Jacobian mode,                     */
+/* ArticulatedOperator.metal:1139, and M = sum_b J_b^T I_b J_b).        */
+/* ------------------------------------------------------------------ */
+static void point_jacobian_k(const OracleWorld* o, const Kin* k, uint32_t body, v3 x, double* J /* 3 x nv */) {
+    const uint32_t nv = o->w.nv;
+    for (uint32_t i = 0; i < 3 * nv; ++i) J[i] = 0.0;
+    uint32_t b = body;
+    while (b != 0 && b != MR_INVALID_INDEX) {
+        const int dof = o->body_dof[b];
+        if (dof >= 0) {
+            const MRModelJointC* j = &o->joints[o->bodies[b].inbound_joint];
+            v3 col;
+            if (j->joint_type == MR_JOINT_PRISMATIC) col = k->joint_axis[b];
+            else col = vcross(k->joint_axis[b], vsub(x, k->joint_pos[b]));
+            J[0 * nv + dof] = col.x; J[1 * nv + dof] = col.y; J[2 * nv + dof] = col.z;
+        }
+        b = o->bodies[b].parent_body;
+    }
+    if (o->floating) {
+        const v3 rr = vsub(x, k->pos[0]);
+        for (int a = 0; a < 3; ++a) {
+            J[a * nv + a] = 1.0;
+            const v3 e = V(a == 0, a == 1, a == 2);
+            const v3 col = vcross(e, rr);
+            J[0 * nv + 3 + a] = col.x; J[1 * nv + 3 + a] = col.y; J[2 * nv + 3 + a] = col.z;
+        }
+    }
+}
+
+static void angular_jacobian_k(const OracleWorld* o, const Kin* k, uint32_t body, double* J /* 3 x nv */) {
+    const uint32_t nv = o->w.nv;
+    for (uint32_t i = 0; i < 3 * nv; ++i) J[i] = 0.0;
+    uint32_t b = body;
+    while (b != 0 && b != MR_INVALID_INDEX) {
+        const int dof = o->body_dof[b];
+        if (dof >= 0) {
+            const MRModelJointC* j = &o->joints[o->bodies[b].inbound_joint];
+            if (j->joint_type != MR_JOINT_PRISMATIC) {
+                J[0 * nv + dof] = k->joint_axis[b].x; J[1 * nv + dof] = k->joint_axis[b].y; J[2 * nv + dof] = k->joint_axis[b].z;
+            }
+        }
+        b = o->bodies[b].parent_body;
+    }
+    if (o->floating)
+        for (int a = 0; a < 3; ++a) J[a * nv + 3 + a] = 1.0;
+}
+
+static void mass_matrix_k(const OracleWorld* o, const Kin* k, double* Mm) {
+    const uint32_t nv = o->w.nv;
+    double Jv[3 * MAXV], Jw[3 * MAXV];
+    for (uint32_t i = 0; i < nv * nv; ++i) Mm[i] = 0.0;
+    for (uint32_t b = 0; b < o->nb; ++b) {
+        const double m = o->bodies[b].mass_inverse_mass[0];
+        double Iw[3][3];
+        world_inertia(&o->bodies[b], k->rot[b], Iw);
+        point_jacobian_k(o, k, b, k->pos[b], Jv);
+        angular_jacobian_k(o, k, b, Jw);
+        if (b == 0 && !o->floating) continue;
+        for (uint32_t i = 0; i < nv; ++i)
+            for (uint32_t j = 0; j < nv; ++j) {
+                double s = 0.0;
+                for (int a = 0; a < 3; ++a) s += m * Jv[a * nv + i] * Jv[a * nv + j];
+                for (int a = 0; a < 3; ++a)
+                    for (int c = 0; c < 3; ++c) s += Jw[a * nv + i] * Iw[a][c] * Jw[c * nv + j];
+                Mm[i * nv + j] += s;
+            }
+    }
+}
+
+uint32_t oracle_mass_matrix(const OracleWorld* o, const double* q, double* mass) {
+    double v0[MAXV] = {0};
+    Kin k;
+    const uint32_t st = kinematics(o, q, v0, &k);
+    if (st != MR_STEP_SUCCESS) return st;
+    mass_matrix_k(o, &k, mass);
+    return MR_STEP_SUCCESS;
+}
+
+uint32_t oracle_point_jacobian(const OracleWorld* o, const double* q, uint32_t body, const double* local_point,
+                               double* world_point, double* jacobian) {
+    double v0[MAXV] = {0};
+    Kin k;
+    const uint32_t st = kinematics(o, q, v0, &k);
+    if (st != MR_STEP_SUCCESS) return st;
+    const v3 x = vadd(k.pos[body], qrot(k.rot[body], vld(local_point)));
+    vst(world_point, x);
+    point_jacobian_k(o, &k, body, x, jacobian);
+    return MR_STEP_SUCCESS;
+}
+
+/* ------------------------------------------------------------------ */
+/* Contact math helpers                                                 */
+/* ------------------------------------------------------------------ */
+void oracle_project_cone(const double* imp, double mu_u, double mu_v, double* out) {
+    /* projectFrictionCone (MetalWorldContact.metal:482-509); no normal cap. */
+    double x = fmax(imp[0], 0.0), y = imp[1], z = imp[2];
+    const double lu = mu_u * x, lv = mu_v * x;
+    if (!(lu > 0.0) || !(lv > 0.0)) {
+        out[0] = x; out[1] = 0.0; out[2] = 0.0;
+        return;
+    }
+    const double ns = (y * y) / (lu * lu) + (z * z) / (lv * lv);
+    if (ns > 1.0) {
+        const double s = 1.0 / sqrt(ns);
+        y *= s;
+        z *= s;
+    }
+    out[0] = x; out[1] = y; out[2] = z;
+}
+
+int oracle_invert3x3(const double* m, double* inv) {
+    /* invert3x3 (MetalWorldContact.metal:540-623). */
+    double scale = 0.0;
+    for (int i = 0; i < 9; ++i) {
+        if (!isfinite(m[i])) return 0;
+        scale = fmax(scale, fabs(m[i]));
+    }
+    if (!(scale > kMatrixFloor)) return 0;
+    double r[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) r[i][j] = 0.5 * (m[i * 3 + j] + m[j * 3 + i]) / scale + (i == j ? kCfm : 0.0);
+    const double c00 = r[1][1] * r[2][2] - r[1][2] * r[2][1];
+    const double c01 = r[1][2] * r[2][0] - r[1][0] * r[2][2];
+    const double c02 = r[1][0] * r[2][1] - r[1][1] * r[2][0];
+    const double det = r[0][0] * c00 + r[0][1] * c01 + r[0][2] * c02;
+    if (!(det > kMatrixFloor) || !isfinite(det)) return 0;
+    const double rc = 1.0 / (det * scale);
+    inv[0] = c00 * rc;
+    inv[1] = (r[0][2] * r[2][1] - r[0][1] * r[2][2]) * rc;
+    inv[2] = (r[0][1] * r[1][2] - r[0][2] * r[1][1]) * rc;
+    inv[3] = c01 * rc;
+    inv[4] = (r[0][0] * r[2][2] - r[0][2] * r[2][0]) * rc;
+    inv[5] = (r[0][2] * r[1][0] - r[0][0] * r[1][2]) * rc;
+    inv[6] = c02 * rc;
+    inv[7] = (r[0][1] * r[2][0] - r[0][0] * r[2][1]) * rc;
+    inv[8] = (r[0][0] * r[1][1] - r[0][1] * r[1][0]) * rc;
+    for (int i = 0; i < 9; ++i)
+        if (!isfinite(inv[i])) return 0;
+    return 1;
+}
+
+static v3 stable_tangent(v3 n) { /* Collision.metal:5133-5145 */
+    const v3 a = V(fabs(n.x), fabs(n.y), fabs(n.z));
+    v3 ref;
+    if (a.x <= a.y && a.x <= a.z) ref = V(1, 0, 0);
+    else if (a.y <= a.z) ref = V(0, 1, 0);
+    else ref = V(0, 0, 1);
+    const v3 t = vcross(ref, n);
+    return vmul(t, 1.0 / vlen(t));
+}
+
+static uint32_t feature_key(uint32_t type, uint32_t local) { return ((type & 0x0fu) << 28u) | (local & 0x0fffffffu); }
+
+/* ------------------------------------------------------------------ */
+/* Collider projection and plane narrowphase (Collision.metal:380-1000, */
+/* 4379-4830, speculative margins :5794-6030).                          */
+/* ------------------------------------------------------------------ */
+typedef struct {
+    uint32_t type;
+    v3 center;
+    q4 rot;
+    v3 body_pos;
+    q4 body_rot;
+    v3 lower, upper, half, ep0, ep1, normal;
+    double radius, half_length, offset;
+} Shape;
+
+static void make_shape(const OracleWorld* o, const Kin* k, uint32_t sh, double margin, Shape* s) {
+    const MRModelShapeC* src = &o->shapes[sh];
+    const MRModelBodyC* body = &o->bodies[src->body];
+    memset(s, 0, sizeof(*s));
+    s->type = src->shape_type;
+    q4 lr;
+    qnormalize(qldf(src->local_rotation), &lr, 0);
+    if (body->articulated) {
+        s->body_pos = k->pos[src->body];
+        s->body_rot = k->rot[src->body];
+    } else {
+        s->body_pos = vldf(body->static_pose);
+        qnormalize(qldf(body->static_pose + 4), &s->body_rot, 0);
+    }
+    s->center = vadd(s->body_pos, qrot(s->body_rot, vldf(src->local_position)));
+    s->rot = qmul(s->body_rot, lr);
+    const double base = src->contact_rest_bound[0];
+    s->offset = base + margin;
+    if (s->type == MR_SHAPE_PLANE) {
+        const v3 n = qrot(s->rot, V(0, 1, 0));
+        s->normal = vmul(n, 1.0 / vlen(n));
+        return;
+    }
+    v3 ext;
+    if (s->type == MR_SHAPE_SPHERE) {
+        s->radius = src->dimensions[0];
+        const double e = s->radius + base;
+        ext = V(e, e, e);
+        s->lower = vsub(s->center, ext);
+        s->upper = vadd(s->center, ext);
+    } else if (s->type == MR_SHAPE_CAPSULE) {
+        s->radius = src->dimensions[0];
+        s->half_length = src->dimensions[1];
+        const v3 ax = qrot(s->rot, V(0, src->dimensions[1], 0));
+        s->ep0 = vsub(s->center, ax);
+        s->ep1 = vadd(s->center, ax);
+        const double e = s->radius + base;
+        s->lower = V(fmin(s->ep0.x, s->ep1.x) - e, fmin(s->ep0.y, s->ep1.y) - e, fmin(s->ep0.z, s->ep1.z) - e);
+        s->upper = V(fmax(s->ep0.x, s->ep1.x) + e, fmax(s->ep0.y, s->ep1.y) + e, fmax(s->ep0.z, s->ep1.z) + e);
+    } else {
+        s->half = vldf(src->dimensions);
+        const v3 bx = qrot(s->rot, V(1, 0, 0)), by = qrot(s->rot, V(0, 1, 0)), bz = qrot(s->rot, V(0, 0, 1));
+        ext = V(fabs(bx.x) * s->half.x + fabs(by.x) * s->half.y + fabs(bz.x) * s->half.z + base,
+                fabs(bx.y) * s->half.x + fabs(by.y) * s->half.y + fabs(bz.y) * s->half.z + base,
+                fabs(bx.z) * s->half.x + fabs(by.z) * s->half.y + fabs(bz.z) * s->half.z + base);
+        s->lower = vsub(s->center, ext);
+        s->upper = vadd(s->center, ext);
+    }
+    const v3 sc = V(fmax(fabs(s->lower.x), fabs(s->upper.x)) + 1.0, fmax(fabs(s->lower.y), fabs(s->upper.y)) + 1.0,
+                    fmax(fabs(s->lower.z), fabs(s->upper.z)) + 1.0);
+    s->lower = vsub(vsub(s->lower, vmul(sc, kPad)), V(margin, margin, margin));
+    s->upper = vadd(vadd(s->upper, vmul(sc, kPad)), V(margin, margin, margin));
+}
+
+static double shape_scale(const Shape* s) { /* worldShapeScale (Collision.metal:125-150) */
+    return fmax(fmax(fmax(vmaxabs(s->center), vmaxabs(s->half)), fmax(vmaxabs(s->ep0), vmaxabs(s->ep1))),
+                fmax(fmax(fabs(s->radius), fabs(s->half_length)), fmax(fabs(s->offset), fmax(vmaxabs(s->lower), vmaxabs(s->upper)))));
+}
+
+typedef struct {
+    v3 normal;
+    double sep;
+    v3 pa, pb;
+    uint32_t fa, fb;
+} Raw;
+
+typedef struct {
+    double la[3], lb[3];
+    uint32_t fa, fb, life;
+    double imp[3];
+    v3 wp;
+    double sep, drift;
+} Cand;
+
+static unsigned long long ckey(const Cand* c) { return ((unsigned long long)c->fa << 32) | c->fb; }
+static int cless(const Cand* a, const Cand* b) {
+    if (a->sep != b->sep) return a->sep < b->sep;
+    return ckey(a) < ckey(b);
+}
+
+/* Pair flag + raw contacts + buildPersistentWorldManifold +
+ * reduceCandidates (Collision.metal:796-850, 4379-4830, 5115-5556). */
+static int pair_manifold(const OracleWorld* o, const Kin* k, const double* margins, uint32_t pair, OracleManifold* slot,
+                         int* candidate) {
+    const MRModelPairC* pr = &o->pairs[pair];
+    Shape A, B;
+    make_shape(o, k, pr->shape_a, margins[pr->shape_a], &A);
+    make_shape(o, k, pr->shape_b, margins[pr->shape_b], &B);
+    const int a_plane = A.type == MR_SHAPE_PLANE;
+    const Shape* plane = a_plane ? &A : &B;
+    const Shape* fin = a_plane ? &B : &A;
+    *candidate = 0;
+    {
+        const v3 c = vmul(vadd(fin->lower, fin->upper), 0.5);
+        const v3 hx = vmul(vsub(fin->upper, fin->lower), 0.5);
+        const double scale = fmax(fmax(vmaxabs(plane->center), vmaxabs(fin->lower)),
+                                  fmax(vmaxabs(fin->upper), fmax(fabs(plane->offset), fabs(fin->offset))));
+        const double qpad = (scale + 1.0) * kPad;
+        const v3 an = V(fabs(plane->normal.x), fabs(plane->normal.y), fabs(plane->normal.z));
+        const double msd = vdot(plane->normal, vsub(c, plane->center)) - vdot(an, hx);
+        if (!(msd <= plane->offset + qpad)) {
+            slot->count = 0;
+            return 0;
+        }
+    }
+    *candidate = 1;
+    const double accepted = A.offset + B.offset + (fmax(shape_scale(&A), shape_scale(&B)) + 1.0) * kPad;
+    Raw raw[8];
+    int nraw = 0;
+#define APPEND(surface, sep_, ffeat)                                                   \
+    do {                                                                               \
+        const v3 pp_ = vsub((surface), vmul(plane->normal, (sep_)));                  \
+        Raw r_;                                                                        \
+        if (!a_plane) {                                                                \
+            r_.normal = vmul(plane->normal, -1.0); r_.pa = (surface); r_.pb = pp_;     \
+            r_.fa = (ffeat); r_.fb = feature_key(MR_SHAPE_PLANE, 0u);                  \
+        } else {                                                                       \
+            r_.normal = plane->normal; r_.pa = pp_; r_.pb = (surface);                 \
+            r_.fa = feature_key(MR_SHAPE_PLANE, 0u); r_.fb = (ffeat);                  \
+        }                                                                              \
+        r_.sep = (sep_);                                                               \
+        raw[nraw++] = r_;                                                              \
+    } while (0)
+    if (pr->pair_class == MR_COLLISION_PAIR_SPHERE_PLANE) {
+        const v3 surface = vsub(fin->center, vmul(plane->normal, fin->radius));
+        const double sep = vdot(plane->normal, vsub(surface, plane->center));
+        if (sep <= accepted) APPEND(surface, sep, feature_key(MR_SHAPE_SPHERE, 0u));
+    } else if (pr->pair_class == MR_COLLISION_PAIR_CAPSULE_PLANE) {
+        for (uint32_t e = 0; e < 2; ++e) {
+            const v3 surface = vsub(e == 0 ? fin->ep0 : fin->ep1, vmul(plane->normal, fin->radius));
+            const double sep = vdot(plane->normal, vsub(surface, plane->center));
+            if (sep <= accepted) APPEND(surface, sep, feature_key(MR_SHAPE_CAPSULE, e));
+        }
+    } else if (pr->pair_class == MR_COLLISION_PAIR_BOX_PLANE) {
+        for (uint32_t vtx = 0; vtx < 8; ++vtx) {
+            const v3 local = V((vtx & 1) ? fin->half.x : -fin->half.x, (vtx & 2) ? fin->half.y : -fin->half.y,
+                               (vtx & 4) ? fin->half.z : -fin->half.z);
+            const v3 wpt = vadd(fin->center, qrot(fin->rot, local));
+            const double sep = vdot(plane->normal, vsub(wpt, plane->center));
+            if (sep <= accepted) APPEND(wpt, sep, feature_key(MR_SHAPE_BOX, vtx));
+        }
+    }
+#undef APPEND
+    if (nraw == 0) {
+        slot->count = 0;
+        return 0;
+    }
+    int deepest = 0;
+    for (int i = 1; i < nraw; ++i) {
+        const Raw* l = &raw[i];
+        const Raw* r = &raw[deepest];
+        if (l->sep < r->sep || (l->sep == r->sep && (l->fa < r->fa || (l->fa == r->fa && l->fb < r->fb)))) deepest = i;
+    }
+    v3 nw = raw[deepest].normal;
+    nw = vmul(nw, 1.0 / vlen(nw));
+    const v3 posA = A.body_pos, posB = B.body_pos;
+    const q4 rotA = A.body_rot, rotB = B.body_rot;
+    const double* thr = NULL;
+    double thr_d[4];
+    for (int i = 0; i < 4; ++i) thr_d[i] = o->w.manifold_thresholds[i];
+    thr = thr_d;
+    Cand c[12];
+    int nc = 0;
+    int old_ok = 0;
+    v3 transported = V(0, 0, 0);
+    double old_age = 0.0;
+    if (slot->count > 0 && slot->count <= MPTS) {
+        v3 on = qrot(rotA, vld(slot->normal_local));
+        on = vmul(on, 1.0 / vlen(on));
+        old_ok = vfinite(on) && vdot(on, nw) >= thr[3];
+        if (old_ok) {
+            const v3 ot = qrot(rotA, vld(slot->tangent_local));
+            transported = vsub(ot, vmul(nw, vdot(ot, nw)));
+            old_age = slot->age;
+            for (uint32_t i = 0; i < slot->count; ++i) {
+                const OraclePoint* op = &slot->points[i];
+                const v3 pa = vadd(posA, qrot(rotA, vld(op->anchor_a)));
+                const v3 pb = vadd(posB, qrot(rotB, vld(op->anchor_b)));
+                const v3 d = vsub(pb, pa);
+                const double sep = vdot(d, nw);
+                const double drift = vlen(vsub(d, vmul(nw, sep)));
+                if (sep > thr[0] || drift > thr[1]) continue;
+                Cand* cc = &c[nc++];
+                for (int a = 0; a < 3; ++a) { cc->la[a] = op->anchor_a[a]; cc->lb[a] = op->anchor_b[a]; cc->imp[a] = op->impulses[a]; }
+                cc->fa = op->feature_a;
+                cc->fb = op->feature_b;
+                cc->life = op->life == 0xffffffffu ? 0xffffffffu : op->life + 1u;
+                cc->wp = vmul(vadd(pa, pb), 0.5);
+                cc->sep = sep;
+                cc->drift = drift;
+            }
+        }
+    }
+    const double merge2 = thr[2] * thr[2];
+    for (int i = 0; i < nraw; ++i) {
+        const Raw* r = &raw[i];
+        const v3 la = qrotinv(rotA, vsub(r->pa, posA));
+        const v3 lb = qrotinv(rotB, vsub(r->pb, posB));
+        int match = -1;
+        for (int m = 0; m < nc; ++m)
+            if (c[m].fa == r->fa && c[m].fb == r->fb) { match = m; break; }
+        if (match < 0)
+            for (int m = 0; m < nc; ++m) {
+                const v3 da = vsub(vld(c[m].la), la), db = vsub(vld(c[m].lb), lb);
+                if (vdot(da, da) + vdot(db, db) <= 2.0 * merge2) { match = m; break; }
+            }
+        if (match < 0) {
+            if (nc >= 12) return -1;
+            match = nc++;
+            c[match].life = 0u;
+            c[match].imp[0] = c[match].imp[1] = c[match].imp[2] = 0.0;
+        }
+        vst(c[match].la, la);
+        vst(c[match].lb, lb);
+        c[match].fa = r->fa;
+        c[match].fb = r->fb;
+        c[match].wp = vmul(vadd(r->pa, r->pb), 0.5);
+        c[match].sep = r->sep;
+        c[match].drift = 0.0;
+    }
+    for (int i = 1; i < nc; ++i) {
+        Cand val = c[i];
+        int d = i;
+        while (d > 0 && cless(&val, &c[d - 1])) { c[d] = c[d - 1]; --d; }
+        c[d] = val;
+    }
+    if (nc > MPTS) {
+        int selected[12] = {0}, chosen[MPTS], count = 1;
+        chosen[0] = 0;
+        selected[0] = 1;
+        for (int stage = 1; stage < MPTS; ++stage) {
+            int best = -1;
+            double best_score = -1.0;
+            unsigned long long best_f = ~0ull;
+            for (int i = 0; i < nc; ++i) {
+                if (selected[i]) continue;
+                double score;
+                if (stage == 1) {
+                    const v3 d = vsub(c[i].wp, c[chosen[0]].wp);
+                    const v3 t = vsub(d, vmul(nw, vdot(d, nw)));
+                    score = vdot(t, t);
+                } else if (stage == 2) {
+                    const v3 a = vsub(c[chosen[1]].wp, c[chosen[0]].wp);
+                    const v3 bb = vsub(c[i].wp, c[chosen[0]].wp);
+                    score = fabs(vdot(vcross(a, bb), nw));
+                } else {
+                    score = INFINITY;
+                    for (int s = 0; s < count; ++s) {
+                        const v3 d = vsub(c[i].wp, c[chosen[s]].wp);
+                        const v3 t = vsub(d, vmul(nw, vdot(d, nw)));
+                        score = fmin(score, vdot(t, t));
+                    }
+                }
+                const unsigned long long f = ckey(&c[i]);
+                if (score > best_score + 1.0e-12 || (fabs(score - best_score) <= 1.0e-12 && f < best_f)) {
+                    best = i; best_score = score; best_f = f;
+                }
+            }
+            if (best >= 0) { chosen[count++] = best; selected[best] = 1; }
+        }
+        Cand red[MPTS];
+        for (int i = 0; i < count; ++i) red[i] = c[chosen[i]];
+        nc = count;
+        for (int i = 0; i < nc; ++i) c[i] = red[i];
+    }
+    for (int i = 1; i < nc; ++i) {
+        Cand val = c[i];
+        const unsigned long long f = ckey(&val);
+        int d = i;
+        while (d > 0 && f < ckey(&c[d - 1])) { c[d] = c[d - 1]; --d; }
+        c[d] = val;
+    }
+    v3 tw = transported;
+    if (!old_ok || !vfinite(tw) || vdot(tw, tw) <= 1.0e-12) tw = stable_tangent(nw);
+    else tw = vmul(tw, 1.0 / vlen(tw));
+    vst(slot->normal_local, qrotinv(rotA, nw));
+    slot->age = old_ok ? fmin(old_age + 1.0, 65535.0) : 0.0;
+    vst(slot->tangent_local, qrotinv(rotA, tw));
+    slot->count = (uint32_t)nc;
+    for (int i = 0; i < MPTS; ++i) {
+        OraclePoint* op = &slot->points[i];
+        memset(op, 0, sizeof(*op));
+        if (i < nc) {
+            for (int a = 0; a < 3; ++a) { op->anchor_a[a] = c[i].la[a]; op->anchor_b[a] = c[i].lb[a]; op->impulses[a] = c[i].imp[a]; }
+            op->feature_a = c[i].fa;
+            op->feature_b = c[i].fb;
+            op->life = c[i].life;
+        }
+    }
+    return nc;
+}
+
+/* ------------------------------------------------------------------ */
+/* Dense factor solves                                                  */
+/* ------------------------------------------------------------------ */
+static int cholesky(double* A, uint32_t n) { /* in place, lower */
+    for (uint32_t j = 0; j < n; ++j) {
+        double d = A[j * n + j];
+        for (uint32_t k = 0; k < j; ++k) d -= A[j * n + k] * A[j * n + k];
+        if (!(d > kPivotFloor) || !isfinite(d)) return 0;
+        A[j * n + j] = sqrt(d);
+        for (uint32_t i = j + 1; i < n; ++i) {
+            double s = A[i * n + j];
+            for (uint32_t k = 0; k < j; ++k) s -= A[i * n + k] * A[j * n + k];
+            A[i * n + j] = s / A[j * n + j];
+        }
+    }
+    return 1;
+}
+
+static void chol_solve(const double* L, uint32_t n, double* x) { /* solveCholesky (MetalWorldContact.metal:406-445) */
+    for (uint32_t i = 0; i < n; ++i) {
+        double s = x[i];
+        for (uint32_t k = 0; k < i; ++k) s -= L[i * n + k] * x[k];
+        x[i] = s / L[i * n + i];
+    }
+    for (int i = (int)n - 1; i >= 0; --i) {
+        double s = x[i];
+        for (uint32_t k = (uint32_t)i + 1; k < n; ++k) s -= L[k * n + i] * x[k];
+        x[i] = s / L[i * n + i];
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* Contact substep: scatter to ConstraintIR (Collision.metal:10253-10620), */
+/* IR evaluation (MetalWorldContact.metal:3580-3990), Wave32 temporalCone */
+/* solve (MetalWorldContact.metal:6142-7216), joint limits (:2878-2968),  */
+/* integration (:8876-9050).                                            */
+/* ------------------------------------------------------------------ */
+typedef struct {
+    uint32_t pair, point, body, new_impact;
+    int b_side;
+    v3 x, n, t, bt;
+    double sep, target[3], reg[3], mu, lambda[3], P[9], relax, delta[3];
+    double G[3][MAXV];
+} Contact;
+
+static uint32_t contact_substep(const OracleWorld* o, double* q, double* v, const double* vf, const Kin* k, OracleManifold* slots,
+                                double friction_scale, int final_substep, OracleTrace* trace, uint32_t* fail_index) {
+    const uint32_t nv = o->w.nv, np = o->w.pair_count, ns = o->w.shape_count;
+    const double h = o->h;
+    double gs = 0.0;
+    for (uint32_t d = 0; d < nv; ++d) gs += fabs(vf[d]);
+    double margins[MAXS];
+    for (uint32_t s = 0; s < ns; ++s) {
+        margins[s] = 0.0;
+        const MRModelShapeC* src = &o->shapes[s];
+        if (o->bodies[src->body].articulated && src->shape_type != MR_SHAPE_PLANE) {
+            double sweep = src->contact_rest_bound[2];
+            if (!(sweep > 0.0) || !isfinite(sweep)) {
+                if (src->shape_type == MR_SHAPE_SPHERE) sweep = src->dimensions[0];
+                else if (src->shape_type == MR_SHAPE_CAPSULE) sweep = src->dimensions[0] + src->dimensions[1];
+                else sweep = vlen(vldf(src->dimensions));
+            }
+            const double env = fmin(h * gs * fmax(sweep, 0.25), h * (double)o->w.speculative[1]);
+            margins[s] = o->w.speculative[0] * env;
+        }
+    }
+    static __thread Contact C[MAXC];
+    uint32_t total = 0, manifolds = 0;
+    int counts[MAXP];
+    for (uint32_t p = 0; p < np; ++p) {
+        int cand = 0;
+        counts[p] = pair_manifold(o, k, margins, p, &slots[p], &cand);
+        if (counts[p] < 0) { *fail_index = p; return MR_STEP_NONFINITE_RESULT; }
+        total += (uint32_t)counts[p];
+        if (counts[p] > 0) manifolds++;
+    }
+    trace->manifold_count = manifolds;
+    if (total > o->w.contact_capacity) { *fail_index = total; return MR_STEP_CONTACT_CAPACITY_OVERFLOW; }
+    uint32_t c = 0;
+    for (uint32_t p = 0; p < np; ++p) {
+        if (counts[p] <= 0) continue;
+        const MRModelPairC* pr = &o->pairs[p];
+        const MRModelShapeC* sa = &o->shapes[pr->shape_a];
+        const MRModelShapeC* sb = &o->shapes[pr->shape_b];
+        const MRModelBodyC* ba = &o->bodies[sa->body];
+        const MRModelBodyC* bb = &o->bodies[sb->body];
+        v3 posA, posB;
+        q4 rotA, rotB;
+        if (ba->articulated) { posA = k->pos[sa->body]; rotA = k->rot[sa->body]; }
+        else { posA = vldf(ba->static_pose); qnormalize(qldf(ba->static_pose + 4), &rotA, 0); }
+        if (bb->articulated) { posB = k->pos[sb->body]; rotB = k->rot[sb->body]; }
+        else { posB = vldf(bb->static_pose); qnormalize(qldf(bb->static_pose + 4), &rotB, 0); }
+        const OracleManifold* slot = &slots[p];
+        v3 nw = qrot(rotA, vld(slot->normal_local));
+        nw = vmul(nw, 1.0 / vlen(nw));
+        v3 tw = qrot(rotA, vld(slot->tangent_local));
+        tw = vsub(tw, vmul(nw, vdot(tw, nw)));
+        tw = vdot(tw, tw) > 1.0e-12 ? vmul(tw, 1.0 / vlen(tw)) : stable_tangent(nw);
+        const v3 bw = vcross(nw, tw);
+        const MRModelMaterialC* ma = &o->materials[sa->material];
+        const MRModelMaterialC* mb = &o->materials[sb->material];
+        const double mu_s = sqrt(fmax(0.0, (double)ma->friction[0] * mb->friction[0])) * friction_scale;
+        const double mu_d = sqrt(fmax(0.0, (double)ma->friction[1] * mb->friction[1])) * friction_scale;
+        const double restitution = fmin(fmax(fmax(ma->response[0], mb->response[0]), 0.0), 1.0);
+        const double rthr = fmax(ma->response[1], mb->response[1]);
+        const double compliance = (double)ma->response[2] + mb->response[2];
+        const double dissipation = (double)ma->response[3] + mb->response[3];
+        const double rest = (double)sa->contact_rest_bound[1] + sb->contact_rest_bound[1];
+        for (int i = 0; i < counts[p]; ++i, ++c) {
+            Contact* ct = &C[c];
+            const OraclePoint* op = &slot->points[i];
+            const v3 pa = vadd(posA, qrot(rotA, vld(op->anchor_a)));
+            const v3 pb = vadd(posB, qrot(rotB, vld(op->anchor_b)));
+            ct->pair = p;
+            ct->point = (uint32_t)i;
+            ct->x = vmul(vadd(pa, pb), 0.5);
+            ct->sep = vdot(vsub(pb, pa), nw) - rest;
+            ct->n = nw; ct->t = tw; ct->bt = bw;
+            ct->new_impact = op->life == 0u;
+            ct->b_side = !ba->articulated;
+            ct->body = ct->b_side ? sb->body : sa->body;
+            for (int a = 0; a < 3; ++a) ct->lambda[a] = op->impulses[a];
+            /* Jacobian rows and relative velocity at v_free. */
+            double J[3 * MAXV];
+            point_jacobian_k(o, k, ct->body, ct->x, J);
+            const double sign = ct->b_side ? 1.0 : -1.0;
+            const v3 dirs[3] = {nw, tw, bw};
+            double rel[3] = {0, 0, 0};
+            for (int r = 0; r < 3; ++r)
+                for (uint32_t d = 0; d < nv; ++d) {
+                    const double g = sign * (vget(dirs[r], 0) * J[d] + vget(dirs[r], 1) * J[nv + d] + vget(dirs[r], 2) * J[2 * nv + d]);
+                    ct->G[r][d] = g;
+                    rel[r] += g * vf[d];
+                }
+            ct->target[0] = ct->sep > 0.0 ? -ct->sep / h : 0.0;
+            ct->target[1] = ct->target[2] = 0.0;
+            ct->reg[0] = fmax(compliance / (h * h) + dissipation / h, 0.0);
+            ct->reg[1] = ct->reg[2] = 0.0;
+            const double tau_c = 2.0 * h;
+            const double err = fmin(ct->sep + o->w.solver_scales[3], 0.0);
+            const double ratio = h / tau_c;
+            const double den = 1.0 + 2.0 * ratio + ratio * ratio;
+            double stab = -h * err / (tau_c * tau_c * den);
+            stab = fmin(fmax(stab, 0.0), o->w.solver_scales[2]);
+            if (ct->new_impact) {
+                const double incoming = rel[0] - ct->target[0];
+                if (incoming < -rthr) stab = fmax(stab, -restitution * incoming);
+            }
+            ct->target[0] += stab;
+            const double slip = sqrt(rel[1] * rel[1] + rel[2] * rel[2]);
+            ct->mu = slip <= 1.0e-3 ? mu_s : mu_d;
+        }
+    }
+    trace->contact_count = total;
+    if (total > trace->max_contacts) trace->max_contacts = total;
+    trace->island_count = total > 0 ? 1u : 0u;
+    for (uint32_t d = 0; d < nv; ++d) v[d] = vf[d];
+    if (total > 0) {
+        double Mm[MAXV * MAXV];
+        mass_matrix_k(o, k, Mm);
+        for (uint32_t d = 0; d < nv; ++d) Mm[d * nv + d] += o->arm_eff[d];
+        if (!cholesky(Mm, nv)) { *fail_index = 0; return MR_STEP_FACTORIZATION_FAILED; }
+        static __thread double Rc[3 * MAXC][MAXV];
+        for (uint32_t i = 0; i < total; ++i)
+            for (int r = 0; r < 3; ++r) {
+                for (uint32_t d = 0; d < nv; ++d) Rc[3 * i + r][d] = C[i].G[r][d];
+                chol_solve(Mm, nv, Rc[3 * i + r]);
+            }
+        for (uint32_t i = 0; i < total; ++i) {
+            Contact* ct = &C[i];
+            double W[9];
+            for (int r = 0; r < 3; ++r)
+                for (int s = 0; s < 3; ++s) {
+                    double acc = 0.0;
+                    for (uint32_t d = 0; d < nv; ++d) acc += ct->G[r][d] * Rc[3 * i + s][d];
+                    W[r * 3 + s] = acc + (r == s ? ct->reg[r] : 0.0);
+                }
+            if (!oracle_invert3x3(W, ct->P)) { *fail_index = i; return MR_STEP_FACTORIZATION_FAILED; }
+            double rowsum = 0.0, diag = 0.0;
+            for (uint32_t j = 0; j < total; ++j) {
+                double acc = 0.0;
+                for (uint32_t d = 0; d < nv; ++d) acc += ct->G[0][d] * Rc[3 * j][d];
+                rowsum += fabs(acc);
+                if (j == i) diag = fabs(acc) + ct->reg[0];
+            }
+            ct->relax = rowsum > fmax(diag, kMatrixFloor) ? fmin(fmax(diag / rowsum, 1.0 / 32.0), 1.0) : 1.0;
+            double warm[3];
+            oracle_project_cone(ct->lambda, ct->mu, ct->mu, warm);
+            for (int a = 0; a < 3; ++a) { ct->lambda[a] = warm[a]; ct->delta[a] = warm[a]; }
+        }
+        const uint32_t iters = o->iters + (final_substep ? o->final_iters : 0u);
+        for (int it = -1; it < (int)iters; ++it) {
+            if (it >= 0) {
+                for (uint32_t i = 0; i < total; ++i) {
+                    Contact* ct = &C[i];
+                    double u[3], rhs[3], prop[3], proj[3];
+                    for (int r = 0; r < 3; ++r) {
+                        u[r] = 0.0;
+                        for (uint32_t d = 0; d < nv; ++d) u[r] += ct->G[r][d] * v[d];
+                        rhs[r] = ct->target[r] - u[r] - ct->reg[r] * ct->lambda[r];
+                    }
+                    for (int r = 0; r < 3; ++r) prop[r] = ct->lambda[r] + ct->P[r * 3] * rhs[0] + ct->P[r * 3 + 1] * rhs[1] + ct->P[r * 3 + 2] * rhs[2];
+                    oracle_project_cone(prop, ct->mu, ct->mu, proj);
+                    for (int r = 0; r < 3; ++r) {
+                        ct->delta[r] = ct->relax * (proj[r] - ct->lambda[r]);
+                    }
+                    int finite = 1;
+                    for (int r = 0; r < 3; ++r) finite &= isfinite(ct->lambda[r] + ct->delta[r]) && isfinite(ct->delta[r]);
+                    if (!finite) { *fail_index = i; return MR_STEP_NONFINITE_RESULT; }
+                    for (int r = 0; r < 3; ++r) ct->lambda[r] += ct->delta[r];
+                }
+            }
+            for (uint32_t d = 0; d < nv; ++d) {
+                double acc = 0.0;
+                for (uint32_t i = 0; i < total; ++i)
+                    for (int r = 0; r < 3; ++r) acc += Rc[3 * i + r][d] * C[i].delta[r];
+                v[d] += acc;
+            }
+        }
+        /* Diagnostics (MetalWorldContact.metal:7052-7110) and impulse write-back. */
+        for (uint32_t i = 0; i < total; ++i) {
+            Contact* ct = &C[i];
+            double un = 0.0;
+            for (uint32_t d = 0; d < nv; ++d) un += ct->G[0][d] * v[d];
+            const double eq = un - ct->target[0] + ct->reg[0] * ct->lambda[0];
+            const double resid = ct->lambda[0] > 1.0e-7 ? fabs(eq) : fmax(-eq, 0.0);
+            if (resid > trace->max_normal_residual) trace->max_normal_residual = resid;
+            const double lu = ct->mu * ct->lambda[0];
+            double viol;
+            if (lu > 0.0) viol = fmax(sqrt((ct->lambda[1] * ct->lambda[1] + ct->lambda[2] * ct->lambda[2]) / (lu * lu)) - 1.0, 0.0);
+            else viol = sqrt(ct->lambda[1] * ct->lambda[1] + ct->lambda[2] * ct->lambda[2]);
+            if (viol > trace->max_cone_violation) trace->max_cone_violation = viol;
+            OraclePoint* op = &slots[ct->pair].points[ct->point];
+            for (int a = 0; a < 3; ++a) op->impulses[a] = ct->lambda[a];
+            OracleContact* oc = &trace->contacts[i];
+            oc->pair = ct->pair;
+            oc->point = ct->point;
+            oc->feature_a = op->feature_a;
+            oc->feature_b = op->feature_b;
+            oc->body = ct->body;
+            oc->new_impact = ct->new_impact;
+            oc->separation = ct->sep;
+            vst(oc->normal, ct->n);
+            for (int a = 0; a < 3; ++a) oc->impulses[a] = ct->lambda[a];
+        }
+    }
+    /* Joint limits on the post-solve velocity. */
+    for (uint32_t d = 0; d < nv; ++d) {
+        const MRModelDofC* dof = &o->dofs[d];
+        double vel = v[d];
+        if (dof->flags & MR_DOF_FLAG_VELOCITY_LIMIT) vel = fmin(fmax(vel, -dof->limits[2]), dof->limits[2]);
+        if ((dof->flags & MR_DOF_FLAG_POSITION_LIMIT) && dof->q_index != MR_INVALID_INDEX) {
+            const double pos = q[dof->q_index];
+            vel = fmin(fmax(vel, (dof->limits[0] - pos) / h), (dof->limits[1] - pos) / h);
+        }
+        if (!isfinite(vel)) { *fail_index = d; return MR_STEP_NONFINITE_RESULT; }
+        v[d] = vel;
+    }
+    /* Integration from the substep-start configuration. */
+    for (uint32_t d = 0; d < nv; ++d) {
+        const MRModelDofC* dof = &o->dofs[d];
+        if (dof->q_index != MR_INVALID_INDEX && !(o->floating && d < 6)) q[dof->q_index] += h * v[d];
+    }
+    if (o->floating) {
+        q[0] += h * v[0];
+        q[1] += h * v[1];
+        q[2] += h * v[2];
+        const q4 inc = so3_increment(V(h * v[3], h * v[4], h * v[5]), 0);
+        q4 out;
+        if (!qnormalize(qmul(inc, Q(q[3], q[4], q[5], q[6])), &out, 0)) { *fail_index = 3; return MR_STEP_NONFINITE_RESULT; }
+        q[3] = out.x; q[4] = out.y; q[5] = out.z; q[6] = out.w;
+    }
+    for (uint32_t i = 0; i < o->w.nq; ++i)
+        if (!isfinite(q[i])) { *fail_index = i; return MR_STEP_NONFINITE_RESULT; }
+    return MR_STEP_SUCCESS;
+}
+
+/* Free-motion commit (ArticulatedABA.metal:1446-1540). */
+static uint32_t integrate_free(const OracleWorld* o, double* q, double* v, const double* qdd) {
+    const uint32_t nv = o->w.nv;
+    for (uint32_t d = 0; d < nv; ++d) {
+        const double nvel = v[d] + o->h * qdd[d];
+        if (!isfinite(nvel)) return MR_STEP_NONFINITE_RESULT;
+        v[d] = nvel;
+    }
+    if (o->floating) {
+        q[0] += o->h * v[0];
+        q[1] += o->h * v[1];
+        q[2] += o->h * v[2];
+        const q4 inc = so3_increment(V(o->h * v[3], o->h * v[4], o->h * v[5]), 1);
+        q4 out;
+        if (!qnormalize(qmul(inc, Q(q[3], q[4], q[5], q[6])), &out, 0)) return MR_STEP_NONFINITE_RESULT;
+        q[3] = out.x; q[4] = out.y; q[5] = out.z; q[6] = out.w;
+    }
+    for (uint32_t b = 1; b < o->nb; ++b) {
+        const int dof = o->body_dof[b];
+        if (dof < 0) continue;
+        const MRModelJointC* j = &o->joints[o->bodies[b].inbound_joint];
+        q[j->q_index] += o->h * v[dof];
+    }
+    for (uint32_t i = 0; i < o->w.nq; ++i)
+        if (!isfinite(q[i])) return MR_STEP_NONFINITE_RESULT;
+    return MR_STEP_SUCCESS;
+}
+
+/* One control step: prepare (reset + checkpoint), substeps, latch,
+ * commit-or-restore (MetalWorld.metal:113-518, MetalWorldContact.metal:9051). */
+uint32_t oracle_control_step(const OracleWorld* o, double* q, double* v, OracleManifold* manifolds, const double* actions,
+                             double friction_scale, int reset, const double* reset_q, const double* reset_v,
+                             OracleTrace* trace) {
+    const uint32_t nq = o->w.nq, nv = o->w.nv, np = o->w.pair_count;
+    OracleTrace local;
+    if (!trace) trace = &local;
+    memset(trace, 0, sizeof(*trace));
+    trace->failing_substep = MR_INVALID_INDEX;
+    trace->failing_index = MR_INVALID_INDEX;
+    if (reset) {
+        memcpy(q, reset_q, sizeof(double) * nq);
+        memcpy(v, reset_v, sizeof(double) * nv);
+        if (np) memset(manifolds, 0, sizeof(OracleManifold) * np);
+    }
+    double qc[MAXQ], vc[MAXV];
+    static __thread OracleManifold mc[MAXP];
+    memcpy(qc, q, sizeof(double) * nq);
+    memcpy(vc, v, sizeof(double) * nv);
+    if (np) memcpy(mc, manifolds, sizeof(OracleManifold) * np);
+    uint32_t status = MR_STEP_SUCCESS;
+    for (uint32_t s = 0; s < o->substeps; ++s) {
+        double tau[MAXV], qdd[MAXV], vf[MAXV];
+        oracle_drive_efforts(o, q, v, actions, tau);
+        Kin k;
+        status = kinematics(o, q, v, &k);
+        uint32_t fail_index = MR_INVALID_INDEX;
+        if (status == MR_STEP_SUCCESS) status = aba_core(o, q, v, tau, &k, qdd);
+        if (status == MR_STEP_SUCCESS) {
+            if (np > 0) {
+                for (uint32_t d = 0; d < nv; ++d) {
+                    vf[d] = v[d] + o->h * qdd[d];
+                    if (!isfinite(vf[d])) status = MR_STEP_NONFINITE_RESULT;
+                }
+                if (status == MR_STEP_SUCCESS)
+                    status = contact_substep(o, q, v, vf, &k, manifolds, friction_scale, s + 1 == o->substeps, trace, &fail_index);
+            } else {
+                status = integrate_free(o, q, v, qdd);
+            }
+        }
+        if (status != MR_STEP_SUCCESS) {
+            trace->failing_substep = s;
+            trace->failing_index = fail_index;
+            break;
+        }
+    }
+    trace->status = status;
+    if (status != MR_STEP_SUCCESS) {
+        memcpy(q, qc, sizeof(double) * nq);
+        memcpy(v, vc, sizeof(double) * nv);
+        if (np) memcpy(manifolds, mc, sizeof(OracleManifold) * np);
+        trace->contact_count = 0;
+    }
+    return status;
+}
+
+/* ------------------------------------------------------------------ */
+void oracle_manifold_from_device(const MRManifoldC* in, OracleManifold* out, uint32_t count) {
+    for (uint32_t m = 0; m < count; ++m) {
+        memset(&out[m], 0, sizeof(OracleManifold));
+        for (int a = 0; a < 3; ++a) { out[m].normal_local[a] = in[m].normal_local[a]; out[m].tangent_local[a] = in[m].tangent_local[a]; }
+        out[m].age = in[m].age;
+        out[m].count = in[m].count;
+        for (int p = 0; p < MPTS; ++p) {
+            for (int a = 0; a < 3; ++a) {
+                out[m].points[p].anchor_a[a] = in[m].points[p].anchor_a[a];
+                out[m].points[p].anchor_b[a] = in[m].points[p].anchor_b[a];
+                out[m].points[p].impulses[a] = in[m].points[p].impulses[a];
+            }
+            out[m].points[p].feature_a = in[m].points[p].feature_a;
+            out[m].points[p].feature_b = in[m].points[p].feature_b;
+            out[m].points[p].life = in[m].points[p].life;
+        }
+    }
+}
+
+void oracle_manifold_to_device(const OracleManifold* in, MRManifoldC* out, uint32_t count) {
+    for (uint32_t m = 0; m < count; ++m) {
+        memset(&out[m], 0, sizeof(MRManifoldC));
+        for (int a = 0; a < 3; ++a) { out[m].normal_local[a] = (float)in[m].normal_local[a]; out[m].tangent_local[a] = (float)in[m].tangent_local[a]; }
+        out[m].age = (float)in[m].age;
+        out[m].count = in[m].count;
+        for (int p = 0; p < MPTS; ++p) {
+            for (int a = 0; a < 3; ++a) {
+                out[m].points[p].anchor_a[a] = (float)in[m].points[p].anchor_a[a];
+                out[m].points[p].anchor_b[a] = (float)in[m].points[p].anchor_b[a];
+                out[m].points[p].impulses[a] = (float)in[m].points[p].impulses[a];
+            }
+            out[m].points[p].feature_a = in[m].points[p].feature_a;
+            out[m].points[p].feature_b = in[m].points[p].feature_b;
+            out[m].points[p].life = in[m].points[p].life;
+        }
+    }
+}
+
+/* Temporal-cone Jacobi iteration on an explicit Delassus problem, with the
+ * same preconditioner / relaxation / projection as the contact substep. */
+void oracle_temporal_cone_dense(uint32_t n, const double* W, const double* u0, const double* mu, uint32_t iterations, double* lambda) {
+    const uint32_t m = 3 * n;
+    double P[MAXC][9], relax[MAXC], delta[3 * MAXC], u[3 * MAXC];
+    for (uint32_t i = 0; i < n; ++i) {
+        double B[9];
+        for (int r = 0; r < 3; ++r)
+            for (int s = 0; s < 3; ++s) B[r * 3 + s] = W[(3 * i + r) * m + 3 * i + s];
+        oracle_invert3x3(B, P[i]);
+        double rowsum = 0.0, diag = 0.0;
+        for (uint32_t j = 0; j < n; ++j) {
+            const double a = W[(3 * i) * m + 3 * j];
+            rowsum += fabs(a);
+            if (i == j) diag = fabs(a);
+        }
+        relax[i] = rowsum > fmax(diag, kMatrixFloor) ? fmin(fmax(diag / rowsum, 1.0 / 32.0), 1.0) : 1.0;
+        double warm[3];
+        oracle_project_cone(&lambda[3 * i], mu[i], mu[i], warm);
+        for (int a = 0; a < 3; ++a) lambda[3 * i + a] = warm[a];
+    }
+    for (uint32_t it = 0; it < iterations; ++it) {
+        for (uint32_t r = 0; r < m; ++r) {
+            double s = u0[r];
+            for (uint32_t c = 0; c < m; ++c) s += W[r * m + c] * lambda[c];
+            u[r] = s;
+        }
+        for (uint32_t i = 0; i < n; ++i) {
+            double rhs[3], prop[3], proj[3];
+            for (int r = 0; r < 3; ++r) rhs[r] = -u[3 * i + r];
+            for (int r = 0; r < 3; ++r) prop[r] = lambda[3 * i + r] + P[i][r * 3] * rhs[0] + P[i][r * 3 + 1] * rhs[1] + P[i][r * 3 + 2] * rhs[2];
+            oracle_project_cone(prop, mu[i], mu[i], proj);
+            for (int r = 0; r < 3; ++r) delta[3 * i + r] = relax[i] * (proj[r] - lambda[3 * i + r]);
+        }
+        for (uint32_t r = 0; r < m; ++r) lambda[r] += delta[r];
+    }
+}

@@ -1,0 +1,385 @@
+// ORACLE (reference side) — test infrastructure only.
+//
+// A C-ABI harness, written for this project, over numi-lab's own FP64 CPU
+// core (compiled out of tree from its sources by oracle/Makefile into
+// oracle/_ref/).  It rebuilds a reference EngineModel from the records this
+// library exports (MRModel*C, include/numi_b200.h) and exposes:
+//   - computeArticulatedForwardDynamics / MassMatrix / PointJacobians
+//     (src/core/ArticulatedDynamics.cpp:2010, 2241, and friends),
+//   - integrateArticulatedState (ArticulatedDynamics.cpp:2333),
+//   - solveReferenceConicProblem (src/core/ReferenceConicSolver.cpp:182),
+//   - stepControlledArticulatedWorldCpu (src/core/ArticulatedWorld.cpp:1232)
+//     and a multi-threaded timing loop over it (the CPU baseline).
+// Implicit PD drives are expressed for the reference the way its own GPU
+// ABA does: armature raised by h kd + h^2 kp and the PD law evaluated as an
+// effort (ArticulatedABA.metal:301-326, MetalWorld.metal:280-370).
+#include "metalrobo/ArticulatedDynamics.hpp"
+#include "metalrobo/ArticulatedWorld.hpp"
+#include "metalrobo/EngineModel.hpp"
+#include "metalrobo/ReferenceConicSolver.hpp"
+
+#define NUMI_B200_OMIT_SHARED_ENUMS
+#include "numi_b200.h"
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <thread>
+#include <vector>
+
+using namespace metalrobo;
+
+namespace {
+
+mr_float4 f4(const float* p) { return mr_float4{p[0], p[1], p[2], p[3]}; }
+mr_float4 f4(double x, double y, double z, double w) {
+    return mr_float4{static_cast<float>(x), static_cast<float>(y), static_cast<float>(z), static_cast<float>(w)};
+}
+
+void write_error(char* err, size_t len, const std::string& msg) {
+    if (err && len) {
+        std::strncpy(err, msg.c_str(), len - 1);
+        err[len - 1] = 0;
+    }
+}
+
+}  // namespace
+
+struct RefModel {
+    EngineModel model;
+    std::vector<MRBodyStateGPU> env_bodies;
+    std::vector<MRShapeGPU> env_shapes;
+    MRModelWorldC world{};
+    std::vector<MRModelDofC> dofs;
+    std::vector<std::uint32_t> action_dof;
+    double h = 0.0;
+    bool implicit = false;
+};
+
+extern "C" {
+
+__attribute__((visibility("default"))) RefModel* ref_model_create(
+    const MRModelWorldC* world, const MRModelJointC* joints, const MRModelBodyC* bodies, const MRModelDofC* dofs,
+    const MRModelShapeC* shapes, const MRModelMaterialC* materials, double h, double friction, char* err, size_t err_len) {
+    try {
+        auto r = std::make_unique<RefModel>();
+        r->world = *world;
+        r->h = h;
+        r->implicit = world->actuation_mode == MR_ACTUATION_IMPLICIT_POSITION;
+        r->dofs.assign(dofs, dofs + world->nv);
+        std::uint32_t na = 0;
+        while (na < world->body_count && bodies[na].articulated) ++na;
+        EngineModel& m = r->model;
+        m.name = "numi_b200_export";
+        m.world.abiVersion = MR_ENGINE_ABI_VERSION;
+        m.world.bodyCount = na;
+        m.world.articulationCount = 1;
+        m.world.jointCount = world->joint_count;
+        m.world.nq = world->nq;
+        m.world.nv = world->nv;
+        m.world.pairCapacity = 2048;
+        m.world.contactCapacity = 1024;
+        m.world.constraintCapacity = 2048;
+        m.world.islandCapacity = 32;
+        m.world.solverType = MR_SOLVER_QUALITY_NEWTON;
+        m.world.frictionConeType = MR_FRICTION_CONE_ELLIPTIC;
+        m.world.gravityAndTimestep = f4(world->gravity[0], world->gravity[1], world->gravity[2], h);
+        m.world.solverScales = f4(world->solver_scales);
+        MRArticulationGPU art{};
+        art.rootBody = 0;
+        art.rootType = world->root_type;
+        art.firstBody = 0;
+        art.bodyCount = na;
+        art.firstJoint = 0;
+        art.jointCount = world->joint_count;
+        art.qOffset = 0;
+        art.nq = world->nq;
+        art.vOffset = 0;
+        art.nv = world->nv;
+        m.articulations.push_back(art);
+        for (std::uint32_t b = 0; b < na; ++b) {
+            const MRModelBodyC& s = bodies[b];
+            MRBodyPropertiesGPU p{};
+            p.articulationIndex = 0;
+            p.parentBody = s.parent_body;
+            p.inboundJoint = s.inbound_joint;
+            p.motionType = MR_MOTION_DYNAMIC;
+            p.massAndInverseMass = f4(s.mass_inverse_mass[0], 1.0 / s.mass_inverse_mass[0], 0.0, 0.0);
+            p.centerOfMass = f4(0, 0, 0, 0);
+            p.inertiaRow0 = f4(s.inertia[0][0], s.inertia[0][1], s.inertia[0][2], 0.0);
+            p.inertiaRow1 = f4(s.inertia[1][0], s.inertia[1][1], s.inertia[1][2], 0.0);
+            p.inertiaRow2 = f4(s.inertia[2][0], s.inertia[2][1], s.inertia[2][2], 0.0);
+            // Inverse of the (diagonal-dominant) body inertia by cofactors.
+            const double a = s.inertia[0][0], bq = s.inertia[0][1], c = s.inertia[0][2];
+            const double d = s.inertia[1][1], e = s.inertia[1][2], f = s.inertia[2][2];
+            const double c00 = d * f - e * e, c01 = c * e - bq * f, c02 = bq * e - c * d;
+            const double det = a * c00 + bq * c01 + c * c02;
+            const double c11 = a * f - c * c, c12 = bq * c - a * e, c22 = a * d - bq * bq;
+            p.inverseInertiaRow0 = f4(c00 / det, c01 / det, c02 / det, 0.0);
+            p.inverseInertiaRow1 = f4(c01 / det, c11 / det, c12 / det, 0.0);
+            p.inverseInertiaRow2 = f4(c02 / det, c12 / det, c22 / det, 0.0);
+            p.dampingAndSpeedLimits = f4(s.damping_speed);
+            m.bodies.push_back(p);
+        }
+        for (std::uint32_t j = 0; j < world->joint_count; ++j) {
+            const MRModelJointC& s = joints[j];
+            MRJointDescriptorGPU d{};
+            d.parentBody = s.parent_body;
+            d.childBody = s.child_body;
+            d.jointType = s.joint_type;
+            d.flags = 0;
+            const bool scalar = s.joint_type != MR_JOINT_FIXED;
+            d.qOffset = scalar ? s.q_index : 0;
+            d.nq = scalar ? 1 : 0;
+            d.vOffset = scalar ? s.v_index : 0;
+            d.nv = scalar ? 1 : 0;
+            d.axis0 = f4(s.axis);
+            d.parentAnchor = f4(s.parent_anchor);
+            d.childAnchor = f4(s.child_anchor);
+            d.parentRotation = f4(s.parent_rotation);
+            d.childRotation = f4(s.child_rotation);
+            m.joints.push_back(d);
+        }
+        for (std::uint32_t k = 0; k < world->nv; ++k) {
+            const MRModelDofC& s = dofs[k];
+            MRDofPropertiesGPU d{};
+            d.articulationIndex = 0;
+            d.jointIndex = s.joint_index;
+            d.qIndex = s.q_index;
+            d.vIndex = k;
+            d.localDof = s.joint_index == MR_INVALID_INDEX ? k : 0;
+            d.flags = s.flags;
+            d.limits = f4(s.limits);
+            double arm = s.drive[2];
+            if (r->implicit && (s.flags & MR_DOF_FLAG_DRIVE)) arm += h * s.drive[1] + h * h * s.drive[0];
+            d.drive = f4(s.drive[0], s.drive[1], arm, s.drive[3]);
+            m.dofs.push_back(d);
+            if ((s.flags & MR_DOF_FLAG_ACTUATED) && r->action_dof.size() < world->action_count) r->action_dof.push_back(k);
+        }
+        for (std::uint32_t i = 0; i < world->material_count; ++i) {
+            MRMaterialGPU mt{};
+            mt.friction = f4(materials[i].friction[0] * friction, materials[i].friction[1] * friction, materials[i].friction[2],
+                             materials[i].friction[3]);
+            mt.response = f4(materials[i].response);
+            m.materials.push_back(mt);
+        }
+        m.world.materialCount = static_cast<mr_u32>(m.materials.size());
+        for (std::uint32_t s = 0; s < world->shape_count; ++s) {
+            const MRModelShapeC& src = shapes[s];
+            MRShapeGPU sh{};
+            sh.shapeType = src.shape_type;
+            sh.materialIndex = src.material;
+            sh.collisionGroup = src.collision_group;
+            sh.collisionMask = src.collision_mask;
+            sh.slotGeneration = 1;
+            sh.localPosition = f4(src.local_position[0], src.local_position[1], src.local_position[2], 1.0);
+            sh.localRotation = f4(src.local_rotation);
+            sh.dimensions = f4(src.dimensions);
+            sh.contactRestAndBoundingRadius = f4(src.contact_rest_bound);
+            if (bodies[src.body].articulated) {
+                sh.bodyIndex = src.body;
+                m.shapes.push_back(sh);
+            } else {
+                const MRModelBodyC& gb = bodies[src.body];
+                MRBodyStateGPU st{};
+                st.position = f4(gb.static_pose[0], gb.static_pose[1], gb.static_pose[2], 0.0);
+                st.orientation = f4(gb.static_pose + 4);
+                st.linearVelocityAndInverseMass = f4(0, 0, 0, 0);
+                st.flagsAndIndices[0] = MR_MOTION_STATIC;
+                st.flagsAndIndices[1] = MR_INVALID_INDEX;
+                st.flagsAndIndices[2] = MR_INVALID_INDEX;
+                st.flagsAndIndices[3] = 0;
+                sh.bodyIndex = static_cast<mr_u32>(r->env_bodies.size());
+                r->env_bodies.push_back(st);
+                r->env_shapes.push_back(sh);
+            }
+        }
+        m.world.shapeCount = static_cast<mr_u32>(m.shapes.size());
+        m.defaultQ.assign(world->nq, 0.0f);
+        m.defaultV.assign(world->nv, 0.0f);
+        if (world->root_type == MR_ROOT_FLOATING) m.defaultQ[6] = 1.0f;
+        std::string reason;
+        if (!m.valid(&reason)) {
+            write_error(err, err_len, "reference EngineModel rejected: " + reason);
+            return nullptr;
+        }
+        return r.release();
+    } catch (const std::exception& e) {
+        write_error(err, err_len, e.what());
+        return nullptr;
+    }
+}
+
+__attribute__((visibility("default"))) void ref_model_destroy(RefModel* r) { delete r; }
+
+static ArticulatedDynamicsConfig dyn_config(const RefModel* r) {
+    ArticulatedDynamicsConfig c{};
+    c.gravity = {r->world.gravity[0], r->world.gravity[1], r->world.gravity[2]};
+    c.timestep = r->h;
+    c.applyBodyDamping = r->world.apply_body_damping != 0;
+    return c;
+}
+
+__attribute__((visibility("default"))) int ref_forward_dynamics(RefModel* r, const double* q, const double* v, const double* tau,
+                                                                double* qdd) {
+    const std::uint32_t nq = r->world.nq, nv = r->world.nv;
+    auto d = computeArticulatedForwardDynamics(r->model, 0, std::span<const double>(q, nq), std::span<const double>(v, nv),
+                                               std::span<const double>(tau, nv), {}, std::span<double>(qdd, nv), dyn_config(r));
+    return static_cast<int>(d.status);
+}
+
+__attribute__((visibility("default"))) int ref_mass_matrix(RefModel* r, const double* q, double* mass) {
+    const std::uint32_t nq = r->world.nq, nv = r->world.nv;
+    auto d = computeArticulatedMassMatrix(r->model, 0, std::span<const double>(q, nq), std::span<double>(mass, nv * nv), dyn_config(r));
+    return static_cast<int>(d.status);
+}
+
+__attribute__((visibility("default"))) int ref_point_jacobian(RefModel* r, const double* q, uint32_t body, const double* local,
+                                                              double* world_point, double* jacobian) {
+    const std::uint32_t nq = r->world.nq, nv = r->world.nv;
+    std::vector<double> v0(nv, 0.0);
+    ArticulatedPointQuery query{};
+    query.bodyIndex = body;
+    query.localPoint = {local[0], local[1], local[2]};
+    ArticulatedPointKinematics pk{};
+    auto d = computeArticulatedPointJacobians(r->model, 0, std::span<const double>(q, nq), v0, std::span<const ArticulatedPointQuery>(&query, 1),
+                                              std::span<ArticulatedPointKinematics>(&pk, 1), std::span<double>(jacobian, 3 * nv), dyn_config(r));
+    world_point[0] = pk.position[0];
+    world_point[1] = pk.position[1];
+    world_point[2] = pk.position[2];
+    return static_cast<int>(d.status);
+}
+
+__attribute__((visibility("default"))) int ref_integrate(RefModel* r, double* q, double* v, const double* tau) {
+    const std::uint32_t nq = r->world.nq, nv = r->world.nv;
+    auto d = integrateArticulatedState(r->model, 0, std::span<double>(q, nq), std::span<double>(v, nv), std::span<const double>(tau, nv),
+                                       {}, dyn_config(r));
+    return static_cast<int>(d.status);
+}
+
+// Converged FP64 conic contact solve on an explicit dense problem.
+// inverse_mass nv x nv, free_velocity nv, jac (3n x nv: n, t, b rows per
+// contact), mu n, target 3n; impulses 3n out, velocity nv out.
+__attribute__((visibility("default"))) int ref_conic_solve(uint32_t nv, const double* inverse_mass, const double* free_velocity, uint32_t n,
+                                                           const double* jac, const double* mu, const double* target, const double* reg,
+                                                           double* impulses, double* velocity, double* cone_violation) {
+    DenseConicProblem p{};
+    p.nv = nv;
+    p.inverseMass.assign(inverse_mass, inverse_mass + nv * nv);
+    p.freeVelocity.assign(free_velocity, free_velocity + nv);
+    for (uint32_t i = 0; i < n; ++i) {
+        DenseContactBlock b{};
+        b.normalJacobian.assign(jac + (3 * i + 0) * nv, jac + (3 * i + 1) * nv);
+        b.tangentUJacobian.assign(jac + (3 * i + 1) * nv, jac + (3 * i + 2) * nv);
+        b.tangentVJacobian.assign(jac + (3 * i + 2) * nv, jac + (3 * i + 3) * nv);
+        b.targetVelocity = {target[3 * i], target[3 * i + 1], target[3 * i + 2]};
+        b.regularization = {reg[3 * i], reg[3 * i + 1], reg[3 * i + 2]};
+        b.warmImpulse = {0.0, 0.0, 0.0};
+        b.friction = mu[i];
+        p.contacts.push_back(b);
+    }
+    ReferenceConicSolverConfig cfg{};
+    auto s = solveReferenceConicProblem(p, cfg);
+    for (uint32_t i = 0; i < 3 * n && i < s.impulses.size(); ++i) impulses[i] = s.impulses[i];
+    for (uint32_t i = 0; i < nv && i < s.velocity.size(); ++i) velocity[i] = s.velocity[i];
+    if (cone_violation) *cone_violation = s.maximumConeViolation;
+    return static_cast<int>(s.code);
+}
+
+// Implicit-drive efforts as the reference GPU prepares them (the CPU world
+// receives them as effort commands together with the raised armature).
+static void drive_efforts(const RefModel* r, const double* q, const double* v, const float* actions, double* tau) {
+    const std::uint32_t nv = r->world.nv;
+    std::vector<double> tgt(nv, 0.0);
+    for (size_t a = 0; a < r->action_dof.size(); ++a) tgt[r->action_dof[a]] = actions[a];
+    for (std::uint32_t k = 0; k < nv; ++k) {
+        const MRModelDofC& d = r->dofs[k];
+        double command = tgt[k];
+        if (r->implicit) {
+            command = 0.0;
+            if ((d.flags & MR_DOF_FLAG_DRIVE) && d.q_index != MR_INVALID_INDEX) {
+                double target = tgt[k];
+                if (d.flags & MR_DOF_FLAG_POSITION_LIMIT) target = std::min<double>(std::max<double>(target, d.limits[0]), d.limits[1]);
+                command = d.drive[0] * (target - q[d.q_index] - r->h * v[k]) - d.drive[1] * v[k];
+                if ((d.flags & MR_DOF_FLAG_EFFORT_LIMIT) && d.limits[3] > 0.0f)
+                    command = std::min<double>(std::max<double>(command, -d.limits[3]), d.limits[3]);
+            }
+        }
+        const double stall = ((d.flags & MR_DOF_FLAG_EFFORT_LIMIT) && d.limits[3] > 0.0f) ? d.limits[3] : std::numeric_limits<float>::max();
+        const double env = std::min<double>(d.limits[3], stall);
+        tau[k] = std::min(std::max(command, -env), env);
+    }
+}
+
+// Runs `steps` control steps x `substeps` physics steps for `envs`
+// environments with `threads` std::threads (static env partition) and
+// returns elapsed wall seconds.  Contact worlds use the reference's
+// transactional CPU world step with its quality (default) or FP64
+// reference-conic solver; free-motion worlds use integrateArticulatedState.
+// q/v are updated in place; failed steps are counted.
+__attribute__((visibility("default"))) double ref_run(RefModel* r, uint32_t envs, double* q, double* v, const float* actions,
+                                                      uint32_t steps, uint32_t substeps, uint32_t threads, int solver,
+                                                      uint64_t* failed_steps) {
+    const std::uint32_t nq = r->world.nq, nv = r->world.nv, na = r->world.action_count;
+    const bool contact = !r->env_shapes.empty();
+    std::atomic<std::uint64_t> failed{0};
+    auto worker = [&](std::uint32_t begin, std::uint32_t end) {
+        ArticulatedWorldConfig cfg{};
+        cfg.dynamics = dyn_config(r);
+        cfg.constraintEvaluation.timestep = r->h;
+        cfg.constraintEvaluation.penetrationSlop = r->world.solver_scales[3];
+        cfg.constraintEvaluation.maximumDepenetrationVelocity = r->world.solver_scales[2];
+        cfg.solverType = solver == 0 ? MR_SOLVER_REFERENCE_FP64 : MR_SOLVER_QUALITY_NEWTON;
+        std::vector<double> tau(nv);
+        std::vector<ArticulatedDofCommand> commands(nv);
+        for (std::uint32_t e = begin; e < end; ++e) {
+            ArticulatedWorldCache cache{};
+            double* qe = q + static_cast<size_t>(e) * nq;
+            double* ve = v + static_cast<size_t>(e) * nv;
+            for (std::uint32_t s = 0; s < steps; ++s) {
+                const float* act = actions + (static_cast<size_t>(s) * envs + e) * na;
+                for (std::uint32_t sub = 0; sub < substeps; ++sub) {
+                    drive_efforts(r, qe, ve, act, tau.data());
+                    bool ok = true;
+                    if (contact) {
+                        for (std::uint32_t k = 0; k < nv; ++k) {
+                            commands[k] = ArticulatedDofCommand{};
+                            if (r->dofs[k].flags & MR_DOF_FLAG_ACTUATED) {
+                                commands[k].mode = ArticulatedActuationMode::effort;
+                                commands[k].feedForward = tau[k];
+                            }
+                        }
+                        auto d = stepControlledArticulatedWorldCpu(r->model, 0, std::span<double>(qe, nq), std::span<double>(ve, nv), commands, {},
+                                                                   r->env_bodies, r->env_shapes, cfg, cache);
+                        ok = d.succeeded();
+                    } else {
+                        auto d = integrateArticulatedState(r->model, 0, std::span<double>(qe, nq), std::span<double>(ve, nv), tau, {}, cfg.dynamics);
+                        ok = d.succeeded();
+                    }
+                    if (!ok) {
+                        failed.fetch_add(1);
+                        break;
+                    }
+                }
+            }
+        }
+    };
+    const auto t0 = std::chrono::steady_clock::now();
+    threads = std::max<std::uint32_t>(1, std::min(threads, envs));
+    std::vector<std::thread> pool;
+    for (std::uint32_t t = 0; t < threads; ++t) {
+        const std::uint32_t b = static_cast<std::uint32_t>(static_cast<std::uint64_t>(envs) * t / threads);
+        const std::uint32_t e = static_cast<std::uint32_t>(static_cast<std::uint64_t>(envs) * (t + 1) / threads);
+        pool.emplace_back(worker, b, e);
+    }
+    for (auto& th : pool) th.join();
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (failed_steps) *failed_steps = failed.load();
+    return secs;
+}
+
+}  // extern "C"

@@ -1,0 +1,187 @@
+"""CUDA microstep vs the oracle, one control step at a time from identical
+FP32 input state (the CUDA path runs through the C ABI).
+
+Tolerances (north-star parity bar for FP32 state): per control step
+|q_gpu - q_oracle| <= 1e-5 * max(1, |q|) and the same for qd; impulses
+within 1e-4 of the largest impulse; discrete decisions (contact sets,
+manifold feature ids, status codes, rollback) identical.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import numi_lab_b200 as nb
+from oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+Q_TOL = 1e-5
+V_TOL = 1e-5
+IMPULSE_TOL = 1e-4
+
+
+def _rel_err(a: np.ndarray, b: np.ndarray) -> float:
+    return float(np.max(np.abs(a - b) / np.maximum(1.0, np.abs(b))))
+
+
+def _manifold_features(manifolds, env: int, pairs: int) -> list[tuple[int, tuple[int, ...]]]:
+    out = []
+    for p in range(pairs):
+        m = manifolds[env * pairs + p]
+        out.append((int(m.count), tuple(int(m.points[i].feature_a) for i in range(m.count))))
+    return out
+
+
+def _oracle_features(man, pairs: int) -> list[tuple[int, tuple[int, ...]]]:
+    return [(int(man[p].count), tuple(int(man[p].points[i].feature_a) for i in range(man[p].count))) for p in range(pairs)]
+
+
+def test_chain7_free_motion_per_step(cuda_device):
+    import torch
+
+    envs, steps, dt = 64, 25, 0.005
+    with nb.World("chain7", envs, substeps=1, control_dt=dt, seed=3) as world:
+        oracle = Oracle(world.model(), dt, 1, 0, 0)
+        gen = torch.Generator(device="cuda").manual_seed(11)
+        worst_q = worst_v = 0.0
+        for k in range(steps):
+            q0, v0, _ = world.state()
+            actions = 5.0 * torch.randn((1, envs, world.action_count), device="cuda", generator=gen)
+            _, status, _ = world.step(actions, wait=True)
+            assert int(status.abs().sum()) == 0
+            q1, v1, _ = world.state()
+            acts = actions.cpu().numpy()[0]
+            for e in range(envs):
+                q = q0[e].astype(np.float64)
+                v = v0[e].astype(np.float64)
+                st, _ = oracle.control_step(q, v, None, acts[e], 1.0)
+                assert st == 0
+                worst_q = max(worst_q, _rel_err(q1[e], q))
+                worst_v = max(worst_v, _rel_err(v1[e], v))
+        assert worst_q <= Q_TOL, worst_q
+        assert worst_v <= V_TOL, worst_v
+
+
+def _tree_world(envs: int, seed: int = 5):
+    return nb.World("tree29", envs, substeps=4, velocity_iterations=8, final_velocity_iterations=0, control_dt=0.02, seed=seed)
+
+
+def test_tree29_contact_per_step(cuda_device):
+    import torch
+
+    envs, warm, steps = 32, 20, 12
+    with _tree_world(envs) as world:
+        oracle = Oracle(world.model(), 0.005, 4, 8, 0)
+        friction = world.friction_scales()
+        gen = torch.Generator(device="cuda").manual_seed(21)
+        warm_actions = 0.3 * torch.randn((warm, envs, world.action_count), device="cuda", generator=gen)
+        _, status, _ = world.step(warm_actions, wait=True)
+        assert int(status.abs().sum()) == 0
+        worst = {"q": 0.0, "v": 0.0, "imp": 0.0}
+        contacts_seen = 0
+        feature_mismatch = 0
+        for k in range(steps):
+            q0, v0, m0 = world.state()
+            actions = 0.3 * torch.randn((1, envs, world.action_count), device="cuda", generator=gen)
+            _, status, _ = world.step(actions, wait=True)
+            assert int(status.abs().sum()) == 0
+            q1, v1, m1 = world.state()
+            acts = actions.cpu().numpy()[0]
+            for e in range(envs):
+                q = q0[e].astype(np.float64)
+                v = v0[e].astype(np.float64)
+                man = oracle.env_manifolds(m0, e)
+                st, trace = oracle.control_step(q, v, man, acts[e], float(friction[e]))
+                assert st == 0
+                worst["q"] = max(worst["q"], _rel_err(q1[e], q))
+                worst["v"] = max(worst["v"], _rel_err(v1[e], v))
+                gpu_feat = _manifold_features(m1, e, world.pair_count)
+                ora_feat = _oracle_features(man, world.pair_count)
+                if gpu_feat != ora_feat:
+                    feature_mismatch += 1
+                    continue
+                contacts_seen += trace.contact_count
+                # impulses of the final substep, in manifold order
+                scale = 1e-12
+                diffs = []
+                for p in range(world.pair_count):
+                    gm = m1[e * world.pair_count + p]
+                    for i in range(gm.count):
+                        g = np.array(gm.points[i].impulses[:], np.float64)
+                        o = np.array(man[p].points[i].impulses[:], np.float64)
+                        scale = max(scale, float(np.max(np.abs(o))))
+                        diffs.append(float(np.max(np.abs(g - o))))
+                if diffs:
+                    worst["imp"] = max(worst["imp"], max(diffs) / max(scale, 1.0))
+        assert contacts_seen > 0, "the workload should produce contacts"
+        assert feature_mismatch == 0, f"{feature_mismatch} env-steps with different manifold feature sets"
+        assert worst["q"] <= Q_TOL, worst
+        assert worst["v"] <= V_TOL, worst
+        assert worst["imp"] <= IMPULSE_TOL, worst
+
+
+def test_invalid_quaternion_rolls_back_only_that_env(cuda_device):
+    import torch
+
+    envs = 8
+    with _tree_world(envs, seed=9) as world:
+        q0, v0, m0 = world.state()
+        bad = q0.copy()
+        bad[3, 3:7] = [0.0, 0.0, 0.0, 2.0]  # norm 2: rejected quaternion
+        world.set_state(bad, v0, m0)
+        actions = torch.zeros((1, envs, world.action_count), device="cuda")
+        _, status, _ = world.step(actions, wait=True)
+        codes = status.cpu().numpy()[0]
+        assert codes[3] == 2  # MR_STEP_NONFINITE_INPUT
+        assert np.all(np.delete(codes, 3) == 0)
+        q1, v1, _ = world.state()
+        np.testing.assert_array_equal(q1[3], bad[3])  # transactional: checkpoint kept
+        np.testing.assert_array_equal(v1[3], v0[3])
+    with _tree_world(envs, seed=9) as clean:
+        clean.set_state(q0, v0, m0)
+        _, status, _ = clean.step(torch.zeros((1, envs, clean.action_count), device="cuda"), wait=True)
+        q2, v2, _ = clean.state()
+        keep = [e for e in range(envs) if e != 3]
+        np.testing.assert_array_equal(q1[keep], q2[keep])  # isolation: other envs unaffected
+        np.testing.assert_array_equal(v1[keep], v2[keep])
+
+
+def test_reset_mask_restores_reset_state(cuda_device):
+    import torch
+
+    envs = 6
+    with _tree_world(envs, seed=2) as world:
+        q_reset, v_reset, _ = world.state()
+        actions = 0.3 * torch.randn((5, envs, world.action_count), device="cuda")
+        world.step(actions, wait=True)
+        mask = torch.zeros((1, envs), dtype=torch.int32, device="cuda")
+        mask[0, 4] = 1
+        zero = torch.zeros((1, envs, world.action_count), device="cuda")
+        world.step(zero, reset_mask=mask, wait=True)
+        q1, _, _ = world.state()
+    with _tree_world(envs, seed=2) as ref:
+        ref.step(zero, wait=True)  # from the reset state, one step
+        q2, _, _ = ref.state()
+    np.testing.assert_array_equal(q1[4], q2[4])
+
+
+def test_bitwise_replay_and_host_path(cuda_device):
+    import torch
+
+    envs, steps = 16, 6
+    actions = 0.3 * torch.randn((steps, envs, 29), device="cuda", generator=torch.Generator(device="cuda").manual_seed(4))
+    results = []
+    for _ in range(2):
+        with _tree_world(envs, seed=12) as world:
+            obs, status, _ = world.step(actions, wait=True)
+            results.append((obs.cpu().numpy(), world.state()[0]))
+    np.testing.assert_array_equal(results[0][0], results[1][0])
+    np.testing.assert_array_equal(results[0][1], results[1][1])
+    with _tree_world(envs, seed=12) as world:
+        world.set_state_readback(True)
+        out = world.advance_host(actions.cpu().numpy())
+        assert out["counters"].successful_environment_steps == steps * envs
+        np.testing.assert_array_equal(out["observations"], results[0][0])
+        np.testing.assert_array_equal(out["final_q"], results[0][1])
