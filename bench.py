@@ -1,0 +1,391 @@
+"""Benchmark: contact env-steps/s of the 29-DoF floating-tree contact
+microstep on B200.
+
+Workload (one GPU): 4096 environments of the floating 29-DoF humanoid tree
+(box feet + 12 sphere proxies on a ground plane, friction U(0.4, 1.0)),
+PD drive targets ~ N(0, 0.3) rad, 20 ms control step = 4 microsteps of 5 ms,
+8 temporalCone iterations per microstep, FP32.  One bench step = one advance
+of 25 control steps (one CUDA graph); the default 20 timed steps cover the
+500-control-step horizon.  Synthetic seeded inputs stand in for a dataset.
+
+Lines printed (rank 0, one JSON line):
+  * value: device-resident throughput (actions already in HBM, zero-copy
+    torch path), CUDA events on the launching stream around each timed
+    advance, L2 flushed (256 MiB write) between timed advances;
+  * e2e: the same metric through the reference-shaped C ABI call
+    mr_task_rollout_advance with host buffers (actions H2D, status /
+    contacts / observations / final q D2H inside the timed region);
+  * roofline of the control-step kernel against measured HBM bandwidth;
+  * cpu_baseline: the reference's own FP64 CPU contact step
+    (stepControlledArticulatedWorldCpu, compiled from its sources) timed on
+    this host's cores over a bounded sample of the same workload.
+
+``--impl reference`` times only that CPU reference (rank 0; other ranks exit).
+Multi-GPU (torchrun): one process per GPU, each running its own 4096-env
+replica; no collective on the data path; value = total env-steps / max time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+ENVS = 4096
+HORIZON = 25          # control steps per advance (one bench step)
+SUBSTEPS = 4
+ITERATIONS = 8
+CONTROL_DT = 0.02
+SEED = 2026
+METRIC = "contact env-steps/s"
+UNIT = "env-steps/s"
+WORKLOAD = "tree29 floating 29-DoF humanoid contact: 4096 envs, 20 ms control = 4 x 5 ms microsteps, 8 temporalCone iterations"
+CPU_SAMPLE_ENVS = 512
+CPU_SAMPLE_STEPS = 10
+
+
+def _config(n_gpus: int) -> dict:
+    return {
+        "workload": WORKLOAD,
+        "envs_per_gpu": ENVS,
+        "control_steps_per_bench_step": HORIZON,
+        "microsteps": SUBSTEPS,
+        "velocity_iterations": ITERATIONS,
+        "dt_ms": 1000.0 * CONTROL_DT / SUBSTEPS,
+        "l2": "flushed (256 MiB write) between timed steps",
+        "parallelism": f"replicas x{n_gpus}",
+    }
+
+
+def _algorithmic_bytes_per_env_step(nq: int, nv: int, n_act: int, points: float, manifolds: float) -> float:
+    # State in+out, actions in, manifold points / headers in+out, status
+    # (no free scene bodies in this world).
+    return 8.0 * (nq + nv) + 4.0 * n_act + 2.0 * (48.0 * points + 24.0 * manifolds) + 4.0
+
+
+def _measured_peaks() -> dict:
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.is_file():
+        data = json.loads(path.read_text())
+        return {"hbm_gbs": float(data["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def _profile_traffic() -> float | None:
+    """DRAM bytes per control-step launch from the committed ncu summary."""
+
+    path = ROOT / "profiles" / "control_step_contact_tree29.md"
+    if not path.is_file():
+        return None
+    for line in path.read_text().splitlines():
+        if line.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    QUERY = (
+        "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+        "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    )
+
+    def __init__(self, device_index: int) -> None:
+        self.device_index = device_index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self) -> "ClockSampler":
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file,
+                stderr=subprocess.DEVNULL,
+            )
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc: object) -> None:
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        self.file.flush()
+        self.file.seek(0)
+        rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax = max(smax, float(r[2]))
+                for name, flag in zip(names, r[5:9]):
+                    if flag.strip().lower() == "active":
+                        reasons.add(name)
+            except (ValueError, IndexError):
+                continue
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": smax or None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+def cpu_reference_sample(world_state, actions_np, threads: int) -> dict:
+    """Times the reference's own CPU contact step over a bounded sample."""
+
+    import numi_lab_b200 as nb
+    from oracle import Reference
+
+    q, v, friction = world_state
+    records = nb.compile_model("tree29", SEED)
+    ref = Reference(records, CONTROL_DT / SUBSTEPS, friction=float(np.mean(friction)))
+    qs = q[:CPU_SAMPLE_ENVS].astype(np.float64).copy()
+    vs = v[:CPU_SAMPLE_ENVS].astype(np.float64).copy()
+    acts = np.ascontiguousarray(actions_np[:CPU_SAMPLE_STEPS, :CPU_SAMPLE_ENVS], np.float32)
+    secs, failed = ref.run(qs, vs, acts, SUBSTEPS, threads, 1)
+    env_steps = CPU_SAMPLE_ENVS * CPU_SAMPLE_STEPS
+    return {
+        "value": env_steps / secs,
+        "unit": UNIT,
+        "cores": threads,
+        "kind": "reference",
+        "sample": f"{CPU_SAMPLE_ENVS} envs x {CPU_SAMPLE_STEPS} control steps of the same workload "
+        f"(stepControlledArticulatedWorldCpu, quality-Newton contact solve, FP64), {failed} failed substeps",
+        "seconds": secs,
+    }
+
+
+def run_reference_arm(args, rank: int) -> None:
+    if rank != 0:
+        return
+    import numi_lab_b200 as nb
+    from oracle import REF_LIB
+
+    if not REF_LIB.is_file():
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU core library oracle/_ref/libnumiref.so was not built"}))
+        return
+    threads = os.cpu_count() or 1
+    q, v, f = nb.sample_reset("tree29", SEED, SEED, 0, CPU_SAMPLE_ENVS)
+    rng = np.random.default_rng(SEED)
+    samples = []
+    for i in range(args.warmup + args.steps):
+        actions = rng.normal(0.0, 0.3, size=(CPU_SAMPLE_STEPS, CPU_SAMPLE_ENVS, 29)).astype(np.float32)
+        res = cpu_reference_sample((q, v, f), actions, threads)
+        if i >= args.warmup:
+            samples.append(res)
+    value = float(np.mean([s["value"] for s in samples]))
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": float(np.mean([s["seconds"] for s in samples]) * 1e3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded)",
+        "config": {**_config(args.gpus), "bench_step": f"{CPU_SAMPLE_ENVS} envs x {CPU_SAMPLE_STEPS} control steps on CPU"},
+        "cpu_baseline": {k: samples[0][k] for k in ("kind", "cores", "sample")} | {"value": value, "unit": UNIT},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main() -> None:
+    parser = argparse.ArgumentParser()
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=20)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", default="native", choices=["native", "reference"])
+    parser.add_argument("--no-cpu-baseline", action="store_true")
+    args = parser.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+
+    import torch
+
+    import numi_lab_b200 as nb
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world_size > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = dist_mod
+
+    device = torch.device("cuda", local_rank)
+    world = nb.World("tree29", ENVS, substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT,
+                     seed=SEED + 7919 * rank)
+    gen = torch.Generator(device=device).manual_seed(SEED + rank)
+    total_steps = args.warmup + args.steps
+    actions = 0.3 * torch.randn((total_steps, HORIZON, ENVS, world.action_count), device=device, generator=gen)
+    obs = torch.empty((HORIZON, ENVS, world.observation_count), device=device)
+    status = torch.empty((HORIZON, ENVS), device=device, dtype=torch.int32)
+    flush = torch.empty(256 * 1024 * 1024 // 4, device=device, dtype=torch.float32)
+    stream = torch.cuda.current_stream(device)
+
+    def barrier():
+        torch.cuda.synchronize(device)
+        if dist is not None:
+            dist.barrier()
+
+    # Warm-up (graph capture happens on the first advance).
+    for i in range(args.warmup):
+        world.step(actions[i], observations=obs, status=status)
+    barrier()
+    warm_state = world.state()
+
+    # Device-resident timed region: per-step CUDA events, L2 flushed between steps.
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    failures = torch.zeros((), device=device, dtype=torch.int64)
+    contacts_hist = []
+    with ClockSampler(device.index if device.index is not None else 0) as clocks:
+        barrier()
+        for i in range(args.steps):
+            flush.fill_(float(i))
+            starts[i].record(stream)
+            world.step(actions[args.warmup + i], observations=obs, status=status)
+            stops[i].record(stream)
+            failures += (status != 0).sum()
+        barrier()
+    clock_summary = clocks.summary()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, stops)]
+    total_ms = float(sum(step_ms))
+    max_ms = total_ms
+    if dist is not None:
+        t = torch.tensor([total_ms], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        max_ms = float(t.item())
+    env_steps = ENVS * HORIZON * args.steps * world_size
+    value = env_steps / (max_ms / 1e3)
+
+    # Contact statistics for the algorithmic byte count (one extra advance
+    # with counters, outside the timed region).
+    _, _, counters = world.step(actions[0], wait=True)
+    q_, v_, man_ = world.state()
+    counts = np.array([m.count for m in man_], np.int64).reshape(ENVS, world.pair_count)
+    mean_points = float(counts.sum(axis=1).mean())
+    mean_manifolds = float((counts > 0).sum(axis=1).mean())
+
+    # End-to-end through the reference-shaped C ABI with host buffers.
+    world.set_state(*warm_state)
+    world.set_state_readback(True)
+    host_actions = [actions[args.warmup + i].cpu().numpy() for i in range(min(args.steps, 5))]
+    world.advance_host(host_actions[0], raise_on_failure=False)  # warm the host path
+    barrier()
+    t0 = time.perf_counter()
+    for a in host_actions:
+        world.advance_host(a, raise_on_failure=False)
+    e2e_secs = time.perf_counter() - t0
+    e2e_value = ENVS * HORIZON * len(host_actions) * world_size / e2e_secs
+    if dist is not None:
+        t = torch.tensor([e2e_secs], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_value = ENVS * HORIZON * len(host_actions) * world_size / float(t.item())
+    h2d = HORIZON * ENVS * world.action_count * 4
+    d2h = HORIZON * ENVS * (4 + 4 + 4 * world.observation_count) + ENVS * world.nq * 4
+    world.set_state_readback(False)
+
+    launches_per_step = HORIZON  # one control-step kernel per control step
+    kernel_ms = (max_ms / world_size if dist is None else total_ms) / (args.steps * launches_per_step)
+    bytes_per_env_step = _algorithmic_bytes_per_env_step(world.nq, world.nv, world.action_count, mean_points, mean_manifolds)
+    achieved = bytes_per_env_step * ENVS / (kernel_ms / 1e3) / 1e9
+    peaks = _measured_peaks()
+    traffic = _profile_traffic()
+
+    cpu = None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        try:
+            host_state = (warm_state[0], warm_state[1], world.friction_scales())
+            cpu = cpu_reference_sample(host_state, actions[args.warmup, :CPU_SAMPLE_STEPS].cpu().numpy(), os.cpu_count() or 1)
+            cpu.pop("seconds", None)
+        except (FileNotFoundError, OSError, RuntimeError) as exc:
+            cpu = {"unavailable": str(exc)}
+
+    if rank == 0:
+        step_sorted = sorted(step_ms)
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world_size,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": max_ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded)",
+            "config": _config(world_size),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": {
+                "bound": "hbm",
+                "achieved": achieved,
+                "peak": peaks["hbm_gbs"],
+                "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"],
+                "traffic": traffic,
+                "peak_source": peaks["source"],
+                "algorithmic_bytes_per_env_step": bytes_per_env_step,
+                "kernel_ms_per_launch": kernel_ms,
+            },
+            "cpu_baseline": cpu,
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": {k: clock_summary[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+            "latency_ms_per_advance": {"p50": step_sorted[len(step_sorted) // 2],
+                                        "p99": step_sorted[min(len(step_sorted) - 1, int(0.99 * len(step_sorted)))]},
+            "failed_env_steps": int(failures.item()),
+            "mean_active_contacts": mean_points,
+            "mean_manifolds": mean_manifolds,
+        }
+        print(json.dumps(line))
+    world.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

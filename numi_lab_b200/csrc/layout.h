@@ -29,8 +29,8 @@ enum ContactWord : int {
 };
 
 struct WarpLayout {
-    int body_pose, body_V, body_CV, body_IA, body_PA, body_U, body_Du, body_A;
-    int dof_S;
+    int body_pose, body_V, body_CV, body_IA, body_PA, body_U, body_Du, body_A, body_r;
+    int dof_S, dof_J;
     int q, qc, qn, v, vc, vf, tau, qdd, tgt;
     int misc;
     int manifolds, contacts, G, R, L;
@@ -52,7 +52,9 @@ __host__ __device__ inline WarpLayout make_layout(int nb, int nv, int nq, int np
     L.body_U = take(nb * 6);
     L.body_Du = take(nb * 2);
     L.body_A = take(nb * 6);
+    L.body_r = take(nb * 4);
     L.dof_S = take(nv * 6);
+    L.dof_J = take(nv * 8);
     L.q = take(nq);
     L.qc = take(nq);
     L.qn = take(nq);

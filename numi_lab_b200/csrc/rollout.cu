@@ -248,6 +248,7 @@ struct MRTaskRolloutHandle {
     std::string device_name;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;  // caller-stream handoff
 
     DeviceBuffer<numi::DeviceModel> d_model;
     DeviceBuffer<float> d_q, d_v, d_manifolds, d_reset_q, d_reset_v, d_friction;
@@ -281,6 +282,8 @@ struct MRTaskRolloutHandle {
         for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
         if (ev_start) cudaEventDestroy(ev_start);
         if (ev_stop) cudaEventDestroy(ev_stop);
+        if (ev_in) cudaEventDestroy(ev_in);
+        if (ev_out) cudaEventDestroy(ev_out);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -491,6 +494,8 @@ MR_API MRTaskRolloutHandle* mr_create_task_rollout(const MRRunManifestC* manifes
         check(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking), "stream");
         check(cudaEventCreate(&h.ev_start), "event");
         check(cudaEventCreate(&h.ev_stop), "event");
+        check(cudaEventCreateWithFlags(&h.ev_in, cudaEventDisableTiming), "event");
+        check(cudaEventCreateWithFlags(&h.ev_out, cudaEventDisableTiming), "event");
         h.d_model.resize(1);
         check(cudaMemcpy(h.d_model.ptr, &h.dmodel, sizeof(numi::DeviceModel), cudaMemcpyHostToDevice), "upload model");
         const size_t nq = m.world.nq, nv = m.world.nv;
@@ -624,7 +629,14 @@ MR_API int mr_task_rollout_advance_device(MRTaskRolloutHandle* handle, const flo
         if (!device_actions) throw std::invalid_argument("device_actions is null");
         if (control_step_count == 0) throw std::invalid_argument("control_step_count must be positive");
         MRTaskRolloutHandle& h = *handle;
-        cudaStream_t s = cuda_stream ? reinterpret_cast<cudaStream_t>(cuda_stream) : h.stream;
+        // The horizon runs (and is graph-captured) on the rollout's own
+        // stream; events order it after the caller's prior work and the
+        // caller's later work after it.  cuda_stream 0 is the legacy default
+        // stream, which a non-blocking stream does not otherwise wait for.
+        cudaStream_t caller = reinterpret_cast<cudaStream_t>(cuda_stream);
+        cudaStream_t s = h.stream;
+        check(cudaEventRecord(h.ev_in, caller), "event");
+        check(cudaStreamWaitEvent(s, h.ev_in, 0), "stream wait");
         const size_t cells = static_cast<size_t>(control_step_count) * h.envs;
         std::uint32_t* status = device_status_codes;
         if (!status) {
@@ -635,6 +647,8 @@ MR_API int mr_task_rollout_advance_device(MRTaskRolloutHandle* handle, const flo
         const auto wall0 = std::chrono::steady_clock::now();
         if (advance) check(cudaEventRecord(h.ev_start, s), "event");
         h.run(control_step_count, device_actions, device_reset_masks, device_observations, status, h.d_contacts.ptr, s);
+        check(cudaEventRecord(h.ev_out, s), "event");
+        check(cudaStreamWaitEvent(caller, h.ev_out, 0), "stream wait");
         if (advance) {
             check(cudaMemcpyAsync(h.h_stats.ptr, h.d_stats.ptr, numi::kStatCount * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "stats D2H");
             check(cudaEventRecord(h.ev_stop, s), "event");

@@ -88,11 +88,76 @@ __device__ void compute_drives(const Warp& w) {
     }
 }
 
+// Packed symmetric 6x6 spatial inertia shift X^T I X for a translation r
+// from a child COM to its parent COM (ArticulatedABA.metal:1230-1262 with
+// motionTransformElement :160-190, written out in 3x3 blocks):
+// I = [[A, B], [B^T, D]], E = [r]x:  A' = A - B E + E B^T - E D E,
+// B' = B + E D, D' = D.
+__device__ void shift_inertia(const float* I, float3 r, float* out) {
+    float A[3][3], B[3][3], D[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            A[i][j] = I[sym6(i, j)];
+            B[i][j] = I[sym6(3 + j, i)];
+            D[i][j] = I[sym6(3 + i, 3 + j)];
+        }
+    const float E[3][3] = {{0.0f, -r.z, r.y}, {r.z, 0.0f, -r.x}, {-r.y, r.x, 0.0f}};
+    float ED[3][3], BE[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            float ed = 0.0f, be = 0.0f;
+            for (int k = 0; k < 3; ++k) {
+                ed = fmaf(E[i][k], D[k][j], ed);
+                be = fmaf(B[i][k], E[k][j], be);
+            }
+            ED[i][j] = ed;
+            BE[i][j] = be;
+        }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j <= i; ++j) {
+            float ede = 0.0f;
+            for (int k = 0; k < 3; ++k) ede = fmaf(ED[i][k], E[k][j], ede);
+            // E B^T (i, j) = sum_k E[i][k] B[j][k] = -(B E)^T... written directly:
+            float ebt = 0.0f;
+            for (int k = 0; k < 3; ++k) ebt = fmaf(E[i][k], B[j][k], ebt);
+            out[sym6(i, j)] = A[i][j] - BE[i][j] + ebt - ede;
+        }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) out[sym6(3 + j, i)] = B[i][j] + ED[i][j];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j <= i; ++j) out[sym6(3 + i, 3 + j)] = D[i][j];
+}
+
+// Body spatial inertia about its own COM in world axes: [[R Ib R^T, 0], [0, m 1]].
+__device__ void body_inertia(const DeviceModel& M, int b, float4 qb, float* I6, float Iw[3][3]) {
+    const float m = M.mass_damping[b].x;
+    const float4 di = M.inertia_diag[b];
+    const float4 of = M.inertia_off[b];
+    const float3 c0 = qrot(qb, f3(1.0f, 0.0f, 0.0f));
+    const float3 c1 = qrot(qb, f3(0.0f, 1.0f, 0.0f));
+    const float3 c2 = qrot(qb, f3(0.0f, 0.0f, 1.0f));
+    const float Ib[3][3] = {{di.x, of.x, of.y}, {of.x, di.y, of.z}, {of.y, of.z, di.z}};
+    const float R[3][3] = {{c0.x, c1.x, c2.x}, {c0.y, c1.y, c2.y}, {c0.z, c1.z, c2.z}};
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            float acc = 0.0f;
+            for (int k = 0; k < 3; ++k)
+                for (int l2 = 0; l2 < 3; ++l2) acc = fmaf(R[i][k] * Ib[k][l2], R[j][l2], acc);
+            Iw[i][j] = acc;
+        }
+    for (int e = 0; e < 21; ++e) I6[e] = 0.0f;
+    for (int i = 0; i < 3; ++i) {
+        for (int j = 0; j <= i; ++j) I6[sym6(i, j)] = Iw[i][j];
+        I6[sym6(3 + i, 3 + i)] = m;
+    }
+}
+
 // ---------------------------------------------------------------------------
-// Articulated-body algorithm (ArticulatedABA.metal:352-1578), level-parallel:
-// lanes own the bodies of one tree level; parents pull their children's
-// articulated inertia and bias in a fixed order, so the result is
-// deterministic without atomics.
+// Articulated-body algorithm (ArticulatedABA.metal:352-1578): per-body COM
+// frames in world axes, classical accelerations, 21-entry inertias; tree
+// levels run lane-parallel.  Each body shifts its articulated inertia and
+// bias into its parent's frame; parents pull their children's shifted
+// contributions in a fixed order, so sums are deterministic without atomics.
 // ---------------------------------------------------------------------------
 __device__ bool aba(const Warp& w) {
     const DeviceModel& M = *w.M;
@@ -104,14 +169,16 @@ __device__ bool aba(const Warp& w) {
     const float* tau = s + L.tau;
     float* qdd = s + L.qdd;
     float* pose = s + L.body_pose;
-    float* V = s + L.body_V;
-    float* CV = s + L.body_CV;
+    float* V = s + L.body_V;     // (omega, v_com)
+    float* CV = s + L.body_CV;   // bias accelerations (angular, linear)
     float* IA = s + L.body_IA;
     float* PA = s + L.body_PA;
     float* U = s + L.body_U;
     float* Du = s + L.body_Du;
     float* A = s + L.body_A;
-    float* S = s + L.dof_S;
+    float* R = s + L.body_r;     // parent COM -> body COM
+    float* S = s + L.dof_S;      // motion subspace about the moving body's COM
+    float* J = s + L.dof_J;      // joint axis (3), origin (3), prismatic flag
     const int lane = w.lane;
 
     // Non-finite inputs fail the step before any use
@@ -123,43 +190,47 @@ __device__ bool aba(const Warp& w) {
     __syncwarp();
     if (as_int(misc[kMiscStatus]) != MR_STEP_SUCCESS) return false;
 
-    // Root pose, velocity and root-DoF motion subspaces.
+    // Root pose and velocity; root-DoF subspaces and Jacobian axes.
     if (lane == 0) {
-        unsigned code = MR_STEP_SUCCESS;
         if (M.floating) {
             float4 rq;
             const float3 c0 = f3(q[0], q[1], q[2]);
             if (!finite3(c0) || !qnormalize(make_float4(q[3], q[4], q[5], q[6]), rq, true)) {
-                code = MR_STEP_NONFINITE_INPUT;
-                set_status(misc, code, 0u);
+                set_status(misc, MR_STEP_NONFINITE_INPUT, 0u);
             } else {
                 st3(pose, c0);
                 st4(pose + 4, rq);
-                st3(misc + kMiscP0, c0);
-                // V = (omega, v_com) about p0 = root COM.
                 V[0] = v[3]; V[1] = v[4]; V[2] = v[5];
                 V[3] = v[0]; V[4] = v[1]; V[5] = v[2];
             }
         } else {
             st3(pose, f3(0.0f, 0.0f, 0.0f));
             st4(pose + 4, make_float4(0.0f, 0.0f, 0.0f, 1.0f));
-            st3(misc + kMiscP0, f3(0.0f, 0.0f, 0.0f));
             for (int i = 0; i < 6; ++i) V[i] = 0.0f;
         }
+        pose[3] = 0.0f;
         for (int i = 0; i < 6; ++i) CV[i] = 0.0f;
-    }
-    if (M.floating && lane < 6) {
-        float* Sd = S + lane * 6;
-        for (int i = 0; i < 6; ++i) Sd[i] = 0.0f;
-        // lin DoF k -> (0, e_k); ang DoF k -> (e_k, 0)
-        if (lane < 3) Sd[3 + lane] = 1.0f;
-        else Sd[lane - 3] = 1.0f;
+        R[0] = R[1] = R[2] = 0.0f;
     }
     __syncwarp();
     if (as_int(misc[kMiscStatus]) != MR_STEP_SUCCESS) return false;
-    const float3 p0 = ld3(misc + kMiscP0);
+    if (M.floating && lane < 6) {
+        float* Sd = S + lane * 6;
+        float* Jd = J + lane * 8;
+        for (int i = 0; i < 6; ++i) Sd[i] = 0.0f;
+        // lin DoF k -> (0, e_k); ang DoF k -> (e_k, 0) about the root COM.
+        if (lane < 3) Sd[3 + lane] = 1.0f;
+        else Sd[lane - 3] = 1.0f;
+        const int k = lane < 3 ? lane : lane - 3;
+        Jd[0] = k == 0 ? 1.0f : 0.0f;
+        Jd[1] = k == 1 ? 1.0f : 0.0f;
+        Jd[2] = k == 2 ? 1.0f : 0.0f;
+        Jd[3] = pose[0]; Jd[4] = pose[1]; Jd[5] = pose[2];
+        Jd[6] = lane < 3 ? 1.0f : 0.0f;  // translational root DoFs act like prismatic axes
+        Jd[7] = 0.0f;
+    }
 
-    // Forward kinematics, velocities, motion subspaces, velocity products.
+    // Forward kinematics: poses, twists, subspaces, bias accelerations.
     for (int l = 0; l < M.n_levels; ++l) {
         const int off = M.level_offsets[l];
         const int cnt = M.level_offsets[l + 1] - off;
@@ -170,7 +241,7 @@ __device__ bool aba(const Warp& w) {
             const int type = M.joint_type[b];
             const float3 cp = ld3(pose + p * 8);
             const float4 qp = ld4(pose + p * 8 + 4);
-            const float4 prj = qmul(qp, M.parent_rotation[b]);
+            const float4 pj = qmul(qp, M.parent_rotation[b]);
             const float3 axis = xyz(M.axis[b]);
             float4 motion = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
             float qj = 0.0f, qdj = 0.0f;
@@ -184,103 +255,73 @@ __device__ bool aba(const Warp& w) {
                 }
             }
             float4 qb;
-            if (!qnormalize(qmul(qmul(prj, motion), M.child_rotation_conj[b]), qb, false)) {
+            if (!qnormalize(qmul(qmul(pj, motion), M.child_rotation_conj[b]), qb, false)) {
                 set_status(misc, MR_STEP_NONFINITE_RESULT, static_cast<unsigned>(b));
                 qb = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
             }
-            const float3 aw = qrot(prj, axis);
+            const float3 ja = qrot(pj, axis);
             const bool prismatic = type == MR_JOINT_PRISMATIC;
-            float3 o = cp + qrot(qp, xyz(M.parent_anchor[b]));
-            if (prismatic) o = o + aw * qj;
-            const float3 cb = o - qrot(qb, xyz(M.child_anchor[b]));
+            const bool has = d >= 0;
+            float3 jp = cp + qrot(qp, xyz(M.parent_anchor[b]));
+            if (prismatic) jp = jp + ja * qj;
+            const float3 ca = qrot(qb, xyz(M.child_anchor[b]));
+            const float3 cb = jp - ca;
+            const float3 ptj = jp - cp;
             st3(pose + b * 8, cb);
             pose[b * 8 + 3] = 0.0f;
             st4(pose + b * 8 + 4, qb);
-            float sv[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-            if (d >= 0) {
-                if (prismatic) {
-                    sv[3] = aw.x; sv[4] = aw.y; sv[5] = aw.z;
-                } else {
-                    const float3 sl = cross3(aw, p0 - o);
-                    sv[0] = aw.x; sv[1] = aw.y; sv[2] = aw.z;
-                    sv[3] = sl.x; sv[4] = sl.y; sv[5] = sl.z;
-                }
-                for (int i = 0; i < 6; ++i) S[d * 6 + i] = sv[i];
+            st3(R + b * 4, cb - cp);
+            const float3 wp = f3(V[p * 6 + 0], V[p * 6 + 1], V[p * 6 + 2]);
+            const float3 vp = f3(V[p * 6 + 3], V[p * 6 + 4], V[p * 6 + 5]);
+            const float3 wb = wp + ((has && !prismatic) ? ja * qdj : f3(0.0f, 0.0f, 0.0f));
+            const float3 vb = vp + cross3(wp, ptj) + (prismatic ? ja * qdj : f3(0.0f, 0.0f, 0.0f)) - cross3(wb, ca);
+            const float3 ma = (has && !prismatic) ? ja : f3(0.0f, 0.0f, 0.0f);
+            const float3 ml = prismatic ? ja : (has ? -cross3(ja, ca) : f3(0.0f, 0.0f, 0.0f));
+            const float3 ba = (has && !prismatic) ? cross3(wp, ja) * qdj : f3(0.0f, 0.0f, 0.0f);
+            const float3 pc = prismatic ? cross3(wp, ja) * (2.0f * qdj) : f3(0.0f, 0.0f, 0.0f);
+            const float3 bl = cross3(wp, cross3(wp, ptj)) + pc - cross3(ba, ca) - cross3(wb, cross3(wb, ca));
+            V[b * 6 + 0] = wb.x; V[b * 6 + 1] = wb.y; V[b * 6 + 2] = wb.z;
+            V[b * 6 + 3] = vb.x; V[b * 6 + 4] = vb.y; V[b * 6 + 5] = vb.z;
+            CV[b * 6 + 0] = ba.x; CV[b * 6 + 1] = ba.y; CV[b * 6 + 2] = ba.z;
+            CV[b * 6 + 3] = bl.x; CV[b * 6 + 4] = bl.y; CV[b * 6 + 5] = bl.z;
+            if (has) {
+                float* Sd = S + d * 6;
+                Sd[0] = ma.x; Sd[1] = ma.y; Sd[2] = ma.z;
+                Sd[3] = ml.x; Sd[4] = ml.y; Sd[5] = ml.z;
+                float* Jd = J + d * 8;
+                Jd[0] = ja.x; Jd[1] = ja.y; Jd[2] = ja.z;
+                Jd[3] = jp.x; Jd[4] = jp.y; Jd[5] = jp.z;
+                Jd[6] = prismatic ? 1.0f : 0.0f;
+                Jd[7] = 0.0f;
             }
-            float Vb[6];
-            for (int i = 0; i < 6; ++i) Vb[i] = V[p * 6 + i] + sv[i] * qdj;
-            for (int i = 0; i < 6; ++i) V[b * 6 + i] = Vb[i];
-            // c = V x_m (S qd)
-            const float3 wv = f3(Vb[0], Vb[1], Vb[2]);
-            const float3 vv = f3(Vb[3], Vb[4], Vb[5]);
-            const float3 ja = f3(sv[0] * qdj, sv[1] * qdj, sv[2] * qdj);
-            const float3 jl = f3(sv[3] * qdj, sv[4] * qdj, sv[5] * qdj);
-            const float3 ca = cross3(wv, ja);
-            const float3 cl = cross3(wv, jl) + cross3(vv, ja);
-            CV[b * 6 + 0] = ca.x; CV[b * 6 + 1] = ca.y; CV[b * 6 + 2] = ca.z;
-            CV[b * 6 + 3] = cl.x; CV[b * 6 + 4] = cl.y; CV[b * 6 + 5] = cl.z;
-            if (!finite3(cb) || !finite3(ca) || !finite3(cl) || !finite3(wv) || !finite3(vv))
+            if (!finite3(cb) || !finite3(wb) || !finite3(vb) || !finite3(bl))
                 set_status(misc, MR_STEP_NONFINITE_RESULT, static_cast<unsigned>(b));
         }
         __syncwarp();
     }
     if (as_int(misc[kMiscStatus]) != MR_STEP_SUCCESS) return false;
 
-    // Spatial inertia about p0 and velocity-dependent bias of every body.
+    // Rigid inertia and velocity-dependent bias of every body about its COM.
     if (lane < M.nb) {
         const int b = lane;
-        const float3 cb = ld3(pose + b * 8);
         const float4 qb = ld4(pose + b * 8 + 4);
         const float4 md = M.mass_damping[b];
-        const float m = md.x;
-        const float4 di = M.inertia_diag[b];
-        const float4 of = M.inertia_off[b];
-        // World inertia about the COM: R Ib R^T.
-        const float3 c0 = qrot(qb, f3(1.0f, 0.0f, 0.0f));
-        const float3 c1 = qrot(qb, f3(0.0f, 1.0f, 0.0f));
-        const float3 c2 = qrot(qb, f3(0.0f, 0.0f, 1.0f));
-        const float Ib[3][3] = {{di.x, of.x, of.y}, {of.x, di.y, of.z}, {of.y, of.z, di.z}};
-        const float R[3][3] = {{c0.x, c1.x, c2.x}, {c0.y, c1.y, c2.y}, {c0.z, c1.z, c2.z}};
         float Iw[3][3];
-        for (int i = 0; i < 3; ++i)
-            for (int j = 0; j < 3; ++j) {
-                float acc = 0.0f;
-                for (int k = 0; k < 3; ++k)
-                    for (int l2 = 0; l2 < 3; ++l2) acc = fmaf(R[i][k] * Ib[k][l2], R[j][l2], acc);
-                Iw[i][j] = acc;
-            }
-        const float3 r = cb - p0;
-        const float rr = dot3(r, r);
-        const float rv[3] = {r.x, r.y, r.z};
         float* I6 = IA + b * 21;
-        for (int i = 0; i < 3; ++i)
-            for (int j = 0; j <= i; ++j) I6[sym6(i, j)] = Iw[i][j] + m * ((i == j ? rr : 0.0f) - rv[i] * rv[j]);
-        // [r]x entries: B = m [r]x at rows 0-2 / cols 3-5; lower triangle holds B^T.
-        const float rx[3][3] = {{0.0f, -r.z, r.y}, {r.z, 0.0f, -r.x}, {-r.y, r.x, 0.0f}};
-        for (int i = 0; i < 3; ++i)
-            for (int j = 0; j < 3; ++j) I6[sym6(3 + j, i)] = m * rx[i][j];
-        for (int i = 0; i < 3; ++i)
-            for (int j = 0; j <= i; ++j) I6[sym6(3 + i, 3 + j)] = i == j ? m : 0.0f;
-        float Vb[6], h6[6];
-        for (int i = 0; i < 6; ++i) Vb[i] = V[b * 6 + i];
-        sym6_mul(I6, Vb, h6);
-        const float3 om = f3(Vb[0], Vb[1], Vb[2]);
-        const float3 vp = f3(Vb[3], Vb[4], Vb[5]);
-        const float3 ha = f3(h6[0], h6[1], h6[2]);
-        const float3 hl = f3(h6[3], h6[4], h6[5]);
-        float3 ba = cross3(om, ha) + cross3(vp, hl);
-        float3 bl = cross3(om, hl);
-        const float3 fg = m * f3(M.gravity[0], M.gravity[1], M.gravity[2]);
-        ba = ba - cross3(r, fg);
-        bl = bl - fg;
+        body_inertia(M, b, qb, I6, Iw);
+        const float3 om = f3(V[b * 6 + 0], V[b * 6 + 1], V[b * 6 + 2]);
+        const float3 vc = f3(V[b * 6 + 3], V[b * 6 + 4], V[b * 6 + 5]);
+        const float3 Iom = f3(Iw[0][0] * om.x + Iw[0][1] * om.y + Iw[0][2] * om.z,
+                              Iw[1][0] * om.x + Iw[1][1] * om.y + Iw[1][2] * om.z,
+                              Iw[2][0] * om.x + Iw[2][1] * om.y + Iw[2][2] * om.z);
+        float3 bt = cross3(om, Iom);
+        float3 bf = -(md.x * f3(M.gravity[0], M.gravity[1], M.gravity[2]));
         if (M.apply_damping) {
-            const float3 vcom = vp + cross3(om, r);
-            const float3 fd = md.y * vcom;
-            ba = ba + md.z * om + cross3(r, fd);
-            bl = bl + fd;
+            bt = bt + md.z * om;
+            bf = bf + md.y * vc;
         }
         float* pa = PA + b * 6;
-        pa[0] = ba.x; pa[1] = ba.y; pa[2] = ba.z; pa[3] = bl.x; pa[4] = bl.y; pa[5] = bl.z;
+        pa[0] = bt.x; pa[1] = bt.y; pa[2] = bt.z; pa[3] = bf.x; pa[4] = bf.y; pa[5] = bf.z;
         if (b == 0 && M.floating) {
             for (int k = 0; k < 3; ++k) {
                 I6[sym6(3 + k, 3 + k)] += M.armature_eff[k];
@@ -292,7 +333,7 @@ __device__ bool aba(const Warp& w) {
     }
     __syncwarp();
 
-    // Backward sweep: articulated inertia and bias, children pulled in order.
+    // Backward sweep.
     for (int l = M.n_levels - 1; l >= 0; --l) {
         const int off = M.level_offsets[l];
         const int cnt = M.level_offsets[l + 1] - off;
@@ -306,9 +347,9 @@ __device__ bool aba(const Warp& w) {
                 for (int e = 0; e < 6; ++e) pa[e] += PA[c * 6 + e];
             }
             const int d = M.body_dof[b];
-            float t[6], ic[6];
+            float prop[6], ic[6];
             sym6_mul(I6, CV + b * 6, ic);
-            for (int e = 0; e < 6; ++e) t[e] = pa[e] + ic[e];
+            for (int e = 0; e < 6; ++e) prop[e] = pa[e] + ic[e];
             if (d >= 0) {
                 const float* sd = S + d * 6;
                 float u6[6];
@@ -320,18 +361,24 @@ __device__ bool aba(const Warp& w) {
                 if (!(D > floor) || !isfinite(D)) {
                     set_status(misc, MR_STEP_FACTORIZATION_FAILED, static_cast<unsigned>(d));
                 } else {
-                    const float u = tau[d] - dot6(sd, t);
+                    const float u = tau[d] - dot6(sd, prop);
                     const float invD = 1.0f / D;
                     for (int e = 0; e < 6; ++e) U[b * 6 + e] = u6[e];
                     Du[b * 2 + 0] = D;
                     Du[b * 2 + 1] = u;
+                    for (int e = 0; e < 6; ++e) prop[e] += u6[e] * (u * invD);
                     for (int i = 0; i < 6; ++i)
                         for (int j = 0; j <= i; ++j) I6[sym6(i, j)] -= u6[i] * u6[j] * invD;
-                    for (int e = 0; e < 6; ++e) pa[e] = t[e] + u6[e] * (u * invD);
                 }
-            } else {
-                for (int e = 0; e < 6; ++e) pa[e] = t[e];
             }
+            // Contribution in the parent's frame, left in this body's slots.
+            const float3 r = ld3(R + b * 4);
+            float shifted[21];
+            shift_inertia(I6, r, shifted);
+            for (int e = 0; e < 21; ++e) I6[e] = shifted[e];
+            const float3 pf = f3(prop[3], prop[4], prop[5]);
+            const float3 pt = f3(prop[0], prop[1], prop[2]) + cross3(r, pf);
+            pa[0] = pt.x; pa[1] = pt.y; pa[2] = pt.z; pa[3] = pf.x; pa[4] = pf.y; pa[5] = pf.z;
         }
         __syncwarp();
     }
@@ -348,7 +395,7 @@ __device__ bool aba(const Warp& w) {
     __syncwarp();
     if (lane == 0) {
         if (M.floating) {
-            // 6x6 Cholesky of the root articulated inertia; A0 = -IA^-1 pA.
+            // 6x6 Cholesky of the root articulated inertia; a0 = -IA^-1 pA.
             float Lf[36];
             float maxI = 0.0f;
             for (int e = 0; e < 21; ++e) maxI = fmaxf(maxI, fabsf(IA[e]));
@@ -379,11 +426,7 @@ __device__ bool aba(const Warp& w) {
                     x[i] = val / Lf[i * 6 + i];
                 }
                 for (int i = 0; i < 6; ++i) A[i] = x[i];
-                // Generalized root acceleration: d/dt of (v_com, omega).
-                const float3 om = f3(V[0], V[1], V[2]);
-                const float3 vc = f3(V[3], V[4], V[5]);
-                const float3 lin = f3(x[3], x[4], x[5]) + cross3(om, vc);
-                qdd[0] = lin.x; qdd[1] = lin.y; qdd[2] = lin.z;
+                qdd[0] = x[3]; qdd[1] = x[4]; qdd[2] = x[5];
                 qdd[3] = x[0]; qdd[4] = x[1]; qdd[5] = x[2];
             }
         } else {
@@ -401,16 +444,22 @@ __device__ bool aba(const Warp& w) {
             const int b = M.level_bodies[off + lane];
             const int p = M.parent[b];
             const int d = M.body_dof[b];
-            float ap[6];
-            for (int e = 0; e < 6; ++e) ap[e] = A[p * 6 + e];
-            float ab[6];
-            for (int e = 0; e < 6; ++e) ab[e] = ap[e] + CV[b * 6 + e];
+            const float3 r = ld3(R + b * 4);
+            const float3 pa_ = f3(A[p * 6 + 0], A[p * 6 + 1], A[p * 6 + 2]);
+            const float3 pl = f3(A[p * 6 + 3], A[p * 6 + 4], A[p * 6 + 5]) + cross3(pa_, r);
+            float3 ang = pa_ + f3(CV[b * 6 + 0], CV[b * 6 + 1], CV[b * 6 + 2]);
+            float3 lin = pl + f3(CV[b * 6 + 3], CV[b * 6 + 4], CV[b * 6 + 5]);
             if (d >= 0) {
-                const float acc = (Du[b * 2 + 1] - dot6(U + b * 6, ap)) / Du[b * 2 + 0];
+                const float* Ub = U + b * 6;
+                const float proj = Ub[0] * pa_.x + Ub[1] * pa_.y + Ub[2] * pa_.z + Ub[3] * pl.x + Ub[4] * pl.y + Ub[5] * pl.z;
+                const float acc = (Du[b * 2 + 1] - proj) / Du[b * 2 + 0];
                 qdd[d] = acc;
-                for (int e = 0; e < 6; ++e) ab[e] += S[d * 6 + e] * acc;
+                const float* sd = S + d * 6;
+                ang = ang + f3(sd[0], sd[1], sd[2]) * acc;
+                lin = lin + f3(sd[3], sd[4], sd[5]) * acc;
             }
-            for (int e = 0; e < 6; ++e) A[b * 6 + e] = ab[e];
+            A[b * 6 + 0] = ang.x; A[b * 6 + 1] = ang.y; A[b * 6 + 2] = ang.z;
+            A[b * 6 + 3] = lin.x; A[b * 6 + 4] = lin.y; A[b * 6 + 5] = lin.z;
         }
         __syncwarp();
     }
@@ -909,7 +958,7 @@ __device__ bool contact_substep(const Warp& w, bool final_substep, int velocity_
     float* Lm = s + L.L;
     const int rs = L.rstride;
     const int ma = M.max_anc;
-    const float3 p0 = ld3(misc + kMiscP0);
+    const float* Jax = s + L.dof_J;
 
     // Speculative margins of articulated colliders (Collision.metal:5882-5915):
     // h * sum|v_free| * max(sweep radius, 0.25), capped by h * speed envelope.
@@ -1040,15 +1089,17 @@ __device__ bool contact_substep(const Warp& w, bool final_substep, int velocity_
         const int b = as_int(c[kCwBody]);
         const int flags = as_int(c[kCwFlags]);
         const float sign = (flags & 256) ? 1.0f : -1.0f;
-        const float3 x = ld3(c + kCwPoint) - p0;
+        const float3 x = ld3(c + kCwPoint);
         const float3 dirs[3] = {ld3(c + kCwNormal), ld3(c + kCwTangent), ld3(c + kCwBitangent)};
         const int na = M.anc_count[b];
         float* g = G + lane * 3 * ma;
         float rel[3] = {0.0f, 0.0f, 0.0f};
         for (int k = 0; k < na; ++k) {
             const int d = M.anc_dofs[b * kMaxDofs + k];
-            const float* sd = S + d * 6;
-            const float3 jc = f3(sd[3], sd[4], sd[5]) + cross3(f3(sd[0], sd[1], sd[2]), x);
+            // Point-Jacobian column: a x (x - o) for rotations, a for translations.
+            const float* jd = Jax + d * 8;
+            const float3 ax = f3(jd[0], jd[1], jd[2]);
+            const float3 jc = jd[6] != 0.0f ? ax : cross3(ax, x - f3(jd[3], jd[4], jd[5]));
             for (int r = 0; r < 3; ++r) {
                 const float gv = sign * dot3(dirs[r], jc);
                 g[r * ma + k] = gv;
@@ -1087,54 +1138,48 @@ __device__ bool contact_substep(const Warp& w, bool final_substep, int velocity_
     for (int d = lane; d < nv; d += 32) vv[d] = vf[d];
     if (total > 0) {
         if (lane == 0) misc[kMiscIslands] = as_float(max(as_int(misc[kMiscIslands]), 1));
-        // Composite rigid-body inertias about p0 (bodies' own inertias are
-        // rebuilt into the ABA inertia area, then accumulated leaf-to-root
-        // with one lane per packed entry).
+        // Composite rigid-body inertias, each about its own body's COM:
+        // rebuilt into the ABA inertia area, then children shifted into
+        // their parent's frame and pulled level by level (deterministic).
         float* IC = s + L.body_IA;
+        const float* Rr = s + L.body_r;
         if (lane < M.nb) {
-            const int b = lane;
-            const float3 cb = ld3(pose + b * 8);
-            const float4 qb = ld4(pose + b * 8 + 4);
-            const float m = M.mass_damping[b].x;
-            const float4 di = M.inertia_diag[b];
-            const float4 of = M.inertia_off[b];
-            const float3 c0 = qrot(qb, f3(1.0f, 0.0f, 0.0f));
-            const float3 c1 = qrot(qb, f3(0.0f, 1.0f, 0.0f));
-            const float3 c2 = qrot(qb, f3(0.0f, 0.0f, 1.0f));
-            const float Ib[3][3] = {{di.x, of.x, of.y}, {of.x, di.y, of.z}, {of.y, of.z, di.z}};
-            const float Rm[3][3] = {{c0.x, c1.x, c2.x}, {c0.y, c1.y, c2.y}, {c0.z, c1.z, c2.z}};
-            const float3 r = cb - p0;
-            const float rr = dot3(r, r);
-            const float rv[3] = {r.x, r.y, r.z};
-            float* I6 = IC + b * 21;
-            for (int i = 0; i < 3; ++i)
-                for (int j = 0; j <= i; ++j) {
-                    float acc = 0.0f;
-                    for (int k = 0; k < 3; ++k)
-                        for (int l2 = 0; l2 < 3; ++l2) acc = fmaf(Rm[i][k] * Ib[k][l2], Rm[j][l2], acc);
-                    I6[sym6(i, j)] = acc + m * ((i == j ? rr : 0.0f) - rv[i] * rv[j]);
+            float Iw[3][3];
+            body_inertia(M, lane, ld4(pose + lane * 8 + 4), IC + lane * 21, Iw);
+        }
+        __syncwarp();
+        for (int l = M.n_levels - 1; l >= -1; --l) {
+            const int off = l >= 0 ? M.level_offsets[l] : 0;
+            const int cnt = l >= 0 ? M.level_offsets[l + 1] - off : 1;
+            if (lane < cnt) {
+                const int b = l >= 0 ? M.level_bodies[off + lane] : 0;
+                float* I6 = IC + b * 21;
+                for (int k = M.child_offsets[b]; k < M.child_offsets[b + 1]; ++k) {
+                    const int c = M.children[k];
+                    float shifted[21];
+                    shift_inertia(IC + c * 21, ld3(Rr + c * 4), shifted);
+                    for (int e = 0; e < 21; ++e) I6[e] += shifted[e];
                 }
-            const float rx[3][3] = {{0.0f, -r.z, r.y}, {r.z, 0.0f, -r.x}, {-r.y, r.x, 0.0f}};
-            for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j) I6[sym6(3 + j, i)] = m * rx[i][j];
-            for (int i = 0; i < 3; ++i)
-                for (int j = 0; j <= i; ++j) I6[sym6(3 + i, 3 + j)] = i == j ? m : 0.0f;
+            }
+            __syncwarp();
         }
-        __syncwarp();
-        if (lane < 21) {
-            for (int b = M.nb - 1; b >= 1; --b) IC[M.parent[b] * 21 + lane] += IC[b * 21 + lane];
-        }
-        __syncwarp();
-        // Mass matrix (packed lower, tree DoF order) M_ij = S_j . (IC_body(i) S_i)
-        // for j ancestor-or-self of i; other entries zero.
+        // Mass matrix (packed lower, tree DoF order): F = IC_body(i) S_i in
+        // body(i)'s frame, moved to each ancestor DoF's body frame,
+        // M_ij = S_j . F.  Entries of unrelated DoFs stay zero.
         for (int i = lane; i < nv; i += 32) {
             float* row = Lm + i * (i + 1) / 2;
             for (int j = 0; j <= i; ++j) row[j] = 0.0f;
             float F[6];
-            sym6_mul(IC + M.dof_body[i] * 21, S + i * 6, F);
+            const int bi = M.dof_body[i];
+            sym6_mul(IC + bi * 21, S + i * 6, F);
+            const float3 ci = ld3(pose + bi * 8);
+            const float3 fl = f3(F[3], F[4], F[5]);
+            const float3 fa = f3(F[0], F[1], F[2]);
             for (int j = i; j >= 0; j = M.dof_parent[j]) {
-                row[j] = dot6(S + j * 6, F);
-                if (M.dof_parent[j] < 0) break;
+                const float3 cj = ld3(pose + M.dof_body[j] * 8);
+                const float3 n = fa + cross3(ci - cj, fl);
+                const float* sj = S + j * 6;
+                row[j] = sj[0] * n.x + sj[1] * n.y + sj[2] * n.z + sj[3] * fl.x + sj[4] * fl.y + sj[5] * fl.z;
             }
             row[i] += M.armature_eff[i];
         }

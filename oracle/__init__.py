@@ -77,9 +77,10 @@ class OracleTrace(ct.Structure):
         ("island_count", ct.c_uint32),
         ("manifold_count", ct.c_uint32),
         ("max_contacts", ct.c_uint32),
-        ("reserved", ct.c_uint32),
+        ("band_decisions", ct.c_uint32),
         ("max_cone_violation", ct.c_double),
         ("max_normal_residual", ct.c_double),
+        ("min_decision_margin", ct.c_double),
         ("contacts", OracleContact * MAX_CONTACTS),
     ]
 

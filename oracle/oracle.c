@@ -23,6 +23,18 @@ static const double kPivotFloor = 1.0e-12;
 static const double kMatrixFloor = 1.0e-10;
 static const double kCfm = 1.0e-2;
 static const double kPad = 0.00000762939453125;
+/* Discrete decisions taken within this distance of their threshold are
+ * "band" decisions: FP32 rounding on the device may legitimately take the
+ * other branch.  Counted per control step (OracleTrace.band_decisions). */
+static const double kBand = 1.0e-5;
+static __thread uint32_t g_band;
+static __thread double g_margin;  /* smallest |value - threshold| over the step's decisions */
+#define BAND(value, threshold)                                                       \
+    do {                                                                             \
+        const double d_ = fabs((double)(value) - (double)(threshold));               \
+        if (d_ < g_margin) g_margin = d_;                                            \
+        if (d_ <= kBand) g_band++;                                                   \
+    } while (0)
 
 struct OracleWorld {
     MRModelWorldC w;
@@ -710,6 +722,7 @@ static int pair_manifold(const OracleWorld* o, const Kin* k, const double* margi
         const double qpad = (scale + 1.0) * kPad;
         const v3 an = V(fabs(plane->normal.x), fabs(plane->normal.y), fabs(plane->normal.z));
         const double msd = vdot(plane->normal, vsub(c, plane->center)) - vdot(an, hx);
+        BAND(msd, plane->offset + qpad);
         if (!(msd <= plane->offset + qpad)) {
             slot->count = 0;
             return 0;
@@ -736,11 +749,13 @@ static int pair_manifold(const OracleWorld* o, const Kin* k, const double* margi
     if (pr->pair_class == MR_COLLISION_PAIR_SPHERE_PLANE) {
         const v3 surface = vsub(fin->center, vmul(plane->normal, fin->radius));
         const double sep = vdot(plane->normal, vsub(surface, plane->center));
+        BAND(sep, accepted);
         if (sep <= accepted) APPEND(surface, sep, feature_key(MR_SHAPE_SPHERE, 0u));
     } else if (pr->pair_class == MR_COLLISION_PAIR_CAPSULE_PLANE) {
         for (uint32_t e = 0; e < 2; ++e) {
             const v3 surface = vsub(e == 0 ? fin->ep0 : fin->ep1, vmul(plane->normal, fin->radius));
             const double sep = vdot(plane->normal, vsub(surface, plane->center));
+            BAND(sep, accepted);
             if (sep <= accepted) APPEND(surface, sep, feature_key(MR_SHAPE_CAPSULE, e));
         }
     } else if (pr->pair_class == MR_COLLISION_PAIR_BOX_PLANE) {
@@ -749,6 +764,7 @@ static int pair_manifold(const OracleWorld* o, const Kin* k, const double* margi
                                (vtx & 4) ? fin->half.z : -fin->half.z);
             const v3 wpt = vadd(fin->center, qrot(fin->rot, local));
             const double sep = vdot(plane->normal, vsub(wpt, plane->center));
+            BAND(sep, accepted);
             if (sep <= accepted) APPEND(wpt, sep, feature_key(MR_SHAPE_BOX, vtx));
         }
     }
@@ -780,6 +796,7 @@ static int pair_manifold(const OracleWorld* o, const Kin* k, const double* margi
         v3 on = qrot(rotA, vld(slot->normal_local));
         on = vmul(on, 1.0 / vlen(on));
         old_ok = vfinite(on) && vdot(on, nw) >= thr[3];
+        BAND(vdot(on, nw), thr[3]);
         if (old_ok) {
             const v3 ot = qrot(rotA, vld(slot->tangent_local));
             transported = vsub(ot, vmul(nw, vdot(ot, nw)));
@@ -791,6 +808,8 @@ static int pair_manifold(const OracleWorld* o, const Kin* k, const double* margi
                 const v3 d = vsub(pb, pa);
                 const double sep = vdot(d, nw);
                 const double drift = vlen(vsub(d, vmul(nw, sep)));
+                BAND(sep, thr[0]);
+                BAND(drift, thr[1]);
                 if (sep > thr[0] || drift > thr[1]) continue;
                 Cand* cc = &c[nc++];
                 for (int a = 0; a < 3; ++a) { cc->la[a] = op->anchor_a[a]; cc->lb[a] = op->anchor_b[a]; cc->imp[a] = op->impulses[a]; }
@@ -814,6 +833,7 @@ static int pair_manifold(const OracleWorld* o, const Kin* k, const double* margi
         if (match < 0)
             for (int m = 0; m < nc; ++m) {
                 const v3 da = vsub(vld(c[m].la), la), db = vsub(vld(c[m].lb), lb);
+                BAND(sqrt(vdot(da, da) + vdot(db, db)), sqrt(2.0 * merge2));
                 if (vdot(da, da) + vdot(db, db) <= 2.0 * merge2) { match = m; break; }
             }
         if (match < 0) {
@@ -837,6 +857,7 @@ static int pair_manifold(const OracleWorld* o, const Kin* k, const double* margi
         c[d] = val;
     }
     if (nc > MPTS) {
+        if (nc > 1 && fabs(c[1].sep - c[0].sep) <= kBand) g_band++;
         int selected[12] = {0}, chosen[MPTS], count = 1;
         chosen[0] = 0;
         selected[0] = 1;
@@ -864,6 +885,7 @@ static int pair_manifold(const OracleWorld* o, const Kin* k, const double* margi
                     }
                 }
                 const unsigned long long f = ckey(&c[i]);
+                if (best >= 0 && fabs(score - best_score) > 1.0e-12 && fabs(score - best_score) <= kBand * kBand) g_band++;
                 if (score > best_score + 1.0e-12 || (fabs(score - best_score) <= 1.0e-12 && f < best_f)) {
                     best = i; best_score = score; best_f = f;
                 }
@@ -1216,6 +1238,8 @@ uint32_t oracle_control_step(const OracleWorld* o, double* q, double* v, OracleM
     OracleTrace local;
     if (!trace) trace = &local;
     memset(trace, 0, sizeof(*trace));
+    g_band = 0;
+    g_margin = INFINITY;
     trace->failing_substep = MR_INVALID_INDEX;
     trace->failing_index = MR_INVALID_INDEX;
     if (reset) {
@@ -1255,6 +1279,8 @@ uint32_t oracle_control_step(const OracleWorld* o, double* q, double* v, OracleM
         }
     }
     trace->status = status;
+    trace->band_decisions = g_band;
+    trace->min_decision_margin = g_margin;
     if (status != MR_STEP_SUCCESS) {
         memcpy(q, qc, sizeof(double) * nq);
         memcpy(v, vc, sizeof(double) * nv);

@@ -315,6 +315,44 @@ static void drive_efforts(const RefModel* r, const double* q, const double* v, c
     }
 }
 
+// World-step configuration: one timestep shared by dynamics, constraint
+// evaluation and joint limits (ArticulatedWorld.cpp:480-520 rejects a
+// mismatch), the evaluation slop / depenetration speed of the world.
+static ArticulatedWorldConfig world_config(const RefModel* r, int solver) {
+    ArticulatedWorldConfig cfg{};
+    cfg.dynamics = dyn_config(r);
+    cfg.constraintEvaluation.timestep = r->h;
+    cfg.jointLimits.timestep = r->h;
+    cfg.constraintEvaluation.penetrationSlop = r->world.solver_scales[3];
+    cfg.constraintEvaluation.maximumDepenetrationVelocity = r->world.solver_scales[2];
+    cfg.solverType = solver == 0 ? MR_SOLVER_REFERENCE_FP64 : MR_SOLVER_QUALITY_NEWTON;
+    return cfg;
+}
+
+// One transactional world step with diagnostics: returns the step status
+// code and writes the failing stage (ArticulatedWorldFailure) and contact
+// count.
+__attribute__((visibility("default"))) int ref_world_step_once(RefModel* r, double* q, double* v, const float* actions, int solver,
+                                                               uint32_t* failure, uint32_t* contacts) {
+    const std::uint32_t nq = r->world.nq, nv = r->world.nv;
+    const ArticulatedWorldConfig cfg = world_config(r, solver);
+    std::vector<double> tau(nv);
+    std::vector<ArticulatedDofCommand> commands(nv);
+    drive_efforts(r, q, v, actions, tau.data());
+    for (std::uint32_t k = 0; k < nv; ++k) {
+        if (r->dofs[k].flags & MR_DOF_FLAG_ACTUATED) {
+            commands[k].mode = ArticulatedActuationMode::effort;
+            commands[k].feedForward = tau[k];
+        }
+    }
+    static thread_local ArticulatedWorldCache cache{};
+    auto d = stepControlledArticulatedWorldCpu(r->model, 0, std::span<double>(q, nq), std::span<double>(v, nv), commands, {},
+                                               r->env_bodies, r->env_shapes, cfg, cache);
+    if (failure) *failure = static_cast<uint32_t>(d.failure);
+    if (contacts) *contacts = d.contactCount;
+    return static_cast<int>(d.code);
+}
+
 // Runs `steps` control steps x `substeps` physics steps for `envs`
 // environments with `threads` std::threads (static env partition) and
 // returns elapsed wall seconds.  Contact worlds use the reference's
@@ -328,12 +366,7 @@ __attribute__((visibility("default"))) double ref_run(RefModel* r, uint32_t envs
     const bool contact = !r->env_shapes.empty();
     std::atomic<std::uint64_t> failed{0};
     auto worker = [&](std::uint32_t begin, std::uint32_t end) {
-        ArticulatedWorldConfig cfg{};
-        cfg.dynamics = dyn_config(r);
-        cfg.constraintEvaluation.timestep = r->h;
-        cfg.constraintEvaluation.penetrationSlop = r->world.solver_scales[3];
-        cfg.constraintEvaluation.maximumDepenetrationVelocity = r->world.solver_scales[2];
-        cfg.solverType = solver == 0 ? MR_SOLVER_REFERENCE_FP64 : MR_SOLVER_QUALITY_NEWTON;
+        const ArticulatedWorldConfig cfg = world_config(r, solver);
         std::vector<double> tau(nv);
         std::vector<ArticulatedDofCommand> commands(nv);
         for (std::uint32_t e = begin; e < end; ++e) {
