@@ -20,7 +20,30 @@ constexpr int kMaxMaterials = 8;
 // Words of one persistent manifold slot in device memory (MRManifoldC).
 constexpr int kManifoldWords = 8 + kManifoldPoints * 12;
 
+// Byte-sized topology tables copied into each CTA's shared memory at kernel
+// start: every cross-lane index lookup of the sweeps reads shared memory,
+// never global memory.  255 marks "none".
+struct alignas(16) DeviceTables {
+    std::uint8_t nb, nv, nq, n_levels;
+    std::uint8_t floating, ns, np, max_anc;
+    std::uint8_t n_dof_levels, reserved[7];
+    std::uint8_t depth[kMaxBodies];          // tree depth of each body (root 0)
+    std::uint8_t parent[kMaxBodies];
+    std::uint8_t body_dof[kMaxBodies];
+    std::uint8_t child_offsets[kMaxBodies + 1];
+    std::uint8_t children[kMaxBodies];
+    std::uint8_t anc_count[kMaxBodies];
+    std::uint8_t dof_body[kMaxDofs];
+    std::uint8_t dof_parent[kMaxDofs];
+    std::uint8_t dof_depth[kMaxDofs];        // number of ancestor DoFs
+    std::uint8_t anc[kMaxBodies][kMaxDofs];  // ancestor DoFs of a body, root first
+    std::uint8_t pos[kMaxBodies][kMaxDofs];  // position of DoF d in anc[b], or 255
+    std::uint8_t lcp[kMaxBodies][kMaxBodies];// common prefix length of anc[a], anc[b]
+    std::uint8_t pad[7];
+};
+
 struct alignas(16) DeviceModel {
+    DeviceTables tables;
     // World.
     std::int32_t nb;              // articulated bodies, DFS preorder, body 0 = root
     std::int32_t nv;

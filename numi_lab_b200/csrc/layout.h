@@ -8,7 +8,7 @@
 namespace numi {
 
 // Words of one solver contact record in shared memory.
-constexpr int kContactWords = 40;
+constexpr int kContactWords = 44;
 enum ContactWord : int {
     kCwPoint = 0,      // world contact point (3)
     kCwSeparation = 3,
@@ -25,39 +25,47 @@ enum ContactWord : int {
     kCwDelta = 34,     // last impulse change (3)
     kCwBody = 37,      // articulated body (int bits)
     kCwFlags = 38,     // bit0 new impact, bit8 articulated side is B (int bits)
-    kCwSlot = 39       // pair * 4 + manifold point (int bits)
+    kCwSlot = 39,      // pair * 4 + manifold point (int bits)
+    kCwUfree = 40      // contact-frame relative velocity at v_free (3)
 };
 
 struct WarpLayout {
-    int body_pose, body_V, body_CV, body_IA, body_PA, body_U, body_Du, body_A, body_r;
+    int body_pose, body_V, body_IA, body_PA, body_A;
     int dof_S, dof_J;
-    int q, qc, qn, v, vc, vf, tau, qdd, tgt;
+    int q, qc, v, vc, vf, tau, qdd, tgt;
     int misc;
-    int manifolds, contacts, G, R, L;
-    int rstride;
-    int total;  // floats per warp
+    int manifolds, contacts, G, L, z, margins;
+    int narrow;  // narrowphase scratch; aliases the contact records and rows
+    int total;   // floats per warp
 };
 
 __host__ __device__ inline int align4(int x) { return (x + 3) & ~3; }
 
-__host__ __device__ inline WarpLayout make_layout(int nb, int nv, int nq, int np, int ncap, int max_anc, bool contact) {
+// Narrowphase scratch of one pair: four kept old points and up to
+// `max_raw` raw contacts, 16 words each, plus 16 candidate-id bytes.
+constexpr int kCandidateWords = 16;
+__host__ __device__ inline int pair_scratch_words(int max_raw) { return (4 + max_raw) * kCandidateWords + 4; }
+
+// Most raw contacts one pair class can produce before manifold reduction.
+__host__ __device__ inline int pair_max_raw(int pair_class) {
+    return pair_class == MR_COLLISION_PAIR_BOX_PLANE ? 8 : (pair_class == MR_COLLISION_PAIR_CAPSULE_PLANE ? 2 : 1);
+}
+
+// `narrow_words` is the sum of pair_scratch_words over the compiled pairs.
+__host__ __device__ inline WarpLayout make_layout(int nb, int nv, int nq, int np, int ncap, int max_anc, int narrow_words,
+                                                  bool contact) {
     WarpLayout L{};
     int o = 0;
     auto take = [&o](int words) { const int at = o; o += align4(words); return at; };
     L.body_pose = take(nb * 8);
     L.body_V = take(nb * 6);
-    L.body_CV = take(nb * 6);
     L.body_IA = take(nb * 21);
     L.body_PA = take(nb * 6);
-    L.body_U = take(nb * 6);
-    L.body_Du = take(nb * 2);
     L.body_A = take(nb * 6);
-    L.body_r = take(nb * 4);
     L.dof_S = take(nv * 6);
     L.dof_J = take(nv * 8);
     L.q = take(nq);
     L.qc = take(nq);
-    L.qn = take(nq);
     L.v = take(nv);
     L.vc = take(nv);
     L.vf = take(nv);
@@ -65,15 +73,20 @@ __host__ __device__ inline WarpLayout make_layout(int nb, int nv, int nq, int np
     L.qdd = take(nv);
     L.tgt = take(nv);
     L.misc = take(32);
-    L.rstride = nv | 1;  // odd column stride: lane-per-column access is bank-conflict free
+    L.z = take(nv);
+    L.margins = take(32);
     if (contact) {
         L.manifolds = take(np * kManifoldWords);
-        L.contacts = take(ncap * kContactWords);
-        L.G = take(ncap * 3 * max_anc);
-        L.R = take(3 * ncap * L.rstride > 32 ? 3 * ncap * L.rstride : 32);  // also stages collider margins
         L.L = take(nv * (nv + 1) / 2);
+        // Contact records and Jacobian rows are written only after the
+        // narrowphase has finished with its scratch, so the three share words.
+        L.contacts = take(ncap * kContactWords);
+        const int rows = align4(ncap * 3 * max_anc);
+        const int need = align4(narrow_words) - align4(ncap * kContactWords);
+        L.G = take(rows > need ? rows : need);
+        L.narrow = L.contacts;
     } else {
-        L.manifolds = L.contacts = L.G = L.R = L.L = o;
+        L.manifolds = L.contacts = L.G = L.L = L.narrow = o;
     }
     L.total = align4(o);
     return L;

@@ -26,9 +26,11 @@
 #include <vector>
 
 namespace numi {
+cudaError_t control_step_occupancy(bool contact, int warps_per_block, size_t smem, int* blocks_per_sm);
 cudaError_t launch_control_step(const StepParams& p, const WarpLayout& layout, bool contact, int warps_per_block,
                                 cudaStream_t stream);
 cudaError_t configure_control_step_kernels(size_t max_dynamic_smem);
+size_t control_step_table_bytes();
 }  // namespace numi
 
 namespace {
@@ -222,6 +224,53 @@ numi::DeviceModel pack_model(const numi::CompiledModel& m, float h) {
         d.pair_class[p] = static_cast<int>(pr.pair_class);
         d.pair_max_points[p] = static_cast<int>(pr.max_points);
     }
+    // Byte tables for the kernels' shared-memory copy.
+    {
+        DeviceTables& t = d.tables;
+        std::memset(&t, 0xff, sizeof(t));
+        t.nb = static_cast<std::uint8_t>(nb);
+        t.nv = static_cast<std::uint8_t>(w.nv);
+        t.nq = static_cast<std::uint8_t>(w.nq);
+        t.n_levels = static_cast<std::uint8_t>(m.level_count);
+        t.floating = static_cast<std::uint8_t>(d.floating);
+        t.ns = static_cast<std::uint8_t>(w.shape_count);
+        t.np = static_cast<std::uint8_t>(w.pair_count);
+        t.max_anc = static_cast<std::uint8_t>(m.max_ancestor_dofs);
+        std::vector<int> depth(nb, 0);
+        for (int b = 1; b < nb; ++b) depth[b] = depth[m.bodies[b].parent_body] + 1;
+        for (int b = 0; b < nb; ++b) {
+            t.depth[b] = static_cast<std::uint8_t>(depth[b]);
+            t.parent[b] = b == 0 ? 255 : static_cast<std::uint8_t>(m.bodies[b].parent_body);
+            t.body_dof[b] = m.body_dof[b] == MR_INVALID_INDEX ? 255 : static_cast<std::uint8_t>(m.body_dof[b]);
+            t.child_offsets[b] = static_cast<std::uint8_t>(d.child_offsets[b]);
+            t.children[b] = static_cast<std::uint8_t>(d.children[b]);
+            t.anc_count[b] = static_cast<std::uint8_t>(m.body_ancestor_count[b]);
+            for (std::uint32_t k = 0; k < m.body_ancestor_count[b]; ++k)
+                t.anc[b][k] = static_cast<std::uint8_t>(m.body_ancestor_dofs[b * m.max_ancestor_dofs + k]);
+            for (std::uint32_t dof = 0; dof < w.nv; ++dof) {
+                t.pos[b][dof] = 255;
+                for (std::uint32_t k = 0; k < m.body_ancestor_count[b]; ++k)
+                    if (m.body_ancestor_dofs[b * m.max_ancestor_dofs + k] == dof) t.pos[b][dof] = static_cast<std::uint8_t>(k);
+            }
+        }
+        t.child_offsets[nb] = static_cast<std::uint8_t>(d.child_offsets[nb]);
+        for (int a = 0; a < nb; ++a)
+            for (int b = 0; b < nb; ++b) {
+                std::uint32_t n = 0;
+                while (n < m.body_ancestor_count[a] && n < m.body_ancestor_count[b] &&
+                       m.body_ancestor_dofs[a * m.max_ancestor_dofs + n] == m.body_ancestor_dofs[b * m.max_ancestor_dofs + n])
+                    ++n;
+                t.lcp[a][b] = static_cast<std::uint8_t>(n);
+            }
+        int levels = 0;
+        for (std::uint32_t k = 0; k < w.nv; ++k) {
+            t.dof_body[k] = static_cast<std::uint8_t>(m.dof_body[k]);
+            t.dof_parent[k] = m.dof_parent[k] == MR_INVALID_INDEX ? 255 : static_cast<std::uint8_t>(m.dof_parent[k]);
+            t.dof_depth[k] = static_cast<std::uint8_t>(d.dof_anc_count[k]);
+            levels = std::max(levels, d.dof_anc_count[k] + 1);
+        }
+        t.n_dof_levels = static_cast<std::uint8_t>(levels);
+    }
     if (w.material_count > kMaxMaterials) throw std::runtime_error("too many materials");
     for (std::uint32_t i = 0; i < w.material_count; ++i) {
         const MRModelMaterialC& mt = m.materials[i];
@@ -239,6 +288,7 @@ struct MRTaskRolloutHandle {
     numi::WarpLayout layout{};
     bool contact = false;
     int warps_per_block = 1;
+    int resident_warps_per_sm = 0;
     MRTaskRolloutConfigC config{};
     std::uint32_t envs = 0;
     float h = 0.0f;
@@ -478,19 +528,37 @@ MR_API MRTaskRolloutHandle* mr_create_task_rollout(const MRRunManifestC* manifes
         h.contact = h.model.world.pair_count > 0;
         h.dmodel = pack_model(h.model, h.h);
         const numi::CompiledModel& m = h.model;
+        int narrow_words = 0;
+        for (const MRModelPairC& pr : m.pairs) narrow_words += numi::pair_scratch_words(numi::pair_max_raw(static_cast<int>(pr.pair_class)));
         h.layout = numi::make_layout(static_cast<int>(m.articulated_body_count), static_cast<int>(m.world.nv),
                                      static_cast<int>(m.world.nq), static_cast<int>(m.world.pair_count),
-                                     static_cast<int>(m.world.contact_capacity), static_cast<int>(m.max_ancestor_dofs), h.contact);
+                                     static_cast<int>(m.world.contact_capacity), static_cast<int>(m.max_ancestor_dofs),
+                                     narrow_words, h.contact);
         check(cudaGetDevice(&h.device), "cudaGetDevice");
         cudaDeviceProp prop{};
         check(cudaGetDeviceProperties(&prop, h.device), "cudaGetDeviceProperties");
         h.device_name = prop.name;
         const size_t per_warp = static_cast<size_t>(h.layout.total) * sizeof(float);
+        const size_t tables = numi::control_step_table_bytes();
         const size_t limit = prop.sharedMemPerBlockOptin;
-        if (per_warp > limit) throw std::runtime_error("per-environment shared memory exceeds the device limit");
-        h.warps_per_block = static_cast<int>(std::min<size_t>(4, std::max<size_t>(1, limit / per_warp)));
-        if (h.contact) h.warps_per_block = 1;
+        if (tables + per_warp > limit) throw std::runtime_error("per-environment shared memory exceeds the device limit");
         check(numi::configure_control_step_kernels(limit), "kernel attributes");
+        // Environments per CTA: the choice that keeps the most warps resident
+        // per SM under the kernel's register and shared-memory footprint
+        // (each CTA carries one copy of the topology tables).
+        {
+            int best = 1, best_warps = 0;
+            for (int wpb = 1; wpb <= 4; wpb *= 2) {
+                const size_t smem = tables + wpb * per_warp;
+                if (smem > limit) break;
+                int blocks = 0;
+                check(numi::control_step_occupancy(h.contact, wpb, smem, &blocks), "occupancy query");
+                if (blocks * wpb > best_warps) { best_warps = blocks * wpb; best = wpb; }
+            }
+            if (best_warps == 0) throw std::runtime_error("the control-step kernel cannot be resident with this model");
+            h.warps_per_block = best;
+            h.resident_warps_per_sm = best_warps;
+        }
         check(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking), "stream");
         check(cudaEventCreate(&h.ev_start), "event");
         check(cudaEventCreate(&h.ev_stop), "event");

@@ -1,23 +1,30 @@
 // Batched articulated-physics control step for B200 (sm_100a).
 //
 // One warp owns one environment for a whole control step (all physics
-// substeps).  The environment's state, manifolds, articulated inertias,
-// contact Jacobians and response columns stay in shared memory; HBM sees the
-// step's inputs (resident q, v, manifolds, actions, reset mask) once and its
-// outputs (committed state, observation, status) once.
+// substeps).  Lane b owns body b of the tree (<= 32 bodies): its constants,
+// articulated inertia, bias, joint subspace and factor live in registers
+// through the tree sweeps, and only values a child or parent needs cross
+// lanes, through shared memory.  Byte-sized topology tables sit in the CTA's
+// shared memory.  HBM sees each control step's inputs (resident q, v,
+// manifolds, actions, reset mask) once and its outputs (committed state,
+// observation, status) once.
 //
 // Stage order per substep follows numi-lab's MetalWorld graph
 // (src/metal/MetalWorld.mm:17075-17370 and encodeContactSubstep
 // :12682-13260): drive refresh -> ABA -> [kinematics, collider projection,
 // pair flags, narrowphase, persistent manifolds, ConstraintIR evaluation,
-// response columns, temporalCone solve, joint limits, integration] ->
-// latch.  The control step is one transaction: the first failing substep
-// latches a status and the environment keeps its step-start checkpoint.
+// contact responses, temporalCone solve, joint limits, integration] -> latch.
+// The control step is one transaction: the first failing substep latches a
+// status and the environment keeps its step-start checkpoint.
 //
-// Spatial algebra uses (angular, linear) vectors about one reference point
-// per environment (the floating root's COM at substep start, or the world
-// origin for a fixed root), so no per-body shift transforms are needed in
-// the tree sweeps.
+// Contact responses use the tree-sparse factor H = L^T L of the joint-space
+// inertia (Featherstone, Rigid Body Dynamics Algorithms, sec. 6.5):
+// Y = L^-T G^T is nonzero only on a contact body's ancestor DoFs, the
+// temporalCone sweeps run on z = Y lambda (contact velocities
+// u = u_free + Y^T z), and one substitution L x = z returns the velocity
+// change x = H^-1 G^T lambda.  It is the reference's Jacobi block iteration
+// in generalized velocities (MetalWorldContact.metal:6655-7000), evaluated
+// without dense response columns.
 #include "device_model.h"
 #include "dmath.cuh"
 #include "layout.h"
@@ -31,18 +38,23 @@ namespace {
 constexpr float kFloatEps = 1.1920928955078125e-7f;
 constexpr float kAbsolutePivotFloor = 1.0e-12f;
 constexpr float kMatrixFloor = 1.0e-10f;
-constexpr float kContactCfm = 1.0e-2f;          // MetalWorldContact.metal:18
+constexpr float kContactCfm = 1.0e-2f;             // MetalWorldContact.metal:18
 constexpr float kQueryPad = 0.00000762939453125f;  // MR_COLLISION_QUERY_RELATIVE_PAD
 constexpr float kAabbPad = 0.00000762939453125f;   // MR_COLLISION_AABB_RELATIVE_PAD
+constexpr unsigned char kNone = 255;
+constexpr int kMaxRawPerPair = 8;
+constexpr float kTieRelative = 1.0e-5f;  // manifold reduction ties
+constexpr float kTieAbsolute = 1.0e-12f;
 
 __device__ __forceinline__ int as_int(float f) { return __float_as_int(f); }
 __device__ __forceinline__ float as_float(int i) { return __int_as_float(i); }
 
 struct Warp {
     int lane;
-    float* s;          // this warp's shared-memory base
+    float* s;  // this warp's shared-memory base
     const WarpLayout* L;
     const DeviceModel* M;
+    const DeviceTables* T;  // shared-memory copy
 };
 
 __device__ __forceinline__ void set_status(float* misc, unsigned code, unsigned index) {
@@ -52,6 +64,51 @@ __device__ __forceinline__ void set_status(float* misc, unsigned code, unsigned 
         misc[kMiscFailIndex] = as_float(static_cast<int>(index));
     }
 }
+
+__device__ __forceinline__ bool warp_ok(const float* misc) {
+    __syncwarp();
+    return as_int(misc[kMiscStatus]) == MR_STEP_SUCCESS;
+}
+
+// Per-lane body constants, loaded once per control step.
+struct BodyConst {
+    int parent, dof, type, qidx;
+    float3 axis, panchor, canchor;
+    float4 prot, crotc;
+    float mass, lin_damp, ang_damp;
+    float4 idiag, ioff;
+};
+
+__device__ void load_body(const DeviceModel& M, int b, BodyConst& c) {
+    c.parent = M.parent[b];
+    c.dof = M.body_dof[b];
+    c.type = M.joint_type[b];
+    c.qidx = c.dof >= 0 ? M.dof_q[c.dof] : -1;
+    c.axis = xyz(M.axis[b]);
+    c.panchor = xyz(M.parent_anchor[b]);
+    c.canchor = xyz(M.child_anchor[b]);
+    c.prot = M.parent_rotation[b];
+    c.crotc = M.child_rotation_conj[b];
+    const float4 md = M.mass_damping[b];
+    c.mass = md.x;
+    c.lin_damp = md.y;
+    c.ang_damp = md.z;
+    c.idiag = M.inertia_diag[b];
+    c.ioff = M.inertia_off[b];
+}
+
+// Per-lane dynamic body state of one substep.
+struct BodyState {
+    float3 c;       // COM position
+    float4 qr;      // orientation
+    float3 w, v;    // angular velocity, COM linear velocity
+    float3 ba, bl;  // velocity-product bias accelerations
+    float3 r;       // parent COM -> body COM
+    float s[6];     // joint motion subspace about this body's COM
+    float I[21];    // articulated (then composite) inertia, packed symmetric
+    float p[6];     // articulated bias force
+    float U[6], D, u;
+};
 
 // ---------------------------------------------------------------------------
 // Drives: implicit PD refresh or effort pass-through with the actuator
@@ -93,9 +150,11 @@ __device__ void compute_drives(const Warp& w) {
 // motionTransformElement :160-190, written out in 3x3 blocks):
 // I = [[A, B], [B^T, D]], E = [r]x:  A' = A - B E + E B^T - E D E,
 // B' = B + E D, D' = D.
-__device__ void shift_inertia(const float* I, float3 r, float* out) {
+__device__ __forceinline__ void shift_inertia(const float* I, float3 r, float* out) {
     float A[3][3], B[3][3], D[3][3];
+#pragma unroll
     for (int i = 0; i < 3; ++i)
+#pragma unroll
         for (int j = 0; j < 3; ++j) {
             A[i][j] = I[sym6(i, j)];
             B[i][j] = I[sym6(3 + j, i)];
@@ -103,9 +162,12 @@ __device__ void shift_inertia(const float* I, float3 r, float* out) {
         }
     const float E[3][3] = {{0.0f, -r.z, r.y}, {r.z, 0.0f, -r.x}, {-r.y, r.x, 0.0f}};
     float ED[3][3], BE[3][3];
+#pragma unroll
     for (int i = 0; i < 3; ++i)
+#pragma unroll
         for (int j = 0; j < 3; ++j) {
             float ed = 0.0f, be = 0.0f;
+#pragma unroll
             for (int k = 0; k < 3; ++k) {
                 ed = fmaf(E[i][k], D[k][j], ed);
                 be = fmaf(B[i][k], E[k][j], be);
@@ -113,54 +175,195 @@ __device__ void shift_inertia(const float* I, float3 r, float* out) {
             ED[i][j] = ed;
             BE[i][j] = be;
         }
+#pragma unroll
     for (int i = 0; i < 3; ++i)
+#pragma unroll
         for (int j = 0; j <= i; ++j) {
-            float ede = 0.0f;
-            for (int k = 0; k < 3; ++k) ede = fmaf(ED[i][k], E[k][j], ede);
-            // E B^T (i, j) = sum_k E[i][k] B[j][k] = -(B E)^T... written directly:
-            float ebt = 0.0f;
-            for (int k = 0; k < 3; ++k) ebt = fmaf(E[i][k], B[j][k], ebt);
+            float ede = 0.0f, ebt = 0.0f;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                ede = fmaf(ED[i][k], E[k][j], ede);
+                ebt = fmaf(E[i][k], B[j][k], ebt);
+            }
             out[sym6(i, j)] = A[i][j] - BE[i][j] + ebt - ede;
         }
+#pragma unroll
     for (int i = 0; i < 3; ++i)
+#pragma unroll
         for (int j = 0; j < 3; ++j) out[sym6(3 + j, i)] = B[i][j] + ED[i][j];
+#pragma unroll
     for (int i = 0; i < 3; ++i)
+#pragma unroll
         for (int j = 0; j <= i; ++j) out[sym6(3 + i, 3 + j)] = D[i][j];
 }
 
-// Body spatial inertia about its own COM in world axes: [[R Ib R^T, 0], [0, m 1]].
-__device__ void body_inertia(const DeviceModel& M, int b, float4 qb, float* I6, float Iw[3][3]) {
-    const float m = M.mass_damping[b].x;
-    const float4 di = M.inertia_diag[b];
-    const float4 of = M.inertia_off[b];
+// Rigid spatial inertia about the COM in world axes: [[R Ib R^T, 0], [0, m 1]].
+__device__ __forceinline__ void body_inertia(const BodyConst& bc, float4 qb, float* I6, float Iw[3][3]) {
     const float3 c0 = qrot(qb, f3(1.0f, 0.0f, 0.0f));
     const float3 c1 = qrot(qb, f3(0.0f, 1.0f, 0.0f));
     const float3 c2 = qrot(qb, f3(0.0f, 0.0f, 1.0f));
-    const float Ib[3][3] = {{di.x, of.x, of.y}, {of.x, di.y, of.z}, {of.y, of.z, di.z}};
+    const float Ib[3][3] = {{bc.idiag.x, bc.ioff.x, bc.ioff.y}, {bc.ioff.x, bc.idiag.y, bc.ioff.z}, {bc.ioff.y, bc.ioff.z, bc.idiag.z}};
     const float R[3][3] = {{c0.x, c1.x, c2.x}, {c0.y, c1.y, c2.y}, {c0.z, c1.z, c2.z}};
+#pragma unroll
     for (int i = 0; i < 3; ++i)
+#pragma unroll
         for (int j = 0; j < 3; ++j) {
             float acc = 0.0f;
+#pragma unroll
             for (int k = 0; k < 3; ++k)
+#pragma unroll
                 for (int l2 = 0; l2 < 3; ++l2) acc = fmaf(R[i][k] * Ib[k][l2], R[j][l2], acc);
             Iw[i][j] = acc;
         }
+#pragma unroll
     for (int e = 0; e < 21; ++e) I6[e] = 0.0f;
+#pragma unroll
     for (int i = 0; i < 3; ++i) {
+#pragma unroll
         for (int j = 0; j <= i; ++j) I6[sym6(i, j)] = Iw[i][j];
-        I6[sym6(3 + i, 3 + i)] = m;
+        I6[sym6(3 + i, 3 + i)] = bc.mass;
     }
 }
 
 // ---------------------------------------------------------------------------
-// Articulated-body algorithm (ArticulatedABA.metal:352-1578): per-body COM
-// frames in world axes, classical accelerations, 21-entry inertias; tree
-// levels run lane-parallel.  Each body shifts its articulated inertia and
-// bias into its parent's frame; parents pull their children's shifted
-// contributions in a fixed order, so sums are deterministic without atomics.
+// Forward kinematics (ArticulatedABA.metal:735-905): lane b computes body b
+// at its tree level from the parent's pose / twist in shared memory.
+// Writes pose and twist to shared memory, joint axis / origin and subspace of
+// the body's DoF to the per-DoF tables; keeps bias and offset in registers.
 // ---------------------------------------------------------------------------
-__device__ bool aba(const Warp& w) {
+__device__ void kinematics(const Warp& w, const BodyConst& bc, BodyState& st) {
+    const DeviceTables& T = *w.T;
+    const WarpLayout& L = *w.L;
+    float* s = w.s;
+    float* misc = s + L.misc;
+    const float* q = s + L.q;
+    const float* v = s + L.v;
+    float* pose = s + L.body_pose;
+    float* vel = s + L.body_V;
+    float* S = s + L.dof_S;
+    float* J = s + L.dof_J;
+    const int b = w.lane;
+    const bool mine = b < T.nb;
+    const int my_depth = mine ? T.depth[b] : -1;
+
+    if (b == 0) {
+        if (T.floating) {
+            float4 rq;
+            const float3 c0 = f3(q[0], q[1], q[2]);
+            if (!finite3(c0) || !qnormalize(make_float4(q[3], q[4], q[5], q[6]), rq, true)) {
+                set_status(misc, MR_STEP_NONFINITE_INPUT, 0u);
+                rq = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+            }
+            st.c = c0;
+            st.qr = rq;
+            st.w = f3(v[3], v[4], v[5]);
+            st.v = f3(v[0], v[1], v[2]);
+        } else {
+            st.c = f3(0.0f, 0.0f, 0.0f);
+            st.qr = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+            st.w = st.v = f3(0.0f, 0.0f, 0.0f);
+        }
+        st.ba = st.bl = st.r = f3(0.0f, 0.0f, 0.0f);
+        for (int i = 0; i < 6; ++i) st.s[i] = 0.0f;
+        st4(pose, make_float4(st.c.x, st.c.y, st.c.z, 0.0f));
+        st4(pose + 4, st.qr);
+        st3(vel, st.w);
+        st3(vel + 3, st.v);
+    }
+    __syncwarp();
+    if (T.floating && b < 6) {
+        // Root DoFs: lin k -> (0, e_k), ang k -> (e_k, 0) about the root COM;
+        // Jacobian: translational axes e_k, rotations about the root COM.
+        float* Sd = S + b * 6;
+        float* Jd = J + b * 8;
+        for (int i = 0; i < 6; ++i) Sd[i] = 0.0f;
+        if (b < 3) Sd[3 + b] = 1.0f;
+        else Sd[b - 3] = 1.0f;
+        const int k = b < 3 ? b : b - 3;
+        Jd[0] = k == 0 ? 1.0f : 0.0f;
+        Jd[1] = k == 1 ? 1.0f : 0.0f;
+        Jd[2] = k == 2 ? 1.0f : 0.0f;
+        Jd[3] = pose[0]; Jd[4] = pose[1]; Jd[5] = pose[2];
+        Jd[6] = b < 3 ? 1.0f : 0.0f;
+        Jd[7] = 0.0f;
+    }
+    for (int l = 1; l <= T.n_levels; ++l) {
+        if (my_depth == l) {
+            const int p = bc.parent;
+            const float3 cp = ld3(pose + p * 8);
+            const float4 qp = ld4(pose + p * 8 + 4);
+            const float3 wp = ld3(vel + p * 6);
+            const float3 vp = ld3(vel + p * 6 + 3);
+            const float4 pj = qmul(qp, bc.prot);
+            float4 motion = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+            float qj = 0.0f, qdj = 0.0f;
+            const bool has = bc.dof >= 0;
+            const bool prismatic = bc.type == MR_JOINT_PRISMATIC;
+            if (has) {
+                qj = q[bc.qidx];
+                qdj = v[bc.dof];
+                if (!prismatic) {
+                    float sh, ch;
+                    sincosf(0.5f * qj, &sh, &ch);
+                    motion = make_float4(bc.axis.x * sh, bc.axis.y * sh, bc.axis.z * sh, ch);
+                }
+            }
+            float4 qb;
+            if (!qnormalize(qmul(qmul(pj, motion), bc.crotc), qb, false)) {
+                set_status(misc, MR_STEP_NONFINITE_RESULT, static_cast<unsigned>(b));
+                qb = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+            }
+            const float3 ja = qrot(pj, bc.axis);
+            float3 jp = cp + qrot(qp, bc.panchor);
+            if (prismatic) jp = jp + ja * qj;
+            const float3 ca = qrot(qb, bc.canchor);
+            const float3 cb = jp - ca;
+            const float3 ptj = jp - cp;
+            const float3 zero = f3(0.0f, 0.0f, 0.0f);
+            const float3 wb = wp + ((has && !prismatic) ? ja * qdj : zero);
+            const float3 vb = vp + cross3(wp, ptj) + (prismatic ? ja * qdj : zero) - cross3(wb, ca);
+            const float3 ma = (has && !prismatic) ? ja : zero;
+            const float3 ml = prismatic ? ja : (has ? -cross3(ja, ca) : zero);
+            st.ba = (has && !prismatic) ? cross3(wp, ja) * qdj : zero;
+            const float3 pc = prismatic ? cross3(wp, ja) * (2.0f * qdj) : zero;
+            st.bl = cross3(wp, cross3(wp, ptj)) + pc - cross3(st.ba, ca) - cross3(wb, cross3(wb, ca));
+            st.c = cb;
+            st.qr = qb;
+            st.w = wb;
+            st.v = vb;
+            st.r = cb - cp;
+            st.s[0] = ma.x; st.s[1] = ma.y; st.s[2] = ma.z;
+            st.s[3] = ml.x; st.s[4] = ml.y; st.s[5] = ml.z;
+            st4(pose + b * 8, make_float4(cb.x, cb.y, cb.z, 0.0f));
+            st4(pose + b * 8 + 4, qb);
+            st3(vel + b * 6, wb);
+            st3(vel + b * 6 + 3, vb);
+            if (has) {
+                float* Sd = S + bc.dof * 6;
+                for (int i = 0; i < 6; ++i) Sd[i] = st.s[i];
+                float* Jd = J + bc.dof * 8;
+                Jd[0] = ja.x; Jd[1] = ja.y; Jd[2] = ja.z;
+                Jd[3] = jp.x; Jd[4] = jp.y; Jd[5] = jp.z;
+                Jd[6] = prismatic ? 1.0f : 0.0f;
+                Jd[7] = 0.0f;
+            }
+            if (!finite3(cb) || !finite3(wb) || !finite3(vb) || !finite3(st.bl))
+                set_status(misc, MR_STEP_NONFINITE_RESULT, static_cast<unsigned>(b));
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Articulated-body algorithm (ArticulatedABA.metal:905-1440): per-body COM
+// frames in world axes, classical accelerations, 21-entry inertias.  Each
+// body shifts its articulated inertia and bias into its parent's frame and
+// leaves them in shared memory; a parent pulls its children's contributions
+// in a fixed order, so the sums are deterministic without atomics.
+// ---------------------------------------------------------------------------
+__device__ bool aba(const Warp& w, const BodyConst& bc, BodyState& st, float* root_factor) {
     const DeviceModel& M = *w.M;
+    const DeviceTables& T = *w.T;
     const WarpLayout& L = *w.L;
     float* s = w.s;
     float* misc = s + L.misc;
@@ -168,311 +371,190 @@ __device__ bool aba(const Warp& w) {
     const float* v = s + L.v;
     const float* tau = s + L.tau;
     float* qdd = s + L.qdd;
-    float* pose = s + L.body_pose;
-    float* V = s + L.body_V;     // (omega, v_com)
-    float* CV = s + L.body_CV;   // bias accelerations (angular, linear)
-    float* IA = s + L.body_IA;
-    float* PA = s + L.body_PA;
-    float* U = s + L.body_U;
-    float* Du = s + L.body_Du;
+    float* IAc = s + L.body_IA;  // shifted contributions for the parent
+    float* PAc = s + L.body_PA;
     float* A = s + L.body_A;
-    float* R = s + L.body_r;     // parent COM -> body COM
-    float* S = s + L.dof_S;      // motion subspace about the moving body's COM
-    float* J = s + L.dof_J;      // joint axis (3), origin (3), prismatic flag
-    const int lane = w.lane;
+    const int b = w.lane;
+    const bool mine = b < T.nb;
 
-    // Non-finite inputs fail the step before any use
-    // (ArticulatedABA.metal:640-662).
-    for (int i = lane; i < M.nq; i += 32)
+    for (int i = b; i < M.nq; i += 32)
         if (!isfinite(q[i])) set_status(misc, MR_STEP_NONFINITE_INPUT, static_cast<unsigned>(i));
-    for (int i = lane; i < M.nv; i += 32)
+    for (int i = b; i < M.nv; i += 32)
         if (!isfinite(v[i]) || !isfinite(tau[i])) set_status(misc, MR_STEP_NONFINITE_INPUT, static_cast<unsigned>(i));
-    __syncwarp();
-    if (as_int(misc[kMiscStatus]) != MR_STEP_SUCCESS) return false;
+    if (!warp_ok(misc)) return false;
 
-    // Root pose and velocity; root-DoF subspaces and Jacobian axes.
-    if (lane == 0) {
-        if (M.floating) {
-            float4 rq;
-            const float3 c0 = f3(q[0], q[1], q[2]);
-            if (!finite3(c0) || !qnormalize(make_float4(q[3], q[4], q[5], q[6]), rq, true)) {
-                set_status(misc, MR_STEP_NONFINITE_INPUT, 0u);
-            } else {
-                st3(pose, c0);
-                st4(pose + 4, rq);
-                V[0] = v[3]; V[1] = v[4]; V[2] = v[5];
-                V[3] = v[0]; V[4] = v[1]; V[5] = v[2];
-            }
-        } else {
-            st3(pose, f3(0.0f, 0.0f, 0.0f));
-            st4(pose + 4, make_float4(0.0f, 0.0f, 0.0f, 1.0f));
-            for (int i = 0; i < 6; ++i) V[i] = 0.0f;
-        }
-        pose[3] = 0.0f;
-        for (int i = 0; i < 6; ++i) CV[i] = 0.0f;
-        R[0] = R[1] = R[2] = 0.0f;
-    }
-    __syncwarp();
-    if (as_int(misc[kMiscStatus]) != MR_STEP_SUCCESS) return false;
-    if (M.floating && lane < 6) {
-        float* Sd = S + lane * 6;
-        float* Jd = J + lane * 8;
-        for (int i = 0; i < 6; ++i) Sd[i] = 0.0f;
-        // lin DoF k -> (0, e_k); ang DoF k -> (e_k, 0) about the root COM.
-        if (lane < 3) Sd[3 + lane] = 1.0f;
-        else Sd[lane - 3] = 1.0f;
-        const int k = lane < 3 ? lane : lane - 3;
-        Jd[0] = k == 0 ? 1.0f : 0.0f;
-        Jd[1] = k == 1 ? 1.0f : 0.0f;
-        Jd[2] = k == 2 ? 1.0f : 0.0f;
-        Jd[3] = pose[0]; Jd[4] = pose[1]; Jd[5] = pose[2];
-        Jd[6] = lane < 3 ? 1.0f : 0.0f;  // translational root DoFs act like prismatic axes
-        Jd[7] = 0.0f;
-    }
+    kinematics(w, bc, st);
+    if (!warp_ok(misc)) return false;
 
-    // Forward kinematics: poses, twists, subspaces, bias accelerations.
-    for (int l = 0; l < M.n_levels; ++l) {
-        const int off = M.level_offsets[l];
-        const int cnt = M.level_offsets[l + 1] - off;
-        if (lane < cnt) {
-            const int b = M.level_bodies[off + lane];
-            const int p = M.parent[b];
-            const int d = M.body_dof[b];
-            const int type = M.joint_type[b];
-            const float3 cp = ld3(pose + p * 8);
-            const float4 qp = ld4(pose + p * 8 + 4);
-            const float4 pj = qmul(qp, M.parent_rotation[b]);
-            const float3 axis = xyz(M.axis[b]);
-            float4 motion = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
-            float qj = 0.0f, qdj = 0.0f;
-            if (d >= 0) {
-                qj = q[M.dof_q[d]];
-                qdj = v[d];
-                if (type == MR_JOINT_REVOLUTE || type == MR_JOINT_CONTINUOUS) {
-                    const float half = 0.5f * qj;
-                    const float sh = sinf(half);
-                    motion = make_float4(axis.x * sh, axis.y * sh, axis.z * sh, cosf(half));
-                }
-            }
-            float4 qb;
-            if (!qnormalize(qmul(qmul(pj, motion), M.child_rotation_conj[b]), qb, false)) {
-                set_status(misc, MR_STEP_NONFINITE_RESULT, static_cast<unsigned>(b));
-                qb = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
-            }
-            const float3 ja = qrot(pj, axis);
-            const bool prismatic = type == MR_JOINT_PRISMATIC;
-            const bool has = d >= 0;
-            float3 jp = cp + qrot(qp, xyz(M.parent_anchor[b]));
-            if (prismatic) jp = jp + ja * qj;
-            const float3 ca = qrot(qb, xyz(M.child_anchor[b]));
-            const float3 cb = jp - ca;
-            const float3 ptj = jp - cp;
-            st3(pose + b * 8, cb);
-            pose[b * 8 + 3] = 0.0f;
-            st4(pose + b * 8 + 4, qb);
-            st3(R + b * 4, cb - cp);
-            const float3 wp = f3(V[p * 6 + 0], V[p * 6 + 1], V[p * 6 + 2]);
-            const float3 vp = f3(V[p * 6 + 3], V[p * 6 + 4], V[p * 6 + 5]);
-            const float3 wb = wp + ((has && !prismatic) ? ja * qdj : f3(0.0f, 0.0f, 0.0f));
-            const float3 vb = vp + cross3(wp, ptj) + (prismatic ? ja * qdj : f3(0.0f, 0.0f, 0.0f)) - cross3(wb, ca);
-            const float3 ma = (has && !prismatic) ? ja : f3(0.0f, 0.0f, 0.0f);
-            const float3 ml = prismatic ? ja : (has ? -cross3(ja, ca) : f3(0.0f, 0.0f, 0.0f));
-            const float3 ba = (has && !prismatic) ? cross3(wp, ja) * qdj : f3(0.0f, 0.0f, 0.0f);
-            const float3 pc = prismatic ? cross3(wp, ja) * (2.0f * qdj) : f3(0.0f, 0.0f, 0.0f);
-            const float3 bl = cross3(wp, cross3(wp, ptj)) + pc - cross3(ba, ca) - cross3(wb, cross3(wb, ca));
-            V[b * 6 + 0] = wb.x; V[b * 6 + 1] = wb.y; V[b * 6 + 2] = wb.z;
-            V[b * 6 + 3] = vb.x; V[b * 6 + 4] = vb.y; V[b * 6 + 5] = vb.z;
-            CV[b * 6 + 0] = ba.x; CV[b * 6 + 1] = ba.y; CV[b * 6 + 2] = ba.z;
-            CV[b * 6 + 3] = bl.x; CV[b * 6 + 4] = bl.y; CV[b * 6 + 5] = bl.z;
-            if (has) {
-                float* Sd = S + d * 6;
-                Sd[0] = ma.x; Sd[1] = ma.y; Sd[2] = ma.z;
-                Sd[3] = ml.x; Sd[4] = ml.y; Sd[5] = ml.z;
-                float* Jd = J + d * 8;
-                Jd[0] = ja.x; Jd[1] = ja.y; Jd[2] = ja.z;
-                Jd[3] = jp.x; Jd[4] = jp.y; Jd[5] = jp.z;
-                Jd[6] = prismatic ? 1.0f : 0.0f;
-                Jd[7] = 0.0f;
-            }
-            if (!finite3(cb) || !finite3(wb) || !finite3(vb) || !finite3(bl))
-                set_status(misc, MR_STEP_NONFINITE_RESULT, static_cast<unsigned>(b));
-        }
-        __syncwarp();
-    }
-    if (as_int(misc[kMiscStatus]) != MR_STEP_SUCCESS) return false;
-
-    // Rigid inertia and velocity-dependent bias of every body about its COM.
-    if (lane < M.nb) {
-        const int b = lane;
-        const float4 qb = ld4(pose + b * 8 + 4);
-        const float4 md = M.mass_damping[b];
+    // Rigid inertia and velocity-dependent bias about the COM.
+    if (mine) {
         float Iw[3][3];
-        float* I6 = IA + b * 21;
-        body_inertia(M, b, qb, I6, Iw);
-        const float3 om = f3(V[b * 6 + 0], V[b * 6 + 1], V[b * 6 + 2]);
-        const float3 vc = f3(V[b * 6 + 3], V[b * 6 + 4], V[b * 6 + 5]);
+        body_inertia(bc, st.qr, st.I, Iw);
+        const float3 om = st.w;
         const float3 Iom = f3(Iw[0][0] * om.x + Iw[0][1] * om.y + Iw[0][2] * om.z,
                               Iw[1][0] * om.x + Iw[1][1] * om.y + Iw[1][2] * om.z,
                               Iw[2][0] * om.x + Iw[2][1] * om.y + Iw[2][2] * om.z);
         float3 bt = cross3(om, Iom);
-        float3 bf = -(md.x * f3(M.gravity[0], M.gravity[1], M.gravity[2]));
+        float3 bf = -(bc.mass * f3(M.gravity[0], M.gravity[1], M.gravity[2]));
         if (M.apply_damping) {
-            bt = bt + md.z * om;
-            bf = bf + md.y * vc;
+            bt = bt + bc.ang_damp * om;
+            bf = bf + bc.lin_damp * st.v;
         }
-        float* pa = PA + b * 6;
-        pa[0] = bt.x; pa[1] = bt.y; pa[2] = bt.z; pa[3] = bf.x; pa[4] = bf.y; pa[5] = bf.z;
-        if (b == 0 && M.floating) {
+        st.p[0] = bt.x; st.p[1] = bt.y; st.p[2] = bt.z; st.p[3] = bf.x; st.p[4] = bf.y; st.p[5] = bf.z;
+        if (b == 0 && T.floating) {
             for (int k = 0; k < 3; ++k) {
-                I6[sym6(3 + k, 3 + k)] += M.armature_eff[k];
-                I6[sym6(k, k)] += M.armature_eff[3 + k];
-                pa[k] -= tau[3 + k];
-                pa[3 + k] -= tau[k];
+                st.I[sym6(3 + k, 3 + k)] += M.armature_eff[k];
+                st.I[sym6(k, k)] += M.armature_eff[3 + k];
+                st.p[k] -= tau[3 + k];
+                st.p[3 + k] -= tau[k];
             }
         }
     }
-    __syncwarp();
-
-    // Backward sweep.
-    for (int l = M.n_levels - 1; l >= 0; --l) {
-        const int off = M.level_offsets[l];
-        const int cnt = M.level_offsets[l + 1] - off;
-        if (lane < cnt) {
-            const int b = M.level_bodies[off + lane];
-            float* I6 = IA + b * 21;
-            float* pa = PA + b * 6;
-            for (int k = M.child_offsets[b]; k < M.child_offsets[b + 1]; ++k) {
-                const int c = M.children[k];
-                for (int e = 0; e < 21; ++e) I6[e] += IA[c * 21 + e];
-                for (int e = 0; e < 6; ++e) pa[e] += PA[c * 6 + e];
+    // Backward sweep, deepest level first; the root (level 0) last.
+    const int my_depth = mine ? T.depth[b] : -1;
+    for (int l = T.n_levels; l >= 0; --l) {
+        if (my_depth == l) {
+            for (int k = T.child_offsets[b]; k < T.child_offsets[b + 1]; ++k) {
+                const int c = T.children[k];
+#pragma unroll
+                for (int e = 0; e < 21; ++e) st.I[e] += IAc[c * 21 + e];
+#pragma unroll
+                for (int e = 0; e < 6; ++e) st.p[e] += PAc[c * 6 + e];
             }
-            const int d = M.body_dof[b];
-            float prop[6], ic[6];
-            sym6_mul(I6, CV + b * 6, ic);
-            for (int e = 0; e < 6; ++e) prop[e] = pa[e] + ic[e];
-            if (d >= 0) {
-                const float* sd = S + d * 6;
-                float u6[6];
-                sym6_mul(I6, sd, u6);
-                const float D = dot6(sd, u6) + M.armature_eff[d];
-                float maxI = 0.0f;
-                for (int e = 0; e < 21; ++e) maxI = fmaxf(maxI, fabsf(I6[e]));
-                const float floor = fmaxf(kAbsolutePivotFloor, maxI * 6.0f * kFloatEps);
-                if (!(D > floor) || !isfinite(D)) {
-                    set_status(misc, MR_STEP_FACTORIZATION_FAILED, static_cast<unsigned>(d));
-                } else {
-                    const float u = tau[d] - dot6(sd, prop);
-                    const float invD = 1.0f / D;
-                    for (int e = 0; e < 6; ++e) U[b * 6 + e] = u6[e];
-                    Du[b * 2 + 0] = D;
-                    Du[b * 2 + 1] = u;
-                    for (int e = 0; e < 6; ++e) prop[e] += u6[e] * (u * invD);
-                    for (int i = 0; i < 6; ++i)
-                        for (int j = 0; j <= i; ++j) I6[sym6(i, j)] -= u6[i] * u6[j] * invD;
+            if (l > 0) {
+                float prop[6], ic[6];
+                const float cv[6] = {st.ba.x, st.ba.y, st.ba.z, st.bl.x, st.bl.y, st.bl.z};
+                sym6_mul(st.I, cv, ic);
+#pragma unroll
+                for (int e = 0; e < 6; ++e) prop[e] = st.p[e] + ic[e];
+                if (bc.dof >= 0) {
+                    sym6_mul(st.I, st.s, st.U);
+                    const float D = dot6(st.s, st.U) + M.armature_eff[bc.dof];
+                    float maxI = 0.0f;
+#pragma unroll
+                    for (int e = 0; e < 21; ++e) maxI = fmaxf(maxI, fabsf(st.I[e]));
+                    const float floor = fmaxf(kAbsolutePivotFloor, maxI * 6.0f * kFloatEps);
+                    if (!(D > floor) || !isfinite(D)) {
+                        set_status(misc, MR_STEP_FACTORIZATION_FAILED, static_cast<unsigned>(bc.dof));
+                        st.D = 1.0f;
+                        st.u = 0.0f;
+                    } else {
+                        st.D = D;
+                        st.u = tau[bc.dof] - dot6(st.s, prop);
+                        const float invD = 1.0f / D;
+#pragma unroll
+                        for (int e = 0; e < 6; ++e) prop[e] += st.U[e] * (st.u * invD);
+#pragma unroll
+                        for (int i = 0; i < 6; ++i)
+#pragma unroll
+                            for (int j = 0; j <= i; ++j) st.I[sym6(i, j)] -= st.U[i] * st.U[j] * invD;
+                    }
                 }
+                float shifted[21];
+                shift_inertia(st.I, st.r, shifted);
+#pragma unroll
+                for (int e = 0; e < 21; ++e) IAc[b * 21 + e] = shifted[e];
+                const float3 pf = f3(prop[3], prop[4], prop[5]);
+                const float3 pt = f3(prop[0], prop[1], prop[2]) + cross3(st.r, pf);
+                float* pc = PAc + b * 6;
+                pc[0] = pt.x; pc[1] = pt.y; pc[2] = pt.z; pc[3] = pf.x; pc[4] = pf.y; pc[5] = pf.z;
+            } else if (T.floating) {
+                // Root articulated inertia in DoF order (linear x, y, z, then
+                // angular x, y, z), factored leaves-first as H0 = L0^T L0: these
+                // are rows 0-5 of the joint-space factor H = L^T L, whose joint
+                // rows are L_kk = sqrt(D_k), L_kj = U_k . S_j / L_kk.  Solves
+                // H0 a0 = -pA for the root acceleration.
+                float Lf[21], r[6];
+                float maxI = 0.0f;
+#pragma unroll
+                for (int e = 0; e < 21; ++e) maxI = fmaxf(maxI, fabsf(st.I[e]));
+                const float floor = fmaxf(kAbsolutePivotFloor, maxI * 6.0f * kFloatEps);
+#pragma unroll
+                for (int k = 0; k < 6; ++k) {
+                    const int pk = k < 3 ? k + 3 : k - 3;
+                    r[k] = -st.p[pk];
+#pragma unroll
+                    for (int j = 0; j <= k; ++j) Lf[sym6(k, j)] = st.I[sym6(pk, j < 3 ? j + 3 : j - 3)];
+                }
+                bool ok = true;
+#pragma unroll
+                for (int k = 5; k >= 0; --k) {
+                    float d = Lf[sym6(k, k)];
+                    if (!(d > floor) || !isfinite(d)) {
+                        ok = false;
+                        d = 1.0f;
+                    }
+                    const float lkk = sqrtf(d);
+                    Lf[sym6(k, k)] = lkk;
+                    const float inv = 1.0f / lkk;
+#pragma unroll
+                    for (int j = 0; j < k; ++j) Lf[sym6(k, j)] *= inv;
+#pragma unroll
+                    for (int i = 0; i < k; ++i)
+#pragma unroll
+                        for (int j = 0; j <= i; ++j) Lf[sym6(i, j)] -= Lf[sym6(k, i)] * Lf[sym6(k, j)];
+                }
+                float y[6], x[6];
+#pragma unroll
+                for (int k = 5; k >= 0; --k) {
+                    float val = r[k];
+#pragma unroll
+                    for (int i = k + 1; i < 6; ++i) val -= Lf[sym6(i, k)] * y[i];
+                    y[k] = val / Lf[sym6(k, k)];
+                }
+#pragma unroll
+                for (int k = 0; k < 6; ++k) {
+                    float val = y[k];
+#pragma unroll
+                    for (int j = 0; j < k; ++j) val -= Lf[sym6(k, j)] * x[j];
+                    x[k] = val / Lf[sym6(k, k)];
+                }
+                if (!ok) set_status(misc, MR_STEP_FACTORIZATION_FAILED, 0u);
+                if (root_factor != nullptr) {
+#pragma unroll
+                    for (int e = 0; e < 21; ++e) root_factor[e] = Lf[e];
+                }
+#pragma unroll
+                for (int k = 0; k < 6; ++k) qdd[k] = x[k];
+                A[0] = x[3]; A[1] = x[4]; A[2] = x[5];
+                A[3] = x[0]; A[4] = x[1]; A[5] = x[2];
+            } else {
+                for (int i = 0; i < 6; ++i) A[i] = 0.0f;
             }
-            // Contribution in the parent's frame, left in this body's slots.
-            const float3 r = ld3(R + b * 4);
-            float shifted[21];
-            shift_inertia(I6, r, shifted);
-            for (int e = 0; e < 21; ++e) I6[e] = shifted[e];
-            const float3 pf = f3(prop[3], prop[4], prop[5]);
-            const float3 pt = f3(prop[0], prop[1], prop[2]) + cross3(r, pf);
-            pa[0] = pt.x; pa[1] = pt.y; pa[2] = pt.z; pa[3] = pf.x; pa[4] = pf.y; pa[5] = pf.z;
         }
         __syncwarp();
     }
-    // Root: pull children (lane per entry), then solve the floating root.
-    if (lane < 27) {
-        float* dst = lane < 21 ? IA + lane : PA + (lane - 21);
-        const int stride = lane < 21 ? 21 : 6;
-        const float* src = lane < 21 ? IA : PA;
-        const int e = lane < 21 ? lane : lane - 21;
-        float acc = *dst;
-        for (int k = M.child_offsets[0]; k < M.child_offsets[1]; ++k) acc += src[M.children[k] * stride + e];
-        *dst = acc;
-    }
-    __syncwarp();
-    if (lane == 0) {
-        if (M.floating) {
-            // 6x6 Cholesky of the root articulated inertia; a0 = -IA^-1 pA.
-            float Lf[36];
-            float maxI = 0.0f;
-            for (int e = 0; e < 21; ++e) maxI = fmaxf(maxI, fabsf(IA[e]));
-            const float floor = fmaxf(kAbsolutePivotFloor, maxI * 6.0f * kFloatEps);
-            bool ok = true;
-            for (int i = 0; i < 6 && ok; ++i) {
-                for (int j = 0; j <= i; ++j) {
-                    float val = IA[sym6(i, j)];
-                    for (int k = 0; k < j; ++k) val -= Lf[i * 6 + k] * Lf[j * 6 + k];
-                    if (i == j) {
-                        if (!(val > floor) || !isfinite(val)) { ok = false; set_status(misc, MR_STEP_FACTORIZATION_FAILED, static_cast<unsigned>(i)); break; }
-                        Lf[i * 6 + i] = sqrtf(val);
-                    } else {
-                        Lf[i * 6 + j] = val / Lf[j * 6 + j];
-                    }
-                }
-            }
-            if (ok) {
-                float y[6], x[6];
-                for (int i = 0; i < 6; ++i) {
-                    float val = -PA[i];
-                    for (int k = 0; k < i; ++k) val -= Lf[i * 6 + k] * y[k];
-                    y[i] = val / Lf[i * 6 + i];
-                }
-                for (int i = 5; i >= 0; --i) {
-                    float val = y[i];
-                    for (int k = i + 1; k < 6; ++k) val -= Lf[k * 6 + i] * x[k];
-                    x[i] = val / Lf[i * 6 + i];
-                }
-                for (int i = 0; i < 6; ++i) A[i] = x[i];
-                qdd[0] = x[3]; qdd[1] = x[4]; qdd[2] = x[5];
-                qdd[3] = x[0]; qdd[4] = x[1]; qdd[5] = x[2];
-            }
-        } else {
-            for (int i = 0; i < 6; ++i) A[i] = 0.0f;
-        }
-    }
-    __syncwarp();
-    if (as_int(misc[kMiscStatus]) != MR_STEP_SUCCESS) return false;
+    if (!warp_ok(misc)) return false;
 
     // Forward acceleration sweep.
-    for (int l = 0; l < M.n_levels; ++l) {
-        const int off = M.level_offsets[l];
-        const int cnt = M.level_offsets[l + 1] - off;
-        if (lane < cnt) {
-            const int b = M.level_bodies[off + lane];
-            const int p = M.parent[b];
-            const int d = M.body_dof[b];
-            const float3 r = ld3(R + b * 4);
-            const float3 pa_ = f3(A[p * 6 + 0], A[p * 6 + 1], A[p * 6 + 2]);
-            const float3 pl = f3(A[p * 6 + 3], A[p * 6 + 4], A[p * 6 + 5]) + cross3(pa_, r);
-            float3 ang = pa_ + f3(CV[b * 6 + 0], CV[b * 6 + 1], CV[b * 6 + 2]);
-            float3 lin = pl + f3(CV[b * 6 + 3], CV[b * 6 + 4], CV[b * 6 + 5]);
-            if (d >= 0) {
-                const float* Ub = U + b * 6;
-                const float proj = Ub[0] * pa_.x + Ub[1] * pa_.y + Ub[2] * pa_.z + Ub[3] * pl.x + Ub[4] * pl.y + Ub[5] * pl.z;
-                const float acc = (Du[b * 2 + 1] - proj) / Du[b * 2 + 0];
-                qdd[d] = acc;
-                const float* sd = S + d * 6;
-                ang = ang + f3(sd[0], sd[1], sd[2]) * acc;
-                lin = lin + f3(sd[3], sd[4], sd[5]) * acc;
+    for (int l = 1; l <= T.n_levels; ++l) {
+        if (my_depth == l) {
+            const int p = bc.parent;
+            const float3 pa = ld3(A + p * 6);
+            const float3 pl = ld3(A + p * 6 + 3) + cross3(pa, st.r);
+            float3 ang = pa + st.ba;
+            float3 lin = pl + st.bl;
+            if (bc.dof >= 0) {
+                const float proj = st.U[0] * pa.x + st.U[1] * pa.y + st.U[2] * pa.z + st.U[3] * pl.x + st.U[4] * pl.y + st.U[5] * pl.z;
+                const float acc = (st.u - proj) / st.D;
+                qdd[bc.dof] = acc;
+                ang = ang + f3(st.s[0], st.s[1], st.s[2]) * acc;
+                lin = lin + f3(st.s[3], st.s[4], st.s[5]) * acc;
             }
-            A[b * 6 + 0] = ang.x; A[b * 6 + 1] = ang.y; A[b * 6 + 2] = ang.z;
-            A[b * 6 + 3] = lin.x; A[b * 6 + 4] = lin.y; A[b * 6 + 5] = lin.z;
+            st3(A + b * 6, ang);
+            st3(A + b * 6 + 3, lin);
         }
         __syncwarp();
     }
     // v_free = v + h qdd.
     float* vf = s + L.vf;
-    for (int d = lane; d < M.nv; d += 32) {
+    for (int d = b; d < M.nv; d += 32) {
         const float a = qdd[d];
         const float nvv = v[d] + M.h * a;
         if (!isfinite(a) || !isfinite(nvv)) set_status(misc, MR_STEP_NONFINITE_RESULT, static_cast<unsigned>(d));
         vf[d] = nvv;
     }
-    __syncwarp();
-    return as_int(misc[kMiscStatus]) == MR_STEP_SUCCESS;
+    return warp_ok(misc);
 }
 
 // Free-motion commit of the ABA candidate (ArticulatedABA.metal:1466-1540):
@@ -508,8 +590,7 @@ __device__ bool integrate_free(const Warp& w) {
         }
         if (!isfinite(q[0]) || !isfinite(q[1]) || !isfinite(q[2])) set_status(misc, MR_STEP_NONFINITE_RESULT, 0u);
     }
-    __syncwarp();
-    return as_int(misc[kMiscStatus]) == MR_STEP_SUCCESS;
+    return warp_ok(misc);
 }
 
 // ---------------------------------------------------------------------------
@@ -517,30 +598,8 @@ __device__ bool integrate_free(const Warp& w) {
 // and persistent manifolds (Collision.metal:380-1000, 4379-4830, 5115-5560,
 // 5712-6030, 9557-9830).  One lane owns one compiled pair.
 // ---------------------------------------------------------------------------
-struct RawContact {
-    float3 normal;
-    float sep;
-    float3 pa, pb;
-    unsigned fa, fb;
-};
-
-struct Candidate {
-    float la[3], lb[3];
-    unsigned fa, fb, life;
-    float imp[3];
-    float3 wp;
-    float sep, drift;
-};
-
 __device__ __forceinline__ unsigned feature_key(unsigned type, unsigned local) {
     return ((type & 0x0fu) << 28u) | (local & 0x0fffffffu);
-}
-__device__ __forceinline__ unsigned long long cand_key(const Candidate& c) {
-    return (static_cast<unsigned long long>(c.fa) << 32) | c.fb;
-}
-__device__ __forceinline__ bool cand_less(const Candidate& a, const Candidate& b) {
-    if (a.sep != b.sep) return a.sep < b.sep;
-    return cand_key(a) < cand_key(b);
 }
 
 __device__ __forceinline__ float3 stable_tangent(float3 n) {
@@ -636,10 +695,28 @@ __device__ __forceinline__ float shape_scale(const ShapeWorld& s) {
                        fmaxf(fabsf(s.offset), fmaxf(maxabs3(s.lower), maxabs3(s.upper)))));
 }
 
-// Builds the new persistent manifold of one pair into `slot` (in/out).
+// Narrowphase candidate record in shared-memory scratch (16 words): local
+// anchors on A and B, feature ids, world midpoint, separation, lifetime and
+// accumulated impulse.  Records 0-3 are the kept points of the old manifold,
+// records 4.. the raw contacts of this substep.
+enum CandidateWord : int {
+    kCdLa = 0, kCdLb = 3, kCdFa = 6, kCdFb = 7, kCdWp = 8, kCdSep = 11, kCdLife = 12, kCdImp = 13
+};
+// A candidate is one byte: low nibble = record that holds its geometry,
+// high nibble = old record it inherits lifetime and impulse from (15: new).
+constexpr unsigned kFresh = 15u;
+
+__device__ __forceinline__ unsigned long long record_key(const float* rec) {
+    return (static_cast<unsigned long long>(static_cast<unsigned>(as_int(rec[kCdFa]))) << 32) |
+           static_cast<unsigned>(as_int(rec[kCdFb]));
+}
+
+// Builds the new persistent manifold of one pair into `slot` (in/out), using
+// `scratch` (pair_scratch_words of the pair class) for its candidates.
 // Returns the number of points, or -1 on a non-finite / overflow failure.
+// Plane pair classes only: every raw contact shares the plane normal.
 __device__ int pair_manifold(const DeviceModel& M, const float* pose, const float* margins, int pair, float* slot,
-                             int& raw_count_out, bool& candidate_out) {
+                             float* scratch, int& raw_count_out, bool& candidate_out) {
     raw_count_out = 0;
     candidate_out = false;
     const int sa = M.pair_a[pair];
@@ -666,25 +743,30 @@ __device__ int pair_manifold(const DeviceModel& M, const float* pose, const floa
     }
     candidate_out = true;
     const float accepted = A.offset + B.offset + (fmaxf(shape_scale(A), shape_scale(B)) + 1.0f) * kQueryPad;
-    RawContact raw[8];
+    const float3 posA = A.body_pos, posB = B.body_pos;
+    const float4 rotA = A.body_rot, rotB = B.body_rot;
+    const unsigned plane_feature = feature_key(MR_SHAPE_PLANE, 0u);
+    const float3 raw_normal = a_plane ? plane.normal : -plane.normal;
+    float* raw = scratch + 4 * kCandidateWords;
     int nraw = 0;
+    bool finite = true;
+    // Raw contact: surface point of the finite shape, its projection on the
+    // plane, normal A -> B (Collision.metal:4379-4830, plane witnesses).
     auto append = [&](float3 surface, float sep, unsigned ffeat) {
         const float3 pp = surface - plane.normal * sep;
-        RawContact r;
-        r.normal = -plane.normal;
-        r.sep = sep;
-        r.pa = surface;
-        r.pb = pp;
-        r.fa = ffeat;
-        r.fb = feature_key(MR_SHAPE_PLANE, 0u);
-        if (a_plane) {  // swapped orientation: A is the plane
-            r.normal = plane.normal;
-            r.pa = pp;
-            r.pb = surface;
-            r.fa = feature_key(MR_SHAPE_PLANE, 0u);
-            r.fb = ffeat;
-        }
-        raw[nraw++] = r;
+        const float3 pa = a_plane ? pp : surface;
+        const float3 pb = a_plane ? surface : pp;
+        float* rec = raw + nraw * kCandidateWords;
+        const float3 la = qrotinv(rotA, pa - posA);
+        const float3 lb = qrotinv(rotB, pb - posB);
+        st3(rec + kCdLa, la);
+        st3(rec + kCdLb, lb);
+        rec[kCdFa] = as_float(static_cast<int>(a_plane ? plane_feature : ffeat));
+        rec[kCdFb] = as_float(static_cast<int>(a_plane ? ffeat : plane_feature));
+        st3(rec + kCdWp, 0.5f * (pa + pb));
+        rec[kCdSep] = sep;
+        finite = finite && isfinite(sep) && finite3(pa) && finite3(pb);
+        ++nraw;
     };
     const int cls = M.pair_class[pair];
     if (cls == MR_COLLISION_PAIR_SPHERE_PLANE) {
@@ -711,24 +793,15 @@ __device__ int pair_manifold(const DeviceModel& M, const float* pose, const floa
         slot[7] = as_float(0);
         return 0;
     }
-    for (int i = 0; i < nraw; ++i)
-        if (!finite3(raw[i].normal) || !isfinite(raw[i].sep) || !finite3(raw[i].pa) || !finite3(raw[i].pb)) return -1;
+    if (!finite || !finite3(raw_normal)) return -1;
 
-    // buildPersistentWorldManifold.
-    int deepest = 0;
-    for (int i = 1; i < nraw; ++i) {
-        const RawContact& l = raw[i];
-        const RawContact& r = raw[deepest];
-        if (l.sep < r.sep || (l.sep == r.sep && (l.fa < r.fa || (l.fa == r.fa && l.fb < r.fb)))) deepest = i;
-    }
-    float3 nw = raw[deepest].normal;
-    nw = nw * (1.0f / len3(nw));
+    // buildPersistentWorldManifold (Collision.metal:5290-5560,
+    // Collision.cpp:2546-2760).
+    float3 nw = raw_normal * (1.0f / len3(raw_normal));
     if (!finite3(nw) || dot3(nw, nw) < 0.9999f) return -1;
-    const float3 posA = A.body_pos, posB = B.body_pos;
-    const float4 rotA = A.body_rot, rotB = B.body_rot;
     const float4 thr = make_float4(M.manifold_thresholds[0], M.manifold_thresholds[1], M.manifold_thresholds[2],
                                    M.manifold_thresholds[3]);
-    Candidate cands[12];
+    unsigned char* ids = reinterpret_cast<unsigned char*>(scratch + (4 + pair_max_raw(cls)) * kCandidateWords);
     int nc = 0;
     bool old_ok = false;
     float3 transported = f3(0.0f, 0.0f, 0.0f);
@@ -749,113 +822,133 @@ __device__ int pair_manifold(const DeviceModel& M, const float* pose, const floa
                 const float3 delta = pb - pa;
                 const float sep = dot3(delta, nw);
                 const float3 tan = delta - nw * sep;
-                const float drift = len3(tan);
-                if (sep > thr.x || drift > thr.y) continue;
-                Candidate& c = cands[nc++];
-                for (int k = 0; k < 3; ++k) { c.la[k] = op[k]; c.lb[k] = op[3 + k]; c.imp[k] = op[9 + k]; }
-                c.fa = static_cast<unsigned>(as_int(op[6]));
-                c.fb = static_cast<unsigned>(as_int(op[7]));
+                if (sep > thr.x || len3(tan) > thr.y) continue;
+                float* rec = scratch + i * kCandidateWords;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) rec[k] = op[k];  // anchors and feature ids
                 const unsigned life = static_cast<unsigned>(as_int(op[8]));
-                c.life = life == 0xffffffffu ? 0xffffffffu : life + 1u;
-                c.wp = 0.5f * (pa + pb);
-                c.sep = sep;
-                c.drift = drift;
+                rec[kCdLife] = as_float(static_cast<int>(life == 0xffffffffu ? 0xffffffffu : life + 1u));
+                rec[kCdImp + 0] = op[9];
+                rec[kCdImp + 1] = op[10];
+                rec[kCdImp + 2] = op[11];
+                st3(rec + kCdWp, 0.5f * (pa + pb));
+                rec[kCdSep] = sep;
+                ids[nc++] = static_cast<unsigned char>((i << 4) | i);
             }
         }
     }
+    // Raw contacts refresh a candidate with the same features, else one
+    // within the merge distance, else join as new points.
     const float merge2 = thr.z * thr.z;
-    for (int i = 0; i < nraw; ++i) {
-        const RawContact& r = raw[i];
-        const float3 la = qrotinv(rotA, r.pa - posA);
-        const float3 lb = qrotinv(rotB, r.pb - posB);
+    for (int r = 0; r < nraw; ++r) {
+        const float* rr = raw + r * kCandidateWords;
+        const float3 la = ld3(rr + kCdLa), lb = ld3(rr + kCdLb);
+        const int fa = as_int(rr[kCdFa]), fb = as_int(rr[kCdFb]);
         int match = -1;
-        for (int k = 0; k < nc; ++k)
-            if (cands[k].fa == r.fa && cands[k].fb == r.fb) { match = k; break; }
+        for (int k = 0; k < nc; ++k) {
+            const float* g = scratch + (ids[k] & 15u) * kCandidateWords;
+            if (as_int(g[kCdFa]) == fa && as_int(g[kCdFb]) == fb) { match = k; break; }
+        }
         if (match < 0) {
             for (int k = 0; k < nc; ++k) {
-                const float3 da = f3(cands[k].la[0], cands[k].la[1], cands[k].la[2]) - la;
-                const float3 db = f3(cands[k].lb[0], cands[k].lb[1], cands[k].lb[2]) - lb;
+                const float* g = scratch + (ids[k] & 15u) * kCandidateWords;
+                const float3 da = ld3(g + kCdLa) - la;
+                const float3 db = ld3(g + kCdLb) - lb;
                 if (dot3(da, da) + dot3(db, db) <= 2.0f * merge2) { match = k; break; }
             }
         }
         if (match < 0) {
-            if (nc >= 12) return -1;
-            match = nc++;
-            Candidate& c = cands[match];
-            c.life = 0u;
-            c.imp[0] = c.imp[1] = c.imp[2] = 0.0f;
+            if (nc >= 4 + kMaxRawPerPair) return -1;
+            ids[nc++] = static_cast<unsigned char>((kFresh << 4) | (4u + r));
+        } else {
+            ids[match] = static_cast<unsigned char>((ids[match] & 0xf0u) | (4u + r));
         }
-        Candidate& c = cands[match];
-        c.la[0] = la.x; c.la[1] = la.y; c.la[2] = la.z;
-        c.lb[0] = lb.x; c.lb[1] = lb.y; c.lb[2] = lb.z;
-        c.fa = r.fa;
-        c.fb = r.fb;
-        c.wp = 0.5f * (r.pa + r.pb);
-        c.sep = r.sep;
-        c.drift = 0.0f;
     }
-    if (nc == 0) return -1;
-    // reduceCandidates: sort by (separation, feature), pick 4 spread points,
-    // then canonical feature order.
-    for (int i = 1; i < nc; ++i) {
-        Candidate val = cands[i];
-        int d = i;
-        while (d > 0 && cand_less(val, cands[d - 1])) { cands[d] = cands[d - 1]; --d; }
-        cands[d] = val;
-    }
+    // reduceCandidates.  With at most four candidates the separation order
+    // cannot change the result (the final order is canonical by feature), so
+    // the separation sort and the reduction run only for larger sets.
     if (nc > kManifoldPoints) {
-        bool selected[12];
-        for (int i = 0; i < 12; ++i) selected[i] = false;
-        int chosen[kManifoldPoints];
-        chosen[0] = 0;
-        selected[0] = true;
+        for (int i = 1; i < nc; ++i) {
+            const unsigned char val = ids[i];
+            const float* gv = scratch + (val & 15u) * kCandidateWords;
+            const float sv = gv[kCdSep];
+            const unsigned long long kv = record_key(gv);
+            int d = i;
+            while (d > 0) {
+                const float* gp = scratch + (ids[d - 1] & 15u) * kCandidateWords;
+                const float sp = gp[kCdSep];
+                if (!(sv < sp || (sv == sp && kv < record_key(gp)))) break;
+                ids[d] = ids[d - 1];
+                --d;
+            }
+            ids[d] = val;
+        }
+        // Greedy selection: deepest, farthest in the tangent plane, largest
+        // area, then largest minimum distance.  Box faces make exact ties
+        // structural (parallel edges give equal distances and areas), so
+        // scores within a relative 1e-5 count as tied and go to the smaller
+        // feature key: the choice no longer depends on FP32 rounding.  The
+        // reference compares with absolute tolerances below the rounding of
+        // these scores (Collision.metal:5247, Collision.cpp:2531-2544).
+        unsigned selected = 1u;
+        unsigned chosen = 0u;  // candidate indices, one byte each
         int chosen_count = 1;
+        const float3 w0 = ld3(scratch + (ids[0] & 15u) * kCandidateWords + kCdWp);
+        float3 w1 = w0;
         for (int stage = 1; stage < kManifoldPoints; ++stage) {
             int best = -1;
             float best_score = -1.0f;
             unsigned long long best_feature = ~0ull;
             for (int i = 0; i < nc; ++i) {
-                if (selected[i]) continue;
+                if (selected & (1u << i)) continue;
+                const float* gi = scratch + (ids[i] & 15u) * kCandidateWords;
+                const float3 wi = ld3(gi + kCdWp);
                 float score;
                 if (stage == 1) {
-                    const float3 dl = cands[i].wp - cands[chosen[0]].wp;
+                    const float3 dl = wi - w0;
                     const float3 t = dl - nw * dot3(dl, nw);
                     score = dot3(t, t);
                 } else if (stage == 2) {
-                    const float3 a = cands[chosen[1]].wp - cands[chosen[0]].wp;
-                    const float3 bb = cands[i].wp - cands[chosen[0]].wp;
-                    score = fabsf(dot3(cross3(a, bb), nw));
+                    score = fabsf(dot3(cross3(w1 - w0, wi - w0), nw));
                 } else {
                     score = INFINITY;
                     for (int k = 0; k < chosen_count; ++k) {
-                        const float3 dl = cands[i].wp - cands[chosen[k]].wp;
+                        const int ck = static_cast<int>((chosen >> (8 * k)) & 0xffu);
+                        const float3 dl = wi - ld3(scratch + (ids[ck] & 15u) * kCandidateWords + kCdWp);
                         const float3 t = dl - nw * dot3(dl, nw);
                         score = fminf(score, dot3(t, t));
                     }
                 }
-                const unsigned long long f = cand_key(cands[i]);
-                if (score > best_score + 1.0e-12f || (fabsf(score - best_score) <= 1.0e-12f && f < best_feature)) {
+                const unsigned long long f = record_key(gi);
+                const float tol = fmaxf(kTieAbsolute, kTieRelative * fmaxf(fabsf(score), fabsf(best_score)));
+                if (score > best_score + tol || (fabsf(score - best_score) <= tol && f < best_feature)) {
                     best = i;
                     best_score = score;
                     best_feature = f;
                 }
             }
             if (best >= 0) {
-                chosen[chosen_count++] = best;
-                selected[best] = true;
+                chosen |= static_cast<unsigned>(best) << (8 * chosen_count);
+                ++chosen_count;
+                selected |= 1u << best;
+                if (stage == 1) w1 = ld3(scratch + (ids[best] & 15u) * kCandidateWords + kCdWp);
             }
         }
-        Candidate reduced[kManifoldPoints];
-        for (int i = 0; i < chosen_count; ++i) reduced[i] = cands[chosen[i]];
+        unsigned packed = 0u;
+        for (int k = 0; k < chosen_count; ++k) packed |= static_cast<unsigned>(ids[(chosen >> (8 * k)) & 0xffu]) << (8 * k);
+        for (int k = 0; k < chosen_count; ++k) ids[k] = static_cast<unsigned char>((packed >> (8 * k)) & 0xffu);
         nc = chosen_count;
-        for (int i = 0; i < nc; ++i) cands[i] = reduced[i];
     }
+    // Canonical order by feature pair.
     for (int i = 1; i < nc; ++i) {
-        Candidate val = cands[i];
-        const unsigned long long f = cand_key(val);
+        const unsigned char val = ids[i];
+        const unsigned long long f = record_key(scratch + (val & 15u) * kCandidateWords);
         int d = i;
-        while (d > 0 && f < cand_key(cands[d - 1])) { cands[d] = cands[d - 1]; --d; }
-        cands[d] = val;
+        while (d > 0 && f < record_key(scratch + (ids[d - 1] & 15u) * kCandidateWords)) {
+            ids[d] = ids[d - 1];
+            --d;
+        }
+        ids[d] = val;
     }
     float3 tw = transported;
     if (!old_ok || !finite3(tw) || dot3(tw, tw) <= 1.0e-12f) tw = stable_tangent(nw);
@@ -867,12 +960,22 @@ __device__ int pair_manifold(const DeviceModel& M, const float* pose, const floa
     for (int i = 0; i < kManifoldPoints; ++i) {
         float* op = slot + 8 + i * 12;
         if (i < nc) {
-            const Candidate& c = cands[i];
-            for (int k = 0; k < 3; ++k) { op[k] = c.la[k]; op[3 + k] = c.lb[k]; op[9 + k] = c.imp[k]; }
-            op[6] = as_float(static_cast<int>(c.fa));
-            op[7] = as_float(static_cast<int>(c.fb));
-            op[8] = as_float(static_cast<int>(c.life));
+            const unsigned id = ids[i];
+            const float* g = scratch + (id & 15u) * kCandidateWords;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) op[k] = g[k];
+            if ((id >> 4) == kFresh) {
+                op[8] = as_float(0);
+                op[9] = op[10] = op[11] = 0.0f;
+            } else {
+                const float* hrec = scratch + (id >> 4) * kCandidateWords;
+                op[8] = hrec[kCdLife];
+                op[9] = hrec[kCdImp + 0];
+                op[10] = hrec[kCdImp + 1];
+                op[11] = hrec[kCdImp + 2];
+            }
         } else {
+#pragma unroll
             for (int k = 0; k < 12; ++k) op[k] = 0.0f;
         }
     }
@@ -934,54 +1037,60 @@ __device__ bool invert3x3_reg(const float m[3][3], float inv[3][3]) {
 }
 
 // ---------------------------------------------------------------------------
-// Contact substep after the ABA: collision, ConstraintIR evaluation, mass
-// factor and response columns, temporalCone solve, joint limits, integration.
+// Contact substep after the ABA: collision, ConstraintIR evaluation, joint
+// inertia factor, temporalCone solve, joint limits, integration.
 // ---------------------------------------------------------------------------
-__device__ bool contact_substep(const Warp& w, bool final_substep, int velocity_iterations, int final_iterations,
-                                float friction_scale) {
+__device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState& st, bool final_substep,
+                                int velocity_iterations, int final_iterations, float friction_scale) {
     const DeviceModel& M = *w.M;
+    const DeviceTables& T = *w.T;
     const WarpLayout& L = *w.L;
     float* s = w.s;
     float* misc = s + L.misc;
     const int lane = w.lane;
     const int nv = M.nv;
     const float h = M.h;
-    float* pose = s + L.body_pose;
+    const float* pose = s + L.body_pose;
     float* q = s + L.q;
     float* v = s + L.v;
     const float* vf = s + L.vf;
-    float* S = s + L.dof_S;
+    const float* Jax = s + L.dof_J;
     float* slots = s + L.manifolds;
     float* C = s + L.contacts;
-    float* G = s + L.G;
-    float* R = s + L.R;
-    float* Lm = s + L.L;
-    const int rs = L.rstride;
-    const int ma = M.max_anc;
-    const float* Jax = s + L.dof_J;
+    float* Y = s + L.G;     // G rows, factored in place into Y = L^-T G^T
+    float* Lm = s + L.L;    // packed lower factor rows
+    float* z = s + L.z;     // L-space image of the accumulated impulses
+    const int ma = T.max_anc;
 
     // Speculative margins of articulated colliders (Collision.metal:5882-5915):
     // h * sum|v_free| * max(sweep radius, 0.25), capped by h * speed envelope.
     float gs = 0.0f;
     for (int d = lane; d < nv; d += 32) gs += fabsf(vf[d]);
     gs = warp_sum(gs);
-    // Per-shape margins live in the tau array's tail? Use registers: lane s holds margin of shape s.
-    float my_margin = 0.0f;
-    if (lane < M.ns && M.shape_body[lane] >= 0 && M.shape_type[lane] != MR_SHAPE_PLANE) {
-        const float env = fminf(h * gs * fmaxf(M.shape_offsets[lane].z, 0.25f), h * M.speed_envelope);
-        my_margin = M.speculative_scale * env;
+    float* margins = s + L.margins;
+    if (lane < M.ns) {
+        float m = 0.0f;
+        if (M.shape_body[lane] >= 0 && M.shape_type[lane] != MR_SHAPE_PLANE)
+            m = M.speculative_scale * fminf(h * gs * fmaxf(M.shape_offsets[lane].z, 0.25f), h * M.speed_envelope);
+        margins[lane] = m;
     }
-    // Stage margins in shared memory (R area is free at this point).
-    float* margins = R;
-    if (lane < M.ns) margins[lane] = my_margin;
     __syncwarp();
 
     // Narrowphase + manifolds: lane per pair.
     int npoints = 0, nraw = 0;
     bool cand = false;
     bool pair_fail = false;
+    // Scratch of each pair: exclusive prefix of the per-class sizes.
+    const int my_words = lane < M.np ? pair_scratch_words(pair_max_raw(M.pair_class[lane])) : 0;
+    int scratch_end = my_words;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, scratch_end, o);
+        if (lane >= o) scratch_end += t;
+    }
     if (lane < M.np) {
-        npoints = pair_manifold(M, pose, margins, lane, slots + lane * kManifoldWords, nraw, cand);
+        npoints = pair_manifold(M, pose, margins, lane, slots + lane * kManifoldWords, s + L.narrow + scratch_end - my_words,
+                                nraw, cand);
         if (npoints < 0) { pair_fail = true; npoints = 0; }
     }
     const unsigned fail_mask = __ballot_sync(0xffffffffu, pair_fail);
@@ -1001,7 +1110,9 @@ __device__ bool contact_substep(const Warp& w, bool final_substep, int velocity_
     const int base = incl - npoints;
     {
         const unsigned mcount = __popc(__ballot_sync(0xffffffffu, npoints > 0));
-        const int raw_total = static_cast<int>(warp_sum(static_cast<float>(nraw)));
+        int raw_total = nraw;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) raw_total += __shfl_xor_sync(0xffffffffu, raw_total, o);
         const unsigned cand_count = __popc(__ballot_sync(0xffffffffu, cand));
         if (lane == 0) {
             misc[kMiscContactCount] = as_float(total);
@@ -1016,8 +1127,8 @@ __device__ bool contact_substep(const Warp& w, bool final_substep, int velocity_
         return false;
     }
 
-    // Contact records (mr_world_scatter_manifold_ir): one lane per pair
-    // emits its points.
+    // Contact records (mr_world_scatter_manifold_ir): the pair lane emits
+    // its points in manifold order.
     if (lane < M.np && npoints > 0) {
         const int pair = lane;
         const float* slot = slots + pair * kManifoldWords;
@@ -1067,23 +1178,23 @@ __device__ bool contact_substep(const Warp& w, bool final_substep, int velocity_
             c[kCwLambda + 0] = op[9];
             c[kCwLambda + 1] = op[10];
             c[kCwLambda + 2] = op[11];
-            // Rows: target velocity (speculative gap), regularisation.
             c[kCwTarget + 0] = sep > 0.0f ? -sep / h : 0.0f;
             c[kCwTarget + 1] = 0.0f;
             c[kCwTarget + 2] = 0.0f;
             c[kCwReg + 0] = fmaxf(compliance / (h * h) + dissipation / h, 0.0f);
             c[kCwReg + 1] = 0.0f;
             c[kCwReg + 2] = 0.0f;
-            c[kCwMuU] = mu_s;   // static coefficient; replaced by the slip test below
-            c[kCwMuV] = mu_d;   // dynamic coefficient (temporarily)
+            c[kCwMuU] = mu_s;
+            c[kCwMuV] = mu_d;
             c[kCwRelax] = restitution;
             c[kCwDelta + 0] = rthreshold;
         }
     }
     __syncwarp();
 
-    // Jacobian rows G (sparse over the body's ancestor DoFs) and evaluation
-    // of the ConstraintIR rows at v_free (MetalWorldContact.metal:3580-3990).
+    // Jacobian rows G over the body's ancestor DoFs (positions in anc[b])
+    // and evaluation of the ConstraintIR rows at v_free
+    // (MetalWorldContact.metal:3580-3990).
     if (lane < total) {
         float* c = C + lane * kContactWords;
         const int b = as_int(c[kCwBody]);
@@ -1091,23 +1202,24 @@ __device__ bool contact_substep(const Warp& w, bool final_substep, int velocity_
         const float sign = (flags & 256) ? 1.0f : -1.0f;
         const float3 x = ld3(c + kCwPoint);
         const float3 dirs[3] = {ld3(c + kCwNormal), ld3(c + kCwTangent), ld3(c + kCwBitangent)};
-        const int na = M.anc_count[b];
-        float* g = G + lane * 3 * ma;
+        const int na = T.anc_count[b];
+        float* g = Y + lane * 3 * ma;
         float rel[3] = {0.0f, 0.0f, 0.0f};
         for (int k = 0; k < na; ++k) {
-            const int d = M.anc_dofs[b * kMaxDofs + k];
+            const int d = T.anc[b][k];
             // Point-Jacobian column: a x (x - o) for rotations, a for translations.
             const float* jd = Jax + d * 8;
             const float3 ax = f3(jd[0], jd[1], jd[2]);
             const float3 jc = jd[6] != 0.0f ? ax : cross3(ax, x - f3(jd[3], jd[4], jd[5]));
+            const float vk = vf[d];
+#pragma unroll
             for (int r = 0; r < 3; ++r) {
                 const float gv = sign * dot3(dirs[r], jc);
                 g[r * ma + k] = gv;
-                rel[r] = fmaf(gv, vf[d], rel[r]);
+                rel[r] = fmaf(gv, vk, rel[r]);
             }
         }
-        for (int k = na; k < ma; ++k)
-            for (int r = 0; r < 3; ++r) g[r * ma + k] = 0.0f;
+        for (int r = 0; r < 3; ++r) c[kCwUfree + r] = rel[r];
         // Normal row: critically damped stabilisation clamped to the maximum
         // depenetration speed, plus restitution on a new impact.
         const float sep = c[kCwSeparation];
@@ -1116,7 +1228,7 @@ __device__ bool contact_substep(const Warp& w, bool final_substep, int velocity_
         const float ratio = h / tau_c;
         const float den = 1.0f + 2.0f * 1.0f * ratio + ratio * ratio;
         float stab = -h * err / (tau_c * tau_c * den);
-        stab = fminf(fmaxf(fmaxf(stab, 0.0f), 0.0f), M.max_depenetration);
+        stab = fminf(fmaxf(stab, 0.0f), M.max_depenetration);
         const float restitution = c[kCwRelax];
         const float rthreshold = c[kCwDelta + 0];
         if (flags & 1) {
@@ -1125,130 +1237,86 @@ __device__ bool contact_substep(const Warp& w, bool final_substep, int velocity_
         }
         c[kCwTarget + 0] += stab;
         const float slip = sqrtf(rel[1] * rel[1] + rel[2] * rel[2]);
-        const bool stat = slip <= fmaxf(1.0e-3f, 1.0e-3f);
-        const float mu = stat ? c[kCwMuU] : c[kCwMuV];
+        const float mu = slip <= 1.0e-3f ? c[kCwMuU] : c[kCwMuV];
         c[kCwMuU] = mu;
         c[kCwMuV] = mu;
         if (!isfinite(c[kCwTarget + 0]) || !isfinite(c[kCwReg + 0])) set_status(misc, MR_STEP_NONFINITE_RESULT, static_cast<unsigned>(lane));
     }
-    __syncwarp();
-    if (as_int(misc[kMiscStatus]) != MR_STEP_SUCCESS) return false;
+    if (!warp_ok(misc)) return false;
 
-    float* vv = v;  // solver velocity
-    for (int d = lane; d < nv; d += 32) vv[d] = vf[d];
+    for (int d = lane; d < nv; d += 32) v[d] = vf[d];
     if (total > 0) {
         if (lane == 0) misc[kMiscIslands] = as_float(max(as_int(misc[kMiscIslands]), 1));
-        // Composite rigid-body inertias, each about its own body's COM:
-        // rebuilt into the ABA inertia area, then children shifted into
-        // their parent's frame and pulled level by level (deterministic).
-        float* IC = s + L.body_IA;
-        const float* Rr = s + L.body_r;
-        if (lane < M.nb) {
-            float Iw[3][3];
-            body_inertia(M, lane, ld4(pose + lane * 8 + 4), IC + lane * 21, Iw);
-        }
-        __syncwarp();
-        for (int l = M.n_levels - 1; l >= -1; --l) {
-            const int off = l >= 0 ? M.level_offsets[l] : 0;
-            const int cnt = l >= 0 ? M.level_offsets[l + 1] - off : 1;
-            if (lane < cnt) {
-                const int b = l >= 0 ? M.level_bodies[off + lane] : 0;
-                float* I6 = IC + b * 21;
-                for (int k = M.child_offsets[b]; k < M.child_offsets[b + 1]; ++k) {
-                    const int c = M.children[k];
-                    float shifted[21];
-                    shift_inertia(IC + c * 21, ld3(Rr + c * 4), shifted);
-                    for (int e = 0; e < 21; ++e) I6[e] += shifted[e];
-                }
-            }
-            __syncwarp();
-        }
-        // Mass matrix (packed lower, tree DoF order): F = IC_body(i) S_i in
-        // body(i)'s frame, moved to each ancestor DoF's body frame,
-        // M_ij = S_j . F.  Entries of unrelated DoFs stay zero.
-        for (int i = lane; i < nv; i += 32) {
-            float* row = Lm + i * (i + 1) / 2;
-            for (int j = 0; j <= i; ++j) row[j] = 0.0f;
-            float F[6];
-            const int bi = M.dof_body[i];
-            sym6_mul(IC + bi * 21, S + i * 6, F);
-            const float3 ci = ld3(pose + bi * 8);
-            const float3 fl = f3(F[3], F[4], F[5]);
-            const float3 fa = f3(F[0], F[1], F[2]);
-            for (int j = i; j >= 0; j = M.dof_parent[j]) {
-                const float3 cj = ld3(pose + M.dof_body[j] * 8);
-                const float3 n = fa + cross3(ci - cj, fl);
-                const float* sj = S + j * 6;
-                row[j] = sj[0] * n.x + sj[1] * n.y + sj[2] * n.z + sj[3] * fl.x + sj[4] * fl.y + sj[5] * fl.z;
-            }
-            row[i] += M.armature_eff[i];
-        }
-        __syncwarp();
-        // LTL factorisation H = L^T L exploiting the tree sparsity
-        // (Featherstone, Rigid Body Dynamics Algorithms, sec. 6.5).
-        for (int k = nv - 1; k >= 0; --k) {
+        // Joint rows of the factor H = L^T L from this substep's ABA pivots
+        // (rows 0-5 of a floating root were stored by the ABA): eliminating a
+        // DoF's descendants leaves the articulated inertia of its body, so
+        // L_kk = sqrt(D_k) and L_kj = U_k . S_j(c_b) / L_kk for the ancestor
+        // DoFs j, with S_j moved to body b's COM.
+        if (lane < T.nb && lane > 0 && bc.dof >= 0) {
+            const int k = bc.dof;
             float* rowk = Lm + k * (k + 1) / 2;
-            if (lane == 0) {
-                const float dkk = rowk[k];
-                if (!(dkk > kAbsolutePivotFloor) || !isfinite(dkk)) set_status(misc, MR_STEP_FACTORIZATION_FAILED, static_cast<unsigned>(k));
-                rowk[k] = sqrtf(fmaxf(dkk, kAbsolutePivotFloor));
-            }
-            __syncwarp();
-            const float lkk = rowk[k];
-            const int* ancs = M.anc_dofs + M.dof_body[k] * kMaxDofs;
-            const int nanc = M.dof_anc_count[k];
-            for (int t = lane; t < nanc; t += 32) rowk[ancs[t]] /= lkk;
-            __syncwarp();
-            for (int t = lane; t < nanc; t += 32) {
-                const int i = ancs[t];
-                const float lki = rowk[i];
-                float* rowi = Lm + i * (i + 1) / 2;
-                for (int u = 0; u <= t; ++u) rowi[ancs[u]] -= lki * rowk[ancs[u]];
-            }
-            __syncwarp();
-        }
-        if (as_int(misc[kMiscStatus]) != MR_STEP_SUCCESS) return false;
-        // Response columns R = H^-1 G^T: one lane per column.
-        const int ncol = 3 * total;
-        for (int col = lane; col < ncol; col += 32) {
-            const int c = col / 3, r = col % 3;
-            float* x = R + col * rs;
-            for (int d = 0; d < nv; ++d) x[d] = 0.0f;
-            const int b = as_int(C[c * kContactWords + kCwBody]);
-            const int na = M.anc_count[b];
-            const float* g = G + c * 3 * ma + r * ma;
-            for (int k = 0; k < na; ++k) x[M.anc_dofs[b * kMaxDofs + k]] = g[k];
-            // L^T y = b
-            for (int k = nv - 1; k >= 0; --k) {
-                const float* rowk = Lm + k * (k + 1) / 2;
-                const float yk = x[k] / rowk[k];
-                x[k] = yk;
-                for (int i = M.dof_parent[k]; i >= 0; i = M.dof_parent[i]) x[i] -= rowk[i] * yk;
-            }
-            // L x = y
-            for (int k = 0; k < nv; ++k) {
-                const float* rowk = Lm + k * (k + 1) / 2;
-                float acc = x[k];
-                for (int i = M.dof_parent[k]; i >= 0; i = M.dof_parent[i]) acc -= rowk[i] * x[i];
-                x[k] = acc / rowk[k];
+            const float lkk = sqrtf(st.D);
+            const float inv = 1.0f / lkk;
+            rowk[k] = lkk;
+            const int na = T.dof_depth[k];
+            for (int t = 0; t < na; ++t) {
+                const int j = T.anc[lane][t];
+                const float* jd = Jax + j * 8;
+                const float3 ax = f3(jd[0], jd[1], jd[2]);
+                float val;
+                if (jd[6] != 0.0f) {
+                    val = st.U[3] * ax.x + st.U[4] * ax.y + st.U[5] * ax.z;
+                } else {
+                    const float3 lin = cross3(ax, st.c - f3(jd[3], jd[4], jd[5]));
+                    val = st.U[0] * ax.x + st.U[1] * ax.y + st.U[2] * ax.z + st.U[3] * lin.x + st.U[4] * lin.y + st.U[5] * lin.z;
+                }
+                rowk[j] = val * inv;
             }
         }
         __syncwarp();
-        // Preconditioners, relaxation and warm start (lane per contact).
+        // Y = L^-T G^T per contact row, in place over the ancestor positions.
+        const int nrows = 3 * total;
+        for (int row = lane; row < nrows; row += 32) {
+            const int c = row / 3, r = row - 3 * (row / 3);
+            const int b = as_int(C[c * kContactWords + kCwBody]);
+            const int na = T.anc_count[b];
+            float* y = Y + c * 3 * ma + r * ma;
+            for (int t = na - 1; t >= 0; --t) {
+                const int k = T.anc[b][t];
+                const float* rowk = Lm + k * (k + 1) / 2;
+                const float yt = y[t] / rowk[k];
+                y[t] = yt;
+                for (int u = 0; u < t; ++u) y[u] -= rowk[T.anc[b][u]] * yt;
+            }
+        }
+        for (int d = lane; d < nv; d += 32) z[d] = 0.0f;
+        __syncwarp();
+        // Preconditioners, relaxation and warm start (lane per contact):
+        // W_cc = Y_c^T Y_c + R, normal row sums over the common ancestor prefix.
         if (lane < total) {
             float* c = C + lane * kContactWords;
             const int b = as_int(c[kCwBody]);
-            const int na = M.anc_count[b];
-            const int* anc = M.anc_dofs + b * kMaxDofs;
-            const float* g = G + lane * 3 * ma;
+            const int na = T.anc_count[b];
+            const float* yc = Y + lane * 3 * ma;
             float Wm[3][3];
             for (int r = 0; r < 3; ++r)
-                for (int cc = 0; cc < 3; ++cc) {
-                    const float* x = R + (lane * 3 + cc) * rs;
+                for (int cc = 0; cc <= r; ++cc) {
                     float acc = 0.0f;
-                    for (int k = 0; k < na; ++k) acc = fmaf(g[r * ma + k], x[anc[k]], acc);
-                    Wm[r][cc] = acc + (r == cc ? c[kCwReg + r] : 0.0f);
+                    for (int t = 0; t < na; ++t) acc = fmaf(yc[r * ma + t], yc[cc * ma + t], acc);
+                    Wm[r][cc] = acc;
+                    Wm[cc][r] = acc;
                 }
+            float rowsum = 0.0f;
+            for (int j = 0; j < total; ++j) {
+                const int bj = as_int(C[j * kContactWords + kCwBody]);
+                const int n = T.lcp[b][bj];
+                const float* yj = Y + j * 3 * ma;
+                float acc = 0.0f;
+                for (int t = 0; t < n; ++t) acc = fmaf(yc[t], yj[t], acc);
+                rowsum += fabsf(acc);
+            }
+            const float diag = fabsf(Wm[0][0]) + c[kCwReg + 0];
+            for (int r = 0; r < 3; ++r) Wm[r][r] += c[kCwReg + r];
             float inv[3][3];
             if (!invert3x3_reg(Wm, inv)) {
                 set_status(misc, MR_STEP_FACTORIZATION_FAILED, static_cast<unsigned>(lane));
@@ -1256,36 +1324,27 @@ __device__ bool contact_substep(const Warp& w, bool final_substep, int velocity_
                 for (int r = 0; r < 3; ++r)
                     for (int cc = 0; cc < 3; ++cc) c[kCwPre + r * 3 + cc] = inv[r][cc];
             }
-            float rowsum = 0.0f, diag = 0.0f;
-            for (int c2 = 0; c2 < total; ++c2) {
-                const float* x = R + (c2 * 3) * rs;
-                float acc = 0.0f;
-                for (int k = 0; k < na; ++k) acc = fmaf(g[k], x[anc[k]], acc);
-                rowsum += fabsf(acc);
-                if (c2 == lane) diag = fabsf(acc) + c[kCwReg + 0];
-            }
             c[kCwRelax] = rowsum > fmaxf(diag, kMatrixFloor) ? fminf(fmaxf(diag / rowsum, 1.0f / 32.0f), 1.0f) : 1.0f;
             const float3 warm = project_cone(ld3(c + kCwLambda), c[kCwMuU], c[kCwMuV]);
             st3(c + kCwLambda, warm);
             st3(c + kCwDelta, warm);
         }
-        __syncwarp();
-        if (as_int(misc[kMiscStatus]) != MR_STEP_SUCCESS) return false;
-        // Jacobi sweeps: lane per contact proposes, lane per DoF applies.
+        if (!warp_ok(misc)) return false;
+        // Jacobi sweeps: lane per contact proposes from u = u_free + Y^T z,
+        // lane per DoF accumulates z += Y delta.  Sweep -1 applies the warm start.
         const int iters = velocity_iterations + (final_substep ? final_iterations : 0);
         for (int it = -1; it < iters; ++it) {
             if (it >= 0 && lane < total) {
                 float* c = C + lane * kContactWords;
                 const int b = as_int(c[kCwBody]);
-                const int na = M.anc_count[b];
-                const int* anc = M.anc_dofs + b * kMaxDofs;
-                const float* g = G + lane * 3 * ma;
-                float u0 = 0.0f, u1 = 0.0f, u2 = 0.0f;
-                for (int k = 0; k < na; ++k) {
-                    const float vk = vv[anc[k]];
-                    u0 = fmaf(g[k], vk, u0);
-                    u1 = fmaf(g[ma + k], vk, u1);
-                    u2 = fmaf(g[2 * ma + k], vk, u2);
+                const int na = T.anc_count[b];
+                const float* yc = Y + lane * 3 * ma;
+                float u0 = c[kCwUfree + 0], u1 = c[kCwUfree + 1], u2 = c[kCwUfree + 2];
+                for (int t = 0; t < na; ++t) {
+                    const float zk = z[T.anc[b][t]];
+                    u0 = fmaf(yc[t], zk, u0);
+                    u1 = fmaf(yc[ma + t], zk, u1);
+                    u2 = fmaf(yc[2 * ma + t], zk, u2);
                 }
                 const float3 prev = ld3(c + kCwLambda);
                 const float r0 = c[kCwTarget + 0] - u0 - c[kCwReg + 0] * prev.x;
@@ -1307,20 +1366,39 @@ __device__ bool contact_substep(const Warp& w, bool final_substep, int velocity_
                 }
             }
             __syncwarp();
-            // it == -1 applies the warm start.
             for (int d = lane; d < nv; d += 32) {
                 float acc = 0.0f;
-                for (int c2 = 0; c2 < total; ++c2) {
-                    const float* dl = C + c2 * kContactWords + kCwDelta;
-                    acc = fmaf(R[(c2 * 3 + 0) * rs + d], dl[0], acc);
-                    acc = fmaf(R[(c2 * 3 + 1) * rs + d], dl[1], acc);
-                    acc = fmaf(R[(c2 * 3 + 2) * rs + d], dl[2], acc);
+                for (int j = 0; j < total; ++j) {
+                    const float* cj = C + j * kContactWords;
+                    const int t = T.pos[as_int(cj[kCwBody])][d];
+                    if (t == kNone) continue;
+                    const float* yj = Y + j * 3 * ma + t;
+                    acc = fmaf(yj[0], cj[kCwDelta + 0], acc);
+                    acc = fmaf(yj[ma], cj[kCwDelta + 1], acc);
+                    acc = fmaf(yj[2 * ma], cj[kCwDelta + 2], acc);
                 }
-                vv[d] += acc;
+                z[d] += acc;
             }
             __syncwarp();
         }
-        if (as_int(misc[kMiscStatus]) != MR_STEP_SUCCESS) return false;
+        if (!warp_ok(misc)) return false;
+        // Velocity change x = L^-1 z by DoF-tree depth (ancestors first).
+        float* x = s + L.qdd;
+        for (int dep = 0; dep < T.n_dof_levels; ++dep) {
+            for (int k = lane; k < nv; k += 32) {
+                if (T.dof_depth[k] != dep) continue;
+                const float* rowk = Lm + k * (k + 1) / 2;
+                const int bk = T.dof_body[k];
+                float acc = z[k];
+                for (int t = 0; t < dep; ++t) {
+                    const int i = T.anc[bk][t];
+                    acc -= rowk[i] * x[i];
+                }
+                x[k] = acc / rowk[k];
+            }
+            __syncwarp();
+        }
+        for (int d = lane; d < nv; d += 32) v[d] += x[d];
         // Impulses back into the manifold points (warm start of the next substep).
         if (lane < total) {
             const float* c = C + lane * kContactWords;
@@ -1336,7 +1414,7 @@ __device__ bool contact_substep(const Warp& w, bool final_substep, int velocity_
     // Joint limits on the post-solve velocity (mr_world_project_joint_limits).
     for (int d = lane; d < nv; d += 32) {
         const unsigned flags = M.dof_flags[d];
-        float vel = vv[d];
+        float vel = v[d];
         if (flags & MR_DOF_FLAG_VELOCITY_LIMIT) vel = fminf(fmaxf(vel, -M.v_max[d]), M.v_max[d]);
         const int qi = M.dof_q[d];
         if ((flags & MR_DOF_FLAG_POSITION_LIMIT) && qi >= 0) {
@@ -1344,40 +1422,44 @@ __device__ bool contact_substep(const Warp& w, bool final_substep, int velocity_
             vel = fminf(fmaxf(vel, (M.q_lower[d] - pos) / h), (M.q_upper[d] - pos) / h);
         }
         if (!isfinite(vel)) set_status(misc, MR_STEP_NONFINITE_RESULT, static_cast<unsigned>(d));
-        vv[d] = vel;
+        v[d] = vel;
     }
     __syncwarp();
     // Integration from the substep-start configuration
     // (mr_world_integrate_contact_state; no angle reduction).
     for (int d = lane; d < nv; d += 32) {
         const int qi = M.dof_q[d];
-        if (qi >= 0 && !(M.floating && d < 6)) q[qi] = q[qi] + h * vv[d];
+        if (qi >= 0 && !(M.floating && d < 6)) q[qi] = q[qi] + h * v[d];
     }
     if (M.floating && lane == 0) {
-        q[0] += h * vv[0];
-        q[1] += h * vv[1];
-        q[2] += h * vv[2];
-        const float4 inc = so3_increment(h * f3(vv[3], vv[4], vv[5]), false);
-        const float4 src = make_float4(q[3], q[4], q[5], q[6]);
-        const float4 prod = qmul(inc, src);
-        float4 out;
+        q[0] += h * v[0];
+        q[1] += h * v[1];
+        q[2] += h * v[2];
+        const float4 inc = so3_increment(h * f3(v[3], v[4], v[5]), false);
+        const float4 prod = qmul(inc, make_float4(q[3], q[4], q[5], q[6]));
         if (!finite4(prod) || !(qdot(prod, prod) > 1.0e-12f)) {
             set_status(misc, MR_STEP_NONFINITE_RESULT, 3u);
         } else {
-            out = qscale(prod, rsqrtf(qdot(prod, prod)));
+            const float4 out = qscale(prod, rsqrtf(qdot(prod, prod)));
             q[3] = out.x; q[4] = out.y; q[5] = out.z; q[6] = out.w;
         }
     }
     __syncwarp();
     for (int i = lane; i < M.nq; i += 32)
         if (!isfinite(q[i])) set_status(misc, MR_STEP_NONFINITE_RESULT, static_cast<unsigned>(i));
-    __syncwarp();
-    return as_int(misc[kMiscStatus]) == MR_STEP_SUCCESS;
+    return warp_ok(misc);
 }
 
 template <bool kContact>
 __global__ void __launch_bounds__(128) control_step_kernel(StepParams p, WarpLayout layout, int warps_per_block) {
     extern __shared__ float4 smem4[];
+    // Topology tables: one copy per CTA.
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(&p.model->tables);
+        uint4* dst = reinterpret_cast<uint4*>(smem4);
+        for (int i = threadIdx.x; i < static_cast<int>(sizeof(DeviceTables) / 16); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int env = blockIdx.x * warps_per_block + warp;
@@ -1385,7 +1467,8 @@ __global__ void __launch_bounds__(128) control_step_kernel(StepParams p, WarpLay
     const DeviceModel& M = *p.model;
     Warp w;
     w.lane = lane;
-    w.s = reinterpret_cast<float*>(smem4) + warp * layout.total;
+    w.T = reinterpret_cast<const DeviceTables*>(smem4);
+    w.s = reinterpret_cast<float*>(smem4) + sizeof(DeviceTables) / sizeof(float) + warp * layout.total;
     w.L = &layout;
     w.M = p.model;
     float* s = w.s;
@@ -1407,7 +1490,7 @@ __global__ void __launch_bounds__(128) control_step_kernel(StepParams p, WarpLay
         s[layout.vc + i] = x;
         s[layout.tgt + i] = 0.0f;
     }
-    if (lane < 32) misc[lane] = 0.0f;
+    misc[lane] = 0.0f;
     __syncwarp();
     for (int a = lane; a < M.action_count; a += 32)
         s[layout.tgt + M.action_dof[a]] = p.actions[static_cast<size_t>(env) * M.action_count + a];
@@ -1423,23 +1506,23 @@ __global__ void __launch_bounds__(128) control_step_kernel(StepParams p, WarpLay
         }
     }
     const float friction_scale = kContact ? p.friction_scale[env] : 1.0f;
+    BodyConst bc;
+    if (lane < M.nb) load_body(M, lane, bc);
+    BodyState st;
     __syncwarp();
 
-    int failing_substep = -1;
     for (int sub = 0; sub < p.substeps; ++sub) {
         compute_drives(w);
         __syncwarp();
-        bool ok = aba(w);
+        bool ok = aba(w, bc, st, kContact ? s + layout.L : nullptr);
         if (ok) {
             if (kContact)
-                ok = contact_substep(w, sub + 1 == p.substeps, p.velocity_iterations, p.final_velocity_iterations, friction_scale);
+                ok = contact_substep(w, bc, st, sub + 1 == p.substeps, p.velocity_iterations, p.final_velocity_iterations,
+                                     friction_scale);
             else
                 ok = integrate_free(w);
         }
-        if (!ok) {
-            failing_substep = sub;
-            break;
-        }
+        if (!ok) break;
     }
     const unsigned code = static_cast<unsigned>(as_int(misc[kMiscStatus]));
     const bool success = code == MR_STEP_SUCCESS;
@@ -1485,23 +1568,30 @@ __global__ void __launch_bounds__(128) control_step_kernel(StepParams p, WarpLay
             atomicMax(p.stats + kStatMaxCandidatePairs, static_cast<unsigned>(as_int(misc[kMiscCandidatePairs])));
             atomicMax(p.stats + kStatMaxIslands, static_cast<unsigned>(as_int(misc[kMiscIslands])));
         }
-        (void)failing_substep;
     }
 }
 
 }  // namespace
 
+size_t control_step_table_bytes() { return sizeof(DeviceTables); }
+
 // Host launcher: one control step of `env_count` environments.
 cudaError_t launch_control_step(const StepParams& p, const WarpLayout& layout, bool contact, int warps_per_block,
                                 cudaStream_t stream) {
     const int blocks = (p.env_count + warps_per_block - 1) / warps_per_block;
-    const size_t smem = static_cast<size_t>(layout.total) * sizeof(float) * warps_per_block;
+    const size_t smem = sizeof(DeviceTables) + static_cast<size_t>(layout.total) * sizeof(float) * warps_per_block;
     if (contact) {
         control_step_kernel<true><<<blocks, 32 * warps_per_block, smem, stream>>>(p, layout, warps_per_block);
     } else {
         control_step_kernel<false><<<blocks, 32 * warps_per_block, smem, stream>>>(p, layout, warps_per_block);
     }
     return cudaGetLastError();
+}
+
+cudaError_t control_step_occupancy(bool contact, int warps_per_block, size_t smem, int* blocks_per_sm) {
+    if (contact)
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, control_step_kernel<true>, 32 * warps_per_block, smem);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, control_step_kernel<false>, 32 * warps_per_block, smem);
 }
 
 cudaError_t configure_control_step_kernels(size_t max_dynamic_smem) {

@@ -27,6 +27,7 @@ static const double kPad = 0.00000762939453125;
  * "band" decisions: FP32 rounding on the device may legitimately take the
  * other branch.  Counted per control step (OracleTrace.band_decisions). */
 static const double kBand = 1.0e-5;
+static const double kTieRelative = 1.0e-5;  /* manifold reduction ties */
 static __thread uint32_t g_band;
 static __thread double g_margin;  /* smallest |value - threshold| over the step's decisions */
 #define BAND(value, threshold)                                                       \
@@ -885,8 +886,17 @@ static int pair_manifold(const OracleWorld* o, const Kin* k, const double* margi
                     }
                 }
                 const unsigned long long f = ckey(&c[i]);
-                if (best >= 0 && fabs(score - best_score) > 1.0e-12 && fabs(score - best_score) <= kBand * kBand) g_band++;
-                if (score > best_score + 1.0e-12 || (fabs(score - best_score) <= 1.0e-12 && f < best_f)) {
+                /* Scores within a relative 1e-5 are ties (smaller feature key
+                 * wins): box faces make exact ties structural, and the
+                 * reference's absolute tolerances (Collision.cpp:2531-2544,
+                 * Collision.metal:5247) leave them to rounding.  A gap within
+                 * 10 % of the tie tolerance is a band decision. */
+                const double tol = fmax(1.0e-12, kTieRelative * fmax(fabs(score), fabs(best_score)));
+                if (best >= 0) {
+                    const double gap = fabs(fabs(score - best_score) - tol);
+                    if (gap <= 0.1 * tol) g_band++;
+                }
+                if (score > best_score + tol || (fabs(score - best_score) <= tol && f < best_f)) {
                     best = i; best_score = score; best_f = f;
                 }
             }
