@@ -447,10 +447,11 @@ MR_API int mr_task_rollout_copy_final_scene_states(
  * (e.g. torch CUDA tensors).  `device_actions` [step][env][action] and the
  * optional `device_reset_masks` [step][env] live on the rollout's device;
  * `device_observations` [step][env][nq+nv] and `device_status_codes`
- * [step][env] may be null.  Work is ordered on `cuda_stream` (0 = the
- * rollout's own stream).  With `advance` non-null the call waits and fills
- * the same counters as mr_task_rollout_advance; with null it returns after
- * enqueueing. */
+ * [step][env] may be null.  The control steps run after all work already
+ * enqueued on `cuda_stream` (a cudaStream_t; 0 = the legacy default
+ * stream), and work enqueued on it afterwards runs after them.  With
+ * `advance` non-null the call waits and fills the same counters as
+ * mr_task_rollout_advance; with null it returns after enqueueing. */
 MR_API int mr_task_rollout_advance_device(
     MRTaskRolloutHandle* handle,
     const float* device_actions,
