@@ -39,6 +39,7 @@ struct alignas(16) DeviceTables {
     std::uint8_t anc[kMaxBodies][kMaxDofs];  // ancestor DoFs of a body, root first
     std::uint8_t pos[kMaxBodies][kMaxDofs];  // position of DoF d in anc[b], or 255
     std::uint8_t lcp[kMaxBodies][kMaxBodies];// common prefix length of anc[a], anc[b]
+    std::uint8_t level_children[kMaxBodies]; // most children of a body at each depth
     std::uint8_t pad[7];
 };
 

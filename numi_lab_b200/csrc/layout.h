@@ -8,7 +8,7 @@
 namespace numi {
 
 // Words of one solver contact record in shared memory.
-constexpr int kContactWords = 44;
+constexpr int kContactWords = 45;  // 44 used; odd stride keeps lane-per-contact access conflict free
 enum ContactWord : int {
     kCwPoint = 0,      // world contact point (3)
     kCwSeparation = 3,
@@ -29,9 +29,14 @@ enum ContactWord : int {
     kCwUfree = 40      // contact-frame relative velocity at v_free (3)
 };
 
+// Shared-memory strides (odd, so lane-per-body / per-DoF / per-pair access
+// hits distinct banks).
+constexpr int kPoseStride = 7;                    // COM position (3), orientation xyzw (4)
+constexpr int kJStride = 7;                       // joint axis (3), origin (3), translation flag
+constexpr int kSlotStride = kManifoldWords + 1;   // manifold slot
+
 struct WarpLayout {
-    int body_pose, body_V, body_IA, body_PA, body_A;
-    int dof_S, dof_J;
+    int body_pose, dof_J;
     int q, qc, v, vc, vf, tau, qdd, tgt;
     int misc;
     int manifolds, contacts, G, L, z, margins;
@@ -57,13 +62,8 @@ __host__ __device__ inline WarpLayout make_layout(int nb, int nv, int nq, int np
     WarpLayout L{};
     int o = 0;
     auto take = [&o](int words) { const int at = o; o += align4(words); return at; };
-    L.body_pose = take(nb * 8);
-    L.body_V = take(nb * 6);
-    L.body_IA = take(nb * 21);
-    L.body_PA = take(nb * 6);
-    L.body_A = take(nb * 6);
-    L.dof_S = take(nv * 6);
-    L.dof_J = take(nv * 8);
+    L.body_pose = take(nb * kPoseStride);
+    L.dof_J = take(nv * kJStride);
     L.q = take(nq);
     L.qc = take(nq);
     L.v = take(nv);
@@ -76,12 +76,12 @@ __host__ __device__ inline WarpLayout make_layout(int nb, int nv, int nq, int np
     L.z = take(nv);
     L.margins = take(32);
     if (contact) {
-        L.manifolds = take(np * kManifoldWords);
+        L.manifolds = take(np * kSlotStride);
         L.L = take(nv * (nv + 1) / 2);
         // Contact records and Jacobian rows are written only after the
         // narrowphase has finished with its scratch, so the three share words.
         L.contacts = take(ncap * kContactWords);
-        const int rows = align4(ncap * 3 * max_anc);
+        const int rows = align4(ncap * 3 * (max_anc | 1));
         const int need = align4(narrow_words) - align4(ncap * kContactWords);
         L.G = take(rows > need ? rows : need);
         L.narrow = L.contacts;

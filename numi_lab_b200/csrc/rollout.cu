@@ -254,6 +254,11 @@ numi::DeviceModel pack_model(const numi::CompiledModel& m, float h) {
             }
         }
         t.child_offsets[nb] = static_cast<std::uint8_t>(d.child_offsets[nb]);
+        std::memset(t.level_children, 0, sizeof(t.level_children));
+        for (int b = 0; b < nb; ++b) {
+            const int children = d.child_offsets[b + 1] - d.child_offsets[b];
+            t.level_children[depth[b]] = static_cast<std::uint8_t>(std::max<int>(t.level_children[depth[b]], children));
+        }
         for (int a = 0; a < nb; ++a)
             for (int b = 0; b < nb; ++b) {
                 std::uint32_t n = 0;

@@ -227,10 +227,19 @@ __device__ __forceinline__ void body_inertia(const BodyConst& bc, float4 qb, flo
 
 // ---------------------------------------------------------------------------
 // Forward kinematics (ArticulatedABA.metal:735-905): lane b computes body b
-// at its tree level from the parent's pose / twist in shared memory.
-// Writes pose and twist to shared memory, joint axis / origin and subspace of
-// the body's DoF to the per-DoF tables; keeps bias and offset in registers.
+// at its tree level from its parent's pose and twist, read from the parent
+// lane's registers by warp shuffle.  Leaves the pose in shared memory (for
+// collision) and the joint axis / origin of the body's DoF in the Jacobian
+// table; bias accelerations, offset and subspace stay in registers.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ float3 shfl3(float3 a, int src) {
+    return f3(__shfl_sync(0xffffffffu, a.x, src), __shfl_sync(0xffffffffu, a.y, src), __shfl_sync(0xffffffffu, a.z, src));
+}
+__device__ __forceinline__ float4 shfl4(float4 a, int src) {
+    return make_float4(__shfl_sync(0xffffffffu, a.x, src), __shfl_sync(0xffffffffu, a.y, src),
+                       __shfl_sync(0xffffffffu, a.z, src), __shfl_sync(0xffffffffu, a.w, src));
+}
+
 __device__ void kinematics(const Warp& w, const BodyConst& bc, BodyState& st) {
     const DeviceTables& T = *w.T;
     const WarpLayout& L = *w.L;
@@ -239,61 +248,45 @@ __device__ void kinematics(const Warp& w, const BodyConst& bc, BodyState& st) {
     const float* q = s + L.q;
     const float* v = s + L.v;
     float* pose = s + L.body_pose;
-    float* vel = s + L.body_V;
-    float* S = s + L.dof_S;
     float* J = s + L.dof_J;
     const int b = w.lane;
     const bool mine = b < T.nb;
     const int my_depth = mine ? T.depth[b] : -1;
+    const int par = (mine && b > 0) ? T.parent[b] : b;
 
-    if (b == 0) {
-        if (T.floating) {
-            float4 rq;
-            const float3 c0 = f3(q[0], q[1], q[2]);
-            if (!finite3(c0) || !qnormalize(make_float4(q[3], q[4], q[5], q[6]), rq, true)) {
-                set_status(misc, MR_STEP_NONFINITE_INPUT, 0u);
-                rq = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
-            }
-            st.c = c0;
-            st.qr = rq;
-            st.w = f3(v[3], v[4], v[5]);
-            st.v = f3(v[0], v[1], v[2]);
-        } else {
-            st.c = f3(0.0f, 0.0f, 0.0f);
-            st.qr = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
-            st.w = st.v = f3(0.0f, 0.0f, 0.0f);
+    st.c = f3(0.0f, 0.0f, 0.0f);
+    st.qr = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+    st.w = st.v = st.ba = st.bl = st.r = f3(0.0f, 0.0f, 0.0f);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) st.s[i] = 0.0f;
+    if (b == 0 && T.floating) {
+        float4 rq;
+        const float3 c0 = f3(q[0], q[1], q[2]);
+        if (!finite3(c0) || !qnormalize(make_float4(q[3], q[4], q[5], q[6]), rq, true)) {
+            set_status(misc, MR_STEP_NONFINITE_INPUT, 0u);
+            rq = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
         }
-        st.ba = st.bl = st.r = f3(0.0f, 0.0f, 0.0f);
-        for (int i = 0; i < 6; ++i) st.s[i] = 0.0f;
-        st4(pose, make_float4(st.c.x, st.c.y, st.c.z, 0.0f));
-        st4(pose + 4, st.qr);
-        st3(vel, st.w);
-        st3(vel + 3, st.v);
+        st.c = c0;
+        st.qr = rq;
+        st.w = f3(v[3], v[4], v[5]);
+        st.v = f3(v[0], v[1], v[2]);
     }
-    __syncwarp();
     if (T.floating && b < 6) {
-        // Root DoFs: lin k -> (0, e_k), ang k -> (e_k, 0) about the root COM;
-        // Jacobian: translational axes e_k, rotations about the root COM.
-        float* Sd = S + b * 6;
-        float* Jd = J + b * 8;
-        for (int i = 0; i < 6; ++i) Sd[i] = 0.0f;
-        if (b < 3) Sd[3 + b] = 1.0f;
-        else Sd[b - 3] = 1.0f;
+        // Root DoFs: translations along e_k, rotations about the root COM.
+        float* Jd = J + b * kJStride;
         const int k = b < 3 ? b : b - 3;
         Jd[0] = k == 0 ? 1.0f : 0.0f;
         Jd[1] = k == 1 ? 1.0f : 0.0f;
         Jd[2] = k == 2 ? 1.0f : 0.0f;
-        Jd[3] = pose[0]; Jd[4] = pose[1]; Jd[5] = pose[2];
+        Jd[3] = q[0]; Jd[4] = q[1]; Jd[5] = q[2];
         Jd[6] = b < 3 ? 1.0f : 0.0f;
-        Jd[7] = 0.0f;
     }
     for (int l = 1; l <= T.n_levels; ++l) {
+        const float3 cp = shfl3(st.c, par);
+        const float4 qp = shfl4(st.qr, par);
+        const float3 wp = shfl3(st.w, par);
+        const float3 vp = shfl3(st.v, par);
         if (my_depth == l) {
-            const int p = bc.parent;
-            const float3 cp = ld3(pose + p * 8);
-            const float4 qp = ld4(pose + p * 8 + 4);
-            const float3 wp = ld3(vel + p * 6);
-            const float3 vp = ld3(vel + p * 6 + 3);
             const float4 pj = qmul(qp, bc.prot);
             float4 motion = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
             float qj = 0.0f, qdj = 0.0f;
@@ -334,34 +327,38 @@ __device__ void kinematics(const Warp& w, const BodyConst& bc, BodyState& st) {
             st.r = cb - cp;
             st.s[0] = ma.x; st.s[1] = ma.y; st.s[2] = ma.z;
             st.s[3] = ml.x; st.s[4] = ml.y; st.s[5] = ml.z;
-            st4(pose + b * 8, make_float4(cb.x, cb.y, cb.z, 0.0f));
-            st4(pose + b * 8 + 4, qb);
-            st3(vel + b * 6, wb);
-            st3(vel + b * 6 + 3, vb);
             if (has) {
-                float* Sd = S + bc.dof * 6;
-                for (int i = 0; i < 6; ++i) Sd[i] = st.s[i];
-                float* Jd = J + bc.dof * 8;
+                float* Jd = J + bc.dof * kJStride;
                 Jd[0] = ja.x; Jd[1] = ja.y; Jd[2] = ja.z;
                 Jd[3] = jp.x; Jd[4] = jp.y; Jd[5] = jp.z;
                 Jd[6] = prismatic ? 1.0f : 0.0f;
-                Jd[7] = 0.0f;
             }
             if (!finite3(cb) || !finite3(wb) || !finite3(vb) || !finite3(st.bl))
                 set_status(misc, MR_STEP_NONFINITE_RESULT, static_cast<unsigned>(b));
         }
-        __syncwarp();
     }
+    if (mine) {
+        float* pb = pose + b * kPoseStride;
+        st3(pb, st.c);
+        st4(pb + 3, st.qr);
+    }
+    __syncwarp();
 }
 
 // ---------------------------------------------------------------------------
 // Articulated-body algorithm (ArticulatedABA.metal:905-1440): per-body COM
 // frames in world axes, classical accelerations, 21-entry inertias.  Each
-// body shifts its articulated inertia and bias into its parent's frame and
-// leaves them in shared memory; a parent pulls its children's contributions
-// in a fixed order, so the sums are deterministic without atomics.
+// body shifts its articulated inertia and bias into its parent's frame in
+// its own registers; the parent pulls its children's contributions by warp
+// shuffle in a fixed order, so the sums are deterministic without atomics.
+// With `factor` non-null (contact worlds) the body lanes also write their
+// rows of the joint-space factor H = L^T L (rows 0-5 of a floating root come
+// from the root's 6x6 factorisation): eliminating a DoF's descendants
+// leaves its body's articulated inertia, so L_kk = sqrt(D_k) and
+// L_kj = U_k . S_j(c_b) / L_kk for the ancestor DoFs j, with S_j moved to
+// body b's COM.
 // ---------------------------------------------------------------------------
-__device__ bool aba(const Warp& w, const BodyConst& bc, BodyState& st, float* root_factor) {
+__device__ bool aba(const Warp& w, const BodyConst& bc, BodyState& st, float* factor) {
     const DeviceModel& M = *w.M;
     const DeviceTables& T = *w.T;
     const WarpLayout& L = *w.L;
@@ -371,9 +368,7 @@ __device__ bool aba(const Warp& w, const BodyConst& bc, BodyState& st, float* ro
     const float* v = s + L.v;
     const float* tau = s + L.tau;
     float* qdd = s + L.qdd;
-    float* IAc = s + L.body_IA;  // shifted contributions for the parent
-    float* PAc = s + L.body_PA;
-    float* A = s + L.body_A;
+    const float* J = s + L.dof_J;
     const int b = w.lane;
     const bool mine = b < T.nb;
 
@@ -387,6 +382,10 @@ __device__ bool aba(const Warp& w, const BodyConst& bc, BodyState& st, float* ro
     if (!warp_ok(misc)) return false;
 
     // Rigid inertia and velocity-dependent bias about the COM.
+#pragma unroll
+    for (int e = 0; e < 21; ++e) st.I[e] = 0.0f;
+#pragma unroll
+    for (int e = 0; e < 6; ++e) st.p[e] = 0.0f;
     if (mine) {
         float Iw[3][3];
         body_inertia(bc, st.qr, st.I, Iw);
@@ -410,128 +409,159 @@ __device__ bool aba(const Warp& w, const BodyConst& bc, BodyState& st, float* ro
             }
         }
     }
-    // Backward sweep, deepest level first; the root (level 0) last.
+    // Backward sweep, deepest level first; the root (level 0) last.  After
+    // its level, a body's I and p hold its contribution in its parent's frame.
     const int my_depth = mine ? T.depth[b] : -1;
+    const int first_child = mine ? T.child_offsets[b] : 0;
+    const int n_children = mine ? T.child_offsets[b + 1] - first_child : 0;
+    float3 acc_ang = f3(0.0f, 0.0f, 0.0f), acc_lin = f3(0.0f, 0.0f, 0.0f);
     for (int l = T.n_levels; l >= 0; --l) {
-        if (my_depth == l) {
-            for (int k = T.child_offsets[b]; k < T.child_offsets[b + 1]; ++k) {
-                const int c = T.children[k];
+        const bool active = my_depth == l;
+        for (int k = 0; k < T.level_children[l]; ++k) {
+            const bool take = active && k < n_children;
+            const int src = take ? T.children[first_child + k] : b;
 #pragma unroll
-                for (int e = 0; e < 21; ++e) st.I[e] += IAc[c * 21 + e];
-#pragma unroll
-                for (int e = 0; e < 6; ++e) st.p[e] += PAc[c * 6 + e];
+            for (int e = 0; e < 21; ++e) {
+                const float x = __shfl_sync(0xffffffffu, st.I[e], src);
+                if (take) st.I[e] += x;
             }
-            if (l > 0) {
-                float prop[6], ic[6];
-                const float cv[6] = {st.ba.x, st.ba.y, st.ba.z, st.bl.x, st.bl.y, st.bl.z};
-                sym6_mul(st.I, cv, ic);
 #pragma unroll
-                for (int e = 0; e < 6; ++e) prop[e] = st.p[e] + ic[e];
-                if (bc.dof >= 0) {
-                    sym6_mul(st.I, st.s, st.U);
-                    const float D = dot6(st.s, st.U) + M.armature_eff[bc.dof];
-                    float maxI = 0.0f;
+            for (int e = 0; e < 6; ++e) {
+                const float x = __shfl_sync(0xffffffffu, st.p[e], src);
+                if (take) st.p[e] += x;
+            }
+        }
+        if (!active) continue;
+        if (l > 0) {
+            float prop[6], ic[6];
+            const float cv[6] = {st.ba.x, st.ba.y, st.ba.z, st.bl.x, st.bl.y, st.bl.z};
+            sym6_mul(st.I, cv, ic);
 #pragma unroll
-                    for (int e = 0; e < 21; ++e) maxI = fmaxf(maxI, fabsf(st.I[e]));
-                    const float floor = fmaxf(kAbsolutePivotFloor, maxI * 6.0f * kFloatEps);
-                    if (!(D > floor) || !isfinite(D)) {
-                        set_status(misc, MR_STEP_FACTORIZATION_FAILED, static_cast<unsigned>(bc.dof));
-                        st.D = 1.0f;
-                        st.u = 0.0f;
-                    } else {
-                        st.D = D;
-                        st.u = tau[bc.dof] - dot6(st.s, prop);
-                        const float invD = 1.0f / D;
+            for (int e = 0; e < 6; ++e) prop[e] = st.p[e] + ic[e];
+            st.D = 1.0f;
+            st.u = 0.0f;
 #pragma unroll
-                        for (int e = 0; e < 6; ++e) prop[e] += st.U[e] * (st.u * invD);
-#pragma unroll
-                        for (int i = 0; i < 6; ++i)
-#pragma unroll
-                            for (int j = 0; j <= i; ++j) st.I[sym6(i, j)] -= st.U[i] * st.U[j] * invD;
-                    }
-                }
-                float shifted[21];
-                shift_inertia(st.I, st.r, shifted);
-#pragma unroll
-                for (int e = 0; e < 21; ++e) IAc[b * 21 + e] = shifted[e];
-                const float3 pf = f3(prop[3], prop[4], prop[5]);
-                const float3 pt = f3(prop[0], prop[1], prop[2]) + cross3(st.r, pf);
-                float* pc = PAc + b * 6;
-                pc[0] = pt.x; pc[1] = pt.y; pc[2] = pt.z; pc[3] = pf.x; pc[4] = pf.y; pc[5] = pf.z;
-            } else if (T.floating) {
-                // Root articulated inertia in DoF order (linear x, y, z, then
-                // angular x, y, z), factored leaves-first as H0 = L0^T L0: these
-                // are rows 0-5 of the joint-space factor H = L^T L, whose joint
-                // rows are L_kk = sqrt(D_k), L_kj = U_k . S_j / L_kk.  Solves
-                // H0 a0 = -pA for the root acceleration.
-                float Lf[21], r[6];
+            for (int e = 0; e < 6; ++e) st.U[e] = 0.0f;
+            if (bc.dof >= 0) {
+                sym6_mul(st.I, st.s, st.U);
+                const float D = dot6(st.s, st.U) + M.armature_eff[bc.dof];
                 float maxI = 0.0f;
 #pragma unroll
                 for (int e = 0; e < 21; ++e) maxI = fmaxf(maxI, fabsf(st.I[e]));
                 const float floor = fmaxf(kAbsolutePivotFloor, maxI * 6.0f * kFloatEps);
+                if (!(D > floor) || !isfinite(D)) {
+                    set_status(misc, MR_STEP_FACTORIZATION_FAILED, static_cast<unsigned>(bc.dof));
+                } else {
+                    st.D = D;
+                    st.u = tau[bc.dof] - dot6(st.s, prop);
+                    const float invD = 1.0f / D;
 #pragma unroll
-                for (int k = 0; k < 6; ++k) {
-                    const int pk = k < 3 ? k + 3 : k - 3;
-                    r[k] = -st.p[pk];
+                    for (int e = 0; e < 6; ++e) prop[e] += st.U[e] * (st.u * invD);
 #pragma unroll
-                    for (int j = 0; j <= k; ++j) Lf[sym6(k, j)] = st.I[sym6(pk, j < 3 ? j + 3 : j - 3)];
+                    for (int i = 0; i < 6; ++i)
+#pragma unroll
+                        for (int j = 0; j <= i; ++j) st.I[sym6(i, j)] -= st.U[i] * st.U[j] * invD;
                 }
-                bool ok = true;
-#pragma unroll
-                for (int k = 5; k >= 0; --k) {
-                    float d = Lf[sym6(k, k)];
-                    if (!(d > floor) || !isfinite(d)) {
-                        ok = false;
-                        d = 1.0f;
-                    }
-                    const float lkk = sqrtf(d);
-                    Lf[sym6(k, k)] = lkk;
-                    const float inv = 1.0f / lkk;
-#pragma unroll
-                    for (int j = 0; j < k; ++j) Lf[sym6(k, j)] *= inv;
-#pragma unroll
-                    for (int i = 0; i < k; ++i)
-#pragma unroll
-                        for (int j = 0; j <= i; ++j) Lf[sym6(i, j)] -= Lf[sym6(k, i)] * Lf[sym6(k, j)];
-                }
-                float y[6], x[6];
-#pragma unroll
-                for (int k = 5; k >= 0; --k) {
-                    float val = r[k];
-#pragma unroll
-                    for (int i = k + 1; i < 6; ++i) val -= Lf[sym6(i, k)] * y[i];
-                    y[k] = val / Lf[sym6(k, k)];
-                }
-#pragma unroll
-                for (int k = 0; k < 6; ++k) {
-                    float val = y[k];
-#pragma unroll
-                    for (int j = 0; j < k; ++j) val -= Lf[sym6(k, j)] * x[j];
-                    x[k] = val / Lf[sym6(k, k)];
-                }
-                if (!ok) set_status(misc, MR_STEP_FACTORIZATION_FAILED, 0u);
-                if (root_factor != nullptr) {
-#pragma unroll
-                    for (int e = 0; e < 21; ++e) root_factor[e] = Lf[e];
-                }
-#pragma unroll
-                for (int k = 0; k < 6; ++k) qdd[k] = x[k];
-                A[0] = x[3]; A[1] = x[4]; A[2] = x[5];
-                A[3] = x[0]; A[4] = x[1]; A[5] = x[2];
-            } else {
-                for (int i = 0; i < 6; ++i) A[i] = 0.0f;
             }
+            float shifted[21];
+            shift_inertia(st.I, st.r, shifted);
+#pragma unroll
+            for (int e = 0; e < 21; ++e) st.I[e] = shifted[e];
+            const float3 pf = f3(prop[3], prop[4], prop[5]);
+            const float3 pt = f3(prop[0], prop[1], prop[2]) + cross3(st.r, pf);
+            st.p[0] = pt.x; st.p[1] = pt.y; st.p[2] = pt.z; st.p[3] = pf.x; st.p[4] = pf.y; st.p[5] = pf.z;
+        } else if (T.floating) {
+            // Root articulated inertia in DoF order (linear x, y, z, then
+            // angular x, y, z), factored leaves-first as H0 = L0^T L0; solves
+            // H0 a0 = -pA for the root acceleration.
+            float Lf[21], r[6];
+            float maxI = 0.0f;
+#pragma unroll
+            for (int e = 0; e < 21; ++e) maxI = fmaxf(maxI, fabsf(st.I[e]));
+            const float floor = fmaxf(kAbsolutePivotFloor, maxI * 6.0f * kFloatEps);
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                const int pk = k < 3 ? k + 3 : k - 3;
+                r[k] = -st.p[pk];
+#pragma unroll
+                for (int j = 0; j <= k; ++j) Lf[sym6(k, j)] = st.I[sym6(pk, j < 3 ? j + 3 : j - 3)];
+            }
+            bool ok = true;
+#pragma unroll
+            for (int k = 5; k >= 0; --k) {
+                float d = Lf[sym6(k, k)];
+                if (!(d > floor) || !isfinite(d)) {
+                    ok = false;
+                    d = 1.0f;
+                }
+                const float lkk = sqrtf(d);
+                Lf[sym6(k, k)] = lkk;
+                const float inv = 1.0f / lkk;
+#pragma unroll
+                for (int j = 0; j < k; ++j) Lf[sym6(k, j)] *= inv;
+#pragma unroll
+                for (int i = 0; i < k; ++i)
+#pragma unroll
+                    for (int j = 0; j <= i; ++j) Lf[sym6(i, j)] -= Lf[sym6(k, i)] * Lf[sym6(k, j)];
+            }
+            float y[6], x[6];
+#pragma unroll
+            for (int k = 5; k >= 0; --k) {
+                float val = r[k];
+#pragma unroll
+                for (int i = k + 1; i < 6; ++i) val -= Lf[sym6(i, k)] * y[i];
+                y[k] = val / Lf[sym6(k, k)];
+            }
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                float val = y[k];
+#pragma unroll
+                for (int j = 0; j < k; ++j) val -= Lf[sym6(k, j)] * x[j];
+                x[k] = val / Lf[sym6(k, k)];
+            }
+            if (!ok) set_status(misc, MR_STEP_FACTORIZATION_FAILED, 0u);
+            if (factor != nullptr) {
+#pragma unroll
+                for (int e = 0; e < 21; ++e) factor[e] = Lf[e];
+            }
+#pragma unroll
+            for (int k = 0; k < 6; ++k) qdd[k] = x[k];
+            acc_ang = f3(x[3], x[4], x[5]);
+            acc_lin = f3(x[0], x[1], x[2]);
         }
-        __syncwarp();
     }
     if (!warp_ok(misc)) return false;
 
-    // Forward acceleration sweep.
+    // Joint rows of the factor.
+    if (factor != nullptr && mine && b > 0 && bc.dof >= 0) {
+        const int k = bc.dof;
+        float* rowk = factor + k * (k + 1) / 2;
+        const float lkk = sqrtf(st.D);
+        const float inv = 1.0f / lkk;
+        rowk[k] = lkk;
+        const int na = T.dof_depth[k];
+        for (int t = 0; t < na; ++t) {
+            const int j = T.anc[b][t];
+            const float* jd = J + j * kJStride;
+            const float3 ax = f3(jd[0], jd[1], jd[2]);
+            float val;
+            if (jd[6] != 0.0f) {
+                val = st.U[3] * ax.x + st.U[4] * ax.y + st.U[5] * ax.z;
+            } else {
+                const float3 lin = cross3(ax, st.c - f3(jd[3], jd[4], jd[5]));
+                val = st.U[0] * ax.x + st.U[1] * ax.y + st.U[2] * ax.z + st.U[3] * lin.x + st.U[4] * lin.y + st.U[5] * lin.z;
+            }
+            rowk[j] = val * inv;
+        }
+    }
+
+    // Forward acceleration sweep: the parent's acceleration by shuffle.
+    const int par = (mine && b > 0) ? T.parent[b] : b;
     for (int l = 1; l <= T.n_levels; ++l) {
+        const float3 pa = shfl3(acc_ang, par);
+        const float3 plin = shfl3(acc_lin, par);
         if (my_depth == l) {
-            const int p = bc.parent;
-            const float3 pa = ld3(A + p * 6);
-            const float3 pl = ld3(A + p * 6 + 3) + cross3(pa, st.r);
+            const float3 pl = plin + cross3(pa, st.r);
             float3 ang = pa + st.ba;
             float3 lin = pl + st.bl;
             if (bc.dof >= 0) {
@@ -541,11 +571,11 @@ __device__ bool aba(const Warp& w, const BodyConst& bc, BodyState& st, float* ro
                 ang = ang + f3(st.s[0], st.s[1], st.s[2]) * acc;
                 lin = lin + f3(st.s[3], st.s[4], st.s[5]) * acc;
             }
-            st3(A + b * 6, ang);
-            st3(A + b * 6 + 3, lin);
+            acc_ang = ang;
+            acc_lin = lin;
         }
-        __syncwarp();
     }
+    __syncwarp();
     // v_free = v + h qdd.
     float* vf = s + L.vf;
     for (int d = b; d < M.nv; d += 32) {
@@ -632,8 +662,8 @@ __device__ void make_shape(const DeviceModel& M, const float* pose, int sh, floa
     const float4 lp = M.shape_position[sh];
     const float4 lr = M.shape_rotation[sh];
     if (b >= 0) {
-        o.body_pos = ld3(pose + b * 8);
-        o.body_rot = ld4(pose + b * 8 + 4);
+        o.body_pos = ld3(pose + b * kPoseStride);
+        o.body_rot = ld4(pose + b * kPoseStride + 3);
         o.center = o.body_pos + qrot(o.body_rot, xyz(lp));
         o.rot = qmul(o.body_rot, lr);
     } else {
@@ -1060,7 +1090,7 @@ __device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState& s
     float* Y = s + L.G;     // G rows, factored in place into Y = L^-T G^T
     float* Lm = s + L.L;    // packed lower factor rows
     float* z = s + L.z;     // L-space image of the accumulated impulses
-    const int ma = T.max_anc;
+    const int ma = T.max_anc | 1;  // odd row stride of Y: lane-per-row access is conflict free
 
     // Speculative margins of articulated colliders (Collision.metal:5882-5915):
     // h * sum|v_free| * max(sweep radius, 0.25), capped by h * speed envelope.
@@ -1089,7 +1119,7 @@ __device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState& s
         if (lane >= o) scratch_end += t;
     }
     if (lane < M.np) {
-        npoints = pair_manifold(M, pose, margins, lane, slots + lane * kManifoldWords, s + L.narrow + scratch_end - my_words,
+        npoints = pair_manifold(M, pose, margins, lane, slots + lane * kSlotStride, s + L.narrow + scratch_end - my_words,
                                 nraw, cand);
         if (npoints < 0) { pair_fail = true; npoints = 0; }
     }
@@ -1131,14 +1161,14 @@ __device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState& s
     // its points in manifold order.
     if (lane < M.np && npoints > 0) {
         const int pair = lane;
-        const float* slot = slots + pair * kManifoldWords;
+        const float* slot = slots + pair * kSlotStride;
         const int sa = M.pair_a[pair], sb = M.pair_b[pair];
         const int ba = M.shape_body[sa], bb = M.shape_body[sb];
         float3 posA, posB;
         float4 rotA, rotB;
-        if (ba >= 0) { posA = ld3(pose + ba * 8); rotA = ld4(pose + ba * 8 + 4); }
+        if (ba >= 0) { posA = ld3(pose + ba * kPoseStride); rotA = ld4(pose + ba * kPoseStride + 3); }
         else { posA = xyz(M.static_body_position[sa]); rotA = M.static_body_rotation[sa]; }
-        if (bb >= 0) { posB = ld3(pose + bb * 8); rotB = ld4(pose + bb * 8 + 4); }
+        if (bb >= 0) { posB = ld3(pose + bb * kPoseStride); rotB = ld4(pose + bb * kPoseStride + 3); }
         else { posB = xyz(M.static_body_position[sb]); rotB = M.static_body_rotation[sb]; }
         float3 nw = qrot(rotA, ld3(slot));
         nw = nw * (1.0f / len3(nw));
@@ -1208,7 +1238,7 @@ __device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState& s
         for (int k = 0; k < na; ++k) {
             const int d = T.anc[b][k];
             // Point-Jacobian column: a x (x - o) for rotations, a for translations.
-            const float* jd = Jax + d * 8;
+            const float* jd = Jax + d * kJStride;
             const float3 ax = f3(jd[0], jd[1], jd[2]);
             const float3 jc = jd[6] != 0.0f ? ax : cross3(ax, x - f3(jd[3], jd[4], jd[5]));
             const float vk = vf[d];
@@ -1247,33 +1277,6 @@ __device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState& s
     for (int d = lane; d < nv; d += 32) v[d] = vf[d];
     if (total > 0) {
         if (lane == 0) misc[kMiscIslands] = as_float(max(as_int(misc[kMiscIslands]), 1));
-        // Joint rows of the factor H = L^T L from this substep's ABA pivots
-        // (rows 0-5 of a floating root were stored by the ABA): eliminating a
-        // DoF's descendants leaves the articulated inertia of its body, so
-        // L_kk = sqrt(D_k) and L_kj = U_k . S_j(c_b) / L_kk for the ancestor
-        // DoFs j, with S_j moved to body b's COM.
-        if (lane < T.nb && lane > 0 && bc.dof >= 0) {
-            const int k = bc.dof;
-            float* rowk = Lm + k * (k + 1) / 2;
-            const float lkk = sqrtf(st.D);
-            const float inv = 1.0f / lkk;
-            rowk[k] = lkk;
-            const int na = T.dof_depth[k];
-            for (int t = 0; t < na; ++t) {
-                const int j = T.anc[lane][t];
-                const float* jd = Jax + j * 8;
-                const float3 ax = f3(jd[0], jd[1], jd[2]);
-                float val;
-                if (jd[6] != 0.0f) {
-                    val = st.U[3] * ax.x + st.U[4] * ax.y + st.U[5] * ax.z;
-                } else {
-                    const float3 lin = cross3(ax, st.c - f3(jd[3], jd[4], jd[5]));
-                    val = st.U[0] * ax.x + st.U[1] * ax.y + st.U[2] * ax.z + st.U[3] * lin.x + st.U[4] * lin.y + st.U[5] * lin.z;
-                }
-                rowk[j] = val * inv;
-            }
-        }
-        __syncwarp();
         // Y = L^-T G^T per contact row, in place over the ancestor positions.
         const int nrows = 3 * total;
         for (int row = lane; row < nrows; row += 32) {
@@ -1403,7 +1406,7 @@ __device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState& s
         if (lane < total) {
             const float* c = C + lane * kContactWords;
             const int slot = as_int(c[kCwSlot]);
-            float* op = slots + (slot >> 2) * kManifoldWords + 8 + (slot & 3) * 12;
+            float* op = slots + (slot >> 2) * kSlotStride + 8 + (slot & 3) * 12;
             op[9] = c[kCwLambda + 0];
             op[10] = c[kCwLambda + 1];
             op[11] = c[kCwLambda + 2];
@@ -1495,14 +1498,14 @@ __global__ void __launch_bounds__(128) control_step_kernel(StepParams p, WarpLay
     for (int a = lane; a < M.action_count; a += 32)
         s[layout.tgt + M.action_dof[a]] = p.actions[static_cast<size_t>(env) * M.action_count + a];
     if (kContact) {
+        // Slots sit at an odd stride in shared memory (lane-per-pair access
+        // is conflict free) and packed in HBM.
         float* slots = s + layout.manifolds;
         const int words = M.np * kManifoldWords;
-        if (reset) {
-            for (int i = lane; i < words; i += 32) slots[i] = 0.0f;
-        } else {
-            const float4* src = reinterpret_cast<const float4*>(p.manifolds + static_cast<size_t>(env) * words);
-            float4* dst = reinterpret_cast<float4*>(slots);
-            for (int i = lane; i < words / 4; i += 32) dst[i] = src[i];
+        const float* src = p.manifolds + static_cast<size_t>(env) * words;
+        for (int i = lane; i < words; i += 32) {
+            const int pair = i / kManifoldWords;
+            slots[pair * kSlotStride + (i - pair * kManifoldWords)] = reset ? 0.0f : src[i];
         }
     }
     const float friction_scale = kContact ? p.friction_scale[env] : 1.0f;
@@ -1544,12 +1547,11 @@ __global__ void __launch_bounds__(128) control_step_kernel(StepParams p, WarpLay
     }
     if (kContact && (success || reset)) {
         const int words = M.np * kManifoldWords;
-        float4* dst = reinterpret_cast<float4*>(p.manifolds + static_cast<size_t>(env) * words);
-        if (success) {
-            const float4* src = reinterpret_cast<const float4*>(s + layout.manifolds);
-            for (int i = lane; i < words / 4; i += 32) dst[i] = src[i];
-        } else {
-            for (int i = lane; i < words / 4; i += 32) dst[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        float* dst = p.manifolds + static_cast<size_t>(env) * words;
+        const float* slots = s + layout.manifolds;
+        for (int i = lane; i < words; i += 32) {
+            const int pair = i / kManifoldWords;
+            dst[i] = success ? slots[pair * kSlotStride + (i - pair * kManifoldWords)] : 0.0f;
         }
     }
     if (lane == 0) {
