@@ -77,7 +77,11 @@ __host__ __device__ inline WarpLayout make_layout(int nb, int nv, int nq, int np
     L.margins = take(32);
     if (contact) {
         L.manifolds = take(np * kSlotStride);
-        L.L = take(nv * (nv + 1) / 2);
+        // Factor rows; past the root block (24 words) they later hold the
+        // per-DoF contact lists (nv x ncap u16).
+        const int factor = nv * (nv + 1) / 2;
+        const int lists = 24 + (nv * ncap + 1) / 2;
+        L.L = take(factor > lists ? factor : lists);
         // Contact records and Jacobian rows are written only after the
         // narrowphase has finished with its scratch, so the three share words.
         L.contacts = take(ncap * kContactWords);

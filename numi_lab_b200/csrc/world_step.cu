@@ -43,6 +43,7 @@ constexpr float kQueryPad = 0.00000762939453125f;  // MR_COLLISION_QUERY_RELATIV
 constexpr float kAabbPad = 0.00000762939453125f;   // MR_COLLISION_AABB_RELATIVE_PAD
 constexpr unsigned char kNone = 255;
 constexpr int kMaxRawPerPair = 8;
+constexpr int kRootFactorWords = 24;  // rows 0-5 of the factor (21 words), padded
 constexpr float kTieRelative = 1.0e-5f;  // manifold reduction ties
 constexpr float kTieAbsolute = 1.0e-12f;
 
@@ -1292,7 +1293,27 @@ __device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState& s
                 for (int u = 0; u < t; ++u) y[u] -= rowk[T.anc[b][u]] * yt;
             }
         }
-        for (int d = lane; d < nv; d += 32) z[d] = 0.0f;
+        __syncwarp();
+        // Per-DoF lists of the contact rows that reach it, as (position in
+        // the contact's ancestor list << 5 | contact), so a sweep's z update
+        // visits only those.  The lists reuse the factor rows past the root
+        // block: once Y exists the sweeps read no joint row of L.
+        std::uint16_t* dlist = reinterpret_cast<std::uint16_t*>(Lm + kRootFactorWords);
+        const int ncap = M.contact_capacity;
+        int dcount[2] = {0, 0};
+#pragma unroll
+        for (int pass = 0; pass < 2; ++pass) {
+            const int d = lane + 32 * pass;
+            if (d < nv) {
+                z[d] = 0.0f;
+                int cnt = 0;
+                for (int j = 0; j < total; ++j) {
+                    const int t = T.pos[as_int(C[j * kContactWords + kCwBody])][d];
+                    if (t != kNone) dlist[d * ncap + cnt++] = static_cast<std::uint16_t>((t << 5) | j);
+                }
+                dcount[pass] = cnt;
+            }
+        }
         __syncwarp();
         // Preconditioners, relaxation and warm start (lane per contact):
         // W_cc = Y_c^T Y_c + R, normal row sums over the common ancestor prefix.
@@ -1369,39 +1390,71 @@ __device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState& s
                 }
             }
             __syncwarp();
-            for (int d = lane; d < nv; d += 32) {
-                float acc = 0.0f;
-                for (int j = 0; j < total; ++j) {
-                    const float* cj = C + j * kContactWords;
-                    const int t = T.pos[as_int(cj[kCwBody])][d];
-                    if (t == kNone) continue;
-                    const float* yj = Y + j * 3 * ma + t;
-                    acc = fmaf(yj[0], cj[kCwDelta + 0], acc);
-                    acc = fmaf(yj[ma], cj[kCwDelta + 1], acc);
-                    acc = fmaf(yj[2 * ma], cj[kCwDelta + 2], acc);
+#pragma unroll
+            for (int pass = 0; pass < 2; ++pass) {
+                const int d = lane + 32 * pass;
+                if (d < nv) {
+                    float acc = 0.0f;
+                    const std::uint16_t* list = dlist + d * ncap;
+#pragma unroll 4
+                    for (int k = 0; k < dcount[pass]; ++k) {
+                        const int e = list[k];
+                        const int j = e & 31;
+                        const float* cj = C + j * kContactWords;
+                        const float* yj = Y + j * 3 * ma + (e >> 5);
+                        acc = fmaf(yj[0], cj[kCwDelta + 0], acc);
+                        acc = fmaf(yj[ma], cj[kCwDelta + 1], acc);
+                        acc = fmaf(yj[2 * ma], cj[kCwDelta + 2], acc);
+                    }
+                    z[d] += acc;
                 }
-                z[d] += acc;
             }
             __syncwarp();
         }
         if (!warp_ok(misc)) return false;
-        // Velocity change x = L^-1 z by DoF-tree depth (ancestors first).
-        float* x = s + L.qdd;
-        for (int dep = 0; dep < T.n_dof_levels; ++dep) {
-            for (int k = lane; k < nv; k += 32) {
-                if (T.dof_depth[k] != dep) continue;
-                const float* rowk = Lm + k * (k + 1) / 2;
-                const int bk = T.dof_body[k];
-                float acc = z[k];
-                for (int t = 0; t < dep; ++t) {
-                    const int i = T.anc[bk][t];
-                    acc -= rowk[i] * x[i];
+        // Velocity change x = L^-1 z as one forward tree sweep: with
+        // L_kj = U_k . S_j(c_k) / L_kk, sum_j L_kj x_j is U_k applied to the
+        // parent's twist change moved to body k's COM, so each body needs
+        // only its parent's twist change (by shuffle), not its ancestors' x.
+        {
+            const bool mine = lane < T.nb;
+            const int my_depth = mine ? T.depth[lane] : -1;
+            const int par = (mine && lane > 0) ? T.parent[lane] : lane;
+            float3 dw = f3(0.0f, 0.0f, 0.0f), dv = f3(0.0f, 0.0f, 0.0f);
+            if (lane == 0 && T.floating) {
+                float xr[6];
+#pragma unroll
+                for (int k = 0; k < 6; ++k) {
+                    const float* rowk = Lm + k * (k + 1) / 2;
+                    float acc = z[k];
+#pragma unroll
+                    for (int j = 0; j < k; ++j) acc -= rowk[j] * xr[j];
+                    xr[k] = acc / rowk[k];
+                    v[k] += xr[k];
                 }
-                x[k] = acc / rowk[k];
+                dv = f3(xr[0], xr[1], xr[2]);
+                dw = f3(xr[3], xr[4], xr[5]);
             }
-            __syncwarp();
+            for (int l = 1; l <= T.n_levels; ++l) {
+                const float3 pw = shfl3(dw, par);
+                const float3 pv = shfl3(dv, par);
+                if (my_depth == l) {
+                    dw = pw;
+                    dv = pv + cross3(pw, st.r);
+                    if (bc.dof >= 0) {
+                        const int k = bc.dof;
+                        const float lkk = sqrtf(st.D);  // = L_kk as written by the ABA
+                        const float sum = st.U[0] * dw.x + st.U[1] * dw.y + st.U[2] * dw.z + st.U[3] * dv.x +
+                                          st.U[4] * dv.y + st.U[5] * dv.z;
+                        const float xk = (z[k] - sum / lkk) / lkk;
+                        v[k] += xk;
+                        dw = dw + f3(st.s[0], st.s[1], st.s[2]) * xk;
+                        dv = dv + f3(st.s[3], st.s[4], st.s[5]) * xk;
+                    }
+                }
+            }
         }
-        for (int d = lane; d < nv; d += 32) v[d] += x[d];
+        __syncwarp();
         // Impulses back into the manifold points (warm start of the next substep).
         if (lane < total) {
             const float* c = C + lane * kContactWords;
