@@ -443,6 +443,18 @@ MR_API int mr_task_rollout_copy_final_scene_states(
 /* Additions of this library                                               */
 /* ---------------------------------------------------------------------- */
 
+/* No counterpart in the reference: arithmetic precision of the articulated
+ * inertia.  MR_PRECISION_FP32 (default) keeps the whole microstep in FP32 like
+ * the reference; MR_PRECISION_FP64_ARTICULATED_INERTIA carries the
+ * articulated inertias, their joint pivots and the floating root's 6x6
+ * factorisation in FP64 (state, contacts and the cone solve stay FP32).
+ * Applies to the next advance. */
+enum MRPrecisionModeC {
+    MR_PRECISION_FP32 = 0u,
+    MR_PRECISION_FP64_ARTICULATED_INERTIA = 1u
+};
+MR_API int mr_task_rollout_set_precision(MRTaskRolloutHandle* handle, uint32_t mode);
+
 /* No counterpart in the reference: zero-copy advance for device buffers
  * (e.g. torch CUDA tensors).  `device_actions` [step][env][action] and the
  * optional `device_reset_masks` [step][env] live on the rollout's device;

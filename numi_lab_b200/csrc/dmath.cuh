@@ -70,13 +70,14 @@ __device__ __forceinline__ float4 so3_increment(float3 rv, bool reduce_angle) {
 // Packed symmetric 6x6 (lower triangle, row-major): index(i, j), i >= j.
 __device__ __forceinline__ int sym6(int i, int j) { return i >= j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i; }
 
-// y = A x for packed symmetric 6x6 A.
-__device__ __forceinline__ void sym6_mul(const float* A, const float* x, float* y) {
+// y = A x for packed symmetric 6x6 A (R = float or double).
+template <typename R>
+__device__ __forceinline__ void sym6_mul(const R* A, const float* x, R* y) {
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
-        float s = 0.0f;
+        R s = R(0);
 #pragma unroll
-        for (int j = 0; j < 6; ++j) s = fmaf(A[sym6(i, j)], x[j], s);
+        for (int j = 0; j < 6; ++j) s = fma(A[sym6(i, j)], static_cast<R>(x[j]), s);
         y[i] = s;
     }
 }

@@ -39,7 +39,7 @@ struct WarpLayout {
     int body_pose, dof_J;
     int q, qc, v, vc, vf, tau, qdd, tgt;
     int misc;
-    int manifolds, contacts, G, L, z, margins;
+    int manifolds, contacts, G, L, z, margins, pair_stats;
     int narrow;  // narrowphase scratch; aliases the contact records and rows
     int total;   // floats per warp
 };
@@ -77,6 +77,7 @@ __host__ __device__ inline WarpLayout make_layout(int nb, int nv, int nq, int np
     L.margins = take(32);
     if (contact) {
         L.manifolds = take(np * kSlotStride);
+        L.pair_stats = take(32);
         // Factor rows; past the root block (24 words) they later hold the
         // per-DoF contact lists (nv x ncap u16).
         const int factor = nv * (nv + 1) / 2;
@@ -90,7 +91,7 @@ __host__ __device__ inline WarpLayout make_layout(int nb, int nv, int nq, int np
         L.G = take(rows > need ? rows : need);
         L.narrow = L.contacts;
     } else {
-        L.manifolds = L.contacts = L.G = L.L = L.narrow = o;
+        L.manifolds = L.contacts = L.G = L.L = L.narrow = L.pair_stats = o;
     }
     L.total = align4(o);
     return L;

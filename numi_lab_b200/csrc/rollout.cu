@@ -26,8 +26,8 @@
 #include <vector>
 
 namespace numi {
-cudaError_t control_step_occupancy(bool contact, int warps_per_block, size_t smem, int* blocks_per_sm);
-cudaError_t launch_control_step(const StepParams& p, const WarpLayout& layout, bool contact, int warps_per_block,
+cudaError_t control_step_occupancy(bool contact, bool fp64_inertia, int warps_per_block, size_t smem, int* blocks_per_sm);
+cudaError_t launch_control_step(const StepParams& p, const WarpLayout& layout, bool contact, bool fp64_inertia, int warps_per_block,
                                 cudaStream_t stream);
 cudaError_t configure_control_step_kernels(size_t max_dynamic_smem);
 size_t control_step_table_bytes();
@@ -292,8 +292,9 @@ struct MRTaskRolloutHandle {
     numi::DeviceModel dmodel{};
     numi::WarpLayout layout{};
     bool contact = false;
-    int warps_per_block = 1;
-    int resident_warps_per_sm = 0;
+    bool fp64_inertia = false;          // MR_PRECISION_FP64_ARTICULATED_INERTIA
+    int warps_per_block[2] = {1, 1};    // per precision (FP32, FP64 inertia)
+    int resident_warps_per_sm[2] = {0, 0};
     MRTaskRolloutConfigC config{};
     std::uint32_t envs = 0;
     float h = 0.0f;
@@ -321,9 +322,10 @@ struct MRTaskRolloutHandle {
         const void* obs;
         const void* status;
         const void* contacts;
+        bool fp64_inertia;
         bool operator<(const GraphKey& o) const {
-            return std::tie(steps, actions, masks, obs, status, contacts) <
-                   std::tie(o.steps, o.actions, o.masks, o.obs, o.status, o.contacts);
+            return std::tie(steps, actions, masks, obs, status, contacts, fp64_inertia) <
+                   std::tie(o.steps, o.actions, o.masks, o.obs, o.status, o.contacts, o.fp64_inertia);
         }
     };
     std::map<GraphKey, cudaGraphExec_t> graphs;
@@ -386,13 +388,14 @@ struct MRTaskRolloutHandle {
             p.substeps = static_cast<int>(config.physics_substeps);
             p.velocity_iterations = static_cast<int>(config.velocity_iterations);
             p.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
-            check(numi::launch_control_step(p, layout, contact, warps_per_block, s), "control step launch");
+            check(numi::launch_control_step(p, layout, contact, fp64_inertia, warps_per_block[fp64_inertia ? 1 : 0], s),
+                  "control step launch");
         }
     }
 
     void run(std::uint32_t steps, const float* actions, const std::uint32_t* masks, float* obs, std::uint32_t* status,
              std::uint32_t* contacts, cudaStream_t s) {
-        const GraphKey key{steps, actions, masks, obs, status, contacts};
+        const GraphKey key{steps, actions, masks, obs, status, contacts, fp64_inertia};
         auto it = graphs.find(key);
         if (it == graphs.end()) {
             cudaGraph_t graph = nullptr;
@@ -551,18 +554,18 @@ MR_API MRTaskRolloutHandle* mr_create_task_rollout(const MRRunManifestC* manifes
         // Environments per CTA: the choice that keeps the most warps resident
         // per SM under the kernel's register and shared-memory footprint
         // (each CTA carries one copy of the topology tables).
-        {
+        for (int prec = 0; prec < 2; ++prec) {
             int best = 1, best_warps = 0;
             for (int wpb = 1; wpb <= 4; wpb *= 2) {
                 const size_t smem = tables + wpb * per_warp;
                 if (smem > limit) break;
                 int blocks = 0;
-                check(numi::control_step_occupancy(h.contact, wpb, smem, &blocks), "occupancy query");
+                check(numi::control_step_occupancy(h.contact, prec == 1, wpb, smem, &blocks), "occupancy query");
                 if (blocks * wpb > best_warps) { best_warps = blocks * wpb; best = wpb; }
             }
             if (best_warps == 0) throw std::runtime_error("the control-step kernel cannot be resident with this model");
-            h.warps_per_block = best;
-            h.resident_warps_per_sm = best_warps;
+            h.warps_per_block[prec] = best;
+            h.resident_warps_per_sm[prec] = best_warps;
         }
         check(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking), "stream");
         check(cudaEventCreate(&h.ev_start), "event");
@@ -621,6 +624,15 @@ MR_API int mr_task_rollout_set_state_readback(MRTaskRolloutHandle* handle, uint3
         if (!handle) throw std::invalid_argument("handle is null");
         handle->readback = enabled != 0;
         if (!handle->readback) handle->have_final_q = false;
+    });
+}
+
+MR_API int mr_task_rollout_set_precision(MRTaskRolloutHandle* handle, uint32_t mode) {
+    return guarded([&] {
+        if (!handle) throw std::invalid_argument("handle is null");
+        if (mode != MR_PRECISION_FP32 && mode != MR_PRECISION_FP64_ARTICULATED_INERTIA)
+            throw std::invalid_argument("unknown precision mode " + std::to_string(mode));
+        handle->fp64_inertia = mode == MR_PRECISION_FP64_ARTICULATED_INERTIA;
     });
 }
 

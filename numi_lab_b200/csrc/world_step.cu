@@ -43,7 +43,9 @@ constexpr float kQueryPad = 0.00000762939453125f;  // MR_COLLISION_QUERY_RELATIV
 constexpr float kAabbPad = 0.00000762939453125f;   // MR_COLLISION_AABB_RELATIVE_PAD
 constexpr unsigned char kNone = 255;
 constexpr int kMaxRawPerPair = 8;
-constexpr int kRootFactorWords = 24;  // rows 0-5 of the factor (21 words), padded
+constexpr int kRootFactorWords = 24;
+constexpr int kRegisterChain = 16;   // longest ancestor chain solved in registers
+constexpr int kMaxCandidates = 4 + kMaxRawPerPair;  // manifold candidates of one pair  // rows 0-5 of the factor (21 words), padded
 constexpr float kTieRelative = 1.0e-5f;  // manifold reduction ties
 constexpr float kTieAbsolute = 1.0e-12f;
 
@@ -71,13 +73,12 @@ __device__ __forceinline__ bool warp_ok(const float* misc) {
     return as_int(misc[kMiscStatus]) == MR_STEP_SUCCESS;
 }
 
-// Per-lane body constants, loaded once per control step.
+// Per-lane body topology, loaded once per control step.  The body's float
+// constants (joint frames, mass, inertia) are read from the model record at
+// their point of use: every warp of an SM reads the same record, so those
+// loads hit L1, and registers stay free for the FP64 articulated inertia.
 struct BodyConst {
     int parent, dof, type, qidx;
-    float3 axis, panchor, canchor;
-    float4 prot, crotc;
-    float mass, lin_damp, ang_damp;
-    float4 idiag, ioff;
 };
 
 __device__ void load_body(const DeviceModel& M, int b, BodyConst& c) {
@@ -85,20 +86,16 @@ __device__ void load_body(const DeviceModel& M, int b, BodyConst& c) {
     c.dof = M.body_dof[b];
     c.type = M.joint_type[b];
     c.qidx = c.dof >= 0 ? M.dof_q[c.dof] : -1;
-    c.axis = xyz(M.axis[b]);
-    c.panchor = xyz(M.parent_anchor[b]);
-    c.canchor = xyz(M.child_anchor[b]);
-    c.prot = M.parent_rotation[b];
-    c.crotc = M.child_rotation_conj[b];
-    const float4 md = M.mass_damping[b];
-    c.mass = md.x;
-    c.lin_damp = md.y;
-    c.ang_damp = md.z;
-    c.idiag = M.inertia_diag[b];
-    c.ioff = M.inertia_off[b];
 }
 
-// Per-lane dynamic body state of one substep.
+// Per-lane dynamic body state of one substep.  R is the precision of the
+// articulated inertia and its joint terms (U = I s, D, u): float (the
+// reference's precision) or double (the FP64 articulated-inertia mode).
+// Shifting a child's inertia to its parent's COM adds parallel-axis terms
+// two to three orders of magnitude larger than the pivots D of light distal
+// links, and FP32 rounding of those terms alone moves joint accelerations by
+// ~3e-5 relative on a 7-link chain.
+template <typename R>
 struct BodyState {
     float3 c;       // COM position
     float4 qr;      // orientation
@@ -106,9 +103,9 @@ struct BodyState {
     float3 ba, bl;  // velocity-product bias accelerations
     float3 r;       // parent COM -> body COM
     float s[6];     // joint motion subspace about this body's COM
-    float I[21];    // articulated (then composite) inertia, packed symmetric
+    R I[21];        // articulated inertia, packed symmetric
     float p[6];     // articulated bias force
-    float U[6], D, u;
+    R U[6], D, u;
 };
 
 // ---------------------------------------------------------------------------
@@ -151,60 +148,52 @@ __device__ void compute_drives(const Warp& w) {
 // motionTransformElement :160-190, written out in 3x3 blocks):
 // I = [[A, B], [B^T, D]], E = [r]x:  A' = A - B E + E B^T - E D E,
 // B' = B + E D, D' = D.
-__device__ __forceinline__ void shift_inertia(const float* I, float3 r, float* out) {
-    float A[3][3], B[3][3], D[3][3];
+template <typename R>
+struct Vec3 {
+    R x, y, z;
+};
+template <typename R>
+__device__ __forceinline__ Vec3<R> vcross(Vec3<R> a, Vec3<R> b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+
+template <typename R>
+__device__ __forceinline__ void shift_inertia(R* I, float3 rf) {
+    // In place.  With E = [r]x: row i of B E is B_i x r, E D column j is
+    // r x D_j, E B^T = -(B E)^T and row i of E D E is (E D)_i x r.
+    const Vec3<R> r{rf.x, rf.y, rf.z};
+    Vec3<R> EDc[3], BE[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        EDc[i] = vcross(r, Vec3<R>{I[sym6(3, 3 + i)], I[sym6(4, 3 + i)], I[sym6(5, 3 + i)]});
+        BE[i] = vcross(Vec3<R>{I[sym6(3, i)], I[sym6(4, i)], I[sym6(5, i)]}, r);
+    }
+    const Vec3<R> E0 = vcross(Vec3<R>{EDc[0].x, EDc[1].x, EDc[2].x}, r);
+    const Vec3<R> E1 = vcross(Vec3<R>{EDc[0].y, EDc[1].y, EDc[2].y}, r);
+    const Vec3<R> E2 = vcross(Vec3<R>{EDc[0].z, EDc[1].z, EDc[2].z}, r);
+    const R bex[3][3] = {{BE[0].x, BE[0].y, BE[0].z}, {BE[1].x, BE[1].y, BE[1].z}, {BE[2].x, BE[2].y, BE[2].z}};
+    const R ede[3][3] = {{E0.x, E0.y, E0.z}, {E1.x, E1.y, E1.z}, {E2.x, E2.y, E2.z}};
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            A[i][j] = I[sym6(i, j)];
-            B[i][j] = I[sym6(3 + j, i)];
-            D[i][j] = I[sym6(3 + i, 3 + j)];
-        }
-    const float E[3][3] = {{0.0f, -r.z, r.y}, {r.z, 0.0f, -r.x}, {-r.y, r.x, 0.0f}};
-    float ED[3][3], BE[3][3];
+        for (int j = 0; j <= i; ++j) I[sym6(i, j)] -= bex[i][j] + bex[j][i] + ede[i][j];
+    const R edx[3][3] = {{EDc[0].x, EDc[1].x, EDc[2].x}, {EDc[0].y, EDc[1].y, EDc[2].y}, {EDc[0].z, EDc[1].z, EDc[2].z}};
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            float ed = 0.0f, be = 0.0f;
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                ed = fmaf(E[i][k], D[k][j], ed);
-                be = fmaf(B[i][k], E[k][j], be);
-            }
-            ED[i][j] = ed;
-            BE[i][j] = be;
-        }
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j <= i; ++j) {
-            float ede = 0.0f, ebt = 0.0f;
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                ede = fmaf(ED[i][k], E[k][j], ede);
-                ebt = fmaf(E[i][k], B[j][k], ebt);
-            }
-            out[sym6(i, j)] = A[i][j] - BE[i][j] + ebt - ede;
-        }
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) out[sym6(3 + j, i)] = B[i][j] + ED[i][j];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j <= i; ++j) out[sym6(3 + i, 3 + j)] = D[i][j];
+        for (int j = 0; j < 3; ++j) I[sym6(3 + j, i)] += edx[i][j];
 }
 
 // Rigid spatial inertia about the COM in world axes: [[R Ib R^T, 0], [0, m 1]].
-__device__ __forceinline__ void body_inertia(const BodyConst& bc, float4 qb, float* I6, float Iw[3][3]) {
+template <typename R>
+__device__ __forceinline__ void body_inertia(const DeviceModel& M, int b, float4 qb, R* I6, float Iw[3][3]) {
+    const float4 idiag = M.inertia_diag[b], ioff = M.inertia_off[b];
+    const float mass = M.mass_damping[b].x;
     const float3 c0 = qrot(qb, f3(1.0f, 0.0f, 0.0f));
     const float3 c1 = qrot(qb, f3(0.0f, 1.0f, 0.0f));
     const float3 c2 = qrot(qb, f3(0.0f, 0.0f, 1.0f));
-    const float Ib[3][3] = {{bc.idiag.x, bc.ioff.x, bc.ioff.y}, {bc.ioff.x, bc.idiag.y, bc.ioff.z}, {bc.ioff.y, bc.ioff.z, bc.idiag.z}};
-    const float R[3][3] = {{c0.x, c1.x, c2.x}, {c0.y, c1.y, c2.y}, {c0.z, c1.z, c2.z}};
+    const float Ib[3][3] = {{idiag.x, ioff.x, ioff.y}, {ioff.x, idiag.y, ioff.z}, {ioff.y, ioff.z, idiag.z}};
+    const float Rot[3][3] = {{c0.x, c1.x, c2.x}, {c0.y, c1.y, c2.y}, {c0.z, c1.z, c2.z}};
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -213,16 +202,16 @@ __device__ __forceinline__ void body_inertia(const BodyConst& bc, float4 qb, flo
 #pragma unroll
             for (int k = 0; k < 3; ++k)
 #pragma unroll
-                for (int l2 = 0; l2 < 3; ++l2) acc = fmaf(R[i][k] * Ib[k][l2], R[j][l2], acc);
+                for (int l2 = 0; l2 < 3; ++l2) acc = fmaf(Rot[i][k] * Ib[k][l2], Rot[j][l2], acc);
             Iw[i][j] = acc;
         }
 #pragma unroll
-    for (int e = 0; e < 21; ++e) I6[e] = 0.0f;
+    for (int e = 0; e < 21; ++e) I6[e] = R(0);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
 #pragma unroll
         for (int j = 0; j <= i; ++j) I6[sym6(i, j)] = Iw[i][j];
-        I6[sym6(3 + i, 3 + i)] = bc.mass;
+        I6[sym6(3 + i, 3 + i)] = mass;
     }
 }
 
@@ -241,7 +230,13 @@ __device__ __forceinline__ float4 shfl4(float4 a, int src) {
                        __shfl_sync(0xffffffffu, a.z, src), __shfl_sync(0xffffffffu, a.w, src));
 }
 
-__device__ void kinematics(const Warp& w, const BodyConst& bc, BodyState& st) {
+__device__ __forceinline__ float3 shfl3g(float3 a, int src, unsigned mask) {
+    return f3(__shfl_sync(mask, a.x, src, 16), __shfl_sync(mask, a.y, src, 16), __shfl_sync(mask, a.z, src, 16));
+}
+
+template <typename R>
+__device__ void kinematics(const Warp& w, const BodyConst& bc, BodyState<R>& st) {
+    const DeviceModel& M = *w.M;
     const DeviceTables& T = *w.T;
     const WarpLayout& L = *w.L;
     float* s = w.s;
@@ -288,7 +283,8 @@ __device__ void kinematics(const Warp& w, const BodyConst& bc, BodyState& st) {
         const float3 wp = shfl3(st.w, par);
         const float3 vp = shfl3(st.v, par);
         if (my_depth == l) {
-            const float4 pj = qmul(qp, bc.prot);
+            const float3 axis = xyz(M.axis[b]);
+            const float4 pj = qmul(qp, M.parent_rotation[b]);
             float4 motion = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
             float qj = 0.0f, qdj = 0.0f;
             const bool has = bc.dof >= 0;
@@ -299,18 +295,18 @@ __device__ void kinematics(const Warp& w, const BodyConst& bc, BodyState& st) {
                 if (!prismatic) {
                     float sh, ch;
                     sincosf(0.5f * qj, &sh, &ch);
-                    motion = make_float4(bc.axis.x * sh, bc.axis.y * sh, bc.axis.z * sh, ch);
+                    motion = make_float4(axis.x * sh, axis.y * sh, axis.z * sh, ch);
                 }
             }
             float4 qb;
-            if (!qnormalize(qmul(qmul(pj, motion), bc.crotc), qb, false)) {
+            if (!qnormalize(qmul(qmul(pj, motion), M.child_rotation_conj[b]), qb, false)) {
                 set_status(misc, MR_STEP_NONFINITE_RESULT, static_cast<unsigned>(b));
                 qb = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
             }
-            const float3 ja = qrot(pj, bc.axis);
-            float3 jp = cp + qrot(qp, bc.panchor);
+            const float3 ja = qrot(pj, axis);
+            float3 jp = cp + qrot(qp, xyz(M.parent_anchor[b]));
             if (prismatic) jp = jp + ja * qj;
-            const float3 ca = qrot(qb, bc.canchor);
+            const float3 ca = qrot(qb, xyz(M.child_anchor[b]));
             const float3 cb = jp - ca;
             const float3 ptj = jp - cp;
             const float3 zero = f3(0.0f, 0.0f, 0.0f);
@@ -359,7 +355,8 @@ __device__ void kinematics(const Warp& w, const BodyConst& bc, BodyState& st) {
 // L_kj = U_k . S_j(c_b) / L_kk for the ancestor DoFs j, with S_j moved to
 // body b's COM.
 // ---------------------------------------------------------------------------
-__device__ bool aba(const Warp& w, const BodyConst& bc, BodyState& st, float* factor) {
+template <typename R>
+__device__ bool aba(const Warp& w, const BodyConst& bc, BodyState<R>& st, float* factor) {
     const DeviceModel& M = *w.M;
     const DeviceTables& T = *w.T;
     const WarpLayout& L = *w.L;
@@ -384,21 +381,22 @@ __device__ bool aba(const Warp& w, const BodyConst& bc, BodyState& st, float* fa
 
     // Rigid inertia and velocity-dependent bias about the COM.
 #pragma unroll
-    for (int e = 0; e < 21; ++e) st.I[e] = 0.0f;
+    for (int e = 0; e < 21; ++e) st.I[e] = R(0);
 #pragma unroll
     for (int e = 0; e < 6; ++e) st.p[e] = 0.0f;
     if (mine) {
         float Iw[3][3];
-        body_inertia(bc, st.qr, st.I, Iw);
+        body_inertia(M, b, st.qr, st.I, Iw);
         const float3 om = st.w;
         const float3 Iom = f3(Iw[0][0] * om.x + Iw[0][1] * om.y + Iw[0][2] * om.z,
                               Iw[1][0] * om.x + Iw[1][1] * om.y + Iw[1][2] * om.z,
                               Iw[2][0] * om.x + Iw[2][1] * om.y + Iw[2][2] * om.z);
         float3 bt = cross3(om, Iom);
-        float3 bf = -(bc.mass * f3(M.gravity[0], M.gravity[1], M.gravity[2]));
+        const float4 md = M.mass_damping[b];
+        float3 bf = -(md.x * f3(M.gravity[0], M.gravity[1], M.gravity[2]));
         if (M.apply_damping) {
-            bt = bt + bc.ang_damp * om;
-            bf = bf + bc.lin_damp * st.v;
+            bt = bt + md.z * om;
+            bf = bf + md.y * st.v;
         }
         st.p[0] = bt.x; st.p[1] = bt.y; st.p[2] = bt.z; st.p[3] = bf.x; st.p[4] = bf.y; st.p[5] = bf.z;
         if (b == 0 && T.floating) {
@@ -423,7 +421,7 @@ __device__ bool aba(const Warp& w, const BodyConst& bc, BodyState& st, float* fa
             const int src = take ? T.children[first_child + k] : b;
 #pragma unroll
             for (int e = 0; e < 21; ++e) {
-                const float x = __shfl_sync(0xffffffffu, st.I[e], src);
+                const R x = __shfl_sync(0xffffffffu, st.I[e], src);
                 if (take) st.I[e] += x;
             }
 #pragma unroll
@@ -434,101 +432,103 @@ __device__ bool aba(const Warp& w, const BodyConst& bc, BodyState& st, float* fa
         }
         if (!active) continue;
         if (l > 0) {
-            float prop[6], ic[6];
+            R prop[6];
             const float cv[6] = {st.ba.x, st.ba.y, st.ba.z, st.bl.x, st.bl.y, st.bl.z};
-            sym6_mul(st.I, cv, ic);
+            sym6_mul(st.I, cv, prop);
 #pragma unroll
-            for (int e = 0; e < 6; ++e) prop[e] = st.p[e] + ic[e];
-            st.D = 1.0f;
-            st.u = 0.0f;
+            for (int e = 0; e < 6; ++e) prop[e] += st.p[e];
+            st.D = R(1);
+            st.u = R(0);
 #pragma unroll
-            for (int e = 0; e < 6; ++e) st.U[e] = 0.0f;
+            for (int e = 0; e < 6; ++e) st.U[e] = R(0);
             if (bc.dof >= 0) {
                 sym6_mul(st.I, st.s, st.U);
-                const float D = dot6(st.s, st.U) + M.armature_eff[bc.dof];
-                float maxI = 0.0f;
+                R D = M.armature_eff[bc.dof];
 #pragma unroll
-                for (int e = 0; e < 21; ++e) maxI = fmaxf(maxI, fabsf(st.I[e]));
-                const float floor = fmaxf(kAbsolutePivotFloor, maxI * 6.0f * kFloatEps);
+                for (int e = 0; e < 6; ++e) D = fma(static_cast<R>(st.s[e]), st.U[e], D);
+                R maxI = R(0);
+#pragma unroll
+                for (int e = 0; e < 21; ++e) maxI = fmax(maxI, fabs(st.I[e]));
+                const R floor = fmax(static_cast<R>(kAbsolutePivotFloor), maxI * R(6) * static_cast<R>(kFloatEps));
                 if (!(D > floor) || !isfinite(D)) {
                     set_status(misc, MR_STEP_FACTORIZATION_FAILED, static_cast<unsigned>(bc.dof));
                 } else {
                     st.D = D;
-                    st.u = tau[bc.dof] - dot6(st.s, prop);
-                    const float invD = 1.0f / D;
+                    R u = tau[bc.dof];
 #pragma unroll
-                    for (int e = 0; e < 6; ++e) prop[e] += st.U[e] * (st.u * invD);
+                    for (int e = 0; e < 6; ++e) u = fma(-static_cast<R>(st.s[e]), prop[e], u);
+                    st.u = u;
+                    const R invD = R(1) / D;
+#pragma unroll
+                    for (int e = 0; e < 6; ++e) prop[e] += st.U[e] * (u * invD);
 #pragma unroll
                     for (int i = 0; i < 6; ++i)
 #pragma unroll
                         for (int j = 0; j <= i; ++j) st.I[sym6(i, j)] -= st.U[i] * st.U[j] * invD;
                 }
             }
-            float shifted[21];
-            shift_inertia(st.I, st.r, shifted);
-#pragma unroll
-            for (int e = 0; e < 21; ++e) st.I[e] = shifted[e];
-            const float3 pf = f3(prop[3], prop[4], prop[5]);
-            const float3 pt = f3(prop[0], prop[1], prop[2]) + cross3(st.r, pf);
+            shift_inertia(st.I, st.r);
+            const float3 pf = f3(static_cast<float>(prop[3]), static_cast<float>(prop[4]), static_cast<float>(prop[5]));
+            const float3 pt = f3(static_cast<float>(prop[0]), static_cast<float>(prop[1]), static_cast<float>(prop[2])) +
+                              cross3(st.r, pf);
             st.p[0] = pt.x; st.p[1] = pt.y; st.p[2] = pt.z; st.p[3] = pf.x; st.p[4] = pf.y; st.p[5] = pf.z;
         } else if (T.floating) {
             // Root articulated inertia in DoF order (linear x, y, z, then
-            // angular x, y, z), factored leaves-first as H0 = L0^T L0; solves
-            // H0 a0 = -pA for the root acceleration.
-            float Lf[21], r[6];
-            float maxI = 0.0f;
+            // angular x, y, z), factored leaves-first in FP64 in place as
+            // H0 = L0^T L0; solves H0 a0 = -pA for the root acceleration.
+            R maxI = R(0);
 #pragma unroll
-            for (int e = 0; e < 21; ++e) maxI = fmaxf(maxI, fabsf(st.I[e]));
-            const float floor = fmaxf(kAbsolutePivotFloor, maxI * 6.0f * kFloatEps);
+            for (int e = 0; e < 21; ++e) maxI = fmax(maxI, fabs(st.I[e]));
+            const R floor = fmax(static_cast<R>(kAbsolutePivotFloor), maxI * R(6) * static_cast<R>(kFloatEps));
+#define NUMI_ROOT(k, j) st.I[sym6((k) < 3 ? (k) + 3 : (k) - 3, (j) < 3 ? (j) + 3 : (j) - 3)]
+            R x[6];
 #pragma unroll
-            for (int k = 0; k < 6; ++k) {
-                const int pk = k < 3 ? k + 3 : k - 3;
-                r[k] = -st.p[pk];
-#pragma unroll
-                for (int j = 0; j <= k; ++j) Lf[sym6(k, j)] = st.I[sym6(pk, j < 3 ? j + 3 : j - 3)];
-            }
+            for (int k = 0; k < 6; ++k) x[k] = -static_cast<R>(st.p[k < 3 ? k + 3 : k - 3]);
             bool ok = true;
 #pragma unroll
             for (int k = 5; k >= 0; --k) {
-                float d = Lf[sym6(k, k)];
+                R d = NUMI_ROOT(k, k);
                 if (!(d > floor) || !isfinite(d)) {
                     ok = false;
-                    d = 1.0f;
+                    d = R(1);
                 }
-                const float lkk = sqrtf(d);
-                Lf[sym6(k, k)] = lkk;
-                const float inv = 1.0f / lkk;
+                const R lkk = sqrt(d);
+                NUMI_ROOT(k, k) = lkk;
+                const R inv = R(1) / lkk;
 #pragma unroll
-                for (int j = 0; j < k; ++j) Lf[sym6(k, j)] *= inv;
+                for (int j = 0; j < k; ++j) NUMI_ROOT(k, j) *= inv;
 #pragma unroll
                 for (int i = 0; i < k; ++i)
 #pragma unroll
-                    for (int j = 0; j <= i; ++j) Lf[sym6(i, j)] -= Lf[sym6(k, i)] * Lf[sym6(k, j)];
+                    for (int j = 0; j <= i; ++j) NUMI_ROOT(i, j) -= NUMI_ROOT(k, i) * NUMI_ROOT(k, j);
             }
-            float y[6], x[6];
+            // L0^T y = r (descending), then L0 x = y (ascending), in place.
 #pragma unroll
             for (int k = 5; k >= 0; --k) {
-                float val = r[k];
+                R val = x[k];
 #pragma unroll
-                for (int i = k + 1; i < 6; ++i) val -= Lf[sym6(i, k)] * y[i];
-                y[k] = val / Lf[sym6(k, k)];
+                for (int i = k + 1; i < 6; ++i) val -= NUMI_ROOT(i, k) * x[i];
+                x[k] = val / NUMI_ROOT(k, k);
             }
 #pragma unroll
             for (int k = 0; k < 6; ++k) {
-                float val = y[k];
+                R val = x[k];
 #pragma unroll
-                for (int j = 0; j < k; ++j) val -= Lf[sym6(k, j)] * x[j];
-                x[k] = val / Lf[sym6(k, k)];
+                for (int j = 0; j < k; ++j) val -= NUMI_ROOT(k, j) * x[j];
+                x[k] = val / NUMI_ROOT(k, k);
             }
             if (!ok) set_status(misc, MR_STEP_FACTORIZATION_FAILED, 0u);
             if (factor != nullptr) {
 #pragma unroll
-                for (int e = 0; e < 21; ++e) factor[e] = Lf[e];
-            }
+                for (int k = 0; k < 6; ++k)
 #pragma unroll
-            for (int k = 0; k < 6; ++k) qdd[k] = x[k];
-            acc_ang = f3(x[3], x[4], x[5]);
-            acc_lin = f3(x[0], x[1], x[2]);
+                    for (int j = 0; j <= k; ++j) factor[sym6(k, j)] = static_cast<float>(NUMI_ROOT(k, j));
+            }
+#undef NUMI_ROOT
+#pragma unroll
+            for (int k = 0; k < 6; ++k) qdd[k] = static_cast<float>(x[k]);
+            acc_ang = f3(static_cast<float>(x[3]), static_cast<float>(x[4]), static_cast<float>(x[5]));
+            acc_lin = f3(static_cast<float>(x[0]), static_cast<float>(x[1]), static_cast<float>(x[2]));
         }
     }
     if (!warp_ok(misc)) return false;
@@ -537,22 +537,22 @@ __device__ bool aba(const Warp& w, const BodyConst& bc, BodyState& st, float* fa
     if (factor != nullptr && mine && b > 0 && bc.dof >= 0) {
         const int k = bc.dof;
         float* rowk = factor + k * (k + 1) / 2;
-        const float lkk = sqrtf(st.D);
-        const float inv = 1.0f / lkk;
-        rowk[k] = lkk;
+        const R lkk = sqrt(st.D);
+        const R inv = R(1) / lkk;
+        rowk[k] = static_cast<float>(lkk);
         const int na = T.dof_depth[k];
         for (int t = 0; t < na; ++t) {
             const int j = T.anc[b][t];
             const float* jd = J + j * kJStride;
             const float3 ax = f3(jd[0], jd[1], jd[2]);
-            float val;
+            R val;
             if (jd[6] != 0.0f) {
                 val = st.U[3] * ax.x + st.U[4] * ax.y + st.U[5] * ax.z;
             } else {
                 const float3 lin = cross3(ax, st.c - f3(jd[3], jd[4], jd[5]));
                 val = st.U[0] * ax.x + st.U[1] * ax.y + st.U[2] * ax.z + st.U[3] * lin.x + st.U[4] * lin.y + st.U[5] * lin.z;
             }
-            rowk[j] = val * inv;
+            rowk[j] = static_cast<float>(val * inv);
         }
     }
 
@@ -566,8 +566,8 @@ __device__ bool aba(const Warp& w, const BodyConst& bc, BodyState& st, float* fa
             float3 ang = pa + st.ba;
             float3 lin = pl + st.bl;
             if (bc.dof >= 0) {
-                const float proj = st.U[0] * pa.x + st.U[1] * pa.y + st.U[2] * pa.z + st.U[3] * pl.x + st.U[4] * pl.y + st.U[5] * pl.z;
-                const float acc = (st.u - proj) / st.D;
+                const R proj = st.U[0] * pa.x + st.U[1] * pa.y + st.U[2] * pa.z + st.U[3] * pl.x + st.U[4] * pl.y + st.U[5] * pl.z;
+                const float acc = static_cast<float>((st.u - proj) / st.D);
                 qdd[bc.dof] = acc;
                 ang = ang + f3(st.s[0], st.s[1], st.s[2]) * acc;
                 lin = lin + f3(st.s[3], st.s[4], st.s[5]) * acc;
@@ -1013,6 +1013,348 @@ __device__ int pair_manifold(const DeviceModel& M, const float* pose, const floa
     return nc;
 }
 
+// Heavy pair classes (more than two raw contacts: box vs plane) are built by
+// a 16-lane group: lanes compute the raw witnesses (one feature each), the
+// kept old points, the match tests and the reduction scores in parallel,
+// and every sequential decision of the reference algorithm (match order,
+// greedy reduction scan, canonical order) is taken uniformly by the group
+// from shuffled values, so the result equals the one-lane build
+// (pair_manifold) decision for decision.  `sl` is the lane in the group,
+// `gbase` the group's first lane in the warp.
+__device__ __forceinline__ unsigned group_ballot(unsigned gmask, int gbase, bool pred) {
+    return (__ballot_sync(gmask, pred) >> gbase) & 0xffffu;
+}
+
+__device__ void group_manifold(const DeviceModel& M, const float* pose, const float* margins, int pair, float* slot,
+                               float* scratch, int sl, int gbase, unsigned gmask, int& npoints_out, int& nraw_out,
+                               bool& cand_out, bool& fail_out) {
+    npoints_out = 0;
+    nraw_out = 0;
+    cand_out = false;
+    fail_out = false;
+    const int sa = M.pair_a[pair];
+    const int sb = M.pair_b[pair];
+    ShapeWorld A, B;
+    make_shape(M, pose, sa, margins[sa], A);
+    make_shape(M, pose, sb, margins[sb], B);
+    const bool a_plane = A.type == MR_SHAPE_PLANE;
+    const ShapeWorld& plane = a_plane ? A : B;
+    const ShapeWorld& fin = a_plane ? B : A;
+    {
+        const float3 center = 0.5f * (fin.lower + fin.upper);
+        const float3 halfx = 0.5f * (fin.upper - fin.lower);
+        const float scale = fmaxf(fmaxf(maxabs3(plane.center), maxabs3(fin.lower)),
+                                  fmaxf(maxabs3(fin.upper), fmaxf(fabsf(plane.offset), fabsf(fin.offset))));
+        const float qpad = (scale + 1.0f) * kQueryPad;
+        const float3 an = f3(fabsf(plane.normal.x), fabsf(plane.normal.y), fabsf(plane.normal.z));
+        const float msd = dot3(plane.normal, center - plane.center) - dot3(an, halfx);
+        if (!(msd <= plane.offset + qpad)) {
+            if (sl == 0) slot[7] = as_float(0);
+            __syncwarp(gmask);
+            return;
+        }
+    }
+    cand_out = true;
+    const float accepted = A.offset + B.offset + (fmaxf(shape_scale(A), shape_scale(B)) + 1.0f) * kQueryPad;
+    const float3 posA = A.body_pos, posB = B.body_pos;
+    const float4 rotA = A.body_rot, rotB = B.body_rot;
+    const unsigned plane_feature = feature_key(MR_SHAPE_PLANE, 0u);
+    const float3 raw_normal = a_plane ? plane.normal : -plane.normal;
+    float* raw = scratch + 4 * kCandidateWords;
+    const int cls = M.pair_class[pair];
+
+    // Raw witnesses, one feature per lane; record r holds feature r.
+    bool racc = false, rbad = false;
+    if (sl < pair_max_raw(cls)) {
+        float3 surface = f3(0.0f, 0.0f, 0.0f);
+        unsigned ffeat = 0u;
+        if (cls == MR_COLLISION_PAIR_BOX_PLANE) {
+            const unsigned vtx = static_cast<unsigned>(sl);
+            const float3 local = f3((vtx & 1u) ? fin.half.x : -fin.half.x, (vtx & 2u) ? fin.half.y : -fin.half.y,
+                                    (vtx & 4u) ? fin.half.z : -fin.half.z);
+            surface = fin.center + qrot(fin.rot, local);
+            ffeat = feature_key(MR_SHAPE_BOX, vtx);
+        } else if (cls == MR_COLLISION_PAIR_CAPSULE_PLANE) {
+            surface = (sl == 0 ? fin.ep0 : fin.ep1) - plane.normal * fin.radius;
+            ffeat = feature_key(MR_SHAPE_CAPSULE, static_cast<unsigned>(sl));
+        } else {
+            surface = fin.center - plane.normal * fin.radius;
+            ffeat = feature_key(MR_SHAPE_SPHERE, 0u);
+        }
+        const float sep = dot3(plane.normal, surface - plane.center);
+        racc = sep <= accepted;
+        if (racc) {
+            const float3 pp = surface - plane.normal * sep;
+            const float3 pa = a_plane ? pp : surface;
+            const float3 pb = a_plane ? surface : pp;
+            float* rec = raw + sl * kCandidateWords;
+            st3(rec + kCdLa, qrotinv(rotA, pa - posA));
+            st3(rec + kCdLb, qrotinv(rotB, pb - posB));
+            rec[kCdFa] = as_float(static_cast<int>(a_plane ? plane_feature : ffeat));
+            rec[kCdFb] = as_float(static_cast<int>(a_plane ? ffeat : plane_feature));
+            st3(rec + kCdWp, 0.5f * (pa + pb));
+            rec[kCdSep] = sep;
+            rbad = !(isfinite(sep) && finite3(pa) && finite3(pb));
+        }
+    }
+    const unsigned raw_mask = group_ballot(gmask, gbase, racc);
+    const bool any_bad = group_ballot(gmask, gbase, rbad) != 0u;
+    nraw_out = __popc(raw_mask);
+    if (raw_mask == 0u) {
+        if (sl == 0) slot[7] = as_float(0);
+        __syncwarp(gmask);
+        return;
+    }
+    if (any_bad || !finite3(raw_normal)) {
+        fail_out = true;
+        return;
+    }
+    const float3 nw = raw_normal * (1.0f / len3(raw_normal));
+    if (!finite3(nw) || dot3(nw, nw) < 0.9999f) {
+        fail_out = true;
+        return;
+    }
+    const float4 thr = make_float4(M.manifold_thresholds[0], M.manifold_thresholds[1], M.manifold_thresholds[2],
+                                   M.manifold_thresholds[3]);
+    // Old manifold: lanes 8-11 test and copy the old points.
+    bool old_ok = false;
+    float3 transported = f3(0.0f, 0.0f, 0.0f);
+    float old_age = 0.0f;
+    const int old_count = as_int(slot[7]);
+    if (old_count > 0 && old_count <= kManifoldPoints) {
+        float3 on = qrot(rotA, ld3(slot));
+        on = on * (1.0f / len3(on));
+        old_ok = finite3(on) && dot3(on, nw) >= thr.w;
+        if (old_ok) {
+            const float3 ot = qrot(rotA, ld3(slot + 4));
+            transported = ot - nw * dot3(ot, nw);
+            old_age = slot[3];
+        }
+    }
+    bool keep = false;
+    const int oi = sl - 8;
+    if (old_ok && oi >= 0 && oi < old_count) {
+        const float* op = slot + 8 + oi * 12;
+        const float3 pa = posA + qrot(rotA, ld3(op));
+        const float3 pb = posB + qrot(rotB, ld3(op + 3));
+        const float3 delta = pb - pa;
+        const float sep = dot3(delta, nw);
+        const float3 tan = delta - nw * sep;
+        keep = !(sep > thr.x || len3(tan) > thr.y);
+        if (keep) {
+            float* rec = scratch + oi * kCandidateWords;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) rec[k] = op[k];
+            const unsigned life = static_cast<unsigned>(as_int(op[8]));
+            rec[kCdLife] = as_float(static_cast<int>(life == 0xffffffffu ? 0xffffffffu : life + 1u));
+            rec[kCdImp + 0] = op[9];
+            rec[kCdImp + 1] = op[10];
+            rec[kCdImp + 2] = op[11];
+            st3(rec + kCdWp, 0.5f * (pa + pb));
+            rec[kCdSep] = sep;
+        }
+    }
+    const unsigned kept_mask = (group_ballot(gmask, gbase, keep) >> 8) & 0xfu;
+    __syncwarp(gmask);
+
+    // Candidate list: lane k holds candidate k's id (geometry record in the
+    // low nibble, inherited old record in the high nibble).
+    int nc = __popc(kept_mask);
+    unsigned my_id = 0xffu;
+    {
+        unsigned m = kept_mask;
+        for (int k = 0; k < sl && m != 0u; ++k) m &= m - 1u;
+        if (sl < nc) {
+            const unsigned i = static_cast<unsigned>(__ffs(m) - 1);
+            my_id = (i << 4) | i;
+        }
+    }
+    // Raw contacts in feature order refresh the first candidate with the
+    // same features, else the first within the merge distance, else join.
+    const float merge2 = thr.z * thr.z;
+    for (unsigned m = raw_mask; m != 0u; m &= m - 1u) {
+        const int r = __ffs(m) - 1;
+        const float* rr = raw + r * kCandidateWords;
+        const float3 la = ld3(rr + kCdLa), lb = ld3(rr + kCdLb);
+        const int fa = as_int(rr[kCdFa]), fb = as_int(rr[kCdFb]);
+        bool feat = false, prox = false;
+        if (sl < nc) {
+            const float* g = scratch + (my_id & 15u) * kCandidateWords;
+            feat = as_int(g[kCdFa]) == fa && as_int(g[kCdFb]) == fb;
+            const float3 da = ld3(g + kCdLa) - la;
+            const float3 db = ld3(g + kCdLb) - lb;
+            prox = dot3(da, da) + dot3(db, db) <= 2.0f * merge2;
+        }
+        const unsigned fm = group_ballot(gmask, gbase, feat);
+        const unsigned pm = group_ballot(gmask, gbase, prox);
+        const int match = fm != 0u ? __ffs(fm) - 1 : (pm != 0u ? __ffs(pm) - 1 : -1);
+        if (match < 0) {
+            if (sl == nc) my_id = (kFresh << 4) | (4u + static_cast<unsigned>(r));
+            ++nc;
+        } else if (sl == match) {
+            my_id = (my_id & 0xf0u) | (4u + static_cast<unsigned>(r));
+        }
+    }
+    // Per-candidate geometry for the ordering and the scores.
+    float my_sep = 0.0f;
+    unsigned my_fa = 0xffffffffu, my_fb = 0xffffffffu;
+    float3 my_wp = f3(0.0f, 0.0f, 0.0f);
+    if (sl < nc) {
+        const float* g = scratch + (my_id & 15u) * kCandidateWords;
+        my_sep = g[kCdSep];
+        my_fa = static_cast<unsigned>(as_int(g[kCdFa]));
+        my_fb = static_cast<unsigned>(as_int(g[kCdFb]));
+        my_wp = ld3(g + kCdWp);
+    }
+    // Final candidate lanes in canonical (feature) order, 4 bits each.
+    unsigned long long final_order = 0ull;
+    int nfinal = 0;
+    if (nc > kManifoldPoints) {
+        // reduceCandidates: order by (separation, features), then greedy
+        // selection with the precision-independent tie rule of pair_manifold.
+        int rank = 0;
+#pragma unroll
+        for (int j = 0; j < kMaxCandidates; ++j) {
+            const float sj = __shfl_sync(gmask, my_sep, j, 16);
+            const unsigned fj = __shfl_sync(gmask, my_fa, j, 16);
+            const unsigned gj = __shfl_sync(gmask, my_fb, j, 16);
+            if (j < nc && sl < nc && j != sl) {
+                const bool less = sj < my_sep || (sj == my_sep && (fj < my_fa || (fj == my_fa && gj < my_fb)));
+                rank += less ? 1 : 0;
+            }
+        }
+        unsigned long long order = 0ull;  // candidate lane of each rank
+#pragma unroll
+        for (int i = 0; i < kMaxCandidates; ++i) {
+            const unsigned who = group_ballot(gmask, gbase, sl < nc && rank == i);
+            if (i < nc) order |= static_cast<unsigned long long>(__ffs(who) - 1) << (4 * i);
+        }
+        const int c0 = static_cast<int>(order & 0xfull);
+        unsigned selected = 1u << c0;
+        unsigned long long chosen = static_cast<unsigned long long>(c0);
+        int chosen_count = 1;
+        const float3 w0 = shfl3g(my_wp, c0, gmask);
+        float3 w1 = w0, w2 = w0;
+        for (int stage = 1; stage < kManifoldPoints; ++stage) {
+            float score;
+            if (stage == 1) {
+                const float3 dl = my_wp - w0;
+                const float3 t = dl - nw * dot3(dl, nw);
+                score = dot3(t, t);
+            } else if (stage == 2) {
+                score = fabsf(dot3(cross3(w1 - w0, my_wp - w0), nw));
+            } else {
+                score = INFINITY;
+                const float3 ws[3] = {w0, w1, w2};
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const float3 dl = my_wp - ws[k];
+                    const float3 t = dl - nw * dot3(dl, nw);
+                    score = fminf(score, dot3(t, t));
+                }
+            }
+            int best = -1;
+            float best_score = -1.0f;
+            unsigned long long best_feature = ~0ull;
+#pragma unroll
+            for (int i = 0; i < kMaxCandidates; ++i) {
+                const int k = static_cast<int>((order >> (4 * i)) & 0xfull);
+                const float sc = __shfl_sync(gmask, score, k, 16);
+                const unsigned fk = __shfl_sync(gmask, my_fa, k, 16);
+                const unsigned gk = __shfl_sync(gmask, my_fb, k, 16);
+                if (i >= nc || (selected & (1u << k))) continue;
+                const unsigned long long f = (static_cast<unsigned long long>(fk) << 32) | gk;
+                const float tol = fmaxf(kTieAbsolute, kTieRelative * fmaxf(fabsf(sc), fabsf(best_score)));
+                if (sc > best_score + tol || (fabsf(sc - best_score) <= tol && f < best_feature)) {
+                    best = k;
+                    best_score = sc;
+                    best_feature = f;
+                }
+            }
+            if (best >= 0) {
+                selected |= 1u << best;
+                chosen |= static_cast<unsigned long long>(best) << (4 * chosen_count);
+                ++chosen_count;
+                if (stage == 1) w1 = shfl3g(my_wp, best, gmask);
+                if (stage == 2) w2 = shfl3g(my_wp, best, gmask);
+            }
+        }
+        // Chosen candidates in feature order.
+        unsigned long long keys[kManifoldPoints];
+        int lanes[kManifoldPoints];
+#pragma unroll
+        for (int i = 0; i < kManifoldPoints; ++i) {
+            const int k = static_cast<int>((chosen >> (4 * i)) & 0xfull);
+            const unsigned fk = __shfl_sync(gmask, my_fa, k, 16);
+            const unsigned gk = __shfl_sync(gmask, my_fb, k, 16);
+            keys[i] = i < chosen_count ? ((static_cast<unsigned long long>(fk) << 32) | gk) : ~0ull;
+            lanes[i] = k;
+        }
+#pragma unroll
+        for (int i = 1; i < kManifoldPoints; ++i)
+#pragma unroll
+            for (int j = i; j > 0; --j)
+                if (keys[j] < keys[j - 1]) {
+                    const unsigned long long tk = keys[j]; keys[j] = keys[j - 1]; keys[j - 1] = tk;
+                    const int tl = lanes[j]; lanes[j] = lanes[j - 1]; lanes[j - 1] = tl;
+                }
+#pragma unroll
+        for (int i = 0; i < kManifoldPoints; ++i) final_order |= static_cast<unsigned long long>(lanes[i]) << (4 * i);
+        nfinal = chosen_count;
+    } else {
+        // Canonical order of all candidates by feature key.
+        int rank = 0;
+#pragma unroll
+        for (int j = 0; j < kManifoldPoints; ++j) {
+            const unsigned fj = __shfl_sync(gmask, my_fa, j, 16);
+            const unsigned gj = __shfl_sync(gmask, my_fb, j, 16);
+            if (j < nc && sl < nc && j != sl && (fj < my_fa || (fj == my_fa && gj < my_fb))) ++rank;
+        }
+#pragma unroll
+        for (int i = 0; i < kManifoldPoints; ++i) {
+            const unsigned who = group_ballot(gmask, gbase, sl < nc && rank == i);
+            if (i < nc) final_order |= static_cast<unsigned long long>(__ffs(who) - 1) << (4 * i);
+        }
+        nfinal = nc;
+    }
+    // Write the slot: lane i < 4 writes point i, lane 0 the header.
+    const int src = sl < nfinal ? static_cast<int>((final_order >> (4 * (sl & 3))) & 0xfull) : 0;
+    const unsigned id = __shfl_sync(gmask, my_id, src, 16);
+    __syncwarp(gmask);
+    if (sl < kManifoldPoints) {
+        float* op = slot + 8 + sl * 12;
+        if (sl < nfinal) {
+            const float* g = scratch + (id & 15u) * kCandidateWords;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) op[k] = g[k];
+            if ((id >> 4) == kFresh) {
+                op[8] = as_float(0);
+                op[9] = op[10] = op[11] = 0.0f;
+            } else {
+                const float* hrec = scratch + (id >> 4) * kCandidateWords;
+                op[8] = hrec[kCdLife];
+                op[9] = hrec[kCdImp + 0];
+                op[10] = hrec[kCdImp + 1];
+                op[11] = hrec[kCdImp + 2];
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 12; ++k) op[k] = 0.0f;
+        }
+    }
+    if (sl == 0) {
+        float3 tw = transported;
+        if (!old_ok || !finite3(tw) || dot3(tw, tw) <= 1.0e-12f) tw = stable_tangent(nw);
+        else tw = tw * (1.0f / len3(tw));
+        st3(slot, qrotinv(rotA, nw));
+        slot[3] = old_ok ? fminf(old_age + 1.0f, 65535.0f) : 0.0f;
+        st3(slot + 4, qrotinv(rotA, tw));
+        slot[7] = as_float(nfinal);
+    }
+    __syncwarp(gmask);
+    npoints_out = nfinal;
+}
+
 __device__ __forceinline__ float3 project_cone(float3 imp, float mu_u, float mu_v) {
     float3 p = imp;
     p.x = fmaxf(p.x, 0.0f);
@@ -1071,7 +1413,8 @@ __device__ bool invert3x3_reg(const float m[3][3], float inv[3][3]) {
 // Contact substep after the ABA: collision, ConstraintIR evaluation, joint
 // inertia factor, temporalCone solve, joint limits, integration.
 // ---------------------------------------------------------------------------
-__device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState& st, bool final_substep,
+template <typename R>
+__device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState<R>& st, bool final_substep,
                                 int velocity_iterations, int final_iterations, float friction_scale) {
     const DeviceModel& M = *w.M;
     const DeviceTables& T = *w.T;
@@ -1119,10 +1462,41 @@ __device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState& s
         const int t = __shfl_up_sync(0xffffffffu, scratch_end, o);
         if (lane >= o) scratch_end += t;
     }
-    if (lane < M.np) {
+    // Light pair classes (at most two raw contacts): one lane per pair.
+    const bool heavy = lane < M.np && pair_max_raw(M.pair_class[lane]) > 2;
+    const unsigned heavy_mask = __ballot_sync(0xffffffffu, heavy);
+    if (lane < M.np && !heavy) {
         npoints = pair_manifold(M, pose, margins, lane, slots + lane * kSlotStride, s + L.narrow + scratch_end - my_words,
                                 nraw, cand);
         if (npoints < 0) { pair_fail = true; npoints = 0; }
+    }
+    // Heavy pair classes: a 16-lane group per pair, two pairs at a time.
+    if (heavy_mask != 0u) {
+        float* pstats = s + L.pair_stats;
+        const int g = lane >> 4, sl = lane & 15, gbase = lane & 16;
+        const unsigned gmask = g ? 0xffff0000u : 0x0000ffffu;
+        const int nheavy = __popc(heavy_mask);
+        for (int first = 0; first < nheavy; first += 2) {
+            unsigned m = heavy_mask;
+            for (int k = 0; k < first + g && m != 0u; ++k) m &= m - 1u;
+            const int pair = m != 0u ? __ffs(m) - 1 : -1;
+            const int off = __shfl_sync(0xffffffffu, scratch_end - my_words, pair >= 0 ? pair : 0);
+            if (pair >= 0) {
+                int gp = 0, gr = 0;
+                bool gc = false, gf = false;
+                group_manifold(M, pose, margins, pair, slots + pair * kSlotStride, s + L.narrow + off, sl, gbase, gmask, gp,
+                               gr, gc, gf);
+                if (sl == 0) pstats[pair] = as_float(gp | (gr << 8) | (gc ? 1 << 16 : 0) | (gf ? 1 << 17 : 0));
+            }
+        }
+        __syncwarp();
+        if (heavy) {
+            const int packed = as_int(pstats[lane]);
+            npoints = packed & 0xff;
+            nraw = (packed >> 8) & 0xff;
+            cand = (packed >> 16) & 1;
+            pair_fail = (packed >> 17) & 1;
+        }
     }
     const unsigned fail_mask = __ballot_sync(0xffffffffu, pair_fail);
     if (fail_mask != 0u) {
@@ -1285,12 +1659,38 @@ __device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState& s
             const int b = as_int(C[c * kContactWords + kCwBody]);
             const int na = T.anc_count[b];
             float* y = Y + c * 3 * ma + r * ma;
-            for (int t = na - 1; t >= 0; --t) {
-                const int k = T.anc[b][t];
-                const float* rowk = Lm + k * (k + 1) / 2;
-                const float yt = y[t] / rowk[k];
-                y[t] = yt;
-                for (int u = 0; u < t; ++u) y[u] -= rowk[T.anc[b][u]] * yt;
+            if (na <= kRegisterChain) {
+                // Register-resident back substitution for chains of up to 16
+                // ancestor DoFs (fully unrolled, predicated on the length).
+                float yr[kRegisterChain];
+                int off[kRegisterChain];
+#pragma unroll
+                for (int t = 0; t < kRegisterChain; ++t) {
+                    const int k = t < na ? T.anc[b][t] : 0;
+                    off[t] = k * (k + 1) / 2;
+                    yr[t] = t < na ? y[t] : 0.0f;
+                }
+#pragma unroll
+                for (int t = kRegisterChain - 1; t >= 0; --t) {
+                    if (t < na) {
+                        const float* rowk = Lm + off[t];
+                        const float yt = yr[t] / rowk[T.anc[b][t]];
+                        yr[t] = yt;
+#pragma unroll
+                        for (int u = 0; u < t; ++u) yr[u] -= rowk[T.anc[b][u]] * yt;
+                    }
+                }
+#pragma unroll
+                for (int t = 0; t < kRegisterChain; ++t)
+                    if (t < na) y[t] = yr[t];
+            } else {
+                for (int t = na - 1; t >= 0; --t) {
+                    const int k = T.anc[b][t];
+                    const float* rowk = Lm + k * (k + 1) / 2;
+                    const float yt = y[t] / rowk[k];
+                    y[t] = yt;
+                    for (int u = 0; u < t; ++u) y[u] -= rowk[T.anc[b][u]] * yt;
+                }
             }
         }
         __syncwarp();
@@ -1443,9 +1843,9 @@ __device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState& s
                     dv = pv + cross3(pw, st.r);
                     if (bc.dof >= 0) {
                         const int k = bc.dof;
-                        const float lkk = sqrtf(st.D);  // = L_kk as written by the ABA
-                        const float sum = st.U[0] * dw.x + st.U[1] * dw.y + st.U[2] * dw.z + st.U[3] * dv.x +
-                                          st.U[4] * dv.y + st.U[5] * dv.z;
+                        const float lkk = static_cast<float>(sqrt(st.D));  // = L_kk as written by the ABA
+                        const float sum = static_cast<float>(st.U[0] * dw.x + st.U[1] * dw.y + st.U[2] * dw.z +
+                                                             st.U[3] * dv.x + st.U[4] * dv.y + st.U[5] * dv.z);
                         const float xk = (z[k] - sum / lkk) / lkk;
                         v[k] += xk;
                         dw = dw + f3(st.s[0], st.s[1], st.s[2]) * xk;
@@ -1506,8 +1906,8 @@ __device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState& s
     return warp_ok(misc);
 }
 
-template <bool kContact>
-__global__ void __launch_bounds__(128) control_step_kernel(StepParams p, WarpLayout layout, int warps_per_block) {
+template <bool kContact, typename R>
+__global__ void __launch_bounds__(128, 3) control_step_kernel(StepParams p, WarpLayout layout, int warps_per_block) {
     extern __shared__ float4 smem4[];
     // Topology tables: one copy per CTA.
     {
@@ -1564,7 +1964,7 @@ __global__ void __launch_bounds__(128) control_step_kernel(StepParams p, WarpLay
     const float friction_scale = kContact ? p.friction_scale[env] : 1.0f;
     BodyConst bc;
     if (lane < M.nb) load_body(M, lane, bc);
-    BodyState st;
+    BodyState<R> st;
     __syncwarp();
 
     for (int sub = 0; sub < p.substeps; ++sub) {
@@ -1631,30 +2031,43 @@ __global__ void __launch_bounds__(128) control_step_kernel(StepParams p, WarpLay
 size_t control_step_table_bytes() { return sizeof(DeviceTables); }
 
 // Host launcher: one control step of `env_count` environments.
-cudaError_t launch_control_step(const StepParams& p, const WarpLayout& layout, bool contact, int warps_per_block,
-                                cudaStream_t stream) {
+// `fp64_inertia` selects the FP64 articulated-inertia kernels.
+cudaError_t launch_control_step(const StepParams& p, const WarpLayout& layout, bool contact, bool fp64_inertia,
+                                int warps_per_block, cudaStream_t stream) {
     const int blocks = (p.env_count + warps_per_block - 1) / warps_per_block;
     const size_t smem = sizeof(DeviceTables) + static_cast<size_t>(layout.total) * sizeof(float) * warps_per_block;
+    const int threads = 32 * warps_per_block;
     if (contact) {
-        control_step_kernel<true><<<blocks, 32 * warps_per_block, smem, stream>>>(p, layout, warps_per_block);
+        if (fp64_inertia) control_step_kernel<true, double><<<blocks, threads, smem, stream>>>(p, layout, warps_per_block);
+        else control_step_kernel<true, float><<<blocks, threads, smem, stream>>>(p, layout, warps_per_block);
     } else {
-        control_step_kernel<false><<<blocks, 32 * warps_per_block, smem, stream>>>(p, layout, warps_per_block);
+        if (fp64_inertia) control_step_kernel<false, double><<<blocks, threads, smem, stream>>>(p, layout, warps_per_block);
+        else control_step_kernel<false, float><<<blocks, threads, smem, stream>>>(p, layout, warps_per_block);
     }
     return cudaGetLastError();
 }
 
-cudaError_t control_step_occupancy(bool contact, int warps_per_block, size_t smem, int* blocks_per_sm) {
+cudaError_t control_step_occupancy(bool contact, bool fp64_inertia, int warps_per_block, size_t smem, int* blocks_per_sm) {
+    const int threads = 32 * warps_per_block;
     if (contact)
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, control_step_kernel<true>, 32 * warps_per_block, smem);
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, control_step_kernel<false>, 32 * warps_per_block, smem);
+        return fp64_inertia
+                   ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, control_step_kernel<true, double>, threads, smem)
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, control_step_kernel<true, float>, threads, smem);
+    return fp64_inertia
+               ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, control_step_kernel<false, double>, threads, smem)
+               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, control_step_kernel<false, float>, threads, smem);
 }
 
 cudaError_t configure_control_step_kernels(size_t max_dynamic_smem) {
-    cudaError_t e = cudaFuncSetAttribute(control_step_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(max_dynamic_smem));
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(control_step_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(max_dynamic_smem));
+    const int bytes = static_cast<int>(max_dynamic_smem);
+    cudaError_t e = cudaFuncSetAttribute(control_step_kernel<true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(control_step_kernel<true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(control_step_kernel<false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(control_step_kernel<false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return e;
 }
 
 }  // namespace numi

@@ -23,6 +23,9 @@ MR_INVALID_INDEX: Final = 0xFFFFFFFF
 MR_RUN_SOURCE_SYNTHETIC_CHAIN7: Final = 100
 MR_RUN_SOURCE_SYNTHETIC_TREE29: Final = 101
 MANIFOLD_POINTS: Final = 4
+MR_PRECISION_FP32: Final = 0
+MR_PRECISION_FP64_ARTICULATED_INERTIA: Final = 1
+PRECISION_MODES: Final = {"fp32": MR_PRECISION_FP32, "fp64-inertia": MR_PRECISION_FP64_ARTICULATED_INERTIA}
 
 STATUS_NAMES: Final = {
     0: "success",
@@ -315,6 +318,7 @@ EXPORTED_SYMBOLS: Final = (
     "mr_task_rollout_copy_environment_parameters",
     "mr_task_rollout_copy_state",
     "mr_task_rollout_set_state",
+    "mr_task_rollout_set_precision",
 )
 
 
@@ -362,6 +366,8 @@ class Bindings:
         L.mr_task_rollout_reset.restype = ct.c_int
         L.mr_task_rollout_set_state_readback.argtypes = [ct.c_void_p, ct.c_uint32]
         L.mr_task_rollout_set_state_readback.restype = ct.c_int
+        L.mr_task_rollout_set_precision.argtypes = [ct.c_void_p, ct.c_uint32]
+        L.mr_task_rollout_set_precision.restype = ct.c_int
         L.mr_task_rollout_advance.argtypes = [
             ct.c_void_p,
             P(ct.c_float),

@@ -131,9 +131,12 @@ class World:
         final_velocity_iterations: int = 0,
         control_dt: float = 0.02,
         seed: int = 0,
+        precision: str = "fp32",
         library: native.Bindings | None = None,
     ) -> None:
         self._lib = library or native.bindings()
+        if precision not in native.PRECISION_MODES:
+            raise ValueError(f"precision must be one of {sorted(native.PRECISION_MODES)}")
         self.source = _source_id(source)
         manifest = native.default_manifest(
             self.source,
@@ -159,6 +162,16 @@ class World:
         model = native.ModelViewC()
         self._lib.check(self._lib.lib.mr_task_rollout_copy_model(self._handle, ct.byref(model)), "copy_model")
         self.pair_count = int(model.world.pair_count)
+        self.set_precision(precision)
+
+    def set_precision(self, precision: str) -> None:
+        """"fp32" (reference precision) or "fp64-inertia" (FP64 articulated inertia)."""
+
+        if precision not in native.PRECISION_MODES:
+            raise ValueError(f"precision must be one of {sorted(native.PRECISION_MODES)}")
+        self._lib.check(self._lib.lib.mr_task_rollout_set_precision(self._handle, native.PRECISION_MODES[precision]),
+                        "set_precision")
+        self.precision = precision
 
     # -- lifecycle -------------------------------------------------------
     def close(self) -> None:

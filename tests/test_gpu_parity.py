@@ -3,7 +3,8 @@ FP32 input state (the CUDA path runs through the C ABI).
 
 Tolerances, per control step, relative to max(1, |x|) of the oracle state:
 
-* chain7 (no contact): q and qd within 1e-5.
+* chain7 (no contact): q within 1e-5; qd within 1e-5 with FP64
+  articulated inertias and 5e-5 in the all-FP32 mode (see CHAIN_V_TOL).
 * tree29 (contact): q within 1e-5; qd and impulses within 1e-5 / 1e-4 at
   the median and within 2e-4 / 1e-3 at the worst env-step.  The worst case
   is set by the problem's FP32 conditioning, not by the kernel: the FP64
@@ -50,11 +51,19 @@ def _oracle_features(man, pairs: int) -> list[tuple[int, tuple[int, ...]]]:
     return [(int(man[p].count), tuple(int(man[p].points[i].feature_a) for i in range(man[p].count))) for p in range(pairs)]
 
 
-def test_chain7_free_motion_per_step(cuda_device):
+# FP32 articulated inertia: rounding the shifted child inertias to FP32
+# alone moves the FP64 oracle's joint velocities by up to ~3e-5 relative on
+# this chain (parallel-axis terms dwarf the distal pivots), so the FP32 mode
+# is held to 5e-5 and the FP64 articulated-inertia mode to 1e-5.
+CHAIN_V_TOL = {"fp32": 5e-5, "fp64-inertia": 1e-5}
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64-inertia"])
+def test_chain7_free_motion_per_step(cuda_device, precision):
     import torch
 
     envs, steps, dt = 64, 25, 0.005
-    with nb.World("chain7", envs, substeps=1, control_dt=dt, seed=3) as world:
+    with nb.World("chain7", envs, substeps=1, control_dt=dt, seed=3, precision=precision) as world:
         oracle = Oracle(world.model(), dt, 1, 0, 0)
         gen = torch.Generator(device="cuda").manual_seed(11)
         worst_q = worst_v = 0.0
@@ -72,19 +81,22 @@ def test_chain7_free_motion_per_step(cuda_device):
                 assert st == 0
                 worst_q = max(worst_q, _rel_err(q1[e], q))
                 worst_v = max(worst_v, _rel_err(v1[e], v))
+        print(f"chain7 {precision}: worst q {worst_q:.2e} qd {worst_v:.2e}")
         assert worst_q <= Q_TOL, worst_q
-        assert worst_v <= V_TOL, worst_v
+        assert worst_v <= CHAIN_V_TOL[precision], worst_v
 
 
-def _tree_world(envs: int, seed: int = 5):
-    return nb.World("tree29", envs, substeps=4, velocity_iterations=8, final_velocity_iterations=0, control_dt=0.02, seed=seed)
+def _tree_world(envs: int, seed: int = 5, precision: str = "fp32"):
+    return nb.World("tree29", envs, substeps=4, velocity_iterations=8, final_velocity_iterations=0, control_dt=0.02, seed=seed,
+                    precision=precision)
 
 
-def test_tree29_contact_per_step(cuda_device):
+@pytest.mark.parametrize("precision", ["fp32", "fp64-inertia"])
+def test_tree29_contact_per_step(cuda_device, precision):
     import torch
 
     envs, warm, steps = 32, 20, 12
-    with _tree_world(envs) as world:
+    with _tree_world(envs, precision=precision) as world:
         oracle = Oracle(world.model(), 0.005, 4, 8, 0)
         friction = world.friction_scales()
         gen = torch.Generator(device="cuda").manual_seed(21)
@@ -142,7 +154,7 @@ def test_tree29_contact_per_step(cuda_device):
         assert band_cases <= envs * steps // 20, f"{band_cases} band cases"
         med_v = float(np.median(errs["v"]))
         med_imp = float(np.median(errs["imp"]))
-        print(f"tree29 per-step parity: worst={worst} median v={med_v:.2e} imp={med_imp:.2e} "
+        print(f"tree29 {precision} per-step parity: worst={worst} median v={med_v:.2e} imp={med_imp:.2e} "
               f"contacts={contacts_seen} band_cases={band_cases}")
         assert worst["q"] <= Q_TOL, worst
         assert med_v <= V_TOL, med_v
