@@ -43,9 +43,9 @@ constexpr float kQueryPad = 0.00000762939453125f;  // MR_COLLISION_QUERY_RELATIV
 constexpr float kAabbPad = 0.00000762939453125f;   // MR_COLLISION_AABB_RELATIVE_PAD
 constexpr unsigned char kNone = 255;
 constexpr int kMaxRawPerPair = 8;
-constexpr int kRootFactorWords = 24;
-constexpr int kRegisterChain = 16;   // longest ancestor chain solved in registers
-constexpr int kMaxCandidates = 4 + kMaxRawPerPair;  // manifold candidates of one pair  // rows 0-5 of the factor (21 words), padded
+constexpr int kRootFactorWords = 24;  // rows 0-5 of the factor (21 words), padded
+constexpr int kRegisterChain = 16;    // longest ancestor chain solved in registers
+constexpr int kMaxCandidates = 4 + kMaxRawPerPair;  // manifold candidates of one pair
 constexpr float kTieRelative = 1.0e-5f;  // manifold reduction ties
 constexpr float kTieAbsolute = 1.0e-12f;
 
