@@ -221,6 +221,79 @@ def run_reference_arm(args, rank: int) -> None:
     print(json.dumps(line))
 
 
+def plain_aba_chain7(device) -> dict:
+    """BASELINE's plain-ABA configuration: 1024 envs of the 7-revolute chain,
+    tau ~ N(0, 5), dt = 5 ms, 1000 steps (one advance), device-resident."""
+
+    import torch
+
+    import numi_lab_b200 as nb
+
+    envs, steps = 1024, 1000
+    with nb.World("chain7", envs, substeps=1, control_dt=0.005, seed=SEED) as world:
+        gen = torch.Generator(device=device).manual_seed(SEED)
+        acts = 5.0 * torch.randn((steps, envs, world.action_count), device=device, generator=gen)
+        status = torch.empty((steps, envs), device=device, dtype=torch.int32)
+        obs = torch.empty((steps, envs, world.observation_count), device=device)
+        for _ in range(3):
+            world.reset(SEED)
+            world.step(acts, observations=obs, status=status, wait=True)
+        world.reset(SEED)
+        torch.cuda.synchronize(device)
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        world.step(acts, observations=obs, status=status)
+        stop.record()
+        torch.cuda.synchronize(device)
+        ms = start.elapsed_time(stop)
+        failed = int((status != 0).sum().item())
+    return {
+        "value": envs * steps / (ms / 1e3),
+        "unit": UNIT,
+        "config": "chain7: 1024 envs, 1000 steps of 5 ms, tau ~ N(0, 5), FP32, one CUDA-graph advance",
+        "ms": ms,
+        "failed_env_steps": failed,
+        "note": "failed env-steps are the chain's own energy blow-up under this torque scale (latched, state kept)",
+    }
+
+
+def run_serving(args) -> None:
+    """Poisson request stream (BASELINE's serving configuration, chain and
+    tree worlds) against the continuous-batching server; latency percentiles
+    at the configured rate plus a sustainable-rate sweep."""
+
+    import torch
+
+    import numi_lab_b200 as nb
+    from numi_lab_b200.serve import poisson_requests, serve_arrivals
+
+    torch.cuda.set_device(0)
+    results = {}
+    for rate, window in ((2000.0, 1.0), (400.0, 2.0), (100.0, 2.0), (25.0, 2.0)):
+        with nb.Server(hbm_budget_bytes=120 * 10**9, model_seed=SEED, max_envs_per_source=16384) as server:
+            reqs = poisson_requests(rate, window, seed=SEED + int(rate))
+            results[str(int(rate))] = serve_arrivals(server, reqs, drain=True, time_limit_s=300.0)
+    head = results["2000"]
+    line = {
+        "metric": "served env-steps/s and request latency (Poisson arrivals)",
+        "value": head["env_steps_per_s"],
+        "unit": UNIT,
+        "latency_p50_s": head["latency_p50_s"],
+        "latency_p99_s": head["latency_p99_s"],
+        "queue_p50_s": head["queue_p50_s"],
+        "queue_p99_s": head["queue_p99_s"],
+        "higher_is_better": True,
+        "config": {"workload": "Poisson arrivals 2000 req/s for 1 s, worlds chain7 | tree29, envs log-uniform 1-512, "
+                               "horizon U(10, 500), actions N(0, 0.3), 120 GB HBM budget, drained",
+                   "rate_sweep_req_per_s": {k: {kk: v[kk] for kk in ("env_steps_per_s", "latency_p50_s", "latency_p99_s",
+                                                                       "queue_p99_s", "completed")}
+                                            for k, v in results.items()}},
+        "data": "synthetic (seeded)",
+        "dtype": "f32",
+    }
+    print(json.dumps(line))
+
+
 def main() -> None:
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
@@ -228,6 +301,8 @@ def main() -> None:
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", default="native", choices=["native", "reference"])
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--serve", action="store_true",
+                        help="serving workload: Poisson request stream, latency percentiles (one JSON line)")
     args = parser.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -238,6 +313,10 @@ def main() -> None:
 
     if args.impl == "reference":
         run_reference_arm(args, rank)
+        return
+    if args.serve:
+        if rank == 0:
+            run_serving(args)
         return
 
     import torch
@@ -333,6 +412,8 @@ def main() -> None:
     peaks = _measured_peaks()
     traffic = _profile_traffic()
 
+    plain = plain_aba_chain7(device) if rank == 0 else None
+
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         try:
@@ -378,6 +459,7 @@ def main() -> None:
             "failed_env_steps": failures,
             "mean_active_contacts": mean_points,
             "mean_manifolds": mean_manifolds,
+            "plain_aba_chain7": plain,
         }
         print(json.dumps(line))
     world.close()

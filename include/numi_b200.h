@@ -508,6 +508,74 @@ MR_API int mr_task_rollout_set_state(
     MRTaskRolloutHandle* handle, const float* q, const float* v,
     const MRManifoldC* manifolds, uint32_t as_reset_state);
 
+/* ---------------------------------------------------------------------- */
+/* Continuous-batching rollout server (no counterpart in the reference)   */
+/* ---------------------------------------------------------------------- */
+
+/* Requests of differing worlds, env counts and horizons are admitted into
+ * resident environment slots as slots and the HBM budget allow, packed with
+ * the requests already running into one control-step launch per world per
+ * tick, and retired when their horizon completes.  An environment's result
+ * depends only on its request (world, seed, env index, actions). */
+typedef struct MRServerHandle MRServerHandle;
+
+typedef struct MRServerConfigC {
+    uint64_t hbm_budget_bytes;         /* slots + request actions              */
+    uint64_t model_seed;               /* seed of the synthetic worlds         */
+    uint32_t physics_substeps;
+    uint32_t velocity_iterations;
+    uint32_t final_velocity_iterations;
+    float control_timestep_seconds;
+    uint32_t max_envs_per_source;      /* slot pool size per world source      */
+    uint32_t reserved;
+} MRServerConfigC;
+
+typedef struct MRServerRequestC {
+    uint32_t source;                   /* MR_RUN_SOURCE_SYNTHETIC_*            */
+    uint32_t env_count;
+    uint32_t horizon;                  /* control steps                        */
+    uint32_t reserved;
+    uint64_t seed;                     /* reset sampling of the request's envs */
+    const float* actions;              /* host [horizon][env][action], copied  */
+} MRServerRequestC;
+
+typedef struct MRServerCompletionC {
+    uint64_t request_id;
+    uint32_t source;
+    uint32_t env_count;
+    uint32_t horizon;
+    uint32_t failed_env_steps;
+    uint32_t first_failure_status;
+    uint32_t reserved;
+    double queue_seconds;              /* submit -> admission                  */
+    double latency_seconds;            /* submit -> final state on the host    */
+} MRServerCompletionC;
+
+typedef struct MRServerStatsC {
+    uint32_t pending_requests;
+    uint32_t running_requests;
+    uint32_t free_slots;
+    uint32_t reserved;
+    uint64_t completed_env_steps;
+    uint64_t hbm_bytes_in_use;
+} MRServerStatsC;
+
+MR_API MRServerHandle* mr_create_server(const MRServerConfigC* config);
+MR_API void mr_server_destroy(MRServerHandle* server);
+/* Slot-pool size and action width of a world source. */
+MR_API int mr_server_capacity(const MRServerHandle* server, uint32_t source, uint32_t* slots, uint32_t* action_count);
+MR_API int mr_server_submit(MRServerHandle* server, const MRServerRequestC* request, uint64_t* request_id);
+/* Admits waiting requests, advances every admitted request by one control
+ * step and retires the finished ones; returns the work of this tick. */
+MR_API int mr_server_tick(MRServerHandle* server, uint32_t* active_requests, uint32_t* active_envs);
+/* Completions not reported yet, oldest first. */
+MR_API int mr_server_poll(MRServerHandle* server, MRServerCompletionC* out, uint32_t capacity, uint32_t* count);
+/* Final q [env][nq] and v [env][nv] of a completed request (kept until released). */
+MR_API int mr_server_copy_result(const MRServerHandle* server, uint64_t request_id, float* q, size_t q_count, float* v,
+                                 size_t v_count);
+MR_API int mr_server_release(MRServerHandle* server, uint64_t request_id);
+MR_API int mr_server_stats(const MRServerHandle* server, MRServerStatsC* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -135,11 +135,13 @@ struct StepParams {
     const float* reset_q;          // [env][nq]
     const float* reset_v;          // [env][nv]
     const float* friction_scale;   // [env]
-    const float* actions;          // [env][action_count] of this control step
-    const std::uint32_t* reset_masks;  // [env] of this control step, or null
-    float* observations;           // [env][nq+nv] of this control step, or null
-    std::uint32_t* status_codes;   // [env] of this control step, or null
-    std::uint32_t* active_contacts;// [env] of this control step, or null
+    const float* actions;          // [item][action_count] of this control step
+    const float* const* action_rows;   // per item: its action row, or null (use `actions`)
+    const std::int32_t* env_index;     // per item: resident environment slot, or null (item = slot)
+    const std::uint32_t* reset_masks;  // [item] of this control step, or null
+    float* observations;           // [item][nq+nv] of this control step, or null
+    std::uint32_t* status_codes;   // [item] of this control step, or null
+    std::uint32_t* active_contacts;// [item] of this control step, or null
     std::uint32_t* stats;          // per-launch counters (see kStat*)
     std::int32_t env_count;
     std::int32_t substeps;

@@ -11,6 +11,7 @@
 #include "layout.h"
 #include "model.h"
 #include "numi_b200.h"
+#include "runtime.h"
 
 #include <cuda_runtime.h>
 
@@ -25,55 +26,21 @@
 #include <string>
 #include <vector>
 
-namespace numi {
-cudaError_t control_step_occupancy(bool contact, bool fp64_inertia, int warps_per_block, size_t smem, int* blocks_per_sm);
-cudaError_t launch_control_step(const StepParams& p, const WarpLayout& layout, bool contact, bool fp64_inertia, int warps_per_block,
-                                cudaStream_t stream);
-cudaError_t configure_control_step_kernels(size_t max_dynamic_smem);
-size_t control_step_table_bytes();
-}  // namespace numi
-
 namespace {
+
+using numi::rt::check;
+using numi::rt::DeviceBuffer;
+using numi::rt::PinnedBuffer;
+using numi::rt::guarded;
 
 thread_local std::string g_last_error;
 
-void check(cudaError_t e, const char* what) {
-    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
-}
+}  // namespace
 
-template <typename T>
-struct DeviceBuffer {
-    T* ptr = nullptr;
-    size_t count = 0;
-    DeviceBuffer() = default;
-    DeviceBuffer(const DeviceBuffer&) = delete;
-    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
-    ~DeviceBuffer() { if (ptr) cudaFree(ptr); }
-    void resize(size_t n) {
-        if (n <= count && ptr) return;
-        if (ptr) { cudaFree(ptr); ptr = nullptr; }
-        check(cudaMalloc(&ptr, std::max<size_t>(n, 1) * sizeof(T)), "cudaMalloc");
-        count = n;
-    }
-};
+void numi::rt::set_last_error(const std::string& message) { g_last_error = message; }
+const char* numi::rt::last_error() { return g_last_error.c_str(); }
 
-template <typename T>
-struct PinnedBuffer {
-    T* ptr = nullptr;
-    size_t count = 0;
-    PinnedBuffer() = default;
-    PinnedBuffer(const PinnedBuffer&) = delete;
-    PinnedBuffer& operator=(const PinnedBuffer&) = delete;
-    ~PinnedBuffer() { if (ptr) cudaFreeHost(ptr); }
-    void resize(size_t n) {
-        if (n <= count && ptr) return;
-        if (ptr) { cudaFreeHost(ptr); ptr = nullptr; }
-        check(cudaMallocHost(&ptr, std::max<size_t>(n, 1) * sizeof(T)), "cudaMallocHost");
-        count = n;
-    }
-};
-
-numi::DeviceModel pack_model(const numi::CompiledModel& m, float h) {
+numi::DeviceModel numi::rt::pack_model(const numi::CompiledModel& m, float h) {
     using namespace numi;
     DeviceModel d{};
     std::memset(&d, 0, sizeof(d));
@@ -285,7 +252,41 @@ numi::DeviceModel pack_model(const numi::CompiledModel& m, float h) {
     return d;
 }
 
-}  // namespace
+void numi::rt::make_plan(const numi::CompiledModel& m, float h, KernelPlan& plan) {
+    plan.contact = m.world.pair_count > 0;
+    plan.dmodel = pack_model(m, h);
+    int narrow_words = 0;
+    for (const MRModelPairC& pr : m.pairs) narrow_words += numi::pair_scratch_words(numi::pair_max_raw(static_cast<int>(pr.pair_class)));
+    plan.layout = numi::make_layout(static_cast<int>(m.articulated_body_count), static_cast<int>(m.world.nv),
+                                    static_cast<int>(m.world.nq), static_cast<int>(m.world.pair_count),
+                                    static_cast<int>(m.world.contact_capacity), static_cast<int>(m.max_ancestor_dofs),
+                                    narrow_words, plan.contact);
+    int device = 0;
+    check(cudaGetDevice(&device), "cudaGetDevice");
+    cudaDeviceProp prop{};
+    check(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+    const size_t per_warp = static_cast<size_t>(plan.layout.total) * sizeof(float);
+    const size_t tables = numi::control_step_table_bytes();
+    const size_t limit = prop.sharedMemPerBlockOptin;
+    if (tables + per_warp > limit) throw std::runtime_error("per-environment shared memory exceeds the device limit");
+    check(numi::configure_control_step_kernels(limit), "kernel attributes");
+    // Environments per CTA: the choice that keeps the most warps resident
+    // per SM under the kernel's register and shared-memory footprint (each
+    // CTA carries one copy of the topology tables).
+    for (int prec = 0; prec < 2; ++prec) {
+        int best = 1, best_warps = 0;
+        for (int wpb = 1; wpb <= 4; wpb *= 2) {
+            const size_t smem = tables + wpb * per_warp;
+            if (smem > limit) break;
+            int blocks = 0;
+            check(numi::control_step_occupancy(plan.contact, prec == 1, wpb, smem, &blocks), "occupancy query");
+            if (blocks * wpb > best_warps) { best_warps = blocks * wpb; best = wpb; }
+        }
+        if (best_warps == 0) throw std::runtime_error("the control-step kernel cannot be resident with this model");
+        plan.warps_per_block[prec] = best;
+        plan.resident_warps_per_sm[prec] = best_warps;
+    }
+}
 
 struct MRTaskRolloutHandle {
     numi::CompiledModel model;
@@ -470,22 +471,6 @@ struct MRTaskRolloutHandle {
     }
 };
 
-namespace {
-
-template <typename F>
-int guarded(F&& f) {
-    try {
-        f();
-        return 0;
-    } catch (const std::exception& e) {
-        g_last_error = e.what();
-    } catch (...) {
-        g_last_error = "unknown native error";
-    }
-    return -1;
-}
-
-}  // namespace
 
 extern "C" {
 
@@ -501,7 +486,7 @@ MR_API uint64_t mr_runtime_abi_fingerprint(void) {
     return h;
 }
 
-MR_API const char* mr_last_error(void) { return g_last_error.c_str(); }
+MR_API const char* mr_last_error(void) { return numi::rt::last_error(); }
 
 MR_API MRTaskRolloutHandle* mr_create_task_rollout(const MRRunManifestC* manifest) {
     std::unique_ptr<MRTaskRolloutHandle> handle;
@@ -533,40 +518,20 @@ MR_API MRTaskRolloutHandle* mr_create_task_rollout(const MRRunManifestC* manifes
         h.envs = cfg.environment_count;
         h.seed = cfg.seed;
         h.h = cfg.control_timestep_seconds / static_cast<float>(cfg.physics_substeps);
-        h.contact = h.model.world.pair_count > 0;
-        h.dmodel = pack_model(h.model, h.h);
+        numi::rt::KernelPlan plan;
+        numi::rt::make_plan(h.model, h.h, plan);
         const numi::CompiledModel& m = h.model;
-        int narrow_words = 0;
-        for (const MRModelPairC& pr : m.pairs) narrow_words += numi::pair_scratch_words(numi::pair_max_raw(static_cast<int>(pr.pair_class)));
-        h.layout = numi::make_layout(static_cast<int>(m.articulated_body_count), static_cast<int>(m.world.nv),
-                                     static_cast<int>(m.world.nq), static_cast<int>(m.world.pair_count),
-                                     static_cast<int>(m.world.contact_capacity), static_cast<int>(m.max_ancestor_dofs),
-                                     narrow_words, h.contact);
+        h.contact = plan.contact;
+        h.dmodel = plan.dmodel;
+        h.layout = plan.layout;
+        for (int prec = 0; prec < 2; ++prec) {
+            h.warps_per_block[prec] = plan.warps_per_block[prec];
+            h.resident_warps_per_sm[prec] = plan.resident_warps_per_sm[prec];
+        }
         check(cudaGetDevice(&h.device), "cudaGetDevice");
         cudaDeviceProp prop{};
         check(cudaGetDeviceProperties(&prop, h.device), "cudaGetDeviceProperties");
         h.device_name = prop.name;
-        const size_t per_warp = static_cast<size_t>(h.layout.total) * sizeof(float);
-        const size_t tables = numi::control_step_table_bytes();
-        const size_t limit = prop.sharedMemPerBlockOptin;
-        if (tables + per_warp > limit) throw std::runtime_error("per-environment shared memory exceeds the device limit");
-        check(numi::configure_control_step_kernels(limit), "kernel attributes");
-        // Environments per CTA: the choice that keeps the most warps resident
-        // per SM under the kernel's register and shared-memory footprint
-        // (each CTA carries one copy of the topology tables).
-        for (int prec = 0; prec < 2; ++prec) {
-            int best = 1, best_warps = 0;
-            for (int wpb = 1; wpb <= 4; wpb *= 2) {
-                const size_t smem = tables + wpb * per_warp;
-                if (smem > limit) break;
-                int blocks = 0;
-                check(numi::control_step_occupancy(h.contact, prec == 1, wpb, smem, &blocks), "occupancy query");
-                if (blocks * wpb > best_warps) { best_warps = blocks * wpb; best = wpb; }
-            }
-            if (best_warps == 0) throw std::runtime_error("the control-step kernel cannot be resident with this model");
-            h.warps_per_block[prec] = best;
-            h.resident_warps_per_sm[prec] = best_warps;
-        }
         check(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking), "stream");
         check(cudaEventCreate(&h.ev_start), "event");
         check(cudaEventCreate(&h.ev_stop), "event");
@@ -750,7 +715,7 @@ MR_API int mr_task_rollout_advance_device(MRTaskRolloutHandle* handle, const flo
 
 MR_API MRTaskRolloutLayoutC mr_task_rollout_layout(const MRTaskRolloutHandle* handle) {
     if (!handle) {
-        g_last_error = "handle is null";
+        numi::rt::set_last_error("handle is null");
         return MRTaskRolloutLayoutC{};
     }
     return handle->stats_layout;

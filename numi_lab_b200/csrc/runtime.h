@@ -1,0 +1,101 @@
+// Host-runtime pieces shared by the task-rollout handle (rollout.cu) and the
+// continuous-batching server (serve.cu): CUDA error checks, owning device /
+// pinned buffers, the C-ABI error convention, and the launch plan of the
+// control-step kernel for a compiled model.
+#pragma once
+
+#include "device_model.h"
+#include "layout.h"
+#include "model.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <stdexcept>
+#include <string>
+
+namespace numi {
+
+cudaError_t control_step_occupancy(bool contact, bool fp64_inertia, int warps_per_block, size_t smem, int* blocks_per_sm);
+cudaError_t launch_control_step(const StepParams& p, const WarpLayout& layout, bool contact, bool fp64_inertia, int warps_per_block,
+                                cudaStream_t stream);
+cudaError_t configure_control_step_kernels(size_t max_dynamic_smem);
+size_t control_step_table_bytes();
+
+namespace rt {
+
+inline void check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+struct DeviceBuffer {
+    T* ptr = nullptr;
+    size_t count = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    ~DeviceBuffer() { if (ptr) cudaFree(ptr); }
+    void reset() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        count = 0;
+    }
+    void resize(size_t n) {
+        if (n <= count && ptr) return;
+        if (ptr) { cudaFree(ptr); ptr = nullptr; }
+        check(cudaMalloc(&ptr, std::max<size_t>(n, 1) * sizeof(T)), "cudaMalloc");
+        count = n;
+    }
+};
+
+template <typename T>
+struct PinnedBuffer {
+    T* ptr = nullptr;
+    size_t count = 0;
+    PinnedBuffer() = default;
+    PinnedBuffer(const PinnedBuffer&) = delete;
+    PinnedBuffer& operator=(const PinnedBuffer&) = delete;
+    ~PinnedBuffer() { if (ptr) cudaFreeHost(ptr); }
+    void resize(size_t n) {
+        if (n <= count && ptr) return;
+        if (ptr) { cudaFreeHost(ptr); ptr = nullptr; }
+        check(cudaMallocHost(&ptr, std::max<size_t>(n, 1) * sizeof(T)), "cudaMallocHost");
+        count = n;
+    }
+};
+
+// The C ABI's error convention: thread-local message, 0 / -1 returns.
+void set_last_error(const std::string& message);
+const char* last_error();
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        f();
+        return 0;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+    } catch (...) {
+        set_last_error("unknown native error");
+    }
+    return -1;
+}
+
+// Everything the control-step kernel needs to know about a compiled model
+// at one substep length: the packed device record, the per-warp
+// shared-memory layout and the launch shape per precision mode.
+struct KernelPlan {
+    DeviceModel dmodel{};
+    WarpLayout layout{};
+    bool contact = false;
+    int warps_per_block[2] = {1, 1};     // FP32, FP64 articulated inertia
+    int resident_warps_per_sm[2] = {0, 0};
+};
+
+DeviceModel pack_model(const CompiledModel& m, float h);
+// Builds the plan for the current device; throws when the model does not fit.
+void make_plan(const CompiledModel& m, float h, KernelPlan& plan);
+
+}  // namespace rt
+}  // namespace numi

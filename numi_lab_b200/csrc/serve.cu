@@ -1,0 +1,442 @@
+// Continuous-batching rollout server behind the C ABI (include/numi_b200.h,
+// mr_create_server ... mr_server_release).
+//
+// Each world source (7-DoF chain, 29-DoF tree) owns a pool of resident
+// environment slots on the device: state, manifolds and friction live there
+// for the whole life of a request.  Requests queue on submit; every tick
+// admits waiting requests into free slots (first-come first-served with
+// backfill, against an HBM budget), then advances every admitted request by
+// one control step -- all requests of a pool packed into one launch of the
+// control-step kernel through a work-item -> slot index and per-item action
+// rows, the pools on their own streams so their work overlaps on the
+// device -- and retires the requests whose horizon is complete, copying
+// their final state out and freeing their slots.  An environment's
+// trajectory depends only on its request (model, seed, index, actions), never
+// on the slot it occupies or on the other requests in the launch.
+#include "numi_b200.h"
+#include "runtime.h"
+
+#include <chrono>
+#include <cstring>
+#include <deque>
+#include <functional>
+#include <map>
+#include <memory>
+#include <vector>
+
+namespace {
+
+using numi::rt::check;
+using numi::rt::DeviceBuffer;
+using numi::rt::guarded;
+using numi::rt::PinnedBuffer;
+
+// rows[i] (width floats) -> slots dst[index[i]]; zero when src is null.
+__global__ void scatter_rows_kernel(float* __restrict__ dst, const float* __restrict__ src, const std::int32_t* __restrict__ index,
+                                    int rows, int width) {
+    const int total = rows * width;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+        const int r = k / width, c = k - r * width;
+        dst[static_cast<size_t>(index[r]) * width + c] = src != nullptr ? src[k] : 0.0f;
+    }
+}
+
+// slots src[index[i]] -> rows dst[i] (width floats).
+__global__ void gather_rows_kernel(float* __restrict__ dst, const float* __restrict__ src, const std::int32_t* __restrict__ index,
+                                   int rows, int width) {
+    const int total = rows * width;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+        const int r = k / width, c = k - r * width;
+        dst[k] = src[static_cast<size_t>(index[r]) * width + c];
+    }
+}
+
+int grid_for(int total) { return std::max(1, std::min(1184, (total + 255) / 256)); }
+
+double now_seconds() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct Request {
+    std::uint64_t id = 0;
+    std::uint32_t source = 0;
+    std::uint32_t envs = 0;
+    std::uint32_t horizon = 0;
+    std::uint64_t seed = 0;
+    std::vector<float> host_actions;  // [horizon][envs][actions]
+    DeviceBuffer<float> d_actions;
+    DeviceBuffer<std::int32_t> d_slots;
+    std::vector<std::int32_t> slots;
+    std::uint32_t step = 0;
+    std::uint32_t failed_env_steps = 0;
+    std::uint32_t first_failure_status = 0;
+    double t_submit = 0.0, t_admit = 0.0, t_finish = 0.0;
+    std::vector<float> final_q, final_v;
+    std::size_t device_bytes = 0;
+};
+
+struct Pool {
+    std::uint32_t source = 0;
+    numi::CompiledModel model;
+    numi::rt::KernelPlan plan;
+    std::uint32_t capacity = 0;
+    std::uint32_t nq = 0, nv = 0, na = 0, manifold_words = 0;
+    cudaStream_t stream = nullptr;
+    DeviceBuffer<numi::DeviceModel> d_model;
+    DeviceBuffer<float> d_q, d_v, d_manifolds, d_friction;
+    DeviceBuffer<std::int32_t> d_index;
+    DeviceBuffer<const float*> d_rows;
+    DeviceBuffer<std::uint32_t> d_status, d_stats;
+    PinnedBuffer<std::int32_t> h_index;
+    PinnedBuffer<const float*> h_rows;
+    PinnedBuffer<std::uint32_t> h_status;
+    std::vector<std::int32_t> free_slots;  // kept sorted descending; back() is the lowest
+    std::vector<Request*> active;          // admission order
+    std::uint32_t launched_items = 0;      // of the current tick
+
+    std::size_t slot_bytes() const { return (static_cast<std::size_t>(nq) + nv + manifold_words + 1) * sizeof(float); }
+    ~Pool() {
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+}  // namespace
+
+struct MRServerHandle {
+    MRServerConfigC config{};
+    float h = 0.0f;
+    std::map<std::uint32_t, std::unique_ptr<Pool>> pools;
+    std::deque<std::unique_ptr<Request>> pending;
+    std::vector<std::unique_ptr<Request>> running;
+    std::map<std::uint64_t, std::unique_ptr<Request>> completed;
+    std::vector<std::uint64_t> unreported;
+    std::uint64_t next_id = 1;
+    std::size_t budget_used = 0;
+    std::uint64_t completed_env_steps = 0;
+
+    Pool& pool(std::uint32_t source) {
+        auto it = pools.find(source);
+        if (it == pools.end()) throw std::invalid_argument("unsupported request source " + std::to_string(source));
+        return *it->second;
+    }
+
+    void add_pool(std::uint32_t source) {
+        auto p = std::make_unique<Pool>();
+        p->source = source;
+        p->model = source == MR_RUN_SOURCE_SYNTHETIC_CHAIN7 ? numi::build_chain7(config.model_seed)
+                                                              : numi::build_tree29(config.model_seed);
+        numi::rt::make_plan(p->model, h, p->plan);
+        p->nq = p->model.world.nq;
+        p->nv = p->model.world.nv;
+        p->na = p->model.world.action_count;
+        p->manifold_words = p->model.world.pair_count * numi::kManifoldWords;
+        // Slots: the configured maximum, bounded by this pool's share of the
+        // HBM budget (half of it split across pools; the rest holds actions).
+        const std::size_t share = config.hbm_budget_bytes / (2 * 2);
+        p->capacity = static_cast<std::uint32_t>(std::min<std::size_t>(config.max_envs_per_source, share / p->slot_bytes()));
+        if (p->capacity == 0) throw std::invalid_argument("the HBM budget holds no environment of source " + std::to_string(source));
+        budget_used += static_cast<std::size_t>(p->capacity) * p->slot_bytes();
+        check(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking), "stream");
+        p->d_model.resize(1);
+        check(cudaMemcpy(p->d_model.ptr, &p->plan.dmodel, sizeof(numi::DeviceModel), cudaMemcpyHostToDevice), "upload model");
+        const std::size_t cap = p->capacity;
+        p->d_q.resize(cap * p->nq);
+        p->d_v.resize(cap * p->nv);
+        if (p->manifold_words) p->d_manifolds.resize(cap * p->manifold_words);
+        p->d_friction.resize(cap);
+        p->d_index.resize(cap);
+        p->d_rows.resize(cap);
+        p->d_status.resize(cap);
+        p->d_stats.resize(numi::kStatCount);
+        p->h_index.resize(cap);
+        p->h_rows.resize(cap);
+        p->h_status.resize(cap);
+        for (std::int32_t s = static_cast<std::int32_t>(cap) - 1; s >= 0; --s) p->free_slots.push_back(s);
+        pools[source] = std::move(p);
+    }
+
+    bool try_admit(Request& r) {
+        Pool& p = pool(r.source);
+        if (p.free_slots.size() < r.envs) return false;
+        const std::size_t bytes = r.host_actions.size() * sizeof(float) + r.envs * sizeof(std::int32_t);
+        if (budget_used + bytes > config.hbm_budget_bytes) return false;
+        budget_used += bytes;
+        r.device_bytes = bytes;
+        for (std::uint32_t e = 0; e < r.envs; ++e) {
+            r.slots.push_back(p.free_slots.back());
+            p.free_slots.pop_back();
+        }
+        r.d_actions.resize(r.host_actions.size());
+        r.d_slots.resize(r.envs);
+        check(cudaMemcpyAsync(r.d_actions.ptr, r.host_actions.data(), r.host_actions.size() * sizeof(float), cudaMemcpyHostToDevice,
+                              p.stream), "request actions H2D");
+        check(cudaMemcpyAsync(r.d_slots.ptr, r.slots.data(), r.envs * sizeof(std::int32_t), cudaMemcpyHostToDevice, p.stream),
+              "request slots H2D");
+        // Reset state of each environment of the request, scattered into its slots.
+        std::vector<float> hq(static_cast<std::size_t>(r.envs) * p.nq), hv(static_cast<std::size_t>(r.envs) * p.nv), hf(r.envs);
+        for (std::uint32_t e = 0; e < r.envs; ++e)
+            numi::sample_reset_state(p.model, r.seed, e, &hq[static_cast<std::size_t>(e) * p.nq],
+                                     &hv[static_cast<std::size_t>(e) * p.nv], &hf[e]);
+        DeviceBuffer<float> tmp_q, tmp_v, tmp_f;
+        tmp_q.resize(hq.size());
+        tmp_v.resize(hv.size());
+        tmp_f.resize(hf.size());
+        check(cudaMemcpyAsync(tmp_q.ptr, hq.data(), hq.size() * sizeof(float), cudaMemcpyHostToDevice, p.stream), "q H2D");
+        check(cudaMemcpyAsync(tmp_v.ptr, hv.data(), hv.size() * sizeof(float), cudaMemcpyHostToDevice, p.stream), "v H2D");
+        check(cudaMemcpyAsync(tmp_f.ptr, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice, p.stream), "friction H2D");
+        const int envs = static_cast<int>(r.envs);
+        scatter_rows_kernel<<<grid_for(envs * p.nq), 256, 0, p.stream>>>(p.d_q.ptr, tmp_q.ptr, r.d_slots.ptr, envs, p.nq);
+        scatter_rows_kernel<<<grid_for(envs * p.nv), 256, 0, p.stream>>>(p.d_v.ptr, tmp_v.ptr, r.d_slots.ptr, envs, p.nv);
+        scatter_rows_kernel<<<grid_for(envs), 256, 0, p.stream>>>(p.d_friction.ptr, tmp_f.ptr, r.d_slots.ptr, envs, 1);
+        if (p.manifold_words)
+            scatter_rows_kernel<<<grid_for(envs * p.manifold_words), 256, 0, p.stream>>>(p.d_manifolds.ptr, nullptr, r.d_slots.ptr,
+                                                                                         envs, p.manifold_words);
+        check(cudaGetLastError(), "admission scatter");
+        check(cudaStreamSynchronize(p.stream), "admission");
+        r.t_admit = now_seconds();
+        p.active.push_back(&r);
+        return true;
+    }
+
+    void launch(Pool& p) {
+        p.launched_items = 0;
+        if (p.active.empty()) return;
+        std::uint32_t n = 0;
+        for (Request* r : p.active) {
+            const float* base = r->d_actions.ptr + static_cast<std::size_t>(r->step) * r->envs * p.na;
+            for (std::uint32_t e = 0; e < r->envs; ++e) {
+                p.h_index.ptr[n] = r->slots[e];
+                p.h_rows.ptr[n] = base + static_cast<std::size_t>(e) * p.na;
+                ++n;
+            }
+        }
+        check(cudaMemcpyAsync(p.d_index.ptr, p.h_index.ptr, n * sizeof(std::int32_t), cudaMemcpyHostToDevice, p.stream), "index H2D");
+        check(cudaMemcpyAsync(p.d_rows.ptr, p.h_rows.ptr, n * sizeof(const float*), cudaMemcpyHostToDevice, p.stream), "rows H2D");
+        check(cudaMemsetAsync(p.d_stats.ptr, 0, numi::kStatCount * sizeof(std::uint32_t), p.stream), "clear stats");
+        numi::StepParams sp{};
+        sp.model = p.d_model.ptr;
+        sp.q = p.d_q.ptr;
+        sp.v = p.d_v.ptr;
+        sp.manifolds = p.d_manifolds.ptr;
+        sp.reset_q = p.d_q.ptr;  // no resets inside a request
+        sp.reset_v = p.d_v.ptr;
+        sp.friction_scale = p.d_friction.ptr;
+        sp.actions = nullptr;
+        sp.action_rows = p.d_rows.ptr;
+        sp.env_index = p.d_index.ptr;
+        sp.status_codes = p.d_status.ptr;
+        sp.stats = p.d_stats.ptr;
+        sp.env_count = static_cast<int>(n);
+        sp.substeps = static_cast<int>(config.physics_substeps);
+        sp.velocity_iterations = static_cast<int>(config.velocity_iterations);
+        sp.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
+        check(numi::launch_control_step(sp, p.plan.layout, p.plan.contact, false, p.plan.warps_per_block[0], p.stream),
+              "control step launch");
+        check(cudaMemcpyAsync(p.h_status.ptr, p.d_status.ptr, n * sizeof(std::uint32_t), cudaMemcpyDeviceToHost, p.stream),
+              "status D2H");
+        p.launched_items = n;
+    }
+
+    void retire(Pool& p, double t_now) {
+        std::uint32_t n = 0;
+        std::vector<Request*> still;
+        for (Request* r : p.active) {
+            for (std::uint32_t e = 0; e < r->envs; ++e, ++n) {
+                const std::uint32_t code = p.h_status.ptr[n];
+                if (code != MR_STEP_SUCCESS) {
+                    if (r->failed_env_steps == 0) r->first_failure_status = code;
+                    ++r->failed_env_steps;
+                }
+            }
+            ++r->step;
+            completed_env_steps += r->envs;
+            if (r->step < r->horizon) {
+                still.push_back(r);
+                continue;
+            }
+            // Final state out, slots and memory back.
+            const int envs = static_cast<int>(r->envs);
+            DeviceBuffer<float> gq, gv;
+            gq.resize(r->envs * p.nq);
+            gv.resize(r->envs * p.nv);
+            gather_rows_kernel<<<grid_for(envs * p.nq), 256, 0, p.stream>>>(gq.ptr, p.d_q.ptr, r->d_slots.ptr, envs, p.nq);
+            gather_rows_kernel<<<grid_for(envs * p.nv), 256, 0, p.stream>>>(gv.ptr, p.d_v.ptr, r->d_slots.ptr, envs, p.nv);
+            check(cudaGetLastError(), "gather");
+            r->final_q.resize(r->envs * p.nq);
+            r->final_v.resize(r->envs * p.nv);
+            check(cudaMemcpyAsync(r->final_q.data(), gq.ptr, r->final_q.size() * sizeof(float), cudaMemcpyDeviceToHost, p.stream),
+                  "final q D2H");
+            check(cudaMemcpyAsync(r->final_v.data(), gv.ptr, r->final_v.size() * sizeof(float), cudaMemcpyDeviceToHost, p.stream),
+                  "final v D2H");
+            check(cudaStreamSynchronize(p.stream), "retire");
+            r->t_finish = t_now;
+            for (std::int32_t s : r->slots) p.free_slots.push_back(s);
+            std::sort(p.free_slots.begin(), p.free_slots.end(), std::greater<std::int32_t>());
+            budget_used -= r->device_bytes;
+            r->d_actions.reset();
+            r->host_actions.clear();
+            r->host_actions.shrink_to_fit();
+            for (auto it = running.begin(); it != running.end(); ++it)
+                if (it->get() == r) {
+                    unreported.push_back(r->id);
+                    completed[r->id] = std::move(*it);
+                    running.erase(it);
+                    break;
+                }
+        }
+        p.active.swap(still);
+    }
+};
+
+extern "C" {
+
+MR_API MRServerHandle* mr_create_server(const MRServerConfigC* config) {
+    std::unique_ptr<MRServerHandle> server;
+    const int rc = guarded([&] {
+        if (config == nullptr) throw std::invalid_argument("config is null");
+        if (config->physics_substeps == 0 || config->physics_substeps > MR_B200_MAX_SUBSTEPS)
+            throw std::invalid_argument("physics_substeps must be in [1, 64]");
+        if (!(config->control_timestep_seconds > 0.0f)) throw std::invalid_argument("control_timestep_seconds must be positive");
+        if (config->velocity_iterations == 0 && config->final_velocity_iterations == 0)
+            throw std::invalid_argument("contact worlds need at least one velocity iteration");
+        if (config->max_envs_per_source == 0) throw std::invalid_argument("max_envs_per_source must be positive");
+        server = std::make_unique<MRServerHandle>();
+        server->config = *config;
+        server->h = config->control_timestep_seconds / static_cast<float>(config->physics_substeps);
+        server->add_pool(MR_RUN_SOURCE_SYNTHETIC_CHAIN7);
+        server->add_pool(MR_RUN_SOURCE_SYNTHETIC_TREE29);
+        if (server->budget_used > config->hbm_budget_bytes) throw std::invalid_argument("HBM budget exhausted by the slot pools");
+    });
+    if (rc != 0) return nullptr;
+    return server.release();
+}
+
+MR_API void mr_server_destroy(MRServerHandle* server) {
+    if (server) {
+        for (auto& kv : server->pools) cudaStreamSynchronize(kv.second->stream);
+        delete server;
+    }
+}
+
+MR_API int mr_server_capacity(const MRServerHandle* server, uint32_t source, uint32_t* slots, uint32_t* action_count) {
+    return guarded([&] {
+        if (!server) throw std::invalid_argument("server is null");
+        auto it = server->pools.find(source);
+        if (it == server->pools.end()) throw std::invalid_argument("unsupported source " + std::to_string(source));
+        if (slots) *slots = it->second->capacity;
+        if (action_count) *action_count = it->second->na;
+    });
+}
+
+MR_API int mr_server_submit(MRServerHandle* server, const MRServerRequestC* request, uint64_t* request_id) {
+    return guarded([&] {
+        if (!server || !request || !request_id) throw std::invalid_argument("null argument");
+        Pool& p = server->pool(request->source);
+        if (request->env_count == 0 || request->env_count > p.capacity)
+            throw std::invalid_argument("env_count must be in [1, " + std::to_string(p.capacity) + "]");
+        if (request->horizon == 0) throw std::invalid_argument("horizon must be positive");
+        const std::size_t count = static_cast<std::size_t>(request->horizon) * request->env_count * p.na;
+        if (count && request->actions == nullptr) throw std::invalid_argument("actions are null");
+        auto r = std::make_unique<Request>();
+        r->id = server->next_id++;
+        r->source = request->source;
+        r->envs = request->env_count;
+        r->horizon = request->horizon;
+        r->seed = request->seed;
+        r->host_actions.assign(request->actions, request->actions + count);  // caller span copied
+        r->t_submit = now_seconds();
+        *request_id = r->id;
+        server->pending.push_back(std::move(r));
+    });
+}
+
+MR_API int mr_server_tick(MRServerHandle* server, uint32_t* active_requests, uint32_t* active_envs) {
+    return guarded([&] {
+        if (!server) throw std::invalid_argument("server is null");
+        // Admission: first come, first served, with backfill of smaller requests.
+        for (auto it = server->pending.begin(); it != server->pending.end();) {
+            if (server->try_admit(**it)) {
+                server->running.push_back(std::move(*it));
+                it = server->pending.erase(it);
+            } else {
+                ++it;
+            }
+        }
+        std::uint32_t reqs = 0, envs = 0;
+        for (auto& kv : server->pools) {
+            server->launch(*kv.second);
+            reqs += static_cast<std::uint32_t>(kv.second->active.size());
+            envs += kv.second->launched_items;
+        }
+        for (auto& kv : server->pools) check(cudaStreamSynchronize(kv.second->stream), "tick");
+        const double t = now_seconds();
+        for (auto& kv : server->pools) server->retire(*kv.second, t);
+        if (active_requests) *active_requests = reqs;
+        if (active_envs) *active_envs = envs;
+    });
+}
+
+MR_API int mr_server_poll(MRServerHandle* server, MRServerCompletionC* out, uint32_t capacity, uint32_t* count) {
+    return guarded([&] {
+        if (!server || !count) throw std::invalid_argument("null argument");
+        std::uint32_t n = 0;
+        while (n < capacity && !server->unreported.empty()) {
+            const std::uint64_t id = server->unreported.front();
+            server->unreported.erase(server->unreported.begin());
+            const Request& r = *server->completed.at(id);
+            MRServerCompletionC c{};
+            c.request_id = r.id;
+            c.source = r.source;
+            c.env_count = r.envs;
+            c.horizon = r.horizon;
+            c.failed_env_steps = r.failed_env_steps;
+            c.first_failure_status = r.first_failure_status;
+            c.queue_seconds = r.t_admit - r.t_submit;
+            c.latency_seconds = r.t_finish - r.t_submit;
+            if (out) out[n] = c;
+            ++n;
+        }
+        *count = n;
+    });
+}
+
+MR_API int mr_server_copy_result(const MRServerHandle* server, uint64_t request_id, float* q, size_t q_count, float* v,
+                                 size_t v_count) {
+    return guarded([&] {
+        if (!server) throw std::invalid_argument("server is null");
+        auto it = server->completed.find(request_id);
+        if (it == server->completed.end()) throw std::invalid_argument("request " + std::to_string(request_id) + " is not complete");
+        const Request& r = *it->second;
+        if (q) {
+            if (q_count < r.final_q.size()) throw std::invalid_argument("q buffer too small");
+            std::memcpy(q, r.final_q.data(), r.final_q.size() * sizeof(float));
+        }
+        if (v) {
+            if (v_count < r.final_v.size()) throw std::invalid_argument("v buffer too small");
+            std::memcpy(v, r.final_v.data(), r.final_v.size() * sizeof(float));
+        }
+    });
+}
+
+MR_API int mr_server_release(MRServerHandle* server, uint64_t request_id) {
+    return guarded([&] {
+        if (!server) throw std::invalid_argument("server is null");
+        if (server->completed.erase(request_id) == 0)
+            throw std::invalid_argument("request " + std::to_string(request_id) + " is not complete");
+    });
+}
+
+MR_API int mr_server_stats(const MRServerHandle* server, MRServerStatsC* stats) {
+    return guarded([&] {
+        if (!server || !stats) throw std::invalid_argument("null argument");
+        MRServerStatsC s{};
+        s.pending_requests = static_cast<std::uint32_t>(server->pending.size());
+        s.running_requests = static_cast<std::uint32_t>(server->running.size());
+        s.completed_env_steps = server->completed_env_steps;
+        s.hbm_bytes_in_use = server->budget_used;
+        for (const auto& kv : server->pools) s.free_slots += static_cast<std::uint32_t>(kv.second->free_slots.size());
+        *stats = s;
+    });
+}
+
+}  // extern "C"

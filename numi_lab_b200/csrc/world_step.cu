@@ -1918,8 +1918,11 @@ __global__ void __launch_bounds__(128, 3) control_step_kernel(StepParams p, Warp
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const int env = blockIdx.x * warps_per_block + warp;
-    if (env >= p.env_count) return;
+    // Work item (compact index of this launch's outputs) and the resident
+    // environment slot it advances.
+    const int item = blockIdx.x * warps_per_block + warp;
+    if (item >= p.env_count) return;
+    const int env = p.env_index != nullptr ? p.env_index[item] : item;
     const DeviceModel& M = *p.model;
     Warp w;
     w.lane = lane;
@@ -1932,7 +1935,7 @@ __global__ void __launch_bounds__(128, 3) control_step_kernel(StepParams p, Warp
     const int nq = M.nq, nv = M.nv;
 
     // Prepare: reset, checkpoint, actions (mr_metal_world_prepare).
-    const bool reset = p.reset_masks != nullptr && p.reset_masks[env] != 0u;
+    const bool reset = p.reset_masks != nullptr && p.reset_masks[item] != 0u;
     const float* srcq = (reset ? p.reset_q : p.q) + static_cast<size_t>(env) * nq;
     const float* srcv = (reset ? p.reset_v : p.v) + static_cast<size_t>(env) * nv;
     for (int i = lane; i < nq; i += 32) {
@@ -1949,7 +1952,8 @@ __global__ void __launch_bounds__(128, 3) control_step_kernel(StepParams p, Warp
     misc[lane] = 0.0f;
     __syncwarp();
     for (int a = lane; a < M.action_count; a += 32)
-        s[layout.tgt + M.action_dof[a]] = p.actions[static_cast<size_t>(env) * M.action_count + a];
+        s[layout.tgt + M.action_dof[a]] =
+            p.action_rows != nullptr ? p.action_rows[item][a] : p.actions[static_cast<size_t>(item) * M.action_count + a];
     if (kContact) {
         // Slots sit at an odd stride in shared memory (lane-per-pair access
         // is conflict free) and packed in HBM.
@@ -1987,7 +1991,7 @@ __global__ void __launch_bounds__(128, 3) control_step_kernel(StepParams p, Warp
     float* vd = p.v + static_cast<size_t>(env) * nv;
     const float* qsrc = s + (success ? layout.q : layout.qc);
     const float* vsrc = s + (success ? layout.v : layout.vc);
-    float* obs = p.observations ? p.observations + static_cast<size_t>(env) * (nq + nv) : nullptr;
+    float* obs = p.observations ? p.observations + static_cast<size_t>(item) * (nq + nv) : nullptr;
     for (int i = lane; i < nq; i += 32) {
         const float x = qsrc[i];
         qd[i] = x;
@@ -2009,8 +2013,8 @@ __global__ void __launch_bounds__(128, 3) control_step_kernel(StepParams p, Warp
     }
     if (lane == 0) {
         const unsigned contacts = kContact ? static_cast<unsigned>(as_int(misc[kMiscContactCount])) : 0u;
-        if (p.status_codes) p.status_codes[env] = code;
-        if (p.active_contacts) p.active_contacts[env] = success ? contacts : 0u;
+        if (p.status_codes) p.status_codes[item] = code;
+        if (p.active_contacts) p.active_contacts[item] = success ? contacts : 0u;
         if (!success) {
             atomicAdd(p.stats + kStatFailedEnvs, 1u);
             atomicMin(p.stats + kStatFirstFailEnv, static_cast<unsigned>(env));

@@ -297,6 +297,55 @@ class ManifoldC(ct.Structure):
 
 # Every C-ABI entry point this binding configures, by name.  Tests check the
 # loaded library exports each of them.
+class ServerConfigC(ct.Structure):
+    _fields_ = [
+        ("hbm_budget_bytes", ct.c_uint64),
+        ("model_seed", ct.c_uint64),
+        ("physics_substeps", ct.c_uint32),
+        ("velocity_iterations", ct.c_uint32),
+        ("final_velocity_iterations", ct.c_uint32),
+        ("control_timestep_seconds", ct.c_float),
+        ("max_envs_per_source", ct.c_uint32),
+        ("reserved", ct.c_uint32),
+    ]
+
+
+class ServerRequestC(ct.Structure):
+    _fields_ = [
+        ("source", ct.c_uint32),
+        ("env_count", ct.c_uint32),
+        ("horizon", ct.c_uint32),
+        ("reserved", ct.c_uint32),
+        ("seed", ct.c_uint64),
+        ("actions", ct.POINTER(ct.c_float)),
+    ]
+
+
+class ServerCompletionC(ct.Structure):
+    _fields_ = [
+        ("request_id", ct.c_uint64),
+        ("source", ct.c_uint32),
+        ("env_count", ct.c_uint32),
+        ("horizon", ct.c_uint32),
+        ("failed_env_steps", ct.c_uint32),
+        ("first_failure_status", ct.c_uint32),
+        ("reserved", ct.c_uint32),
+        ("queue_seconds", ct.c_double),
+        ("latency_seconds", ct.c_double),
+    ]
+
+
+class ServerStatsC(ct.Structure):
+    _fields_ = [
+        ("pending_requests", ct.c_uint32),
+        ("running_requests", ct.c_uint32),
+        ("free_slots", ct.c_uint32),
+        ("reserved", ct.c_uint32),
+        ("completed_env_steps", ct.c_uint64),
+        ("hbm_bytes_in_use", ct.c_uint64),
+    ]
+
+
 EXPORTED_SYMBOLS: Final = (
     "mr_version",
     "mr_runtime_abi_fingerprint",
@@ -319,6 +368,15 @@ EXPORTED_SYMBOLS: Final = (
     "mr_task_rollout_copy_state",
     "mr_task_rollout_set_state",
     "mr_task_rollout_set_precision",
+    "mr_create_server",
+    "mr_server_destroy",
+    "mr_server_capacity",
+    "mr_server_submit",
+    "mr_server_tick",
+    "mr_server_poll",
+    "mr_server_copy_result",
+    "mr_server_release",
+    "mr_server_stats",
 )
 
 
@@ -411,6 +469,24 @@ class Bindings:
         L.mr_task_rollout_copy_state.restype = ct.c_int
         L.mr_task_rollout_set_state.argtypes = [ct.c_void_p, P(ct.c_float), P(ct.c_float), ct.c_void_p, ct.c_uint32]
         L.mr_task_rollout_set_state.restype = ct.c_int
+        L.mr_create_server.argtypes = [P(ServerConfigC)]
+        L.mr_create_server.restype = ct.c_void_p
+        L.mr_server_destroy.argtypes = [ct.c_void_p]
+        L.mr_server_destroy.restype = None
+        L.mr_server_capacity.argtypes = [ct.c_void_p, ct.c_uint32, P(ct.c_uint32), P(ct.c_uint32)]
+        L.mr_server_capacity.restype = ct.c_int
+        L.mr_server_submit.argtypes = [ct.c_void_p, P(ServerRequestC), P(ct.c_uint64)]
+        L.mr_server_submit.restype = ct.c_int
+        L.mr_server_tick.argtypes = [ct.c_void_p, P(ct.c_uint32), P(ct.c_uint32)]
+        L.mr_server_tick.restype = ct.c_int
+        L.mr_server_poll.argtypes = [ct.c_void_p, P(ServerCompletionC), ct.c_uint32, P(ct.c_uint32)]
+        L.mr_server_poll.restype = ct.c_int
+        L.mr_server_copy_result.argtypes = [ct.c_void_p, ct.c_uint64, P(ct.c_float), ct.c_size_t, P(ct.c_float), ct.c_size_t]
+        L.mr_server_copy_result.restype = ct.c_int
+        L.mr_server_release.argtypes = [ct.c_void_p, ct.c_uint64]
+        L.mr_server_release.restype = ct.c_int
+        L.mr_server_stats.argtypes = [ct.c_void_p, P(ServerStatsC)]
+        L.mr_server_stats.restype = ct.c_int
 
     def last_error(self) -> str:
         value = self.lib.mr_last_error()

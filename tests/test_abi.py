@@ -56,6 +56,10 @@ def test_struct_sizes_match_header_layout(tmp_path):
         "MRModelPairC": native.ModelPairC,
         "MRModelViewC": native.ModelViewC,
         "MRManifoldC": native.ManifoldC,
+        "MRServerConfigC": native.ServerConfigC,
+        "MRServerRequestC": native.ServerRequestC,
+        "MRServerCompletionC": native.ServerCompletionC,
+        "MRServerStatsC": native.ServerStatsC,
     }
     src = tmp_path / "sizes.c"
     body = "".join(f'printf("%zu\\n", sizeof({name}));' for name in records)
