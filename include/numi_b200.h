@@ -38,6 +38,8 @@ extern "C" {
 #define MR_B200_MAX_Q 41u          /* generalized coordinates per world      */
 #define MR_B200_MAX_SHAPES 32u     /* colliders per world                    */
 #define MR_B200_MAX_PAIRS 32u      /* compiled eligible collider pairs       */
+#define MR_B200_SCENE_MANIFOLDS 128u  /* persistent manifold slots per pile   */
+#define MR_B200_SCENE_SLOT_WORDS 57u  /* MRManifoldC + pair key               */
 #define MR_B200_MAX_CONTACTS 32u   /* solver contacts per environment        */
 #define MR_B200_MANIFOLD_POINTS 4u /* persistent points per manifold         */
 #define MR_B200_MAX_SUBSTEPS 64u   /* physics substeps per control step      */
@@ -96,9 +98,12 @@ enum MRDofFlags {
 /* reference: include/metalrobo/engine_types.h:149-163 (same values). */
 enum MRCollisionPairClass {
     MR_COLLISION_PAIR_UNSUPPORTED = 0u,
+    MR_COLLISION_PAIR_SPHERE_SPHERE = 1u,
     MR_COLLISION_PAIR_SPHERE_PLANE = 2u,
     MR_COLLISION_PAIR_CAPSULE_PLANE = 3u,
-    MR_COLLISION_PAIR_BOX_PLANE = 4u
+    MR_COLLISION_PAIR_BOX_PLANE = 4u,
+    MR_COLLISION_PAIR_SPHERE_BOX = 8u,
+    MR_COLLISION_PAIR_BOX_BOX = 10u
 };
 #endif /* NUMI_B200_OMIT_SHARED_ENUMS */
 
@@ -162,7 +167,10 @@ enum MRRunManifestSourceC {
     /* Floating 29-DoF humanoid tree (pelvis, 2x6 legs, 3 waist, 2x7 arms),
      * implicit PD position drives, box feet and 12 sphere proxies on a
      * ground plane. */
-    MR_RUN_SOURCE_SYNTHETIC_TREE29 = 101u
+    MR_RUN_SOURCE_SYNTHETIC_TREE29 = 101u,
+    /* Pile of 8-64 free spheres and boxes dropped onto a ground plane (body
+     * count drawn from the seed); scene bodies, no actuation. */
+    MR_RUN_SOURCE_SYNTHETIC_PILE = 102u
 };
 
 /* reference: include/metalrobo/c_api.h:171-190 (same shape). */
@@ -496,7 +504,11 @@ MR_API int mr_task_rollout_copy_environment_parameters(
 
 /* No counterpart in the reference: copies the resident state of every
  * environment, q [env][nq], v [env][nv] and manifolds [env][pair_count];
- * any pointer may be null. */
+ * any pointer may be null.  Pile worlds (scene bodies) store instead a
+ * table of MR_B200_SCENE_MANIFOLDS slots per environment, each one
+ * MRManifoldC followed by its pair key (a * 65 + b; b = body count for the
+ * ground plane) as a uint32 word, live slots first in ascending key order
+ * (MR_B200_SCENE_SLOT_WORDS floats per slot). */
 MR_API int mr_task_rollout_copy_state(
     const MRTaskRolloutHandle* handle, float* q, float* v, MRManifoldC* manifolds);
 

@@ -99,6 +99,21 @@ std::uint64_t hash_bytes(std::uint64_t h, const void* data, std::size_t n) {
 
 void CompiledModel::finalize() {
     const std::uint32_t nb = world.body_count;
+    if (scene) {
+        if (scene_bodies == 0 || scene_bodies > 64 || nb != scene_bodies + 1) throw std::runtime_error("scene body count outside capacity");
+        if (world.nq != 7 * scene_bodies || world.nv != 6 * scene_bodies) throw std::runtime_error("scene nq/nv mismatch");
+        articulated_body_count = 0;
+        std::uint64_t h = 0x9e3779b97f4a7c15ull;
+        auto mixin = [&](const void* data, std::size_t bytes) {
+            const unsigned char* p = static_cast<const unsigned char*>(data);
+            for (std::size_t i = 0; i < bytes; ++i) h = (h ^ p[i]) * 0x100000001b3ull;
+        };
+        mixin(&world, sizeof(world));
+        mixin(bodies.data(), bodies.size() * sizeof(MRModelBodyC));
+        mixin(shapes.data(), shapes.size() * sizeof(MRModelShapeC));
+        fingerprint = h;
+        return;
+    }
     if (nb == 0 || nb > MR_B200_MAX_BODIES + 1) throw std::runtime_error("body count outside capacity");
     if (world.nv == 0 || world.nv > MR_B200_MAX_DOFS || world.nq > MR_B200_MAX_Q)
         throw std::runtime_error("nq/nv outside capacity");
@@ -459,9 +474,163 @@ CompiledModel build_tree29(std::uint64_t seed) {
     return m;
 }
 
+CompiledModel build_pile(std::uint64_t seed, std::uint32_t count) {
+    CompiledModel m;
+    m.name = "synthetic_pile";
+    m.scene = true;
+    std::uint64_t k = 0;
+    auto draw = [&](double lo, double hi) { return uniform(seed, kStreamModel, k++, lo, hi); };
+    const std::uint32_t n = count ? count : 8u + static_cast<std::uint32_t>(mix64(seed ^ 0x5ca1ab1eull) % 57u);
+    if (n < 1 || n > 64) throw std::invalid_argument("pile body count must be in [1, 64]");
+    m.scene_bodies = n;
+    double largest = 0.0;
+    for (std::uint32_t b = 0; b < n; ++b) {
+        const bool box = draw(0.0, 1.0) < 0.5;
+        const double size = draw(0.05, 0.3);
+        const double density = draw(500.0, 2000.0);
+        double hx = 0.5 * size, hy = 0.5 * size, hz = 0.5 * size;
+        if (box) {
+            hx *= draw(0.7, 1.0);
+            hy *= draw(0.7, 1.0);
+            hz *= draw(0.7, 1.0);
+        }
+        MRModelBodyC body{};
+        body.parent_body = MR_INVALID_INDEX;
+        body.inbound_joint = MR_INVALID_INDEX;
+        body.motion_type = MR_MOTION_DYNAMIC;
+        body.articulated = 0u;
+        double mass, ixx, iyy, izz, bound;
+        if (box) {
+            mass = density * 8.0 * hx * hy * hz;
+            ixx = mass / 3.0 * (hy * hy + hz * hz);
+            iyy = mass / 3.0 * (hx * hx + hz * hz);
+            izz = mass / 3.0 * (hx * hx + hy * hy);
+            bound = std::sqrt(hx * hx + hy * hy + hz * hz);
+        } else {
+            const double r = hx;
+            mass = density * 4.0 / 3.0 * 3.141592653589793 * r * r * r;
+            ixx = iyy = izz = 0.4 * mass * r * r;
+            bound = r;
+        }
+        largest = std::max(largest, bound);
+        set4(body.mass_inverse_mass, mass, 1.0 / mass, 0.0, 0.0);
+        set4(body.inertia[0], ixx, 0.0, 0.0, 0.0);
+        set4(body.inertia[1], 0.0, iyy, 0.0, 0.0);
+        set4(body.inertia[2], 0.0, 0.0, izz, 0.0);
+        set4(body.damping_speed, 0.0, 0.0, 100.0, 100.0);
+        set4(body.static_pose, 0.0, 0.0, 0.0, 0.0);
+        set4(body.static_pose + 4, 0.0, 0.0, 0.0, 1.0);
+        m.bodies.push_back(body);
+        MRModelShapeC s{};
+        s.body = b;
+        s.shape_type = box ? MR_SHAPE_BOX : MR_SHAPE_SPHERE;
+        s.material = 0;
+        s.collision_group = 1u;
+        s.collision_mask = 3u;
+        set4(s.local_position, 0.0, 0.0, 0.0, 0.0);
+        set4(s.local_rotation, 0.0, 0.0, 0.0, 1.0);
+        set4(s.dimensions, hx, box ? hy : 0.0, box ? hz : 0.0, 0.0);
+        set4(s.contact_rest_bound, 0.002, 0.0, bound, 0.0);
+        m.shapes.push_back(s);
+    }
+    MRModelBodyC ground{};
+    ground.parent_body = MR_INVALID_INDEX;
+    ground.inbound_joint = MR_INVALID_INDEX;
+    ground.motion_type = MR_MOTION_STATIC;
+    set4(ground.static_pose + 4, 0.0, 0.0, 0.0, 1.0);
+    m.bodies.push_back(ground);
+    {
+        MRModelShapeC plane{};
+        plane.body = n;
+        plane.shape_type = MR_SHAPE_PLANE;
+        plane.material = 1;
+        plane.collision_group = 2u;
+        plane.collision_mask = 1u;
+        const double h = std::sqrt(0.5);
+        set4(plane.local_rotation, h, 0.0, 0.0, h);  // local +Y -> world +Z
+        m.shapes.push_back(plane);
+    }
+    MRModelMaterialC mat{};
+    set4(mat.friction, 0.6, 0.6, 0.0, 0.0);
+    set4(mat.response, 0.0, 0.5, 0.0, 0.0);
+    m.materials.push_back(mat);
+    m.materials.push_back(mat);
+    auto cls = [&](std::uint32_t a, std::uint32_t b) {
+        const std::uint32_t ta = m.shapes[a].shape_type, tb = m.shapes[b].shape_type;
+        if (tb == MR_SHAPE_PLANE) return ta == MR_SHAPE_BOX ? MR_COLLISION_PAIR_BOX_PLANE : MR_COLLISION_PAIR_SPHERE_PLANE;
+        if (ta == MR_SHAPE_SPHERE && tb == MR_SHAPE_SPHERE) return MR_COLLISION_PAIR_SPHERE_SPHERE;
+        if (ta == MR_SHAPE_BOX && tb == MR_SHAPE_BOX) return MR_COLLISION_PAIR_BOX_BOX;
+        return MR_COLLISION_PAIR_SPHERE_BOX;
+    };
+    // Compiled pairs in key order (a, b), b = n for the plane.
+    for (std::uint32_t a = 0; a < n; ++a) {
+        for (std::uint32_t b = a + 1; b < n; ++b) {
+            MRModelPairC pr{a, b, static_cast<std::uint32_t>(cls(a, b)), 4u};
+            m.pairs.push_back(pr);
+        }
+        MRModelPairC pr{a, n, static_cast<std::uint32_t>(cls(a, n)), 4u};
+        m.pairs.push_back(pr);
+    }
+    m.world.body_count = n + 1;
+    m.world.joint_count = 0;
+    m.world.nq = 7 * n;
+    m.world.nv = 6 * n;
+    m.world.shape_count = n + 1;
+    m.world.material_count = 2;
+    m.world.pair_count = static_cast<std::uint32_t>(m.pairs.size());
+    m.world.root_type = MR_ROOT_FIXED;
+    m.world.actuation_mode = MR_ACTUATION_EFFORT;
+    m.world.action_count = 0;
+    m.world.contact_capacity = 256;
+    m.world.apply_body_damping = 1u;
+    set4(m.world.gravity, 0.0, 0.0, -9.81, 0.0);
+    set4(m.world.solver_scales, 1.0e-7, 1.0e-9, 2.0, 1.0e-4);
+    set4(m.world.manifold_thresholds, 0.02, 0.02, 0.002, 0.95);
+    set4(m.world.speculative, 1.0, 1.0e4, 0.0, 0.0);
+    m.scene_cell = static_cast<float>(2.0 * largest + 0.05);
+    m.nominal_q.assign(m.world.nq, 0.0f);
+    m.friction_scale_lo = 1.0f;
+    m.friction_scale_hi = 1.0f;
+    m.finalize();
+    return m;
+}
+
 void sample_reset_state(const CompiledModel& model, std::uint64_t seed, std::uint32_t env,
                         float* q, float* v, float* friction_scale) {
     const std::uint32_t nq = model.world.nq, nv = model.world.nv;
+    if (model.scene) {
+        // Bodies on a jittered square grid, dropped from U(0.1, 1) m above
+        // the plane with a uniformly random orientation, at rest.
+        const std::uint32_t n = model.scene_bodies;
+        const std::uint32_t side = static_cast<std::uint32_t>(std::ceil(std::sqrt(static_cast<double>(n))));
+        const std::uint64_t base = static_cast<std::uint64_t>(env) * 1024u;
+        for (std::uint32_t b = 0; b < n; ++b) {
+            const double cell = model.scene_cell;
+            const double x = (static_cast<double>(b % side) - 0.5 * (side - 1)) * cell +
+                             uniform(seed, kStreamResetQ, base + 8 * b, -0.02, 0.02);
+            const double y = (static_cast<double>(b / side) - 0.5 * (side - 1)) * cell +
+                             uniform(seed, kStreamResetQ, base + 8 * b + 1, -0.02, 0.02);
+            const double bound = model.shapes[b].contact_rest_bound[2];
+            const double z = bound + uniform(seed, kStreamResetQ, base + 8 * b + 2, 0.1, 1.0);
+            // Uniform rotation (Shoemake): three uniforms -> unit quaternion.
+            const double u1 = uniform01(seed, kStreamResetRoot, base + 8 * b);
+            const double u2 = uniform01(seed, kStreamResetRoot, base + 8 * b + 1);
+            const double u3 = uniform01(seed, kStreamResetRoot, base + 8 * b + 2);
+            const double a = std::sqrt(1.0 - u1), c = std::sqrt(u1), tp = 6.283185307179586;
+            float* qb = q + 7 * b;
+            qb[0] = static_cast<float>(x);
+            qb[1] = static_cast<float>(y);
+            qb[2] = static_cast<float>(z);
+            qb[3] = static_cast<float>(a * std::sin(tp * u2));
+            qb[4] = static_cast<float>(a * std::cos(tp * u2));
+            qb[5] = static_cast<float>(c * std::sin(tp * u3));
+            qb[6] = static_cast<float>(c * std::cos(tp * u3));
+        }
+        for (std::uint32_t i = 0; i < nv; ++i) v[i] = 0.0f;
+        *friction_scale = static_cast<float>(
+            uniform(seed, kStreamFriction, env, model.friction_scale_lo, model.friction_scale_hi));
+        return;
+    }
     for (std::uint32_t i = 0; i < nq; ++i) q[i] = model.nominal_q[i];
     for (std::uint32_t i = 0; i < nv; ++i) v[i] = 0.0f;
     const std::uint64_t base = static_cast<std::uint64_t>(env) * 64u;

@@ -53,11 +53,23 @@ struct CompiledModel {
 
     std::uint64_t fingerprint = 0;
 
+    // Free-body scene (pile) instead of an articulation: bodies [0, scene_bodies)
+    // are dynamic, each with one collider at its COM; the last body is the
+    // static ground with the plane collider.  q = [body][position, orientation],
+    // v = [body][linear, angular velocity]; pairs are all collider pairs.
+    bool scene = false;
+    std::uint32_t scene_bodies = 0;
+    float scene_cell = 0.0f;  // reset grid spacing
+
     void finalize();  // validates and fills derived tables; throws on error
 };
 
 CompiledModel build_chain7(std::uint64_t seed);
 CompiledModel build_tree29(std::uint64_t seed);
+// Pile of 8-64 free spheres and boxes (size U(0.05, 0.3) m, density
+// U(500, 2000) kg/m^3) dropped onto a ground plane; the body count is drawn
+// from the seed unless `bodies` is non-zero.
+CompiledModel build_pile(std::uint64_t seed, std::uint32_t bodies = 0);
 
 // Reset state for environment `env` (q: nq, v: nv) and its friction scale.
 void sample_reset_state(const CompiledModel& model, std::uint64_t seed, std::uint32_t env,

@@ -12,6 +12,7 @@
 #include "model.h"
 #include "numi_b200.h"
 #include "runtime.h"
+#include "scene.h"
 
 #include <cuda_runtime.h>
 
@@ -288,11 +289,75 @@ void numi::rt::make_plan(const numi::CompiledModel& m, float h, KernelPlan& plan
     }
 }
 
+numi::SceneModel pack_scene(const numi::CompiledModel& m, float h) {
+    numi::SceneModel d{};
+    const std::uint32_t n = m.scene_bodies;
+    if (m.pairs.size() > static_cast<size_t>(numi::kSceneMaxPairs)) throw std::runtime_error("scene pair count outside capacity");
+    if (m.materials.size() > static_cast<size_t>(numi::kSceneMaxMaterials)) throw std::runtime_error("too many scene materials");
+    d.nb = static_cast<int>(n);
+    d.np = static_cast<int>(m.pairs.size());
+    d.h = h;
+    d.slop = m.world.solver_scales[3];
+    for (int i = 0; i < 3; ++i) d.gravity[i] = m.world.gravity[i];
+    d.max_depenetration = m.world.solver_scales[2];
+    d.speculative_scale = m.world.speculative[0];
+    d.speed_envelope = m.world.speculative[1];
+    for (int i = 0; i < 4; ++i) d.thresholds[i] = m.world.manifold_thresholds[i];
+    const MRModelShapeC& plane = m.shapes[n];
+    const MRModelBodyC& ground = m.bodies[n];
+    d.plane_position = make_float4(ground.static_pose[0] + plane.local_position[0], ground.static_pose[1] + plane.local_position[1],
+                                   ground.static_pose[2] + plane.local_position[2], 0.0f);
+    {
+        const double qw[4] = {plane.local_rotation[0], plane.local_rotation[1], plane.local_rotation[2], plane.local_rotation[3]};
+        const double nrm = std::sqrt(qw[0] * qw[0] + qw[1] * qw[1] + qw[2] * qw[2] + qw[3] * qw[3]);
+        d.plane_rotation = make_float4(static_cast<float>(qw[0] / nrm), static_cast<float>(qw[1] / nrm), static_cast<float>(qw[2] / nrm),
+                                       static_cast<float>(qw[3] / nrm));
+    }
+    d.plane_offsets = make_float4(plane.contact_rest_bound[0], plane.contact_rest_bound[1], 0.0f, 0.0f);
+    d.ground_position = make_float4(ground.static_pose[0], ground.static_pose[1], ground.static_pose[2], 0.0f);
+    {
+        const double qw[4] = {ground.static_pose[4], ground.static_pose[5], ground.static_pose[6], ground.static_pose[7]};
+        const double nrm = std::sqrt(qw[0] * qw[0] + qw[1] * qw[1] + qw[2] * qw[2] + qw[3] * qw[3]);
+        d.ground_rotation = make_float4(static_cast<float>(qw[0] / nrm), static_cast<float>(qw[1] / nrm), static_cast<float>(qw[2] / nrm),
+                                        static_cast<float>(qw[3] / nrm));
+    }
+    d.plane_material = static_cast<int>(plane.material);
+    for (std::uint32_t b = 0; b < n; ++b) {
+        const MRModelShapeC& sh = m.shapes[b];
+        const MRModelBodyC& body = m.bodies[b];
+        d.shape_type[b] = static_cast<int>(sh.shape_type);
+        d.material[b] = static_cast<int>(sh.material);
+        d.dims[b] = make_float4(sh.dimensions[0], sh.dimensions[1], sh.dimensions[2], 0.0f);
+        const float damp_lin = m.world.apply_body_damping ? body.damping_speed[0] : 0.0f;
+        const float damp_ang = m.world.apply_body_damping ? body.damping_speed[1] : 0.0f;
+        d.mass[b] = make_float4(body.mass_inverse_mass[0], body.mass_inverse_mass[1], damp_lin, damp_ang);
+        d.inv_inertia[b] = make_float4(1.0f / body.inertia[0][0], 1.0f / body.inertia[1][1], 1.0f / body.inertia[2][2],
+                                       body.damping_speed[2]);
+        d.offsets[b] = make_float4(sh.contact_rest_bound[0], sh.contact_rest_bound[1], sh.contact_rest_bound[2], body.damping_speed[3]);
+    }
+    for (std::size_t i = 0; i < m.materials.size(); ++i) {
+        const MRModelMaterialC& mt = m.materials[i];
+        d.material_friction[i] = make_float4(mt.friction[0], mt.friction[1], mt.friction[2], mt.friction[3]);
+        d.material_response[i] = make_float4(mt.response[0], mt.response[1], mt.response[2], mt.response[3]);
+    }
+    for (std::size_t p = 0; p < m.pairs.size(); ++p) {
+        d.pair_a[p] = static_cast<std::uint8_t>(m.pairs[p].shape_a);
+        d.pair_b[p] = static_cast<std::uint8_t>(m.pairs[p].shape_b);
+        d.pair_class[p] = static_cast<std::uint8_t>(m.pairs[p].pair_class);
+    }
+    return d;
+}
+
 struct MRTaskRolloutHandle {
     numi::CompiledModel model;
     numi::DeviceModel dmodel{};
     numi::WarpLayout layout{};
     bool contact = false;
+    bool scene = false;                 // free-body pile world (scene_step kernel)
+    numi::SceneModel smodel{};
+    DeviceBuffer<numi::SceneModel> d_smodel;
+    DeviceBuffer<std::uint32_t> d_mcount;
+    DeviceBuffer<float> d_workspace;    // scene substep tables, contacts, narrowphase scratch
     bool fp64_inertia = false;          // MR_PRECISION_FP64_ARTICULATED_INERTIA
     int warps_per_block[2] = {1, 1};    // per precision (FP32, FP64 inertia)
     int resident_warps_per_sm[2] = {0, 0};
@@ -358,10 +423,14 @@ struct MRTaskRolloutHandle {
         check(cudaMemcpyAsync(d_q.ptr, d_reset_q.ptr, reset_q.size() * sizeof(float), cudaMemcpyDeviceToDevice, stream), "init q");
         check(cudaMemcpyAsync(d_v.ptr, d_reset_v.ptr, reset_v.size() * sizeof(float), cudaMemcpyDeviceToDevice, stream), "init v");
         if (d_manifolds.count) check(cudaMemsetAsync(d_manifolds.ptr, 0, d_manifolds.count * sizeof(float), stream), "clear manifolds");
+        if (d_mcount.count) check(cudaMemsetAsync(d_mcount.ptr, 0, d_mcount.count * sizeof(std::uint32_t), stream), "clear manifold counts");
         check(cudaStreamSynchronize(stream), "reset");
     }
 
-    size_t manifold_words() const { return static_cast<size_t>(model.world.pair_count) * numi::kManifoldWords; }
+    size_t manifold_words() const {
+        return scene ? static_cast<size_t>(numi::kSceneManifolds) * numi::kSceneSlotWords
+                     : static_cast<size_t>(model.world.pair_count) * numi::kManifoldWords;
+    }
 
     // Enqueue `steps` control steps reading actions/masks from device memory.
     void enqueue(std::uint32_t steps, const float* actions, const std::uint32_t* masks, float* obs,
@@ -370,6 +439,33 @@ struct MRTaskRolloutHandle {
         const std::uint32_t nobs = model.world.nq + model.world.nv;
         check(cudaMemsetAsync(d_stats.ptr, 0, numi::kStatCount * sizeof(std::uint32_t), s), "clear stats");
         check(cudaMemsetAsync(d_stats.ptr + numi::kStatFirstFailEnv, 0xff, sizeof(std::uint32_t), s), "clear stats");
+        if (scene) {
+            for (std::uint32_t k = 0; k < steps; ++k) {
+                numi::SceneParams p{};
+                p.model = d_smodel.ptr;
+                p.q = d_q.ptr;
+                p.v = d_v.ptr;
+                p.manifolds = d_manifolds.ptr;
+                p.manifold_count = d_mcount.ptr;
+                p.reset_q = d_reset_q.ptr;
+                p.reset_v = d_reset_v.ptr;
+                p.friction_scale = d_friction.ptr;
+                p.reset_masks = masks ? masks + static_cast<size_t>(k) * envs : nullptr;
+                p.observations = obs ? obs + static_cast<size_t>(k) * envs * nobs : nullptr;
+                p.status_codes = status ? status + static_cast<size_t>(k) * envs : nullptr;
+                p.active_contacts = contacts ? contacts + static_cast<size_t>(k) * envs : nullptr;
+                p.stats = d_stats.ptr;
+                p.workspace = d_workspace.ptr;
+                p.env_count = static_cast<int>(envs);
+                p.substeps = static_cast<int>(config.physics_substeps);
+                p.velocity_iterations = static_cast<int>(config.velocity_iterations);
+                p.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
+                check(numi::launch_scene_step(p, s), "scene step launch");
+            }
+            (void)actions;
+            (void)na;
+            return;
+        }
         for (std::uint32_t k = 0; k < steps; ++k) {
             numi::StepParams p{};
             p.model = d_model.ptr;
@@ -507,10 +603,11 @@ MR_API MRTaskRolloutHandle* mr_create_task_rollout(const MRRunManifestC* manifes
         switch (manifest->source) {
             case MR_RUN_SOURCE_SYNTHETIC_CHAIN7: h.model = numi::build_chain7(cfg.seed); break;
             case MR_RUN_SOURCE_SYNTHETIC_TREE29: h.model = numi::build_tree29(cfg.seed); break;
+            case MR_RUN_SOURCE_SYNTHETIC_PILE: h.model = numi::build_pile(cfg.seed); break;
             default:
                 throw std::invalid_argument("unsupported run source " + std::to_string(manifest->source) +
                                             " (robot assets, URDF and world packs are not compiled by this library; "
-                                            "use MR_RUN_SOURCE_SYNTHETIC_CHAIN7 or MR_RUN_SOURCE_SYNTHETIC_TREE29)");
+                                            "use MR_RUN_SOURCE_SYNTHETIC_CHAIN7, _TREE29 or _PILE)");
         }
         if (h.model.world.pair_count > 0 && cfg.velocity_iterations == 0 && cfg.final_velocity_iterations == 0)
             throw std::invalid_argument("contact worlds need at least one velocity iteration");
@@ -518,15 +615,22 @@ MR_API MRTaskRolloutHandle* mr_create_task_rollout(const MRRunManifestC* manifes
         h.envs = cfg.environment_count;
         h.seed = cfg.seed;
         h.h = cfg.control_timestep_seconds / static_cast<float>(cfg.physics_substeps);
-        numi::rt::KernelPlan plan;
-        numi::rt::make_plan(h.model, h.h, plan);
         const numi::CompiledModel& m = h.model;
-        h.contact = plan.contact;
-        h.dmodel = plan.dmodel;
-        h.layout = plan.layout;
-        for (int prec = 0; prec < 2; ++prec) {
-            h.warps_per_block[prec] = plan.warps_per_block[prec];
-            h.resident_warps_per_sm[prec] = plan.resident_warps_per_sm[prec];
+        if (m.scene) {
+            h.scene = true;
+            h.contact = true;
+            h.smodel = pack_scene(m, h.h);
+            check(numi::configure_scene_step_kernel(), "scene kernel attributes");
+        } else {
+            numi::rt::KernelPlan plan;
+            numi::rt::make_plan(h.model, h.h, plan);
+            h.contact = plan.contact;
+            h.dmodel = plan.dmodel;
+            h.layout = plan.layout;
+            for (int prec = 0; prec < 2; ++prec) {
+                h.warps_per_block[prec] = plan.warps_per_block[prec];
+                h.resident_warps_per_sm[prec] = plan.resident_warps_per_sm[prec];
+            }
         }
         check(cudaGetDevice(&h.device), "cudaGetDevice");
         cudaDeviceProp prop{};
@@ -537,8 +641,15 @@ MR_API MRTaskRolloutHandle* mr_create_task_rollout(const MRRunManifestC* manifes
         check(cudaEventCreate(&h.ev_stop), "event");
         check(cudaEventCreateWithFlags(&h.ev_in, cudaEventDisableTiming), "event");
         check(cudaEventCreateWithFlags(&h.ev_out, cudaEventDisableTiming), "event");
-        h.d_model.resize(1);
-        check(cudaMemcpy(h.d_model.ptr, &h.dmodel, sizeof(numi::DeviceModel), cudaMemcpyHostToDevice), "upload model");
+        if (h.scene) {
+            h.d_smodel.resize(1);
+            check(cudaMemcpy(h.d_smodel.ptr, &h.smodel, sizeof(numi::SceneModel), cudaMemcpyHostToDevice), "upload scene model");
+            h.d_mcount.resize(h.envs);
+            h.d_workspace.resize(h.envs * numi::scene_workspace_words());
+        } else {
+            h.d_model.resize(1);
+            check(cudaMemcpy(h.d_model.ptr, &h.dmodel, sizeof(numi::DeviceModel), cudaMemcpyHostToDevice), "upload model");
+        }
         const size_t nq = m.world.nq, nv = m.world.nv;
         h.d_q.resize(h.envs * nq);
         h.d_v.resize(h.envs * nv);
@@ -555,7 +666,7 @@ MR_API MRTaskRolloutHandle* mr_create_task_rollout(const MRRunManifestC* manifes
         h.stats_layout.action_count = m.world.action_count;
         h.stats_layout.actor_observation_count = m.world.nq + m.world.nv;
         h.stats_layout.critic_observation_count = m.world.nq + m.world.nv;
-        h.stats_layout.scene_body_count = 0;
+        h.stats_layout.scene_body_count = m.scene ? m.scene_bodies : 0u;
         h.stats_layout.world_fingerprint = m.fingerprint;
         h.stats_layout.run_fingerprint = m.fingerprint ^ (cfg.seed * 0x9e3779b97f4a7c15ull);
         h.stats_layout.robot_fingerprint = m.fingerprint;
@@ -676,7 +787,7 @@ MR_API int mr_task_rollout_advance_device(MRTaskRolloutHandle* handle, const flo
                                           uint64_t cuda_stream, MRTaskRolloutAdvanceC* advance) {
     return guarded([&] {
         if (!handle) throw std::invalid_argument("handle is null");
-        if (!device_actions) throw std::invalid_argument("device_actions is null");
+        if (!device_actions && handle->model.world.action_count > 0) throw std::invalid_argument("device_actions is null");
         if (control_step_count == 0) throw std::invalid_argument("control_step_count must be positive");
         MRTaskRolloutHandle& h = *handle;
         // The horizon runs (and is graph-captured) on the rollout's own
@@ -745,7 +856,23 @@ MR_API int mr_task_rollout_copy_final_scene_states(const MRTaskRolloutHandle* ha
     return guarded([&] {
         if (!handle) throw std::invalid_argument("handle is null");
         if (output_count != 0 && output == nullptr) throw std::invalid_argument("output is null");
-        if (output_count != 0) throw std::invalid_argument("this world has no scene bodies; output_count must be 0");
+        const MRTaskRolloutHandle& h = *handle;
+        if (!h.scene) {
+            if (output_count != 0) throw std::invalid_argument("this world has no scene bodies; output_count must be 0");
+            return;
+        }
+        const size_t n = h.model.scene_bodies;
+        const size_t need = static_cast<size_t>(h.envs) * n * 13;
+        if (output_count != need) throw std::invalid_argument("output_count must be envs x scene bodies x 13 = " + std::to_string(need));
+        check(cudaStreamSynchronize(h.stream), "sync");
+        std::vector<float> q(static_cast<size_t>(h.envs) * n * 7), v(static_cast<size_t>(h.envs) * n * 6);
+        check(cudaMemcpy(q.data(), h.d_q.ptr, q.size() * sizeof(float), cudaMemcpyDeviceToHost), "q D2H");
+        check(cudaMemcpy(v.data(), h.d_v.ptr, v.size() * sizeof(float), cudaMemcpyDeviceToHost), "v D2H");
+        // Packed [env][body][position xyz, orientation xyzw, linear xyz, angular xyz].
+        for (size_t i = 0; i < static_cast<size_t>(h.envs) * n; ++i) {
+            std::memcpy(output + i * 13, q.data() + i * 7, 7 * sizeof(float));
+            std::memcpy(output + i * 13 + 7, v.data() + i * 6, 6 * sizeof(float));
+        }
     });
 }
 
@@ -767,6 +894,7 @@ static numi::CompiledModel compile_source(uint32_t source, uint64_t seed) {
     switch (source) {
         case MR_RUN_SOURCE_SYNTHETIC_CHAIN7: return numi::build_chain7(seed);
         case MR_RUN_SOURCE_SYNTHETIC_TREE29: return numi::build_tree29(seed);
+        case MR_RUN_SOURCE_SYNTHETIC_PILE: return numi::build_pile(seed);
         default: throw std::invalid_argument("unsupported synthetic source " + std::to_string(source));
     }
 }
@@ -832,6 +960,26 @@ MR_API int mr_task_rollout_set_state(MRTaskRolloutHandle* handle, const float* q
                                  cudaMemcpyHostToDevice), "manifolds H2D");
             else
                 check(cudaMemset(h.d_manifolds.ptr, 0, h.d_manifolds.count * sizeof(float)), "clear manifolds");
+        }
+        if (h.scene) {
+            // Scene tables: leading slots with a non-zero point count are live.
+            std::vector<std::uint32_t> counts(h.envs, 0u);
+            if (manifolds) {
+                const float* words = reinterpret_cast<const float*>(manifolds);
+                for (std::uint32_t e = 0; e < h.envs; ++e) {
+                    const float* t = words + static_cast<size_t>(e) * h.manifold_words();
+                    std::uint32_t c = 0;
+                    while (c < static_cast<std::uint32_t>(numi::kSceneManifolds)) {
+                        std::uint32_t pts;
+                        std::memcpy(&pts, t + c * numi::kSceneSlotWords + 7, sizeof(pts));
+                        if (pts == 0u) break;
+                        ++c;
+                    }
+                    counts[e] = c;
+                }
+            }
+            check(cudaMemcpy(h.d_mcount.ptr, counts.data(), counts.size() * sizeof(std::uint32_t), cudaMemcpyHostToDevice),
+                  "manifold counts H2D");
         }
         if (as_reset_state) {
             h.reset_q.assign(q, q + nq);

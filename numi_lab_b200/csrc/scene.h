@@ -1,0 +1,82 @@
+// Free-body ("scene") worlds: piles of spheres and boxes on a ground plane.
+// Device record, launch parameters and per-environment capacities of the
+// free-body control-step kernel (scene_step.cu).
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "numi_b200.h"
+
+namespace numi {
+
+constexpr int kSceneMaxBodies = 64;
+constexpr int kSceneMaxPairs = kSceneMaxBodies * (kSceneMaxBodies - 1) / 2 + kSceneMaxBodies;
+constexpr int kSceneManifolds = MR_B200_SCENE_MANIFOLDS;  // persistent manifolds per environment
+constexpr int kSceneContacts = 256;    // solver contacts per environment
+constexpr int kSceneCandidates = 512;  // broadphase candidate pairs per environment
+constexpr int kSceneMaxMaterials = 4;
+// Words of one manifold slot of a scene (MRManifoldC layout) plus its pair key.
+constexpr int kSceneSlotWords = MR_B200_SCENE_SLOT_WORDS;
+
+struct alignas(16) SceneModel {
+    std::int32_t nb;  // free bodies; the ground plane is collider nb
+    std::int32_t np;  // compiled pairs
+    float h;
+    float slop;
+    float gravity[4];
+    float max_depenetration;
+    float speculative_scale;
+    float speed_envelope;
+    float reserved0;
+    float thresholds[4];  // breaking separation, drift, merge, normal cosine
+    float4 plane_position;
+    float4 plane_rotation;
+    float4 plane_offsets;  // contact offset, rest offset
+    float4 ground_position;  // pose of the plane's (static) body: manifold
+    float4 ground_rotation;  // anchors on the plane live in this frame
+    std::int32_t plane_material;
+    std::int32_t reserved1[3];
+    // Bodies (one collider each, at the body's centre of mass).
+    std::int32_t shape_type[kSceneMaxBodies];
+    std::int32_t material[kSceneMaxBodies];
+    float4 dims[kSceneMaxBodies];         // sphere radius; box half extents
+    float4 mass[kSceneMaxBodies];         // mass, inverse mass, linear damping, angular damping
+    float4 inv_inertia[kSceneMaxBodies];  // body-frame principal inverse inertia, max linear speed
+    float4 offsets[kSceneMaxBodies];      // contact offset, rest offset, sweep radius, max angular speed
+    float4 material_friction[kSceneMaxMaterials];
+    float4 material_response[kSceneMaxMaterials];
+    // Compiled pairs, ascending by key a * (kSceneMaxBodies + 1) + b (b = nb: plane).
+    std::uint8_t pair_a[kSceneMaxPairs];
+    std::uint8_t pair_b[kSceneMaxPairs];
+    std::uint8_t pair_class[kSceneMaxPairs];
+};
+
+struct SceneParams {
+    const SceneModel* model;
+    float* q;                  // [env][nb][7]: position, orientation xyzw
+    float* v;                  // [env][nb][6]: linear, angular velocity (world)
+    float* manifolds;          // [env][kSceneManifolds][kSceneSlotWords]
+    std::uint32_t* manifold_count;  // [env]
+    const float* reset_q;
+    const float* reset_v;
+    const float* friction_scale;    // [env]
+    const std::uint32_t* reset_masks;  // [env] of this control step, or null
+    float* observations;       // [env][nq + nv] of this control step, or null
+    std::uint32_t* status_codes;
+    std::uint32_t* active_contacts;
+    std::uint32_t* stats;
+    float* workspace;          // [env][scene_workspace_words()]: substep tables, contacts, narrowphase scratch
+    std::int32_t env_count;
+    std::int32_t substeps;
+    std::int32_t velocity_iterations;
+    std::int32_t final_velocity_iterations;
+};
+
+size_t scene_step_smem_bytes();
+size_t scene_workspace_words();
+cudaError_t configure_scene_step_kernel();
+cudaError_t launch_scene_step(const SceneParams& p, cudaStream_t stream);
+
+}  // namespace numi

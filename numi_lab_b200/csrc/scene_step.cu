@@ -1,0 +1,1083 @@
+// Free-body control step on B200: piles of spheres and boxes on a ground
+// plane (numi-lab's scene bodies).  One warp per environment for a whole
+// control step; lanes own bodies (two per lane), compiled pairs, candidate
+// pairs, manifolds and contacts in turn.
+//
+// Stage order per substep follows the reference's MetalWorld graph for scene
+// bodies: prediction (mr_world_predict_scene, MetalWorldContact.metal:
+// 2509-2570: exponential damping and gravity, no gyroscopic term),
+// collider projection with the speculative sweep (Collision.metal:
+// 5960-6030), pair flags over the compiled all-pairs list (Collision.metal:
+// 7905-8180), analytic narrowphase (Collision.cpp:1106-2175 restated:
+// sphere-sphere, sphere-box witness, box-box separating axes with vertex
+// clipping, sphere/box vs plane), persistent manifolds keyed by collider
+// pair, ConstraintIR evaluation, islands (min-root union find,
+// ConstraintSolver.cpp:848-900), the temporalCone block-Jacobi solve with
+// free-body responses, speed clamps and integration, and the per-environment
+// latch: a failed control step publishes nothing, so the environment keeps
+// its step-start state.
+#include "contact.cuh"
+#include "dmath.cuh"
+#include "numi_b200.h"
+#include "scene.h"
+
+#include <cstdint>
+
+namespace numi {
+namespace {
+
+constexpr float kQueryPadS = 0.00000762939453125f;  // MR_COLLISION_QUERY_RELATIVE_PAD
+constexpr float kAabbPadS = 0.00000762939453125f;   // MR_COLLISION_AABB_RELATIVE_PAD
+constexpr float kTinyS = 1.0e-12f;
+constexpr float kTieRel = 1.0e-5f;
+constexpr float kTieAbs = 1.0e-12f;
+constexpr int kRawCap = 8;
+constexpr int kRecWords = 16;                                   // candidate record
+constexpr int kLaneScratch = (4 + kRawCap) * kRecWords + 4 + 56;  // records, ids, new slot
+constexpr int kCw = 40;                                          // contact record words
+
+// Shared-memory layout of one environment (floats): body state, swept
+// bounds, candidate pairs and per-body contact lists -- about 9 KB, so that
+// registers, not shared memory, bound the resident warps.
+constexpr int kOffPos = 0;
+constexpr int kOffQuat = kOffPos + kSceneMaxBodies * 3;
+constexpr int kOffLin = kOffQuat + kSceneMaxBodies * 4;
+constexpr int kOffAng = kOffLin + kSceneMaxBodies * 3;
+constexpr int kOffIiw = kOffAng + kSceneMaxBodies * 3;   // world inverse inertia, sym 6
+constexpr int kOffLo = kOffIiw + kSceneMaxBodies * 6;
+constexpr int kOffHi = kOffLo + kSceneMaxBodies * 3;
+constexpr int kOffMargin = kOffHi + kSceneMaxBodies * 3;
+constexpr int kOffCand = kOffMargin + kSceneMaxBodies;   // u16 candidates
+constexpr int kOffLists = kOffCand + kSceneCandidates / 2;  // start[65], fill[65] (ints)
+constexpr int kOffEntries = kOffLists + 2 * (kSceneMaxBodies + 1);  // 2 * contacts u16 entries
+constexpr int kOffMisc = kOffEntries + kSceneContacts;
+constexpr int kSceneSmemWords = kOffMisc + 32;
+
+// Global workspace of one environment (floats, L2-resident while the
+// environment runs): two substep manifold tables, the contact records and
+// one narrowphase scratch block per lane.
+constexpr int kTableWords = kSceneManifolds * kSceneSlotWords;
+constexpr int kWsTable0 = 0;
+constexpr int kWsTable1 = kWsTable0 + kTableWords;
+constexpr int kWsContacts = kWsTable1 + kTableWords;
+constexpr int kWsLanes = kWsContacts + kSceneContacts * kCw;
+constexpr int kWsWords = (kWsLanes + 32 * kLaneScratch + 31) / 32 * 32;
+
+enum SceneMisc : int { kSmStatus = 0, kSmFail = 1, kSmContacts = 2, kSmManifolds = 3, kSmRaw = 4, kSmCand = 5, kSmIslands = 6 };
+enum SceneCw : int {
+    kScA = 0, kScB = 1, kScRa = 2, kScRb = 5, kScN = 8, kScT = 11, kScBt = 14, kScTarget = 17, kScReg = 20, kScMu = 21,
+    kScLambda = 22, kScPre = 25, kScRelax = 34, kScDelta = 35, kScSlot = 38, kScFlags = 39
+};
+enum CandWord : int { kCdLaS = 0, kCdLbS = 3, kCdFaS = 6, kCdFbS = 7, kCdWpS = 8, kCdSepS = 11, kCdLifeS = 12, kCdImpS = 13 };
+
+__device__ __forceinline__ int ai(float f) { return __float_as_int(f); }
+__device__ __forceinline__ float af(int i) { return __int_as_float(i); }
+
+__device__ __forceinline__ void fail(float* misc, unsigned code, unsigned index) {
+    if (ai(misc[kSmStatus]) == MR_STEP_SUCCESS) {
+        misc[kSmStatus] = af(static_cast<int>(code));
+        misc[kSmFail] = af(static_cast<int>(index));
+    }
+}
+__device__ __forceinline__ bool ok(const float* misc) {
+    __syncwarp();
+    return ai(misc[kSmStatus]) == MR_STEP_SUCCESS;
+}
+
+// World collider of a body or of the ground plane (index nb).
+struct Collider {
+    int type;
+    float3 c;        // centre (= body position; colliders sit at the COM)
+    float4 r;        // orientation
+    float3 half;     // box half extents
+    float radius;
+    float offset;    // contact offset incl. speculative margin
+    float3 lo, hi;   // swept, inflated bounds (finite shapes)
+    float3 normal;   // plane normal
+    float3 bpos;     // pose of the collider's body: the frame of its
+    float4 brot;     // manifold anchors (the ground body for the plane)
+};
+
+__device__ void load_collider(const SceneModel& M, const float* s, int b, Collider& o) {
+    if (b >= M.nb) {
+        o.type = MR_SHAPE_PLANE;
+        o.c = xyz(M.plane_position);
+        o.r = M.plane_rotation;
+        const float3 n = qrot(o.r, f3(0.0f, 1.0f, 0.0f));
+        o.normal = n * rsqrtf(dot3(n, n));
+        o.half = f3(0.0f, 0.0f, 0.0f);
+        o.radius = 0.0f;
+        o.offset = M.plane_offsets.x;
+        o.lo = o.hi = f3(0.0f, 0.0f, 0.0f);
+        o.bpos = xyz(M.ground_position);
+        o.brot = M.ground_rotation;
+        return;
+    }
+    o.type = M.shape_type[b];
+    o.c = ld3(s + kOffPos + b * 3);
+    o.r = ld4(s + kOffQuat + b * 4);
+    const float4 d = M.dims[b];
+    o.half = xyz(d);
+    o.radius = d.x;
+    o.offset = M.offsets[b].x + s[kOffMargin + b];
+    o.lo = ld3(s + kOffLo + b * 3);
+    o.hi = ld3(s + kOffHi + b * 3);
+    o.normal = f3(0.0f, 0.0f, 0.0f);
+    o.bpos = o.c;
+    o.brot = o.r;
+}
+
+__device__ __forceinline__ float collider_scale(const Collider& k) {
+    return fmaxf(fmaxf(maxabs3(k.c), maxabs3(k.half)), fmaxf(fabsf(k.radius), fmaxf(fabsf(k.offset),
+                 fmaxf(maxabs3(k.lo), maxabs3(k.hi)))));
+}
+
+__device__ __forceinline__ float3 box_axis(const Collider& b, int axis) {
+    return qrot(b.r, f3(axis == 0 ? 1.0f : 0.0f, axis == 1 ? 1.0f : 0.0f, axis == 2 ? 1.0f : 0.0f));
+}
+__device__ __forceinline__ float box_radius(const Collider& b, float3 axis) {
+    return fabsf(dot3(axis, box_axis(b, 0))) * b.half.x + fabsf(dot3(axis, box_axis(b, 1))) * b.half.y +
+           fabsf(dot3(axis, box_axis(b, 2))) * b.half.z;
+}
+__device__ __forceinline__ float3 box_vertex(const Collider& b, int v) {
+    return b.c + qrot(b.r, f3((v & 1) ? b.half.x : -b.half.x, (v & 2) ? b.half.y : -b.half.y, (v & 4) ? b.half.z : -b.half.z));
+}
+__device__ __forceinline__ bool inside_inflated(float3 p, const Collider& b, float inflation) {
+    const float3 l = qrotinv(b.r, p - b.c);
+    return fabsf(l.x) <= b.half.x + inflation && fabsf(l.y) <= b.half.y + inflation && fabsf(l.z) <= b.half.z + inflation;
+}
+__device__ __forceinline__ float3 box_support(const Collider& b, float3 d) {
+    float3 out = b.c;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float3 ax = box_axis(b, a);
+        const float he = a == 0 ? b.half.x : (a == 1 ? b.half.y : b.half.z);
+        out = out + ax * (dot3(d, ax) >= 0.0f ? he : -he);
+    }
+    return out;
+}
+__device__ __forceinline__ float3 coincident_normal(unsigned a, unsigned b) {
+    const unsigned hsh = a * 73856093u ^ b * 19349663u;
+    const unsigned axis = hsh % 3u;
+    const float sign = (hsh & 4u) == 0u ? 1.0f : -1.0f;
+    return f3(axis == 0u ? sign : 0.0f, axis == 1u ? sign : 0.0f, axis == 2u ? sign : 0.0f);
+}
+
+// Raw contacts of one pair into candidate records (anchors in the bodies'
+// frames, features, world midpoint, separation); returns the count and the
+// pair's normal (A -> B).  Collision.cpp generateContacts, restated.
+struct RawSink {
+    float* rec;
+    int count;
+    float3 posA, posB;
+    float4 rotA, rotB;
+    __device__ void add(float3 pa, float3 pb, float sep, unsigned fa, unsigned fb) {
+        if (count >= kRawCap) return;
+        float* r = rec + count * kRecWords;
+        st3(r + kCdLaS, qrotinv(rotA, pa - posA));
+        st3(r + kCdLbS, qrotinv(rotB, pb - posB));
+        r[kCdFaS] = af(static_cast<int>(fa));
+        r[kCdFbS] = af(static_cast<int>(fb));
+        st3(r + kCdWpS, 0.5f * (pa + pb));
+        r[kCdSepS] = sep;
+        ++count;
+    }
+};
+
+__device__ bool narrowphase(const Collider& A, const Collider& B, int cls, unsigned ia, unsigned ib, float accepted,
+                            RawSink& sink, float3& normal) {
+    if (cls == MR_COLLISION_PAIR_SPHERE_SPHERE) {
+        const float3 delta = B.c - A.c;
+        const float d = len3(delta);
+        normal = d > kTinyS ? delta * (1.0f / d) : coincident_normal(ia, ib);
+        const float sep = d - A.radius - B.radius;
+        if (sep <= accepted)
+            sink.add(A.c + normal * A.radius, B.c - normal * B.radius, sep, feature_key(MR_SHAPE_SPHERE, 0u),
+                     feature_key(MR_SHAPE_SPHERE, 0u));
+        return true;
+    }
+    if (cls == MR_COLLISION_PAIR_SPHERE_BOX) {
+        const bool sphere_a = A.type == MR_SHAPE_SPHERE;
+        const Collider& sp = sphere_a ? A : B;
+        const Collider& bx = sphere_a ? B : A;
+        const float3 lc = qrotinv(bx.r, sp.c - bx.c);
+        float3 cl = f3(fminf(fmaxf(lc.x, -bx.half.x), bx.half.x), fminf(fmaxf(lc.y, -bx.half.y), bx.half.y),
+                       fminf(fmaxf(lc.z, -bx.half.z), bx.half.z));
+        const float3 ld = cl - lc;
+        const float dist = len3(ld);
+        float3 n;
+        float sep;
+        unsigned feat;
+        if (dist > kTinyS) {
+            n = qrot(bx.r, ld * (1.0f / dist));
+            sep = dist - sp.radius;
+            auto region = [](float c, float he) { return c < -he ? 0u : (c > he ? 2u : 1u); };
+            feat = region(lc.x, bx.half.x) + 3u * region(lc.y, bx.half.y) + 9u * region(lc.z, bx.half.z);
+        } else {
+            const float dx = bx.half.x - fabsf(lc.x), dy = bx.half.y - fabsf(lc.y), dz = bx.half.z - fabsf(lc.z);
+            int axis = 0;
+            float dm = dx;
+            if (dy < dm) { axis = 1; dm = dy; }
+            if (dz < dm) { axis = 2; dm = dz; }
+            const float coord = axis == 0 ? lc.x : (axis == 1 ? lc.y : lc.z);
+            const float sign = coord >= 0.0f ? 1.0f : -1.0f;
+            const float3 outward = f3(axis == 0 ? sign : 0.0f, axis == 1 ? sign : 0.0f, axis == 2 ? sign : 0.0f);
+            if (axis == 0) cl.x = sign * bx.half.x;
+            else if (axis == 1) cl.y = sign * bx.half.y;
+            else cl.z = sign * bx.half.z;
+            n = qrot(bx.r, -outward);
+            sep = -dm - sp.radius;
+            feat = 27u + 2u * static_cast<unsigned>(axis) + (sign > 0.0f ? 1u : 0u);
+        }
+        const float3 box_point = bx.c + qrot(bx.r, cl);
+        if (sep <= accepted) {
+            const float3 sphere_point = sp.c + n * sp.radius;
+            if (sphere_a)
+                sink.add(sphere_point, box_point, sep, feature_key(MR_SHAPE_SPHERE, 0u), feature_key(MR_SHAPE_BOX, feat));
+            else
+                sink.add(box_point, sphere_point, sep, feature_key(MR_SHAPE_BOX, feat), feature_key(MR_SHAPE_SPHERE, 0u));
+        }
+        normal = sphere_a ? n : -n;
+        return true;
+    }
+    if (cls == MR_COLLISION_PAIR_BOX_BOX) {
+        const float3 cd = B.c - A.c;
+        float best_sep = -INFINITY;
+        float3 best_n = coincident_normal(ia, ib);
+        int best_axis = 0;
+        // Axes are numbered in the list of accepted axes: a skipped
+        // (parallel-edge) cross axis shifts the later indices, and the
+        // index names the face feature (128 + index).
+        int index = -1;
+        for (int k = 0; k < 15; ++k) {
+            float3 axis;
+            if (k < 3) axis = box_axis(A, k);
+            else if (k < 6) axis = box_axis(B, k - 3);
+            else {
+                const float3 cr = cross3(box_axis(A, (k - 6) / 3), box_axis(B, (k - 6) % 3));
+                const float sq = dot3(cr, cr);
+                if (!(sq > 1.0e-24f)) continue;
+                axis = cr * rsqrtf(sq);
+            }
+            ++index;
+            const float proj = dot3(cd, axis);
+            if (proj < 0.0f || (proj == 0.0f && dot3(axis, best_n) < 0.0f)) axis = -axis;
+            const float sep = fabsf(proj) - box_radius(A, axis) - box_radius(B, axis);
+            if (sep > accepted) {
+                normal = axis;
+                return true;  // separated: no contact
+            }
+            const float tol = 1.0e-12f * (1.0f + fmaxf(fabsf(best_sep), fabsf(sep)));
+            if (!isfinite(best_sep) || sep > best_sep + tol || (fabsf(sep - best_sep) <= tol && index < best_axis)) {
+                best_sep = sep;
+                best_n = axis;
+                best_axis = index;
+            }
+        }
+        normal = best_n;
+        const float near_b = dot3(B.c, best_n) - box_radius(B, best_n);
+        const float far_a = dot3(A.c, best_n) + box_radius(A, best_n);
+        for (int v = 0; v < 8; ++v) {
+            const float3 pa = box_vertex(A, v);
+            if (!inside_inflated(pa, B, accepted)) continue;
+            const float sep = near_b - dot3(pa, best_n);
+            if (sep <= accepted)
+                sink.add(pa, pa + best_n * sep, sep, feature_key(MR_SHAPE_BOX, static_cast<unsigned>(v)),
+                         feature_key(MR_SHAPE_BOX, 128u + static_cast<unsigned>(best_axis)));
+        }
+        for (int v = 0; v < 8; ++v) {
+            const float3 pb = box_vertex(B, v);
+            if (!inside_inflated(pb, A, accepted)) continue;
+            const float sep = dot3(pb, best_n) - far_a;
+            if (sep <= accepted)
+                sink.add(pb - best_n * sep, pb, sep, feature_key(MR_SHAPE_BOX, 128u + static_cast<unsigned>(best_axis)),
+                         feature_key(MR_SHAPE_BOX, static_cast<unsigned>(v)));
+        }
+        if (sink.count == 0) {
+            const float3 pa = box_support(A, best_n);
+            const float3 pb = box_support(B, -best_n);
+            sink.add(pa, pb, dot3(pb - pa, best_n), feature_key(MR_SHAPE_BOX, 256u + static_cast<unsigned>(best_axis)),
+                     feature_key(MR_SHAPE_BOX, 256u + static_cast<unsigned>(best_axis)));
+        }
+        return true;
+    }
+    // Finite shape (A) against the plane (B).
+    const float3 pn = B.normal;
+    normal = -pn;
+    const unsigned plane_key = feature_key(MR_SHAPE_PLANE, 0u);
+    if (cls == MR_COLLISION_PAIR_SPHERE_PLANE) {
+        const float3 surface = A.c - pn * A.radius;
+        const float sep = dot3(pn, surface - B.c);
+        if (sep <= accepted) sink.add(surface, surface - pn * sep, sep, feature_key(MR_SHAPE_SPHERE, 0u), plane_key);
+        return true;
+    }
+    if (cls == MR_COLLISION_PAIR_BOX_PLANE) {
+        for (int v = 0; v < 8; ++v) {
+            const float3 w = box_vertex(A, v);
+            const float sep = dot3(pn, w - B.c);
+            if (sep <= accepted) sink.add(w, w - pn * sep, sep, feature_key(MR_SHAPE_BOX, static_cast<unsigned>(v)), plane_key);
+        }
+        return true;
+    }
+    return false;
+}
+
+// Persistent manifold of one pair from its raw records and old slot
+// (buildPersistentWorldManifold): break thresholds, feature-then-proximity
+// matching, greedy reduction to four with the precision-independent tie
+// rule (scores within a relative 1e-5 go to the smaller feature key), then
+// canonical feature order.  `scratch` holds four old records ahead of the
+// raw records, and 16 candidate-id bytes after them.  Returns the point
+// count, or -1 when non-finite.
+__device__ __forceinline__ unsigned long long rkey(const float* r) {
+    return (static_cast<unsigned long long>(static_cast<unsigned>(ai(r[kCdFaS]))) << 32) | static_cast<unsigned>(ai(r[kCdFbS]));
+}
+
+__device__ int build_manifold(const SceneModel& M, const float* old_slot, int nraw, float3 raw_normal, float* scratch,
+                              float* out, float3 posA, float4 rotA, float3 posB, float4 rotB) {
+    const float* raw = scratch + 4 * kRecWords;
+    unsigned char* ids = reinterpret_cast<unsigned char*>(scratch + (4 + kRawCap) * kRecWords);
+    if (nraw == 0) {
+        for (int k = 0; k < 56; ++k) out[k] = 0.0f;
+        return 0;
+    }
+    for (int i = 0; i < nraw; ++i) {
+        const float* r = raw + i * kRecWords;
+        if (!isfinite(r[kCdSepS]) || !finite3(ld3(r + kCdWpS)) || !finite3(ld3(r + kCdLaS)) || !finite3(ld3(r + kCdLbS)))
+            return -1;
+    }
+    const float3 nw = raw_normal * (1.0f / len3(raw_normal));
+    if (!finite3(nw) || dot3(nw, nw) < 0.9999f) return -1;
+    const float4 thr = make_float4(M.thresholds[0], M.thresholds[1], M.thresholds[2], M.thresholds[3]);
+    int nc = 0;
+    bool old_ok = false;
+    float3 transported = f3(0.0f, 0.0f, 0.0f);
+    float old_age = 0.0f;
+    const int old_count = old_slot ? ai(old_slot[7]) : 0;
+    if (old_count > 0 && old_count <= 4) {
+        float3 on = qrot(rotA, ld3(old_slot));
+        on = on * (1.0f / len3(on));
+        old_ok = finite3(on) && dot3(on, nw) >= thr.w;
+        if (old_ok) {
+            const float3 ot = qrot(rotA, ld3(old_slot + 4));
+            transported = ot - nw * dot3(ot, nw);
+            old_age = old_slot[3];
+            for (int i = 0; i < old_count; ++i) {
+                const float* op = old_slot + 8 + i * 12;
+                const float3 pa = posA + qrot(rotA, ld3(op));
+                const float3 pb = posB + qrot(rotB, ld3(op + 3));
+                const float3 delta = pb - pa;
+                const float sep = dot3(delta, nw);
+                const float3 tan = delta - nw * sep;
+                if (sep > thr.x || len3(tan) > thr.y) continue;
+                float* rec = scratch + i * kRecWords;
+                for (int k = 0; k < 8; ++k) rec[k] = op[k];
+                const unsigned life = static_cast<unsigned>(ai(op[8]));
+                rec[kCdLifeS] = af(static_cast<int>(life == 0xffffffffu ? 0xffffffffu : life + 1u));
+                rec[kCdImpS + 0] = op[9];
+                rec[kCdImpS + 1] = op[10];
+                rec[kCdImpS + 2] = op[11];
+                st3(rec + kCdWpS, 0.5f * (pa + pb));
+                rec[kCdSepS] = sep;
+                ids[nc++] = static_cast<unsigned char>((i << 4) | i);
+            }
+        }
+    }
+    const float merge2 = thr.z * thr.z;
+    for (int r = 0; r < nraw; ++r) {
+        const float* rr = raw + r * kRecWords;
+        const float3 la = ld3(rr + kCdLaS), lb = ld3(rr + kCdLbS);
+        const int fa = ai(rr[kCdFaS]), fb = ai(rr[kCdFbS]);
+        int match = -1;
+        for (int k = 0; k < nc && match < 0; ++k) {
+            const float* g = scratch + (ids[k] & 15u) * kRecWords;
+            if (ai(g[kCdFaS]) == fa && ai(g[kCdFbS]) == fb) match = k;
+        }
+        for (int k = 0; k < nc && match < 0; ++k) {
+            const float* g = scratch + (ids[k] & 15u) * kRecWords;
+            const float3 da = ld3(g + kCdLaS) - la, db = ld3(g + kCdLbS) - lb;
+            if (dot3(da, da) + dot3(db, db) <= 2.0f * merge2) match = k;
+        }
+        if (match < 0) {
+            if (nc >= 4 + kRawCap) return -1;
+            ids[nc++] = static_cast<unsigned char>((15u << 4) | (4u + r));
+        } else {
+            ids[match] = static_cast<unsigned char>((ids[match] & 0xf0u) | (4u + r));
+        }
+    }
+    if (nc > 4) {
+        for (int i = 1; i < nc; ++i) {
+            const unsigned char val = ids[i];
+            const float* gv = scratch + (val & 15u) * kRecWords;
+            const float sv = gv[kCdSepS];
+            const unsigned long long kv = rkey(gv);
+            int d = i;
+            while (d > 0) {
+                const float* gp = scratch + (ids[d - 1] & 15u) * kRecWords;
+                const float sp = gp[kCdSepS];
+                if (!(sv < sp || (sv == sp && kv < rkey(gp)))) break;
+                ids[d] = ids[d - 1];
+                --d;
+            }
+            ids[d] = val;
+        }
+        unsigned selected = 1u;
+        unsigned chosen = 0u;
+        int chosen_count = 1;
+        const float3 w0 = ld3(scratch + (ids[0] & 15u) * kRecWords + kCdWpS);
+        float3 w1 = w0;
+        for (int stage = 1; stage < 4; ++stage) {
+            int best = -1;
+            float best_score = -1.0f;
+            unsigned long long best_f = ~0ull;
+            for (int i = 0; i < nc; ++i) {
+                if (selected & (1u << i)) continue;
+                const float* gi = scratch + (ids[i] & 15u) * kRecWords;
+                const float3 wi = ld3(gi + kCdWpS);
+                float score;
+                if (stage == 1) {
+                    const float3 dl = wi - w0;
+                    const float3 t = dl - nw * dot3(dl, nw);
+                    score = dot3(t, t);
+                } else if (stage == 2) {
+                    score = fabsf(dot3(cross3(w1 - w0, wi - w0), nw));
+                } else {
+                    score = INFINITY;
+                    for (int k = 0; k < chosen_count; ++k) {
+                        const int ck = static_cast<int>((chosen >> (8 * k)) & 0xffu);
+                        const float3 dl = wi - ld3(scratch + (ids[ck] & 15u) * kRecWords + kCdWpS);
+                        const float3 t = dl - nw * dot3(dl, nw);
+                        score = fminf(score, dot3(t, t));
+                    }
+                }
+                const unsigned long long f = rkey(gi);
+                const float tol = fmaxf(kTieAbs, kTieRel * fmaxf(fabsf(score), fabsf(best_score)));
+                if (score > best_score + tol || (fabsf(score - best_score) <= tol && f < best_f)) {
+                    best = i;
+                    best_score = score;
+                    best_f = f;
+                }
+            }
+            if (best >= 0) {
+                chosen |= static_cast<unsigned>(best) << (8 * chosen_count);
+                ++chosen_count;
+                selected |= 1u << best;
+                if (stage == 1) w1 = ld3(scratch + (ids[best] & 15u) * kRecWords + kCdWpS);
+            }
+        }
+        unsigned packed = 0u;
+        for (int k = 0; k < chosen_count; ++k) packed |= static_cast<unsigned>(ids[(chosen >> (8 * k)) & 0xffu]) << (8 * k);
+        for (int k = 0; k < chosen_count; ++k) ids[k] = static_cast<unsigned char>((packed >> (8 * k)) & 0xffu);
+        nc = chosen_count;
+    }
+    for (int i = 1; i < nc; ++i) {
+        const unsigned char val = ids[i];
+        const unsigned long long f = rkey(scratch + (val & 15u) * kRecWords);
+        int d = i;
+        while (d > 0 && f < rkey(scratch + (ids[d - 1] & 15u) * kRecWords)) {
+            ids[d] = ids[d - 1];
+            --d;
+        }
+        ids[d] = val;
+    }
+    float3 tw = transported;
+    if (!old_ok || !finite3(tw) || dot3(tw, tw) <= 1.0e-12f) tw = stable_tangent(nw);
+    else tw = tw * (1.0f / len3(tw));
+    st3(out, qrotinv(rotA, nw));
+    out[3] = old_ok ? fminf(old_age + 1.0f, 65535.0f) : 0.0f;
+    st3(out + 4, qrotinv(rotA, tw));
+    out[7] = af(nc);
+    for (int i = 0; i < 4; ++i) {
+        float* op = out + 8 + i * 12;
+        if (i < nc) {
+            const unsigned id = ids[i];
+            const float* g = scratch + (id & 15u) * kRecWords;
+            for (int k = 0; k < 8; ++k) op[k] = g[k];
+            if ((id >> 4) == 15u) {
+                op[8] = af(0);
+                op[9] = op[10] = op[11] = 0.0f;
+            } else {
+                const float* hrec = scratch + (id >> 4) * kRecWords;
+                op[8] = hrec[kCdLifeS];
+                op[9] = hrec[kCdImpS + 0];
+                op[10] = hrec[kCdImpS + 1];
+                op[11] = hrec[kCdImpS + 2];
+            }
+        } else {
+            for (int k = 0; k < 12; ++k) op[k] = 0.0f;
+        }
+    }
+    return nc;
+}
+
+// World inverse inertia R diag(inv) R^T, packed (xx, yx, yy, zx, zy, zz).
+__device__ __forceinline__ void world_inv_inertia(float4 q, float4 inv, float* out) {
+    const float3 c0 = qrot(q, f3(1.0f, 0.0f, 0.0f)), c1 = qrot(q, f3(0.0f, 1.0f, 0.0f)), c2 = qrot(q, f3(0.0f, 0.0f, 1.0f));
+    const float R[3][3] = {{c0.x, c1.x, c2.x}, {c0.y, c1.y, c2.y}, {c0.z, c1.z, c2.z}};
+    const float d[3] = {inv.x, inv.y, inv.z};
+    int k = 0;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j <= i; ++j) {
+            float acc = 0.0f;
+            for (int m = 0; m < 3; ++m) acc = fmaf(R[i][m] * d[m], R[j][m], acc);
+            out[k++] = acc;
+        }
+}
+__device__ __forceinline__ float3 sym3_mul(const float* S, float3 x) {
+    return f3(S[0] * x.x + S[1] * x.y + S[3] * x.z, S[1] * x.x + S[2] * x.y + S[4] * x.z, S[3] * x.x + S[4] * x.y + S[5] * x.z);
+}
+
+__global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
+    extern __shared__ float4 smem4[];
+    float* s = reinterpret_cast<float*>(smem4);
+    const int env = blockIdx.x;
+    if (env >= p.env_count) return;
+    const int lane = threadIdx.x;
+    const SceneModel& M = *p.model;
+    const int nb = M.nb;
+    const int nq = nb * 7, nv = nb * 6;
+    float* misc = s + kOffMisc;
+    const float h = M.h;
+    if (lane < 32) misc[lane] = 0.0f;
+    const bool reset = p.reset_masks != nullptr && p.reset_masks[env] != 0u;
+    const float* srcq = (reset ? p.reset_q : p.q) + static_cast<size_t>(env) * nq;
+    const float* srcv = (reset ? p.reset_v : p.v) + static_cast<size_t>(env) * nv;
+    for (int b = lane; b < nb; b += 32) {
+        st3(s + kOffPos + b * 3, ld3(srcq + b * 7));
+        st4(s + kOffQuat + b * 4, ld4(srcq + b * 7 + 3));
+        st3(s + kOffLin + b * 3, ld3(srcv + b * 6));
+        st3(s + kOffAng + b * 3, ld3(srcv + b * 6 + 3));
+    }
+    // Manifold table (sorted by pair key); a reset clears it.  Substeps
+    // alternate between the two workspace tables; the environment's own
+    // table is read by the first substep and written only on success.
+    float* ws = p.workspace + static_cast<size_t>(env) * kWsWords;
+    float* persistent = p.manifolds + static_cast<size_t>(env) * kTableWords;
+    const float* cur_table = persistent;
+    int mcount = reset ? 0 : static_cast<int>(p.manifold_count[env]);
+    const float friction_scale = p.friction_scale[env];
+    __syncwarp();
+
+    for (int sub = 0; sub < p.substeps; ++sub) {
+        const bool final_substep = sub + 1 == p.substeps;
+        // Prediction, world inverse inertia, swept bounds.
+        for (int b = lane; b < nb; b += 32) {
+            const float4 m = M.mass[b];
+            float3 lin = ld3(s + kOffLin + b * 3), ang = ld3(s + kOffAng + b * 3);
+            lin = expf(-h * m.z) * lin + h * f3(M.gravity[0], M.gravity[1], M.gravity[2]);
+            ang = expf(-h * m.w) * ang;
+            if (!finite3(lin) || !finite3(ang)) fail(misc, MR_STEP_NONFINITE_RESULT, static_cast<unsigned>(b));
+            st3(s + kOffLin + b * 3, lin);
+            st3(s + kOffAng + b * 3, ang);
+            float4 q = ld4(s + kOffQuat + b * 4);
+            float4 qn;
+            if (!qnormalize(q, qn, true)) {
+                fail(misc, MR_STEP_NONFINITE_INPUT, static_cast<unsigned>(b));
+                qn = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+            }
+            const float3 c = ld3(s + kOffPos + b * 3);
+            if (!finite3(c)) fail(misc, MR_STEP_NONFINITE_INPUT, static_cast<unsigned>(b));
+            world_inv_inertia(qn, M.inv_inertia[b], s + kOffIiw + b * 6);
+            // Speculative sweep over the substep (Collision.metal:5960-6030).
+            const float4 off = M.offsets[b];
+            const float3 fc = c + h * lin;
+            float4 fr = qmul(so3_increment(h * ang, false), qn);
+            fr = qscale(fr, rsqrtf(qdot(fr, fr)));
+            const float cosv = fminf(fmaxf(fabsf(qdot(qn, fr)), 0.0f), 1.0f);
+            const float chord = 2.0f * off.z * sqrtf(fmaxf(0.0f, 1.0f - cosv * cosv));
+            const float envelope = fminf(len3(fc - c) + chord, h * M.speed_envelope);
+            const float margin = M.speculative_scale * envelope;
+            s[kOffMargin + b] = margin;
+            const float4 dm = M.dims[b];
+            float3 e0, e1;
+            if (M.shape_type[b] == MR_SHAPE_SPHERE) {
+                e0 = e1 = f3(dm.x, dm.x, dm.x);
+            } else {
+                auto ext = [&](float4 r) {
+                    const float3 bx = qrot(r, f3(1.0f, 0.0f, 0.0f)), by = qrot(r, f3(0.0f, 1.0f, 0.0f)), bz = qrot(r, f3(0.0f, 0.0f, 1.0f));
+                    return f3(fabsf(bx.x), fabsf(bx.y), fabsf(bx.z)) * dm.x + f3(fabsf(by.x), fabsf(by.y), fabsf(by.z)) * dm.y +
+                           f3(fabsf(bz.x), fabsf(bz.y), fabsf(bz.z)) * dm.z;
+                };
+                e0 = ext(qn);
+                e1 = ext(fr);
+            }
+            const float3 oo = f3(off.x, off.x, off.x);
+            float3 lo = f3(fminf(c.x - e0.x, fc.x - e1.x), fminf(c.y - e0.y, fc.y - e1.y), fminf(c.z - e0.z, fc.z - e1.z)) - oo;
+            float3 hi = f3(fmaxf(c.x + e0.x, fc.x + e1.x), fmaxf(c.y + e0.y, fc.y + e1.y), fmaxf(c.z + e0.z, fc.z + e1.z)) + oo;
+            const float3 sc = f3(fmaxf(fabsf(lo.x), fabsf(hi.x)) + 1.0f, fmaxf(fabsf(lo.y), fabsf(hi.y)) + 1.0f,
+                                 fmaxf(fabsf(lo.z), fabsf(hi.z)) + 1.0f);
+            lo = lo - sc * kAabbPadS - f3(margin, margin, margin);
+            hi = hi + sc * kAabbPadS + f3(margin, margin, margin);
+            st3(s + kOffLo + b * 3, lo);
+            st3(s + kOffHi + b * 3, hi);
+            st4(s + kOffQuat + b * 4, qn);
+        }
+        if (!ok(misc)) break;
+
+        // Pair flags over the compiled list, compacted in pair order.
+        std::uint16_t* cand = reinterpret_cast<std::uint16_t*>(s + kOffCand);
+        int ncand = 0;
+        bool overflow = false;
+        for (int base = 0; base < M.np; base += 32) {
+            const int pi = base + lane;
+            bool flag = false;
+            if (pi < M.np) {
+                const int a = M.pair_a[pi], b = M.pair_b[pi];
+                const float3 la = ld3(s + kOffLo + a * 3), ha = ld3(s + kOffHi + a * 3);
+                if (b >= nb) {
+                    const float3 pn = qrot(M.plane_rotation, f3(0.0f, 1.0f, 0.0f));
+                    const float3 n = pn * rsqrtf(dot3(pn, pn));
+                    const float3 center = 0.5f * (la + ha), halfx = 0.5f * (ha - la);
+                    const float off = M.offsets[a].x + s[kOffMargin + a];
+                    const float scale = fmaxf(fmaxf(maxabs3(xyz(M.plane_position)), maxabs3(la)),
+                                              fmaxf(maxabs3(ha), fmaxf(fabsf(M.plane_offsets.x), fabsf(off))));
+                    const float3 an = f3(fabsf(n.x), fabsf(n.y), fabsf(n.z));
+                    flag = dot3(n, center - xyz(M.plane_position)) - dot3(an, halfx) <= M.plane_offsets.x + (scale + 1.0f) * kQueryPadS;
+                } else {
+                    const float3 lb = ld3(s + kOffLo + b * 3), hb = ld3(s + kOffHi + b * 3);
+                    flag = la.x <= hb.x && lb.x <= ha.x && la.y <= hb.y && lb.y <= ha.y && la.z <= hb.z && lb.z <= ha.z;
+                }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, flag);
+            const int at = ncand + __popc(m & ((1u << lane) - 1u));
+            if (flag) {
+                if (at < kSceneCandidates) cand[at] = static_cast<std::uint16_t>(pi);
+                else overflow = true;
+            }
+            ncand += __popc(m);
+        }
+        if (__any_sync(0xffffffffu, overflow)) {
+            if (lane == 0) fail(misc, MR_STEP_PAIR_CAPACITY_OVERFLOW, static_cast<unsigned>(ncand));
+            __syncwarp();
+            break;
+        }
+        if (lane == 0) misc[kSmCand] = af(max(ai(misc[kSmCand]), ncand));
+        __syncwarp();
+
+        // Narrowphase + manifolds, 32 candidates at a time.
+        const float* old_table = cur_table;
+        float* new_table = ws + ((sub & 1) ? kWsTable1 : kWsTable0);
+        float* scratch = ws + kWsLanes + lane * kLaneScratch;
+        float* staged = scratch + (4 + kRawCap) * kRecWords + 4;
+        int ncount = 0, raw_total = 0;
+        bool bad = false, mover = false;
+        for (int base = 0; base < ncand; base += 32) {
+            const int ci = base + lane;
+            int np_ = 0, nraw = 0;
+            unsigned key = 0u;
+            if (ci < ncand) {
+                const int pi = cand[ci];
+                const int a = M.pair_a[pi], b = M.pair_b[pi];
+                key = static_cast<unsigned>(a * (kSceneMaxBodies + 1) + b);
+                // Old manifold of this pair (table sorted by key).
+                const float* old_slot = nullptr;
+                int lo_i = 0, hi_i = mcount - 1;
+                while (lo_i <= hi_i) {
+                    const int mid = (lo_i + hi_i) >> 1;
+                    const unsigned mk = static_cast<unsigned>(ai(old_table[mid * kSceneSlotWords + 56]));
+                    if (mk == key) { old_slot = old_table + mid * kSceneSlotWords; break; }
+                    if (mk < key) lo_i = mid + 1;
+                    else hi_i = mid - 1;
+                }
+                Collider A, B;
+                load_collider(M, s, a, A);
+                load_collider(M, s, b, B);
+                const float accepted = A.offset + B.offset + (fmaxf(collider_scale(A), collider_scale(B)) + 1.0f) * kQueryPadS;
+                RawSink sink{scratch + 4 * kRecWords, 0, A.bpos, B.bpos, A.brot, B.brot};
+                float3 normal = f3(0.0f, 0.0f, 1.0f);
+                narrowphase(A, B, M.pair_class[pi], static_cast<unsigned>(a), static_cast<unsigned>(b), accepted, sink, normal);
+                nraw = sink.count;
+                np_ = build_manifold(M, old_slot, nraw, normal, scratch, staged, A.bpos, A.brot, B.bpos, B.brot);
+                if (np_ < 0) { bad = true; np_ = 0; }
+            }
+            raw_total += nraw;
+            const unsigned m = __ballot_sync(0xffffffffu, np_ > 0);
+            const int at = ncount + __popc(m & ((1u << lane) - 1u));
+            if (np_ > 0) {
+                if (at < kSceneManifolds) {
+                    float* dst = new_table + at * kSceneSlotWords;
+                    for (int k = 0; k < 56; ++k) dst[k] = staged[k];
+                    dst[56] = af(static_cast<int>(key));
+                } else {
+                    mover = true;
+                }
+            }
+            ncount += __popc(m);
+        }
+        raw_total = __reduce_add_sync(0xffffffffu, raw_total);
+        if (__any_sync(0xffffffffu, bad)) {
+            if (lane == 0) fail(misc, MR_STEP_NONFINITE_RESULT, 0u);
+            __syncwarp();
+            break;
+        }
+        if (__any_sync(0xffffffffu, mover)) {
+            if (lane == 0) fail(misc, MR_STEP_MANIFOLD_CAPACITY_OVERFLOW, static_cast<unsigned>(ncount));
+            __syncwarp();
+            break;
+        }
+        __syncwarp();
+        cur_table = new_table;
+        mcount = ncount;
+        float* tab = new_table;
+        if (lane == 0) {
+            misc[kSmManifolds] = af(max(ai(misc[kSmManifolds]), mcount));
+            misc[kSmRaw] = af(max(ai(misc[kSmRaw]), raw_total));
+        }
+        __syncwarp();
+
+        // Contact records in manifold order (lane per manifold).
+        float* C = ws + kWsContacts;
+        int total = 0;
+        for (int base = 0; base < mcount; base += 32) {
+            const int mi = base + lane;
+            const int cnt = mi < mcount ? ai(tab[mi * kSceneSlotWords + 7]) : 0;
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const int first = total + incl - cnt;
+            total += __shfl_sync(0xffffffffu, incl, 31);
+            if (cnt > 0 && first + cnt <= kSceneContacts) {
+                const float* slot = tab + mi * kSceneSlotWords;
+                const unsigned key = static_cast<unsigned>(ai(slot[56]));
+                const int a = static_cast<int>(key / (kSceneMaxBodies + 1)), b = static_cast<int>(key % (kSceneMaxBodies + 1));
+                const bool plane_b = b >= nb;
+                const float3 posA = ld3(s + kOffPos + a * 3);
+                const float4 rotA = ld4(s + kOffQuat + a * 4);
+                const float3 posB = plane_b ? xyz(M.ground_position) : ld3(s + kOffPos + b * 3);
+                const float4 rotB = plane_b ? M.ground_rotation : ld4(s + kOffQuat + b * 4);
+                float3 nw = qrot(rotA, ld3(slot));
+                nw = nw * (1.0f / len3(nw));
+                float3 tw = qrot(rotA, ld3(slot + 4));
+                tw = tw - nw * dot3(tw, nw);
+                tw = dot3(tw, tw) > 1.0e-12f ? tw * (1.0f / len3(tw)) : stable_tangent(nw);
+                const float3 bw = cross3(nw, tw);
+                const int ma = M.material[a], mb = plane_b ? M.plane_material : M.material[b];
+                const float4 fa = M.material_friction[ma], fb = M.material_friction[mb];
+                const float mu_s = sqrtf(fmaxf(0.0f, fa.x * fb.x)) * friction_scale;
+                const float mu_d = sqrtf(fmaxf(0.0f, fa.y * fb.y)) * friction_scale;
+                const float4 ra = M.material_response[ma], rb = M.material_response[mb];
+                const float rest = M.offsets[a].y + (plane_b ? M.plane_offsets.y : M.offsets[b].y);
+                for (int i = 0; i < cnt; ++i) {
+                    const float* op = slot + 8 + i * 12;
+                    float* c = C + (first + i) * kCw;
+                    const float3 pa = posA + qrot(rotA, ld3(op));
+                    const float3 pb = posB + qrot(rotB, ld3(op + 3));
+                    const float3 pw = 0.5f * (pa + pb);
+                    const float sep = dot3(pb - pa, nw) - rest;
+                    c[kScA] = af(a);
+                    c[kScB] = af(plane_b ? -1 : b);
+                    st3(c + kScRa, pw - posA);
+                    st3(c + kScRb, pw - posB);
+                    st3(c + kScN, nw);
+                    st3(c + kScT, tw);
+                    st3(c + kScBt, bw);
+                    const bool new_impact = static_cast<unsigned>(ai(op[8])) == 0u;
+                    c[kScFlags] = af(new_impact ? 1 : 0);
+                    c[kScSlot] = af(mi * 4 + i);
+                    c[kScLambda + 0] = op[9];
+                    c[kScLambda + 1] = op[10];
+                    c[kScLambda + 2] = op[11];
+                    c[kScTarget + 0] = sep > 0.0f ? -sep / h : 0.0f;
+                    c[kScTarget + 1] = 0.0f;
+                    c[kScTarget + 2] = 0.0f;
+                    c[kScReg] = fmaxf((ra.z + rb.z) / (h * h) + (ra.w + rb.w) / h, 0.0f);
+                    c[kScMu] = mu_s;
+                    c[kScRelax] = fminf(fmaxf(fmaxf(ra.x, rb.x), 0.0f), 1.0f);  // restitution until evaluated
+                    c[kScDelta + 0] = fmaxf(ra.y, rb.y);                          // restitution threshold
+                    c[kScDelta + 1] = mu_d;
+                    c[kScDelta + 2] = sep;
+                }
+            }
+        }
+        if (total > kSceneContacts) {
+            if (lane == 0) fail(misc, MR_STEP_CONTACT_CAPACITY_OVERFLOW, static_cast<unsigned>(total));
+            __syncwarp();
+            break;
+        }
+        if (lane == 0) misc[kSmContacts] = af(total);
+        __syncwarp();
+
+        // Per-body contact lists (ascending contact index; side bit 1 = B).
+        int* start = reinterpret_cast<int*>(s + kOffLists);
+        int* fill = start + kSceneMaxBodies + 1;
+        std::uint16_t* entries = reinterpret_cast<std::uint16_t*>(s + kOffEntries);
+        for (int b = lane; b < nb; b += 32) {
+            int cnt = 0;
+            for (int c = 0; c < total; ++c) {
+                const float* cr = C + c * kCw;
+                cnt += (ai(cr[kScA]) == b) + (ai(cr[kScB]) == b);
+            }
+            fill[b] = cnt;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            int acc = 0;
+            for (int b = 0; b < nb; ++b) { start[b] = acc; acc += fill[b]; }
+            start[nb] = acc;
+        }
+        __syncwarp();
+        for (int b = lane; b < nb; b += 32) {
+            int at = start[b];
+            for (int c = 0; c < total; ++c) {
+                const float* cr = C + c * kCw;
+                if (ai(cr[kScA]) == b) entries[at++] = static_cast<std::uint16_t>(c << 1);
+                if (ai(cr[kScB]) == b) entries[at++] = static_cast<std::uint16_t>((c << 1) | 1);
+            }
+        }
+        __syncwarp();
+
+        // ConstraintIR evaluation at the predicted velocities, blocks,
+        // preconditioners, relaxation and warm start (lane per contact).
+        auto point_velocity = [&](int body, float3 r) {
+            if (body < 0) return f3(0.0f, 0.0f, 0.0f);
+            return ld3(s + kOffLin + body * 3) + cross3(ld3(s + kOffAng + body * 3), r);
+        };
+        for (int c = lane; c < total; c += 32) {
+            float* cr = C + c * kCw;
+            const int a = ai(cr[kScA]), b = ai(cr[kScB]);
+            const float3 ra = ld3(cr + kScRa), rb = ld3(cr + kScRb);
+            const float3 dv = point_velocity(b, rb) - point_velocity(a, ra);
+            const float3 dirs[3] = {ld3(cr + kScN), ld3(cr + kScT), ld3(cr + kScBt)};
+            const float rel[3] = {dot3(dv, dirs[0]), dot3(dv, dirs[1]), dot3(dv, dirs[2])};
+            const float sep = cr[kScDelta + 2];
+            const float tau_c = 2.0f * h;
+            const float err = fminf(sep + M.slop, 0.0f);
+            const float ratio = h / tau_c;
+            float stab = -h * err / (tau_c * tau_c * (1.0f + 2.0f * ratio + ratio * ratio));
+            stab = fminf(fmaxf(stab, 0.0f), M.max_depenetration);
+            if (ai(cr[kScFlags]) & 1) {
+                const float incoming = rel[0] - cr[kScTarget + 0];
+                if (incoming < -cr[kScDelta + 0]) stab = fmaxf(stab, -cr[kScRelax] * incoming);
+            }
+            cr[kScTarget + 0] += stab;
+            const float slip = sqrtf(rel[1] * rel[1] + rel[2] * rel[2]);
+            if (!(slip <= 1.0e-3f)) cr[kScMu] = cr[kScDelta + 1];
+            // W = sum over dynamic sides of m^-1 d_i.d_j + (r x d_i)^T I^-1 (r x d_j).
+            float W[3][3];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) W[i][j] = 0.0f;
+            for (int side = 0; side < 2; ++side) {
+                const int body = side ? b : a;
+                if (body < 0) continue;
+                const float3 r = side ? rb : ra;
+                const float im = M.mass[body].y;
+                const float* S = s + kOffIiw + body * 6;
+                float3 rd[3], ird[3];
+                for (int i = 0; i < 3; ++i) { rd[i] = cross3(r, dirs[i]); ird[i] = sym3_mul(S, rd[i]); }
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) W[i][j] += im * dot3(dirs[i], dirs[j]) + dot3(rd[i], ird[j]);
+            }
+            // Row sum of normal couplings over contacts sharing a body.
+            float rowsum = 0.0f;
+            const float3 n_i = dirs[0];
+            for (int side = 0; side < 2; ++side) {
+                const int body = side ? b : a;
+                if (body < 0) continue;
+                for (int k = start[body]; k < start[body + 1]; ++k) {
+                    const int cj = entries[k] >> 1, sj = entries[k] & 1;
+                    const float* crj = C + cj * kCw;
+                    const int oa = ai(crj[kScA]), ob = ai(crj[kScB]);
+                    // Skip on the second body when the first one already counted j.
+                    if (side == 1 && (oa == a || ob == a) && a >= 0) continue;
+                    float w = 0.0f;
+                    for (int t = 0; t < 2; ++t) {
+                        const int bi = t ? b : a;
+                        if (bi < 0) continue;
+                        const int tj = (oa == bi) ? 0 : ((ob == bi) ? 1 : -1);
+                        if (tj < 0) continue;
+                        const float si = t ? 1.0f : -1.0f, sjn = tj ? 1.0f : -1.0f;
+                        const float3 ri = t ? rb : ra, rj = ld3(crj + (tj ? kScRb : kScRa));
+                        const float3 n_j = ld3(crj + kScN);
+                        const float3 rni = cross3(ri, n_i), rnj = cross3(rj, n_j);
+                        w += si * sjn * (M.mass[bi].y * dot3(n_i, n_j) + dot3(rni, sym3_mul(s + kOffIiw + bi * 6, rnj)));
+                    }
+                    (void)sj;
+                    rowsum += fabsf(w);
+                }
+            }
+            const float reg[3] = {cr[kScReg], 0.0f, 0.0f};
+            const float diag = fabsf(W[0][0]) + reg[0];
+            for (int i = 0; i < 3; ++i) W[i][i] += reg[i];
+            float inv[3][3];
+            if (!invert3x3_reg(W, inv)) {
+                fail(misc, MR_STEP_FACTORIZATION_FAILED, static_cast<unsigned>(c));
+            } else {
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) cr[kScPre + i * 3 + j] = inv[i][j];
+            }
+            cr[kScRelax] = rowsum > fmaxf(diag, kMatrixFloor) ? fminf(fmaxf(diag / rowsum, 1.0f / 32.0f), 1.0f) : 1.0f;
+            const float3 warm = project_cone(ld3(cr + kScLambda), cr[kScMu], cr[kScMu]);
+            st3(cr + kScLambda, warm);
+            st3(cr + kScDelta, warm);
+            if (!isfinite(cr[kScTarget])) fail(misc, MR_STEP_NONFINITE_RESULT, static_cast<unsigned>(c));
+        }
+        if (!ok(misc)) break;
+        // Islands: min-root union find over dynamic bodies joined by contacts.
+        if (lane == 0 && total > 0) {
+            int parent[kSceneMaxBodies];
+            for (int b = 0; b < nb; ++b) parent[b] = b;
+            auto root = [&](int x) { while (parent[x] != x) x = parent[x] = parent[parent[x]]; return x; };
+            unsigned touched[2] = {0u, 0u};
+            for (int c = 0; c < total; ++c) {
+                const int a = ai(C[c * kCw + kScA]), b = ai(C[c * kCw + kScB]);
+                touched[a >> 5] |= 1u << (a & 31);
+                if (b >= 0) {
+                    touched[b >> 5] |= 1u << (b & 31);
+                    const int x = root(a), y = root(b);
+                    if (x != y) parent[max(x, y)] = min(x, y);
+                }
+            }
+            int islands = 0;
+            for (int b = 0; b < nb; ++b)
+                if (((touched[b >> 5] >> (b & 31)) & 1u) && root(b) == b) ++islands;
+            misc[kSmIslands] = af(max(ai(misc[kSmIslands]), islands));
+        }
+        __syncwarp();
+        // Jacobi sweeps (sweep -1 applies the warm start).
+        const int iters = p.velocity_iterations + (final_substep ? p.final_velocity_iterations : 0);
+        for (int it = -1; it < iters; ++it) {
+            if (it >= 0) {
+                for (int c = lane; c < total; c += 32) {
+                    float* cr = C + c * kCw;
+                    const int a = ai(cr[kScA]), b = ai(cr[kScB]);
+                    const float3 dv = point_velocity(b, ld3(cr + kScRb)) - point_velocity(a, ld3(cr + kScRa));
+                    const float3 prev = ld3(cr + kScLambda);
+                    const float r0 = cr[kScTarget + 0] - dot3(dv, ld3(cr + kScN)) - cr[kScReg] * prev.x;
+                    const float r1 = cr[kScTarget + 1] - dot3(dv, ld3(cr + kScT));
+                    const float r2 = cr[kScTarget + 2] - dot3(dv, ld3(cr + kScBt));
+                    const float* P = cr + kScPre;
+                    float3 prop = f3(prev.x + P[0] * r0 + P[1] * r1 + P[2] * r2, prev.y + P[3] * r0 + P[4] * r1 + P[5] * r2,
+                                     prev.z + P[6] * r0 + P[7] * r1 + P[8] * r2);
+                    prop = project_cone(prop, cr[kScMu], cr[kScMu]);
+                    const float3 delta = cr[kScRelax] * (prop - prev);
+                    const float3 next = prev + delta;
+                    if (!finite3(next) || !finite3(delta)) {
+                        fail(misc, MR_STEP_NONFINITE_RESULT, static_cast<unsigned>(c));
+                        st3(cr + kScDelta, f3(0.0f, 0.0f, 0.0f));
+                    } else {
+                        st3(cr + kScLambda, next);
+                        st3(cr + kScDelta, delta);
+                    }
+                }
+                __syncwarp();
+            }
+            for (int b = lane; b < nb; b += 32) {
+                float3 dl = f3(0.0f, 0.0f, 0.0f), dw = f3(0.0f, 0.0f, 0.0f);
+                for (int k = start[b]; k < start[b + 1]; ++k) {
+                    const int c = entries[k] >> 1, side = entries[k] & 1;
+                    const float* cr = C + c * kCw;
+                    const float3 d = ld3(cr + kScDelta);
+                    const float3 imp = ld3(cr + kScN) * d.x + ld3(cr + kScT) * d.y + ld3(cr + kScBt) * d.z;
+                    const float3 f = side ? imp : -imp;
+                    dl = dl + f;
+                    dw = dw + cross3(ld3(cr + (side ? kScRb : kScRa)), f);
+                }
+                const float im = M.mass[b].y;
+                st3(s + kOffLin + b * 3, ld3(s + kOffLin + b * 3) + im * dl);
+                st3(s + kOffAng + b * 3, ld3(s + kOffAng + b * 3) + sym3_mul(s + kOffIiw + b * 6, dw));
+            }
+            __syncwarp();
+        }
+        if (!ok(misc)) break;
+        // Impulses back into the manifold points.
+        for (int c = lane; c < total; c += 32) {
+            const float* cr = C + c * kCw;
+            const int slot = ai(cr[kScSlot]);
+            float* op = tab + (slot >> 2) * kSceneSlotWords + 8 + (slot & 3) * 12;
+            op[9] = cr[kScLambda + 0];
+            op[10] = cr[kScLambda + 1];
+            op[11] = cr[kScLambda + 2];
+        }
+        // Speed clamps and integration (exponential map of the orientation).
+        for (int b = lane; b < nb; b += 32) {
+            float3 lin = ld3(s + kOffLin + b * 3), ang = ld3(s + kOffAng + b * 3);
+            const float vmax = M.inv_inertia[b].w, wmax = M.offsets[b].w;
+            const float ls = len3(lin), ws = len3(ang);
+            if (vmax > 0.0f && ls > vmax) lin = lin * (vmax / ls);
+            if (wmax > 0.0f && ws > wmax) ang = ang * (wmax / ws);
+            const float3 c = ld3(s + kOffPos + b * 3) + h * lin;
+            float4 q = qmul(so3_increment(h * ang, false), ld4(s + kOffQuat + b * 4));
+            const float qq = qdot(q, q);
+            if (!finite4(q) || !(qq > 1.0e-12f) || !finite3(c) || !finite3(lin) || !finite3(ang)) {
+                fail(misc, MR_STEP_NONFINITE_RESULT, static_cast<unsigned>(b));
+            } else {
+                q = qscale(q, rsqrtf(qq));
+            }
+            st3(s + kOffLin + b * 3, lin);
+            st3(s + kOffAng + b * 3, ang);
+            st3(s + kOffPos + b * 3, c);
+            st4(s + kOffQuat + b * 4, q);
+        }
+        if (!ok(misc)) break;
+    }
+
+    // Commit: a failed control step publishes nothing (HBM keeps the
+    // step-start state), except that a failed reset publishes the reset state.
+    const unsigned code = static_cast<unsigned>(ai(misc[kSmStatus]));
+    const bool success = code == MR_STEP_SUCCESS;
+    float* qd = p.q + static_cast<size_t>(env) * nq;
+    float* vd = p.v + static_cast<size_t>(env) * nv;
+    float* obs = p.observations ? p.observations + static_cast<size_t>(env) * (nq + nv) : nullptr;
+    if (success) {
+        for (int b = lane; b < nb; b += 32) {
+            st3(qd + b * 7, ld3(s + kOffPos + b * 3));
+            st4(qd + b * 7 + 3, ld4(s + kOffQuat + b * 4));
+            st3(vd + b * 6, ld3(s + kOffLin + b * 3));
+            st3(vd + b * 6 + 3, ld3(s + kOffAng + b * 3));
+        }
+        if (cur_table != persistent)
+            for (int i = lane; i < mcount * kSceneSlotWords; i += 32) persistent[i] = cur_table[i];
+        if (lane == 0) {
+            p.manifold_count[env] = static_cast<std::uint32_t>(mcount);
+            // A zero point count ends the table for host readers.
+            if (mcount < kSceneManifolds) persistent[mcount * kSceneSlotWords + 7] = af(0);
+        }
+    } else if (reset) {
+        for (int i = lane; i < nq; i += 32) qd[i] = srcq[i];
+        for (int i = lane; i < nv; i += 32) vd[i] = srcv[i];
+        if (lane == 0) {
+            p.manifold_count[env] = 0u;
+            p.manifolds[static_cast<size_t>(env) * kTableWords + 7] = af(0);
+        }
+    }
+    __syncwarp();
+    if (obs) {
+        for (int i = lane; i < nq; i += 32) obs[i] = qd[i];
+        for (int i = lane; i < nv; i += 32) obs[nq + i] = vd[i];
+    }
+    if (lane == 0) {
+        const unsigned contacts = static_cast<unsigned>(ai(misc[kSmContacts]));
+        if (p.status_codes) p.status_codes[env] = code;
+        if (p.active_contacts) p.active_contacts[env] = success ? contacts : 0u;
+        if (!success) {
+            atomicAdd(p.stats + 0, 1u);
+            atomicMin(p.stats + 6, static_cast<unsigned>(env));
+        }
+        if (reset) atomicAdd(p.stats + 8, 1u);
+        atomicMax(p.stats + 1, contacts);
+        atomicMax(p.stats + 2, static_cast<unsigned>(ai(misc[kSmManifolds])));
+        atomicMax(p.stats + 3, static_cast<unsigned>(ai(misc[kSmRaw])));
+        atomicMax(p.stats + 4, static_cast<unsigned>(ai(misc[kSmCand])));
+        atomicMax(p.stats + 5, static_cast<unsigned>(ai(misc[kSmIslands])));
+    }
+}
+
+}  // namespace
+
+size_t scene_step_smem_bytes() { return static_cast<size_t>(kSceneSmemWords) * sizeof(float); }
+size_t scene_workspace_words() { return static_cast<size_t>(kWsWords); }
+
+cudaError_t configure_scene_step_kernel() {
+    return cudaFuncSetAttribute(scene_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(scene_step_smem_bytes()));
+}
+
+cudaError_t launch_scene_step(const SceneParams& p, cudaStream_t stream) {
+    scene_step_kernel<<<p.env_count, 32, scene_step_smem_bytes(), stream>>>(p);
+    return cudaGetLastError();
+}
+
+}  // namespace numi

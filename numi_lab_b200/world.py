@@ -24,7 +24,10 @@ from .native import MetalRoboError
 SOURCES = {
     "chain7": native.MR_RUN_SOURCE_SYNTHETIC_CHAIN7,
     "tree29": native.MR_RUN_SOURCE_SYNTHETIC_TREE29,
+    "pile": native.MR_RUN_SOURCE_SYNTHETIC_PILE,
 }
+SCENE_MANIFOLDS = 128      # manifold slots per scene environment
+SCENE_SLOT_WORDS = 57      # MRManifoldC words + pair key
 
 
 def _source_id(source: str | int) -> int:
@@ -162,6 +165,8 @@ class World:
         model = native.ModelViewC()
         self._lib.check(self._lib.lib.mr_task_rollout_copy_model(self._handle, ct.byref(model)), "copy_model")
         self.pair_count = int(model.world.pair_count)
+        self.scene_bodies = int(layout.scene_body_count)
+        self.scene = self.scene_bodies > 0
         self.set_precision(precision)
 
     def set_precision(self, precision: str) -> None:
@@ -223,8 +228,21 @@ class World:
         self._lib.check(self._lib.lib.mr_task_rollout_reset(self._handle, self.seed), "mr_task_rollout_reset")
 
     def state(self) -> tuple[np.ndarray, np.ndarray, Any]:
+        """q, v and the persistent manifolds: a ctypes MRManifoldC array
+        [env][pair] for articulated worlds, a float32 array [env][slot][57]
+        (manifold words + pair key, sorted by key) for scene worlds."""
+
         q = np.zeros((self.envs, self.nq), np.float32)
         v = np.zeros((self.envs, self.nv), np.float32)
+        if self.scene:
+            table = np.zeros((self.envs, SCENE_MANIFOLDS, SCENE_SLOT_WORDS), np.float32)
+            self._lib.check(
+                self._lib.lib.mr_task_rollout_copy_state(
+                    self._handle, q.ctypes.data_as(ct.POINTER(ct.c_float)), v.ctypes.data_as(ct.POINTER(ct.c_float)),
+                    ct.c_void_p(table.ctypes.data)),
+                "copy_state",
+            )
+            return q, v, table
         manifolds = (native.ManifoldC * max(self.envs * self.pair_count, 1))()
         self._lib.check(
             self._lib.lib.mr_task_rollout_copy_state(
@@ -247,7 +265,8 @@ class World:
                 self._handle,
                 q.ctypes.data_as(ct.POINTER(ct.c_float)),
                 v.ctypes.data_as(ct.POINTER(ct.c_float)),
-                ct.cast(manifolds, ct.c_void_p) if manifolds is not None else None,
+                (ct.c_void_p(np.ascontiguousarray(manifolds, np.float32).ctypes.data) if isinstance(manifolds, np.ndarray)
+                 else ct.cast(manifolds, ct.c_void_p)) if manifolds is not None else None,
                 1 if as_reset_state else 0,
             ),
             "set_state",

@@ -313,3 +313,145 @@ class Reference:
         secs = self.lib.ref_run(self.handle, envs, _dp(q), _dp(v), acts.ctypes.data_as(ct.POINTER(ct.c_float)), steps, substeps,
                                 threads, solver, ct.byref(failed))
         return secs, int(failed.value)
+
+
+SCENE_MANIFOLDS = 128
+SCENE_SLOT_WORDS = 57
+
+
+class OracleSceneSlot(ct.Structure):
+    _fields_ = [("key", ct.c_uint32), ("reserved", ct.c_uint32), ("m", OracleManifold)]
+
+
+class OracleSceneTrace(ct.Structure):
+    _fields_ = [
+        ("status", ct.c_uint32),
+        ("failing_index", ct.c_uint32),
+        ("contact_count", ct.c_uint32),
+        ("manifold_count", ct.c_uint32),
+        ("raw_count", ct.c_uint32),
+        ("candidate_pairs", ct.c_uint32),
+        ("islands", ct.c_uint32),
+        ("band_decisions", ct.c_uint32),
+        ("min_decision_margin", ct.c_double),
+    ]
+
+
+class SceneTable:
+    """Persistent manifolds of one pile environment, sorted by pair key."""
+
+    def __init__(self) -> None:
+        self.slots = (OracleSceneSlot * SCENE_MANIFOLDS)()
+        self.count = ct.c_uint32(0)
+
+    def keys(self) -> list[int]:
+        return [int(self.slots[i].key) for i in range(self.count.value)]
+
+
+class SceneOracle:
+    """The C restatement of the free-body (pile) control step."""
+
+    def __init__(self, records, h: float, substeps: int, velocity_iterations: int, final_velocity_iterations: int) -> None:
+        if not ORACLE_LIB.is_file():
+            build(reference=False)
+        lib = ct.CDLL(str(ORACLE_LIB))
+        self.lib = lib
+        lib.oracle_scene_create.restype = ct.c_void_p
+        lib.oracle_scene_create.argtypes = [ct.c_void_p] * 5 + [ct.c_double, ct.c_uint32, ct.c_uint32, ct.c_uint32]
+        lib.oracle_scene_destroy.argtypes = [ct.c_void_p]
+        lib.oracle_scene_step.restype = ct.c_uint32
+        lib.oracle_scene_step.argtypes = [ct.c_void_p, _DP, _DP, ct.c_void_p, ct.POINTER(ct.c_uint32), ct.c_double, ct.c_void_p]
+        lib.oracle_scene_collide.restype = ct.c_uint32
+        lib.oracle_scene_collide.argtypes = [ct.c_void_p, _DP, ct.c_void_p, ct.POINTER(ct.c_uint32), _DP, ct.c_uint32,
+                                             ct.POINTER(ct.c_uint32)]
+        lib.oracle_scene_table_from_device.argtypes = [ct.POINTER(ct.c_float), ct.c_uint32, ct.c_void_p]
+        lib.oracle_scene_raw_contacts.restype = ct.c_uint32
+        lib.oracle_scene_raw_contacts.argtypes = [ct.c_void_p, _DP, ct.c_uint32, ct.c_uint32, ct.c_double, ct.c_double, _DP]
+        self.records = records
+        w = records.world
+        self.nb = int(w.body_count) - 1
+        self.h = h
+        self.handle = lib.oracle_scene_create(
+            ct.byref(records.world), ct.cast(records.bodies, ct.c_void_p), ct.cast(records.shapes, ct.c_void_p),
+            ct.cast(records.materials, ct.c_void_p), ct.cast(records.pairs, ct.c_void_p), h, substeps, velocity_iterations,
+            final_velocity_iterations)
+        if not self.handle:
+            raise RuntimeError("oracle_scene_create failed")
+
+    def __del__(self) -> None:
+        try:
+            if self.handle:
+                self.lib.oracle_scene_destroy(self.handle)
+        except Exception:
+            pass
+
+    def table_from_device(self, words: np.ndarray, count: int) -> SceneTable:
+        """Oracle copy of one environment's device manifold table ([slot][57] float32)."""
+
+        t = SceneTable()
+        w = np.ascontiguousarray(words, np.float32)
+        self.lib.oracle_scene_table_from_device(w.ctypes.data_as(ct.POINTER(ct.c_float)), int(count), ct.cast(t.slots, ct.c_void_p))
+        t.count.value = int(count)
+        return t
+
+    def step(self, q: np.ndarray, v: np.ndarray, table: SceneTable, friction: float):
+        """One control step of one env; q, v (float64) and table in place."""
+
+        assert q.dtype == np.float64 and v.dtype == np.float64
+        trace = OracleSceneTrace()
+        status = self.lib.oracle_scene_step(self.handle, _dp(q), _dp(v), ct.cast(table.slots, ct.c_void_p), ct.byref(table.count),
+                                            float(friction), ct.byref(trace))
+        return int(status), trace
+
+    def collide(self, q: np.ndarray, table: SceneTable, raw_cap: int = 1024):
+        """Narrowphase + manifold update over all compiled pairs; returns (status, raw rows [n, 16])."""
+
+        raw = np.zeros((raw_cap, 16))
+        n = ct.c_uint32(0)
+        st = self.lib.oracle_scene_collide(self.handle, _dp(np.ascontiguousarray(q, np.float64)), ct.cast(table.slots, ct.c_void_p),
+                                           ct.byref(table.count), _dp(raw), raw_cap, ct.byref(n))
+        return int(st), raw[: n.value].copy()
+
+    def raw_contacts(self, q: np.ndarray, a: int, b: int, margin_a: float = 0.0, margin_b: float = 0.0) -> np.ndarray:
+        out = np.zeros((8, 12))
+        n = self.lib.oracle_scene_raw_contacts(self.handle, _dp(np.ascontiguousarray(q, np.float64)), a, b, margin_a, margin_b,
+                                               _dp(out))
+        return out[:n].copy()
+
+
+class ReferenceScene:
+    """The reference's FP64 collision oracle (collideCpuReference) over one pile."""
+
+    def __init__(self, records) -> None:
+        if not REF_LIB.is_file():
+            raise FileNotFoundError(f"{REF_LIB} is missing; build it with `make -C oracle ref` where the reference sources exist")
+        lib = ct.CDLL(str(REF_LIB))
+        self.lib = lib
+        lib.ref_scene_create.restype = ct.c_void_p
+        lib.ref_scene_create.argtypes = [ct.c_void_p] * 3 + [ct.c_char_p, ct.c_size_t]
+        lib.ref_scene_destroy.argtypes = [ct.c_void_p]
+        lib.ref_scene_collide.restype = ct.c_int
+        lib.ref_scene_collide.argtypes = [ct.c_void_p, _DP, ct.c_uint32, _DP, ct.POINTER(ct.c_uint32), ct.c_uint32, _DP,
+                                          ct.POINTER(ct.c_uint32)]
+        err = ct.create_string_buffer(512)
+        self.handle = lib.ref_scene_create(ct.byref(records.world), ct.cast(records.bodies, ct.c_void_p),
+                                           ct.cast(records.shapes, ct.c_void_p), err, len(err))
+        if not self.handle:
+            raise RuntimeError(err.value.decode())
+
+    def __del__(self) -> None:
+        try:
+            if self.handle:
+                self.lib.ref_scene_destroy(self.handle)
+        except Exception:
+            pass
+
+    def collide(self, q: np.ndarray, raw_cap: int = 1024, manifold_cap: int = 512):
+        """Returns (status, raw rows [n, 16], manifold rows [m, 58]); manifolds persist across calls."""
+
+        raw = np.zeros((raw_cap, 16))
+        man = np.zeros((manifold_cap, 58))
+        nr, nm = ct.c_uint32(0), ct.c_uint32(0)
+        st = self.lib.ref_scene_collide(self.handle, _dp(np.ascontiguousarray(q, np.float64)), raw_cap, _dp(raw), ct.byref(nr),
+                                        manifold_cap, _dp(man), ct.byref(nm))
+        return int(st), raw[: nr.value].copy(), man[: nm.value].copy()

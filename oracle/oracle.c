@@ -1376,3 +1376,973 @@ void oracle_temporal_cone_dense(uint32_t n, const double* W, const double* u0, c
         for (uint32_t r = 0; r < m; ++r) lambda[r] += delta[r];
     }
 }
+
+/* ================================================================== */
+/* Free-body scene worlds: piles of spheres and boxes on a plane.       */
+/* FP64 restatement of the device scene step (same stage order):       */
+/* prediction (MetalWorldContact.metal:2509-2570), speculative sweep    */
+/* (Collision.metal:5960-6030), pair flags (Collision.metal:7905-8180), */
+/* analytic narrowphase (Collision.cpp:1106-2175: sphere-sphere,        */
+/* sphere-box witness, box-box separating axes with vertex clipping,    */
+/* sphere/box vs plane), persistent manifolds keyed by collider pair,   */
+/* ConstraintIR, islands (ConstraintSolver.cpp:848-900), temporalCone   */
+/* with free-body responses, speed clamps and exponential-map           */
+/* integration.                                                         */
+/* ================================================================== */
+
+#define SNB ORACLE_SCENE_MAX_BODIES
+#define SMAN ORACLE_SCENE_MANIFOLDS
+#define SCON ORACLE_SCENE_CONTACTS
+#define SCAND ORACLE_SCENE_CANDIDATES
+#define SPAIRS (SNB * (SNB - 1) / 2 + SNB)
+
+struct OracleScene {
+    uint32_t nb, np;
+    double h;
+    uint32_t substeps, iters, final_iters;
+    double gravity[3], slop, max_dep, spec_scale, speed_env, thr[4];
+    v3 plane_pos, ground_pos;
+    q4 plane_rot, ground_rot;
+    double plane_offset, plane_rest;
+    uint32_t plane_material;
+    uint32_t type[SNB], material[SNB];
+    double dims[SNB][3], mass[SNB], inv_mass[SNB], damp_lin[SNB], damp_ang[SNB];
+    double inv_inertia[SNB][3], max_lin[SNB], max_ang[SNB];
+    double offset[SNB], rest[SNB], sweep[SNB];
+    double fric[4][2], resp[4][4];
+    uint8_t pa[SPAIRS], pb[SPAIRS], pc[SPAIRS];
+};
+
+OracleScene* oracle_scene_create(const MRModelWorldC* w, const MRModelBodyC* bodies, const MRModelShapeC* shapes,
+                                 const MRModelMaterialC* materials, const MRModelPairC* pairs, double h,
+                                 uint32_t substeps, uint32_t iters, uint32_t final_iters) {
+    OracleScene* s = (OracleScene*)calloc(1, sizeof(OracleScene));
+    const uint32_t n = w->body_count - 1;
+    s->nb = n;
+    s->np = w->pair_count;
+    s->h = h;
+    s->substeps = substeps;
+    s->iters = iters;
+    s->final_iters = final_iters;
+    for (int i = 0; i < 3; ++i) s->gravity[i] = w->gravity[i];
+    s->slop = w->solver_scales[3];
+    s->max_dep = w->solver_scales[2];
+    s->spec_scale = w->speculative[0];
+    s->speed_env = w->speculative[1];
+    for (int i = 0; i < 4; ++i) s->thr[i] = w->manifold_thresholds[i];
+    const MRModelShapeC* plane = &shapes[n];
+    const MRModelBodyC* ground = &bodies[n];
+    s->plane_pos = V(ground->static_pose[0] + plane->local_position[0], ground->static_pose[1] + plane->local_position[1],
+                     ground->static_pose[2] + plane->local_position[2]);
+    /* The device stores the normalised rotation in FP32. */
+    {
+        const double qx = plane->local_rotation[0], qy = plane->local_rotation[1], qz = plane->local_rotation[2],
+                     qw = plane->local_rotation[3];
+        const double nr = sqrt(qx * qx + qy * qy + qz * qz + qw * qw);
+        s->plane_rot = Q((float)(qx / nr), (float)(qy / nr), (float)(qz / nr), (float)(qw / nr));
+    }
+    s->ground_pos = V(ground->static_pose[0], ground->static_pose[1], ground->static_pose[2]);
+    {
+        const double qx = ground->static_pose[4], qy = ground->static_pose[5], qz = ground->static_pose[6],
+                     qw = ground->static_pose[7];
+        const double nr = sqrt(qx * qx + qy * qy + qz * qz + qw * qw);
+        s->ground_rot = Q((float)(qx / nr), (float)(qy / nr), (float)(qz / nr), (float)(qw / nr));
+    }
+    s->plane_offset = plane->contact_rest_bound[0];
+    s->plane_rest = plane->contact_rest_bound[1];
+    s->plane_material = plane->material;
+    for (uint32_t b = 0; b < n; ++b) {
+        s->type[b] = shapes[b].shape_type;
+        s->material[b] = shapes[b].material;
+        for (int i = 0; i < 3; ++i) s->dims[b][i] = shapes[b].dimensions[i];
+        s->mass[b] = bodies[b].mass_inverse_mass[0];
+        s->inv_mass[b] = bodies[b].mass_inverse_mass[1];
+        s->damp_lin[b] = w->apply_body_damping ? bodies[b].damping_speed[0] : 0.0;
+        s->damp_ang[b] = w->apply_body_damping ? bodies[b].damping_speed[1] : 0.0;
+        for (int i = 0; i < 3; ++i) s->inv_inertia[b][i] = (float)(1.0f / bodies[b].inertia[i][i]);
+        s->max_lin[b] = bodies[b].damping_speed[2];
+        s->max_ang[b] = bodies[b].damping_speed[3];
+        s->offset[b] = shapes[b].contact_rest_bound[0];
+        s->rest[b] = shapes[b].contact_rest_bound[1];
+        s->sweep[b] = shapes[b].contact_rest_bound[2];
+    }
+    for (uint32_t i = 0; i < w->material_count && i < 4; ++i) {
+        s->fric[i][0] = materials[i].friction[0];
+        s->fric[i][1] = materials[i].friction[1];
+        for (int k = 0; k < 4; ++k) s->resp[i][k] = materials[i].response[k];
+    }
+    for (uint32_t p = 0; p < s->np; ++p) {
+        s->pa[p] = (uint8_t)pairs[p].shape_a;
+        s->pb[p] = (uint8_t)pairs[p].shape_b;
+        s->pc[p] = (uint8_t)pairs[p].pair_class;
+    }
+    return s;
+}
+
+void oracle_scene_destroy(OracleScene* s) { free(s); }
+
+typedef struct {
+    int type;
+    v3 c;
+    q4 r;
+    v3 half;
+    double radius, offset;
+    v3 lo, hi, normal;
+    v3 bpos; /* pose of the collider's body: the frame of its manifold anchors */
+    q4 brot;
+} SCol;
+
+typedef struct {
+    double lo[SNB][3], hi[SNB][3], margin[SNB];
+    v3 pos[SNB], lin[SNB], ang[SNB];
+    q4 rot[SNB];
+    double iiw[SNB][6];
+} SState;
+
+static void scol(const OracleScene* s, const SState* st, uint32_t b, SCol* o) {
+    if (b >= s->nb) {
+        o->type = MR_SHAPE_PLANE;
+        o->c = s->plane_pos;
+        o->r = s->plane_rot;
+        const v3 n = qrot(o->r, V(0, 1, 0));
+        o->normal = vmul(n, 1.0 / vlen(n));
+        o->half = V(0, 0, 0);
+        o->radius = 0.0;
+        o->offset = s->plane_offset;
+        o->lo = o->hi = V(0, 0, 0);
+        o->bpos = s->ground_pos;
+        o->brot = s->ground_rot;
+        return;
+    }
+    o->type = (int)s->type[b];
+    o->c = st->pos[b];
+    o->r = st->rot[b];
+    o->half = V(s->dims[b][0], s->dims[b][1], s->dims[b][2]);
+    o->radius = s->dims[b][0];
+    o->offset = s->offset[b] + st->margin[b];
+    o->lo = V(st->lo[b][0], st->lo[b][1], st->lo[b][2]);
+    o->hi = V(st->hi[b][0], st->hi[b][1], st->hi[b][2]);
+    o->normal = V(0, 0, 0);
+    o->bpos = o->c;
+    o->brot = o->r;
+}
+
+static double scol_scale(const SCol* k) {
+    return fmax(fmax(vmaxabs(k->c), vmaxabs(k->half)),
+                fmax(fabs(k->radius), fmax(fabs(k->offset), fmax(vmaxabs(k->lo), vmaxabs(k->hi)))));
+}
+static v3 sbox_axis(const SCol* b, int a) { return qrot(b->r, V(a == 0, a == 1, a == 2)); }
+static double sbox_radius(const SCol* b, v3 ax) {
+    return fabs(vdot(ax, sbox_axis(b, 0))) * b->half.x + fabs(vdot(ax, sbox_axis(b, 1))) * b->half.y +
+           fabs(vdot(ax, sbox_axis(b, 2))) * b->half.z;
+}
+static v3 sbox_vertex(const SCol* b, int v) {
+    return vadd(b->c, qrot(b->r, V((v & 1) ? b->half.x : -b->half.x, (v & 2) ? b->half.y : -b->half.y,
+                                   (v & 4) ? b->half.z : -b->half.z)));
+}
+static int sinside(v3 p, const SCol* b, double infl) {
+    const v3 l = qrotinv(b->r, vsub(p, b->c));
+    BAND(fabs(l.x), b->half.x + infl);
+    BAND(fabs(l.y), b->half.y + infl);
+    BAND(fabs(l.z), b->half.z + infl);
+    return fabs(l.x) <= b->half.x + infl && fabs(l.y) <= b->half.y + infl && fabs(l.z) <= b->half.z + infl;
+}
+static v3 sbox_support(const SCol* b, v3 d) {
+    v3 out = b->c;
+    for (int a = 0; a < 3; ++a) {
+        const v3 ax = sbox_axis(b, a);
+        const double he = a == 0 ? b->half.x : (a == 1 ? b->half.y : b->half.z);
+        BAND(vdot(d, ax), 0.0); /* an edge across the normal: either end supports */
+        out = vadd(out, vmul(ax, vdot(d, ax) >= 0.0 ? he : -he));
+    }
+    return out;
+}
+static v3 scoincident(uint32_t a, uint32_t b) {
+    const uint32_t hsh = a * 73856093u ^ b * 19349663u;
+    const uint32_t axis = hsh % 3u;
+    const double sign = (hsh & 4u) == 0u ? 1.0 : -1.0;
+    return V(axis == 0 ? sign : 0.0, axis == 1 ? sign : 0.0, axis == 2 ? sign : 0.0);
+}
+
+typedef struct {
+    int n;
+    double sep[8];
+    v3 pa[8], pb[8];
+    uint32_t fa[8], fb[8];
+} SRaw;
+
+static void sraw_add(SRaw* r, v3 pa, v3 pb, double sep, uint32_t fa, uint32_t fb) {
+    if (r->n >= 8) return;
+    r->pa[r->n] = pa;
+    r->pb[r->n] = pb;
+    r->sep[r->n] = sep;
+    r->fa[r->n] = fa;
+    r->fb[r->n] = fb;
+    r->n++;
+}
+
+static v3 snarrow(const SCol* A, const SCol* B, int cls, uint32_t ia, uint32_t ib, double acc, SRaw* raw) {
+    raw->n = 0;
+    if (cls == MR_COLLISION_PAIR_SPHERE_SPHERE) {
+        const v3 d = vsub(B->c, A->c);
+        const double len = vlen(d);
+        const v3 n = len > 1e-12 ? vmul(d, 1.0 / len) : scoincident(ia, ib);
+        const double sep = len - A->radius - B->radius;
+        BAND(sep, acc);
+        if (sep <= acc) sraw_add(raw, vadd(A->c, vmul(n, A->radius)), vsub(B->c, vmul(n, B->radius)), sep,
+                                 feature_key(MR_SHAPE_SPHERE, 0), feature_key(MR_SHAPE_SPHERE, 0));
+        return n;
+    }
+    if (cls == MR_COLLISION_PAIR_SPHERE_BOX) {
+        const int sphere_a = A->type == MR_SHAPE_SPHERE;
+        const SCol* sp = sphere_a ? A : B;
+        const SCol* bx = sphere_a ? B : A;
+        const v3 lc = qrotinv(bx->r, vsub(sp->c, bx->c));
+        v3 cl = V(fmin(fmax(lc.x, -bx->half.x), bx->half.x), fmin(fmax(lc.y, -bx->half.y), bx->half.y),
+                  fmin(fmax(lc.z, -bx->half.z), bx->half.z));
+        BAND(fabs(lc.x), bx->half.x);
+        BAND(fabs(lc.y), bx->half.y);
+        BAND(fabs(lc.z), bx->half.z);
+        const v3 ld = vsub(cl, lc);
+        const double dist = vlen(ld);
+        v3 n;
+        double sep;
+        uint32_t feat;
+        if (dist > 1e-12) {
+            n = qrot(bx->r, vmul(ld, 1.0 / dist));
+            sep = dist - sp->radius;
+#define SREG(c, he) ((c) < -(he) ? 0u : ((c) > (he) ? 2u : 1u))
+            feat = SREG(lc.x, bx->half.x) + 3u * SREG(lc.y, bx->half.y) + 9u * SREG(lc.z, bx->half.z);
+#undef SREG
+        } else {
+            const double dx = bx->half.x - fabs(lc.x), dy = bx->half.y - fabs(lc.y), dz = bx->half.z - fabs(lc.z);
+            int axis = 0;
+            double dm = dx;
+            if (dy < dm) { axis = 1; dm = dy; }
+            if (dz < dm) { axis = 2; dm = dz; }
+            const double coord = axis == 0 ? lc.x : (axis == 1 ? lc.y : lc.z);
+            const double sign = coord >= 0.0 ? 1.0 : -1.0;
+            const v3 outward = V(axis == 0 ? sign : 0.0, axis == 1 ? sign : 0.0, axis == 2 ? sign : 0.0);
+            if (axis == 0) cl.x = sign * bx->half.x;
+            else if (axis == 1) cl.y = sign * bx->half.y;
+            else cl.z = sign * bx->half.z;
+            n = qrot(bx->r, vmul(outward, -1.0));
+            sep = -dm - sp->radius;
+            feat = 27u + 2u * (uint32_t)axis + (sign > 0.0 ? 1u : 0u);
+        }
+        const v3 box_point = vadd(bx->c, qrot(bx->r, cl));
+        BAND(sep, acc);
+        if (sep <= acc) {
+            const v3 sphere_point = vadd(sp->c, vmul(n, sp->radius));
+            if (sphere_a) sraw_add(raw, sphere_point, box_point, sep, feature_key(MR_SHAPE_SPHERE, 0), feature_key(MR_SHAPE_BOX, feat));
+            else sraw_add(raw, box_point, sphere_point, sep, feature_key(MR_SHAPE_BOX, feat), feature_key(MR_SHAPE_SPHERE, 0));
+        }
+        return sphere_a ? n : vmul(n, -1.0);
+    }
+    if (cls == MR_COLLISION_PAIR_BOX_BOX) {
+        const v3 cd = vsub(B->c, A->c);
+        double best_sep = -INFINITY;
+        v3 best_n = scoincident(ia, ib);
+        int best_axis = 0;
+        double best_err = 0.0;
+        const double reach = vlen(A->half) + vlen(B->half);
+        int index = -1; /* position in the list of accepted axes (Collision.cpp:1818-1842) */
+        for (int k = 0; k < 15; ++k) {
+            v3 axis;
+            double axis_len = 1.0;
+            if (k < 3) axis = sbox_axis(A, k);
+            else if (k < 6) axis = sbox_axis(B, k - 3);
+            else {
+                const v3 cr = vcross(sbox_axis(A, (k - 6) / 3), sbox_axis(B, (k - 6) % 3));
+                const double sq = vdot(cr, cr);
+                if (sq <= 1e-12) g_band++; /* the FP32 cross product may fall under the floor */
+                if (!(sq > 1e-24)) continue;
+                axis_len = sqrt(sq);
+                axis = vmul(cr, 1.0 / axis_len);
+            }
+            ++index;
+            const double proj = vdot(cd, axis);
+            if (proj < 0.0 || (proj == 0.0 && vdot(axis, best_n) < 0.0)) axis = vmul(axis, -1.0);
+            const double sep = fabs(proj) - sbox_radius(A, axis) - sbox_radius(B, axis);
+            /* FP32 sensitivity of this axis' separation: an edge-edge axis
+             * carries the rounding of its cross product amplified by 1/|cross|. */
+            const double err = 8.0 * kFloatEps * (vlen(cd) + reach) / axis_len;
+            if (fabs(sep - acc) <= err) g_band++;
+            BAND(sep, acc);
+            if (sep > acc) return axis;
+            const double tol = 1.0e-12 * (1.0 + fmax(fabs(best_sep), fabs(sep)));
+            if (isfinite(best_sep) && fabs(sep - best_sep) <= err + best_err) g_band++;
+            if (!isfinite(best_sep) || sep > best_sep + tol || (fabs(sep - best_sep) <= tol && index < best_axis)) {
+                best_sep = sep;
+                best_n = axis;
+                best_axis = index;
+                best_err = err;
+            }
+        }
+        const double near_b = vdot(B->c, best_n) - sbox_radius(B, best_n);
+        const double far_a = vdot(A->c, best_n) + sbox_radius(A, best_n);
+        for (int v = 0; v < 8; ++v) {
+            const v3 pa = sbox_vertex(A, v);
+            if (!sinside(pa, B, acc)) continue;
+            const double sep = near_b - vdot(pa, best_n);
+            BAND(sep, acc);
+            if (sep <= acc)
+                sraw_add(raw, pa, vadd(pa, vmul(best_n, sep)), sep, feature_key(MR_SHAPE_BOX, (uint32_t)v),
+                         feature_key(MR_SHAPE_BOX, 128u + (uint32_t)best_axis));
+        }
+        for (int v = 0; v < 8; ++v) {
+            const v3 pb = sbox_vertex(B, v);
+            if (!sinside(pb, A, acc)) continue;
+            const double sep = vdot(pb, best_n) - far_a;
+            BAND(sep, acc);
+            if (sep <= acc)
+                sraw_add(raw, vsub(pb, vmul(best_n, sep)), pb, sep, feature_key(MR_SHAPE_BOX, 128u + (uint32_t)best_axis),
+                         feature_key(MR_SHAPE_BOX, (uint32_t)v));
+        }
+        if (raw->n == 0) {
+            const v3 pa = sbox_support(A, best_n), pb = sbox_support(B, vmul(best_n, -1.0));
+            sraw_add(raw, pa, pb, vdot(vsub(pb, pa), best_n), feature_key(MR_SHAPE_BOX, 256u + (uint32_t)best_axis),
+                     feature_key(MR_SHAPE_BOX, 256u + (uint32_t)best_axis));
+        }
+        return best_n;
+    }
+    {
+        const v3 pn = B->normal;
+        const uint32_t plane_key = feature_key(MR_SHAPE_PLANE, 0);
+        if (cls == MR_COLLISION_PAIR_SPHERE_PLANE) {
+            const v3 surface = vsub(A->c, vmul(pn, A->radius));
+            const double sep = vdot(pn, vsub(surface, B->c));
+            BAND(sep, acc);
+            if (sep <= acc) sraw_add(raw, surface, vsub(surface, vmul(pn, sep)), sep, feature_key(MR_SHAPE_SPHERE, 0), plane_key);
+        } else if (cls == MR_COLLISION_PAIR_BOX_PLANE) {
+            for (int v = 0; v < 8; ++v) {
+                const v3 w = sbox_vertex(A, v);
+                const double sep = vdot(pn, vsub(w, B->c));
+                BAND(sep, acc);
+                if (sep <= acc) sraw_add(raw, w, vsub(w, vmul(pn, sep)), sep, feature_key(MR_SHAPE_BOX, (uint32_t)v), plane_key);
+            }
+        }
+        return vmul(pn, -1.0);
+    }
+}
+
+typedef struct {
+    double la[3], lb[3];
+    uint32_t fa, fb, life;
+    double imp[3];
+    v3 wp;
+    double sep;
+} SCand;
+
+static unsigned long long sckey(const SCand* c) { return ((unsigned long long)c->fa << 32) | c->fb; }
+
+/* Persistent manifold of one pair (same decisions as the device builder). */
+static int sbuild(const OracleScene* s, const OracleManifold* old, const SRaw* raw, v3 raw_normal, OracleManifold* out, v3 posA,
+                  q4 rotA, v3 posB, q4 rotB) {
+    memset(out, 0, sizeof(*out));
+    if (raw->n == 0) return 0;
+    for (int i = 0; i < raw->n; ++i)
+        if (!isfinite(raw->sep[i]) || !vfinite(raw->pa[i]) || !vfinite(raw->pb[i])) return -1;
+    const v3 nw = vmul(raw_normal, 1.0 / vlen(raw_normal));
+    if (!vfinite(nw)) return -1;
+    SCand c[12];
+    int nc = 0, old_ok = 0;
+    v3 transported = V(0, 0, 0);
+    double old_age = 0.0;
+    const int old_count = old ? (int)old->count : 0;
+    if (old_count > 0 && old_count <= 4) {
+        v3 on = qrot(rotA, vld(old->normal_local));
+        on = vmul(on, 1.0 / vlen(on));
+        BAND(vdot(on, nw), s->thr[3]);
+        old_ok = vfinite(on) && vdot(on, nw) >= s->thr[3];
+        if (old_ok) {
+            const v3 ot = qrot(rotA, vld(old->tangent_local));
+            transported = vsub(ot, vmul(nw, vdot(ot, nw)));
+            old_age = old->age;
+            for (int i = 0; i < old_count; ++i) {
+                const OraclePoint* op = &old->points[i];
+                const v3 pa = vadd(posA, qrot(rotA, vld(op->anchor_a)));
+                const v3 pb = vadd(posB, qrot(rotB, vld(op->anchor_b)));
+                const v3 d = vsub(pb, pa);
+                const double sep = vdot(d, nw);
+                const double drift = vlen(vsub(d, vmul(nw, sep)));
+                BAND(sep, s->thr[0]);
+                BAND(drift, s->thr[1]);
+                if (sep > s->thr[0] || drift > s->thr[1]) continue;
+                SCand* k = &c[nc++];
+                for (int a = 0; a < 3; ++a) { k->la[a] = op->anchor_a[a]; k->lb[a] = op->anchor_b[a]; k->imp[a] = op->impulses[a]; }
+                k->fa = op->feature_a;
+                k->fb = op->feature_b;
+                k->life = op->life == 0xffffffffu ? 0xffffffffu : op->life + 1u;
+                k->wp = vmul(vadd(pa, pb), 0.5);
+                k->sep = sep;
+            }
+        }
+    }
+    const double merge2 = s->thr[2] * s->thr[2];
+    for (int r = 0; r < raw->n; ++r) {
+        const v3 la = qrotinv(rotA, vsub(raw->pa[r], posA));
+        const v3 lb = qrotinv(rotB, vsub(raw->pb[r], posB));
+        int match = -1;
+        for (int k = 0; k < nc && match < 0; ++k)
+            if (c[k].fa == raw->fa[r] && c[k].fb == raw->fb[r]) match = k;
+        for (int k = 0; k < nc && match < 0; ++k) {
+            const v3 da = vsub(vld(c[k].la), la), db = vsub(vld(c[k].lb), lb);
+            BAND(sqrt(vdot(da, da) + vdot(db, db)), sqrt(2.0 * merge2));
+            if (vdot(da, da) + vdot(db, db) <= 2.0 * merge2) match = k;
+        }
+        if (match < 0) {
+            if (nc >= 12) return -1;
+            match = nc++;
+            c[match].life = 0u;
+            c[match].imp[0] = c[match].imp[1] = c[match].imp[2] = 0.0;
+        }
+        vst(c[match].la, la);
+        vst(c[match].lb, lb);
+        c[match].fa = raw->fa[r];
+        c[match].fb = raw->fb[r];
+        c[match].wp = vmul(vadd(raw->pa[r], raw->pb[r]), 0.5);
+        c[match].sep = raw->sep[r];
+    }
+    if (nc > 4) {
+        for (int i = 1; i < nc; ++i) {
+            SCand val = c[i];
+            int d = i;
+            while (d > 0 && (val.sep < c[d - 1].sep || (val.sep == c[d - 1].sep && sckey(&val) < sckey(&c[d - 1])))) {
+                c[d] = c[d - 1];
+                --d;
+            }
+            c[d] = val;
+        }
+        if (fabs(c[1].sep - c[0].sep) <= kBand) g_band++;
+        int selected[12] = {0}, chosen[4], count = 1;
+        chosen[0] = 0;
+        selected[0] = 1;
+        for (int stage = 1; stage < 4; ++stage) {
+            int best = -1;
+            double best_score = -1.0;
+            unsigned long long best_f = ~0ull;
+            for (int i = 0; i < nc; ++i) {
+                if (selected[i]) continue;
+                double score;
+                if (stage == 1) {
+                    const v3 d = vsub(c[i].wp, c[chosen[0]].wp);
+                    const v3 t = vsub(d, vmul(nw, vdot(d, nw)));
+                    score = vdot(t, t);
+                } else if (stage == 2) {
+                    score = fabs(vdot(vcross(vsub(c[chosen[1]].wp, c[chosen[0]].wp), vsub(c[i].wp, c[chosen[0]].wp)), nw));
+                } else {
+                    score = INFINITY;
+                    for (int k = 0; k < count; ++k) {
+                        const v3 d = vsub(c[i].wp, c[chosen[k]].wp);
+                        const v3 t = vsub(d, vmul(nw, vdot(d, nw)));
+                        score = fmin(score, vdot(t, t));
+                    }
+                }
+                const unsigned long long f = sckey(&c[i]);
+                const double tol = fmax(1.0e-12, kTieRelative * fmax(fabs(score), fabs(best_score)));
+                if (best >= 0 && fabs(fabs(score - best_score) - tol) <= 0.1 * tol) g_band++;
+                if (score > best_score + tol || (fabs(score - best_score) <= tol && f < best_f)) {
+                    best = i;
+                    best_score = score;
+                    best_f = f;
+                }
+            }
+            if (best >= 0) { chosen[count++] = best; selected[best] = 1; }
+        }
+        SCand red[4];
+        for (int i = 0; i < count; ++i) red[i] = c[chosen[i]];
+        nc = count;
+        for (int i = 0; i < nc; ++i) c[i] = red[i];
+    }
+    for (int i = 1; i < nc; ++i) {
+        SCand val = c[i];
+        int d = i;
+        while (d > 0 && sckey(&val) < sckey(&c[d - 1])) { c[d] = c[d - 1]; --d; }
+        c[d] = val;
+    }
+    v3 tw = transported;
+    if (!old_ok || !vfinite(tw) || vdot(tw, tw) <= 1.0e-12) tw = stable_tangent(nw);
+    else tw = vmul(tw, 1.0 / vlen(tw));
+    vst(out->normal_local, qrotinv(rotA, nw));
+    out->age = old_ok ? fmin(old_age + 1.0, 65535.0) : 0.0;
+    vst(out->tangent_local, qrotinv(rotA, tw));
+    out->count = (uint32_t)nc;
+    for (int i = 0; i < nc; ++i) {
+        OraclePoint* op = &out->points[i];
+        for (int a = 0; a < 3; ++a) { op->anchor_a[a] = c[i].la[a]; op->anchor_b[a] = c[i].lb[a]; op->impulses[a] = c[i].imp[a]; }
+        op->feature_a = c[i].fa;
+        op->feature_b = c[i].fb;
+        op->life = c[i].life;
+    }
+    return nc;
+}
+
+static void sym3_world(q4 q, const double* inv, double* out) {
+    const v3 c0 = qrot(q, V(1, 0, 0)), c1 = qrot(q, V(0, 1, 0)), c2 = qrot(q, V(0, 0, 1));
+    const double R[3][3] = {{c0.x, c1.x, c2.x}, {c0.y, c1.y, c2.y}, {c0.z, c1.z, c2.z}};
+    int k = 0;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j <= i; ++j) {
+            double acc = 0.0;
+            for (int m = 0; m < 3; ++m) acc += R[i][m] * inv[m] * R[j][m];
+            out[k++] = acc;
+        }
+}
+static v3 sym3_apply(const double* S, v3 x) {
+    return V(S[0] * x.x + S[1] * x.y + S[3] * x.z, S[1] * x.x + S[2] * x.y + S[4] * x.z, S[3] * x.x + S[4] * x.y + S[5] * x.z);
+}
+
+typedef struct {
+    int a, b;  /* b < 0: plane */
+    v3 ra, rb, n, t, bt;
+    double target[3], reg, mu, lambda[3], P[9], relax, delta[3];
+    int slot, point, new_impact;
+    double sep, rthr, restitution, mu_d;
+} SCon;
+
+static void sprepare(const OracleScene* s, SState* st) {
+    const double h = s->h;
+    for (uint32_t b = 0; b < s->nb; ++b) {
+        st->lin[b] = vadd(vmul(st->lin[b], exp(-h * s->damp_lin[b])), vmul(V(s->gravity[0], s->gravity[1], s->gravity[2]), h));
+        st->ang[b] = vmul(st->ang[b], exp(-h * s->damp_ang[b]));
+    }
+}
+
+static uint32_t sbounds(const OracleScene* s, SState* st, uint32_t* fail_index) {
+    const double h = s->h;
+    for (uint32_t b = 0; b < s->nb; ++b) {
+        q4 qn;
+        if (!qnormalize(st->rot[b], &qn, 1)) { *fail_index = b; return MR_STEP_NONFINITE_INPUT; }
+        st->rot[b] = qn;
+        sym3_world(qn, s->inv_inertia[b], st->iiw[b]);
+        const v3 c = st->pos[b];
+        const v3 fc = vadd(c, vmul(st->lin[b], h));
+        q4 fr = qmul(so3_increment(vmul(st->ang[b], h), 0), qn);
+        fr = Q(fr.x / sqrt(qdot(fr, fr)), fr.y / sqrt(qdot(fr, fr)), fr.z / sqrt(qdot(fr, fr)), fr.w / sqrt(qdot(fr, fr)));
+        const double cosv = fmin(fmax(fabs(qdot(qn, fr)), 0.0), 1.0);
+        const double chord = 2.0 * s->sweep[b] * sqrt(fmax(0.0, 1.0 - cosv * cosv));
+        const double env = fmin(vlen(vsub(fc, c)) + chord, h * s->speed_env);
+        const double margin = s->spec_scale * env;
+        st->margin[b] = margin;
+        v3 e0, e1;
+        if (s->type[b] == MR_SHAPE_SPHERE) {
+            e0 = e1 = V(s->dims[b][0], s->dims[b][0], s->dims[b][0]);
+        } else {
+            const q4 rs[2] = {qn, fr};
+            v3 ex[2];
+            for (int k = 0; k < 2; ++k) {
+                const v3 bx = qrot(rs[k], V(1, 0, 0)), by = qrot(rs[k], V(0, 1, 0)), bz = qrot(rs[k], V(0, 0, 1));
+                ex[k] = vadd(vadd(vmul(V(fabs(bx.x), fabs(bx.y), fabs(bx.z)), s->dims[b][0]),
+                                  vmul(V(fabs(by.x), fabs(by.y), fabs(by.z)), s->dims[b][1])),
+                             vmul(V(fabs(bz.x), fabs(bz.y), fabs(bz.z)), s->dims[b][2]));
+            }
+            e0 = ex[0];
+            e1 = ex[1];
+        }
+        const double o = s->offset[b];
+        double lo[3] = {fmin(c.x - e0.x, fc.x - e1.x) - o, fmin(c.y - e0.y, fc.y - e1.y) - o, fmin(c.z - e0.z, fc.z - e1.z) - o};
+        double hi[3] = {fmax(c.x + e0.x, fc.x + e1.x) + o, fmax(c.y + e0.y, fc.y + e1.y) + o, fmax(c.z + e0.z, fc.z + e1.z) + o};
+        for (int i = 0; i < 3; ++i) {
+            const double sc = fmax(fabs(lo[i]), fabs(hi[i])) + 1.0;
+            st->lo[b][i] = lo[i] - sc * kPad - margin;
+            st->hi[b][i] = hi[i] + sc * kPad + margin;
+        }
+    }
+    return MR_STEP_SUCCESS;
+}
+
+static int sflag(const OracleScene* s, const SState* st, uint32_t a, uint32_t b) {
+    if (b >= s->nb) {
+        const v3 pn = qrot(s->plane_rot, V(0, 1, 0));
+        const v3 n = vmul(pn, 1.0 / vlen(pn));
+        const v3 la = V(st->lo[a][0], st->lo[a][1], st->lo[a][2]), ha = V(st->hi[a][0], st->hi[a][1], st->hi[a][2]);
+        const v3 center = vmul(vadd(la, ha), 0.5), halfx = vmul(vsub(ha, la), 0.5);
+        const double off = s->offset[a] + st->margin[a];
+        const double scale = fmax(fmax(vmaxabs(s->plane_pos), vmaxabs(la)), fmax(vmaxabs(ha), fmax(fabs(s->plane_offset), fabs(off))));
+        const v3 an = V(fabs(n.x), fabs(n.y), fabs(n.z));
+        const double msd = vdot(n, vsub(center, s->plane_pos)) - vdot(an, halfx);
+        BAND(msd, s->plane_offset + (scale + 1.0) * kPad);
+        return msd <= s->plane_offset + (scale + 1.0) * kPad;
+    }
+    int ok = 1;
+    for (int i = 0; i < 3; ++i) {
+        BAND(st->lo[a][i], st->hi[b][i]);
+        BAND(st->lo[b][i], st->hi[a][i]);
+        ok = ok && st->lo[a][i] <= st->hi[b][i] && st->lo[b][i] <= st->hi[a][i];
+    }
+    return ok;
+}
+
+uint32_t oracle_scene_raw_contacts(const OracleScene* s, const double* q, uint32_t a, uint32_t b, double margin_a,
+                                   double margin_b, double* out) {
+    SState* st = (SState*)calloc(1, sizeof(SState));
+    for (uint32_t k = 0; k < s->nb; ++k) {
+        st->pos[k] = vld(q + 7 * k);
+        q4 r = Q(q[7 * k + 3], q[7 * k + 4], q[7 * k + 5], q[7 * k + 6]);
+        qnormalize(r, &st->rot[k], 0);
+    }
+    st->margin[a] = margin_a;
+    if (b < s->nb) st->margin[b] = margin_b;
+    SCol A, B;
+    scol(s, st, a, &A);
+    scol(s, st, b, &B);
+    uint32_t cls = MR_COLLISION_PAIR_UNSUPPORTED;
+    for (uint32_t p = 0; p < s->np; ++p)
+        if (s->pa[p] == a && s->pb[p] == b) cls = s->pc[p];
+    const double acc = A.offset + B.offset + (fmax(scol_scale(&A), scol_scale(&B)) + 1.0) * kPad;
+    SRaw raw;
+    const v3 n = snarrow(&A, &B, (int)cls, a, b, acc, &raw);
+    for (int i = 0; i < raw.n; ++i) {
+        double* o = out + 12 * i;
+        vst(o, n);
+        o[3] = raw.sep[i];
+        vst(o + 4, raw.pa[i]);
+        vst(o + 7, raw.pb[i]);
+        o[10] = raw.fa[i];
+        o[11] = raw.fb[i];
+    }
+    free(st);
+    return (uint32_t)raw.n;
+}
+
+void oracle_scene_table_from_device(const float* words, uint32_t count, OracleSceneSlot* out) {
+    for (uint32_t i = 0; i < count; ++i) {
+        const float* w = words + (size_t)i * 57;
+        memcpy(&out[i].key, w + 56, 4);
+        oracle_manifold_from_device((const MRManifoldC*)w, &out[i].m, 1);
+    }
+}
+
+uint32_t oracle_scene_step(const OracleScene* s, double* q, double* v, OracleSceneSlot* table, uint32_t* count, double friction,
+                           OracleSceneTrace* trace) {
+    memset(trace, 0, sizeof(*trace));
+    g_band = 0;
+    g_margin = INFINITY;
+    const uint32_t nb = s->nb;
+    const double h = s->h;
+    SState* st = (SState*)calloc(1, sizeof(SState));
+    OracleSceneSlot* cur = (OracleSceneSlot*)calloc(SMAN, sizeof(OracleSceneSlot));
+    OracleSceneSlot* nxt = (OracleSceneSlot*)calloc(SMAN, sizeof(OracleSceneSlot));
+    SCon* C = (SCon*)calloc(SCON, sizeof(SCon));
+    uint32_t mcount = *count, status = MR_STEP_SUCCESS, fail_index = 0;
+    memcpy(cur, table, mcount * sizeof(OracleSceneSlot));
+    for (uint32_t b = 0; b < nb; ++b) {
+        st->pos[b] = vld(q + 7 * b);
+        st->rot[b] = Q(q[7 * b + 3], q[7 * b + 4], q[7 * b + 5], q[7 * b + 6]);
+        st->lin[b] = vld(v + 6 * b);
+        st->ang[b] = vld(v + 6 * b + 3);
+    }
+    for (uint32_t sub = 0; sub < s->substeps && status == MR_STEP_SUCCESS; ++sub) {
+        const int final_substep = sub + 1 == s->substeps;
+        sprepare(s, st);
+        for (uint32_t b = 0; b < nb; ++b)
+            if (!vfinite(st->lin[b]) || !vfinite(st->ang[b])) { status = MR_STEP_NONFINITE_RESULT; fail_index = b; }
+        if (status) break;
+        status = sbounds(s, st, &fail_index);
+        if (status) break;
+        uint16_t cand[SCAND];
+        uint32_t ncand = 0;
+        for (uint32_t p = 0; p < s->np; ++p)
+            if (sflag(s, st, s->pa[p], s->pb[p])) {
+                if (ncand >= SCAND) { status = MR_STEP_PAIR_CAPACITY_OVERFLOW; fail_index = ncand; break; }
+                cand[ncand++] = (uint16_t)p;
+            }
+        if (status) break;
+        if (ncand > trace->candidate_pairs) trace->candidate_pairs = ncand;
+        uint32_t ncount = 0, raw_total = 0;
+        for (uint32_t ci = 0; ci < ncand && !status; ++ci) {
+            const uint32_t p = cand[ci], a = s->pa[p], b = s->pb[p];
+            const uint32_t key = a * 65u + b;
+            const OracleManifold* old = NULL;
+            for (uint32_t m = 0; m < mcount; ++m)
+                if (cur[m].key == key) old = &cur[m].m;
+            SCol A, B;
+            scol(s, st, a, &A);
+            scol(s, st, b, &B);
+            const double acc = A.offset + B.offset + (fmax(scol_scale(&A), scol_scale(&B)) + 1.0) * kPad;
+            SRaw raw;
+            const v3 n = snarrow(&A, &B, s->pc[p], a, b, acc, &raw);
+            raw_total += (uint32_t)raw.n;
+            OracleManifold built;
+            const int np_ = sbuild(s, old, &raw, n, &built, A.bpos, A.brot, B.bpos, B.brot);
+            if (np_ < 0) { status = MR_STEP_NONFINITE_RESULT; break; }
+            if (np_ > 0) {
+                if (ncount >= SMAN) { status = MR_STEP_MANIFOLD_CAPACITY_OVERFLOW; fail_index = ncount + 1; break; }
+                nxt[ncount].key = key;
+                nxt[ncount].m = built;
+                ++ncount;
+            }
+        }
+        if (status) break;
+        { OracleSceneSlot* t = cur; cur = nxt; nxt = t; }
+        mcount = ncount;
+        if (mcount > trace->manifold_count) trace->manifold_count = mcount;
+        if (raw_total > trace->raw_count) trace->raw_count = raw_total;
+        /* Contacts in manifold order. */
+        uint32_t total = 0;
+        for (uint32_t m = 0; m < mcount; ++m) total += cur[m].m.count;
+        if (total > SCON) { status = MR_STEP_CONTACT_CAPACITY_OVERFLOW; fail_index = total; break; }
+        total = 0;
+        for (uint32_t m = 0; m < mcount; ++m) {
+            const OracleManifold* mf = &cur[m].m;
+            const uint32_t a = cur[m].key / 65u, b = cur[m].key % 65u;
+            const int plane_b = b >= nb;
+            const v3 posA = st->pos[a];
+            const q4 rotA = st->rot[a];
+            const v3 posB = plane_b ? s->ground_pos : st->pos[b];
+            const q4 rotB = plane_b ? s->ground_rot : st->rot[b];
+            v3 nw = qrot(rotA, vld(mf->normal_local));
+            nw = vmul(nw, 1.0 / vlen(nw));
+            v3 tw = qrot(rotA, vld(mf->tangent_local));
+            tw = vsub(tw, vmul(nw, vdot(tw, nw)));
+            tw = vdot(tw, tw) > 1e-12 ? vmul(tw, 1.0 / vlen(tw)) : stable_tangent(nw);
+            const v3 bw = vcross(nw, tw);
+            const uint32_t ma = s->material[a], mb = plane_b ? s->plane_material : s->material[b];
+            const double mu_s = sqrt(fmax(0.0, s->fric[ma][0] * s->fric[mb][0])) * friction;
+            const double mu_d = sqrt(fmax(0.0, s->fric[ma][1] * s->fric[mb][1])) * friction;
+            const double rest = s->rest[a] + (plane_b ? s->plane_rest : s->rest[b]);
+            for (uint32_t i = 0; i < mf->count; ++i) {
+                const OraclePoint* op = &mf->points[i];
+                SCon* c = &C[total++];
+                const v3 pa = vadd(posA, qrot(rotA, vld(op->anchor_a)));
+                const v3 pb = vadd(posB, qrot(rotB, vld(op->anchor_b)));
+                const v3 pw = vmul(vadd(pa, pb), 0.5);
+                c->sep = vdot(vsub(pb, pa), nw) - rest;
+                c->a = (int)a;
+                c->b = plane_b ? -1 : (int)b;
+                c->ra = vsub(pw, posA);
+                c->rb = vsub(pw, posB);
+                c->n = nw;
+                c->t = tw;
+                c->bt = bw;
+                c->new_impact = op->life == 0u;
+                c->slot = (int)m;
+                c->point = (int)i;
+                for (int k = 0; k < 3; ++k) c->lambda[k] = op->impulses[k];
+                c->target[0] = c->sep > 0.0 ? -c->sep / h : 0.0;
+                c->target[1] = c->target[2] = 0.0;
+                c->reg = fmax((s->resp[ma][2] + s->resp[mb][2]) / (h * h) + (s->resp[ma][3] + s->resp[mb][3]) / h, 0.0);
+                c->mu = mu_s;
+                c->mu_d = mu_d;
+                c->restitution = fmin(fmax(fmax(s->resp[ma][0], s->resp[mb][0]), 0.0), 1.0);
+                c->rthr = fmax(s->resp[ma][1], s->resp[mb][1]);
+            }
+        }
+        trace->contact_count = total;
+        /* IR evaluation at the predicted velocities; blocks; relaxation. */
+        for (uint32_t i = 0; i < total; ++i) {
+            SCon* c = &C[i];
+            const v3 va = vadd(st->lin[c->a], vcross(st->ang[c->a], c->ra));
+            const v3 vb = c->b >= 0 ? vadd(st->lin[c->b], vcross(st->ang[c->b], c->rb)) : V(0, 0, 0);
+            const v3 dv = vsub(vb, va);
+            const v3 dirs[3] = {c->n, c->t, c->bt};
+            const double rel[3] = {vdot(dv, dirs[0]), vdot(dv, dirs[1]), vdot(dv, dirs[2])};
+            const double tau_c = 2.0 * h, ratio = h / tau_c;
+            const double err = fmin(c->sep + s->slop, 0.0);
+            double stab = -h * err / (tau_c * tau_c * (1.0 + 2.0 * ratio + ratio * ratio));
+            stab = fmin(fmax(stab, 0.0), s->max_dep);
+            if (c->new_impact) {
+                const double incoming = rel[0] - c->target[0];
+                if (c->restitution > 0.0) BAND(incoming, -c->rthr);
+                if (incoming < -c->rthr) stab = fmax(stab, -c->restitution * incoming);
+            }
+            c->target[0] += stab;
+            const double slip = sqrt(rel[1] * rel[1] + rel[2] * rel[2]);
+            if (c->mu_d != c->mu) BAND(slip, 1e-3);
+            if (!(slip <= 1e-3)) c->mu = c->mu_d;
+            double W[9] = {0};
+            for (int side = 0; side < 2; ++side) {
+                const int body = side ? c->b : c->a;
+                if (body < 0) continue;
+                const v3 r = side ? c->rb : c->ra;
+                for (int x = 0; x < 3; ++x)
+                    for (int y = 0; y < 3; ++y) {
+                        const v3 rx = vcross(r, dirs[x]), ry = vcross(r, dirs[y]);
+                        W[x * 3 + y] += s->inv_mass[body] * vdot(dirs[x], dirs[y]) + vdot(rx, sym3_apply(st->iiw[body], ry));
+                    }
+            }
+            double rowsum = 0.0;
+            for (uint32_t j = 0; j < total; ++j) {
+                const SCon* d = &C[j];
+                double w = 0.0;
+                int shared = 0;
+                for (int t = 0; t < 2; ++t) {
+                    const int bi = t ? c->b : c->a;
+                    if (bi < 0) continue;
+                    const int tj = d->a == bi ? 0 : (d->b == bi ? 1 : -1);
+                    if (tj < 0) continue;
+                    shared = 1;
+                    const double si = t ? 1.0 : -1.0, sj = tj ? 1.0 : -1.0;
+                    const v3 ri = t ? c->rb : c->ra, rj = tj ? d->rb : d->ra;
+                    w += si * sj * (s->inv_mass[bi] * vdot(c->n, d->n) + vdot(vcross(ri, c->n), sym3_apply(st->iiw[bi], vcross(rj, d->n))));
+                }
+                if (shared) rowsum += fabs(w);
+            }
+            const double diag = fabs(W[0]) + c->reg;
+            W[0] += c->reg;
+            if (!oracle_invert3x3(W, c->P)) { status = MR_STEP_FACTORIZATION_FAILED; fail_index = i; break; }
+            c->relax = rowsum > fmax(diag, kMatrixFloor) ? fmin(fmax(diag / rowsum, 1.0 / 32.0), 1.0) : 1.0;
+            double warm[3];
+            oracle_project_cone(c->lambda, c->mu, c->mu, warm);
+            for (int k = 0; k < 3; ++k) { c->lambda[k] = warm[k]; c->delta[k] = warm[k]; }
+        }
+        if (status) break;
+        /* Islands (min-root union find over dynamic bodies). */
+        if (total > 0) {
+            int parent[SNB], touched[SNB] = {0};
+            for (uint32_t b = 0; b < nb; ++b) parent[b] = (int)b;
+            for (uint32_t i = 0; i < total; ++i) {
+                int x = C[i].a;
+                touched[x] = 1;
+                if (C[i].b >= 0) {
+                    int y = C[i].b;
+                    touched[y] = 1;
+                    while (parent[x] != x) x = parent[x];
+                    while (parent[y] != y) y = parent[y];
+                    if (x != y) parent[x > y ? x : y] = x < y ? x : y;
+                }
+            }
+            uint32_t islands = 0;
+            for (uint32_t b = 0; b < nb; ++b) {
+                int r = (int)b;
+                while (parent[r] != r) r = parent[r];
+                if (touched[b] && r == (int)b) ++islands;
+            }
+            if (islands > trace->islands) trace->islands = islands;
+        }
+        /* Jacobi sweeps; sweep -1 applies the warm start. */
+        const int iters = (int)s->iters + (final_substep ? (int)s->final_iters : 0);
+        for (int it = -1; it < iters && !status; ++it) {
+            if (it >= 0) {
+                for (uint32_t i = 0; i < total; ++i) {
+                    SCon* c = &C[i];
+                    const v3 va = vadd(st->lin[c->a], vcross(st->ang[c->a], c->ra));
+                    const v3 vb = c->b >= 0 ? vadd(st->lin[c->b], vcross(st->ang[c->b], c->rb)) : V(0, 0, 0);
+                    const v3 dv = vsub(vb, va);
+                    const double r0 = c->target[0] - vdot(dv, c->n) - c->reg * c->lambda[0];
+                    const double r1 = c->target[1] - vdot(dv, c->t);
+                    const double r2 = c->target[2] - vdot(dv, c->bt);
+                    double prop[3], proj[3];
+                    for (int k = 0; k < 3; ++k) prop[k] = c->lambda[k] + c->P[3 * k] * r0 + c->P[3 * k + 1] * r1 + c->P[3 * k + 2] * r2;
+                    oracle_project_cone(prop, c->mu, c->mu, proj);
+                    for (int k = 0; k < 3; ++k) c->delta[k] = c->relax * (proj[k] - c->lambda[k]);
+                    int finite = 1;
+                    for (int k = 0; k < 3; ++k) finite &= isfinite(c->lambda[k] + c->delta[k]) && isfinite(c->delta[k]);
+                    if (!finite) { status = MR_STEP_NONFINITE_RESULT; fail_index = i; break; }
+                    for (int k = 0; k < 3; ++k) c->lambda[k] += c->delta[k];
+                }
+                if (status) break;
+            }
+            for (uint32_t b = 0; b < nb; ++b) {
+                v3 dl = V(0, 0, 0), dw = V(0, 0, 0);
+                for (uint32_t i = 0; i < total; ++i) {
+                    const SCon* c = &C[i];
+                    for (int side = 0; side < 2; ++side) {
+                        if ((side ? c->b : c->a) != (int)b) continue;
+                        const v3 imp = vadd(vadd(vmul(c->n, c->delta[0]), vmul(c->t, c->delta[1])), vmul(c->bt, c->delta[2]));
+                        const v3 f = side ? imp : vmul(imp, -1.0);
+                        dl = vadd(dl, f);
+                        dw = vadd(dw, vcross(side ? c->rb : c->ra, f));
+                    }
+                }
+                st->lin[b] = vadd(st->lin[b], vmul(dl, s->inv_mass[b]));
+                st->ang[b] = vadd(st->ang[b], sym3_apply(st->iiw[b], dw));
+            }
+        }
+        if (status) break;
+        for (uint32_t i = 0; i < total; ++i)
+            for (int k = 0; k < 3; ++k) cur[C[i].slot].m.points[C[i].point].impulses[k] = C[i].lambda[k];
+        for (uint32_t b = 0; b < nb; ++b) {
+            v3 lin = st->lin[b], ang = st->ang[b];
+            const double ls = vlen(lin), ws = vlen(ang);
+            if (s->max_lin[b] > 0.0 && ls > s->max_lin[b]) lin = vmul(lin, s->max_lin[b] / ls);
+            if (s->max_ang[b] > 0.0 && ws > s->max_ang[b]) ang = vmul(ang, s->max_ang[b] / ws);
+            const v3 c = vadd(st->pos[b], vmul(lin, h));
+            q4 qn = qmul(so3_increment(vmul(ang, h), 0), st->rot[b]);
+            const double qq = qdot(qn, qn);
+            if (!qfinite(qn) || !(qq > 1e-12) || !vfinite(c)) { status = MR_STEP_NONFINITE_RESULT; fail_index = b; break; }
+            const double inv = 1.0 / sqrt(qq);
+            st->rot[b] = Q(qn.x * inv, qn.y * inv, qn.z * inv, qn.w * inv);
+            st->pos[b] = c;
+            st->lin[b] = lin;
+            st->ang[b] = ang;
+        }
+    }
+    trace->status = status;
+    trace->failing_index = fail_index;
+    trace->band_decisions = g_band;
+    trace->min_decision_margin = g_margin;
+    if (status == MR_STEP_SUCCESS) {
+        for (uint32_t b = 0; b < nb; ++b) {
+            vst(q + 7 * b, st->pos[b]);
+            q[7 * b + 3] = st->rot[b].x;
+            q[7 * b + 4] = st->rot[b].y;
+            q[7 * b + 5] = st->rot[b].z;
+            q[7 * b + 6] = st->rot[b].w;
+            vst(v + 6 * b, st->lin[b]);
+            vst(v + 6 * b + 3, st->ang[b]);
+        }
+        memcpy(table, cur, mcount * sizeof(OracleSceneSlot));
+        *count = mcount;
+    }
+    free(st);
+    free(cur);
+    free(nxt);
+    free(C);
+    return status;
+}
+
+uint32_t oracle_scene_collide(const OracleScene* s, const double* q, OracleSceneSlot* table, uint32_t* count, double* raw_out,
+                              uint32_t raw_cap, uint32_t* raw_count) {
+    g_band = 0;
+    g_margin = INFINITY;
+    SState* st = (SState*)calloc(1, sizeof(SState));
+    OracleSceneSlot* nxt = (OracleSceneSlot*)calloc(SMAN, sizeof(OracleSceneSlot));
+    uint32_t status = MR_STEP_SUCCESS, ncount = 0, nraw = 0;
+    for (uint32_t b = 0; b < s->nb; ++b) {
+        st->pos[b] = vld(q + 7 * b);
+        if (!qnormalize(Q(q[7 * b + 3], q[7 * b + 4], q[7 * b + 5], q[7 * b + 6]), &st->rot[b], 1)) status = MR_STEP_NONFINITE_INPUT;
+    }
+    for (uint32_t p = 0; p < s->np && status == MR_STEP_SUCCESS; ++p) {
+        const uint32_t a = s->pa[p], b = s->pb[p], key = a * 65u + b;
+        const OracleManifold* old = NULL;
+        for (uint32_t m = 0; m < *count; ++m)
+            if (table[m].key == key) old = &table[m].m;
+        SCol A, B;
+        scol(s, st, a, &A);
+        scol(s, st, b, &B);
+        const double acc = A.offset + B.offset + (fmax(scol_scale(&A), scol_scale(&B)) + 1.0) * kPad;
+        SRaw raw;
+        const v3 n = snarrow(&A, &B, s->pc[p], a, b, acc, &raw);
+        for (int i = 0; i < raw.n && nraw < raw_cap; ++i, ++nraw) {
+            double* o = raw_out + 16 * nraw;
+            o[0] = a;
+            o[1] = b;
+            vst(o + 2, n);
+            o[5] = raw.sep[i];
+            vst(o + 6, raw.pa[i]);
+            vst(o + 9, raw.pb[i]);
+            o[12] = raw.fa[i];
+            o[13] = raw.fb[i];
+            o[14] = o[15] = 0.0;
+        }
+        OracleManifold built;
+        const int np_ = sbuild(s, old, &raw, n, &built, A.bpos, A.brot, B.bpos, B.brot);
+        if (np_ < 0) { status = MR_STEP_NONFINITE_RESULT; break; }
+        if (np_ > 0) {
+            if (ncount >= SMAN) { status = MR_STEP_MANIFOLD_CAPACITY_OVERFLOW; break; }
+            nxt[ncount].key = key;
+            nxt[ncount].m = built;
+            ++ncount;
+        }
+    }
+    if (status == MR_STEP_SUCCESS) {
+        memcpy(table, nxt, ncount * sizeof(OracleSceneSlot));
+        *count = ncount;
+        *raw_count = nraw;
+    }
+    free(st);
+    free(nxt);
+    return status;
+}

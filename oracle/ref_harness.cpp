@@ -9,12 +9,15 @@
 //   - integrateArticulatedState (ArticulatedDynamics.cpp:2333),
 //   - solveReferenceConicProblem (src/core/ReferenceConicSolver.cpp:182),
 //   - stepControlledArticulatedWorldCpu (src/core/ArticulatedWorld.cpp:1232)
-//     and a multi-threaded timing loop over it (the CPU baseline).
+//     and a multi-threaded timing loop over it (the CPU baseline),
+//   - collideCpuReference (src/core/Collision.cpp:2959) over a free-body
+//     pile: raw contacts and persistent manifolds of every touching pair.
 // Implicit PD drives are expressed for the reference the way its own GPU
 // ABA does: armature raised by h kd + h^2 kp and the PD law evaluated as an
 // effort (ArticulatedABA.metal:301-326, MetalWorld.metal:280-370).
 #include "metalrobo/ArticulatedDynamics.hpp"
 #include "metalrobo/ArticulatedWorld.hpp"
+#include "metalrobo/Collision.hpp"
 #include "metalrobo/EngineModel.hpp"
 #include "metalrobo/ReferenceConicSolver.hpp"
 
@@ -413,6 +416,139 @@ __attribute__((visibility("default"))) double ref_run(RefModel* r, uint32_t envs
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (failed_steps) *failed_steps = failed.load();
     return secs;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Free-body piles: the reference's FP64 collision oracle over one pile.
+// ---------------------------------------------------------------------------
+
+struct RefScene {
+    std::vector<MRShapeGPU> shapes;
+    std::vector<MRBodyStateGPU> bodies;
+    CollisionConfig config;
+    PersistentManifoldCache cache;
+    std::uint32_t nb = 0;
+};
+
+extern "C" {
+
+__attribute__((visibility("default"))) RefScene* ref_scene_create(const MRModelWorldC* world, const MRModelBodyC* bodies,
+                                                                  const MRModelShapeC* shapes, char* err, size_t err_len) {
+    try {
+        auto r = std::make_unique<RefScene>();
+        r->nb = world->body_count - 1;
+        for (std::uint32_t b = 0; b < world->body_count; ++b) {
+            MRBodyStateGPU st{};
+            const bool ground = b == r->nb;
+            st.position = ground ? f4(bodies[b].static_pose[0], bodies[b].static_pose[1], bodies[b].static_pose[2], 0.0)
+                                 : f4(0.0, 0.0, 0.0, 0.0);
+            st.orientation = ground ? f4(bodies[b].static_pose + 4) : f4(0.0, 0.0, 0.0, 1.0);
+            st.flagsAndIndices[0] = ground ? MR_MOTION_STATIC : MR_MOTION_DYNAMIC;
+            st.flagsAndIndices[1] = MR_INVALID_INDEX;
+            st.flagsAndIndices[2] = MR_INVALID_INDEX;
+            r->bodies.push_back(st);
+        }
+        for (std::uint32_t s = 0; s < world->shape_count; ++s) {
+            const MRModelShapeC& src = shapes[s];
+            MRShapeGPU sh{};
+            sh.bodyIndex = src.body;
+            sh.shapeType = src.shape_type;
+            sh.materialIndex = src.material;
+            sh.collisionGroup = src.collision_group;
+            sh.collisionMask = src.collision_mask;
+            sh.slotGeneration = 1;
+            sh.localPosition = f4(src.local_position[0], src.local_position[1], src.local_position[2], 1.0);
+            sh.localRotation = f4(src.local_rotation);
+            sh.dimensions = f4(src.dimensions);
+            sh.contactRestAndBoundingRadius = f4(src.contact_rest_bound);
+            r->shapes.push_back(sh);
+        }
+        r->config.capacities = CollisionCapacities{4096u, 8192u, 2048u};
+        r->config.manifoldBreakingSeparation = world->manifold_thresholds[0];
+        r->config.manifoldBreakingTangential = world->manifold_thresholds[1];
+        r->config.manifoldMergeDistance = world->manifold_thresholds[2];
+        r->config.manifoldNormalCosine = world->manifold_thresholds[3];
+        return r.release();
+    } catch (const std::exception& e) {
+        write_error(err, err_len, e.what());
+        return nullptr;
+    }
+}
+
+__attribute__((visibility("default"))) void ref_scene_destroy(RefScene* r) { delete r; }
+
+// One collision pass at body poses q ([nb][7], xyzw).  Raw contacts: 16
+// doubles each (collider a, b, normal xyz, separation, point A xyz, point B
+// xyz, feature A, feature B, 0, 0).  Manifolds: 58 doubles each (a, b,
+// count, normal xyz, age, tangent xyz, then four points of anchor A xyz,
+// anchor B xyz, impulses xyz, feature A, feature B, life).  Returns the
+// reference's status code; the cache carries manifolds to the next call.
+__attribute__((visibility("default"))) int ref_scene_collide(RefScene* r, const double* q, std::uint32_t raw_cap, double* raw,
+                                                             std::uint32_t* raw_count, std::uint32_t manifold_cap, double* manifolds,
+                                                             std::uint32_t* manifold_count) {
+    for (std::uint32_t b = 0; b < r->nb; ++b) {
+        r->bodies[b].position = f4(q[7 * b], q[7 * b + 1], q[7 * b + 2], 0.0);
+        r->bodies[b].orientation = f4(q[7 * b + 3], q[7 * b + 4], q[7 * b + 5], q[7 * b + 6]);
+    }
+    const CollisionFrame f = collideCpuReference(r->shapes, r->bodies, r->config, r->cache);
+    *raw_count = 0;
+    *manifold_count = 0;
+    if (!f.succeeded()) return static_cast<int>(f.diagnostics.code);
+    for (std::size_t i = 0; i < f.rawContacts.size() && i < raw_cap; ++i) {
+        const MRRawContactGPU& c = f.rawContacts[i];
+        const MRCandidatePairGPU& p = f.pairs[f.rawContactPairIndices[i]];
+        double* o = raw + 16 * i;
+        o[0] = p.colliderA;
+        o[1] = p.colliderB;
+        o[2] = c.normalAndSeparation.x;
+        o[3] = c.normalAndSeparation.y;
+        o[4] = c.normalAndSeparation.z;
+        o[5] = c.normalAndSeparation.w;
+        o[6] = c.pointAWorld.x;
+        o[7] = c.pointAWorld.y;
+        o[8] = c.pointAWorld.z;
+        o[9] = c.pointBWorld.x;
+        o[10] = c.pointBWorld.y;
+        o[11] = c.pointBWorld.z;
+        o[12] = c.featureAndFlags[0];
+        o[13] = c.featureAndFlags[1];
+        o[14] = o[15] = 0.0;
+        *raw_count = static_cast<std::uint32_t>(i + 1);
+    }
+    for (std::size_t m = 0; m < f.manifoldHeaders.size() && m < manifold_cap; ++m) {
+        const MRManifoldHeaderGPU& hd = f.manifoldHeaders[m];
+        double* o = manifolds + 58 * m;
+        o[0] = hd.pairAndCount[1];
+        o[1] = hd.pairAndCount[2];
+        o[2] = hd.pairAndCount[3];
+        o[3] = hd.normalAndAge.x;
+        o[4] = hd.normalAndAge.y;
+        o[5] = hd.normalAndAge.z;
+        o[6] = hd.normalAndAge.w;
+        o[7] = hd.tangentAndMetric.x;
+        o[8] = hd.tangentAndMetric.y;
+        o[9] = hd.tangentAndMetric.z;
+        for (int k = 0; k < 4; ++k) {
+            const MRManifoldPointGPU& pt = f.manifoldPoints[4 * m + k];
+            double* po = o + 10 + 12 * k;
+            po[0] = pt.localAnchorA.x;
+            po[1] = pt.localAnchorA.y;
+            po[2] = pt.localAnchorA.z;
+            po[3] = pt.localAnchorB.x;
+            po[4] = pt.localAnchorB.y;
+            po[5] = pt.localAnchorB.z;
+            po[6] = pt.impulses.x;
+            po[7] = pt.impulses.y;
+            po[8] = pt.impulses.z;
+            po[9] = pt.featureAndLife[0];
+            po[10] = pt.featureAndLife[1];
+            po[11] = pt.featureAndLife[2];
+        }
+        *manifold_count = static_cast<std::uint32_t>(m + 1);
+    }
+    return 0;
 }
 
 }  // extern "C"

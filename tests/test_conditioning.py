@@ -64,3 +64,53 @@ def test_oracle_sensitivity_to_fp32_input_rounding_is_below_gpu_tolerance():
     assert worst > 1e-6
     # ... and stays below the tolerance the GPU parity test applies.
     assert worst < TREE_V_WORST
+
+
+PILE_V_WORST = 1e-3  # tests/test_scene_parity.py
+PERTURBATION = 8 * 2.0 ** -24  # eight FP32 roundings
+
+
+def test_pile_oracle_sensitivity_to_fp32_input_rounding_is_below_gpu_tolerance():
+    # Piles stack contacts body on body.  The device forms every world
+    # contact point from body-frame anchors by a quaternion rotation and a
+    # translation in FP32 -- a chain of about eight rounded operations per
+    # component -- so its positions carry relative errors of several parts
+    # in 1e7 before the -sep / h targets amplify them.  The FP64 oracle's
+    # response to an input perturbation of that size bounds what the
+    # per-step comparison can resolve.
+    from oracle import SceneOracle, SceneTable
+
+    rng = np.random.default_rng(9)
+    sens = []
+    contacts = 0
+    for seed in (1, 13):
+        rec = nb.compile_model("pile", seed)
+        oracle = SceneOracle(rec, H, 4, 8, 0)
+        q0, v0, f = nb.sample_reset("pile", seed, 1, 0, 1)
+        q = q0[0].astype(np.float64)
+        v = v0[0].astype(np.float64)
+        table = SceneTable()
+        for k in range(60):
+            assert oracle.step(q, v, table, float(f[0]))[0] == 0
+            if k < 30 or k % 3:
+                continue
+            qa = q.astype(np.float32).astype(np.float64)
+            va = v.astype(np.float32).astype(np.float64)
+            qb = qa * (1.0 + PERTURBATION * rng.standard_normal(qa.size))
+            vb = va * (1.0 + PERTURBATION * rng.standard_normal(va.size))
+            ta, tb = SceneTable(), SceneTable()
+            ct.memmove(ta.slots, table.slots, ct.sizeof(ta.slots))
+            ct.memmove(tb.slots, table.slots, ct.sizeof(tb.slots))
+            ta.count.value = tb.count.value = table.count.value
+            sa, tr = oracle.step(qa, va, ta, float(f[0]))
+            sb, trb = oracle.step(qb, vb, tb, float(f[0]))
+            assert sa == 0 and sb == 0
+            if tr.band_decisions or trb.band_decisions or ta.keys() != tb.keys():
+                continue
+            contacts += tr.contact_count
+            sens.append(float(np.max(np.abs(va - vb)) / max(1.0, float(np.max(np.abs(va))))))
+    worst = max(sens)
+    print(f"pile oracle velocity response to {PERTURBATION:.0e} input perturbation: median {np.median(sens):.2e} worst {worst:.2e}")
+    assert contacts > 0
+    assert worst > 1e-6
+    assert worst < PILE_V_WORST
