@@ -73,6 +73,23 @@ enum CandWord : int { kCdLaS = 0, kCdLbS = 3, kCdFaS = 6, kCdFbS = 7, kCdWpS = 8
 __device__ __forceinline__ int ai(float f) { return __float_as_int(f); }
 __device__ __forceinline__ float af(int i) { return __int_as_float(i); }
 
+// One contact record.  Records are stored word-major ([word][contact]), so
+// the lanes of a warp reading one word of consecutive contacts touch one
+// cache line.
+struct Rec {
+    float* p;
+    __device__ __forceinline__ float& operator[](int w) const { return p[w * kSceneContacts]; }
+    __device__ __forceinline__ float3 v3(int w) const {
+        return f3(p[w * kSceneContacts], p[(w + 1) * kSceneContacts], p[(w + 2) * kSceneContacts]);
+    }
+    __device__ __forceinline__ void set3(int w, float3 v) const {
+        p[w * kSceneContacts] = v.x;
+        p[(w + 1) * kSceneContacts] = v.y;
+        p[(w + 2) * kSceneContacts] = v.z;
+    }
+};
+__device__ __forceinline__ Rec rec(float* C, int c) { return Rec{C + c}; }
+
 __device__ __forceinline__ void fail(float* misc, unsigned code, unsigned index) {
     if (ai(misc[kSmStatus]) == MR_STEP_SUCCESS) {
         misc[kSmStatus] = af(static_cast<int>(code));
@@ -762,18 +779,18 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
                 const float rest = M.offsets[a].y + (plane_b ? M.plane_offsets.y : M.offsets[b].y);
                 for (int i = 0; i < cnt; ++i) {
                     const float* op = slot + 8 + i * 12;
-                    float* c = C + (first + i) * kCw;
+                    const Rec c = rec(C, first + i);
                     const float3 pa = posA + qrot(rotA, ld3(op));
                     const float3 pb = posB + qrot(rotB, ld3(op + 3));
                     const float3 pw = 0.5f * (pa + pb);
                     const float sep = dot3(pb - pa, nw) - rest;
                     c[kScA] = af(a);
                     c[kScB] = af(plane_b ? -1 : b);
-                    st3(c + kScRa, pw - posA);
-                    st3(c + kScRb, pw - posB);
-                    st3(c + kScN, nw);
-                    st3(c + kScT, tw);
-                    st3(c + kScBt, bw);
+                    c.set3(kScRa, pw - posA);
+                    c.set3(kScRb, pw - posB);
+                    c.set3(kScN, nw);
+                    c.set3(kScT, tw);
+                    c.set3(kScBt, bw);
                     const bool new_impact = static_cast<unsigned>(ai(op[8])) == 0u;
                     c[kScFlags] = af(new_impact ? 1 : 0);
                     c[kScSlot] = af(mi * 4 + i);
@@ -807,7 +824,7 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
         for (int b = lane; b < nb; b += 32) {
             int cnt = 0;
             for (int c = 0; c < total; ++c) {
-                const float* cr = C + c * kCw;
+                const Rec cr = rec(C, c);
                 cnt += (ai(cr[kScA]) == b) + (ai(cr[kScB]) == b);
             }
             fill[b] = cnt;
@@ -822,7 +839,7 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
         for (int b = lane; b < nb; b += 32) {
             int at = start[b];
             for (int c = 0; c < total; ++c) {
-                const float* cr = C + c * kCw;
+                const Rec cr = rec(C, c);
                 if (ai(cr[kScA]) == b) entries[at++] = static_cast<std::uint16_t>(c << 1);
                 if (ai(cr[kScB]) == b) entries[at++] = static_cast<std::uint16_t>((c << 1) | 1);
             }
@@ -836,11 +853,11 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
             return ld3(s + kOffLin + body * 3) + cross3(ld3(s + kOffAng + body * 3), r);
         };
         for (int c = lane; c < total; c += 32) {
-            float* cr = C + c * kCw;
+            const Rec cr = rec(C, c);
             const int a = ai(cr[kScA]), b = ai(cr[kScB]);
-            const float3 ra = ld3(cr + kScRa), rb = ld3(cr + kScRb);
+            const float3 ra = cr.v3(kScRa), rb = cr.v3(kScRb);
             const float3 dv = point_velocity(b, rb) - point_velocity(a, ra);
-            const float3 dirs[3] = {ld3(cr + kScN), ld3(cr + kScT), ld3(cr + kScBt)};
+            const float3 dirs[3] = {cr.v3(kScN), cr.v3(kScT), cr.v3(kScBt)};
             const float rel[3] = {dot3(dv, dirs[0]), dot3(dv, dirs[1]), dot3(dv, dirs[2])};
             const float sep = cr[kScDelta + 2];
             const float tau_c = 2.0f * h;
@@ -878,7 +895,7 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
                 if (body < 0) continue;
                 for (int k = start[body]; k < start[body + 1]; ++k) {
                     const int cj = entries[k] >> 1, sj = entries[k] & 1;
-                    const float* crj = C + cj * kCw;
+                    const Rec crj = rec(C, cj);
                     const int oa = ai(crj[kScA]), ob = ai(crj[kScB]);
                     // Skip on the second body when the first one already counted j.
                     if (side == 1 && (oa == a || ob == a) && a >= 0) continue;
@@ -889,8 +906,8 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
                         const int tj = (oa == bi) ? 0 : ((ob == bi) ? 1 : -1);
                         if (tj < 0) continue;
                         const float si = t ? 1.0f : -1.0f, sjn = tj ? 1.0f : -1.0f;
-                        const float3 ri = t ? rb : ra, rj = ld3(crj + (tj ? kScRb : kScRa));
-                        const float3 n_j = ld3(crj + kScN);
+                        const float3 ri = t ? rb : ra, rj = crj.v3(tj ? kScRb : kScRa);
+                        const float3 n_j = crj.v3(kScN);
                         const float3 rni = cross3(ri, n_i), rnj = cross3(rj, n_j);
                         w += si * sjn * (M.mass[bi].y * dot3(n_i, n_j) + dot3(rni, sym3_mul(s + kOffIiw + bi * 6, rnj)));
                     }
@@ -909,20 +926,20 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
                     for (int j = 0; j < 3; ++j) cr[kScPre + i * 3 + j] = inv[i][j];
             }
             cr[kScRelax] = rowsum > fmaxf(diag, kMatrixFloor) ? fminf(fmaxf(diag / rowsum, 1.0f / 32.0f), 1.0f) : 1.0f;
-            const float3 warm = project_cone(ld3(cr + kScLambda), cr[kScMu], cr[kScMu]);
-            st3(cr + kScLambda, warm);
-            st3(cr + kScDelta, warm);
+            const float3 warm = project_cone(cr.v3(kScLambda), cr[kScMu], cr[kScMu]);
+            cr.set3(kScLambda, warm);
+            cr.set3(kScDelta, warm);
             if (!isfinite(cr[kScTarget])) fail(misc, MR_STEP_NONFINITE_RESULT, static_cast<unsigned>(c));
         }
         if (!ok(misc)) break;
         // Islands: min-root union find over dynamic bodies joined by contacts.
         if (lane == 0 && total > 0) {
-            int parent[kSceneMaxBodies];
+            int* parent = reinterpret_cast<int*>(s + kOffCand);  // candidates are consumed by now
             for (int b = 0; b < nb; ++b) parent[b] = b;
             auto root = [&](int x) { while (parent[x] != x) x = parent[x] = parent[parent[x]]; return x; };
             unsigned touched[2] = {0u, 0u};
             for (int c = 0; c < total; ++c) {
-                const int a = ai(C[c * kCw + kScA]), b = ai(C[c * kCw + kScB]);
+                const int a = ai(rec(C, c)[kScA]), b = ai(rec(C, c)[kScB]);
                 touched[a >> 5] |= 1u << (a & 31);
                 if (b >= 0) {
                     touched[b >> 5] |= 1u << (b & 31);
@@ -941,25 +958,25 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
         for (int it = -1; it < iters; ++it) {
             if (it >= 0) {
                 for (int c = lane; c < total; c += 32) {
-                    float* cr = C + c * kCw;
+                    const Rec cr = rec(C, c);
                     const int a = ai(cr[kScA]), b = ai(cr[kScB]);
-                    const float3 dv = point_velocity(b, ld3(cr + kScRb)) - point_velocity(a, ld3(cr + kScRa));
-                    const float3 prev = ld3(cr + kScLambda);
-                    const float r0 = cr[kScTarget + 0] - dot3(dv, ld3(cr + kScN)) - cr[kScReg] * prev.x;
-                    const float r1 = cr[kScTarget + 1] - dot3(dv, ld3(cr + kScT));
-                    const float r2 = cr[kScTarget + 2] - dot3(dv, ld3(cr + kScBt));
-                    const float* P = cr + kScPre;
-                    float3 prop = f3(prev.x + P[0] * r0 + P[1] * r1 + P[2] * r2, prev.y + P[3] * r0 + P[4] * r1 + P[5] * r2,
-                                     prev.z + P[6] * r0 + P[7] * r1 + P[8] * r2);
+                    const float3 dv = point_velocity(b, cr.v3(kScRb)) - point_velocity(a, cr.v3(kScRa));
+                    const float3 prev = cr.v3(kScLambda);
+                    const float r0 = cr[kScTarget + 0] - dot3(dv, cr.v3(kScN)) - cr[kScReg] * prev.x;
+                    const float r1 = cr[kScTarget + 1] - dot3(dv, cr.v3(kScT));
+                    const float r2 = cr[kScTarget + 2] - dot3(dv, cr.v3(kScBt));
+                    float3 prop = f3(prev.x + cr[kScPre + 0] * r0 + cr[kScPre + 1] * r1 + cr[kScPre + 2] * r2,
+                                     prev.y + cr[kScPre + 3] * r0 + cr[kScPre + 4] * r1 + cr[kScPre + 5] * r2,
+                                     prev.z + cr[kScPre + 6] * r0 + cr[kScPre + 7] * r1 + cr[kScPre + 8] * r2);
                     prop = project_cone(prop, cr[kScMu], cr[kScMu]);
                     const float3 delta = cr[kScRelax] * (prop - prev);
                     const float3 next = prev + delta;
                     if (!finite3(next) || !finite3(delta)) {
                         fail(misc, MR_STEP_NONFINITE_RESULT, static_cast<unsigned>(c));
-                        st3(cr + kScDelta, f3(0.0f, 0.0f, 0.0f));
+                        cr.set3(kScDelta, f3(0.0f, 0.0f, 0.0f));
                     } else {
-                        st3(cr + kScLambda, next);
-                        st3(cr + kScDelta, delta);
+                        cr.set3(kScLambda, next);
+                        cr.set3(kScDelta, delta);
                     }
                 }
                 __syncwarp();
@@ -968,12 +985,12 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
                 float3 dl = f3(0.0f, 0.0f, 0.0f), dw = f3(0.0f, 0.0f, 0.0f);
                 for (int k = start[b]; k < start[b + 1]; ++k) {
                     const int c = entries[k] >> 1, side = entries[k] & 1;
-                    const float* cr = C + c * kCw;
-                    const float3 d = ld3(cr + kScDelta);
-                    const float3 imp = ld3(cr + kScN) * d.x + ld3(cr + kScT) * d.y + ld3(cr + kScBt) * d.z;
+                    const Rec cr = rec(C, c);
+                    const float3 d = cr.v3(kScDelta);
+                    const float3 imp = cr.v3(kScN) * d.x + cr.v3(kScT) * d.y + cr.v3(kScBt) * d.z;
                     const float3 f = side ? imp : -imp;
                     dl = dl + f;
-                    dw = dw + cross3(ld3(cr + (side ? kScRb : kScRa)), f);
+                    dw = dw + cross3(cr.v3(side ? kScRb : kScRa), f);
                 }
                 const float im = M.mass[b].y;
                 st3(s + kOffLin + b * 3, ld3(s + kOffLin + b * 3) + im * dl);
@@ -984,7 +1001,7 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
         if (!ok(misc)) break;
         // Impulses back into the manifold points.
         for (int c = lane; c < total; c += 32) {
-            const float* cr = C + c * kCw;
+            const Rec cr = rec(C, c);
             const int slot = ai(cr[kScSlot]);
             float* op = tab + (slot >> 2) * kSceneSlotWords + 8 + (slot & 3) * 12;
             op[9] = cr[kScLambda + 0];
