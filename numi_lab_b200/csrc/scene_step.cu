@@ -33,7 +33,7 @@ constexpr float kTieRel = 1.0e-5f;
 constexpr float kTieAbs = 1.0e-12f;
 constexpr int kRawCap = 8;
 constexpr int kRecWords = 16;                                   // candidate record
-constexpr int kLaneScratch = (4 + kRawCap) * kRecWords + 4 + 56;  // records, ids, new slot
+constexpr int kLaneScratch = (4 + kRawCap) * kRecWords + 4;  // records, candidate ids
 constexpr int kCw = 40;                                          // contact record words
 
 // Shared-memory layout of one environment (floats): body state, swept
@@ -47,10 +47,15 @@ constexpr int kOffIiw = kOffAng + kSceneMaxBodies * 3;   // world inverse inerti
 constexpr int kOffLo = kOffIiw + kSceneMaxBodies * 6;
 constexpr int kOffHi = kOffLo + kSceneMaxBodies * 3;
 constexpr int kOffMargin = kOffHi + kSceneMaxBodies * 3;
-constexpr int kOffCand = kOffMargin + kSceneMaxBodies;   // u16 candidates
-constexpr int kOffLists = kOffCand + kSceneCandidates / 2;  // start[65], fill[65] (ints)
-constexpr int kOffEntries = kOffLists + 2 * (kSceneMaxBodies + 1);  // 2 * contacts u16 entries
-constexpr int kOffMisc = kOffEntries + kSceneContacts;
+// Candidate pairs (u16) live only until the narrowphase has consumed them;
+// the per-body contact list entries (u16) reuse their words afterwards.
+constexpr int kOffCand = kOffMargin + kSceneMaxBodies;
+constexpr int kOffEntries = kOffCand;
+constexpr int kCandWords = (kSceneCandidates > 2 * kSceneContacts ? kSceneCandidates : 2 * kSceneContacts) / 2;
+constexpr int kOffLists = kOffCand + kCandWords;  // start[65], fill[65] (ints)
+constexpr int kOffKeys = kOffLists + 2 * (kSceneMaxBodies + 1);  // pair keys of the two tables (u32)
+constexpr int kOffFirst = kOffKeys + 2 * kSceneManifolds;  // first contact of each manifold (u16, +1)
+constexpr int kOffMisc = kOffFirst + (kSceneManifolds + 2) / 2;
 constexpr int kSceneSmemWords = kOffMisc + 32;
 
 // Global workspace of one environment (floats, L2-resident while the
@@ -544,6 +549,8 @@ __device__ __forceinline__ float3 sym3_mul(const float* S, float3 x) {
     return f3(S[0] * x.x + S[1] * x.y + S[3] * x.z, S[1] * x.x + S[2] * x.y + S[4] * x.z, S[3] * x.x + S[4] * x.y + S[5] * x.z);
 }
 
+// 128 registers: 16 resident warps per SM.  More warps (96 registers) ran
+// slower: their narrowphase scratch no longer fits the L1 cache.
 __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
     extern __shared__ float4 smem4[];
     float* s = reinterpret_cast<float*>(smem4);
@@ -572,6 +579,11 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
     float* persistent = p.manifolds + static_cast<size_t>(env) * kTableWords;
     const float* cur_table = persistent;
     int mcount = reset ? 0 : static_cast<int>(p.manifold_count[env]);
+    // Shared copies of the current table's pair keys (binary search) and of
+    // the next one's, built as the narrowphase writes it.
+    std::uint32_t* keys_cur = reinterpret_cast<std::uint32_t*>(s + kOffKeys);
+    std::uint32_t* keys_next = keys_cur + kSceneManifolds;
+    for (int i = lane; i < mcount; i += 32) keys_cur[i] = static_cast<std::uint32_t>(ai(persistent[i * kSceneSlotWords + 56]));
     const float friction_scale = p.friction_scale[env];
     __syncwarp();
 
@@ -671,27 +683,31 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
         if (lane == 0) misc[kSmCand] = af(max(ai(misc[kSmCand]), ncand));
         __syncwarp();
 
-        // Narrowphase + manifolds, 32 candidates at a time.
+        // Narrowphase + manifolds, 32 candidates at a time.  A pair with raw
+        // contacts always yields a manifold, so its table position is known
+        // before the manifold is built, and it is built in place.
         const float* old_table = cur_table;
         float* new_table = ws + ((sub & 1) ? kWsTable1 : kWsTable0);
         float* scratch = ws + kWsLanes + lane * kLaneScratch;
-        float* staged = scratch + (4 + kRawCap) * kRecWords + 4;
         int ncount = 0, raw_total = 0;
         bool bad = false, mover = false;
         for (int base = 0; base < ncand; base += 32) {
             const int ci = base + lane;
-            int np_ = 0, nraw = 0;
+            int nraw = 0;
             unsigned key = 0u;
+            const float* old_slot = nullptr;
+            float3 normal = f3(0.0f, 0.0f, 1.0f);
+            float3 posA = f3(0.0f, 0.0f, 0.0f), posB = posA;
+            float4 rotA = make_float4(0.0f, 0.0f, 0.0f, 1.0f), rotB = rotA;
             if (ci < ncand) {
                 const int pi = cand[ci];
                 const int a = M.pair_a[pi], b = M.pair_b[pi];
                 key = static_cast<unsigned>(a * (kSceneMaxBodies + 1) + b);
-                // Old manifold of this pair (table sorted by key).
-                const float* old_slot = nullptr;
+                // Old manifold of this pair (keys ascending).
                 int lo_i = 0, hi_i = mcount - 1;
                 while (lo_i <= hi_i) {
                     const int mid = (lo_i + hi_i) >> 1;
-                    const unsigned mk = static_cast<unsigned>(ai(old_table[mid * kSceneSlotWords + 56]));
+                    const unsigned mk = keys_cur[mid];
                     if (mk == key) { old_slot = old_table + mid * kSceneSlotWords; break; }
                     if (mk < key) lo_i = mid + 1;
                     else hi_i = mid - 1;
@@ -701,20 +717,22 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
                 load_collider(M, s, b, B);
                 const float accepted = A.offset + B.offset + (fmaxf(collider_scale(A), collider_scale(B)) + 1.0f) * kQueryPadS;
                 RawSink sink{scratch + 4 * kRecWords, 0, A.bpos, B.bpos, A.brot, B.brot};
-                float3 normal = f3(0.0f, 0.0f, 1.0f);
                 narrowphase(A, B, M.pair_class[pi], static_cast<unsigned>(a), static_cast<unsigned>(b), accepted, sink, normal);
                 nraw = sink.count;
-                np_ = build_manifold(M, old_slot, nraw, normal, scratch, staged, A.bpos, A.brot, B.bpos, B.brot);
-                if (np_ < 0) { bad = true; np_ = 0; }
+                posA = A.bpos;
+                rotA = A.brot;
+                posB = B.bpos;
+                rotB = B.brot;
             }
             raw_total += nraw;
-            const unsigned m = __ballot_sync(0xffffffffu, np_ > 0);
+            const unsigned m = __ballot_sync(0xffffffffu, nraw > 0);
             const int at = ncount + __popc(m & ((1u << lane) - 1u));
-            if (np_ > 0) {
+            if (nraw > 0) {
                 if (at < kSceneManifolds) {
                     float* dst = new_table + at * kSceneSlotWords;
-                    for (int k = 0; k < 56; ++k) dst[k] = staged[k];
+                    if (build_manifold(M, old_slot, nraw, normal, scratch, dst, posA, rotA, posB, rotB) <= 0) bad = true;
                     dst[56] = af(static_cast<int>(key));
+                    keys_next[at] = key;
                 } else {
                     mover = true;
                 }
@@ -736,6 +754,11 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
         cur_table = new_table;
         mcount = ncount;
         float* tab = new_table;
+        {
+            std::uint32_t* t = keys_cur;
+            keys_cur = keys_next;
+            keys_next = t;
+        }
         if (lane == 0) {
             misc[kSmManifolds] = af(max(ai(misc[kSmManifolds]), mcount));
             misc[kSmRaw] = af(max(ai(misc[kSmRaw]), raw_total));
@@ -744,6 +767,7 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
 
         // Contact records in manifold order (lane per manifold).
         float* C = ws + kWsContacts;
+        std::uint16_t* mfirst = reinterpret_cast<std::uint16_t*>(s + kOffFirst);
         int total = 0;
         for (int base = 0; base < mcount; base += 32) {
             const int mi = base + lane;
@@ -756,6 +780,7 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
             }
             const int first = total + incl - cnt;
             total += __shfl_sync(0xffffffffu, incl, 31);
+            if (mi < mcount) mfirst[mi] = static_cast<std::uint16_t>(min(first, kSceneContacts));
             if (cnt > 0 && first + cnt <= kSceneContacts) {
                 const float* slot = tab + mi * kSceneSlotWords;
                 const unsigned key = static_cast<unsigned>(ai(slot[56]));
@@ -814,18 +839,23 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
             __syncwarp();
             break;
         }
-        if (lane == 0) misc[kSmContacts] = af(total);
+        if (lane == 0) {
+            misc[kSmContacts] = af(total);
+            mfirst[mcount] = static_cast<std::uint16_t>(total);
+        }
         __syncwarp();
 
-        // Per-body contact lists (ascending contact index; side bit 1 = B).
+        // Per-body contact lists (ascending contact index; side bit 1 = B),
+        // walked manifold by manifold: a manifold's contacts are contiguous.
         int* start = reinterpret_cast<int*>(s + kOffLists);
         int* fill = start + kSceneMaxBodies + 1;
         std::uint16_t* entries = reinterpret_cast<std::uint16_t*>(s + kOffEntries);
         for (int b = lane; b < nb; b += 32) {
             int cnt = 0;
-            for (int c = 0; c < total; ++c) {
-                const Rec cr = rec(C, c);
-                cnt += (ai(cr[kScA]) == b) + (ai(cr[kScB]) == b);
+            for (int mi = 0; mi < mcount; ++mi) {
+                const unsigned k = keys_cur[mi];
+                if (static_cast<int>(k / (kSceneMaxBodies + 1)) == b || static_cast<int>(k % (kSceneMaxBodies + 1)) == b)
+                    cnt += mfirst[mi + 1] - mfirst[mi];
             }
             fill[b] = cnt;
         }
@@ -838,10 +868,12 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
         __syncwarp();
         for (int b = lane; b < nb; b += 32) {
             int at = start[b];
-            for (int c = 0; c < total; ++c) {
-                const Rec cr = rec(C, c);
-                if (ai(cr[kScA]) == b) entries[at++] = static_cast<std::uint16_t>(c << 1);
-                if (ai(cr[kScB]) == b) entries[at++] = static_cast<std::uint16_t>((c << 1) | 1);
+            for (int mi = 0; mi < mcount; ++mi) {
+                const unsigned k = keys_cur[mi];
+                const int side = static_cast<int>(k / (kSceneMaxBodies + 1)) == b ? 0
+                                 : (static_cast<int>(k % (kSceneMaxBodies + 1)) == b ? 1 : -1);
+                if (side < 0) continue;
+                for (int c = mfirst[mi]; c < mfirst[mi + 1]; ++c) entries[at++] = static_cast<std::uint16_t>((c << 1) | side);
             }
         }
         __syncwarp();
@@ -933,8 +965,11 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
         }
         if (!ok(misc)) break;
         // Islands: min-root union find over dynamic bodies joined by contacts.
-        if (lane == 0 && total > 0) {
-            int* parent = reinterpret_cast<int*>(s + kOffCand);  // candidates are consumed by now
+        // The solve treats all contacts of an environment together (islands
+        // do not interact in a Jacobi sweep), so islands are a diagnostic
+        // here, counted on the final substep.
+        if (lane == 0 && total > 0 && final_substep) {
+            int* parent = reinterpret_cast<int*>(keys_next);  // the previous table's keys are dead by now
             for (int b = 0; b < nb; ++b) parent[b] = b;
             auto root = [&](int x) { while (parent[x] != x) x = parent[x] = parent[parent[x]]; return x; };
             unsigned touched[2] = {0u, 0u};
@@ -1088,6 +1123,8 @@ size_t scene_step_smem_bytes() { return static_cast<size_t>(kSceneSmemWords) * s
 size_t scene_workspace_words() { return static_cast<size_t>(kWsWords); }
 
 cudaError_t configure_scene_step_kernel() {
+    // The driver's default carveout keeps most of the unified L1 as cache,
+    // which the narrowphase scratch and contact records rely on.
     return cudaFuncSetAttribute(scene_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(scene_step_smem_bytes()));
 }
