@@ -294,6 +294,192 @@ def run_serving(args) -> None:
     print(json.dumps(line))
 
 
+PILE_SEED = 60            # a 36-body pile (the mean pile of the heterogeneous mix)
+PILE_BODIES = 36
+# Heterogeneous mix: pile worlds whose body counts span 8-64 (mean 36.4).
+MIX_PILE_SEEDS = (10, 13, 6, 9, 8, 1, 16, 31)
+
+
+def _pile_cpu_port_sample(records, q0: np.ndarray, v0: np.ndarray, friction: float, steps: int) -> dict:
+    """The oracle (FP64 C restatement, one core) on a bounded sample of one
+    pile environment: `steps` control steps from a settled state."""
+
+    from oracle import SceneOracle, SceneTable
+
+    oracle = SceneOracle(records, CONTROL_DT / SUBSTEPS, SUBSTEPS, ITERATIONS, 0)
+    q = q0.astype(np.float64)
+    v = v0.astype(np.float64)
+    table = SceneTable()
+    for _ in range(60):  # settle (untimed)
+        oracle.step(q, v, table, friction)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        oracle.step(q, v, table, friction)
+    secs = time.perf_counter() - t0
+    return {"value": steps / secs, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"1 env x {steps} control steps of the {records.world.body_count - 1}-body pile after a 60-step settle, "
+                      "oracle/oracle.c (FP64, scalar)"}
+
+
+def _timed_advances(worlds, args, horizon: int, device, streams=None, episodic=()):
+    """Warm-up then `args.steps` timed advances of every world (each on its
+    own stream when given); CUDA events on the default stream bracket each
+    step after a join of all streams; L2 flushed before each step.  Worlds
+    listed in `episodic` reset every environment on the first control step
+    of each advance (episodes of `horizon` control steps)."""
+
+    import torch
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, device=device, dtype=torch.float32)
+    acts = [torch.zeros((horizon, w.envs, w.action_count), device=device) if w.action_count == 0 else
+            0.3 * torch.randn((horizon, w.envs, w.action_count), device=device, generator=torch.Generator(device=device).manual_seed(SEED))
+            for w in worlds]
+    status = [torch.empty((horizon, w.envs), device=device, dtype=torch.int32) for w in worlds]
+    obs = [torch.empty((horizon, w.envs, w.observation_count), device=device) for w in worlds]
+    masks = []
+    for i, w in enumerate(worlds):
+        if i in episodic:
+            m = torch.zeros((horizon, w.envs), device=device, dtype=torch.int32)
+            m[0] = 1
+            masks.append(m)
+        else:
+            masks.append(None)
+    main = torch.cuda.current_stream(device)
+    streams = streams or [main] * len(worlds)
+
+    def one_step():
+        for w, a, st, ob, sm, mk in zip(worlds, acts, status, obs, streams, masks):
+            sm.wait_stream(main)
+            with torch.cuda.stream(sm):
+                w.step(a, reset_mask=mk, observations=ob, status=st)
+        for sm in streams:
+            main.wait_stream(sm)
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize(device)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with ClockSampler(device.index if device.index is not None else 0) as clocks:
+        for i in range(args.steps):
+            flush.fill_(float(i))
+            starts[i].record(main)
+            one_step()
+            stops[i].record(main)
+        torch.cuda.synchronize(device)
+    failures = [int((st != 0).sum().item()) for st in status]
+    ms = float(sum(a.elapsed_time(b) for a, b in zip(starts, stops)))
+    return ms, failures, clocks.summary()
+
+
+def run_pile(args) -> None:
+    """Free-body piles: 16,384 environments of a 36-body pile of boxes and
+    spheres on a plane (settled), 4 x 5 ms substeps, 8 iterations."""
+
+    import torch
+
+    import numi_lab_b200 as nb
+
+    torch.cuda.set_device(0)
+    device = torch.device("cuda", 0)
+    envs, horizon = 16384, 25
+    with nb.World("pile", envs, substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT, seed=PILE_SEED) as world:
+        assert world.scene_bodies == PILE_BODIES
+        settle = torch.zeros((100, envs, 0), device=device)
+        world.step(settle, wait=True)  # drop and settle (2 s), untimed
+        ms, failures, clock_summary = _timed_advances([world], args, horizon, device)
+        q_, v_, tab = world.state()
+        counts = tab[:, :, 7].view(np.uint32)
+        live = counts.astype(np.int64)
+        mean_points = float(live.sum(axis=1).mean())
+        mean_manifolds = float((live > 0).sum(axis=1).mean())
+        cpu = None
+        if not args.no_cpu_baseline:
+            rq, rv, rf = nb.sample_reset("pile", PILE_SEED, PILE_SEED, 0, 1)
+            cpu = _pile_cpu_port_sample(world.model(), rq[0], rv[0], float(rf[0]), 40)
+    value = envs * horizon * args.steps / (ms / 1e3)
+    line = {
+        "metric": "pile env-steps/s",
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": f"free-body piles: {envs} envs x {PILE_BODIES} boxes/spheres (size U(0.05, 0.3) m, density 500-2000) "
+                               "settled on a plane, 20 ms control = 4 x 5 ms substeps, 8 temporalCone iterations, "
+                               f"{horizon} control steps per bench step", "l2": "flushed (256 MiB write) between steps"},
+        "cpu_baseline": cpu,
+        "gpu_launches": horizon * args.steps,
+        "clocks": {k: clock_summary[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        "failed_env_steps": sum(failures),
+        "mean_active_contacts": mean_points,
+        "mean_manifolds": mean_manifolds,
+    }
+    print(json.dumps(line))
+
+
+def run_mix(args) -> None:
+    """Heterogeneous mix: 16,384 environments, 40 % 7-link chains (one 5 ms
+    step per control step), 30 % 29-DoF trees and 30 % piles of 8-64 bodies
+    (eight pile worlds), every world on its own stream."""
+
+    import torch
+
+    import numi_lab_b200 as nb
+
+    torch.cuda.set_device(0)
+    device = torch.device("cuda", 0)
+    total, horizon = 16384, 25
+    n_chain = int(0.4 * total)
+    n_tree = int(0.3 * total)
+    n_pile = total - n_chain - n_tree
+    worlds = [nb.World("chain7", n_chain, substeps=1, control_dt=0.005, seed=SEED),
+              nb.World("tree29", n_tree, substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT, seed=SEED)]
+    per = [n_pile // len(MIX_PILE_SEEDS) + (1 if i < n_pile % len(MIX_PILE_SEEDS) else 0) for i in range(len(MIX_PILE_SEEDS))]
+    for seed, n in zip(MIX_PILE_SEEDS, per):
+        worlds.append(nb.World("pile", n, substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT, seed=seed))
+    try:
+        for w in worlds[2:]:
+            w.step(torch.zeros((100, w.envs, 0), device=device), wait=True)  # settle piles
+        streams = [torch.cuda.Stream(device) for _ in worlds]
+        ms, failures, clock_summary = _timed_advances(worlds, args, horizon, device, streams, episodic=(0,))
+        bodies = [w.scene_bodies for w in worlds[2:]]
+    finally:
+        for w in worlds:
+            w.close()
+    value = total * horizon * args.steps / (ms / 1e3)
+    line = {
+        "metric": "heterogeneous env-steps/s",
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": f"{total} envs: {n_chain} chain7 (5 ms steps, tau ~ N(0, 0.3), episodes of {horizon} steps), "
+                               f"{n_tree} tree29 (PD targets ~ N(0, 0.3)), "
+                               f"{n_pile} settled piles of {bodies} bodies (mean {float(np.mean(bodies)):.1f}); "
+                               f"{horizon} control steps per bench step; one stream per world",
+                   "l2": "flushed (256 MiB write) between steps"},
+        "gpu_launches": horizon * args.steps * len(worlds),
+        "clocks": {k: clock_summary[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        "failed_env_steps": sum(failures),
+        "failed_env_steps_by_world": dict(zip(["chain7", "tree29"] + [f"pile{b}" for b in bodies], failures)),
+    }
+    print(json.dumps(line))
+
+
 def main() -> None:
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
@@ -301,6 +487,8 @@ def main() -> None:
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", default="native", choices=["native", "reference"])
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--workload", default="tree29", choices=["tree29", "pile", "mix"],
+                        help="tree29 (the headline), pile (36-body piles) or mix (chains, trees and piles)")
     parser.add_argument("--serve", action="store_true",
                         help="serving workload: Poisson request stream, latency percentiles (one JSON line)")
     args = parser.parse_args()
@@ -317,6 +505,10 @@ def main() -> None:
     if args.serve:
         if rank == 0:
             run_serving(args)
+        return
+    if args.workload != "tree29":
+        if rank == 0:
+            (run_pile if args.workload == "pile" else run_mix)(args)
         return
 
     import torch
