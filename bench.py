@@ -222,7 +222,7 @@ def run_reference_arm(args, rank: int) -> None:
 
 
 def plain_aba_chain7(device) -> dict:
-    """BASELINE's plain-ABA configuration: 1024 envs of the 7-revolute chain,
+    """The plain-ABA configuration: 1024 envs of the 7-revolute chain,
     tau ~ N(0, 5), dt = 5 ms, 1000 steps (one advance), device-resident."""
 
     import torch
@@ -258,8 +258,8 @@ def plain_aba_chain7(device) -> dict:
 
 
 def run_serving(args) -> None:
-    """Poisson request stream (BASELINE's serving configuration, chain and
-    tree worlds) against the continuous-batching server; latency percentiles
+    """Poisson request stream (the serving configuration: chain, tree and
+    pile worlds) against the continuous-batching server; latency percentiles
     at the configured rate plus a sustainable-rate sweep."""
 
     import torch
@@ -283,7 +283,7 @@ def run_serving(args) -> None:
         "queue_p50_s": head["queue_p50_s"],
         "queue_p99_s": head["queue_p99_s"],
         "higher_is_better": True,
-        "config": {"workload": "Poisson arrivals 2000 req/s for 1 s, worlds chain7 | tree29, envs log-uniform 1-512, "
+        "config": {"workload": "Poisson arrivals 2000 req/s for 1 s, worlds chain7 | tree29 | pile, envs log-uniform 1-512, "
                                "horizon U(10, 500), actions N(0, 0.3), 120 GB HBM budget, drained",
                    "rate_sweep_req_per_s": {k: {kk: v[kk] for kk in ("env_steps_per_s", "latency_p50_s", "latency_p99_s",
                                                                        "queue_p99_s", "completed")}

@@ -289,7 +289,7 @@ void numi::rt::make_plan(const numi::CompiledModel& m, float h, KernelPlan& plan
     }
 }
 
-numi::SceneModel pack_scene(const numi::CompiledModel& m, float h) {
+numi::SceneModel numi::rt::pack_scene(const numi::CompiledModel& m, float h) {
     numi::SceneModel d{};
     const std::uint32_t n = m.scene_bodies;
     if (m.pairs.size() > static_cast<size_t>(numi::kSceneMaxPairs)) throw std::runtime_error("scene pair count outside capacity");
@@ -619,7 +619,7 @@ MR_API MRTaskRolloutHandle* mr_create_task_rollout(const MRRunManifestC* manifes
         if (m.scene) {
             h.scene = true;
             h.contact = true;
-            h.smodel = pack_scene(m, h.h);
+            h.smodel = numi::rt::pack_scene(m, h.h);
             check(numi::configure_scene_step_kernel(), "scene kernel attributes");
         } else {
             numi::rt::KernelPlan plan;

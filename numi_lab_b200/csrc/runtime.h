@@ -7,6 +7,7 @@
 #include "device_model.h"
 #include "layout.h"
 #include "model.h"
+#include "scene.h"
 
 #include <cuda_runtime.h>
 
@@ -96,6 +97,8 @@ struct KernelPlan {
 DeviceModel pack_model(const CompiledModel& m, float h);
 // Builds the plan for the current device; throws when the model does not fit.
 void make_plan(const CompiledModel& m, float h, KernelPlan& plan);
+// Packs a pile (scene) world for the free-body kernel at substep length h.
+SceneModel pack_scene(const CompiledModel& m, float h);
 
 }  // namespace rt
 }  // namespace numi

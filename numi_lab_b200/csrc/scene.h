@@ -53,22 +53,27 @@ struct alignas(16) SceneModel {
     std::uint8_t pair_class[kSceneMaxPairs];
 };
 
+// Environments ("slots") hold resident state; a launch processes work
+// items, item i advancing slot env_index[i] (or slot i when env_index is
+// null).  Per-item arrays: reset masks, observations, status codes, active
+// contacts.  Per-slot arrays: everything else.
 struct SceneParams {
     const SceneModel* model;
-    float* q;                  // [env][nb][7]: position, orientation xyzw
-    float* v;                  // [env][nb][6]: linear, angular velocity (world)
-    float* manifolds;          // [env][kSceneManifolds][kSceneSlotWords]
-    std::uint32_t* manifold_count;  // [env]
-    const float* reset_q;
+    float* q;                  // [slot][nb][7]: position, orientation xyzw
+    float* v;                  // [slot][nb][6]: linear, angular velocity (world)
+    float* manifolds;          // [slot][kSceneManifolds][kSceneSlotWords]
+    std::uint32_t* manifold_count;  // [slot]
+    const float* reset_q;      // [slot]
     const float* reset_v;
-    const float* friction_scale;    // [env]
-    const std::uint32_t* reset_masks;  // [env] of this control step, or null
-    float* observations;       // [env][nq + nv] of this control step, or null
-    std::uint32_t* status_codes;
-    std::uint32_t* active_contacts;
+    const float* friction_scale;    // [slot]
+    const std::int32_t* env_index;  // [item] -> slot, or null
+    const std::uint32_t* reset_masks;  // [item] of this control step, or null
+    float* observations;       // [item][nq + nv] of this control step, or null
+    std::uint32_t* status_codes;     // [item]
+    std::uint32_t* active_contacts;  // [item]
     std::uint32_t* stats;
-    float* workspace;          // [env][scene_workspace_words()]: substep tables, contacts, narrowphase scratch
-    std::int32_t env_count;
+    float* workspace;          // [slot][scene_workspace_words()]: substep tables, contacts, narrowphase scratch
+    std::int32_t env_count;    // items in this launch
     std::int32_t substeps;
     std::int32_t velocity_iterations;
     std::int32_t final_velocity_iterations;

@@ -554,8 +554,9 @@ __device__ __forceinline__ float3 sym3_mul(const float* S, float3 x) {
 __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
     extern __shared__ float4 smem4[];
     float* s = reinterpret_cast<float*>(smem4);
-    const int env = blockIdx.x;
-    if (env >= p.env_count) return;
+    const int item = blockIdx.x;
+    if (item >= p.env_count) return;
+    const int env = p.env_index != nullptr ? p.env_index[item] : item;
     const int lane = threadIdx.x;
     const SceneModel& M = *p.model;
     const int nb = M.nb;
@@ -563,7 +564,7 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
     float* misc = s + kOffMisc;
     const float h = M.h;
     if (lane < 32) misc[lane] = 0.0f;
-    const bool reset = p.reset_masks != nullptr && p.reset_masks[env] != 0u;
+    const bool reset = p.reset_masks != nullptr && p.reset_masks[item] != 0u;
     const float* srcq = (reset ? p.reset_q : p.q) + static_cast<size_t>(env) * nq;
     const float* srcv = (reset ? p.reset_v : p.v) + static_cast<size_t>(env) * nv;
     for (int b = lane; b < nb; b += 32) {
@@ -1072,7 +1073,7 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
     const bool success = code == MR_STEP_SUCCESS;
     float* qd = p.q + static_cast<size_t>(env) * nq;
     float* vd = p.v + static_cast<size_t>(env) * nv;
-    float* obs = p.observations ? p.observations + static_cast<size_t>(env) * (nq + nv) : nullptr;
+    float* obs = p.observations ? p.observations + static_cast<size_t>(item) * (nq + nv) : nullptr;
     if (success) {
         for (int b = lane; b < nb; b += 32) {
             st3(qd + b * 7, ld3(s + kOffPos + b * 3));
@@ -1102,8 +1103,8 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
     }
     if (lane == 0) {
         const unsigned contacts = static_cast<unsigned>(ai(misc[kSmContacts]));
-        if (p.status_codes) p.status_codes[env] = code;
-        if (p.active_contacts) p.active_contacts[env] = success ? contacts : 0u;
+        if (p.status_codes) p.status_codes[item] = code;
+        if (p.active_contacts) p.active_contacts[item] = success ? contacts : 0u;
         if (!success) {
             atomicAdd(p.stats + 0, 1u);
             atomicMin(p.stats + 6, static_cast<unsigned>(env));

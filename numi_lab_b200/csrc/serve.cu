@@ -1,7 +1,7 @@
 // Continuous-batching rollout server behind the C ABI (include/numi_b200.h,
 // mr_create_server ... mr_server_release).
 //
-// Each world source (7-DoF chain, 29-DoF tree) owns a pool of resident
+// Each world source (7-DoF chain, 29-DoF tree, pile) owns a pool of resident
 // environment slots on the device: state, manifolds and friction live there
 // for the whole life of a request.  Requests queue on submit; every tick
 // admits waiting requests into free slots (first-come first-served with
@@ -53,6 +53,8 @@ __global__ void gather_rows_kernel(float* __restrict__ dst, const float* __restr
 
 int grid_for(int total) { return std::max(1, std::min(1184, (total + 255) / 256)); }
 
+constexpr std::size_t kPoolCount = 3;  // chain, tree, pile
+
 double now_seconds() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
@@ -79,11 +81,15 @@ struct Pool {
     std::uint32_t source = 0;
     numi::CompiledModel model;
     numi::rt::KernelPlan plan;
+    bool scene = false;              // pile world: free-body kernel
+    numi::SceneModel smodel{};
     std::uint32_t capacity = 0;
-    std::uint32_t nq = 0, nv = 0, na = 0, manifold_words = 0;
+    std::uint32_t nq = 0, nv = 0, na = 0, manifold_words = 0, workspace_words = 0;
     cudaStream_t stream = nullptr;
     DeviceBuffer<numi::DeviceModel> d_model;
-    DeviceBuffer<float> d_q, d_v, d_manifolds, d_friction;
+    DeviceBuffer<numi::SceneModel> d_smodel;
+    DeviceBuffer<float> d_q, d_v, d_manifolds, d_friction, d_workspace;
+    DeviceBuffer<std::uint32_t> d_mcount;  // live manifolds per slot (piles)
     DeviceBuffer<std::int32_t> d_index;
     DeviceBuffer<const float*> d_rows;
     DeviceBuffer<std::uint32_t> d_status, d_stats;
@@ -94,7 +100,9 @@ struct Pool {
     std::vector<Request*> active;          // admission order
     std::uint32_t launched_items = 0;      // of the current tick
 
-    std::size_t slot_bytes() const { return (static_cast<std::size_t>(nq) + nv + manifold_words + 1) * sizeof(float); }
+    std::size_t slot_bytes() const {
+        return (static_cast<std::size_t>(nq) + nv + manifold_words + workspace_words + 1 + (scene ? 1 : 0)) * sizeof(float);
+    }
     ~Pool() {
         if (stream) cudaStreamDestroy(stream);
     }
@@ -123,26 +131,44 @@ struct MRServerHandle {
     void add_pool(std::uint32_t source) {
         auto p = std::make_unique<Pool>();
         p->source = source;
-        p->model = source == MR_RUN_SOURCE_SYNTHETIC_CHAIN7 ? numi::build_chain7(config.model_seed)
-                                                              : numi::build_tree29(config.model_seed);
-        numi::rt::make_plan(p->model, h, p->plan);
+        p->model = source == MR_RUN_SOURCE_SYNTHETIC_CHAIN7   ? numi::build_chain7(config.model_seed)
+                   : source == MR_RUN_SOURCE_SYNTHETIC_TREE29 ? numi::build_tree29(config.model_seed)
+                                                              : numi::build_pile(config.model_seed);
+        p->scene = p->model.scene;
         p->nq = p->model.world.nq;
         p->nv = p->model.world.nv;
         p->na = p->model.world.action_count;
-        p->manifold_words = p->model.world.pair_count * numi::kManifoldWords;
+        if (p->scene) {
+            p->smodel = numi::rt::pack_scene(p->model, h);
+            check(numi::configure_scene_step_kernel(), "scene kernel attributes");
+            p->manifold_words = static_cast<std::uint32_t>(numi::kSceneManifolds * numi::kSceneSlotWords);
+            p->workspace_words = static_cast<std::uint32_t>(numi::scene_workspace_words());
+        } else {
+            numi::rt::make_plan(p->model, h, p->plan);
+            p->manifold_words = p->model.world.pair_count * numi::kManifoldWords;
+        }
         // Slots: the configured maximum, bounded by this pool's share of the
-        // HBM budget (half of it split across pools; the rest holds actions).
-        const std::size_t share = config.hbm_budget_bytes / (2 * 2);
+        // HBM budget (half of it split across the pools; the rest holds actions).
+        const std::size_t share = config.hbm_budget_bytes / (2 * kPoolCount);
         p->capacity = static_cast<std::uint32_t>(std::min<std::size_t>(config.max_envs_per_source, share / p->slot_bytes()));
         if (p->capacity == 0) throw std::invalid_argument("the HBM budget holds no environment of source " + std::to_string(source));
         budget_used += static_cast<std::size_t>(p->capacity) * p->slot_bytes();
         check(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking), "stream");
-        p->d_model.resize(1);
-        check(cudaMemcpy(p->d_model.ptr, &p->plan.dmodel, sizeof(numi::DeviceModel), cudaMemcpyHostToDevice), "upload model");
+        if (p->scene) {
+            p->d_smodel.resize(1);
+            check(cudaMemcpy(p->d_smodel.ptr, &p->smodel, sizeof(numi::SceneModel), cudaMemcpyHostToDevice), "upload scene model");
+        } else {
+            p->d_model.resize(1);
+            check(cudaMemcpy(p->d_model.ptr, &p->plan.dmodel, sizeof(numi::DeviceModel), cudaMemcpyHostToDevice), "upload model");
+        }
         const std::size_t cap = p->capacity;
         p->d_q.resize(cap * p->nq);
         p->d_v.resize(cap * p->nv);
         if (p->manifold_words) p->d_manifolds.resize(cap * p->manifold_words);
+        if (p->scene) {
+            p->d_mcount.resize(cap);
+            p->d_workspace.resize(cap * p->workspace_words);
+        }
         p->d_friction.resize(cap);
         p->d_index.resize(cap);
         p->d_rows.resize(cap);
@@ -191,6 +217,9 @@ struct MRServerHandle {
         if (p.manifold_words)
             scatter_rows_kernel<<<grid_for(envs * p.manifold_words), 256, 0, p.stream>>>(p.d_manifolds.ptr, nullptr, r.d_slots.ptr,
                                                                                          envs, p.manifold_words);
+        if (p.scene)  // no live manifolds (zero words are a zero count)
+            scatter_rows_kernel<<<grid_for(envs), 256, 0, p.stream>>>(reinterpret_cast<float*>(p.d_mcount.ptr), nullptr,
+                                                                      r.d_slots.ptr, envs, 1);
         check(cudaGetLastError(), "admission scatter");
         check(cudaStreamSynchronize(p.stream), "admission");
         r.t_admit = now_seconds();
@@ -213,6 +242,26 @@ struct MRServerHandle {
         check(cudaMemcpyAsync(p.d_index.ptr, p.h_index.ptr, n * sizeof(std::int32_t), cudaMemcpyHostToDevice, p.stream), "index H2D");
         check(cudaMemcpyAsync(p.d_rows.ptr, p.h_rows.ptr, n * sizeof(const float*), cudaMemcpyHostToDevice, p.stream), "rows H2D");
         check(cudaMemsetAsync(p.d_stats.ptr, 0, numi::kStatCount * sizeof(std::uint32_t), p.stream), "clear stats");
+        if (p.scene) {
+            numi::SceneParams sp{};
+            sp.model = p.d_smodel.ptr;
+            sp.q = p.d_q.ptr;
+            sp.v = p.d_v.ptr;
+            sp.manifolds = p.d_manifolds.ptr;
+            sp.manifold_count = p.d_mcount.ptr;
+            sp.reset_q = p.d_q.ptr;  // no resets inside a request
+            sp.reset_v = p.d_v.ptr;
+            sp.friction_scale = p.d_friction.ptr;
+            sp.env_index = p.d_index.ptr;
+            sp.status_codes = p.d_status.ptr;
+            sp.stats = p.d_stats.ptr;
+            sp.workspace = p.d_workspace.ptr;
+            sp.env_count = static_cast<int>(n);
+            sp.substeps = static_cast<int>(config.physics_substeps);
+            sp.velocity_iterations = static_cast<int>(config.velocity_iterations);
+            sp.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
+            check(numi::launch_scene_step(sp, p.stream), "scene step launch");
+        } else {
         numi::StepParams sp{};
         sp.model = p.d_model.ptr;
         sp.q = p.d_q.ptr;
@@ -232,6 +281,7 @@ struct MRServerHandle {
         sp.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
         check(numi::launch_control_step(sp, p.plan.layout, p.plan.contact, false, p.plan.warps_per_block[0], p.stream),
               "control step launch");
+        }
         check(cudaMemcpyAsync(p.h_status.ptr, p.d_status.ptr, n * sizeof(std::uint32_t), cudaMemcpyDeviceToHost, p.stream),
               "status D2H");
         p.launched_items = n;
@@ -305,6 +355,7 @@ MR_API MRServerHandle* mr_create_server(const MRServerConfigC* config) {
         server->h = config->control_timestep_seconds / static_cast<float>(config->physics_substeps);
         server->add_pool(MR_RUN_SOURCE_SYNTHETIC_CHAIN7);
         server->add_pool(MR_RUN_SOURCE_SYNTHETIC_TREE29);
+        server->add_pool(MR_RUN_SOURCE_SYNTHETIC_PILE);
         if (server->budget_used > config->hbm_budget_bytes) throw std::invalid_argument("HBM budget exhausted by the slot pools");
     });
     if (rc != 0) return nullptr;

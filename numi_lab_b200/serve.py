@@ -23,7 +23,8 @@ import numpy as np
 from . import native
 from .native import MetalRoboError
 
-SOURCES = {"chain7": native.MR_RUN_SOURCE_SYNTHETIC_CHAIN7, "tree29": native.MR_RUN_SOURCE_SYNTHETIC_TREE29}
+SOURCES = {"chain7": native.MR_RUN_SOURCE_SYNTHETIC_CHAIN7, "tree29": native.MR_RUN_SOURCE_SYNTHETIC_TREE29,
+           "pile": native.MR_RUN_SOURCE_SYNTHETIC_PILE}
 
 
 @dataclass
@@ -63,11 +64,16 @@ class Server:
         if not handle:
             raise MetalRoboError(f"mr_create_server: {self._lib.last_error()}")
         self._handle = ct.c_void_p(handle)
+        from .world import compile_model
+
         self.shapes = {}
+        self.state_dims = {}
         for name, sid in SOURCES.items():
             slots, na = ct.c_uint32(), ct.c_uint32()
             self._lib.check(self._lib.lib.mr_server_capacity(self._handle, sid, ct.byref(slots), ct.byref(na)), "capacity")
             self.shapes[sid] = (int(slots.value), int(na.value))
+            w = compile_model(sid, model_seed, library=self._lib).world
+            self.state_dims[sid] = (int(w.nq), int(w.nv))
         self._dims = {}
 
     def close(self) -> None:
@@ -118,7 +124,7 @@ class Server:
 
     def result(self, request_id: int, *, release: bool = True) -> tuple[np.ndarray, np.ndarray]:
         sid, envs = self._dims[request_id]
-        nq, nv = (7, 7) if sid == native.MR_RUN_SOURCE_SYNTHETIC_CHAIN7 else (36, 35)
+        nq, nv = self.state_dims[sid]
         q = np.zeros((envs, nq), np.float32)
         v = np.zeros((envs, nv), np.float32)
         self._lib.check(self._lib.lib.mr_server_copy_result(
@@ -136,7 +142,7 @@ class Server:
 
 
 def poisson_requests(rate_hz: float, window_s: float, seed: int, *, max_envs: int = 512, horizon: tuple[int, int] = (10, 500),
-                     sources: tuple[str, ...] = ("chain7", "tree29")) -> list[dict]:
+                     sources: tuple[str, ...] = ("chain7", "tree29", "pile")) -> list[dict]:
     """Seeded Poisson request stream: arrival time, world, env count
     (log-uniform 1..max_envs), horizon U(lo, hi), seed; actions are drawn
     N(0, 0.3) at submission (``request_actions``)."""

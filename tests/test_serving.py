@@ -15,7 +15,8 @@ def test_poisson_stream_is_seeded_and_bounded():
     b = poisson_requests(200.0, 1.0, seed=3)
     assert a == b and len(a) > 100
     assert all(1 <= r["env_count"] <= 512 and 10 <= r["horizon"] <= 500 for r in a)
-    assert all(r["source"] in ("chain7", "tree29") for r in a)
+    assert all(r["source"] in ("chain7", "tree29", "pile") for r in a)
+    assert {r["source"] for r in a} == {"chain7", "tree29", "pile"}
     arrivals = [r["arrival"] for r in a]
     assert arrivals == sorted(arrivals) and arrivals[-1] < 1.0
 
@@ -78,4 +79,32 @@ def test_admission_waits_for_free_slots(cuda_device):
         assert done[second].queue_seconds > done[first].queue_seconds
         for rid in (first, second):
             server.result(rid)
-        assert server.stats().free_slots == 8 + server.shapes[nb.native.MR_RUN_SOURCE_SYNTHETIC_TREE29][0]
+        assert server.stats().free_slots == (8 + server.shapes[nb.native.MR_RUN_SOURCE_SYNTHETIC_TREE29][0]
+                                             + server.shapes[nb.native.MR_RUN_SOURCE_SYNTHETIC_PILE][0])
+
+
+@pytest.mark.gpu
+def test_pile_request_matches_a_rollout_alone_and_in_a_mix(cuda_device):
+    import torch
+
+    seed, envs, horizon = 10, 3, 30  # an 8-body pile, dropped onto the plane
+    with nb.Server(model_seed=seed, max_envs_per_source=64) as server:
+        assert server.action_count("pile") == 0
+        rid = server.submit("pile", envs, horizon, seed, np.zeros((horizon, envs, 0), np.float32))
+        _run_until_done(server, [rid])
+        q_alone, v_alone = server.result(rid)
+    with nb.Server(model_seed=seed, max_envs_per_source=64) as server:
+        other = [server.submit("pile", 5, 7, 77, np.zeros((7, 5, 0), np.float32)),
+                 server.submit("chain7", 4, 9, 78, np.zeros((9, 4, server.action_count("chain7")), np.float32))]
+        server.tick()
+        rid = server.submit("pile", envs, horizon, seed, np.zeros((horizon, envs, 0), np.float32))
+        done = _run_until_done(server, other + [rid])
+        assert done[rid].failed_env_steps == 0
+        q_mix, v_mix = server.result(rid)
+    np.testing.assert_array_equal(q_mix, q_alone)
+    np.testing.assert_array_equal(v_mix, v_alone)
+    with nb.World("pile", envs, substeps=4, velocity_iterations=8, control_dt=0.02, seed=seed) as world:
+        world.step(torch.zeros((horizon, envs, 0), device="cuda"), wait=True)
+        q_w, v_w, _ = world.state()
+    np.testing.assert_array_equal(q_w, q_alone)
+    np.testing.assert_array_equal(v_w, v_alone)
