@@ -528,7 +528,8 @@ MR_API int mr_task_rollout_set_state(
  * resident environment slots as slots and the HBM budget allow, packed with
  * the requests already running into one control-step launch per world per
  * tick, and retired when their horizon completes.  An environment's result
- * depends only on its request (world, seed, env index, actions). */
+ * depends only on its request (world, seed, env index, actions).  Worlds:
+ * MR_RUN_SOURCE_SYNTHETIC_CHAIN7, _TREE29 and _PILE (no actions). */
 typedef struct MRServerHandle MRServerHandle;
 
 typedef struct MRServerConfigC {
