@@ -382,7 +382,7 @@ def run_pile(args) -> None:
 
     torch.cuda.set_device(0)
     device = torch.device("cuda", 0)
-    envs, horizon = 16384, 25
+    envs, horizon = args.envs or 16384, 25
     with nb.World("pile", envs, substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT, seed=PILE_SEED) as world:
         assert world.scene_bodies == PILE_BODIES
         settle = torch.zeros((100, envs, 0), device=device)
@@ -487,6 +487,7 @@ def main() -> None:
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", default="native", choices=["native", "reference"])
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--envs", type=int, default=0, help="pile workload: environments (default 16384; smaller for profiling)")
     parser.add_argument("--workload", default="tree29", choices=["tree29", "pile", "mix"],
                         help="tree29 (the headline), pile (36-body piles) or mix (chains, trees and piles)")
     parser.add_argument("--serve", action="store_true",
