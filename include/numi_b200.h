@@ -170,7 +170,11 @@ enum MRRunManifestSourceC {
     MR_RUN_SOURCE_SYNTHETIC_TREE29 = 101u,
     /* Pile of 8-64 free spheres and boxes dropped onto a ground plane (body
      * count drawn from the seed); scene bodies, no actuation. */
-    MR_RUN_SOURCE_SYNTHETIC_PILE = 102u
+    MR_RUN_SOURCE_SYNTHETIC_PILE = 102u,
+    /* Stack of 32 0.1 m, 1 kg boxes (friction 0.6) resting on a ground
+     * plane, the stack yawed U(0, 2 pi) and each box offset N(0, 2 mm) at
+     * reset; scene bodies, no actuation. */
+    MR_RUN_SOURCE_SYNTHETIC_STACK = 103u
 };
 
 /* reference: include/metalrobo/c_api.h:171-190 (same shape). */

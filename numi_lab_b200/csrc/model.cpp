@@ -474,6 +474,71 @@ CompiledModel build_tree29(std::uint64_t seed) {
     return m;
 }
 
+// Ground body with the plane collider, materials, the all-pairs list in key
+// order (a, b), b = n for the plane, and the world record of a scene with
+// `n` free bodies already in m.bodies / m.shapes.
+static void finish_scene(CompiledModel& m, std::uint32_t n, double friction) {
+    MRModelBodyC ground{};
+    ground.parent_body = MR_INVALID_INDEX;
+    ground.inbound_joint = MR_INVALID_INDEX;
+    ground.motion_type = MR_MOTION_STATIC;
+    set4(ground.static_pose + 4, 0.0, 0.0, 0.0, 1.0);
+    m.bodies.push_back(ground);
+    {
+        MRModelShapeC plane{};
+        plane.body = n;
+        plane.shape_type = MR_SHAPE_PLANE;
+        plane.material = 1;
+        plane.collision_group = 2u;
+        plane.collision_mask = 1u;
+        const double h = std::sqrt(0.5);
+        set4(plane.local_rotation, h, 0.0, 0.0, h);  // local +Y -> world +Z
+        m.shapes.push_back(plane);
+    }
+    MRModelMaterialC mat{};
+    set4(mat.friction, friction, friction, 0.0, 0.0);
+    set4(mat.response, 0.0, 0.5, 0.0, 0.0);
+    m.materials.push_back(mat);
+    m.materials.push_back(mat);
+    auto cls = [&](std::uint32_t a, std::uint32_t b) {
+        const std::uint32_t ta = m.shapes[a].shape_type, tb = m.shapes[b].shape_type;
+        if (tb == MR_SHAPE_PLANE) return ta == MR_SHAPE_BOX ? MR_COLLISION_PAIR_BOX_PLANE : MR_COLLISION_PAIR_SPHERE_PLANE;
+        if (ta == MR_SHAPE_SPHERE && tb == MR_SHAPE_SPHERE) return MR_COLLISION_PAIR_SPHERE_SPHERE;
+        if (ta == MR_SHAPE_BOX && tb == MR_SHAPE_BOX) return MR_COLLISION_PAIR_BOX_BOX;
+        return MR_COLLISION_PAIR_SPHERE_BOX;
+    };
+    // Compiled pairs in key order (a, b), b = n for the plane.
+    for (std::uint32_t a = 0; a < n; ++a) {
+        for (std::uint32_t b = a + 1; b < n; ++b) {
+            MRModelPairC pr{a, b, static_cast<std::uint32_t>(cls(a, b)), 4u};
+            m.pairs.push_back(pr);
+        }
+        MRModelPairC pr{a, n, static_cast<std::uint32_t>(cls(a, n)), 4u};
+        m.pairs.push_back(pr);
+    }
+    m.world.body_count = n + 1;
+    m.world.joint_count = 0;
+    m.world.nq = 7 * n;
+    m.world.nv = 6 * n;
+    m.world.shape_count = n + 1;
+    m.world.material_count = 2;
+    m.world.pair_count = static_cast<std::uint32_t>(m.pairs.size());
+    m.world.root_type = MR_ROOT_FIXED;
+    m.world.actuation_mode = MR_ACTUATION_EFFORT;
+    m.world.action_count = 0;
+    m.world.contact_capacity = 256;
+    m.world.apply_body_damping = 1u;
+    set4(m.world.gravity, 0.0, 0.0, -9.81, 0.0);
+    set4(m.world.solver_scales, 1.0e-7, 1.0e-9, 2.0, 1.0e-4);
+    set4(m.world.manifold_thresholds, 0.02, 0.02, 0.002, 0.95);
+    set4(m.world.speculative, 1.0, 1.0e4, 0.0, 0.0);
+    m.nominal_q.assign(m.world.nq, 0.0f);
+    m.friction_scale_lo = 1.0f;
+    m.friction_scale_hi = 1.0f;
+    m.finalize();
+}
+
+
 CompiledModel build_pile(std::uint64_t seed, std::uint32_t count) {
     CompiledModel m;
     m.name = "synthetic_pile";
@@ -533,71 +598,78 @@ CompiledModel build_pile(std::uint64_t seed, std::uint32_t count) {
         set4(s.contact_rest_bound, 0.002, 0.0, bound, 0.0);
         m.shapes.push_back(s);
     }
-    MRModelBodyC ground{};
-    ground.parent_body = MR_INVALID_INDEX;
-    ground.inbound_joint = MR_INVALID_INDEX;
-    ground.motion_type = MR_MOTION_STATIC;
-    set4(ground.static_pose + 4, 0.0, 0.0, 0.0, 1.0);
-    m.bodies.push_back(ground);
-    {
-        MRModelShapeC plane{};
-        plane.body = n;
-        plane.shape_type = MR_SHAPE_PLANE;
-        plane.material = 1;
-        plane.collision_group = 2u;
-        plane.collision_mask = 1u;
-        const double h = std::sqrt(0.5);
-        set4(plane.local_rotation, h, 0.0, 0.0, h);  // local +Y -> world +Z
-        m.shapes.push_back(plane);
-    }
-    MRModelMaterialC mat{};
-    set4(mat.friction, 0.6, 0.6, 0.0, 0.0);
-    set4(mat.response, 0.0, 0.5, 0.0, 0.0);
-    m.materials.push_back(mat);
-    m.materials.push_back(mat);
-    auto cls = [&](std::uint32_t a, std::uint32_t b) {
-        const std::uint32_t ta = m.shapes[a].shape_type, tb = m.shapes[b].shape_type;
-        if (tb == MR_SHAPE_PLANE) return ta == MR_SHAPE_BOX ? MR_COLLISION_PAIR_BOX_PLANE : MR_COLLISION_PAIR_SPHERE_PLANE;
-        if (ta == MR_SHAPE_SPHERE && tb == MR_SHAPE_SPHERE) return MR_COLLISION_PAIR_SPHERE_SPHERE;
-        if (ta == MR_SHAPE_BOX && tb == MR_SHAPE_BOX) return MR_COLLISION_PAIR_BOX_BOX;
-        return MR_COLLISION_PAIR_SPHERE_BOX;
-    };
-    // Compiled pairs in key order (a, b), b = n for the plane.
-    for (std::uint32_t a = 0; a < n; ++a) {
-        for (std::uint32_t b = a + 1; b < n; ++b) {
-            MRModelPairC pr{a, b, static_cast<std::uint32_t>(cls(a, b)), 4u};
-            m.pairs.push_back(pr);
-        }
-        MRModelPairC pr{a, n, static_cast<std::uint32_t>(cls(a, n)), 4u};
-        m.pairs.push_back(pr);
-    }
-    m.world.body_count = n + 1;
-    m.world.joint_count = 0;
-    m.world.nq = 7 * n;
-    m.world.nv = 6 * n;
-    m.world.shape_count = n + 1;
-    m.world.material_count = 2;
-    m.world.pair_count = static_cast<std::uint32_t>(m.pairs.size());
-    m.world.root_type = MR_ROOT_FIXED;
-    m.world.actuation_mode = MR_ACTUATION_EFFORT;
-    m.world.action_count = 0;
-    m.world.contact_capacity = 256;
-    m.world.apply_body_damping = 1u;
-    set4(m.world.gravity, 0.0, 0.0, -9.81, 0.0);
-    set4(m.world.solver_scales, 1.0e-7, 1.0e-9, 2.0, 1.0e-4);
-    set4(m.world.manifold_thresholds, 0.02, 0.02, 0.002, 0.95);
-    set4(m.world.speculative, 1.0, 1.0e4, 0.0, 0.0);
     m.scene_cell = static_cast<float>(2.0 * largest + 0.05);
-    m.nominal_q.assign(m.world.nq, 0.0f);
-    m.friction_scale_lo = 1.0f;
-    m.friction_scale_hi = 1.0f;
-    m.finalize();
+    finish_scene(m, n, 0.6);
+    return m;
+}
+
+CompiledModel build_stack(std::uint64_t seed, std::uint32_t boxes) {
+    CompiledModel m;
+    m.name = "synthetic_stack";
+    m.scene = true;
+    m.scene_layout = CompiledModel::SceneLayout::stack;
+    m.stack_offset_sigma = 0.002f;
+    (void)seed;  // every box is the same; the seed drives the reset layout
+    if (boxes < 1 || boxes > 64) throw std::invalid_argument("stack box count must be in [1, 64]");
+    m.scene_bodies = boxes;
+    const double he = 0.05, mass = 1.0;
+    const double inertia = mass / 3.0 * (2.0 * he * he);
+    for (std::uint32_t b = 0; b < boxes; ++b) {
+        MRModelBodyC body{};
+        body.parent_body = MR_INVALID_INDEX;
+        body.inbound_joint = MR_INVALID_INDEX;
+        body.motion_type = MR_MOTION_DYNAMIC;
+        body.articulated = 0u;
+        set4(body.mass_inverse_mass, mass, 1.0 / mass, 0.0, 0.0);
+        set4(body.inertia[0], inertia, 0.0, 0.0, 0.0);
+        set4(body.inertia[1], 0.0, inertia, 0.0, 0.0);
+        set4(body.inertia[2], 0.0, 0.0, inertia, 0.0);
+        set4(body.damping_speed, 0.0, 0.0, 100.0, 100.0);
+        set4(body.static_pose, 0.0, 0.0, 0.0, 0.0);
+        set4(body.static_pose + 4, 0.0, 0.0, 0.0, 1.0);
+        m.bodies.push_back(body);
+        MRModelShapeC s{};
+        s.body = b;
+        s.shape_type = MR_SHAPE_BOX;
+        s.material = 0;
+        s.collision_group = 1u;
+        s.collision_mask = 3u;
+        set4(s.local_position, 0.0, 0.0, 0.0, 0.0);
+        set4(s.local_rotation, 0.0, 0.0, 0.0, 1.0);
+        set4(s.dimensions, he, he, he, 0.0);
+        set4(s.contact_rest_bound, 0.002, 0.0, std::sqrt(3.0) * he, 0.0);
+        m.shapes.push_back(s);
+    }
+    m.scene_cell = static_cast<float>(2.0 * he);  // stack pitch
+    finish_scene(m, boxes, 0.6);
     return m;
 }
 
 void sample_reset_state(const CompiledModel& model, std::uint64_t seed, std::uint32_t env,
                         float* q, float* v, float* friction_scale) {
     const std::uint32_t nq = model.world.nq, nv = model.world.nv;
+    if (model.scene && model.scene_layout == CompiledModel::SceneLayout::stack) {
+        // Boxes resting on each other (box k's centre at (k + 1/2) pitch),
+        // the stack yawed U(0, 2 pi) as a whole and each box offset
+        // horizontally by N(0, sigma).
+        const std::uint32_t n = model.scene_bodies;
+        const std::uint64_t base = static_cast<std::uint64_t>(env) * 1024u;
+        const double pitch = model.scene_cell;
+        const double yaw = uniform(seed, kStreamResetRoot, base, 0.0, 6.283185307179586);
+        for (std::uint32_t b = 0; b < n; ++b) {
+            float* qb = q + 7 * b;
+            qb[0] = static_cast<float>(model.stack_offset_sigma * normal(seed, kStreamResetQ, base + 8 * b));
+            qb[1] = static_cast<float>(model.stack_offset_sigma * normal(seed, kStreamResetQ, base + 8 * b + 1));
+            qb[2] = static_cast<float>((b + 0.5) * pitch);
+            qb[3] = 0.0f;
+            qb[4] = 0.0f;
+            qb[5] = static_cast<float>(std::sin(0.5 * yaw));
+            qb[6] = static_cast<float>(std::cos(0.5 * yaw));
+        }
+        for (std::uint32_t i = 0; i < nv; ++i) v[i] = 0.0f;
+        *friction_scale = 1.0f;
+        return;
+    }
     if (model.scene) {
         // Bodies on a jittered square grid, dropped from U(0.1, 1) m above
         // the plane with a uniformly random orientation, at rest.

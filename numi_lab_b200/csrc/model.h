@@ -60,6 +60,10 @@ struct CompiledModel {
     bool scene = false;
     std::uint32_t scene_bodies = 0;
     float scene_cell = 0.0f;  // reset grid spacing
+    // Reset layout of a scene: a dropped pile, or a box stack on the plane.
+    enum class SceneLayout : std::uint32_t { pile = 0, stack = 1 };
+    SceneLayout scene_layout = SceneLayout::pile;
+    float stack_offset_sigma = 0.0f;  // horizontal offsets of stacked boxes ~ N(0, sigma)
 
     void finalize();  // validates and fills derived tables; throws on error
 };
@@ -70,6 +74,10 @@ CompiledModel build_tree29(std::uint64_t seed);
 // U(500, 2000) kg/m^3) dropped onto a ground plane; the body count is drawn
 // from the seed unless `bodies` is non-zero.
 CompiledModel build_pile(std::uint64_t seed, std::uint32_t bodies = 0);
+// Stack of `boxes` 0.1 m, 1 kg cubes (friction 0.6) resting on a ground
+// plane, the stack yawed U(0, 2 pi) and each box offset horizontally by
+// N(0, 2 mm) at reset.
+CompiledModel build_stack(std::uint64_t seed, std::uint32_t boxes = 32);
 
 // Reset state for environment `env` (q: nq, v: nv) and its friction scale.
 void sample_reset_state(const CompiledModel& model, std::uint64_t seed, std::uint32_t env,

@@ -604,10 +604,11 @@ MR_API MRTaskRolloutHandle* mr_create_task_rollout(const MRRunManifestC* manifes
             case MR_RUN_SOURCE_SYNTHETIC_CHAIN7: h.model = numi::build_chain7(cfg.seed); break;
             case MR_RUN_SOURCE_SYNTHETIC_TREE29: h.model = numi::build_tree29(cfg.seed); break;
             case MR_RUN_SOURCE_SYNTHETIC_PILE: h.model = numi::build_pile(cfg.seed); break;
+            case MR_RUN_SOURCE_SYNTHETIC_STACK: h.model = numi::build_stack(cfg.seed); break;
             default:
                 throw std::invalid_argument("unsupported run source " + std::to_string(manifest->source) +
                                             " (robot assets, URDF and world packs are not compiled by this library; "
-                                            "use MR_RUN_SOURCE_SYNTHETIC_CHAIN7, _TREE29 or _PILE)");
+                                            "use MR_RUN_SOURCE_SYNTHETIC_CHAIN7, _TREE29, _PILE or _STACK)");
         }
         if (h.model.world.pair_count > 0 && cfg.velocity_iterations == 0 && cfg.final_velocity_iterations == 0)
             throw std::invalid_argument("contact worlds need at least one velocity iteration");
@@ -895,6 +896,7 @@ static numi::CompiledModel compile_source(uint32_t source, uint64_t seed) {
         case MR_RUN_SOURCE_SYNTHETIC_CHAIN7: return numi::build_chain7(seed);
         case MR_RUN_SOURCE_SYNTHETIC_TREE29: return numi::build_tree29(seed);
         case MR_RUN_SOURCE_SYNTHETIC_PILE: return numi::build_pile(seed);
+        case MR_RUN_SOURCE_SYNTHETIC_STACK: return numi::build_stack(seed);
         default: throw std::invalid_argument("unsupported synthetic source " + std::to_string(source));
     }
 }

@@ -32,6 +32,12 @@ constexpr float kTinyS = 1.0e-12f;
 constexpr float kTieRel = 1.0e-5f;
 constexpr float kTieAbs = 1.0e-12f;
 constexpr int kRawCap = 8;
+// Box-box separating axes, FP32 rules of the GPU collision
+// (Collision.metal:1600-1650): edge pairs closer to parallel than
+// |sin| = 1e-6 give no axis, and separations within a relative 1e-7 tie
+// (the first axis wins).  The FP64 CPU collision uses 1e-24 and 1e-12.
+constexpr float kParallelEdges = 1.0e-12f;
+constexpr float kAxisTie = 1.0e-7f;
 constexpr int kRecWords = 16;                                   // candidate record
 constexpr int kLaneScratch = (4 + kRawCap) * kRecWords + 4;  // records, candidate ids
 constexpr int kCw = 40;                                          // contact record words
@@ -278,7 +284,7 @@ __device__ bool narrowphase(const Collider& A, const Collider& B, int cls, unsig
             else {
                 const float3 cr = cross3(box_axis(A, (k - 6) / 3), box_axis(B, (k - 6) % 3));
                 const float sq = dot3(cr, cr);
-                if (!(sq > 1.0e-24f)) continue;
+                if (!(sq > kParallelEdges)) continue;
                 axis = cr * rsqrtf(sq);
             }
             ++index;
@@ -289,7 +295,7 @@ __device__ bool narrowphase(const Collider& A, const Collider& B, int cls, unsig
                 normal = axis;
                 return true;  // separated: no contact
             }
-            const float tol = 1.0e-12f * (1.0f + fmaxf(fabsf(best_sep), fabsf(sep)));
+            const float tol = kAxisTie * (1.0f + fmaxf(fabsf(best_sep), fabsf(sep)));
             if (!isfinite(best_sep) || sep > best_sep + tol || (fabsf(sep - best_sep) <= tol && index < best_axis)) {
                 best_sep = sep;
                 best_n = axis;

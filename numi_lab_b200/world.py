@@ -25,6 +25,7 @@ SOURCES = {
     "chain7": native.MR_RUN_SOURCE_SYNTHETIC_CHAIN7,
     "tree29": native.MR_RUN_SOURCE_SYNTHETIC_TREE29,
     "pile": native.MR_RUN_SOURCE_SYNTHETIC_PILE,
+    "stack32": native.MR_RUN_SOURCE_SYNTHETIC_STACK,
 }
 SCENE_MANIFOLDS = 128      # manifold slots per scene environment
 SCENE_SLOT_WORDS = 57      # MRManifoldC words + pair key

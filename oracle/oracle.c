@@ -1660,8 +1660,11 @@ static v3 snarrow(const SCol* A, const SCol* B, int cls, uint32_t ia, uint32_t i
             else {
                 const v3 cr = vcross(sbox_axis(A, (k - 6) / 3), sbox_axis(B, (k - 6) % 3));
                 const double sq = vdot(cr, cr);
-                if (sq <= 1e-12) g_band++; /* the FP32 cross product may fall under the floor */
-                if (!(sq > 1e-24)) continue;
+                /* Edge pairs within |sin| = 1e-6 of parallel give no axis
+                 * (Collision.metal:1600-1612); near the floor the FP32 cross
+                 * product may fall on the other side. */
+                if (fabs(sq - 1e-12) <= 16.0 * kFloatEps * (sq + 1e-12) + 1e-13) g_band++;
+                if (!(sq > 1e-12)) continue;
                 axis_len = sqrt(sq);
                 axis = vmul(cr, 1.0 / axis_len);
             }
@@ -1675,7 +1678,7 @@ static v3 snarrow(const SCol* A, const SCol* B, int cls, uint32_t ia, uint32_t i
             if (fabs(sep - acc) <= err) g_band++;
             BAND(sep, acc);
             if (sep > acc) return axis;
-            const double tol = 1.0e-12 * (1.0 + fmax(fabs(best_sep), fabs(sep)));
+            const double tol = 1.0e-7 * (1.0 + fmax(fabs(best_sep), fabs(sep))); /* Collision.metal:1628-1638 */
             if (isfinite(best_sep) && fabs(sep - best_sep) <= err + best_err) g_band++;
             if (!isfinite(best_sep) || sep > best_sep + tol || (fabs(sep - best_sep) <= tol && index < best_axis)) {
                 best_sep = sep;
