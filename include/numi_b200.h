@@ -102,7 +102,10 @@ enum MRCollisionPairClass {
     MR_COLLISION_PAIR_SPHERE_PLANE = 2u,
     MR_COLLISION_PAIR_CAPSULE_PLANE = 3u,
     MR_COLLISION_PAIR_BOX_PLANE = 4u,
+    MR_COLLISION_PAIR_SPHERE_CAPSULE = 6u,
+    MR_COLLISION_PAIR_CAPSULE_CAPSULE = 7u,
     MR_COLLISION_PAIR_SPHERE_BOX = 8u,
+    MR_COLLISION_PAIR_CAPSULE_BOX = 9u,
     MR_COLLISION_PAIR_BOX_BOX = 10u
 };
 #endif /* NUMI_B200_OMIT_SHARED_ENUMS */
@@ -168,7 +171,7 @@ enum MRRunManifestSourceC {
      * implicit PD position drives, box feet and 12 sphere proxies on a
      * ground plane. */
     MR_RUN_SOURCE_SYNTHETIC_TREE29 = 101u,
-    /* Pile of 8-64 free spheres and boxes dropped onto a ground plane (body
+    /* Pile of 8-64 free boxes, spheres and capsules dropped onto a ground plane (body
      * count drawn from the seed); scene bodies, no actuation. */
     MR_RUN_SOURCE_SYNTHETIC_PILE = 102u,
     /* Stack of 32 0.1 m, 1 kg boxes (friction 0.6) resting on a ground

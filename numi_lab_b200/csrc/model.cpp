@@ -502,10 +502,18 @@ static void finish_scene(CompiledModel& m, std::uint32_t n, double friction) {
     m.materials.push_back(mat);
     auto cls = [&](std::uint32_t a, std::uint32_t b) {
         const std::uint32_t ta = m.shapes[a].shape_type, tb = m.shapes[b].shape_type;
-        if (tb == MR_SHAPE_PLANE) return ta == MR_SHAPE_BOX ? MR_COLLISION_PAIR_BOX_PLANE : MR_COLLISION_PAIR_SPHERE_PLANE;
-        if (ta == MR_SHAPE_SPHERE && tb == MR_SHAPE_SPHERE) return MR_COLLISION_PAIR_SPHERE_SPHERE;
-        if (ta == MR_SHAPE_BOX && tb == MR_SHAPE_BOX) return MR_COLLISION_PAIR_BOX_BOX;
-        return MR_COLLISION_PAIR_SPHERE_BOX;
+        if (tb == MR_SHAPE_PLANE)
+            return ta == MR_SHAPE_BOX ? MR_COLLISION_PAIR_BOX_PLANE
+                   : (ta == MR_SHAPE_CAPSULE ? MR_COLLISION_PAIR_CAPSULE_PLANE : MR_COLLISION_PAIR_SPHERE_PLANE);
+        const bool sphere = ta == MR_SHAPE_SPHERE || tb == MR_SHAPE_SPHERE;
+        const bool capsule = ta == MR_SHAPE_CAPSULE || tb == MR_SHAPE_CAPSULE;
+        const bool box = ta == MR_SHAPE_BOX || tb == MR_SHAPE_BOX;
+        if (ta == tb)
+            return ta == MR_SHAPE_SPHERE ? MR_COLLISION_PAIR_SPHERE_SPHERE
+                   : (ta == MR_SHAPE_BOX ? MR_COLLISION_PAIR_BOX_BOX : MR_COLLISION_PAIR_CAPSULE_CAPSULE);
+        if (sphere && box) return MR_COLLISION_PAIR_SPHERE_BOX;
+        if (sphere && capsule) return MR_COLLISION_PAIR_SPHERE_CAPSULE;
+        return MR_COLLISION_PAIR_CAPSULE_BOX;
     };
     // Compiled pairs in key order (a, b), b = n for the plane.
     for (std::uint32_t a = 0; a < n; ++a) {
@@ -550,7 +558,10 @@ CompiledModel build_pile(std::uint64_t seed, std::uint32_t count) {
     m.scene_bodies = n;
     double largest = 0.0;
     for (std::uint32_t b = 0; b < n; ++b) {
-        const bool box = draw(0.0, 1.0) < 0.5;
+        // One third each of boxes, spheres and capsules.
+        const double kind = draw(0.0, 1.0);
+        const bool box = kind < 1.0 / 3.0;
+        const bool capsule = kind >= 2.0 / 3.0;
         const double size = draw(0.05, 0.3);
         const double density = draw(500.0, 2000.0);
         double hx = 0.5 * size, hy = 0.5 * size, hz = 0.5 * size;
@@ -559,6 +570,9 @@ CompiledModel build_pile(std::uint64_t seed, std::uint32_t count) {
             hy *= draw(0.7, 1.0);
             hz *= draw(0.7, 1.0);
         }
+        // Capsule: overall length `size` along local +Y, radius size x U(0.15, 0.3).
+        const double cap_r = capsule ? size * draw(0.15, 0.3) : 0.0;
+        const double cap_hl = capsule ? 0.5 * size - cap_r : 0.0;
         MRModelBodyC body{};
         body.parent_body = MR_INVALID_INDEX;
         body.inbound_joint = MR_INVALID_INDEX;
@@ -571,6 +585,16 @@ CompiledModel build_pile(std::uint64_t seed, std::uint32_t count) {
             iyy = mass / 3.0 * (hx * hx + hz * hz);
             izz = mass / 3.0 * (hx * hx + hy * hy);
             bound = std::sqrt(hx * hx + hy * hy + hz * hz);
+        } else if (capsule) {
+            // Cylinder of height 2 hl plus two hemispherical caps.
+            const double pi = 3.141592653589793, r = cap_r, hgt = 2.0 * cap_hl;
+            const double m_cyl = density * pi * r * r * hgt;
+            const double m_cap = density * 2.0 / 3.0 * pi * r * r * r;  // one hemisphere
+            mass = m_cyl + 2.0 * m_cap;
+            iyy = 0.5 * m_cyl * r * r + 2.0 * m_cap * 0.4 * r * r;
+            ixx = izz = m_cyl * (hgt * hgt / 12.0 + 0.25 * r * r) +
+                        2.0 * m_cap * (0.4 * r * r + 0.25 * hgt * hgt + 0.375 * hgt * r);
+            bound = cap_hl + r;
         } else {
             const double r = hx;
             mass = density * 4.0 / 3.0 * 3.141592653589793 * r * r * r;
@@ -588,13 +612,14 @@ CompiledModel build_pile(std::uint64_t seed, std::uint32_t count) {
         m.bodies.push_back(body);
         MRModelShapeC s{};
         s.body = b;
-        s.shape_type = box ? MR_SHAPE_BOX : MR_SHAPE_SPHERE;
+        s.shape_type = box ? MR_SHAPE_BOX : (capsule ? MR_SHAPE_CAPSULE : MR_SHAPE_SPHERE);
         s.material = 0;
         s.collision_group = 1u;
         s.collision_mask = 3u;
         set4(s.local_position, 0.0, 0.0, 0.0, 0.0);
         set4(s.local_rotation, 0.0, 0.0, 0.0, 1.0);
-        set4(s.dimensions, hx, box ? hy : 0.0, box ? hz : 0.0, 0.0);
+        if (capsule) set4(s.dimensions, cap_r, cap_hl, 0.0, 0.0);
+        else set4(s.dimensions, hx, box ? hy : 0.0, box ? hz : 0.0, 0.0);
         set4(s.contact_rest_bound, 0.002, 0.0, bound, 0.0);
         m.shapes.push_back(s);
     }

@@ -70,7 +70,7 @@ struct CompiledModel {
 
 CompiledModel build_chain7(std::uint64_t seed);
 CompiledModel build_tree29(std::uint64_t seed);
-// Pile of 8-64 free spheres and boxes (size U(0.05, 0.3) m, density
+// Pile of 8-64 free boxes, spheres and capsules (size U(0.05, 0.3) m, density
 // U(500, 2000) kg/m^3) dropped onto a ground plane; the body count is drawn
 // from the seed unless `bodies` is non-zero.
 CompiledModel build_pile(std::uint64_t seed, std::uint32_t bodies = 0);

@@ -28,7 +28,7 @@ namespace {
 
 constexpr float kQueryPadS = 0.00000762939453125f;  // MR_COLLISION_QUERY_RELATIVE_PAD
 constexpr float kAabbPadS = 0.00000762939453125f;   // MR_COLLISION_AABB_RELATIVE_PAD
-constexpr float kTinyS = 1.0e-12f;
+constexpr float kTinyS = 1.0e-14f;  // Collision.metal:10
 constexpr float kTieRel = 1.0e-5f;
 constexpr float kTieAbs = 1.0e-12f;
 constexpr int kRawCap = 8;
@@ -121,6 +121,7 @@ struct Collider {
     float radius;
     float offset;    // contact offset incl. speculative margin
     float3 lo, hi;   // swept, inflated bounds (finite shapes)
+    float3 e0, e1;   // capsule segment endpoints (local -Y / +Y ends)
     float3 normal;   // plane normal
     float3 bpos;     // pose of the collider's body: the frame of its
     float4 brot;     // manifold anchors (the ground body for the plane)
@@ -150,6 +151,13 @@ __device__ void load_collider(const SceneModel& M, const float* s, int b, Collid
     o.offset = M.offsets[b].x + s[kOffMargin + b];
     o.lo = ld3(s + kOffLo + b * 3);
     o.hi = ld3(s + kOffHi + b * 3);
+    if (o.type == MR_SHAPE_CAPSULE) {
+        const float3 axis = qrot(o.r, f3(0.0f, d.y, 0.0f));
+        o.e0 = o.c - axis;
+        o.e1 = o.c + axis;
+    } else {
+        o.e0 = o.e1 = o.c;
+    }
     o.normal = f3(0.0f, 0.0f, 0.0f);
     o.bpos = o.c;
     o.brot = o.r;
@@ -189,6 +197,168 @@ __device__ __forceinline__ float3 coincident_normal(unsigned a, unsigned b) {
     const unsigned axis = hsh % 3u;
     const float sign = (hsh & 4u) == 0u ? 1.0f : -1.0f;
     return f3(axis == 0u ? sign : 0.0f, axis == 1u ? sign : 0.0f, axis == 2u ? sign : 0.0f);
+}
+
+// Segment helpers of the capsule classes (Collision.metal:965-1125,
+// Collision.cpp:1169-1336, restated).
+__device__ __forceinline__ unsigned capsule_feature(float t) { return t <= 0.0f ? 0u : (t >= 1.0f ? 1u : 2u); }
+
+__device__ float3 stable_segment_normal(float3 da, float3 db, unsigned ia, unsigned ib) {
+    const float3 cr = cross3(da, db);
+    if (dot3(cr, cr) > kTinyS) return cr * rsqrtf(dot3(cr, cr));
+    float3 dir;
+    if (dot3(da, da) > kTinyS) dir = da * rsqrtf(dot3(da, da));
+    else if (dot3(db, db) > kTinyS) dir = db * rsqrtf(dot3(db, db));
+    else return coincident_normal(ia, ib);
+    const float ax = fabsf(dir.x), ay = fabsf(dir.y), az = fabsf(dir.z);
+    const float3 ref = (ax <= ay && ax <= az) ? f3(1.0f, 0.0f, 0.0f) : (ay <= az ? f3(0.0f, 1.0f, 0.0f) : f3(0.0f, 0.0f, 1.0f));
+    float3 out = cross3(dir, ref);
+    out = out * rsqrtf(dot3(out, out));
+    return ((ia * 73856093u) ^ (ib * 19349663u)) & 4u ? -out : out;
+}
+
+__device__ __forceinline__ float3 closest_on_segment(float3 x, float3 e0, float3 e1, float& t) {
+    const float3 seg = e1 - e0;
+    const float sq = dot3(seg, seg);
+    if (!(sq > kTinyS)) {
+        t = 0.0f;
+        return e0;
+    }
+    t = fminf(fmaxf(dot3(x - e0, seg) / sq, 0.0f), 1.0f);
+    return e0 + seg * t;
+}
+
+__device__ void closest_segments(float3 a0, float3 a1, float3 b0, float3 b1, float3& pa, float3& pb, float& ta, float& tb) {
+    const float3 da = a1 - a0, db = b1 - b0, off = a0 - b0;
+    const float sa = dot3(da, da), sb = dot3(db, db), pa_ = dot3(da, off), pb_ = dot3(db, off);
+    ta = 0.0f;
+    tb = 0.0f;
+    if (!(sa > kTinyS) && !(sb > kTinyS)) {
+        pa = a0;
+        pb = b0;
+        return;
+    }
+    if (!(sa > kTinyS)) {
+        tb = fminf(fmaxf(pb_ / sb, 0.0f), 1.0f);
+    } else {
+        const float cp = dot3(da, db);
+        if (!(sb > kTinyS)) {
+            ta = fminf(fmaxf(-pa_ / sa, 0.0f), 1.0f);
+        } else {
+            const float den = sa * sb - cp * cp;
+            if (den > kTinyS * sa * sb) ta = fminf(fmaxf((cp * pb_ - pa_ * sb) / den, 0.0f), 1.0f);
+            tb = (cp * ta + pb_) / sb;
+            if (tb < 0.0f) {
+                tb = 0.0f;
+                ta = fminf(fmaxf(-pa_ / sa, 0.0f), 1.0f);
+            } else if (tb > 1.0f) {
+                tb = 1.0f;
+                ta = fminf(fmaxf((cp - pa_) / sa, 0.0f), 1.0f);
+            }
+        }
+    }
+    pa = a0 + da * ta;
+    pb = b0 + db * tb;
+}
+
+// Capsule-box witness in the box frame (Collision.metal:1241,
+// Collision.cpp:1462): the segment's deepest point when it pierces the box,
+// else the closest of the two clamped endpoints and the twelve edges.
+// Normal from the capsule to the box, world frame.
+struct CapsuleBoxWitness {
+    float3 normal, cap_point, box_point;
+    float sep, t_cap;
+    unsigned box_feature;
+};
+
+__device__ __forceinline__ CapsuleBoxWitness capsule_box_witness(float3 ce0, float3 ce1, float cap_radius, float3 bc, float4 br,
+                                                             float3 half, unsigned ic, unsigned ib) {
+    CapsuleBoxWitness w;
+    const float3 s0 = qrotinv(br, ce0 - bc), s1 = qrotinv(br, ce1 - bc);
+    const float3 dir = s1 - s0;
+    const float he[3] = {half.x, half.y, half.z};
+    const float st[3] = {s0.x, s0.y, s0.z}, dd[3] = {dir.x, dir.y, dir.z};
+    float enter = 0.0f, exit = 1.0f;
+    bool inside = true;
+    for (int a = 0; a < 3; ++a) {
+        if (fabsf(dd[a]) <= kTinyS) {
+            if (st[a] < -he[a] || st[a] > he[a]) inside = false;
+            continue;
+        }
+        float t0 = (-he[a] - st[a]) / dd[a], t1 = (he[a] - st[a]) / dd[a];
+        if (t0 > t1) { const float t = t0; t0 = t1; t1 = t; }
+        enter = fmaxf(enter, t0);
+        exit = fminf(exit, t1);
+        if (enter > exit) inside = false;
+    }
+    if (inside) {
+        const float t_cap = fminf(fmaxf(0.5f * (enter + exit), 0.0f), 1.0f);
+        const float3 core = s0 + dir * t_cap;
+        const float cc[3] = {core.x, core.y, core.z};
+        const float dist[3] = {he[0] - fabsf(cc[0]), he[1] - fabsf(cc[1]), he[2] - fabsf(cc[2])};
+        int axis = 0;
+        if (dist[1] < dist[axis]) axis = 1;
+        if (dist[2] < dist[axis]) axis = 2;
+        const float sign = cc[axis] >= 0.0f ? 1.0f : -1.0f;
+        const float3 outward = f3(axis == 0 ? sign : 0.0f, axis == 1 ? sign : 0.0f, axis == 2 ? sign : 0.0f);
+        float3 lbox = core;
+        if (axis == 0) lbox.x = sign * he[0];
+        else if (axis == 1) lbox.y = sign * he[1];
+        else lbox.z = sign * he[2];
+        const float3 ln = -outward;
+        w.normal = qrot(br, ln);
+        w.cap_point = bc + qrot(br, core + ln * cap_radius);
+        w.box_point = bc + qrot(br, lbox);
+        w.sep = -dist[axis] - cap_radius;
+        w.t_cap = t_cap;
+        w.box_feature = 27u + 2u * static_cast<unsigned>(axis) + (sign > 0.0f ? 1u : 0u);
+        return w;
+    }
+    float best = INFINITY, best_t = 0.0f;
+    float3 best_seg = s0, best_box = s0;
+    unsigned best_f = 0xffffffffu;
+    auto consider = [&](float3 sp, float3 bp, float t, unsigned f) {
+        const float3 d = bp - sp;
+        const float sq = dot3(d, d);
+        const float tol = 1.0e-12f * (1.0f + fmaxf(best, sq));
+        if (!isfinite(best) || sq < best - tol || (fabsf(sq - best) <= tol && f < best_f)) {
+            best = sq;
+            best_seg = sp;
+            best_box = bp;
+            best_t = t;
+            best_f = f;
+        }
+    };
+    for (int e = 0; e < 2; ++e) {
+        const float3 sp = e == 0 ? s0 : s1;
+        consider(sp, f3(fminf(fmaxf(sp.x, -he[0]), he[0]), fminf(fmaxf(sp.y, -he[1]), he[1]), fminf(fmaxf(sp.z, -he[2]), he[2])),
+                 static_cast<float>(e), static_cast<unsigned>(e));
+    }
+    unsigned feature = 2u;
+    for (int va = 0; va < 3; ++va) {
+        const int f0 = (va + 1) % 3, f1 = (va + 2) % 3;
+        for (int sg = 0; sg < 4; ++sg) {
+            float c0[3], c1[3];
+            c0[va] = -he[va];
+            c1[va] = he[va];
+            c0[f0] = c1[f0] = ((sg & 1) ? 1.0f : -1.0f) * he[f0];
+            c0[f1] = c1[f1] = ((sg & 2) ? 1.0f : -1.0f) * he[f1];
+            float3 pa, pb;
+            float ta, tb;
+            closest_segments(s0, s1, f3(c0[0], c0[1], c0[2]), f3(c1[0], c1[1], c1[2]), pa, pb, ta, tb);
+            consider(pa, pb, ta, feature);
+            ++feature;
+        }
+    }
+    const float dist = sqrtf(fmaxf(best, 0.0f));
+    const float3 ln = dist > kTinyS ? (best_box - best_seg) * (1.0f / dist) : qrotinv(br, coincident_normal(ic, ib));
+    w.normal = qrot(br, ln);
+    w.cap_point = bc + qrot(br, best_seg + ln * cap_radius);
+    w.box_point = bc + qrot(br, best_box);
+    w.sep = dist - cap_radius;
+    w.t_cap = best_t;
+    w.box_feature = 64u + best_f;
+    return w;
 }
 
 // Raw contacts of one pair into candidate records (anchors in the bodies'
@@ -268,6 +438,53 @@ __device__ bool narrowphase(const Collider& A, const Collider& B, int cls, unsig
         normal = sphere_a ? n : -n;
         return true;
     }
+    if (cls == MR_COLLISION_PAIR_SPHERE_CAPSULE) {
+        const bool sphere_a = A.type == MR_SHAPE_SPHERE;
+        const Collider& sp = sphere_a ? A : B;
+        const Collider& cp = sphere_a ? B : A;
+        float t;
+        const float3 on = closest_on_segment(sp.c, cp.e0, cp.e1, t);
+        const float3 delta = on - sp.c;
+        const float d = len3(delta);
+        const float3 n = d > kTinyS ? delta * (1.0f / d)
+                                    : stable_segment_normal(cp.e1 - cp.e0, f3(0.0f, 0.0f, 0.0f), sphere_a ? ia : ib, sphere_a ? ib : ia);
+        const float sep = d - sp.radius - cp.radius;
+        if (sep <= accepted) {
+            const float3 ps = sp.c + n * sp.radius, pc = on - n * cp.radius;
+            const unsigned fs = feature_key(MR_SHAPE_SPHERE, 0u), fc = feature_key(MR_SHAPE_CAPSULE, capsule_feature(t));
+            if (sphere_a) sink.add(ps, pc, sep, fs, fc);
+            else sink.add(pc, ps, sep, fc, fs);
+        }
+        normal = sphere_a ? n : -n;
+        return true;
+    }
+    if (cls == MR_COLLISION_PAIR_CAPSULE_CAPSULE) {
+        float3 pa, pb;
+        float ta, tb;
+        closest_segments(A.e0, A.e1, B.e0, B.e1, pa, pb, ta, tb);
+        const float3 delta = pb - pa;
+        const float d = len3(delta);
+        normal = d > kTinyS ? delta * (1.0f / d) : stable_segment_normal(A.e1 - A.e0, B.e1 - B.e0, ia, ib);
+        const float sep = d - A.radius - B.radius;
+        if (sep <= accepted)
+            sink.add(pa + normal * A.radius, pb - normal * B.radius, sep, feature_key(MR_SHAPE_CAPSULE, capsule_feature(ta)),
+                     feature_key(MR_SHAPE_CAPSULE, capsule_feature(tb)));
+        return true;
+    }
+    if (cls == MR_COLLISION_PAIR_CAPSULE_BOX) {
+        const bool capsule_a = A.type == MR_SHAPE_CAPSULE;
+        const Collider& cp = capsule_a ? A : B;
+        const Collider& bx = capsule_a ? B : A;
+        const CapsuleBoxWitness w =
+            capsule_box_witness(cp.e0, cp.e1, cp.radius, bx.c, bx.r, bx.half, capsule_a ? ia : ib, capsule_a ? ib : ia);
+        if (w.sep <= accepted) {
+            const unsigned fc = feature_key(MR_SHAPE_CAPSULE, capsule_feature(w.t_cap)), fb = feature_key(MR_SHAPE_BOX, w.box_feature);
+            if (capsule_a) sink.add(w.cap_point, w.box_point, w.sep, fc, fb);
+            else sink.add(w.box_point, w.cap_point, w.sep, fb, fc);
+        }
+        normal = capsule_a ? w.normal : -w.normal;
+        return true;
+    }
     if (cls == MR_COLLISION_PAIR_BOX_BOX) {
         const float3 cd = B.c - A.c;
         float best_sep = -INFINITY;
@@ -337,6 +554,15 @@ __device__ bool narrowphase(const Collider& A, const Collider& B, int cls, unsig
         const float3 surface = A.c - pn * A.radius;
         const float sep = dot3(pn, surface - B.c);
         if (sep <= accepted) sink.add(surface, surface - pn * sep, sep, feature_key(MR_SHAPE_SPHERE, 0u), plane_key);
+        return true;
+    }
+    if (cls == MR_COLLISION_PAIR_CAPSULE_PLANE) {
+        for (int e = 0; e < 2; ++e) {
+            const float3 surface = (e == 0 ? A.e0 : A.e1) - pn * A.radius;
+            const float sep = dot3(pn, surface - B.c);
+            if (sep <= accepted)
+                sink.add(surface, surface - pn * sep, sep, feature_key(MR_SHAPE_CAPSULE, static_cast<unsigned>(e)), plane_key);
+        }
         return true;
     }
     if (cls == MR_COLLISION_PAIR_BOX_PLANE) {
@@ -555,9 +781,9 @@ __device__ __forceinline__ float3 sym3_mul(const float* S, float3 x) {
     return f3(S[0] * x.x + S[1] * x.y + S[3] * x.z, S[1] * x.x + S[2] * x.y + S[4] * x.z, S[3] * x.x + S[4] * x.y + S[5] * x.z);
 }
 
-// 128 registers: 16 resident warps per SM.  More warps (96 registers) ran
-// slower: their narrowphase scratch no longer fits the L1 cache.
-__global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
+// At most 128 registers: 16 resident warps per SM.  More warps (96
+// registers) ran slower: their narrowphase scratch no longer fits the L1.
+__global__ void __launch_bounds__(32, 16) scene_step_kernel(SceneParams p) {
     extern __shared__ float4 smem4[];
     float* s = reinterpret_cast<float*>(smem4);
     const int item = blockIdx.x;
@@ -619,8 +845,11 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
             const float3 fc = c + h * lin;
             float4 fr = qmul(so3_increment(h * ang, false), qn);
             fr = qscale(fr, rsqrtf(qdot(fr, fr)));
-            const float cosv = fminf(fmaxf(fabsf(qdot(qn, fr)), 0.0f), 1.0f);
-            const float chord = 2.0f * off.z * sqrtf(fmaxf(0.0f, 1.0f - cosv * cosv));
+            // Chord of the sweep sphere: the reference's 2 r sqrt(1 - cos^2)
+            // with cos = |q . q_next| is 2 r |sin(h |w| / 2)|; written so,
+            // FP32 has no cancellation near rest (1 - cos^2 of a resting body
+            // would otherwise carry a spurious ~1e-4 m margin).
+            const float chord = 2.0f * off.z * fabsf(sinf(0.5f * h * len3(ang)));
             const float envelope = fminf(len3(fc - c) + chord, h * M.speed_envelope);
             const float margin = M.speculative_scale * envelope;
             s[kOffMargin + b] = margin;
@@ -628,6 +857,10 @@ __global__ void __launch_bounds__(32) scene_step_kernel(SceneParams p) {
             float3 e0, e1;
             if (M.shape_type[b] == MR_SHAPE_SPHERE) {
                 e0 = e1 = f3(dm.x, dm.x, dm.x);
+            } else if (M.shape_type[b] == MR_SHAPE_CAPSULE) {
+                const float3 a0 = qrot(qn, f3(0.0f, dm.y, 0.0f)), a1 = qrot(fr, f3(0.0f, dm.y, 0.0f));
+                e0 = f3(fabsf(a0.x) + dm.x, fabsf(a0.y) + dm.x, fabsf(a0.z) + dm.x);
+                e1 = f3(fabsf(a1.x) + dm.x, fabsf(a1.y) + dm.x, fabsf(a1.z) + dm.x);
             } else {
                 auto ext = [&](float4 r) {
                     const float3 bx = qrot(r, f3(1.0f, 0.0f, 0.0f)), by = qrot(r, f3(0.0f, 1.0f, 0.0f)), bz = qrot(r, f3(0.0f, 0.0f, 1.0f));

@@ -1493,6 +1493,7 @@ typedef struct {
     v3 half;
     double radius, offset;
     v3 lo, hi, normal;
+    v3 e0, e1; /* capsule segment endpoints (local -Y / +Y ends) */
     v3 bpos; /* pose of the collider's body: the frame of its manifold anchors */
     q4 brot;
 } SCol;
@@ -1515,6 +1516,7 @@ static void scol(const OracleScene* s, const SState* st, uint32_t b, SCol* o) {
         o->radius = 0.0;
         o->offset = s->plane_offset;
         o->lo = o->hi = V(0, 0, 0);
+        o->e0 = o->e1 = o->c;
         o->bpos = s->ground_pos;
         o->brot = s->ground_rot;
         return;
@@ -1527,6 +1529,13 @@ static void scol(const OracleScene* s, const SState* st, uint32_t b, SCol* o) {
     o->offset = s->offset[b] + st->margin[b];
     o->lo = V(st->lo[b][0], st->lo[b][1], st->lo[b][2]);
     o->hi = V(st->hi[b][0], st->hi[b][1], st->hi[b][2]);
+    if (o->type == MR_SHAPE_CAPSULE) {
+        const v3 axis = qrot(o->r, V(0, s->dims[b][1], 0));
+        o->e0 = vsub(o->c, axis);
+        o->e1 = vadd(o->c, axis);
+    } else {
+        o->e0 = o->e1 = o->c;
+    }
     o->normal = V(0, 0, 0);
     o->bpos = o->c;
     o->brot = o->r;
@@ -1586,12 +1595,185 @@ static void sraw_add(SRaw* r, v3 pa, v3 pb, double sep, uint32_t fa, uint32_t fb
     r->n++;
 }
 
+/* Segment helpers of the capsule classes (Collision.cpp:1169-1336). */
+static const double kSceneTiny = 1.0e-14; /* Collision.cpp:48, Collision.metal:10 */
+static uint32_t scap_feature(double t) { return t <= 0.0 ? 0u : (t >= 1.0 ? 1u : 2u); }
+
+static v3 sstable_segment_normal(v3 da, v3 db, uint32_t ia, uint32_t ib) {
+    const v3 cr = vcross(da, db);
+    if (vdot(cr, cr) > kSceneTiny) return vmul(cr, 1.0 / vlen(cr));
+    v3 dir;
+    if (vdot(da, da) > kSceneTiny) dir = vmul(da, 1.0 / vlen(da));
+    else if (vdot(db, db) > kSceneTiny) dir = vmul(db, 1.0 / vlen(db));
+    else return scoincident(ia, ib);
+    const double ax = fabs(dir.x), ay = fabs(dir.y), az = fabs(dir.z);
+    const v3 ref = (ax <= ay && ax <= az) ? V(1, 0, 0) : (ay <= az ? V(0, 1, 0) : V(0, 0, 1));
+    v3 out = vcross(dir, ref);
+    out = vmul(out, 1.0 / vlen(out));
+    return (((ia * 73856093u) ^ (ib * 19349663u)) & 4u) ? vmul(out, -1.0) : out;
+}
+
+/* Clamp of a segment parameter with the feature decisions at 0 and 1 taken
+ * in length units (band). */
+static double sclamp01(double t, double len) {
+    BAND(t * len, 0.0);
+    BAND(t * len, len);
+    return fmin(fmax(t, 0.0), 1.0);
+}
+
+static v3 sclosest_on_segment(v3 x, v3 e0, v3 e1, double* t) {
+    const v3 seg = vsub(e1, e0);
+    const double sq = vdot(seg, seg);
+    if (!(sq > kSceneTiny)) { *t = 0.0; return e0; }
+    *t = sclamp01(vdot(vsub(x, e0), seg) / sq, sqrt(sq));
+    return vadd(e0, vmul(seg, *t));
+}
+
+static void sclosest_segments(v3 a0, v3 a1, v3 b0, v3 b1, v3* pa, v3* pb, double* ta, double* tb) {
+    const v3 da = vsub(a1, a0), db = vsub(b1, b0), off = vsub(a0, b0);
+    const double sa = vdot(da, da), sb = vdot(db, db), pa_ = vdot(da, off), pb_ = vdot(db, off);
+    const double la = sqrt(sa), lb = sqrt(sb);
+    *ta = 0.0;
+    *tb = 0.0;
+    if (!(sa > kSceneTiny) && !(sb > kSceneTiny)) { *pa = a0; *pb = b0; return; }
+    if (!(sa > kSceneTiny)) {
+        *tb = sclamp01(pb_ / sb, lb);
+    } else {
+        const double cp = vdot(da, db);
+        if (!(sb > kSceneTiny)) {
+            *ta = sclamp01(-pa_ / sa, la);
+        } else {
+            const double den = sa * sb - cp * cp;
+            /* Near-parallel segments: the FP32 test may go the other way. */
+            if (fabs(den - kSceneTiny * sa * sb) <= 64.0 * kFloatEps * sa * sb) g_band++;
+            if (den > kSceneTiny * sa * sb) *ta = sclamp01((cp * pb_ - pa_ * sb) / den, la);
+            *tb = (cp * *ta + pb_) / sb;
+            BAND(*tb * lb, 0.0);
+            BAND(*tb * lb, lb);
+            if (*tb < 0.0) {
+                *tb = 0.0;
+                *ta = sclamp01(-pa_ / sa, la);
+            } else if (*tb > 1.0) {
+                *tb = 1.0;
+                *ta = sclamp01((cp - pa_) / sa, la);
+            }
+        }
+    }
+    *pa = vadd(a0, vmul(da, *ta));
+    *pb = vadd(b0, vmul(db, *tb));
+}
+
+typedef struct {
+    v3 normal, cap_point, box_point;
+    double sep, t_cap;
+    uint32_t box_feature;
+} SCapBox;
+
+/* Capsule-box witness (Collision.cpp:1462-1690, Collision.metal:1241). */
+static SCapBox scapsule_box(const SCol* cap, const SCol* box, uint32_t ic, uint32_t ib) {
+    SCapBox w;
+    const v3 s0 = qrotinv(box->r, vsub(cap->e0, box->c)), s1 = qrotinv(box->r, vsub(cap->e1, box->c));
+    const v3 dir = vsub(s1, s0);
+    const double he[3] = {box->half.x, box->half.y, box->half.z};
+    const double st[3] = {s0.x, s0.y, s0.z}, dd[3] = {dir.x, dir.y, dir.z};
+    const double seglen = vlen(dir);
+    double enter = 0.0, exit_ = 1.0;
+    int inside = 1;
+    for (int a = 0; a < 3; ++a) {
+        if (fabs(dd[a]) <= kSceneTiny) {
+            BAND(fabs(st[a]), he[a]);
+            if (st[a] < -he[a] || st[a] > he[a]) inside = 0;
+            continue;
+        }
+        double t0 = (-he[a] - st[a]) / dd[a], t1 = (he[a] - st[a]) / dd[a];
+        if (t0 > t1) { const double t = t0; t0 = t1; t1 = t; }
+        enter = fmax(enter, t0);
+        exit_ = fmin(exit_, t1);
+        BAND(enter * seglen, exit_ * seglen);
+        if (enter > exit_) inside = 0;
+    }
+    if (inside) {
+        w.t_cap = fmin(fmax(0.5 * (enter + exit_), 0.0), 1.0);
+        const v3 core = vadd(s0, vmul(dir, w.t_cap));
+        const double cc[3] = {core.x, core.y, core.z};
+        const double dist[3] = {he[0] - fabs(cc[0]), he[1] - fabs(cc[1]), he[2] - fabs(cc[2])};
+        int axis = 0;
+        BAND(dist[1], dist[0]);
+        if (dist[1] < dist[axis]) axis = 1;
+        BAND(dist[2], dist[axis]);
+        if (dist[2] < dist[axis]) axis = 2;
+        BAND(cc[axis], 0.0);
+        const double sign = cc[axis] >= 0.0 ? 1.0 : -1.0;
+        const v3 outward = V(axis == 0 ? sign : 0.0, axis == 1 ? sign : 0.0, axis == 2 ? sign : 0.0);
+        v3 lbox = core;
+        if (axis == 0) lbox.x = sign * he[0];
+        else if (axis == 1) lbox.y = sign * he[1];
+        else lbox.z = sign * he[2];
+        const v3 ln = vmul(outward, -1.0);
+        w.normal = qrot(box->r, ln);
+        w.cap_point = vadd(box->c, qrot(box->r, vadd(core, vmul(ln, cap->radius))));
+        w.box_point = vadd(box->c, qrot(box->r, lbox));
+        w.sep = -dist[axis] - cap->radius;
+        w.box_feature = 27u + 2u * (uint32_t)axis + (sign > 0.0 ? 1u : 0u);
+        return w;
+    }
+    double best = INFINITY, best_t = 0.0, best_d = INFINITY;
+    v3 best_seg = s0, best_box = s0;
+    uint32_t best_f = 0xffffffffu;
+#define SCONSIDER(SP, BP, T, F)                                                                  \
+    do {                                                                                         \
+        const v3 d_ = vsub((BP), (SP));                                                          \
+        const double sq_ = vdot(d_, d_);                                                         \
+        const double tol_ = 1.0e-12 * (1.0 + fmax(isfinite(best) ? best : 0.0, sq_));          \
+        if (isfinite(best_d)) BAND(sqrt(sq_), best_d);                                           \
+        if (!isfinite(best) || sq_ < best - tol_ || (fabs(sq_ - best) <= tol_ && (F) < best_f)) { \
+            best = sq_;                                                                          \
+            best_d = sqrt(sq_);                                                                  \
+            best_seg = (SP);                                                                     \
+            best_box = (BP);                                                                     \
+            best_t = (T);                                                                        \
+            best_f = (F);                                                                        \
+        }                                                                                        \
+    } while (0)
+    for (int e = 0; e < 2; ++e) {
+        const v3 sp = e == 0 ? s0 : s1;
+        const v3 bp = V(fmin(fmax(sp.x, -he[0]), he[0]), fmin(fmax(sp.y, -he[1]), he[1]), fmin(fmax(sp.z, -he[2]), he[2]));
+        SCONSIDER(sp, bp, (double)e, (uint32_t)e);
+    }
+    uint32_t feature = 2u;
+    for (int va = 0; va < 3; ++va) {
+        const int f0 = (va + 1) % 3, f1 = (va + 2) % 3;
+        for (int sg = 0; sg < 4; ++sg) {
+            double c0[3], c1[3];
+            c0[va] = -he[va];
+            c1[va] = he[va];
+            c0[f0] = c1[f0] = ((sg & 1) ? 1.0 : -1.0) * he[f0];
+            c0[f1] = c1[f1] = ((sg & 2) ? 1.0 : -1.0) * he[f1];
+            v3 pa, pb;
+            double ta, tb;
+            sclosest_segments(s0, s1, V(c0[0], c0[1], c0[2]), V(c1[0], c1[1], c1[2]), &pa, &pb, &ta, &tb);
+            SCONSIDER(pa, pb, ta, feature);
+            ++feature;
+        }
+    }
+#undef SCONSIDER
+    const double dist = sqrt(fmax(best, 0.0));
+    const v3 ln = dist > kSceneTiny ? vmul(vsub(best_box, best_seg), 1.0 / dist) : qrotinv(box->r, scoincident(ic, ib));
+    w.normal = qrot(box->r, ln);
+    w.cap_point = vadd(box->c, qrot(box->r, vadd(best_seg, vmul(ln, cap->radius))));
+    w.box_point = vadd(box->c, qrot(box->r, best_box));
+    w.sep = dist - cap->radius;
+    w.t_cap = best_t;
+    w.box_feature = 64u + best_f;
+    return w;
+}
+
 static v3 snarrow(const SCol* A, const SCol* B, int cls, uint32_t ia, uint32_t ib, double acc, SRaw* raw) {
     raw->n = 0;
     if (cls == MR_COLLISION_PAIR_SPHERE_SPHERE) {
         const v3 d = vsub(B->c, A->c);
         const double len = vlen(d);
-        const v3 n = len > 1e-12 ? vmul(d, 1.0 / len) : scoincident(ia, ib);
+        const v3 n = len > kSceneTiny ? vmul(d, 1.0 / len) : scoincident(ia, ib);
         const double sep = len - A->radius - B->radius;
         BAND(sep, acc);
         if (sep <= acc) sraw_add(raw, vadd(A->c, vmul(n, A->radius)), vsub(B->c, vmul(n, B->radius)), sep,
@@ -1613,7 +1795,7 @@ static v3 snarrow(const SCol* A, const SCol* B, int cls, uint32_t ia, uint32_t i
         v3 n;
         double sep;
         uint32_t feat;
-        if (dist > 1e-12) {
+        if (dist > kSceneTiny) {
             n = qrot(bx->r, vmul(ld, 1.0 / dist));
             sep = dist - sp->radius;
 #define SREG(c, he) ((c) < -(he) ? 0u : ((c) > (he) ? 2u : 1u))
@@ -1643,6 +1825,53 @@ static v3 snarrow(const SCol* A, const SCol* B, int cls, uint32_t ia, uint32_t i
             else sraw_add(raw, box_point, sphere_point, sep, feature_key(MR_SHAPE_BOX, feat), feature_key(MR_SHAPE_SPHERE, 0));
         }
         return sphere_a ? n : vmul(n, -1.0);
+    }
+    if (cls == MR_COLLISION_PAIR_SPHERE_CAPSULE) {
+        const int sphere_a = A->type == MR_SHAPE_SPHERE;
+        const SCol* sp = sphere_a ? A : B;
+        const SCol* cp = sphere_a ? B : A;
+        double t;
+        const v3 on = sclosest_on_segment(sp->c, cp->e0, cp->e1, &t);
+        const v3 delta = vsub(on, sp->c);
+        const double d = vlen(delta);
+        const v3 n = d > kSceneTiny ? vmul(delta, 1.0 / d)
+                                    : sstable_segment_normal(vsub(cp->e1, cp->e0), V(0, 0, 0), sphere_a ? ia : ib, sphere_a ? ib : ia);
+        const double sep = d - sp->radius - cp->radius;
+        BAND(sep, acc);
+        if (sep <= acc) {
+            const v3 ps = vadd(sp->c, vmul(n, sp->radius)), pc = vsub(on, vmul(n, cp->radius));
+            const uint32_t fs = feature_key(MR_SHAPE_SPHERE, 0), fc = feature_key(MR_SHAPE_CAPSULE, scap_feature(t));
+            if (sphere_a) sraw_add(raw, ps, pc, sep, fs, fc);
+            else sraw_add(raw, pc, ps, sep, fc, fs);
+        }
+        return sphere_a ? n : vmul(n, -1.0);
+    }
+    if (cls == MR_COLLISION_PAIR_CAPSULE_CAPSULE) {
+        v3 pa, pb;
+        double ta, tb;
+        sclosest_segments(A->e0, A->e1, B->e0, B->e1, &pa, &pb, &ta, &tb);
+        const v3 delta = vsub(pb, pa);
+        const double d = vlen(delta);
+        const v3 n = d > kSceneTiny ? vmul(delta, 1.0 / d) : sstable_segment_normal(vsub(A->e1, A->e0), vsub(B->e1, B->e0), ia, ib);
+        const double sep = d - A->radius - B->radius;
+        BAND(sep, acc);
+        if (sep <= acc)
+            sraw_add(raw, vadd(pa, vmul(n, A->radius)), vsub(pb, vmul(n, B->radius)), sep,
+                     feature_key(MR_SHAPE_CAPSULE, scap_feature(ta)), feature_key(MR_SHAPE_CAPSULE, scap_feature(tb)));
+        return n;
+    }
+    if (cls == MR_COLLISION_PAIR_CAPSULE_BOX) {
+        const int capsule_a = A->type == MR_SHAPE_CAPSULE;
+        const SCol* cp = capsule_a ? A : B;
+        const SCol* bx = capsule_a ? B : A;
+        const SCapBox w = scapsule_box(cp, bx, capsule_a ? ia : ib, capsule_a ? ib : ia);
+        BAND(w.sep, acc);
+        if (w.sep <= acc) {
+            const uint32_t fc = feature_key(MR_SHAPE_CAPSULE, scap_feature(w.t_cap)), fb = feature_key(MR_SHAPE_BOX, w.box_feature);
+            if (capsule_a) sraw_add(raw, w.cap_point, w.box_point, w.sep, fc, fb);
+            else sraw_add(raw, w.box_point, w.cap_point, w.sep, fb, fc);
+        }
+        return capsule_a ? w.normal : vmul(w.normal, -1.0);
     }
     if (cls == MR_COLLISION_PAIR_BOX_BOX) {
         const v3 cd = vsub(B->c, A->c);
@@ -1722,6 +1951,14 @@ static v3 snarrow(const SCol* A, const SCol* B, int cls, uint32_t ia, uint32_t i
             const double sep = vdot(pn, vsub(surface, B->c));
             BAND(sep, acc);
             if (sep <= acc) sraw_add(raw, surface, vsub(surface, vmul(pn, sep)), sep, feature_key(MR_SHAPE_SPHERE, 0), plane_key);
+        } else if (cls == MR_COLLISION_PAIR_CAPSULE_PLANE) {
+            for (int e = 0; e < 2; ++e) {
+                const v3 surface = vsub(e == 0 ? A->e0 : A->e1, vmul(pn, A->radius));
+                const double sep = vdot(pn, vsub(surface, B->c));
+                BAND(sep, acc);
+                if (sep <= acc)
+                    sraw_add(raw, surface, vsub(surface, vmul(pn, sep)), sep, feature_key(MR_SHAPE_CAPSULE, (uint32_t)e), plane_key);
+            }
         } else if (cls == MR_COLLISION_PAIR_BOX_PLANE) {
             for (int v = 0; v < 8; ++v) {
                 const v3 w = sbox_vertex(A, v);
@@ -1928,14 +2165,21 @@ static uint32_t sbounds(const OracleScene* s, SState* st, uint32_t* fail_index) 
         const v3 fc = vadd(c, vmul(st->lin[b], h));
         q4 fr = qmul(so3_increment(vmul(st->ang[b], h), 0), qn);
         fr = Q(fr.x / sqrt(qdot(fr, fr)), fr.y / sqrt(qdot(fr, fr)), fr.z / sqrt(qdot(fr, fr)), fr.w / sqrt(qdot(fr, fr)));
-        const double cosv = fmin(fmax(fabs(qdot(qn, fr)), 0.0), 1.0);
-        const double chord = 2.0 * s->sweep[b] * sqrt(fmax(0.0, 1.0 - cosv * cosv));
+        /* Chord of the sweep sphere over the substep's rotation: the
+         * reference's 2 r sqrt(1 - cos^2), cos = |q . q_next|, written as
+         * 2 r |sin(h |w| / 2)| (the same value; no cancellation near rest). */
+        const double chord = 2.0 * s->sweep[b] * fabs(sin(0.5 * h * vlen(st->ang[b])));
         const double env = fmin(vlen(vsub(fc, c)) + chord, h * s->speed_env);
         const double margin = s->spec_scale * env;
         st->margin[b] = margin;
         v3 e0, e1;
         if (s->type[b] == MR_SHAPE_SPHERE) {
             e0 = e1 = V(s->dims[b][0], s->dims[b][0], s->dims[b][0]);
+        } else if (s->type[b] == MR_SHAPE_CAPSULE) {
+            const double r = s->dims[b][0];
+            const v3 a0 = qrot(qn, V(0, s->dims[b][1], 0)), a1 = qrot(fr, V(0, s->dims[b][1], 0));
+            e0 = V(fabs(a0.x) + r, fabs(a0.y) + r, fabs(a0.z) + r);
+            e1 = V(fabs(a1.x) + r, fabs(a1.y) + r, fabs(a1.z) + r);
         } else {
             const q4 rs[2] = {qn, fr};
             v3 ex[2];
