@@ -480,6 +480,190 @@ def run_mix(args) -> None:
     print(json.dumps(line))
 
 
+def _stack_energy(records, q: np.ndarray, v: np.ndarray) -> float:
+    """Kinetic + potential energy of one scene environment (J)."""
+
+    n = records.world.body_count - 1
+    g = -float(records.world.gravity[2])
+    e = 0.0
+    for b in range(n):
+        m = float(records.bodies[b].mass_inverse_mass[0])
+        inertia = np.array([float(records.bodies[b].inertia[i][i]) for i in range(3)])
+        x, y, z, w = (float(c) for c in q[7 * b + 3: 7 * b + 7])
+        rot = np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                        [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                        [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
+        lin = v[6 * b: 6 * b + 3]
+        ang = rot.T @ v[6 * b + 3: 6 * b + 6]
+        e += 0.5 * m * float(lin @ lin) + 0.5 * float(ang @ (inertia * ang)) + m * g * float(q[7 * b + 2])
+    return e
+
+
+def _tree_energy(oracle, records, q: np.ndarray, v: np.ndarray) -> float:
+    """0.5 v^T M(q) v + sum of m g z over the articulated bodies (J)."""
+
+    mass = oracle.mass_matrix(q)
+    g = -float(records.world.gravity[2])
+    e = 0.5 * float(v @ mass @ v)
+    for b in range(records.world.body_count):
+        if not records.bodies[b].articulated:
+            continue
+        wp, _ = oracle.point_jacobian(q, b, np.zeros(3))
+        e += float(records.bodies[b].mass_inverse_mass[0]) * g * float(wp[2])
+    return e
+
+
+def _cone_violation_rows(impulses: np.ndarray, mu: np.ndarray) -> float:
+    """Largest elliptic-cone violation of impulse rows [.., 3] (normal,
+    tangent, bitangent), relative to max(1, normal)."""
+
+    n, t, b = impulses[..., 0], impulses[..., 1], impulses[..., 2]
+    scale = np.maximum(1.0, np.abs(n))
+    viol = np.maximum(np.maximum(-n, 0.0), np.hypot(t, b) - mu * np.maximum(n, 0.0)) / scale
+    return float(viol.max()) if viol.size else 0.0
+
+
+def run_precision(args) -> None:
+    """Precision configuration: 1024 envs of 32-box stacks plus 512 29-DoF
+    trees for 10,000 microsteps (2,500 control steps of 4 x 5 ms), FP32 and,
+    for the trees, the FP64 articulated-inertia mode; a seeded subset of
+    environments is replayed by the FP64 oracle (the checker) and the line
+    reports position drift, energy drift and cone violation against it at
+    checkpoints, beside the device throughput."""
+
+    import torch
+
+    import numi_lab_b200 as nb
+    from oracle import Oracle, SceneOracle, SceneTable
+
+    torch.cuda.set_device(0)
+    device = torch.device("cuda", 0)
+    n_stack, n_tree, subset = 1024, 512, 4
+    checkpoints = (1, 10, 100, 1000, 2500)
+    h = CONTROL_DT / SUBSTEPS
+    report: dict = {}
+    timing: dict = {}
+    # --- stacks (free bodies; FP32) ---
+    with nb.World("stack32", n_stack, substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT, seed=SEED) as world:
+        rec = world.model()
+        q0, v0, _ = world.state()
+        acts = torch.zeros((checkpoints[-1], n_stack, 0), device=device)
+        gpu = {}
+        done, ms = 0, 0.0
+        for cp in checkpoints:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            world.step(acts[: cp - done], wait=False)
+            e1.record()
+            torch.cuda.synchronize(device)
+            ms += e0.elapsed_time(e1)
+            done = cp
+            gpu[cp] = world.state()
+        timing["stack32"] = n_stack * checkpoints[-1] / (ms / 1e3)
+        oracle = SceneOracle(rec, h, SUBSTEPS, ITERATIONS, 0)
+        rows = {cp: {"position_drift_m": 0.0, "energy_drift_gpu_J": 0.0, "energy_drift_oracle_J": 0.0, "cone_violation": 0.0}
+                for cp in checkpoints}
+        for e in range(subset):
+            q = q0[e].astype(np.float64)
+            v = v0[e].astype(np.float64)
+            table = SceneTable()
+            energy0 = _stack_energy(rec, q, v)
+            k = 0
+            for cp in checkpoints:
+                while k < cp:
+                    oracle.step(q, v, table, 1.0)
+                    k += 1
+                gq, gv, gt = gpu[cp]
+                r = rows[cp]
+                pos_g = gq[e].reshape(-1, 7)[:, :3]
+                pos_o = q.reshape(-1, 7)[:, :3]
+                r["position_drift_m"] = max(r["position_drift_m"], float(np.abs(pos_g - pos_o).max()))
+                r["energy_drift_gpu_J"] = max(r["energy_drift_gpu_J"], abs(_stack_energy(rec, gq[e].astype(np.float64), gv[e].astype(np.float64)) - energy0))
+                r["energy_drift_oracle_J"] = max(r["energy_drift_oracle_J"], abs(_stack_energy(rec, q, v) - energy0))
+        for cp in checkpoints:
+            tab = gpu[cp][2]
+            pts = tab[:, :, 8:56].reshape(n_stack, -1, 4, 12)[..., 9:12]
+            counts = tab[:, :, 7].view(np.uint32)
+            live = np.arange(4)[None, None, :] < counts[:, :, None]
+            rows[cp]["cone_violation"] = _cone_violation_rows(pts[live], 0.6)
+        report["stack32_fp32"] = rows
+    # --- trees: FP32 and FP64 articulated inertia ---
+    gen = torch.Generator(device=device).manual_seed(SEED)
+    for precision in ("fp32", "fp64-inertia"):
+        with nb.World("tree29", n_tree, substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT, seed=SEED,
+                      precision=precision) as world:
+            rec = world.model()
+            if precision == "fp32":
+                tree_actions = 0.3 * torch.randn((checkpoints[-1], n_tree, world.action_count), device=device, generator=gen)
+            q0, v0, m0 = world.state()
+            fr = world.friction_scales()
+            gpu = {}
+            done, ms = 0, 0.0
+            for cp in checkpoints:
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                world.step(tree_actions[done:cp], wait=False)
+                e1.record()
+                torch.cuda.synchronize(device)
+                ms += e0.elapsed_time(e1)
+                done = cp
+                gpu[cp] = world.state()
+            timing[f"tree29_{precision}"] = n_tree * checkpoints[-1] / (ms / 1e3)
+            oracle = Oracle(rec, h, SUBSTEPS, ITERATIONS, 0)
+            if precision == "fp32":
+                # The FP64 replay of the subset, shared by both device modes
+                # (same reset state and actions).
+                acts_host = tree_actions[:, :subset].cpu().numpy().astype(np.float64)
+                replay = {}
+                for e in range(subset):
+                    q = q0[e].astype(np.float64)
+                    v = v0[e].astype(np.float64)
+                    man = oracle.env_manifolds(m0, e)
+                    replay[(e, 0)] = (q.copy(), v.copy())
+                    k = 0
+                    for cp in checkpoints:
+                        while k < cp:
+                            oracle.control_step(q, v, man, acts_host[k, e], float(fr[e]))
+                            k += 1
+                        replay[(e, cp)] = (q.copy(), v.copy())
+            rows = {cp: {"q_drift": 0.0, "energy_drift_gpu_J": 0.0, "energy_drift_oracle_J": 0.0, "cone_violation": 0.0}
+                    for cp in checkpoints}
+            for e in range(subset):
+                energy0 = _tree_energy(oracle, rec, *replay[(e, 0)])
+                for cp in checkpoints:
+                    q, v = replay[(e, cp)]
+                    gq, gv, _ = gpu[cp]
+                    r = rows[cp]
+                    r["q_drift"] = max(r["q_drift"], float(np.abs(gq[e] - q).max()))
+                    r["energy_drift_gpu_J"] = max(r["energy_drift_gpu_J"],
+                                                  abs(_tree_energy(oracle, rec, gq[e].astype(np.float64), gv[e].astype(np.float64)) - energy0))
+                    r["energy_drift_oracle_J"] = max(r["energy_drift_oracle_J"], abs(_tree_energy(oracle, rec, q, v) - energy0))
+            for cp in checkpoints:
+                man = gpu[cp][2]
+                imp = np.array([[list(man[i].points[p].impulses) if p < man[i].count else [0.0, 0.0, 0.0] for p in range(4)]
+                                for i in range(len(man))]).reshape(n_tree, -1, 4, 3)
+                rows[cp]["cone_violation"] = _cone_violation_rows(imp, fr[:, None, None].astype(np.float64))
+            report[f"tree29_{precision}"] = rows
+    line = {
+        "metric": "precision report (drift vs the FP64 oracle)",
+        "value": (n_stack + n_tree) * checkpoints[-1] / sum(n * checkpoints[-1] / timing[k] for k, n in
+                                                        (("stack32", n_stack), ("tree29_fp32", n_tree))),
+        "unit": UNIT,
+        "higher_is_better": True,
+        "n_gpus": 1,
+        "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": f"{n_stack} envs of 32-box stacks (0.1 m, 1 kg, mu 0.6, stack yaw U(0, 2 pi), offsets N(0, 2 mm)) "
+                               f"plus {n_tree} tree29 envs (PD targets ~ N(0, 0.3)), {checkpoints[-1]} control steps "
+                               f"= {4 * checkpoints[-1]} microsteps of 5 ms; oracle subset {subset} stacks and {subset} trees",
+                   "checkpoints_control_steps": list(checkpoints)},
+        "throughput_env_steps_per_s": timing,
+        "report": report,
+        "notes": "value: stacks and FP32 trees run one after the other; drift is the max over the subset at each checkpoint",
+    }
+    print(json.dumps(line))
+
+
 def main() -> None:
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
@@ -488,8 +672,9 @@ def main() -> None:
     parser.add_argument("--impl", default="native", choices=["native", "reference"])
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--envs", type=int, default=0, help="pile workload: environments (default 16384; smaller for profiling)")
-    parser.add_argument("--workload", default="tree29", choices=["tree29", "pile", "mix"],
-                        help="tree29 (the headline), pile (36-body piles) or mix (chains, trees and piles)")
+    parser.add_argument("--workload", default="tree29", choices=["tree29", "pile", "mix", "precision"],
+                        help="tree29 (the headline), pile (36-body piles), mix (chains, trees and piles) or "
+                             "precision (box stacks and trees against the FP64 oracle)")
     parser.add_argument("--serve", action="store_true",
                         help="serving workload: Poisson request stream, latency percentiles (one JSON line)")
     args = parser.parse_args()
@@ -509,7 +694,7 @@ def main() -> None:
         return
     if args.workload != "tree29":
         if rank == 0:
-            (run_pile if args.workload == "pile" else run_mix)(args)
+            {"pile": run_pile, "mix": run_mix, "precision": run_precision}[args.workload](args)
         return
 
     import torch
