@@ -450,7 +450,7 @@ MR_API const float* mr_task_rollout_actor_observations(const MRTaskRolloutHandle
 MR_API const float* mr_task_rollout_final_q(const MRTaskRolloutHandle* handle);
 /* reference: include/metalrobo/c_api.h:742-746.  Packed [env][scene body]
  * [position xyz, orientation xyzw, linear xyz, angular xyz]; scene bodies
- * are the non-articulated dynamic bodies (none in the synthetic worlds). */
+ * are the free bodies of the pile and stack worlds. */
 MR_API int mr_task_rollout_copy_final_scene_states(
     const MRTaskRolloutHandle* handle, float* output, size_t output_count);
 
