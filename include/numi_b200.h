@@ -596,6 +596,49 @@ MR_API int mr_server_copy_result(const MRServerHandle* server, uint64_t request_
 MR_API int mr_server_release(MRServerHandle* server, uint64_t request_id);
 MR_API int mr_server_stats(const MRServerHandle* server, MRServerStatsC* stats);
 
+/* ---------------------------------------------------------------------- */
+/* Stepping without device allocation (no counterpart in the reference)   */
+/* ---------------------------------------------------------------------- */
+
+/* Most environments one mr_pile_step_no_alloc call may step. */
+#define MR_B200_NO_ALLOC_MAX_ENVS 64u
+
+/* No counterpart in the reference.  Advances `environment_count` pile or
+ * stack environments by `control_step_count` control steps on buffers the
+ * caller owns, without allocating any device memory: for hosts that manage
+ * all GPU memory themselves (a framework's own allocator, a fixed memory
+ * budget) or cannot afford cudaMalloc's device-wide synchronisation inside
+ * their loop, and so cannot use the rollout handle, which allocates its
+ * state and workspace.  The kernel is the rollout's pile kernel; its
+ * workspace (at most MR_B200_NO_ALLOC_MAX_ENVS environments), launch
+ * counters and packed world record live in fixed device arrays of the
+ * library, about 8 MB that every GPU loading the library holds until exit.
+ *
+ * Device buffers (in/out unless noted): q [env][bodies * 7] (position,
+ * orientation xyzw), v [env][bodies * 6], manifolds [env]
+ * [MR_B200_SCENE_MANIFOLDS][MR_B200_SCENE_SLOT_WORDS] and manifold_counts
+ * [env] (all zero for fresh environments), friction_scale [env] (in),
+ * status_codes [control step][env] (out; may be null).  The body count
+ * comes from mr_compile_synthetic_model(source, model_seed).  Work is
+ * enqueued on `cuda_stream` and the call returns without waiting.
+ *
+ * The first call on a device resolves the device addresses of those arrays
+ * (with that device current); make that first call before any stream
+ * capture.  The first call for a new (source, model_seed, substep length)
+ * also compiles that world on the host and uploads its record.  Every call
+ * shares the arrays, so calls whose work overlaps on the GPU (other streams,
+ * other host threads) race with each other; nothing in the workspace needs
+ * to start at zero, since the kernel writes every word before reading it.
+ * environment_count above MR_B200_NO_ALLOC_MAX_ENVS is rejected with a
+ * message (-1). */
+MR_API int mr_pile_step_no_alloc(
+    uint32_t source, uint64_t model_seed, uint32_t environment_count,
+    float* q, float* v, float* manifolds, uint32_t* manifold_counts,
+    const float* friction_scale, uint32_t* status_codes,
+    uint32_t control_step_count, float control_timestep_seconds,
+    uint32_t physics_substeps, uint32_t velocity_iterations,
+    uint32_t final_velocity_iterations, uint64_t cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

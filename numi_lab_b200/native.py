@@ -379,6 +379,7 @@ EXPORTED_SYMBOLS: Final = (
     "mr_server_copy_result",
     "mr_server_release",
     "mr_server_stats",
+    "mr_pile_step_no_alloc",
 )
 
 
@@ -489,6 +490,9 @@ class Bindings:
         L.mr_server_release.restype = ct.c_int
         L.mr_server_stats.argtypes = [ct.c_void_p, P(ServerStatsC)]
         L.mr_server_stats.restype = ct.c_int
+        L.mr_pile_step_no_alloc.argtypes = [ct.c_uint32, ct.c_uint64, ct.c_uint32] + [ct.c_void_p] * 6 + [
+            ct.c_uint32, ct.c_float, ct.c_uint32, ct.c_uint32, ct.c_uint32, ct.c_uint64]
+        L.mr_pile_step_no_alloc.restype = ct.c_int
 
     def last_error(self) -> str:
         value = self.lib.mr_last_error()
