@@ -790,6 +790,7 @@ def main() -> None:
     peaks = _measured_peaks()
     traffic = _profile_traffic()
 
+    launch_shape = world.launch_shape()
     plain = plain_aba_chain7(device) if rank == 0 else None
 
     cpu = None
@@ -816,7 +817,7 @@ def main() -> None:
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic (seeded)",
-            "config": _config(world_size),
+            "config": {**_config(world_size), "launch": dict(zip(("envs_per_cta", "resident_envs_per_sm"), launch_shape))},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {
                 "bound": "hbm",

@@ -509,6 +509,13 @@ MR_API int mr_sample_synthetic_reset(uint32_t source, uint64_t model_seed, uint6
 MR_API int mr_task_rollout_copy_environment_parameters(
     const MRTaskRolloutHandle* handle, float* friction_scale);
 
+/* No counterpart in the reference: the control-step kernel's launch shape
+ * for the current precision mode (environments per CTA and resident
+ * environments per SM, from the occupancy query at creation; 1 and 0 for
+ * pile and stack worlds, whose kernel runs one environment per CTA). */
+MR_API int mr_task_rollout_launch_shape(const MRTaskRolloutHandle* handle, uint32_t* warps_per_block,
+                                        uint32_t* resident_warps_per_sm);
+
 /* No counterpart in the reference: copies the resident state of every
  * environment, q [env][nq], v [env][nv] and manifolds [env][pair_count];
  * any pointer may be null.  Pile worlds (scene bodies) store instead a

@@ -276,7 +276,7 @@ void numi::rt::make_plan(const numi::CompiledModel& m, float h, KernelPlan& plan
     // CTA carries one copy of the topology tables).
     for (int prec = 0; prec < 2; ++prec) {
         int best = 1, best_warps = 0;
-        for (int wpb = 1; wpb <= 4; wpb *= 2) {
+        for (int wpb = 1; wpb <= 4; ++wpb) {
             const size_t smem = tables + wpb * per_warp;
             if (smem > limit) break;
             int blocks = 0;
@@ -930,6 +930,16 @@ MR_API int mr_task_rollout_copy_environment_parameters(const MRTaskRolloutHandle
     return guarded([&] {
         if (!handle || !friction_scale) throw std::invalid_argument("handle or output is null");
         std::memcpy(friction_scale, handle->friction.data(), handle->friction.size() * sizeof(float));
+    });
+}
+
+MR_API int mr_task_rollout_launch_shape(const MRTaskRolloutHandle* handle, uint32_t* warps_per_block,
+                                        uint32_t* resident_warps_per_sm) {
+    return guarded([&] {
+        if (!handle) throw std::invalid_argument("handle is null");
+        const int prec = handle->fp64_inertia ? 1 : 0;
+        if (warps_per_block) *warps_per_block = handle->scene ? 1u : static_cast<uint32_t>(handle->warps_per_block[prec]);
+        if (resident_warps_per_sm) *resident_warps_per_sm = handle->scene ? 0u : static_cast<uint32_t>(handle->resident_warps_per_sm[prec]);
     });
 }
 

@@ -368,6 +368,7 @@ EXPORTED_SYMBOLS: Final = (
     "mr_task_rollout_copy_model",
     "mr_task_rollout_copy_environment_parameters",
     "mr_task_rollout_copy_state",
+    "mr_task_rollout_launch_shape",
     "mr_task_rollout_set_state",
     "mr_task_rollout_set_precision",
     "mr_create_server",
@@ -470,6 +471,8 @@ class Bindings:
         L.mr_task_rollout_copy_environment_parameters.restype = ct.c_int
         L.mr_task_rollout_copy_state.argtypes = [ct.c_void_p, P(ct.c_float), P(ct.c_float), ct.c_void_p]
         L.mr_task_rollout_copy_state.restype = ct.c_int
+        L.mr_task_rollout_launch_shape.argtypes = [ct.c_void_p, P(ct.c_uint32), P(ct.c_uint32)]
+        L.mr_task_rollout_launch_shape.restype = ct.c_int
         L.mr_task_rollout_set_state.argtypes = [ct.c_void_p, P(ct.c_float), P(ct.c_float), ct.c_void_p, ct.c_uint32]
         L.mr_task_rollout_set_state.restype = ct.c_int
         L.mr_create_server.argtypes = [P(ServerConfigC)]

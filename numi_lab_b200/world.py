@@ -201,6 +201,14 @@ class World:
     def layout(self) -> native.TaskRolloutLayoutC:
         return self._lib.lib.mr_task_rollout_layout(self._handle)
 
+    def launch_shape(self) -> tuple[int, int]:
+        """(environments per CTA, resident environments per SM) of the
+        control-step kernel in the current precision mode."""
+
+        wpb, res = ct.c_uint32(), ct.c_uint32()
+        self._lib.check(self._lib.lib.mr_task_rollout_launch_shape(self._handle, ct.byref(wpb), ct.byref(res)), "launch_shape")
+        return int(wpb.value), int(res.value)
+
     def device_name(self) -> str:
         name = self._lib.lib.mr_task_rollout_device_name(self._handle)
         return name.decode() if name else ""
