@@ -525,8 +525,9 @@ def _cone_violation_rows(impulses: np.ndarray, mu: np.ndarray) -> float:
 
 def run_precision(args) -> None:
     """Precision configuration: 1024 envs of 32-box stacks plus 512 29-DoF
-    trees for 10,000 microsteps (2,500 control steps of 4 x 5 ms), FP32 and,
-    for the trees, the FP64 articulated-inertia mode; a seeded subset of
+    trees for 10,000 microsteps (2,500 control steps of 4 x 5 ms) in FP32,
+    in the compensated-sum mode and, for the trees, in the FP64
+    articulated-inertia mode; a seeded subset of
     environments is replayed by the FP64 oracle (the checker) and the line
     reports position drift, energy drift and cone violation against it at
     checkpoints, beside the device throughput."""
@@ -543,36 +544,47 @@ def run_precision(args) -> None:
     h = CONTROL_DT / SUBSTEPS
     report: dict = {}
     timing: dict = {}
-    # --- stacks (free bodies; FP32) ---
-    with nb.World("stack32", n_stack, substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT, seed=SEED) as world:
-        rec = world.model()
-        q0, v0, _ = world.state()
-        acts = torch.zeros((checkpoints[-1], n_stack, 0), device=device)
-        gpu = {}
-        done, ms = 0, 0.0
-        for cp in checkpoints:
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            world.step(acts[: cp - done], wait=False)
-            e1.record()
-            torch.cuda.synchronize(device)
-            ms += e0.elapsed_time(e1)
-            done = cp
-            gpu[cp] = world.state()
-        timing["stack32"] = n_stack * checkpoints[-1] / (ms / 1e3)
-        oracle = SceneOracle(rec, h, SUBSTEPS, ITERATIONS, 0)
+    # --- stacks (free bodies): FP32 and compensated sums ---
+    oracle_rows = None
+    for precision in ("fp32", "compensated"):
+        with nb.World("stack32", n_stack, substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT, seed=SEED,
+                      precision=precision) as world:
+            rec = world.model()
+            q0, v0, _ = world.state()
+            acts = torch.zeros((checkpoints[-1], n_stack, 0), device=device)
+            gpu = {}
+            done, ms = 0, 0.0
+            for cp in checkpoints:
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                world.step(acts[: cp - done], wait=False)
+                e1.record()
+                torch.cuda.synchronize(device)
+                ms += e0.elapsed_time(e1)
+                done = cp
+                gpu[cp] = world.state()
+        timing[f"stack32_{precision}"] = n_stack * checkpoints[-1] / (ms / 1e3)
+        if oracle_rows is None:
+            # The FP64 replay of the subset, shared by both device modes.
+            oracle = SceneOracle(rec, h, SUBSTEPS, ITERATIONS, 0)
+            oracle_rows = {}
+            for e in range(subset):
+                q = q0[e].astype(np.float64)
+                v = v0[e].astype(np.float64)
+                table = SceneTable()
+                oracle_rows[(e, 0)] = (q.copy(), v.copy())
+                k = 0
+                for cp in checkpoints:
+                    while k < cp:
+                        oracle.step(q, v, table, 1.0)
+                        k += 1
+                    oracle_rows[(e, cp)] = (q.copy(), v.copy())
         rows = {cp: {"position_drift_m": 0.0, "energy_drift_gpu_J": 0.0, "energy_drift_oracle_J": 0.0, "cone_violation": 0.0}
                 for cp in checkpoints}
         for e in range(subset):
-            q = q0[e].astype(np.float64)
-            v = v0[e].astype(np.float64)
-            table = SceneTable()
-            energy0 = _stack_energy(rec, q, v)
-            k = 0
+            energy0 = _stack_energy(rec, *oracle_rows[(e, 0)])
             for cp in checkpoints:
-                while k < cp:
-                    oracle.step(q, v, table, 1.0)
-                    k += 1
+                q, v = oracle_rows[(e, cp)]
                 gq, gv, gt = gpu[cp]
                 r = rows[cp]
                 pos_g = gq[e].reshape(-1, 7)[:, :3]
@@ -586,10 +598,10 @@ def run_precision(args) -> None:
             counts = tab[:, :, 7].view(np.uint32)
             live = np.arange(4)[None, None, :] < counts[:, :, None]
             rows[cp]["cone_violation"] = _cone_violation_rows(pts[live], 0.6)
-        report["stack32_fp32"] = rows
-    # --- trees: FP32 and FP64 articulated inertia ---
+        report[f"stack32_{precision}"] = rows
+    # --- trees: FP32, FP64 articulated inertia, compensated sums ---
     gen = torch.Generator(device=device).manual_seed(SEED)
-    for precision in ("fp32", "fp64-inertia"):
+    for precision in ("fp32", "fp64-inertia", "compensated"):
         with nb.World("tree29", n_tree, substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT, seed=SEED,
                       precision=precision) as world:
             rec = world.model()
@@ -647,7 +659,7 @@ def run_precision(args) -> None:
     line = {
         "metric": "precision report (drift vs the FP64 oracle)",
         "value": (n_stack + n_tree) * checkpoints[-1] / sum(n * checkpoints[-1] / timing[k] for k, n in
-                                                        (("stack32", n_stack), ("tree29_fp32", n_tree))),
+                                                        (("stack32_fp32", n_stack), ("tree29_fp32", n_tree))),
         "unit": UNIT,
         "higher_is_better": True,
         "n_gpus": 1,
@@ -659,7 +671,8 @@ def run_precision(args) -> None:
                    "checkpoints_control_steps": list(checkpoints)},
         "throughput_env_steps_per_s": timing,
         "report": report,
-        "notes": "value: stacks and FP32 trees run one after the other; drift is the max over the subset at each checkpoint",
+        "notes": "value: FP32 stacks and FP32 trees run one after the other; drift is the max over the subset at each "
+                 "checkpoint; compensated = FP64 articulated inertia plus Kahan position and impulse sums",
     }
     print(json.dumps(line))
 

@@ -458,15 +458,23 @@ MR_API int mr_task_rollout_copy_final_scene_states(
 /* Additions of this library                                               */
 /* ---------------------------------------------------------------------- */
 
-/* No counterpart in the reference: arithmetic precision of the articulated
- * inertia.  MR_PRECISION_FP32 (default) keeps the whole microstep in FP32 like
- * the reference; MR_PRECISION_FP64_ARTICULATED_INERTIA carries the
- * articulated inertias, their joint pivots and the floating root's 6x6
- * factorisation in FP64 (state, contacts and the cone solve stay FP32).
- * Applies to the next advance. */
+/* No counterpart in the reference: arithmetic precision of the microstep.
+ * MR_PRECISION_FP32 (default) keeps the whole microstep in FP32 like the
+ * reference; MR_PRECISION_FP64_ARTICULATED_INERTIA carries the articulated
+ * inertias, their joint pivots and the floating root's 6x6 factorisation in
+ * FP64 (state, contacts and the cone solve stay FP32);
+ * MR_PRECISION_COMPENSATED adds to that compensated (Kahan) FP32 sums for the
+ * position integration -- joint coordinates, the floating root's and free
+ * bodies' positions, whose compensation terms persist across control steps
+ * beside the resident state -- and for the impulse accumulation of the cone
+ * solve's sweeps.  Piles and stacks have no articulated inertia: there the
+ * FP64 mode equals FP32 and the compensated mode adds only the sums.
+ * Applies to the next advance; a change of mode, a reset and set_state
+ * clear the compensation terms. */
 enum MRPrecisionModeC {
     MR_PRECISION_FP32 = 0u,
-    MR_PRECISION_FP64_ARTICULATED_INERTIA = 1u
+    MR_PRECISION_FP64_ARTICULATED_INERTIA = 1u,
+    MR_PRECISION_COMPENSATED = 2u
 };
 MR_API int mr_task_rollout_set_precision(MRTaskRolloutHandle* handle, uint32_t mode);
 

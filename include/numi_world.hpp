@@ -49,7 +49,11 @@ struct WorldBatch {
     std::size_t reset_mask_count = 0;
 };
 
-enum class PrecisionMode : std::uint32_t { fp32 = MR_PRECISION_FP32, fp64_articulated_inertia = MR_PRECISION_FP64_ARTICULATED_INERTIA };
+enum class PrecisionMode : std::uint32_t {
+    fp32 = MR_PRECISION_FP32,
+    fp64_articulated_inertia = MR_PRECISION_FP64_ARTICULATED_INERTIA,
+    compensated = MR_PRECISION_COMPENSATED
+};
 
 struct WorldStepConfig {
     float timestep_seconds = 0.02f;  // control period

@@ -147,6 +147,7 @@ struct StepParams {
     std::int32_t substeps;
     std::int32_t velocity_iterations;
     std::int32_t final_velocity_iterations;
+    float* q_comp;                 // [env][nq] compensation terms of q's running sums (compensated precision), or null
 };
 
 enum StatIndex : int {

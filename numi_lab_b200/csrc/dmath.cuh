@@ -110,4 +110,18 @@ __device__ __forceinline__ unsigned warp_umin(unsigned x) {
     return x;
 }
 
+// Compensated running sum x + a * b (Kahan's summation): `c` carries the
+// low-order part that earlier additions to x rounded away; the product
+// arrives with c subtracted in one rounding.  The explicit _rn intrinsics
+// keep the correction from being contracted or reassociated.
+__device__ __forceinline__ float kahan_madd(float x, float a, float b, float& c) {
+    const float y = __fmaf_rn(a, b, -c);
+    const float t = __fadd_rn(x, y);
+    c = __fsub_rn(__fsub_rn(t, x), y);
+    return t;
+}
+__device__ __forceinline__ float3 kahan_madd3(float3 x, float a, float3 b, float* c) {
+    return f3(kahan_madd(x.x, a, b.x, c[0]), kahan_madd(x.y, a, b.y, c[1]), kahan_madd(x.z, a, b.z, c[2]));
+}
+
 }  // namespace numi

@@ -41,6 +41,7 @@ struct WarpLayout {
     int misc;
     int manifolds, contacts, G, L, z, margins, pair_stats;
     int narrow;  // narrowphase scratch; aliases the contact records and rows
+    int qcomp;   // compensation terms of q's running sums (compensated precision only)
     int total;   // floats per warp
 };
 
@@ -57,8 +58,10 @@ __host__ __device__ inline int pair_max_raw(int pair_class) {
 }
 
 // `narrow_words` is the sum of pair_scratch_words over the compiled pairs.
+// `compensated` appends the q compensation section (the other sections keep
+// their offsets).
 __host__ __device__ inline WarpLayout make_layout(int nb, int nv, int nq, int np, int ncap, int max_anc, int narrow_words,
-                                                  bool contact) {
+                                                  bool contact, bool compensated = false) {
     WarpLayout L{};
     int o = 0;
     auto take = [&o](int words) { const int at = o; o += align4(words); return at; };
@@ -93,6 +96,7 @@ __host__ __device__ inline WarpLayout make_layout(int nb, int nv, int nq, int np
     } else {
         L.manifolds = L.contacts = L.G = L.L = L.narrow = L.pair_stats = o;
     }
+    L.qcomp = compensated ? take(nq) : o;
     L.total = align4(o);
     return L;
 }

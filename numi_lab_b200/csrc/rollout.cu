@@ -258,29 +258,32 @@ void numi::rt::make_plan(const numi::CompiledModel& m, float h, KernelPlan& plan
     plan.dmodel = pack_model(m, h);
     int narrow_words = 0;
     for (const MRModelPairC& pr : m.pairs) narrow_words += numi::pair_scratch_words(numi::pair_max_raw(static_cast<int>(pr.pair_class)));
-    plan.layout = numi::make_layout(static_cast<int>(m.articulated_body_count), static_cast<int>(m.world.nv),
-                                    static_cast<int>(m.world.nq), static_cast<int>(m.world.pair_count),
-                                    static_cast<int>(m.world.contact_capacity), static_cast<int>(m.max_ancestor_dofs),
-                                    narrow_words, plan.contact);
+    for (const bool compensated : {false, true})
+        (compensated ? plan.layout_comp : plan.layout) =
+            numi::make_layout(static_cast<int>(m.articulated_body_count), static_cast<int>(m.world.nv),
+                              static_cast<int>(m.world.nq), static_cast<int>(m.world.pair_count),
+                              static_cast<int>(m.world.contact_capacity), static_cast<int>(m.max_ancestor_dofs),
+                              narrow_words, plan.contact, compensated);
     int device = 0;
     check(cudaGetDevice(&device), "cudaGetDevice");
     cudaDeviceProp prop{};
     check(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
-    const size_t per_warp = static_cast<size_t>(plan.layout.total) * sizeof(float);
     const size_t tables = numi::control_step_table_bytes();
     const size_t limit = prop.sharedMemPerBlockOptin;
-    if (tables + per_warp > limit) throw std::runtime_error("per-environment shared memory exceeds the device limit");
+    if (tables + static_cast<size_t>(plan.layout.total) * sizeof(float) > limit)
+        throw std::runtime_error("per-environment shared memory exceeds the device limit");
     check(numi::configure_control_step_kernels(limit), "kernel attributes");
     // Environments per CTA: the choice that keeps the most warps resident
     // per SM under the kernel's register and shared-memory footprint (each
     // CTA carries one copy of the topology tables).
-    for (int prec = 0; prec < 2; ++prec) {
+    for (std::uint32_t prec = 0; prec < static_cast<std::uint32_t>(numi::rt::kPrecisionModes); ++prec) {
+        const size_t per_warp = static_cast<size_t>(plan.layout_for(prec).total) * sizeof(float);
         int best = 1, best_warps = 0;
         for (int wpb = 1; wpb <= 4; ++wpb) {
             const size_t smem = tables + wpb * per_warp;
             if (smem > limit) break;
             int blocks = 0;
-            check(numi::control_step_occupancy(plan.contact, prec == 1, wpb, smem, &blocks), "occupancy query");
+            check(numi::control_step_occupancy(plan.contact, prec, wpb, smem, &blocks), "occupancy query");
             if (blocks * wpb > best_warps) { best_warps = blocks * wpb; best = wpb; }
         }
         if (best_warps == 0) throw std::runtime_error("the control-step kernel cannot be resident with this model");
@@ -352,15 +355,16 @@ struct MRTaskRolloutHandle {
     numi::CompiledModel model;
     numi::DeviceModel dmodel{};
     numi::WarpLayout layout{};
+    numi::WarpLayout layout_comp{};     // with the q compensation section
     bool contact = false;
     bool scene = false;                 // free-body pile world (scene_step kernel)
     numi::SceneModel smodel{};
     DeviceBuffer<numi::SceneModel> d_smodel;
     DeviceBuffer<std::uint32_t> d_mcount;
     DeviceBuffer<float> d_workspace;    // scene substep tables, contacts, narrowphase scratch
-    bool fp64_inertia = false;          // MR_PRECISION_FP64_ARTICULATED_INERTIA
-    int warps_per_block[2] = {1, 1};    // per precision (FP32, FP64 inertia)
-    int resident_warps_per_sm[2] = {0, 0};
+    std::uint32_t precision = MR_PRECISION_FP32;  // MRPrecisionModeC
+    int warps_per_block[numi::rt::kPrecisionModes] = {1, 1, 1};  // per precision mode
+    int resident_warps_per_sm[numi::rt::kPrecisionModes] = {0, 0, 0};
     MRTaskRolloutConfigC config{};
     std::uint32_t envs = 0;
     float h = 0.0f;
@@ -374,6 +378,7 @@ struct MRTaskRolloutHandle {
 
     DeviceBuffer<numi::DeviceModel> d_model;
     DeviceBuffer<float> d_q, d_v, d_manifolds, d_reset_q, d_reset_v, d_friction;
+    DeviceBuffer<float> d_qcomp;        // [env][nq] compensation of q's running sums (compensated precision)
     DeviceBuffer<float> d_actions, d_obs;
     DeviceBuffer<std::uint32_t> d_masks, d_status, d_contacts, d_stats;
     PinnedBuffer<float> h_actions, h_obs, h_final_q;
@@ -388,10 +393,10 @@ struct MRTaskRolloutHandle {
         const void* obs;
         const void* status;
         const void* contacts;
-        bool fp64_inertia;
+        std::uint32_t precision;
         bool operator<(const GraphKey& o) const {
-            return std::tie(steps, actions, masks, obs, status, contacts, fp64_inertia) <
-                   std::tie(o.steps, o.actions, o.masks, o.obs, o.status, o.contacts, o.fp64_inertia);
+            return std::tie(steps, actions, masks, obs, status, contacts, precision) <
+                   std::tie(o.steps, o.actions, o.masks, o.obs, o.status, o.contacts, o.precision);
         }
     };
     std::map<GraphKey, cudaGraphExec_t> graphs;
@@ -424,7 +429,14 @@ struct MRTaskRolloutHandle {
         check(cudaMemcpyAsync(d_v.ptr, d_reset_v.ptr, reset_v.size() * sizeof(float), cudaMemcpyDeviceToDevice, stream), "init v");
         if (d_manifolds.count) check(cudaMemsetAsync(d_manifolds.ptr, 0, d_manifolds.count * sizeof(float), stream), "clear manifolds");
         if (d_mcount.count) check(cudaMemsetAsync(d_mcount.ptr, 0, d_mcount.count * sizeof(std::uint32_t), stream), "clear manifold counts");
+        clear_compensation();
         check(cudaStreamSynchronize(stream), "reset");
+    }
+
+    // The compensation terms belong to the state they were accumulated on:
+    // any new state starts without them.
+    void clear_compensation() {
+        if (d_qcomp.count) check(cudaMemsetAsync(d_qcomp.ptr, 0, d_qcomp.count * sizeof(float), stream), "clear compensation");
     }
 
     size_t manifold_words() const {
@@ -460,6 +472,7 @@ struct MRTaskRolloutHandle {
                 p.substeps = static_cast<int>(config.physics_substeps);
                 p.velocity_iterations = static_cast<int>(config.velocity_iterations);
                 p.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
+                p.q_comp = precision == MR_PRECISION_COMPENSATED ? d_qcomp.ptr : nullptr;
                 check(numi::launch_scene_step(p, s), "scene step launch");
             }
             (void)actions;
@@ -485,14 +498,16 @@ struct MRTaskRolloutHandle {
             p.substeps = static_cast<int>(config.physics_substeps);
             p.velocity_iterations = static_cast<int>(config.velocity_iterations);
             p.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
-            check(numi::launch_control_step(p, layout, contact, fp64_inertia, warps_per_block[fp64_inertia ? 1 : 0], s),
+            p.q_comp = precision == MR_PRECISION_COMPENSATED ? d_qcomp.ptr : nullptr;
+            check(numi::launch_control_step(p, precision == MR_PRECISION_COMPENSATED ? layout_comp : layout, contact, precision,
+                                            warps_per_block[precision], s),
                   "control step launch");
         }
     }
 
     void run(std::uint32_t steps, const float* actions, const std::uint32_t* masks, float* obs, std::uint32_t* status,
              std::uint32_t* contacts, cudaStream_t s) {
-        const GraphKey key{steps, actions, masks, obs, status, contacts, fp64_inertia};
+        const GraphKey key{steps, actions, masks, obs, status, contacts, precision};
         auto it = graphs.find(key);
         if (it == graphs.end()) {
             cudaGraph_t graph = nullptr;
@@ -628,7 +643,8 @@ MR_API MRTaskRolloutHandle* mr_create_task_rollout(const MRRunManifestC* manifes
             h.contact = plan.contact;
             h.dmodel = plan.dmodel;
             h.layout = plan.layout;
-            for (int prec = 0; prec < 2; ++prec) {
+            h.layout_comp = plan.layout_comp;
+            for (int prec = 0; prec < numi::rt::kPrecisionModes; ++prec) {
                 h.warps_per_block[prec] = plan.warps_per_block[prec];
                 h.resident_warps_per_sm[prec] = plan.resident_warps_per_sm[prec];
             }
@@ -657,6 +673,7 @@ MR_API MRTaskRolloutHandle* mr_create_task_rollout(const MRRunManifestC* manifes
         h.d_reset_q.resize(h.envs * nq);
         h.d_reset_v.resize(h.envs * nv);
         h.d_friction.resize(h.envs);
+        h.d_qcomp.resize(h.envs * nq);
         if (h.contact) h.d_manifolds.resize(h.envs * h.manifold_words());
         h.d_stats.resize(numi::kStatCount);
         h.h_stats.resize(numi::kStatCount);
@@ -707,9 +724,12 @@ MR_API int mr_task_rollout_set_state_readback(MRTaskRolloutHandle* handle, uint3
 MR_API int mr_task_rollout_set_precision(MRTaskRolloutHandle* handle, uint32_t mode) {
     return guarded([&] {
         if (!handle) throw std::invalid_argument("handle is null");
-        if (mode != MR_PRECISION_FP32 && mode != MR_PRECISION_FP64_ARTICULATED_INERTIA)
+        if (mode != MR_PRECISION_FP32 && mode != MR_PRECISION_FP64_ARTICULATED_INERTIA && mode != MR_PRECISION_COMPENSATED)
             throw std::invalid_argument("unknown precision mode " + std::to_string(mode));
-        handle->fp64_inertia = mode == MR_PRECISION_FP64_ARTICULATED_INERTIA;
+        // Compensation terms accumulated before a change of mode do not
+        // describe the state the new mode starts from.
+        if (mode != handle->precision) handle->clear_compensation();
+        handle->precision = mode;
     });
 }
 
@@ -937,7 +957,7 @@ MR_API int mr_task_rollout_launch_shape(const MRTaskRolloutHandle* handle, uint3
                                         uint32_t* resident_warps_per_sm) {
     return guarded([&] {
         if (!handle) throw std::invalid_argument("handle is null");
-        const int prec = handle->fp64_inertia ? 1 : 0;
+        const std::uint32_t prec = handle->precision;
         if (warps_per_block) *warps_per_block = handle->scene ? 1u : static_cast<uint32_t>(handle->warps_per_block[prec]);
         if (resident_warps_per_sm) *resident_warps_per_sm = handle->scene ? 0u : static_cast<uint32_t>(handle->resident_warps_per_sm[prec]);
     });
@@ -966,6 +986,7 @@ MR_API int mr_task_rollout_set_state(MRTaskRolloutHandle* handle, const float* q
         check(cudaStreamSynchronize(h.stream), "sync");
         check(cudaMemcpy(h.d_q.ptr, q, nq * sizeof(float), cudaMemcpyHostToDevice), "q H2D");
         check(cudaMemcpy(h.d_v.ptr, v, nv * sizeof(float), cudaMemcpyHostToDevice), "v H2D");
+        h.clear_compensation();
         if (h.contact) {
             if (manifolds)
                 check(cudaMemcpy(h.d_manifolds.ptr, manifolds, static_cast<size_t>(h.envs) * h.manifold_words() * sizeof(float),

@@ -17,9 +17,11 @@
 
 namespace numi {
 
-cudaError_t control_step_occupancy(bool contact, bool fp64_inertia, int warps_per_block, size_t smem, int* blocks_per_sm);
-cudaError_t launch_control_step(const StepParams& p, const WarpLayout& layout, bool contact, bool fp64_inertia, int warps_per_block,
-                                cudaStream_t stream);
+// `precision` is an MRPrecisionModeC value; MR_PRECISION_COMPENSATED needs
+// p.q_comp and the layout made with its compensation section.
+cudaError_t control_step_occupancy(bool contact, std::uint32_t precision, int warps_per_block, size_t smem, int* blocks_per_sm);
+cudaError_t launch_control_step(const StepParams& p, const WarpLayout& layout, bool contact, std::uint32_t precision,
+                                int warps_per_block, cudaStream_t stream);
 cudaError_t configure_control_step_kernels(size_t max_dynamic_smem);
 size_t control_step_table_bytes();
 
@@ -86,12 +88,17 @@ int guarded(F&& f) {
 // Everything the control-step kernel needs to know about a compiled model
 // at one substep length: the packed device record, the per-warp
 // shared-memory layout and the launch shape per precision mode.
+constexpr int kPrecisionModes = 3;       // indexed by MRPrecisionModeC
 struct KernelPlan {
     DeviceModel dmodel{};
-    WarpLayout layout{};
+    WarpLayout layout{};                 // FP32 and FP64 articulated inertia
+    WarpLayout layout_comp{};            // compensated: layout plus the q compensation section
     bool contact = false;
-    int warps_per_block[2] = {1, 1};     // FP32, FP64 articulated inertia
-    int resident_warps_per_sm[2] = {0, 0};
+    int warps_per_block[kPrecisionModes] = {1, 1, 1};
+    int resident_warps_per_sm[kPrecisionModes] = {0, 0, 0};
+    const WarpLayout& layout_for(std::uint32_t precision) const {
+        return precision == MR_PRECISION_COMPENSATED ? layout_comp : layout;
+    }
 };
 
 DeviceModel pack_model(const CompiledModel& m, float h);

@@ -77,9 +77,10 @@ struct SceneParams {
     std::int32_t substeps;
     std::int32_t velocity_iterations;
     std::int32_t final_velocity_iterations;
+    float* q_comp;             // [slot][nb][7]: compensation of the position sums (entries 0-2), or null (FP32 sums)
 };
 
-size_t scene_step_smem_bytes();
+size_t scene_step_smem_bytes(bool compensated = false);
 size_t scene_workspace_words();
 cudaError_t configure_scene_step_kernel();
 cudaError_t launch_scene_step(const SceneParams& p, cudaStream_t stream);

@@ -63,6 +63,13 @@ constexpr int kOffKeys = kOffLists + 2 * (kSceneMaxBodies + 1);  // pair keys of
 constexpr int kOffFirst = kOffKeys + 2 * kSceneManifolds;  // first contact of each manifold (u16, +1)
 constexpr int kOffMisc = kOffFirst + (kSceneManifolds + 2) / 2;
 constexpr int kSceneSmemWords = kOffMisc + 32;
+// Compensated precision only, past the FP32 layout: compensation terms of
+// the body positions' running sums (persistent, [env][body][7] entries 0-2
+// in HBM) and of the substep's velocity sums over the Jacobi sweeps.
+constexpr int kOffPosComp = kSceneSmemWords;
+constexpr int kOffLinComp = kOffPosComp + kSceneMaxBodies * 3;
+constexpr int kOffAngComp = kOffLinComp + kSceneMaxBodies * 3;
+constexpr int kSceneSmemWordsComp = kOffAngComp + kSceneMaxBodies * 3;
 
 // Global workspace of one environment (floats, L2-resident while the
 // environment runs): two substep manifold tables, the contact records and
@@ -783,6 +790,9 @@ __device__ __forceinline__ float3 sym3_mul(const float* S, float3 x) {
 
 // At most 128 registers: 16 resident warps per SM.  More warps (96
 // registers) ran slower: their narrowphase scratch no longer fits the L1.
+// kComp: compensated sums for positions (across control steps, through
+// p.q_comp) and for the velocity increments of the sweeps.
+template <bool kComp>
 __global__ void __launch_bounds__(32, 16) scene_step_kernel(SceneParams p) {
     extern __shared__ float4 smem4[];
     float* s = reinterpret_cast<float*>(smem4);
@@ -804,6 +814,7 @@ __global__ void __launch_bounds__(32, 16) scene_step_kernel(SceneParams p) {
         st4(s + kOffQuat + b * 4, ld4(srcq + b * 7 + 3));
         st3(s + kOffLin + b * 3, ld3(srcv + b * 6));
         st3(s + kOffAng + b * 3, ld3(srcv + b * 6 + 3));
+        if (kComp) st3(s + kOffPosComp + b * 3, reset ? f3(0.0f, 0.0f, 0.0f) : ld3(p.q_comp + static_cast<size_t>(env) * nq + b * 7));
     }
     // Manifold table (sorted by pair key); a reset clears it.  Substeps
     // alternate between the two workspace tables; the environment's own
@@ -1229,6 +1240,12 @@ __global__ void __launch_bounds__(32, 16) scene_step_kernel(SceneParams p) {
         }
         __syncwarp();
         // Jacobi sweeps (sweep -1 applies the warm start).
+        if (kComp) {
+            for (int i = lane; i < nb * 3; i += 32) {
+                s[kOffLinComp + i] = 0.0f;
+                s[kOffAngComp + i] = 0.0f;
+            }
+        }
         const int iters = p.velocity_iterations + (final_substep ? p.final_velocity_iterations : 0);
         for (int it = -1; it < iters; ++it) {
             if (it >= 0) {
@@ -1268,8 +1285,14 @@ __global__ void __launch_bounds__(32, 16) scene_step_kernel(SceneParams p) {
                     dw = dw + cross3(cr.v3(side ? kScRb : kScRa), f);
                 }
                 const float im = M.mass[b].y;
-                st3(s + kOffLin + b * 3, ld3(s + kOffLin + b * 3) + im * dl);
-                st3(s + kOffAng + b * 3, ld3(s + kOffAng + b * 3) + sym3_mul(s + kOffIiw + b * 6, dw));
+                if (kComp) {
+                    st3(s + kOffLin + b * 3, kahan_madd3(ld3(s + kOffLin + b * 3), im, dl, s + kOffLinComp + b * 3));
+                    st3(s + kOffAng + b * 3,
+                        kahan_madd3(ld3(s + kOffAng + b * 3), 1.0f, sym3_mul(s + kOffIiw + b * 6, dw), s + kOffAngComp + b * 3));
+                } else {
+                    st3(s + kOffLin + b * 3, ld3(s + kOffLin + b * 3) + im * dl);
+                    st3(s + kOffAng + b * 3, ld3(s + kOffAng + b * 3) + sym3_mul(s + kOffIiw + b * 6, dw));
+                }
             }
             __syncwarp();
         }
@@ -1290,7 +1313,8 @@ __global__ void __launch_bounds__(32, 16) scene_step_kernel(SceneParams p) {
             const float ls = len3(lin), ws = len3(ang);
             if (vmax > 0.0f && ls > vmax) lin = lin * (vmax / ls);
             if (wmax > 0.0f && ws > wmax) ang = ang * (wmax / ws);
-            const float3 c = ld3(s + kOffPos + b * 3) + h * lin;
+            const float3 c = kComp ? kahan_madd3(ld3(s + kOffPos + b * 3), h, lin, s + kOffPosComp + b * 3)
+                                   : ld3(s + kOffPos + b * 3) + h * lin;
             float4 q = qmul(so3_increment(h * ang, false), ld4(s + kOffQuat + b * 4));
             const float qq = qdot(q, q);
             if (!finite4(q) || !(qq > 1.0e-12f) || !finite3(c) || !finite3(lin) || !finite3(ang)) {
@@ -1319,6 +1343,7 @@ __global__ void __launch_bounds__(32, 16) scene_step_kernel(SceneParams p) {
             st4(qd + b * 7 + 3, ld4(s + kOffQuat + b * 4));
             st3(vd + b * 6, ld3(s + kOffLin + b * 3));
             st3(vd + b * 6 + 3, ld3(s + kOffAng + b * 3));
+            if (kComp) st3(p.q_comp + static_cast<size_t>(env) * nq + b * 7, ld3(s + kOffPosComp + b * 3));
         }
         if (cur_table != persistent)
             for (int i = lane; i < mcount * kSceneSlotWords; i += 32) persistent[i] = cur_table[i];
@@ -1330,6 +1355,8 @@ __global__ void __launch_bounds__(32, 16) scene_step_kernel(SceneParams p) {
     } else if (reset) {
         for (int i = lane; i < nq; i += 32) qd[i] = srcq[i];
         for (int i = lane; i < nv; i += 32) vd[i] = srcv[i];
+        if (kComp)
+            for (int b = lane; b < nb; b += 32) st3(p.q_comp + static_cast<size_t>(env) * nq + b * 7, f3(0.0f, 0.0f, 0.0f));
         if (lane == 0) {
             p.manifold_count[env] = 0u;
             p.manifolds[static_cast<size_t>(env) * kTableWords + 7] = af(0);
@@ -1359,18 +1386,27 @@ __global__ void __launch_bounds__(32, 16) scene_step_kernel(SceneParams p) {
 
 }  // namespace
 
-size_t scene_step_smem_bytes() { return static_cast<size_t>(kSceneSmemWords) * sizeof(float); }
+size_t scene_step_smem_bytes(bool compensated) {
+    return static_cast<size_t>(compensated ? kSceneSmemWordsComp : kSceneSmemWords) * sizeof(float);
+}
 size_t scene_workspace_words() { return static_cast<size_t>(kWsWords); }
 
 cudaError_t configure_scene_step_kernel() {
     // The driver's default carveout keeps most of the unified L1 as cache,
     // which the narrowphase scratch and contact records rely on.
-    return cudaFuncSetAttribute(scene_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(scene_step_smem_bytes()));
+    cudaError_t e = cudaFuncSetAttribute(scene_step_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(scene_step_smem_bytes(false)));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(scene_step_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(scene_step_smem_bytes(true)));
+    return e;
 }
 
 cudaError_t launch_scene_step(const SceneParams& p, cudaStream_t stream) {
-    scene_step_kernel<<<p.env_count, 32, scene_step_smem_bytes(), stream>>>(p);
+    if (p.q_comp != nullptr)
+        scene_step_kernel<true><<<p.env_count, 32, scene_step_smem_bytes(true), stream>>>(p);
+    else
+        scene_step_kernel<false><<<p.env_count, 32, scene_step_smem_bytes(false), stream>>>(p);
     return cudaGetLastError();
 }
 

@@ -589,7 +589,8 @@ __device__ bool aba(const Warp& w, const BodyConst& bc, BodyState<R>& st, float*
 
 // Free-motion commit of the ABA candidate (ArticulatedABA.metal:1466-1540):
 // v' = v_free, joints q' = q + h v', root exponential map with the angle
-// reduced modulo 2 pi.
+// reduced modulo 2 pi.  kComp: joint and root positions as compensated sums.
+template <bool kComp>
 __device__ bool integrate_free(const Warp& w) {
     const DeviceModel& M = *w.M;
     const WarpLayout& L = *w.L;
@@ -597,20 +598,25 @@ __device__ bool integrate_free(const Warp& w) {
     float* misc = s + L.misc;
     float* q = s + L.q;
     float* v = s + L.v;
+    float* qc = s + L.qcomp;
     const float* vf = s + L.vf;
     for (int d = w.lane; d < M.nv; d += 32) {
         v[d] = vf[d];
         const int qi = M.dof_q[d];
         if (qi >= 0 && !(M.floating && d < 6)) {
-            const float nq = q[qi] + M.h * vf[d];
+            const float nq = kComp ? kahan_madd(q[qi], M.h, vf[d], qc[qi]) : q[qi] + M.h * vf[d];
             if (!isfinite(nq)) set_status(misc, MR_STEP_NONFINITE_RESULT, static_cast<unsigned>(qi));
             q[qi] = nq;
         }
     }
     if (M.floating && w.lane == 0) {
-        q[0] += M.h * vf[0];
-        q[1] += M.h * vf[1];
-        q[2] += M.h * vf[2];
+        if (kComp) {
+            for (int i = 0; i < 3; ++i) q[i] = kahan_madd(q[i], M.h, vf[i], qc[i]);
+        } else {
+            q[0] += M.h * vf[0];
+            q[1] += M.h * vf[1];
+            q[2] += M.h * vf[2];
+        }
         const float4 inc = so3_increment(M.h * f3(vf[3], vf[4], vf[5]), true);
         float4 out;
         if (!qnormalize(qmul(inc, make_float4(q[3], q[4], q[5], q[6])), out, false)) {
@@ -1344,7 +1350,7 @@ __device__ void group_manifold(const DeviceModel& M, const float* pose, const fl
 // Contact substep after the ABA: collision, ConstraintIR evaluation, joint
 // inertia factor, temporalCone solve, joint limits, integration.
 // ---------------------------------------------------------------------------
-template <typename R>
+template <bool kComp, typename R>
 __device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState<R>& st, bool final_substep,
                                 int velocity_iterations, int final_iterations, float friction_scale) {
     const DeviceModel& M = *w.M;
@@ -1688,6 +1694,7 @@ __device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState<R>
         // Jacobi sweeps: lane per contact proposes from u = u_free + Y^T z,
         // lane per DoF accumulates z += Y delta.  Sweep -1 applies the warm start.
         const int iters = velocity_iterations + (final_substep ? final_iterations : 0);
+        float zcomp[2] = {0.0f, 0.0f};  // kComp: compensation of the z sums
         for (int it = -1; it < iters; ++it) {
             if (it >= 0 && lane < total) {
                 float* c = C + lane * kContactWords;
@@ -1737,7 +1744,8 @@ __device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState<R>
                         acc = fmaf(yj[ma], cj[kCwDelta + 1], acc);
                         acc = fmaf(yj[2 * ma], cj[kCwDelta + 2], acc);
                     }
-                    z[d] += acc;
+                    if (kComp) z[d] = kahan_madd(z[d], 1.0f, acc, zcomp[pass]);
+                    else z[d] += acc;
                 }
             }
             __syncwarp();
@@ -1814,14 +1822,19 @@ __device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState<R>
     __syncwarp();
     // Integration from the substep-start configuration
     // (mr_world_integrate_contact_state; no angle reduction).
+    float* qc = s + L.qcomp;
     for (int d = lane; d < nv; d += 32) {
         const int qi = M.dof_q[d];
-        if (qi >= 0 && !(M.floating && d < 6)) q[qi] = q[qi] + h * v[d];
+        if (qi >= 0 && !(M.floating && d < 6)) q[qi] = kComp ? kahan_madd(q[qi], h, v[d], qc[qi]) : q[qi] + h * v[d];
     }
     if (M.floating && lane == 0) {
-        q[0] += h * v[0];
-        q[1] += h * v[1];
-        q[2] += h * v[2];
+        if (kComp) {
+            for (int i = 0; i < 3; ++i) q[i] = kahan_madd(q[i], h, v[i], qc[i]);
+        } else {
+            q[0] += h * v[0];
+            q[1] += h * v[1];
+            q[2] += h * v[2];
+        }
         const float4 inc = so3_increment(h * f3(v[3], v[4], v[5]), false);
         const float4 prod = qmul(inc, make_float4(q[3], q[4], q[5], q[6]));
         if (!finite4(prod) || !(qdot(prod, prod) > 1.0e-12f)) {
@@ -1837,7 +1850,9 @@ __device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState<R>
     return warp_ok(misc);
 }
 
-template <bool kContact, typename R>
+// kComp (compensated precision): q's running sums carry compensation terms
+// in the layout's qcomp section, loaded from and committed to p.q_comp.
+template <bool kContact, typename R, bool kComp>
 __global__ void __launch_bounds__(128, 3) control_step_kernel(StepParams p, WarpLayout layout, int warps_per_block) {
     extern __shared__ float4 smem4[];
     // Topology tables: one copy per CTA.
@@ -1880,6 +1895,10 @@ __global__ void __launch_bounds__(128, 3) control_step_kernel(StepParams p, Warp
         s[layout.vc + i] = x;
         s[layout.tgt + i] = 0.0f;
     }
+    if (kComp) {
+        const float* srcc = p.q_comp + static_cast<size_t>(env) * nq;
+        for (int i = lane; i < nq; i += 32) s[layout.qcomp + i] = reset ? 0.0f : srcc[i];
+    }
     misc[lane] = 0.0f;
     __syncwarp();
     for (int a = lane; a < M.action_count; a += 32)
@@ -1908,10 +1927,10 @@ __global__ void __launch_bounds__(128, 3) control_step_kernel(StepParams p, Warp
         bool ok = aba(w, bc, st, kContact ? s + layout.L : nullptr);
         if (ok) {
             if (kContact)
-                ok = contact_substep(w, bc, st, sub + 1 == p.substeps, p.velocity_iterations, p.final_velocity_iterations,
-                                     friction_scale);
+                ok = contact_substep<kComp>(w, bc, st, sub + 1 == p.substeps, p.velocity_iterations,
+                                            p.final_velocity_iterations, friction_scale);
             else
-                ok = integrate_free(w);
+                ok = integrate_free<kComp>(w);
         }
         if (!ok) break;
     }
@@ -1932,6 +1951,11 @@ __global__ void __launch_bounds__(128, 3) control_step_kernel(StepParams p, Warp
         const float x = vsrc[i];
         vd[i] = x;
         if (obs) obs[nq + i] = x;
+    }
+    if (kComp && (success || reset)) {
+        // A failed step keeps the step-start terms (a failed reset, zeros).
+        float* cd = p.q_comp + static_cast<size_t>(env) * nq;
+        for (int i = lane; i < nq; i += 32) cd[i] = success ? s[layout.qcomp + i] : 0.0f;
     }
     if (kContact && (success || reset)) {
         const int words = M.np * kManifoldWords;
@@ -1966,42 +1990,61 @@ __global__ void __launch_bounds__(128, 3) control_step_kernel(StepParams p, Warp
 size_t control_step_table_bytes() { return sizeof(DeviceTables); }
 
 // Host launcher: one control step of `env_count` environments.
-// `fp64_inertia` selects the FP64 articulated-inertia kernels.
-cudaError_t launch_control_step(const StepParams& p, const WarpLayout& layout, bool contact, bool fp64_inertia,
+// `precision` (MRPrecisionModeC) selects the kernel instance: FP32, FP64
+// articulated inertia, or FP64 articulated inertia with compensated sums.
+cudaError_t launch_control_step(const StepParams& p, const WarpLayout& layout, bool contact, std::uint32_t precision,
                                 int warps_per_block, cudaStream_t stream) {
     const int blocks = (p.env_count + warps_per_block - 1) / warps_per_block;
     const size_t smem = sizeof(DeviceTables) + static_cast<size_t>(layout.total) * sizeof(float) * warps_per_block;
     const int threads = 32 * warps_per_block;
+    if (precision == MR_PRECISION_COMPENSATED && p.q_comp == nullptr) return cudaErrorInvalidValue;
+#define NUMI_LAUNCH(C, R, K) control_step_kernel<C, R, K><<<blocks, threads, smem, stream>>>(p, layout, warps_per_block)
     if (contact) {
-        if (fp64_inertia) control_step_kernel<true, double><<<blocks, threads, smem, stream>>>(p, layout, warps_per_block);
-        else control_step_kernel<true, float><<<blocks, threads, smem, stream>>>(p, layout, warps_per_block);
+        if (precision == MR_PRECISION_COMPENSATED) NUMI_LAUNCH(true, double, true);
+        else if (precision == MR_PRECISION_FP64_ARTICULATED_INERTIA) NUMI_LAUNCH(true, double, false);
+        else NUMI_LAUNCH(true, float, false);
     } else {
-        if (fp64_inertia) control_step_kernel<false, double><<<blocks, threads, smem, stream>>>(p, layout, warps_per_block);
-        else control_step_kernel<false, float><<<blocks, threads, smem, stream>>>(p, layout, warps_per_block);
+        if (precision == MR_PRECISION_COMPENSATED) NUMI_LAUNCH(false, double, true);
+        else if (precision == MR_PRECISION_FP64_ARTICULATED_INERTIA) NUMI_LAUNCH(false, double, false);
+        else NUMI_LAUNCH(false, float, false);
     }
+#undef NUMI_LAUNCH
     return cudaGetLastError();
 }
 
-cudaError_t control_step_occupancy(bool contact, bool fp64_inertia, int warps_per_block, size_t smem, int* blocks_per_sm) {
+namespace {
+
+template <typename F>
+cudaError_t for_kernel(bool contact, std::uint32_t precision, F&& f) {
+    if (contact) {
+        if (precision == MR_PRECISION_COMPENSATED) return f(control_step_kernel<true, double, true>);
+        if (precision == MR_PRECISION_FP64_ARTICULATED_INERTIA) return f(control_step_kernel<true, double, false>);
+        return f(control_step_kernel<true, float, false>);
+    }
+    if (precision == MR_PRECISION_COMPENSATED) return f(control_step_kernel<false, double, true>);
+    if (precision == MR_PRECISION_FP64_ARTICULATED_INERTIA) return f(control_step_kernel<false, double, false>);
+    return f(control_step_kernel<false, float, false>);
+}
+
+}  // namespace
+
+cudaError_t control_step_occupancy(bool contact, std::uint32_t precision, int warps_per_block, size_t smem, int* blocks_per_sm) {
     const int threads = 32 * warps_per_block;
-    if (contact)
-        return fp64_inertia
-                   ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, control_step_kernel<true, double>, threads, smem)
-                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, control_step_kernel<true, float>, threads, smem);
-    return fp64_inertia
-               ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, control_step_kernel<false, double>, threads, smem)
-               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, control_step_kernel<false, float>, threads, smem);
+    return for_kernel(contact, precision, [&](auto kernel) {
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, threads, smem);
+    });
 }
 
 cudaError_t configure_control_step_kernels(size_t max_dynamic_smem) {
     const int bytes = static_cast<int>(max_dynamic_smem);
-    cudaError_t e = cudaFuncSetAttribute(control_step_kernel<true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(control_step_kernel<true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(control_step_kernel<false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(control_step_kernel<false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaError_t e = cudaSuccess;
+    for (const bool contact : {true, false})
+        for (const std::uint32_t precision :
+             {std::uint32_t(MR_PRECISION_FP32), std::uint32_t(MR_PRECISION_FP64_ARTICULATED_INERTIA), std::uint32_t(MR_PRECISION_COMPENSATED)})
+            if (e == cudaSuccess)
+                e = for_kernel(contact, precision, [&](auto kernel) {
+                    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+                });
     return e;
 }
 

@@ -27,7 +27,12 @@ MR_RUN_SOURCE_SYNTHETIC_STACK: Final = 103
 MANIFOLD_POINTS: Final = 4
 MR_PRECISION_FP32: Final = 0
 MR_PRECISION_FP64_ARTICULATED_INERTIA: Final = 1
-PRECISION_MODES: Final = {"fp32": MR_PRECISION_FP32, "fp64-inertia": MR_PRECISION_FP64_ARTICULATED_INERTIA}
+MR_PRECISION_COMPENSATED: Final = 2
+PRECISION_MODES: Final = {
+    "fp32": MR_PRECISION_FP32,
+    "fp64-inertia": MR_PRECISION_FP64_ARTICULATED_INERTIA,
+    "compensated": MR_PRECISION_COMPENSATED,
+}
 
 STATUS_NAMES: Final = {
     0: "success",

@@ -171,7 +171,9 @@ class World:
         self.set_precision(precision)
 
     def set_precision(self, precision: str) -> None:
-        """"fp32" (reference precision) or "fp64-inertia" (FP64 articulated inertia)."""
+        """"fp32" (reference precision), "fp64-inertia" (FP64 articulated
+        inertia) or "compensated" (FP64 articulated inertia plus compensated
+        FP32 position and impulse sums)."""
 
         if precision not in native.PRECISION_MODES:
             raise ValueError(f"precision must be one of {sorted(native.PRECISION_MODES)}")

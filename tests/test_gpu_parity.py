@@ -54,11 +54,11 @@ def _oracle_features(man, pairs: int) -> list[tuple[int, tuple[int, ...]]]:
 # FP32 articulated inertia: rounding the shifted child inertias to FP32
 # alone moves the FP64 oracle's joint velocities by up to ~3e-5 relative on
 # this chain (parallel-axis terms dwarf the distal pivots), so the FP32 mode
-# is held to 5e-5 and the FP64 articulated-inertia mode to 1e-5.
-CHAIN_V_TOL = {"fp32": 5e-5, "fp64-inertia": 1e-5}
+# is held to 5e-5 and the FP64 articulated-inertia modes to 1e-5.
+CHAIN_V_TOL = {"fp32": 5e-5, "fp64-inertia": 1e-5, "compensated": 1e-5}
 
 
-@pytest.mark.parametrize("precision", ["fp32", "fp64-inertia"])
+@pytest.mark.parametrize("precision", ["fp32", "fp64-inertia", "compensated"])
 def test_chain7_free_motion_per_step(cuda_device, precision):
     import torch
 
@@ -91,7 +91,7 @@ def _tree_world(envs: int, seed: int = 5, precision: str = "fp32"):
                     precision=precision)
 
 
-@pytest.mark.parametrize("precision", ["fp32", "fp64-inertia"])
+@pytest.mark.parametrize("precision", ["fp32", "fp64-inertia", "compensated"])
 def test_tree29_contact_per_step(cuda_device, precision):
     import torch
 

@@ -1,4 +1,4 @@
-"""Horizon drift of the two precision modes against the FP64 oracle.
+"""Horizon drift of the precision modes against the FP64 oracle.
 
 The 29-DoF contact world is chaotic: any perturbation -- FP32 rounding
 included -- grows over the horizon, so per-step parity (test_gpu_parity)
@@ -49,7 +49,7 @@ def test_horizon_drift_and_cone_feasibility(cuda_device):
     acts = actions.cpu().numpy()
     report = {}
     oracle_q = None
-    for precision in ("fp32", "fp64-inertia"):
+    for precision in ("fp32", "fp64-inertia", "compensated"):
         with nb.World("tree29", envs, substeps=4, velocity_iterations=8, control_dt=0.02, seed=seed,
                       precision=precision) as world:
             if oracle_q is None:

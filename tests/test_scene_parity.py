@@ -48,12 +48,13 @@ def _keys(table: np.ndarray, env: int, count: int) -> list[int]:
     return [int(table[env, i, 56].view(np.uint32)) for i in range(count)]
 
 
-def _compare_run(seed: int, envs: int, steps: int):
+def _compare_run(seed: int, envs: int, steps: int, precision: str = "fp32"):
     import torch
 
     substeps, iters = 4, 8
     rows = []
-    with nb.World("pile", envs, substeps=substeps, velocity_iterations=iters, control_dt=0.02, seed=seed) as world:
+    with nb.World("pile", envs, substeps=substeps, velocity_iterations=iters, control_dt=0.02, seed=seed,
+                  precision=precision) as world:
         oracle = SceneOracle(world.model(), 0.02 / substeps, substeps, iters, 0)
         fr = world.friction_scales()
         acts = torch.zeros((1, envs, 0), device="cuda")
@@ -96,9 +97,10 @@ def _compare_run(seed: int, envs: int, steps: int):
     return rows
 
 
-@pytest.mark.parametrize("seed", [3, 10, 13, 1])  # 10, 8, 17 and 50 bodies
-def test_pile_control_steps_match_oracle(cuda_device, seed):
-    rows = _compare_run(seed, 8, 60)
+@pytest.mark.parametrize("seed,precision", [(3, "fp32"), (10, "fp32"), (13, "fp32"), (1, "fp32"),  # 10, 8, 17, 50 bodies
+                                            (13, "compensated"), (1, "compensated")])
+def test_pile_control_steps_match_oracle(cuda_device, seed, precision):
+    rows = _compare_run(seed, 8, 60, precision)
     assert all(r["status"][0] == r["status"][1] == 0 for r in rows)
     clean = [r for r in rows if r["band"] == 0]
     assert len(clean) >= len(rows) // 2, "too many band steps for a meaningful comparison"
