@@ -372,9 +372,11 @@ def _timed_advances(worlds, args, horizon: int, device, streams=None, episodic=(
     return ms, failures, clocks.summary()
 
 
-def run_pile(args) -> None:
-    """Free-body piles: 16,384 environments of a 36-body pile of boxes and
-    spheres on a plane (settled), 4 x 5 ms substeps, 8 iterations."""
+def run_pile(args, source: str = "pile") -> None:
+    """Free-body piles: 16,384 environments of a 36-body pile of boxes,
+    spheres and capsules (source "pile") or of boxes, spheres, capsules and
+    cylinders ("cylinder_pile": cylinder pairs take the support-mapped GJK /
+    EPA narrowphase) on a plane (settled), 4 x 5 ms substeps, 8 iterations."""
 
     import torch
 
@@ -383,7 +385,7 @@ def run_pile(args) -> None:
     torch.cuda.set_device(0)
     device = torch.device("cuda", 0)
     envs, horizon = args.envs or 16384, 25
-    with nb.World("pile", envs, substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT, seed=PILE_SEED) as world:
+    with nb.World(source, envs, substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT, seed=PILE_SEED) as world:
         assert world.scene_bodies == PILE_BODIES
         settle = torch.zeros((100, envs, 0), device=device)
         world.step(settle, wait=True)  # drop and settle (2 s), untimed
@@ -395,11 +397,11 @@ def run_pile(args) -> None:
         mean_manifolds = float((live > 0).sum(axis=1).mean())
         cpu = None
         if not args.no_cpu_baseline:
-            rq, rv, rf = nb.sample_reset("pile", PILE_SEED, PILE_SEED, 0, 1)
+            rq, rv, rf = nb.sample_reset(source, PILE_SEED, PILE_SEED, 0, 1)
             cpu = _pile_cpu_port_sample(world.model(), rq[0], rv[0], float(rf[0]), 40)
     value = envs * horizon * args.steps / (ms / 1e3)
     line = {
-        "metric": "pile env-steps/s",
+        "metric": f"{source.replace('_', ' ')} env-steps/s",
         "value": value,
         "unit": UNIT,
         "n_gpus": 1,
@@ -411,7 +413,9 @@ def run_pile(args) -> None:
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded)",
-        "config": {"workload": f"free-body piles: {envs} envs x {PILE_BODIES} boxes/spheres (size U(0.05, 0.3) m, density 500-2000) "
+        "config": {"workload": f"free-body piles: {envs} envs x {PILE_BODIES} "
+                               f"{'boxes/spheres/capsules' if source == 'pile' else 'boxes/spheres/capsules/cylinders'} "
+                               "(size U(0.05, 0.3) m, density 500-2000) "
                                "settled on a plane, 20 ms control = 4 x 5 ms substeps, 8 temporalCone iterations, "
                                f"{horizon} control steps per bench step", "l2": "flushed (256 MiB write) between steps"},
         "cpu_baseline": cpu,
@@ -685,9 +689,10 @@ def main() -> None:
     parser.add_argument("--impl", default="native", choices=["native", "reference"])
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--envs", type=int, default=0, help="pile workload: environments (default 16384; smaller for profiling)")
-    parser.add_argument("--workload", default="tree29", choices=["tree29", "pile", "mix", "precision"],
-                        help="tree29 (the headline), pile (36-body piles), mix (chains, trees and piles) or "
-                             "precision (box stacks and trees against the FP64 oracle)")
+    parser.add_argument("--workload", default="tree29", choices=["tree29", "pile", "cylinder_pile", "mix", "precision"],
+                        help="tree29 (the headline), pile (36-body piles), cylinder_pile (36-body piles with cylinders: "
+                             "GJK / EPA pairs), mix (chains, trees and piles) or precision (box stacks and trees against the "
+                             "FP64 oracle)")
     parser.add_argument("--serve", action="store_true",
                         help="serving workload: Poisson request stream, latency percentiles (one JSON line)")
     args = parser.parse_args()
@@ -707,7 +712,8 @@ def main() -> None:
         return
     if args.workload != "tree29":
         if rank == 0:
-            {"pile": run_pile, "mix": run_mix, "precision": run_precision}[args.workload](args)
+            {"pile": run_pile, "cylinder_pile": lambda a: run_pile(a, "cylinder_pile"), "mix": run_mix,
+             "precision": run_precision}[args.workload](args)
         return
 
     import torch

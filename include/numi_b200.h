@@ -71,7 +71,8 @@ enum MRShapeType {
     MR_SHAPE_SPHERE = 0u,
     MR_SHAPE_CAPSULE = 1u,
     MR_SHAPE_BOX = 2u,
-    MR_SHAPE_PLANE = 3u
+    MR_SHAPE_PLANE = 3u,
+    MR_SHAPE_CYLINDER = 4u   /* radius dimensions.x, half length dimensions.y along local +Y */
 };
 
 /* reference: include/metalrobo/engine_types.h:114-134 (same values). */
@@ -102,11 +103,13 @@ enum MRCollisionPairClass {
     MR_COLLISION_PAIR_SPHERE_PLANE = 2u,
     MR_COLLISION_PAIR_CAPSULE_PLANE = 3u,
     MR_COLLISION_PAIR_BOX_PLANE = 4u,
+    MR_COLLISION_PAIR_CYLINDER_PLANE = 5u,
     MR_COLLISION_PAIR_SPHERE_CAPSULE = 6u,
     MR_COLLISION_PAIR_CAPSULE_CAPSULE = 7u,
     MR_COLLISION_PAIR_SPHERE_BOX = 8u,
     MR_COLLISION_PAIR_CAPSULE_BOX = 9u,
-    MR_COLLISION_PAIR_BOX_BOX = 10u
+    MR_COLLISION_PAIR_BOX_BOX = 10u,
+    MR_COLLISION_PAIR_CONVEX = 11u   /* support-mapped (GJK / EPA): here, a cylinder against a finite shape */
 };
 #endif /* NUMI_B200_OMIT_SHARED_ENUMS */
 
@@ -177,7 +180,11 @@ enum MRRunManifestSourceC {
     /* Stack of 32 0.1 m, 1 kg boxes (friction 0.6) resting on a ground
      * plane, the stack yawed U(0, 2 pi) and each box offset N(0, 2 mm) at
      * reset; scene bodies, no actuation. */
-    MR_RUN_SOURCE_SYNTHETIC_STACK = 103u
+    MR_RUN_SOURCE_SYNTHETIC_STACK = 103u,
+    /* Pile of 8-64 free boxes, spheres, capsules and cylinders (one quarter
+     * each) dropped onto a ground plane; cylinder pairs take the
+     * support-mapped (GJK / EPA) narrowphase. */
+    MR_RUN_SOURCE_SYNTHETIC_CYLINDER_PILE = 104u
 };
 
 /* reference: include/metalrobo/c_api.h:171-190 (same shape). */

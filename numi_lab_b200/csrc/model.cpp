@@ -500,11 +500,16 @@ static void finish_scene(CompiledModel& m, std::uint32_t n, double friction) {
     set4(mat.response, 0.0, 0.5, 0.0, 0.0);
     m.materials.push_back(mat);
     m.materials.push_back(mat);
+    // Pair classes as the reference compiles them (MetalWorld.mm:1413-1500):
+    // a cylinder against the plane is analytic, against any finite shape
+    // support-mapped (GJK / EPA).
     auto cls = [&](std::uint32_t a, std::uint32_t b) {
         const std::uint32_t ta = m.shapes[a].shape_type, tb = m.shapes[b].shape_type;
         if (tb == MR_SHAPE_PLANE)
             return ta == MR_SHAPE_BOX ? MR_COLLISION_PAIR_BOX_PLANE
-                   : (ta == MR_SHAPE_CAPSULE ? MR_COLLISION_PAIR_CAPSULE_PLANE : MR_COLLISION_PAIR_SPHERE_PLANE);
+                   : (ta == MR_SHAPE_CAPSULE ? MR_COLLISION_PAIR_CAPSULE_PLANE
+                   : (ta == MR_SHAPE_CYLINDER ? MR_COLLISION_PAIR_CYLINDER_PLANE : MR_COLLISION_PAIR_SPHERE_PLANE));
+        if (ta == MR_SHAPE_CYLINDER || tb == MR_SHAPE_CYLINDER) return MR_COLLISION_PAIR_CONVEX;
         const bool sphere = ta == MR_SHAPE_SPHERE || tb == MR_SHAPE_SPHERE;
         const bool capsule = ta == MR_SHAPE_CAPSULE || tb == MR_SHAPE_CAPSULE;
         const bool box = ta == MR_SHAPE_BOX || tb == MR_SHAPE_BOX;
@@ -547,9 +552,9 @@ static void finish_scene(CompiledModel& m, std::uint32_t n, double friction) {
 }
 
 
-CompiledModel build_pile(std::uint64_t seed, std::uint32_t count) {
+CompiledModel build_pile(std::uint64_t seed, std::uint32_t count, bool cylinders) {
     CompiledModel m;
-    m.name = "synthetic_pile";
+    m.name = cylinders ? "synthetic_cylinder_pile" : "synthetic_pile";
     m.scene = true;
     std::uint64_t k = 0;
     auto draw = [&](double lo, double hi) { return uniform(seed, kStreamModel, k++, lo, hi); };
@@ -558,10 +563,12 @@ CompiledModel build_pile(std::uint64_t seed, std::uint32_t count) {
     m.scene_bodies = n;
     double largest = 0.0;
     for (std::uint32_t b = 0; b < n; ++b) {
-        // One third each of boxes, spheres and capsules.
+        // One third each of boxes, spheres and capsules; with cylinders,
+        // one quarter each of boxes, spheres, capsules and cylinders.
         const double kind = draw(0.0, 1.0);
-        const bool box = kind < 1.0 / 3.0;
-        const bool capsule = kind >= 2.0 / 3.0;
+        const bool box = cylinders ? kind < 0.25 : kind < 1.0 / 3.0;
+        const bool capsule = cylinders ? (kind >= 0.5 && kind < 0.75) : kind >= 2.0 / 3.0;
+        const bool cylinder = cylinders && kind >= 0.75;
         const double size = draw(0.05, 0.3);
         const double density = draw(500.0, 2000.0);
         double hx = 0.5 * size, hy = 0.5 * size, hz = 0.5 * size;
@@ -573,6 +580,9 @@ CompiledModel build_pile(std::uint64_t seed, std::uint32_t count) {
         // Capsule: overall length `size` along local +Y, radius size x U(0.15, 0.3).
         const double cap_r = capsule ? size * draw(0.15, 0.3) : 0.0;
         const double cap_hl = capsule ? 0.5 * size - cap_r : 0.0;
+        // Cylinder: radius and half length each 0.5 size x U(0.5, 1) (local +Y axis).
+        const double cyl_r = cylinder ? 0.5 * size * draw(0.5, 1.0) : 0.0;
+        const double cyl_hl = cylinder ? 0.5 * size * draw(0.5, 1.0) : 0.0;
         MRModelBodyC body{};
         body.parent_body = MR_INVALID_INDEX;
         body.inbound_joint = MR_INVALID_INDEX;
@@ -595,6 +605,12 @@ CompiledModel build_pile(std::uint64_t seed, std::uint32_t count) {
             ixx = izz = m_cyl * (hgt * hgt / 12.0 + 0.25 * r * r) +
                         2.0 * m_cap * (0.4 * r * r + 0.25 * hgt * hgt + 0.375 * hgt * r);
             bound = cap_hl + r;
+        } else if (cylinder) {
+            const double r = cyl_r, hgt = 2.0 * cyl_hl;
+            mass = density * 3.141592653589793 * r * r * hgt;
+            iyy = 0.5 * mass * r * r;
+            ixx = izz = mass * (3.0 * r * r + hgt * hgt) / 12.0;
+            bound = std::sqrt(r * r + cyl_hl * cyl_hl);  // Collision.metal:5731-5734
         } else {
             const double r = hx;
             mass = density * 4.0 / 3.0 * 3.141592653589793 * r * r * r;
@@ -612,13 +628,14 @@ CompiledModel build_pile(std::uint64_t seed, std::uint32_t count) {
         m.bodies.push_back(body);
         MRModelShapeC s{};
         s.body = b;
-        s.shape_type = box ? MR_SHAPE_BOX : (capsule ? MR_SHAPE_CAPSULE : MR_SHAPE_SPHERE);
+        s.shape_type = box ? MR_SHAPE_BOX : (capsule ? MR_SHAPE_CAPSULE : (cylinder ? MR_SHAPE_CYLINDER : MR_SHAPE_SPHERE));
         s.material = 0;
         s.collision_group = 1u;
         s.collision_mask = 3u;
         set4(s.local_position, 0.0, 0.0, 0.0, 0.0);
         set4(s.local_rotation, 0.0, 0.0, 0.0, 1.0);
         if (capsule) set4(s.dimensions, cap_r, cap_hl, 0.0, 0.0);
+        else if (cylinder) set4(s.dimensions, cyl_r, cyl_hl, 0.0, 0.0);
         else set4(s.dimensions, hx, box ? hy : 0.0, box ? hz : 0.0, 0.0);
         set4(s.contact_rest_bound, 0.002, 0.0, bound, 0.0);
         m.shapes.push_back(s);

@@ -73,7 +73,8 @@ CompiledModel build_tree29(std::uint64_t seed);
 // Pile of 8-64 free boxes, spheres and capsules (size U(0.05, 0.3) m, density
 // U(500, 2000) kg/m^3) dropped onto a ground plane; the body count is drawn
 // from the seed unless `bodies` is non-zero.
-CompiledModel build_pile(std::uint64_t seed, std::uint32_t bodies = 0);
+// `cylinders`: one quarter each of boxes, spheres, capsules and cylinders.
+CompiledModel build_pile(std::uint64_t seed, std::uint32_t bodies = 0, bool cylinders = false);
 // Stack of `boxes` 0.1 m, 1 kg cubes (friction 0.6) resting on a ground
 // plane, the stack yawed U(0, 2 pi) and each box offset horizontally by
 // N(0, 2 mm) at reset.

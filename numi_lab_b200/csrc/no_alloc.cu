@@ -127,6 +127,7 @@ MR_API int mr_pile_step_no_alloc(uint32_t source, uint64_t model_seed, uint32_t 
             p.substeps = static_cast<int>(physics_substeps);
             p.velocity_iterations = static_cast<int>(velocity_iterations);
             p.final_velocity_iterations = static_cast<int>(final_velocity_iterations);
+            p.support_mapped = d.host_model.support_mapped;
             check(numi::launch_scene_step(p, stream), "scene step launch");
         }
     });

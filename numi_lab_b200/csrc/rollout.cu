@@ -325,6 +325,9 @@ numi::SceneModel numi::rt::pack_scene(const numi::CompiledModel& m, float h) {
                                         static_cast<float>(qw[3] / nrm));
     }
     d.plane_material = static_cast<int>(plane.material);
+    d.support_mapped = 0;
+    for (const MRModelPairC& pr : m.pairs)
+        if (pr.pair_class == MR_COLLISION_PAIR_CONVEX) d.support_mapped = 1;
     for (std::uint32_t b = 0; b < n; ++b) {
         const MRModelShapeC& sh = m.shapes[b];
         const MRModelBodyC& body = m.bodies[b];
@@ -473,6 +476,7 @@ struct MRTaskRolloutHandle {
                 p.velocity_iterations = static_cast<int>(config.velocity_iterations);
                 p.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
                 p.q_comp = precision == MR_PRECISION_COMPENSATED ? d_qcomp.ptr : nullptr;
+                p.support_mapped = smodel.support_mapped;
                 check(numi::launch_scene_step(p, s), "scene step launch");
             }
             (void)actions;
@@ -619,6 +623,7 @@ MR_API MRTaskRolloutHandle* mr_create_task_rollout(const MRRunManifestC* manifes
             case MR_RUN_SOURCE_SYNTHETIC_CHAIN7: h.model = numi::build_chain7(cfg.seed); break;
             case MR_RUN_SOURCE_SYNTHETIC_TREE29: h.model = numi::build_tree29(cfg.seed); break;
             case MR_RUN_SOURCE_SYNTHETIC_PILE: h.model = numi::build_pile(cfg.seed); break;
+            case MR_RUN_SOURCE_SYNTHETIC_CYLINDER_PILE: h.model = numi::build_pile(cfg.seed, 0, true); break;
             case MR_RUN_SOURCE_SYNTHETIC_STACK: h.model = numi::build_stack(cfg.seed); break;
             default:
                 throw std::invalid_argument("unsupported run source " + std::to_string(manifest->source) +
@@ -916,6 +921,7 @@ static numi::CompiledModel compile_source(uint32_t source, uint64_t seed) {
         case MR_RUN_SOURCE_SYNTHETIC_CHAIN7: return numi::build_chain7(seed);
         case MR_RUN_SOURCE_SYNTHETIC_TREE29: return numi::build_tree29(seed);
         case MR_RUN_SOURCE_SYNTHETIC_PILE: return numi::build_pile(seed);
+        case MR_RUN_SOURCE_SYNTHETIC_CYLINDER_PILE: return numi::build_pile(seed, 0, true);
         case MR_RUN_SOURCE_SYNTHETIC_STACK: return numi::build_stack(seed);
         default: throw std::invalid_argument("unsupported synthetic source " + std::to_string(source));
     }

@@ -1,4 +1,5 @@
-// Free-body ("scene") worlds: piles of spheres and boxes on a ground plane.
+// Free-body ("scene") worlds: piles of spheres, capsules, boxes and
+// cylinders on a ground plane.
 // Device record, launch parameters and per-environment capacities of the
 // free-body control-step kernel (scene_step.cu).
 #pragma once
@@ -37,7 +38,8 @@ struct alignas(16) SceneModel {
     float4 ground_position;  // pose of the plane's (static) body: manifold
     float4 ground_rotation;  // anchors on the plane live in this frame
     std::int32_t plane_material;
-    std::int32_t reserved1[3];
+    std::int32_t support_mapped;  // some pair is MR_COLLISION_PAIR_CONVEX (GJK / EPA)
+    std::int32_t reserved1[2];
     // Bodies (one collider each, at the body's centre of mass).
     std::int32_t shape_type[kSceneMaxBodies];
     std::int32_t material[kSceneMaxBodies];
@@ -78,6 +80,7 @@ struct SceneParams {
     std::int32_t velocity_iterations;
     std::int32_t final_velocity_iterations;
     float* q_comp;             // [slot][nb][7]: compensation of the position sums (entries 0-2), or null (FP32 sums)
+    std::int32_t support_mapped;  // the model has support-mapped (cylinder) pairs: SceneModel::support_mapped
 };
 
 size_t scene_step_smem_bytes(bool compensated = false);

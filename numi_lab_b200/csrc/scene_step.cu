@@ -129,6 +129,8 @@ struct Collider {
     float offset;    // contact offset incl. speculative margin
     float3 lo, hi;   // swept, inflated bounds (finite shapes)
     float3 e0, e1;   // capsule segment endpoints (local -Y / +Y ends)
+    float3 axis, bx, bz;  // cylinder axis (local +Y) and disk basis
+    float hl;        // cylinder half length
     float3 normal;   // plane normal
     float3 bpos;     // pose of the collider's body: the frame of its
     float4 brot;     // manifold anchors (the ground body for the plane)
@@ -145,6 +147,8 @@ __device__ void load_collider(const SceneModel& M, const float* s, int b, Collid
         o.radius = 0.0f;
         o.offset = M.plane_offsets.x;
         o.lo = o.hi = f3(0.0f, 0.0f, 0.0f);
+        o.axis = o.bx = o.bz = f3(0.0f, 0.0f, 0.0f);
+        o.hl = 0.0f;
         o.bpos = xyz(M.ground_position);
         o.brot = M.ground_rotation;
         return;
@@ -164,6 +168,22 @@ __device__ void load_collider(const SceneModel& M, const float* s, int b, Collid
         o.e1 = o.c + axis;
     } else {
         o.e0 = o.e1 = o.c;
+    }
+    o.hl = d.y;
+    if (o.type == MR_SHAPE_CYLINDER) {
+        // Collision.metal:759-784: unit axis, disk basis X orthogonalised
+        // against it, Z = X x axis.
+        float3 ax = qrot(o.r, f3(0.0f, 1.0f, 0.0f));
+        ax = ax * rsqrtf(dot3(ax, ax));
+        float3 bx = qrot(o.r, f3(1.0f, 0.0f, 0.0f));
+        bx = bx - ax * dot3(ax, bx);
+        bx = bx * rsqrtf(dot3(bx, bx));
+        float3 bz = cross3(bx, ax);
+        o.axis = ax;
+        o.bx = bx;
+        o.bz = bz * rsqrtf(dot3(bz, bz));
+    } else {
+        o.axis = o.bx = o.bz = f3(0.0f, 0.0f, 0.0f);
     }
     o.normal = f3(0.0f, 0.0f, 0.0f);
     o.bpos = o.c;
@@ -389,8 +409,550 @@ struct RawSink {
     }
 };
 
-__device__ bool narrowphase(const Collider& A, const Collider& B, int cls, unsigned ia, unsigned ib, float accepted,
-                            RawSink& sink, float3& normal) {
+// ---------------------------------------------------------------------------
+// Support-mapped narrowphase: cylinder pairs (the reference's primitive-GJK
+// class, MR_WORLD_WORK_PRIMITIVE_GJK): GJK distance (Collision.metal:
+// 2298-2427), on overlap EPA (2511-2783) with MPR as the fallback
+// (2786-3193), then the cylinder's contact patch (3327-3432).  One lane runs
+// one pair; the simplex, the EPA polytope and the MPR portal are per-thread
+// local arrays (about 6 KB, in the interleaved local space).  Two choices
+// differ from the reference's text, in the device and the oracle alike:
+// EPA orients a face against an interior point of the polytope rather than
+// the origin (the same unless the origin lies on the face plane, where the
+// origin test is ambiguous), and EPA reports the closest face's outward
+// normal -- the A -> B normal of every other class -- where the reference
+// writes its negation.  No query cache warm-starts GJK.
+// ---------------------------------------------------------------------------
+constexpr int kGjkIterations = 32;  // MR_GJK_MAX_ITERATIONS
+constexpr int kEpaIterations = 48;  // MR_EPA_MAX_ITERATIONS
+constexpr int kEpaVertices = 64;    // MR_EPA_VERTEX_CAPACITY
+constexpr int kEpaFaces = 128;      // MR_EPA_FACE_CAPACITY
+constexpr float kCylAlign = 1.0e-6f;  // Collision.metal:21
+enum : unsigned { kCylNegRing = 0u, kCylPosRing = 4u, kCylNegSide = 8u, kCylPosSide = 9u, kCylNegRim = 10u, kCylPosRim = 11u };
+constexpr float kFltEps = 1.1920929e-7f;
+
+struct Sup {
+    float3 w, pa, pb;  // Minkowski point A - B and its supports
+    unsigned fa, fb;
+};
+
+struct SmQuery {
+    float3 normal, pa, pb;
+    float sep;
+    unsigned fa, fb;
+};
+
+__device__ __forceinline__ float3 deterministic_direction(unsigned key) {
+    const unsigned axis = key % 3u;
+    const float sign = (key & 4u) == 0u ? 1.0f : -1.0f;
+    return f3(axis == 0u ? sign : 0.0f, axis == 1u ? sign : 0.0f, axis == 2u ? sign : 0.0f);
+}
+
+__device__ float3 shape_support(const Collider& k, unsigned index, float3 d, unsigned& feat) {
+    const float dd = dot3(d, d);
+    d = (!(dd > kTinyS) || !isfinite(dd)) ? deterministic_direction(index) : d * rsqrtf(dd);
+    if (k.type == MR_SHAPE_SPHERE) {
+        feat = feature_key(MR_SHAPE_SPHERE, 0u);
+        return k.c + d * k.radius;
+    }
+    if (k.type == MR_SHAPE_CAPSULE) {
+        const bool pos = dot3(d, k.e1 - k.e0) >= 0.0f;
+        feat = feature_key(MR_SHAPE_CAPSULE, pos ? 1u : 0u);
+        return (pos ? k.e1 : k.e0) + d * k.radius;
+    }
+    if (k.type == MR_SHAPE_BOX) {
+        const float3 l = qrotinv(k.r, d);
+        unsigned v = 0u;
+        float3 p = f3(-k.half.x, -k.half.y, -k.half.z);
+        if (l.x >= 0.0f) { v |= 1u; p.x = k.half.x; }
+        if (l.y >= 0.0f) { v |= 2u; p.y = k.half.y; }
+        if (l.z >= 0.0f) { v |= 4u; p.z = k.half.z; }
+        feat = feature_key(MR_SHAPE_BOX, v);
+        return k.c + qrot(k.r, p);
+    }
+    // cylinder
+    const float axial = dot3(d, k.axis);
+    const float3 radial = d - k.axis * axial;
+    const float rsq = dot3(radial, radial);
+    const float3 rdir = rsq > kTinyS ? radial * rsqrtf(rsq) : k.bx;
+    const bool pos = axial >= 0.0f;
+    unsigned local = pos ? kCylPosRim : kCylNegRim;
+    if (fabsf(axial) <= kCylAlign) {
+        const float x = dot3(rdir, k.bx), z = dot3(rdir, k.bz);
+        local = 32u + (fabsf(x) >= fabsf(z) ? (x >= 0.0f ? 0u : 1u) : (z >= 0.0f ? 2u : 3u));
+    } else if (rsq <= kTinyS) {
+        local = pos ? 17u : 16u;
+    }
+    feat = feature_key(MR_SHAPE_CYLINDER, local);
+    return k.c + k.axis * (pos ? k.hl : -k.hl) + rdir * k.radius;
+}
+
+__device__ __forceinline__ void minkowski(const Collider& A, const Collider& B, unsigned ia, unsigned ib, float3 d, Sup& o) {
+    o.pa = shape_support(A, ia, d, o.fa);
+    o.pb = shape_support(B, ib, -d, o.fb);
+    o.w = o.pa - o.pb;
+}
+
+// Closest point to the origin on triangle abc with barycentric weights
+// (the Voronoi-region walk of Ericson, Real-Time Collision Detection 5.1.5).
+__device__ float3 closest_triangle(float3 a, float3 b, float3 c, float* wt) {
+    const float3 ab = b - a, ac = c - a, ap = -a;
+    const float d1 = dot3(ab, ap), d2 = dot3(ac, ap);
+    if (d1 <= 0.0f && d2 <= 0.0f) { wt[0] = 1.0f; wt[1] = 0.0f; wt[2] = 0.0f; return a; }
+    const float3 bp = -b;
+    const float d3 = dot3(ab, bp), d4 = dot3(ac, bp);
+    if (d3 >= 0.0f && d4 <= d3) { wt[0] = 0.0f; wt[1] = 1.0f; wt[2] = 0.0f; return b; }
+    const float vc = d1 * d4 - d3 * d2;
+    if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
+        const float den = d1 - d3, v = den > kTinyS ? d1 / den : 0.0f;
+        wt[0] = 1.0f - v; wt[1] = v; wt[2] = 0.0f;
+        return a + ab * v;
+    }
+    const float3 cp = -c;
+    const float d5 = dot3(ab, cp), d6 = dot3(ac, cp);
+    if (d6 >= 0.0f && d5 <= d6) { wt[0] = 0.0f; wt[1] = 0.0f; wt[2] = 1.0f; return c; }
+    const float vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
+        const float den = d2 - d6, w = den > kTinyS ? d2 / den : 0.0f;
+        wt[0] = 1.0f - w; wt[1] = 0.0f; wt[2] = w;
+        return a + ac * w;
+    }
+    const float va = d3 * d6 - d5 * d4;
+    if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f) {
+        const float den = (d4 - d3) + (d5 - d6), w = den > kTinyS ? (d4 - d3) / den : 0.0f;
+        wt[0] = 0.0f; wt[1] = 1.0f - w; wt[2] = w;
+        return b + (c - b) * w;
+    }
+    const float den = va + vb + vc;
+    if (!(fabsf(den) > kTinyS) || !isfinite(den)) { wt[0] = 1.0f; wt[1] = 0.0f; wt[2] = 0.0f; return a; }
+    const float v = vb / den, w = vc / den;
+    wt[0] = 1.0f - v - w; wt[1] = v; wt[2] = w;
+    return a + ab * v + ac * w;
+}
+
+// a . (b x c) with error-free products and sums (the FMA two-product and
+// Knuth's two-sum of Ogita, Rump and Oishi, "Accurate sum and dot product",
+// 2005): the tetrahedron containment test of near-degenerate simplices.
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+    s = a + b;
+    const float bb = s - a;
+    e = (a - (s - bb)) + (b - bb);
+}
+__device__ float accurate_triple(float3 a, float3 b, float3 c) {
+    // cross components as (value, error) from two products each
+    auto cross_comp = [](float p, float q, float r, float s, float& v, float& e) {
+        const float x = p * q, ex = __fmaf_rn(p, q, -x);
+        const float y = r * s, ey = __fmaf_rn(r, s, -y);
+        float d, ed;
+        two_sum(x, -y, d, ed);
+        v = d;
+        e = ed + (ex - ey);
+    };
+    float cx, ecx, cy, ecy, cz, ecz;
+    cross_comp(b.y, c.z, b.z, c.y, cx, ecx);
+    cross_comp(b.z, c.x, b.x, c.z, cy, ecy);
+    cross_comp(b.x, c.y, b.y, c.x, cz, ecz);
+    const float tx = a.x * cx, etx = __fmaf_rn(a.x, cx, -tx) + a.x * ecx;
+    const float ty = a.y * cy, ety = __fmaf_rn(a.y, cy, -ty) + a.y * ecy;
+    const float tz = a.z * cz, etz = __fmaf_rn(a.z, cz, -tz) + a.z * ecz;
+    float s1, e1, s2, e2;
+    two_sum(tx, ty, s1, e1);
+    two_sum(s1, tz, s2, e2);
+    return s2 + (e1 + e2 + etx + ety + etz);
+}
+
+__device__ void compress_simplex(Sup* sx, int& n, float* wt) {
+    Sup keep[4];
+    float kw[4];
+    int m = 0, best = 0;
+    for (int i = 1; i < n; ++i)
+        if (wt[i] > wt[best]) best = i;
+    for (int i = 0; i < n; ++i)
+        if (wt[i] > 1.0e-7f) { keep[m] = sx[i]; kw[m] = wt[i]; ++m; }
+    if (m == 0) { keep[0] = sx[best]; kw[0] = 1.0f; m = 1; }
+    float tot = 0.0f;
+    for (int i = 0; i < m; ++i) tot += kw[i];
+    const float inv = tot > kTinyS ? 1.0f / tot : 1.0f;
+    for (int i = 0; i < m; ++i) { sx[i] = keep[i]; wt[i] = kw[i] * inv; }
+    n = m;
+}
+
+__device__ bool closest_simplex(Sup* sx, int& n, float* wt, float3& closest) {
+    if (n == 1) { wt[0] = 1.0f; closest = sx[0].w; return false; }
+    if (n == 2) {
+        const float3 a = sx[0].w, e = sx[1].w - a;
+        const float den = dot3(e, e);
+        const float t = den > kTinyS ? fminf(fmaxf(-dot3(a, e) / den, 0.0f), 1.0f) : 0.0f;
+        wt[0] = 1.0f - t;
+        wt[1] = t;
+        closest = a + e * t;
+        compress_simplex(sx, n, wt);
+        return false;
+    }
+    if (n == 3) {
+        closest = closest_triangle(sx[0].w, sx[1].w, sx[2].w, wt);
+        compress_simplex(sx, n, wt);
+        return false;
+    }
+    const float3 a = sx[0].w, ab = sx[1].w - a, ac = sx[2].w - a, ad = sx[3].w - a;
+    const float det = accurate_triple(ab, ac, ad);
+    if (fabsf(det) > kTinyS && isfinite(det)) {
+        const float inv = 1.0f / det;
+        const float u = accurate_triple(-a, ac, ad) * inv, v = accurate_triple(ab, -a, ad) * inv,
+                    w = accurate_triple(ab, ac, -a) * inv;
+        const float base = 1.0f - u - v - w, tol = -2.0e-6f;
+        if (base >= tol && u >= tol && v >= tol && w >= tol) {
+            wt[0] = base; wt[1] = u; wt[2] = v; wt[3] = w;
+            closest = f3(0.0f, 0.0f, 0.0f);
+            return true;
+        }
+    }
+    const int faces[4][3] = {{0, 1, 2}, {0, 3, 1}, {0, 2, 3}, {1, 3, 2}};
+    float best = INFINITY, bw[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    float3 bp = f3(0.0f, 0.0f, 0.0f);
+    for (int f = 0; f < 4; ++f) {
+        float tw[3];
+        const float3 p = closest_triangle(sx[faces[f][0]].w, sx[faces[f][1]].w, sx[faces[f][2]].w, tw);
+        const float dist = dot3(p, p);
+        if (dist < best) {
+            best = dist;
+            bp = p;
+            bw[0] = bw[1] = bw[2] = bw[3] = 0.0f;
+            for (int k = 0; k < 3; ++k) bw[faces[f][k]] = tw[k];
+        }
+    }
+    closest = bp;
+    for (int i = 0; i < 4; ++i) wt[i] = bw[i];
+    compress_simplex(sx, n, wt);
+    return false;
+}
+
+// GJK distance: returns 1 on overlap (the simplex seeds EPA), 0 apart (q
+// holds the witness), -1 without convergence.
+__device__ int gjk(const Collider& A, const Collider& B, unsigned ia, unsigned ib, float scale, Sup* sx, int& n, float* wt,
+                   SmQuery& q) {
+    const float tol = 32.0f * kFltEps * scale;
+    float3 d = B.c - A.c;
+    if (dot3(d, d) <= kTinyS) d = deterministic_direction(ia * 65537u + ib);
+    n = 1;
+    minkowski(A, B, ia, ib, d, sx[0]);
+    wt[0] = 1.0f;
+    float3 closest = sx[0].w;
+    float prev = INFINITY;
+    for (int it = 0; it < kGjkIterations; ++it) {
+        if (dot3(closest, closest) <= tol * tol) return 1;
+        d = -closest;
+        Sup cand;
+        minkowski(A, B, ia, ib, d, cand);
+        bool dup = false;
+        for (int i = 0; i < n; ++i) {
+            const float3 e = cand.w - sx[i].w;
+            dup = dup || dot3(e, e) <= tol * tol;
+        }
+        const float advance = dot3(cand.w, d) - dot3(closest, d);
+        bool done = dup || advance <= tol * fmaxf(len3(d), 1.0f);
+        if (!done) {
+            sx[n++] = cand;
+            if (closest_simplex(sx, n, wt, closest)) return 1;
+            const float upd = dot3(closest, closest);
+            done = prev < INFINITY && prev - upd <= tol * tol;
+            prev = upd;
+        }
+        if (done) {
+            q.pa = q.pb = f3(0.0f, 0.0f, 0.0f);
+            int best = 0;
+            for (int i = 0; i < n; ++i) {
+                q.pa = q.pa + sx[i].pa * wt[i];
+                q.pb = q.pb + sx[i].pb * wt[i];
+                if (wt[i] > wt[best]) best = i;
+            }
+            q.fa = sx[best].fa;
+            q.fb = sx[best].fb;
+            const float3 delta = q.pb - q.pa;
+            const float dist = len3(delta);
+            q.normal = dist > tol ? delta * (1.0f / dist) : d * rsqrtf(dot3(d, d));
+            q.sep = dist;
+            return 0;
+        }
+    }
+    return -1;
+}
+
+struct EpaFace {
+    int a, b, c, active;
+    float3 n;
+    float dist;
+};
+
+// Outward unit normal against `inside` (a point interior to the polytope)
+// and the origin's distance to the face plane.
+__device__ bool make_face(const Sup* vx, int a, int b, int c, float3 inside, EpaFace& f) {
+    float3 n = cross3(vx[b].w - vx[a].w, vx[c].w - vx[a].w);
+    const float nn = dot3(n, n);
+    if (!(nn > kTinyS) || !isfinite(nn)) return false;
+    n = n * rsqrtf(nn);
+    int second = b, third = c;
+    if (dot3(n, vx[a].w - inside) < 0.0f) { n = -n; second = c; third = b; }
+    f.a = a; f.b = second; f.c = third; f.active = 1; f.n = n; f.dist = dot3(n, vx[a].w);
+    return isfinite(f.dist);
+}
+
+__device__ __forceinline__ void horizon_edge(unsigned short* edges, int& ne, int a, int b) {
+    const unsigned short fwd = static_cast<unsigned short>(a | (b << 8)), rev = static_cast<unsigned short>(b | (a << 8));
+    for (int e = 0; e < ne; ++e)
+        if (edges[e] == rev) {
+            edges[e] = edges[--ne];
+            return;
+        }
+    if (ne < 3 * kEpaFaces) edges[ne++] = fwd;
+}
+
+__device__ bool epa(const Collider& A, const Collider& B, unsigned ia, unsigned ib, float scale, const Sup* seed, int nseed,
+                    SmQuery& q) {
+    Sup vx[kEpaVertices];
+    EpaFace fc[kEpaFaces];
+    unsigned short edges[3 * kEpaFaces];
+    int nv = nseed;
+    for (int i = 0; i < nseed; ++i) vx[i] = seed[i];
+    for (int k = 0; nv < 4 && k < 6; ++k) {
+        const float s = k < 3 ? 1.0f : -1.0f;
+        const int ax = k % 3;
+        Sup cand;
+        minkowski(A, B, ia, ib, f3(ax == 0 ? s : 0.0f, ax == 1 ? s : 0.0f, ax == 2 ? s : 0.0f), cand);
+        bool dup = false;
+        for (int i = 0; i < nv; ++i) {
+            const float3 e = cand.w - vx[i].w;
+            dup = dup || dot3(e, e) <= 1.0e-12f;
+        }
+        if (!dup) vx[nv++] = cand;
+    }
+    if (nv < 4) return false;
+    for (int f = 0; f < kEpaFaces; ++f) fc[f].active = 0;
+    const float3 inside = 0.25f * ((vx[0].w + vx[1].w) + (vx[2].w + vx[3].w));
+    const int init[4][3] = {{0, 1, 2}, {0, 3, 1}, {0, 2, 3}, {1, 3, 2}};
+    int nf = 0;
+    for (int f = 0; f < 4; ++f)
+        if (make_face(vx, init[f][0], init[f][1], init[f][2], inside, fc[nf])) ++nf;
+    if (nf < 4) return false;
+    const float tol = 64.0f * kFltEps * scale;
+    for (int it = 0; it < kEpaIterations; ++it) {
+        int best = -1;
+        float bd = INFINITY;
+        for (int f = 0; f < nf; ++f)
+            if (fc[f].active && fc[f].dist < bd) { bd = fc[f].dist; best = f; }
+        if (best < 0) return false;
+        Sup cand;
+        minkowski(A, B, ia, ib, fc[best].n, cand);
+        const float sd = dot3(fc[best].n, cand.w);
+        bool dup = false;
+        for (int i = 0; i < nv; ++i) {
+            const float3 e = cand.w - vx[i].w;
+            dup = dup || dot3(e, e) <= tol * tol;
+        }
+        if (dup || sd - bd <= tol) {
+            const EpaFace F = fc[best];
+            float bc[3];
+            closest_triangle(vx[F.a].w, vx[F.b].w, vx[F.c].w, bc);
+            q.pa = vx[F.a].pa * bc[0] + vx[F.b].pa * bc[1] + vx[F.c].pa * bc[2];
+            q.pb = vx[F.a].pb * bc[0] + vx[F.b].pb * bc[1] + vx[F.c].pb * bc[2];
+            int fv = F.a;
+            float fw = bc[0];
+            if (bc[1] > fw) { fv = F.b; fw = bc[1]; }
+            if (bc[2] > fw) fv = F.c;
+            q.fa = vx[fv].fa;
+            q.fb = vx[fv].fb;
+            q.normal = F.n;
+            q.sep = -bd;
+            return finite3(q.pa) && finite3(q.pb) && finite3(q.normal) && isfinite(q.sep);
+        }
+        if (nv >= kEpaVertices) return false;
+        const int nvx = nv++;
+        vx[nvx] = cand;
+        int ne = 0;
+        for (int f = 0; f < nf; ++f) {
+            if (!fc[f].active || dot3(fc[f].n, cand.w - vx[fc[f].a].w) <= tol) continue;
+            horizon_edge(edges, ne, fc[f].a, fc[f].b);
+            horizon_edge(edges, ne, fc[f].b, fc[f].c);
+            horizon_edge(edges, ne, fc[f].c, fc[f].a);
+            fc[f].active = 0;
+        }
+        if (ne == 0) return false;
+        for (int e = 0; e < ne; ++e) {
+            int dst = -1;
+            for (int f = 0; f < nf; ++f)
+                if (!fc[f].active) { dst = f; break; }
+            if (dst < 0) {
+                if (nf >= kEpaFaces) return false;
+                dst = nf++;
+            }
+            if (!make_face(vx, edges[e] & 0xff, edges[e] >> 8, nvx, inside, fc[dst])) fc[dst].active = 0;
+        }
+    }
+    return false;
+}
+
+__device__ bool mpr_witness(const Collider& A, const Collider& B, unsigned ia, unsigned ib, const Sup* portal, SmQuery& q) {
+    float wt[3];
+    const float3 closest = closest_triangle(portal[1].w, portal[2].w, portal[3].w, wt);
+    q.pa = portal[1].pa * wt[0] + portal[2].pa * wt[1] + portal[3].pa * wt[2];
+    q.pb = portal[1].pb * wt[0] + portal[2].pb * wt[1] + portal[3].pb * wt[2];
+    int fv = 1;
+    float fw = wt[0];
+    if (wt[1] > fw) { fv = 2; fw = wt[1]; }
+    if (wt[2] > fw) fv = 3;
+    q.fa = portal[fv].fa;
+    q.fb = portal[fv].fb;
+    float3 d = closest;
+    float dist = len3(d);
+    const float3 centres = B.c - A.c;
+    if (!(dist > kTinyS)) { d = centres; dist = len3(d); }
+    d = !(dist > kTinyS) ? deterministic_direction(ia * 65537u + ib) : d * (1.0f / dist);
+    if (dot3(d, centres) < 0.0f) d = -d;
+    float sep = dot3(q.pb - q.pa, d);
+    if (sep > 0.0f) { d = -d; sep = -sep; }
+    q.normal = d;
+    q.sep = fminf(sep, -0.0f);
+    return finite3(q.pa) && finite3(q.pb) && finite3(q.normal) && isfinite(q.sep);
+}
+
+__device__ bool mpr(const Collider& A, const Collider& B, unsigned ia, unsigned ib, float scale, SmQuery& q) {
+    Sup portal[4];
+    portal[0].pa = A.c;
+    portal[0].pb = B.c;
+    portal[0].w = A.c - B.c;
+    portal[0].fa = portal[0].fb = 0u;
+    const float tol = 64.0f * kFltEps * scale;
+    if (dot3(portal[0].w, portal[0].w) <= tol * tol) portal[0].w = portal[0].w + deterministic_direction(ia * 65537u + ib) * tol;
+    float3 d = -portal[0].w;
+    d = d * rsqrtf(dot3(d, d));
+    minkowski(A, B, ia, ib, d, portal[1]);
+    if (dot3(portal[1].w, d) < -tol) return false;
+    d = cross3(portal[0].w, portal[1].w);
+    float dd = dot3(d, d);
+    if (!(dd > tol * tol)) { portal[2] = portal[3] = portal[1]; return mpr_witness(A, B, ia, ib, portal, q); }
+    d = d * rsqrtf(dd);
+    minkowski(A, B, ia, ib, d, portal[2]);
+    if (dot3(portal[2].w, d) < -tol) return false;
+    d = cross3(portal[1].w - portal[0].w, portal[2].w - portal[0].w);
+    dd = dot3(d, d);
+    if (!(dd > tol * tol)) { portal[3] = portal[2]; return mpr_witness(A, B, ia, ib, portal, q); }
+    d = d * rsqrtf(dd);
+    if (dot3(d, portal[0].w) > 0.0f) {
+        const Sup t = portal[1];
+        portal[1] = portal[2];
+        portal[2] = t;
+        d = -d;
+    }
+    bool found = false;
+    for (int it = 0; it < kGjkIterations; ++it) {
+        minkowski(A, B, ia, ib, d, portal[3]);
+        if (dot3(portal[3].w, d) < -tol) return false;
+        if (dot3(cross3(portal[1].w, portal[3].w), portal[0].w) < -tol) {
+            portal[2] = portal[3];
+        } else if (dot3(cross3(portal[3].w, portal[2].w), portal[0].w) < -tol) {
+            portal[1] = portal[3];
+        } else {
+            found = true;
+            break;
+        }
+        d = cross3(portal[1].w - portal[0].w, portal[2].w - portal[0].w);
+        dd = dot3(d, d);
+        if (!(dd > tol * tol)) { portal[3] = portal[2]; return mpr_witness(A, B, ia, ib, portal, q); }
+        d = d * rsqrtf(dd);
+    }
+    if (!found) return false;
+    for (int it = 0; it < kEpaIterations; ++it) {
+        d = cross3(portal[2].w - portal[1].w, portal[3].w - portal[1].w);
+        dd = dot3(d, d);
+        if (!(dd > kTinyS) || !isfinite(dd)) return mpr_witness(A, B, ia, ib, portal, q);
+        d = d * rsqrtf(dd);
+        Sup cand;
+        minkowski(A, B, ia, ib, d, cand);
+        const float cp = dot3(cand.w, d);
+        const float pp = fminf(dot3(portal[1].w, d), fminf(dot3(portal[2].w, d), dot3(portal[3].w, d)));
+        if (cp - pp <= tol || it + 1 == kEpaIterations) return mpr_witness(A, B, ia, ib, portal, q);
+        const float3 cc = cross3(cand.w, portal[0].w);
+        if (dot3(portal[1].w, cc) > 0.0f) {
+            if (dot3(portal[2].w, cc) > 0.0f) portal[1] = cand;
+            else portal[3] = cand;
+        } else if (dot3(portal[3].w, cc) > 0.0f) {
+            portal[2] = cand;
+        } else {
+            portal[1] = cand;
+        }
+    }
+    return false;
+}
+
+// Contacts of a support-mapped pair into `sink`; the pair's normal (A -> B)
+// in `normal`.  Returns MR_STEP_SUCCESS or MR_STEP_DID_NOT_CONVERGE.
+__device__ __noinline__ unsigned support_mapped_contacts(const Collider& A, const Collider& B, unsigned ia, unsigned ib, float accepted,
+                                                         RawSink& sink, float3& normal) {
+    const float scale = fmaxf(collider_scale(A), collider_scale(B)) + 1.0f;
+    Sup sx[4];
+    float wt[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    int n = 0;
+    SmQuery q;
+    q.normal = f3(0.0f, 0.0f, 1.0f);
+    const int g = gjk(A, B, ia, ib, scale, sx, n, wt, q);
+    if (g == 1) {
+        // Primitive pairs resolve with EPA first, MPR second (Collision.metal:3518-3560).
+        if (!epa(A, B, ia, ib, scale, sx, n, q) && !mpr(A, B, ia, ib, scale, q)) return MR_STEP_DID_NOT_CONVERGE;
+    } else if (g < 0) {
+        if (!mpr(A, B, ia, ib, scale, q)) return MR_STEP_DID_NOT_CONVERGE;
+    }
+    normal = q.normal;
+    if (q.sep > accepted) return MR_STEP_SUCCESS;
+    float3 wa[kRawCap], wb[kRawCap];
+    int nw = 0;
+    sink.add(q.pa, q.pb, q.sep, q.fa, q.fb);
+    wa[nw] = q.pa;
+    wb[nw] = q.pb;
+    ++nw;
+    // Patch: supports along the normal tilted by 2e-4 towards the disk basis
+    // (cap contact) or the axis (side contact) of the cylinder.
+    const bool cyl_a = A.type == MR_SHAPE_CYLINDER;
+    const Collider& k = cyl_a ? A : B;
+    const unsigned kidx = cyl_a ? ia : ib;
+    const float3 sn = cyl_a ? q.normal : -q.normal;
+    const float align = fabsf(dot3(sn, k.axis));
+    int nd = 0;
+    float3 dirs[4];
+    if (align >= 0.95f) {
+        dirs[0] = k.bx; dirs[1] = -k.bx; dirs[2] = k.bz; dirs[3] = -k.bz;
+        nd = 4;
+    } else if (align <= 0.20f) {
+        dirs[0] = k.axis; dirs[1] = -k.axis;
+        nd = 2;
+    }
+    const float dtol = 32.0f * kFltEps * scale;
+    for (int i = 0; i < nd; ++i) {
+        unsigned f;
+        const float3 p = shape_support(k, kidx, sn + dirs[i] * 2.0e-4f, f);
+        const float3 pa = cyl_a ? p : p - q.normal * q.sep;
+        const float3 pb = cyl_a ? p + q.normal * q.sep : p;
+        bool dup = false;
+        for (int j = 0; j < nw; ++j) {
+            const float3 da = wa[j] - pa, db = wb[j] - pb;
+            dup = dup || (dot3(da, da) <= dtol * dtol && dot3(db, db) <= dtol * dtol);
+        }
+        if (dup || nw >= kRawCap) continue;
+        sink.add(pa, pb, q.sep, cyl_a ? f : q.fa, cyl_a ? q.fb : f);
+        wa[nw] = pa;
+        wb[nw] = pb;
+        ++nw;
+    }
+    return MR_STEP_SUCCESS;
+}
+
+// Returns MR_STEP_SUCCESS, or the code of a support-mapped query that did
+// not resolve.
+template <bool kConvex>
+__device__ unsigned narrowphase(const Collider& A, const Collider& B, int cls, unsigned ia, unsigned ib, float accepted,
+                                RawSink& sink, float3& normal) {
+    if constexpr (kConvex) {
+        if (cls == MR_COLLISION_PAIR_CONVEX) return support_mapped_contacts(A, B, ia, ib, accepted, sink, normal);
+    }
     if (cls == MR_COLLISION_PAIR_SPHERE_SPHERE) {
         const float3 delta = B.c - A.c;
         const float d = len3(delta);
@@ -399,7 +961,7 @@ __device__ bool narrowphase(const Collider& A, const Collider& B, int cls, unsig
         if (sep <= accepted)
             sink.add(A.c + normal * A.radius, B.c - normal * B.radius, sep, feature_key(MR_SHAPE_SPHERE, 0u),
                      feature_key(MR_SHAPE_SPHERE, 0u));
-        return true;
+        return MR_STEP_SUCCESS;
     }
     if (cls == MR_COLLISION_PAIR_SPHERE_BOX) {
         const bool sphere_a = A.type == MR_SHAPE_SPHERE;
@@ -443,7 +1005,7 @@ __device__ bool narrowphase(const Collider& A, const Collider& B, int cls, unsig
                 sink.add(box_point, sphere_point, sep, feature_key(MR_SHAPE_BOX, feat), feature_key(MR_SHAPE_SPHERE, 0u));
         }
         normal = sphere_a ? n : -n;
-        return true;
+        return MR_STEP_SUCCESS;
     }
     if (cls == MR_COLLISION_PAIR_SPHERE_CAPSULE) {
         const bool sphere_a = A.type == MR_SHAPE_SPHERE;
@@ -463,7 +1025,7 @@ __device__ bool narrowphase(const Collider& A, const Collider& B, int cls, unsig
             else sink.add(pc, ps, sep, fc, fs);
         }
         normal = sphere_a ? n : -n;
-        return true;
+        return MR_STEP_SUCCESS;
     }
     if (cls == MR_COLLISION_PAIR_CAPSULE_CAPSULE) {
         float3 pa, pb;
@@ -476,7 +1038,7 @@ __device__ bool narrowphase(const Collider& A, const Collider& B, int cls, unsig
         if (sep <= accepted)
             sink.add(pa + normal * A.radius, pb - normal * B.radius, sep, feature_key(MR_SHAPE_CAPSULE, capsule_feature(ta)),
                      feature_key(MR_SHAPE_CAPSULE, capsule_feature(tb)));
-        return true;
+        return MR_STEP_SUCCESS;
     }
     if (cls == MR_COLLISION_PAIR_CAPSULE_BOX) {
         const bool capsule_a = A.type == MR_SHAPE_CAPSULE;
@@ -490,7 +1052,7 @@ __device__ bool narrowphase(const Collider& A, const Collider& B, int cls, unsig
             else sink.add(w.box_point, w.cap_point, w.sep, fb, fc);
         }
         normal = capsule_a ? w.normal : -w.normal;
-        return true;
+        return MR_STEP_SUCCESS;
     }
     if (cls == MR_COLLISION_PAIR_BOX_BOX) {
         const float3 cd = B.c - A.c;
@@ -517,7 +1079,7 @@ __device__ bool narrowphase(const Collider& A, const Collider& B, int cls, unsig
             const float sep = fabsf(proj) - box_radius(A, axis) - box_radius(B, axis);
             if (sep > accepted) {
                 normal = axis;
-                return true;  // separated: no contact
+                return MR_STEP_SUCCESS;  // separated: no contact
             }
             const float tol = kAxisTie * (1.0f + fmaxf(fabsf(best_sep), fabsf(sep)));
             if (!isfinite(best_sep) || sep > best_sep + tol || (fabsf(sep - best_sep) <= tol && index < best_axis)) {
@@ -551,7 +1113,7 @@ __device__ bool narrowphase(const Collider& A, const Collider& B, int cls, unsig
             sink.add(pa, pb, dot3(pb - pa, best_n), feature_key(MR_SHAPE_BOX, 256u + static_cast<unsigned>(best_axis)),
                      feature_key(MR_SHAPE_BOX, 256u + static_cast<unsigned>(best_axis)));
         }
-        return true;
+        return MR_STEP_SUCCESS;
     }
     // Finite shape (A) against the plane (B).
     const float3 pn = B.normal;
@@ -561,7 +1123,7 @@ __device__ bool narrowphase(const Collider& A, const Collider& B, int cls, unsig
         const float3 surface = A.c - pn * A.radius;
         const float sep = dot3(pn, surface - B.c);
         if (sep <= accepted) sink.add(surface, surface - pn * sep, sep, feature_key(MR_SHAPE_SPHERE, 0u), plane_key);
-        return true;
+        return MR_STEP_SUCCESS;
     }
     if (cls == MR_COLLISION_PAIR_CAPSULE_PLANE) {
         for (int e = 0; e < 2; ++e) {
@@ -570,7 +1132,7 @@ __device__ bool narrowphase(const Collider& A, const Collider& B, int cls, unsig
             if (sep <= accepted)
                 sink.add(surface, surface - pn * sep, sep, feature_key(MR_SHAPE_CAPSULE, static_cast<unsigned>(e)), plane_key);
         }
-        return true;
+        return MR_STEP_SUCCESS;
     }
     if (cls == MR_COLLISION_PAIR_BOX_PLANE) {
         for (int v = 0; v < 8; ++v) {
@@ -578,9 +1140,41 @@ __device__ bool narrowphase(const Collider& A, const Collider& B, int cls, unsig
             const float sep = dot3(pn, w - B.c);
             if (sep <= accepted) sink.add(w, w - pn * sep, sep, feature_key(MR_SHAPE_BOX, static_cast<unsigned>(v)), plane_key);
         }
-        return true;
+        return MR_STEP_SUCCESS;
     }
-    return false;
+    if (cls == MR_COLLISION_PAIR_CYLINDER_PLANE) {
+        // Collision.metal:4627-4800: a cap face parallel to the plane gives
+        // its four-point ring plus the exact rim support, a side parallel to
+        // it the two rim ends, any other pose the one extremal rim point.
+        const float axial = dot3(pn, A.axis), rx = dot3(pn, A.bx), rz = dot3(pn, A.bz);
+        const float3 rproj = A.bx * rx + A.bz * rz;
+        const float rsq = fmaxf(0.0f, rx * rx + rz * rz);
+        auto add = [&](float3 surface, unsigned local) {
+            const float sep = dot3(pn, surface - B.c);
+            if (sep <= accepted) sink.add(surface, surface - pn * sep, sep, feature_key(MR_SHAPE_CYLINDER, local), plane_key);
+        };
+        if (rsq <= kCylAlign * kCylAlign) {
+            const bool pos = axial < 0.0f;
+            const float3 cap = A.c + A.axis * (pos ? A.hl : -A.hl);
+            const unsigned base = pos ? kCylPosRing : kCylNegRing;
+            add(cap + A.bx * A.radius, base + 0u);
+            add(cap - A.bx * A.radius, base + 1u);
+            add(cap + A.bz * A.radius, base + 2u);
+            add(cap - A.bz * A.radius, base + 3u);
+            if (rsq > 0.0f) add(cap - rproj * (A.radius * rsqrtf(rsq)), pos ? kCylPosRim : kCylNegRim);
+            return MR_STEP_SUCCESS;
+        }
+        const float3 rdir = -rproj * rsqrtf(rsq);
+        if (fabsf(axial) <= kCylAlign) {
+            add(A.c - A.axis * A.hl + rdir * A.radius, kCylNegSide);
+            add(A.c + A.axis * A.hl + rdir * A.radius, kCylPosSide);
+            return MR_STEP_SUCCESS;
+        }
+        const bool pos = axial < 0.0f;
+        add(A.c + A.axis * (pos ? A.hl : -A.hl) + rdir * A.radius, pos ? kCylPosRim : kCylNegRim);
+        return MR_STEP_SUCCESS;
+    }
+    return MR_STEP_SUCCESS;
 }
 
 // Persistent manifold of one pair from its raw records and old slot
@@ -791,8 +1385,9 @@ __device__ __forceinline__ float3 sym3_mul(const float* S, float3 x) {
 // At most 128 registers: 16 resident warps per SM.  More warps (96
 // registers) ran slower: their narrowphase scratch no longer fits the L1.
 // kComp: compensated sums for positions (across control steps, through
-// p.q_comp) and for the velocity increments of the sweeps.
-template <bool kComp>
+// p.q_comp) and for the velocity increments of the sweeps.  kConvex: the
+// world has support-mapped (cylinder) pairs.
+template <bool kComp, bool kConvex>
 __global__ void __launch_bounds__(32, 16) scene_step_kernel(SceneParams p) {
     extern __shared__ float4 smem4[];
     float* s = reinterpret_cast<float*>(smem4);
@@ -872,6 +1467,16 @@ __global__ void __launch_bounds__(32, 16) scene_step_kernel(SceneParams p) {
                 const float3 a0 = qrot(qn, f3(0.0f, dm.y, 0.0f)), a1 = qrot(fr, f3(0.0f, dm.y, 0.0f));
                 e0 = f3(fabsf(a0.x) + dm.x, fabsf(a0.y) + dm.x, fabsf(a0.z) + dm.x);
                 e1 = f3(fabsf(a1.x) + dm.x, fabsf(a1.y) + dm.x, fabsf(a1.z) + dm.x);
+            } else if (M.shape_type[b] == MR_SHAPE_CYLINDER) {
+                // Collision.cpp:719-740: per component |a_i| hl + sqrt(1 - a_i^2) r.
+                auto ext = [&](float4 r) {
+                    const float3 a = qrot(r, f3(0.0f, 1.0f, 0.0f));
+                    return f3(fabsf(a.x) * dm.y + sqrtf(fmaxf(0.0f, 1.0f - a.x * a.x)) * dm.x,
+                              fabsf(a.y) * dm.y + sqrtf(fmaxf(0.0f, 1.0f - a.y * a.y)) * dm.x,
+                              fabsf(a.z) * dm.y + sqrtf(fmaxf(0.0f, 1.0f - a.z * a.z)) * dm.x);
+                };
+                e0 = ext(qn);
+                e1 = ext(fr);
             } else {
                 auto ext = [&](float4 r) {
                     const float3 bx = qrot(r, f3(1.0f, 0.0f, 0.0f)), by = qrot(r, f3(0.0f, 1.0f, 0.0f)), bz = qrot(r, f3(0.0f, 0.0f, 1.0f));
@@ -941,7 +1546,7 @@ __global__ void __launch_bounds__(32, 16) scene_step_kernel(SceneParams p) {
         float* new_table = ws + ((sub & 1) ? kWsTable1 : kWsTable0);
         float* scratch = ws + kWsLanes + lane * kLaneScratch;
         int ncount = 0, raw_total = 0;
-        bool bad = false, mover = false;
+        bool bad = false, mover = false, unresolved = false;
         for (int base = 0; base < ncand; base += 32) {
             const int ci = base + lane;
             int nraw = 0;
@@ -968,7 +1573,9 @@ __global__ void __launch_bounds__(32, 16) scene_step_kernel(SceneParams p) {
                 load_collider(M, s, b, B);
                 const float accepted = A.offset + B.offset + (fmaxf(collider_scale(A), collider_scale(B)) + 1.0f) * kQueryPadS;
                 RawSink sink{scratch + 4 * kRecWords, 0, A.bpos, B.bpos, A.brot, B.brot};
-                narrowphase(A, B, M.pair_class[pi], static_cast<unsigned>(a), static_cast<unsigned>(b), accepted, sink, normal);
+                if (narrowphase<kConvex>(A, B, M.pair_class[pi], static_cast<unsigned>(a), static_cast<unsigned>(b), accepted, sink,
+                                         normal) != MR_STEP_SUCCESS)
+                    unresolved = true;
                 nraw = sink.count;
                 posA = A.bpos;
                 rotA = A.brot;
@@ -991,6 +1598,11 @@ __global__ void __launch_bounds__(32, 16) scene_step_kernel(SceneParams p) {
             ncount += __popc(m);
         }
         raw_total = __reduce_add_sync(0xffffffffu, raw_total);
+        if (__any_sync(0xffffffffu, unresolved)) {
+            if (lane == 0) fail(misc, MR_STEP_DID_NOT_CONVERGE, 0u);
+            __syncwarp();
+            break;
+        }
         if (__any_sync(0xffffffffu, bad)) {
             if (lane == 0) fail(misc, MR_STEP_NONFINITE_RESULT, 0u);
             __syncwarp();
@@ -1391,23 +2003,37 @@ size_t scene_step_smem_bytes(bool compensated) {
 }
 size_t scene_workspace_words() { return static_cast<size_t>(kWsWords); }
 
+namespace {
+
+template <typename F>
+cudaError_t for_scene_kernel(bool compensated, bool convex, F&& f) {
+    if (compensated) return convex ? f(scene_step_kernel<true, true>) : f(scene_step_kernel<true, false>);
+    return convex ? f(scene_step_kernel<false, true>) : f(scene_step_kernel<false, false>);
+}
+
+}  // namespace
+
 cudaError_t configure_scene_step_kernel() {
     // The driver's default carveout keeps most of the unified L1 as cache,
     // which the narrowphase scratch and contact records rely on.
-    cudaError_t e = cudaFuncSetAttribute(scene_step_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(scene_step_smem_bytes(false)));
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(scene_step_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(scene_step_smem_bytes(true)));
+    cudaError_t e = cudaSuccess;
+    for (const bool compensated : {false, true})
+        for (const bool convex : {false, true})
+            if (e == cudaSuccess)
+                e = for_scene_kernel(compensated, convex, [&](auto kernel) {
+                    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                static_cast<int>(scene_step_smem_bytes(compensated)));
+                });
     return e;
 }
 
 cudaError_t launch_scene_step(const SceneParams& p, cudaStream_t stream) {
-    if (p.q_comp != nullptr)
-        scene_step_kernel<true><<<p.env_count, 32, scene_step_smem_bytes(true), stream>>>(p);
-    else
-        scene_step_kernel<false><<<p.env_count, 32, scene_step_smem_bytes(false), stream>>>(p);
-    return cudaGetLastError();
+    const bool compensated = p.q_comp != nullptr;
+    const size_t smem = scene_step_smem_bytes(compensated);
+    return for_scene_kernel(compensated, p.support_mapped != 0, [&](auto kernel) {
+        kernel<<<p.env_count, 32, smem, stream>>>(p);
+        return cudaGetLastError();
+    });
 }
 
 }  // namespace numi

@@ -260,6 +260,7 @@ struct MRServerHandle {
             sp.substeps = static_cast<int>(config.physics_substeps);
             sp.velocity_iterations = static_cast<int>(config.velocity_iterations);
             sp.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
+            sp.support_mapped = p.smodel.support_mapped;
             check(numi::launch_scene_step(sp, p.stream), "scene step launch");
         } else {
         numi::StepParams sp{};

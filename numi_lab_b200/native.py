@@ -24,6 +24,7 @@ MR_RUN_SOURCE_SYNTHETIC_CHAIN7: Final = 100
 MR_RUN_SOURCE_SYNTHETIC_TREE29: Final = 101
 MR_RUN_SOURCE_SYNTHETIC_PILE: Final = 102
 MR_RUN_SOURCE_SYNTHETIC_STACK: Final = 103
+MR_RUN_SOURCE_SYNTHETIC_CYLINDER_PILE: Final = 104
 MANIFOLD_POINTS: Final = 4
 MR_PRECISION_FP32: Final = 0
 MR_PRECISION_FP64_ARTICULATED_INERTIA: Final = 1

@@ -26,6 +26,7 @@ SOURCES = {
     "tree29": native.MR_RUN_SOURCE_SYNTHETIC_TREE29,
     "pile": native.MR_RUN_SOURCE_SYNTHETIC_PILE,
     "stack32": native.MR_RUN_SOURCE_SYNTHETIC_STACK,
+    "cylinder_pile": native.MR_RUN_SOURCE_SYNTHETIC_CYLINDER_PILE,
 }
 SCENE_MANIFOLDS = 128      # manifold slots per scene environment
 SCENE_SLOT_WORDS = 57      # MRManifoldC words + pair key

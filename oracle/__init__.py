@@ -367,6 +367,9 @@ class SceneOracle:
         lib.oracle_scene_table_from_device.argtypes = [ct.POINTER(ct.c_float), ct.c_uint32, ct.c_void_p]
         lib.oracle_scene_raw_contacts.restype = ct.c_uint32
         lib.oracle_scene_raw_contacts.argtypes = [ct.c_void_p, _DP, ct.c_uint32, ct.c_uint32, ct.c_double, ct.c_double, _DP]
+        lib.oracle_scene_pair_query.restype = ct.c_uint32
+        lib.oracle_scene_pair_query.argtypes = [ct.c_void_p, _DP, ct.c_uint32, ct.c_uint32, ct.c_uint32, _DP,
+                                                ct.POINTER(ct.c_uint32), ct.POINTER(ct.c_uint32)]
         self.records = records
         w = records.world
         self.nb = int(w.body_count) - 1
@@ -417,6 +420,16 @@ class SceneOracle:
         n = self.lib.oracle_scene_raw_contacts(self.handle, _dp(np.ascontiguousarray(q, np.float64)), a, b, margin_a, margin_b,
                                                _dp(out))
         return out[:n].copy()
+
+    def pair_query(self, q: np.ndarray, a: int, b: int, pair_class: int) -> tuple[int, np.ndarray, int]:
+        """Raw contacts of pair (a, b) under `pair_class` (11: support-mapped GJK / EPA / MPR);
+        (status, rows [n, 12], path: 0 GJK distance, 3 EPA, 1 MPR)."""
+
+        out = np.zeros((8, 12))
+        st, path = ct.c_uint32(0), ct.c_uint32(0)
+        n = self.lib.oracle_scene_pair_query(self.handle, _dp(np.ascontiguousarray(q, np.float64)), a, b, pair_class, _dp(out),
+                                             ct.byref(st), ct.byref(path))
+        return int(st.value), out[:n].copy(), int(path.value)
 
 
 class ReferenceScene:

@@ -1494,6 +1494,8 @@ typedef struct {
     double radius, offset;
     v3 lo, hi, normal;
     v3 e0, e1; /* capsule segment endpoints (local -Y / +Y ends) */
+    v3 axis, bx, bz; /* cylinder axis (local +Y) and disk basis */
+    double hl;       /* cylinder half length */
     v3 bpos; /* pose of the collider's body: the frame of its manifold anchors */
     q4 brot;
 } SCol;
@@ -1517,6 +1519,8 @@ static void scol(const OracleScene* s, const SState* st, uint32_t b, SCol* o) {
         o->offset = s->plane_offset;
         o->lo = o->hi = V(0, 0, 0);
         o->e0 = o->e1 = o->c;
+        o->axis = o->bx = o->bz = V(0, 0, 0);
+        o->hl = 0.0;
         o->bpos = s->ground_pos;
         o->brot = s->ground_rot;
         return;
@@ -1535,6 +1539,20 @@ static void scol(const OracleScene* s, const SState* st, uint32_t b, SCol* o) {
         o->e1 = vadd(o->c, axis);
     } else {
         o->e0 = o->e1 = o->c;
+    }
+    o->hl = s->dims[b][1];
+    if (o->type == MR_SHAPE_CYLINDER) {
+        /* Collision.metal:759-784: unit axis, disk basis X orthogonalised
+         * against it, Z = X x axis. */
+        const v3 ax = qrot(o->r, V(0, 1, 0));
+        o->axis = vmul(ax, 1.0 / vlen(ax));
+        v3 bx = qrot(o->r, V(1, 0, 0));
+        bx = vsub(bx, vmul(o->axis, vdot(o->axis, bx)));
+        o->bx = vmul(bx, 1.0 / vlen(bx));
+        const v3 bz = vcross(o->bx, o->axis);
+        o->bz = vmul(bz, 1.0 / vlen(bz));
+    } else {
+        o->axis = o->bx = o->bz = V(0, 0, 0);
     }
     o->normal = V(0, 0, 0);
     o->bpos = o->c;
@@ -1580,6 +1598,8 @@ static v3 scoincident(uint32_t a, uint32_t b) {
 
 typedef struct {
     int n;
+    uint32_t status; /* a support-mapped query that failed (MR_STEP_*), else 0 */
+    uint32_t path;   /* support-mapped queries: 0 GJK distance, 3 EPA, 1 MPR */
     double sep[8];
     v3 pa[8], pb[8];
     uint32_t fa[8], fb[8];
@@ -1768,8 +1788,620 @@ static SCapBox scapsule_box(const SCol* cap, const SCol* box, uint32_t ic, uint3
     return w;
 }
 
+/* ---- Support-mapped queries: GJK, EPA and the cylinder patch ---------------
+ * Restates the reference's primitive-GJK class (MR_WORLD_WORK_PRIMITIVE_GJK,
+ * Collision.metal:8026-8045): supports 1756-1972, simplex reduction
+ * 1974-2296, gjkDistance 2298-2427, epaPenetration 2511-2783, the support
+ * patch 3279-3432 and supportMappedContacts 3434-3620.  The device kernel
+ * runs the same steps in FP32; the query cache that warm-starts the
+ * reference's GJK direction is not kept (the first direction is always the
+ * centre difference).  EPA orients its faces against an interior point
+ * (see sface).  A query that neither EPA nor the MPR fallback resolves
+ * fails the step with MR_STEP_DID_NOT_CONVERGE, as in the reference. */
+#define GJK_ITERS 32  /* MR_GJK_MAX_ITERATIONS, engine_types.h:56 */
+#define EPA_ITERS 48  /* MR_EPA_MAX_ITERATIONS */
+#define EPA_VERTS 64  /* MR_EPA_VERTEX_CAPACITY */
+#define EPA_FACES 128 /* MR_EPA_FACE_CAPACITY */
+static const double kCylAlign = 1.0e-6; /* Collision.metal:21 */
+enum { kCylNegRing = 0u, kCylPosRing = 4u, kCylNegSide = 8u, kCylPosSide = 9u, kCylNegRim = 10u, kCylPosRim = 11u };
+/* Weight / barycentric near-ties that may pick another feature in FP32. */
+static const double kFeatureTie = 1.0e-4;
+
+typedef struct {
+    v3 w, pa, pb; /* Minkowski point A - B and its two supports */
+    uint32_t fa, fb;
+} SSup;
+
+static v3 sdeterministic(uint32_t key) {
+    const uint32_t axis = key % 3u;
+    const double sign = (key & 4u) == 0u ? 1.0 : -1.0;
+    return V(axis == 0 ? sign : 0.0, axis == 1 ? sign : 0.0, axis == 2 ? sign : 0.0);
+}
+
+/* Support point of a finite shape along d (normalised here). */
+static v3 ssupport(const SCol* k, uint32_t index, v3 d, uint32_t* feat) {
+    const double dd = vdot(d, d);
+    d = (!(dd > kSceneTiny) || !isfinite(dd)) ? sdeterministic(index) : vmul(d, 1.0 / sqrt(dd));
+    if (k->type == MR_SHAPE_SPHERE) {
+        *feat = feature_key(MR_SHAPE_SPHERE, 0u);
+        return vadd(k->c, vmul(d, k->radius));
+    }
+    if (k->type == MR_SHAPE_CAPSULE) {
+        const double proj = vdot(d, vsub(k->e1, k->e0));
+        BAND(proj, 0.0);
+        const int pos = proj >= 0.0;
+        *feat = feature_key(MR_SHAPE_CAPSULE, pos ? 1u : 0u);
+        return vadd(pos ? k->e1 : k->e0, vmul(d, k->radius));
+    }
+    if (k->type == MR_SHAPE_BOX) {
+        const v3 l = qrotinv(k->r, d);
+        /* A direction across a face or edge picks its vertex by rounding. */
+        BAND(l.x, 0.0);
+        BAND(l.y, 0.0);
+        BAND(l.z, 0.0);
+        uint32_t v = 0u;
+        v3 p = V(-k->half.x, -k->half.y, -k->half.z);
+        if (l.x >= 0.0) { v |= 1u; p.x = k->half.x; }
+        if (l.y >= 0.0) { v |= 2u; p.y = k->half.y; }
+        if (l.z >= 0.0) { v |= 4u; p.z = k->half.z; }
+        *feat = feature_key(MR_SHAPE_BOX, v);
+        return vadd(k->c, qrot(k->r, p));
+    }
+    /* cylinder */
+    const double axial = vdot(d, k->axis);
+    const v3 radial = vsub(d, vmul(k->axis, axial));
+    const double rsq = vdot(radial, radial);
+    const v3 rdir = rsq > kSceneTiny ? vmul(radial, 1.0 / sqrt(rsq)) : k->bx;
+    const int pos = axial >= 0.0;
+    uint32_t local = pos ? kCylPosRim : kCylNegRim;
+    BAND(fabs(axial), kCylAlign);
+    if (fabs(axial) <= kCylAlign) {
+        const double x = vdot(rdir, k->bx), z = vdot(rdir, k->bz);
+        local = 32u + (fabs(x) >= fabs(z) ? (x >= 0.0 ? 0u : 1u) : (z >= 0.0 ? 2u : 3u));
+    } else if (rsq <= kSceneTiny) {
+        local = pos ? 17u : 16u;
+    }
+    *feat = feature_key(MR_SHAPE_CYLINDER, local);
+    return vadd(vadd(k->c, vmul(k->axis, pos ? k->hl : -k->hl)), vmul(rdir, k->radius));
+}
+
+static void sminkowski(const SCol* A, const SCol* B, uint32_t ia, uint32_t ib, v3 d, SSup* o) {
+    o->pa = ssupport(A, ia, d, &o->fa);
+    o->pb = ssupport(B, ib, vmul(d, -1.0), &o->fb);
+    o->w = vsub(o->pa, o->pb);
+}
+
+/* Closest point to the origin on triangle abc with its barycentric weights
+ * (the Voronoi-region walk of Ericson, Real-Time Collision Detection 5.1.5). */
+static v3 sclosest_triangle(v3 a, v3 b, v3 c, double* wt) {
+    const v3 ab = vsub(b, a), ac = vsub(c, a), ap = vmul(a, -1.0);
+    const double d1 = vdot(ab, ap), d2 = vdot(ac, ap);
+    if (d1 <= 0.0 && d2 <= 0.0) { wt[0] = 1; wt[1] = 0; wt[2] = 0; return a; }
+    const v3 bp = vmul(b, -1.0);
+    const double d3 = vdot(ab, bp), d4 = vdot(ac, bp);
+    if (d3 >= 0.0 && d4 <= d3) { wt[0] = 0; wt[1] = 1; wt[2] = 0; return b; }
+    const double vc = d1 * d4 - d3 * d2;
+    if (vc <= 0.0 && d1 >= 0.0 && d3 <= 0.0) {
+        const double den = d1 - d3, v = den > kSceneTiny ? d1 / den : 0.0;
+        wt[0] = 1.0 - v; wt[1] = v; wt[2] = 0;
+        return vadd(a, vmul(ab, v));
+    }
+    const v3 cp = vmul(c, -1.0);
+    const double d5 = vdot(ab, cp), d6 = vdot(ac, cp);
+    if (d6 >= 0.0 && d5 <= d6) { wt[0] = 0; wt[1] = 0; wt[2] = 1; return c; }
+    const double vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) {
+        const double den = d2 - d6, w = den > kSceneTiny ? d2 / den : 0.0;
+        wt[0] = 1.0 - w; wt[1] = 0; wt[2] = w;
+        return vadd(a, vmul(ac, w));
+    }
+    const double va = d3 * d6 - d5 * d4;
+    if (va <= 0.0 && (d4 - d3) >= 0.0 && (d5 - d6) >= 0.0) {
+        const double den = (d4 - d3) + (d5 - d6), w = den > kSceneTiny ? (d4 - d3) / den : 0.0;
+        wt[0] = 0; wt[1] = 1.0 - w; wt[2] = w;
+        return vadd(b, vmul(vsub(c, b), w));
+    }
+    const double den = va + vb + vc;
+    if (!(fabs(den) > kSceneTiny) || !isfinite(den)) { wt[0] = 1; wt[1] = 0; wt[2] = 0; return a; }
+    const double v = vb / den, w = vc / den;
+    wt[0] = 1.0 - v - w; wt[1] = v; wt[2] = w;
+    return vadd(vadd(a, vmul(ab, v)), vmul(ac, w));
+}
+
+/* Drops vertices of weight <= 1e-7 (keeps the heaviest if none is left)
+ * and renormalises. */
+static void scompress(SSup* sx, int* n, double* wt) {
+    SSup keep[4];
+    double kw[4];
+    int m = 0, best = 0;
+    for (int i = 1; i < *n; ++i)
+        if (wt[i] > wt[best]) best = i;
+    for (int i = 0; i < *n; ++i)
+        if (wt[i] > 1.0e-7) { keep[m] = sx[i]; kw[m] = wt[i]; ++m; }
+    if (m == 0) { keep[0] = sx[best]; kw[0] = 1.0; m = 1; }
+    double tot = 0.0;
+    for (int i = 0; i < m; ++i) tot += kw[i];
+    const double inv = tot > kSceneTiny ? 1.0 / tot : 1.0;
+    for (int i = 0; i < m; ++i) { sx[i] = keep[i]; wt[i] = kw[i] * inv; }
+    *n = m;
+}
+
+static double striple(v3 a, v3 b, v3 c) { return vdot(a, vcross(b, c)); }
+
+/* Closest point of the simplex to the origin; returns 1 when a tetrahedron
+ * contains it. */
+static int sclosest_simplex(SSup* sx, int* n, double* wt, v3* closest) {
+    if (*n == 1) { wt[0] = 1.0; *closest = sx[0].w; return 0; }
+    if (*n == 2) {
+        const v3 a = sx[0].w, e = vsub(sx[1].w, a);
+        const double den = vdot(e, e);
+        const double t = den > kSceneTiny ? fmin(fmax(-vdot(a, e) / den, 0.0), 1.0) : 0.0;
+        wt[0] = 1.0 - t;
+        wt[1] = t;
+        *closest = vadd(a, vmul(e, t));
+        scompress(sx, n, wt);
+        return 0;
+    }
+    if (*n == 3) {
+        *closest = sclosest_triangle(sx[0].w, sx[1].w, sx[2].w, wt);
+        scompress(sx, n, wt);
+        return 0;
+    }
+    const v3 a = sx[0].w, ab = vsub(sx[1].w, a), ac = vsub(sx[2].w, a), ad = vsub(sx[3].w, a);
+    const double det = striple(ab, ac, ad);
+    if (fabs(det) > kSceneTiny && isfinite(det)) {
+        const v3 na = vmul(a, -1.0);
+        const double u = striple(na, ac, ad) / det, v = striple(ab, na, ad) / det, w = striple(ab, ac, na) / det;
+        const double base = 1.0 - u - v - w, tol = -2.0e-6;
+        if (base >= tol && u >= tol && v >= tol && w >= tol) {
+            wt[0] = base; wt[1] = u; wt[2] = v; wt[3] = w;
+            *closest = V(0, 0, 0);
+            return 1;
+        }
+    }
+    static const int faces[4][3] = {{0, 1, 2}, {0, 3, 1}, {0, 2, 3}, {1, 3, 2}};
+    double best = INFINITY, bw[4] = {0, 0, 0, 0};
+    v3 bp = V(0, 0, 0);
+    for (int f = 0; f < 4; ++f) {
+        double tw[3];
+        const v3 p = sclosest_triangle(sx[faces[f][0]].w, sx[faces[f][1]].w, sx[faces[f][2]].w, tw);
+        const double dist = vdot(p, p);
+        if (dist < best) {
+            best = dist;
+            bp = p;
+            bw[0] = bw[1] = bw[2] = bw[3] = 0.0;
+            for (int k = 0; k < 3; ++k) bw[faces[f][k]] = tw[k];
+        }
+    }
+    *closest = bp;
+    for (int i = 0; i < 4; ++i) wt[i] = bw[i];
+    scompress(sx, n, wt);
+    return 0;
+}
+
+typedef struct {
+    uint32_t status;
+    uint32_t path; /* how it was resolved: 0 GJK distance, 3 EPA, 1 MPR (the reference's `fallback`) */
+    v3 normal, pa, pb;
+    double sep;
+    uint32_t fa, fb;
+} SQuery;
+
+/* Witness of the simplex: weighted supports, features of the heaviest vertex. */
+static void switness(const SSup* sx, int n, const double* wt, SQuery* q) {
+    q->pa = q->pb = V(0, 0, 0);
+    int best = 0;
+    for (int i = 0; i < n; ++i) {
+        q->pa = vadd(q->pa, vmul(sx[i].pa, wt[i]));
+        q->pb = vadd(q->pb, vmul(sx[i].pb, wt[i]));
+        if (wt[i] > wt[best]) best = i;
+    }
+    for (int i = 0; i < n; ++i)
+        if (i != best && wt[best] - wt[i] <= kFeatureTie) g_band++;
+    q->fa = sx[best].fa;
+    q->fb = sx[best].fb;
+}
+
+/* GJK distance; returns 1 on overlap (the simplex then seeds EPA). */
+static int sgjk(const SCol* A, const SCol* B, uint32_t ia, uint32_t ib, double scale, SSup* sx, int* n, double* wt,
+                SQuery* q) {
+    const double tol = 32.0 * kFloatEps * scale;
+    v3 d = vsub(B->c, A->c);
+    if (vdot(d, d) <= kSceneTiny) d = sdeterministic(ia * 65537u + ib);
+    *n = 1;
+    sminkowski(A, B, ia, ib, d, &sx[0]);
+    wt[0] = 1.0;
+    v3 closest = sx[0].w;
+    double prev = INFINITY;
+    for (int it = 0; it < GJK_ITERS; ++it) {
+        const double dsq = vdot(closest, closest);
+        if (dsq <= tol * tol) { q->status = MR_STEP_SUCCESS; q->sep = -0.0; return 1; }
+        d = vmul(closest, -1.0);
+        SSup cand;
+        sminkowski(A, B, ia, ib, d, &cand);
+        int dup = 0;
+        for (int i = 0; i < *n; ++i) {
+            const v3 e = vsub(cand.w, sx[i].w);
+            dup = dup || vdot(e, e) <= tol * tol;
+        }
+        const double advance = vdot(cand.w, d) - vdot(closest, d);
+        int done = dup || advance <= tol * fmax(vlen(d), 1.0);
+        if (!done) {
+            sx[(*n)++] = cand;
+            if (sclosest_simplex(sx, n, wt, &closest)) { q->status = MR_STEP_SUCCESS; q->sep = -0.0; return 1; }
+            const double upd = vdot(closest, closest);
+            done = prev < INFINITY && prev - upd <= tol * tol;
+            prev = upd;
+        }
+        if (done) {
+            switness(sx, *n, wt, q);
+            const v3 delta = vsub(q->pb, q->pa);
+            const double dist = vlen(delta);
+            q->normal = dist > tol ? vmul(delta, 1.0 / dist) : vmul(d, 1.0 / vlen(d));
+            q->sep = dist;
+            q->status = MR_STEP_SUCCESS;
+            return 0;
+        }
+    }
+    q->status = MR_STEP_DID_NOT_CONVERGE;
+    return 0;
+}
+
+typedef struct {
+    int a, b, c, active;
+    v3 n;
+    double dist;
+} SFace;
+
+/* Face abc with its outward unit normal and the origin's distance to its
+ * plane.  Outward is taken against `inside`, a point interior to the
+ * polytope (the centroid of the initial tetrahedron); the reference orients
+ * by the origin's side, which is the same whenever the origin is off the
+ * face plane, and ambiguous for a face through the origin (the simplex of a
+ * touching or collinear GJK exit), which this keeps outward. */
+static int sface(const SSup* vx, int a, int b, int c, v3 inside, SFace* f) {
+    v3 n = vcross(vsub(vx[b].w, vx[a].w), vsub(vx[c].w, vx[a].w));
+    const double nn = vdot(n, n);
+    if (!(nn > kSceneTiny) || !isfinite(nn)) return 0;
+    n = vmul(n, 1.0 / sqrt(nn));
+    int second = b, third = c;
+    if (vdot(n, vsub(vx[a].w, inside)) < 0.0) { n = vmul(n, -1.0); second = c; third = b; }
+    const double dist = vdot(n, vx[a].w);
+    f->a = a; f->b = second; f->c = third; f->active = 1; f->n = n; f->dist = dist;
+    return isfinite(dist);
+}
+
+static void shorizon(int* ea, int* eb, int* ne, int a, int b) {
+    for (int e = 0; e < *ne; ++e)
+        if (ea[e] == b && eb[e] == a) {
+            --*ne;
+            ea[e] = ea[*ne];
+            eb[e] = eb[*ne];
+            return;
+        }
+    if (*ne < 3 * EPA_FACES) { ea[*ne] = a; eb[*ne] = b; ++*ne; }
+}
+
+/* EPA from the GJK simplex; returns 1 with the penetration witness. */
+static int sepa(const SCol* A, const SCol* B, uint32_t ia, uint32_t ib, double scale, const SSup* seed, int nseed, SQuery* q) {
+    static __thread SSup vx[EPA_VERTS];
+    static __thread SFace fc[EPA_FACES];
+    static __thread int ea[3 * EPA_FACES], eb[3 * EPA_FACES];
+    int nv = nseed;
+    for (int i = 0; i < nseed; ++i) vx[i] = seed[i];
+    static const double dirs[6][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {-1, 0, 0}, {0, -1, 0}, {0, 0, -1}};
+    for (int k = 0; nv < 4 && k < 6; ++k) {
+        SSup cand;
+        sminkowski(A, B, ia, ib, V(dirs[k][0], dirs[k][1], dirs[k][2]), &cand);
+        int dup = 0;
+        for (int i = 0; i < nv; ++i) {
+            const v3 e = vsub(cand.w, vx[i].w);
+            dup = dup || vdot(e, e) <= 1.0e-12;
+        }
+        if (!dup) vx[nv++] = cand;
+    }
+    if (nv < 4) return 0;
+    for (int f = 0; f < EPA_FACES; ++f) fc[f].active = 0;
+    const v3 inside = vmul(vadd(vadd(vx[0].w, vx[1].w), vadd(vx[2].w, vx[3].w)), 0.25);
+    static const int init[4][3] = {{0, 1, 2}, {0, 3, 1}, {0, 2, 3}, {1, 3, 2}};
+    int nf = 0;
+    for (int f = 0; f < 4; ++f)
+        if (sface(vx, init[f][0], init[f][1], init[f][2], inside, &fc[nf])) ++nf;
+    if (nf < 4) return 0;
+    const double tol = 64.0 * kFloatEps * scale;
+    for (int it = 0; it < EPA_ITERS; ++it) {
+        int best = -1;
+        double bd = INFINITY;
+        for (int f = 0; f < nf; ++f)
+            if (fc[f].active && fc[f].dist < bd) { bd = fc[f].dist; best = f; }
+        if (best < 0) return 0;
+        SSup cand;
+        sminkowski(A, B, ia, ib, fc[best].n, &cand);
+        const double sd = vdot(fc[best].n, cand.w);
+        int dup = 0;
+        for (int i = 0; i < nv; ++i) {
+            const v3 e = vsub(cand.w, vx[i].w);
+            dup = dup || vdot(e, e) <= tol * tol;
+        }
+        if (dup || sd - bd <= tol) {
+            const SFace F = fc[best];
+            double bc[3];
+            sclosest_triangle(vx[F.a].w, vx[F.b].w, vx[F.c].w, bc);
+            q->pa = vadd(vadd(vmul(vx[F.a].pa, bc[0]), vmul(vx[F.b].pa, bc[1])), vmul(vx[F.c].pa, bc[2]));
+            q->pb = vadd(vadd(vmul(vx[F.a].pb, bc[0]), vmul(vx[F.b].pb, bc[1])), vmul(vx[F.c].pb, bc[2]));
+            int fv = F.a;
+            double fw = bc[0];
+            if (bc[1] > fw) { fv = F.b; fw = bc[1]; }
+            if (bc[2] > fw) { fv = F.c; fw = bc[2]; }
+            for (int k = 0; k < 3; ++k) {
+                const int vk = k == 0 ? F.a : (k == 1 ? F.b : F.c);
+                if (vk != fv && fw - bc[k] <= kFeatureTie) g_band++;
+            }
+            q->fa = vx[fv].fa;
+            q->fb = vx[fv].fb;
+            /* The closest face's outward normal of A - B is the direction
+             * that separates B from A: the A -> B contact normal of every
+             * other class.  (Collision.metal:2680 writes its negation.) */
+            q->normal = F.n;
+            q->sep = -bd;
+            q->status = MR_STEP_SUCCESS;
+            q->path = 3u;
+            return vfinite(q->pa) && vfinite(q->pb) && vfinite(q->normal) && isfinite(q->sep);
+        }
+        if (nv >= EPA_VERTS) return 0;
+        const int nvx = nv++;
+        vx[nvx] = cand;
+        int ne = 0;
+        for (int f = 0; f < nf; ++f) {
+            if (!fc[f].active || vdot(fc[f].n, vsub(cand.w, vx[fc[f].a].w)) <= tol) continue;
+            shorizon(ea, eb, &ne, fc[f].a, fc[f].b);
+            shorizon(ea, eb, &ne, fc[f].b, fc[f].c);
+            shorizon(ea, eb, &ne, fc[f].c, fc[f].a);
+            fc[f].active = 0;
+        }
+        if (ne == 0) return 0;
+        for (int e = 0; e < ne; ++e) {
+            int dst = -1;
+            for (int f = 0; f < nf; ++f)
+                if (!fc[f].active) { dst = f; break; }
+            if (dst < 0) {
+                if (nf >= EPA_FACES) return 0;
+                dst = nf++;
+            }
+            if (!sface(vx, ea[e], eb[e], nvx, inside, &fc[dst])) fc[dst].active = 0;
+        }
+    }
+    return 0;
+}
+
+/* MPR fallback (Collision.metal:2786-3193): portal discovery from the
+ * centres' difference, then portal refinement; the witness is the portal
+ * triangle's point nearest the origin, taken along that direction and
+ * never reported as separation (the fallback runs only after an overlap or
+ * a GJK that did not converge). */
+static int smpr_witness(const SCol* A, const SCol* B, uint32_t ia, uint32_t ib, const SSup* portal, SQuery* q) {
+    double wt[3];
+    const v3 closest = sclosest_triangle(portal[1].w, portal[2].w, portal[3].w, wt);
+    q->pa = vadd(vadd(vmul(portal[1].pa, wt[0]), vmul(portal[2].pa, wt[1])), vmul(portal[3].pa, wt[2]));
+    q->pb = vadd(vadd(vmul(portal[1].pb, wt[0]), vmul(portal[2].pb, wt[1])), vmul(portal[3].pb, wt[2]));
+    int fv = 1;
+    double fw = wt[0];
+    if (wt[1] > fw) { fv = 2; fw = wt[1]; }
+    if (wt[2] > fw) { fv = 3; fw = wt[2]; }
+    for (int k = 0; k < 3; ++k)
+        if (k + 1 != fv && fw - wt[k] <= kFeatureTie) g_band++;
+    q->fa = portal[fv].fa;
+    q->fb = portal[fv].fb;
+    v3 d = closest;
+    double dist = vlen(d);
+    const v3 centres = vsub(B->c, A->c);
+    if (!(dist > kSceneTiny)) { d = centres; dist = vlen(d); }
+    d = !(dist > kSceneTiny) ? sdeterministic(ia * 65537u + ib) : vmul(d, 1.0 / dist);
+    if (vdot(d, centres) < 0.0) d = vmul(d, -1.0);
+    double sep = vdot(vsub(q->pb, q->pa), d);
+    if (sep > 0.0) { d = vmul(d, -1.0); sep = -sep; }
+    q->status = MR_STEP_SUCCESS;
+    q->path = 1u;
+    q->normal = d;
+    q->sep = fmin(sep, -0.0);
+    return vfinite(q->pa) && vfinite(q->pb) && vfinite(q->normal) && isfinite(q->sep);
+}
+
+static int smpr(const SCol* A, const SCol* B, uint32_t ia, uint32_t ib, double scale, SQuery* q) {
+    SSup portal[4];
+    memset(portal, 0, sizeof(portal));
+    portal[0].pa = A->c;
+    portal[0].pb = B->c;
+    portal[0].w = vsub(A->c, B->c);
+    const double tol = 64.0 * kFloatEps * scale;
+    if (vdot(portal[0].w, portal[0].w) <= tol * tol) portal[0].w = vadd(portal[0].w, vmul(sdeterministic(ia * 65537u + ib), tol));
+    v3 d = vmul(portal[0].w, -1.0);
+    d = vmul(d, 1.0 / vlen(d));
+    sminkowski(A, B, ia, ib, d, &portal[1]);
+    if (vdot(portal[1].w, d) < -tol) return 0;
+    d = vcross(portal[0].w, portal[1].w);
+    double dd = vdot(d, d);
+    if (!(dd > tol * tol)) { portal[2] = portal[3] = portal[1]; return smpr_witness(A, B, ia, ib, portal, q); }
+    d = vmul(d, 1.0 / sqrt(dd));
+    sminkowski(A, B, ia, ib, d, &portal[2]);
+    if (vdot(portal[2].w, d) < -tol) return 0;
+    d = vcross(vsub(portal[1].w, portal[0].w), vsub(portal[2].w, portal[0].w));
+    dd = vdot(d, d);
+    if (!(dd > tol * tol)) { portal[3] = portal[2]; return smpr_witness(A, B, ia, ib, portal, q); }
+    d = vmul(d, 1.0 / sqrt(dd));
+    if (vdot(d, portal[0].w) > 0.0) {
+        const SSup t = portal[1];
+        portal[1] = portal[2];
+        portal[2] = t;
+        d = vmul(d, -1.0);
+    }
+    int found = 0;
+    for (int it = 0; it < GJK_ITERS; ++it) {
+        sminkowski(A, B, ia, ib, d, &portal[3]);
+        if (vdot(portal[3].w, d) < -tol) return 0;
+        if (vdot(vcross(portal[1].w, portal[3].w), portal[0].w) < -tol) {
+            portal[2] = portal[3];
+        } else if (vdot(vcross(portal[3].w, portal[2].w), portal[0].w) < -tol) {
+            portal[1] = portal[3];
+        } else {
+            found = 1;
+            break;
+        }
+        d = vcross(vsub(portal[1].w, portal[0].w), vsub(portal[2].w, portal[0].w));
+        dd = vdot(d, d);
+        if (!(dd > tol * tol)) { portal[3] = portal[2]; return smpr_witness(A, B, ia, ib, portal, q); }
+        d = vmul(d, 1.0 / sqrt(dd));
+    }
+    if (!found) return 0;
+    for (int it = 0; it < EPA_ITERS; ++it) {
+        d = vcross(vsub(portal[2].w, portal[1].w), vsub(portal[3].w, portal[1].w));
+        dd = vdot(d, d);
+        if (!(dd > kSceneTiny) || !isfinite(dd)) return smpr_witness(A, B, ia, ib, portal, q);
+        d = vmul(d, 1.0 / sqrt(dd));
+        SSup cand;
+        sminkowski(A, B, ia, ib, d, &cand);
+        const double cp = vdot(cand.w, d);
+        const double pp = fmin(vdot(portal[1].w, d), fmin(vdot(portal[2].w, d), vdot(portal[3].w, d)));
+        if (cp - pp <= tol || it + 1 == EPA_ITERS) return smpr_witness(A, B, ia, ib, portal, q);
+        const v3 cc = vcross(cand.w, portal[0].w);
+        if (vdot(portal[1].w, cc) > 0.0) {
+            if (vdot(portal[2].w, cc) > 0.0) portal[1] = cand;
+            else portal[3] = cand;
+        } else if (vdot(portal[3].w, cc) > 0.0) {
+            portal[2] = cand;
+        } else {
+            portal[1] = cand;
+        }
+    }
+    return 0;
+}
+
+static void spatch_add(SRaw* raw, v3 pa, v3 pb, double sep, uint32_t fa, uint32_t fb, double tol2) {
+    for (int i = 0; i < raw->n; ++i) {
+        const v3 da = vsub(raw->pa[i], pa), db = vsub(raw->pb[i], pb);
+        if (vdot(da, da) <= tol2 && vdot(db, db) <= tol2) return;
+    }
+    sraw_add(raw, pa, pb, sep, fa, fb);
+}
+
+/* Extra points of a cylinder's face or side contact: supports along the
+ * query normal tilted by 2e-4 towards the disk basis (cap contact) or the
+ * axis (side contact). */
+static void spatch(const SCol* A, const SCol* B, uint32_t ia, uint32_t ib, double scale, const SQuery* q, SRaw* raw) {
+    const int cyl_a = A->type == MR_SHAPE_CYLINDER;
+    if (!cyl_a && B->type != MR_SHAPE_CYLINDER) return;
+    const double dtol = 32.0 * kFloatEps * scale;
+    const SCol* k = cyl_a ? A : B;
+    const uint32_t kidx = cyl_a ? ia : ib;
+    const v3 sn = cyl_a ? q->normal : vmul(q->normal, -1.0);
+    v3 dirs[4];
+    int nd = 0;
+    const double align = fabs(vdot(sn, k->axis));
+    BAND(align, 0.95);
+    BAND(align, 0.20);
+    if (align >= 0.95) {
+        dirs[0] = k->bx; dirs[1] = vmul(k->bx, -1.0); dirs[2] = k->bz; dirs[3] = vmul(k->bz, -1.0);
+        nd = 4;
+    } else if (align <= 0.20) {
+        dirs[0] = k->axis; dirs[1] = vmul(k->axis, -1.0);
+        nd = 2;
+    }
+    for (int i = 0; i < nd; ++i) {
+        uint32_t f;
+        const v3 p = ssupport(k, kidx, vadd(sn, vmul(dirs[i], 2.0e-4)), &f);
+        const v3 pa = cyl_a ? p : vsub(p, vmul(q->normal, q->sep));
+        const v3 pb = cyl_a ? vadd(p, vmul(q->normal, q->sep)) : p;
+        spatch_add(raw, pa, pb, q->sep, cyl_a ? f : q->fa, cyl_a ? q->fb : f, dtol * dtol);
+    }
+}
+
+/* Contacts of a support-mapped (cylinder) pair; the pair's normal (A -> B). */
+static v3 ssupport_mapped(const SCol* A, const SCol* B, uint32_t ia, uint32_t ib, double acc, SRaw* raw) {
+    const double scale = fmax(scol_scale(A), scol_scale(B)) + 1.0;
+    SSup sx[4];
+    double wt[4] = {0, 0, 0, 0};
+    int n = 0;
+    SQuery q;
+    memset(&q, 0, sizeof(q));
+    q.normal = V(0, 0, 1);
+    const int overlap = sgjk(A, B, ia, ib, scale, sx, &n, wt, &q);
+    if (q.status != MR_STEP_SUCCESS && q.status != MR_STEP_DID_NOT_CONVERGE) { raw->status = q.status; return q.normal; }
+    if (overlap) {
+        /* Primitive pairs resolve with EPA first, MPR second (Collision.metal:3518-3560). */
+        if (!sepa(A, B, ia, ib, scale, sx, n, &q) && !smpr(A, B, ia, ib, scale, &q)) {
+            raw->status = MR_STEP_DID_NOT_CONVERGE;
+            return q.normal;
+        }
+    } else if (q.status == MR_STEP_DID_NOT_CONVERGE) {
+        if (!smpr(A, B, ia, ib, scale, &q)) { raw->status = MR_STEP_DID_NOT_CONVERGE; return q.normal; }
+    }
+    raw->path = q.path;
+    BAND(q.sep, acc);
+    if (q.sep <= acc) {
+        sraw_add(raw, q.pa, q.pb, q.sep, q.fa, q.fb);
+        spatch(A, B, ia, ib, scale, &q, raw);
+    }
+    return q.normal;
+}
+
+/* Cylinder on the plane (Collision.metal:4627-4800, Collision.cpp:2240-2390):
+ * a cap face parallel to the plane gives its four-point ring plus the exact
+ * rim support, a side parallel to it the two rim ends, any other pose the
+ * one extremal rim point. */
+static void scylinder_plane(const SCol* A, const SCol* P, double acc, SRaw* raw) {
+    const v3 pn = P->normal;
+    const uint32_t plane_key = feature_key(MR_SHAPE_PLANE, 0);
+    const double axial = vdot(pn, A->axis), rx = vdot(pn, A->bx), rz = vdot(pn, A->bz);
+    const v3 rproj = vadd(vmul(A->bx, rx), vmul(A->bz, rz));
+    const double rsq = fmax(0.0, rx * rx + rz * rz);
+    BAND(rsq, kCylAlign * kCylAlign);
+    if (rsq <= kCylAlign * kCylAlign) {
+        const int pos = axial < 0.0;
+        const v3 cap = vadd(A->c, vmul(A->axis, pos ? A->hl : -A->hl));
+        const uint32_t base = pos ? kCylPosRing : kCylNegRing;
+        const v3 dirs[4] = {A->bx, vmul(A->bx, -1.0), A->bz, vmul(A->bz, -1.0)};
+        for (int i = 0; i < 4; ++i) {
+            const v3 surface = vadd(cap, vmul(dirs[i], A->radius));
+            const double sep = vdot(pn, vsub(surface, P->c));
+            BAND(sep, acc);
+            if (sep <= acc) sraw_add(raw, surface, vsub(surface, vmul(pn, sep)), sep, feature_key(MR_SHAPE_CYLINDER, base + (uint32_t)i), plane_key);
+        }
+        if (rsq > 0.0) {
+            const v3 surface = vadd(cap, vmul(rproj, -A->radius / sqrt(rsq)));
+            const double sep = vdot(pn, vsub(surface, P->c));
+            BAND(sep, acc);
+            if (sep <= acc)
+                sraw_add(raw, surface, vsub(surface, vmul(pn, sep)), sep, feature_key(MR_SHAPE_CYLINDER, pos ? kCylPosRim : kCylNegRim),
+                         plane_key);
+        }
+        return;
+    }
+    const v3 rdir = vmul(rproj, -1.0 / sqrt(rsq));
+    BAND(fabs(axial), kCylAlign);
+    if (fabs(axial) <= kCylAlign) {
+        for (int i = 0; i < 2; ++i) {
+            const v3 surface = vadd(vadd(A->c, vmul(A->axis, i ? A->hl : -A->hl)), vmul(rdir, A->radius));
+            const double sep = vdot(pn, vsub(surface, P->c));
+            BAND(sep, acc);
+            if (sep <= acc)
+                sraw_add(raw, surface, vsub(surface, vmul(pn, sep)), sep, feature_key(MR_SHAPE_CYLINDER, i ? kCylPosSide : kCylNegSide),
+                         plane_key);
+        }
+        return;
+    }
+    const int pos = axial < 0.0;
+    const v3 surface = vadd(vadd(A->c, vmul(A->axis, pos ? A->hl : -A->hl)), vmul(rdir, A->radius));
+    const double sep = vdot(pn, vsub(surface, P->c));
+    BAND(sep, acc);
+    if (sep <= acc)
+        sraw_add(raw, surface, vsub(surface, vmul(pn, sep)), sep, feature_key(MR_SHAPE_CYLINDER, pos ? kCylPosRim : kCylNegRim), plane_key);
+}
+
 static v3 snarrow(const SCol* A, const SCol* B, int cls, uint32_t ia, uint32_t ib, double acc, SRaw* raw) {
     raw->n = 0;
+    raw->status = 0;
+    raw->path = 0;
+    if (cls == MR_COLLISION_PAIR_CONVEX) return ssupport_mapped(A, B, ia, ib, acc, raw);
     if (cls == MR_COLLISION_PAIR_SPHERE_SPHERE) {
         const v3 d = vsub(B->c, A->c);
         const double len = vlen(d);
@@ -1959,6 +2591,8 @@ static v3 snarrow(const SCol* A, const SCol* B, int cls, uint32_t ia, uint32_t i
                 if (sep <= acc)
                     sraw_add(raw, surface, vsub(surface, vmul(pn, sep)), sep, feature_key(MR_SHAPE_CAPSULE, (uint32_t)e), plane_key);
             }
+        } else if (cls == MR_COLLISION_PAIR_CYLINDER_PLANE) {
+            scylinder_plane(A, B, acc, raw);
         } else if (cls == MR_COLLISION_PAIR_BOX_PLANE) {
             for (int v = 0; v < 8; ++v) {
                 const v3 w = sbox_vertex(A, v);
@@ -2180,6 +2814,19 @@ static uint32_t sbounds(const OracleScene* s, SState* st, uint32_t* fail_index) 
             const v3 a0 = qrot(qn, V(0, s->dims[b][1], 0)), a1 = qrot(fr, V(0, s->dims[b][1], 0));
             e0 = V(fabs(a0.x) + r, fabs(a0.y) + r, fabs(a0.z) + r);
             e1 = V(fabs(a1.x) + r, fabs(a1.y) + r, fabs(a1.z) + r);
+        } else if (s->type[b] == MR_SHAPE_CYLINDER) {
+            /* Collision.cpp:719-740: per component |a_i| hl + sqrt(1 - a_i^2) r. */
+            const double r = s->dims[b][0], hl = s->dims[b][1];
+            const q4 rs[2] = {qn, fr};
+            v3 ex[2];
+            for (int k = 0; k < 2; ++k) {
+                const v3 a = qrot(rs[k], V(0, 1, 0));
+                ex[k] = V(fabs(a.x) * hl + sqrt(fmax(0.0, 1.0 - a.x * a.x)) * r,
+                          fabs(a.y) * hl + sqrt(fmax(0.0, 1.0 - a.y * a.y)) * r,
+                          fabs(a.z) * hl + sqrt(fmax(0.0, 1.0 - a.z * a.z)) * r);
+            }
+            e0 = ex[0];
+            e1 = ex[1];
         } else {
             const q4 rs[2] = {qn, fr};
             v3 ex[2];
@@ -2226,8 +2873,8 @@ static int sflag(const OracleScene* s, const SState* st, uint32_t a, uint32_t b)
     return ok;
 }
 
-uint32_t oracle_scene_raw_contacts(const OracleScene* s, const double* q, uint32_t a, uint32_t b, double margin_a,
-                                   double margin_b, double* out) {
+static uint32_t squery(const OracleScene* s, const double* q, uint32_t a, uint32_t b, double margin_a, double margin_b, int cls,
+                       double* out, uint32_t* status, uint32_t* path) {
     SState* st = (SState*)calloc(1, sizeof(SState));
     for (uint32_t k = 0; k < s->nb; ++k) {
         st->pos[k] = vld(q + 7 * k);
@@ -2239,12 +2886,14 @@ uint32_t oracle_scene_raw_contacts(const OracleScene* s, const double* q, uint32
     SCol A, B;
     scol(s, st, a, &A);
     scol(s, st, b, &B);
-    uint32_t cls = MR_COLLISION_PAIR_UNSUPPORTED;
-    for (uint32_t p = 0; p < s->np; ++p)
-        if (s->pa[p] == a && s->pb[p] == b) cls = s->pc[p];
+    if (cls < 0) {
+        cls = MR_COLLISION_PAIR_UNSUPPORTED;
+        for (uint32_t p = 0; p < s->np; ++p)
+            if (s->pa[p] == a && s->pb[p] == b) cls = s->pc[p];
+    }
     const double acc = A.offset + B.offset + (fmax(scol_scale(&A), scol_scale(&B)) + 1.0) * kPad;
     SRaw raw;
-    const v3 n = snarrow(&A, &B, (int)cls, a, b, acc, &raw);
+    const v3 n = snarrow(&A, &B, cls, a, b, acc, &raw);
     for (int i = 0; i < raw.n; ++i) {
         double* o = out + 12 * i;
         vst(o, n);
@@ -2254,8 +2903,25 @@ uint32_t oracle_scene_raw_contacts(const OracleScene* s, const double* q, uint32
         o[10] = raw.fa[i];
         o[11] = raw.fb[i];
     }
+    if (status) *status = raw.status;
+    if (path) *path = raw.path;
     free(st);
     return (uint32_t)raw.n;
+}
+
+uint32_t oracle_scene_raw_contacts(const OracleScene* s, const double* q, uint32_t a, uint32_t b, double margin_a,
+                                   double margin_b, double* out) {
+    return squery(s, q, a, b, margin_a, margin_b, -1, out, NULL, NULL);
+}
+
+/* One pair under a given pair class: MR_COLLISION_PAIR_CONVEX runs the
+ * support-mapped query (GJK / EPA / MPR) on shapes an analytic class also
+ * handles, so the two can be compared.  `out` as oracle_scene_raw_contacts;
+ * `status` receives a failed query's MR_STEP_* code (0 on success), `path`
+ * how a support-mapped query was resolved (0 GJK distance, 3 EPA, 1 MPR). */
+uint32_t oracle_scene_pair_query(const OracleScene* s, const double* q, uint32_t a, uint32_t b, uint32_t pair_class, double* out,
+                                 uint32_t* status, uint32_t* path) {
+    return squery(s, q, a, b, 0.0, 0.0, (int)pair_class, out, status, path);
 }
 
 void oracle_scene_table_from_device(const float* words, uint32_t count, OracleSceneSlot* out) {
@@ -2316,6 +2982,7 @@ uint32_t oracle_scene_step(const OracleScene* s, double* q, double* v, OracleSce
             const double acc = A.offset + B.offset + (fmax(scol_scale(&A), scol_scale(&B)) + 1.0) * kPad;
             SRaw raw;
             const v3 n = snarrow(&A, &B, s->pc[p], a, b, acc, &raw);
+            if (raw.status) { status = raw.status; fail_index = key; break; }
             raw_total += (uint32_t)raw.n;
             OracleManifold built;
             const int np_ = sbuild(s, old, &raw, n, &built, A.bpos, A.brot, B.bpos, B.brot);
@@ -2570,6 +3237,7 @@ uint32_t oracle_scene_collide(const OracleScene* s, const double* q, OracleScene
         const double acc = A.offset + B.offset + (fmax(scol_scale(&A), scol_scale(&B)) + 1.0) * kPad;
         SRaw raw;
         const v3 n = snarrow(&A, &B, s->pc[p], a, b, acc, &raw);
+        if (raw.status) { status = raw.status; break; }
         for (int i = 0; i < raw.n && nraw < raw_cap; ++i, ++nraw) {
             double* o = raw_out + 16 * nraw;
             o[0] = a;

@@ -2,7 +2,8 @@
 CPU collision (collideCpuReference, src/core/Collision.cpp:2959, compiled
 from its sources into oracle/_ref by oracle/Makefile).
 
-For three seeded synthetic piles (10, 17 and 61 bodies on a plane) the
+For three seeded synthetic piles (10, 17 and 61 bodies on a plane), and
+two piles with cylinders (keys cylinder_seed*), the
 fixture holds a run of consecutive body configurations -- taken from the
 oracle's own simulation of the pile settling, so that boxes and spheres
 rest on the plane and on each other -- and, for each configuration in
@@ -27,16 +28,19 @@ import numi_lab_b200 as nb  # noqa: E402
 from oracle import ReferenceScene, SceneOracle, SceneTable  # noqa: E402
 
 SEEDS = (3, 13, 14)
+# Piles with cylinders ("cylinder_pile"): the reference's CPU collision
+# handles cylinder on the plane and skips cylinder-finite pairs.
+CYLINDER_SEEDS = (5, 11)
 FIRST, COUNT = 30, 8
 OUT = Path(__file__).resolve().parent / "pile_collision.npz"
 
 
 def main() -> None:
     data: dict[str, np.ndarray] = {}
-    for seed in SEEDS:
-        rec = nb.compile_model("pile", seed)
+    for source, seed in [("pile", s) for s in SEEDS] + [("cylinder_pile", s) for s in CYLINDER_SEEDS]:
+        rec = nb.compile_model(source, seed)
         oracle = SceneOracle(rec, 0.005, 4, 8, 0)
-        q, v, f = nb.sample_reset("pile", seed, 1, 0, 1)
+        q, v, f = nb.sample_reset(source, seed, 1, 0, 1)
         q = q[0].astype(np.float64)
         v = v[0].astype(np.float64)
         table = SceneTable()
@@ -51,7 +55,7 @@ def main() -> None:
                 qs.append(q.copy())
                 raws.append(raw)
                 mans.append(man)
-        p = f"seed{seed}_"
+        p = f"seed{seed}_" if source == "pile" else f"cylinder_seed{seed}_"
         data[p + "q"] = np.array(qs)
         data[p + "raw_rows"] = np.array([len(r) for r in raws])
         data[p + "raw"] = np.concatenate(raws)

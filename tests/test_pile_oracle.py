@@ -146,3 +146,103 @@ def test_failed_step_publishes_nothing():
     np.testing.assert_array_equal(np.isnan(q), np.isnan(q0))
     np.testing.assert_array_equal(v, v0)
     assert table.keys() == keys0
+
+
+CYLINDER, CONVEX_CLASS = 4, 11
+RIM_FEATURES = (10, 11)  # general rim points of a cylinder (Collision.metal:26-27)
+
+
+def _rim_conditioning(rec, q):
+    """Rounding bound of a cylinder's general-rim point on the plane: the
+    rim azimuth is -radial / |radial| of the plane normal in the disk basis,
+    so a normal perturbation of ~2e-7 (FP32 plane rotation) moves the point
+    by radius x 2e-7 / |radial| -- large when the cylinder stands nearly
+    upright on its cap."""
+    body = q.reshape(-1, 7)
+
+    def bound(pair, feat, row):
+        a = pair[0]
+        if (feat[0] >> 28) != CYLINDER:
+            return 0.0
+        x, y, z, w = body[a, 3:]
+        u = np.array([x, y, z])
+        v = np.array([0.0, 1.0, 0.0])
+        axis = v + 2.0 * np.cross(u, np.cross(u, v) + w * v)
+        axial = abs(float(np.dot(axis / np.linalg.norm(axis), row[2:5])))
+        radial = np.sqrt(max(1e-30, 1.0 - axial * axial))
+        # The cap-ring and side-rim classes are taken at |axial| or
+        # |radial| <= 1e-6 (Collision.metal:21): within rounding of that
+        # threshold either side may take the other class.
+        if axial <= 1e-5 or radial <= 1e-5:
+            return np.inf
+        if (feat[0] & 0x0FFFFFFF) not in RIM_FEATURES:
+            return 0.0
+        radius = float(rec.shapes[a].dimensions[0])
+        return 4.0 * radius * 2e-7 / radial
+
+    return bound
+
+
+@pytest.mark.reference
+@pytest.mark.parametrize("seed", [5, 8, 11])
+def test_cylinder_pile_collision_matches_reference_live(reference_available, seed):
+    """Piles with cylinders: every class the reference's CPU collision
+    handles -- cylinder on the plane among them -- against the oracle; the
+    reference's CPU skips cylinder-finite pairs (no CPU GJK), so the
+    oracle's support-mapped pairs are left out (they are pinned in
+    tests/test_support_mapped_oracle.py)."""
+    from oracle import ReferenceScene
+
+    rec = nb.compile_model("cylinder_pile", seed)
+    cls = {(int(rec.pairs[i].shape_a), int(rec.pairs[i].shape_b)): int(rec.pairs[i].pair_class)
+           for i in range(int(rec.world.pair_count))}
+    oracle = SceneOracle(rec, H, 4, 8, 0)
+    q, v, f = nb.sample_reset("cylinder_pile", seed, 1, 0, 1)
+    q = q[0].astype(np.float64)
+    v = v[0].astype(np.float64)
+    table, ctable, ref = SceneTable(), SceneTable(), ReferenceScene(rec)
+    tainted: set = set()
+    matched = checked = cylinder_plane = 0
+    for _ in range(100):
+        status, _ = oracle.step(q, v, table, float(f[0]))
+        assert status == 0
+        s1, raw = oracle.collide(q, ctable)
+        s2, raw_ref, man_ref = ref.collide(q)
+        assert s1 == 0 and s2 == 0
+        keep = np.array([cls[(int(r[0]), int(r[1]))] != CONVEX_CLASS for r in raw], bool)
+        tainted |= {(int(r[0]), int(r[1])) for r in raw[~keep]}
+        matched += _pile.compare_raw(rec, raw[keep], raw_ref, tainted, _rim_conditioning(rec, q))["matched"]
+        cylinder_plane += sum(1 for r in raw_ref if cls[(int(r[0]), int(r[1]))] == 5)
+        checked += _pile.compare_manifolds(ctable, man_ref, tainted)
+    assert matched > 1000 and checked > 100
+    assert cylinder_plane > 50
+
+
+@pytest.mark.parametrize("seed", [5, 11])
+def test_cylinder_pile_collision_matches_reference_golden(golden, seed):
+    """The fixture's cylinder piles: the reference's CPU contacts (cylinder
+    on the plane included) against the oracle's, support-mapped pairs left
+    out as in the live test."""
+    p = f"cylinder_seed{seed}_"
+    rec = nb.compile_model("cylinder_pile", seed)
+    fp = np.frombuffer(bytes(rec.bodies) + bytes(rec.shapes), np.uint8)
+    assert np.array_equal(fp, golden[p + "fingerprint"]), "cylinder pile model drifted from the fixture"
+    cls = {(int(rec.pairs[i].shape_a), int(rec.pairs[i].shape_b)): int(rec.pairs[i].pair_class)
+           for i in range(int(rec.world.pair_count))}
+    oracle = SceneOracle(rec, H, 4, 8, 0)
+    table = SceneTable()
+    tainted: set = set()
+    raw_at = np.concatenate([[0], np.cumsum(golden[p + "raw_rows"])])
+    man_at = np.concatenate([[0], np.cumsum(golden[p + "manifold_rows"])])
+    matched = checked = cylinder_plane = 0
+    for k, q in enumerate(golden[p + "q"]):
+        status, raw = oracle.collide(q, table)
+        assert status == 0
+        keep = np.array([cls[(int(r[0]), int(r[1]))] != CONVEX_CLASS for r in raw], bool)
+        tainted |= {(int(r[0]), int(r[1])) for r in raw[~keep]}
+        ref_raw = golden[p + "raw"][raw_at[k]:raw_at[k + 1]]
+        matched += _pile.compare_raw(rec, raw[keep], ref_raw, tainted, _rim_conditioning(rec, q))["matched"]
+        cylinder_plane += sum(1 for r in ref_raw if cls[(int(r[0]), int(r[1]))] == 5)
+        checked += _pile.compare_manifolds(table, golden[p + "manifolds"][man_at[k]:man_at[k + 1]], tainted)
+    assert matched > 0 and checked > 0 and cylinder_plane > 0
+
