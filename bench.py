@@ -783,15 +783,22 @@ def main() -> None:
     mean_points = float(counts.sum(axis=1).mean())
     mean_manifolds = float((counts > 0).sum(axis=1).mean())
 
-    # End-to-end through the reference-shaped C ABI with host buffers.
+    # End-to-end through the reference-shaped C ABI with host buffers: each
+    # advance copies its actions from pinned host memory to the device, runs
+    # the control steps and reads statuses, contacts, observations and the
+    # final q back to host memory, where the caller reads them through the
+    # pointers the C ABI returns (valid until the next advance).  L2 is
+    # flushed before each advance, inside the timed region.
     world.set_state(*warm_state)
     world.set_state_readback(True)
-    host_actions = [actions[args.warmup + i].cpu().numpy() for i in range(min(args.steps, 5))]
-    world.advance_host(host_actions[0], raise_on_failure=False)  # warm the host path
+    host_actions = [actions[args.warmup + i].cpu().pin_memory().numpy() for i in range(min(args.steps, 5))]
+    world.advance_host(host_actions[0], raise_on_failure=False, copy=False)  # warm the host path
     barrier()
     t0 = time.perf_counter()
-    for a in host_actions:
-        world.advance_host(a, raise_on_failure=False)
+    for i, a in enumerate(host_actions):
+        flush.fill_(float(i))
+        torch.cuda.synchronize(device)
+        world.advance_host(a, raise_on_failure=False, copy=False)
     e2e_secs = time.perf_counter() - t0
     e2e_value = ENVS * HORIZON * len(host_actions) * world_size / e2e_secs
     if dist is not None:

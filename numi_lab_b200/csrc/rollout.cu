@@ -378,14 +378,18 @@ struct MRTaskRolloutHandle {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;  // caller-stream handoff
+    // Observation read-back of the host-buffer advance: each control step's
+    // slice is copied on copy_stream while the next step computes.
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_step = nullptr, ev_copies = nullptr;
 
     DeviceBuffer<numi::DeviceModel> d_model;
     DeviceBuffer<float> d_q, d_v, d_manifolds, d_reset_q, d_reset_v, d_friction;
     DeviceBuffer<float> d_qcomp;        // [env][nq] compensation of q's running sums (compensated precision)
     DeviceBuffer<float> d_actions, d_obs;
     DeviceBuffer<std::uint32_t> d_masks, d_status, d_contacts, d_stats;
-    PinnedBuffer<float> h_actions, h_obs, h_final_q;
-    PinnedBuffer<std::uint32_t> h_masks, h_status, h_contacts, h_stats;
+    PinnedBuffer<float> h_obs, h_final_q;
+    PinnedBuffer<std::uint32_t> h_status, h_contacts, h_stats;
     std::vector<float> reset_q, reset_v, friction;
 
     // graph cache keyed by (steps, has masks, obs/status targets)
@@ -397,9 +401,10 @@ struct MRTaskRolloutHandle {
         const void* status;
         const void* contacts;
         std::uint32_t precision;
+        const void* host_obs;
         bool operator<(const GraphKey& o) const {
-            return std::tie(steps, actions, masks, obs, status, contacts, precision) <
-                   std::tie(o.steps, o.actions, o.masks, o.obs, o.status, o.contacts, o.precision);
+            return std::tie(steps, actions, masks, obs, status, contacts, precision, host_obs) <
+                   std::tie(o.steps, o.actions, o.masks, o.obs, o.status, o.contacts, o.precision, o.host_obs);
         }
     };
     std::map<GraphKey, cudaGraphExec_t> graphs;
@@ -415,6 +420,9 @@ struct MRTaskRolloutHandle {
         if (ev_stop) cudaEventDestroy(ev_stop);
         if (ev_in) cudaEventDestroy(ev_in);
         if (ev_out) cudaEventDestroy(ev_out);
+        if (ev_step) cudaEventDestroy(ev_step);
+        if (ev_copies) cudaEventDestroy(ev_copies);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -448,8 +456,11 @@ struct MRTaskRolloutHandle {
     }
 
     // Enqueue `steps` control steps reading actions/masks from device memory.
+    // With `host_obs` (pinned), step k's observation slice is copied there on
+    // copy_stream once step k is done, overlapping step k + 1; `s` waits for
+    // the last copy.
     void enqueue(std::uint32_t steps, const float* actions, const std::uint32_t* masks, float* obs,
-                 std::uint32_t* status, std::uint32_t* contacts, cudaStream_t s) {
+                 std::uint32_t* status, std::uint32_t* contacts, cudaStream_t s, float* host_obs = nullptr) {
         const std::uint32_t na = model.world.action_count;
         const std::uint32_t nobs = model.world.nq + model.world.nv;
         check(cudaMemsetAsync(d_stats.ptr, 0, numi::kStatCount * sizeof(std::uint32_t), s), "clear stats");
@@ -478,7 +489,9 @@ struct MRTaskRolloutHandle {
                 p.q_comp = precision == MR_PRECISION_COMPENSATED ? d_qcomp.ptr : nullptr;
                 p.support_mapped = smodel.support_mapped;
                 check(numi::launch_scene_step(p, s), "scene step launch");
+                if (host_obs && obs) copy_observations(k, obs, host_obs, s);
             }
+            if (host_obs && obs) join_copies(s);
             (void)actions;
             (void)na;
             return;
@@ -506,18 +519,32 @@ struct MRTaskRolloutHandle {
             check(numi::launch_control_step(p, precision == MR_PRECISION_COMPENSATED ? layout_comp : layout, contact, precision,
                                             warps_per_block[precision], s),
                   "control step launch");
+            if (host_obs && obs) copy_observations(k, obs, host_obs, s);
         }
+        if (host_obs && obs) join_copies(s);
+    }
+
+    void copy_observations(std::uint32_t k, const float* obs, float* host_obs, cudaStream_t s) {
+        const size_t slice = static_cast<size_t>(envs) * (model.world.nq + model.world.nv);
+        check(cudaEventRecord(ev_step, s), "event");
+        check(cudaStreamWaitEvent(copy_stream, ev_step, 0), "stream wait");
+        check(cudaMemcpyAsync(host_obs + k * slice, obs + k * slice, slice * sizeof(float), cudaMemcpyDeviceToHost, copy_stream),
+              "observations D2H");
+    }
+    void join_copies(cudaStream_t s) {
+        check(cudaEventRecord(ev_copies, copy_stream), "event");
+        check(cudaStreamWaitEvent(s, ev_copies, 0), "stream wait");
     }
 
     void run(std::uint32_t steps, const float* actions, const std::uint32_t* masks, float* obs, std::uint32_t* status,
-             std::uint32_t* contacts, cudaStream_t s) {
-        const GraphKey key{steps, actions, masks, obs, status, contacts, precision};
+             std::uint32_t* contacts, cudaStream_t s, float* host_obs = nullptr) {
+        const GraphKey key{steps, actions, masks, obs, status, contacts, precision, host_obs};
         auto it = graphs.find(key);
         if (it == graphs.end()) {
             cudaGraph_t graph = nullptr;
             check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
             try {
-                enqueue(steps, actions, masks, obs, status, contacts, s);
+                enqueue(steps, actions, masks, obs, status, contacts, s, host_obs);
             } catch (...) {
                 cudaStreamEndCapture(s, &graph);
                 if (graph) cudaGraphDestroy(graph);
@@ -659,6 +686,9 @@ MR_API MRTaskRolloutHandle* mr_create_task_rollout(const MRRunManifestC* manifes
         check(cudaGetDeviceProperties(&prop, h.device), "cudaGetDeviceProperties");
         h.device_name = prop.name;
         check(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking), "stream");
+        check(cudaStreamCreateWithFlags(&h.copy_stream, cudaStreamNonBlocking), "copy stream");
+        check(cudaEventCreateWithFlags(&h.ev_step, cudaEventDisableTiming), "event");
+        check(cudaEventCreateWithFlags(&h.ev_copies, cudaEventDisableTiming), "event");
         check(cudaEventCreate(&h.ev_start), "event");
         check(cudaEventCreate(&h.ev_stop), "event");
         check(cudaEventCreateWithFlags(&h.ev_in, cudaEventDisableTiming), "event");
@@ -757,16 +787,12 @@ MR_API int mr_task_rollout_advance(MRTaskRolloutHandle* handle, const float* nor
         if (reset_mask_count != 0 && (reset_mask_count != mask_expected || reset_masks == nullptr))
             throw std::invalid_argument("reset_mask_count must be 0 or control_step_count * environment_count");
         const auto wall0 = std::chrono::steady_clock::now();
-        // Caller spans are copied before return (into pinned staging).
-        h.h_actions.resize(expected);
-        std::memcpy(h.h_actions.ptr, normalized_actions, expected * sizeof(float));
+        // Caller spans are copied to the device straight from the caller's
+        // memory; the call returns only after the copies have finished, so
+        // nothing of them is kept past return.
         h.d_actions.resize(expected);
         const bool masks = reset_mask_count != 0;
-        if (masks) {
-            h.h_masks.resize(mask_expected);
-            std::memcpy(h.h_masks.ptr, reset_masks, mask_expected * sizeof(uint32_t));
-            h.d_masks.resize(mask_expected);
-        }
+        if (masks) h.d_masks.resize(mask_expected);
         const size_t nobs = h.model.world.nq + h.model.world.nv;
         h.d_status.resize(mask_expected);
         h.d_contacts.resize(mask_expected);
@@ -779,15 +805,16 @@ MR_API int mr_task_rollout_advance(MRTaskRolloutHandle* handle, const float* nor
         }
         cudaStream_t s = h.stream;
         check(cudaEventRecord(h.ev_start, s), "event");
-        check(cudaMemcpyAsync(h.d_actions.ptr, h.h_actions.ptr, expected * sizeof(float), cudaMemcpyHostToDevice, s), "actions H2D");
-        if (masks) check(cudaMemcpyAsync(h.d_masks.ptr, h.h_masks.ptr, mask_expected * sizeof(uint32_t), cudaMemcpyHostToDevice, s), "masks H2D");
+        if (expected > 0)
+            check(cudaMemcpyAsync(h.d_actions.ptr, normalized_actions, expected * sizeof(float), cudaMemcpyHostToDevice, s),
+                  "actions H2D");
+        if (masks) check(cudaMemcpyAsync(h.d_masks.ptr, reset_masks, mask_expected * sizeof(uint32_t), cudaMemcpyHostToDevice, s), "masks H2D");
         h.run(control_step_count, h.d_actions.ptr, masks ? h.d_masks.ptr : nullptr, h.readback ? h.d_obs.ptr : nullptr,
-              h.d_status.ptr, h.d_contacts.ptr, s);
+              h.d_status.ptr, h.d_contacts.ptr, s, h.readback ? h.h_obs.ptr : nullptr);
         check(cudaMemcpyAsync(h.h_status.ptr, h.d_status.ptr, mask_expected * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "status D2H");
         check(cudaMemcpyAsync(h.h_contacts.ptr, h.d_contacts.ptr, mask_expected * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "contacts D2H");
         check(cudaMemcpyAsync(h.h_stats.ptr, h.d_stats.ptr, numi::kStatCount * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "stats D2H");
         if (h.readback) {
-            check(cudaMemcpyAsync(h.h_obs.ptr, h.d_obs.ptr, mask_expected * nobs * sizeof(float), cudaMemcpyDeviceToHost, s), "obs D2H");
             check(cudaMemcpyAsync(h.h_final_q.ptr, h.d_q.ptr, static_cast<size_t>(h.envs) * h.model.world.nq * sizeof(float),
                                   cudaMemcpyDeviceToHost, s), "final q D2H");
         }

@@ -343,9 +343,13 @@ class World:
         self._lib.check(self._lib.lib.mr_task_rollout_set_state_readback(self._handle, 1 if enabled else 0), "set_state_readback")
 
     def advance_host(
-        self, actions: np.ndarray, reset_masks: np.ndarray | None = None, *, raise_on_failure: bool = True
+        self, actions: np.ndarray, reset_masks: np.ndarray | None = None, *, raise_on_failure: bool = True, copy: bool = True
     ) -> dict[str, Any]:
-        """Reference-shaped synchronous advance with host buffers."""
+        """Reference-shaped synchronous advance with host buffers.
+
+        With ``copy=False`` the returned arrays are views of the rollout's
+        own result memory, valid until the next advance, reset or close --
+        the C ABI's rule for the pointers it returns (c_api.h:680-681)."""
 
         actions = np.ascontiguousarray(actions, np.float32)
         steps = actions.shape[0] if actions.ndim == 3 else 1
@@ -371,15 +375,17 @@ class World:
             raise MetalRoboError(f"mr_task_rollout_advance: {self._lib.last_error()}")
         cells = steps * self.envs
         out: dict[str, Any] = {"counters": counters, "rc": rc}
-        sc = self._lib.lib.mr_task_rollout_status_codes(self._handle)
-        ac = self._lib.lib.mr_task_rollout_active_contacts(self._handle)
-        out["status"] = np.ctypeslib.as_array(sc, shape=(cells,)).reshape(steps, self.envs).copy() if sc else None
-        out["contacts"] = np.ctypeslib.as_array(ac, shape=(cells,)).reshape(steps, self.envs).copy() if ac else None
+
+        def view(ptr, count, shape):
+            if not ptr:
+                return None
+            a = np.ctypeslib.as_array(ptr, shape=(count,)).reshape(shape)
+            return a.copy() if copy else a
+
+        out["status"] = view(self._lib.lib.mr_task_rollout_status_codes(self._handle), cells, (steps, self.envs))
+        out["contacts"] = view(self._lib.lib.mr_task_rollout_active_contacts(self._handle), cells, (steps, self.envs))
         obs = self._lib.lib.mr_task_rollout_actor_observations(self._handle)
         if obs:
-            out["observations"] = (
-                np.ctypeslib.as_array(obs, shape=(cells * self.observation_count,)).reshape(steps, self.envs, -1).copy()
-            )
-            fq = self._lib.lib.mr_task_rollout_final_q(self._handle)
-            out["final_q"] = np.ctypeslib.as_array(fq, shape=(self.envs * self.nq,)).reshape(self.envs, self.nq).copy()
+            out["observations"] = view(obs, cells * self.observation_count, (steps, self.envs, self.observation_count))
+            out["final_q"] = view(self._lib.lib.mr_task_rollout_final_q(self._handle), self.envs * self.nq, (self.envs, self.nq))
         return out
