@@ -455,6 +455,88 @@ MR_API const float* mr_task_rollout_actor_observations(const MRTaskRolloutHandle
 /* reference: include/metalrobo/c_api.h:736-738.  [env][nq]; null unless
  * state readback is enabled. */
 MR_API const float* mr_task_rollout_final_q(const MRTaskRolloutHandle* handle);
+
+/* ---------------------------------------------------------------------- */
+/* Native policy (reference: include/metalrobo/c_api.h:326-372, 597-616,   */
+/* 722-735; src/metal/PolicyInference.metal)                               */
+/* ---------------------------------------------------------------------- */
+
+/* reference: c_api.h:326-332 (same values). */
+typedef enum MRPolicyActivationC {
+    MR_POLICY_ACTIVATION_C_IDENTITY = 0,
+    MR_POLICY_ACTIVATION_C_RELU = 1,
+    MR_POLICY_ACTIVATION_C_TANH = 2,
+    MR_POLICY_ACTIVATION_C_ELU = 3,
+    MR_POLICY_ACTIVATION_C_SILU = 4
+} MRPolicyActivationC;
+
+/* reference: c_api.h:334-342 (same shape).  weights [output][input]. */
+typedef struct MRPolicyDenseLayerC {
+    uint32_t input_count;
+    uint32_t output_count;
+    uint32_t activation;
+    const float* weights;
+    size_t weight_count;
+    const float* bias;
+    size_t bias_count;
+} MRPolicyDenseLayerC;
+
+/* reference: c_api.h:344-372 (same shape).  The actor maps the actor
+ * observation ([q, v], nq + nv values; normalised and clipped to
+ * +-observation_clip when a mean is given) to the action mean; actions are
+ * clamp(action_scale * latent + action_bias, +-action_clip), the latent
+ * being the mean, plus exp(log sigma) times a standard normal draw when
+ * action_log_standard_deviation is given.  The optional critic (one output)
+ * gives the value.  Layers are at most 256 wide, at most 8 deep.  The
+ * fingerprints and contract version are kept and not checked: this
+ * library's worlds are synthetic. */
+typedef struct MRPolicyPackC {
+    const char* id;
+    uint64_t revision;
+    uint64_t contract_version;
+    uint64_t world_fingerprint;
+    uint64_t task_fingerprint;
+    uint64_t observation_fingerprint;
+    uint64_t action_fingerprint;
+    const float* observation_mean;
+    size_t observation_mean_count;
+    const float* observation_inverse_standard_deviation;
+    size_t observation_inverse_standard_deviation_count;
+    const MRPolicyDenseLayerC* layers;
+    size_t layer_count;
+    const float* critic_observation_mean;
+    size_t critic_observation_mean_count;
+    const float* critic_observation_inverse_standard_deviation;
+    size_t critic_observation_inverse_standard_deviation_count;
+    const MRPolicyDenseLayerC* critic_layers;
+    size_t critic_layer_count;
+    const float* action_log_standard_deviation;
+    size_t action_log_standard_deviation_count;
+    const float* action_bias;
+    size_t action_bias_count;
+    const float* action_scale;
+    size_t action_scale_count;
+    float observation_clip;
+    float action_clip;
+} MRPolicyPackC;
+
+/* reference: c_api.h:597-603.  Copies every span; later advances take no
+ * action stream (action count 0) and evaluate the policy on the device
+ * before each control step, from the resident state. */
+MR_API int mr_task_rollout_set_policy(MRTaskRolloutHandle* handle, const MRPolicyPackC* policy);
+/* reference: c_api.h:610-614.  0 when no policy is installed. */
+MR_API uint64_t mr_task_rollout_policy_revision(const MRTaskRolloutHandle* handle);
+/* reference: c_api.h:615-616. */
+MR_API int mr_task_rollout_clear_policy(MRTaskRolloutHandle* handle);
+/* reference: c_api.h:722-735.  Outputs of the last policy-driven advance:
+ * latents [step][env][action], log-probabilities and values [step][env],
+ * bootstrap values [env] (the critic on the final state when the advance
+ * asked for evaluate_final_policy; zeros without a critic).  Null when the
+ * last advance ran no policy. */
+MR_API const float* mr_task_rollout_policy_latents(const MRTaskRolloutHandle* handle);
+MR_API const float* mr_task_rollout_policy_log_probabilities(const MRTaskRolloutHandle* handle);
+MR_API const float* mr_task_rollout_policy_values(const MRTaskRolloutHandle* handle);
+MR_API const float* mr_task_rollout_bootstrap_policy_values(const MRTaskRolloutHandle* handle);
 /* reference: include/metalrobo/c_api.h:742-746.  Packed [env][scene body]
  * [position xyz, orientation xyzw, linear xyz, angular xyz]; scene bodies
  * are the free bodies of the pile and stack worlds. */

@@ -11,6 +11,7 @@
 #include "layout.h"
 #include "model.h"
 #include "numi_b200.h"
+#include "policy.h"
 #include "runtime.h"
 #include "scene.h"
 
@@ -354,6 +355,16 @@ numi::SceneModel numi::rt::pack_scene(const numi::CompiledModel& m, float h) {
     return d;
 }
 
+// A policy installed on a rollout (mr_task_rollout_set_policy): every span
+// copied into one device arena, the launch parameters pointing into it.
+struct InstalledPolicy {
+    std::uint64_t revision = 0;
+    std::string id;
+    DeviceBuffer<float> arena;
+    numi::PolicyParams params{};  // arena pointers; state and output pointers are set per launch
+    bool has_critic = false;
+};
+
 struct MRTaskRolloutHandle {
     numi::CompiledModel model;
     numi::DeviceModel dmodel{};
@@ -386,6 +397,14 @@ struct MRTaskRolloutHandle {
     DeviceBuffer<numi::DeviceModel> d_model;
     DeviceBuffer<float> d_q, d_v, d_manifolds, d_reset_q, d_reset_v, d_friction;
     DeviceBuffer<float> d_qcomp;        // [env][nq] compensation of q's running sums (compensated precision)
+    // Native policy: outputs of the last policy-driven advance and the
+    // control-step counter that keys its draws.
+    std::unique_ptr<InstalledPolicy> policy;
+    DeviceBuffer<float> d_latents, d_log_prob, d_values;
+    PinnedBuffer<float> h_latents, h_log_prob, h_values;
+    DeviceBuffer<unsigned long long> d_policy_steps;
+    bool have_policy_outputs = false;
+    std::uint32_t last_policy_steps = 0;
     DeviceBuffer<float> d_actions, d_obs;
     DeviceBuffer<std::uint32_t> d_masks, d_status, d_contacts, d_stats;
     PinnedBuffer<float> h_obs, h_final_q;
@@ -402,9 +421,16 @@ struct MRTaskRolloutHandle {
         const void* contacts;
         std::uint32_t precision;
         const void* host_obs;
+        const void* policy;  // installed policy's arena, or null
+        bool evaluate_final;
+        const void* latents;  // policy outputs (reallocated when an advance needs more room)
+        const void* log_prob;
+        const void* values;
         bool operator<(const GraphKey& o) const {
-            return std::tie(steps, actions, masks, obs, status, contacts, precision, host_obs) <
-                   std::tie(o.steps, o.actions, o.masks, o.obs, o.status, o.contacts, o.precision, o.host_obs);
+            return std::tie(steps, actions, masks, obs, status, contacts, precision, host_obs, policy, evaluate_final, latents,
+                            log_prob, values) <
+                   std::tie(o.steps, o.actions, o.masks, o.obs, o.status, o.contacts, o.precision, o.host_obs, o.policy,
+                            o.evaluate_final, o.latents, o.log_prob, o.values);
         }
     };
     std::map<GraphKey, cudaGraphExec_t> graphs;
@@ -496,7 +522,9 @@ struct MRTaskRolloutHandle {
             (void)na;
             return;
         }
+        const bool driven = policy != nullptr;
         for (std::uint32_t k = 0; k < steps; ++k) {
+            if (driven) enqueue_policy(k, const_cast<float*>(actions) + static_cast<size_t>(k) * envs * na, true, s);
             numi::StepParams p{};
             p.model = d_model.ptr;
             p.q = d_q.ptr;
@@ -521,7 +549,71 @@ struct MRTaskRolloutHandle {
                   "control step launch");
             if (host_obs && obs) copy_observations(k, obs, host_obs, s);
         }
+        if (driven) {
+            if (evaluate_final) enqueue_policy(steps, nullptr, false, s);
+            check(numi::launch_policy_counter(d_policy_steps.ptr, steps, s), "policy counter");
+        }
         if (host_obs && obs) join_copies(s);
+    }
+
+    // Checks an advance's policy arguments and sizes the policy outputs.
+    void prepare_policy(std::uint32_t steps, std::uint64_t revision, std::uint32_t evaluate_final_policy) {
+        have_policy_outputs = false;
+        if (!policy) {
+            if (revision != 0 || evaluate_final_policy != 0)
+                throw std::invalid_argument("no native policy is installed on this rollout (mr_task_rollout_set_policy)");
+            evaluate_final = false;
+            return;
+        }
+        if (revision != 0 && revision != policy->revision)
+            throw std::invalid_argument("policy_revision " + std::to_string(revision) + " differs from the installed revision " +
+                                        std::to_string(policy->revision));
+        evaluate_final = evaluate_final_policy != 0;
+        const size_t cells = static_cast<size_t>(steps) * envs;
+        const size_t na = model.world.action_count;
+        d_actions.resize(cells * na);
+        d_latents.resize(cells * na);
+        d_log_prob.resize(cells);
+        d_values.resize(cells + envs);
+        if (!d_policy_steps.ptr) {
+            d_policy_steps.resize(1);
+            check(cudaMemsetAsync(d_policy_steps.ptr, 0, sizeof(unsigned long long), stream), "policy counter");
+        }
+    }
+    void read_policy_outputs(std::uint32_t steps, cudaStream_t s) {
+        if (!policy) return;
+        const size_t cells = static_cast<size_t>(steps) * envs;
+        const size_t na = model.world.action_count;
+        h_latents.resize(cells * na);
+        h_log_prob.resize(cells);
+        h_values.resize(cells + envs);
+        check(cudaMemcpyAsync(h_latents.ptr, d_latents.ptr, cells * na * sizeof(float), cudaMemcpyDeviceToHost, s), "latents D2H");
+        check(cudaMemcpyAsync(h_log_prob.ptr, d_log_prob.ptr, cells * sizeof(float), cudaMemcpyDeviceToHost, s), "log-probabilities D2H");
+        if (!evaluate_final) check(cudaMemsetAsync(d_values.ptr + cells, 0, envs * sizeof(float), s), "bootstrap values");
+        check(cudaMemcpyAsync(h_values.ptr, d_values.ptr, (cells + envs) * sizeof(float), cudaMemcpyDeviceToHost, s), "values D2H");
+        have_policy_outputs = true;
+        last_policy_steps = steps;
+    }
+
+    // Policy evaluation before control step k (k == steps: the final state,
+    // values into the bootstrap slot) writing step k's actions.
+    bool evaluate_final = false;
+    void enqueue_policy(std::uint32_t k, float* actions_k, bool step, cudaStream_t s) {
+        numi::PolicyParams pp = policy->params;
+        pp.q = d_q.ptr;
+        pp.v = d_v.ptr;
+        pp.nq = static_cast<int>(model.world.nq);
+        pp.nv = static_cast<int>(model.world.nv);
+        pp.envs = static_cast<int>(envs);
+        pp.na = static_cast<int>(model.world.action_count);
+        const size_t cells = static_cast<size_t>(k) * envs;
+        pp.actions = step ? actions_k : nullptr;
+        pp.latents = step ? d_latents.ptr + cells * pp.na : nullptr;
+        pp.log_prob = step ? d_log_prob.ptr + cells : nullptr;
+        pp.values = d_values.ptr + cells;  // slot `steps` holds the bootstrap values
+        pp.step_base = d_policy_steps.ptr;
+        pp.step_offset = static_cast<int>(k);
+        check(numi::launch_policy(pp, s), "policy launch");
     }
 
     void copy_observations(std::uint32_t k, const float* obs, float* host_obs, cudaStream_t s) {
@@ -538,7 +630,10 @@ struct MRTaskRolloutHandle {
 
     void run(std::uint32_t steps, const float* actions, const std::uint32_t* masks, float* obs, std::uint32_t* status,
              std::uint32_t* contacts, cudaStream_t s, float* host_obs = nullptr) {
-        const GraphKey key{steps, actions, masks, obs, status, contacts, precision, host_obs};
+        const bool driven = policy != nullptr;
+        const GraphKey key{steps, actions, masks, obs, status, contacts, precision, host_obs,
+                           driven ? static_cast<const void*>(policy->arena.ptr) : nullptr, driven && evaluate_final,
+                           driven ? d_latents.ptr : nullptr, driven ? d_log_prob.ptr : nullptr, driven ? d_values.ptr : nullptr};
         auto it = graphs.find(key);
         if (it == graphs.end()) {
             cudaGraph_t graph = nullptr;
@@ -756,6 +851,176 @@ MR_API int mr_task_rollout_set_state_readback(MRTaskRolloutHandle* handle, uint3
     });
 }
 
+namespace {
+
+// Validates a policy pack against the rollout's world and uploads it
+// (transposed weights, vectors with their defaults) as one device arena.
+std::unique_ptr<InstalledPolicy> compile_policy(const MRTaskRolloutHandle& h, const MRPolicyPackC& pk) {
+    using numi::kPolicyMaxLayers;
+    using numi::kPolicyMaxWidth;
+    const std::uint32_t nobs = h.model.world.nq + h.model.world.nv, na = h.model.world.action_count;
+    if (!pk.id || !pk.id[0] || !pk.layers || pk.layer_count == 0)
+        throw std::invalid_argument("policy identity and dense layers are required");
+    if (pk.revision == 0) throw std::invalid_argument("policy revision must be non-zero (zero means no policy)");
+    if (na == 0) throw std::invalid_argument("this world takes no actions; a policy cannot drive it");
+    if (pk.layer_count > static_cast<size_t>(kPolicyMaxLayers) || pk.critic_layer_count > static_cast<size_t>(kPolicyMaxLayers))
+        throw std::invalid_argument("at most " + std::to_string(kPolicyMaxLayers) + " dense layers per network");
+    if (pk.critic_layer_count != 0 && !pk.critic_layers) throw std::invalid_argument("critic layers are null");
+    if (nobs > static_cast<std::uint32_t>(kPolicyMaxWidth))
+        throw std::invalid_argument("the observation is wider than " + std::to_string(kPolicyMaxWidth));
+    if (!(pk.action_clip > 0.0f)) throw std::invalid_argument("action_clip must be positive");
+    auto optional = [](const float* v, size_t n, size_t want, const char* what) {
+        if (n != 0 && (n != want || !v))
+            throw std::invalid_argument(std::string(what) + " must have " + std::to_string(want) + " values (or none)");
+        return n != 0;
+    };
+    const bool norm = optional(pk.observation_mean, pk.observation_mean_count, nobs, "observation_mean");
+    if (optional(pk.observation_inverse_standard_deviation, pk.observation_inverse_standard_deviation_count, nobs,
+                 "observation_inverse_standard_deviation") != norm)
+        throw std::invalid_argument("observation mean and inverse standard deviation go together");
+    const bool cnorm = optional(pk.critic_observation_mean, pk.critic_observation_mean_count, nobs, "critic_observation_mean");
+    if (optional(pk.critic_observation_inverse_standard_deviation, pk.critic_observation_inverse_standard_deviation_count, nobs,
+                 "critic_observation_inverse_standard_deviation") != cnorm)
+        throw std::invalid_argument("critic observation mean and inverse standard deviation go together");
+    if ((norm || cnorm) && !(pk.observation_clip > 0.0f)) throw std::invalid_argument("observation_clip must be positive");
+    const bool stochastic = optional(pk.action_log_standard_deviation, pk.action_log_standard_deviation_count, na,
+                                     "action_log_standard_deviation");
+    const bool has_bias = optional(pk.action_bias, pk.action_bias_count, na, "action_bias");
+    const bool has_scale = optional(pk.action_scale, pk.action_scale_count, na, "action_scale");
+    auto check_chain = [&](const MRPolicyDenseLayerC* L, size_t n, std::uint32_t out, const char* net) {
+        std::uint32_t in = nobs;
+        for (size_t l = 0; l < n; ++l) {
+            const MRPolicyDenseLayerC& d = L[l];
+            const std::string where = std::string(net) + " layer " + std::to_string(l);
+            if (d.input_count != in) throw std::invalid_argument(where + " takes " + std::to_string(d.input_count) + " inputs, expected " + std::to_string(in));
+            if (d.output_count == 0 || d.output_count > static_cast<std::uint32_t>(kPolicyMaxWidth))
+                throw std::invalid_argument(where + " must have 1-" + std::to_string(kPolicyMaxWidth) + " outputs");
+            if (d.activation > MR_POLICY_ACTIVATION_C_SILU) throw std::invalid_argument(where + " has an unknown activation");
+            if (!d.weights || d.weight_count != static_cast<size_t>(d.input_count) * d.output_count)
+                throw std::invalid_argument(where + " needs input_count x output_count weights");
+            if (d.bias_count != 0 && (d.bias_count != d.output_count || !d.bias))
+                throw std::invalid_argument(where + " bias must have output_count values (or none)");
+            in = d.output_count;
+        }
+        if (in != out) throw std::invalid_argument(std::string(net) + " must end in " + std::to_string(out) + " outputs");
+    };
+    check_chain(pk.layers, pk.layer_count, na, "actor");
+    if (pk.critic_layer_count) check_chain(pk.critic_layers, pk.critic_layer_count, 1u, "critic");
+
+    // Arena: per layer [in][out] weights then bias; then the vectors.
+    std::vector<float> arena;
+    auto put = [&](const float* v, size_t n, float fill) {
+        const size_t at = arena.size();
+        for (size_t i = 0; i < n; ++i) arena.push_back(v ? v[i] : fill);
+        while (arena.size() % 4) arena.push_back(0.0f);  // 16-byte aligned spans
+        return at;
+    };
+    std::vector<size_t> w_at, b_at, cw_at, cb_at;
+    auto put_layers = [&](const MRPolicyDenseLayerC* L, size_t n, std::vector<size_t>& wa, std::vector<size_t>& ba) {
+        for (size_t l = 0; l < n; ++l) {
+            const MRPolicyDenseLayerC& d = L[l];
+            std::vector<float> t(static_cast<size_t>(d.input_count) * d.output_count);
+            for (std::uint32_t o = 0; o < d.output_count; ++o)
+                for (std::uint32_t i = 0; i < d.input_count; ++i) t[static_cast<size_t>(i) * d.output_count + o] = d.weights[static_cast<size_t>(o) * d.input_count + i];
+            wa.push_back(put(t.data(), t.size(), 0.0f));
+            ba.push_back(put(d.bias_count ? d.bias : nullptr, d.output_count, 0.0f));
+        }
+    };
+    put_layers(pk.layers, pk.layer_count, w_at, b_at);
+    put_layers(pk.critic_layers, pk.critic_layer_count, cw_at, cb_at);
+    const size_t mean_at = norm ? put(pk.observation_mean, nobs, 0.0f) : 0, inv_at = norm ? put(pk.observation_inverse_standard_deviation, nobs, 0.0f) : 0;
+    const size_t cmean_at = cnorm ? put(pk.critic_observation_mean, nobs, 0.0f) : 0,
+                 cinv_at = cnorm ? put(pk.critic_observation_inverse_standard_deviation, nobs, 0.0f) : 0;
+    const size_t ls_at = stochastic ? put(pk.action_log_standard_deviation, na, 0.0f) : 0;
+    const size_t ab_at = put(has_bias ? pk.action_bias : nullptr, na, 0.0f);
+    const size_t as_at = put(has_scale ? pk.action_scale : nullptr, na, 1.0f);
+
+    auto out = std::make_unique<InstalledPolicy>();
+    out->revision = pk.revision;
+    out->id = pk.id;
+    out->has_critic = pk.critic_layer_count != 0;
+    out->arena.resize(arena.size());
+    check(cudaMemcpy(out->arena.ptr, arena.data(), arena.size() * sizeof(float), cudaMemcpyHostToDevice), "policy upload");
+    const float* base = out->arena.ptr;
+    numi::PolicyParams& pp = out->params;
+    pp.actor_layers = static_cast<int>(pk.layer_count);
+    pp.critic_layers = static_cast<int>(pk.critic_layer_count);
+    for (size_t l = 0; l < pk.layer_count; ++l)
+        pp.actor[l] = numi::PolicyLayer{static_cast<int>(pk.layers[l].input_count), static_cast<int>(pk.layers[l].output_count),
+                                        static_cast<int>(pk.layers[l].activation), 0, base + w_at[l], base + b_at[l]};
+    for (size_t l = 0; l < pk.critic_layer_count; ++l)
+        pp.critic[l] = numi::PolicyLayer{static_cast<int>(pk.critic_layers[l].input_count),
+                                         static_cast<int>(pk.critic_layers[l].output_count),
+                                         static_cast<int>(pk.critic_layers[l].activation), 0, base + cw_at[l], base + cb_at[l]};
+    pp.obs_mean = norm ? base + mean_at : nullptr;
+    pp.obs_inv_std = norm ? base + inv_at : nullptr;
+    pp.critic_mean = cnorm ? base + cmean_at : nullptr;
+    pp.critic_inv_std = cnorm ? base + cinv_at : nullptr;
+    pp.obs_clip = pk.observation_clip;
+    pp.action_clip = pk.action_clip;
+    pp.log_std = stochastic ? base + ls_at : nullptr;
+    pp.action_bias = base + ab_at;
+    pp.action_scale = base + as_at;
+    // Draw key: the rollout seed and the policy revision, mixed (SplitMix64).
+    auto mix = [](std::uint64_t x) {
+        x += 0x9e3779b97f4a7c15ull;
+        x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+        x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+        return x ^ (x >> 31);
+    };
+    pp.key = mix(h.seed) ^ mix(pk.revision ^ 0x5bd1e995ull);
+    return out;
+}
+
+void drop_graphs(MRTaskRolloutHandle& h) {
+    check(cudaStreamSynchronize(h.stream), "sync");
+    for (auto& kv : h.graphs) cudaGraphExecDestroy(kv.second);
+    h.graphs.clear();
+}
+
+}  // namespace
+
+MR_API int mr_task_rollout_set_policy(MRTaskRolloutHandle* handle, const MRPolicyPackC* policy) {
+    return guarded([&] {
+        if (!handle) throw std::invalid_argument("handle is null");
+        if (!policy) throw std::invalid_argument("task-rollout policy is null");
+        if (handle->scene) throw std::invalid_argument("pile and stack worlds take no actions; a policy cannot drive them");
+        check(numi::configure_policy_kernel(), "policy kernel attributes");
+        std::unique_ptr<InstalledPolicy> compiled = compile_policy(*handle, *policy);
+        // Captured graphs hold the previous policy's arena: drop them.
+        drop_graphs(*handle);
+        handle->policy = std::move(compiled);
+        handle->have_policy_outputs = false;
+    });
+}
+
+MR_API uint64_t mr_task_rollout_policy_revision(const MRTaskRolloutHandle* handle) {
+    return handle && handle->policy ? handle->policy->revision : 0u;
+}
+
+MR_API int mr_task_rollout_clear_policy(MRTaskRolloutHandle* handle) {
+    return guarded([&] {
+        if (!handle) throw std::invalid_argument("handle is null");
+        drop_graphs(*handle);
+        handle->policy.reset();
+        handle->have_policy_outputs = false;
+    });
+}
+
+MR_API const float* mr_task_rollout_policy_latents(const MRTaskRolloutHandle* handle) {
+    return handle && handle->have_policy_outputs ? handle->h_latents.ptr : nullptr;
+}
+MR_API const float* mr_task_rollout_policy_log_probabilities(const MRTaskRolloutHandle* handle) {
+    return handle && handle->have_policy_outputs ? handle->h_log_prob.ptr : nullptr;
+}
+MR_API const float* mr_task_rollout_policy_values(const MRTaskRolloutHandle* handle) {
+    return handle && handle->have_policy_outputs ? handle->h_values.ptr : nullptr;
+}
+MR_API const float* mr_task_rollout_bootstrap_policy_values(const MRTaskRolloutHandle* handle) {
+    return handle && handle->have_policy_outputs ? handle->h_values.ptr + static_cast<size_t>(handle->last_policy_steps) * handle->envs
+                                                 : nullptr;
+}
+
 MR_API int mr_task_rollout_set_precision(MRTaskRolloutHandle* handle, uint32_t mode) {
     return guarded([&] {
         if (!handle) throw std::invalid_argument("handle is null");
@@ -774,15 +1039,19 @@ MR_API int mr_task_rollout_advance(MRTaskRolloutHandle* handle, const float* nor
     return guarded([&] {
         if (!handle) throw std::invalid_argument("handle is null");
         if (!advance) throw std::invalid_argument("advance output is null");
-        if (policy_revision != 0 || evaluate_final_policy != 0)
-            throw std::invalid_argument("native policies are not installed on this rollout");
         MRTaskRolloutHandle& h = *handle;
         if (control_step_count == 0) throw std::invalid_argument("control_step_count must be positive");
+        h.prepare_policy(control_step_count, policy_revision, evaluate_final_policy);
+        const bool driven = h.policy != nullptr;
         const size_t na = h.model.world.action_count;
         const size_t expected = static_cast<size_t>(control_step_count) * h.envs * na;
-        if (normalized_action_count != expected || (expected > 0 && normalized_actions == nullptr))
-            throw std::invalid_argument("normalized_action_count must equal control_step_count * environment_count * action_count (" +
-                                        std::to_string(expected) + ")");
+        // With a native policy the advance takes no action stream (c_api.cpp:3783-3795).
+        const size_t action_span = driven ? 0 : expected;
+        if (normalized_action_count != action_span || (action_span > 0 && normalized_actions == nullptr))
+            throw std::invalid_argument("normalized_action_count must equal " +
+                                        std::string(driven ? "0 with a native policy installed" :
+                                                             "control_step_count * environment_count * action_count (" +
+                                                                 std::to_string(expected) + ")"));
         const size_t mask_expected = static_cast<size_t>(control_step_count) * h.envs;
         if (reset_mask_count != 0 && (reset_mask_count != mask_expected || reset_masks == nullptr))
             throw std::invalid_argument("reset_mask_count must be 0 or control_step_count * environment_count");
@@ -805,7 +1074,7 @@ MR_API int mr_task_rollout_advance(MRTaskRolloutHandle* handle, const float* nor
         }
         cudaStream_t s = h.stream;
         check(cudaEventRecord(h.ev_start, s), "event");
-        if (expected > 0)
+        if (action_span > 0)
             check(cudaMemcpyAsync(h.d_actions.ptr, normalized_actions, expected * sizeof(float), cudaMemcpyHostToDevice, s),
                   "actions H2D");
         if (masks) check(cudaMemcpyAsync(h.d_masks.ptr, reset_masks, mask_expected * sizeof(uint32_t), cudaMemcpyHostToDevice, s), "masks H2D");
@@ -814,6 +1083,7 @@ MR_API int mr_task_rollout_advance(MRTaskRolloutHandle* handle, const float* nor
         check(cudaMemcpyAsync(h.h_status.ptr, h.d_status.ptr, mask_expected * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "status D2H");
         check(cudaMemcpyAsync(h.h_contacts.ptr, h.d_contacts.ptr, mask_expected * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "contacts D2H");
         check(cudaMemcpyAsync(h.h_stats.ptr, h.d_stats.ptr, numi::kStatCount * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "stats D2H");
+        h.read_policy_outputs(control_step_count, s);
         if (h.readback) {
             check(cudaMemcpyAsync(h.h_final_q.ptr, h.d_q.ptr, static_cast<size_t>(h.envs) * h.model.world.nq * sizeof(float),
                                   cudaMemcpyDeviceToHost, s), "final q D2H");
@@ -840,9 +1110,15 @@ MR_API int mr_task_rollout_advance_device(MRTaskRolloutHandle* handle, const flo
                                           uint64_t cuda_stream, MRTaskRolloutAdvanceC* advance) {
     return guarded([&] {
         if (!handle) throw std::invalid_argument("handle is null");
-        if (!device_actions && handle->model.world.action_count > 0) throw std::invalid_argument("device_actions is null");
         if (control_step_count == 0) throw std::invalid_argument("control_step_count must be positive");
         MRTaskRolloutHandle& h = *handle;
+        h.prepare_policy(control_step_count, 0, 0);
+        if (h.policy) {
+            // The policy writes the actions; device_actions is not read.
+            h.d_actions.resize(static_cast<size_t>(control_step_count) * h.envs * h.model.world.action_count);
+            device_actions = h.d_actions.ptr;
+        }
+        if (!device_actions && handle->model.world.action_count > 0) throw std::invalid_argument("device_actions is null");
         // The horizon runs (and is graph-captured) on the rollout's own
         // stream; events order it after the caller's prior work and the
         // caller's later work after it.  cuda_stream 0 is the legacy default
@@ -861,6 +1137,7 @@ MR_API int mr_task_rollout_advance_device(MRTaskRolloutHandle* handle, const flo
         const auto wall0 = std::chrono::steady_clock::now();
         if (advance) check(cudaEventRecord(h.ev_start, s), "event");
         h.run(control_step_count, device_actions, device_reset_masks, device_observations, status, h.d_contacts.ptr, s);
+        h.read_policy_outputs(control_step_count, s);
         check(cudaEventRecord(h.ev_out, s), "event");
         check(cudaStreamWaitEvent(caller, h.ev_out, 0), "stream wait");
         if (advance) {

@@ -163,6 +163,57 @@ class StageHighWaterC(ct.Structure):
     ]
 
 
+class PolicyDenseLayerC(ct.Structure):
+    """MRPolicyDenseLayerC (reference c_api.h:334-342); weights [output][input]."""
+
+    _fields_ = [
+        ("input_count", ct.c_uint32),
+        ("output_count", ct.c_uint32),
+        ("activation", ct.c_uint32),
+        ("weights", ct.POINTER(ct.c_float)),
+        ("weight_count", ct.c_size_t),
+        ("bias", ct.POINTER(ct.c_float)),
+        ("bias_count", ct.c_size_t),
+    ]
+
+
+class PolicyPackC(ct.Structure):
+    """MRPolicyPackC (reference c_api.h:344-372)."""
+
+    _fields_ = [
+        ("id", ct.c_char_p),
+        ("revision", ct.c_uint64),
+        ("contract_version", ct.c_uint64),
+        ("world_fingerprint", ct.c_uint64),
+        ("task_fingerprint", ct.c_uint64),
+        ("observation_fingerprint", ct.c_uint64),
+        ("action_fingerprint", ct.c_uint64),
+        ("observation_mean", ct.POINTER(ct.c_float)),
+        ("observation_mean_count", ct.c_size_t),
+        ("observation_inverse_standard_deviation", ct.POINTER(ct.c_float)),
+        ("observation_inverse_standard_deviation_count", ct.c_size_t),
+        ("layers", ct.POINTER(PolicyDenseLayerC)),
+        ("layer_count", ct.c_size_t),
+        ("critic_observation_mean", ct.POINTER(ct.c_float)),
+        ("critic_observation_mean_count", ct.c_size_t),
+        ("critic_observation_inverse_standard_deviation", ct.POINTER(ct.c_float)),
+        ("critic_observation_inverse_standard_deviation_count", ct.c_size_t),
+        ("critic_layers", ct.POINTER(PolicyDenseLayerC)),
+        ("critic_layer_count", ct.c_size_t),
+        ("action_log_standard_deviation", ct.POINTER(ct.c_float)),
+        ("action_log_standard_deviation_count", ct.c_size_t),
+        ("action_bias", ct.POINTER(ct.c_float)),
+        ("action_bias_count", ct.c_size_t),
+        ("action_scale", ct.POINTER(ct.c_float)),
+        ("action_scale_count", ct.c_size_t),
+        ("observation_clip", ct.c_float),
+        ("action_clip", ct.c_float),
+    ]
+
+
+POLICY_ACTIVATIONS: Final = {"identity": 0, "relu": 1, "tanh": 2, "elu": 3, "silu": 4}
+
+
 class TaskRolloutAdvanceC(ct.Structure):
     _fields_ = [
         ("control_step_count", ct.c_uint32),
@@ -387,6 +438,13 @@ EXPORTED_SYMBOLS: Final = (
     "mr_server_release",
     "mr_server_stats",
     "mr_pile_step_no_alloc",
+    "mr_task_rollout_set_policy",
+    "mr_task_rollout_policy_revision",
+    "mr_task_rollout_clear_policy",
+    "mr_task_rollout_policy_latents",
+    "mr_task_rollout_policy_log_probabilities",
+    "mr_task_rollout_policy_values",
+    "mr_task_rollout_bootstrap_policy_values",
 )
 
 
@@ -436,6 +494,18 @@ class Bindings:
         L.mr_task_rollout_set_state_readback.restype = ct.c_int
         L.mr_task_rollout_set_precision.argtypes = [ct.c_void_p, ct.c_uint32]
         L.mr_task_rollout_set_precision.restype = ct.c_int
+        L.mr_task_rollout_set_policy.argtypes = [ct.c_void_p, ct.POINTER(PolicyPackC)]
+        L.mr_task_rollout_set_policy.restype = ct.c_int
+        L.mr_task_rollout_policy_revision.argtypes = [ct.c_void_p]
+        L.mr_task_rollout_policy_revision.restype = ct.c_uint64
+        L.mr_task_rollout_clear_policy.argtypes = [ct.c_void_p]
+        L.mr_task_rollout_clear_policy.restype = ct.c_int
+        for name in ("latents", "log_probabilities", "values"):
+            fn = getattr(L, f"mr_task_rollout_policy_{name}")
+            fn.argtypes = [ct.c_void_p]
+            fn.restype = ct.POINTER(ct.c_float)
+        L.mr_task_rollout_bootstrap_policy_values.argtypes = [ct.c_void_p]
+        L.mr_task_rollout_bootstrap_policy_values.restype = ct.POINTER(ct.c_float)
         L.mr_task_rollout_advance.argtypes = [
             ct.c_void_p,
             P(ct.c_float),

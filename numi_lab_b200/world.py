@@ -14,7 +14,7 @@ from __future__ import annotations
 
 import ctypes as ct
 from dataclasses import dataclass
-from typing import Any
+from typing import Any, Sequence
 
 import numpy as np
 
@@ -339,11 +339,128 @@ class World:
         )
         return observations, status, counters
 
+    # -- native policy ---------------------------------------------------
+    def set_policy(
+        self,
+        layers: Sequence[tuple[np.ndarray, np.ndarray | None, str]],
+        *,
+        revision: int,
+        action_clip: float,
+        policy_id: str = "policy",
+        observation_mean: np.ndarray | None = None,
+        observation_inverse_std: np.ndarray | None = None,
+        observation_clip: float = 0.0,
+        critic_layers: Sequence[tuple[np.ndarray, np.ndarray | None, str]] = (),
+        critic_observation_mean: np.ndarray | None = None,
+        critic_observation_inverse_std: np.ndarray | None = None,
+        action_log_std: np.ndarray | None = None,
+        action_bias: np.ndarray | None = None,
+        action_scale: np.ndarray | None = None,
+    ) -> None:
+        """Installs a dense policy (mr_task_rollout_set_policy).  `layers`
+        are (weights [out][in], bias [out] or None, activation name); the
+        actor maps [q, v] to the action mean."""
+
+        keep: list[Any] = []
+
+        def arr(a):
+            if a is None:
+                return None, 0
+            a = np.ascontiguousarray(a, np.float32).reshape(-1)
+            keep.append(a)
+            return a.ctypes.data_as(ct.POINTER(ct.c_float)), a.size
+
+        def dense(spec):
+            out = (native.PolicyDenseLayerC * max(len(spec), 1))()
+            for i, (w, b, act) in enumerate(spec):
+                w = np.asarray(w, np.float32)
+                wp, wn = arr(w)
+                bp, bn = arr(b)
+                out[i] = native.PolicyDenseLayerC(w.shape[1], w.shape[0], native.POLICY_ACTIVATIONS[act], wp, wn, bp, bn)
+            keep.append(out)
+            return out, len(spec)
+
+        pk = native.PolicyPackC()
+        pk.id = policy_id.encode()
+        pk.revision = int(revision)
+        pk.layers, pk.layer_count = dense(layers)
+        if critic_layers:
+            pk.critic_layers, pk.critic_layer_count = dense(critic_layers)
+        pk.observation_mean, pk.observation_mean_count = arr(observation_mean)
+        pk.observation_inverse_standard_deviation, pk.observation_inverse_standard_deviation_count = arr(observation_inverse_std)
+        pk.critic_observation_mean, pk.critic_observation_mean_count = arr(critic_observation_mean)
+        (pk.critic_observation_inverse_standard_deviation,
+         pk.critic_observation_inverse_standard_deviation_count) = arr(critic_observation_inverse_std)
+        pk.action_log_standard_deviation, pk.action_log_standard_deviation_count = arr(action_log_std)
+        pk.action_bias, pk.action_bias_count = arr(action_bias)
+        pk.action_scale, pk.action_scale_count = arr(action_scale)
+        pk.observation_clip = float(observation_clip)
+        pk.action_clip = float(action_clip)
+        self._lib.check(self._lib.lib.mr_task_rollout_set_policy(self._handle, ct.byref(pk)), "mr_task_rollout_set_policy")
+
+    def clear_policy(self) -> None:
+        self._lib.check(self._lib.lib.mr_task_rollout_clear_policy(self._handle), "mr_task_rollout_clear_policy")
+
+    @property
+    def policy_revision(self) -> int:
+        return int(self._lib.lib.mr_task_rollout_policy_revision(self._handle))
+
+    def step_policy(self, steps: int, *, reset_mask: Any = None, wait: bool = True):
+        """Advances `steps` control steps driven by the installed policy on
+        the device (no action stream).  Returns (observations, status)."""
+
+        import torch
+
+        device = torch.device("cuda", torch.cuda.current_device())
+        observations = torch.empty((steps, self.envs, self.observation_count), device=device, dtype=torch.float32)
+        status = torch.empty((steps, self.envs), device=device, dtype=torch.int32)
+        mask_ptr = None
+        if reset_mask is not None:
+            reset_mask = reset_mask.contiguous()
+            mask_ptr = ct.c_void_p(reset_mask.data_ptr())
+        counters = native.TaskRolloutAdvanceC() if wait else None
+        self._lib.check(
+            self._lib.lib.mr_task_rollout_advance_device(
+                self._handle, None, mask_ptr, steps, ct.c_void_p(observations.data_ptr()), ct.c_void_p(status.data_ptr()),
+                ct.c_uint64(torch.cuda.current_stream(device).cuda_stream), ct.byref(counters) if counters is not None else None),
+            "mr_task_rollout_advance_device")
+        self._last_policy_steps = steps
+        return observations, status
+
+    def policy_outputs(self) -> dict[str, np.ndarray] | None:
+        """Latents [step][env][action], log-probabilities and values
+        [step][env], bootstrap values [env] of the last policy-driven advance
+        (copies; after the advance has completed)."""
+
+        L = self._lib.lib
+        lat = L.mr_task_rollout_policy_latents(self._handle)
+        if not lat:
+            return None
+        import torch
+
+        torch.cuda.synchronize()
+        lp = L.mr_task_rollout_policy_log_probabilities(self._handle)
+        steps = self._last_policy_steps
+        cells = steps * self.envs
+        return {
+            "latents": np.ctypeslib.as_array(lat, shape=(cells * self.action_count,)).reshape(steps, self.envs, -1).copy(),
+            "log_probabilities": np.ctypeslib.as_array(lp, shape=(cells,)).reshape(steps, self.envs).copy(),
+            "values": np.ctypeslib.as_array(L.mr_task_rollout_policy_values(self._handle), shape=(cells,)).reshape(steps, self.envs).copy(),
+            "bootstrap_values": np.ctypeslib.as_array(L.mr_task_rollout_bootstrap_policy_values(self._handle), shape=(self.envs,)).copy(),
+        }
+
     def set_state_readback(self, enabled: bool) -> None:
         self._lib.check(self._lib.lib.mr_task_rollout_set_state_readback(self._handle, 1 if enabled else 0), "set_state_readback")
 
     def advance_host(
-        self, actions: np.ndarray, reset_masks: np.ndarray | None = None, *, raise_on_failure: bool = True, copy: bool = True
+        self,
+        actions: np.ndarray | None,
+        reset_masks: np.ndarray | None = None,
+        *,
+        raise_on_failure: bool = True,
+        copy: bool = True,
+        steps: int | None = None,
+        evaluate_final_policy: bool = False,
     ) -> dict[str, Any]:
         """Reference-shaped synchronous advance with host buffers.
 
@@ -351,8 +468,15 @@ class World:
         own result memory, valid until the next advance, reset or close --
         the C ABI's rule for the pointers it returns (c_api.h:680-681)."""
 
-        actions = np.ascontiguousarray(actions, np.float32)
-        steps = actions.shape[0] if actions.ndim == 3 else 1
+        if actions is None:
+            # Policy-driven: no action stream.
+            if steps is None:
+                raise ValueError("steps is required without actions")
+            actions = np.zeros((0,), np.float32)
+            self._last_policy_steps = int(steps)
+        else:
+            actions = np.ascontiguousarray(actions, np.float32)
+            steps = actions.shape[0] if actions.ndim == 3 else 1
         counters = native.TaskRolloutAdvanceC()
         masks_ptr = None
         mask_count = 0
@@ -367,8 +491,8 @@ class World:
             masks_ptr,
             mask_count,
             steps,
-            0,
-            0,
+            self.policy_revision if evaluate_final_policy else 0,
+            1 if evaluate_final_policy else 0,
             ct.byref(counters),
         )
         if rc != 0 and (raise_on_failure or counters.control_step_count == 0):
