@@ -1,16 +1,18 @@
 // Native policy on the device: the reference's dense layer operator
 // (mr_policy_dense_layer, PolicyInference.metal:80-160) and action sampler
 // (mr_policy_sample_and_score, :162-268) fused into one kernel per control
-// step.  A CTA takes kPolicyTile environments through every actor layer
+// step.  A CTA takes kPolicyTile (8) environments through every actor layer
 // (and the critic), the activations of the tile living in shared memory;
 // thread j owns output neuron j and keeps one accumulator per environment,
 // so each weight is read once per CTA and used kPolicyTile times.  Weights
 // are stored [input][output] so a warp's weight loads are contiguous; the
 // environment's input value is a shared-memory broadcast.  Each output
 // starts from its bias and accumulates inputs in ascending order with FMA,
-// the reference's order.  FP32 throughout, as the reference evaluates: the
-// policy costs ~1 % of a contact control step, so tensor-core precision
-// (bf16 / tf32 operands) would change actions for no measurable gain.
+// the reference's order.  FP32 throughout, as the reference evaluates: at
+// 4096 environments a 71-256-128-29 actor plus a 71-64-1 critic take 85 us
+// per launch against 1.22 ms for the contact control step it feeds, so
+// tensor-core operands (bf16 / tf32) would change the actions to save at
+// most 7 % of a step.
 #include "policy.h"
 
 #include <cstdint>
@@ -81,7 +83,23 @@ __device__ float* forward(const PolicyLayer* layers, int count, float* x, float*
 #pragma unroll
             for (int e = 0; e < kPolicyTile; ++e) acc[e] = b;
             const float* w = L.weights_t + j;
-            for (int k = 0; k < L.in; ++k) {
+            // Four inputs per shared-memory load (rows are 16-byte aligned),
+            // still accumulated in ascending input order.
+            const int in4 = L.in & ~3;
+            for (int k = 0; k < in4; k += 4) {
+                const float w0 = w[static_cast<size_t>(k) * L.out], w1 = w[static_cast<size_t>(k + 1) * L.out],
+                            w2 = w[static_cast<size_t>(k + 2) * L.out], w3 = w[static_cast<size_t>(k + 3) * L.out];
+#pragma unroll
+                for (int e = 0; e < kPolicyTile; ++e) {
+                    const float4 xv = *reinterpret_cast<const float4*>(x + e * kPolicyMaxWidth + k);
+                    float a = acc[e];
+                    a = __fmaf_rn(w0, xv.x, a);
+                    a = __fmaf_rn(w1, xv.y, a);
+                    a = __fmaf_rn(w2, xv.z, a);
+                    acc[e] = __fmaf_rn(w3, xv.w, a);
+                }
+            }
+            for (int k = in4; k < L.in; ++k) {
                 const float wk = w[static_cast<size_t>(k) * L.out];
 #pragma unroll
                 for (int e = 0; e < kPolicyTile; ++e) acc[e] = __fmaf_rn(wk, x[e * kPolicyMaxWidth + k], acc[e]);

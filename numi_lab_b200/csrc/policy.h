@@ -11,7 +11,7 @@ namespace numi {
 
 constexpr int kPolicyMaxLayers = 8;
 constexpr int kPolicyMaxWidth = 256;  // widest layer (inputs and outputs)
-constexpr int kPolicyTile = 16;       // environments per CTA
+constexpr int kPolicyTile = 8;        // environments per CTA
 
 struct PolicyLayer {
     std::int32_t in, out, activation, reserved;
