@@ -428,6 +428,73 @@ def run_pile(args, source: str = "pile") -> None:
     print(json.dumps(line))
 
 
+def run_policy(args) -> None:
+    """Closed loop: 4096 tree29 environments driven by a native policy on
+    the device (mr_task_rollout_set_policy) -- a seeded random actor
+    71-256-128-29 (elu, silu, tanh) with observation normalisation and
+    Gaussian sampling, plus a 71-64-1 critic -- 25 policy-driven control
+    steps per bench step."""
+
+    import torch
+
+    import numi_lab_b200 as nb
+
+    torch.cuda.set_device(0)
+    device = torch.device("cuda", 0)
+    envs, horizon = args.envs or ENVS, HORIZON
+    rng = np.random.default_rng(SEED)
+
+    def dense(sizes, acts):
+        return [(rng.normal(0.0, 1.0 / np.sqrt(a), (b, a)).astype(np.float32), rng.normal(0.0, 0.1, b).astype(np.float32), f)
+                for (a, b), f in zip(zip(sizes[:-1], sizes[1:]), acts)]
+
+    with nb.World("tree29", envs, substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT, seed=SEED) as world:
+        nobs, na = world.observation_count, world.action_count
+        world.set_policy(layers=dense([nobs, 256, 128, na], ["elu", "silu", "tanh"]), critic_layers=dense([nobs, 64, 1], ["relu", "identity"]),
+                         revision=1, action_clip=2.5, observation_mean=np.zeros(nobs, np.float32),
+                         observation_inverse_std=np.ones(nobs, np.float32), observation_clip=10.0,
+                         action_scale=np.full(na, 0.5, np.float32), action_log_std=np.full(na, -1.5, np.float32))
+        flush = torch.empty(256 * 1024 * 1024 // 4, device=device, dtype=torch.float32)
+        status = None
+        for _ in range(args.warmup):  # the same allocation pattern as the timed loop (graphs keyed on buffers)
+            _, status = world.step_policy(horizon, wait=False)
+        torch.cuda.synchronize(device)
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        stream = torch.cuda.current_stream(device)
+        failures = 0
+        with ClockSampler(0) as clocks:
+            for i in range(args.steps):
+                flush.fill_(float(i))
+                starts[i].record(stream)
+                _, status = world.step_policy(horizon, wait=False)
+                stops[i].record(stream)
+                failures += int((status != 0).sum().item()) if i + 1 == args.steps else 0
+            torch.cuda.synchronize(device)
+        clock_summary = clocks.summary()
+        ms = float(sum(a.elapsed_time(b) for a, b in zip(starts, stops)))
+    line = {
+        "metric": "closed-loop env-steps/s",
+        "value": envs * horizon * args.steps / (ms / 1e3),
+        "unit": UNIT,
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded random policy weights)",
+        "config": {"workload": f"tree29 x {envs} envs driven by a native policy (actor 71-256-128-29, critic 71-64-1, "
+                               f"stochastic), {horizon} control steps per bench step", "l2": "flushed (256 MiB write) between steps"},
+        "gpu_launches": 2 * horizon * args.steps + args.steps,
+        "clocks": {k: clock_summary[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        "failed_env_steps_last_step": failures,
+    }
+    print(json.dumps(line))
+
+
 def run_mix(args) -> None:
     """Heterogeneous mix: 16,384 environments, 40 % 7-link chains (one 5 ms
     step per control step), 30 % 29-DoF trees and 30 % piles of 8-64 bodies
@@ -689,10 +756,10 @@ def main() -> None:
     parser.add_argument("--impl", default="native", choices=["native", "reference"])
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--envs", type=int, default=0, help="pile workload: environments (default 16384; smaller for profiling)")
-    parser.add_argument("--workload", default="tree29", choices=["tree29", "pile", "cylinder_pile", "mix", "precision"],
+    parser.add_argument("--workload", default="tree29", choices=["tree29", "pile", "cylinder_pile", "mix", "precision", "policy"],
                         help="tree29 (the headline), pile (36-body piles), cylinder_pile (36-body piles with cylinders: "
                              "GJK / EPA pairs), mix (chains, trees and piles) or precision (box stacks and trees against the "
-                             "FP64 oracle)")
+                             "FP64 oracle) or policy (tree29 closed loop under a native policy)")
     parser.add_argument("--serve", action="store_true",
                         help="serving workload: Poisson request stream, latency percentiles (one JSON line)")
     args = parser.parse_args()
@@ -713,7 +780,7 @@ def main() -> None:
     if args.workload != "tree29":
         if rank == 0:
             {"pile": run_pile, "cylinder_pile": lambda a: run_pile(a, "cylinder_pile"), "mix": run_mix,
-             "precision": run_precision}[args.workload](args)
+             "precision": run_precision, "policy": run_policy}[args.workload](args)
         return
 
     import torch
