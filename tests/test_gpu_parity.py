@@ -226,3 +226,15 @@ def test_bitwise_replay_and_host_path(cuda_device):
         assert out["counters"].successful_environment_steps == steps * envs
         np.testing.assert_array_equal(out["observations"], results[0][0])
         np.testing.assert_array_equal(out["final_q"], results[0][1])
+    # The host path again in uneven pieces (each advance its own captured
+    # graph with per-step observation read-back on the copy stream), read
+    # through views of the rollout's result memory.
+    with _tree_world(envs, seed=12) as world:
+        world.set_state_readback(True)
+        host = actions.cpu().numpy()
+        done = 0
+        for n in (1, 3, 2):
+            out = world.advance_host(host[done:done + n], copy=False)
+            np.testing.assert_array_equal(out["observations"], results[0][0][done:done + n])
+            done += n
+        np.testing.assert_array_equal(out["final_q"], results[0][1])
