@@ -876,8 +876,11 @@ def main() -> None:
     d2h = HORIZON * ENVS * (4 + 4 + 4 * world.observation_count) + ENVS * world.nq * 4
     world.set_state_readback(False)
 
-    launches_per_step = HORIZON  # one control-step kernel per control step
-    kernel_ms = (max_ms / world_size if dist is None else total_ms) / (args.steps * launches_per_step)
+    chains = world.environment_chains
+    launches_per_step = HORIZON * chains  # one control-step launch per chain per control step
+    # The chains' launches of one control step run concurrently, so the
+    # kernel is timed per control step (all chains, all environments).
+    kernel_ms = (max_ms / world_size if dist is None else total_ms) / (args.steps * HORIZON)
     bytes_per_env_step = _algorithmic_bytes_per_env_step(world.nq, world.nv, world.action_count, mean_points, mean_manifolds)
     achieved = bytes_per_env_step * ENVS / (kernel_ms / 1e3) / 1e9
     peaks = _measured_peaks()
@@ -910,7 +913,8 @@ def main() -> None:
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic (seeded)",
-            "config": {**_config(world_size), "launch": dict(zip(("envs_per_cta", "resident_envs_per_sm"), launch_shape))},
+            "config": {**_config(world_size), "launch": {**dict(zip(("envs_per_cta", "resident_envs_per_sm"), launch_shape)),
+                                                          "environment_chains": chains}},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {
                 "bound": "hbm",
@@ -921,7 +925,8 @@ def main() -> None:
                 "traffic": traffic,
                 "peak_source": peaks["source"],
                 "algorithmic_bytes_per_env_step": bytes_per_env_step,
-                "kernel_ms_per_launch": kernel_ms,
+                "kernel_ms_per_control_step": kernel_ms,
+                "launches_per_control_step": chains,
             },
             "cpu_baseline": cpu,
             "gpu_launches": launches_per_step * args.steps,

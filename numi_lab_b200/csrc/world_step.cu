@@ -1972,7 +1972,7 @@ __global__ void __launch_bounds__(128, 3) control_step_kernel(StepParams p, Warp
         if (p.active_contacts) p.active_contacts[item] = success ? contacts : 0u;
         if (!success) {
             atomicAdd(p.stats + kStatFailedEnvs, 1u);
-            atomicMin(p.stats + kStatFirstFailEnv, static_cast<unsigned>(env));
+            atomicMin(p.stats + kStatFirstFailEnv, static_cast<unsigned>(env + p.env_base));
         }
         if (reset) atomicAdd(p.stats + kStatResets, 1u);
         if (kContact) {

@@ -439,6 +439,7 @@ EXPORTED_SYMBOLS: Final = (
     "mr_server_stats",
     "mr_pile_step_no_alloc",
     "mr_task_rollout_set_policy",
+    "mr_task_rollout_environment_chains",
     "mr_task_rollout_policy_revision",
     "mr_task_rollout_clear_policy",
     "mr_task_rollout_policy_latents",
@@ -494,6 +495,8 @@ class Bindings:
         L.mr_task_rollout_set_state_readback.restype = ct.c_int
         L.mr_task_rollout_set_precision.argtypes = [ct.c_void_p, ct.c_uint32]
         L.mr_task_rollout_set_precision.restype = ct.c_int
+        L.mr_task_rollout_environment_chains.argtypes = [ct.c_void_p]
+        L.mr_task_rollout_environment_chains.restype = ct.c_uint32
         L.mr_task_rollout_set_policy.argtypes = [ct.c_void_p, ct.POINTER(PolicyPackC)]
         L.mr_task_rollout_set_policy.restype = ct.c_int
         L.mr_task_rollout_policy_revision.argtypes = [ct.c_void_p]

@@ -339,6 +339,11 @@ class World:
         )
         return observations, status, counters
 
+    @property
+    def environment_chains(self) -> int:
+        """Environment chains (launches per control step) of a policy-free advance."""
+        return int(self._lib.lib.mr_task_rollout_environment_chains(self._handle))
+
     # -- native policy ---------------------------------------------------
     def set_policy(
         self,

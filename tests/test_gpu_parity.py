@@ -238,3 +238,27 @@ def test_bitwise_replay_and_host_path(cuda_device):
             np.testing.assert_array_equal(out["observations"], results[0][0][done:done + n])
             done += n
         np.testing.assert_array_equal(out["final_q"], results[0][1])
+
+
+def test_environment_chains_are_bitwise_equal_and_report_absolute_slots(cuda_device, monkeypatch):
+    """An advance run as several environment chains (contiguous blocks on
+    their own streams inside the graph) equals the single chain bit for bit,
+    also for an uneven split, and counters name the absolute slot."""
+    import torch
+
+    envs, steps = 50, 4
+    actions = 0.3 * torch.randn((steps, envs, 29), device="cuda", generator=torch.Generator(device="cuda").manual_seed(9))
+    results = {}
+    for chains in ("1", "3"):
+        monkeypatch.setenv("NUMI_B200_CHAINS", chains)
+        with _tree_world(envs, seed=21) as world:
+            q0, v0, m0 = world.state()
+            bad = q0.copy()
+            bad[37, 3:7] = [0.0, 0.0, 0.0, 2.0]  # rejected quaternion in the third block
+            world.set_state(bad, v0, m0)
+            obs, status, counters = world.step(actions, wait=True)
+            results[chains] = (obs.cpu().numpy(), status.cpu().numpy(), world.state()[0], counters.first_failing_environment)
+    a, b = results["1"], results["3"]
+    for x, y in zip(a[:3], b[:3]):
+        np.testing.assert_array_equal(x, y)
+    assert a[3] == b[3] == 37
