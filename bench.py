@@ -473,6 +473,7 @@ def run_policy(args) -> None:
             torch.cuda.synchronize(device)
         clock_summary = clocks.summary()
         ms = float(sum(a.elapsed_time(b) for a, b in zip(starts, stops)))
+        chains = world.environment_chains
     line = {
         "metric": "closed-loop env-steps/s",
         "value": envs * horizon * args.steps / (ms / 1e3),
@@ -488,7 +489,8 @@ def run_policy(args) -> None:
         "data": "synthetic (seeded random policy weights)",
         "config": {"workload": f"tree29 x {envs} envs driven by a native policy (actor 71-256-128-29, critic 71-64-1, "
                                f"stochastic), {horizon} control steps per bench step", "l2": "flushed (256 MiB write) between steps"},
-        "gpu_launches": 2 * horizon * args.steps + args.steps,
+        "gpu_launches": 2 * chains * horizon * args.steps + args.steps,  # policy + control step per chain and step, one counter
+        "environment_chains": chains,
         "clocks": {k: clock_summary[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
         "failed_env_steps_last_step": failures,
     }

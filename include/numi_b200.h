@@ -612,8 +612,8 @@ MR_API int mr_task_rollout_copy_environment_parameters(
  * pile and stack worlds, whose kernel runs one environment per CTA). */
 MR_API int mr_task_rollout_launch_shape(const MRTaskRolloutHandle* handle, uint32_t* warps_per_block,
                                         uint32_t* resident_warps_per_sm);
-/* No counterpart in the reference: how many environment chains a
- * policy-free articulated advance runs as (contiguous blocks of
+/* No counterpart in the reference: how many environment chains an
+ * articulated advance runs as (contiguous blocks of
  * environments, each a chain of per-step launches on its own stream inside
  * the advance's graph; launches per control step = chains). */
 MR_API uint32_t mr_task_rollout_environment_chains(const MRTaskRolloutHandle* handle);

@@ -130,7 +130,8 @@ __global__ void __launch_bounds__(kThreads) policy_kernel(PolicyParams p) {
     if (e < kPolicyTile && env0 + e < p.envs) {
         const int env = env0 + e;
         const unsigned long long step = *p.step_base + static_cast<unsigned long long>(p.step_offset);
-        const unsigned long long key = mix64(p.key ^ mix64((static_cast<unsigned long long>(env) << 32) ^ step));
+        const unsigned long long slot = static_cast<unsigned long long>(env + p.env_base);
+        const unsigned long long key = mix64(p.key ^ mix64((slot << 32) ^ step));
         float log_prob = 0.0f;
         constexpr float kHalfLogTwoPi = 0.91893853320467274178f;
         for (int act = 0; act < p.na; ++act) {

@@ -45,6 +45,7 @@ struct PolicyParams {
     const unsigned long long* step_base;
     std::int32_t step_offset;
     unsigned long long key;
+    std::int32_t env_base;  // slot of this launch's environment 0 (state and outputs start there): keys the draws
 };
 
 cudaError_t configure_policy_kernel();

@@ -537,9 +537,9 @@ struct MRTaskRolloutHandle {
             return;
         }
         const bool driven = policy != nullptr;
-        // A policy reads every environment's state before each step, so a
-        // policy-driven advance stays one chain.
-        const int nchains = driven ? 1 : static_cast<int>(std::min<std::uint32_t>(static_cast<std::uint32_t>(chains), envs));
+        // With a policy each chain evaluates it on its own block before each
+        // of its steps.
+        const int nchains = static_cast<int>(std::min<std::uint32_t>(static_cast<std::uint32_t>(chains), envs));
         if (nchains > 1) {
             check(cudaEventRecord(ev_fork, s), "event");
             for (int c = 0; c < nchains; ++c) check(cudaStreamWaitEvent(chain_stream[c], ev_fork, 0), "stream wait");
@@ -549,7 +549,7 @@ struct MRTaskRolloutHandle {
             const std::uint32_t n = static_cast<std::uint32_t>(static_cast<std::uint64_t>(envs) * (c + 1) / nchains) - o;
             cudaStream_t cs = nchains > 1 ? chain_stream[c] : s;
             for (std::uint32_t k = 0; k < steps; ++k) {
-                if (driven) enqueue_policy(k, const_cast<float*>(actions) + static_cast<size_t>(k) * envs * na, true, cs);
+                if (driven) enqueue_policy(k, o, n, const_cast<float*>(actions) + static_cast<size_t>(k) * envs * na, true, cs);
                 const size_t item0 = static_cast<size_t>(k) * envs + o;  // this chain's first item of step k
                 numi::StepParams p{};
                 p.model = d_model.ptr;
@@ -576,6 +576,7 @@ struct MRTaskRolloutHandle {
                       "control step launch");
                 if (host_obs && obs) copy_observation_rows(k, o, n, obs, host_obs, cs);
             }
+            if (driven && evaluate_final) enqueue_policy(steps, o, n, nullptr, false, cs);
         }
         if (nchains > 1) {
             for (int c = 0; c < nchains; ++c) {
@@ -583,10 +584,7 @@ struct MRTaskRolloutHandle {
                 check(cudaStreamWaitEvent(s, ev_chain[c], 0), "stream wait");
             }
         }
-        if (driven) {
-            if (evaluate_final) enqueue_policy(steps, nullptr, false, s);
-            check(numi::launch_policy_counter(d_policy_steps.ptr, steps, s), "policy counter");
-        }
+        if (driven) check(numi::launch_policy_counter(d_policy_steps.ptr, steps, s), "policy counter");
         if (host_obs && obs) join_copies(s);
     }
 
@@ -632,19 +630,21 @@ struct MRTaskRolloutHandle {
     // Policy evaluation before control step k (k == steps: the final state,
     // values into the bootstrap slot) writing step k's actions.
     bool evaluate_final = false;
-    void enqueue_policy(std::uint32_t k, float* actions_k, bool step, cudaStream_t s) {
+    // Environments [o, o + n) only (one chain's block).
+    void enqueue_policy(std::uint32_t k, std::uint32_t o, std::uint32_t n, float* actions_k, bool step, cudaStream_t s) {
         numi::PolicyParams pp = policy->params;
-        pp.q = d_q.ptr;
-        pp.v = d_v.ptr;
         pp.nq = static_cast<int>(model.world.nq);
         pp.nv = static_cast<int>(model.world.nv);
-        pp.envs = static_cast<int>(envs);
+        pp.q = d_q.ptr + static_cast<size_t>(o) * pp.nq;
+        pp.v = d_v.ptr + static_cast<size_t>(o) * pp.nv;
+        pp.envs = static_cast<int>(n);
+        pp.env_base = static_cast<int>(o);
         pp.na = static_cast<int>(model.world.action_count);
-        const size_t cells = static_cast<size_t>(k) * envs;
-        pp.actions = step ? actions_k : nullptr;
+        const size_t cells = static_cast<size_t>(k) * envs + o;
+        pp.actions = step ? actions_k + static_cast<size_t>(o) * pp.na : nullptr;
         pp.latents = step ? d_latents.ptr + cells * pp.na : nullptr;
         pp.log_prob = step ? d_log_prob.ptr + cells : nullptr;
-        pp.values = d_values.ptr + cells;  // slot `steps` holds the bootstrap values
+        pp.values = d_values.ptr + cells;  // step `steps` holds the bootstrap values
         pp.step_base = d_policy_steps.ptr;
         pp.step_offset = static_cast<int>(k);
         check(numi::launch_policy(pp, s), "policy launch");
@@ -1320,7 +1320,7 @@ MR_API int mr_task_rollout_copy_environment_parameters(const MRTaskRolloutHandle
 
 MR_API uint32_t mr_task_rollout_environment_chains(const MRTaskRolloutHandle* handle) {
     if (!handle) return 0u;
-    if (handle->scene || handle->policy) return 1u;
+    if (handle->scene) return 1u;
     return static_cast<uint32_t>(std::min<std::uint32_t>(static_cast<std::uint32_t>(handle->chains), handle->envs));
 }
 

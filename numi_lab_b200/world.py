@@ -341,7 +341,7 @@ class World:
 
     @property
     def environment_chains(self) -> int:
-        """Environment chains (launches per control step) of a policy-free advance."""
+        """Environment chains (control-step launches per control step) of an articulated advance."""
         return int(self._lib.lib.mr_task_rollout_environment_chains(self._handle))
 
     # -- native policy ---------------------------------------------------

@@ -69,8 +69,10 @@ def test_policy_oracle_restates_the_layer_order_and_sampler():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("stochastic", [False, True])
-def test_policy_actions_match_the_oracle(cuda_device, stochastic):
+@pytest.mark.parametrize("stochastic,chains", [(False, "1"), (True, "1"), (True, "3")])
+def test_policy_actions_match_the_oracle(cuda_device, monkeypatch, stochastic, chains):
+    """Three chains: each block's draws are keyed on the absolute slot."""
+    monkeypatch.setenv("NUMI_B200_CHAINS", chains)
     rng = np.random.default_rng(11 if stochastic else 12)
     envs, steps = 64, 3
     with nb.World("tree29", envs, substeps=4, velocity_iterations=8, control_dt=0.02, seed=SEED) as world:
@@ -96,12 +98,14 @@ def test_policy_actions_match_the_oracle(cuda_device, stochastic):
 
 
 @pytest.mark.gpu
-def test_policy_closed_loop_equals_open_loop_with_its_actions(cuda_device):
+@pytest.mark.parametrize("chains", ["1", "3"])
+def test_policy_closed_loop_equals_open_loop_with_its_actions(cuda_device, monkeypatch, chains):
     """A policy-driven advance applies exactly the actions it reports: an
     open-loop rollout fed clamp(scale x latent + bias) ends bit-identical,
     and evaluate_final_policy gives the critic on the final state."""
     import torch
 
+    monkeypatch.setenv("NUMI_B200_CHAINS", chains)  # three chains: each evaluates the policy on its own block
     rng = np.random.default_rng(3)
     envs, steps = 32, 6
     with nb.World("tree29", envs, substeps=4, velocity_iterations=8, control_dt=0.02, seed=SEED) as a, \
