@@ -112,10 +112,28 @@ class ClockSampler:
         self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         self.proc = None
 
+    def _smi_id(self) -> str:
+        """nvidia-smi's name for the CUDA device: its PCI bus id (CUDA's
+        device index need not match nvidia-smi's order, e.g. under
+        CUDA_VISIBLE_DEVICES)."""
+
+        try:
+            import torch
+
+            props = torch.cuda.get_device_properties(self.device_index)
+            bus = f"{props.pci_domain_id:08X}:{props.pci_bus_id:02X}:{props.pci_device_id:02X}.0"
+            probe = subprocess.run(["nvidia-smi", f"--id={bus}", "--query-gpu=index", "--format=csv,noheader"],
+                                   capture_output=True, text=True, timeout=30)
+            if probe.returncode == 0 and probe.stdout.strip():
+                return bus
+        except (AttributeError, RuntimeError, AssertionError, OSError, subprocess.TimeoutExpired):
+            pass
+        return str(self.device_index)
+
     def __enter__(self) -> "ClockSampler":
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200"],
+                ["nvidia-smi", f"--id={self._smi_id()}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=self.file,
                 stderr=subprocess.DEVNULL,
             )
@@ -155,48 +173,53 @@ class ClockSampler:
         }
 
 
-def cpu_reference_sample(world_state, actions_np, threads: int) -> dict:
-    """Times the reference's own CPU contact step over a bounded sample."""
+REFERENCE_WORKLOAD = "tree29_seed2026"  # oracle/workloads/: records + reset states of the first 512 envs
 
-    import numi_lab_b200 as nb
-    from oracle import Reference
 
-    q, v, friction = world_state
-    records = nb.compile_model("tree29", SEED)
-    ref = Reference(records, CONTROL_DT / SUBSTEPS, friction=float(np.mean(friction)))
-    qs = q[:CPU_SAMPLE_ENVS].astype(np.float64).copy()
-    vs = v[:CPU_SAMPLE_ENVS].astype(np.float64).copy()
-    acts = np.ascontiguousarray(actions_np[:CPU_SAMPLE_STEPS, :CPU_SAMPLE_ENVS], np.float32)
-    secs, failed = ref.run(qs, vs, acts, SUBSTEPS, threads, 1)
-    env_steps = CPU_SAMPLE_ENVS * CPU_SAMPLE_STEPS
+def _reference_sample(threads: int, actions: np.ndarray) -> dict:
+    """Times the reference's own CPU contact step on a bounded sample of the
+    workload: the first CPU_SAMPLE_ENVS environments of the benchmark (the
+    same compiled world, reset states and per-environment friction, read
+    from a committed fixture, so no CUDA library is loaded), stepped for
+    actions.shape[0] control steps from their reset states."""
+
+    from oracle import ReferenceBatch, workloads
+
+    records, arrays = workloads.load(workloads.path(REFERENCE_WORKLOAD))
+    q = arrays["q"][:CPU_SAMPLE_ENVS].astype(np.float64)
+    v = arrays["v"][:CPU_SAMPLE_ENVS].astype(np.float64)
+    batch = ReferenceBatch(records, CONTROL_DT / SUBSTEPS, arrays["friction"][:CPU_SAMPLE_ENVS])
+    secs, failed = batch.run(q, v, np.ascontiguousarray(actions, np.float32), SUBSTEPS, threads, 1)
+    env_steps = CPU_SAMPLE_ENVS * actions.shape[0]
     return {
         "value": env_steps / secs,
         "unit": UNIT,
         "cores": threads,
         "kind": "reference",
-        "sample": f"{CPU_SAMPLE_ENVS} envs x {CPU_SAMPLE_STEPS} control steps of the same workload "
-        f"(stepControlledArticulatedWorldCpu, quality-Newton contact solve, FP64, friction scale fixed at the "
-        f"sample mean), {failed} failed substeps",
+        "sample": f"{CPU_SAMPLE_ENVS} envs x {actions.shape[0]} control steps of the same workload from its reset states "
+        f"(stepControlledArticulatedWorldCpu with the reference's default quality-Newton contact solve, FP64, per-env friction), "
+        f"{failed} substeps failed in the reference (quality-Newton MR_STEP_DID_NOT_CONVERGE)",
         "seconds": secs,
+        "failed_substeps": failed,
     }
+
+
+def _reference_actions(i: int) -> np.ndarray:
+    return np.random.default_rng(SEED + i).normal(0.0, 0.3, size=(CPU_SAMPLE_STEPS, CPU_SAMPLE_ENVS, 29)).astype(np.float32)
 
 
 def run_reference_arm(args, rank: int) -> None:
     if rank != 0:
         return
-    import numi_lab_b200 as nb
     from oracle import REF_LIB
 
     if not REF_LIB.is_file():
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU core library oracle/_ref/libnumiref.so was not built"}))
         return
     threads = os.cpu_count() or 1
-    q, v, f = nb.sample_reset("tree29", SEED, SEED, 0, CPU_SAMPLE_ENVS)
-    rng = np.random.default_rng(SEED)
     samples = []
     for i in range(args.warmup + args.steps):
-        actions = rng.normal(0.0, 0.3, size=(CPU_SAMPLE_STEPS, CPU_SAMPLE_ENVS, 29)).astype(np.float32)
-        res = cpu_reference_sample((q, v, f), actions, threads)
+        res = _reference_sample(threads, _reference_actions(i))
         if i >= args.warmup:
             samples.append(res)
     value = float(np.mean([s["value"] for s in samples]))
@@ -214,16 +237,26 @@ def run_reference_arm(args, rank: int) -> None:
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded)",
-        "config": {**_config(args.gpus), "bench_step": f"{CPU_SAMPLE_ENVS} envs x {CPU_SAMPLE_STEPS} control steps on CPU"},
+        "config": _config(args.gpus),
+        "bench_step": f"{CPU_SAMPLE_ENVS} envs x {CPU_SAMPLE_STEPS} control steps on the host CPU",
         "cpu_baseline": {k: samples[0][k] for k in ("kind", "cores", "sample")} | {"value": value, "unit": UNIT},
+        "failed_substeps": int(sum(s["failed_substeps"] for s in samples)),
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
 
 
+C1_EPISODE = 40  # control steps per episode of the plain-ABA chain
+
+
 def plain_aba_chain7(device) -> dict:
     """The plain-ABA configuration: 1024 envs of the 7-revolute chain,
-    tau ~ N(0, 5), dt = 5 ms, 1000 steps (one advance), device-resident."""
+    tau ~ N(0, 5), dt = 5 ms, 1000 steps in one advance (one CUDA graph),
+    device-resident.  Under that torque scale the chain (no armature, no
+    damping) gains energy until its velocities overflow after 80-310 steps,
+    on the device and in the FP64 oracle alike, so the 1000 steps run as 25
+    episodes of 40 steps (every environment resets on the first step of an
+    episode) and every timed env-step is a successful one."""
 
     import torch
 
@@ -233,27 +266,35 @@ def plain_aba_chain7(device) -> dict:
     with nb.World("chain7", envs, substeps=1, control_dt=0.005, seed=SEED) as world:
         gen = torch.Generator(device=device).manual_seed(SEED)
         acts = 5.0 * torch.randn((steps, envs, world.action_count), device=device, generator=gen)
+        masks = torch.zeros((steps, envs), device=device, dtype=torch.int32)
+        masks[::C1_EPISODE] = 1
         status = torch.empty((steps, envs), device=device, dtype=torch.int32)
         obs = torch.empty((steps, envs, world.observation_count), device=device)
         for _ in range(3):
-            world.reset(SEED)
-            world.step(acts, observations=obs, status=status, wait=True)
-        world.reset(SEED)
+            world.step(acts, reset_mask=masks, observations=obs, status=status, wait=True)
         torch.cuda.synchronize(device)
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record()
-        world.step(acts, observations=obs, status=status)
+        world.step(acts, reset_mask=masks, observations=obs, status=status)
         stop.record()
         torch.cuda.synchronize(device)
         ms = start.elapsed_time(stop)
         failed = int((status != 0).sum().item())
+    ok = envs * steps - failed
+    bytes_per_env_step = 8.0 * (7 + 7) + 4.0 * 7
+    peaks = _measured_peaks()
     return {
-        "value": envs * steps / (ms / 1e3),
+        "value": ok / (ms / 1e3),
         "unit": UNIT,
-        "config": "chain7: 1024 envs, 1000 steps of 5 ms, tau ~ N(0, 5), FP32, one CUDA-graph advance",
+        "config": f"chain7: 1024 envs, 1000 steps of 5 ms, tau ~ N(0, 5), FP32, one CUDA-graph advance, "
+                  f"episodes of {C1_EPISODE} steps (reset on each episode's first step)",
         "ms": ms,
+        "successful_env_steps": ok,
         "failed_env_steps": failed,
-        "note": "failed env-steps are the chain's own energy blow-up under this torque scale (latched, state kept)",
+        "roofline": {"bound": "hbm", "algorithmic_bytes_per_env_step": bytes_per_env_step,
+                     "achieved": bytes_per_env_step * ok / (ms / 1e3) / 1e9, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": bytes_per_env_step * ok / (ms / 1e3) / 1e9 / peaks["hbm_gbs"]},
+        "gpu_launches": steps,
     }
 
 
@@ -785,9 +826,18 @@ def main() -> None:
              "precision": run_precision, "policy": run_policy}[args.workload](args)
         return
 
+    run_headline(args, rank, local_rank, world_size)
+
+
+def run_headline(args, rank: int, local_rank: int, world_size: int) -> None:
+    """The 29-DoF contact workload: device-resident throughput, end to end
+    through the host-buffer C ABI, roofline, the reference CPU baseline and
+    the plain-ABA chain configuration."""
+
     import torch
 
     import numi_lab_b200 as nb
+    from numi_lab_b200.sharding import HorizonStats, reduce_stats, shard_range
 
     torch.cuda.set_device(local_rank)
     dist = None
@@ -800,13 +850,20 @@ def main() -> None:
         dist = dist_mod
 
     device = torch.device("cuda", local_rank)
-    world = nb.World("tree29", ENVS, substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT,
-                     seed=SEED + 7919 * rank)
+    # Weak scaling: the job is world_size x ENVS environments of one world;
+    # rank r steps its contiguous range of them (reset states of those global
+    # environment indices), with no collective on the data path.
+    begin, end = shard_range(ENVS * world_size, rank, world_size)
+    world = nb.World("tree29", end - begin, substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT, seed=SEED)
+    if begin != 0:
+        rq, rv, _ = nb.sample_reset("tree29", SEED, SEED, begin, end - begin)
+        world.set_state(rq, rv, as_reset_state=True)  # current and reset state
+    envs = world.envs
     gen = torch.Generator(device=device).manual_seed(SEED + rank)
     total_steps = args.warmup + args.steps
-    actions = 0.3 * torch.randn((total_steps, HORIZON, ENVS, world.action_count), device=device, generator=gen)
-    obs = torch.empty((HORIZON, ENVS, world.observation_count), device=device)
-    status = torch.empty((args.steps, HORIZON, ENVS), device=device, dtype=torch.int32)
+    actions = 0.3 * torch.randn((total_steps, HORIZON, envs, world.action_count), device=device, generator=gen)
+    obs = torch.empty((HORIZON, envs, world.observation_count), device=device)
+    status = torch.empty((args.steps, HORIZON, envs), device=device, dtype=torch.int32)
     flush = torch.empty(256 * 1024 * 1024 // 4, device=device, dtype=torch.float32)
     stream = torch.cuda.current_stream(device)
 
@@ -834,25 +891,22 @@ def main() -> None:
         barrier()
     failures = int((status != 0).sum().item())
     clock_summary = clocks.summary()
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, stops)]
+    step_ms = [s_.elapsed_time(e_) for s_, e_ in zip(starts, stops)]
     total_ms = float(sum(step_ms))
-    max_ms = total_ms
-    if dist is not None:
-        t = torch.tensor([total_ms], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        max_ms = float(t.item())
-    env_steps = ENVS * HORIZON * args.steps * world_size
-    value = env_steps / (max_ms / 1e3)
+    stats = reduce_stats(HorizonStats(envs * HORIZON * args.steps, failures, total_ms), dist, device)
+    max_ms = stats.device_ms
+    value = stats.env_steps / (max_ms / 1e3)
 
     # Contact statistics for the algorithmic byte count (one extra advance
     # with counters, outside the timed region).
-    _, _, counters = world.step(actions[0], wait=True)
+    world.step(actions[0], wait=True)
     q_, v_, man_ = world.state()
-    counts = np.array([m.count for m in man_], np.int64).reshape(ENVS, world.pair_count)
+    counts = np.array([m.count for m in man_], np.int64).reshape(envs, world.pair_count)
     mean_points = float(counts.sum(axis=1).mean())
     mean_manifolds = float((counts > 0).sum(axis=1).mean())
 
-    # End-to-end through the reference-shaped C ABI with host buffers: each
+    # End to end through the reference-shaped C ABI with host buffers, over
+    # the same number of advances as the device-resident figure: each
     # advance copies its actions from pinned host memory to the device, runs
     # the control steps and reads statuses, contacts, observations and the
     # final q back to host memory, where the caller reads them through the
@@ -860,7 +914,7 @@ def main() -> None:
     # flushed before each advance, inside the timed region.
     world.set_state(*warm_state)
     world.set_state_readback(True)
-    host_actions = [actions[args.warmup + i].cpu().pin_memory().numpy() for i in range(min(args.steps, 5))]
+    host_actions = [actions[args.warmup + i].cpu().pin_memory().numpy() for i in range(args.steps)]
     world.advance_host(host_actions[0], raise_on_failure=False, copy=False)  # warm the host path
     barrier()
     t0 = time.perf_counter()
@@ -868,34 +922,31 @@ def main() -> None:
         flush.fill_(float(i))
         torch.cuda.synchronize(device)
         world.advance_host(a, raise_on_failure=False, copy=False)
-    e2e_secs = time.perf_counter() - t0
-    e2e_value = ENVS * HORIZON * len(host_actions) * world_size / e2e_secs
-    if dist is not None:
-        t = torch.tensor([e2e_secs], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_value = ENVS * HORIZON * len(host_actions) * world_size / float(t.item())
-    h2d = HORIZON * ENVS * world.action_count * 4
-    d2h = HORIZON * ENVS * (4 + 4 + 4 * world.observation_count) + ENVS * world.nq * 4
+    e2e_stats = reduce_stats(HorizonStats(envs * HORIZON * len(host_actions), 0, 1e3 * (time.perf_counter() - t0)), dist, device)
+    e2e_value = e2e_stats.env_steps / (e2e_stats.device_ms / 1e3)
+    h2d = HORIZON * envs * world.action_count * 4
+    d2h = HORIZON * envs * (4 + 4 + 4 * world.observation_count) + envs * world.nq * 4
     world.set_state_readback(False)
+    del host_actions
 
     chains = world.environment_chains
     launches_per_step = HORIZON * chains  # one control-step launch per chain per control step
     # The chains' launches of one control step run concurrently, so the
     # kernel is timed per control step (all chains, all environments).
-    kernel_ms = (max_ms / world_size if dist is None else total_ms) / (args.steps * HORIZON)
+    kernel_ms = total_ms / (args.steps * HORIZON)
     bytes_per_env_step = _algorithmic_bytes_per_env_step(world.nq, world.nv, world.action_count, mean_points, mean_manifolds)
-    achieved = bytes_per_env_step * ENVS / (kernel_ms / 1e3) / 1e9
+    achieved = bytes_per_env_step * envs / (kernel_ms / 1e3) / 1e9
     peaks = _measured_peaks()
     traffic = _profile_traffic()
 
     launch_shape = world.launch_shape()
+    world.close()
     plain = plain_aba_chain7(device) if rank == 0 else None
 
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         try:
-            host_state = (warm_state[0], warm_state[1], world.friction_scales())
-            cpu = cpu_reference_sample(host_state, actions[args.warmup, :CPU_SAMPLE_STEPS].cpu().numpy(), os.cpu_count() or 1)
+            cpu = _reference_sample(os.cpu_count() or 1, _reference_actions(0))
             cpu.pop("seconds", None)
         except (FileNotFoundError, OSError, RuntimeError) as exc:
             cpu = {"unavailable": str(exc)}
@@ -915,9 +966,10 @@ def main() -> None:
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic (seeded)",
-            "config": {**_config(world_size), "launch": {**dict(zip(("envs_per_cta", "resident_envs_per_sm"), launch_shape)),
-                                                          "environment_chains": chains}},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "config": _config(world_size),
+            "launch": {**dict(zip(("envs_per_cta", "resident_envs_per_sm"), launch_shape)), "environment_chains": chains},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "advances_timed": args.steps},
             "roofline": {
                 "bound": "hbm",
                 "achieved": achieved,
@@ -935,17 +987,15 @@ def main() -> None:
             "clocks": {k: clock_summary[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
             "latency_ms_per_advance": {"p50": step_sorted[len(step_sorted) // 2],
                                         "p99": step_sorted[min(len(step_sorted) - 1, int(0.99 * len(step_sorted)))]},
-            "failed_env_steps": failures,
+            "failed_env_steps": stats.failed_env_steps,
             "mean_active_contacts": mean_points,
             "mean_manifolds": mean_manifolds,
             "plain_aba_chain7": plain,
         }
         print(json.dumps(line))
-    world.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
-
 
 if __name__ == "__main__":
     main()

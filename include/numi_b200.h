@@ -739,7 +739,17 @@ MR_API int mr_server_stats(const MRServerHandle* server, MRServerStatsC* stats);
  * other host threads) race with each other; nothing in the workspace needs
  * to start at zero, since the kernel writes every word before reading it.
  * environment_count above MR_B200_NO_ALLOC_MAX_ENVS is rejected with a
- * message (-1). */
+ * message (-1).
+ *
+ * The world record is shared too: only one world is resident per device.
+ * Each upload gets a new tag and each launch carries the tag current when it
+ * was enqueued, so work that runs after another world was uploaded (work
+ * the caller recorded into a graph and replays later, say) steps nothing:
+ * such an environment
+ * keeps q, v and manifolds untouched and reports MR_STEP_UNSUPPORTED in
+ * status_codes and in counter 9 of mr_pile_step_no_alloc_counters.  Work
+ * enqueued by this call therefore depends on the world record current when
+ * it runs, not only on the arguments. */
 MR_API int mr_pile_step_no_alloc(
     uint32_t source, uint64_t model_seed, uint32_t environment_count,
     float* q, float* v, float* manifolds, uint32_t* manifold_counts,
@@ -747,6 +757,16 @@ MR_API int mr_pile_step_no_alloc(
     uint32_t control_step_count, float control_timestep_seconds,
     uint32_t physics_substeps, uint32_t velocity_iterations,
     uint32_t final_velocity_iterations, uint64_t cuda_stream);
+
+/* No counterpart in the reference.  Copies the first `count` (<= 16) launch
+ * counters of the last mr_pile_step_no_alloc call on the current device into
+ * host memory, after the work on `cuda_stream` has finished (the call waits
+ * for that stream).  Counters: 0 failed environment-steps, 1 most active
+ * contacts, 2 most manifolds, 3 most raw contacts, 4 most candidate pairs,
+ * 5 most islands, 6 lowest failing environment (0xffffffff: none), 8 resets,
+ * 9 environment-steps skipped because the world record had been replaced.
+ * Allocates nothing. */
+MR_API int mr_pile_step_no_alloc_counters(uint32_t* counters, uint32_t count, uint64_t cuda_stream);
 
 #ifdef __cplusplus
 }

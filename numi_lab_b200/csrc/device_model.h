@@ -161,6 +161,7 @@ enum StatIndex : int {
     kStatFirstFailEnv = 6,
     kStatFirstFailCode = 7,
     kStatResets = 8,
+    kStatWorldMismatch = 9,  // scene items skipped: the world record was not the one the launch was enqueued for
     kStatCount = 16
 };
 

@@ -12,6 +12,7 @@
 // arrays (about 8 MB) until the process exits.
 #include "numi_b200.h"
 #include "runtime.h"
+#include "device_model.h"
 #include "scene.h"
 
 #include <cstdint>
@@ -47,6 +48,11 @@ struct DeviceState {
     std::uint32_t source = 0;
     std::uint64_t seed = 0;
     float h = 0.0f;
+    // Tag of the record in g_model: bumped by every upload, stored in the
+    // record and passed with every launch, so a launch recorded for one
+    // world (a captured graph, say) and run after another world's upload
+    // reports a mismatch instead of stepping the wrong world.
+    std::uint32_t generation = 0;
     numi::SceneModel host_model{};  // source of the last model upload
 };
 
@@ -104,6 +110,8 @@ MR_API int mr_pile_step_no_alloc(uint32_t source, uint64_t model_seed, uint32_t 
             const numi::CompiledModel m = source == MR_RUN_SOURCE_SYNTHETIC_PILE ? numi::build_pile(model_seed)
                                                                                  : numi::build_stack(model_seed);
             d.host_model = numi::rt::pack_scene(m, h);
+            d.generation = d.generation == 0xffffffffu ? 1u : d.generation + 1u;
+            d.host_model.world_tag = d.generation;
             check(cudaMemcpyAsync(d.model, &d.host_model, sizeof(numi::SceneModel), cudaMemcpyHostToDevice, stream),
                   "world record upload");
             d.have_model = true;
@@ -112,6 +120,7 @@ MR_API int mr_pile_step_no_alloc(uint32_t source, uint64_t model_seed, uint32_t 
             d.h = h;
         }
         check(cudaMemsetAsync(d.stats, 0, kStatWords * sizeof(std::uint32_t), stream), "clear counters");
+        check(cudaMemsetAsync(d.stats + numi::kStatFirstFailEnv, 0xff, sizeof(std::uint32_t), stream), "clear counters");
         for (std::uint32_t k = 0; k < control_step_count; ++k) {
             numi::SceneParams p{};
             p.model = d.model;
@@ -128,8 +137,24 @@ MR_API int mr_pile_step_no_alloc(uint32_t source, uint64_t model_seed, uint32_t 
             p.velocity_iterations = static_cast<int>(velocity_iterations);
             p.final_velocity_iterations = static_cast<int>(final_velocity_iterations);
             p.support_mapped = d.host_model.support_mapped;
+            p.world_tag = d.generation;
             check(numi::launch_scene_step(p, stream), "scene step launch");
         }
+    });
+}
+
+MR_API int mr_pile_step_no_alloc_counters(uint32_t* counters, uint32_t count, uint64_t cuda_stream) {
+    return guarded([&] {
+        if (!counters) throw std::invalid_argument("counters must be a non-null host pointer");
+        if (count == 0 || count > kStatWords)
+            throw std::invalid_argument("count must be in [1, " + std::to_string(kStatWords) + "]");
+        cudaStream_t stream = reinterpret_cast<cudaStream_t>(cuda_stream);
+        std::lock_guard<std::mutex> lock(g_mutex);
+        DeviceState& d = device_state();
+        // Pageable host memory: the copy completes before the call returns.
+        check(cudaMemcpyAsync(counters, d.stats, count * sizeof(std::uint32_t), cudaMemcpyDeviceToHost, stream),
+              "counter read-back");
+        check(cudaStreamSynchronize(stream), "counter read-back");
     });
 }
 

@@ -402,6 +402,10 @@ struct MRTaskRolloutHandle {
     int chains = 1;
     cudaStream_t chain_stream[kMaxChains] = {};
     cudaEvent_t ev_fork = nullptr, ev_chain[kMaxChains] = {};
+    // Chain c > 0 reads its observations back on its own copy stream (chain 0
+    // uses copy_stream), so no chain's copies queue behind another chain's.
+    cudaStream_t chain_copy_stream[kMaxChains] = {};
+    cudaEvent_t ev_chain_copies[kMaxChains] = {};
 
     DeviceBuffer<numi::DeviceModel> d_model;
     DeviceBuffer<float> d_q, d_v, d_manifolds, d_reset_q, d_reset_v, d_friction;
@@ -458,6 +462,8 @@ struct MRTaskRolloutHandle {
         for (int c = 0; c < kMaxChains; ++c) {
             if (ev_chain[c]) cudaEventDestroy(ev_chain[c]);
             if (chain_stream[c]) cudaStreamDestroy(chain_stream[c]);
+            if (ev_chain_copies[c]) cudaEventDestroy(ev_chain_copies[c]);
+            if (chain_copy_stream[c]) cudaStreamDestroy(chain_copy_stream[c]);
         }
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_step) cudaEventDestroy(ev_step);
@@ -574,7 +580,7 @@ struct MRTaskRolloutHandle {
                 check(numi::launch_control_step(p, precision == MR_PRECISION_COMPENSATED ? layout_comp : layout, contact, precision,
                                                 warps_per_block[precision], cs),
                       "control step launch");
-                if (host_obs && obs) copy_observation_rows(k, o, n, obs, host_obs, cs);
+                if (host_obs && obs) copy_observation_rows(k, o, n, obs, host_obs, cs, c);
             }
             if (driven && evaluate_final) enqueue_policy(steps, o, n, nullptr, false, cs);
         }
@@ -585,7 +591,7 @@ struct MRTaskRolloutHandle {
             }
         }
         if (driven) check(numi::launch_policy_counter(d_policy_steps.ptr, steps, s), "policy counter");
-        if (host_obs && obs) join_copies(s);
+        if (host_obs && obs) join_copies(s, nchains);
     }
 
     // Checks an advance's policy arguments and sizes the policy outputs.
@@ -655,17 +661,25 @@ struct MRTaskRolloutHandle {
     }
     // Rows [o, o + n) of step k's observations, once the work enqueued on
     // `s` so far is done.
-    void copy_observation_rows(std::uint32_t k, std::uint32_t o, std::uint32_t n, const float* obs, float* host_obs, cudaStream_t s) {
+    // Chain `chain` copies on its own copy stream.
+    void copy_observation_rows(std::uint32_t k, std::uint32_t o, std::uint32_t n, const float* obs, float* host_obs, cudaStream_t s,
+                               int chain = 0) {
         const size_t nobs = model.world.nq + model.world.nv;
         const size_t at = (static_cast<size_t>(k) * envs + o) * nobs;
+        cudaStream_t cs = chain == 0 ? copy_stream : chain_copy_stream[chain];
         check(cudaEventRecord(ev_step, s), "event");
-        check(cudaStreamWaitEvent(copy_stream, ev_step, 0), "stream wait");
-        check(cudaMemcpyAsync(host_obs + at, obs + at, static_cast<size_t>(n) * nobs * sizeof(float), cudaMemcpyDeviceToHost, copy_stream),
+        check(cudaStreamWaitEvent(cs, ev_step, 0), "stream wait");
+        check(cudaMemcpyAsync(host_obs + at, obs + at, static_cast<size_t>(n) * nobs * sizeof(float), cudaMemcpyDeviceToHost, cs),
               "observations D2H");
     }
-    void join_copies(cudaStream_t s) {
+    // `s` waits for the copies of chains [0, chains).
+    void join_copies(cudaStream_t s, int chains_used = 1) {
         check(cudaEventRecord(ev_copies, copy_stream), "event");
         check(cudaStreamWaitEvent(s, ev_copies, 0), "stream wait");
+        for (int c = 1; c < chains_used; ++c) {
+            check(cudaEventRecord(ev_chain_copies[c], chain_copy_stream[c]), "event");
+            check(cudaStreamWaitEvent(s, ev_chain_copies[c], 0), "stream wait");
+        }
     }
 
     void run(std::uint32_t steps, const float* actions, const std::uint32_t* masks, float* obs, std::uint32_t* status,
@@ -830,6 +844,10 @@ MR_API MRTaskRolloutHandle* mr_create_task_rollout(const MRRunManifestC* manifes
         for (int c = 0; c < MRTaskRolloutHandle::kMaxChains; ++c) {
             check(cudaStreamCreateWithFlags(&h.chain_stream[c], cudaStreamNonBlocking), "chain stream");
             check(cudaEventCreateWithFlags(&h.ev_chain[c], cudaEventDisableTiming), "event");
+            if (c > 0) {
+                check(cudaStreamCreateWithFlags(&h.chain_copy_stream[c], cudaStreamNonBlocking), "chain copy stream");
+                check(cudaEventCreateWithFlags(&h.ev_chain_copies[c], cudaEventDisableTiming), "event");
+            }
         }
         // Two chains once the batch exceeds one resident wave of the FP32
         // kernel (at 4096 tree29 envs: 2.3 waves; measured +18 % over one

@@ -39,7 +39,8 @@ struct alignas(16) SceneModel {
     float4 ground_rotation;  // anchors on the plane live in this frame
     std::int32_t plane_material;
     std::int32_t support_mapped;  // some pair is MR_COLLISION_PAIR_CONVEX (GJK / EPA)
-    std::int32_t reserved1[2];
+    std::uint32_t world_tag;  // identifies this record to launches that check SceneParams::world_tag (0: untagged)
+    std::int32_t reserved1;
     // Bodies (one collider each, at the body's centre of mass).
     std::int32_t shape_type[kSceneMaxBodies];
     std::int32_t material[kSceneMaxBodies];
@@ -81,6 +82,12 @@ struct SceneParams {
     std::int32_t final_velocity_iterations;
     float* q_comp;             // [slot][nb][7]: compensation of the position sums (entries 0-2), or null (FP32 sums)
     std::int32_t support_mapped;  // the model has support-mapped (cylinder) pairs: SceneModel::support_mapped
+    // Non-zero: the launch was enqueued for the record with this tag.  A
+    // launch that finds another record behind `model` (a shared record
+    // replaced after the launch was recorded, e.g. in a replayed graph)
+    // leaves every buffer of the item untouched and reports
+    // MR_STEP_UNSUPPORTED in its status code and kStatWorldMismatch.
+    std::uint32_t world_tag;
 };
 
 size_t scene_step_smem_bytes(bool compensated = false);

@@ -1396,6 +1396,19 @@ __global__ void __launch_bounds__(32, 16) scene_step_kernel(SceneParams p) {
     const int env = p.env_index != nullptr ? p.env_index[item] : item;
     const int lane = threadIdx.x;
     const SceneModel& M = *p.model;
+    if (p.world_tag != 0u && M.world_tag != p.world_tag) {
+        // The record behind p.model is not the world this launch was
+        // enqueued for: its body count need not match the caller's buffers,
+        // so touch none of them.
+        if (lane == 0) {
+            if (p.status_codes) p.status_codes[item] = MR_STEP_UNSUPPORTED;
+            if (p.active_contacts) p.active_contacts[item] = 0u;
+            atomicAdd(p.stats + 0, 1u);
+            atomicMin(p.stats + 6, static_cast<unsigned>(env));
+            atomicAdd(p.stats + 9, 1u);
+        }
+        return;
+    }
     const int nb = M.nb;
     const int nq = nb * 7, nv = nb * 6;
     float* misc = s + kOffMisc;

@@ -438,6 +438,7 @@ EXPORTED_SYMBOLS: Final = (
     "mr_server_release",
     "mr_server_stats",
     "mr_pile_step_no_alloc",
+    "mr_pile_step_no_alloc_counters",
     "mr_task_rollout_set_policy",
     "mr_task_rollout_environment_chains",
     "mr_task_rollout_policy_revision",
@@ -575,6 +576,8 @@ class Bindings:
         L.mr_pile_step_no_alloc.argtypes = [ct.c_uint32, ct.c_uint64, ct.c_uint32] + [ct.c_void_p] * 6 + [
             ct.c_uint32, ct.c_float, ct.c_uint32, ct.c_uint32, ct.c_uint32, ct.c_uint64]
         L.mr_pile_step_no_alloc.restype = ct.c_int
+        L.mr_pile_step_no_alloc_counters.argtypes = [P(ct.c_uint32), ct.c_uint32, ct.c_uint64]
+        L.mr_pile_step_no_alloc_counters.restype = ct.c_int
 
     def last_error(self) -> str:
         value = self.lib.mr_last_error()

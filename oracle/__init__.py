@@ -315,6 +315,33 @@ class Reference:
         return secs, int(failed.value)
 
 
+class ReferenceBatch:
+    """One reference model per environment, each with that environment's
+    friction scale, stepped together by the reference's CPU world step
+    (stepControlledArticulatedWorldCpu) on `threads` host threads."""
+
+    def __init__(self, records, h: float, friction: np.ndarray) -> None:
+        self.models = [Reference(records, h, float(f)) for f in np.asarray(friction, np.float64)]
+        lib = self.models[0].lib
+        lib.ref_run_envs.restype = ct.c_double
+        lib.ref_run_envs.argtypes = [ct.POINTER(ct.c_void_p), ct.c_uint32, _DP, _DP, ct.POINTER(ct.c_float), ct.c_uint32,
+                                     ct.c_uint32, ct.c_uint32, ct.c_int, ct.POINTER(ct.c_uint64)]
+        self.lib = lib
+        self.handles = (ct.c_void_p * len(self.models))(*[m.handle for m in self.models])
+
+    def run(self, q: np.ndarray, v: np.ndarray, actions: np.ndarray, substeps: int, threads: int, solver: int = 1):
+        """Steps env e (q[e], v[e], float64, in place) for actions.shape[0]
+        control steps; returns (seconds, failed substeps)."""
+
+        envs = q.shape[0]
+        assert envs == len(self.models) and q.dtype == np.float64 and v.dtype == np.float64
+        failed = ct.c_uint64(0)
+        acts = np.ascontiguousarray(actions, np.float32)
+        secs = self.lib.ref_run_envs(self.handles, envs, _dp(q), _dp(v), acts.ctypes.data_as(ct.POINTER(ct.c_float)),
+                                     actions.shape[0], substeps, threads, solver, ct.byref(failed))
+        return secs, int(failed.value)
+
+
 SCENE_MANIFOLDS = 128
 SCENE_SLOT_WORDS = 57
 

@@ -362,17 +362,21 @@ __attribute__((visibility("default"))) int ref_world_step_once(RefModel* r, doub
 // transactional CPU world step with its quality (default) or FP64
 // reference-conic solver; free-motion worlds use integrateArticulatedState.
 // q/v are updated in place; failed steps are counted.
-__attribute__((visibility("default"))) double ref_run(RefModel* r, uint32_t envs, double* q, double* v, const float* actions,
-                                                      uint32_t steps, uint32_t substeps, uint32_t threads, int solver,
-                                                      uint64_t* failed_steps) {
-    const std::uint32_t nq = r->world.nq, nv = r->world.nv, na = r->world.action_count;
-    const bool contact = !r->env_shapes.empty();
+// `models` holds one model per environment (they differ only in their
+// material friction: each environment's friction scale), all of one world.
+__attribute__((visibility("default"))) double ref_run_envs(RefModel* const* models, uint32_t envs, double* q, double* v,
+                                                           const float* actions, uint32_t steps, uint32_t substeps, uint32_t threads,
+                                                           int solver, uint64_t* failed_steps) {
+    const RefModel* r0 = models[0];
+    const std::uint32_t nq = r0->world.nq, nv = r0->world.nv, na = r0->world.action_count;
+    const bool contact = !r0->env_shapes.empty();
     std::atomic<std::uint64_t> failed{0};
     auto worker = [&](std::uint32_t begin, std::uint32_t end) {
-        const ArticulatedWorldConfig cfg = world_config(r, solver);
         std::vector<double> tau(nv);
         std::vector<ArticulatedDofCommand> commands(nv);
         for (std::uint32_t e = begin; e < end; ++e) {
+            RefModel* r = models[e];
+            const ArticulatedWorldConfig cfg = world_config(r, solver);
             ArticulatedWorldCache cache{};
             double* qe = q + static_cast<size_t>(e) * nq;
             double* ve = v + static_cast<size_t>(e) * nv;
@@ -416,6 +420,14 @@ __attribute__((visibility("default"))) double ref_run(RefModel* r, uint32_t envs
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (failed_steps) *failed_steps = failed.load();
     return secs;
+}
+
+// All environments share model `r` (one friction scale).
+__attribute__((visibility("default"))) double ref_run(RefModel* r, uint32_t envs, double* q, double* v, const float* actions,
+                                                      uint32_t steps, uint32_t substeps, uint32_t threads, int solver,
+                                                      uint64_t* failed_steps) {
+    std::vector<RefModel*> models(envs, r);
+    return ref_run_envs(models.data(), envs, q, v, actions, steps, substeps, threads, solver, failed_steps);
 }
 
 }  // extern "C"
