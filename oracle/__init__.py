@@ -29,6 +29,7 @@ REFERENCE_SOURCES = Path(os.environ.get("NUMI_REFERENCE_ROOT", "/root/reference"
 
 MAX_CONTACTS = 32
 MANIFOLD_POINTS = 4
+CONTACT_ROW = 24  # doubles per contact row (oracle_articulated_contacts, ref_articulated_contacts)
 
 
 class OraclePoint(ct.Structure):
@@ -220,6 +221,24 @@ class Oracle:
         ok = self.lib.oracle_invert3x3(_dp(np.ascontiguousarray(m, np.float64).reshape(9)), _dp(out))
         return bool(ok), out.reshape(3, 3)
 
+    def articulated_contacts(self, q, vf, manifolds, friction: float, speculative: bool = False):
+        """Collision + ConstraintIR rows at (q, vf); manifolds updated in place.
+        Returns (status, raw [n, 16], rows [m, CONTACT_ROW])."""
+
+        L = self.lib
+        if not getattr(self, "_contacts_bound", False):
+            L.oracle_articulated_contacts.restype = ct.c_uint32
+            L.oracle_articulated_contacts.argtypes = [ct.c_void_p, _DP, _DP, ct.c_void_p, ct.c_double, ct.c_int, _DP, ct.c_uint32,
+                                                      ct.POINTER(ct.c_uint32), _DP, ct.c_uint32, ct.POINTER(ct.c_uint32)]
+            self._contacts_bound = True
+        raw = np.zeros((256, 16))
+        rows = np.zeros((MAX_CONTACTS * 4, CONTACT_ROW))
+        nr, nc = ct.c_uint32(0), ct.c_uint32(0)
+        st = L.oracle_articulated_contacts(self.handle, _dp(np.ascontiguousarray(q, np.float64)), _dp(np.ascontiguousarray(vf, np.float64)),
+                                           ct.cast(manifolds, ct.c_void_p), float(friction), 1 if speculative else 0, _dp(raw), 256,
+                                           ct.byref(nr), _dp(rows), rows.shape[0], ct.byref(nc))
+        return int(st), raw[: nr.value].copy(), rows[: nc.value].copy()
+
     def temporal_cone_dense(self, W, u0, mu, iterations: int, lam0=None) -> np.ndarray:
         n = len(mu)
         lam = np.zeros(3 * n) if lam0 is None else np.array(lam0, np.float64)
@@ -303,6 +322,42 @@ class Reference:
                                       _dp(imp), _dp(vel), ct.byref(viol))
         return st, imp, vel, viol.value
 
+    def contact_cache(self):
+        """A persistent-manifold cache for articulated_contacts (one per environment)."""
+
+        L = self.lib
+        L.ref_contact_cache_create.restype = ct.c_void_p
+        L.ref_contact_cache_destroy.argtypes = [ct.c_void_p]
+        handle = L.ref_contact_cache_create()
+
+        class _Cache:
+            def __init__(self, h):
+                self.handle = h
+
+            def __del__(self):
+                try:
+                    L.ref_contact_cache_destroy(self.handle)
+                except Exception:
+                    pass
+
+        return _Cache(handle)
+
+    def articulated_contacts(self, cache, q, vf):
+        """The reference CPU world step's collision and ConstraintIR
+        evaluation at (q, vf).  Returns (status, raw [n, 16], manifolds
+        [m, 58], rows [k, CONTACT_ROW]); shape indices are record indices."""
+
+        L = self.lib
+        L.ref_articulated_contacts.restype = ct.c_int
+        L.ref_articulated_contacts.argtypes = [ct.c_void_p, ct.c_void_p, _DP, _DP, ct.c_uint32, _DP, ct.POINTER(ct.c_uint32),
+                                               ct.c_uint32, _DP, ct.POINTER(ct.c_uint32), ct.c_uint32, _DP, ct.POINTER(ct.c_uint32)]
+        raw, man, rows = np.zeros((256, 16)), np.zeros((128, 58)), np.zeros((256, CONTACT_ROW))
+        nr, nm, nc = ct.c_uint32(0), ct.c_uint32(0), ct.c_uint32(0)
+        st = L.ref_articulated_contacts(self.handle, cache.handle, _dp(np.ascontiguousarray(q, np.float64)),
+                                        _dp(np.ascontiguousarray(vf, np.float64)), 256, _dp(raw), ct.byref(nr), 128, _dp(man),
+                                        ct.byref(nm), 256, _dp(rows), ct.byref(nc))
+        return int(st), raw[: nr.value].copy(), man[: nm.value].copy(), rows[: nc.value].copy()
+
     def run(self, q: np.ndarray, v: np.ndarray, actions: np.ndarray, substeps: int, threads: int, solver: int = 1):
         """Steps every env for actions.shape[0] control steps; returns (seconds, failed)."""
 
@@ -313,6 +368,23 @@ class Reference:
         secs = self.lib.ref_run(self.handle, envs, _dp(q), _dp(v), acts.ctypes.data_as(ct.POINTER(ct.c_float)), steps, substeps,
                                 threads, solver, ct.byref(failed))
         return secs, int(failed.value)
+
+
+def reference_islands(dynamic: np.ndarray, pairs: np.ndarray) -> tuple[int, np.ndarray]:
+    """buildConstraintIslands (ConstraintSolver.cpp:848) over a contact set of
+    (bodyA, bodyB) pairs: (island count, island index per body, 0xffffffff
+    for a body in no island)."""
+
+    lib = ct.CDLL(str(REF_LIB))
+    lib.ref_build_islands.restype = ct.c_uint32
+    lib.ref_build_islands.argtypes = [ct.c_uint32, ct.POINTER(ct.c_uint8), ct.c_uint32, ct.POINTER(ct.c_uint32),
+                                      ct.POINTER(ct.c_uint32)]
+    dyn = np.ascontiguousarray(dynamic, np.uint8)
+    pr = np.ascontiguousarray(pairs, np.uint32).reshape(-1)
+    out = np.zeros(len(dyn), np.uint32)
+    n = lib.ref_build_islands(len(dyn), dyn.ctypes.data_as(ct.POINTER(ct.c_uint8)), len(pr) // 2,
+                              pr.ctypes.data_as(ct.POINTER(ct.c_uint32)), out.ctypes.data_as(ct.POINTER(ct.c_uint32)))
+    return int(n), out
 
 
 class ReferenceBatch:
@@ -361,6 +433,9 @@ class OracleSceneTrace(ct.Structure):
         ("islands", ct.c_uint32),
         ("band_decisions", ct.c_uint32),
         ("min_decision_margin", ct.c_double),
+        ("island_contacts", ct.c_uint32),
+        ("island_pairs", ct.c_int32 * 512),
+        ("island_of", ct.c_uint32 * 64),
     ]
 
 

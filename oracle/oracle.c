@@ -711,7 +711,7 @@ static int cless(const Cand* a, const Cand* b) {
 /* Pair flag + raw contacts + buildPersistentWorldManifold +
  * reduceCandidates (Collision.metal:796-850, 4379-4830, 5115-5556). */
 static int pair_manifold(const OracleWorld* o, const Kin* k, const double* margins, uint32_t pair, OracleManifold* slot,
-                         int* candidate) {
+                         int* candidate, Raw* raw_out, int* nraw_out) {
     const MRModelPairC* pr = &o->pairs[pair];
     Shape A, B;
     make_shape(o, k, pr->shape_a, margins[pr->shape_a], &A);
@@ -775,6 +775,10 @@ static int pair_manifold(const OracleWorld* o, const Kin* k, const double* margi
         }
     }
 #undef APPEND
+    if (raw_out) {
+        for (int i = 0; i < nraw; ++i) raw_out[i] = raw[i];
+        *nraw_out = nraw;
+    }
     if (nraw == 0) {
         slot->count = 0;
         return 0;
@@ -980,17 +984,96 @@ typedef struct {
     uint32_t pair, point, body, new_impact;
     int b_side;
     v3 x, n, t, bt;
-    double sep, target[3], reg[3], mu, lambda[3], P[9], relax, delta[3];
+    double sep, target[3], reg[3], mu, lambda[3], P[9], relax, delta[3], rel[3];
     double G[3][MAXV];
 } Contact;
 
-static uint32_t contact_substep(const OracleWorld* o, double* q, double* v, const double* vf, const Kin* k, OracleManifold* slots,
-                                double friction_scale, int final_substep, OracleTrace* trace, uint32_t* fail_index) {
-    const uint32_t nv = o->w.nv, np = o->w.pair_count, ns = o->w.shape_count;
+/* One manifold point as a solver contact: world frame, Jacobian rows at
+ * the free velocity, ConstraintIR evaluation (target velocity with the
+ * speculative approach term, critically damped stabilisation and
+ * restitution on a new impact; regularisation; static or dynamic friction
+ * by slip) -- Collision.metal:10253-10620, MetalWorldContact.metal:3580-3990. */
+static void prepare_contact(const OracleWorld* o, const Kin* k, const OracleManifold* slot, uint32_t p, int i, const double* vf,
+                            double friction_scale, Contact* ct) {
+    const uint32_t nv = o->w.nv;
+    const double h = o->h;
+    const MRModelPairC* pr = &o->pairs[p];
+    const MRModelShapeC* sa = &o->shapes[pr->shape_a];
+    const MRModelShapeC* sb = &o->shapes[pr->shape_b];
+    const MRModelBodyC* ba = &o->bodies[sa->body];
+    const MRModelBodyC* bb = &o->bodies[sb->body];
+    v3 posA, posB;
+    q4 rotA, rotB;
+    if (ba->articulated) { posA = k->pos[sa->body]; rotA = k->rot[sa->body]; }
+    else { posA = vldf(ba->static_pose); qnormalize(qldf(ba->static_pose + 4), &rotA, 0); }
+    if (bb->articulated) { posB = k->pos[sb->body]; rotB = k->rot[sb->body]; }
+    else { posB = vldf(bb->static_pose); qnormalize(qldf(bb->static_pose + 4), &rotB, 0); }
+    v3 nw = qrot(rotA, vld(slot->normal_local));
+    nw = vmul(nw, 1.0 / vlen(nw));
+    v3 tw = qrot(rotA, vld(slot->tangent_local));
+    tw = vsub(tw, vmul(nw, vdot(tw, nw)));
+    tw = vdot(tw, tw) > 1.0e-12 ? vmul(tw, 1.0 / vlen(tw)) : stable_tangent(nw);
+    const v3 bw = vcross(nw, tw);
+    const MRModelMaterialC* ma = &o->materials[sa->material];
+    const MRModelMaterialC* mb = &o->materials[sb->material];
+    const double mu_s = sqrt(fmax(0.0, (double)ma->friction[0] * mb->friction[0])) * friction_scale;
+    const double mu_d = sqrt(fmax(0.0, (double)ma->friction[1] * mb->friction[1])) * friction_scale;
+    const double restitution = fmin(fmax(fmax(ma->response[0], mb->response[0]), 0.0), 1.0);
+    const double rthr = fmax(ma->response[1], mb->response[1]);
+    const double compliance = (double)ma->response[2] + mb->response[2];
+    const double dissipation = (double)ma->response[3] + mb->response[3];
+    const double rest = (double)sa->contact_rest_bound[1] + sb->contact_rest_bound[1];
+    const OraclePoint* op = &slot->points[i];
+    const v3 pa = vadd(posA, qrot(rotA, vld(op->anchor_a)));
+    const v3 pb = vadd(posB, qrot(rotB, vld(op->anchor_b)));
+    ct->pair = p;
+    ct->point = (uint32_t)i;
+    ct->x = vmul(vadd(pa, pb), 0.5);
+    ct->sep = vdot(vsub(pb, pa), nw) - rest;
+    ct->n = nw; ct->t = tw; ct->bt = bw;
+    ct->new_impact = op->life == 0u;
+    ct->b_side = !ba->articulated;
+    ct->body = ct->b_side ? sb->body : sa->body;
+    for (int a = 0; a < 3; ++a) ct->lambda[a] = op->impulses[a];
+    /* Jacobian rows and relative velocity at v_free. */
+    double J[3 * MAXV];
+    point_jacobian_k(o, k, ct->body, ct->x, J);
+    const double sign = ct->b_side ? 1.0 : -1.0;
+    const v3 dirs[3] = {nw, tw, bw};
+    for (int r = 0; r < 3; ++r) {
+        ct->rel[r] = 0.0;
+        for (uint32_t d = 0; d < nv; ++d) {
+            const double g = sign * (vget(dirs[r], 0) * J[d] + vget(dirs[r], 1) * J[nv + d] + vget(dirs[r], 2) * J[2 * nv + d]);
+            ct->G[r][d] = g;
+            ct->rel[r] += g * vf[d];
+        }
+    }
+    ct->target[0] = ct->sep > 0.0 ? -ct->sep / h : 0.0;
+    ct->target[1] = ct->target[2] = 0.0;
+    ct->reg[0] = fmax(compliance / (h * h) + dissipation / h, 0.0);
+    ct->reg[1] = ct->reg[2] = 0.0;
+    const double tau_c = 2.0 * h;
+    const double err = fmin(ct->sep + o->w.solver_scales[3], 0.0);
+    const double ratio = h / tau_c;
+    const double den = 1.0 + 2.0 * ratio + ratio * ratio;
+    double stab = -h * err / (tau_c * tau_c * den);
+    stab = fmin(fmax(stab, 0.0), o->w.solver_scales[2]);
+    if (ct->new_impact) {
+        const double incoming = ct->rel[0] - ct->target[0];
+        if (incoming < -rthr) stab = fmax(stab, -restitution * incoming);
+    }
+    ct->target[0] += stab;
+    const double slip = sqrt(ct->rel[1] * ct->rel[1] + ct->rel[2] * ct->rel[2]);
+    ct->mu = slip <= 1.0e-3 ? mu_s : mu_d;
+}
+
+/* Speculative collision margins of the articulated shapes for a substep
+ * whose free velocity is vf (Collision.metal:5794-6030). */
+static void speculative_margins(const OracleWorld* o, const double* vf, double* margins) {
+    const uint32_t nv = o->w.nv, ns = o->w.shape_count;
     const double h = o->h;
     double gs = 0.0;
     for (uint32_t d = 0; d < nv; ++d) gs += fabs(vf[d]);
-    double margins[MAXS];
     for (uint32_t s = 0; s < ns; ++s) {
         margins[s] = 0.0;
         const MRModelShapeC* src = &o->shapes[s];
@@ -1005,12 +1088,20 @@ static uint32_t contact_substep(const OracleWorld* o, double* q, double* v, cons
             margins[s] = o->w.speculative[0] * env;
         }
     }
+}
+
+static uint32_t contact_substep(const OracleWorld* o, double* q, double* v, const double* vf, const Kin* k, OracleManifold* slots,
+                                double friction_scale, int final_substep, OracleTrace* trace, uint32_t* fail_index) {
+    const uint32_t nv = o->w.nv, np = o->w.pair_count;
+    const double h = o->h;
+    double margins[MAXS];
+    speculative_margins(o, vf, margins);
     static __thread Contact C[MAXC];
     uint32_t total = 0, manifolds = 0;
     int counts[MAXP];
     for (uint32_t p = 0; p < np; ++p) {
         int cand = 0;
-        counts[p] = pair_manifold(o, k, margins, p, &slots[p], &cand);
+        counts[p] = pair_manifold(o, k, margins, p, &slots[p], &cand, NULL, NULL);
         if (counts[p] < 0) { *fail_index = p; return MR_STEP_NONFINITE_RESULT; }
         total += (uint32_t)counts[p];
         if (counts[p] > 0) manifolds++;
@@ -1018,80 +1109,8 @@ static uint32_t contact_substep(const OracleWorld* o, double* q, double* v, cons
     trace->manifold_count = manifolds;
     if (total > o->w.contact_capacity) { *fail_index = total; return MR_STEP_CONTACT_CAPACITY_OVERFLOW; }
     uint32_t c = 0;
-    for (uint32_t p = 0; p < np; ++p) {
-        if (counts[p] <= 0) continue;
-        const MRModelPairC* pr = &o->pairs[p];
-        const MRModelShapeC* sa = &o->shapes[pr->shape_a];
-        const MRModelShapeC* sb = &o->shapes[pr->shape_b];
-        const MRModelBodyC* ba = &o->bodies[sa->body];
-        const MRModelBodyC* bb = &o->bodies[sb->body];
-        v3 posA, posB;
-        q4 rotA, rotB;
-        if (ba->articulated) { posA = k->pos[sa->body]; rotA = k->rot[sa->body]; }
-        else { posA = vldf(ba->static_pose); qnormalize(qldf(ba->static_pose + 4), &rotA, 0); }
-        if (bb->articulated) { posB = k->pos[sb->body]; rotB = k->rot[sb->body]; }
-        else { posB = vldf(bb->static_pose); qnormalize(qldf(bb->static_pose + 4), &rotB, 0); }
-        const OracleManifold* slot = &slots[p];
-        v3 nw = qrot(rotA, vld(slot->normal_local));
-        nw = vmul(nw, 1.0 / vlen(nw));
-        v3 tw = qrot(rotA, vld(slot->tangent_local));
-        tw = vsub(tw, vmul(nw, vdot(tw, nw)));
-        tw = vdot(tw, tw) > 1.0e-12 ? vmul(tw, 1.0 / vlen(tw)) : stable_tangent(nw);
-        const v3 bw = vcross(nw, tw);
-        const MRModelMaterialC* ma = &o->materials[sa->material];
-        const MRModelMaterialC* mb = &o->materials[sb->material];
-        const double mu_s = sqrt(fmax(0.0, (double)ma->friction[0] * mb->friction[0])) * friction_scale;
-        const double mu_d = sqrt(fmax(0.0, (double)ma->friction[1] * mb->friction[1])) * friction_scale;
-        const double restitution = fmin(fmax(fmax(ma->response[0], mb->response[0]), 0.0), 1.0);
-        const double rthr = fmax(ma->response[1], mb->response[1]);
-        const double compliance = (double)ma->response[2] + mb->response[2];
-        const double dissipation = (double)ma->response[3] + mb->response[3];
-        const double rest = (double)sa->contact_rest_bound[1] + sb->contact_rest_bound[1];
-        for (int i = 0; i < counts[p]; ++i, ++c) {
-            Contact* ct = &C[c];
-            const OraclePoint* op = &slot->points[i];
-            const v3 pa = vadd(posA, qrot(rotA, vld(op->anchor_a)));
-            const v3 pb = vadd(posB, qrot(rotB, vld(op->anchor_b)));
-            ct->pair = p;
-            ct->point = (uint32_t)i;
-            ct->x = vmul(vadd(pa, pb), 0.5);
-            ct->sep = vdot(vsub(pb, pa), nw) - rest;
-            ct->n = nw; ct->t = tw; ct->bt = bw;
-            ct->new_impact = op->life == 0u;
-            ct->b_side = !ba->articulated;
-            ct->body = ct->b_side ? sb->body : sa->body;
-            for (int a = 0; a < 3; ++a) ct->lambda[a] = op->impulses[a];
-            /* Jacobian rows and relative velocity at v_free. */
-            double J[3 * MAXV];
-            point_jacobian_k(o, k, ct->body, ct->x, J);
-            const double sign = ct->b_side ? 1.0 : -1.0;
-            const v3 dirs[3] = {nw, tw, bw};
-            double rel[3] = {0, 0, 0};
-            for (int r = 0; r < 3; ++r)
-                for (uint32_t d = 0; d < nv; ++d) {
-                    const double g = sign * (vget(dirs[r], 0) * J[d] + vget(dirs[r], 1) * J[nv + d] + vget(dirs[r], 2) * J[2 * nv + d]);
-                    ct->G[r][d] = g;
-                    rel[r] += g * vf[d];
-                }
-            ct->target[0] = ct->sep > 0.0 ? -ct->sep / h : 0.0;
-            ct->target[1] = ct->target[2] = 0.0;
-            ct->reg[0] = fmax(compliance / (h * h) + dissipation / h, 0.0);
-            ct->reg[1] = ct->reg[2] = 0.0;
-            const double tau_c = 2.0 * h;
-            const double err = fmin(ct->sep + o->w.solver_scales[3], 0.0);
-            const double ratio = h / tau_c;
-            const double den = 1.0 + 2.0 * ratio + ratio * ratio;
-            double stab = -h * err / (tau_c * tau_c * den);
-            stab = fmin(fmax(stab, 0.0), o->w.solver_scales[2]);
-            if (ct->new_impact) {
-                const double incoming = rel[0] - ct->target[0];
-                if (incoming < -rthr) stab = fmax(stab, -restitution * incoming);
-            }
-            ct->target[0] += stab;
-            const double slip = sqrt(rel[1] * rel[1] + rel[2] * rel[2]);
-            ct->mu = slip <= 1.0e-3 ? mu_s : mu_d;
-        }
-    }
+    for (uint32_t p = 0; p < np; ++p)
+        for (int i = 0; i < counts[p]; ++i, ++c) prepare_contact(o, k, &slots[p], p, i, vf, friction_scale, &C[c]);
     trace->contact_count = total;
     if (total > trace->max_contacts) trace->max_contacts = total;
     trace->island_count = total > 0 ? 1u : 0u;
@@ -1213,6 +1232,76 @@ static uint32_t contact_substep(const OracleWorld* o, double* q, double* v, cons
     }
     for (uint32_t i = 0; i < o->w.nq; ++i)
         if (!isfinite(q[i])) { *fail_index = i; return MR_STEP_NONFINITE_RESULT; }
+    return MR_STEP_SUCCESS;
+}
+
+/* Collision and ConstraintIR evaluation of one articulated environment at
+ * configuration q with free velocity vf, for pinning against the reference's
+ * CPU path (collideCpuReference, Collision.cpp:2959; assembleContactConstraints,
+ * RigidBodyWorld.cpp:564; evaluateConstraintIR, ConstraintIR.cpp:1414).
+ * `manifolds` [pair_count] are read and updated like a substep's.  With
+ * speculative != 0 the shapes carry the substep's speculative margins, else
+ * none (the CPU reference has none).  Raw contacts: 16 doubles each (shape
+ * a, shape b, normal xyz, separation, point A xyz, point B xyz, feature A,
+ * feature B, 0, 0).  Contact rows: ORACLE_CONTACT_ROW doubles each (shape a,
+ * shape b, feature A, feature B, separation, normal xyz, point xyz, target
+ * velocity n/t/b, regularisation n/t/b, effective mu, relative velocity
+ * n/t/b at vf, new impact, speculative approach term -sep/h or 0).  Returns
+ * a step status code. */
+uint32_t oracle_articulated_contacts(const OracleWorld* o, const double* q, const double* vf, OracleManifold* manifolds,
+                                     double friction_scale, int speculative, double* raw_out, uint32_t raw_cap,
+                                     uint32_t* raw_count, double* rows_out, uint32_t rows_cap, uint32_t* row_count) {
+    const uint32_t np = o->w.pair_count;
+    g_band = 0;
+    g_margin = INFINITY;
+    *raw_count = 0;
+    *row_count = 0;
+    Kin k;
+    uint32_t status = kinematics(o, q, vf, &k);
+    if (status != MR_STEP_SUCCESS) return status;
+    double margins[MAXS];
+    if (speculative) speculative_margins(o, vf, margins);
+    else for (uint32_t s = 0; s < o->w.shape_count; ++s) margins[s] = 0.0;
+    int counts[MAXP];
+    for (uint32_t p = 0; p < np; ++p) {
+        int cand = 0, nraw = 0;
+        Raw raw[8];
+        counts[p] = pair_manifold(o, &k, margins, p, &manifolds[p], &cand, raw, &nraw);
+        if (counts[p] < 0) return MR_STEP_NONFINITE_RESULT;
+        for (int i = 0; i < nraw && *raw_count < raw_cap; ++i) {
+            double* r = raw_out + 16 * (*raw_count)++;
+            r[0] = o->pairs[p].shape_a;
+            r[1] = o->pairs[p].shape_b;
+            vst(r + 2, raw[i].normal);
+            r[5] = raw[i].sep;
+            vst(r + 6, raw[i].pa);
+            vst(r + 9, raw[i].pb);
+            r[12] = raw[i].fa;
+            r[13] = raw[i].fb;
+            r[14] = r[15] = 0.0;
+        }
+    }
+    for (uint32_t p = 0; p < np; ++p)
+        for (int i = 0; i < counts[p] && *row_count < rows_cap; ++i) {
+            Contact ct;
+            prepare_contact(o, &k, &manifolds[p], p, i, vf, friction_scale, &ct);
+            double* r = rows_out + ORACLE_CONTACT_ROW * (*row_count)++;
+            r[0] = o->pairs[p].shape_a;
+            r[1] = o->pairs[p].shape_b;
+            r[2] = manifolds[p].points[i].feature_a;
+            r[3] = manifolds[p].points[i].feature_b;
+            r[4] = ct.sep;
+            vst(r + 5, ct.n);
+            vst(r + 8, ct.x);
+            for (int a = 0; a < 3; ++a) {
+                r[11 + a] = ct.target[a];
+                r[14 + a] = ct.reg[a];
+                r[18 + a] = ct.rel[a];
+            }
+            r[17] = ct.mu;
+            r[21] = ct.new_impact;
+            r[22] = ct.sep > 0.0 ? -ct.sep / o->h : 0.0;
+        }
     return MR_STEP_SUCCESS;
 }
 
@@ -2935,6 +3024,7 @@ void oracle_scene_table_from_device(const float* words, uint32_t count, OracleSc
 uint32_t oracle_scene_step(const OracleScene* s, double* q, double* v, OracleSceneSlot* table, uint32_t* count, double friction,
                            OracleSceneTrace* trace) {
     memset(trace, 0, sizeof(*trace));
+    for (uint32_t b = 0; b < 64; ++b) trace->island_of[b] = 0xffffffffu;
     g_band = 0;
     g_band_width = kSceneBand;
     g_margin = INFINITY;
@@ -3124,13 +3214,25 @@ uint32_t oracle_scene_step(const OracleScene* s, double* q, double* v, OracleSce
                     if (x != y) parent[x > y ? x : y] = x < y ? x : y;
                 }
             }
-            uint32_t islands = 0;
+            uint32_t islands = 0, island_of_root[SNB];
             for (uint32_t b = 0; b < nb; ++b) {
                 int r = (int)b;
                 while (parent[r] != r) r = parent[r];
-                if (touched[b] && r == (int)b) ++islands;
+                island_of_root[b] = 0xffffffffu;
+                if (touched[b] && r == (int)b) island_of_root[b] = islands++;
             }
             if (islands > trace->islands) trace->islands = islands;
+            trace->island_contacts = total < 256 ? total : 256;
+            for (uint32_t i = 0; i < trace->island_contacts; ++i) {
+                trace->island_pairs[2 * i] = C[i].a;
+                trace->island_pairs[2 * i + 1] = C[i].b;
+            }
+            for (uint32_t b = 0; b < 64; ++b) trace->island_of[b] = 0xffffffffu;
+            for (uint32_t b = 0; b < nb && b < 64; ++b) {
+                int r = (int)b;
+                while (parent[r] != r) r = parent[r];
+                trace->island_of[b] = island_of_root[r];
+            }
         }
         /* Jacobi sweeps; sweep -1 applies the warm start. */
         const int iters = (int)s->iters + (final_substep ? (int)s->final_iters : 0);

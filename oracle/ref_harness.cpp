@@ -18,6 +18,9 @@
 #include "metalrobo/ArticulatedDynamics.hpp"
 #include "metalrobo/ArticulatedWorld.hpp"
 #include "metalrobo/Collision.hpp"
+#include "metalrobo/ConstraintIR.hpp"
+#include "metalrobo/ConstraintSolver.hpp"
+#include "metalrobo/RigidBodyWorld.hpp"
 #include "metalrobo/EngineModel.hpp"
 #include "metalrobo/ReferenceConicSolver.hpp"
 
@@ -61,6 +64,10 @@ struct RefModel {
     std::vector<std::uint32_t> action_dof;
     double h = 0.0;
     bool implicit = false;
+    // Record shape index -> collider index of the reference's combined
+    // shape list (articulated shapes first, then the environment's).
+    std::vector<std::uint32_t> collider_of_shape;
+    std::vector<std::uint32_t> shape_of_collider;
 };
 
 extern "C" {
@@ -202,6 +209,17 @@ __attribute__((visibility("default"))) RefModel* ref_model_create(
             }
         }
         m.world.shapeCount = static_cast<mr_u32>(m.shapes.size());
+        {
+            std::uint32_t art = 0, env = 0;
+            const std::uint32_t nart = static_cast<std::uint32_t>(m.shapes.size());
+            r->collider_of_shape.resize(world->shape_count);
+            r->shape_of_collider.resize(world->shape_count);
+            for (std::uint32_t s2 = 0; s2 < world->shape_count; ++s2) {
+                const std::uint32_t c = bodies[shapes[s2].body].articulated ? art++ : nart + env++;
+                r->collider_of_shape[s2] = c;
+                r->shape_of_collider[c] = s2;
+            }
+        }
         m.defaultQ.assign(world->nq, 0.0f);
         m.defaultV.assign(world->nv, 0.0f);
         if (world->root_type == MR_ROOT_FLOATING) m.defaultQ[6] = 1.0f;
@@ -428,6 +446,199 @@ __attribute__((visibility("default"))) double ref_run(RefModel* r, uint32_t envs
                                                       uint64_t* failed_steps) {
     std::vector<RefModel*> models(envs, r);
     return ref_run_envs(models.data(), envs, q, v, actions, steps, substeps, threads, solver, failed_steps);
+}
+
+// Persistent manifolds of one articulated environment across calls.
+struct RefContactCache {
+    PersistentManifoldCache manifolds;
+};
+
+__attribute__((visibility("default"))) RefContactCache* ref_contact_cache_create() { return new RefContactCache(); }
+__attribute__((visibility("default"))) void ref_contact_cache_destroy(RefContactCache* c) { delete c; }
+
+// The reference CPU world step's contact front end, up to the evaluated
+// ConstraintIR, at configuration q with free velocity vf
+// (ArticulatedWorld.cpp:573-800): link kinematics, projected body states,
+// collideCpuReference with the parent/child-link exclusions, contact
+// assembly, the v1 -> ConstraintIR adapter, world-point relative velocities
+// and evaluateConstraintIR.  The evaluation uses the substep h, the world's
+// slop and depenetration cap and no regularisation floor (the GPU world's
+// semantics; the CPU world step adds a 1e-6 floor for its Newton solver).
+// Raw contacts and manifolds as ref_scene_collide writes them, colliders
+// translated to record shape indices.  Contact rows (24 doubles): shape a,
+// shape b, feature A, feature B, separation, normal xyz, point xyz, target
+// velocity n/t/u, regularisation n/t/u, effective mu, relative velocity
+// n/t/u, new impact, pre-solve normal velocity.  Returns a status code.
+__attribute__((visibility("default"))) int ref_articulated_contacts(RefModel* r, RefContactCache* cache, const double* q,
+                                                                   const double* vf, std::uint32_t raw_cap, double* raw,
+                                                                   std::uint32_t* raw_count, std::uint32_t manifold_cap,
+                                                                   double* manifolds, std::uint32_t* manifold_count,
+                                                                   std::uint32_t row_cap, double* rows, std::uint32_t* row_count) {
+    *raw_count = *manifold_count = *row_count = 0;
+    const EngineModel& model = r->model;
+    const std::uint32_t nq = r->world.nq, nv = r->world.nv;
+    const MRArticulationGPU& art = model.articulations[0];
+    std::vector<ArticulatedBodyKinematics> bk(art.bodyCount);
+    auto kd = computeArticulatedBodyKinematics(model, 0, std::span<const double>(q, nq), std::span<const double>(vf, nv), bk,
+                                               dyn_config(r));
+    if (!kd.succeeded()) return MR_STEP_NONFINITE_INPUT;
+    std::vector<MRBodyStateGPU> states(model.bodies.size() + r->env_bodies.size());
+    for (const ArticulatedBodyKinematics& b : bk) {
+        const MRBodyPropertiesGPU& pr = model.bodies[b.bodyIndex];
+        MRBodyStateGPU st{};
+        st.position = f4(b.centerOfMassPosition[0], b.centerOfMassPosition[1], b.centerOfMassPosition[2], 1.0);
+        st.orientation = f4(b.orientation[0], b.orientation[1], b.orientation[2], b.orientation[3]);
+        st.linearVelocityAndInverseMass = f4(b.linearVelocity[0], b.linearVelocity[1], b.linearVelocity[2], pr.massAndInverseMass.y);
+        st.angularVelocity = f4(b.angularVelocity[0], b.angularVelocity[1], b.angularVelocity[2], 0.0);
+        st.flagsAndIndices[0] = MR_MOTION_DYNAMIC;
+        states[b.bodyIndex] = st;
+    }
+    std::copy(r->env_bodies.begin(), r->env_bodies.end(), states.begin() + model.bodies.size());
+    std::vector<MRShapeGPU> shapes = model.shapes;
+    for (MRShapeGPU sh : r->env_shapes) {
+        sh.bodyIndex += static_cast<std::uint32_t>(model.bodies.size());
+        shapes.push_back(sh);
+    }
+    std::vector<CollisionPairExclusion> exclusions;
+    for (std::uint32_t j = 0; j < art.jointCount; ++j) {
+        const MRJointDescriptorGPU& jd = model.joints[art.firstJoint + j];
+        for (std::uint32_t a = 0; a < model.shapes.size(); ++a) {
+            if (model.shapes[a].bodyIndex != jd.parentBody) continue;
+            for (std::uint32_t b = 0; b < model.shapes.size(); ++b)
+                if (model.shapes[b].bodyIndex == jd.childBody) exclusions.push_back({a, b});
+        }
+    }
+    CollisionConfig ccfg{};
+    ccfg.capacities = CollisionCapacities{4096u, 8192u, 2048u};
+    ccfg.manifoldBreakingSeparation = r->world.manifold_thresholds[0];
+    ccfg.manifoldBreakingTangential = r->world.manifold_thresholds[1];
+    ccfg.manifoldMergeDistance = r->world.manifold_thresholds[2];
+    ccfg.manifoldNormalCosine = r->world.manifold_thresholds[3];
+    const CollisionFrame f = collideCpuReference(shapes, states, ccfg, cache->manifolds, exclusions);
+    if (!f.succeeded()) return static_cast<int>(f.diagnostics.code);
+    auto shape_of = [&](std::uint32_t collider) -> double { return r->shape_of_collider[collider]; };
+    for (std::size_t i = 0; i < f.rawContacts.size() && i < raw_cap; ++i) {
+        const MRRawContactGPU& c = f.rawContacts[i];
+        const MRCandidatePairGPU& p = f.pairs[f.rawContactPairIndices[i]];
+        double* o = raw + 16 * i;
+        o[0] = shape_of(p.colliderA);
+        o[1] = shape_of(p.colliderB);
+        o[2] = c.normalAndSeparation.x;
+        o[3] = c.normalAndSeparation.y;
+        o[4] = c.normalAndSeparation.z;
+        o[5] = c.normalAndSeparation.w;
+        o[6] = c.pointAWorld.x;
+        o[7] = c.pointAWorld.y;
+        o[8] = c.pointAWorld.z;
+        o[9] = c.pointBWorld.x;
+        o[10] = c.pointBWorld.y;
+        o[11] = c.pointBWorld.z;
+        o[12] = c.featureAndFlags[0];
+        o[13] = c.featureAndFlags[1];
+        o[14] = o[15] = 0.0;
+        *raw_count = static_cast<std::uint32_t>(i + 1);
+    }
+    for (std::size_t m = 0; m < f.manifoldHeaders.size() && m < manifold_cap; ++m) {
+        const MRManifoldHeaderGPU& hd = f.manifoldHeaders[m];
+        double* o = manifolds + 58 * m;
+        o[0] = shape_of(hd.pairAndCount[1]);
+        o[1] = shape_of(hd.pairAndCount[2]);
+        o[2] = hd.pairAndCount[3];
+        o[3] = hd.normalAndAge.x;
+        o[4] = hd.normalAndAge.y;
+        o[5] = hd.normalAndAge.z;
+        o[6] = hd.normalAndAge.w;
+        o[7] = hd.tangentAndMetric.x;
+        o[8] = hd.tangentAndMetric.y;
+        o[9] = hd.tangentAndMetric.z;
+        for (int k = 0; k < 4; ++k) {
+            const MRManifoldPointGPU& pt = f.manifoldPoints[4 * m + k];
+            double* po = o + 10 + 12 * k;
+            po[0] = pt.localAnchorA.x;
+            po[1] = pt.localAnchorA.y;
+            po[2] = pt.localAnchorA.z;
+            po[3] = pt.localAnchorB.x;
+            po[4] = pt.localAnchorB.y;
+            po[5] = pt.localAnchorB.z;
+            po[6] = pt.impulses.x;
+            po[7] = pt.impulses.y;
+            po[8] = pt.impulses.z;
+            po[9] = pt.featureAndLife[0];
+            po[10] = pt.featureAndLife[1];
+            po[11] = pt.featureAndLife[2];
+        }
+        *manifold_count = static_cast<std::uint32_t>(m + 1);
+    }
+    ContactAssemblyResult assembly = assembleContactConstraints(f, shapes, model.materials, states, 4096u);
+    if (!assembly.diagnostics.succeeded()) return static_cast<int>(assembly.diagnostics.code);
+    if (assembly.constraints.empty()) return 0;
+    const ConstraintIRV1AdapterResult compiled = adaptV1ContactsToConstraintIR(assembly.constraints, ConstraintIRV1AdapterConfig{});
+    if (!compiled.succeeded()) return MR_STEP_NONFINITE_RESULT;
+    const ConstraintIRVelocityResult vel = computeConstraintIRWorldPointVelocities(compiled.ir, states);
+    if (!vel.succeeded()) return MR_STEP_NONFINITE_RESULT;
+    ConstraintIREvaluationConfig ecfg{};
+    ecfg.timestep = r->h;
+    ecfg.penetrationSlop = r->world.solver_scales[3];
+    ecfg.maximumDepenetrationVelocity = r->world.solver_scales[2];
+    ecfg.minimumRegularization = 0.0;
+    const ConstraintIREvaluationResult ev =
+        evaluateConstraintIR(compiled.ir, {vel.relativeVelocities, compiled.preSolveVelocities}, ecfg);
+    if (!ev.succeeded()) return MR_STEP_NONFINITE_RESULT;
+    for (std::size_t b = 0; b < ev.evaluated.blocks.size() && *row_count < row_cap; ++b) {
+        const ConstraintIRBlock& blk = ev.evaluated.blocks[b];
+        if (blk.type != MR_CONSTRAINT_CONTACT) continue;
+        const MRContactConstraintGPU& c = assembly.constraints[compiled.sourceConstraintIndices[b]];
+        double* o = rows + 24 * (*row_count)++;
+        o[0] = shape_of(static_cast<std::uint32_t>(c.pairKey >> 32u));
+        o[1] = shape_of(static_cast<std::uint32_t>(c.pairKey & 0xffffffffu));
+        o[2] = static_cast<double>(static_cast<std::uint32_t>(c.featureKey >> 32u));
+        o[3] = static_cast<double>(static_cast<std::uint32_t>(c.featureKey & 0xffffffffu));
+        o[4] = c.pointAndSeparation.w;
+        o[5] = c.normal.x;
+        o[6] = c.normal.y;
+        o[7] = c.normal.z;
+        o[8] = c.pointAndSeparation.x;
+        o[9] = c.pointAndSeparation.y;
+        o[10] = c.pointAndSeparation.z;
+        for (std::uint32_t k = 0; k < 3; ++k) {
+            const EvaluatedConstraintIRRow& row = ev.evaluated.rows[blk.rowOffset + k];
+            o[11 + k] = row.targetVelocity;
+            o[14 + k] = row.regularization;
+            o[18 + k] = row.relativeVelocity;
+        }
+        o[17] = ev.evaluated.cones[blk.coneIndex].effectiveFrictionU;
+        o[21] = (c.flags & MR_CONSTRAINT_FLAG_NEW_IMPACT) ? 1.0 : 0.0;
+        o[22] = c.targetVelocityAndPreSolveNormal.w;
+        o[23] = 0.0;
+    }
+    return 0;
+}
+
+// Island partition of a contact set by the reference (buildConstraintIslands,
+// ConstraintSolver.cpp:848): `dynamic[b]` != 0 marks dynamic bodies, contacts
+// are (bodyA, bodyB) pairs (MR_INVALID_INDEX-free).  Writes each body's
+// island index (MR_INVALID_INDEX: in no island) and returns the island count.
+__attribute__((visibility("default"))) std::uint32_t ref_build_islands(std::uint32_t bodies, const std::uint8_t* dynamic,
+                                                                      std::uint32_t contacts, const std::uint32_t* pairs,
+                                                                      std::uint32_t* body_island) {
+    std::vector<MRBodyStateGPU> states(bodies);
+    for (std::uint32_t b = 0; b < bodies; ++b) {
+        states[b] = MRBodyStateGPU{};
+        states[b].orientation = f4(0.0, 0.0, 0.0, 1.0);
+        states[b].linearVelocityAndInverseMass = f4(0.0, 0.0, 0.0, dynamic[b] ? 1.0 : 0.0);
+        states[b].flagsAndIndices[0] = dynamic[b] ? MR_MOTION_DYNAMIC : MR_MOTION_STATIC;
+    }
+    std::vector<MRContactConstraintGPU> cs(contacts);
+    for (std::uint32_t i = 0; i < contacts; ++i) {
+        cs[i] = MRContactConstraintGPU{};
+        cs[i].bodyA = pairs[2 * i];
+        cs[i].bodyB = pairs[2 * i + 1];
+    }
+    const std::vector<ConstraintIsland> islands = buildConstraintIslands(states, cs);
+    for (std::uint32_t b = 0; b < bodies; ++b) body_island[b] = MR_INVALID_INDEX;
+    for (std::size_t i = 0; i < islands.size(); ++i)
+        for (std::uint32_t b : islands[i].dynamicBodies) body_island[b] = static_cast<std::uint32_t>(i);
+    return static_cast<std::uint32_t>(islands.size());
 }
 
 }  // extern "C"
