@@ -628,6 +628,19 @@ MR_API uint32_t mr_task_rollout_environment_chains(const MRTaskRolloutHandle* ha
 MR_API int mr_task_rollout_copy_state(
     const MRTaskRolloutHandle* handle, float* q, float* v, MRManifoldC* manifolds);
 
+/* No counterpart in the reference (its islands, ConstraintSolver.cpp:848
+ * and MetalWorldContact.metal:4002, are internal): while enabled, every
+ * control step of a free-body (scene) world records the island partition
+ * of its final substep's contacts, per environment and body: the island
+ * index, islands numbered by ascending smallest body as
+ * buildConstraintIslands numbers them, or 0xff for a body in no island.
+ * Enabling allocates [env][64] bytes; only scene worlds accept it. */
+MR_API int mr_task_rollout_set_island_labels(MRTaskRolloutHandle* handle, uint32_t enabled);
+/* No counterpart in the reference: copies the labels of the last control
+ * step ([env][64] bytes; entries beyond the body count are undefined;
+ * meaningful for environments whose step succeeded). */
+MR_API int mr_task_rollout_copy_island_labels(const MRTaskRolloutHandle* handle, uint8_t* labels, size_t count);
+
 /* No counterpart in the reference: replaces the resident state (same
  * layouts as mr_task_rollout_copy_state; null manifolds clears them).
  * The new state also becomes every environment's reset state when

@@ -377,6 +377,10 @@ struct MRTaskRolloutHandle {
     DeviceBuffer<numi::SceneModel> d_smodel;
     DeviceBuffer<std::uint32_t> d_mcount;
     DeviceBuffer<float> d_workspace;    // scene substep tables, contacts, narrowphase scratch
+    // Scene worlds: island index per body on each control step's final
+    // substep ([env][kSceneMaxBodies]), written while enabled.
+    DeviceBuffer<std::uint8_t> d_island_labels;
+    bool island_labels = false;
     std::uint32_t precision = MR_PRECISION_FP32;  // MRPrecisionModeC
     int warps_per_block[numi::rt::kPrecisionModes] = {1, 1, 1};  // per precision mode
     int resident_warps_per_sm[numi::rt::kPrecisionModes] = {0, 0, 0};
@@ -534,6 +538,7 @@ struct MRTaskRolloutHandle {
                 p.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
                 p.q_comp = precision == MR_PRECISION_COMPENSATED ? d_qcomp.ptr : nullptr;
                 p.support_mapped = smodel.support_mapped;
+                p.island_labels = island_labels ? d_island_labels.ptr : nullptr;
                 check(numi::launch_scene_step(p, s), "scene step launch");
                 if (host_obs && obs) copy_observations(k, obs, host_obs, s);
             }
@@ -1362,6 +1367,36 @@ MR_API int mr_task_rollout_copy_state(const MRTaskRolloutHandle* handle, float* 
         if (manifolds && h.contact)
             check(cudaMemcpy(manifolds, h.d_manifolds.ptr, static_cast<size_t>(h.envs) * h.manifold_words() * sizeof(float),
                              cudaMemcpyDeviceToHost), "manifolds D2H");
+    });
+}
+
+MR_API int mr_task_rollout_set_island_labels(MRTaskRolloutHandle* handle, uint32_t enabled) {
+    return guarded([&] {
+        if (!handle) throw std::invalid_argument("handle is null");
+        MRTaskRolloutHandle& h = *handle;
+        if (!h.scene) throw std::invalid_argument("island labels are recorded for free-body (scene) worlds only");
+        const bool on = enabled != 0;
+        if (on == h.island_labels) return;
+        check(cudaStreamSynchronize(h.stream), "sync");
+        if (on) {
+            h.d_island_labels.resize(static_cast<size_t>(h.envs) * numi::kSceneMaxBodies);
+            check(cudaMemset(h.d_island_labels.ptr, 0xff, h.d_island_labels.count), "clear island labels");
+        }
+        h.island_labels = on;
+        drop_graphs(h);  // captured launches hold the previous setting
+    });
+}
+
+MR_API int mr_task_rollout_copy_island_labels(const MRTaskRolloutHandle* handle, uint8_t* labels, size_t count) {
+    return guarded([&] {
+        if (!handle || !labels) throw std::invalid_argument("handle and labels must be non-null");
+        const MRTaskRolloutHandle& h = *handle;
+        if (!h.island_labels) throw std::invalid_argument("island labels are not enabled (mr_task_rollout_set_island_labels)");
+        const size_t need = static_cast<size_t>(h.envs) * numi::kSceneMaxBodies;
+        if (count != need) throw std::invalid_argument("labels must hold environments x " + std::to_string(numi::kSceneMaxBodies) +
+                                                       " = " + std::to_string(need) + " entries");
+        check(cudaStreamSynchronize(h.stream), "sync");
+        check(cudaMemcpy(labels, h.d_island_labels.ptr, need, cudaMemcpyDeviceToHost), "island labels D2H");
     });
 }
 

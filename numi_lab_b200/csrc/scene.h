@@ -88,6 +88,10 @@ struct SceneParams {
     // leaves every buffer of the item untouched and reports
     // MR_STEP_UNSUPPORTED in its status code and kStatWorldMismatch.
     std::uint32_t world_tag;
+    // [slot][kSceneMaxBodies] island index of each body on the final
+    // substep, islands numbered by ascending root (smallest) body as
+    // buildConstraintIslands numbers them; 0xff: in no island.  Or null.
+    std::uint8_t* island_labels;
 };
 
 size_t scene_step_smem_bytes(bool compensated = false);

@@ -1859,9 +1859,18 @@ __global__ void __launch_bounds__(32, 16) scene_step_kernel(SceneParams p) {
                 }
             }
             int islands = 0;
-            for (int b = 0; b < nb; ++b)
-                if (((touched[b >> 5] >> (b & 31)) & 1u) && root(b) == b) ++islands;
+            std::uint8_t* labels = p.island_labels ? p.island_labels + static_cast<size_t>(env) * kSceneMaxBodies : nullptr;
+            for (int b = 0; b < nb; ++b) {
+                // A root precedes every member of its set, so its island
+                // index is known before any member asks for it.
+                const int r = root(b);
+                const bool island_root = ((touched[b >> 5] >> (b & 31)) & 1u) && r == b;
+                if (labels) labels[b] = island_root ? static_cast<std::uint8_t>(islands) : (r == b ? 0xffu : labels[r]);
+                if (island_root) ++islands;
+            }
             misc[kSmIslands] = af(max(ai(misc[kSmIslands]), islands));
+        } else if (lane == 0 && final_substep && p.island_labels) {
+            for (int b = 0; b < nb; ++b) p.island_labels[static_cast<size_t>(env) * kSceneMaxBodies + b] = 0xffu;
         }
         __syncwarp();
         // Jacobi sweeps (sweep -1 applies the warm start).

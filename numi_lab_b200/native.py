@@ -439,6 +439,8 @@ EXPORTED_SYMBOLS: Final = (
     "mr_server_stats",
     "mr_pile_step_no_alloc",
     "mr_pile_step_no_alloc_counters",
+    "mr_task_rollout_set_island_labels",
+    "mr_task_rollout_copy_island_labels",
     "mr_task_rollout_set_policy",
     "mr_task_rollout_environment_chains",
     "mr_task_rollout_policy_revision",
@@ -578,6 +580,10 @@ class Bindings:
         L.mr_pile_step_no_alloc.restype = ct.c_int
         L.mr_pile_step_no_alloc_counters.argtypes = [P(ct.c_uint32), ct.c_uint32, ct.c_uint64]
         L.mr_pile_step_no_alloc_counters.restype = ct.c_int
+        L.mr_task_rollout_set_island_labels.argtypes = [ct.c_void_p, ct.c_uint32]
+        L.mr_task_rollout_set_island_labels.restype = ct.c_int
+        L.mr_task_rollout_copy_island_labels.argtypes = [ct.c_void_p, P(ct.c_uint8), ct.c_size_t]
+        L.mr_task_rollout_copy_island_labels.restype = ct.c_int
 
     def last_error(self) -> str:
         value = self.lib.mr_last_error()

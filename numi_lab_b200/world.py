@@ -284,6 +284,20 @@ class World:
             "set_state",
         )
 
+    def set_island_labels(self, enabled: bool) -> None:
+        """Scene worlds: record each control step's island partition."""
+
+        self._lib.check(self._lib.lib.mr_task_rollout_set_island_labels(self._handle, 1 if enabled else 0), "set_island_labels")
+
+    def island_labels(self) -> np.ndarray:
+        """[env, bodies] island index of each body on the last control step's
+        final substep (255: in no island)."""
+
+        out = np.zeros((self.envs, 64), np.uint8)
+        self._lib.check(self._lib.lib.mr_task_rollout_copy_island_labels(
+            self._handle, out.ctypes.data_as(ct.POINTER(ct.c_uint8)), out.size), "copy_island_labels")
+        return out[:, : self.scene_bodies].copy()
+
     # -- stepping ----------------------------------------------------------
     def step(
         self,
