@@ -86,6 +86,16 @@ class OracleTrace(ct.Structure):
     ]
 
 
+def set_rounding_noise(seed: int) -> None:
+    """Test-only Monte Carlo rounding mode of the C restatement on this
+    thread: seed != 0 perturbs every FP32-rounded intermediate by a random
+    relative 2^-24 (one rounding to nearest); 0 is exact FP64."""
+
+    lib = ct.CDLL(str(ORACLE_LIB))
+    lib.oracle_set_rounding_noise.argtypes = [ct.c_uint64]
+    lib.oracle_set_rounding_noise(int(seed) & 0xFFFFFFFFFFFFFFFF)
+
+
 def build(reference: bool = True) -> None:
     """Compiles the checker libraries (the C restatement always; the
     reference core when its sources are present)."""

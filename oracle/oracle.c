@@ -35,6 +35,24 @@ static const double kSceneBand = 5.0e-5;
 static __thread uint32_t g_band;
 static __thread double g_band_width = 1.0e-5;
 static __thread double g_margin;  /* smallest |value - threshold| over the step's decisions */
+/* Rounding-noise mode (test infrastructure for per-step parity bounds):
+ * with a non-zero state, rn() multiplies a value by (1 + d), d uniform in
+ * [-2^-24, 2^-24], the relative error of one FP32 rounding to nearest --
+ * Monte Carlo arithmetic (Parker, 1997).  Applied to the intermediates an
+ * FP32 implementation rounds (body poses and twists, joint accelerations,
+ * contact Jacobians and response terms, impulse and velocity updates,
+ * integration), a few noisy runs estimate how far FP32 rounding alone can
+ * move this step's result.  Zero (the default) is exact FP64. */
+static __thread uint64_t g_noise;
+static double rn(double x) {
+    if (!g_noise) return x;
+    g_noise ^= g_noise << 13;
+    g_noise ^= g_noise >> 7;
+    g_noise ^= g_noise << 17;
+    const double u = (double)(g_noise >> 11) * (1.0 / 9007199254740992.0);
+    return x * (1.0 + (2.0 * u - 1.0) * 5.9604644775390625e-08);
+}
+void oracle_set_rounding_noise(uint64_t seed) { g_noise = seed ? (seed | 1u) : 0u; }
 #define BAND(value, threshold)                                                       \
     do {                                                                             \
         const double d_ = fabs((double)(value) - (double)(threshold));               \
@@ -78,6 +96,7 @@ static v3 vld(const double* p) { return V(p[0], p[1], p[2]); }
 static v3 vldf(const float* p) { return V(p[0], p[1], p[2]); }
 static void vst(double* p, v3 a) { p[0] = a.x; p[1] = a.y; p[2] = a.z; }
 static double vget(v3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
+static v3 rn3(v3 a) { return V(rn(a.x), rn(a.y), rn(a.z)); }
 
 static q4 Q(double x, double y, double z, double w) { q4 r = {x, y, z, w}; return r; }
 static q4 qconj(q4 q) { return Q(-q.x, -q.y, -q.z, q.w); }
@@ -280,6 +299,15 @@ static uint32_t kinematics(const OracleWorld* o, const double* q, const double* 
         k->ba[b] = (has && !prismatic) ? vmul(vcross(k->w[p], ja), qdj) : V(0, 0, 0);
         const v3 pc = prismatic ? vmul(vcross(k->w[p], ja), 2.0 * qdj) : V(0, 0, 0);
         k->bl[b] = vsub(vsub(vadd(vcross(k->w[p], vcross(k->w[p], ptj)), pc), vcross(k->ba[b], ca)), vcross(k->w[b], vcross(k->w[b], ca)));
+        if (g_noise) {
+            k->pos[b] = rn3(k->pos[b]);
+            k->r[b] = rn3(k->r[b]);
+            k->w[b] = rn3(k->w[b]);
+            k->v[b] = rn3(k->v[b]);
+            k->bl[b] = rn3(k->bl[b]);
+            k->ba[b] = rn3(k->ba[b]);
+            k->rot[b] = Q(rn(k->rot[b].x), rn(k->rot[b].y), rn(k->rot[b].z), rn(k->rot[b].w));
+        }
         if (!vfinite(k->pos[b]) || !vfinite(k->w[b]) || !vfinite(k->v[b]) || !vfinite(k->bl[b])) return MR_STEP_NONFINITE_RESULT;
     }
     return MR_STEP_SUCCESS;
@@ -446,8 +474,10 @@ static uint32_t aba_core(const OracleWorld* o, const double* q, const double* v,
         aa[b] = ang;
         al[b] = lin;
     }
-    for (uint32_t d = 0; d < o->w.nv; ++d)
+    for (uint32_t d = 0; d < o->w.nv; ++d) {
+        qdd[d] = rn(qdd[d]);
         if (!isfinite(qdd[d])) return MR_STEP_NONFINITE_RESULT;
+    }
     (void)q; (void)v;
     return MR_STEP_SUCCESS;
 }
@@ -1024,12 +1054,12 @@ static void prepare_contact(const OracleWorld* o, const Kin* k, const OracleMani
     const double dissipation = (double)ma->response[3] + mb->response[3];
     const double rest = (double)sa->contact_rest_bound[1] + sb->contact_rest_bound[1];
     const OraclePoint* op = &slot->points[i];
-    const v3 pa = vadd(posA, qrot(rotA, vld(op->anchor_a)));
-    const v3 pb = vadd(posB, qrot(rotB, vld(op->anchor_b)));
+    const v3 pa = rn3(vadd(posA, rn3(qrot(rotA, vld(op->anchor_a)))));
+    const v3 pb = rn3(vadd(posB, rn3(qrot(rotB, vld(op->anchor_b)))));
     ct->pair = p;
     ct->point = (uint32_t)i;
     ct->x = vmul(vadd(pa, pb), 0.5);
-    ct->sep = vdot(vsub(pb, pa), nw) - rest;
+    ct->sep = rn(vdot(vsub(pb, pa), nw) - rest);
     ct->n = nw; ct->t = tw; ct->bt = bw;
     ct->new_impact = op->life == 0u;
     ct->b_side = !ba->articulated;
@@ -1043,7 +1073,7 @@ static void prepare_contact(const OracleWorld* o, const Kin* k, const OracleMani
     for (int r = 0; r < 3; ++r) {
         ct->rel[r] = 0.0;
         for (uint32_t d = 0; d < nv; ++d) {
-            const double g = sign * (vget(dirs[r], 0) * J[d] + vget(dirs[r], 1) * J[nv + d] + vget(dirs[r], 2) * J[2 * nv + d]);
+            const double g = rn(sign * (vget(dirs[r], 0) * J[d] + vget(dirs[r], 1) * J[nv + d] + vget(dirs[r], 2) * J[2 * nv + d]));
             ct->G[r][d] = g;
             ct->rel[r] += g * vf[d];
         }
@@ -1125,6 +1155,7 @@ static uint32_t contact_substep(const OracleWorld* o, double* q, double* v, cons
             for (int r = 0; r < 3; ++r) {
                 for (uint32_t d = 0; d < nv; ++d) Rc[3 * i + r][d] = C[i].G[r][d];
                 chol_solve(Mm, nv, Rc[3 * i + r]);
+                for (uint32_t d = 0; d < nv; ++d) Rc[3 * i + r][d] = rn(Rc[3 * i + r][d]);
             }
         for (uint32_t i = 0; i < total; ++i) {
             Contact* ct = &C[i];
@@ -1133,9 +1164,10 @@ static uint32_t contact_substep(const OracleWorld* o, double* q, double* v, cons
                 for (int s = 0; s < 3; ++s) {
                     double acc = 0.0;
                     for (uint32_t d = 0; d < nv; ++d) acc += ct->G[r][d] * Rc[3 * i + s][d];
-                    W[r * 3 + s] = acc + (r == s ? ct->reg[r] : 0.0);
+                    W[r * 3 + s] = rn(acc + (r == s ? ct->reg[r] : 0.0));
                 }
             if (!oracle_invert3x3(W, ct->P)) { *fail_index = i; return MR_STEP_FACTORIZATION_FAILED; }
+            for (int e = 0; e < 9; ++e) ct->P[e] = rn(ct->P[e]);
             double rowsum = 0.0, diag = 0.0;
             for (uint32_t j = 0; j < total; ++j) {
                 double acc = 0.0;
@@ -1157,12 +1189,12 @@ static uint32_t contact_substep(const OracleWorld* o, double* q, double* v, cons
                     for (int r = 0; r < 3; ++r) {
                         u[r] = 0.0;
                         for (uint32_t d = 0; d < nv; ++d) u[r] += ct->G[r][d] * v[d];
-                        rhs[r] = ct->target[r] - u[r] - ct->reg[r] * ct->lambda[r];
+                        rhs[r] = rn(ct->target[r] - rn(u[r]) - ct->reg[r] * ct->lambda[r]);
                     }
                     for (int r = 0; r < 3; ++r) prop[r] = ct->lambda[r] + ct->P[r * 3] * rhs[0] + ct->P[r * 3 + 1] * rhs[1] + ct->P[r * 3 + 2] * rhs[2];
                     oracle_project_cone(prop, ct->mu, ct->mu, proj);
                     for (int r = 0; r < 3; ++r) {
-                        ct->delta[r] = ct->relax * (proj[r] - ct->lambda[r]);
+                        ct->delta[r] = rn(ct->relax * (proj[r] - ct->lambda[r]));
                     }
                     int finite = 1;
                     for (int r = 0; r < 3; ++r) finite &= isfinite(ct->lambda[r] + ct->delta[r]) && isfinite(ct->delta[r]);
@@ -1174,7 +1206,7 @@ static uint32_t contact_substep(const OracleWorld* o, double* q, double* v, cons
                 double acc = 0.0;
                 for (uint32_t i = 0; i < total; ++i)
                     for (int r = 0; r < 3; ++r) acc += Rc[3 * i + r][d] * C[i].delta[r];
-                v[d] += acc;
+                v[d] = rn(v[d] + acc);
             }
         }
         /* Diagnostics (MetalWorldContact.metal:7052-7110) and impulse write-back. */
@@ -1219,12 +1251,12 @@ static uint32_t contact_substep(const OracleWorld* o, double* q, double* v, cons
     /* Integration from the substep-start configuration. */
     for (uint32_t d = 0; d < nv; ++d) {
         const MRModelDofC* dof = &o->dofs[d];
-        if (dof->q_index != MR_INVALID_INDEX && !(o->floating && d < 6)) q[dof->q_index] += h * v[d];
+        if (dof->q_index != MR_INVALID_INDEX && !(o->floating && d < 6)) q[dof->q_index] = rn(q[dof->q_index] + h * v[d]);
     }
     if (o->floating) {
-        q[0] += h * v[0];
-        q[1] += h * v[1];
-        q[2] += h * v[2];
+        q[0] = rn(q[0] + h * v[0]);
+        q[1] = rn(q[1] + h * v[1]);
+        q[2] = rn(q[2] + h * v[2]);
         const q4 inc = so3_increment(V(h * v[3], h * v[4], h * v[5]), 0);
         q4 out;
         if (!qnormalize(qmul(inc, Q(q[3], q[4], q[5], q[6])), &out, 0)) { *fail_index = 3; return MR_STEP_NONFINITE_RESULT; }
@@ -1306,11 +1338,24 @@ uint32_t oracle_articulated_contacts(const OracleWorld* o, const double* q, cons
 }
 
 /* Free-motion commit (ArticulatedABA.metal:1446-1540). */
+/* The device latches a free-motion step as non-finite when its FP32
+ * arithmetic overflows.  The FP64 restatement takes the same decision when
+ * a joint acceleration, the squared velocity that drives the bias forces
+ * (their products reach |v|^2 x inertia) or the new velocity exceeds
+ * FLT_MAX; a magnitude within a factor 1e6 of FLT_MAX is a band decision
+ * (the device's intermediates may overflow a little earlier or later). */
+static int beyond_float(double x) {
+    const double a = fabs(x);
+    if (a > (double)FLT_MAX * 1.0e-6 && a < (double)FLT_MAX * 1.0e6) g_band++;
+    return !(a <= (double)FLT_MAX);
+}
+
 static uint32_t integrate_free(const OracleWorld* o, double* q, double* v, const double* qdd) {
     const uint32_t nv = o->w.nv;
     for (uint32_t d = 0; d < nv; ++d) {
-        const double nvel = v[d] + o->h * qdd[d];
-        if (!isfinite(nvel)) return MR_STEP_NONFINITE_RESULT;
+        const double nvel = rn(v[d] + o->h * qdd[d]);
+        const int over = beyond_float(qdd[d]) | beyond_float(v[d] * v[d]) | beyond_float(nvel);
+        if (!isfinite(nvel) || over) return MR_STEP_NONFINITE_RESULT;
         v[d] = nvel;
     }
     if (o->floating) {
@@ -1326,7 +1371,7 @@ static uint32_t integrate_free(const OracleWorld* o, double* q, double* v, const
         const int dof = o->body_dof[b];
         if (dof < 0) continue;
         const MRModelJointC* j = &o->joints[o->bodies[b].inbound_joint];
-        q[j->q_index] += o->h * v[dof];
+        q[j->q_index] = rn(q[j->q_index] + o->h * v[dof]);
     }
     for (uint32_t i = 0; i < o->w.nq; ++i)
         if (!isfinite(q[i])) return MR_STEP_NONFINITE_RESULT;
@@ -1367,7 +1412,7 @@ uint32_t oracle_control_step(const OracleWorld* o, double* q, double* v, OracleM
         if (status == MR_STEP_SUCCESS) {
             if (np > 0) {
                 for (uint32_t d = 0; d < nv; ++d) {
-                    vf[d] = v[d] + o->h * qdd[d];
+                    vf[d] = rn(v[d] + o->h * qdd[d]);
                     if (!isfinite(vf[d])) status = MR_STEP_NONFINITE_RESULT;
                 }
                 if (status == MR_STEP_SUCCESS)
@@ -1696,9 +1741,9 @@ typedef struct {
 
 static void sraw_add(SRaw* r, v3 pa, v3 pb, double sep, uint32_t fa, uint32_t fb) {
     if (r->n >= 8) return;
-    r->pa[r->n] = pa;
-    r->pb[r->n] = pb;
-    r->sep[r->n] = sep;
+    r->pa[r->n] = rn3(pa);
+    r->pb[r->n] = rn3(pb);
+    r->sep[r->n] = rn(sep);
     r->fa[r->n] = fa;
     r->fb[r->n] = fb;
     r->n++;
@@ -2872,8 +2917,8 @@ typedef struct {
 static void sprepare(const OracleScene* s, SState* st) {
     const double h = s->h;
     for (uint32_t b = 0; b < s->nb; ++b) {
-        st->lin[b] = vadd(vmul(st->lin[b], exp(-h * s->damp_lin[b])), vmul(V(s->gravity[0], s->gravity[1], s->gravity[2]), h));
-        st->ang[b] = vmul(st->ang[b], exp(-h * s->damp_ang[b]));
+        st->lin[b] = rn3(vadd(vmul(st->lin[b], exp(-h * s->damp_lin[b])), vmul(V(s->gravity[0], s->gravity[1], s->gravity[2]), h)));
+        st->ang[b] = rn3(vmul(st->ang[b], exp(-h * s->damp_ang[b])));
     }
 }
 
@@ -3115,14 +3160,14 @@ uint32_t oracle_scene_step(const OracleScene* s, double* q, double* v, OracleSce
             for (uint32_t i = 0; i < mf->count; ++i) {
                 const OraclePoint* op = &mf->points[i];
                 SCon* c = &C[total++];
-                const v3 pa = vadd(posA, qrot(rotA, vld(op->anchor_a)));
-                const v3 pb = vadd(posB, qrot(rotB, vld(op->anchor_b)));
+                const v3 pa = rn3(vadd(posA, rn3(qrot(rotA, vld(op->anchor_a)))));
+                const v3 pb = rn3(vadd(posB, rn3(qrot(rotB, vld(op->anchor_b)))));
                 const v3 pw = vmul(vadd(pa, pb), 0.5);
-                c->sep = vdot(vsub(pb, pa), nw) - rest;
+                c->sep = rn(vdot(vsub(pb, pa), nw) - rest);
                 c->a = (int)a;
                 c->b = plane_b ? -1 : (int)b;
-                c->ra = vsub(pw, posA);
-                c->rb = vsub(pw, posB);
+                c->ra = rn3(vsub(pw, posA));
+                c->rb = rn3(vsub(pw, posB));
                 c->n = nw;
                 c->t = tw;
                 c->bt = bw;
@@ -3143,8 +3188,8 @@ uint32_t oracle_scene_step(const OracleScene* s, double* q, double* v, OracleSce
         /* IR evaluation at the predicted velocities; blocks; relaxation. */
         for (uint32_t i = 0; i < total; ++i) {
             SCon* c = &C[i];
-            const v3 va = vadd(st->lin[c->a], vcross(st->ang[c->a], c->ra));
-            const v3 vb = c->b >= 0 ? vadd(st->lin[c->b], vcross(st->ang[c->b], c->rb)) : V(0, 0, 0);
+            const v3 va = rn3(vadd(st->lin[c->a], rn3(vcross(st->ang[c->a], c->ra))));
+            const v3 vb = c->b >= 0 ? rn3(vadd(st->lin[c->b], rn3(vcross(st->ang[c->b], c->rb)))) : V(0, 0, 0);
             const v3 dv = vsub(vb, va);
             const v3 dirs[3] = {c->n, c->t, c->bt};
             const double rel[3] = {vdot(dv, dirs[0]), vdot(dv, dirs[1]), vdot(dv, dirs[2])};
@@ -3157,7 +3202,7 @@ uint32_t oracle_scene_step(const OracleScene* s, double* q, double* v, OracleSce
                 if (c->restitution > 0.0) BAND(incoming, -c->rthr);
                 if (incoming < -c->rthr) stab = fmax(stab, -c->restitution * incoming);
             }
-            c->target[0] += stab;
+            c->target[0] = rn(c->target[0] + stab);
             const double slip = sqrt(rel[1] * rel[1] + rel[2] * rel[2]);
             if (c->mu_d != c->mu) BAND(slip, 1e-3);
             if (!(slip <= 1e-3)) c->mu = c->mu_d;
@@ -3169,7 +3214,7 @@ uint32_t oracle_scene_step(const OracleScene* s, double* q, double* v, OracleSce
                 for (int x = 0; x < 3; ++x)
                     for (int y = 0; y < 3; ++y) {
                         const v3 rx = vcross(r, dirs[x]), ry = vcross(r, dirs[y]);
-                        W[x * 3 + y] += s->inv_mass[body] * vdot(dirs[x], dirs[y]) + vdot(rx, sym3_apply(st->iiw[body], ry));
+                        W[x * 3 + y] = rn(W[x * 3 + y] + s->inv_mass[body] * vdot(dirs[x], dirs[y]) + vdot(rx, sym3_apply(st->iiw[body], ry)));
                     }
             }
             double rowsum = 0.0;
@@ -3191,7 +3236,9 @@ uint32_t oracle_scene_step(const OracleScene* s, double* q, double* v, OracleSce
             }
             const double diag = fabs(W[0]) + c->reg;
             W[0] += c->reg;
+            for (int e = 0; e < 9; ++e) W[e] = rn(W[e]);
             if (!oracle_invert3x3(W, c->P)) { status = MR_STEP_FACTORIZATION_FAILED; fail_index = i; break; }
+            for (int e = 0; e < 9; ++e) c->P[e] = rn(c->P[e]);
             c->relax = rowsum > fmax(diag, kMatrixFloor) ? fmin(fmax(diag / rowsum, 1.0 / 32.0), 1.0) : 1.0;
             double warm[3];
             oracle_project_cone(c->lambda, c->mu, c->mu, warm);
@@ -3240,16 +3287,16 @@ uint32_t oracle_scene_step(const OracleScene* s, double* q, double* v, OracleSce
             if (it >= 0) {
                 for (uint32_t i = 0; i < total; ++i) {
                     SCon* c = &C[i];
-                    const v3 va = vadd(st->lin[c->a], vcross(st->ang[c->a], c->ra));
-                    const v3 vb = c->b >= 0 ? vadd(st->lin[c->b], vcross(st->ang[c->b], c->rb)) : V(0, 0, 0);
+                    const v3 va = rn3(vadd(st->lin[c->a], rn3(vcross(st->ang[c->a], c->ra))));
+                    const v3 vb = c->b >= 0 ? rn3(vadd(st->lin[c->b], rn3(vcross(st->ang[c->b], c->rb)))) : V(0, 0, 0);
                     const v3 dv = vsub(vb, va);
-                    const double r0 = c->target[0] - vdot(dv, c->n) - c->reg * c->lambda[0];
-                    const double r1 = c->target[1] - vdot(dv, c->t);
-                    const double r2 = c->target[2] - vdot(dv, c->bt);
+                    const double r0 = rn(c->target[0] - vdot(dv, c->n) - c->reg * c->lambda[0]);
+                    const double r1 = rn(c->target[1] - vdot(dv, c->t));
+                    const double r2 = rn(c->target[2] - vdot(dv, c->bt));
                     double prop[3], proj[3];
                     for (int k = 0; k < 3; ++k) prop[k] = c->lambda[k] + c->P[3 * k] * r0 + c->P[3 * k + 1] * r1 + c->P[3 * k + 2] * r2;
                     oracle_project_cone(prop, c->mu, c->mu, proj);
-                    for (int k = 0; k < 3; ++k) c->delta[k] = c->relax * (proj[k] - c->lambda[k]);
+                    for (int k = 0; k < 3; ++k) c->delta[k] = rn(c->relax * (proj[k] - c->lambda[k]));
                     int finite = 1;
                     for (int k = 0; k < 3; ++k) finite &= isfinite(c->lambda[k] + c->delta[k]) && isfinite(c->delta[k]);
                     if (!finite) { status = MR_STEP_NONFINITE_RESULT; fail_index = i; break; }
@@ -3265,12 +3312,12 @@ uint32_t oracle_scene_step(const OracleScene* s, double* q, double* v, OracleSce
                         if ((side ? c->b : c->a) != (int)b) continue;
                         const v3 imp = vadd(vadd(vmul(c->n, c->delta[0]), vmul(c->t, c->delta[1])), vmul(c->bt, c->delta[2]));
                         const v3 f = side ? imp : vmul(imp, -1.0);
-                        dl = vadd(dl, f);
-                        dw = vadd(dw, vcross(side ? c->rb : c->ra, f));
+                        dl = rn3(vadd(dl, f));
+                        dw = rn3(vadd(dw, vcross(side ? c->rb : c->ra, f)));
                     }
                 }
-                st->lin[b] = vadd(st->lin[b], vmul(dl, s->inv_mass[b]));
-                st->ang[b] = vadd(st->ang[b], sym3_apply(st->iiw[b], dw));
+                st->lin[b] = rn3(vadd(st->lin[b], vmul(dl, s->inv_mass[b])));
+                st->ang[b] = rn3(vadd(st->ang[b], sym3_apply(st->iiw[b], dw)));
             }
         }
         if (status) break;
@@ -3281,12 +3328,12 @@ uint32_t oracle_scene_step(const OracleScene* s, double* q, double* v, OracleSce
             const double ls = vlen(lin), ws = vlen(ang);
             if (s->max_lin[b] > 0.0 && ls > s->max_lin[b]) lin = vmul(lin, s->max_lin[b] / ls);
             if (s->max_ang[b] > 0.0 && ws > s->max_ang[b]) ang = vmul(ang, s->max_ang[b] / ws);
-            const v3 c = vadd(st->pos[b], vmul(lin, h));
+            const v3 c = rn3(vadd(st->pos[b], vmul(lin, h)));
             q4 qn = qmul(so3_increment(vmul(ang, h), 0), st->rot[b]);
             const double qq = qdot(qn, qn);
             if (!qfinite(qn) || !(qq > 1e-12) || !vfinite(c)) { status = MR_STEP_NONFINITE_RESULT; fail_index = b; break; }
             const double inv = 1.0 / sqrt(qq);
-            st->rot[b] = Q(qn.x * inv, qn.y * inv, qn.z * inv, qn.w * inv);
+            st->rot[b] = Q(rn(qn.x * inv), rn(qn.y * inv), rn(qn.z * inv), rn(qn.w * inv));
             st->pos[b] = c;
             st->lin[b] = lin;
             st->ang[b] = ang;

@@ -6,11 +6,12 @@ oracle for 25 control steps, each from the device's FP32 state at the start
 of the step.
 
 Every env-step is held to the per-step bound of tests/_sensitivity.py:
-max(1e-5, K x the oracle's own FP32-input sensitivity) for q and qd and
-max(1e-4, K x sensitivity) for impulses.  Status codes and manifold feature
-ids / lifetimes must be identical, except on env-steps where the oracle
-took a decision within its band of a threshold or where rounding the inputs
-flips a decision in the oracle itself (band steps: counted, at most 5 %).
+max(1e-5, K x the spread of the oracle's Monte Carlo FP32-rounding runs)
+for q and qd and max(1e-4, K x that spread) for impulses.  Status codes and
+manifold feature ids / lifetimes must be identical.  Only on env-steps
+where the oracle took a decision within its band of a threshold, or where
+rounding flipped a decision in one of its noisy runs, may the device differ
+(band steps: counted, at most 5 %).
 The test reports the fraction of env-steps that meet the plain 1e-5 / 1e-4
 tolerances."""
 
@@ -68,18 +69,20 @@ def test_tree29_bench_configuration_per_step(cuda_device):
                 stats["env_steps"] += 1
                 assert int(st[e]) == res["status"] == 0, (k, e, int(st[e]), res["status"])
                 imp, feats = _gpu_impulses(m1, int(e), pairs)
-                if res["band"] or not np.isfinite(res["sens"]["v"]):
+                same = feats == res["features"]
+                dq, dv = S.rel_err(q1[e], res["q"]), S.rel_err(v1[e], res["v"])
+                di = (float(np.max(np.abs(imp - res["imp"]))) / max(1.0, float(np.max(np.abs(res["imp"]))))
+                      if same and imp.size else 0.0)
+                verdict, misses = S.judge(res, same, {"q": dq, "v": dv, "imp": di})
+                if verdict == "band":
                     stats["band"] += 1
                     continue
-                assert feats == res["features"], (k, e)
+                if verdict == "fail":
+                    failures.append((k, int(e), misses))
+                    continue
                 stats["contacts"] += res["contacts"]
-                dq, dv = S.rel_err(q1[e], res["q"]), S.rel_err(v1[e], res["v"])
-                di = float(np.max(np.abs(imp - res["imp"]))) / max(1.0, float(np.max(np.abs(res["imp"])))) if imp.size else 0.0
-                for name, err, base in (("q", dq, Q_TOL), ("v", dv, V_TOL), ("imp", di, IMP_TOL)):
-                    ok, bound = S.bounded(err, res["sens"][name], base)
-                    worst[name] = max(worst[name], err / bound)
-                    if not ok:
-                        failures.append((k, int(e), name, err, bound, res["sens"][name]))
+                for name, err in (("q", dq), ("v", dv), ("imp", di)):
+                    worst[name] = max(worst[name], err / S.bounded(err, res["sens"][name], S.BASES[name], res["k"])[1])
                 stats["plain_q"] += dq <= Q_TOL
                 stats["plain_v"] += dv <= V_TOL
                 if imp.size:
