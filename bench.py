@@ -338,8 +338,6 @@ def run_serving(args) -> None:
 
 PILE_SEED = 60            # a 36-body pile (the mean pile of the heterogeneous mix)
 PILE_BODIES = 36
-# Heterogeneous mix: pile worlds whose body counts span 8-64 (mean 36.4).
-MIX_PILE_SEEDS = (10, 13, 6, 9, 8, 1, 16, 31)
 
 
 def _pile_cpu_port_sample(records, q0: np.ndarray, v0: np.ndarray, friction: float, steps: int) -> dict:
@@ -539,58 +537,163 @@ def run_policy(args) -> None:
     print(json.dumps(line))
 
 
-def run_mix(args) -> None:
-    """Heterogeneous mix: 16,384 environments, 40 % 7-link chains (one 5 ms
-    step per control step), 30 % 29-DoF trees and 30 % piles of 8-64 bodies
-    (eight pile worlds), every world on its own stream."""
+MIX_TOTAL = 16384
+MIX_HORIZON = 25
+
+
+def _mix_worlds(total: int):
+    """The heterogeneous mix: 40 % 7-link chains (one 5 ms step per control
+    step), 30 % 29-DoF trees and 30 % piles whose body count is drawn per
+    environment from U{8..64} (boxes, spheres and capsules of size
+    U(0.05, 0.3) m, density 500-2000 kg/m^3); one world per distinct
+    configuration, as the reference compiles one topology per context."""
+
+    import numi_lab_b200 as nb
+
+    n_chain = int(0.4 * total)
+    n_tree = int(0.3 * total)
+    n_pile = total - n_chain - n_tree
+    counts = np.random.default_rng(SEED).integers(8, 65, size=n_pile)
+    per = {int(n): int((counts == n).sum()) for n in np.unique(counts)}
+    seeds = nb.world.pile_seeds_by_body_count(per)
+    worlds = [nb.World("chain7", n_chain, substeps=1, control_dt=0.005, seed=SEED),
+              nb.World("tree29", n_tree, substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT, seed=SEED)]
+    for n in sorted(per):
+        worlds.append(nb.World("pile", per[n], substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT, seed=seeds[n]))
+    return worlds, {"chain7": n_chain, "tree29": n_tree, "pile": n_pile, "pile_configs": len(per),
+                    "mean_pile_bodies": float(counts.mean())}
+
+
+def measure_mix(args, device) -> dict:
+    """Three arms over the same settled start state: the batch (one
+    persistent launch per control step over all worlds, autotuned, one
+    CUDA graph per horizon), plain per-config kernels (each world's own
+    launches, one world after another, as one context per topology would
+    run them) and per-world launches on concurrent streams."""
 
     import torch
 
     import numi_lab_b200 as nb
 
-    torch.cuda.set_device(0)
-    device = torch.device("cuda", 0)
-    total, horizon = 16384, 25
-    n_chain = int(0.4 * total)
-    n_tree = int(0.3 * total)
-    n_pile = total - n_chain - n_tree
-    worlds = [nb.World("chain7", n_chain, substeps=1, control_dt=0.005, seed=SEED),
-              nb.World("tree29", n_tree, substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT, seed=SEED)]
-    per = [n_pile // len(MIX_PILE_SEEDS) + (1 if i < n_pile % len(MIX_PILE_SEEDS) else 0) for i in range(len(MIX_PILE_SEEDS))]
-    for seed, n in zip(MIX_PILE_SEEDS, per):
-        worlds.append(nb.World("pile", n, substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT, seed=seed))
+    worlds, mix = _mix_worlds(MIX_TOTAL)
+    horizon = MIX_HORIZON
     try:
+        gen = torch.Generator(device=device).manual_seed(SEED)
+        acts = [0.3 * torch.randn((horizon, w.envs, w.action_count), device=device, generator=gen) if w.action_count else
+                torch.zeros((horizon, w.envs, 0), device=device) for w in worlds]
+        # Chains run episodes of one horizon: every chain resets on the
+        # first control step of an advance.
+        masks = [None] * len(worlds)
+        masks[0] = torch.zeros((horizon, worlds[0].envs), dtype=torch.int32, device=device)
+        masks[0][0] = 1
+        status = [torch.empty((horizon, w.envs), dtype=torch.int32, device=device) for w in worlds]
         for w in worlds[2:]:
-            w.step(torch.zeros((100, w.envs, 0), device=device), wait=True)  # settle piles
+            w.step(torch.zeros((100, w.envs, 0), device=device), wait=True)  # drop and settle the piles (2 s), untimed
+        start = [w.state() for w in worlds]
+        flush = torch.empty(256 * 1024 * 1024 // 4, device=device, dtype=torch.float32)
+        main = torch.cuda.current_stream(device)
+
+        def restore():
+            torch.cuda.synchronize(device)
+            for w, st in zip(worlds, start):
+                w.set_state(*st)
+
+        def timed(one_step) -> tuple[float, int]:
+            for _ in range(args.warmup):
+                one_step()
+            torch.cuda.synchronize(device)
+            ms = 0.0
+            failures = 0
+            for i in range(args.steps):
+                flush.fill_(float(i))
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(main)
+                one_step()
+                b.record(main)
+                torch.cuda.synchronize(device)
+                ms += a.elapsed_time(b)
+                failures += sum(int((st != 0).sum().item()) for st in status)
+            return ms / args.steps, failures
+
+        env_steps = MIX_TOTAL * horizon
+        # Batched: one launch per control step over every environment.
+        restore()
+        batch = nb.Batch(worlds)
+        try:
+            batch.tune([a[:5] for a in acts])
+            restore()
+            batch_ms, batch_fail = timed(lambda: batch.step(acts, masks, status))
+            shape = batch.launch_shape()
+        finally:
+            batch.close()
+        # Plain per-config kernels: each world's own advance, one after another.
+        restore()
+
+        def plain_step():
+            for w, a, m, st in zip(worlds, acts, masks, status):
+                w.step(a, reset_mask=m, status=st)
+
+        plain_ms, plain_fail = timed(plain_step)
+        # Per-world launches on concurrent streams.
+        restore()
         streams = [torch.cuda.Stream(device) for _ in worlds]
-        ms, failures, clock_summary = _timed_advances(worlds, args, horizon, device, streams, episodic=(0,))
-        bodies = [w.scene_bodies for w in worlds[2:]]
+
+        def concurrent_step():
+            for w, a, m, st, sm in zip(worlds, acts, masks, status, streams):
+                sm.wait_stream(main)
+                with torch.cuda.stream(sm):
+                    w.step(a, reset_mask=m, status=st)
+            for sm in streams:
+                main.wait_stream(sm)
+
+        conc_ms, conc_fail = timed(concurrent_step)
     finally:
         for w in worlds:
             w.close()
-    value = total * horizon * args.steps / (ms / 1e3)
+    return {
+        "value": env_steps / (batch_ms / 1e3),
+        "unit": UNIT,
+        "plain_per_config_value": env_steps / (plain_ms / 1e3),
+        "concurrent_streams_value": env_steps / (conc_ms / 1e3),
+        "mix_vs_plain": plain_ms / batch_ms,
+        "ms_per_step": {"batched": batch_ms, "plain_per_config": plain_ms, "concurrent_streams": conc_ms},
+        "config": {"workload": f"{MIX_TOTAL} envs: {mix['chain7']} chain7 (5 ms steps, actions N(0, 0.3), one-horizon episodes), "
+                               f"{mix['tree29']} tree29 (PD targets N(0, 0.3)), {mix['pile']} settled piles with body counts "
+                               f"drawn per env from U{{8..64}} (mean {mix['mean_pile_bodies']:.1f}; {mix['pile_configs']} configurations), "
+                               f"{horizon} control steps per bench step", "worlds": len(worlds),
+                   "l2": "flushed (256 MiB write) between steps"},
+        "batch_launch": shape,
+        "gpu_launches_per_step": {"batched": horizon, "plain_per_config": horizon * len(worlds)},
+        "failed_env_steps": {"batched": batch_fail, "plain_per_config": plain_fail, "concurrent_streams": conc_fail},
+    }
+
+
+def run_mix(args) -> None:
+    import torch
+
+    torch.cuda.set_device(0)
+    device = torch.device("cuda", 0)
+    with ClockSampler(0) as clocks:
+        r = measure_mix(args, device)
+    clock_summary = clocks.summary()
     line = {
         "metric": "heterogeneous env-steps/s",
-        "value": value,
+        "value": r["value"],
         "unit": UNIT,
         "n_gpus": 1,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": ms / args.steps,
+        "ms_per_step": r["ms_per_step"]["batched"],
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded)",
-        "config": {"workload": f"{total} envs: {n_chain} chain7 (5 ms steps, tau ~ N(0, 0.3), episodes of {horizon} steps), "
-                               f"{n_tree} tree29 (PD targets ~ N(0, 0.3)), "
-                               f"{n_pile} settled piles of {bodies} bodies (mean {float(np.mean(bodies)):.1f}); "
-                               f"{horizon} control steps per bench step; one stream per world",
-                   "l2": "flushed (256 MiB write) between steps"},
-        "gpu_launches": horizon * args.steps * len(worlds),
+        "config": r["config"],
+        "gpu_launches": MIX_HORIZON * args.steps,
         "clocks": {k: clock_summary[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
-        "failed_env_steps": sum(failures),
-        "failed_env_steps_by_world": dict(zip(["chain7", "tree29"] + [f"pile{b}" for b in bodies], failures)),
+        **{k: v for k, v in r.items() if k not in ("value", "unit", "config", "ms_per_step")},
+        "ms_per_step_by_arm": r["ms_per_step"],
     }
     print(json.dumps(line))
 

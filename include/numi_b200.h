@@ -719,6 +719,64 @@ MR_API int mr_server_release(MRServerHandle* server, uint64_t request_id);
 MR_API int mr_server_stats(const MRServerHandle* server, MRServerStatsC* stats);
 
 /* ---------------------------------------------------------------------- */
+/* Heterogeneous batch (no counterpart in the reference)                  */
+/* ---------------------------------------------------------------------- */
+/* The reference compiles one topology per context and dispatches each
+ * world on its own.  A batch groups existing rollouts -- any mix of
+ * articulated chains and trees and free-body piles of any body count, each
+ * with its own substeps and iterations -- and advances all their
+ * environments with ONE persistent launch per control step: resident warps
+ * claim (world, environment) items from a device queue in a claim order
+ * (longest item first, or round robin over the worlds), each item running
+ * its world's own device code.  A horizon of control steps is captured as
+ * one CUDA graph.  The rollouts keep owning their state; a batch stores
+ * pointers to them (destroy the batch before its rollouts).  Rollouts must
+ * be FP32, without a native policy and without support-mapped pairs. */
+typedef struct MRBatchHandle MRBatchHandle;
+
+enum MRBatchOrderC {
+    MR_BATCH_ORDER_LONGEST_FIRST = 0u,
+    MR_BATCH_ORDER_ROUND_ROBIN = 1u
+};
+
+typedef struct MRBatchLaunchShapeC {
+    uint32_t worlds;
+    uint32_t items;                  /* environments over all rollouts */
+    uint32_t warps_per_block;
+    uint32_t blocks;                 /* persistent grid: SMs x resident CTAs */
+    uint32_t resident_warps_per_sm;
+    uint32_t shared_bytes_per_warp;
+    uint32_t order;                  /* MRBatchOrderC */
+    uint32_t tuned;                  /* 1 after mr_batch_tune */
+    float tuned_step_milliseconds;   /* the tuner's best time of one control step */
+    uint32_t reserved[3];
+} MRBatchLaunchShapeC;
+
+/* No counterpart in the reference.  Null with mr_last_error on failure. */
+MR_API MRBatchHandle* mr_create_batch(MRTaskRolloutHandle* const* rollouts, size_t count);
+MR_API void mr_batch_destroy(MRBatchHandle* batch);
+/* No counterpart in the reference.  Advances every environment of every
+ * rollout by control_step_count steps.  Per rollout w (arrays of `count`
+ * device pointers, as in mr_create_batch): actions[w] [steps][envs][action
+ * count] (required when the world takes actions), reset_masks[w]
+ * [steps][envs] and status_codes[w] [steps][envs] (arrays or entries may
+ * be null).  Stream-ordered on cuda_stream; returns without waiting.  Each
+ * rollout's launch counters describe the advance. */
+MR_API int mr_batch_advance(MRBatchHandle* batch, uint32_t control_step_count, const float* const* actions,
+                            const uint32_t* const* reset_masks, uint32_t* const* status_codes, uint64_t cuda_stream);
+/* No counterpart in the reference.  Autotuner: measures each rollout's item
+ * latency (a launch of its environments alone), orders the queue by it,
+ * then times control_step_count steps of the whole batch for 1, 2 and 4
+ * warps per CTA under both claim orders and keeps the fastest.  Steps the
+ * rollouts with `actions` (as in mr_batch_advance) and restores their
+ * state afterwards; synchronous. */
+MR_API int mr_batch_tune(MRBatchHandle* batch, uint32_t control_step_count, const float* const* actions);
+MR_API int mr_batch_launch_shape(const MRBatchHandle* batch, MRBatchLaunchShapeC* out);
+/* Item latency per rollout (ms per control step of one environment), the
+ * key of the longest-first claim order. */
+MR_API int mr_batch_world_costs(const MRBatchHandle* batch, float* milliseconds, size_t count);
+
+/* ---------------------------------------------------------------------- */
 /* Stepping without device allocation (no counterpart in the reference)   */
 /* ---------------------------------------------------------------------- */
 

@@ -3,12 +3,13 @@
 The CUDA library ``libnumi_b200.so`` (built in-tree by ``numi_lab_b200.build``)
 implements the task-rollout C ABI of ``include/numi_b200.h``; this package is
 the thin Python layer over it: ``native`` (ctypes binding), ``world``
-(world / reset / step with zero-copy torch tensors) and ``serve``
+(world / reset / step with zero-copy torch tensors; ``Batch``, several
+worlds in one launch per control step) and ``serve``
 (continuous-batching request server).
 """
 
 from .native import MetalRoboError, bindings
 from .serve import Server
-from .world import World, compile_model, sample_reset
+from .world import Batch, World, compile_model, sample_reset
 
-__all__ = ["MetalRoboError", "Server", "World", "bindings", "compile_model", "sample_reset"]
+__all__ = ["Batch", "MetalRoboError", "Server", "World", "bindings", "compile_model", "sample_reset"]

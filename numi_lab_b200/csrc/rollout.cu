@@ -9,6 +9,7 @@
 // control-step launches (no contact-count readback inside a horizon).
 #include "device_model.h"
 #include "layout.h"
+#include "mix.h"
 #include "model.h"
 #include "numi_b200.h"
 #include "policy.h"
@@ -474,6 +475,58 @@ struct MRTaskRolloutHandle {
         if (ev_copies) cudaEventDestroy(ev_copies);
         if (copy_stream) cudaStreamDestroy(copy_stream);
         if (stream) cudaStreamDestroy(stream);
+    }
+
+    // This world's work at control step k of a heterogeneous batch: the
+    // parameters its own kernel would get (FP32, all environments, items
+    // indexed by slot).  actions [steps][env][action], masks [steps][env]
+    // and status [steps][env] are device buffers or null.
+    numi::MixWorld mix_world(std::uint32_t k, const float* actions, const std::uint32_t* masks, std::uint32_t* status) const {
+        numi::MixWorld w{};
+        w.envs = static_cast<std::int32_t>(envs);
+        const size_t item0 = static_cast<size_t>(k) * envs;
+        if (scene) {
+            w.kind = numi::kMixScene;
+            numi::SceneParams& p = w.scene;
+            p.model = d_smodel.ptr;
+            p.q = d_q.ptr;
+            p.v = d_v.ptr;
+            p.manifolds = d_manifolds.ptr;
+            p.manifold_count = d_mcount.ptr;
+            p.reset_q = d_reset_q.ptr;
+            p.reset_v = d_reset_v.ptr;
+            p.friction_scale = d_friction.ptr;
+            p.reset_masks = masks ? masks + item0 : nullptr;
+            p.status_codes = status ? status + item0 : nullptr;
+            p.stats = d_stats.ptr;
+            p.workspace = d_workspace.ptr;
+            p.env_count = static_cast<int>(envs);
+            p.substeps = static_cast<int>(config.physics_substeps);
+            p.velocity_iterations = static_cast<int>(config.velocity_iterations);
+            p.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
+            p.support_mapped = smodel.support_mapped;
+            p.island_labels = island_labels ? d_island_labels.ptr : nullptr;
+            return w;
+        }
+        w.kind = contact ? numi::kMixContact : numi::kMixFreeMotion;
+        w.layout = layout;
+        numi::StepParams& p = w.step;
+        p.model = d_model.ptr;
+        p.q = d_q.ptr;
+        p.v = d_v.ptr;
+        p.manifolds = d_manifolds.ptr;
+        p.reset_q = d_reset_q.ptr;
+        p.reset_v = d_reset_v.ptr;
+        p.friction_scale = d_friction.ptr;
+        p.actions = actions ? actions + item0 * model.world.action_count : nullptr;
+        p.reset_masks = masks ? masks + item0 : nullptr;
+        p.status_codes = status ? status + item0 : nullptr;
+        p.stats = d_stats.ptr;
+        p.env_count = static_cast<int>(envs);
+        p.substeps = static_cast<int>(config.physics_substeps);
+        p.velocity_iterations = static_cast<int>(config.velocity_iterations);
+        p.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
+        return w;
     }
 
     void sample_resets() {
@@ -1444,6 +1497,343 @@ MR_API int mr_task_rollout_set_state(MRTaskRolloutHandle* handle, const float* q
             check(cudaMemcpy(h.d_reset_q.ptr, q, nq * sizeof(float), cudaMemcpyHostToDevice), "reset q H2D");
             check(cudaMemcpy(h.d_reset_v.ptr, v, nv * sizeof(float), cudaMemcpyHostToDevice), "reset v H2D");
         }
+    });
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Heterogeneous batch: several rollouts advanced by one persistent launch per
+// control step (mix.h, mix_step.cu).
+// ---------------------------------------------------------------------------
+
+struct MRBatchHandle {
+    std::vector<MRTaskRolloutHandle*> worlds;
+    int device = 0;
+    int sms = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr, ev_a = nullptr, ev_b = nullptr;
+    int smem_floats_per_warp = 0;
+    int warps_per_block = 2;
+    int blocks_per_sm = 0;
+    std::uint32_t order = MR_BATCH_ORDER_LONGEST_FIRST;
+    bool tuned = false;
+    float tuned_step_ms = 0.0f;
+    std::vector<float> cost;            // per world: latency of one item (ms), the claim-order key
+    std::vector<std::uint32_t> items;   // claim order
+    DeviceBuffer<std::uint32_t> d_items;
+    DeviceBuffer<numi::MixWorld> d_worlds;  // [steps][worlds] of the cached advance
+    DeviceBuffer<unsigned> d_next;          // one queue counter per control step
+    PinnedBuffer<numi::MixWorld> h_worlds;
+    std::vector<numi::MixWorld> cached;     // descriptors behind d_worlds and the graph
+    cudaGraphExec_t graph = nullptr;
+    std::uint32_t graph_steps = 0;
+
+    ~MRBatchHandle() {
+        if (graph) cudaGraphExecDestroy(graph);
+        for (cudaEvent_t e : {ev_in, ev_out, ev_a, ev_b})
+            if (e) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    int grid() const { return std::max(1, blocks_per_sm) * sms; }
+    std::uint32_t item_count() const { return static_cast<std::uint32_t>(items.size()); }
+
+    void plan_launch() {
+        const size_t smem = static_cast<size_t>(smem_floats_per_warp) * sizeof(float) * warps_per_block;
+        check(numi::mix_occupancy(warps_per_block, smem, &blocks_per_sm), "batch occupancy");
+        if (blocks_per_sm < 1) throw std::runtime_error("the batch's per-warp shared memory does not fit one CTA on this device");
+    }
+
+    // Claim order: every item of every world, the longest first (cost,
+    // then world, then slot) or round robin over the worlds.
+    void order_items() {
+        items.clear();
+        std::vector<std::uint32_t> world_order(worlds.size());
+        for (std::uint32_t w = 0; w < worlds.size(); ++w) world_order[w] = w;
+        std::stable_sort(world_order.begin(), world_order.end(), [&](std::uint32_t a, std::uint32_t b) { return cost[a] > cost[b]; });
+        if (order == MR_BATCH_ORDER_LONGEST_FIRST) {
+            for (std::uint32_t w : world_order)
+                for (std::uint32_t e = 0; e < worlds[w]->envs; ++e) items.push_back((w << numi::kMixWorldShift) | e);
+        } else {
+            std::uint32_t most = 0;
+            for (auto* h : worlds) most = std::max(most, h->envs);
+            for (std::uint32_t e = 0; e < most; ++e)
+                for (std::uint32_t w : world_order)
+                    if (e < worlds[w]->envs) items.push_back((w << numi::kMixWorldShift) | e);
+        }
+        d_items.resize(items.size());
+        check(cudaMemcpy(d_items.ptr, items.data(), items.size() * sizeof(std::uint32_t), cudaMemcpyHostToDevice), "batch items H2D");
+    }
+
+    void drop_graph() {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        cached.clear();
+    }
+
+    // Enqueues `steps` control steps of `item_list` (device, `n` items) on
+    // `s` with descriptors already in d_worlds.
+    void enqueue(std::uint32_t steps, const std::uint32_t* item_list, int n, cudaStream_t s) {
+        check(cudaMemsetAsync(d_next.ptr, 0, steps * sizeof(unsigned), s), "batch queue reset");
+        for (std::uint32_t k = 0; k < steps; ++k)
+            check(numi::launch_mix_step(d_worlds.ptr + static_cast<size_t>(k) * worlds.size(), item_list, n, d_next.ptr + k,
+                                        warps_per_block, smem_floats_per_warp, grid(), s),
+                  "batch step launch");
+    }
+
+    void clear_stats(cudaStream_t s) {
+        for (auto* h : worlds) {
+            check(cudaMemsetAsync(h->d_stats.ptr, 0, numi::kStatCount * sizeof(std::uint32_t), s), "clear stats");
+            check(cudaMemsetAsync(h->d_stats.ptr + numi::kStatFirstFailEnv, 0xff, sizeof(std::uint32_t), s), "clear stats");
+        }
+    }
+
+    // Uploads the descriptors of an advance (when they differ from the
+    // cached ones, which also drops the captured graph).
+    void upload(std::uint32_t steps, const float* const* actions, const std::uint32_t* const* masks, std::uint32_t* const* status) {
+        std::vector<numi::MixWorld> desc(static_cast<size_t>(steps) * worlds.size());
+        for (std::uint32_t k = 0; k < steps; ++k)
+            for (size_t w = 0; w < worlds.size(); ++w)
+                desc[k * worlds.size() + w] = worlds[w]->mix_world(k, actions ? actions[w] : nullptr, masks ? masks[w] : nullptr,
+                                                                   status ? status[w] : nullptr);
+        if (desc.size() == cached.size() && std::memcmp(desc.data(), cached.data(), desc.size() * sizeof(numi::MixWorld)) == 0) return;
+        drop_graph();
+        d_worlds.resize(desc.size());
+        d_next.resize(std::max<size_t>(steps, 1));
+        h_worlds.resize(desc.size());
+        std::memcpy(h_worlds.ptr, desc.data(), desc.size() * sizeof(numi::MixWorld));
+        check(cudaMemcpyAsync(d_worlds.ptr, h_worlds.ptr, desc.size() * sizeof(numi::MixWorld), cudaMemcpyHostToDevice, stream),
+              "batch descriptors H2D");
+        check(cudaStreamSynchronize(stream), "batch descriptors H2D");
+        cached = std::move(desc);
+    }
+
+    void run(std::uint32_t steps, cudaStream_t caller) {
+        check(cudaEventRecord(ev_in, caller), "event");
+        check(cudaStreamWaitEvent(stream, ev_in, 0), "stream wait");
+        if (!graph || graph_steps != steps) {
+            if (graph) cudaGraphExecDestroy(graph);
+            graph = nullptr;
+            cudaGraph_t g = nullptr;
+            check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+            try {
+                clear_stats(stream);
+                enqueue(steps, d_items.ptr, static_cast<int>(items.size()), stream);
+            } catch (...) {
+                cudaStreamEndCapture(stream, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            check(cudaStreamEndCapture(stream, &g), "end capture");
+            cudaGraphExec_t exec = nullptr;
+            const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+            cudaGraphDestroy(g);
+            check(e, "graph instantiate");
+            graph = exec;
+            graph_steps = steps;
+        }
+        check(cudaGraphLaunch(graph, stream), "graph launch");
+        check(cudaEventRecord(ev_out, stream), "event");
+        check(cudaStreamWaitEvent(caller, ev_out, 0), "stream wait");
+    }
+
+    // Device state of every world (q, v, manifolds, manifold counts): the
+    // tuner steps the worlds and puts them back.
+    struct Snapshot {
+        std::vector<std::unique_ptr<DeviceBuffer<float>>> f;
+        std::vector<std::unique_ptr<DeviceBuffer<std::uint32_t>>> u;
+    };
+    static void copy_f(DeviceBuffer<float>& dst, const DeviceBuffer<float>& src, bool to_snapshot) {
+        if (!src.count) return;
+        if (to_snapshot) dst.resize(src.count);
+        check(cudaMemcpy(to_snapshot ? dst.ptr : src.ptr, to_snapshot ? src.ptr : dst.ptr, src.count * sizeof(float),
+                         cudaMemcpyDeviceToDevice), "batch snapshot");
+    }
+    void snapshot(Snapshot& snap, bool take) {
+        check(cudaStreamSynchronize(stream), "sync");
+        size_t fi = 0, ui = 0;
+        for (auto* h : worlds) {
+            for (DeviceBuffer<float>* b : {&h->d_q, &h->d_v, &h->d_manifolds}) {
+                if (take) snap.f.push_back(std::make_unique<DeviceBuffer<float>>());
+                copy_f(*snap.f[fi++], *b, take);
+            }
+            if (h->d_mcount.count) {
+                if (take) {
+                    snap.u.push_back(std::make_unique<DeviceBuffer<std::uint32_t>>());
+                    snap.u.back()->resize(h->d_mcount.count);
+                }
+                DeviceBuffer<std::uint32_t>& d = *snap.u[ui++];
+                check(cudaMemcpy(take ? d.ptr : h->d_mcount.ptr, take ? h->d_mcount.ptr : d.ptr,
+                                 h->d_mcount.count * sizeof(std::uint32_t), cudaMemcpyDeviceToDevice), "batch snapshot");
+            }
+        }
+    }
+
+    float time_steps(std::uint32_t steps, const std::uint32_t* item_list, int n, int repeats) {
+        float best = 1e30f;
+        for (int r = 0; r < repeats + 1; ++r) {
+            check(cudaEventRecord(ev_a, stream), "event");
+            enqueue(steps, item_list, n, stream);
+            check(cudaEventRecord(ev_b, stream), "event");
+            check(cudaEventSynchronize(ev_b), "sync");
+            float ms = 0.0f;
+            check(cudaEventElapsedTime(&ms, ev_a, ev_b), "elapsed");
+            if (r > 0) best = std::min(best, ms);  // the first run warms up
+        }
+        return best / static_cast<float>(steps);
+    }
+
+    // Autotuner: calibrates each world's item latency (one launch of that
+    // world's items alone), then times the whole batch for every
+    // (warps per CTA, claim order) candidate and keeps the fastest.  The
+    // worlds' state is put back afterwards.
+    void tune(std::uint32_t steps, const float* const* actions) {
+        Snapshot snap;
+        snapshot(snap, true);
+        upload(steps, actions, nullptr, nullptr);
+        // Per-world item latency at the default shape.
+        plan_launch();
+        for (size_t w = 0; w < worlds.size(); ++w) {
+            std::vector<std::uint32_t> own;
+            for (std::uint32_t e = 0; e < worlds[w]->envs; ++e) own.push_back((static_cast<std::uint32_t>(w) << numi::kMixWorldShift) | e);
+            DeviceBuffer<std::uint32_t> d_own;
+            d_own.resize(own.size());
+            check(cudaMemcpy(d_own.ptr, own.data(), own.size() * sizeof(std::uint32_t), cudaMemcpyHostToDevice), "tuner items");
+            const float ms = time_steps(1, d_own.ptr, static_cast<int>(own.size()), 2);
+            const double slots = static_cast<double>(grid()) * warps_per_block;
+            const double waves = std::ceil(static_cast<double>(own.size()) / slots);
+            cost[w] = static_cast<float>(ms / std::max(1.0, waves));
+        }
+        float best = 1e30f;
+        int best_wpb = warps_per_block;
+        std::uint32_t best_order = order;
+        for (const std::uint32_t ord : {std::uint32_t(MR_BATCH_ORDER_LONGEST_FIRST), std::uint32_t(MR_BATCH_ORDER_ROUND_ROBIN)})
+            for (const int wpb : {1, 2, 4}) {
+                warps_per_block = wpb;
+                order = ord;
+                try {
+                    plan_launch();
+                } catch (const std::exception&) {
+                    continue;
+                }
+                order_items();
+                const float ms = time_steps(steps, d_items.ptr, static_cast<int>(items.size()), 2);
+                if (ms < best) {
+                    best = ms;
+                    best_wpb = wpb;
+                    best_order = ord;
+                }
+            }
+        warps_per_block = best_wpb;
+        order = best_order;
+        plan_launch();
+        order_items();
+        tuned = true;
+        tuned_step_ms = best;
+        drop_graph();
+        snapshot(snap, false);
+    }
+};
+
+extern "C" {
+
+MR_API MRBatchHandle* mr_create_batch(MRTaskRolloutHandle* const* rollouts, size_t count) {
+    std::unique_ptr<MRBatchHandle> b;
+    const int rc = guarded([&] {
+        if (!rollouts || count == 0) throw std::invalid_argument("rollouts must hold at least one handle");
+        if (count > static_cast<size_t>(numi::kMixMaxWorlds))
+            throw std::invalid_argument("a batch holds at most " + std::to_string(numi::kMixMaxWorlds) + " rollouts");
+        b = std::make_unique<MRBatchHandle>();
+        check(cudaGetDevice(&b->device), "cudaGetDevice");
+        cudaDeviceProp prop{};
+        check(cudaGetDeviceProperties(&prop, b->device), "cudaGetDeviceProperties");
+        b->sms = prop.multiProcessorCount;
+        int floats = 0;
+        for (size_t i = 0; i < count; ++i) {
+            MRTaskRolloutHandle* h = rollouts[i];
+            if (!h) throw std::invalid_argument("rollout " + std::to_string(i) + " is null");
+            if (h->device != b->device) throw std::invalid_argument("every rollout of a batch must live on the current device");
+            if (h->precision != MR_PRECISION_FP32) throw std::invalid_argument("batched rollouts run in FP32 precision only");
+            if (h->policy) throw std::invalid_argument("batched rollouts take their actions from the caller (no native policy)");
+            if (h->scene && h->smodel.support_mapped)
+                throw std::invalid_argument("worlds with support-mapped (cylinder) pairs are not batched");
+            if (h->envs > numi::kMixEnvMask) throw std::invalid_argument("a batched rollout holds at most 2^24 - 1 environments");
+            for (size_t j = 0; j < i; ++j)
+                if (rollouts[j] == h) throw std::invalid_argument("a rollout appears twice in the batch");
+            floats = std::max(floats, h->scene ? numi::mix_scene_warp_floats() : numi::mix_articulated_warp_floats(h->layout));
+            b->worlds.push_back(h);
+            // First estimate of an item's latency (ms), replaced by the tuner.
+            const double bodies = h->scene ? h->smodel.nb : h->dmodel.nb;
+            b->cost.push_back(static_cast<float>(h->scene ? 0.02 * std::pow(bodies, 1.2) : (h->contact ? 0.4 : 0.02 * bodies)));
+        }
+        b->smem_floats_per_warp = (floats + 3) & ~3;
+        check(numi::configure_mix_kernel(static_cast<size_t>(b->smem_floats_per_warp) * sizeof(float) * 4 <
+                                                 static_cast<size_t>(prop.sharedMemPerBlockOptin)
+                                             ? static_cast<size_t>(b->smem_floats_per_warp) * sizeof(float) * 4
+                                             : static_cast<size_t>(prop.sharedMemPerBlockOptin)),
+              "batch kernel attributes");
+        check(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "stream");
+        for (cudaEvent_t* e : {&b->ev_in, &b->ev_out}) check(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "event");
+        for (cudaEvent_t* e : {&b->ev_a, &b->ev_b}) check(cudaEventCreate(e), "event");
+        b->plan_launch();
+        b->order_items();
+    });
+    return rc == 0 ? b.release() : nullptr;
+}
+
+MR_API void mr_batch_destroy(MRBatchHandle* batch) {
+    if (!batch) return;
+    cudaStreamSynchronize(batch->stream);
+    delete batch;
+}
+
+MR_API int mr_batch_advance(MRBatchHandle* batch, uint32_t control_step_count, const float* const* actions,
+                            const uint32_t* const* reset_masks, uint32_t* const* status_codes, uint64_t cuda_stream) {
+    return guarded([&] {
+        if (!batch) throw std::invalid_argument("batch is null");
+        if (control_step_count == 0) throw std::invalid_argument("control_step_count must be positive");
+        for (size_t w = 0; w < batch->worlds.size(); ++w)
+            if (batch->worlds[w]->model.world.action_count > 0 && (!actions || !actions[w]))
+                throw std::invalid_argument("rollout " + std::to_string(w) + " takes actions: actions[" + std::to_string(w) +
+                                            "] must be a device buffer [steps][envs][actions]");
+        batch->upload(control_step_count, actions, reset_masks, status_codes);
+        batch->run(control_step_count, reinterpret_cast<cudaStream_t>(cuda_stream));
+    });
+}
+
+MR_API int mr_batch_tune(MRBatchHandle* batch, uint32_t control_step_count, const float* const* actions) {
+    return guarded([&] {
+        if (!batch) throw std::invalid_argument("batch is null");
+        if (control_step_count == 0) throw std::invalid_argument("control_step_count must be positive");
+        for (size_t w = 0; w < batch->worlds.size(); ++w)
+            if (batch->worlds[w]->model.world.action_count > 0 && (!actions || !actions[w]))
+                throw std::invalid_argument("the tuner steps every rollout: actions[" + std::to_string(w) + "] is required");
+        batch->tune(control_step_count, actions);
+    });
+}
+
+MR_API int mr_batch_launch_shape(const MRBatchHandle* batch, MRBatchLaunchShapeC* out) {
+    return guarded([&] {
+        if (!batch || !out) throw std::invalid_argument("batch and out must be non-null");
+        *out = MRBatchLaunchShapeC{};
+        out->worlds = static_cast<uint32_t>(batch->worlds.size());
+        out->items = batch->item_count();
+        out->warps_per_block = static_cast<uint32_t>(batch->warps_per_block);
+        out->blocks = static_cast<uint32_t>(batch->grid());
+        out->resident_warps_per_sm = static_cast<uint32_t>(batch->blocks_per_sm * batch->warps_per_block);
+        out->shared_bytes_per_warp = static_cast<uint32_t>(batch->smem_floats_per_warp * sizeof(float));
+        out->order = batch->order;
+        out->tuned = batch->tuned ? 1u : 0u;
+        out->tuned_step_milliseconds = batch->tuned_step_ms;
+    });
+}
+
+MR_API int mr_batch_world_costs(const MRBatchHandle* batch, float* milliseconds, size_t count) {
+    return guarded([&] {
+        if (!batch || !milliseconds) throw std::invalid_argument("batch and milliseconds must be non-null");
+        if (count != batch->worlds.size()) throw std::invalid_argument("milliseconds must hold one entry per rollout of the batch");
+        for (size_t w = 0; w < count; ++w) milliseconds[w] = batch->cost[w];
     });
 }
 

