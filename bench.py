@@ -663,7 +663,9 @@ def measure_mix(args, device) -> dict:
                                f"{horizon} control steps per bench step", "worlds": len(worlds),
                    "l2": "flushed (256 MiB write) between steps"},
         "batch_launch": shape,
-        "gpu_launches_per_step": {"batched": horizon, "plain_per_config": horizon * len(worlds)},
+        # Batched: the queue reset plus one persistent launch per horizon (fused)
+        # or one per device-code family; plain: one launch per world and step.
+        "gpu_launches_per_step": {"batched": 1 if shape["mode"] == 0 else 2, "plain_per_config": horizon * len(worlds)},
         "failed_env_steps": {"batched": batch_fail, "plain_per_config": plain_fail, "concurrent_streams": conc_fail},
     }
 
@@ -690,7 +692,7 @@ def run_mix(args) -> None:
         "dtype": "f32",
         "data": "synthetic (seeded)",
         "config": r["config"],
-        "gpu_launches": MIX_HORIZON * args.steps,
+        "gpu_launches": r["gpu_launches_per_step"]["batched"] * args.steps,
         "clocks": {k: clock_summary[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
         **{k: v for k, v in r.items() if k not in ("value", "unit", "config", "ms_per_step")},
         "ms_per_step_by_arm": r["ms_per_step"],

@@ -725,11 +725,13 @@ MR_API int mr_server_stats(const MRServerHandle* server, MRServerStatsC* stats);
  * world on its own.  A batch groups existing rollouts -- any mix of
  * articulated chains and trees and free-body piles of any body count, each
  * with its own substeps and iterations -- and advances all their
- * environments with ONE persistent launch per control step: resident warps
- * claim (world, environment) items from a device queue in a claim order
- * (longest item first, or round robin over the worlds), each item running
- * its world's own device code.  A horizon of control steps is captured as
- * one CUDA graph.  The rollouts keep owning their state; a batch stores
+ * environments with ONE persistent launch per horizon of control steps
+ * (or one per device-code family, MRBatchLaunchModeC): resident warps claim
+ * (world, environment) items from a device queue in a claim order (longest
+ * item first, or round robin over the worlds) and run that environment's
+ * control steps back to back with its world's own device code;
+ * environments never wait for each other.  The queue reset and the launches
+ * are captured as one CUDA graph.  The rollouts keep owning their state; a batch stores
  * pointers to them (destroy the batch before its rollouts).  Rollouts must
  * be FP32, without a native policy and without support-mapped pairs. */
 typedef struct MRBatchHandle MRBatchHandle;
@@ -739,17 +741,28 @@ enum MRBatchOrderC {
     MR_BATCH_ORDER_ROUND_ROBIN = 1u
 };
 
+/* FUSED: one kernel runs every item (register budget of the most demanding
+ * world).  PER_FAMILY: one persistent launch per device-code family --
+ * articulated and free-body -- running concurrently, each at its own
+ * kernel's register budget and occupancy. */
+enum MRBatchLaunchModeC {
+    MR_BATCH_LAUNCH_FUSED = 0u,
+    MR_BATCH_LAUNCH_PER_FAMILY = 1u
+};
+
 typedef struct MRBatchLaunchShapeC {
     uint32_t worlds;
     uint32_t items;                  /* environments over all rollouts */
-    uint32_t warps_per_block;
+    uint32_t warps_per_block;        /* fused / articulated launch */
     uint32_t blocks;                 /* persistent grid: SMs x resident CTAs */
     uint32_t resident_warps_per_sm;
     uint32_t shared_bytes_per_warp;
     uint32_t order;                  /* MRBatchOrderC */
     uint32_t tuned;                  /* 1 after mr_batch_tune */
     float tuned_step_milliseconds;   /* the tuner's best time of one control step */
-    uint32_t reserved[3];
+    uint32_t mode;                   /* MRBatchLaunchModeC */
+    uint32_t scene_blocks;           /* PER_FAMILY: the free-body launch's grid (one warp per CTA) */
+    uint32_t scene_resident_warps_per_sm;
 } MRBatchLaunchShapeC;
 
 /* No counterpart in the reference.  Null with mr_last_error on failure. */
@@ -766,8 +779,9 @@ MR_API int mr_batch_advance(MRBatchHandle* batch, uint32_t control_step_count, c
                             const uint32_t* const* reset_masks, uint32_t* const* status_codes, uint64_t cuda_stream);
 /* No counterpart in the reference.  Autotuner: measures each rollout's item
  * latency (a launch of its environments alone), orders the queue by it,
- * then times control_step_count steps of the whole batch for 1, 2 and 4
- * warps per CTA under both claim orders and keeps the fastest.  Steps the
+ * then times control_step_count steps of the whole batch for both launch
+ * modes, 1, 2 and 4 warps per CTA and both claim orders and keeps the
+ * fastest.  Steps the
  * rollouts with `actions` (as in mr_batch_advance) and restores their
  * state afterwards; synchronous. */
 MR_API int mr_batch_tune(MRBatchHandle* batch, uint32_t control_step_count, const float* const* actions);

@@ -1,11 +1,13 @@
 // Heterogeneous batch: several worlds (articulated chains and trees, free-
 // body piles of any body count) advanced by ONE persistent launch per
-// control step.  Every resident warp repeatedly claims the next work item
-// from a device queue (an atomic counter over a claim-ordered item list)
-// and advances that environment of that world by one control step with the
-// world's own device code path, until the queue is empty.  The claim order
-// is the host's choice (longest items first by default), so the long-
-// running environments start first and short ones fill the tail.
+// horizon of control steps.  Every resident warp repeatedly claims the next
+// work item from a device queue (an atomic counter over a claim-ordered
+// item list) and advances that environment of that world through the
+// horizon with the world's own device code path, until the queue is empty.
+// Environments are independent, so no environment waits for another between
+// control steps.  The claim order is the host's choice (longest items first
+// by default), so the long-running environments start first and short
+// ones fill the tail.
 #pragma once
 
 #include <cstddef>
@@ -42,12 +44,19 @@ int mix_articulated_warp_floats(const WarpLayout& layout);
 // ... and for a free-body world.
 int mix_scene_warp_floats();
 
-cudaError_t configure_mix_kernel(size_t max_dynamic_smem);
-cudaError_t mix_occupancy(int warps_per_block, size_t smem_per_block, int* blocks_per_sm);
-// One control step of every item: `worlds` (device) holds this step's
-// descriptors, `items` (device) the claim order, `next_item` (device) a
-// counter that must be zero at launch.
-cudaError_t launch_mix_step(const MixWorld* worlds, const std::uint32_t* items, int item_count, unsigned* next_item,
-                            int warps_per_block, int smem_floats_per_warp, int grid, cudaStream_t stream);
+// Kernel families: the fused kernel runs every item; the per-family
+// kernels run one family's items at that family's own register budget.
+enum MixFamily : int { kMixFamilyFused = 0, kMixFamilyArticulated = 1, kMixFamilyScene = 2 };
+
+cudaError_t configure_mix_kernel(int family, size_t max_dynamic_smem);
+cudaError_t mix_occupancy(int family, int warps_per_block, size_t smem_per_block, int* blocks_per_sm);
+// `steps` control steps of every item: `worlds` (device) holds the
+// descriptors [steps][world_count], `items` (device) the claim order,
+// `next_item` (device) a counter that must be zero at launch.  A claimed
+// environment runs all its steps before the warp claims the next one.
+// The scene family runs one warp per CTA.
+cudaError_t launch_mix_horizon(int family, const MixWorld* worlds, int world_count, int steps, const std::uint32_t* items,
+                               int item_count, unsigned* next_item, int warps_per_block, int smem_floats_per_warp, int grid,
+                               cudaStream_t stream);
 
 }  // namespace numi

@@ -1511,19 +1511,23 @@ struct MRBatchHandle {
     std::vector<MRTaskRolloutHandle*> worlds;
     int device = 0;
     int sms = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev_in = nullptr, ev_out = nullptr, ev_a = nullptr, ev_b = nullptr;
-    int smem_floats_per_warp = 0;
-    int warps_per_block = 2;
-    int blocks_per_sm = 0;
+    cudaStream_t stream = nullptr, side = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr, ev_fork = nullptr, ev_join = nullptr, ev_a = nullptr, ev_b = nullptr;
+    // Shared memory per warp (floats) and resident CTAs per SM of each
+    // kernel family (numi::MixFamily: fused, articulated, scene).
+    int smem_floats[3] = {0, 0, 0};
+    int blocks_per_sm[3] = {0, 0, 0};
+    int warps_per_block = 2;            // fused and articulated kernels; the scene kernel runs one warp per CTA
+    std::uint32_t mode = MR_BATCH_LAUNCH_FUSED;
     std::uint32_t order = MR_BATCH_ORDER_LONGEST_FIRST;
     bool tuned = false;
     float tuned_step_ms = 0.0f;
     std::vector<float> cost;            // per world: latency of one item (ms), the claim-order key
-    std::vector<std::uint32_t> items;   // claim order
-    DeviceBuffer<std::uint32_t> d_items;
+    // Claim orders: every item (fused) and each family's items.
+    std::vector<std::uint32_t> items[3];
+    DeviceBuffer<std::uint32_t> d_items[3];
     DeviceBuffer<numi::MixWorld> d_worlds;  // [steps][worlds] of the cached advance
-    DeviceBuffer<unsigned> d_next;          // one queue counter per control step
+    DeviceBuffer<unsigned> d_next;          // one queue counter per family
     PinnedBuffer<numi::MixWorld> h_worlds;
     std::vector<numi::MixWorld> cached;     // descriptors behind d_worlds and the graph
     cudaGraphExec_t graph = nullptr;
@@ -1531,39 +1535,55 @@ struct MRBatchHandle {
 
     ~MRBatchHandle() {
         if (graph) cudaGraphExecDestroy(graph);
-        for (cudaEvent_t e : {ev_in, ev_out, ev_a, ev_b})
+        for (cudaEvent_t e : {ev_in, ev_out, ev_fork, ev_join, ev_a, ev_b})
             if (e) cudaEventDestroy(e);
-        if (stream) cudaStreamDestroy(stream);
+        for (cudaStream_t st : {stream, side})
+            if (st) cudaStreamDestroy(st);
     }
 
-    int grid() const { return std::max(1, blocks_per_sm) * sms; }
-    std::uint32_t item_count() const { return static_cast<std::uint32_t>(items.size()); }
+    int wpb(int family) const { return family == numi::kMixFamilyScene ? 1 : warps_per_block; }
+    int grid(int family) const { return std::max(1, blocks_per_sm[family]) * sms; }
+    std::uint32_t item_count() const { return static_cast<std::uint32_t>(items[numi::kMixFamilyFused].size()); }
+    bool is_scene(std::uint32_t w) const { return worlds[w]->scene; }
 
     void plan_launch() {
-        const size_t smem = static_cast<size_t>(smem_floats_per_warp) * sizeof(float) * warps_per_block;
-        check(numi::mix_occupancy(warps_per_block, smem, &blocks_per_sm), "batch occupancy");
-        if (blocks_per_sm < 1) throw std::runtime_error("the batch's per-warp shared memory does not fit one CTA on this device");
+        for (int f = 0; f < 3; ++f) {
+            blocks_per_sm[f] = 0;
+            if (!smem_floats[f]) continue;
+            const size_t smem = static_cast<size_t>(smem_floats[f]) * sizeof(float) * wpb(f);
+            check(numi::mix_occupancy(f, wpb(f), smem, &blocks_per_sm[f]), "batch occupancy");
+            if (blocks_per_sm[f] < 1) throw std::runtime_error("the batch's per-warp shared memory does not fit one CTA on this device");
+        }
     }
 
-    // Claim order: every item of every world, the longest first (cost,
-    // then world, then slot) or round robin over the worlds.
+    // Claim orders: the longest item first (cost, then world, then slot) or
+    // round robin over the worlds; the family lists keep the same order.
     void order_items() {
-        items.clear();
+        for (auto& l : items) l.clear();
         std::vector<std::uint32_t> world_order(worlds.size());
         for (std::uint32_t w = 0; w < worlds.size(); ++w) world_order[w] = w;
         std::stable_sort(world_order.begin(), world_order.end(), [&](std::uint32_t a, std::uint32_t b) { return cost[a] > cost[b]; });
+        auto push = [&](std::uint32_t w, std::uint32_t e) {
+            const std::uint32_t code = (w << numi::kMixWorldShift) | e;
+            items[numi::kMixFamilyFused].push_back(code);
+            items[is_scene(w) ? numi::kMixFamilyScene : numi::kMixFamilyArticulated].push_back(code);
+        };
         if (order == MR_BATCH_ORDER_LONGEST_FIRST) {
             for (std::uint32_t w : world_order)
-                for (std::uint32_t e = 0; e < worlds[w]->envs; ++e) items.push_back((w << numi::kMixWorldShift) | e);
+                for (std::uint32_t e = 0; e < worlds[w]->envs; ++e) push(w, e);
         } else {
             std::uint32_t most = 0;
             for (auto* h : worlds) most = std::max(most, h->envs);
             for (std::uint32_t e = 0; e < most; ++e)
                 for (std::uint32_t w : world_order)
-                    if (e < worlds[w]->envs) items.push_back((w << numi::kMixWorldShift) | e);
+                    if (e < worlds[w]->envs) push(w, e);
         }
-        d_items.resize(items.size());
-        check(cudaMemcpy(d_items.ptr, items.data(), items.size() * sizeof(std::uint32_t), cudaMemcpyHostToDevice), "batch items H2D");
+        for (int f = 0; f < 3; ++f) {
+            d_items[f].resize(items[f].size());
+            if (!items[f].empty())
+                check(cudaMemcpy(d_items[f].ptr, items[f].data(), items[f].size() * sizeof(std::uint32_t), cudaMemcpyHostToDevice),
+                      "batch items H2D");
+        }
     }
 
     void drop_graph() {
@@ -1572,14 +1592,33 @@ struct MRBatchHandle {
         cached.clear();
     }
 
-    // Enqueues `steps` control steps of `item_list` (device, `n` items) on
-    // `s` with descriptors already in d_worlds.
-    void enqueue(std::uint32_t steps, const std::uint32_t* item_list, int n, cudaStream_t s) {
-        check(cudaMemsetAsync(d_next.ptr, 0, steps * sizeof(unsigned), s), "batch queue reset");
-        for (std::uint32_t k = 0; k < steps; ++k)
-            check(numi::launch_mix_step(d_worlds.ptr + static_cast<size_t>(k) * worlds.size(), item_list, n, d_next.ptr + k,
-                                        warps_per_block, smem_floats_per_warp, grid(), s),
-                  "batch step launch");
+    void launch(int family, std::uint32_t steps, const std::uint32_t* item_list, int n, cudaStream_t s) {
+        check(numi::launch_mix_horizon(family, d_worlds.ptr, static_cast<int>(worlds.size()), static_cast<int>(steps), item_list, n,
+                                       d_next.ptr + family, wpb(family), smem_floats[family], grid(family), s),
+              "batch horizon launch");
+    }
+
+    // Enqueues `steps` control steps of every item on `s`: one fused launch,
+    // or one launch per family (the scene family on the side stream).
+    void enqueue(std::uint32_t steps, cudaStream_t s) {
+        check(cudaMemsetAsync(d_next.ptr, 0, 3 * sizeof(unsigned), s), "batch queue reset");
+        if (mode == MR_BATCH_LAUNCH_FUSED) {
+            launch(numi::kMixFamilyFused, steps, d_items[0].ptr, static_cast<int>(items[0].size()), s);
+            return;
+        }
+        const bool art = !items[numi::kMixFamilyArticulated].empty(), scn = !items[numi::kMixFamilyScene].empty();
+        if (art && scn) {
+            check(cudaEventRecord(ev_fork, s), "event");
+            check(cudaStreamWaitEvent(side, ev_fork, 0), "stream wait");
+        }
+        if (art)
+            launch(numi::kMixFamilyArticulated, steps, d_items[1].ptr, static_cast<int>(items[1].size()), s);
+        if (scn)
+            launch(numi::kMixFamilyScene, steps, d_items[2].ptr, static_cast<int>(items[2].size()), art ? side : s);
+        if (art && scn) {
+            check(cudaEventRecord(ev_join, side), "event");
+            check(cudaStreamWaitEvent(s, ev_join, 0), "stream wait");
+        }
     }
 
     void clear_stats(cudaStream_t s) {
@@ -1600,7 +1639,7 @@ struct MRBatchHandle {
         if (desc.size() == cached.size() && std::memcmp(desc.data(), cached.data(), desc.size() * sizeof(numi::MixWorld)) == 0) return;
         drop_graph();
         d_worlds.resize(desc.size());
-        d_next.resize(std::max<size_t>(steps, 1));
+        d_next.resize(3);
         h_worlds.resize(desc.size());
         std::memcpy(h_worlds.ptr, desc.data(), desc.size() * sizeof(numi::MixWorld));
         check(cudaMemcpyAsync(d_worlds.ptr, h_worlds.ptr, desc.size() * sizeof(numi::MixWorld), cudaMemcpyHostToDevice, stream),
@@ -1619,7 +1658,7 @@ struct MRBatchHandle {
             check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
             try {
                 clear_stats(stream);
-                enqueue(steps, d_items.ptr, static_cast<int>(items.size()), stream);
+                enqueue(steps, stream);
             } catch (...) {
                 cudaStreamEndCapture(stream, &g);
                 if (g) cudaGraphDestroy(g);
@@ -1644,19 +1683,19 @@ struct MRBatchHandle {
         std::vector<std::unique_ptr<DeviceBuffer<float>>> f;
         std::vector<std::unique_ptr<DeviceBuffer<std::uint32_t>>> u;
     };
-    static void copy_f(DeviceBuffer<float>& dst, const DeviceBuffer<float>& src, bool to_snapshot) {
-        if (!src.count) return;
-        if (to_snapshot) dst.resize(src.count);
-        check(cudaMemcpy(to_snapshot ? dst.ptr : src.ptr, to_snapshot ? src.ptr : dst.ptr, src.count * sizeof(float),
-                         cudaMemcpyDeviceToDevice), "batch snapshot");
-    }
     void snapshot(Snapshot& snap, bool take) {
         check(cudaStreamSynchronize(stream), "sync");
         size_t fi = 0, ui = 0;
         for (auto* h : worlds) {
             for (DeviceBuffer<float>* b : {&h->d_q, &h->d_v, &h->d_manifolds}) {
-                if (take) snap.f.push_back(std::make_unique<DeviceBuffer<float>>());
-                copy_f(*snap.f[fi++], *b, take);
+                if (take) {
+                    snap.f.push_back(std::make_unique<DeviceBuffer<float>>());
+                    if (b->count) snap.f.back()->resize(b->count);
+                }
+                DeviceBuffer<float>& d = *snap.f[fi++];
+                if (b->count)
+                    check(cudaMemcpy(take ? d.ptr : b->ptr, take ? b->ptr : d.ptr, b->count * sizeof(float), cudaMemcpyDeviceToDevice),
+                          "batch snapshot");
             }
             if (h->d_mcount.count) {
                 if (take) {
@@ -1670,63 +1709,71 @@ struct MRBatchHandle {
         }
     }
 
-    float time_steps(std::uint32_t steps, const std::uint32_t* item_list, int n, int repeats) {
+    template <typename F>
+    float best_ms(int repeats, F&& body) {
         float best = 1e30f;
         for (int r = 0; r < repeats + 1; ++r) {
             check(cudaEventRecord(ev_a, stream), "event");
-            enqueue(steps, item_list, n, stream);
+            body();
             check(cudaEventRecord(ev_b, stream), "event");
             check(cudaEventSynchronize(ev_b), "sync");
             float ms = 0.0f;
             check(cudaEventElapsedTime(&ms, ev_a, ev_b), "elapsed");
             if (r > 0) best = std::min(best, ms);  // the first run warms up
         }
-        return best / static_cast<float>(steps);
+        return best;
     }
 
-    // Autotuner: calibrates each world's item latency (one launch of that
-    // world's items alone), then times the whole batch for every
-    // (warps per CTA, claim order) candidate and keeps the fastest.  The
-    // worlds' state is put back afterwards.
+    // Autotuner: calibrates each world's item latency (its environments
+    // alone, one control step, in its family's kernel), orders the queues by
+    // it, then times the whole batch for every (launch mode, warps per CTA,
+    // claim order) candidate and keeps the fastest.  The worlds' state is
+    // put back afterwards.
     void tune(std::uint32_t steps, const float* const* actions) {
         Snapshot snap;
         snapshot(snap, true);
         upload(steps, actions, nullptr, nullptr);
-        // Per-world item latency at the default shape.
         plan_launch();
-        for (size_t w = 0; w < worlds.size(); ++w) {
+        for (std::uint32_t w = 0; w < worlds.size(); ++w) {
             std::vector<std::uint32_t> own;
-            for (std::uint32_t e = 0; e < worlds[w]->envs; ++e) own.push_back((static_cast<std::uint32_t>(w) << numi::kMixWorldShift) | e);
+            for (std::uint32_t e = 0; e < worlds[w]->envs; ++e) own.push_back((w << numi::kMixWorldShift) | e);
             DeviceBuffer<std::uint32_t> d_own;
             d_own.resize(own.size());
             check(cudaMemcpy(d_own.ptr, own.data(), own.size() * sizeof(std::uint32_t), cudaMemcpyHostToDevice), "tuner items");
-            const float ms = time_steps(1, d_own.ptr, static_cast<int>(own.size()), 2);
-            const double slots = static_cast<double>(grid()) * warps_per_block;
-            const double waves = std::ceil(static_cast<double>(own.size()) / slots);
-            cost[w] = static_cast<float>(ms / std::max(1.0, waves));
+            const int family = is_scene(w) ? numi::kMixFamilyScene : numi::kMixFamilyArticulated;
+            const float ms = best_ms(2, [&] {
+                check(cudaMemsetAsync(d_next.ptr, 0, 3 * sizeof(unsigned), stream), "batch queue reset");
+                launch(family, 1, d_own.ptr, static_cast<int>(own.size()), stream);
+            });
+            const double slots = static_cast<double>(grid(family)) * wpb(family);
+            cost[w] = static_cast<float>(ms / std::max(1.0, std::ceil(static_cast<double>(own.size()) / slots)));
         }
         float best = 1e30f;
         int best_wpb = warps_per_block;
-        std::uint32_t best_order = order;
-        for (const std::uint32_t ord : {std::uint32_t(MR_BATCH_ORDER_LONGEST_FIRST), std::uint32_t(MR_BATCH_ORDER_ROUND_ROBIN)})
-            for (const int wpb : {1, 2, 4}) {
-                warps_per_block = wpb;
-                order = ord;
-                try {
-                    plan_launch();
-                } catch (const std::exception&) {
-                    continue;
+        std::uint32_t best_order = order, best_mode = mode;
+        for (const std::uint32_t md : {std::uint32_t(MR_BATCH_LAUNCH_FUSED), std::uint32_t(MR_BATCH_LAUNCH_PER_FAMILY)})
+            for (const std::uint32_t ord : {std::uint32_t(MR_BATCH_ORDER_LONGEST_FIRST), std::uint32_t(MR_BATCH_ORDER_ROUND_ROBIN)})
+                for (const int wp : {1, 2, 4}) {
+                    mode = md;
+                    order = ord;
+                    warps_per_block = wp;
+                    try {
+                        plan_launch();
+                    } catch (const std::exception&) {
+                        continue;
+                    }
+                    order_items();
+                    const float ms = best_ms(2, [&] { enqueue(steps, stream); }) / static_cast<float>(steps);
+                    if (ms < best) {
+                        best = ms;
+                        best_wpb = wp;
+                        best_order = ord;
+                        best_mode = md;
+                    }
                 }
-                order_items();
-                const float ms = time_steps(steps, d_items.ptr, static_cast<int>(items.size()), 2);
-                if (ms < best) {
-                    best = ms;
-                    best_wpb = wpb;
-                    best_order = ord;
-                }
-            }
         warps_per_block = best_wpb;
         order = best_order;
+        mode = best_mode;
         plan_launch();
         order_items();
         tuned = true;
@@ -1749,7 +1796,7 @@ MR_API MRBatchHandle* mr_create_batch(MRTaskRolloutHandle* const* rollouts, size
         cudaDeviceProp prop{};
         check(cudaGetDeviceProperties(&prop, b->device), "cudaGetDeviceProperties");
         b->sms = prop.multiProcessorCount;
-        int floats = 0;
+        int floats_art = 0, floats_scene = 0;
         for (size_t i = 0; i < count; ++i) {
             MRTaskRolloutHandle* h = rollouts[i];
             if (!h) throw std::invalid_argument("rollout " + std::to_string(i) + " is null");
@@ -1761,20 +1808,25 @@ MR_API MRBatchHandle* mr_create_batch(MRTaskRolloutHandle* const* rollouts, size
             if (h->envs > numi::kMixEnvMask) throw std::invalid_argument("a batched rollout holds at most 2^24 - 1 environments");
             for (size_t j = 0; j < i; ++j)
                 if (rollouts[j] == h) throw std::invalid_argument("a rollout appears twice in the batch");
-            floats = std::max(floats, h->scene ? numi::mix_scene_warp_floats() : numi::mix_articulated_warp_floats(h->layout));
+            if (h->scene) floats_scene = numi::mix_scene_warp_floats();
+            else floats_art = std::max(floats_art, numi::mix_articulated_warp_floats(h->layout));
             b->worlds.push_back(h);
             // First estimate of an item's latency (ms), replaced by the tuner.
             const double bodies = h->scene ? h->smodel.nb : h->dmodel.nb;
             b->cost.push_back(static_cast<float>(h->scene ? 0.02 * std::pow(bodies, 1.2) : (h->contact ? 0.4 : 0.02 * bodies)));
         }
-        b->smem_floats_per_warp = (floats + 3) & ~3;
-        check(numi::configure_mix_kernel(static_cast<size_t>(b->smem_floats_per_warp) * sizeof(float) * 4 <
-                                                 static_cast<size_t>(prop.sharedMemPerBlockOptin)
-                                             ? static_cast<size_t>(b->smem_floats_per_warp) * sizeof(float) * 4
-                                             : static_cast<size_t>(prop.sharedMemPerBlockOptin)),
-              "batch kernel attributes");
-        check(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "stream");
-        for (cudaEvent_t* e : {&b->ev_in, &b->ev_out}) check(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "event");
+        auto round4 = [](int x) { return (x + 3) & ~3; };
+        b->smem_floats[numi::kMixFamilyArticulated] = floats_art ? round4(floats_art) : 0;
+        b->smem_floats[numi::kMixFamilyScene] = floats_scene ? round4(floats_scene) : 0;
+        b->smem_floats[numi::kMixFamilyFused] = round4(std::max(floats_art, floats_scene));
+        for (int f = 0; f < 3; ++f) {
+            if (!b->smem_floats[f]) continue;
+            const size_t bytes = std::min(static_cast<size_t>(b->smem_floats[f]) * sizeof(float) * 4,
+                                          static_cast<size_t>(prop.sharedMemPerBlockOptin));
+            check(numi::configure_mix_kernel(f, bytes), "batch kernel attributes");
+        }
+        for (cudaStream_t* st : {&b->stream, &b->side}) check(cudaStreamCreateWithFlags(st, cudaStreamNonBlocking), "stream");
+        for (cudaEvent_t* e : {&b->ev_in, &b->ev_out, &b->ev_fork, &b->ev_join}) check(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "event");
         for (cudaEvent_t* e : {&b->ev_a, &b->ev_b}) check(cudaEventCreate(e), "event");
         b->plan_launch();
         b->order_items();
@@ -1819,10 +1871,15 @@ MR_API int mr_batch_launch_shape(const MRBatchHandle* batch, MRBatchLaunchShapeC
         *out = MRBatchLaunchShapeC{};
         out->worlds = static_cast<uint32_t>(batch->worlds.size());
         out->items = batch->item_count();
+        const int main_family = batch->mode == MR_BATCH_LAUNCH_FUSED ? numi::kMixFamilyFused : numi::kMixFamilyArticulated;
         out->warps_per_block = static_cast<uint32_t>(batch->warps_per_block);
-        out->blocks = static_cast<uint32_t>(batch->grid());
-        out->resident_warps_per_sm = static_cast<uint32_t>(batch->blocks_per_sm * batch->warps_per_block);
-        out->shared_bytes_per_warp = static_cast<uint32_t>(batch->smem_floats_per_warp * sizeof(float));
+        out->blocks = static_cast<uint32_t>(batch->grid(main_family));
+        out->resident_warps_per_sm = static_cast<uint32_t>(batch->blocks_per_sm[main_family] * batch->warps_per_block);
+        out->shared_bytes_per_warp = static_cast<uint32_t>(batch->smem_floats[main_family] * sizeof(float));
+        out->scene_blocks = batch->mode == MR_BATCH_LAUNCH_PER_FAMILY ? static_cast<uint32_t>(batch->grid(numi::kMixFamilyScene)) : 0u;
+        out->scene_resident_warps_per_sm =
+            batch->mode == MR_BATCH_LAUNCH_PER_FAMILY ? static_cast<uint32_t>(batch->blocks_per_sm[numi::kMixFamilyScene]) : 0u;
+        out->mode = batch->mode;
         out->order = batch->order;
         out->tuned = batch->tuned ? 1u : 0u;
         out->tuned_step_milliseconds = batch->tuned_step_ms;

@@ -126,12 +126,16 @@ class BatchLaunchShapeC(ct.Structure):
         ("order", ct.c_uint32),
         ("tuned", ct.c_uint32),
         ("tuned_step_milliseconds", ct.c_float),
-        ("reserved", ct.c_uint32 * 3),
+        ("mode", ct.c_uint32),
+        ("scene_blocks", ct.c_uint32),
+        ("scene_resident_warps_per_sm", ct.c_uint32),
     ]
 
 
 MR_BATCH_ORDER_LONGEST_FIRST: Final = 0
 MR_BATCH_ORDER_ROUND_ROBIN: Final = 1
+MR_BATCH_LAUNCH_FUSED: Final = 0
+MR_BATCH_LAUNCH_PER_FAMILY: Final = 1
 
 
 class TaskRolloutLayoutC(ct.Structure):

@@ -553,9 +553,9 @@ class World:
 
 
 class Batch:
-    """Several worlds advanced together: one persistent launch per control
-    step over every environment of every world (mr_create_batch).  The
-    worlds keep their state; close the batch before them."""
+    """Several worlds advanced together: one persistent launch per horizon
+    over every environment of every world (mr_create_batch).  The worlds
+    keep their state; close the batch before them."""
 
     def __init__(self, worlds: Sequence["World"], *, library: native.Bindings | None = None) -> None:
         self._lib = library or native.bindings()
@@ -613,7 +613,7 @@ class Batch:
     def launch_shape(self) -> dict:
         out = native.BatchLaunchShapeC()
         self._lib.check(self._lib.lib.mr_batch_launch_shape(self._handle, ct.byref(out)), "mr_batch_launch_shape")
-        return {name: getattr(out, name) for name, _ in out._fields_ if name != "reserved"}
+        return {name: getattr(out, name) for name, _ in out._fields_}
 
     def world_costs(self) -> np.ndarray:
         out = np.zeros(len(self.worlds), np.float32)
