@@ -18,11 +18,18 @@ Lines printed (rank 0, one JSON line):
   * roofline of the control-step kernel against measured HBM bandwidth;
   * cpu_baseline: the reference's own FP64 CPU contact step
     (stepControlledArticulatedWorldCpu, compiled from its sources) timed on
-    this host's cores over a bounded sample of the same workload.
+    this host's cores over a bounded sample of the same workload;
+  * plain_aba_chain7: the plain-ABA chain configuration;
+  * heterogeneous_mix: 16,384 chains, trees and piles of 8-64 bodies as a
+    batch (one persistent launch per horizon) against plain per-config
+    kernels (mix_vs_plain) and per-world launches on concurrent streams;
+  * serving: Poisson request streams against the continuous-batching
+    server (p50 / p99 latency).
 
 ``--impl reference`` times only that CPU reference (rank 0; other ranks exit).
-Multi-GPU (torchrun): one process per GPU, each running its own 4096-env
-replica; no collective on the data path; value = total env-steps / max time.
+Multi-GPU (torchrun): one process per GPU; the job is world_size x 4096
+environments of one world, each rank stepping its contiguous range; no
+collective on the data path; value = total env-steps / max time.
 """
 
 from __future__ import annotations
@@ -299,10 +306,14 @@ def plain_aba_chain7(device) -> dict:
     }
 
 
-def run_serving(args) -> None:
-    """Poisson request stream (the serving configuration: chain, tree and
-    pile worlds) against the continuous-batching server; latency percentiles
-    at the configured rate plus a sustainable-rate sweep."""
+SERVE_RATES = ((2000.0, 1.0), (400.0, 2.0), (100.0, 2.0), (25.0, 2.0))
+
+
+def measure_serving(rates=SERVE_RATES) -> dict:
+    """Poisson request streams (the serving configuration: chain, tree and
+    pile worlds, envs log-uniform 1-512, horizons U(10, 500)) against the
+    continuous-batching server: served env-steps/s and request latency
+    percentiles per arrival rate (each window drained)."""
 
     import torch
 
@@ -311,28 +322,30 @@ def run_serving(args) -> None:
 
     torch.cuda.set_device(0)
     results = {}
-    for rate, window in ((2000.0, 1.0), (400.0, 2.0), (100.0, 2.0), (25.0, 2.0)):
+    for rate, window in rates:
         with nb.Server(hbm_budget_bytes=120 * 10**9, model_seed=SEED, max_envs_per_source=16384) as server:
             reqs = poisson_requests(rate, window, seed=SEED + int(rate))
             results[str(int(rate))] = serve_arrivals(server, reqs, drain=True, time_limit_s=300.0)
-    head = results["2000"]
-    line = {
-        "metric": "served env-steps/s and request latency (Poisson arrivals)",
+    head = results[str(int(rates[0][0]))]
+    return {
         "value": head["env_steps_per_s"],
         "unit": UNIT,
         "latency_p50_s": head["latency_p50_s"],
         "latency_p99_s": head["latency_p99_s"],
         "queue_p50_s": head["queue_p50_s"],
         "queue_p99_s": head["queue_p99_s"],
-        "higher_is_better": True,
-        "config": {"workload": "Poisson arrivals 2000 req/s for 1 s, worlds chain7 | tree29 | pile, envs log-uniform 1-512, "
-                               "horizon U(10, 500), actions N(0, 0.3), 120 GB HBM budget, drained",
+        "config": {"workload": f"Poisson arrivals {rates[0][0]:.0f} req/s for {rates[0][1]:.0f} s, worlds chain7 | tree29 | pile, "
+                               "envs log-uniform 1-512, horizon U(10, 500), actions N(0, 0.3), 120 GB HBM budget, drained",
                    "rate_sweep_req_per_s": {k: {kk: v[kk] for kk in ("env_steps_per_s", "latency_p50_s", "latency_p99_s",
                                                                        "queue_p99_s", "completed")}
                                             for k, v in results.items()}},
-        "data": "synthetic (seeded)",
-        "dtype": "f32",
     }
+
+
+def run_serving(args) -> None:
+    r = measure_serving()
+    line = {"metric": "served env-steps/s and request latency (Poisson arrivals)", **r, "higher_is_better": True,
+            "data": "synthetic (seeded)", "dtype": "f32"}
     print(json.dumps(line))
 
 
@@ -909,6 +922,8 @@ def main() -> None:
                         help="tree29 (the headline), pile (36-body piles), cylinder_pile (36-body piles with cylinders: "
                              "GJK / EPA pairs), mix (chains, trees and piles) or precision (box stacks and trees against the "
                              "FP64 oracle) or policy (tree29 closed loop under a native policy)")
+    parser.add_argument("--headline-only", action="store_true",
+                        help="the 29-DoF contact line without the mix and serving measurements")
     parser.add_argument("--serve", action="store_true",
                         help="serving workload: Poisson request stream, latency percentiles (one JSON line)")
     args = parser.parse_args()
@@ -1048,6 +1063,14 @@ def run_headline(args, rank: int, local_rank: int, world_size: int) -> None:
     launch_shape = world.launch_shape()
     world.close()
     plain = plain_aba_chain7(device) if rank == 0 else None
+    # The heterogeneous mix (batched vs plain per-config kernels) and the
+    # serving stream, on rank 0 (bounded: a few horizons, one arrival rate).
+    mix = serving = None
+    if rank == 0 and not args.headline_only:
+        mix_args = argparse.Namespace(steps=min(args.steps, 5), warmup=3)
+        mix = measure_mix(mix_args, device)
+        mix["steps"] = mix_args.steps
+        serving = measure_serving(SERVE_RATES[:1] + SERVE_RATES[2:3])
 
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
@@ -1097,6 +1120,8 @@ def run_headline(args, rank: int, local_rank: int, world_size: int) -> None:
             "mean_active_contacts": mean_points,
             "mean_manifolds": mean_manifolds,
             "plain_aba_chain7": plain,
+            "heterogeneous_mix": mix,
+            "serving": serving,
         }
         print(json.dumps(line))
     if dist is not None:
