@@ -23,7 +23,7 @@ BUILD_DIR = PACKAGE_DIR / "_build"
 
 SOURCES = ["model.cpp", "world_step.cu", "scene_step.cu", "mix_step.cu", "policy.cu", "rollout.cu", "serve.cu", "no_alloc.cu"]
 HEADERS = ["model.h", "device_model.h", "layout.h", "dmath.cuh", "runtime.h", "contact.cuh", "scene.h", "policy.h",
-           "world_step.cuh", "scene_step.cuh", "mix.h"]
+           "world_step.cuh", "scene_step.cuh", "mix.h", "audit.cuh"]
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -149,6 +149,7 @@ struct StepParams {
     std::int32_t final_velocity_iterations;
     float* q_comp;                 // [env][nq] compensation terms of q's running sums (compensated precision), or null
     std::int32_t env_base;         // slot index of this launch's slot 0 (counters report absolute slots)
+    double* audit;                 // [env][kAuditWords] FP64 energy / momentum audit (audit.cuh), or null
 };
 
 enum StatIndex : int {

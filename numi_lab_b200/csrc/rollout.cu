@@ -9,6 +9,7 @@
 // control-step launches (no contact-count readback inside a horizon).
 #include "device_model.h"
 #include "layout.h"
+#include "audit.cuh"
 #include "mix.h"
 #include "model.h"
 #include "numi_b200.h"
@@ -382,6 +383,9 @@ struct MRTaskRolloutHandle {
     // substep ([env][kSceneMaxBodies]), written while enabled.
     DeviceBuffer<std::uint8_t> d_island_labels;
     bool island_labels = false;
+    // FP64 energy / momentum audit records ([env][kAuditWords]) while enabled.
+    DeviceBuffer<double> d_audit;
+    bool audit = false;
     std::uint32_t precision = MR_PRECISION_FP32;  // MRPrecisionModeC
     int warps_per_block[numi::rt::kPrecisionModes] = {1, 1, 1};  // per precision mode
     int resident_warps_per_sm[numi::rt::kPrecisionModes] = {0, 0, 0};
@@ -506,6 +510,7 @@ struct MRTaskRolloutHandle {
             p.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
             p.support_mapped = smodel.support_mapped;
             p.island_labels = island_labels ? d_island_labels.ptr : nullptr;
+            p.audit = audit ? d_audit.ptr : nullptr;
             return w;
         }
         w.kind = contact ? numi::kMixContact : numi::kMixFreeMotion;
@@ -526,6 +531,7 @@ struct MRTaskRolloutHandle {
         p.substeps = static_cast<int>(config.physics_substeps);
         p.velocity_iterations = static_cast<int>(config.velocity_iterations);
         p.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
+        p.audit = audit ? d_audit.ptr : nullptr;
         return w;
     }
 
@@ -548,9 +554,10 @@ struct MRTaskRolloutHandle {
     }
 
     // The compensation terms belong to the state they were accumulated on:
-    // any new state starts without them.
+    // any new state starts without them; the audit takes a new reference.
     void clear_compensation() {
         if (d_qcomp.count) check(cudaMemsetAsync(d_qcomp.ptr, 0, d_qcomp.count * sizeof(float), stream), "clear compensation");
+        if (audit) check(cudaMemsetAsync(d_audit.ptr, 0, d_audit.count * sizeof(double), stream), "clear audit");
     }
 
     size_t manifold_words() const {
@@ -592,6 +599,7 @@ struct MRTaskRolloutHandle {
                 p.q_comp = precision == MR_PRECISION_COMPENSATED ? d_qcomp.ptr : nullptr;
                 p.support_mapped = smodel.support_mapped;
                 p.island_labels = island_labels ? d_island_labels.ptr : nullptr;
+                p.audit = audit ? d_audit.ptr : nullptr;
                 check(numi::launch_scene_step(p, s), "scene step launch");
                 if (host_obs && obs) copy_observations(k, obs, host_obs, s);
             }
@@ -635,6 +643,7 @@ struct MRTaskRolloutHandle {
                 p.velocity_iterations = static_cast<int>(config.velocity_iterations);
                 p.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
                 p.q_comp = precision == MR_PRECISION_COMPENSATED ? d_qcomp.ptr + static_cast<size_t>(o) * model.world.nq : nullptr;
+                p.audit = audit ? d_audit.ptr + static_cast<size_t>(o) * numi::kAuditWords : nullptr;
                 check(numi::launch_control_step(p, precision == MR_PRECISION_COMPENSATED ? layout_comp : layout, contact, precision,
                                                 warps_per_block[precision], cs),
                       "control step launch");
@@ -1420,6 +1429,33 @@ MR_API int mr_task_rollout_copy_state(const MRTaskRolloutHandle* handle, float* 
         if (manifolds && h.contact)
             check(cudaMemcpy(manifolds, h.d_manifolds.ptr, static_cast<size_t>(h.envs) * h.manifold_words() * sizeof(float),
                              cudaMemcpyDeviceToHost), "manifolds D2H");
+    });
+}
+
+MR_API int mr_task_rollout_set_audit(MRTaskRolloutHandle* handle, uint32_t enabled) {
+    return guarded([&] {
+        if (!handle) throw std::invalid_argument("handle is null");
+        MRTaskRolloutHandle& h = *handle;
+        const bool on = enabled != 0;
+        check(cudaStreamSynchronize(h.stream), "sync");
+        if (on) {
+            h.d_audit.resize(static_cast<size_t>(h.envs) * numi::kAuditWords);
+            check(cudaMemset(h.d_audit.ptr, 0, h.d_audit.count * sizeof(double)), "clear audit");
+        }
+        if (on != h.audit) drop_graphs(h);  // captured launches hold the previous setting
+        h.audit = on;
+    });
+}
+
+MR_API int mr_task_rollout_copy_audit(const MRTaskRolloutHandle* handle, double* records, size_t count) {
+    return guarded([&] {
+        if (!handle || !records) throw std::invalid_argument("handle and records must be non-null");
+        const MRTaskRolloutHandle& h = *handle;
+        if (!h.audit) throw std::invalid_argument("the audit is not enabled (mr_task_rollout_set_audit)");
+        const size_t need = static_cast<size_t>(h.envs) * numi::kAuditWords;
+        if (count != need) throw std::invalid_argument("records must hold environments x 12 = " + std::to_string(need) + " doubles");
+        check(cudaStreamSynchronize(h.stream), "sync");
+        check(cudaMemcpy(records, h.d_audit.ptr, need * sizeof(double), cudaMemcpyDeviceToHost), "audit D2H");
     });
 }
 

@@ -92,6 +92,7 @@ struct SceneParams {
     // substep, islands numbered by ascending root (smallest) body as
     // buildConstraintIslands numbers them; 0xff: in no island.  Or null.
     std::uint8_t* island_labels;
+    double* audit;             // [slot][kAuditWords] FP64 energy / momentum audit (audit.cuh), or null
 };
 
 size_t scene_step_smem_bytes(bool compensated = false);

@@ -32,6 +32,7 @@
 #include "device_model.h"
 #include "dmath.cuh"
 #include "layout.h"
+#include "audit.cuh"
 #include "contact.cuh"
 
 #include <cfloat>
@@ -1854,6 +1855,22 @@ __device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState<R>
     return warp_ok(misc);
 }
 
+// FP64 audit of the committed state (audit.cuh): forward kinematics of the
+// committed q and v, then each lane's body.  Kept out of line so that the
+// control step's register allocation does not carry it.
+template <typename R>
+__device__ __noinline__ void audit_articulated(const Warp& w, const BodyConst& bc, double* rec, bool reset) {
+    const DeviceModel& M = *w.M;
+    BodyState<R> st;
+    kinematics(w, bc, st);
+    __syncwarp();
+    AuditSum a{};
+    const int b = w.lane;
+    if (b < M.nb)
+        audit_body(a, M.mass_damping[b].x, st.c, st.qr, st.v, st.w, xyz(M.inertia_diag[b]), xyz(M.inertia_off[b]), M.gravity);
+    audit_commit(a, rec, reset, w.lane);
+}
+
 // kComp (compensated precision): q's running sums carry compensation terms
 // in the layout's qcomp section, loaded from and committed to p.q_comp.
 //
@@ -1934,6 +1951,7 @@ __device__ __forceinline__ void control_step_item(const StepParams& p, const War
     }
     const unsigned code = static_cast<unsigned>(as_int(misc[kMiscStatus]));
     const bool success = code == MR_STEP_SUCCESS;
+    if (p.audit != nullptr && success) audit_articulated<R>(w, bc, p.audit + static_cast<size_t>(env) * kAuditWords, reset);
     // Capture + commit: a failed step publishes (and keeps) its checkpoint.
     float* qd = p.q + static_cast<size_t>(env) * nq;
     float* vd = p.v + static_cast<size_t>(env) * nv;

@@ -464,6 +464,8 @@ EXPORTED_SYMBOLS: Final = (
     "mr_pile_step_no_alloc_counters",
     "mr_task_rollout_set_island_labels",
     "mr_task_rollout_copy_island_labels",
+    "mr_task_rollout_set_audit",
+    "mr_task_rollout_copy_audit",
     "mr_create_batch",
     "mr_batch_destroy",
     "mr_batch_advance",
@@ -613,6 +615,10 @@ class Bindings:
         L.mr_task_rollout_set_island_labels.restype = ct.c_int
         L.mr_task_rollout_copy_island_labels.argtypes = [ct.c_void_p, P(ct.c_uint8), ct.c_size_t]
         L.mr_task_rollout_copy_island_labels.restype = ct.c_int
+        L.mr_task_rollout_set_audit.argtypes = [ct.c_void_p, ct.c_uint32]
+        L.mr_task_rollout_set_audit.restype = ct.c_int
+        L.mr_task_rollout_copy_audit.argtypes = [ct.c_void_p, P(ct.c_double), ct.c_size_t]
+        L.mr_task_rollout_copy_audit.restype = ct.c_int
         PP = ct.POINTER(ct.c_void_p)
         L.mr_create_batch.argtypes = [PP, ct.c_size_t]
         L.mr_create_batch.restype = ct.c_void_p

@@ -302,6 +302,22 @@ class World:
             "set_state",
         )
 
+    AUDIT_FIELDS = ("kinetic", "potential", "total", "reference_total", "max_total_drift", "px", "py", "pz", "lx", "ly", "lz",
+                    "steps")
+
+    def set_audit(self, enabled: bool) -> None:
+        """Per-environment FP64 energy and momentum audit on the device."""
+
+        self._lib.check(self._lib.lib.mr_task_rollout_set_audit(self._handle, 1 if enabled else 0), "set_audit")
+
+    def audit(self) -> np.ndarray:
+        """[env, 12] audit records (fields in AUDIT_FIELDS order)."""
+
+        out = np.zeros((self.envs, 12), np.float64)
+        self._lib.check(self._lib.lib.mr_task_rollout_copy_audit(self._handle, out.ctypes.data_as(ct.POINTER(ct.c_double)), out.size),
+                        "copy_audit")
+        return out
+
     def set_island_labels(self, enabled: bool) -> None:
         """Scene worlds: record each control step's island partition."""
 
