@@ -558,8 +558,9 @@ def _mix_worlds(total: int):
     """The heterogeneous mix: 40 % 7-link chains (one 5 ms step per control
     step), 30 % 29-DoF trees and 30 % piles whose body count is drawn per
     environment from U{8..64} (boxes, spheres and capsules of size
-    U(0.05, 0.3) m, density 500-2000 kg/m^3); one world per distinct
-    configuration, as the reference compiles one topology per context."""
+    U(0.05, 0.3) m, density 500-2000 kg/m^3, dropped as a heap; capsule-box
+    pairs through GJK / EPA); one world per distinct configuration, as the
+    reference compiles one topology per context."""
 
     import numi_lab_b200 as nb
 
@@ -572,7 +573,8 @@ def _mix_worlds(total: int):
     worlds = [nb.World("chain7", n_chain, substeps=1, control_dt=0.005, seed=SEED),
               nb.World("tree29", n_tree, substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT, seed=SEED)]
     for n in sorted(per):
-        worlds.append(nb.World("pile", per[n], substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT, seed=seeds[n]))
+        worlds.append(nb.World("pile_gjk", per[n], substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT,
+                               seed=seeds[n]))
     return worlds, {"chain7": n_chain, "tree29": n_tree, "pile": n_pile, "pile_configs": len(per),
                     "mean_pile_bodies": float(counts.mean())}
 
@@ -672,7 +674,8 @@ def measure_mix(args, device) -> dict:
         "ms_per_step": {"batched": batch_ms, "plain_per_config": plain_ms, "concurrent_streams": conc_ms},
         "config": {"workload": f"{MIX_TOTAL} envs: {mix['chain7']} chain7 (5 ms steps, actions N(0, 0.3), one-horizon episodes), "
                                f"{mix['tree29']} tree29 (PD targets N(0, 0.3)), {mix['pile']} settled piles with body counts "
-                               f"drawn per env from U{{8..64}} (mean {mix['mean_pile_bodies']:.1f}; {mix['pile_configs']} configurations), "
+                               f"drawn per env from U{{8..64}} (mean {mix['mean_pile_bodies']:.1f}; {mix['pile_configs']} configurations; "
+                               "dropped as heaps; capsule-box pairs through GJK / EPA), "
                                f"{horizon} control steps per bench step", "worlds": len(worlds),
                    "l2": "flushed (256 MiB write) between steps"},
         "batch_launch": shape,

@@ -184,7 +184,11 @@ enum MRRunManifestSourceC {
     /* Pile of 8-64 free boxes, spheres, capsules and cylinders (one quarter
      * each) dropped onto a ground plane; cylinder pairs take the
      * support-mapped (GJK / EPA) narrowphase. */
-    MR_RUN_SOURCE_SYNTHETIC_CYLINDER_PILE = 104u
+    MR_RUN_SOURCE_SYNTHETIC_CYLINDER_PILE = 104u,
+    /* The pile of MR_RUN_SOURCE_SYNTHETIC_PILE (same bodies for the same
+     * seed) with every capsule-box pair taking the support-mapped (GJK /
+     * EPA, MPR fallback) narrowphase instead of the analytic witness. */
+    MR_RUN_SOURCE_SYNTHETIC_PILE_GJK = 105u
 };
 
 /* reference: include/metalrobo/c_api.h:171-190 (same shape). */
@@ -747,7 +751,8 @@ MR_API int mr_server_stats(const MRServerHandle* server, MRServerStatsC* stats);
  * environments never wait for each other.  The queue reset and the launches
  * are captured as one CUDA graph.  The rollouts keep owning their state; a batch stores
  * pointers to them (destroy the batch before its rollouts).  Rollouts must
- * be FP32, without a native policy and without support-mapped pairs. */
+ * be FP32 and without a native policy; a batch with support-mapped (GJK /
+ * EPA) pairs runs per family. */
 typedef struct MRBatchHandle MRBatchHandle;
 
 enum MRBatchOrderC {

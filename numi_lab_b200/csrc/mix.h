@@ -46,7 +46,9 @@ int mix_scene_warp_floats();
 
 // Kernel families: the fused kernel runs every item; the per-family
 // kernels run one family's items at that family's own register budget.
-enum MixFamily : int { kMixFamilyFused = 0, kMixFamilyArticulated = 1, kMixFamilyScene = 2 };
+// kMixFamilySceneConvex is the free-body kernel with the support-mapped
+// (GJK / EPA) narrowphase, for batches with such pairs.
+enum MixFamily : int { kMixFamilyFused = 0, kMixFamilyArticulated = 1, kMixFamilyScene = 2, kMixFamilySceneConvex = 3 };
 
 cudaError_t configure_mix_kernel(int family, size_t max_dynamic_smem);
 cudaError_t mix_occupancy(int family, int warps_per_block, size_t smem_per_block, int* blocks_per_sm);

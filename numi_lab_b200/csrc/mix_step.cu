@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(128, 3) mix_step_kernel(const MixWorld* __rest
 // one like the articulated kernel (3 CTAs of 4 warps), the free-body one
 // like the scene kernel (16 resident warps, at most 128 registers) -- so a
 // batch can run each family at its own kernel's occupancy.
-template <bool kScene>
+template <bool kScene, bool kConvex>
 __device__ __forceinline__ void family_loop(const MixWorld* __restrict__ worlds, int world_count, int steps,
                                             const std::uint32_t* __restrict__ items, int item_count, unsigned* next_item,
                                             int smem_floats_per_warp) {
@@ -83,7 +83,7 @@ __device__ __forceinline__ void family_loop(const MixWorld* __restrict__ worlds,
         const int env = static_cast<int>(code & kMixEnvMask);
         if (kScene) {
             for (int k = 0; k < steps; ++k) {
-                scene_step_item<false, false>(worlds[static_cast<size_t>(k) * world_count + world].scene, base, env, env);
+                scene_step_item<false, kConvex>(worlds[static_cast<size_t>(k) * world_count + world].scene, base, env, env);
                 __syncwarp();
             }
         } else {
@@ -107,19 +107,22 @@ __device__ __forceinline__ void family_loop(const MixWorld* __restrict__ worlds,
 __global__ void __launch_bounds__(128, 3) mix_articulated_kernel(const MixWorld* __restrict__ worlds, int world_count, int steps,
                                                                  const std::uint32_t* __restrict__ items, int item_count,
                                                                  unsigned* next_item, int smem_floats_per_warp) {
-    family_loop<false>(worlds, world_count, steps, items, item_count, next_item, smem_floats_per_warp);
+    family_loop<false, false>(worlds, world_count, steps, items, item_count, next_item, smem_floats_per_warp);
 }
 
+// kConvex: some free-body world has support-mapped (GJK / EPA) pairs.
+template <bool kConvex>
 __global__ void __launch_bounds__(32, 16) mix_scene_kernel(const MixWorld* __restrict__ worlds, int world_count, int steps,
                                                            const std::uint32_t* __restrict__ items, int item_count,
                                                            unsigned* next_item, int smem_floats_per_warp) {
-    family_loop<true>(worlds, world_count, steps, items, item_count, next_item, smem_floats_per_warp);
+    family_loop<true, kConvex>(worlds, world_count, steps, items, item_count, next_item, smem_floats_per_warp);
 }
 
 template <typename F>
 cudaError_t for_mix_kernel(int family, F&& f) {
     if (family == kMixFamilyArticulated) return f(mix_articulated_kernel);
-    if (family == kMixFamilyScene) return f(mix_scene_kernel);
+    if (family == kMixFamilyScene) return f(mix_scene_kernel<false>);
+    if (family == kMixFamilySceneConvex) return f(mix_scene_kernel<true>);
     return f(mix_step_kernel);
 }
 
@@ -143,7 +146,7 @@ cudaError_t mix_occupancy(int family, int warps_per_block, size_t smem_per_block
 cudaError_t launch_mix_horizon(int family, const MixWorld* worlds, int world_count, int steps, const std::uint32_t* items,
                                int item_count, unsigned* next_item, int warps_per_block, int smem_floats_per_warp, int grid,
                                cudaStream_t stream) {
-    const int max_warps = family == kMixFamilyScene ? 1 : 4;
+    const int max_warps = family == kMixFamilyScene || family == kMixFamilySceneConvex ? 1 : 4;
     if (warps_per_block < 1 || warps_per_block > max_warps || grid < 1 || steps < 1 || world_count < 1 ||
         smem_floats_per_warp < kLayoutFloats || (smem_floats_per_warp & 3) != 0)
         return cudaErrorInvalidValue;

@@ -477,7 +477,7 @@ CompiledModel build_tree29(std::uint64_t seed) {
 // Ground body with the plane collider, materials, the all-pairs list in key
 // order (a, b), b = n for the plane, and the world record of a scene with
 // `n` free bodies already in m.bodies / m.shapes.
-static void finish_scene(CompiledModel& m, std::uint32_t n, double friction) {
+static void finish_scene(CompiledModel& m, std::uint32_t n, double friction, bool gjk_capsule_box = false) {
     MRModelBodyC ground{};
     ground.parent_body = MR_INVALID_INDEX;
     ground.inbound_joint = MR_INVALID_INDEX;
@@ -518,7 +518,7 @@ static void finish_scene(CompiledModel& m, std::uint32_t n, double friction) {
                    : (ta == MR_SHAPE_BOX ? MR_COLLISION_PAIR_BOX_BOX : MR_COLLISION_PAIR_CAPSULE_CAPSULE);
         if (sphere && box) return MR_COLLISION_PAIR_SPHERE_BOX;
         if (sphere && capsule) return MR_COLLISION_PAIR_SPHERE_CAPSULE;
-        return MR_COLLISION_PAIR_CAPSULE_BOX;
+        return gjk_capsule_box ? MR_COLLISION_PAIR_CONVEX : MR_COLLISION_PAIR_CAPSULE_BOX;
     };
     // Compiled pairs in key order (a, b), b = n for the plane.
     for (std::uint32_t a = 0; a < n; ++a) {
@@ -552,9 +552,9 @@ static void finish_scene(CompiledModel& m, std::uint32_t n, double friction) {
 }
 
 
-CompiledModel build_pile(std::uint64_t seed, std::uint32_t count, bool cylinders) {
+CompiledModel build_pile(std::uint64_t seed, std::uint32_t count, bool cylinders, bool gjk_capsule_box) {
     CompiledModel m;
-    m.name = cylinders ? "synthetic_cylinder_pile" : "synthetic_pile";
+    m.name = cylinders ? "synthetic_cylinder_pile" : (gjk_capsule_box ? "synthetic_pile_gjk" : "synthetic_pile");
     m.scene = true;
     std::uint64_t k = 0;
     auto draw = [&](double lo, double hi) { return uniform(seed, kStreamModel, k++, lo, hi); };
@@ -641,7 +641,8 @@ CompiledModel build_pile(std::uint64_t seed, std::uint32_t count, bool cylinders
         m.shapes.push_back(s);
     }
     m.scene_cell = static_cast<float>(2.0 * largest + 0.05);
-    finish_scene(m, n, 0.6);
+    if (gjk_capsule_box) m.scene_layout = CompiledModel::SceneLayout::heap;
+    finish_scene(m, n, 0.6, gjk_capsule_box);
     return m;
 }
 
@@ -714,18 +715,26 @@ void sample_reset_state(const CompiledModel& model, std::uint64_t seed, std::uin
     }
     if (model.scene) {
         // Bodies on a jittered square grid, dropped from U(0.1, 1) m above
-        // the plane with a uniformly random orientation, at rest.
+        // the plane with a uniformly random orientation, at rest.  A heap
+        // puts the grid in three layers one cell apart in height, each layer
+        // shifted by half a cell: no two bodies overlap at the start, and
+        // the upper layers fall onto the lower ones.
         const std::uint32_t n = model.scene_bodies;
-        const std::uint32_t side = static_cast<std::uint32_t>(std::ceil(std::sqrt(static_cast<double>(n))));
+        const bool heap = model.scene_layout == CompiledModel::SceneLayout::heap;
+        const std::uint32_t per_layer = heap ? (n + 2) / 3 : n;
+        const std::uint32_t side = static_cast<std::uint32_t>(std::ceil(std::sqrt(static_cast<double>(per_layer))));
         const std::uint64_t base = static_cast<std::uint64_t>(env) * 1024u;
         for (std::uint32_t b = 0; b < n; ++b) {
             const double cell = model.scene_cell;
-            const double x = (static_cast<double>(b % side) - 0.5 * (side - 1)) * cell +
+            const std::uint32_t layer = b / per_layer, i = b % per_layer;
+            const double shift = heap ? 0.5 * cell * static_cast<double>(layer % 2) : 0.0;
+            const double x = (static_cast<double>(i % side) - 0.5 * (side - 1)) * cell + shift +
                              uniform(seed, kStreamResetQ, base + 8 * b, -0.02, 0.02);
-            const double y = (static_cast<double>(b / side) - 0.5 * (side - 1)) * cell +
+            const double y = (static_cast<double>(i / side) - 0.5 * (side - 1)) * cell + shift +
                              uniform(seed, kStreamResetQ, base + 8 * b + 1, -0.02, 0.02);
             const double bound = model.shapes[b].contact_rest_bound[2];
-            const double z = bound + uniform(seed, kStreamResetQ, base + 8 * b + 2, 0.1, 1.0);
+            const double z = heap ? 0.5 * cell + layer * cell + uniform(seed, kStreamResetQ, base + 8 * b + 2, 0.0, 0.05)
+                                  : bound + uniform(seed, kStreamResetQ, base + 8 * b + 2, 0.1, 1.0);
             // Uniform rotation (Shoemake): three uniforms -> unit quaternion.
             const double u1 = uniform01(seed, kStreamResetRoot, base + 8 * b);
             const double u2 = uniform01(seed, kStreamResetRoot, base + 8 * b + 1);

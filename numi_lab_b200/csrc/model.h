@@ -61,7 +61,10 @@ struct CompiledModel {
     std::uint32_t scene_bodies = 0;
     float scene_cell = 0.0f;  // reset grid spacing
     // Reset layout of a scene: a dropped pile, or a box stack on the plane.
-    enum class SceneLayout : std::uint32_t { pile = 0, stack = 1 };
+    // pile: one body per cell of a square grid, dropped from U(0.1, 1) m;
+    // stack: a yawed column of boxes; heap: the grid in three offset layers
+    // one cell apart in height, so that falling bodies land on each other.
+    enum class SceneLayout : std::uint32_t { pile = 0, stack = 1, heap = 2 };
     SceneLayout scene_layout = SceneLayout::pile;
     float stack_offset_sigma = 0.0f;  // horizontal offsets of stacked boxes ~ N(0, sigma)
 
@@ -74,7 +77,9 @@ CompiledModel build_tree29(std::uint64_t seed);
 // U(500, 2000) kg/m^3) dropped onto a ground plane; the body count is drawn
 // from the seed unless `bodies` is non-zero.
 // `cylinders`: one quarter each of boxes, spheres, capsules and cylinders.
-CompiledModel build_pile(std::uint64_t seed, std::uint32_t bodies = 0, bool cylinders = false);
+// gjk_capsule_box: capsule-box pairs take the support-mapped (GJK / EPA)
+// narrowphase instead of the analytic witness.
+CompiledModel build_pile(std::uint64_t seed, std::uint32_t bodies = 0, bool cylinders = false, bool gjk_capsule_box = false);
 // Stack of `boxes` 0.1 m, 1 kg cubes (friction 0.6) resting on a ground
 // plane, the stack yawed U(0, 2 pi) and each box offset horizontally by
 // N(0, 2 mm) at reset.

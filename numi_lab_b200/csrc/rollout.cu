@@ -869,6 +869,7 @@ MR_API MRTaskRolloutHandle* mr_create_task_rollout(const MRRunManifestC* manifes
             case MR_RUN_SOURCE_SYNTHETIC_TREE29: h.model = numi::build_tree29(cfg.seed); break;
             case MR_RUN_SOURCE_SYNTHETIC_PILE: h.model = numi::build_pile(cfg.seed); break;
             case MR_RUN_SOURCE_SYNTHETIC_CYLINDER_PILE: h.model = numi::build_pile(cfg.seed, 0, true); break;
+            case MR_RUN_SOURCE_SYNTHETIC_PILE_GJK: h.model = numi::build_pile(cfg.seed, 0, false, true); break;
             case MR_RUN_SOURCE_SYNTHETIC_STACK: h.model = numi::build_stack(cfg.seed); break;
             default:
                 throw std::invalid_argument("unsupported run source " + std::to_string(manifest->source) +
@@ -1366,6 +1367,7 @@ static numi::CompiledModel compile_source(uint32_t source, uint64_t seed) {
         case MR_RUN_SOURCE_SYNTHETIC_TREE29: return numi::build_tree29(seed);
         case MR_RUN_SOURCE_SYNTHETIC_PILE: return numi::build_pile(seed);
         case MR_RUN_SOURCE_SYNTHETIC_CYLINDER_PILE: return numi::build_pile(seed, 0, true);
+        case MR_RUN_SOURCE_SYNTHETIC_PILE_GJK: return numi::build_pile(seed, 0, false, true);
         case MR_RUN_SOURCE_SYNTHETIC_STACK: return numi::build_stack(seed);
         default: throw std::invalid_argument("unsupported synthetic source " + std::to_string(source));
     }
@@ -1577,6 +1579,10 @@ struct MRBatchHandle {
             if (st) cudaStreamDestroy(st);
     }
 
+    // Some free-body world has support-mapped (GJK / EPA) pairs: its family
+    // runs the kernel instance with that narrowphase, and only per family.
+    bool convex = false;
+    int kernel_of(int family) const { return family == numi::kMixFamilyScene && convex ? numi::kMixFamilySceneConvex : family; }
     int wpb(int family) const { return family == numi::kMixFamilyScene ? 1 : warps_per_block; }
     int grid(int family) const { return std::max(1, blocks_per_sm[family]) * sms; }
     std::uint32_t item_count() const { return static_cast<std::uint32_t>(items[numi::kMixFamilyFused].size()); }
@@ -1587,7 +1593,7 @@ struct MRBatchHandle {
             blocks_per_sm[f] = 0;
             if (!smem_floats[f]) continue;
             const size_t smem = static_cast<size_t>(smem_floats[f]) * sizeof(float) * wpb(f);
-            check(numi::mix_occupancy(f, wpb(f), smem, &blocks_per_sm[f]), "batch occupancy");
+            check(numi::mix_occupancy(kernel_of(f), wpb(f), smem, &blocks_per_sm[f]), "batch occupancy");
             if (blocks_per_sm[f] < 1) throw std::runtime_error("the batch's per-warp shared memory does not fit one CTA on this device");
         }
     }
@@ -1629,7 +1635,7 @@ struct MRBatchHandle {
     }
 
     void launch(int family, std::uint32_t steps, const std::uint32_t* item_list, int n, cudaStream_t s) {
-        check(numi::launch_mix_horizon(family, d_worlds.ptr, static_cast<int>(worlds.size()), static_cast<int>(steps), item_list, n,
+        check(numi::launch_mix_horizon(kernel_of(family), d_worlds.ptr, static_cast<int>(worlds.size()), static_cast<int>(steps), item_list, n,
                                        d_next.ptr + family, wpb(family), smem_floats[family], grid(family), s),
               "batch horizon launch");
     }
@@ -1790,6 +1796,7 @@ struct MRBatchHandle {
         for (const std::uint32_t md : {std::uint32_t(MR_BATCH_LAUNCH_FUSED), std::uint32_t(MR_BATCH_LAUNCH_PER_FAMILY)})
             for (const std::uint32_t ord : {std::uint32_t(MR_BATCH_ORDER_LONGEST_FIRST), std::uint32_t(MR_BATCH_ORDER_ROUND_ROBIN)})
                 for (const int wp : {1, 2, 4}) {
+                    if (convex && md == MR_BATCH_LAUNCH_FUSED) continue;
                     mode = md;
                     order = ord;
                     warps_per_block = wp;
@@ -1839,8 +1846,7 @@ MR_API MRBatchHandle* mr_create_batch(MRTaskRolloutHandle* const* rollouts, size
             if (h->device != b->device) throw std::invalid_argument("every rollout of a batch must live on the current device");
             if (h->precision != MR_PRECISION_FP32) throw std::invalid_argument("batched rollouts run in FP32 precision only");
             if (h->policy) throw std::invalid_argument("batched rollouts take their actions from the caller (no native policy)");
-            if (h->scene && h->smodel.support_mapped)
-                throw std::invalid_argument("worlds with support-mapped (cylinder) pairs are not batched");
+            if (h->scene && h->smodel.support_mapped) b->convex = true;
             if (h->envs > numi::kMixEnvMask) throw std::invalid_argument("a batched rollout holds at most 2^24 - 1 environments");
             for (size_t j = 0; j < i; ++j)
                 if (rollouts[j] == h) throw std::invalid_argument("a rollout appears twice in the batch");
@@ -1859,8 +1865,9 @@ MR_API MRBatchHandle* mr_create_batch(MRTaskRolloutHandle* const* rollouts, size
             if (!b->smem_floats[f]) continue;
             const size_t bytes = std::min(static_cast<size_t>(b->smem_floats[f]) * sizeof(float) * 4,
                                           static_cast<size_t>(prop.sharedMemPerBlockOptin));
-            check(numi::configure_mix_kernel(f, bytes), "batch kernel attributes");
+            check(numi::configure_mix_kernel(b->kernel_of(f), bytes), "batch kernel attributes");
         }
+        if (b->convex) b->mode = MR_BATCH_LAUNCH_PER_FAMILY;
         for (cudaStream_t* st : {&b->stream, &b->side}) check(cudaStreamCreateWithFlags(st, cudaStreamNonBlocking), "stream");
         for (cudaEvent_t* e : {&b->ev_in, &b->ev_out, &b->ev_fork, &b->ev_join}) check(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "event");
         for (cudaEvent_t* e : {&b->ev_a, &b->ev_b}) check(cudaEventCreate(e), "event");

@@ -654,8 +654,13 @@ __device__ int gjk(const Collider& A, const Collider& B, unsigned ia, unsigned i
             const float3 e = cand.w - sx[i].w;
             dup = dup || dot3(e, e) <= tol * tol;
         }
+        // Stop once the support advances less than tol along the UNIT
+        // direction.  (The reference measures it along the unnormalised
+        // direction, which below 1 m lets the reported distance exceed the
+        // true one by tol / distance -- millimetres near contact, enough to
+        // report a 0.7 mm capsule-box overlap as 1.6 mm apart.)
         const float advance = dot3(cand.w, d) - dot3(closest, d);
-        bool done = dup || advance <= tol * fmaxf(len3(d), 1.0f);
+        bool done = dup || advance <= tol * len3(d);
         if (!done) {
             sx[n++] = cand;
             if (closest_simplex(sx, n, wt, closest)) return 1;
@@ -911,6 +916,9 @@ __device__ __noinline__ unsigned support_mapped_contacts(const Collider& A, cons
     float3 wa[kRawCap], wb[kRawCap];
     int nw = 0;
     sink.add(q.pa, q.pb, q.sep, q.fa, q.fb);
+    // Only a cylinder has a contact patch; other support-mapped pairs (a
+    // capsule against a box) keep the query's witness alone.
+    if (A.type != MR_SHAPE_CYLINDER && B.type != MR_SHAPE_CYLINDER) return MR_STEP_SUCCESS;
     wa[nw] = q.pa;
     wb[nw] = q.pb;
     ++nw;

@@ -25,6 +25,7 @@ MR_RUN_SOURCE_SYNTHETIC_TREE29: Final = 101
 MR_RUN_SOURCE_SYNTHETIC_PILE: Final = 102
 MR_RUN_SOURCE_SYNTHETIC_STACK: Final = 103
 MR_RUN_SOURCE_SYNTHETIC_CYLINDER_PILE: Final = 104
+MR_RUN_SOURCE_SYNTHETIC_PILE_GJK: Final = 105
 MANIFOLD_POINTS: Final = 4
 MR_PRECISION_FP32: Final = 0
 MR_PRECISION_FP64_ARTICULATED_INERTIA: Final = 1

@@ -27,6 +27,7 @@ SOURCES = {
     "pile": native.MR_RUN_SOURCE_SYNTHETIC_PILE,
     "stack32": native.MR_RUN_SOURCE_SYNTHETIC_STACK,
     "cylinder_pile": native.MR_RUN_SOURCE_SYNTHETIC_CYLINDER_PILE,
+    "pile_gjk": native.MR_RUN_SOURCE_SYNTHETIC_PILE_GJK,
 }
 SCENE_MANIFOLDS = 128      # manifold slots per scene environment
 SCENE_SLOT_WORDS = 57      # MRManifoldC words + pair key

@@ -2158,8 +2158,11 @@ static int sgjk(const SCol* A, const SCol* B, uint32_t ia, uint32_t ib, double s
             const v3 e = vsub(cand.w, sx[i].w);
             dup = dup || vdot(e, e) <= tol * tol;
         }
+        /* Advance measured along the unit direction; the reference's
+         * unnormalised measure (Collision.metal:2372-2376) lets the distance
+         * exceed the true one by tol / distance below 1 m. */
         const double advance = vdot(cand.w, d) - vdot(closest, d);
-        int done = dup || advance <= tol * fmax(vlen(d), 1.0);
+        int done = dup || advance <= tol * vlen(d);
         if (!done) {
             sx[(*n)++] = cand;
             if (sclosest_simplex(sx, n, wt, &closest)) { q->status = MR_STEP_SUCCESS; q->sep = -0.0; return 1; }

@@ -16,11 +16,15 @@ pytestmark = pytest.mark.gpu
 PILE_BODIES = (9, 30, 64)
 
 
-def _worlds():
+def _worlds(gjk: bool = False):
     seeds = nb.world.pile_seeds_by_body_count(PILE_BODIES)
     worlds = [nb.World("chain7", 40, substeps=1, control_dt=0.005, seed=3),
               nb.World("tree29", 24, substeps=4, velocity_iterations=8, control_dt=0.02, seed=5)]
     worlds += [nb.World("pile", 12, substeps=4, velocity_iterations=8, control_dt=0.02, seed=seeds[n]) for n in PILE_BODIES]
+    if gjk:
+        # Capsule-box pairs through GJK / EPA: the batch runs per family with
+        # the support-mapped free-body kernel.
+        worlds.append(nb.World("pile_gjk", 12, substeps=4, velocity_iterations=8, control_dt=0.02, seed=seeds[30]))
     return worlds
 
 
@@ -44,10 +48,11 @@ def _assert_same(a, b):
         np.testing.assert_array_equal(x, y)
 
 
-def test_batch_matches_each_world_alone(cuda_device):
+@pytest.mark.parametrize("gjk", [False, True])
+def test_batch_matches_each_world_alone(cuda_device, gjk):
     import torch
 
-    alone, batched = _worlds(), _worlds()
+    alone, batched = _worlds(gjk), _worlds(gjk)
     try:
         with nb.Batch(batched) as batch:
             shape = batch.launch_shape()

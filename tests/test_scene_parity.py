@@ -188,3 +188,12 @@ def test_cylinder_pile_control_steps_match_oracle(cuda_device, seed):
     # vertex by the sign of a rounding-level component every substep, so a
     # large pile has few env-steps without any band decision.
     _check_rows(rows, max(40, len(rows) // 10))
+
+
+@pytest.mark.parametrize("seed", [3, 13, 1])  # 10, 17 and 50 bodies
+def test_gjk_capsule_box_pile_control_steps_match_oracle(cuda_device, seed):
+    """Piles whose capsule-box pairs take the support-mapped narrowphase
+    (GJK, EPA with MPR fallback; MR_RUN_SOURCE_SYNTHETIC_PILE_GJK) on the
+    device against the oracle's FP64 restatement of the same query."""
+    rows = _compare_run(seed, 8, 60, "fp32", "pile_gjk")
+    _check_rows(rows, len(rows) // 4)
