@@ -90,19 +90,33 @@ def _measured_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def _profile_traffic() -> float | None:
-    """DRAM bytes per control-step launch from the committed ncu summary."""
+def _profile_value(key: str, name: str = "control_step_contact_tree29.md") -> float | None:
+    """A `key: value` figure of a committed ncu summary under profiles/."""
 
-    path = ROOT / "profiles" / "control_step_contact_tree29.md"
+    path = ROOT / "profiles" / name
     if not path.is_file():
         return None
     for line in path.read_text().splitlines():
-        if line.strip().startswith("traffic_bytes_per_launch:"):
+        if line.strip().startswith(key + ":"):
             try:
                 return float(line.split(":", 1)[1].strip())
             except ValueError:
                 return None
     return None
+
+
+def _issue_peak() -> dict:
+    """FP32 FMA peak and warp-instruction issue rate of this device
+    (mr_measure_issue_peak, CUDA events)."""
+
+    import ctypes as ct
+
+    import numi_lab_b200 as nb
+
+    lib = nb.bindings()
+    tf, ips = ct.c_double(), ct.c_double()
+    lib.check(lib.lib.mr_measure_issue_peak(ct.byref(tf), ct.byref(ips)), "mr_measure_issue_peak")
+    return {"fma_tflops": tf.value, "warp_instructions_per_s": ips.value}
 
 
 class ClockSampler:
@@ -590,7 +604,8 @@ def measure_mix(args, device) -> dict:
 
     import numi_lab_b200 as nb
 
-    worlds, mix = _mix_worlds(MIX_TOTAL)
+    total = getattr(args, "envs", 0) or MIX_TOTAL
+    worlds, mix = _mix_worlds(total)
     horizon = MIX_HORIZON
     try:
         gen = torch.Generator(device=device).manual_seed(SEED)
@@ -630,7 +645,7 @@ def measure_mix(args, device) -> dict:
                 failures += sum(int((st != 0).sum().item()) for st in status)
             return ms / args.steps, failures
 
-        env_steps = MIX_TOTAL * horizon
+        env_steps = total * horizon
         # Batched: one launch per control step over every environment.
         restore()
         batch = nb.Batch(worlds)
@@ -672,7 +687,7 @@ def measure_mix(args, device) -> dict:
         "concurrent_streams_value": env_steps / (conc_ms / 1e3),
         "mix_vs_plain": plain_ms / batch_ms,
         "ms_per_step": {"batched": batch_ms, "plain_per_config": plain_ms, "concurrent_streams": conc_ms},
-        "config": {"workload": f"{MIX_TOTAL} envs: {mix['chain7']} chain7 (5 ms steps, actions N(0, 0.3), one-horizon episodes), "
+        "config": {"workload": f"{total} envs: {mix['chain7']} chain7 (5 ms steps, actions N(0, 0.3), one-horizon episodes), "
                                f"{mix['tree29']} tree29 (PD targets N(0, 0.3)), {mix['pile']} settled piles with body counts "
                                f"drawn per env from U{{8..64}} (mean {mix['mean_pile_bodies']:.1f}; {mix['pile_configs']} configurations; "
                                "dropped as heaps; capsule-box pairs through GJK / EPA), "
@@ -1061,7 +1076,13 @@ def run_headline(args, rank: int, local_rank: int, world_size: int) -> None:
     bytes_per_env_step = _algorithmic_bytes_per_env_step(world.nq, world.nv, world.action_count, mean_points, mean_manifolds)
     achieved = bytes_per_env_step * envs / (kernel_ms / 1e3) / 1e9
     peaks = _measured_peaks()
-    traffic = _profile_traffic()
+    traffic = _profile_value("traffic_bytes_per_launch")
+    # Issue roofline: the kernel's warp instructions per env-step (from the
+    # committed ncu summary) at the measured control-step time, against the
+    # measured warp-instruction issue rate of this device.
+    issue = _issue_peak()
+    inst_per_env_step = _profile_value("warp_instructions_per_env_step")
+    issue_achieved = inst_per_env_step * envs / (kernel_ms / 1e3) if inst_per_env_step else None
 
     launch_shape = world.launch_shape()
     world.close()
@@ -1070,7 +1091,7 @@ def run_headline(args, rank: int, local_rank: int, world_size: int) -> None:
     # serving stream, on rank 0 (bounded: a few horizons, one arrival rate).
     mix = serving = None
     if rank == 0 and not args.headline_only:
-        mix_args = argparse.Namespace(steps=min(args.steps, 5), warmup=3)
+        mix_args = argparse.Namespace(steps=min(args.steps, 5), warmup=3, envs=0)
         mix = measure_mix(mix_args, device)
         mix["steps"] = mix_args.steps
         serving = measure_serving(SERVE_RATES[:1] + SERVE_RATES[2:3])
@@ -1113,6 +1134,13 @@ def run_headline(args, rank: int, local_rank: int, world_size: int) -> None:
                 "algorithmic_bytes_per_env_step": bytes_per_env_step,
                 "kernel_ms_per_control_step": kernel_ms,
                 "launches_per_control_step": chains,
+                "issue_frac": issue_achieved / issue["warp_instructions_per_s"] if issue_achieved else None,
+                "issue": {"achieved_warp_instructions_per_s": issue_achieved,
+                          "peak_warp_instructions_per_s": issue["warp_instructions_per_s"],
+                          "peak_source": "measured (mr_measure_issue_peak: FP32 FMA chains, CUDA events)",
+                          "fma_tflops_peak": issue["fma_tflops"],
+                          "warp_instructions_per_env_step": inst_per_env_step,
+                          "instructions_source": "profiles/control_step_contact_tree29.md (ncu smsp__inst_executed.sum)"},
             },
             "cpu_baseline": cpu,
             "gpu_launches": launches_per_step * args.steps,

@@ -736,6 +736,12 @@ MR_API int mr_server_copy_result(const MRServerHandle* server, uint64_t request_
 MR_API int mr_server_release(MRServerHandle* server, uint64_t request_id);
 MR_API int mr_server_stats(const MRServerHandle* server, MRServerStatsC* stats);
 
+/* No counterpart in the reference.  Measures the current device's FP32 FMA
+ * peak (TFLOP/s) and its warp-instruction issue rate (warp instructions per
+ * second of FMA issue) with CUDA events: the denominators of the issue
+ * roofline of the control-step kernels.  Synchronous; allocates 1 KB. */
+MR_API int mr_measure_issue_peak(double* fma_tflops, double* warp_instructions_per_second);
+
 /* ---------------------------------------------------------------------- */
 /* Heterogeneous batch (no counterpart in the reference)                  */
 /* ---------------------------------------------------------------------- */

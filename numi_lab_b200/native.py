@@ -467,6 +467,7 @@ EXPORTED_SYMBOLS: Final = (
     "mr_task_rollout_copy_island_labels",
     "mr_task_rollout_set_audit",
     "mr_task_rollout_copy_audit",
+    "mr_measure_issue_peak",
     "mr_create_batch",
     "mr_batch_destroy",
     "mr_batch_advance",
@@ -620,6 +621,8 @@ class Bindings:
         L.mr_task_rollout_set_audit.restype = ct.c_int
         L.mr_task_rollout_copy_audit.argtypes = [ct.c_void_p, P(ct.c_double), ct.c_size_t]
         L.mr_task_rollout_copy_audit.restype = ct.c_int
+        L.mr_measure_issue_peak.argtypes = [P(ct.c_double), P(ct.c_double)]
+        L.mr_measure_issue_peak.restype = ct.c_int
         PP = ct.POINTER(ct.c_void_p)
         L.mr_create_batch.argtypes = [PP, ct.c_size_t]
         L.mr_create_batch.restype = ct.c_void_p
