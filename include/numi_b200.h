@@ -633,15 +633,16 @@ MR_API int mr_task_rollout_copy_state(
     const MRTaskRolloutHandle* handle, float* q, float* v, MRManifoldC* manifolds);
 
 /* No counterpart in the reference: a per-environment FP64 energy and
- * momentum audit.  While enabled, every successful control step adds each
- * body's kinetic energy, potential energy (-m g . c), linear momentum and
- * angular momentum about the world origin in FP64 from the committed FP32
- * state, reduced per environment in FP64, into a resident record of 12
+ * momentum audit.  While enabled, a kernel after every control step adds
+ * each body's kinetic energy, potential energy (-m g . c), linear momentum
+ * and angular momentum about the world origin in FP64 from the committed
+ * FP32 state (a failed step's checkpoint), reduced per environment in
+ * FP64, into a resident record of 12
  * doubles: kinetic, potential, total, reference total (taken on the first
  * audited step after enabling, a reset, mr_task_rollout_reset or a new
  * state), largest |total - reference| so far, linear momentum xyz, angular
  * momentum xyz, audited steps since the reference.  Enabling allocates
- * [env][12] doubles. */
+ * [env][12] doubles.  Batch advances (mr_batch_advance) do not audit. */
 MR_API int mr_task_rollout_set_audit(MRTaskRolloutHandle* handle, uint32_t enabled);
 /* No counterpart in the reference: copies the audit records ([env][12]). */
 MR_API int mr_task_rollout_copy_audit(const MRTaskRolloutHandle* handle, double* records, size_t count);

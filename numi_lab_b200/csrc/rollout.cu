@@ -510,7 +510,6 @@ struct MRTaskRolloutHandle {
             p.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
             p.support_mapped = smodel.support_mapped;
             p.island_labels = island_labels ? d_island_labels.ptr : nullptr;
-            p.audit = audit ? d_audit.ptr : nullptr;
             return w;
         }
         w.kind = contact ? numi::kMixContact : numi::kMixFreeMotion;
@@ -531,7 +530,6 @@ struct MRTaskRolloutHandle {
         p.substeps = static_cast<int>(config.physics_substeps);
         p.velocity_iterations = static_cast<int>(config.velocity_iterations);
         p.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
-        p.audit = audit ? d_audit.ptr : nullptr;
         return w;
     }
 
@@ -601,6 +599,7 @@ struct MRTaskRolloutHandle {
                 p.island_labels = island_labels ? d_island_labels.ptr : nullptr;
                 p.audit = audit ? d_audit.ptr : nullptr;
                 check(numi::launch_scene_step(p, s), "scene step launch");
+                if (audit) check(numi::launch_scene_audit(p, s), "audit launch");
                 if (host_obs && obs) copy_observations(k, obs, host_obs, s);
             }
             if (host_obs && obs) join_copies(s);
@@ -647,6 +646,10 @@ struct MRTaskRolloutHandle {
                 check(numi::launch_control_step(p, precision == MR_PRECISION_COMPENSATED ? layout_comp : layout, contact, precision,
                                                 warps_per_block[precision], cs),
                       "control step launch");
+                if (audit)
+                    check(numi::launch_audit_step(p, precision == MR_PRECISION_COMPENSATED ? layout_comp : layout,
+                                                  precision != MR_PRECISION_FP32, warps_per_block[precision], cs),
+                          "audit launch");
                 if (host_obs && obs) copy_observation_rows(k, o, n, obs, host_obs, cs, c);
             }
             if (driven && evaluate_final) enqueue_policy(steps, o, n, nullptr, false, cs);

@@ -23,6 +23,10 @@ cudaError_t control_step_occupancy(bool contact, std::uint32_t precision, int wa
 cudaError_t launch_control_step(const StepParams& p, const WarpLayout& layout, bool contact, std::uint32_t precision,
                                 int warps_per_block, cudaStream_t stream);
 cudaError_t configure_control_step_kernels(size_t max_dynamic_smem);
+// FP64 energy / momentum audit (audit.cuh) of the state the control-step
+// launch with the same parameters committed; p.audit must be set.
+cudaError_t launch_audit_step(const StepParams& p, const WarpLayout& layout, bool fp64_inertia, int warps_per_block,
+                              cudaStream_t stream);
 size_t control_step_table_bytes();
 
 namespace rt {

@@ -99,5 +99,8 @@ size_t scene_step_smem_bytes(bool compensated = false);
 size_t scene_workspace_words();
 cudaError_t configure_scene_step_kernel();
 cudaError_t launch_scene_step(const SceneParams& p, cudaStream_t stream);
+// FP64 energy / momentum audit (audit.cuh) of the bodies the scene launch
+// with the same parameters committed; p.audit must be set.
+cudaError_t launch_scene_audit(const SceneParams& p, cudaStream_t stream);
 
 }  // namespace numi

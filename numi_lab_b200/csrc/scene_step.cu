@@ -16,6 +16,18 @@ __global__ void __launch_bounds__(32, 16) scene_step_kernel(SceneParams p) {
     scene_step_item<kComp, kConvex>(p, reinterpret_cast<float*>(smem4), item, env);
 }
 
+// The FP64 audit of the bodies each environment committed in the launch with
+// the same parameters.
+__global__ void __launch_bounds__(32) scene_audit_kernel(SceneParams p) {
+    const int item = blockIdx.x;
+    if (item >= p.env_count || p.audit == nullptr) return;
+    const int env = p.env_index != nullptr ? p.env_index[item] : item;
+    const SceneModel& M = *p.model;
+    const bool reset = p.reset_masks != nullptr && p.reset_masks[item] != 0u;
+    audit_scene(M, p.q + static_cast<size_t>(env) * M.nb * 7, p.v + static_cast<size_t>(env) * M.nb * 6,
+                p.audit + static_cast<size_t>(env) * kAuditWords, reset, static_cast<int>(threadIdx.x));
+}
+
 }  // namespace
 
 size_t scene_step_smem_bytes(bool compensated) {
@@ -45,6 +57,11 @@ cudaError_t configure_scene_step_kernel() {
                                                 static_cast<int>(scene_step_smem_bytes(compensated)));
                 });
     return e;
+}
+
+cudaError_t launch_scene_audit(const SceneParams& p, cudaStream_t stream) {
+    scene_audit_kernel<<<p.env_count, 32, 0, stream>>>(p);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_scene_step(const SceneParams& p, cudaStream_t stream) {

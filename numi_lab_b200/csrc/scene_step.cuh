@@ -1395,14 +1395,16 @@ __device__ __forceinline__ float3 sym3_mul(const float* S, float3 x) {
     return f3(S[0] * x.x + S[1] * x.y + S[3] * x.z, S[1] * x.x + S[2] * x.y + S[4] * x.z, S[3] * x.x + S[4] * x.y + S[5] * x.z);
 }
 
-// FP64 audit of the committed bodies (audit.cuh), out of line.
-__device__ __noinline__ void audit_scene(const SceneModel& M, const float* s, double* rec, bool reset, int lane) {
+// FP64 audit of one environment's bodies (audit.cuh), read from its
+// resident q [body][7] and v [body][6]; run by its own kernel after the
+// control step.
+__device__ void audit_scene(const SceneModel& M, const float* q, const float* v, double* rec, bool reset, int lane) {
     AuditSum a{};
     for (int b = lane; b < M.nb; b += 32) {
         const float4 ii = M.inv_inertia[b];
         const float3 id = f3(ii.x > 0.0f ? 1.0f / ii.x : 0.0f, ii.y > 0.0f ? 1.0f / ii.y : 0.0f, ii.z > 0.0f ? 1.0f / ii.z : 0.0f);
-        audit_body(a, M.mass[b].x, ld3(s + kOffPos + b * 3), ld4(s + kOffQuat + b * 4), ld3(s + kOffLin + b * 3),
-                   ld3(s + kOffAng + b * 3), id, f3(0.0f, 0.0f, 0.0f), M.gravity);
+        audit_body(a, M.mass[b].x, ld3(q + b * 7), ld4(q + b * 7 + 3), ld3(v + b * 6), ld3(v + b * 6 + 3), id, f3(0.0f, 0.0f, 0.0f),
+                   M.gravity);
     }
     audit_commit(a, rec, reset, lane);
 }
@@ -1993,7 +1995,6 @@ __device__ __forceinline__ void scene_step_item(const SceneParams& p, float* s, 
     float* qd = p.q + static_cast<size_t>(env) * nq;
     float* vd = p.v + static_cast<size_t>(env) * nv;
     float* obs = p.observations ? p.observations + static_cast<size_t>(item) * (nq + nv) : nullptr;
-    if (success && p.audit != nullptr) audit_scene(M, s, p.audit + static_cast<size_t>(env) * kAuditWords, reset, lane);
     if (success) {
         for (int b = lane; b < nb; b += 32) {
             st3(qd + b * 7, ld3(s + kOffPos + b * 3));

@@ -26,7 +26,53 @@ __global__ void __launch_bounds__(128, 3) control_step_kernel(StepParams p, Warp
                                           item, env);
 }
 
+// The FP64 audit of the state each environment committed in the launch
+// with the same parameters (one warp per environment, like that launch).
+template <typename R>
+__global__ void __launch_bounds__(128) audit_step_kernel(StepParams p, WarpLayout layout, int warps_per_block) {
+    extern __shared__ float4 smem4[];
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(&p.model->tables);
+        uint4* dst = reinterpret_cast<uint4*>(smem4);
+        for (int i = threadIdx.x; i < static_cast<int>(sizeof(DeviceTables) / 16); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5;
+    const int item = blockIdx.x * warps_per_block + warp;
+    if (item >= p.env_count || p.audit == nullptr) return;
+    const int env = p.env_index != nullptr ? p.env_index[item] : item;
+    const int lane = threadIdx.x & 31;
+    const DeviceModel& M = *p.model;
+    Warp w;
+    w.lane = lane;
+    w.T = reinterpret_cast<const DeviceTables*>(smem4);
+    w.s = reinterpret_cast<float*>(smem4) + sizeof(DeviceTables) / sizeof(float) + warp * layout.total;
+    w.L = &layout;
+    w.M = p.model;
+    const float* q = p.q + static_cast<size_t>(env) * M.nq;
+    const float* v = p.v + static_cast<size_t>(env) * M.nv;
+    for (int i = lane; i < M.nq; i += 32) w.s[layout.q + i] = q[i];
+    for (int i = lane; i < M.nv; i += 32) w.s[layout.v + i] = v[i];
+    if (lane == 0) w.s[layout.misc] = 0.0f;
+    BodyConst bc;
+    if (lane < M.nb) load_body(M, lane, bc);
+    __syncwarp();
+    const bool reset = p.reset_masks != nullptr && p.reset_masks[item] != 0u;
+    audit_articulated<R>(w, bc, p.audit + static_cast<size_t>(env) * kAuditWords, reset);
+}
+
 }  // namespace
+
+cudaError_t launch_audit_step(const StepParams& p, const WarpLayout& layout, bool fp64_inertia, int warps_per_block,
+                              cudaStream_t stream) {
+    const int blocks = (p.env_count + warps_per_block - 1) / warps_per_block;
+    const size_t smem = sizeof(DeviceTables) + static_cast<size_t>(layout.total) * sizeof(float) * warps_per_block;
+    if (fp64_inertia)
+        audit_step_kernel<double><<<blocks, 32 * warps_per_block, smem, stream>>>(p, layout, warps_per_block);
+    else
+        audit_step_kernel<float><<<blocks, 32 * warps_per_block, smem, stream>>>(p, layout, warps_per_block);
+    return cudaGetLastError();
+}
 
 size_t control_step_table_bytes() { return sizeof(DeviceTables); }
 
@@ -86,6 +132,8 @@ cudaError_t configure_control_step_kernels(size_t max_dynamic_smem) {
                 e = for_kernel(contact, precision, [&](auto kernel) {
                     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
                 });
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(audit_step_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(audit_step_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     return e;
 }
 

@@ -1855,11 +1855,11 @@ __device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState<R>
     return warp_ok(misc);
 }
 
-// FP64 audit of the committed state (audit.cuh): forward kinematics of the
-// committed q and v, then each lane's body.  Kept out of line so that the
-// control step's register allocation does not carry it.
+// FP64 audit of one environment's state (audit.cuh): forward kinematics of
+// the q and v in the warp's layout, then each lane's body.  Run by its own
+// kernel after the control step, so the step kernel carries none of it.
 template <typename R>
-__device__ __noinline__ void audit_articulated(const Warp& w, const BodyConst& bc, double* rec, bool reset) {
+__device__ void audit_articulated(const Warp& w, const BodyConst& bc, double* rec, bool reset) {
     const DeviceModel& M = *w.M;
     BodyState<R> st;
     kinematics(w, bc, st);
@@ -1951,7 +1951,6 @@ __device__ __forceinline__ void control_step_item(const StepParams& p, const War
     }
     const unsigned code = static_cast<unsigned>(as_int(misc[kMiscStatus]));
     const bool success = code == MR_STEP_SUCCESS;
-    if (p.audit != nullptr && success) audit_articulated<R>(w, bc, p.audit + static_cast<size_t>(env) * kAuditWords, reset);
     // Capture + commit: a failed step publishes (and keeps) its checkpoint.
     float* qd = p.q + static_cast<size_t>(env) * nq;
     float* vd = p.v + static_cast<size_t>(env) * nv;
