@@ -1076,7 +1076,8 @@ def run_headline(args, rank: int, local_rank: int, world_size: int) -> None:
     bytes_per_env_step = _algorithmic_bytes_per_env_step(world.nq, world.nv, world.action_count, mean_points, mean_manifolds)
     achieved = bytes_per_env_step * envs / (kernel_ms / 1e3) / 1e9
     peaks = _measured_peaks()
-    traffic = _profile_value("traffic_bytes_per_launch")
+    # DRAM bytes of the control step's launches (both environment chains).
+    traffic = _profile_value("traffic_bytes_per_control_step")
     # Issue roofline: the kernel's warp instructions per env-step (from the
     # committed ncu summary) at the measured control-step time, against the
     # measured warp-instruction issue rate of this device.
