@@ -688,7 +688,7 @@ typedef struct MRServerConfigC {
     uint32_t final_velocity_iterations;
     float control_timestep_seconds;
     uint32_t max_envs_per_source;      /* slot pool size per world source      */
-    uint32_t reserved;
+    uint32_t control_steps_per_tick;   /* control steps one tick advances (0: 1) */
 } MRServerConfigC;
 
 typedef struct MRServerRequestC {
@@ -726,8 +726,12 @@ MR_API void mr_server_destroy(MRServerHandle* server);
 /* Slot-pool size and action width of a world source. */
 MR_API int mr_server_capacity(const MRServerHandle* server, uint32_t source, uint32_t* slots, uint32_t* action_count);
 MR_API int mr_server_submit(MRServerHandle* server, const MRServerRequestC* request, uint64_t* request_id);
-/* Admits waiting requests, advances every admitted request by one control
- * step and retires the finished ones; returns the work of this tick. */
+/* Admits waiting requests (slots and a range of the pool's preallocated
+ * action arena: no device allocation), advances every admitted request by
+ * control_steps_per_tick control steps (fewer when its horizon ends first;
+ * one launch per pool and step, the pools on their own streams), retires
+ * the finished ones, and synchronises once.  active_envs receives the
+ * environment-steps this tick advanced. */
 MR_API int mr_server_tick(MRServerHandle* server, uint32_t* active_requests, uint32_t* active_envs);
 /* Completions not reported yet, oldest first. */
 MR_API int mr_server_poll(MRServerHandle* server, MRServerCompletionC* out, uint32_t capacity, uint32_t* count);

@@ -41,6 +41,22 @@ __global__ void scatter_rows_kernel(float* __restrict__ dst, const float* __rest
     }
 }
 
+// Staged reset rows [i][nq + nv + 1] -> q, v and friction of slot index[i].
+__global__ void scatter_staged_kernel(float* __restrict__ q, float* __restrict__ v, float* __restrict__ friction,
+                                      const float* __restrict__ stage, const std::int32_t* __restrict__ index, int rows, int nq,
+                                      int nv) {
+    const int width = nq + nv + 1;
+    const int total = rows * width;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+        const int r = k / width, c = k - r * width;
+        const size_t slot = static_cast<size_t>(index[r]);
+        const float x = stage[k];
+        if (c < nq) q[slot * nq + c] = x;
+        else if (c < nq + nv) v[slot * nv + (c - nq)] = x;
+        else friction[slot] = x;
+    }
+}
+
 // slots src[index[i]] -> rows dst[i] (width floats).
 __global__ void gather_rows_kernel(float* __restrict__ dst, const float* __restrict__ src, const std::int32_t* __restrict__ index,
                                    int rows, int width) {
@@ -54,10 +70,54 @@ __global__ void gather_rows_kernel(float* __restrict__ dst, const float* __restr
 int grid_for(int total) { return std::max(1, std::min(1184, (total + 255) / 256)); }
 
 constexpr std::size_t kPoolCount = 3;  // chain, tree, pile
+// Longest horizon the action arena is sized for (longer requests still fit
+// when the arena has room: it is a shared pool, not per request).
+constexpr std::size_t kArenaHorizon = 500;
 
 double now_seconds() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
+
+// First-fit allocator over a preallocated device arena (offsets in floats):
+// admission and retirement move ranges, never device memory.
+struct Arena {
+    std::map<std::size_t, std::size_t> free_ranges;  // offset -> length
+    void reset(std::size_t words) {
+        free_ranges.clear();
+        if (words) free_ranges[0] = words;
+    }
+    bool take(std::size_t words, std::size_t& at) {
+        if (words == 0) {
+            at = 0;
+            return true;
+        }
+        for (auto it = free_ranges.begin(); it != free_ranges.end(); ++it) {
+            if (it->second < words) continue;
+            at = it->first;
+            const std::size_t rest = it->second - words;
+            free_ranges.erase(it);
+            if (rest) free_ranges[at + words] = rest;
+            return true;
+        }
+        return false;
+    }
+    void give(std::size_t at, std::size_t words) {
+        if (words == 0) return;
+        auto next = free_ranges.lower_bound(at);
+        if (next != free_ranges.end() && at + words == next->first) {
+            words += next->second;
+            next = free_ranges.erase(next);
+        }
+        if (next != free_ranges.begin()) {
+            auto prev = std::prev(next);
+            if (prev->first + prev->second == at) {
+                prev->second += words;
+                return;
+            }
+        }
+        free_ranges[at] = words;
+    }
+};
 
 struct Request {
     std::uint64_t id = 0;
@@ -65,16 +125,15 @@ struct Request {
     std::uint32_t envs = 0;
     std::uint32_t horizon = 0;
     std::uint64_t seed = 0;
-    std::vector<float> host_actions;  // [horizon][envs][actions]
-    DeviceBuffer<float> d_actions;
-    DeviceBuffer<std::int32_t> d_slots;
+    std::vector<float> host_actions;  // [horizon][envs][actions], until admitted
+    std::size_t arena_at = 0, arena_words = 0;  // actions in the pool's arena
     std::vector<std::int32_t> slots;
     std::uint32_t step = 0;
     std::uint32_t failed_env_steps = 0;
     std::uint32_t first_failure_status = 0;
     double t_submit = 0.0, t_admit = 0.0, t_finish = 0.0;
     std::vector<float> final_q, final_v;
-    std::size_t device_bytes = 0;
+    std::size_t out_at = 0;  // rows in the pool's result staging while retiring
 };
 
 struct Pool {
@@ -90,15 +149,24 @@ struct Pool {
     DeviceBuffer<numi::SceneModel> d_smodel;
     DeviceBuffer<float> d_q, d_v, d_manifolds, d_friction, d_workspace;
     DeviceBuffer<std::uint32_t> d_mcount;  // live manifolds per slot (piles)
-    DeviceBuffer<std::int32_t> d_index;
+    // Preallocated per pool: request actions, the per-step item -> slot
+    // index and action rows of a tick, statuses, reset-state staging of the
+    // tick's admissions and result staging of its retirements.
+    DeviceBuffer<float> d_arena;
+    Arena arena;
+    DeviceBuffer<std::int32_t> d_index, d_admit_slots, d_out_slots;
     DeviceBuffer<const float*> d_rows;
     DeviceBuffer<std::uint32_t> d_status, d_stats;
-    PinnedBuffer<std::int32_t> h_index;
+    DeviceBuffer<float> d_stage, d_out;
+    PinnedBuffer<std::int32_t> h_index, h_admit_slots, h_out_slots;
     PinnedBuffer<const float*> h_rows;
     PinnedBuffer<std::uint32_t> h_status;
+    PinnedBuffer<float> h_stage, h_out;
     std::vector<std::int32_t> free_slots;  // kept sorted descending; back() is the lowest
     std::vector<Request*> active;          // admission order
-    std::uint32_t launched_items = 0;      // of the current tick
+    std::vector<Request*> admitted;        // admitted in this tick (reset states staged)
+    std::vector<std::uint32_t> step_items; // items of each control step of the tick
+    std::uint32_t tick_env_steps = 0;
 
     std::size_t slot_bytes() const {
         return (static_cast<std::size_t>(nq) + nv + manifold_words + workspace_words + 1 + (scene ? 1 : 0)) * sizeof(float);
@@ -113,6 +181,7 @@ struct Pool {
 struct MRServerHandle {
     MRServerConfigC config{};
     float h = 0.0f;
+    std::uint32_t steps_per_tick = 1;
     std::map<std::uint32_t, std::unique_ptr<Pool>> pools;
     std::deque<std::unique_ptr<Request>> pending;
     std::vector<std::unique_ptr<Request>> running;
@@ -148,11 +217,16 @@ struct MRServerHandle {
             p->manifold_words = p->model.world.pair_count * numi::kManifoldWords;
         }
         // Slots: the configured maximum, bounded by this pool's share of the
-        // HBM budget (half of it split across the pools; the rest holds actions).
+        // HBM budget (half of it split across the pools); the action arena
+        // takes the pool's share of the other half, at most what a full
+        // pool of kArenaHorizon-step requests needs.
         const std::size_t share = config.hbm_budget_bytes / (2 * kPoolCount);
         p->capacity = static_cast<std::uint32_t>(std::min<std::size_t>(config.max_envs_per_source, share / p->slot_bytes()));
         if (p->capacity == 0) throw std::invalid_argument("the HBM budget holds no environment of source " + std::to_string(source));
-        budget_used += static_cast<std::size_t>(p->capacity) * p->slot_bytes();
+        const std::size_t cap = p->capacity;
+        const std::size_t arena_words =
+            std::min<std::size_t>(share / sizeof(float), cap * kArenaHorizon * static_cast<std::size_t>(p->na));
+        budget_used += cap * p->slot_bytes() + arena_words * sizeof(float);
         check(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking), "stream");
         if (p->scene) {
             p->d_smodel.resize(1);
@@ -161,7 +235,6 @@ struct MRServerHandle {
             p->d_model.resize(1);
             check(cudaMemcpy(p->d_model.ptr, &p->plan.dmodel, sizeof(numi::DeviceModel), cudaMemcpyHostToDevice), "upload model");
         }
-        const std::size_t cap = p->capacity;
         p->d_q.resize(cap * p->nq);
         p->d_v.resize(cap * p->nv);
         if (p->manifold_words) p->d_manifolds.resize(cap * p->manifold_words);
@@ -170,163 +243,218 @@ struct MRServerHandle {
             p->d_workspace.resize(cap * p->workspace_words);
         }
         p->d_friction.resize(cap);
-        p->d_index.resize(cap);
-        p->d_rows.resize(cap);
-        p->d_status.resize(cap);
+        p->d_arena.resize(std::max<std::size_t>(arena_words, 1));
+        p->arena.reset(arena_words);
+        const std::size_t items = cap * steps_per_tick;
+        p->d_index.resize(items);
+        p->d_rows.resize(items);
+        p->d_status.resize(items);
         p->d_stats.resize(numi::kStatCount);
-        p->h_index.resize(cap);
-        p->h_rows.resize(cap);
-        p->h_status.resize(cap);
+        p->d_admit_slots.resize(cap);
+        p->d_out_slots.resize(cap);
+        const std::size_t row = static_cast<std::size_t>(p->nq) + p->nv + 1;
+        p->d_stage.resize(cap * row);
+        p->d_out.resize(cap * (p->nq + p->nv));
+        p->h_index.resize(items);
+        p->h_rows.resize(items);
+        p->h_status.resize(items);
+        p->h_admit_slots.resize(cap);
+        p->h_out_slots.resize(cap);
+        p->h_stage.resize(cap * row);
+        p->h_out.resize(cap * (p->nq + p->nv));
         for (std::int32_t s = static_cast<std::int32_t>(cap) - 1; s >= 0; --s) p->free_slots.push_back(s);
         pools[source] = std::move(p);
     }
 
+    // Reserves slots and arena room; stages the request's reset states and
+    // enqueues its actions (no device allocation, no synchronisation).
     bool try_admit(Request& r) {
         Pool& p = pool(r.source);
         if (p.free_slots.size() < r.envs) return false;
-        const std::size_t bytes = r.host_actions.size() * sizeof(float) + r.envs * sizeof(std::int32_t);
-        if (budget_used + bytes > config.hbm_budget_bytes) return false;
-        budget_used += bytes;
-        r.device_bytes = bytes;
+        const std::size_t words = r.host_actions.size();
+        std::size_t at = 0;
+        if (!p.arena.take(words, at)) return false;
+        r.arena_at = at;
+        r.arena_words = words;
         for (std::uint32_t e = 0; e < r.envs; ++e) {
             r.slots.push_back(p.free_slots.back());
             p.free_slots.pop_back();
         }
-        r.d_actions.resize(r.host_actions.size());
-        r.d_slots.resize(r.envs);
-        check(cudaMemcpyAsync(r.d_actions.ptr, r.host_actions.data(), r.host_actions.size() * sizeof(float), cudaMemcpyHostToDevice,
-                              p.stream), "request actions H2D");
-        check(cudaMemcpyAsync(r.d_slots.ptr, r.slots.data(), r.envs * sizeof(std::int32_t), cudaMemcpyHostToDevice, p.stream),
-              "request slots H2D");
-        // Reset state of each environment of the request, scattered into its slots.
-        std::vector<float> hq(static_cast<std::size_t>(r.envs) * p.nq), hv(static_cast<std::size_t>(r.envs) * p.nv), hf(r.envs);
-        for (std::uint32_t e = 0; e < r.envs; ++e)
-            numi::sample_reset_state(p.model, r.seed, e, &hq[static_cast<std::size_t>(e) * p.nq],
-                                     &hv[static_cast<std::size_t>(e) * p.nv], &hf[e]);
-        DeviceBuffer<float> tmp_q, tmp_v, tmp_f;
-        tmp_q.resize(hq.size());
-        tmp_v.resize(hv.size());
-        tmp_f.resize(hf.size());
-        check(cudaMemcpyAsync(tmp_q.ptr, hq.data(), hq.size() * sizeof(float), cudaMemcpyHostToDevice, p.stream), "q H2D");
-        check(cudaMemcpyAsync(tmp_v.ptr, hv.data(), hv.size() * sizeof(float), cudaMemcpyHostToDevice, p.stream), "v H2D");
-        check(cudaMemcpyAsync(tmp_f.ptr, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice, p.stream), "friction H2D");
-        const int envs = static_cast<int>(r.envs);
-        scatter_rows_kernel<<<grid_for(envs * p.nq), 256, 0, p.stream>>>(p.d_q.ptr, tmp_q.ptr, r.d_slots.ptr, envs, p.nq);
-        scatter_rows_kernel<<<grid_for(envs * p.nv), 256, 0, p.stream>>>(p.d_v.ptr, tmp_v.ptr, r.d_slots.ptr, envs, p.nv);
-        scatter_rows_kernel<<<grid_for(envs), 256, 0, p.stream>>>(p.d_friction.ptr, tmp_f.ptr, r.d_slots.ptr, envs, 1);
-        if (p.manifold_words)
-            scatter_rows_kernel<<<grid_for(envs * p.manifold_words), 256, 0, p.stream>>>(p.d_manifolds.ptr, nullptr, r.d_slots.ptr,
-                                                                                         envs, p.manifold_words);
-        if (p.scene)  // no live manifolds (zero words are a zero count)
-            scatter_rows_kernel<<<grid_for(envs), 256, 0, p.stream>>>(reinterpret_cast<float*>(p.d_mcount.ptr), nullptr,
-                                                                      r.d_slots.ptr, envs, 1);
-        check(cudaGetLastError(), "admission scatter");
-        check(cudaStreamSynchronize(p.stream), "admission");
+        if (words)  // from pageable memory: the span is consumed when the call returns
+            check(cudaMemcpyAsync(p.d_arena.ptr + at, r.host_actions.data(), words * sizeof(float), cudaMemcpyHostToDevice, p.stream),
+                  "request actions H2D");
+        r.host_actions.clear();
+        r.host_actions.shrink_to_fit();
+        // Reset states packed after the tick's earlier admissions:
+        // [env][nq + nv + 1 (friction)].
+        std::size_t staged = 0;
+        for (Request* a : p.admitted) staged += a->envs;
+        const std::size_t row = static_cast<std::size_t>(p.nq) + p.nv + 1;
+        for (std::uint32_t e = 0; e < r.envs; ++e) {
+            float* dst = p.h_stage.ptr + (staged + e) * row;
+            numi::sample_reset_state(p.model, r.seed, e, dst, dst + p.nq, dst + p.nq + p.nv);
+            p.h_admit_slots.ptr[staged + e] = r.slots[e];
+        }
         r.t_admit = now_seconds();
+        p.admitted.push_back(&r);
         p.active.push_back(&r);
         return true;
     }
 
+    // The tick's admissions of a pool: one staging copy and one scatter per
+    // field into their slots.
+    void scatter_admissions(Pool& p) {
+        std::size_t n = 0;
+        for (Request* a : p.admitted) n += a->envs;
+        if (n == 0) return;
+        const std::size_t row = static_cast<std::size_t>(p.nq) + p.nv + 1;
+        check(cudaMemcpyAsync(p.d_stage.ptr, p.h_stage.ptr, n * row * sizeof(float), cudaMemcpyHostToDevice, p.stream), "reset H2D");
+        check(cudaMemcpyAsync(p.d_admit_slots.ptr, p.h_admit_slots.ptr, n * sizeof(std::int32_t), cudaMemcpyHostToDevice, p.stream),
+              "slots H2D");
+        const int envs = static_cast<int>(n);
+        scatter_staged_kernel<<<grid_for(envs * static_cast<int>(row)), 256, 0, p.stream>>>(
+            p.d_q.ptr, p.d_v.ptr, p.d_friction.ptr, p.d_stage.ptr, p.d_admit_slots.ptr, envs, static_cast<int>(p.nq),
+            static_cast<int>(p.nv));
+        if (p.manifold_words)
+            scatter_rows_kernel<<<grid_for(envs * static_cast<int>(p.manifold_words)), 256, 0, p.stream>>>(
+                p.d_manifolds.ptr, nullptr, p.d_admit_slots.ptr, envs, static_cast<int>(p.manifold_words));
+        if (p.scene)  // no live manifolds (zero words are a zero count)
+            scatter_rows_kernel<<<grid_for(envs), 256, 0, p.stream>>>(reinterpret_cast<float*>(p.d_mcount.ptr), nullptr,
+                                                                      p.d_admit_slots.ptr, envs, 1);
+        check(cudaGetLastError(), "admission scatter");
+        p.admitted.clear();
+    }
+
+    // Up to steps_per_tick control steps of every active request of the
+    // pool (a request stops at its horizon), one launch per step.
     void launch(Pool& p) {
-        p.launched_items = 0;
+        p.step_items.assign(steps_per_tick, 0);
+        p.tick_env_steps = 0;
         if (p.active.empty()) return;
         std::uint32_t n = 0;
-        for (Request* r : p.active) {
-            const float* base = r->d_actions.ptr + static_cast<std::size_t>(r->step) * r->envs * p.na;
-            for (std::uint32_t e = 0; e < r->envs; ++e) {
-                p.h_index.ptr[n] = r->slots[e];
-                p.h_rows.ptr[n] = base + static_cast<std::size_t>(e) * p.na;
-                ++n;
+        for (std::uint32_t j = 0; j < steps_per_tick; ++j) {
+            std::uint32_t items = 0;
+            for (Request* r : p.active) {
+                if (r->step + j >= r->horizon) continue;
+                const float* base = p.d_arena.ptr + r->arena_at + static_cast<std::size_t>(r->step + j) * r->envs * p.na;
+                for (std::uint32_t e = 0; e < r->envs; ++e) {
+                    p.h_index.ptr[n] = r->slots[e];
+                    p.h_rows.ptr[n] = base + static_cast<std::size_t>(e) * p.na;
+                    ++n;
+                    ++items;
+                }
             }
+            p.step_items[j] = items;
         }
+        p.tick_env_steps = n;
+        if (n == 0) return;
         check(cudaMemcpyAsync(p.d_index.ptr, p.h_index.ptr, n * sizeof(std::int32_t), cudaMemcpyHostToDevice, p.stream), "index H2D");
         check(cudaMemcpyAsync(p.d_rows.ptr, p.h_rows.ptr, n * sizeof(const float*), cudaMemcpyHostToDevice, p.stream), "rows H2D");
         check(cudaMemsetAsync(p.d_stats.ptr, 0, numi::kStatCount * sizeof(std::uint32_t), p.stream), "clear stats");
-        if (p.scene) {
-            numi::SceneParams sp{};
-            sp.model = p.d_smodel.ptr;
-            sp.q = p.d_q.ptr;
-            sp.v = p.d_v.ptr;
-            sp.manifolds = p.d_manifolds.ptr;
-            sp.manifold_count = p.d_mcount.ptr;
-            sp.reset_q = p.d_q.ptr;  // no resets inside a request
-            sp.reset_v = p.d_v.ptr;
-            sp.friction_scale = p.d_friction.ptr;
-            sp.env_index = p.d_index.ptr;
-            sp.status_codes = p.d_status.ptr;
-            sp.stats = p.d_stats.ptr;
-            sp.workspace = p.d_workspace.ptr;
-            sp.env_count = static_cast<int>(n);
-            sp.substeps = static_cast<int>(config.physics_substeps);
-            sp.velocity_iterations = static_cast<int>(config.velocity_iterations);
-            sp.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
-            sp.support_mapped = p.smodel.support_mapped;
-            check(numi::launch_scene_step(sp, p.stream), "scene step launch");
-        } else {
-        numi::StepParams sp{};
-        sp.model = p.d_model.ptr;
-        sp.q = p.d_q.ptr;
-        sp.v = p.d_v.ptr;
-        sp.manifolds = p.d_manifolds.ptr;
-        sp.reset_q = p.d_q.ptr;  // no resets inside a request
-        sp.reset_v = p.d_v.ptr;
-        sp.friction_scale = p.d_friction.ptr;
-        sp.actions = nullptr;
-        sp.action_rows = p.d_rows.ptr;
-        sp.env_index = p.d_index.ptr;
-        sp.status_codes = p.d_status.ptr;
-        sp.stats = p.d_stats.ptr;
-        sp.env_count = static_cast<int>(n);
-        sp.substeps = static_cast<int>(config.physics_substeps);
-        sp.velocity_iterations = static_cast<int>(config.velocity_iterations);
-        sp.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
-        check(numi::launch_control_step(sp, p.plan.layout, p.plan.contact, MR_PRECISION_FP32, p.plan.warps_per_block[0], p.stream),
-              "control step launch");
+        std::uint32_t off = 0;
+        for (std::uint32_t j = 0; j < steps_per_tick; ++j) {
+            const std::uint32_t items = p.step_items[j];
+            if (items == 0) break;
+            if (p.scene) {
+                numi::SceneParams sp{};
+                sp.model = p.d_smodel.ptr;
+                sp.q = p.d_q.ptr;
+                sp.v = p.d_v.ptr;
+                sp.manifolds = p.d_manifolds.ptr;
+                sp.manifold_count = p.d_mcount.ptr;
+                sp.reset_q = p.d_q.ptr;  // no resets inside a request
+                sp.reset_v = p.d_v.ptr;
+                sp.friction_scale = p.d_friction.ptr;
+                sp.env_index = p.d_index.ptr + off;
+                sp.status_codes = p.d_status.ptr + off;
+                sp.stats = p.d_stats.ptr;
+                sp.workspace = p.d_workspace.ptr;
+                sp.env_count = static_cast<int>(items);
+                sp.substeps = static_cast<int>(config.physics_substeps);
+                sp.velocity_iterations = static_cast<int>(config.velocity_iterations);
+                sp.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
+                sp.support_mapped = p.smodel.support_mapped;
+                check(numi::launch_scene_step(sp, p.stream), "scene step launch");
+            } else {
+                numi::StepParams sp{};
+                sp.model = p.d_model.ptr;
+                sp.q = p.d_q.ptr;
+                sp.v = p.d_v.ptr;
+                sp.manifolds = p.d_manifolds.ptr;
+                sp.reset_q = p.d_q.ptr;  // no resets inside a request
+                sp.reset_v = p.d_v.ptr;
+                sp.friction_scale = p.d_friction.ptr;
+                sp.actions = nullptr;
+                sp.action_rows = p.d_rows.ptr + off;
+                sp.env_index = p.d_index.ptr + off;
+                sp.status_codes = p.d_status.ptr + off;
+                sp.stats = p.d_stats.ptr;
+                sp.env_count = static_cast<int>(items);
+                sp.substeps = static_cast<int>(config.physics_substeps);
+                sp.velocity_iterations = static_cast<int>(config.velocity_iterations);
+                sp.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
+                check(numi::launch_control_step(sp, p.plan.layout, p.plan.contact, MR_PRECISION_FP32, p.plan.warps_per_block[0],
+                                                p.stream),
+                      "control step launch");
+            }
+            off += items;
         }
         check(cudaMemcpyAsync(p.h_status.ptr, p.d_status.ptr, n * sizeof(std::uint32_t), cudaMemcpyDeviceToHost, p.stream),
               "status D2H");
-        p.launched_items = n;
+        // Final states of the requests this tick completes, gathered into the
+        // result staging and copied out with the statuses.
+        std::size_t rows = 0;
+        for (Request* r : p.active) {
+            if (r->step + steps_per_tick < r->horizon) continue;
+            r->out_at = rows;
+            for (std::uint32_t e = 0; e < r->envs; ++e) p.h_out_slots.ptr[rows + e] = r->slots[e];
+            rows += r->envs;
+        }
+        if (rows) {
+            const int m = static_cast<int>(rows);
+            check(cudaMemcpyAsync(p.d_out_slots.ptr, p.h_out_slots.ptr, rows * sizeof(std::int32_t), cudaMemcpyHostToDevice, p.stream),
+                  "result slots H2D");
+            gather_rows_kernel<<<grid_for(m * static_cast<int>(p.nq)), 256, 0, p.stream>>>(p.d_out.ptr, p.d_q.ptr, p.d_out_slots.ptr, m,
+                                                                                          static_cast<int>(p.nq));
+            gather_rows_kernel<<<grid_for(m * static_cast<int>(p.nv)), 256, 0, p.stream>>>(
+                p.d_out.ptr + rows * p.nq, p.d_v.ptr, p.d_out_slots.ptr, m, static_cast<int>(p.nv));
+            check(cudaGetLastError(), "gather");
+            check(cudaMemcpyAsync(p.h_out.ptr, p.d_out.ptr, rows * (p.nq + p.nv) * sizeof(float), cudaMemcpyDeviceToHost, p.stream),
+                  "results D2H");
+        }
     }
 
     void retire(Pool& p, double t_now) {
-        std::uint32_t n = 0;
+        std::vector<std::uint32_t> off(steps_per_tick, 0);
+        for (std::uint32_t j = 1; j < steps_per_tick; ++j) off[j] = off[j - 1] + p.step_items[j - 1];
+        std::vector<std::uint32_t> seen(steps_per_tick, 0);
         std::vector<Request*> still;
+        std::size_t rows = 0;
+        for (Request* r : p.active) rows += (r->step + steps_per_tick >= r->horizon) ? r->envs : 0;
         for (Request* r : p.active) {
-            for (std::uint32_t e = 0; e < r->envs; ++e, ++n) {
-                const std::uint32_t code = p.h_status.ptr[n];
-                if (code != MR_STEP_SUCCESS) {
-                    if (r->failed_env_steps == 0) r->first_failure_status = code;
-                    ++r->failed_env_steps;
+            const std::uint32_t steps = std::min(steps_per_tick, r->horizon - r->step);
+            for (std::uint32_t j = 0; j < steps; ++j) {
+                for (std::uint32_t e = 0; e < r->envs; ++e) {
+                    const std::uint32_t code = p.h_status.ptr[off[j] + seen[j] + e];
+                    if (code != MR_STEP_SUCCESS) {
+                        if (r->failed_env_steps == 0) r->first_failure_status = code;
+                        ++r->failed_env_steps;
+                    }
                 }
+                seen[j] += r->envs;
             }
-            ++r->step;
-            completed_env_steps += r->envs;
+            r->step += steps;
+            completed_env_steps += static_cast<std::uint64_t>(r->envs) * steps;
             if (r->step < r->horizon) {
                 still.push_back(r);
                 continue;
             }
-            // Final state out, slots and memory back.
-            const int envs = static_cast<int>(r->envs);
-            DeviceBuffer<float> gq, gv;
-            gq.resize(r->envs * p.nq);
-            gv.resize(r->envs * p.nv);
-            gather_rows_kernel<<<grid_for(envs * p.nq), 256, 0, p.stream>>>(gq.ptr, p.d_q.ptr, r->d_slots.ptr, envs, p.nq);
-            gather_rows_kernel<<<grid_for(envs * p.nv), 256, 0, p.stream>>>(gv.ptr, p.d_v.ptr, r->d_slots.ptr, envs, p.nv);
-            check(cudaGetLastError(), "gather");
-            r->final_q.resize(r->envs * p.nq);
-            r->final_v.resize(r->envs * p.nv);
-            check(cudaMemcpyAsync(r->final_q.data(), gq.ptr, r->final_q.size() * sizeof(float), cudaMemcpyDeviceToHost, p.stream),
-                  "final q D2H");
-            check(cudaMemcpyAsync(r->final_v.data(), gv.ptr, r->final_v.size() * sizeof(float), cudaMemcpyDeviceToHost, p.stream),
-                  "final v D2H");
-            check(cudaStreamSynchronize(p.stream), "retire");
+            r->final_q.assign(p.h_out.ptr + r->out_at * p.nq, p.h_out.ptr + (r->out_at + r->envs) * p.nq);
+            r->final_v.assign(p.h_out.ptr + rows * p.nq + r->out_at * p.nv, p.h_out.ptr + rows * p.nq + (r->out_at + r->envs) * p.nv);
             r->t_finish = t_now;
             for (std::int32_t s : r->slots) p.free_slots.push_back(s);
             std::sort(p.free_slots.begin(), p.free_slots.end(), std::greater<std::int32_t>());
-            budget_used -= r->device_bytes;
-            r->d_actions.reset();
-            r->host_actions.clear();
-            r->host_actions.shrink_to_fit();
+            p.arena.give(r->arena_at, r->arena_words);
             for (auto it = running.begin(); it != running.end(); ++it)
                 if (it->get() == r) {
                     unreported.push_back(r->id);
@@ -354,6 +482,8 @@ MR_API MRServerHandle* mr_create_server(const MRServerConfigC* config) {
         server = std::make_unique<MRServerHandle>();
         server->config = *config;
         server->h = config->control_timestep_seconds / static_cast<float>(config->physics_substeps);
+        server->steps_per_tick = config->control_steps_per_tick ? config->control_steps_per_tick : 1u;
+        if (server->steps_per_tick > 64) throw std::invalid_argument("control_steps_per_tick must be at most 64");
         server->add_pool(MR_RUN_SOURCE_SYNTHETIC_CHAIN7);
         server->add_pool(MR_RUN_SOURCE_SYNTHETIC_TREE29);
         server->add_pool(MR_RUN_SOURCE_SYNTHETIC_PILE);
@@ -416,10 +546,13 @@ MR_API int mr_server_tick(MRServerHandle* server, uint32_t* active_requests, uin
         }
         std::uint32_t reqs = 0, envs = 0;
         for (auto& kv : server->pools) {
+            server->scatter_admissions(*kv.second);
             server->launch(*kv.second);
             reqs += static_cast<std::uint32_t>(kv.second->active.size());
-            envs += kv.second->launched_items;
+            envs += kv.second->tick_env_steps;
         }
+        // The tick's one synchronisation: statuses and results are in
+        // pinned host memory once the pools' streams drain.
         for (auto& kv : server->pools) check(cudaStreamSynchronize(kv.second->stream), "tick");
         const double t = now_seconds();
         for (auto& kv : server->pools) server->retire(*kv.second, t);

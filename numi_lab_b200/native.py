@@ -389,7 +389,7 @@ class ServerConfigC(ct.Structure):
         ("final_velocity_iterations", ct.c_uint32),
         ("control_timestep_seconds", ct.c_float),
         ("max_envs_per_source", ct.c_uint32),
-        ("reserved", ct.c_uint32),
+        ("control_steps_per_tick", ct.c_uint32),
     ]
 
 

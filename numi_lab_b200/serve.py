@@ -3,8 +3,10 @@
 A ``Server`` holds resident environment slots for the 7-DoF chain and the
 29-DoF tree on one GPU.  ``submit`` queues a request (world, env count,
 horizon, seed, actions); every ``tick`` admits waiting requests into free
-slots within the HBM budget, advances all admitted requests by one control
-step in one launch per world, and retires finished requests.  ``poll``
+slots within the HBM budget (request actions in a preallocated per-world
+arena), advances all admitted requests by ``steps_per_tick`` control steps
+(one launch per world and step), and retires finished requests; one
+synchronisation per tick.  ``poll``
 returns completions with queueing delay and latency; ``result`` returns a
 finished request's final state.
 
@@ -49,6 +51,7 @@ class Server:
         final_velocity_iterations: int = 0,
         control_dt: float = 0.02,
         max_envs_per_source: int = 8192,
+        steps_per_tick: int = 1,
         library: native.Bindings | None = None,
     ) -> None:
         self._lib = library or native.bindings()
@@ -58,6 +61,7 @@ class Server:
         cfg.physics_substeps = substeps
         cfg.velocity_iterations = velocity_iterations
         cfg.final_velocity_iterations = final_velocity_iterations
+        cfg.control_steps_per_tick = steps_per_tick
         cfg.control_timestep_seconds = control_dt
         cfg.max_envs_per_source = max_envs_per_source
         handle = self._lib.lib.mr_create_server(ct.byref(cfg))

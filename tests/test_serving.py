@@ -33,18 +33,21 @@ def _run_until_done(server, ids):
 
 
 @pytest.mark.gpu
-def test_request_result_is_the_same_alone_in_a_mix_and_through_a_rollout(cuda_device):
+@pytest.mark.parametrize("steps_per_tick", [1, 4])
+def test_request_result_is_the_same_alone_in_a_mix_and_through_a_rollout(cuda_device, steps_per_tick):
+    """With one or several control steps per tick (horizons that are not
+    multiples of it end mid-tick)."""
     import torch
 
     seed, envs, horizon = 11, 3, 6
-    with nb.Server(model_seed=seed, max_envs_per_source=256) as server:
+    with nb.Server(model_seed=seed, max_envs_per_source=256, steps_per_tick=steps_per_tick) as server:
         na = server.action_count("tree29")
         acts = (0.3 * np.random.default_rng(1).standard_normal((horizon, envs, na))).astype(np.float32)
         rid = server.submit("tree29", envs, horizon, seed, acts)
         _run_until_done(server, [rid])
         q_alone, v_alone = server.result(rid)
 
-    with nb.Server(model_seed=seed, max_envs_per_source=256) as server:
+    with nb.Server(model_seed=seed, max_envs_per_source=256, steps_per_tick=steps_per_tick) as server:
         other = []
         for k, (src, n, hz) in enumerate([("chain7", 17, 9), ("tree29", 5, 4), ("tree29", 9, 12), ("chain7", 2, 3)]):
             a = (0.3 * np.random.default_rng(100 + k).standard_normal((hz, n, server.action_count(src)))).astype(np.float32)
