@@ -323,6 +323,9 @@ def plain_aba_chain7(device) -> dict:
 SERVE_RATES = ((2000.0, 1.0), (400.0, 2.0), (100.0, 2.0), (25.0, 2.0))
 
 
+SERVE_STEPS_PER_TICK = 2  # control steps per server tick (1-8 measured within 3 % of each other)
+
+
 def measure_serving(rates=SERVE_RATES) -> dict:
     """Poisson request streams (the serving configuration: chain, tree and
     pile worlds, envs log-uniform 1-512, horizons U(10, 500)) against the
@@ -337,7 +340,8 @@ def measure_serving(rates=SERVE_RATES) -> dict:
     torch.cuda.set_device(0)
     results = {}
     for rate, window in rates:
-        with nb.Server(hbm_budget_bytes=120 * 10**9, model_seed=SEED, max_envs_per_source=16384) as server:
+        with nb.Server(hbm_budget_bytes=120 * 10**9, model_seed=SEED, max_envs_per_source=16384,
+                       steps_per_tick=SERVE_STEPS_PER_TICK) as server:
             reqs = poisson_requests(rate, window, seed=SEED + int(rate))
             results[str(int(rate))] = serve_arrivals(server, reqs, drain=True, time_limit_s=300.0)
     head = results[str(int(rates[0][0]))]
@@ -349,7 +353,8 @@ def measure_serving(rates=SERVE_RATES) -> dict:
         "queue_p50_s": head["queue_p50_s"],
         "queue_p99_s": head["queue_p99_s"],
         "config": {"workload": f"Poisson arrivals {rates[0][0]:.0f} req/s for {rates[0][1]:.0f} s, worlds chain7 | tree29 | pile, "
-                               "envs log-uniform 1-512, horizon U(10, 500), actions N(0, 0.3), 120 GB HBM budget, drained",
+                               "envs log-uniform 1-512, horizon U(10, 500), actions N(0, 0.3), 120 GB HBM budget, drained, "
+                               f"{SERVE_STEPS_PER_TICK} control steps per tick",
                    "rate_sweep_req_per_s": {k: {kk: v[kk] for kk in ("env_steps_per_s", "latency_p50_s", "latency_p99_s",
                                                                        "queue_p99_s", "completed")}
                                             for k, v in results.items()}},
