@@ -2040,14 +2040,6 @@ __device__ __forceinline__ void scene_step_item(const SceneParams& p, float* s, 
         atomicMax(p.stats + 4, static_cast<unsigned>(ai(misc[kSmCand])));
         atomicMax(p.stats + 5, static_cast<unsigned>(ai(misc[kSmIslands])));
     }
-    // The workspace (substep tables, contact records, narrowphase scratch) is
-    // dead once the control step has committed -- the next step writes every
-    // word before reading it -- so its L2 lines are dropped without being
-    // written back to HBM: of a launch's DRAM traffic these write-backs were
-    // the bulk (tens of KB per environment against ~20 KB of state).
-    __syncwarp();
-    for (int line = lane; line < kWsWords / 32; line += 32)
-        asm volatile("discard.global.L2 [%0], 128;" ::"l"(ws + static_cast<size_t>(line) * 32) : "memory");
 }
 
 }  // namespace
