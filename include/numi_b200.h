@@ -66,6 +66,14 @@ enum MRStepStatusCode {
     MR_STEP_CCD_CAPACITY_OVERFLOW = 13u
 };
 
+/* reference: include/metalrobo/engine_types.h:159-164 (same values). */
+enum MRSolverType {
+    MR_SOLVER_REFERENCE_FP64 = 0u,
+    MR_SOLVER_QUALITY_NEWTON = 1u,
+    MR_SOLVER_TEMPORAL_CONE = 2u,
+    MR_SOLVER_THROUGHPUT_PGS = 3u
+};
+
 /* reference: include/metalrobo/gpu_types.h:41-49 (same values). */
 enum MRShapeType {
     MR_SHAPE_SPHERE = 0u,
@@ -570,6 +578,96 @@ enum MRPrecisionModeC {
     MR_PRECISION_COMPENSATED = 2u
 };
 MR_API int mr_task_rollout_set_precision(MRTaskRolloutHandle* handle, uint32_t mode);
+
+/* Contact solver of a rollout (reference: MetalWorldSolverMode,
+ * include/metalrobo/MetalWorld.hpp:31-39, and MetalWorldQualityConfig,
+ * :41-52).  MR_SOLVER_TEMPORAL_CONE (default) runs the fixed-budget
+ * temporalCone sweeps; MR_SOLVER_QUALITY_NEWTON solves every substep's
+ * contact problem to convergence instead:
+ *
+ *   min 0.5 l' (G H^-1 G' + R) l + (G v_free - v_target)' l
+ *   s.t. l_n >= 0, ||l_t|| <= mu l_n
+ *
+ * with R = max(the ConstraintIR regularisation, regularization_floor) per
+ * row (the reference's CPU world uses minimumRegularization 1e-6,
+ * ArticulatedWorld.hpp:58), in FP64, by a semismooth Newton iteration with
+ * a direct (Cholesky) solve of its nv x nv system and an exact line search.
+ * The optimality measure is ||zeta - Y l|| / (1 + ||zeta|| + ||Y l||)
+ * (inf-norms) for the factor rows Y of G H^-1 G' = Y'Y and zeta the
+ * iterate (zeta = Y l at the solution).  A solve
+ * that does not reach `optimality_tolerance` within the budgets latches
+ * MR_STEP_DID_NOT_CONVERGE and the environment keeps its checkpoint, like
+ * any failed step.  Articulated contact worlds only (tree29); pile and
+ * stack worlds and batched rollouts keep temporalCone.  Zero / non-positive
+ * fields take the defaults in brackets.  Applies from the next advance. */
+typedef struct MRQualitySolverConfigC {
+    uint32_t maximum_newton_iterations;        /* [100]                                       */
+    uint32_t maximum_line_search_iterations;   /* [50] line-search evaluations per Newton step */
+    double optimality_tolerance;               /* [1e-9] on the optimality measure above       */
+    double line_search_tolerance;              /* [1e-12] directional derivative, relative     */
+    double regularization_floor;               /* [1e-6] per-row minimum of R                  */
+    double reserved;
+} MRQualitySolverConfigC;
+MR_API int mr_task_rollout_set_solver(MRTaskRolloutHandle* handle, uint32_t solver, const MRQualitySolverConfigC* quality);
+
+/* Certificates of the last advance's quality solves (all zero under
+ * temporalCone): the most Newton steps of one solve, the line-search
+ * evaluations summed, and the largest scaled optimality residual, cone
+ * violation max(-l_n, ||l_t|| - mu l_n) and conic complementarity
+ * |l' (G v - v_target + R l)| over every environment-substep (reference:
+ * MRUnifiedQualityStatusGPU certificates, unified_quality_shared.h:124-146). */
+typedef struct MRQualityDiagnosticsC {
+    uint32_t maximum_newton_iterations;
+    uint32_t line_search_iterations;
+    float maximum_scaled_optimality;
+    float maximum_cone_violation;
+    float maximum_complementarity;
+    uint32_t reserved[3];
+} MRQualityDiagnosticsC;
+MR_API int mr_task_rollout_quality_diagnostics(const MRTaskRolloutHandle* handle, MRQualityDiagnosticsC* out);
+
+/* Batched converged contact solve of independent dense problems (reference:
+ * solveMetalUnifiedQuality, include/metalrobo/MetalUnifiedQualitySolver.hpp:
+ * 85-90, whose problems also carry the dynamics operator and the Jacobian
+ * rather than the Delassus matrix).  Problem p has `nv` generalized
+ * velocities and contact_counts[p] (or, with null, `contact_capacity`)
+ * contacts; arrays are problem-major with the capacity as stride:
+ *   mass            [p][nv][nv]   symmetric positive definite H
+ *   jacobian        [p][3 cap][nv] rows normal, tangent, bitangent per contact
+ *   free_velocity   [p][nv]
+ *   target_velocity, regularization, warm_impulses (may be null): [p][3 cap]
+ *   friction        [p][cap]      mu >= 0 (0: frictionless)
+ * The two tangent regularisations of a frictional contact must be equal.
+ * Solves on the current device in FP64 (one warp per problem; 1 <= nv <= 64,
+ * cap <= 32) with the settings of `config` (null: defaults) and writes the
+ * impulses [p][3 cap], the post-impulse velocity v_free + H^-1 G' l [p][nv]
+ * and one result per problem (host arrays; the call is synchronous). */
+typedef struct MRQualityResultC {
+    uint32_t code;                 /* MRStepStatusCode: SUCCESS, DID_NOT_CONVERGE, FACTORIZATION_FAILED, NONFINITE_RESULT */
+    uint32_t newton_iterations;
+    uint32_t line_search_iterations;
+    uint32_t reserved;
+    double scaled_optimality;
+    double cone_violation;
+    double complementarity;
+    double objective;              /* dual objective of the returned impulses */
+} MRQualityResultC;
+MR_API int mr_quality_solve_batch(
+    uint32_t problem_count,
+    uint32_t nv,
+    uint32_t contact_capacity,
+    const uint32_t* contact_counts,
+    const double* mass,
+    const double* jacobian,
+    const double* free_velocity,
+    const double* target_velocity,
+    const double* regularization,
+    const double* friction,
+    const double* warm_impulses,
+    const MRQualitySolverConfigC* config,
+    double* impulses,
+    double* velocity,
+    MRQualityResultC* results);
 
 /* No counterpart in the reference: zero-copy advance for device buffers
  * (e.g. torch CUDA tensors).  `device_actions` [step][env][action] and the

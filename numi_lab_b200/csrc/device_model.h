@@ -126,6 +126,16 @@ struct alignas(16) DeviceModel {
     float4 material_response[kMaxMaterials];
 };
 
+// Settings of the converged (quality) contact solve, MRQualitySolverConfigC
+// with its defaults applied (quality.cuh).
+struct QualityConfig {
+    std::int32_t max_newton;
+    std::int32_t max_line_search;  // evaluations of the line search's phi' per Newton step
+    double tolerance;              // on ||zeta - Y lambda||_inf / (1 + ||zeta||_inf + ||Y lambda||_inf)
+    double line_search_tolerance;  // |phi'(t)| relative to |phi'(0)|
+    double regularization_floor;
+};
+
 // Launch parameters of one control step of one rollout.
 struct StepParams {
     const DeviceModel* model;
@@ -150,6 +160,7 @@ struct StepParams {
     float* q_comp;                 // [env][nq] compensation terms of q's running sums (compensated precision), or null
     std::int32_t env_base;         // slot index of this launch's slot 0 (counters report absolute slots)
     double* audit;                 // [env][kAuditWords] FP64 energy / momentum audit (audit.cuh), or null
+    QualityConfig quality;         // read by the quality-solver kernel instances only
 };
 
 enum StatIndex : int {
@@ -163,6 +174,13 @@ enum StatIndex : int {
     kStatFirstFailCode = 7,
     kStatResets = 8,
     kStatWorldMismatch = 9,  // scene items skipped: the world record was not the one the launch was enqueued for
+    // Quality solver (largest over the launch's environment-substeps; the
+    // FP32 bit patterns of non-negative values order like the values).
+    kStatQualityNewton = 10,       // Newton steps of one solve
+    kStatQualityLineSearch = 11,   // line-search evaluations, summed
+    kStatQualityResidual = 12,     // scaled optimality (FP32 bits)
+    kStatQualityCone = 13,         // cone violation (FP32 bits)
+    kStatQualityComplementarity = 14,  // conic complementarity (FP32 bits)
     kStatCount = 16
 };
 

@@ -42,6 +42,7 @@ struct WarpLayout {
     int manifolds, contacts, G, L, z, margins, pair_stats;
     int narrow;  // narrowphase scratch; aliases the contact records and rows
     int qcomp;   // compensation terms of q's running sums (compensated precision only)
+    int quality; // FP64 workspace of the quality solver (quality.cuh; quality-solver instances only)
     int total;   // floats per warp
 };
 
@@ -58,10 +59,11 @@ __host__ __device__ inline int pair_max_raw(int pair_class) {
 }
 
 // `narrow_words` is the sum of pair_scratch_words over the compiled pairs.
-// `compensated` appends the q compensation section (the other sections keep
-// their offsets).
+// `compensated` appends the q compensation section and `quality_doubles`
+// (quality_workspace_doubles, or 0) the quality solver's FP64 workspace;
+// the other sections keep their offsets.
 __host__ __device__ inline WarpLayout make_layout(int nb, int nv, int nq, int np, int ncap, int max_anc, int narrow_words,
-                                                  bool contact, bool compensated = false) {
+                                                  bool contact, bool compensated = false, int quality_doubles = 0) {
     WarpLayout L{};
     int o = 0;
     auto take = [&o](int words) { const int at = o; o += align4(words); return at; };
@@ -97,6 +99,7 @@ __host__ __device__ inline WarpLayout make_layout(int nb, int nv, int nq, int np
         L.manifolds = L.contacts = L.G = L.L = L.narrow = L.pair_stats = o;
     }
     L.qcomp = compensated ? take(nq) : o;
+    L.quality = quality_doubles > 0 ? take(2 * quality_doubles) : o;
     L.total = align4(o);
     return L;
 }
@@ -111,7 +114,14 @@ enum MiscWord : int {
     kMiscRawCount = 8,
     kMiscCandidatePairs = 9,
     kMiscIslands = 10,
-    kMiscPairBase = 12   // prefix offsets of pairs (up to 20 words here would overflow; pairs use manifold slots)
+    // Quality solver, over the control step's substeps: most Newton steps,
+    // total line-search evaluations (int bits), largest scaled optimality,
+    // cone violation and conic complementarity.
+    kMiscQualityNewton = 16,
+    kMiscQualityLineSearch = 17,
+    kMiscQualityResidual = 18,
+    kMiscQualityCone = 19,
+    kMiscQualityComplementarity = 20
 };
 
 }  // namespace numi

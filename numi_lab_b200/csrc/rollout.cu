@@ -14,6 +14,7 @@
 #include "model.h"
 #include "numi_b200.h"
 #include "policy.h"
+#include "quality.cuh"
 #include "runtime.h"
 #include "scene.h"
 
@@ -262,38 +263,44 @@ void numi::rt::make_plan(const numi::CompiledModel& m, float h, KernelPlan& plan
     plan.dmodel = pack_model(m, h);
     int narrow_words = 0;
     for (const MRModelPairC& pr : m.pairs) narrow_words += numi::pair_scratch_words(numi::pair_max_raw(static_cast<int>(pr.pair_class)));
-    for (const bool compensated : {false, true})
-        (compensated ? plan.layout_comp : plan.layout) =
-            numi::make_layout(static_cast<int>(m.articulated_body_count), static_cast<int>(m.world.nv),
-                              static_cast<int>(m.world.nq), static_cast<int>(m.world.pair_count),
-                              static_cast<int>(m.world.contact_capacity), static_cast<int>(m.max_ancestor_dofs),
-                              narrow_words, plan.contact, compensated);
+    const int nv = static_cast<int>(m.world.nv), ncap = static_cast<int>(m.world.contact_capacity);
+    const int solvers = plan.contact ? kSolverModes : 1;
+    for (int quality = 0; quality < solvers; ++quality)
+        for (const bool compensated : {false, true})
+            (compensated ? plan.layout_comp : plan.layout)[quality] =
+                numi::make_layout(static_cast<int>(m.articulated_body_count), nv, static_cast<int>(m.world.nq),
+                                  static_cast<int>(m.world.pair_count), ncap, static_cast<int>(m.max_ancestor_dofs), narrow_words,
+                                  plan.contact, compensated, quality ? numi::quality_workspace_doubles(nv, ncap) : 0);
     int device = 0;
     check(cudaGetDevice(&device), "cudaGetDevice");
     cudaDeviceProp prop{};
     check(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
     const size_t tables = numi::control_step_table_bytes();
     const size_t limit = prop.sharedMemPerBlockOptin;
-    if (tables + static_cast<size_t>(plan.layout.total) * sizeof(float) > limit)
+    if (tables + static_cast<size_t>(plan.layout[0].total) * sizeof(float) > limit)
         throw std::runtime_error("per-environment shared memory exceeds the device limit");
     check(numi::configure_control_step_kernels(limit), "kernel attributes");
     // Environments per CTA: the choice that keeps the most warps resident
     // per SM under the kernel's register and shared-memory footprint (each
     // CTA carries one copy of the topology tables).
-    for (std::uint32_t prec = 0; prec < static_cast<std::uint32_t>(numi::rt::kPrecisionModes); ++prec) {
-        const size_t per_warp = static_cast<size_t>(plan.layout_for(prec).total) * sizeof(float);
-        int best = 1, best_warps = 0;
-        for (int wpb = 1; wpb <= 4; ++wpb) {
-            const size_t smem = tables + wpb * per_warp;
-            if (smem > limit) break;
-            int blocks = 0;
-            check(numi::control_step_occupancy(plan.contact, prec, wpb, smem, &blocks), "occupancy query");
-            if (blocks * wpb > best_warps) { best_warps = blocks * wpb; best = wpb; }
+    for (int quality = 0; quality < solvers; ++quality)
+        for (std::uint32_t prec = 0; prec < static_cast<std::uint32_t>(numi::rt::kPrecisionModes); ++prec) {
+            const size_t per_warp = static_cast<size_t>(plan.layout_for(prec, quality != 0).total) * sizeof(float);
+            int best = 1, best_warps = 0;
+            for (int wpb = 1; wpb <= 4; ++wpb) {
+                const size_t smem = tables + wpb * per_warp;
+                if (smem > limit) break;
+                int blocks = 0;
+                check(numi::control_step_occupancy(plan.contact, prec, quality != 0, wpb, smem, &blocks), "occupancy query");
+                if (blocks * wpb > best_warps) { best_warps = blocks * wpb; best = wpb; }
+            }
+            if (best_warps == 0) {
+                if (quality) continue;  // the quality solver stays unavailable for this model
+                throw std::runtime_error("the control-step kernel cannot be resident with this model");
+            }
+            plan.warps_per_block[quality][prec] = best;
+            plan.resident_warps_per_sm[quality][prec] = best_warps;
         }
-        if (best_warps == 0) throw std::runtime_error("the control-step kernel cannot be resident with this model");
-        plan.warps_per_block[prec] = best;
-        plan.resident_warps_per_sm[prec] = best_warps;
-    }
 }
 
 numi::SceneModel numi::rt::pack_scene(const numi::CompiledModel& m, float h) {
@@ -373,6 +380,16 @@ struct MRTaskRolloutHandle {
     numi::DeviceModel dmodel{};
     numi::WarpLayout layout{};
     numi::WarpLayout layout_comp{};     // with the q compensation section
+    // Converged contact solve (MR_SOLVER_QUALITY_NEWTON) in place of the
+    // temporalCone sweeps: its kernel instances, layouts (with the solver
+    // workspace) and launch shapes.
+    bool quality = false;
+    numi::QualityConfig quality_cfg{};
+    numi::WarpLayout layout_q{};
+    numi::WarpLayout layout_q_comp{};
+    int warps_per_block_q[numi::rt::kPrecisionModes] = {1, 1, 1};
+    int resident_warps_per_sm_q[numi::rt::kPrecisionModes] = {0, 0, 0};
+    MRQualityDiagnosticsC last_quality{};  // of the last advance (zeros under temporalCone)
     bool contact = false;
     bool scene = false;                 // free-body pile world (scene_step kernel)
     numi::SceneModel smodel{};
@@ -558,6 +575,14 @@ struct MRTaskRolloutHandle {
         if (audit) check(cudaMemsetAsync(d_audit.ptr, 0, d_audit.count * sizeof(double), stream), "clear audit");
     }
 
+    // Layout and environments per CTA of the current (solver, precision).
+    const numi::WarpLayout& step_layout() const {
+        if (quality) return precision == MR_PRECISION_COMPENSATED ? layout_q_comp : layout_q;
+        return precision == MR_PRECISION_COMPENSATED ? layout_comp : layout;
+    }
+    int step_warps_per_block() const { return quality ? warps_per_block_q[precision] : warps_per_block[precision]; }
+    int step_resident_warps_per_sm() const { return quality ? resident_warps_per_sm_q[precision] : resident_warps_per_sm[precision]; }
+
     size_t manifold_words() const {
         return scene ? static_cast<size_t>(numi::kSceneManifolds) * numi::kSceneSlotWords
                      : static_cast<size_t>(model.world.pair_count) * numi::kManifoldWords;
@@ -643,12 +668,11 @@ struct MRTaskRolloutHandle {
                 p.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
                 p.q_comp = precision == MR_PRECISION_COMPENSATED ? d_qcomp.ptr + static_cast<size_t>(o) * model.world.nq : nullptr;
                 p.audit = audit ? d_audit.ptr + static_cast<size_t>(o) * numi::kAuditWords : nullptr;
-                check(numi::launch_control_step(p, precision == MR_PRECISION_COMPENSATED ? layout_comp : layout, contact, precision,
-                                                warps_per_block[precision], cs),
+                p.quality = quality_cfg;
+                check(numi::launch_control_step(p, step_layout(), contact, precision, quality, step_warps_per_block(), cs),
                       "control step launch");
                 if (audit)
-                    check(numi::launch_audit_step(p, precision == MR_PRECISION_COMPENSATED ? layout_comp : layout,
-                                                  precision != MR_PRECISION_FP32, warps_per_block[precision], cs),
+                    check(numi::launch_audit_step(p, step_layout(), precision != MR_PRECISION_FP32, step_warps_per_block(), cs),
                           "audit launch");
                 if (host_obs && obs) copy_observation_rows(k, o, n, obs, host_obs, cs, c);
             }
@@ -822,6 +846,17 @@ struct MRTaskRolloutHandle {
         a.high_water.islands = host_stats[numi::kStatMaxIslands];
         a.high_water.articulation_point_queries = 2u * host_stats[numi::kStatMaxContacts];
         a.high_water.dynamic_nodes = 1u;
+        last_quality = MRQualityDiagnosticsC{};
+        if (quality) {
+            a.high_water.quality_generalized_velocities = model.world.nv;
+            a.high_water.quality_rows = 3u * host_stats[numi::kStatMaxContacts];
+            a.high_water.quality_direct_tiles = host_stats[numi::kStatMaxContacts] > 0 ? 1u : 0u;
+            last_quality.maximum_newton_iterations = host_stats[numi::kStatQualityNewton];
+            last_quality.line_search_iterations = host_stats[numi::kStatQualityLineSearch];
+            std::memcpy(&last_quality.maximum_scaled_optimality, &host_stats[numi::kStatQualityResidual], sizeof(float));
+            std::memcpy(&last_quality.maximum_cone_violation, &host_stats[numi::kStatQualityCone], sizeof(float));
+            std::memcpy(&last_quality.maximum_complementarity, &host_stats[numi::kStatQualityComplementarity], sizeof(float));
+        }
         a.high_water.operator_velocity_elements = model.world.nv;
         a.gpu_milliseconds = gpu_ms;
         a.submission_milliseconds = wall_ms;
@@ -896,11 +931,15 @@ MR_API MRTaskRolloutHandle* mr_create_task_rollout(const MRRunManifestC* manifes
             numi::rt::make_plan(h.model, h.h, plan);
             h.contact = plan.contact;
             h.dmodel = plan.dmodel;
-            h.layout = plan.layout;
-            h.layout_comp = plan.layout_comp;
+            h.layout = plan.layout[0];
+            h.layout_comp = plan.layout_comp[0];
+            h.layout_q = plan.layout[1];
+            h.layout_q_comp = plan.layout_comp[1];
             for (int prec = 0; prec < numi::rt::kPrecisionModes; ++prec) {
-                h.warps_per_block[prec] = plan.warps_per_block[prec];
-                h.resident_warps_per_sm[prec] = plan.resident_warps_per_sm[prec];
+                h.warps_per_block[prec] = plan.warps_per_block[0][prec];
+                h.resident_warps_per_sm[prec] = plan.resident_warps_per_sm[0][prec];
+                h.warps_per_block_q[prec] = plan.warps_per_block[1][prec];
+                h.resident_warps_per_sm_q[prec] = plan.resident_warps_per_sm[1][prec];
             }
         }
         check(cudaGetDevice(&h.device), "cudaGetDevice");
@@ -1177,6 +1216,33 @@ MR_API int mr_task_rollout_set_precision(MRTaskRolloutHandle* handle, uint32_t m
     });
 }
 
+MR_API int mr_task_rollout_set_solver(MRTaskRolloutHandle* handle, uint32_t solver, const MRQualitySolverConfigC* quality) {
+    return guarded([&] {
+        if (!handle) throw std::invalid_argument("handle is null");
+        if (solver != MR_SOLVER_TEMPORAL_CONE && solver != MR_SOLVER_QUALITY_NEWTON)
+            throw std::invalid_argument("solver " + std::to_string(solver) +
+                                        " is not available: MR_SOLVER_TEMPORAL_CONE or MR_SOLVER_QUALITY_NEWTON");
+        const bool q = solver == MR_SOLVER_QUALITY_NEWTON;
+        if (q && handle->scene)
+            throw std::invalid_argument("MR_SOLVER_QUALITY_NEWTON runs articulated contact worlds; pile and stack worlds take temporalCone");
+        if (q && !handle->contact) throw std::invalid_argument("MR_SOLVER_QUALITY_NEWTON needs a contact world");
+        if (q && handle->resident_warps_per_sm_q[0] == 0)
+            throw std::invalid_argument("the quality solver's workspace does not fit this model's shared-memory budget");
+        const numi::QualityConfig cfg = q ? numi::rt::quality_config(quality) : numi::QualityConfig{};
+        // Captured graphs hold the previous solver's kernel and settings.
+        drop_graphs(*handle);
+        handle->quality = q;
+        handle->quality_cfg = cfg;
+    });
+}
+
+MR_API int mr_task_rollout_quality_diagnostics(const MRTaskRolloutHandle* handle, MRQualityDiagnosticsC* out) {
+    return guarded([&] {
+        if (!handle || !out) throw std::invalid_argument("handle or output is null");
+        *out = handle->last_quality;
+    });
+}
+
 MR_API int mr_task_rollout_advance(MRTaskRolloutHandle* handle, const float* normalized_actions, size_t normalized_action_count,
                                    const uint32_t* reset_masks, size_t reset_mask_count, uint32_t control_step_count,
                                    uint64_t policy_revision, uint32_t evaluate_final_policy, MRTaskRolloutAdvanceC* advance) {
@@ -1419,8 +1485,8 @@ MR_API int mr_task_rollout_launch_shape(const MRTaskRolloutHandle* handle, uint3
     return guarded([&] {
         if (!handle) throw std::invalid_argument("handle is null");
         const std::uint32_t prec = handle->precision;
-        if (warps_per_block) *warps_per_block = handle->scene ? 1u : static_cast<uint32_t>(handle->warps_per_block[prec]);
-        if (resident_warps_per_sm) *resident_warps_per_sm = handle->scene ? 0u : static_cast<uint32_t>(handle->resident_warps_per_sm[prec]);
+        if (warps_per_block) *warps_per_block = handle->scene ? 1u : static_cast<uint32_t>(handle->step_warps_per_block());
+        if (resident_warps_per_sm) *resident_warps_per_sm = handle->scene ? 0u : static_cast<uint32_t>(handle->step_resident_warps_per_sm());
     });
 }
 
@@ -1848,6 +1914,7 @@ MR_API MRBatchHandle* mr_create_batch(MRTaskRolloutHandle* const* rollouts, size
             if (!h) throw std::invalid_argument("rollout " + std::to_string(i) + " is null");
             if (h->device != b->device) throw std::invalid_argument("every rollout of a batch must live on the current device");
             if (h->precision != MR_PRECISION_FP32) throw std::invalid_argument("batched rollouts run in FP32 precision only");
+            if (h->quality) throw std::invalid_argument("batched rollouts run the temporalCone solver only");
             if (h->policy) throw std::invalid_argument("batched rollouts take their actions from the caller (no native policy)");
             if (h->scene && h->smodel.support_mapped) b->convex = true;
             if (h->envs > numi::kMixEnvMask) throw std::invalid_argument("a batched rollout holds at most 2^24 - 1 environments");

@@ -19,8 +19,12 @@ namespace numi {
 
 // `precision` is an MRPrecisionModeC value; MR_PRECISION_COMPENSATED needs
 // p.q_comp and the layout made with its compensation section.
-cudaError_t control_step_occupancy(bool contact, std::uint32_t precision, int warps_per_block, size_t smem, int* blocks_per_sm);
-cudaError_t launch_control_step(const StepParams& p, const WarpLayout& layout, bool contact, std::uint32_t precision,
+// `quality` selects the instances with the converged contact solve
+// (quality.cuh) in place of the temporalCone sweeps; their layout carries
+// the solver's workspace.
+cudaError_t control_step_occupancy(bool contact, std::uint32_t precision, bool quality, int warps_per_block, size_t smem,
+                                   int* blocks_per_sm);
+cudaError_t launch_control_step(const StepParams& p, const WarpLayout& layout, bool contact, std::uint32_t precision, bool quality,
                                 int warps_per_block, cudaStream_t stream);
 cudaError_t configure_control_step_kernels(size_t max_dynamic_smem);
 // FP64 energy / momentum audit (audit.cuh) of the state the control-step
@@ -91,17 +95,20 @@ int guarded(F&& f) {
 
 // Everything the control-step kernel needs to know about a compiled model
 // at one substep length: the packed device record, the per-warp
-// shared-memory layout and the launch shape per precision mode.
+// shared-memory layout and the launch shape per (solver, precision mode).
 constexpr int kPrecisionModes = 3;       // indexed by MRPrecisionModeC
+constexpr int kSolverModes = 2;          // 0 temporalCone, 1 quality (contact worlds)
 struct KernelPlan {
     DeviceModel dmodel{};
-    WarpLayout layout{};                 // FP32 and FP64 articulated inertia
-    WarpLayout layout_comp{};            // compensated: layout plus the q compensation section
+    // [solver]: FP32 and FP64 articulated inertia; compensated adds the q
+    // compensation section.  The quality layouts add the solver workspace.
+    WarpLayout layout[kSolverModes]{};
+    WarpLayout layout_comp[kSolverModes]{};
     bool contact = false;
-    int warps_per_block[kPrecisionModes] = {1, 1, 1};
-    int resident_warps_per_sm[kPrecisionModes] = {0, 0, 0};
-    const WarpLayout& layout_for(std::uint32_t precision) const {
-        return precision == MR_PRECISION_COMPENSATED ? layout_comp : layout;
+    int warps_per_block[kSolverModes][kPrecisionModes] = {{1, 1, 1}, {1, 1, 1}};
+    int resident_warps_per_sm[kSolverModes][kPrecisionModes] = {{0, 0, 0}, {0, 0, 0}};
+    const WarpLayout& layout_for(std::uint32_t precision, bool quality = false) const {
+        return precision == MR_PRECISION_COMPENSATED ? layout_comp[quality] : layout[quality];
     }
 };
 
@@ -110,6 +117,9 @@ DeviceModel pack_model(const CompiledModel& m, float h);
 void make_plan(const CompiledModel& m, float h, KernelPlan& plan);
 // Packs a pile (scene) world for the free-body kernel at substep length h.
 SceneModel pack_scene(const CompiledModel& m, float h);
+// MRQualitySolverConfigC (null: all defaults) with its defaults applied;
+// throws on out-of-range settings.
+QualityConfig quality_config(const MRQualitySolverConfigC* c);
 
 }  // namespace rt
 }  // namespace numi

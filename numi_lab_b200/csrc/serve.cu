@@ -393,7 +393,7 @@ struct MRServerHandle {
                 sp.substeps = static_cast<int>(config.physics_substeps);
                 sp.velocity_iterations = static_cast<int>(config.velocity_iterations);
                 sp.final_velocity_iterations = static_cast<int>(config.final_velocity_iterations);
-                check(numi::launch_control_step(sp, p.plan.layout, p.plan.contact, MR_PRECISION_FP32, p.plan.warps_per_block[0],
+                check(numi::launch_control_step(sp, p.plan.layout[0], p.plan.contact, MR_PRECISION_FP32, false, p.plan.warps_per_block[0][0],
                                                 p.stream),
                       "control step launch");
             }

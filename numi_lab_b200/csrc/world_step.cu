@@ -5,7 +5,7 @@
 namespace numi {
 namespace {
 
-template <bool kContact, typename R, bool kComp>
+template <bool kContact, typename R, bool kComp, bool kQuality>
 __global__ void __launch_bounds__(128, 3) control_step_kernel(StepParams p, WarpLayout layout, int warps_per_block) {
     extern __shared__ float4 smem4[];
     // Topology tables: one copy per CTA.
@@ -21,7 +21,7 @@ __global__ void __launch_bounds__(128, 3) control_step_kernel(StepParams p, Warp
     const int item = blockIdx.x * warps_per_block + warp;
     if (item >= p.env_count) return;
     const int env = p.env_index != nullptr ? p.env_index[item] : item;
-    control_step_item<kContact, R, kComp>(p, layout, reinterpret_cast<const DeviceTables*>(smem4),
+    control_step_item<kContact, R, kComp, kQuality>(p, layout, reinterpret_cast<const DeviceTables*>(smem4),
                                           reinterpret_cast<float*>(smem4) + sizeof(DeviceTables) / sizeof(float) + warp * layout.total,
                                           item, env);
 }
@@ -76,48 +76,51 @@ cudaError_t launch_audit_step(const StepParams& p, const WarpLayout& layout, boo
 
 size_t control_step_table_bytes() { return sizeof(DeviceTables); }
 
+namespace {
+
+// The kernel instance of (contact, precision, quality solver); the quality
+// solver runs in contact worlds only.
+template <typename F>
+cudaError_t for_kernel(bool contact, std::uint32_t precision, bool quality, F&& f) {
+    if (contact && quality) {
+        if (precision == MR_PRECISION_COMPENSATED) return f(control_step_kernel<true, double, true, true>);
+        if (precision == MR_PRECISION_FP64_ARTICULATED_INERTIA) return f(control_step_kernel<true, double, false, true>);
+        return f(control_step_kernel<true, float, false, true>);
+    }
+    if (contact) {
+        if (precision == MR_PRECISION_COMPENSATED) return f(control_step_kernel<true, double, true, false>);
+        if (precision == MR_PRECISION_FP64_ARTICULATED_INERTIA) return f(control_step_kernel<true, double, false, false>);
+        return f(control_step_kernel<true, float, false, false>);
+    }
+    if (precision == MR_PRECISION_COMPENSATED) return f(control_step_kernel<false, double, true, false>);
+    if (precision == MR_PRECISION_FP64_ARTICULATED_INERTIA) return f(control_step_kernel<false, double, false, false>);
+    return f(control_step_kernel<false, float, false, false>);
+}
+
+}  // namespace
+
 // Host launcher: one control step of `env_count` environments.
 // `precision` (MRPrecisionModeC) selects the kernel instance: FP32, FP64
-// articulated inertia, or FP64 articulated inertia with compensated sums.
-cudaError_t launch_control_step(const StepParams& p, const WarpLayout& layout, bool contact, std::uint32_t precision,
+// articulated inertia, or FP64 articulated inertia with compensated sums;
+// `quality` the converged contact solve in place of the temporalCone sweeps
+// (the layout must carry its workspace).
+cudaError_t launch_control_step(const StepParams& p, const WarpLayout& layout, bool contact, std::uint32_t precision, bool quality,
                                 int warps_per_block, cudaStream_t stream) {
     const int blocks = (p.env_count + warps_per_block - 1) / warps_per_block;
     const size_t smem = sizeof(DeviceTables) + static_cast<size_t>(layout.total) * sizeof(float) * warps_per_block;
     const int threads = 32 * warps_per_block;
     if (precision == MR_PRECISION_COMPENSATED && p.q_comp == nullptr) return cudaErrorInvalidValue;
-#define NUMI_LAUNCH(C, R, K) control_step_kernel<C, R, K><<<blocks, threads, smem, stream>>>(p, layout, warps_per_block)
-    if (contact) {
-        if (precision == MR_PRECISION_COMPENSATED) NUMI_LAUNCH(true, double, true);
-        else if (precision == MR_PRECISION_FP64_ARTICULATED_INERTIA) NUMI_LAUNCH(true, double, false);
-        else NUMI_LAUNCH(true, float, false);
-    } else {
-        if (precision == MR_PRECISION_COMPENSATED) NUMI_LAUNCH(false, double, true);
-        else if (precision == MR_PRECISION_FP64_ARTICULATED_INERTIA) NUMI_LAUNCH(false, double, false);
-        else NUMI_LAUNCH(false, float, false);
-    }
-#undef NUMI_LAUNCH
-    return cudaGetLastError();
+    if (quality && (!contact || layout.quality >= layout.total)) return cudaErrorInvalidValue;
+    return for_kernel(contact, precision, quality, [&](auto kernel) {
+        kernel<<<blocks, threads, smem, stream>>>(p, layout, warps_per_block);
+        return cudaGetLastError();
+    });
 }
 
-namespace {
-
-template <typename F>
-cudaError_t for_kernel(bool contact, std::uint32_t precision, F&& f) {
-    if (contact) {
-        if (precision == MR_PRECISION_COMPENSATED) return f(control_step_kernel<true, double, true>);
-        if (precision == MR_PRECISION_FP64_ARTICULATED_INERTIA) return f(control_step_kernel<true, double, false>);
-        return f(control_step_kernel<true, float, false>);
-    }
-    if (precision == MR_PRECISION_COMPENSATED) return f(control_step_kernel<false, double, true>);
-    if (precision == MR_PRECISION_FP64_ARTICULATED_INERTIA) return f(control_step_kernel<false, double, false>);
-    return f(control_step_kernel<false, float, false>);
-}
-
-}  // namespace
-
-cudaError_t control_step_occupancy(bool contact, std::uint32_t precision, int warps_per_block, size_t smem, int* blocks_per_sm) {
+cudaError_t control_step_occupancy(bool contact, std::uint32_t precision, bool quality, int warps_per_block, size_t smem,
+                                   int* blocks_per_sm) {
     const int threads = 32 * warps_per_block;
-    return for_kernel(contact, precision, [&](auto kernel) {
+    return for_kernel(contact, precision, quality, [&](auto kernel) {
         return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, threads, smem);
     });
 }
@@ -126,12 +129,13 @@ cudaError_t configure_control_step_kernels(size_t max_dynamic_smem) {
     const int bytes = static_cast<int>(max_dynamic_smem);
     cudaError_t e = cudaSuccess;
     for (const bool contact : {true, false})
-        for (const std::uint32_t precision :
-             {std::uint32_t(MR_PRECISION_FP32), std::uint32_t(MR_PRECISION_FP64_ARTICULATED_INERTIA), std::uint32_t(MR_PRECISION_COMPENSATED)})
-            if (e == cudaSuccess)
-                e = for_kernel(contact, precision, [&](auto kernel) {
-                    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-                });
+        for (const bool quality : {false, true})
+            for (const std::uint32_t precision :
+                 {std::uint32_t(MR_PRECISION_FP32), std::uint32_t(MR_PRECISION_FP64_ARTICULATED_INERTIA), std::uint32_t(MR_PRECISION_COMPENSATED)})
+                if (e == cudaSuccess && (contact || !quality))
+                    e = for_kernel(contact, precision, quality, [&](auto kernel) {
+                        return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+                    });
     if (e == cudaSuccess) e = cudaFuncSetAttribute(audit_step_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(audit_step_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     return e;

@@ -34,6 +34,7 @@
 #include "layout.h"
 #include "audit.cuh"
 #include "contact.cuh"
+#include "quality.cuh"
 
 #include <cfloat>
 #include <cstdint>
@@ -1352,12 +1353,82 @@ __device__ void group_manifold(const DeviceModel& M, const float* pose, const fl
 }
 
 // ---------------------------------------------------------------------------
+// Rows of Y = L^-T G^T over each contact body's ancestor DoFs, as the
+// quality solver reads them (quality.cuh).
+struct TreeRows {
+    const DeviceTables* T;
+    const float* Y;
+    const float* C;
+    int ma;
+    __device__ __forceinline__ int body(int c) const { return as_int(C[c * kContactWords + kCwBody]); }
+    __device__ __forceinline__ int count(int c) const { return T->anc_count[body(c)]; }
+    __device__ __forceinline__ int dof(int c, int k) const { return T->anc[body(c)][k]; }
+    __device__ __forceinline__ int pos(int c, int d) const {
+        const int t = T->pos[body(c)][d];
+        return t == kNone ? -1 : t;
+    }
+    __device__ __forceinline__ double y(int c, int r, int k) const { return static_cast<double>(Y[(c * 3 + r) * ma + k]); }
+};
+
+// Converged contact solve (qualityNewton) of the `total` evaluated contacts
+// in place of the temporalCone sweeps: the regularisation floor, the warm
+// impulses of the manifold points, the FP64 Newton solve, then z = Y lambda
+// and the impulses back into the contact records.  A solve that does not
+// converge latches MR_STEP_DID_NOT_CONVERGE (the step keeps its checkpoint).
+__device__ bool quality_contacts(const Warp& w, int total, int ma, const QualityConfig& cfg) {
+    const WarpLayout& L = *w.L;
+    float* s = w.s;
+    float* misc = s + L.misc;
+    float* C = s + L.contacts;
+    float* z = s + L.z;
+    const int nv = w.M->nv, lane = w.lane;
+    double* ws = reinterpret_cast<double*>(s + L.quality);
+    double* K = ws + quality_contact_offset(nv);
+    if (lane < total) {
+        const float* c = C + lane * kContactWords;
+        double* k = K + lane * kQuWords;
+        for (int r = 0; r < 3; ++r) {
+            k[kQuFree + r] = c[kCwUfree + r];
+            k[kQuTarget + r] = c[kCwTarget + r];
+            k[kQuReg + r] = fmax(static_cast<double>(c[kCwReg + r]), cfg.regularization_floor);
+        }
+        k[kQuMu] = c[kCwMuU];
+        const float3 warm = project_cone(ld3(c + kCwLambda), c[kCwMuU], c[kCwMuV]);
+        k[kQuLambda + 0] = warm.x;
+        k[kQuLambda + 1] = warm.y;
+        k[kQuLambda + 2] = warm.z;
+    }
+    __syncwarp();
+    const TreeRows rows{w.T, s + L.G, C, ma};
+    const QualityOutcome o = quality_solve(rows, nv, total, ws, cfg, lane);
+    for (int d = lane; d < nv; d += 32) z[d] = static_cast<float>(quality_y_lambda(rows, total, K, d));
+    if (lane < total) {
+        const double* k = K + lane * kQuWords + kQuLambda;
+        st3(C + lane * kContactWords + kCwLambda, f3(static_cast<float>(k[0]), static_cast<float>(k[1]), static_cast<float>(k[2])));
+    }
+    if (lane == 0) {
+        misc[kMiscQualityNewton] = as_float(max(as_int(misc[kMiscQualityNewton]), o.newton));
+        misc[kMiscQualityLineSearch] = as_float(as_int(misc[kMiscQualityLineSearch]) + o.line_search);
+        misc[kMiscQualityResidual] = fmaxf(misc[kMiscQualityResidual], static_cast<float>(o.residual));
+        misc[kMiscQualityCone] = fmaxf(misc[kMiscQualityCone], static_cast<float>(o.cone));
+        misc[kMiscQualityComplementarity] = fmaxf(misc[kMiscQualityComplementarity], static_cast<float>(o.complementarity));
+        if (o.status != kQualityConverged)
+            set_status(misc,
+                       o.status == kQualityFactorization ? MR_STEP_FACTORIZATION_FAILED
+                                                         : (o.status == kQualityNonfinite ? MR_STEP_NONFINITE_RESULT : MR_STEP_DID_NOT_CONVERGE),
+                       static_cast<unsigned>(o.newton));
+    }
+    __syncwarp();
+    return warp_ok(misc);
+}
+
 // Contact substep after the ABA: collision, ConstraintIR evaluation, joint
-// inertia factor, temporalCone solve, joint limits, integration.
+// inertia factor, temporalCone (or quality) solve, joint limits, integration.
 // ---------------------------------------------------------------------------
-template <bool kComp, typename R>
+template <bool kComp, bool kQuality, typename R>
 __device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState<R>& st, bool final_substep,
-                                int velocity_iterations, int final_iterations, float friction_scale) {
+                                int velocity_iterations, int final_iterations, float friction_scale,
+                                const QualityConfig& quality) {
     const DeviceModel& M = *w.M;
     const DeviceTables& T = *w.T;
     const WarpLayout& L = *w.L;
@@ -1636,6 +1707,9 @@ __device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState<R>
             }
         }
         __syncwarp();
+        if constexpr (kQuality) {
+            if (!quality_contacts(w, total, ma, quality)) return false;
+        } else {
         // Per-DoF lists of the contact rows that reach it, as (position in
         // the contact's ancestor list << 5 | contact), so a sweep's z update
         // visits only those.  The lists reuse the factor rows past the root
@@ -1756,6 +1830,7 @@ __device__ bool contact_substep(const Warp& w, const BodyConst& bc, BodyState<R>
             __syncwarp();
         }
         if (!warp_ok(misc)) return false;
+        }  // temporalCone
         // Velocity change x = L^-1 z as one forward tree sweep: with
         // L_kj = U_k . S_j(c_k) / L_kk, sum_j L_kj x_j is U_k applied to the
         // parent's twist change moved to body k's COM, so each body needs
@@ -1880,7 +1955,7 @@ __device__ void audit_articulated(const Warp& w, const BodyConst& bc, double* re
 // shared-memory copy or the model record itself), `warp_smem` the warp's
 // layout.total floats of shared memory.  Only warp-level synchronisation is
 // used, so warps of one CTA may run different items, or different worlds.
-template <bool kContact, typename R, bool kComp>
+template <bool kContact, typename R, bool kComp, bool kQuality = false>
 __device__ __forceinline__ void control_step_item(const StepParams& p, const WarpLayout& layout, const DeviceTables* tables,
                                                   float* warp_smem, int item, int env) {
     const int lane = threadIdx.x & 31;
@@ -1942,8 +2017,8 @@ __device__ __forceinline__ void control_step_item(const StepParams& p, const War
         bool ok = aba(w, bc, st, kContact ? s + layout.L : nullptr);
         if (ok) {
             if (kContact)
-                ok = contact_substep<kComp>(w, bc, st, sub + 1 == p.substeps, p.velocity_iterations,
-                                            p.final_velocity_iterations, friction_scale);
+                ok = contact_substep<kComp, kQuality>(w, bc, st, sub + 1 == p.substeps, p.velocity_iterations,
+                                                      p.final_velocity_iterations, friction_scale, p.quality);
             else
                 ok = integrate_free<kComp>(w);
         }
@@ -1996,6 +2071,13 @@ __device__ __forceinline__ void control_step_item(const StepParams& p, const War
             atomicMax(p.stats + kStatMaxRawContacts, static_cast<unsigned>(as_int(misc[kMiscRawCount])));
             atomicMax(p.stats + kStatMaxCandidatePairs, static_cast<unsigned>(as_int(misc[kMiscCandidatePairs])));
             atomicMax(p.stats + kStatMaxIslands, static_cast<unsigned>(as_int(misc[kMiscIslands])));
+        }
+        if (kQuality) {
+            atomicMax(p.stats + kStatQualityNewton, static_cast<unsigned>(as_int(misc[kMiscQualityNewton])));
+            atomicAdd(p.stats + kStatQualityLineSearch, static_cast<unsigned>(as_int(misc[kMiscQualityLineSearch])));
+            atomicMax(p.stats + kStatQualityResidual, static_cast<unsigned>(as_int(misc[kMiscQualityResidual])));
+            atomicMax(p.stats + kStatQualityCone, static_cast<unsigned>(as_int(misc[kMiscQualityCone])));
+            atomicMax(p.stats + kStatQualityComplementarity, static_cast<unsigned>(as_int(misc[kMiscQualityComplementarity])));
         }
     }
 }

@@ -133,6 +133,48 @@ class BatchLaunchShapeC(ct.Structure):
     ]
 
 
+MR_SOLVER_QUALITY_NEWTON: Final = 1
+MR_SOLVER_TEMPORAL_CONE: Final = 2
+SOLVERS: Final = {"temporal_cone": MR_SOLVER_TEMPORAL_CONE, "quality_newton": MR_SOLVER_QUALITY_NEWTON}
+
+
+class QualitySolverConfigC(ct.Structure):
+    """MRQualitySolverConfigC (zero / non-positive fields take the defaults)."""
+
+    _fields_ = [
+        ("maximum_newton_iterations", ct.c_uint32),
+        ("maximum_line_search_iterations", ct.c_uint32),
+        ("optimality_tolerance", ct.c_double),
+        ("line_search_tolerance", ct.c_double),
+        ("regularization_floor", ct.c_double),
+        ("reserved", ct.c_double),
+    ]
+
+
+class QualityDiagnosticsC(ct.Structure):
+    _fields_ = [
+        ("maximum_newton_iterations", ct.c_uint32),
+        ("line_search_iterations", ct.c_uint32),
+        ("maximum_scaled_optimality", ct.c_float),
+        ("maximum_cone_violation", ct.c_float),
+        ("maximum_complementarity", ct.c_float),
+        ("reserved", ct.c_uint32 * 3),
+    ]
+
+
+class QualityResultC(ct.Structure):
+    _fields_ = [
+        ("code", ct.c_uint32),
+        ("newton_iterations", ct.c_uint32),
+        ("line_search_iterations", ct.c_uint32),
+        ("reserved", ct.c_uint32),
+        ("scaled_optimality", ct.c_double),
+        ("cone_violation", ct.c_double),
+        ("complementarity", ct.c_double),
+        ("objective", ct.c_double),
+    ]
+
+
 MR_BATCH_ORDER_LONGEST_FIRST: Final = 0
 MR_BATCH_ORDER_ROUND_ROBIN: Final = 1
 MR_BATCH_LAUNCH_FUSED: Final = 0
@@ -482,6 +524,9 @@ EXPORTED_SYMBOLS: Final = (
     "mr_task_rollout_policy_log_probabilities",
     "mr_task_rollout_policy_values",
     "mr_task_rollout_bootstrap_policy_values",
+    "mr_task_rollout_set_solver",
+    "mr_task_rollout_quality_diagnostics",
+    "mr_quality_solve_batch",
 )
 
 
@@ -636,6 +681,14 @@ class Bindings:
         L.mr_batch_launch_shape.restype = ct.c_int
         L.mr_batch_world_costs.argtypes = [ct.c_void_p, P(ct.c_float), ct.c_size_t]
         L.mr_batch_world_costs.restype = ct.c_int
+        L.mr_task_rollout_set_solver.argtypes = [ct.c_void_p, ct.c_uint32, P(QualitySolverConfigC)]
+        L.mr_task_rollout_set_solver.restype = ct.c_int
+        L.mr_task_rollout_quality_diagnostics.argtypes = [ct.c_void_p, P(QualityDiagnosticsC)]
+        L.mr_task_rollout_quality_diagnostics.restype = ct.c_int
+        PD = P(ct.c_double)
+        L.mr_quality_solve_batch.argtypes = [ct.c_uint32, ct.c_uint32, ct.c_uint32, P(ct.c_uint32), PD, PD, PD, PD, PD, PD, PD,
+                                             P(QualitySolverConfigC), PD, PD, P(QualityResultC)]
+        L.mr_quality_solve_batch.restype = ct.c_int
 
     def last_error(self) -> str:
         value = self.lib.mr_last_error()

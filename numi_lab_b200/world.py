@@ -142,6 +142,43 @@ def pile_seeds_by_body_count(bodies: Sequence[int], first_seed: int = 0) -> dict
     return out
 
 
+def quality_solve(mass: np.ndarray, jacobian: np.ndarray, free_velocity: np.ndarray, target: np.ndarray,
+                  regularization: np.ndarray, friction: np.ndarray, *, counts: np.ndarray | None = None,
+                  warm: np.ndarray | None = None, max_newton: int = 0, tolerance: float = 0.0,
+                  regularization_floor: float = 0.0, library: native.Bindings | None = None):
+    """Converged contact solves of a batch of dense problems on the GPU
+    (mr_quality_solve_batch).  Shapes: mass [P, nv, nv], jacobian
+    [P, 3 cap, nv], free_velocity [P, nv], target / regularization / warm
+    [P, 3 cap], friction [P, cap], counts [P] (contacts used per problem).
+    Returns (impulses [P, 3 cap], velocity [P, nv], results: list of dicts)."""
+
+    lib = library or native.bindings()
+    mass = np.ascontiguousarray(mass, np.float64)
+    P, nv = mass.shape[0], mass.shape[1]
+    jac = np.ascontiguousarray(jacobian, np.float64).reshape(P, -1, nv)
+    cap = jac.shape[1] // 3
+    vf = np.ascontiguousarray(free_velocity, np.float64).reshape(P, nv)
+    tgt = np.ascontiguousarray(target, np.float64).reshape(P, 3 * cap)
+    reg = np.ascontiguousarray(regularization, np.float64).reshape(P, 3 * cap)
+    mu = np.ascontiguousarray(friction, np.float64).reshape(P, cap)
+    dp = lambda a: a.ctypes.data_as(ct.POINTER(ct.c_double))  # noqa: E731
+    cnt = None if counts is None else np.ascontiguousarray(counts, np.uint32).reshape(P)
+    wm = None if warm is None else np.ascontiguousarray(warm, np.float64).reshape(P, 3 * cap)
+    imp = np.zeros((P, 3 * cap), np.float64)
+    vel = np.zeros((P, nv), np.float64)
+    res = (native.QualityResultC * P)()
+    cfg = native.QualitySolverConfigC(max_newton, 0, tolerance, 0.0, regularization_floor, 0.0)
+    lib.check(lib.lib.mr_quality_solve_batch(P, nv, cap, None if cnt is None else cnt.ctypes.data_as(ct.POINTER(ct.c_uint32)),
+                                             dp(mass), dp(jac), dp(vf), dp(tgt), dp(reg), dp(mu),
+                                             None if wm is None else dp(wm), ct.byref(cfg), dp(imp), dp(vel), res),
+              "quality_solve")
+    results = [{"code": int(r.code), "newton_iterations": int(r.newton_iterations),
+                "line_search_iterations": int(r.line_search_iterations), "scaled_optimality": float(r.scaled_optimality),
+                "cone_violation": float(r.cone_violation), "complementarity": float(r.complementarity),
+                "objective": float(r.objective)} for r in res]
+    return imp, vel, results
+
+
 class World:
     """A batch of environments of one synthetic world on the current CUDA device."""
 
@@ -188,6 +225,7 @@ class World:
         self.pair_count = int(model.world.pair_count)
         self.scene_bodies = int(layout.scene_body_count)
         self.scene = self.scene_bodies > 0
+        self.solver = "temporal_cone"
         self.set_precision(precision)
 
     def set_precision(self, precision: str) -> None:
@@ -200,6 +238,35 @@ class World:
         self._lib.check(self._lib.lib.mr_task_rollout_set_precision(self._handle, native.PRECISION_MODES[precision]),
                         "set_precision")
         self.precision = precision
+
+    def set_solver(self, solver: str, *, max_newton: int = 0, max_line_search: int = 0, tolerance: float = 0.0,
+                   line_search_tolerance: float = 0.0, regularization_floor: float = 0.0) -> None:
+        """"temporal_cone" (default, fixed sweep budget) or "quality_newton"
+        (every substep's contact problem solved to convergence in FP64;
+        articulated contact worlds).  Zero settings take the library's
+        defaults (100 Newton steps, 50 line-search evaluations per step,
+        tolerance 1e-9, line-search tolerance 1e-12, regularisation floor
+        1e-6)."""
+
+        if solver not in native.SOLVERS:
+            raise ValueError(f"solver must be one of {sorted(native.SOLVERS)}")
+        cfg = native.QualitySolverConfigC(max_newton, max_line_search, tolerance, line_search_tolerance, regularization_floor, 0.0)
+        self._lib.check(self._lib.lib.mr_task_rollout_set_solver(self._handle, native.SOLVERS[solver], ct.byref(cfg)),
+                        "set_solver")
+        self.solver = solver
+
+    def quality_diagnostics(self) -> dict[str, float]:
+        """Certificates of the last advance's quality solves."""
+
+        out = native.QualityDiagnosticsC()
+        self._lib.check(self._lib.lib.mr_task_rollout_quality_diagnostics(self._handle, ct.byref(out)), "quality_diagnostics")
+        return {
+            "newton_iterations": int(out.maximum_newton_iterations),
+            "line_search_iterations": int(out.line_search_iterations),
+            "scaled_optimality": float(out.maximum_scaled_optimality),
+            "cone_violation": float(out.maximum_cone_violation),
+            "complementarity": float(out.maximum_complementarity),
+        }
 
     # -- lifecycle -------------------------------------------------------
     def close(self) -> None:

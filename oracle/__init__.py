@@ -112,6 +112,89 @@ def _dp(a: np.ndarray):
     return a.ctypes.data_as(_DP)
 
 
+class QualityConfig(ct.Structure):
+    """OracleQualityConfig (the library's defaults)."""
+
+    _fields_ = [
+        ("max_newton", ct.c_int32),
+        ("max_line_search", ct.c_int32),
+        ("tolerance", ct.c_double),
+        ("line_search_tolerance", ct.c_double),
+        ("regularization_floor", ct.c_double),
+    ]
+
+
+def quality_config(max_newton: int = 100, max_line_search: int = 50, tolerance: float = 1e-9, line_search_tolerance: float = 1e-12,
+                   regularization_floor: float = 1e-6) -> QualityConfig:
+    return QualityConfig(max_newton, max_line_search, tolerance, line_search_tolerance, regularization_floor)
+
+
+class QualityOutcome(ct.Structure):
+    _fields_ = [
+        ("status", ct.c_uint32),
+        ("newton", ct.c_uint32),
+        ("line_search", ct.c_uint32),
+        ("reserved", ct.c_uint32),
+        ("residual", ct.c_double),
+        ("cone", ct.c_double),
+        ("complementarity", ct.c_double),
+        ("objective", ct.c_double),
+    ]
+
+
+def _oracle_lib():
+    if not ORACLE_LIB.is_file():
+        build(reference=False)
+    lib = ct.CDLL(str(ORACLE_LIB))
+    lib.oracle_quality_dense.restype = ct.c_uint32
+    lib.oracle_quality_dense.argtypes = [ct.c_uint32, ct.c_uint32] + [_DP] * 7 + [ct.POINTER(QualityConfig), _DP, _DP,
+                                                                                   ct.POINTER(QualityOutcome)]
+    lib.oracle_world_set_quality.argtypes = [ct.c_void_p, ct.POINTER(QualityConfig)]
+    return lib
+
+
+def quality_dense(mass, jacobian, free_velocity, target, reg, mu, warm=None, cfg: QualityConfig | None = None):
+    """The oracle's converged contact solve of one dense problem (the inputs
+    of mr_quality_solve_batch for one problem, nc = len(mu)).  Returns
+    (status, impulses [3 nc], velocity [nv], outcome)."""
+
+    lib = _oracle_lib()
+    mass = np.ascontiguousarray(mass, np.float64)
+    nv, nc = mass.shape[0], len(mu)
+    lam = np.zeros(3 * nc)
+    vel = np.zeros(nv)
+    out = QualityOutcome()
+    st = lib.oracle_quality_dense(nv, nc, _dp(mass), _dp(np.ascontiguousarray(jacobian, np.float64)),
+                                  _dp(np.ascontiguousarray(free_velocity, np.float64)), _dp(np.ascontiguousarray(target, np.float64)),
+                                  _dp(np.ascontiguousarray(reg, np.float64)), _dp(np.ascontiguousarray(mu, np.float64)),
+                                  None if warm is None else _dp(np.ascontiguousarray(warm, np.float64)),
+                                  ct.byref(cfg or quality_config()), _dp(lam), _dp(vel), ct.byref(out))
+    return int(st), lam, vel, out
+
+
+def reference_quality_solve(inverse_mass, free_velocity, jacobian, mu, target, reg):
+    """The reference's solveQualityContactProblem on one dense problem.
+    Returns (status, impulses, velocity, certificates dict)."""
+
+    if not REF_LIB.is_file():
+        raise FileNotFoundError(f"{REF_LIB} is missing; build it with `make -C oracle ref` where the reference sources exist")
+    lib = ct.CDLL(str(REF_LIB))
+    lib.ref_quality_solve.restype = ct.c_int
+    lib.ref_quality_solve.argtypes = [ct.c_uint32, _DP, _DP, ct.c_uint32] + [_DP] * 7 + [ct.POINTER(ct.c_uint32)]
+    inverse_mass = np.ascontiguousarray(inverse_mass, np.float64)
+    nv, n = inverse_mass.shape[0], len(mu)
+    imp = np.zeros(3 * n)
+    vel = np.zeros(nv)
+    cert = np.zeros(8)
+    iters = ct.c_uint32(0)
+    st = lib.ref_quality_solve(nv, _dp(inverse_mass), _dp(np.ascontiguousarray(free_velocity, np.float64)), n,
+                               _dp(np.ascontiguousarray(jacobian, np.float64)), _dp(np.ascontiguousarray(mu, np.float64)),
+                               _dp(np.ascontiguousarray(target, np.float64)), _dp(np.ascontiguousarray(reg, np.float64)),
+                               _dp(imp), _dp(vel), _dp(cert), ct.byref(iters))
+    names = ("kkt", "natural_residual", "primal_cone", "dual_cone", "complementarity", "gap", "objective", "normal")
+    return int(st), imp, vel, dict(zip(names, cert.tolist()), iterations=int(iters.value))
+
+
 class Oracle:
     """The C restatement, bound to one compiled world."""
 
@@ -157,6 +240,13 @@ class Oracle:
         )
         if not self.handle:
             raise RuntimeError("oracle_world_create failed")
+        lib.oracle_world_set_quality.argtypes = [ct.c_void_p, ct.POINTER(QualityConfig)]
+
+    def set_quality(self, cfg: QualityConfig | None) -> None:
+        """Converged contact solves (cfg) or the temporalCone sweeps (None)."""
+
+        self._quality = cfg
+        self.lib.oracle_world_set_quality(self.handle, ct.byref(cfg) if cfg is not None else None)
 
     def __del__(self) -> None:
         try:

@@ -75,6 +75,8 @@ struct OracleWorld {
     int body_dof[MAXB];     /* -1 when none */
     double arm_eff[MAXV];
     int action_dof[MAXV];
+    int quality;            /* contacts solved to convergence (oracle_world_set_quality) */
+    OracleQualityConfig qcfg;
 };
 
 /* ------------------------------------------------------------------ */
@@ -1005,6 +1007,222 @@ static void chol_solve(const double* L, uint32_t n, double* x) { /* solveCholesk
 }
 
 /* ------------------------------------------------------------------ */
+/* Converged contact solve (quality mode).  The problem is numi-lab's      */
+/* exact-cone QP (QualityContactSolver.hpp:55-80): min 0.5 l'(W + R)l +    */
+/* (u_free - u_target)'l over the friction cones.  Restated from the       */
+/* library's solver: Newton steps on the factor-space primal              */
+/* f(z) = 0.5|z|^2 + sum_c psi_c(u_free + Y_c'z), W = Y'Y, with the        */
+/* closed-form R-metric cone projection, an exact line search (the root   */
+/* of the monotone phi'(t) by safeguarded Newton steps in a bracket) and  */
+/* the stopping test |z - Y l|_inf <= tol (1 + |z|_inf + |Y l|_inf).  Its */
+/* answers are pinned to the reference's solveQualityContactProblem.      */
+/* ------------------------------------------------------------------ */
+static double q_project(const double* u, const double* tg, const double* rg, double mu, double* lam, double* D) {
+    const double e0 = u[0] - tg[0], e1 = u[1] - tg[1], e2 = u[2] - tg[2];
+    const double a0 = -e0 / rg[0], a1 = -e1 / rg[1], a2 = -e2 / rg[2];
+    for (int i = 0; i < 6; ++i) D[i] = 0.0;
+    if (!(mu > 0.0)) {
+        lam[0] = fmax(a0, 0.0);
+        lam[1] = lam[2] = 0.0;
+        if (lam[0] > 0.0) D[0] = 1.0 / rg[0];
+    } else {
+        const double b1 = a1 / mu, b2 = a2 / mu, s = sqrt(b1 * b1 + b2 * b2);
+        const double d0 = rg[0], dt = rg[1] * mu * mu;
+        if (s <= a0) { /* sticking */
+            lam[0] = a0; lam[1] = a1; lam[2] = a2;
+            D[0] = 1.0 / rg[0]; D[3] = 1.0 / rg[1]; D[5] = 1.0 / rg[2];
+        } else if (d0 * a0 <= -dt * s) { /* separating */
+            lam[0] = lam[1] = lam[2] = 0.0;
+        } else { /* sliding: on the cone surface */
+            const double inv = 1.0 / (d0 + dt), rho = (d0 * a0 + dt * s) * inv, n1 = b1 / s, n2 = b2 / s;
+            const double w = rho / (s * rg[1]);
+            lam[0] = rho; lam[1] = mu * rho * n1; lam[2] = mu * rho * n2;
+            D[0] = inv; D[1] = inv * mu * n1; D[2] = inv * mu * n2;
+            D[3] = inv * mu * mu * n1 * n1 + w * (1.0 - n1 * n1);
+            D[4] = inv * mu * mu * n1 * n2 - w * n1 * n2;
+            D[5] = inv * mu * mu * n2 * n2 + w * (1.0 - n2 * n2);
+        }
+    }
+    return -(0.5 * (rg[0] * lam[0] * lam[0] + rg[1] * lam[1] * lam[1] + rg[2] * lam[2] * lam[2]) + e0 * lam[0] + e1 * lam[1] +
+             e2 * lam[2]);
+}
+
+/* f at x; impulses, derivatives and gradient when the outputs are given. */
+static double q_eval(uint32_t nv, uint32_t nc, const double* Y, const double* uf, const double* tg, const double* rg,
+                     const double* mu, const double* x, double* lam, double* D, double* grad) {
+    double f = 0.0, l[3], d[6];
+    for (uint32_t d0 = 0; d0 < nv; ++d0) f += 0.5 * x[d0] * x[d0];
+    for (uint32_t c = 0; c < nc; ++c) {
+        double u[3];
+        for (int r = 0; r < 3; ++r) {
+            u[r] = uf[3 * c + r];
+            for (uint32_t k = 0; k < nv; ++k) u[r] += Y[(3 * c + r) * nv + k] * x[k];
+        }
+        f += q_project(u, tg + 3 * c, rg + 3 * c, mu[c], l, d);
+        if (lam) for (int r = 0; r < 3; ++r) lam[3 * c + r] = l[r];
+        if (D) for (int i = 0; i < 6; ++i) D[6 * c + i] = d[i];
+    }
+    if (grad) {
+        for (uint32_t k = 0; k < nv; ++k) {
+            double acc = 0.0;
+            for (uint32_t row = 0; row < 3 * nc; ++row) acc += Y[row * nv + k] * lam[row];
+            grad[k] = x[k] - acc;
+        }
+    }
+    return f;
+}
+
+uint32_t oracle_quality_solve(uint32_t nv, uint32_t nc, const double* Y, const double* ufree, const double* target,
+                              const double* reg, const double* mu, const double* warm, const OracleQualityConfig* cfg,
+                              double* lambda, double* zeta, OracleQualityOutcome* out) {
+    double z[MAXV], grad[MAXV], dir[MAXV], trial[MAXV], H[MAXV * MAXV], D[6 * MAXC], U[3 * MAXC], Wd[3 * MAXC];
+    OracleQualityOutcome o;
+    memset(&o, 0, sizeof(o));
+    o.status = 1;
+    for (uint32_t k = 0; k < nv; ++k) {
+        double acc = 0.0;
+        if (warm)
+            for (uint32_t row = 0; row < 3 * nc; ++row) acc += Y[row * nv + k] * warm[row];
+        z[k] = acc;
+    }
+    double f = q_eval(nv, nc, Y, ufree, target, reg, mu, z, lambda, D, grad);
+    double scaled = 0.0;
+    for (int it = 0;; ++it) {
+        double gm = 0.0, zm = 0.0, ym = 0.0;
+        int finite = isfinite(f);
+        for (uint32_t k = 0; k < nv; ++k) {
+            gm = fmax(gm, fabs(grad[k]));
+            zm = fmax(zm, fabs(z[k]));
+            ym = fmax(ym, fabs(z[k] - grad[k]));
+            finite &= isfinite(grad[k]) && isfinite(z[k]);
+        }
+        if (!finite) { o.status = 3; break; }
+        scaled = gm / (1.0 + zm + ym);
+        if (scaled <= cfg->tolerance) { o.status = 0; break; }
+        if (it >= cfg->max_newton) break;
+        /* I + sum_c Y_c D_c Y_c' */
+        for (uint32_t i = 0; i < nv; ++i)
+            for (uint32_t j = 0; j < nv; ++j) H[i * nv + j] = i == j ? 1.0 : 0.0;
+        for (uint32_t c = 0; c < nc; ++c) {
+            const double* Dc = D + 6 * c;
+            const double M3[3][3] = {{Dc[0], Dc[1], Dc[2]}, {Dc[1], Dc[3], Dc[4]}, {Dc[2], Dc[4], Dc[5]}};
+            for (uint32_t j = 0; j < nv; ++j) {
+                double e[3];
+                for (int r = 0; r < 3; ++r) {
+                    e[r] = 0.0;
+                    for (int t = 0; t < 3; ++t) e[r] += M3[r][t] * Y[(3 * c + t) * nv + j];
+                }
+                for (uint32_t i = j; i < nv; ++i)
+                    H[i * nv + j] += Y[(3 * c) * nv + i] * e[0] + Y[(3 * c + 1) * nv + i] * e[1] + Y[(3 * c + 2) * nv + i] * e[2];
+            }
+        }
+        for (uint32_t i = 0; i < nv; ++i)
+            for (uint32_t j = i + 1; j < nv; ++j) H[i * nv + j] = H[j * nv + i];
+        if (!cholesky(H, nv)) { o.status = 2; break; }
+        for (uint32_t k = 0; k < nv; ++k) dir[k] = -grad[k];
+        chol_solve(H, nv, dir);
+        double slope = 0.0;
+        for (uint32_t k = 0; k < nv; ++k) slope += grad[k] * dir[k];
+        if (!(slope < 0.0))
+            for (uint32_t k = 0; k < nv; ++k) dir[k] = -grad[k];
+        /* Exact line search: phi'(t) = a + t b - sum_c l_c(u_c + t w_c)' w_c. */
+        double a = 0.0, b = 0.0, slope0 = 0.0;
+        for (uint32_t k = 0; k < nv; ++k) { a += dir[k] * z[k]; b += dir[k] * dir[k]; slope0 += dir[k] * grad[k]; }
+        for (uint32_t c = 0; c < nc; ++c)
+            for (int r = 0; r < 3; ++r) {
+                double u = ufree[3 * c + r], w = 0.0;
+                for (uint32_t k = 0; k < nv; ++k) { u += Y[(3 * c + r) * nv + k] * z[k]; w += Y[(3 * c + r) * nv + k] * dir[k]; }
+                U[3 * c + r] = u;
+                Wd[3 * c + r] = w;
+            }
+        double lo = 0.0, hi = INFINITY, t = 1.0, best = INFINITY, best_t = 1.0;
+        for (int ls = 0; ls < cfg->max_line_search; ++ls) {
+            double dt = a + t * b, h2 = b, l[3], Dc[6], u[3];
+            for (uint32_t c = 0; c < nc; ++c) {
+                const double* w = Wd + 3 * c;
+                for (int r = 0; r < 3; ++r) u[r] = U[3 * c + r] + t * w[r];
+                q_project(u, target + 3 * c, reg + 3 * c, mu[c], l, Dc);
+                dt -= l[0] * w[0] + l[1] * w[1] + l[2] * w[2];
+                h2 += w[0] * (Dc[0] * w[0] + Dc[1] * w[1] + Dc[2] * w[2]) + w[1] * (Dc[1] * w[0] + Dc[3] * w[1] + Dc[4] * w[2]) +
+                      w[2] * (Dc[2] * w[0] + Dc[4] * w[1] + Dc[5] * w[2]);
+            }
+            o.line_search++;
+            if (fabs(dt) < best) { best = fabs(dt); best_t = t; }
+            if (fabs(dt) <= cfg->line_search_tolerance * fabs(slope0)) break;
+            if (dt < 0.0) lo = t;
+            else hi = t;
+            double tn = t - dt / h2;
+            if (!(tn > lo && tn < hi)) tn = isfinite(hi) ? 0.5 * (lo + hi) : 2.0 * t;
+            if (isfinite(hi) && hi - lo <= 1.0e-14 * hi) break;
+            t = tn;
+        }
+        for (uint32_t k = 0; k < nv; ++k) trial[k] = z[k] + best_t * dir[k];
+        for (uint32_t k = 0; k < nv; ++k) z[k] = trial[k];
+        f = q_eval(nv, nc, Y, ufree, target, reg, mu, z, lambda, D, grad);
+        o.newton++;
+    }
+    o.residual = scaled;
+    o.objective = f;
+    for (uint32_t c = 0; c < nc; ++c) {
+        const double* l = lambda + 3 * c;
+        const double lt = sqrt(l[1] * l[1] + l[2] * l[2]);
+        o.cone = fmax(o.cone, fmax(-l[0], mu[c] > 0.0 ? lt - mu[c] * l[0] : lt));
+        double w = 0.0;
+        for (int r = 0; r < 3; ++r) {
+            double u = ufree[3 * c + r];
+            for (uint32_t k = 0; k < nv; ++k) u += Y[(3 * c + r) * nv + k] * z[k];
+            w += l[r] * (u - target[3 * c + r] + reg[3 * c + r] * l[r]);
+        }
+        o.complementarity = fmax(o.complementarity, fabs(w));
+    }
+    if (zeta) for (uint32_t k = 0; k < nv; ++k) zeta[k] = z[k];
+    if (out) *out = o;
+    return o.status;
+}
+
+uint32_t oracle_quality_dense(uint32_t nv, uint32_t nc, const double* mass, const double* jacobian, const double* vf,
+                              const double* target, const double* reg, const double* mu, const double* warm,
+                              const OracleQualityConfig* cfg, double* lambda, double* velocity, OracleQualityOutcome* out) {
+    static __thread double L[MAXV * MAXV], Y[3 * MAXC * MAXV];
+    double uf[3 * MAXC], rg[3 * MAXC], w[MAXV];
+    if (nv > MAXV || nc > MAXC) return 3;
+    memcpy(L, mass, sizeof(double) * nv * nv);
+    if (!cholesky(L, nv)) {
+        if (out) { memset(out, 0, sizeof(*out)); out->status = 2; }
+        return 2;
+    }
+    for (uint32_t row = 0; row < 3 * nc; ++row) {
+        const double* g = jacobian + (size_t)row * nv;
+        double* y = Y + (size_t)row * nv;
+        for (uint32_t k = 0; k < nv; ++k) {
+            double acc = g[k];
+            for (uint32_t j = 0; j < k; ++j) acc -= L[k * nv + j] * y[j];
+            y[k] = acc / L[k * nv + k];
+        }
+        uf[row] = 0.0;
+        for (uint32_t d = 0; d < nv; ++d) uf[row] += g[d] * vf[d];
+        rg[row] = fmax(reg[row], cfg->regularization_floor);
+    }
+    const uint32_t st = oracle_quality_solve(nv, nc, Y, uf, target, rg, mu, warm, cfg, lambda, NULL, out);
+    for (uint32_t k = 0; k < nv; ++k) {
+        w[k] = 0.0;
+        for (uint32_t row = 0; row < 3 * nc; ++row) w[k] += Y[row * nv + k] * lambda[row];
+    }
+    for (int i = (int)nv - 1; i >= 0; --i) { /* L' x = w */
+        double s = w[i];
+        for (uint32_t k = (uint32_t)i + 1; k < nv; ++k) s -= L[k * nv + i] * w[k];
+        w[i] = s / L[i * nv + i];
+    }
+    for (uint32_t k = 0; k < nv; ++k) velocity[k] = vf[k] + w[k];
+    return st;
+}
+
+void oracle_world_set_quality(OracleWorld* world, const OracleQualityConfig* cfg) {
+    world->quality = cfg != NULL;
+    if (cfg) world->qcfg = *cfg;
+}
+
+/* ------------------------------------------------------------------ */
 /* Contact substep: scatter to ConstraintIR (Collision.metal:10253-10620), */
 /* IR evaluation (MetalWorldContact.metal:3580-3990), Wave32 temporalCone */
 /* solve (MetalWorldContact.metal:6142-7216), joint limits (:2878-2968),  */
@@ -1157,7 +1375,44 @@ static uint32_t contact_substep(const OracleWorld* o, double* q, double* v, cons
                 chol_solve(Mm, nv, Rc[3 * i + r]);
                 for (uint32_t d = 0; d < nv; ++d) Rc[3 * i + r][d] = rn(Rc[3 * i + r][d]);
             }
-        for (uint32_t i = 0; i < total; ++i) {
+        if (o->quality) {
+            /* Converged solve of the same contact problem: factor rows
+             * Y = L^-1 G' (W = G M^-1 G' = Y'Y), FP32-stored inputs. */
+            static __thread double Yq[3 * MAXC * MAXV];
+            double uf[3 * MAXC], tg[3 * MAXC], rg[3 * MAXC], muv[MAXC], warm[3 * MAXC], lam[3 * MAXC];
+            for (uint32_t i = 0; i < total; ++i) {
+                Contact* ct = &C[i];
+                for (int r = 0; r < 3; ++r) {
+                    double* y = Yq + (size_t)(3 * i + r) * nv;
+                    for (uint32_t k = 0; k < nv; ++k) {
+                        double acc = ct->G[r][k];
+                        for (uint32_t j = 0; j < k; ++j) acc -= Mm[k * nv + j] * y[j];
+                        y[k] = acc / Mm[k * nv + k];
+                    }
+                    for (uint32_t k = 0; k < nv; ++k) y[k] = rn(y[k]);
+                    uf[3 * i + r] = rn(ct->rel[r]);
+                    tg[3 * i + r] = ct->target[r];
+                    rg[3 * i + r] = fmax(ct->reg[r], o->qcfg.regularization_floor);
+                }
+                muv[i] = ct->mu;
+                oracle_project_cone(ct->lambda, ct->mu, ct->mu, warm + 3 * i);
+            }
+            OracleQualityOutcome qo;
+            const uint32_t qs = oracle_quality_solve(nv, total, Yq, uf, tg, rg, muv, warm, &o->qcfg, lam, NULL, &qo);
+            if (qs != 0) {
+                *fail_index = qo.newton;
+                return qs == 2 ? MR_STEP_FACTORIZATION_FAILED : (qs == 3 ? MR_STEP_NONFINITE_RESULT : MR_STEP_DID_NOT_CONVERGE);
+            }
+            for (uint32_t i = 0; i < total; ++i)
+                for (int r = 0; r < 3; ++r) C[i].lambda[r] = lam[3 * i + r];
+            for (uint32_t d = 0; d < nv; ++d) {
+                double acc = 0.0;
+                for (uint32_t i = 0; i < total; ++i)
+                    for (int r = 0; r < 3; ++r) acc += Rc[3 * i + r][d] * lam[3 * i + r];
+                v[d] = rn(v[d] + acc);
+            }
+        }
+        for (uint32_t i = 0; i < total && !o->quality; ++i) {
             Contact* ct = &C[i];
             double W[9];
             for (int r = 0; r < 3; ++r)
@@ -1180,8 +1435,8 @@ static uint32_t contact_substep(const OracleWorld* o, double* q, double* v, cons
             oracle_project_cone(ct->lambda, ct->mu, ct->mu, warm);
             for (int a = 0; a < 3; ++a) { ct->lambda[a] = warm[a]; ct->delta[a] = warm[a]; }
         }
-        const uint32_t iters = o->iters + (final_substep ? o->final_iters : 0u);
-        for (int it = -1; it < (int)iters; ++it) {
+        const uint32_t iters = o->quality ? 0u : o->iters + (final_substep ? o->final_iters : 0u);
+        for (int it = o->quality ? 0 : -1; it < (int)iters; ++it) {
             if (it >= 0) {
                 for (uint32_t i = 0; i < total; ++i) {
                     Contact* ct = &C[i];

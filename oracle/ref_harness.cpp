@@ -22,6 +22,7 @@
 #include "metalrobo/ConstraintSolver.hpp"
 #include "metalrobo/RigidBodyWorld.hpp"
 #include "metalrobo/EngineModel.hpp"
+#include "metalrobo/QualityContactSolver.hpp"
 #include "metalrobo/ReferenceConicSolver.hpp"
 
 #define NUMI_B200_OMIT_SHARED_ENUMS
@@ -308,6 +309,49 @@ __attribute__((visibility("default"))) int ref_conic_solve(uint32_t nv, const do
     for (uint32_t i = 0; i < 3 * n && i < s.impulses.size(); ++i) impulses[i] = s.impulses[i];
     for (uint32_t i = 0; i < nv && i < s.velocity.size(); ++i) velocity[i] = s.velocity[i];
     if (cone_violation) *cone_violation = s.maximumConeViolation;
+    return static_cast<int>(s.code);
+}
+
+// Converged quality solve of the same dense problem: the reference's
+// globalized semismooth Newton (solveQualityContactProblem,
+// src/core/QualityContactSolver.cpp:1480) with its default configuration.
+// certificates[8]: scaled KKT certificate, scaled natural residual, primal
+// and dual cone violation, conic complementarity, complementarity gap,
+// objective, normal-impulse violation.  Returns the status code.
+__attribute__((visibility("default"))) int ref_quality_solve(uint32_t nv, const double* inverse_mass, const double* free_velocity, uint32_t n,
+                                                             const double* jac, const double* mu, const double* target, const double* reg,
+                                                             double* impulses, double* velocity, double* certificates,
+                                                             uint32_t* iterations) {
+    DenseConicProblem p{};
+    p.nv = nv;
+    p.inverseMass.assign(inverse_mass, inverse_mass + nv * nv);
+    p.freeVelocity.assign(free_velocity, free_velocity + nv);
+    for (uint32_t i = 0; i < n; ++i) {
+        DenseContactBlock b{};
+        b.normalJacobian.assign(jac + (3 * i + 0) * nv, jac + (3 * i + 1) * nv);
+        b.tangentUJacobian.assign(jac + (3 * i + 1) * nv, jac + (3 * i + 2) * nv);
+        b.tangentVJacobian.assign(jac + (3 * i + 2) * nv, jac + (3 * i + 3) * nv);
+        b.targetVelocity = {target[3 * i], target[3 * i + 1], target[3 * i + 2]};
+        b.regularization = {reg[3 * i], reg[3 * i + 1], reg[3 * i + 2]};
+        b.warmImpulse = {0.0, 0.0, 0.0};
+        b.friction = mu[i];
+        p.contacts.push_back(b);
+    }
+    QualityContactSolverConfig cfg{};
+    const QualityContactSolution s = solveQualityContactProblem(p, cfg);
+    for (uint32_t i = 0; i < 3 * n && i < s.impulses.size(); ++i) impulses[i] = s.impulses[i];
+    for (uint32_t i = 0; i < nv && i < s.velocity.size(); ++i) velocity[i] = s.velocity[i];
+    if (certificates) {
+        certificates[0] = s.scaledKktCertificate;
+        certificates[1] = s.scaledNaturalResidual;
+        certificates[2] = s.maximumPrimalConeViolation;
+        certificates[3] = s.maximumDualConeViolation;
+        certificates[4] = s.maximumConicComplementarityResidual;
+        certificates[5] = s.complementarityGap;
+        certificates[6] = s.objective;
+        certificates[7] = s.maximumNormalImpulseViolation;
+    }
+    if (iterations) *iterations = s.iterations;
     return static_cast<int>(s.code);
 }
 

@@ -51,12 +51,15 @@ def rel_err(a: np.ndarray, b: np.ndarray) -> float:
 
 
 @functools.lru_cache(maxsize=8)
-def _tree_oracle(source: str, seed: int, h: float, substeps: int, iters: int):
+def _tree_oracle(source: str, seed: int, h: float, substeps: int, iters: int, quality: bool = False):
     import numi_lab_b200 as nb
-    from oracle import Oracle
+    from oracle import Oracle, quality_config
 
     rec = nb.compile_model(source, seed)
-    return rec, Oracle(rec, h, substeps, iters, 0)
+    oracle = Oracle(rec, h, substeps, iters, 0)
+    if quality:
+        oracle.set_quality(quality_config())
+    return rec, oracle
 
 
 @functools.lru_cache(maxsize=8)
@@ -83,11 +86,11 @@ def tree_env_step(job: dict) -> dict:
     """One articulated control step of one environment in the oracle, plus
     its input sensitivity.  job: source, seed, h, substeps, iters, q, v
     (float32), manifolds (bytes of the env's MRManifoldC slots), actions,
-    friction, rng."""
+    friction, rng; optional quality (the converged contact solve)."""
 
     from numi_lab_b200 import native
 
-    rec, oracle = _tree_oracle(job["source"], job["seed"], job["h"], job["substeps"], job["iters"])
+    rec, oracle = _tree_oracle(job["source"], job["seed"], job["h"], job["substeps"], job["iters"], bool(job.get("quality")))
     pairs = int(rec.world.pair_count)
 
     def run(q, v, rng=None):
