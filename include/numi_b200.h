@@ -604,7 +604,7 @@ typedef struct MRQualitySolverConfigC {
     uint32_t maximum_newton_iterations;        /* [100]                                       */
     uint32_t maximum_line_search_iterations;   /* [50] line-search evaluations per Newton step */
     double optimality_tolerance;               /* [1e-9] on the optimality measure above       */
-    double line_search_tolerance;              /* [1e-12] directional derivative, relative     */
+    double line_search_tolerance;              /* [0.1] |phi'(t)| relative to |phi'(0)|        */
     double regularization_floor;               /* [1e-6] per-row minimum of R                  */
     double reserved;
 } MRQualitySolverConfigC;

@@ -23,7 +23,7 @@ QualityConfig quality_config(const MRQualitySolverConfigC* c) {
     q.max_newton = c && c->maximum_newton_iterations ? static_cast<int>(c->maximum_newton_iterations) : 100;
     q.max_line_search = c && c->maximum_line_search_iterations ? static_cast<int>(c->maximum_line_search_iterations) : 50;
     q.tolerance = c && c->optimality_tolerance > 0.0 ? c->optimality_tolerance : 1.0e-9;
-    q.line_search_tolerance = c && c->line_search_tolerance > 0.0 ? c->line_search_tolerance : 1.0e-12;
+    q.line_search_tolerance = c && c->line_search_tolerance > 0.0 ? c->line_search_tolerance : 0.1;
     q.regularization_floor = c && c->regularization_floor > 0.0 ? c->regularization_floor : 1.0e-6;
     if (q.max_newton > 1000 || q.max_line_search > 200)
         throw std::invalid_argument("quality solver budgets are limited to 1000 Newton steps and 200 line-search evaluations");

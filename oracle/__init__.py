@@ -83,6 +83,8 @@ class OracleTrace(ct.Structure):
         ("max_normal_residual", ct.c_double),
         ("min_decision_margin", ct.c_double),
         ("contacts", OracleContact * MAX_CONTACTS),
+        ("quality_newton", ct.c_uint32),
+        ("quality_line_search", ct.c_uint32),
     ]
 
 
@@ -124,7 +126,7 @@ class QualityConfig(ct.Structure):
     ]
 
 
-def quality_config(max_newton: int = 100, max_line_search: int = 50, tolerance: float = 1e-9, line_search_tolerance: float = 1e-12,
+def quality_config(max_newton: int = 100, max_line_search: int = 50, tolerance: float = 1e-9, line_search_tolerance: float = 0.1,
                    regularization_floor: float = 1e-6) -> QualityConfig:
     return QualityConfig(max_newton, max_line_search, tolerance, line_search_tolerance, regularization_floor)
 

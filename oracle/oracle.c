@@ -1013,11 +1013,13 @@ static void chol_solve(const double* L, uint32_t n, double* x) { /* solveCholesk
 /* library's solver: Newton steps on the factor-space primal              */
 /* f(z) = 0.5|z|^2 + sum_c psi_c(u_free + Y_c'z), W = Y'Y, with the        */
 /* closed-form R-metric cone projection, an exact line search (the root   */
-/* of the monotone phi'(t) by safeguarded Newton steps in a bracket) and  */
-/* the stopping test |z - Y l|_inf <= tol (1 + |z|_inf + |Y l|_inf).  Its */
+/* of the monotone phi'(t) by safeguarded Newton steps in a bracket), a   */
+/* continuation on the regularisation floor, and the stopping test        */
+/* |z - Y l|_inf <= tol (1 + |z|_inf + |Y l|_inf).  Its                   */
 /* answers are pinned to the reference's solveQualityContactProblem.      */
 /* ------------------------------------------------------------------ */
-static double q_project(const double* u, const double* tg, const double* rg, double mu, double* lam, double* D) {
+static double q_project(const double* u, const double* tg, const double* rg_in, double mu, double rho, double* lam, double* D) {
+    const double rg[3] = {fmax(rg_in[0], rho), fmax(rg_in[1], rho), fmax(rg_in[2], rho)};
     const double e0 = u[0] - tg[0], e1 = u[1] - tg[1], e2 = u[2] - tg[2];
     const double a0 = -e0 / rg[0], a1 = -e1 / rg[1], a2 = -e2 / rg[2];
     for (int i = 0; i < 6; ++i) D[i] = 0.0;
@@ -1049,7 +1051,7 @@ static double q_project(const double* u, const double* tg, const double* rg, dou
 
 /* f at x; impulses, derivatives and gradient when the outputs are given. */
 static double q_eval(uint32_t nv, uint32_t nc, const double* Y, const double* uf, const double* tg, const double* rg,
-                     const double* mu, const double* x, double* lam, double* D, double* grad) {
+                     const double* mu, double rho, const double* x, double* lam, double* D, double* grad) {
     double f = 0.0, l[3], d[6];
     for (uint32_t d0 = 0; d0 < nv; ++d0) f += 0.5 * x[d0] * x[d0];
     for (uint32_t c = 0; c < nc; ++c) {
@@ -1058,7 +1060,7 @@ static double q_eval(uint32_t nv, uint32_t nc, const double* Y, const double* uf
             u[r] = uf[3 * c + r];
             for (uint32_t k = 0; k < nv; ++k) u[r] += Y[(3 * c + r) * nv + k] * x[k];
         }
-        f += q_project(u, tg + 3 * c, rg + 3 * c, mu[c], l, d);
+        f += q_project(u, tg + 3 * c, rg + 3 * c, mu[c], rho, l, d);
         if (lam) for (int r = 0; r < 3; ++r) lam[3 * c + r] = l[r];
         if (D) for (int i = 0; i < 6; ++i) D[6 * c + i] = d[i];
     }
@@ -1072,10 +1074,16 @@ static double q_eval(uint32_t nv, uint32_t nc, const double* Y, const double* uf
     return f;
 }
 
+/* Regularisation continuation: stages with every row's regularisation
+ * raised to 3000x and 30x the floor (to scaled optimality 1e-3), then the
+ * problem's own, each warm-started by the last. */
+static const double kQStageFloor[2] = {3000.0, 30.0};
+static const double kQStageTolerance = 1.0e-3;
+
 uint32_t oracle_quality_solve(uint32_t nv, uint32_t nc, const double* Y, const double* ufree, const double* target,
                               const double* reg, const double* mu, const double* warm, const OracleQualityConfig* cfg,
                               double* lambda, double* zeta, OracleQualityOutcome* out) {
-    double z[MAXV], grad[MAXV], dir[MAXV], trial[MAXV], H[MAXV * MAXV], D[6 * MAXC], U[3 * MAXC], Wd[3 * MAXC];
+    double z[MAXV], grad[MAXV], dir[MAXV], H[MAXV * MAXV], D[6 * MAXC], U[3 * MAXC], Wd[3 * MAXC];
     OracleQualityOutcome o;
     memset(&o, 0, sizeof(o));
     o.status = 1;
@@ -1085,81 +1093,88 @@ uint32_t oracle_quality_solve(uint32_t nv, uint32_t nc, const double* Y, const d
             for (uint32_t row = 0; row < 3 * nc; ++row) acc += Y[row * nv + k] * warm[row];
         z[k] = acc;
     }
-    double f = q_eval(nv, nc, Y, ufree, target, reg, mu, z, lambda, D, grad);
-    double scaled = 0.0;
-    for (int it = 0;; ++it) {
-        double gm = 0.0, zm = 0.0, ym = 0.0;
-        int finite = isfinite(f);
-        for (uint32_t k = 0; k < nv; ++k) {
-            gm = fmax(gm, fabs(grad[k]));
-            zm = fmax(zm, fabs(z[k]));
-            ym = fmax(ym, fabs(z[k] - grad[k]));
-            finite &= isfinite(grad[k]) && isfinite(z[k]);
-        }
-        if (!finite) { o.status = 3; break; }
-        scaled = gm / (1.0 + zm + ym);
-        if (scaled <= cfg->tolerance) { o.status = 0; break; }
-        if (it >= cfg->max_newton) break;
-        /* I + sum_c Y_c D_c Y_c' */
-        for (uint32_t i = 0; i < nv; ++i)
-            for (uint32_t j = 0; j < nv; ++j) H[i * nv + j] = i == j ? 1.0 : 0.0;
-        for (uint32_t c = 0; c < nc; ++c) {
-            const double* Dc = D + 6 * c;
-            const double M3[3][3] = {{Dc[0], Dc[1], Dc[2]}, {Dc[1], Dc[3], Dc[4]}, {Dc[2], Dc[4], Dc[5]}};
-            for (uint32_t j = 0; j < nv; ++j) {
-                double e[3];
-                for (int r = 0; r < 3; ++r) {
-                    e[r] = 0.0;
-                    for (int t = 0; t < 3; ++t) e[r] += M3[r][t] * Y[(3 * c + t) * nv + j];
-                }
-                for (uint32_t i = j; i < nv; ++i)
-                    H[i * nv + j] += Y[(3 * c) * nv + i] * e[0] + Y[(3 * c + 1) * nv + i] * e[1] + Y[(3 * c + 2) * nv + i] * e[2];
+    double f = 0.0, scaled = 0.0;
+    int broken = 0;
+    for (int stage = 0; stage < 3 && !broken; ++stage) {
+        const double rho = stage < 2 ? kQStageFloor[stage] * cfg->regularization_floor : 0.0;
+        const double tol = stage < 2 ? kQStageTolerance : cfg->tolerance;
+        f = q_eval(nv, nc, Y, ufree, target, reg, mu, rho, z, lambda, D, grad);
+        for (;;) {
+            double gm = 0.0, zm = 0.0, ym = 0.0;
+            int finite = isfinite(f);
+            for (uint32_t k = 0; k < nv; ++k) {
+                gm = fmax(gm, fabs(grad[k]));
+                zm = fmax(zm, fabs(z[k]));
+                ym = fmax(ym, fabs(z[k] - grad[k]));
+                finite &= isfinite(grad[k]) && isfinite(z[k]);
             }
-        }
-        for (uint32_t i = 0; i < nv; ++i)
-            for (uint32_t j = i + 1; j < nv; ++j) H[i * nv + j] = H[j * nv + i];
-        if (!cholesky(H, nv)) { o.status = 2; break; }
-        for (uint32_t k = 0; k < nv; ++k) dir[k] = -grad[k];
-        chol_solve(H, nv, dir);
-        double slope = 0.0;
-        for (uint32_t k = 0; k < nv; ++k) slope += grad[k] * dir[k];
-        if (!(slope < 0.0))
-            for (uint32_t k = 0; k < nv; ++k) dir[k] = -grad[k];
-        /* Exact line search: phi'(t) = a + t b - sum_c l_c(u_c + t w_c)' w_c. */
-        double a = 0.0, b = 0.0, slope0 = 0.0;
-        for (uint32_t k = 0; k < nv; ++k) { a += dir[k] * z[k]; b += dir[k] * dir[k]; slope0 += dir[k] * grad[k]; }
-        for (uint32_t c = 0; c < nc; ++c)
-            for (int r = 0; r < 3; ++r) {
-                double u = ufree[3 * c + r], w = 0.0;
-                for (uint32_t k = 0; k < nv; ++k) { u += Y[(3 * c + r) * nv + k] * z[k]; w += Y[(3 * c + r) * nv + k] * dir[k]; }
-                U[3 * c + r] = u;
-                Wd[3 * c + r] = w;
+            if (!finite) { o.status = 3; broken = 1; break; }
+            scaled = gm / (1.0 + zm + ym);
+            if (scaled <= tol) {
+                if (stage == 2) o.status = 0;
+                break;
             }
-        double lo = 0.0, hi = INFINITY, t = 1.0, best = INFINITY, best_t = 1.0;
-        for (int ls = 0; ls < cfg->max_line_search; ++ls) {
-            double dt = a + t * b, h2 = b, l[3], Dc[6], u[3];
+            if ((int)o.newton >= cfg->max_newton) { broken = 1; break; }
+            /* I + sum_c Y_c D_c Y_c' */
+            for (uint32_t i = 0; i < nv; ++i)
+                for (uint32_t j = 0; j < nv; ++j) H[i * nv + j] = i == j ? 1.0 : 0.0;
             for (uint32_t c = 0; c < nc; ++c) {
-                const double* w = Wd + 3 * c;
-                for (int r = 0; r < 3; ++r) u[r] = U[3 * c + r] + t * w[r];
-                q_project(u, target + 3 * c, reg + 3 * c, mu[c], l, Dc);
-                dt -= l[0] * w[0] + l[1] * w[1] + l[2] * w[2];
-                h2 += w[0] * (Dc[0] * w[0] + Dc[1] * w[1] + Dc[2] * w[2]) + w[1] * (Dc[1] * w[0] + Dc[3] * w[1] + Dc[4] * w[2]) +
-                      w[2] * (Dc[2] * w[0] + Dc[4] * w[1] + Dc[5] * w[2]);
+                const double* Dc = D + 6 * c;
+                const double M3[3][3] = {{Dc[0], Dc[1], Dc[2]}, {Dc[1], Dc[3], Dc[4]}, {Dc[2], Dc[4], Dc[5]}};
+                for (uint32_t j = 0; j < nv; ++j) {
+                    double e[3];
+                    for (int r = 0; r < 3; ++r) {
+                        e[r] = 0.0;
+                        for (int t = 0; t < 3; ++t) e[r] += M3[r][t] * Y[(3 * c + t) * nv + j];
+                    }
+                    for (uint32_t i = j; i < nv; ++i)
+                        H[i * nv + j] += Y[(3 * c) * nv + i] * e[0] + Y[(3 * c + 1) * nv + i] * e[1] + Y[(3 * c + 2) * nv + i] * e[2];
+                }
             }
-            o.line_search++;
-            if (fabs(dt) < best) { best = fabs(dt); best_t = t; }
-            if (fabs(dt) <= cfg->line_search_tolerance * fabs(slope0)) break;
-            if (dt < 0.0) lo = t;
-            else hi = t;
-            double tn = t - dt / h2;
-            if (!(tn > lo && tn < hi)) tn = isfinite(hi) ? 0.5 * (lo + hi) : 2.0 * t;
-            if (isfinite(hi) && hi - lo <= 1.0e-14 * hi) break;
-            t = tn;
+            for (uint32_t i = 0; i < nv; ++i)
+                for (uint32_t j = i + 1; j < nv; ++j) H[i * nv + j] = H[j * nv + i];
+            if (!cholesky(H, nv)) { o.status = 2; broken = 1; break; }
+            for (uint32_t k = 0; k < nv; ++k) dir[k] = -grad[k];
+            chol_solve(H, nv, dir);
+            double slope = 0.0;
+            for (uint32_t k = 0; k < nv; ++k) slope += grad[k] * dir[k];
+            if (!(slope < 0.0))
+                for (uint32_t k = 0; k < nv; ++k) dir[k] = -grad[k];
+            /* Exact line search: phi'(t) = a + t b - sum_c l_c(u_c + t w_c)' w_c. */
+            double a = 0.0, b = 0.0, slope0 = 0.0;
+            for (uint32_t k = 0; k < nv; ++k) { a += dir[k] * z[k]; b += dir[k] * dir[k]; slope0 += dir[k] * grad[k]; }
+            for (uint32_t c = 0; c < nc; ++c)
+                for (int r = 0; r < 3; ++r) {
+                    double u = ufree[3 * c + r], w = 0.0;
+                    for (uint32_t k = 0; k < nv; ++k) { u += Y[(3 * c + r) * nv + k] * z[k]; w += Y[(3 * c + r) * nv + k] * dir[k]; }
+                    U[3 * c + r] = u;
+                    Wd[3 * c + r] = w;
+                }
+            double lo = 0.0, hi = INFINITY, t = 1.0, best = INFINITY, best_t = 1.0;
+            for (int ls = 0; ls < cfg->max_line_search; ++ls) {
+                double dt = a + t * b, h2 = b, l[3], Dc[6], u[3];
+                for (uint32_t c = 0; c < nc; ++c) {
+                    const double* w = Wd + 3 * c;
+                    for (int r = 0; r < 3; ++r) u[r] = U[3 * c + r] + t * w[r];
+                    q_project(u, target + 3 * c, reg + 3 * c, mu[c], rho, l, Dc);
+                    dt -= l[0] * w[0] + l[1] * w[1] + l[2] * w[2];
+                    h2 += w[0] * (Dc[0] * w[0] + Dc[1] * w[1] + Dc[2] * w[2]) + w[1] * (Dc[1] * w[0] + Dc[3] * w[1] + Dc[4] * w[2]) +
+                          w[2] * (Dc[2] * w[0] + Dc[4] * w[1] + Dc[5] * w[2]);
+                }
+                o.line_search++;
+                if (fabs(dt) < best) { best = fabs(dt); best_t = t; }
+                if (fabs(dt) <= cfg->line_search_tolerance * fabs(slope0)) break;
+                if (dt < 0.0) lo = t;
+                else hi = t;
+                double tn = t - dt / h2;
+                if (!(tn > lo && tn < hi)) tn = isfinite(hi) ? 0.5 * (lo + hi) : 2.0 * t;
+                if (isfinite(hi) && hi - lo <= 1.0e-14 * hi) break;
+                t = tn;
+            }
+            for (uint32_t k = 0; k < nv; ++k) z[k] += best_t * dir[k];
+            f = q_eval(nv, nc, Y, ufree, target, reg, mu, rho, z, lambda, D, grad);
+            o.newton++;
         }
-        for (uint32_t k = 0; k < nv; ++k) trial[k] = z[k] + best_t * dir[k];
-        for (uint32_t k = 0; k < nv; ++k) z[k] = trial[k];
-        f = q_eval(nv, nc, Y, ufree, target, reg, mu, z, lambda, D, grad);
-        o.newton++;
     }
     o.residual = scaled;
     o.objective = f;
@@ -1215,6 +1230,47 @@ uint32_t oracle_quality_dense(uint32_t nv, uint32_t nc, const double* mass, cons
     }
     for (uint32_t k = 0; k < nv; ++k) velocity[k] = vf[k] + w[k];
     return st;
+}
+
+/* The last contact problem a control step on this thread handed to the
+ * converged solve (for diagnosing the solver on recorded problems). */
+static __thread uint32_t g_qlast_nv, g_qlast_nc;
+static __thread double g_qlast[3 * MAXC * MAXV + 16 * MAXC];
+
+uint32_t oracle_quality_last_problem(double* Y, double* ufree, double* target, double* reg, double* mu, double* warm, uint32_t* nv) {
+    const uint32_t n = g_qlast_nc, m = g_qlast_nv;
+    const double* p = g_qlast;
+    if (Y) memcpy(Y, p, sizeof(double) * 3 * n * m);
+    p += 3 * n * m;
+    if (ufree) memcpy(ufree, p, sizeof(double) * 3 * n);
+    p += 3 * n;
+    if (target) memcpy(target, p, sizeof(double) * 3 * n);
+    p += 3 * n;
+    if (reg) memcpy(reg, p, sizeof(double) * 3 * n);
+    p += 3 * n;
+    if (mu) memcpy(mu, p, sizeof(double) * n);
+    p += n;
+    if (warm) memcpy(warm, p, sizeof(double) * 3 * n);
+    if (nv) *nv = m;
+    return n;
+}
+
+static void quality_record(uint32_t nv, uint32_t nc, const double* Y, const double* uf, const double* tg, const double* rg,
+                           const double* mu, const double* warm) {
+    double* p = g_qlast;
+    g_qlast_nv = nv;
+    g_qlast_nc = nc;
+    memcpy(p, Y, sizeof(double) * 3 * nc * nv);
+    p += 3 * nc * nv;
+    memcpy(p, uf, sizeof(double) * 3 * nc);
+    p += 3 * nc;
+    memcpy(p, tg, sizeof(double) * 3 * nc);
+    p += 3 * nc;
+    memcpy(p, rg, sizeof(double) * 3 * nc);
+    p += 3 * nc;
+    memcpy(p, mu, sizeof(double) * nc);
+    p += nc;
+    memcpy(p, warm, sizeof(double) * 3 * nc);
 }
 
 void oracle_world_set_quality(OracleWorld* world, const OracleQualityConfig* cfg) {
@@ -1398,7 +1454,10 @@ static uint32_t contact_substep(const OracleWorld* o, double* q, double* v, cons
                 oracle_project_cone(ct->lambda, ct->mu, ct->mu, warm + 3 * i);
             }
             OracleQualityOutcome qo;
+            quality_record(nv, total, Yq, uf, tg, rg, muv, warm);
             const uint32_t qs = oracle_quality_solve(nv, total, Yq, uf, tg, rg, muv, warm, &o->qcfg, lam, NULL, &qo);
+            if (qo.newton > trace->quality_newton) trace->quality_newton = qo.newton;
+            trace->quality_line_search += qo.line_search;
             if (qs != 0) {
                 *fail_index = qo.newton;
                 return qs == 2 ? MR_STEP_FACTORIZATION_FAILED : (qs == 3 ? MR_STEP_NONFINITE_RESULT : MR_STEP_DID_NOT_CONVERGE);
