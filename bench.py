@@ -24,7 +24,10 @@ Lines printed (rank 0, one JSON line):
     batch (one persistent launch per horizon) against plain per-config
     kernels (mix_vs_plain) and per-world launches on concurrent streams;
   * serving: Poisson request streams against the continuous-batching
-    server (p50 / p99 latency).
+    server (p50 / p99 latency);
+  * quality_newton: the same world with the converged FP64 contact solve,
+    the solver class of the reference's CPU world step (cpu_baseline), and
+    its ratio to cpu_baseline.
 
 ``--impl reference`` times only that CPU reference (rank 0; other ranks exit).
 Multi-GPU (torchrun): one process per GPU; the job is world_size x 4096
@@ -318,6 +321,64 @@ def plain_aba_chain7(device) -> dict:
                      "frac": bytes_per_env_step * ok / (ms / 1e3) / 1e9 / peaks["hbm_gbs"]},
         "gpu_launches": steps,
     }
+
+
+def measure_quality(device, steps: int = 5) -> dict:
+    """The benchmark world (4096 tree29 environments, seed 2026, 4 x 5 ms
+    substeps) with the converged contact solve (MR_SOLVER_QUALITY_NEWTON):
+    every substep's contact problem solved in FP64 to scaled optimality
+    1e-9 -- the solver class the reference's CPU world step (the
+    cpu_baseline / reference arm) runs.  Device-resident, one CUDA-graph
+    advance of `steps` control steps after one warm-up advance."""
+
+    import torch
+
+    import numi_lab_b200 as nb
+
+    envs = ENVS
+    with nb.World("tree29", envs, substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT, seed=SEED) as world:
+        world.set_solver("quality_newton")
+        gen = torch.Generator(device=device).manual_seed(SEED)
+        acts = 0.3 * torch.randn((steps, envs, world.action_count), device=device, generator=gen)
+        status = torch.empty((steps, envs), device=device, dtype=torch.int32)
+        world.step(acts, status=status, wait=True)
+        torch.cuda.synchronize(device)
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        world.step(acts, status=status)
+        stop.record()
+        torch.cuda.synchronize(device)
+        ms = start.elapsed_time(stop)
+        failed = int((status != 0).sum().item())
+        diag = world.quality_diagnostics()
+    ok = envs * steps - failed
+    return {
+        "value": ok / (ms / 1e3),
+        "unit": UNIT,
+        "config": f"tree29: {envs} envs, {steps} control steps of 4 x 5 ms, PD targets ~ N(0, 0.3), converged FP64 contact "
+                  "solve (tolerance 1e-9, regularisation floor 1e-6), FP32 state, one CUDA-graph advance",
+        "ms_per_control_step": ms / steps,
+        "successful_env_steps": ok,
+        "failed_env_steps": failed,
+        "certificates": diag,
+        "gpu_launches": 2 * steps,
+    }
+
+
+def run_quality(args) -> None:
+    """One JSON line: the tree29 world with the converged contact solve
+    (measure_quality), `--envs` environments (default 4096) and `--steps`
+    control steps per timed advance."""
+
+    import torch
+
+    global ENVS
+    torch.cuda.set_device(0)
+    if args.envs:
+        ENVS = args.envs
+    line = {"metric": "quality contact env-steps/s", "workload": "quality", **measure_quality(torch.device("cuda", 0),
+                                                                                           steps=max(1, args.steps))}
+    print(json.dumps(line))
 
 
 SERVE_RATES = ((2000.0, 1.0), (400.0, 2.0), (100.0, 2.0), (25.0, 2.0))
@@ -941,10 +1002,12 @@ def main() -> None:
     parser.add_argument("--impl", default="native", choices=["native", "reference"])
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--envs", type=int, default=0, help="pile workload: environments (default 16384; smaller for profiling)")
-    parser.add_argument("--workload", default="tree29", choices=["tree29", "pile", "cylinder_pile", "mix", "precision", "policy"],
+    parser.add_argument("--workload", default="tree29",
+                        choices=["tree29", "pile", "cylinder_pile", "mix", "precision", "policy", "quality"],
                         help="tree29 (the headline), pile (36-body piles), cylinder_pile (36-body piles with cylinders: "
                              "GJK / EPA pairs), mix (chains, trees and piles) or precision (box stacks and trees against the "
-                             "FP64 oracle) or policy (tree29 closed loop under a native policy)")
+                             "FP64 oracle) or policy (tree29 closed loop under a native policy) or quality (tree29 with the "
+                             "converged FP64 contact solve)")
     parser.add_argument("--headline-only", action="store_true",
                         help="the 29-DoF contact line without the mix and serving measurements")
     parser.add_argument("--serve", action="store_true",
@@ -967,7 +1030,7 @@ def main() -> None:
     if args.workload != "tree29":
         if rank == 0:
             {"pile": run_pile, "cylinder_pile": lambda a: run_pile(a, "cylinder_pile"), "mix": run_mix,
-             "precision": run_precision, "policy": run_policy}[args.workload](args)
+             "precision": run_precision, "policy": run_policy, "quality": run_quality}[args.workload](args)
         return
 
     run_headline(args, rank, local_rank, world_size)
@@ -1095,12 +1158,13 @@ def run_headline(args, rank: int, local_rank: int, world_size: int) -> None:
     plain = plain_aba_chain7(device) if rank == 0 else None
     # The heterogeneous mix (batched vs plain per-config kernels) and the
     # serving stream, on rank 0 (bounded: a few horizons, one arrival rate).
-    mix = serving = None
+    mix = serving = quality = None
     if rank == 0 and not args.headline_only:
         mix_args = argparse.Namespace(steps=min(args.steps, 5), warmup=3, envs=0)
         mix = measure_mix(mix_args, device)
         mix["steps"] = mix_args.steps
         serving = measure_serving(SERVE_RATES[:1] + SERVE_RATES[2:3])
+        quality = measure_quality(device)
 
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
@@ -1159,7 +1223,11 @@ def run_headline(args, rank: int, local_rank: int, world_size: int) -> None:
             "plain_aba_chain7": plain,
             "heterogeneous_mix": mix,
             "serving": serving,
+            "quality_newton": quality,
         }
+        if quality and cpu and cpu.get("value"):
+            # The reference CPU arm runs the same (converged) solver class.
+            quality["vs_cpu_baseline"] = quality["value"] / cpu["value"]
         print(json.dumps(line))
     if dist is not None:
         dist.barrier()
