@@ -532,6 +532,52 @@ typedef struct MRPolicyPackC {
     float action_clip;
 } MRPolicyPackC;
 
+/* Persisted PolicyPacks (reference: c_api.h:562-573, 604-608; the file is
+ * numi-lab's learning-pack container, src/core/LearningPacks.cpp: a 32-byte
+ * header -- "MRLEARN\0", format version, kind 2, payload bytes, FNV-1a 64
+ * payload hash -- and the policy fields in MRPolicyPackC order).
+ * mr_write_policy_pack validates the pack (identity, non-zero revision, an
+ * exact contract: version 1 and non-zero fingerprints, positive finite
+ * clips, layer shapes, finite values, a critic for a stochastic actor) and
+ * writes a version-4 file atomically.  mr_learning_pack_content_hash is the
+ * payload hash.  mr_task_rollout_load_policy_pack reads a version 3 or 4
+ * file, applies the same rules and installs the policy as
+ * mr_task_rollout_set_policy does; a failed load leaves the installed
+ * policy unchanged.  Version-3 packs carry no contract and are refused, as
+ * the reference refuses them outside its migration path.  The contract's
+ * fingerprints are kept, not compared: this library's worlds are synthetic
+ * and carry no task program. */
+MR_API int mr_write_policy_pack(const MRPolicyPackC* policy, const char* policy_pack_path);
+MR_API uint64_t mr_learning_pack_content_hash(const void* payload, size_t byte_count);
+MR_API int mr_task_rollout_load_policy_pack(MRTaskRolloutHandle* handle, const char* policy_pack_path);
+
+/* No counterpart in the reference: reads a PolicyPack file without a
+ * device (header and payload checks as above, without the artifact rules)
+ * and reports its fields; with `parameters` non-null also copies every FP32
+ * table in file order (actor normalisation, actor layers' weights and bias,
+ * critic normalisation, critic layers, action log sigma, bias, scale). */
+typedef struct MRPolicyPackInfoC {
+    uint32_t format_version;
+    uint32_t layer_count;
+    uint32_t critic_layer_count;
+    uint32_t observation_count;     /* inputs of the first actor layer  */
+    uint32_t action_count;          /* outputs of the last actor layer  */
+    uint32_t stochastic;            /* action log sigma present         */
+    uint64_t revision;
+    uint64_t content_hash;
+    uint64_t contract_version;
+    uint64_t world_fingerprint;
+    uint64_t task_fingerprint;
+    uint64_t observation_fingerprint;
+    uint64_t action_fingerprint;
+    uint64_t parameter_count;       /* FP32 values in all tables        */
+    float observation_clip;
+    float action_clip;
+    char id[64];                    /* truncated, NUL-terminated        */
+} MRPolicyPackInfoC;
+MR_API int mr_policy_pack_inspect(const char* policy_pack_path, MRPolicyPackInfoC* info, float* parameters,
+                                  size_t parameter_capacity);
+
 /* reference: c_api.h:597-603.  Copies every span; later advances take no
  * action stream (action count 0) and evaluate the policy on the device
  * before each control step, from the resident state. */

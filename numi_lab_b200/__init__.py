@@ -10,6 +10,7 @@ worlds in one launch per control step) and ``serve``
 
 from .native import MetalRoboError, bindings
 from .serve import Server
-from .world import Batch, World, compile_model, quality_solve, sample_reset
+from .world import Batch, World, compile_model, inspect_policy_pack, quality_solve, sample_reset, write_policy_pack
 
-__all__ = ["Batch", "MetalRoboError", "Server", "World", "bindings", "compile_model", "quality_solve", "sample_reset"]
+__all__ = ["Batch", "MetalRoboError", "Server", "World", "bindings", "compile_model", "inspect_policy_pack", "quality_solve",
+           "sample_reset", "write_policy_pack"]

@@ -1,0 +1,420 @@
+// PolicyPack reading and writing (packs.h) and the C-ABI entry points that
+// need no rollout: mr_write_policy_pack, mr_learning_pack_content_hash and
+// mr_policy_pack_inspect.  mr_task_rollout_load_policy_pack (rollout.cu)
+// reads through read_policy_pack and installs like mr_task_rollout_set_policy.
+#include "packs.h"
+
+#include <cerrno>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <stdexcept>
+
+#include <fcntl.h>
+#include <unistd.h>
+
+namespace numi {
+namespace rt {
+void set_last_error(const std::string& message);
+}  // namespace rt
+
+namespace {
+
+constexpr char kMagic[8] = {'M', 'R', 'L', 'E', 'A', 'R', 'N', '\0'};
+constexpr std::size_t kHeaderBytes = 32;
+constexpr std::uint64_t kMaxPayload = 0xffffffffull;
+
+// Appends little-endian fields (the host is little-endian: x86-64, aarch64).
+struct Sink {
+    std::vector<std::uint8_t> bytes;
+    void raw(const void* p, std::size_t n) {
+        const auto* b = static_cast<const std::uint8_t*>(p);
+        bytes.insert(bytes.end(), b, b + n);
+    }
+    void u32(std::uint32_t v) { raw(&v, 4); }
+    void u64(std::uint64_t v) { raw(&v, 8); }
+    void f32(float v) { raw(&v, 4); }
+    void text(const std::string& s) {
+        u64(s.size());
+        raw(s.data(), s.size());
+    }
+    void floats(const std::vector<float>& v) {
+        u64(v.size());
+        if (!v.empty()) raw(v.data(), v.size() * sizeof(float));
+    }
+    void layers(const std::vector<PolicyPackLayer>& ls) {
+        u64(ls.size());
+        for (const PolicyPackLayer& l : ls) {
+            u32(l.input_count);
+            u32(l.output_count);
+            u32(l.activation);
+            floats(l.weights);
+            floats(l.bias);
+        }
+    }
+};
+
+// Bounded reads; every accessor returns false past the end.
+struct Source {
+    const std::uint8_t* p;
+    std::size_t n, at = 0;
+    bool raw(void* out, std::size_t k) {
+        if (k > n - at) return false;
+        std::memcpy(out, p + at, k);
+        at += k;
+        return true;
+    }
+    bool u32(std::uint32_t& v) { return raw(&v, 4); }
+    bool u64(std::uint64_t& v) { return raw(&v, 8); }
+    bool f32(float& v) { return raw(&v, 4); }
+    bool text(std::string& s) {
+        std::uint64_t k = 0;
+        if (!u64(k) || k > n - at || k > kMaxPayload) return false;
+        s.assign(reinterpret_cast<const char*>(p + at), static_cast<std::size_t>(k));
+        at += static_cast<std::size_t>(k);
+        return true;
+    }
+    bool floats(std::vector<float>& v) {
+        std::uint64_t k = 0;
+        if (!u64(k) || k > kMaxPayload || k > (n - at) / sizeof(float)) return false;
+        v.resize(static_cast<std::size_t>(k));
+        return k == 0 || raw(v.data(), v.size() * sizeof(float));
+    }
+    bool layers(std::vector<PolicyPackLayer>& ls) {
+        std::uint64_t k = 0;
+        // Each layer takes at least 28 bytes: a corrupt count fails here.
+        if (!u64(k) || k > kMaxPayload || k > (n - at) / 28) return false;
+        ls.resize(static_cast<std::size_t>(k));
+        for (PolicyPackLayer& l : ls)
+            if (!u32(l.input_count) || !u32(l.output_count) || !u32(l.activation) || !floats(l.weights) || !floats(l.bias))
+                return false;
+        return true;
+    }
+    bool done() const { return at == n; }
+};
+
+std::vector<std::uint8_t> encode(const PolicyPackData& d) {
+    Sink s;
+    s.text(d.id);
+    s.u64(d.revision);
+    s.floats(d.observation_mean);
+    s.floats(d.observation_inverse_std);
+    s.layers(d.layers);
+    s.floats(d.critic_observation_mean);
+    s.floats(d.critic_observation_inverse_std);
+    s.layers(d.critic_layers);
+    s.floats(d.action_log_std);
+    s.floats(d.action_bias);
+    s.floats(d.action_scale);
+    s.f32(d.observation_clip);
+    s.f32(d.action_clip);
+    s.u64(d.contract_version);
+    s.u64(d.world_fingerprint);
+    s.u64(d.task_fingerprint);
+    s.u64(d.observation_fingerprint);
+    s.u64(d.action_fingerprint);
+    return s.bytes;
+}
+
+bool contract_exact(const PolicyPackData& d) {
+    return d.contract_version == 1 && d.world_fingerprint != 0 && d.task_fingerprint != 0 && d.observation_fingerprint != 0 &&
+           d.action_fingerprint != 0;
+}
+
+bool decode(const std::uint8_t* bytes, std::size_t count, std::uint32_t version, PolicyPackData& d) {
+    Source s{bytes, count};
+    if (!(s.text(d.id) && s.u64(d.revision) && s.floats(d.observation_mean) && s.floats(d.observation_inverse_std) &&
+          s.layers(d.layers) && s.floats(d.critic_observation_mean) && s.floats(d.critic_observation_inverse_std) &&
+          s.layers(d.critic_layers) && s.floats(d.action_log_std) && s.floats(d.action_bias) && s.floats(d.action_scale) &&
+          s.f32(d.observation_clip) && s.f32(d.action_clip)))
+        return false;
+    if (version < 4) return s.done();  // no contract before version 4
+    return s.u64(d.contract_version) && s.u64(d.world_fingerprint) && s.u64(d.task_fingerprint) &&
+           s.u64(d.observation_fingerprint) && s.u64(d.action_fingerprint) && contract_exact(d) && s.done();
+}
+
+bool finite(const std::vector<float>& v) {
+    for (float x : v)
+        if (!std::isfinite(x)) return false;
+    return true;
+}
+
+void copy_floats(std::vector<float>& out, const float* p, size_t n, const char* what) {
+    if (n != 0 && !p) throw std::invalid_argument(std::string(what) + " is null with a non-zero count");
+    out.assign(p, p + n);
+}
+
+void copy_layers(std::vector<PolicyPackLayer>& out, const MRPolicyDenseLayerC* ls, size_t n, const char* what) {
+    if (n != 0 && !ls) throw std::invalid_argument(std::string(what) + " are null with a non-zero count");
+    out.resize(n);
+    for (size_t i = 0; i < n; ++i) {
+        out[i].input_count = ls[i].input_count;
+        out[i].output_count = ls[i].output_count;
+        out[i].activation = ls[i].activation;
+        copy_floats(out[i].weights, ls[i].weights, ls[i].weight_count, "layer weights");
+        copy_floats(out[i].bias, ls[i].bias, ls[i].bias_count, "layer bias");
+    }
+}
+
+}  // namespace
+
+std::uint64_t learning_pack_hash(const void* bytes, std::size_t count) {
+    std::uint64_t h = 14695981039346656037ull;  // FNV-1a 64 offset basis
+    const auto* b = static_cast<const std::uint8_t*>(bytes);
+    for (std::size_t i = 0; i < count; ++i) {
+        h ^= b[i];
+        h *= 1099511628211ull;  // FNV 64 prime
+    }
+    return h == 0 ? 1 : h;
+}
+
+PolicyPackData policy_pack_from_c(const MRPolicyPackC& c) {
+    PolicyPackData d;
+    d.id = c.id ? c.id : "";
+    d.revision = c.revision;
+    d.contract_version = c.contract_version;
+    d.world_fingerprint = c.world_fingerprint;
+    d.task_fingerprint = c.task_fingerprint;
+    d.observation_fingerprint = c.observation_fingerprint;
+    d.action_fingerprint = c.action_fingerprint;
+    copy_floats(d.observation_mean, c.observation_mean, c.observation_mean_count, "observation_mean");
+    copy_floats(d.observation_inverse_std, c.observation_inverse_standard_deviation,
+                c.observation_inverse_standard_deviation_count, "observation_inverse_standard_deviation");
+    copy_layers(d.layers, c.layers, c.layer_count, "layers");
+    copy_floats(d.critic_observation_mean, c.critic_observation_mean, c.critic_observation_mean_count, "critic_observation_mean");
+    copy_floats(d.critic_observation_inverse_std, c.critic_observation_inverse_standard_deviation,
+                c.critic_observation_inverse_standard_deviation_count, "critic_observation_inverse_standard_deviation");
+    copy_layers(d.critic_layers, c.critic_layers, c.critic_layer_count, "critic_layers");
+    copy_floats(d.action_log_std, c.action_log_standard_deviation, c.action_log_standard_deviation_count,
+                "action_log_standard_deviation");
+    copy_floats(d.action_bias, c.action_bias, c.action_bias_count, "action_bias");
+    copy_floats(d.action_scale, c.action_scale, c.action_scale_count, "action_scale");
+    d.observation_clip = c.observation_clip;
+    d.action_clip = c.action_clip;
+    return d;
+}
+
+MRPolicyPackC policy_pack_view(const PolicyPackData& d, std::vector<MRPolicyDenseLayerC>& storage) {
+    storage.clear();
+    storage.reserve(d.layers.size() + d.critic_layers.size());
+    auto add = [&](const PolicyPackLayer& l) {
+        storage.push_back(MRPolicyDenseLayerC{l.input_count, l.output_count, l.activation, l.weights.data(), l.weights.size(),
+                                              l.bias.data(), l.bias.size()});
+    };
+    for (const PolicyPackLayer& l : d.layers) add(l);
+    for (const PolicyPackLayer& l : d.critic_layers) add(l);
+    MRPolicyPackC c{};
+    c.id = d.id.c_str();
+    c.revision = d.revision;
+    c.contract_version = d.contract_version;
+    c.world_fingerprint = d.world_fingerprint;
+    c.task_fingerprint = d.task_fingerprint;
+    c.observation_fingerprint = d.observation_fingerprint;
+    c.action_fingerprint = d.action_fingerprint;
+    c.observation_mean = d.observation_mean.data();
+    c.observation_mean_count = d.observation_mean.size();
+    c.observation_inverse_standard_deviation = d.observation_inverse_std.data();
+    c.observation_inverse_standard_deviation_count = d.observation_inverse_std.size();
+    c.layers = storage.data();
+    c.layer_count = d.layers.size();
+    c.critic_observation_mean = d.critic_observation_mean.data();
+    c.critic_observation_mean_count = d.critic_observation_mean.size();
+    c.critic_observation_inverse_standard_deviation = d.critic_observation_inverse_std.data();
+    c.critic_observation_inverse_standard_deviation_count = d.critic_observation_inverse_std.size();
+    c.critic_layers = storage.data() + d.layers.size();
+    c.critic_layer_count = d.critic_layers.size();
+    c.action_log_standard_deviation = d.action_log_std.data();
+    c.action_log_standard_deviation_count = d.action_log_std.size();
+    c.action_bias = d.action_bias.data();
+    c.action_bias_count = d.action_bias.size();
+    c.action_scale = d.action_scale.data();
+    c.action_scale_count = d.action_scale.size();
+    c.observation_clip = d.observation_clip;
+    c.action_clip = d.action_clip;
+    return c;
+}
+
+void validate_policy_pack(const PolicyPackData& d) {
+    if (d.id.empty() || d.revision == 0 || d.layers.empty())
+        throw std::invalid_argument("PolicyPack needs an id, a non-zero revision and at least one actor layer");
+    if (!contract_exact(d))
+        throw std::invalid_argument("PolicyPack semantic contract is not exact (version 1 and non-zero world, task, "
+                                    "observation and action fingerprints)");
+    if (!std::isfinite(d.observation_clip) || !(d.observation_clip > 0.0f) || !std::isfinite(d.action_clip) ||
+        !(d.action_clip > 0.0f))
+        throw std::invalid_argument("PolicyPack clips must be positive and finite");
+    auto check = [](const std::vector<PolicyPackLayer>& ls, const char* net) {
+        for (size_t i = 0; i < ls.size(); ++i) {
+            const PolicyPackLayer& l = ls[i];
+            if (l.input_count == 0 || l.output_count == 0 || l.activation > MR_POLICY_ACTIVATION_C_SILU ||
+                l.weights.size() != static_cast<size_t>(l.input_count) * l.output_count || l.bias.size() != l.output_count ||
+                !finite(l.weights) || !finite(l.bias))
+                throw std::invalid_argument(std::string("PolicyPack ") + net + " layer " + std::to_string(i) +
+                                            " has an invalid shape, activation or value");
+        }
+    };
+    check(d.layers, "actor");
+    check(d.critic_layers, "critic");
+    if (!d.action_log_std.empty() && d.critic_layers.empty())
+        throw std::invalid_argument("a stochastic PolicyPack (action_log_standard_deviation) needs a critic");
+    if (!finite(d.observation_mean) || !finite(d.observation_inverse_std) || !finite(d.critic_observation_mean) ||
+        !finite(d.critic_observation_inverse_std) || !finite(d.action_log_std) || !finite(d.action_bias) ||
+        !finite(d.action_scale))
+        throw std::invalid_argument("PolicyPack normalisation and action tables must be finite");
+}
+
+void write_policy_pack(const PolicyPackData& d, const std::string& path) {
+    if (path.empty()) throw std::invalid_argument("PolicyPack output path is empty");
+    validate_policy_pack(d);
+    const std::vector<std::uint8_t> payload = encode(d);
+    if (payload.size() > kMaxPayload) throw std::invalid_argument("PolicyPack payload exceeds 4 GiB");
+    std::uint8_t header[kHeaderBytes];
+    const std::uint32_t version = kPolicyPackVersion, kind = kPolicyPackKind;
+    const std::uint64_t bytes = payload.size(), hash = learning_pack_hash(payload.data(), payload.size());
+    std::memcpy(header, kMagic, 8);
+    std::memcpy(header + 8, &version, 4);
+    std::memcpy(header + 12, &kind, 4);
+    std::memcpy(header + 16, &bytes, 8);
+    std::memcpy(header + 24, &hash, 8);
+    // Publish atomically: write a sibling temporary, flush it, rename it.
+    std::string tmpl = path + ".tmp.XXXXXX";
+    std::vector<char> name(tmpl.begin(), tmpl.end());
+    name.push_back('\0');
+    const int fd = ::mkstemp(name.data());
+    if (fd < 0) throw std::runtime_error("cannot create a temporary beside " + path + ": " + std::strerror(errno));
+    auto put = [&](const std::uint8_t* p, std::size_t n) {
+        while (n > 0) {
+            const ssize_t w = ::write(fd, p, n);
+            if (w < 0) {
+                if (errno == EINTR) continue;
+                return false;
+            }
+            p += w;
+            n -= static_cast<std::size_t>(w);
+        }
+        return true;
+    };
+    const bool ok = put(header, kHeaderBytes) && put(payload.data(), payload.size()) && ::fsync(fd) == 0;
+    const int err = errno;
+    const bool closed = ::close(fd) == 0;
+    if (!ok || !closed || ::rename(name.data(), path.c_str()) != 0) {
+        const int e = ok && closed ? errno : err;
+        ::unlink(name.data());
+        throw std::runtime_error("cannot write " + path + ": " + std::strerror(e));
+    }
+}
+
+PolicyPackData read_policy_pack(const std::string& path) {
+    std::ifstream in(path, std::ios::binary | std::ios::ate);
+    if (!in) throw std::invalid_argument("cannot open PolicyPack " + path);
+    const std::streamoff size = in.tellg();
+    if (size < static_cast<std::streamoff>(kHeaderBytes) || static_cast<std::uint64_t>(size) > kHeaderBytes + kMaxPayload)
+        throw std::invalid_argument("PolicyPack " + path + " has an invalid length");
+    in.seekg(0);
+    std::uint8_t header[kHeaderBytes];
+    if (!in.read(reinterpret_cast<char*>(header), kHeaderBytes)) throw std::invalid_argument("cannot read the PolicyPack header");
+    std::uint32_t version = 0, kind = 0;
+    std::uint64_t bytes = 0, hash = 0;
+    std::memcpy(&version, header + 8, 4);
+    std::memcpy(&kind, header + 12, 4);
+    std::memcpy(&bytes, header + 16, 8);
+    std::memcpy(&hash, header + 24, 8);
+    if (std::memcmp(header, kMagic, 8) != 0 || kind != kPolicyPackKind)
+        throw std::invalid_argument("not a PolicyPack (learning-pack magic or artifact kind differs)");
+    if (version < kPolicyPackOldestVersion || version > kPolicyPackVersion)
+        throw std::invalid_argument("PolicyPack format version " + std::to_string(version) + " is not supported (3-4)");
+    if (bytes != static_cast<std::uint64_t>(size) - kHeaderBytes)
+        throw std::invalid_argument("PolicyPack payload length does not match the file");
+    std::vector<std::uint8_t> payload(static_cast<std::size_t>(bytes));
+    if (bytes && !in.read(reinterpret_cast<char*>(payload.data()), static_cast<std::streamsize>(bytes)))
+        throw std::invalid_argument("cannot read the PolicyPack payload");
+    if (learning_pack_hash(payload.data(), payload.size()) != hash)
+        throw std::invalid_argument("PolicyPack payload hash does not match its header (corrupt file)");
+    PolicyPackData d;
+    if (!decode(payload.data(), payload.size(), version, d)) throw std::invalid_argument("PolicyPack payload is malformed");
+    d.format_version = version;
+    d.content_hash = hash;
+    return d;
+}
+
+}  // namespace numi
+
+extern "C" {
+
+MR_API int mr_write_policy_pack(const MRPolicyPackC* policy, const char* policy_pack_path) {
+    try {
+        if (!policy || !policy_pack_path || !policy_pack_path[0])
+            throw std::invalid_argument("a PolicyPack and an output path are required");
+        numi::write_policy_pack(numi::policy_pack_from_c(*policy), policy_pack_path);
+        return 0;
+    } catch (const std::exception& e) {
+        numi::rt::set_last_error(std::string("PolicyPack write failed: ") + e.what());
+    }
+    return -1;
+}
+
+MR_API uint64_t mr_learning_pack_content_hash(const void* payload, size_t byte_count) {
+    if (!payload && byte_count != 0) return 0;
+    return numi::learning_pack_hash(payload, byte_count);
+}
+
+MR_API int mr_policy_pack_inspect(const char* policy_pack_path, MRPolicyPackInfoC* info, float* parameters,
+                                  size_t parameter_capacity) {
+    try {
+        if (!policy_pack_path || !info) throw std::invalid_argument("a path and an info output are required");
+        const numi::PolicyPackData d = numi::read_policy_pack(policy_pack_path);
+        MRPolicyPackInfoC out{};
+        out.format_version = d.format_version;
+        out.layer_count = static_cast<uint32_t>(d.layers.size());
+        out.critic_layer_count = static_cast<uint32_t>(d.critic_layers.size());
+        out.observation_count = d.layers.empty() ? 0u : d.layers.front().input_count;
+        out.action_count = d.layers.empty() ? 0u : d.layers.back().output_count;
+        out.stochastic = d.action_log_std.empty() ? 0u : 1u;
+        out.revision = d.revision;
+        out.content_hash = d.content_hash;
+        out.contract_version = d.contract_version;
+        out.world_fingerprint = d.world_fingerprint;
+        out.task_fingerprint = d.task_fingerprint;
+        out.observation_fingerprint = d.observation_fingerprint;
+        out.action_fingerprint = d.action_fingerprint;
+        out.observation_clip = d.observation_clip;
+        out.action_clip = d.action_clip;
+        std::snprintf(out.id, sizeof(out.id), "%s", d.id.c_str());
+        // Every FP32 table in wire order.
+        std::vector<const std::vector<float>*> tables{&d.observation_mean, &d.observation_inverse_std};
+        for (const numi::PolicyPackLayer& l : d.layers) {
+            tables.push_back(&l.weights);
+            tables.push_back(&l.bias);
+        }
+        tables.push_back(&d.critic_observation_mean);
+        tables.push_back(&d.critic_observation_inverse_std);
+        for (const numi::PolicyPackLayer& l : d.critic_layers) {
+            tables.push_back(&l.weights);
+            tables.push_back(&l.bias);
+        }
+        tables.push_back(&d.action_log_std);
+        tables.push_back(&d.action_bias);
+        tables.push_back(&d.action_scale);
+        std::size_t total = 0;
+        for (const auto* t : tables) total += t->size();
+        out.parameter_count = total;
+        if (parameters) {
+            if (parameter_capacity < total)
+                throw std::invalid_argument("parameters holds " + std::to_string(parameter_capacity) + " floats; the pack has " +
+                                            std::to_string(total));
+            std::size_t at = 0;
+            for (const auto* t : tables) {
+                if (!t->empty()) std::memcpy(parameters + at, t->data(), t->size() * sizeof(float));
+                at += t->size();
+            }
+        }
+        *info = out;
+        return 0;
+    } catch (const std::exception& e) {
+        numi::rt::set_last_error(e.what());
+    }
+    return -1;
+}
+
+}  // extern "C"

@@ -13,6 +13,7 @@
 #include "mix.h"
 #include "model.h"
 #include "numi_b200.h"
+#include "packs.h"
 #include "policy.h"
 #include "quality.cuh"
 #include "runtime.h"
@@ -1163,6 +1164,27 @@ void drop_graphs(MRTaskRolloutHandle& h) {
 
 }  // namespace
 
+MR_API int mr_task_rollout_load_policy_pack(MRTaskRolloutHandle* handle, const char* policy_pack_path) {
+    return guarded([&] {
+        if (!handle) throw std::invalid_argument("handle is null");
+        if (!policy_pack_path || !policy_pack_path[0]) throw std::invalid_argument("PolicyPack path is empty");
+        if (handle->scene) throw std::invalid_argument("pile and stack worlds take no actions; a policy cannot drive them");
+        const numi::PolicyPackData pack = numi::read_policy_pack(policy_pack_path);
+        // The artifact rules of the reference's compile step: an exact
+        // semantic contract (so version-3 packs, which carry none, need the
+        // reference's explicit migration first), shapes and values.
+        numi::validate_policy_pack(pack);
+        std::vector<MRPolicyDenseLayerC> layers;
+        const MRPolicyPackC view = numi::policy_pack_view(pack, layers);
+        check(numi::configure_policy_kernel(), "policy kernel attributes");
+        std::unique_ptr<InstalledPolicy> compiled = compile_policy(*handle, view);
+        // A failed load returns above and leaves the installed policy in place.
+        drop_graphs(*handle);
+        handle->policy = std::move(compiled);
+        handle->have_policy_outputs = false;
+    });
+}
+
 MR_API int mr_task_rollout_set_policy(MRTaskRolloutHandle* handle, const MRPolicyPackC* policy) {
     return guarded([&] {
         if (!handle) throw std::invalid_argument("handle is null");
@@ -1484,7 +1506,6 @@ MR_API int mr_task_rollout_launch_shape(const MRTaskRolloutHandle* handle, uint3
                                         uint32_t* resident_warps_per_sm) {
     return guarded([&] {
         if (!handle) throw std::invalid_argument("handle is null");
-        const std::uint32_t prec = handle->precision;
         if (warps_per_block) *warps_per_block = handle->scene ? 1u : static_cast<uint32_t>(handle->step_warps_per_block());
         if (resident_warps_per_sm) *resident_warps_per_sm = handle->scene ? 0u : static_cast<uint32_t>(handle->step_resident_warps_per_sm());
     });

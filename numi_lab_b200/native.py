@@ -162,6 +162,28 @@ class QualityDiagnosticsC(ct.Structure):
     ]
 
 
+class PolicyPackInfoC(ct.Structure):
+    _fields_ = [
+        ("format_version", ct.c_uint32),
+        ("layer_count", ct.c_uint32),
+        ("critic_layer_count", ct.c_uint32),
+        ("observation_count", ct.c_uint32),
+        ("action_count", ct.c_uint32),
+        ("stochastic", ct.c_uint32),
+        ("revision", ct.c_uint64),
+        ("content_hash", ct.c_uint64),
+        ("contract_version", ct.c_uint64),
+        ("world_fingerprint", ct.c_uint64),
+        ("task_fingerprint", ct.c_uint64),
+        ("observation_fingerprint", ct.c_uint64),
+        ("action_fingerprint", ct.c_uint64),
+        ("parameter_count", ct.c_uint64),
+        ("observation_clip", ct.c_float),
+        ("action_clip", ct.c_float),
+        ("id", ct.c_char * 64),
+    ]
+
+
 class QualityResultC(ct.Structure):
     _fields_ = [
         ("code", ct.c_uint32),
@@ -527,6 +549,10 @@ EXPORTED_SYMBOLS: Final = (
     "mr_task_rollout_set_solver",
     "mr_task_rollout_quality_diagnostics",
     "mr_quality_solve_batch",
+    "mr_write_policy_pack",
+    "mr_learning_pack_content_hash",
+    "mr_task_rollout_load_policy_pack",
+    "mr_policy_pack_inspect",
 )
 
 
@@ -689,6 +715,14 @@ class Bindings:
         L.mr_quality_solve_batch.argtypes = [ct.c_uint32, ct.c_uint32, ct.c_uint32, P(ct.c_uint32), PD, PD, PD, PD, PD, PD, PD,
                                              P(QualitySolverConfigC), PD, PD, P(QualityResultC)]
         L.mr_quality_solve_batch.restype = ct.c_int
+        L.mr_write_policy_pack.argtypes = [P(PolicyPackC), ct.c_char_p]
+        L.mr_write_policy_pack.restype = ct.c_int
+        L.mr_learning_pack_content_hash.argtypes = [ct.c_void_p, ct.c_size_t]
+        L.mr_learning_pack_content_hash.restype = ct.c_uint64
+        L.mr_task_rollout_load_policy_pack.argtypes = [ct.c_void_p, ct.c_char_p]
+        L.mr_task_rollout_load_policy_pack.restype = ct.c_int
+        L.mr_policy_pack_inspect.argtypes = [ct.c_char_p, P(PolicyPackInfoC), P(ct.c_float), ct.c_size_t]
+        L.mr_policy_pack_inspect.restype = ct.c_int
 
     def last_error(self) -> str:
         value = self.lib.mr_last_error()

@@ -13,6 +13,7 @@ pointers and shapes.  A missing library raises ``FileNotFoundError``.
 from __future__ import annotations
 
 import ctypes as ct
+import os
 from dataclasses import dataclass
 from typing import Any, Sequence
 
@@ -140,6 +141,97 @@ def pile_seeds_by_body_count(bodies: Sequence[int], first_seed: int = 0) -> dict
             out[n] = seed
         seed += 1
     return out
+
+
+def policy_pack_c(
+    layers: Sequence[tuple[np.ndarray, np.ndarray | None, str]],
+    *,
+    revision: int,
+    action_clip: float,
+    policy_id: str = "policy",
+    observation_mean: np.ndarray | None = None,
+    observation_inverse_std: np.ndarray | None = None,
+    observation_clip: float = 0.0,
+    critic_layers: Sequence[tuple[np.ndarray, np.ndarray | None, str]] = (),
+    critic_observation_mean: np.ndarray | None = None,
+    critic_observation_inverse_std: np.ndarray | None = None,
+    action_log_std: np.ndarray | None = None,
+    action_bias: np.ndarray | None = None,
+    action_scale: np.ndarray | None = None,
+    contract: tuple[int, int, int, int, int] = (0, 0, 0, 0, 0),
+):
+    """An MRPolicyPackC over the given arrays, and the list of objects that
+    must outlive it.  `layers` are (weights [out][in], bias [out] or None,
+    activation name); `contract` is (version, world, task, observation,
+    action fingerprints)."""
+
+    keep: list[Any] = []
+
+    def arr(a):
+        if a is None:
+            return None, 0
+        a = np.ascontiguousarray(a, np.float32).reshape(-1)
+        keep.append(a)
+        return a.ctypes.data_as(ct.POINTER(ct.c_float)), a.size
+
+    def dense(spec):
+        out = (native.PolicyDenseLayerC * max(len(spec), 1))()
+        for i, (w, b, act) in enumerate(spec):
+            w = np.asarray(w, np.float32)
+            wp, wn = arr(w)
+            bp, bn = arr(b)
+            out[i] = native.PolicyDenseLayerC(w.shape[1], w.shape[0], native.POLICY_ACTIVATIONS[act], wp, wn, bp, bn)
+        keep.append(out)
+        return out, len(spec)
+
+    pk = native.PolicyPackC()
+    ident = policy_id.encode()
+    keep.append(ident)
+    pk.id = ident
+    pk.revision = int(revision)
+    (pk.contract_version, pk.world_fingerprint, pk.task_fingerprint, pk.observation_fingerprint,
+     pk.action_fingerprint) = (int(x) for x in contract)
+    pk.layers, pk.layer_count = dense(layers)
+    if critic_layers:
+        pk.critic_layers, pk.critic_layer_count = dense(critic_layers)
+    pk.observation_mean, pk.observation_mean_count = arr(observation_mean)
+    pk.observation_inverse_standard_deviation, pk.observation_inverse_standard_deviation_count = arr(observation_inverse_std)
+    pk.critic_observation_mean, pk.critic_observation_mean_count = arr(critic_observation_mean)
+    (pk.critic_observation_inverse_standard_deviation,
+     pk.critic_observation_inverse_standard_deviation_count) = arr(critic_observation_inverse_std)
+    pk.action_log_standard_deviation, pk.action_log_standard_deviation_count = arr(action_log_std)
+    pk.action_bias, pk.action_bias_count = arr(action_bias)
+    pk.action_scale, pk.action_scale_count = arr(action_scale)
+    pk.observation_clip = float(observation_clip)
+    pk.action_clip = float(action_clip)
+    return pk, keep
+
+
+def write_policy_pack(path: str | os.PathLike[str], layers, *, library: native.Bindings | None = None, **fields) -> None:
+    """Writes a PolicyPack file (mr_write_policy_pack); arguments as
+    policy_pack_c.  The pack needs an exact contract (version 1, non-zero
+    fingerprints)."""
+
+    lib = library or native.bindings()
+    pk, keep = policy_pack_c(layers, **fields)
+    lib.check(lib.lib.mr_write_policy_pack(ct.byref(pk), os.fsencode(path)), "mr_write_policy_pack")
+    del keep
+
+
+def inspect_policy_pack(path: str | os.PathLike[str], *, library: native.Bindings | None = None) -> tuple[dict, np.ndarray]:
+    """Reads a PolicyPack file without a device (mr_policy_pack_inspect):
+    its fields and every FP32 table concatenated in file order."""
+
+    lib = library or native.bindings()
+    info = native.PolicyPackInfoC()
+    lib.check(lib.lib.mr_policy_pack_inspect(os.fsencode(path), ct.byref(info), None, 0), "mr_policy_pack_inspect")
+    params = np.zeros(int(info.parameter_count), np.float32)
+    lib.check(lib.lib.mr_policy_pack_inspect(os.fsencode(path), ct.byref(info),
+                                             params.ctypes.data_as(ct.POINTER(ct.c_float)), params.size),
+              "mr_policy_pack_inspect")
+    fields = {name: getattr(info, name) for name, _ in native.PolicyPackInfoC._fields_}
+    fields["id"] = info.id.decode()
+    return fields, params
 
 
 def quality_solve(mass: np.ndarray, jacobian: np.ndarray, free_velocity: np.ndarray, target: np.ndarray,
@@ -482,42 +574,19 @@ class World:
         are (weights [out][in], bias [out] or None, activation name); the
         actor maps [q, v] to the action mean."""
 
-        keep: list[Any] = []
-
-        def arr(a):
-            if a is None:
-                return None, 0
-            a = np.ascontiguousarray(a, np.float32).reshape(-1)
-            keep.append(a)
-            return a.ctypes.data_as(ct.POINTER(ct.c_float)), a.size
-
-        def dense(spec):
-            out = (native.PolicyDenseLayerC * max(len(spec), 1))()
-            for i, (w, b, act) in enumerate(spec):
-                w = np.asarray(w, np.float32)
-                wp, wn = arr(w)
-                bp, bn = arr(b)
-                out[i] = native.PolicyDenseLayerC(w.shape[1], w.shape[0], native.POLICY_ACTIVATIONS[act], wp, wn, bp, bn)
-            keep.append(out)
-            return out, len(spec)
-
-        pk = native.PolicyPackC()
-        pk.id = policy_id.encode()
-        pk.revision = int(revision)
-        pk.layers, pk.layer_count = dense(layers)
-        if critic_layers:
-            pk.critic_layers, pk.critic_layer_count = dense(critic_layers)
-        pk.observation_mean, pk.observation_mean_count = arr(observation_mean)
-        pk.observation_inverse_standard_deviation, pk.observation_inverse_standard_deviation_count = arr(observation_inverse_std)
-        pk.critic_observation_mean, pk.critic_observation_mean_count = arr(critic_observation_mean)
-        (pk.critic_observation_inverse_standard_deviation,
-         pk.critic_observation_inverse_standard_deviation_count) = arr(critic_observation_inverse_std)
-        pk.action_log_standard_deviation, pk.action_log_standard_deviation_count = arr(action_log_std)
-        pk.action_bias, pk.action_bias_count = arr(action_bias)
-        pk.action_scale, pk.action_scale_count = arr(action_scale)
-        pk.observation_clip = float(observation_clip)
-        pk.action_clip = float(action_clip)
+        pk, keep = policy_pack_c(layers, revision=revision, action_clip=action_clip, policy_id=policy_id,
+                                 observation_mean=observation_mean, observation_inverse_std=observation_inverse_std,
+                                 observation_clip=observation_clip, critic_layers=critic_layers,
+                                 critic_observation_mean=critic_observation_mean,
+                                 critic_observation_inverse_std=critic_observation_inverse_std, action_log_std=action_log_std,
+                                 action_bias=action_bias, action_scale=action_scale)
         self._lib.check(self._lib.lib.mr_task_rollout_set_policy(self._handle, ct.byref(pk)), "mr_task_rollout_set_policy")
+
+    def load_policy_pack(self, path: str | os.PathLike[str]) -> None:
+        """Reads a PolicyPack file and installs it (mr_task_rollout_load_policy_pack)."""
+
+        self._lib.check(self._lib.lib.mr_task_rollout_load_policy_pack(self._handle, os.fsencode(path)),
+                        "mr_task_rollout_load_policy_pack")
 
     def clear_policy(self) -> None:
         self._lib.check(self._lib.lib.mr_task_rollout_clear_policy(self._handle), "mr_task_rollout_clear_policy")

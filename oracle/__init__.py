@@ -197,6 +197,48 @@ def reference_quality_solve(inverse_mass, free_velocity, jacobian, mu, target, r
     return int(st), imp, vel, dict(zip(names, cert.tolist()), iterations=int(iters.value))
 
 
+def _ref_lib():
+    if not REF_LIB.is_file():
+        raise FileNotFoundError(f"{REF_LIB} is missing; build it with `make -C oracle ref` where the reference sources exist")
+    return ct.CDLL(str(REF_LIB))
+
+
+def reference_write_policy_pack(pack, path) -> None:
+    """The reference's writePolicyPack on a pack given as an MRPolicyPackC
+    (numi_lab_b200.native.PolicyPackC)."""
+
+    lib = _ref_lib()
+    lib.ref_write_policy_pack.restype = ct.c_int
+    lib.ref_write_policy_pack.argtypes = [ct.c_void_p, ct.c_char_p, ct.c_char_p, ct.c_size_t]
+    err = ct.create_string_buffer(512)
+    st = lib.ref_write_policy_pack(ct.addressof(pack), os.fsencode(path), err, len(err))
+    if st != 0:
+        raise ValueError(f"reference writePolicyPack failed ({st}): {err.value.decode()}")
+
+
+def reference_inspect_policy_pack(path):
+    """The reference's readPolicyPack: (fields, FP32 tables in file order)
+    in the layout of mr_policy_pack_inspect."""
+
+    from numi_lab_b200 import native
+
+    lib = _ref_lib()
+    lib.ref_policy_pack_inspect.restype = ct.c_int
+    lib.ref_policy_pack_inspect.argtypes = [ct.c_char_p, ct.c_void_p, ct.POINTER(ct.c_float), ct.c_size_t, ct.c_char_p,
+                                            ct.c_size_t]
+    info = native.PolicyPackInfoC()
+    err = ct.create_string_buffer(512)
+    st = lib.ref_policy_pack_inspect(os.fsencode(path), ct.addressof(info), None, 0, err, len(err))
+    if st != 0:
+        raise ValueError(f"reference readPolicyPack failed ({st}): {err.value.decode()}")
+    params = np.zeros(int(info.parameter_count), np.float32)
+    lib.ref_policy_pack_inspect(os.fsencode(path), ct.addressof(info), params.ctypes.data_as(ct.POINTER(ct.c_float)), params.size,
+                                err, len(err))
+    fields = {name: getattr(info, name) for name, _ in native.PolicyPackInfoC._fields_}
+    fields["id"] = info.id.decode()
+    return fields, params
+
+
 class Oracle:
     """The C restatement, bound to one compiled world."""
 

@@ -11,7 +11,8 @@
 //   - stepControlledArticulatedWorldCpu (src/core/ArticulatedWorld.cpp:1232)
 //     and a multi-threaded timing loop over it (the CPU baseline),
 //   - collideCpuReference (src/core/Collision.cpp:2959) over a free-body
-//     pile: raw contacts and persistent manifolds of every touching pair.
+//     pile: raw contacts and persistent manifolds of every touching pair,
+//   - writePolicyPack / readPolicyPack (src/core/LearningPacks.cpp:2428-2470).
 // Implicit PD drives are expressed for the reference the way its own GPU
 // ABA does: armature raised by h kd + h^2 kp and the PD law evaluated as an
 // effort (ArticulatedABA.metal:301-326, MetalWorld.metal:280-370).
@@ -22,6 +23,8 @@
 #include "metalrobo/ConstraintSolver.hpp"
 #include "metalrobo/RigidBodyWorld.hpp"
 #include "metalrobo/EngineModel.hpp"
+#include "metalrobo/LearningPacks.hpp"
+#include "metalrobo/PolicyProgram.hpp"
 #include "metalrobo/QualityContactSolver.hpp"
 #include "metalrobo/ReferenceConicSolver.hpp"
 
@@ -32,6 +35,7 @@
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <limits>
 #include <string>
@@ -815,6 +819,94 @@ __attribute__((visibility("default"))) int ref_scene_collide(RefScene* r, const 
         }
         *manifold_count = static_cast<std::uint32_t>(m + 1);
     }
+    return 0;
+}
+
+}  // extern "C"
+
+// PolicyPack files through the reference's own writer and reader.  The pack
+// is given in this library's MRPolicyPackC (the field set of the
+// reference's c_api.h:344-372).  Errors go to `err`.
+static void ref_copy_layers(std::vector<PolicyDenseLayer>& out, const MRPolicyDenseLayerC* ls, size_t n) {
+    out.resize(n);
+    for (size_t i = 0; i < n; ++i) {
+        out[i].inputCount = ls[i].input_count;
+        out[i].outputCount = ls[i].output_count;
+        out[i].activation = static_cast<PolicyActivation>(ls[i].activation);
+        out[i].weights.assign(ls[i].weights, ls[i].weights + ls[i].weight_count);
+        out[i].bias.assign(ls[i].bias, ls[i].bias + ls[i].bias_count);
+    }
+}
+
+extern "C" {
+
+__attribute__((visibility("default"))) int ref_write_policy_pack(const MRPolicyPackC* c, const char* path, char* err, size_t err_len) {
+    PolicyPack p;
+    p.id = c->id;
+    p.revision = c->revision;
+    p.contract.version = c->contract_version;
+    p.contract.worldFingerprint = c->world_fingerprint;
+    p.contract.taskFingerprint = c->task_fingerprint;
+    p.contract.observationFingerprint = c->observation_fingerprint;
+    p.contract.actionFingerprint = c->action_fingerprint;
+    auto vec = [](const float* v, size_t n) { return std::vector<float>(v, v + n); };
+    p.observationMean = vec(c->observation_mean, c->observation_mean_count);
+    p.observationInverseStandardDeviation = vec(c->observation_inverse_standard_deviation, c->observation_inverse_standard_deviation_count);
+    ref_copy_layers(p.layers, c->layers, c->layer_count);
+    p.criticObservationMean = vec(c->critic_observation_mean, c->critic_observation_mean_count);
+    p.criticObservationInverseStandardDeviation =
+        vec(c->critic_observation_inverse_standard_deviation, c->critic_observation_inverse_standard_deviation_count);
+    ref_copy_layers(p.criticLayers, c->critic_layers, c->critic_layer_count);
+    p.actionLogStandardDeviation = vec(c->action_log_standard_deviation, c->action_log_standard_deviation_count);
+    p.actionBias = vec(c->action_bias, c->action_bias_count);
+    p.actionScale = vec(c->action_scale, c->action_scale_count);
+    p.observationClip = c->observation_clip;
+    p.actionClip = c->action_clip;
+    const LearningPackResult r = writePolicyPack(p, path);
+    if (!r.succeeded() && err && err_len) std::snprintf(err, err_len, "%s", r.message.c_str());
+    return r.succeeded() ? 0 : static_cast<int>(r.status);
+}
+
+__attribute__((visibility("default"))) int ref_policy_pack_inspect(const char* path, MRPolicyPackInfoC* info, float* params, size_t cap,
+                                                                   char* err, size_t err_len) {
+    PolicyPack p;
+    const LearningPackResult r = readPolicyPack(path, p);
+    if (!r.succeeded()) {
+        if (err && err_len) std::snprintf(err, err_len, "%s", r.message.c_str());
+        return static_cast<int>(r.status);
+    }
+    MRPolicyPackInfoC o{};
+    o.layer_count = static_cast<uint32_t>(p.layers.size());
+    o.critic_layer_count = static_cast<uint32_t>(p.criticLayers.size());
+    o.observation_count = p.layers.empty() ? 0u : p.layers.front().inputCount;
+    o.action_count = p.layers.empty() ? 0u : p.layers.back().outputCount;
+    o.stochastic = p.actionLogStandardDeviation.empty() ? 0u : 1u;
+    o.revision = p.revision;
+    o.content_hash = r.contentHash;
+    o.contract_version = p.contract.version;
+    o.world_fingerprint = p.contract.worldFingerprint;
+    o.task_fingerprint = p.contract.taskFingerprint;
+    o.observation_fingerprint = p.contract.observationFingerprint;
+    o.action_fingerprint = p.contract.actionFingerprint;
+    o.observation_clip = p.observationClip;
+    o.action_clip = p.actionClip;
+    std::snprintf(o.id, sizeof(o.id), "%s", p.id.c_str());
+    std::vector<const std::vector<float>*> t{&p.observationMean, &p.observationInverseStandardDeviation};
+    for (const PolicyDenseLayer& l : p.layers) { t.push_back(&l.weights); t.push_back(&l.bias); }
+    t.push_back(&p.criticObservationMean);
+    t.push_back(&p.criticObservationInverseStandardDeviation);
+    for (const PolicyDenseLayer& l : p.criticLayers) { t.push_back(&l.weights); t.push_back(&l.bias); }
+    t.push_back(&p.actionLogStandardDeviation);
+    t.push_back(&p.actionBias);
+    t.push_back(&p.actionScale);
+    size_t total = 0;
+    for (const auto* v : t) total += v->size();
+    o.parameter_count = total;
+    if (params && cap >= total) {
+        size_t at = 0;
+        for (const auto* v : t) { std::copy(v->begin(), v->end(), params + at); at += v->size(); }
+    }
+    *info = o;
     return 0;
 }
 

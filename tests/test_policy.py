@@ -152,3 +152,45 @@ def test_policy_install_rejects_mismatched_networks(cuda_device):
         with pytest.raises(nb.MetalRoboError, match="outputs"):
             world.set_policy(**dict(spec, layers=wide))
         assert world.policy_revision == 0
+
+
+@pytest.mark.gpu
+def test_policy_pack_file_drives_the_rollout_like_the_in_memory_policy(cuda_device, tmp_path):
+    """A PolicyPack written by the reference's own writer (oracle/_ref) or by
+    this library, loaded with mr_task_rollout_load_policy_pack, drives a
+    rollout bit-identically to the same policy installed from memory; a
+    failed load (a corrupt file) leaves the installed policy in place."""
+
+    from test_packs import CONTRACT
+
+    rng = np.random.default_rng(8)
+    envs, steps = 32, 5
+    kw = dict(substeps=4, velocity_iterations=8, control_dt=0.02, seed=SEED)
+    with nb.World("tree29", envs, **kw) as a, nb.World("tree29", envs, **kw) as b:
+        spec = dict(_policy(a, rng, True), policy_id="g1-walk", contract=CONTRACT, observation_clip=5.0)
+        path = tmp_path / "policy.mrpolicy"
+        try:
+            from oracle import reference_write_policy_pack
+
+            pk, keep = nb.world.policy_pack_c(**spec)
+            reference_write_policy_pack(pk, path)
+            del keep
+        except FileNotFoundError:  # no reference core on this host: this library's writer (byte-identical)
+            nb.write_policy_pack(path, **spec)
+        a.set_policy(**{k: v for k, v in spec.items() if k != "contract"})
+        b.load_policy_pack(path)
+        assert a.policy_revision == b.policy_revision == spec["revision"]
+        a.advance_host(None, steps=steps, raise_on_failure=False)
+        b.advance_host(None, steps=steps, raise_on_failure=False)
+        qa, va, _ = a.state()
+        qb, vb, _ = b.state()
+        assert np.array_equal(qa, qb) and np.array_equal(va, vb)
+        assert np.array_equal(a.policy_outputs()["latents"], b.policy_outputs()["latents"])
+        corrupt = tmp_path / "corrupt.mrpolicy"
+        data = bytearray(path.read_bytes())
+        data[-60] ^= 0x10
+        corrupt.write_bytes(bytes(data))
+        with pytest.raises(nb.MetalRoboError, match="hash"):
+            b.load_policy_pack(corrupt)
+        assert b.policy_revision == spec["revision"]
+        b.advance_host(None, steps=1, raise_on_failure=False)  # the installed policy still drives it
