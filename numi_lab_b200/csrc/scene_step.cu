@@ -2,6 +2,8 @@
 // device code lives in scene_step.cuh.
 #include "scene_step.cuh"
 
+#include <cstdlib>
+
 namespace numi {
 namespace {
 
@@ -33,6 +35,35 @@ __global__ void __launch_bounds__(32) scene_audit_kernel(SceneParams p) {
 size_t scene_step_smem_bytes(bool compensated) {
     return static_cast<size_t>(compensated ? kSceneSmemWordsComp : kSceneSmemWords) * sizeof(float);
 }
+
+namespace {
+
+// Resident environments per SM of the per-world launch (0: as many as the
+// registers allow).  NUMI_B200_SCENE_RESIDENT, read once, overrides it; a
+// lower count is reached by asking each one-warp CTA for more shared memory.
+int scene_resident_limit() {
+    static const int limit = [] {
+        const char* env = std::getenv("NUMI_B200_SCENE_RESIDENT");
+        const int v = env ? std::atoi(env) : 0;
+        return v > 0 && v <= 32 ? v : 0;
+    }();
+    return limit;
+}
+
+size_t scene_launch_smem(bool compensated) {
+    size_t smem = scene_step_smem_bytes(compensated);
+    if (const int limit = scene_resident_limit()) {
+        int dev = 0, per_sm = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) == cudaSuccess && per_sm > 0) {
+            const size_t padded = static_cast<size_t>(per_sm / limit) - 1024;  // 1 KB reserved per CTA
+            if (padded > smem) smem = padded;
+        }
+    }
+    return smem;
+}
+
+}  // namespace
 size_t scene_workspace_words() { return static_cast<size_t>(kWsWords); }
 
 namespace {
@@ -54,7 +85,7 @@ cudaError_t configure_scene_step_kernel() {
             if (e == cudaSuccess)
                 e = for_scene_kernel(compensated, convex, [&](auto kernel) {
                     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                static_cast<int>(scene_step_smem_bytes(compensated)));
+                                                static_cast<int>(scene_launch_smem(compensated)));
                 });
     return e;
 }
@@ -66,7 +97,7 @@ cudaError_t launch_scene_audit(const SceneParams& p, cudaStream_t stream) {
 
 cudaError_t launch_scene_step(const SceneParams& p, cudaStream_t stream) {
     const bool compensated = p.q_comp != nullptr;
-    const size_t smem = scene_step_smem_bytes(compensated);
+    const size_t smem = scene_launch_smem(compensated);
     return for_scene_kernel(compensated, p.support_mapped != 0, [&](auto kernel) {
         kernel<<<p.env_count, 32, smem, stream>>>(p);
         return cudaGetLastError();

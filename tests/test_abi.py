@@ -60,6 +60,13 @@ def test_struct_sizes_match_header_layout(tmp_path):
         "MRServerRequestC": native.ServerRequestC,
         "MRServerCompletionC": native.ServerCompletionC,
         "MRServerStatsC": native.ServerStatsC,
+        "MRPolicyDenseLayerC": native.PolicyDenseLayerC,
+        "MRPolicyPackC": native.PolicyPackC,
+        "MRPolicyPackInfoC": native.PolicyPackInfoC,
+        "MRQualitySolverConfigC": native.QualitySolverConfigC,
+        "MRQualityDiagnosticsC": native.QualityDiagnosticsC,
+        "MRQualityResultC": native.QualityResultC,
+        "MRBatchLaunchShapeC": native.BatchLaunchShapeC,
     }
     src = tmp_path / "sizes.c"
     body = "".join(f'printf("%zu\\n", sizeof({name}));' for name in records)
