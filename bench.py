@@ -547,7 +547,7 @@ def run_pile(args, source: str = "pile") -> None:
         "dtype": "f32",
         "data": "synthetic (seeded)",
         "config": {"workload": f"free-body piles: {envs} envs x {PILE_BODIES} "
-                               f"{'boxes/spheres/capsules' if source == 'pile' else 'boxes/spheres/capsules/cylinders'} "
+                               f"{ {'pile': 'boxes/spheres/capsules', 'hull_pile': 'boxes/spheres/capsules/12-vertex convex hulls'}.get(source, 'boxes/spheres/capsules/cylinders')} "
                                "(size U(0.05, 0.3) m, density 500-2000) "
                                "settled on a plane, 20 ms control = 4 x 5 ms substeps, 8 temporalCone iterations, "
                                f"{horizon} control steps per bench step", "l2": "flushed (256 MiB write) between steps"},
@@ -1003,7 +1003,7 @@ def main() -> None:
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--envs", type=int, default=0, help="pile workload: environments (default 16384; smaller for profiling)")
     parser.add_argument("--workload", default="tree29",
-                        choices=["tree29", "pile", "cylinder_pile", "mix", "precision", "policy", "quality"],
+                        choices=["tree29", "pile", "cylinder_pile", "hull_pile", "mix", "precision", "policy", "quality"],
                         help="tree29 (the headline), pile (36-body piles), cylinder_pile (36-body piles with cylinders: "
                              "GJK / EPA pairs), mix (chains, trees and piles) or precision (box stacks and trees against the "
                              "FP64 oracle) or policy (tree29 closed loop under a native policy) or quality (tree29 with the "
@@ -1029,7 +1029,8 @@ def main() -> None:
         return
     if args.workload != "tree29":
         if rank == 0:
-            {"pile": run_pile, "cylinder_pile": lambda a: run_pile(a, "cylinder_pile"), "mix": run_mix,
+            {"pile": run_pile, "cylinder_pile": lambda a: run_pile(a, "cylinder_pile"),
+             "hull_pile": lambda a: run_pile(a, "hull_pile"), "mix": run_mix,
              "precision": run_precision, "policy": run_policy, "quality": run_quality}[args.workload](args)
         return
 

@@ -80,7 +80,8 @@ enum MRShapeType {
     MR_SHAPE_CAPSULE = 1u,
     MR_SHAPE_BOX = 2u,
     MR_SHAPE_PLANE = 3u,
-    MR_SHAPE_CYLINDER = 4u   /* radius dimensions.x, half length dimensions.y along local +Y */
+    MR_SHAPE_CYLINDER = 4u,  /* radius dimensions.x, half length dimensions.y along local +Y */
+    MR_SHAPE_CONVEX = 5u     /* hull vertices (MRModelViewC.hull_vertices) scaled by dimensions.xyz */
 };
 
 /* reference: include/metalrobo/engine_types.h:114-134 (same values). */
@@ -196,7 +197,13 @@ enum MRRunManifestSourceC {
     /* The pile of MR_RUN_SOURCE_SYNTHETIC_PILE (same bodies for the same
      * seed) with every capsule-box pair taking the support-mapped (GJK /
      * EPA, MPR fallback) narrowphase instead of the analytic witness. */
-    MR_RUN_SOURCE_SYNTHETIC_PILE_GJK = 105u
+    MR_RUN_SOURCE_SYNTHETIC_PILE_GJK = 105,
+    /* Pile of 8-64 free boxes, spheres, capsules and convex hulls (one
+     * quarter each; each hull 12 vertices) dropped onto a ground plane;
+     * pairs with a hull take the hull path of the support-mapped
+     * narrowphase (GJK distance, support-axis penetration witness, sampled
+     * patch; a hull on the plane: its deepest vertex). */
+    MR_RUN_SOURCE_SYNTHETIC_HULL_PILE = 106u
 };
 
 /* reference: include/metalrobo/c_api.h:171-190 (same shape). */
@@ -371,7 +378,10 @@ typedef struct MRModelShapeC {
     uint32_t flags;
     uint32_t collision_group;
     uint32_t collision_mask;
-    uint32_t reserved[2];
+    /* MR_SHAPE_CONVEX: first vertex and vertex count of its hull in the
+     * model's hull vertex table; 0 otherwise.                              */
+    uint32_t hull_first;
+    uint32_t hull_count;
     float local_position[4];
     float local_rotation[4];
     float dimensions[4];           /* sphere r; capsule r, half length; box half extents */
@@ -400,6 +410,13 @@ typedef struct MRModelViewC {
     MRModelShapeC* shapes;
     MRModelMaterialC* materials;
     MRModelPairC* pairs;
+    /* Unit-scale local hull vertices of every MR_SHAPE_CONVEX shape, xyz
+     * plus one unused float each ([hull_vertex_count][4]); written when
+     * non-null and hull_vertex_capacity (vertices) suffices.  The count is
+     * always reported. */
+    float* hull_vertices;
+    uint32_t hull_vertex_capacity;
+    uint32_t hull_vertex_count;
 } MRModelViewC;
 
 /* Persistent contact state of one environment: one slot per compiled pair.

@@ -111,6 +111,7 @@ void CompiledModel::finalize() {
         mixin(&world, sizeof(world));
         mixin(bodies.data(), bodies.size() * sizeof(MRModelBodyC));
         mixin(shapes.data(), shapes.size() * sizeof(MRModelShapeC));
+        if (!hull_vertices.empty()) mixin(hull_vertices.data(), hull_vertices.size() * sizeof(float));
         fingerprint = h;
         return;
     }
@@ -502,9 +503,12 @@ static void finish_scene(CompiledModel& m, std::uint32_t n, double friction, boo
     m.materials.push_back(mat);
     // Pair classes as the reference compiles them (MetalWorld.mm:1413-1500):
     // a cylinder against the plane is analytic, against any finite shape
-    // support-mapped (GJK / EPA).
+    // support-mapped (GJK / EPA); a hull against anything, the plane
+    // included, takes the hull path of the support-mapped query
+    // (Collision.metal:8026-8045, 3623-3720).
     auto cls = [&](std::uint32_t a, std::uint32_t b) {
         const std::uint32_t ta = m.shapes[a].shape_type, tb = m.shapes[b].shape_type;
+        if (ta == MR_SHAPE_CONVEX || tb == MR_SHAPE_CONVEX) return MR_COLLISION_PAIR_CONVEX;
         if (tb == MR_SHAPE_PLANE)
             return ta == MR_SHAPE_BOX ? MR_COLLISION_PAIR_BOX_PLANE
                    : (ta == MR_SHAPE_CAPSULE ? MR_COLLISION_PAIR_CAPSULE_PLANE
@@ -552,9 +556,12 @@ static void finish_scene(CompiledModel& m, std::uint32_t n, double friction, boo
 }
 
 
-CompiledModel build_pile(std::uint64_t seed, std::uint32_t count, bool cylinders, bool gjk_capsule_box) {
+constexpr int kHullVertices = 12;  // vertices of each synthetic hull
+
+CompiledModel build_pile(std::uint64_t seed, std::uint32_t count, bool cylinders, bool gjk_capsule_box, bool hulls) {
     CompiledModel m;
-    m.name = cylinders ? "synthetic_cylinder_pile" : (gjk_capsule_box ? "synthetic_pile_gjk" : "synthetic_pile");
+    m.name = hulls ? "synthetic_hull_pile"
+                   : (cylinders ? "synthetic_cylinder_pile" : (gjk_capsule_box ? "synthetic_pile_gjk" : "synthetic_pile"));
     m.scene = true;
     std::uint64_t k = 0;
     auto draw = [&](double lo, double hi) { return uniform(seed, kStreamModel, k++, lo, hi); };
@@ -566,9 +573,11 @@ CompiledModel build_pile(std::uint64_t seed, std::uint32_t count, bool cylinders
         // One third each of boxes, spheres and capsules; with cylinders,
         // one quarter each of boxes, spheres, capsules and cylinders.
         const double kind = draw(0.0, 1.0);
-        const bool box = cylinders ? kind < 0.25 : kind < 1.0 / 3.0;
-        const bool capsule = cylinders ? (kind >= 0.5 && kind < 0.75) : kind >= 2.0 / 3.0;
+        const bool quarters = cylinders || hulls;
+        const bool box = quarters ? kind < 0.25 : kind < 1.0 / 3.0;
+        const bool capsule = quarters ? (kind >= 0.5 && kind < 0.75) : kind >= 2.0 / 3.0;
         const bool cylinder = cylinders && kind >= 0.75;
+        const bool hull = hulls && kind >= 0.75;
         const double size = draw(0.05, 0.3);
         const double density = draw(500.0, 2000.0);
         double hx = 0.5 * size, hy = 0.5 * size, hz = 0.5 * size;
@@ -583,6 +592,29 @@ CompiledModel build_pile(std::uint64_t seed, std::uint32_t count, bool cylinders
         // Cylinder: radius and half length each 0.5 size x U(0.5, 1) (local +Y axis).
         const double cyl_r = cylinder ? 0.5 * size * draw(0.5, 1.0) : 0.0;
         const double cyl_hl = cylinder ? 0.5 * size * draw(0.5, 1.0) : 0.0;
+        // Hull: 12 unit vertices -- seeded directions with radii U(0.75, 1)
+        // -- scaled by per-axis half sizes 0.5 size x U(0.7, 1).
+        std::uint32_t hull_first = 0;
+        double hull_bound = 0.0;
+        if (hull) {
+            hx *= draw(0.7, 1.0);
+            hy *= draw(0.7, 1.0);
+            hz *= draw(0.7, 1.0);
+            hull_first = static_cast<std::uint32_t>(m.hull_vertices.size() / 4);
+            for (int i = 0; i < kHullVertices; ++i) {
+                double d[3];
+                double len = 0.0;
+                do {
+                    for (double& c : d) c = draw(-1.0, 1.0);
+                    len = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+                } while (len < 0.2 || len > 1.0);
+                const double r = draw(0.75, 1.0) / len;
+                const double p[3] = {d[0] * r, d[1] * r, d[2] * r};
+                for (double c : p) m.hull_vertices.push_back(static_cast<float>(c));
+                m.hull_vertices.push_back(0.0f);
+                hull_bound = std::max(hull_bound, std::sqrt(p[0] * p[0] * hx * hx + p[1] * p[1] * hy * hy + p[2] * p[2] * hz * hz));
+            }
+        }
         MRModelBodyC body{};
         body.parent_body = MR_INVALID_INDEX;
         body.inbound_joint = MR_INVALID_INDEX;
@@ -611,6 +643,15 @@ CompiledModel build_pile(std::uint64_t seed, std::uint32_t count, bool cylinders
             iyy = 0.5 * mass * r * r;
             ixx = izz = mass * (3.0 * r * r + hgt * hgt) / 12.0;
             bound = std::sqrt(r * r + cyl_hl * cyl_hl);  // Collision.metal:5731-5734
+        } else if (hull) {
+            // Mass properties of the ellipsoid with semi-axes 0.875 x the
+            // half sizes (the mean vertex radius), a stand-in for the hull's.
+            const double a = 0.875 * hx, bb = 0.875 * hy, c = 0.875 * hz;
+            mass = density * 4.0 / 3.0 * 3.141592653589793 * a * bb * c;
+            ixx = 0.2 * mass * (bb * bb + c * c);
+            iyy = 0.2 * mass * (a * a + c * c);
+            izz = 0.2 * mass * (a * a + bb * bb);
+            bound = hull_bound;
         } else {
             const double r = hx;
             mass = density * 4.0 / 3.0 * 3.141592653589793 * r * r * r;
@@ -628,7 +669,13 @@ CompiledModel build_pile(std::uint64_t seed, std::uint32_t count, bool cylinders
         m.bodies.push_back(body);
         MRModelShapeC s{};
         s.body = b;
-        s.shape_type = box ? MR_SHAPE_BOX : (capsule ? MR_SHAPE_CAPSULE : (cylinder ? MR_SHAPE_CYLINDER : MR_SHAPE_SPHERE));
+        s.shape_type = box ? MR_SHAPE_BOX
+                           : (capsule ? MR_SHAPE_CAPSULE
+                                      : (cylinder ? MR_SHAPE_CYLINDER : (hull ? MR_SHAPE_CONVEX : MR_SHAPE_SPHERE)));
+        if (hull) {
+            s.hull_first = hull_first;
+            s.hull_count = kHullVertices;
+        }
         s.material = 0;
         s.collision_group = 1u;
         s.collision_mask = 3u;
@@ -636,7 +683,7 @@ CompiledModel build_pile(std::uint64_t seed, std::uint32_t count, bool cylinders
         set4(s.local_rotation, 0.0, 0.0, 0.0, 1.0);
         if (capsule) set4(s.dimensions, cap_r, cap_hl, 0.0, 0.0);
         else if (cylinder) set4(s.dimensions, cyl_r, cyl_hl, 0.0, 0.0);
-        else set4(s.dimensions, hx, box ? hy : 0.0, box ? hz : 0.0, 0.0);
+        else set4(s.dimensions, hx, box || hull ? hy : 0.0, box || hull ? hz : 0.0, 0.0);
         set4(s.contact_rest_bound, 0.002, 0.0, bound, 0.0);
         m.shapes.push_back(s);
     }

@@ -28,6 +28,7 @@ struct CompiledModel {
     std::vector<MRModelShapeC> shapes;
     std::vector<MRModelMaterialC> materials;
     std::vector<MRModelPairC> pairs;
+    std::vector<float> hull_vertices;  // [vertex][4] unit-scale local hull vertices (MR_SHAPE_CONVEX)
     std::string name;
 
     // Reset-state generation parameters.
@@ -79,7 +80,10 @@ CompiledModel build_tree29(std::uint64_t seed);
 // `cylinders`: one quarter each of boxes, spheres, capsules and cylinders.
 // gjk_capsule_box: capsule-box pairs take the support-mapped (GJK / EPA)
 // narrowphase instead of the analytic witness.
-CompiledModel build_pile(std::uint64_t seed, std::uint32_t bodies = 0, bool cylinders = false, bool gjk_capsule_box = false);
+// `hulls`: one quarter each of boxes, spheres, capsules and convex hulls of
+// 12 vertices (unit directions with radii U(0.75, 1), scaled per axis).
+CompiledModel build_pile(std::uint64_t seed, std::uint32_t bodies = 0, bool cylinders = false, bool gjk_capsule_box = false,
+                         bool hulls = false);
 // Stack of `boxes` 0.1 m, 1 kg cubes (friction 0.6) resting on a ground
 // plane, the stack yawed U(0, 2 pi) and each box offset horizontally by
 // N(0, 2 mm) at reset.

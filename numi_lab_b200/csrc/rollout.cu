@@ -363,6 +363,20 @@ numi::SceneModel numi::rt::pack_scene(const numi::CompiledModel& m, float h) {
         d.pair_b[p] = static_cast<std::uint8_t>(m.pairs[p].shape_b);
         d.pair_class[p] = static_cast<std::uint8_t>(m.pairs[p].pair_class);
     }
+    int used = 0;
+    for (std::uint32_t b = 0; b < n; ++b) {
+        const MRModelShapeC& sh = m.shapes[b];
+        if (sh.shape_type != MR_SHAPE_CONVEX) continue;
+        if (sh.hull_count == 0 || used + static_cast<int>(sh.hull_count) > numi::kSceneMaxHullVertices ||
+            (static_cast<size_t>(sh.hull_first) + sh.hull_count) * 4 > m.hull_vertices.size())
+            throw std::runtime_error("convex hull vertices outside the scene capacity");
+        d.hull_first[b] = used;
+        d.hull_count[b] = static_cast<int>(sh.hull_count);
+        for (std::uint32_t i = 0; i < sh.hull_count; ++i) {
+            const float* v = m.hull_vertices.data() + (static_cast<size_t>(sh.hull_first) + i) * 4;
+            d.hull_vertices[used++] = make_float4(v[0] * sh.dimensions[0], v[1] * sh.dimensions[1], v[2] * sh.dimensions[2], 0.0f);
+        }
+    }
     return d;
 }
 
@@ -909,6 +923,7 @@ MR_API MRTaskRolloutHandle* mr_create_task_rollout(const MRRunManifestC* manifes
             case MR_RUN_SOURCE_SYNTHETIC_PILE: h.model = numi::build_pile(cfg.seed); break;
             case MR_RUN_SOURCE_SYNTHETIC_CYLINDER_PILE: h.model = numi::build_pile(cfg.seed, 0, true); break;
             case MR_RUN_SOURCE_SYNTHETIC_PILE_GJK: h.model = numi::build_pile(cfg.seed, 0, false, true); break;
+            case MR_RUN_SOURCE_SYNTHETIC_HULL_PILE: h.model = numi::build_pile(cfg.seed, 0, false, false, true); break;
             case MR_RUN_SOURCE_SYNTHETIC_STACK: h.model = numi::build_stack(cfg.seed); break;
             default:
                 throw std::invalid_argument("unsupported run source " + std::to_string(manifest->source) +
@@ -1438,6 +1453,18 @@ MR_API int mr_task_rollout_copy_final_scene_states(const MRTaskRolloutHandle* ha
     });
 }
 
+// The hull vertex table of a model view (MRModelViewC::hull_vertices).
+static void copy_hull_vertices(const numi::CompiledModel& m, MRModelViewC* view) {
+    const std::uint32_t count = static_cast<std::uint32_t>(m.hull_vertices.size() / 4);
+    view->hull_vertex_count = count;
+    if (view->hull_vertices && count > 0) {
+        if (view->hull_vertex_capacity < count)
+            throw std::invalid_argument("hull_vertices holds " + std::to_string(view->hull_vertex_capacity) + " vertices; the model has " +
+                                        std::to_string(count));
+        std::memcpy(view->hull_vertices, m.hull_vertices.data(), m.hull_vertices.size() * sizeof(float));
+    }
+}
+
 MR_API int mr_task_rollout_copy_model(const MRTaskRolloutHandle* handle, MRModelViewC* view) {
     return guarded([&] {
         if (!handle || !view) throw std::invalid_argument("handle or view is null");
@@ -1449,6 +1476,7 @@ MR_API int mr_task_rollout_copy_model(const MRTaskRolloutHandle* handle, MRModel
         if (view->shapes) std::memcpy(view->shapes, m.shapes.data(), m.shapes.size() * sizeof(MRModelShapeC));
         if (view->materials) std::memcpy(view->materials, m.materials.data(), m.materials.size() * sizeof(MRModelMaterialC));
         if (view->pairs) std::memcpy(view->pairs, m.pairs.data(), m.pairs.size() * sizeof(MRModelPairC));
+        copy_hull_vertices(m, view);
     });
 }
 
@@ -1459,6 +1487,7 @@ static numi::CompiledModel compile_source(uint32_t source, uint64_t seed) {
         case MR_RUN_SOURCE_SYNTHETIC_PILE: return numi::build_pile(seed);
         case MR_RUN_SOURCE_SYNTHETIC_CYLINDER_PILE: return numi::build_pile(seed, 0, true);
         case MR_RUN_SOURCE_SYNTHETIC_PILE_GJK: return numi::build_pile(seed, 0, false, true);
+        case MR_RUN_SOURCE_SYNTHETIC_HULL_PILE: return numi::build_pile(seed, 0, false, false, true);
         case MR_RUN_SOURCE_SYNTHETIC_STACK: return numi::build_stack(seed);
         default: throw std::invalid_argument("unsupported synthetic source " + std::to_string(source));
     }
@@ -1475,6 +1504,7 @@ MR_API int mr_compile_synthetic_model(uint32_t source, uint64_t seed, MRModelVie
         if (view->shapes) std::memcpy(view->shapes, m.shapes.data(), m.shapes.size() * sizeof(MRModelShapeC));
         if (view->materials) std::memcpy(view->materials, m.materials.data(), m.materials.size() * sizeof(MRModelMaterialC));
         if (view->pairs) std::memcpy(view->pairs, m.pairs.data(), m.pairs.size() * sizeof(MRModelPairC));
+        copy_hull_vertices(m, view);
     });
 }
 

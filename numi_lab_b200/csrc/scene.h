@@ -18,6 +18,7 @@ constexpr int kSceneManifolds = MR_B200_SCENE_MANIFOLDS;  // persistent manifold
 constexpr int kSceneContacts = 256;    // solver contacts per environment
 constexpr int kSceneCandidates = 512;  // broadphase candidate pairs per environment
 constexpr int kSceneMaxMaterials = 4;
+constexpr int kSceneMaxHullVertices = 1024;  // hull vertices of all convex bodies of a world
 // Words of one manifold slot of a scene (MRManifoldC layout) plus its pair key.
 constexpr int kSceneSlotWords = MR_B200_SCENE_SLOT_WORDS;
 
@@ -54,6 +55,12 @@ struct alignas(16) SceneModel {
     std::uint8_t pair_a[kSceneMaxPairs];
     std::uint8_t pair_b[kSceneMaxPairs];
     std::uint8_t pair_class[kSceneMaxPairs];
+    // Convex bodies: their hull vertices, already scaled by the body's
+    // dimensions (vertex x dimensions, rounded once to FP32 as the reference
+    // rounds it per query), at [hull_first[b], hull_first[b] + hull_count[b]).
+    std::int32_t hull_first[kSceneMaxBodies];
+    std::int32_t hull_count[kSceneMaxBodies];
+    float4 hull_vertices[kSceneMaxHullVertices];
 };
 
 // Environments ("slots") hold resident state; a launch processes work

@@ -139,6 +139,8 @@ struct Collider {
     float3 normal;   // plane normal
     float3 bpos;     // pose of the collider's body: the frame of its
     float4 brot;     // manifold anchors (the ground body for the plane)
+    const float4* hull;  // convex: scaled local hull vertices
+    int hull_count;
 };
 
 __device__ void load_collider(const SceneModel& M, const float* s, int b, Collider& o) {
@@ -156,6 +158,8 @@ __device__ void load_collider(const SceneModel& M, const float* s, int b, Collid
         o.hl = 0.0f;
         o.bpos = xyz(M.ground_position);
         o.brot = M.ground_rotation;
+        o.hull = nullptr;
+        o.hull_count = 0;
         return;
     }
     o.type = M.shape_type[b];
@@ -193,6 +197,8 @@ __device__ void load_collider(const SceneModel& M, const float* s, int b, Collid
     o.normal = f3(0.0f, 0.0f, 0.0f);
     o.bpos = o.c;
     o.brot = o.r;
+    o.hull = M.hull_vertices + M.hull_first[b];
+    o.hull_count = o.type == MR_SHAPE_CONVEX ? M.hull_count[b] : 0;
 }
 
 __device__ __forceinline__ float collider_scale(const Collider& k) {
@@ -474,6 +480,24 @@ __device__ float3 shape_support(const Collider& k, unsigned index, float3 d, uns
         if (l.z >= 0.0f) { v |= 4u; p.z = k.half.z; }
         feat = feature_key(MR_SHAPE_BOX, v);
         return k.c + qrot(k.r, p);
+    }
+    if (k.type == MR_SHAPE_CONVEX) {
+        // The vertex of largest projection, the lowest index on a tie
+        // (Collision.metal:1899-1936).
+        const float3 l = qrotinv(k.r, d);
+        float best = -INFINITY;
+        int bi = 0;
+        for (int i = 0; i < k.hull_count; ++i) {
+            const float4 v = k.hull[i];
+            const float pr = dot3(f3(v.x, v.y, v.z), l);
+            if (pr > best) {
+                best = pr;
+                bi = i;
+            }
+        }
+        feat = feature_key(MR_SHAPE_CONVEX, static_cast<unsigned>(bi));
+        const float4 v = k.hull[bi];
+        return k.c + qrot(k.r, f3(v.x, v.y, v.z));
     }
     // cylinder
     const float axial = dot3(d, k.axis);
@@ -894,10 +918,63 @@ __device__ bool mpr(const Collider& A, const Collider& B, unsigned ia, unsigned 
     return false;
 }
 
+// Penetration witness of the hull path (Collision.metal:3129-3260, the
+// reference's replacement for EPA when a hull is involved): among the
+// centre-to-centre direction and the three local axes of each collider,
+// oriented from A towards B, the axis of largest separation
+// dot(support_B(-axis) - support_A(axis), axis).  (The reference also
+// tries the previous substep's query normal; no query cache is kept here.)
+__device__ bool support_axis_witness(const Collider& A, const Collider& B, unsigned ia, unsigned ib, SmQuery& q) {
+    const float3 delta = B.c - A.c;
+    bool found = false;
+    auto update = [&](float3 axis) {
+        const float a2 = dot3(axis, axis);
+        if (!(a2 > kTinyS) || !isfinite(a2)) return true;
+        axis = axis * rsqrtf(a2);
+        if (dot3(delta, delta) > kTinyS && dot3(axis, delta) < 0.0f) axis = -axis;
+        unsigned fa, fb;
+        const float3 pa = shape_support(A, ia, axis, fa);
+        const float3 pb = shape_support(B, ib, -axis, fb);
+        const float sep = dot3(pb - pa, axis);
+        if (!isfinite(sep)) return false;
+        if (!found || sep > q.sep) {
+            found = true;
+            q.normal = axis;
+            q.sep = sep;
+            q.pa = pa;
+            q.pb = pb;
+            q.fa = fa;
+            q.fb = fb;
+        }
+        return true;
+    };
+    if (!update(delta)) return false;
+    for (int axis = 0; axis < 3; ++axis) {
+        const float3 e = f3(axis == 0 ? 1.0f : 0.0f, axis == 1 ? 1.0f : 0.0f, axis == 2 ? 1.0f : 0.0f);
+        if (!update(qrot(A.r, e)) || !update(qrot(B.r, e))) return false;
+    }
+    if (!found) return false;
+    q.sep = fminf(q.sep, -0.0f);
+    return finite3(q.pa) && finite3(q.pb) && finite3(q.normal) && isfinite(q.sep);
+}
+
 // Contacts of a support-mapped pair into `sink`; the pair's normal (A -> B)
 // in `normal`.  Returns MR_STEP_SUCCESS or MR_STEP_DID_NOT_CONVERGE.
+// Cylinder pairs resolve an overlap by EPA, then MPR (the primitive-GJK
+// class); pairs with a hull by the support-axis witness (the hull class,
+// Collision.metal:3623-3720), and a hull on the plane by its deepest vertex.
 __device__ __noinline__ unsigned support_mapped_contacts(const Collider& A, const Collider& B, unsigned ia, unsigned ib, float accepted,
                                                          RawSink& sink, float3& normal) {
+    if (B.type == MR_SHAPE_PLANE) {
+        // The deepest vertex against the plane (the plane is always B here).
+        unsigned f;
+        const float3 p = shape_support(A, ia, -B.normal, f);
+        const float sep = dot3(B.normal, p - B.c);
+        normal = -B.normal;
+        if (sep <= accepted) sink.add(p, p - B.normal * sep, sep, f, feature_key(MR_SHAPE_PLANE, 0u));
+        return MR_STEP_SUCCESS;
+    }
+    const bool hull = A.type == MR_SHAPE_CONVEX || B.type == MR_SHAPE_CONVEX;
     const float scale = fmaxf(collider_scale(A), collider_scale(B)) + 1.0f;
     Sup sx[4];
     float wt[4] = {0.0f, 0.0f, 0.0f, 0.0f};
@@ -905,7 +982,9 @@ __device__ __noinline__ unsigned support_mapped_contacts(const Collider& A, cons
     SmQuery q;
     q.normal = f3(0.0f, 0.0f, 1.0f);
     const int g = gjk(A, B, ia, ib, scale, sx, n, wt, q);
-    if (g == 1) {
+    if (hull) {
+        if (g != 0 && !support_axis_witness(A, B, ia, ib, q)) return MR_STEP_DID_NOT_CONVERGE;
+    } else if (g == 1) {
         // Primitive pairs resolve with EPA first, MPR second (Collision.metal:3518-3560).
         if (!epa(A, B, ia, ib, scale, sx, n, q) && !mpr(A, B, ia, ib, scale, q)) return MR_STEP_DID_NOT_CONVERGE;
     } else if (g < 0) {
@@ -916,41 +995,56 @@ __device__ __noinline__ unsigned support_mapped_contacts(const Collider& A, cons
     float3 wa[kRawCap], wb[kRawCap];
     int nw = 0;
     sink.add(q.pa, q.pb, q.sep, q.fa, q.fb);
-    // Only a cylinder has a contact patch; other support-mapped pairs (a
-    // capsule against a box) keep the query's witness alone.
-    if (A.type != MR_SHAPE_CYLINDER && B.type != MR_SHAPE_CYLINDER) return MR_STEP_SUCCESS;
+    // Only cylinders and hulls have a contact patch; other support-mapped
+    // pairs (a capsule against a box) keep the query's witness alone.
+    const bool cyl_a = A.type == MR_SHAPE_CYLINDER, cyl_b = B.type == MR_SHAPE_CYLINDER;
+    if (!cyl_a && !cyl_b && !hull) return MR_STEP_SUCCESS;
     wa[nw] = q.pa;
     wb[nw] = q.pb;
     ++nw;
-    // Patch: supports along the normal tilted by 2e-4 towards the disk basis
-    // (cap contact) or the axis (side contact) of the cylinder.
-    const bool cyl_a = A.type == MR_SHAPE_CYLINDER;
-    const Collider& k = cyl_a ? A : B;
-    const unsigned kidx = cyl_a ? ia : ib;
-    const float3 sn = cyl_a ? q.normal : -q.normal;
-    const float align = fabsf(dot3(sn, k.axis));
+    // Patch (Collision.metal:3327-3432): supports of the sampled shape -- a
+    // cylinder, else a hull, A first -- along the normal tilted by 2e-4
+    // towards the disk basis (cylinder cap contact), the axis (cylinder side
+    // contact) or the contact plane's tangents (hull).
+    const bool sample_a = cyl_a || (!cyl_b && A.type == MR_SHAPE_CONVEX);
+    const Collider& k = sample_a ? A : B;
+    const unsigned kidx = sample_a ? ia : ib;
+    const float3 sn = sample_a ? q.normal : -q.normal;
     int nd = 0;
     float3 dirs[4];
-    if (align >= 0.95f) {
-        dirs[0] = k.bx; dirs[1] = -k.bx; dirs[2] = k.bz; dirs[3] = -k.bz;
+    if (k.type == MR_SHAPE_CYLINDER) {
+        const float align = fabsf(dot3(sn, k.axis));
+        if (align >= 0.95f) {
+            dirs[0] = k.bx; dirs[1] = -k.bx; dirs[2] = k.bz; dirs[3] = -k.bz;
+            nd = 4;
+        } else if (align <= 0.20f) {
+            dirs[0] = k.axis; dirs[1] = -k.axis;
+            nd = 2;
+        }
+    } else {
+        // contactPatchTangent: the normal crossed with the world axis of its
+        // smallest absolute component.
+        const float3 an = f3(fabsf(q.normal.x), fabsf(q.normal.y), fabsf(q.normal.z));
+        const float3 ref = an.x <= an.y && an.x <= an.z ? f3(1.0f, 0.0f, 0.0f) : (an.y <= an.z ? f3(0.0f, 1.0f, 0.0f) : f3(0.0f, 0.0f, 1.0f));
+        float3 t = cross3(q.normal, ref);
+        t = t * rsqrtf(dot3(t, t));
+        const float3 bt = cross3(q.normal, t);
+        dirs[0] = t; dirs[1] = -t; dirs[2] = bt; dirs[3] = -bt;
         nd = 4;
-    } else if (align <= 0.20f) {
-        dirs[0] = k.axis; dirs[1] = -k.axis;
-        nd = 2;
     }
     const float dtol = 32.0f * kFltEps * scale;
     for (int i = 0; i < nd; ++i) {
         unsigned f;
         const float3 p = shape_support(k, kidx, sn + dirs[i] * 2.0e-4f, f);
-        const float3 pa = cyl_a ? p : p - q.normal * q.sep;
-        const float3 pb = cyl_a ? p + q.normal * q.sep : p;
+        const float3 pa = sample_a ? p : p - q.normal * q.sep;
+        const float3 pb = sample_a ? p + q.normal * q.sep : p;
         bool dup = false;
         for (int j = 0; j < nw; ++j) {
             const float3 da = wa[j] - pa, db = wb[j] - pb;
             dup = dup || (dot3(da, da) <= dtol * dtol && dot3(db, db) <= dtol * dtol);
         }
         if (dup || nw >= kRawCap) continue;
-        sink.add(pa, pb, q.sep, cyl_a ? f : q.fa, cyl_a ? q.fb : f);
+        sink.add(pa, pb, q.sep, sample_a ? f : q.fa, sample_a ? q.fb : f);
         wa[nw] = pa;
         wb[nw] = pb;
         ++nw;

@@ -26,6 +26,8 @@ MR_RUN_SOURCE_SYNTHETIC_PILE: Final = 102
 MR_RUN_SOURCE_SYNTHETIC_STACK: Final = 103
 MR_RUN_SOURCE_SYNTHETIC_CYLINDER_PILE: Final = 104
 MR_RUN_SOURCE_SYNTHETIC_PILE_GJK: Final = 105
+MR_RUN_SOURCE_SYNTHETIC_HULL_PILE: Final = 106
+MR_SHAPE_CONVEX: Final = 5
 MANIFOLD_POINTS: Final = 4
 MR_PRECISION_FP32: Final = 0
 MR_PRECISION_FP64_ARTICULATED_INERTIA: Final = 1
@@ -388,7 +390,8 @@ class ModelShapeC(ct.Structure):
         ("flags", ct.c_uint32),
         ("collision_group", ct.c_uint32),
         ("collision_mask", ct.c_uint32),
-        ("reserved", ct.c_uint32 * 2),
+        ("hull_first", ct.c_uint32),
+        ("hull_count", ct.c_uint32),
         ("local_position", ct.c_float * 4),
         ("local_rotation", ct.c_float * 4),
         ("dimensions", ct.c_float * 4),
@@ -418,6 +421,9 @@ class ModelViewC(ct.Structure):
         ("shapes", ct.POINTER(ModelShapeC)),
         ("materials", ct.POINTER(ModelMaterialC)),
         ("pairs", ct.POINTER(ModelPairC)),
+        ("hull_vertices", ct.POINTER(ct.c_float)),
+        ("hull_vertex_capacity", ct.c_uint32),
+        ("hull_vertex_count", ct.c_uint32),
     ]
 
 

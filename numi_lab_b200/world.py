@@ -29,6 +29,7 @@ SOURCES = {
     "stack32": native.MR_RUN_SOURCE_SYNTHETIC_STACK,
     "cylinder_pile": native.MR_RUN_SOURCE_SYNTHETIC_CYLINDER_PILE,
     "pile_gjk": native.MR_RUN_SOURCE_SYNTHETIC_PILE_GJK,
+    "hull_pile": native.MR_RUN_SOURCE_SYNTHETIC_HULL_PILE,
 }
 SCENE_MANIFOLDS = 128      # manifold slots per scene environment
 SCENE_SLOT_WORDS = 57      # MRManifoldC words + pair key
@@ -53,6 +54,7 @@ class ModelRecords:
     shapes: Any
     materials: Any
     pairs: Any
+    hull_vertices: Any = None  # [n][4] float32 unit-scale hull vertices (convex shapes), or None
 
     def view(self) -> native.ModelViewC:
         v = native.ModelViewC()
@@ -63,6 +65,9 @@ class ModelRecords:
         v.shapes = ct.cast(self.shapes, ct.POINTER(native.ModelShapeC))
         v.materials = ct.cast(self.materials, ct.POINTER(native.ModelMaterialC))
         v.pairs = ct.cast(self.pairs, ct.POINTER(native.ModelPairC))
+        if self.hull_vertices is not None and len(self.hull_vertices):
+            v.hull_vertices = self.hull_vertices.ctypes.data_as(ct.POINTER(ct.c_float))
+            v.hull_vertex_capacity = len(self.hull_vertices)
         return v
 
 
@@ -86,6 +91,8 @@ def compile_model(source: str | int, seed: int, *, library: native.Bindings | No
     probe = native.ModelViewC()
     lib.check(lib.lib.mr_compile_synthetic_model(sid, seed, ct.byref(probe)), "mr_compile_synthetic_model")
     records = _alloc_records(probe.world)
+    if probe.hull_vertex_count:
+        records.hull_vertices = np.zeros((probe.hull_vertex_count, 4), np.float32)
     view = records.view()
     lib.check(lib.lib.mr_compile_synthetic_model(sid, seed, ct.byref(view)), "mr_compile_synthetic_model")
     records.world = view.world
@@ -398,6 +405,8 @@ class World:
         probe = native.ModelViewC()
         self._lib.check(self._lib.lib.mr_task_rollout_copy_model(self._handle, ct.byref(probe)), "copy_model")
         records = _alloc_records(probe.world)
+        if probe.hull_vertex_count:
+            records.hull_vertices = np.zeros((probe.hull_vertex_count, 4), np.float32)
         view = records.view()
         self._lib.check(self._lib.lib.mr_task_rollout_copy_model(self._handle, ct.byref(view)), "copy_model")
         records.world = view.world

@@ -603,7 +603,7 @@ class SceneOracle:
         lib = ct.CDLL(str(ORACLE_LIB))
         self.lib = lib
         lib.oracle_scene_create.restype = ct.c_void_p
-        lib.oracle_scene_create.argtypes = [ct.c_void_p] * 5 + [ct.c_double, ct.c_uint32, ct.c_uint32, ct.c_uint32]
+        lib.oracle_scene_create.argtypes = [ct.c_void_p] * 6 + [ct.c_uint32, ct.c_double, ct.c_uint32, ct.c_uint32, ct.c_uint32]
         lib.oracle_scene_destroy.argtypes = [ct.c_void_p]
         lib.oracle_scene_step.restype = ct.c_uint32
         lib.oracle_scene_step.argtypes = [ct.c_void_p, _DP, _DP, ct.c_void_p, ct.POINTER(ct.c_uint32), ct.c_double, ct.c_void_p]
@@ -620,10 +620,13 @@ class SceneOracle:
         w = records.world
         self.nb = int(w.body_count) - 1
         self.h = h
+        hull = getattr(records, "hull_vertices", None)
+        self._hull = None if hull is None else np.ascontiguousarray(hull, np.float32)
         self.handle = lib.oracle_scene_create(
             ct.byref(records.world), ct.cast(records.bodies, ct.c_void_p), ct.cast(records.shapes, ct.c_void_p),
-            ct.cast(records.materials, ct.c_void_p), ct.cast(records.pairs, ct.c_void_p), h, substeps, velocity_iterations,
-            final_velocity_iterations)
+            ct.cast(records.materials, ct.c_void_p), ct.cast(records.pairs, ct.c_void_p),
+            None if self._hull is None else self._hull.ctypes.data_as(ct.c_void_p),
+            0 if self._hull is None else len(self._hull), h, substeps, velocity_iterations, final_velocity_iterations)
         if not self.handle:
             raise RuntimeError("oracle_scene_create failed")
 

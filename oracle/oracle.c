@@ -1848,6 +1848,7 @@ void oracle_temporal_cone_dense(uint32_t n, const double* W, const double* u0, c
 #define SCON ORACLE_SCENE_CONTACTS
 #define SCAND ORACLE_SCENE_CANDIDATES
 #define SPAIRS (SNB * (SNB - 1) / 2 + SNB)
+#define SHULL 1024 /* hull vertices of a scene's convex bodies */
 
 struct OracleScene {
     uint32_t nb, np;
@@ -1864,11 +1865,14 @@ struct OracleScene {
     double offset[SNB], rest[SNB], sweep[SNB];
     double fric[4][2], resp[4][4];
     uint8_t pa[SPAIRS], pb[SPAIRS], pc[SPAIRS];
+    /* Convex bodies: hull vertices scaled by the body's dimensions. */
+    int hull_first[SNB], hull_count[SNB];
+    double hull[SHULL][3];
 };
 
 OracleScene* oracle_scene_create(const MRModelWorldC* w, const MRModelBodyC* bodies, const MRModelShapeC* shapes,
-                                 const MRModelMaterialC* materials, const MRModelPairC* pairs, double h,
-                                 uint32_t substeps, uint32_t iters, uint32_t final_iters) {
+                                 const MRModelMaterialC* materials, const MRModelPairC* pairs, const float* hull_vertices,
+                                 uint32_t hull_vertex_count, double h, uint32_t substeps, uint32_t iters, uint32_t final_iters) {
     OracleScene* s = (OracleScene*)calloc(1, sizeof(OracleScene));
     const uint32_t n = w->body_count - 1;
     s->nb = n;
@@ -1908,6 +1912,20 @@ OracleScene* oracle_scene_create(const MRModelWorldC* w, const MRModelBodyC* bod
         s->type[b] = shapes[b].shape_type;
         s->material[b] = shapes[b].material;
         for (int i = 0; i < 3; ++i) s->dims[b][i] = shapes[b].dimensions[i];
+        if (shapes[b].shape_type == MR_SHAPE_CONVEX) {
+            int used = 0;
+            for (uint32_t a = 0; a < b; ++a) used += s->hull_count[a];
+            if (!hull_vertices || shapes[b].hull_count == 0 || used + (int)shapes[b].hull_count > SHULL ||
+                shapes[b].hull_first + shapes[b].hull_count > hull_vertex_count) {
+                free(s);
+                return NULL;
+            }
+            s->hull_first[b] = used;
+            s->hull_count[b] = (int)shapes[b].hull_count;
+            for (uint32_t i = 0; i < shapes[b].hull_count; ++i)
+                for (int c = 0; c < 3; ++c)
+                    s->hull[used + i][c] = (double)hull_vertices[4 * (shapes[b].hull_first + i) + c] * shapes[b].dimensions[c];
+        }
         s->mass[b] = bodies[b].mass_inverse_mass[0];
         s->inv_mass[b] = bodies[b].mass_inverse_mass[1];
         s->damp_lin[b] = w->apply_body_damping ? bodies[b].damping_speed[0] : 0.0;
@@ -1946,6 +1964,8 @@ typedef struct {
     double hl;       /* cylinder half length */
     v3 bpos; /* pose of the collider's body: the frame of its manifold anchors */
     q4 brot;
+    const double* hull; /* convex: scaled local hull vertices, xyz each */
+    int hull_count;
 } SCol;
 
 typedef struct {
@@ -1971,9 +1991,13 @@ static void scol(const OracleScene* s, const SState* st, uint32_t b, SCol* o) {
         o->hl = 0.0;
         o->bpos = s->ground_pos;
         o->brot = s->ground_rot;
+        o->hull = NULL;
+        o->hull_count = 0;
         return;
     }
     o->type = (int)s->type[b];
+    o->hull = s->hull[s->hull_first[b]];
+    o->hull_count = o->type == MR_SHAPE_CONVEX ? s->hull_count[b] : 0;
     o->c = st->pos[b];
     o->r = st->rot[b];
     o->half = V(s->dims[b][0], s->dims[b][1], s->dims[b][2]);
@@ -2295,6 +2319,21 @@ static v3 ssupport(const SCol* k, uint32_t index, v3 d, uint32_t* feat) {
         *feat = feature_key(MR_SHAPE_BOX, v);
         return vadd(k->c, qrot(k->r, p));
     }
+    if (k->type == MR_SHAPE_CONVEX) {
+        /* The vertex of largest projection, the lowest index on a tie
+         * (Collision.metal:1899-1936); a near tie is a band decision. */
+        const v3 l = qrotinv(k->r, d);
+        double best = -INFINITY, second = -INFINITY;
+        int bi = 0;
+        for (int i = 0; i < k->hull_count; ++i) {
+            const double pr = k->hull[3 * i] * l.x + k->hull[3 * i + 1] * l.y + k->hull[3 * i + 2] * l.z;
+            if (pr > best) { second = best; best = pr; bi = i; }
+            else if (pr > second) second = pr;
+        }
+        if (k->hull_count > 1) BAND(best - second, 0.0);
+        *feat = feature_key(MR_SHAPE_CONVEX, (uint32_t)bi);
+        return vadd(k->c, qrot(k->r, V(k->hull[3 * bi], k->hull[3 * bi + 1], k->hull[3 * bi + 2])));
+    }
     /* cylinder */
     const double axial = vdot(d, k->axis);
     const v3 radial = vsub(d, vmul(k->axis, axial));
@@ -2429,7 +2468,7 @@ static int sclosest_simplex(SSup* sx, int* n, double* wt, v3* closest) {
 
 typedef struct {
     uint32_t status;
-    uint32_t path; /* how it was resolved: 0 GJK distance, 3 EPA, 1 MPR (the reference's `fallback`) */
+    uint32_t path; /* how it was resolved: 0 GJK distance, 3 EPA, 1 MPR, 2 support-axis witness (the reference's `fallback`) */
     v3 normal, pa, pb;
     double sep;
     uint32_t fa, fb;
@@ -2735,39 +2774,116 @@ static void spatch_add(SRaw* raw, v3 pa, v3 pb, double sep, uint32_t fa, uint32_
     sraw_add(raw, pa, pb, sep, fa, fb);
 }
 
-/* Extra points of a cylinder's face or side contact: supports along the
- * query normal tilted by 2e-4 towards the disk basis (cap contact) or the
- * axis (side contact). */
+/* Extra points of a cylinder's or hull's contact patch
+ * (Collision.metal:3327-3432): supports of the sampled shape -- a cylinder,
+ * else a hull, A first -- along the query normal tilted by 2e-4 towards the
+ * disk basis (cylinder cap contact), the axis (cylinder side contact) or
+ * the contact plane's tangents (hull). */
 static void spatch(const SCol* A, const SCol* B, uint32_t ia, uint32_t ib, double scale, const SQuery* q, SRaw* raw) {
-    const int cyl_a = A->type == MR_SHAPE_CYLINDER;
-    if (!cyl_a && B->type != MR_SHAPE_CYLINDER) return;
+    const int cyl_a = A->type == MR_SHAPE_CYLINDER, cyl_b = B->type == MR_SHAPE_CYLINDER;
+    const int hull = A->type == MR_SHAPE_CONVEX || B->type == MR_SHAPE_CONVEX;
+    if (!cyl_a && !cyl_b && !hull) return;
     const double dtol = 32.0 * kFloatEps * scale;
-    const SCol* k = cyl_a ? A : B;
-    const uint32_t kidx = cyl_a ? ia : ib;
-    const v3 sn = cyl_a ? q->normal : vmul(q->normal, -1.0);
+    const int sample_a = cyl_a || (!cyl_b && A->type == MR_SHAPE_CONVEX);
+    const SCol* k = sample_a ? A : B;
+    const uint32_t kidx = sample_a ? ia : ib;
+    const v3 sn = sample_a ? q->normal : vmul(q->normal, -1.0);
     v3 dirs[4];
     int nd = 0;
-    const double align = fabs(vdot(sn, k->axis));
-    BAND(align, 0.95);
-    BAND(align, 0.20);
-    if (align >= 0.95) {
-        dirs[0] = k->bx; dirs[1] = vmul(k->bx, -1.0); dirs[2] = k->bz; dirs[3] = vmul(k->bz, -1.0);
+    if (k->type == MR_SHAPE_CYLINDER) {
+        const double align = fabs(vdot(sn, k->axis));
+        BAND(align, 0.95);
+        BAND(align, 0.20);
+        if (align >= 0.95) {
+            dirs[0] = k->bx; dirs[1] = vmul(k->bx, -1.0); dirs[2] = k->bz; dirs[3] = vmul(k->bz, -1.0);
+            nd = 4;
+        } else if (align <= 0.20) {
+            dirs[0] = k->axis; dirs[1] = vmul(k->axis, -1.0);
+            nd = 2;
+        }
+    } else {
+        /* contactPatchTangent: the normal crossed with the world axis of
+         * its smallest absolute component. */
+        const v3 n = q->normal;
+        const double ax = fabs(n.x), ay = fabs(n.y), az = fabs(n.z);
+        const v3 ref = ax <= ay && ax <= az ? V(1, 0, 0) : (ay <= az ? V(0, 1, 0) : V(0, 0, 1));
+        v3 t = vcross(n, ref);
+        t = vmul(t, 1.0 / vlen(t));
+        const v3 bt = vcross(n, t);
+        dirs[0] = t; dirs[1] = vmul(t, -1.0); dirs[2] = bt; dirs[3] = vmul(bt, -1.0);
         nd = 4;
-    } else if (align <= 0.20) {
-        dirs[0] = k->axis; dirs[1] = vmul(k->axis, -1.0);
-        nd = 2;
     }
     for (int i = 0; i < nd; ++i) {
         uint32_t f;
         const v3 p = ssupport(k, kidx, vadd(sn, vmul(dirs[i], 2.0e-4)), &f);
-        const v3 pa = cyl_a ? p : vsub(p, vmul(q->normal, q->sep));
-        const v3 pb = cyl_a ? vadd(p, vmul(q->normal, q->sep)) : p;
-        spatch_add(raw, pa, pb, q->sep, cyl_a ? f : q->fa, cyl_a ? q->fb : f, dtol * dtol);
+        const v3 pa = sample_a ? p : vsub(p, vmul(q->normal, q->sep));
+        const v3 pb = sample_a ? vadd(p, vmul(q->normal, q->sep)) : p;
+        spatch_add(raw, pa, pb, q->sep, sample_a ? f : q->fa, sample_a ? q->fb : f, dtol * dtol);
     }
 }
 
-/* Contacts of a support-mapped (cylinder) pair; the pair's normal (A -> B). */
+/* Penetration witness of the hull path (Collision.metal:3129-3260): among
+ * the centre-to-centre direction and the three local axes of each collider,
+ * oriented from A towards B, the axis of largest separation
+ * dot(support_B(-axis) - support_A(axis), axis).  No previous-substep query
+ * direction is tried (no query cache is kept). */
+static int ssupport_axis_witness(const SCol* A, const SCol* B, uint32_t ia, uint32_t ib, SQuery* q) {
+    const v3 delta = vsub(B->c, A->c);
+    v3 axes[7];
+    axes[0] = delta;
+    for (int a = 0; a < 3; ++a) {
+        const v3 e = V(a == 0, a == 1, a == 2);
+        axes[1 + 2 * a] = qrot(A->r, e);
+        axes[2 + 2 * a] = qrot(B->r, e);
+    }
+    int found = 0;
+    double second = -INFINITY;
+    for (int i = 0; i < 7; ++i) {
+        v3 axis = axes[i];
+        const double a2 = vdot(axis, axis);
+        if (!(a2 > kSceneTiny) || !isfinite(a2)) continue;
+        axis = vmul(axis, 1.0 / sqrt(a2));
+        if (vdot(delta, delta) > kSceneTiny && vdot(axis, delta) < 0.0) axis = vmul(axis, -1.0);
+        uint32_t fa, fb;
+        const v3 pa = ssupport(A, ia, axis, &fa);
+        const v3 pb = ssupport(B, ib, vmul(axis, -1.0), &fb);
+        const double sep = vdot(vsub(pb, pa), axis);
+        if (!isfinite(sep)) return 0;
+        if (!found || sep > q->sep) {
+            if (found) second = q->sep;
+            found = 1;
+            q->normal = axis;
+            q->sep = sep;
+            q->pa = pa;
+            q->pb = pb;
+            q->fa = fa;
+            q->fb = fb;
+        } else if (sep > second) {
+            second = sep;
+        }
+    }
+    if (!found) return 0;
+    if (isfinite(second)) BAND(q->sep - second, 0.0);
+    q->sep = fmin(q->sep, -0.0);
+    q->status = MR_STEP_SUCCESS;
+    q->path = 2;
+    return vfinite(q->pa) && vfinite(q->pb) && vfinite(q->normal) && isfinite(q->sep);
+}
+
+/* Contacts of a support-mapped pair; the pair's normal (A -> B).  Cylinder
+ * pairs resolve an overlap by EPA, then MPR; pairs with a hull by the
+ * support-axis witness (Collision.metal:3623-3720), a hull on the plane by
+ * its deepest vertex. */
 static v3 ssupport_mapped(const SCol* A, const SCol* B, uint32_t ia, uint32_t ib, double acc, SRaw* raw) {
+    if (B->type == MR_SHAPE_PLANE) {
+        uint32_t f;
+        const v3 p = ssupport(A, ia, vmul(B->normal, -1.0), &f);
+        const double sep = vdot(B->normal, vsub(p, B->c));
+        BAND(sep, acc);
+        if (sep <= acc) sraw_add(raw, p, vsub(p, vmul(B->normal, sep)), sep, f, feature_key(MR_SHAPE_PLANE, 0u));
+        return vmul(B->normal, -1.0);
+    }
+    const int hull = A->type == MR_SHAPE_CONVEX || B->type == MR_SHAPE_CONVEX;
     const double scale = fmax(scol_scale(A), scol_scale(B)) + 1.0;
     SSup sx[4];
     double wt[4] = {0, 0, 0, 0};
@@ -2777,7 +2893,12 @@ static v3 ssupport_mapped(const SCol* A, const SCol* B, uint32_t ia, uint32_t ib
     q.normal = V(0, 0, 1);
     const int overlap = sgjk(A, B, ia, ib, scale, sx, &n, wt, &q);
     if (q.status != MR_STEP_SUCCESS && q.status != MR_STEP_DID_NOT_CONVERGE) { raw->status = q.status; return q.normal; }
-    if (overlap) {
+    if (hull) {
+        if ((overlap || q.status == MR_STEP_DID_NOT_CONVERGE) && !ssupport_axis_witness(A, B, ia, ib, &q)) {
+            raw->status = MR_STEP_DID_NOT_CONVERGE;
+            return q.normal;
+        }
+    } else if (overlap) {
         /* Primitive pairs resolve with EPA first, MPR second (Collision.metal:3518-3560). */
         if (!sepa(A, B, ia, ib, scale, sx, n, &q) && !smpr(A, B, ia, ib, scale, &q)) {
             raw->status = MR_STEP_DID_NOT_CONVERGE;

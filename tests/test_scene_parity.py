@@ -190,6 +190,18 @@ def test_cylinder_pile_control_steps_match_oracle(cuda_device, seed):
     _check_rows(rows, max(40, len(rows) // 10))
 
 
+@pytest.mark.parametrize("seed", [3, 7, 5])  # one quarter convex hulls of 12 vertices
+def test_hull_pile_control_steps_match_oracle(cuda_device, seed):
+    """Piles with convex hulls (MR_RUN_SOURCE_SYNTHETIC_HULL_PILE): the hull
+    path of the support-mapped narrowphase -- GJK distance, the
+    support-axis penetration witness, the sampled patch, the deepest vertex
+    on the plane -- on the device against the oracle's FP64 restatement,
+    under the pile tolerances.  A hull vertex or witness axis picked within
+    rounding of a tie is a band decision."""
+    rows = _compare_run(seed, 8, 60, "fp32", "hull_pile")
+    _check_rows(rows, max(40, len(rows) // 10))
+
+
 @pytest.mark.parametrize("seed", [3, 13, 1])  # 10, 17 and 50 bodies
 def test_gjk_capsule_box_pile_control_steps_match_oracle(cuda_device, seed):
     """Piles whose capsule-box pairs take the support-mapped narrowphase
