@@ -176,6 +176,86 @@ def test_pile_failed_step_keeps_state_and_reset_restores(cuda_device):
         assert np.max(np.abs(q3[1] - qo)) <= Q_TOL * max(1.0, np.max(np.abs(qo)))
 
 
+def _overflow_states(world) -> np.ndarray:
+    """Four states of the 64-body pile (seed 31: 14 spheres, 24 capsules,
+    26 boxes), each the first substep of a capacity limit in the oracle:
+    every body at one point (2016 overlapping body pairs for 512 candidate
+    slots ->
+    MR_STEP_PAIR_CAPACITY_OVERFLOW), the bodies 4 cm apart on a line (more
+    touching pairs than the 128 manifold slots -> MANIFOLD), boxes face to
+    face in a row, spheres in a row and capsules apart, all resting 1 mm
+    deep on the plane (283 contact points for 256 solver rows -> CONTACT),
+    and a settled state that fits."""
+
+    model = world.model()
+    n = int(model.world.body_count) - 1
+    types = [int(model.shapes[i].shape_type) for i in range(n)]
+    dims = [np.array(model.shapes[i].dimensions[:3], np.float64) for i in range(n)]
+    q = np.zeros((4, n, 7))
+    q[..., 6] = 1.0
+    q[0, :, 2] = 0.5
+    q[1, :, 0] = 0.04 * np.arange(n)
+    q[1, :, 2] = 0.2
+    pen, end = 0.001, {0: None, 2: None}
+    for i, t in enumerate(types):
+        if t in end:  # spheres and boxes in rows, each 1 mm into the previous one
+            half = dims[i][0]
+            q[2, i, 0] = 0.0 if end[t] is None else end[t] + half - pen
+            end[t] = q[2, i, 0] + half
+            q[2, i, 1] = 0.0 if t == 2 else 1.0
+            q[2, i, 2] = (dims[i][2] if t == 2 else dims[i][0]) - pen
+        else:  # capsules lie along their local y axis, apart
+            q[2, i, :3] = [0.5 * i, 2.0, dims[i][0] - pen]
+    return q
+
+
+def test_pile_capacity_overflows_latch_like_the_oracle(cuda_device):
+    """Capacity limits are statuses, not truncations: an environment whose
+    candidate pairs, manifolds or solver contacts exceed their capacity
+    reports the same status code as the oracle and keeps its state
+    bit for bit; the other environments step on."""
+
+    import torch
+
+    from oracle import SceneTable
+
+    envs = 4
+    with nb.World("pile", envs, seed=31) as world:
+        acts = torch.zeros((1, envs, 0), device="cuda")
+        for _ in range(5):
+            world.step(acts, wait=True)
+        q0, v0, _ = world.state()
+        n = q0.shape[1] // 7
+        states = _overflow_states(world)
+        q = q0.copy()
+        v = np.zeros_like(v0)
+        for e in range(3):
+            q[e] = states[e].reshape(-1)
+        v[3] = v0[3]
+        empty = np.zeros((envs,) + world.state()[2].shape[1:], np.float32)
+        world.set_state(q, v, empty)
+        q_in, v_in, _ = world.state()
+        oracle = SceneOracle(world.model(), 0.005, 4, 8, 0)
+        friction = world.friction_scales()
+        want = []
+        for e in range(envs):
+            qo, vo = q_in[e].astype(np.float64), v_in[e].astype(np.float64)
+            st, _ = oracle.step(qo, vo, SceneTable(), float(friction[e]))
+            want.append((st, qo))
+        assert [w[0] for w in want] == [4, 6, 5, 0]
+        for k in range(2):  # the failed environments fail again from the kept state
+            _, status, _ = world.step(acts, wait=True)
+            st = status.cpu().numpy()[0].tolist()
+            assert st[:3] == [w[0] for w in want[:3]] and st[3] == 0
+            q1, v1, _ = world.state()
+            np.testing.assert_array_equal(q1[:3], q_in[:3])
+            np.testing.assert_array_equal(v1[:3], v_in[:3])
+            if k == 0:
+                qo = want[3][1]
+                assert np.max(np.abs(q1[3] - qo)) <= Q_TOL * max(1.0, np.max(np.abs(qo)))
+        assert n == 64
+
+
 @pytest.mark.parametrize("seed", [3, 11, 5])  # 10, 25 and 49 bodies, one quarter cylinders
 def test_cylinder_pile_control_steps_match_oracle(cuda_device, seed):
     """Piles with cylinders: the support-mapped narrowphase (GJK, EPA, MPR,
