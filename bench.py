@@ -561,16 +561,20 @@ def run_pile(args, source: str = "pile") -> None:
     print(json.dumps(line))
 
 
-def run_policy(args) -> None:
+def run_policy(args, task: bool = False) -> None:
     """Closed loop: 4096 tree29 environments driven by a native policy on
     the device (mr_task_rollout_set_policy) -- a seeded random actor
-    71-256-128-29 (elu, silu, tanh) with observation normalisation and
-    Gaussian sampling, plus a 71-64-1 critic -- 25 policy-driven control
-    steps per bench step."""
+    obs-256-128-29 (elu, silu, tanh) with observation normalisation and
+    Gaussian sampling, plus an obs-64-1 critic -- 25 policy-driven control
+    steps per bench step.  The policy reads [q, v] (71 values), or with
+    `task` the actor frames of a velocity-tracking locomotion task
+    (numi_lab_b200.task.locomotion_task: 99 values) whose observe, apply and
+    complete kernels run around every control step."""
 
     import torch
 
     import numi_lab_b200 as nb
+    from numi_lab_b200 import task as T
 
     torch.cuda.set_device(0)
     device = torch.device("cuda", 0)
@@ -582,6 +586,11 @@ def run_policy(args) -> None:
                 for (a, b), f in zip(zip(sizes[:-1], sizes[1:]), acts)]
 
     with nb.World("tree29", envs, substeps=SUBSTEPS, velocity_iterations=ITERATIONS, control_dt=CONTROL_DT, seed=SEED) as world:
+        if task:
+            q0, _, _ = nb.sample_reset("tree29", SEED, SEED, 0, 1)
+            default_q = np.zeros(world.nq, np.float32)
+            default_q[2], default_q[6] = q0[0, 2], 1.0
+            world.set_task(T.locomotion_task(world.model(), default_q, maximum_episode_steps=500, noise=0.01))
         nobs, na = world.observation_count, world.action_count
         world.set_policy(layers=dense([nobs, 256, 128, na], ["elu", "silu", "tanh"]), critic_layers=dense([nobs, 64, 1], ["relu", "identity"]),
                          revision=1, action_clip=2.5, observation_mean=np.zeros(nobs, np.float32),
@@ -607,6 +616,14 @@ def run_policy(args) -> None:
         clock_summary = clocks.summary()
         ms = float(sum(a.elapsed_time(b) for a, b in zip(starts, stops)))
         chains = world.environment_chains
+        episodes = None
+        if task:
+            tr = world.transitions(horizon)
+            episodes = {"mean_reward": float(tr["reward"].mean()), "episodes_ended": int(tr["done"].sum()),
+                        "timeouts": int(tr["timeout"].sum()), "height_or_tilt": int(np.isin(tr["termination_reason"], (1, 2)).sum())}
+    workload = (f"tree29 x {envs} envs driven by a native policy (actor {nobs}-256-128-29, critic {nobs}-64-1, stochastic)"
+                + (" through a locomotion task layer (observe, apply, complete kernels per control step)" if task else "")
+                + f", {horizon} control steps per bench step")
     line = {
         "metric": "closed-loop env-steps/s",
         "value": envs * horizon * args.steps / (ms / 1e3),
@@ -620,14 +637,20 @@ def run_policy(args) -> None:
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded random policy weights)",
-        "config": {"workload": f"tree29 x {envs} envs driven by a native policy (actor 71-256-128-29, critic 71-64-1, "
-                               f"stochastic), {horizon} control steps per bench step", "l2": "flushed (256 MiB write) between steps"},
-        "gpu_launches": 2 * chains * horizon * args.steps + args.steps,  # policy + control step per chain and step, one counter
+        "config": {"workload": workload, "l2": "flushed (256 MiB write) between steps"},
+        # policy + control step (+ observe, apply, complete) per chain and control step, one counter per bench step
+        "gpu_launches": (5 if task else 2) * chains * horizon * args.steps + args.steps,
         "environment_chains": chains,
         "clocks": {k: clock_summary[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
         "failed_env_steps_last_step": failures,
     }
+    if task:
+        line["last_step_transitions"] = episodes
     print(json.dumps(line))
+
+
+def run_task(args) -> None:
+    run_policy(args, task=True)
 
 
 MIX_TOTAL = 16384
@@ -1003,7 +1026,7 @@ def main() -> None:
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--envs", type=int, default=0, help="pile workload: environments (default 16384; smaller for profiling)")
     parser.add_argument("--workload", default="tree29",
-                        choices=["tree29", "pile", "cylinder_pile", "hull_pile", "mix", "precision", "policy", "quality"],
+                        choices=["tree29", "pile", "cylinder_pile", "hull_pile", "mix", "precision", "policy", "task", "quality"],
                         help="tree29 (the headline), pile (36-body piles), cylinder_pile (36-body piles with cylinders: "
                              "GJK / EPA pairs), mix (chains, trees and piles) or precision (box stacks and trees against the "
                              "FP64 oracle) or policy (tree29 closed loop under a native policy) or quality (tree29 with the "
@@ -1031,7 +1054,7 @@ def main() -> None:
         if rank == 0:
             {"pile": run_pile, "cylinder_pile": lambda a: run_pile(a, "cylinder_pile"),
              "hull_pile": lambda a: run_pile(a, "hull_pile"), "mix": run_mix,
-             "precision": run_precision, "policy": run_policy, "quality": run_quality}[args.workload](args)
+             "precision": run_precision, "policy": run_policy, "task": run_task, "quality": run_quality}[args.workload](args)
         return
 
     run_headline(args, rank, local_rank, world_size)

@@ -619,6 +619,238 @@ MR_API int mr_task_rollout_copy_final_scene_states(
     const MRTaskRolloutHandle* handle, float* output, size_t output_count);
 
 /* ---------------------------------------------------------------------- */
+/* Task layer (reference: include/metalrobo/task_program_types.h,         */
+/* src/metal/LocomotionTask.metal observe / apply_actions / complete)      */
+/* ---------------------------------------------------------------------- */
+
+/* Operator codes: the reference's MRTaskObservationOpcode,
+ * MRTaskRewardOpcode, MRTaskTerminationOpcode, MRTaskTerminationReason and
+ * MRTaskRandomizationOpcode (task_program_types.h:68-300), same values.
+ * The task layer evaluates the subset listed here; mr_task_rollout_set_task
+ * refuses any other code. */
+enum {
+    MR_TASK_OBSERVE_ROOT_ANGULAR_VELOCITY_LOCAL = 0u,
+    MR_TASK_OBSERVE_PROJECTED_GRAVITY = 1u,
+    MR_TASK_OBSERVE_COMMAND = 2u,
+    MR_TASK_OBSERVE_JOINT_POSITION_ERROR = 3u,
+    MR_TASK_OBSERVE_JOINT_VELOCITY = 4u,
+    MR_TASK_OBSERVE_PREVIOUS_ACTION = 5u,
+    MR_TASK_OBSERVE_ROOT_LINEAR_VELOCITY_LOCAL = 6u,
+    MR_TASK_OBSERVE_ROOT_HEIGHT = 7u,
+    MR_TASK_OBSERVE_GAIT_PHASE = 14u,
+    MR_TASK_OBSERVE_DELAYED_ACTION = 26u,
+    MR_TASK_OBSERVE_JOINT_FINITE_DIFFERENCE_VELOCITY = 27u
+};
+enum { MR_TASK_OBSERVATION_NORMALIZE_VECTOR3 = 1u };
+enum {
+    MR_TASK_REWARD_LINEAR_VELOCITY_TRACKING = 0u,
+    MR_TASK_REWARD_YAW_VELOCITY_TRACKING = 1u,
+    MR_TASK_REWARD_CONSTANT = 2u,
+    MR_TASK_REWARD_ROOT_VERTICAL_VELOCITY_SQUARED = 3u,
+    MR_TASK_REWARD_ROOT_ROLL_PITCH_VELOCITY_SQUARED = 4u,
+    MR_TASK_REWARD_TILT_SQUARED = 5u,
+    MR_TASK_REWARD_ROOT_HEIGHT_ERROR_SQUARED = 6u,
+    MR_TASK_REWARD_JOINT_VELOCITY_SQUARED = 7u,
+    MR_TASK_REWARD_JOINT_ACCELERATION_SQUARED = 8u,
+    MR_TASK_REWARD_ACTION_RATE_SQUARED = 9u,
+    MR_TASK_REWARD_JOINT_LIMIT_VIOLATION_SQUARED = 10u,
+    MR_TASK_REWARD_JOINT_GROUP_POSTURE_SQUARED = 12u,
+    MR_TASK_REWARD_JOINT_GROUP_POSTURE_ABSOLUTE = 17u,
+    MR_TASK_REWARD_PROJECTED_GRAVITY_HORIZONTAL_SQUARED = 18u,
+    MR_TASK_REWARD_JOINT_LIMIT_VIOLATION_ABSOLUTE = 20u,
+    MR_TASK_REWARD_ROOT_HEIGHT_NORMALIZED = 21u,
+    MR_TASK_REWARD_ROOT_HEIGHT_PROGRESS = 22u,
+    MR_TASK_REWARD_UPRIGHTNESS = 23u
+};
+enum {
+    MR_TASK_TERMINATE_MINIMUM_ROOT_HEIGHT = 0u,
+    MR_TASK_TERMINATE_MAXIMUM_TILT = 1u
+};
+enum {
+    MR_TASK_TERMINATION_CONTINUING = 0u,
+    MR_TASK_TERMINATION_HEIGHT = 1u,
+    MR_TASK_TERMINATION_TILT = 2u,
+    MR_TASK_TERMINATION_CONTACT = 3u,
+    MR_TASK_TERMINATION_TIMEOUT = 4u,
+    MR_TASK_TERMINATION_PHYSICS_ERROR = 5u
+};
+enum {
+    MR_TASK_RANDOMIZE_ROOT_POSITION = 0u,
+    MR_TASK_RANDOMIZE_ROOT_YAW = 1u,
+    MR_TASK_RANDOMIZE_ACTION_POSITION = 2u,
+    MR_TASK_RANDOMIZE_VELOCITY = 3u,
+    MR_TASK_RANDOMIZE_ACTION_VELOCITY = 9u,
+    MR_TASK_RANDOMIZE_ROOT_HEIGHT = 10u,
+    MR_TASK_RANDOMIZE_JOINT_POSITION = 12u
+};
+
+/* reference: MRTaskActionBindingGPU (task_program_types.h:443-458), the
+ * joint-position actuator.  Action `index` of the policy sets the drive
+ * target of DoF `dof_index` (its coordinate q_index, velocity v_index):
+ * clamp(default_q[q_index] + scale x filtered action, lower_target,
+ * upper_target), the filtered action following the delayed raw action with
+ * a first-order response of `response_time_seconds` (0: none). */
+typedef struct MRTaskActionBindingC {
+    uint32_t dof_index;
+    uint32_t q_index;
+    uint32_t v_index;
+    uint32_t reserved;
+    float scale;
+    float lower_target;
+    float upper_target;
+    float response_time_seconds;
+} MRTaskActionBindingC;
+
+/* reference: MRTaskObservationOperatorGPU (:460-467).  One actor
+ * observation: transform_scale x source + transform_offset, plus
+ * noise_amplitude x a uniform draw in [-1, 1] on noise_channel.  `source`
+ * is the action index for joint sources; `component` the vector lane (for
+ * DELAYED_ACTION: how many raw actions back). */
+typedef struct MRTaskObservationOperatorC {
+    uint32_t opcode;
+    uint32_t source;
+    uint32_t component;
+    uint32_t flags;
+    float transform_scale;
+    float transform_offset;
+    float noise_amplitude;
+    uint32_t noise_channel;
+} MRTaskObservationOperatorC;
+
+/* reference: MRTaskRewardOperatorGPU (:496-504).  The step's reward is
+ * control_dt x sum(weight x value). */
+typedef struct MRTaskRewardOperatorC {
+    uint32_t opcode;
+    uint32_t group;      /* joint group of the posture rewards */
+    float weight;
+    float parameters[3]; /* the reference's parameters.yzw */
+} MRTaskRewardOperatorC;
+
+/* reference: MRTaskTerminationOperatorGPU (:506-513). */
+typedef struct MRTaskTerminationOperatorC {
+    uint32_t opcode;
+    uint32_t reason;
+    uint32_t priority;
+    uint32_t reserved;
+    float threshold;
+    float failure_penalty;
+} MRTaskTerminationOperatorC;
+
+/* reference: MRTaskRandomizationOperatorGPU (:515-520); `target` is the q
+ * index of JOINT_POSITION. */
+typedef struct MRTaskRandomizationOperatorC {
+    uint32_t opcode;
+    uint32_t target;
+    float parameters[4];
+} MRTaskRandomizationOperatorC;
+
+/* reference: MRTaskIndexGroupGPU (:491-494): action indices
+ * joint_members[first, first + count). */
+typedef struct MRTaskIndexGroupC {
+    uint32_t first;
+    uint32_t count;
+} MRTaskIndexGroupC;
+
+/* A compiled task program: the tables and constants of the reference's
+ * MRTaskProgramHeaderGPU (:358-441) that the evaluated subset reads.  One
+ * actor history frame, one difficulty band, no terrain, pushes, contact
+ * groups or sensor biases. */
+typedef struct MRTaskProgramC {
+    const MRTaskActionBindingC* actions;
+    uint32_t action_count;          /* equals the world's action count */
+    const MRTaskObservationOperatorC* actor;
+    uint32_t actor_count;
+    const MRTaskRewardOperatorC* rewards;
+    uint32_t reward_count;
+    const MRTaskTerminationOperatorC* terminations;
+    uint32_t termination_count;
+    const MRTaskRandomizationOperatorC* randomization;
+    uint32_t randomization_count;
+    const MRTaskIndexGroupC* joint_groups;
+    uint32_t joint_group_count;
+    const uint32_t* joint_members;
+    uint32_t joint_member_count;
+    const float* default_q;         /* [nq]: the reset pose and posture reference */
+    uint32_t default_q_count;
+    uint32_t maximum_episode_steps; /* timeout */
+    uint32_t action_history;        /* delay-line slots including the filter slot, 3..8 */
+    uint32_t action_delay_steps;    /* raw actions of delay; at most action_history - 2 take effect */
+    float base_height_target;       /* program.locomotion.x */
+    float gait_period_seconds;      /* program.locomotion.y */
+    float root_reference[3];        /* root link origin from the root's q position, root axes */
+    float command_lower[3];         /* x, y velocity and yaw rate */
+    float command_upper[3];
+    float standing_probability;     /* a drawn command is zeroed with it */
+    float command_duration_seconds[2];
+    uint64_t task_fingerprint;
+} MRTaskProgramC;
+
+/* reference: include/metalrobo/c_api.h:261-295 (same layout, 128 bytes). */
+typedef struct MRTaskTransitionC {
+    float reward;
+    float tracking_score;
+    float root_height;
+    float tilt;
+    uint32_t done;
+    uint32_t timeout;
+    uint32_t physics_error;
+    uint32_t termination_reason;
+    float task_reward;
+    float base_reward;
+    float joint_velocity_reward;
+    float joint_acceleration_reward;
+    float control_reward;
+    float posture_reward;
+    float energy_reward;
+    float contact_reward;
+    float task_outcome_channel_0;
+    float task_outcome_channel_1;
+    float task_outcome_channel_2;
+    float task_outcome_channel_3;
+    float task_outcome_channel_4;
+    float task_outcome_channel_5;
+    float task_outcome_channel_6;
+    float task_outcome_channel_7;
+    uint64_t policy_revision;
+    float timeout_bootstrap_value;
+    float episode_tracking_score;
+    uint32_t difficulty_band;
+    uint32_t terrain_level;
+    uint32_t impact_sequence_index;
+    uint32_t impact_event_flags;
+} MRTaskTransitionC;
+
+/* No counterpart in the reference's C ABI, which compiles its task from the
+ * run manifest's TaskPack; this installs a compiled task program on an
+ * articulated rollout (the synthetic sources).  From the next advance each
+ * control step runs, per environment: observe (a pending reset draws the
+ * reset state from default_q and the randomization operators, starts an
+ * episode and a command, and writes the actor frame of the reset state);
+ * the policy, when one is installed, on that frame; apply (actions through
+ * the bindings to drive targets); the physics step; complete (rewards,
+ * terminations, timeout, the next command and the next actor frame).
+ * Observations become the actor frames the step's actions were taken on
+ * (actor_count values), actions the policy's normalised outputs.  Every
+ * environment starts a new episode at the next advance.  Refused: an
+ * operator outside the subset above, an index out of range, a pile or
+ * stack world. */
+MR_API int mr_task_rollout_set_task(MRTaskRolloutHandle* handle, const MRTaskProgramC* task);
+/* No counterpart in the reference: removes the task (raw PD targets and
+ * [q, v] observations again). */
+MR_API int mr_task_rollout_clear_task(MRTaskRolloutHandle* handle);
+/* reference: c_api.h:700-702.  [step][env] of the last advance; null
+ * without a task or before the first advance. */
+MR_API const MRTaskTransitionC* mr_task_rollout_transitions(const MRTaskRolloutHandle* handle);
+/* No counterpart in the reference: device address of the last advance's
+ * transitions ([step][env], valid until the next advance), 0 without a
+ * task. */
+MR_API uint64_t mr_task_rollout_device_transitions(const MRTaskRolloutHandle* handle);
+/* No counterpart in the reference: copies the first `count` transitions of
+ * the last advance ([step][env]) into host memory after its work finished;
+ * count must not exceed its steps x environments. */
+MR_API int mr_task_rollout_copy_transitions(const MRTaskRolloutHandle* handle, MRTaskTransitionC* output, size_t count);
+
+/* ---------------------------------------------------------------------- */
 /* Additions of this library                                               */
 /* ---------------------------------------------------------------------- */
 

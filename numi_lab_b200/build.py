@@ -22,7 +22,7 @@ LIBRARY = PACKAGE_DIR / "libnumi_b200.so"
 BUILD_DIR = PACKAGE_DIR / "_build"
 
 SOURCES = ["model.cpp", "world_step.cu", "scene_step.cu", "mix_step.cu", "policy.cu", "rollout.cu", "serve.cu", "no_alloc.cu",
-           "peaks.cu", "quality.cu", "packs.cpp"]
+           "peaks.cu", "quality.cu", "packs.cpp", "task.cu"]
 HEADERS = ["model.h", "device_model.h", "layout.h", "dmath.cuh", "runtime.h", "contact.cuh", "scene.h", "policy.h",
            "world_step.cuh", "scene_step.cuh", "mix.h", "audit.cuh", "quality.cuh", "packs.h"]
 

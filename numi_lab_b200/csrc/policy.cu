@@ -57,13 +57,16 @@ __device__ __forceinline__ float normal_draw(unsigned long long key, int action)
 // Observation feature i of the tile's environment e into x (normalised).
 __device__ __forceinline__ void load_observation(const PolicyParams& p, const float* mean, const float* inv_std, int env0,
                                                  float* x) {
-    const int nobs = p.nq + p.nv;
+    const int nobs = p.frame ? p.frame_count : p.nq + p.nv;
     for (int idx = threadIdx.x; idx < kPolicyTile * nobs; idx += blockDim.x) {
         const int e = idx / nobs, i = idx - e * nobs;
         const int env = env0 + e;
         float value = 0.0f;
         if (env < p.envs) {
-            value = i < p.nq ? p.q[static_cast<size_t>(env) * p.nq + i] : p.v[static_cast<size_t>(env) * p.nv + (i - p.nq)];
+            if (p.frame)
+                value = p.frame[static_cast<size_t>(env) * nobs + i];
+            else
+                value = i < p.nq ? p.q[static_cast<size_t>(env) * p.nq + i] : p.v[static_cast<size_t>(env) * p.nv + (i - p.nq)];
             if (mean) value = fminf(fmaxf((value - mean[i]) * inv_std[i], -p.obs_clip), p.obs_clip);
         }
         x[e * kPolicyMaxWidth + i] = value;

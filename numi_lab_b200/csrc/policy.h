@@ -23,17 +23,20 @@ struct PolicyParams {
     PolicyLayer actor[kPolicyMaxLayers];
     PolicyLayer critic[kPolicyMaxLayers];
     std::int32_t actor_layers, critic_layers;
-    const float* obs_mean;      // [nq + nv] or null (no normalisation)
+    const float* obs_mean;      // [observation count] or null (no normalisation)
     const float* obs_inv_std;
-    const float* critic_mean;   // [nq + nv] or null
+    const float* critic_mean;   // [observation count] or null
     const float* critic_inv_std;
     float obs_clip, action_clip;
     const float* log_std;       // [na] or null (deterministic)
     const float* action_bias;   // [na]
     const float* action_scale;  // [na]
-    // Observation source: the resident state.
+    // Observation source: the task layer's actor frames ([env][frame_count])
+    // when `frame` is set, else the resident state [q, v].
     const float* q;
     const float* v;
+    const float* frame;
+    std::int32_t frame_count;
     std::int32_t nq, nv, envs, na;
     // Outputs of this control step (per env), any of them null to skip.
     float* actions;    // [env][na]: fed to the control step

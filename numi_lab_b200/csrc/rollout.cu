@@ -18,6 +18,7 @@
 #include "quality.cuh"
 #include "runtime.h"
 #include "scene.h"
+#include "task.h"
 
 #include <cuda_runtime.h>
 
@@ -390,6 +391,14 @@ struct InstalledPolicy {
     bool has_critic = false;
 };
 
+// A task program installed on a rollout (mr_task_rollout_set_task): its
+// tables in one device arena, the launch constants pointing into it.
+struct InstalledTask {
+    DeviceBuffer<unsigned char> arena;
+    numi::TaskProgramDevice prog{};
+    std::uint64_t fingerprint = 0;
+};
+
 struct MRTaskRolloutHandle {
     numi::CompiledModel model;
     numi::DeviceModel dmodel{};
@@ -459,6 +468,17 @@ struct MRTaskRolloutHandle {
     DeviceBuffer<unsigned long long> d_policy_steps;
     bool have_policy_outputs = false;
     std::uint32_t last_policy_steps = 0;
+    // Task layer: the installed program, per-environment task records, the
+    // drive targets of the step in flight, the steps' reset masks and
+    // transitions ([step][env]) of the last advance.
+    std::unique_ptr<InstalledTask> task;
+    DeviceBuffer<numi::TaskEnvState> d_task_state;
+    DeviceBuffer<float> d_task_history, d_task_previous, d_task_frame, d_task_targets;
+    DeviceBuffer<std::uint32_t> d_task_masks;
+    DeviceBuffer<MRTaskTransitionC> d_transitions;
+    PinnedBuffer<MRTaskTransitionC> h_transitions;
+    std::uint32_t transition_steps = 0;   // steps of d_transitions written by the last advance
+    bool have_host_transitions = false;
     DeviceBuffer<float> d_actions, d_obs;
     DeviceBuffer<std::uint32_t> d_masks, d_status, d_contacts, d_stats;
     PinnedBuffer<float> h_obs, h_final_q;
@@ -480,11 +500,14 @@ struct MRTaskRolloutHandle {
         const void* latents;  // policy outputs (reallocated when an advance needs more room)
         const void* log_prob;
         const void* values;
+        const void* task;         // installed task's arena, or null
+        const void* task_masks;   // task-layer buffers (reallocated when an advance needs more room)
+        const void* transitions;
         bool operator<(const GraphKey& o) const {
             return std::tie(steps, actions, masks, obs, status, contacts, precision, host_obs, policy, evaluate_final, latents,
-                            log_prob, values) <
+                            log_prob, values, task, task_masks, transitions) <
                    std::tie(o.steps, o.actions, o.masks, o.obs, o.status, o.contacts, o.precision, o.host_obs, o.policy,
-                            o.evaluate_final, o.latents, o.log_prob, o.values);
+                            o.evaluate_final, o.latents, o.log_prob, o.values, o.task, o.task_masks, o.transitions);
         }
     };
     std::map<GraphKey, cudaGraphExec_t> graphs;
@@ -648,8 +671,10 @@ struct MRTaskRolloutHandle {
             return;
         }
         const bool driven = policy != nullptr;
+        const bool tasked = task != nullptr;
         // With a policy each chain evaluates it on its own block before each
-        // of its steps.
+        // of its steps; with a task, observe runs before the policy, apply
+        // after it and complete after the physics step.
         const int nchains = static_cast<int>(std::min<std::uint32_t>(static_cast<std::uint32_t>(chains), envs));
         if (nchains > 1) {
             check(cudaEventRecord(ev_fork, s), "event");
@@ -660,7 +685,9 @@ struct MRTaskRolloutHandle {
             const std::uint32_t n = static_cast<std::uint32_t>(static_cast<std::uint64_t>(envs) * (c + 1) / nchains) - o;
             cudaStream_t cs = nchains > 1 ? chain_stream[c] : s;
             for (std::uint32_t k = 0; k < steps; ++k) {
+                if (tasked) check(numi::launch_task_observe(task_params(k, o, n, actions, masks, obs, status), cs), "task observe launch");
                 if (driven) enqueue_policy(k, o, n, const_cast<float*>(actions) + static_cast<size_t>(k) * envs * na, true, cs);
+                if (tasked) check(numi::launch_task_apply(task_params(k, o, n, actions, masks, obs, status), cs), "task apply launch");
                 const size_t item0 = static_cast<size_t>(k) * envs + o;  // this chain's first item of step k
                 numi::StepParams p{};
                 p.model = d_model.ptr;
@@ -670,9 +697,9 @@ struct MRTaskRolloutHandle {
                 p.reset_q = d_reset_q.ptr + static_cast<size_t>(o) * model.world.nq;
                 p.reset_v = d_reset_v.ptr + static_cast<size_t>(o) * model.world.nv;
                 p.friction_scale = d_friction.ptr + o;
-                p.actions = actions + item0 * na;
-                p.reset_masks = masks ? masks + item0 : nullptr;
-                p.observations = obs ? obs + item0 * nobs : nullptr;
+                p.actions = tasked ? d_task_targets.ptr + static_cast<size_t>(o) * na : actions + item0 * na;
+                p.reset_masks = tasked ? d_task_masks.ptr + item0 : (masks ? masks + item0 : nullptr);
+                p.observations = obs && !tasked ? obs + item0 * nobs : nullptr;
                 p.status_codes = status ? status + item0 : nullptr;
                 p.active_contacts = contacts ? contacts + item0 : nullptr;
                 p.stats = d_stats.ptr;
@@ -689,6 +716,8 @@ struct MRTaskRolloutHandle {
                 if (audit)
                     check(numi::launch_audit_step(p, step_layout(), precision != MR_PRECISION_FP32, step_warps_per_block(), cs),
                           "audit launch");
+                if (tasked)
+                    check(numi::launch_task_complete(task_params(k, o, n, actions, masks, obs, status), cs), "task complete launch");
                 if (host_obs && obs) copy_observation_rows(k, o, n, obs, host_obs, cs, c);
             }
             if (driven && evaluate_final) enqueue_policy(steps, o, n, nullptr, false, cs);
@@ -742,6 +771,65 @@ struct MRTaskRolloutHandle {
         last_policy_steps = steps;
     }
 
+    // Values per environment in an observation row: the task's actor frame,
+    // else [q, v].
+    std::uint32_t observation_count() const {
+        return task ? static_cast<std::uint32_t>(task->prog.nobs) : model.world.nq + model.world.nv;
+    }
+
+    // Task-layer launch over environments [o, o + n) of control step k.
+    numi::TaskParams task_params(std::uint32_t k, std::uint32_t o, std::uint32_t n, const float* actions, const std::uint32_t* masks,
+                                 float* obs, const std::uint32_t* status) {
+        const numi::TaskProgramDevice& P = task->prog;
+        const size_t item0 = static_cast<size_t>(k) * envs + o;
+        numi::TaskParams t{};
+        t.prog = P;
+        t.state = d_task_state.ptr + o;
+        t.action_history = d_task_history.ptr + static_cast<size_t>(o) * P.history * P.na;
+        t.previous_joint = d_task_previous.ptr + static_cast<size_t>(o) * 2 * P.na;
+        t.frame = d_task_frame.ptr + static_cast<size_t>(o) * P.nobs;
+        t.reset_q = d_reset_q.ptr + static_cast<size_t>(o) * P.nq;
+        t.reset_v = d_reset_v.ptr + static_cast<size_t>(o) * P.nv;
+        t.q = d_q.ptr + static_cast<size_t>(o) * P.nq;
+        t.v = d_v.ptr + static_cast<size_t>(o) * P.nv;
+        t.masks_in = masks ? masks + item0 : nullptr;
+        t.masks_out = d_task_masks.ptr + item0;
+        t.observations = obs ? obs + item0 * P.nobs : nullptr;
+        t.actions = actions ? actions + item0 * P.na : nullptr;
+        t.targets = d_task_targets.ptr + static_cast<size_t>(o) * P.na;
+        t.status = status + item0;
+        t.transitions = d_transitions.ptr + item0;
+        t.policy_revision = policy ? policy->revision : 0u;
+        t.env_count = static_cast<int>(n);
+        t.env_base = static_cast<int>(o);
+        return t;
+    }
+
+    // Every environment starts a new episode at the next advance.
+    void clear_task_state() {
+        check(cudaMemsetAsync(d_task_state.ptr, 0, d_task_state.count * sizeof(numi::TaskEnvState), stream), "clear task state");
+        check(cudaStreamSynchronize(stream), "clear task state");
+        transition_steps = 0;
+        have_host_transitions = false;
+    }
+
+    void drop_all_graphs() {
+        check(cudaStreamSynchronize(stream), "sync");
+        for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+        graphs.clear();
+    }
+
+    // Sizes the task layer's per-advance buffers (reset masks, transitions).
+    void prepare_task(std::uint32_t steps) {
+        transition_steps = 0;
+        have_host_transitions = false;
+        if (!task) return;
+        const size_t cells = static_cast<size_t>(steps) * envs;
+        d_task_masks.resize(cells);
+        d_transitions.resize(cells);
+        transition_steps = steps;
+    }
+
     // Policy evaluation before control step k (k == steps: the final state,
     // values into the bootstrap slot) writing step k's actions.
     bool evaluate_final = false;
@@ -752,6 +840,8 @@ struct MRTaskRolloutHandle {
         pp.nv = static_cast<int>(model.world.nv);
         pp.q = d_q.ptr + static_cast<size_t>(o) * pp.nq;
         pp.v = d_v.ptr + static_cast<size_t>(o) * pp.nv;
+        pp.frame = task ? d_task_frame.ptr + static_cast<size_t>(o) * task->prog.nobs : nullptr;
+        pp.frame_count = task ? task->prog.nobs : 0;
         pp.envs = static_cast<int>(n);
         pp.env_base = static_cast<int>(o);
         pp.na = static_cast<int>(model.world.action_count);
@@ -773,7 +863,7 @@ struct MRTaskRolloutHandle {
     // Chain `chain` copies on its own copy stream.
     void copy_observation_rows(std::uint32_t k, std::uint32_t o, std::uint32_t n, const float* obs, float* host_obs, cudaStream_t s,
                                int chain = 0) {
-        const size_t nobs = model.world.nq + model.world.nv;
+        const size_t nobs = observation_count();
         const size_t at = (static_cast<size_t>(k) * envs + o) * nobs;
         cudaStream_t cs = chain == 0 ? copy_stream : chain_copy_stream[chain];
         check(cudaEventRecord(ev_step, s), "event");
@@ -794,9 +884,12 @@ struct MRTaskRolloutHandle {
     void run(std::uint32_t steps, const float* actions, const std::uint32_t* masks, float* obs, std::uint32_t* status,
              std::uint32_t* contacts, cudaStream_t s, float* host_obs = nullptr) {
         const bool driven = policy != nullptr;
+        const bool tasked = task != nullptr;
         const GraphKey key{steps, actions, masks, obs, status, contacts, precision, host_obs,
                            driven ? static_cast<const void*>(policy->arena.ptr) : nullptr, driven && evaluate_final,
-                           driven ? d_latents.ptr : nullptr, driven ? d_log_prob.ptr : nullptr, driven ? d_values.ptr : nullptr};
+                           driven ? d_latents.ptr : nullptr, driven ? d_log_prob.ptr : nullptr, driven ? d_values.ptr : nullptr,
+                           tasked ? static_cast<const void*>(task->arena.ptr) : nullptr, tasked ? d_task_masks.ptr : nullptr,
+                           tasked ? d_transitions.ptr : nullptr};
         auto it = graphs.find(key);
         if (it == graphs.end()) {
             cudaGraph_t graph = nullptr;
@@ -1039,6 +1132,12 @@ MR_API int mr_task_rollout_reset(MRTaskRolloutHandle* handle, uint64_t seed) {
         handle->sample_resets();
         handle->last_steps = 0;
         handle->have_final_q = false;
+        if (handle->task) {
+            // Every environment starts a new episode under the new seed's draws.
+            handle->task->prog.seed = seed;
+            handle->clear_task_state();
+            handle->drop_all_graphs();
+        }
     });
 }
 
@@ -1057,7 +1156,7 @@ namespace {
 std::unique_ptr<InstalledPolicy> compile_policy(const MRTaskRolloutHandle& h, const MRPolicyPackC& pk) {
     using numi::kPolicyMaxLayers;
     using numi::kPolicyMaxWidth;
-    const std::uint32_t nobs = h.model.world.nq + h.model.world.nv, na = h.model.world.action_count;
+    const std::uint32_t nobs = h.observation_count(), na = h.model.world.action_count;
     if (!pk.id || !pk.id[0] || !pk.layers || pk.layer_count == 0)
         throw std::invalid_argument("policy identity and dense layers are required");
     if (pk.revision == 0) throw std::invalid_argument("policy revision must be non-zero (zero means no policy)");
@@ -1171,10 +1270,221 @@ std::unique_ptr<InstalledPolicy> compile_policy(const MRTaskRolloutHandle& h, co
     return out;
 }
 
-void drop_graphs(MRTaskRolloutHandle& h) {
-    check(cudaStreamSynchronize(h.stream), "sync");
-    for (auto& kv : h.graphs) cudaGraphExecDestroy(kv.second);
-    h.graphs.clear();
+void drop_graphs(MRTaskRolloutHandle& h) { h.drop_all_graphs(); }
+
+bool finite_value(float x) { return std::isfinite(x); }
+
+// Validates a task program against the rollout's world (the operator subset
+// of include/numi_b200.h, every index in range) and uploads its tables as one
+// device arena.
+std::unique_ptr<InstalledTask> compile_task(const MRTaskRolloutHandle& h, const MRTaskProgramC& t) {
+    using std::to_string;
+    const numi::DeviceModel& M = h.dmodel;
+    const std::uint32_t nq = h.model.world.nq, nv = h.model.world.nv, na = h.model.world.action_count;
+    auto need = [](bool ok, const std::string& what) {
+        if (!ok) throw std::invalid_argument("task program: " + what);
+    };
+    need(na > 0 && na <= static_cast<std::uint32_t>(numi::kTaskMaxActions), "the world must take 1-64 actions");
+    need(t.actions != nullptr && t.action_count == na, "action_count must equal the world's " + to_string(na) + " actions");
+    need(t.actor != nullptr && t.actor_count > 0 && t.actor_count <= static_cast<std::uint32_t>(numi::kTaskMaxObservations),
+         "1-256 actor observation operators are required");
+    need(t.default_q != nullptr && t.default_q_count == nq, "default_q must hold nq = " + to_string(nq) + " values");
+    for (std::uint32_t i = 0; i < nq; ++i) need(finite_value(t.default_q[i]), "default_q must be finite");
+    need(t.action_history >= 3 && t.action_history <= static_cast<std::uint32_t>(numi::kTaskMaxHistory), "action_history must be 3-8");
+    need(t.maximum_episode_steps >= 1, "maximum_episode_steps must be positive");
+    need(finite_value(t.gait_period_seconds) && t.gait_period_seconds > 0.0f, "gait_period_seconds must be positive");
+    need(finite_value(t.command_duration_seconds[0]) && finite_value(t.command_duration_seconds[1]) &&
+             t.command_duration_seconds[0] > 0.0f && t.command_duration_seconds[0] <= t.command_duration_seconds[1],
+         "command durations must satisfy 0 < minimum <= maximum");
+    need(finite_value(t.standing_probability) && t.standing_probability >= 0.0f && t.standing_probability <= 1.0f,
+         "standing_probability must lie in [0, 1]");
+    need(finite_value(t.base_height_target), "base_height_target must be finite");
+    for (int k = 0; k < 3; ++k) {
+        need(finite_value(t.command_lower[k]) && finite_value(t.command_upper[k]) && t.command_lower[k] <= t.command_upper[k],
+             "command bounds must be finite with lower <= upper");
+        need(finite_value(t.root_reference[k]), "root_reference must be finite");
+    }
+    for (std::uint32_t a = 0; a < na; ++a) {
+        const MRTaskActionBindingC& b = t.actions[a];
+        const std::string where = "action " + to_string(a);
+        need(b.dof_index == static_cast<std::uint32_t>(M.action_dof[a]), where + " must bind DoF " + to_string(M.action_dof[a]) +
+                                                                             ", the DoF the world drives from it");
+        need(b.v_index == b.dof_index && M.dof_q[b.dof_index] >= 0 && b.q_index == static_cast<std::uint32_t>(M.dof_q[b.dof_index]),
+             where + ": q_index and v_index must be the DoF's coordinate and velocity");
+        need(finite_value(b.scale) && finite_value(b.lower_target) && finite_value(b.upper_target) && b.lower_target <= b.upper_target,
+             where + ": scale and target bounds must be finite with lower <= upper");
+        need(finite_value(b.response_time_seconds) && b.response_time_seconds >= 0.0f, where + ": response time must be >= 0");
+    }
+    for (std::uint32_t i = 0; i < t.actor_count; ++i) {
+        const MRTaskObservationOperatorC& o = t.actor[i];
+        const std::string where = "actor operator " + to_string(i);
+        need(finite_value(o.transform_scale) && finite_value(o.transform_offset) && finite_value(o.noise_amplitude) &&
+                 o.noise_amplitude >= 0.0f, where + ": transform and noise must be finite");
+        need((o.flags & ~static_cast<std::uint32_t>(MR_TASK_OBSERVATION_NORMALIZE_VECTOR3)) == 0u &&
+                 (o.flags == 0u || o.opcode == MR_TASK_OBSERVE_PROJECTED_GRAVITY), where + ": only projected gravity may be normalised");
+        switch (o.opcode) {
+        case MR_TASK_OBSERVE_ROOT_ANGULAR_VELOCITY_LOCAL:
+        case MR_TASK_OBSERVE_PROJECTED_GRAVITY:
+        case MR_TASK_OBSERVE_ROOT_LINEAR_VELOCITY_LOCAL:
+            need(o.component < 3u, where + ": component must be 0-2");
+            break;
+        case MR_TASK_OBSERVE_COMMAND:
+            need(o.component < 4u, where + ": component must be 0-3");
+            break;
+        case MR_TASK_OBSERVE_GAIT_PHASE:
+            need(o.component < 2u, where + ": component must be 0-1");
+            break;
+        case MR_TASK_OBSERVE_ROOT_HEIGHT:
+            break;
+        case MR_TASK_OBSERVE_JOINT_POSITION_ERROR:
+        case MR_TASK_OBSERVE_JOINT_VELOCITY:
+        case MR_TASK_OBSERVE_PREVIOUS_ACTION:
+        case MR_TASK_OBSERVE_JOINT_FINITE_DIFFERENCE_VELOCITY:
+            need(o.source < na, where + ": source must be an action index");
+            break;
+        case MR_TASK_OBSERVE_DELAYED_ACTION:
+            need(o.source < na && o.component <= t.action_history - 2, where + ": source must be an action index and component at most "
+                                                                               "action_history - 2");
+            break;
+        default:
+            need(false, where + ": opcode " + to_string(o.opcode) + " is outside the evaluated subset");
+        }
+    }
+    need(t.joint_group_count == 0 || t.joint_groups != nullptr, "joint_groups is null");
+    need(t.joint_member_count == 0 || t.joint_members != nullptr, "joint_members is null");
+    for (std::uint32_t g = 0; g < t.joint_group_count; ++g) {
+        const MRTaskIndexGroupC& G = t.joint_groups[g];
+        need(static_cast<std::uint64_t>(G.first) + G.count <= t.joint_member_count, "joint group " + to_string(g) + " overruns joint_members");
+    }
+    for (std::uint32_t m = 0; m < t.joint_member_count; ++m) need(t.joint_members[m] < na, "joint members must be action indices");
+    need(t.reward_count == 0 || t.rewards != nullptr, "rewards is null");
+    for (std::uint32_t i = 0; i < t.reward_count; ++i) {
+        const MRTaskRewardOperatorC& r = t.rewards[i];
+        const std::string where = "reward operator " + to_string(i);
+        need(finite_value(r.weight) && finite_value(r.parameters[0]) && finite_value(r.parameters[1]) && finite_value(r.parameters[2]),
+             where + ": weight and parameters must be finite");
+        switch (r.opcode) {
+        case MR_TASK_REWARD_JOINT_GROUP_POSTURE_SQUARED:
+        case MR_TASK_REWARD_JOINT_GROUP_POSTURE_ABSOLUTE:
+            need(r.group < t.joint_group_count, where + ": group must be a joint group index");
+            break;
+        case MR_TASK_REWARD_LINEAR_VELOCITY_TRACKING:
+        case MR_TASK_REWARD_YAW_VELOCITY_TRACKING:
+        case MR_TASK_REWARD_CONSTANT:
+        case MR_TASK_REWARD_ROOT_VERTICAL_VELOCITY_SQUARED:
+        case MR_TASK_REWARD_ROOT_ROLL_PITCH_VELOCITY_SQUARED:
+        case MR_TASK_REWARD_TILT_SQUARED:
+        case MR_TASK_REWARD_ROOT_HEIGHT_ERROR_SQUARED:
+        case MR_TASK_REWARD_JOINT_VELOCITY_SQUARED:
+        case MR_TASK_REWARD_JOINT_ACCELERATION_SQUARED:
+        case MR_TASK_REWARD_ACTION_RATE_SQUARED:
+        case MR_TASK_REWARD_JOINT_LIMIT_VIOLATION_SQUARED:
+        case MR_TASK_REWARD_PROJECTED_GRAVITY_HORIZONTAL_SQUARED:
+        case MR_TASK_REWARD_JOINT_LIMIT_VIOLATION_ABSOLUTE:
+        case MR_TASK_REWARD_ROOT_HEIGHT_NORMALIZED:
+        case MR_TASK_REWARD_ROOT_HEIGHT_PROGRESS:
+        case MR_TASK_REWARD_UPRIGHTNESS:
+            break;
+        default:
+            need(false, where + ": opcode " + to_string(r.opcode) + " is outside the evaluated subset");
+        }
+    }
+    const bool terminations = h.config.disable_task_terminations == 0u;  // the reference clears them (c_api.cpp:1415-1417)
+    need(t.termination_count == 0 || t.terminations != nullptr, "terminations is null");
+    for (std::uint32_t i = 0; i < t.termination_count; ++i) {
+        const MRTaskTerminationOperatorC& o = t.terminations[i];
+        need(o.opcode == MR_TASK_TERMINATE_MINIMUM_ROOT_HEIGHT || o.opcode == MR_TASK_TERMINATE_MAXIMUM_TILT,
+             "termination operator " + to_string(i) + ": opcode " + to_string(o.opcode) + " is outside the evaluated subset");
+        need(finite_value(o.threshold) && finite_value(o.failure_penalty), "termination operator " + to_string(i) + " must be finite");
+    }
+    need(t.randomization_count == 0 || t.randomization != nullptr, "randomization is null");
+    for (std::uint32_t i = 0; i < t.randomization_count; ++i) {
+        const MRTaskRandomizationOperatorC& o = t.randomization[i];
+        const std::string where = "randomization operator " + to_string(i);
+        for (int k = 0; k < 4; ++k) need(finite_value(o.parameters[k]), where + ": parameters must be finite");
+        switch (o.opcode) {
+        case MR_TASK_RANDOMIZE_ROOT_POSITION:
+        case MR_TASK_RANDOMIZE_ROOT_YAW:
+        case MR_TASK_RANDOMIZE_ROOT_HEIGHT:
+            need(M.floating != 0, where + ": root operators need a floating root");
+            break;
+        case MR_TASK_RANDOMIZE_JOINT_POSITION:
+            need(o.target < nq, where + ": target must be a q index");
+            break;
+        case MR_TASK_RANDOMIZE_ACTION_POSITION:
+        case MR_TASK_RANDOMIZE_VELOCITY:
+        case MR_TASK_RANDOMIZE_ACTION_VELOCITY:
+            break;
+        default:
+            need(false, where + ": opcode " + to_string(o.opcode) + " is outside the evaluated subset");
+        }
+    }
+
+    // One arena, every table 16-byte aligned.
+    std::vector<unsigned char> arena;
+    auto put = [&arena](const void* src, size_t bytes) {
+        const size_t at = (arena.size() + 15) & ~static_cast<size_t>(15);
+        arena.resize(at + bytes);
+        if (bytes) std::memcpy(arena.data() + at, src, bytes);
+        return at;
+    };
+    std::vector<float> lower(na), upper(na);
+    for (std::uint32_t a = 0; a < na; ++a) {
+        lower[a] = M.q_lower[t.actions[a].dof_index];
+        upper[a] = M.q_upper[t.actions[a].dof_index];
+    }
+    const std::uint32_t nterm = terminations ? t.termination_count : 0u;
+    const size_t at_actions = put(t.actions, na * sizeof(MRTaskActionBindingC));
+    const size_t at_actor = put(t.actor, t.actor_count * sizeof(MRTaskObservationOperatorC));
+    const size_t at_rewards = put(t.rewards, t.reward_count * sizeof(MRTaskRewardOperatorC));
+    const size_t at_terms = put(t.terminations, nterm * sizeof(MRTaskTerminationOperatorC));
+    const size_t at_random = put(t.randomization, t.randomization_count * sizeof(MRTaskRandomizationOperatorC));
+    const size_t at_groups = put(t.joint_groups, t.joint_group_count * sizeof(MRTaskIndexGroupC));
+    const size_t at_members = put(t.joint_members, t.joint_member_count * sizeof(std::uint32_t));
+    const size_t at_default = put(t.default_q, nq * sizeof(float));
+    const size_t at_lower = put(lower.data(), na * sizeof(float));
+    const size_t at_upper = put(upper.data(), na * sizeof(float));
+    auto out = std::make_unique<InstalledTask>();
+    out->arena.resize(arena.size());
+    check(cudaMemcpy(out->arena.ptr, arena.data(), arena.size(), cudaMemcpyHostToDevice), "task upload");
+    const unsigned char* base = out->arena.ptr;
+    numi::TaskProgramDevice& P = out->prog;
+    P.actions = reinterpret_cast<const MRTaskActionBindingC*>(base + at_actions);
+    P.actor = reinterpret_cast<const MRTaskObservationOperatorC*>(base + at_actor);
+    P.rewards = reinterpret_cast<const MRTaskRewardOperatorC*>(base + at_rewards);
+    P.terminations = reinterpret_cast<const MRTaskTerminationOperatorC*>(base + at_terms);
+    P.randomization = reinterpret_cast<const MRTaskRandomizationOperatorC*>(base + at_random);
+    P.groups = reinterpret_cast<const MRTaskIndexGroupC*>(base + at_groups);
+    P.members = reinterpret_cast<const std::uint32_t*>(base + at_members);
+    P.default_q = reinterpret_cast<const float*>(base + at_default);
+    P.limit_lower = reinterpret_cast<const float*>(base + at_lower);
+    P.limit_upper = reinterpret_cast<const float*>(base + at_upper);
+    P.na = static_cast<int>(na);
+    P.nobs = static_cast<int>(t.actor_count);
+    P.nrewards = static_cast<int>(t.reward_count);
+    P.nterminations = static_cast<int>(nterm);
+    P.nrandom = static_cast<int>(t.randomization_count);
+    P.ngroups = static_cast<int>(t.joint_group_count);
+    P.history = static_cast<int>(t.action_history);
+    P.delay = static_cast<int>(std::min<std::uint32_t>(t.action_delay_steps, t.action_history - 2));
+    P.max_episode_steps = static_cast<int>(t.maximum_episode_steps);
+    P.nq = static_cast<int>(nq);
+    P.nv = static_cast<int>(nv);
+    P.fixed_root = M.floating ? 0 : 1;
+    P.dt = h.config.control_timestep_seconds;
+    P.base_height = t.base_height_target;
+    P.gait_period = t.gait_period_seconds;
+    P.standing_probability = t.standing_probability;
+    P.duration_min = t.command_duration_seconds[0];
+    P.duration_max = t.command_duration_seconds[1];
+    for (int k = 0; k < 3; ++k) {
+        P.root_reference[k] = t.root_reference[k];
+        P.command_lower[k] = t.command_lower[k];
+        P.command_upper[k] = t.command_upper[k];
+    }
+    P.seed = h.seed;
+    out->fingerprint = t.task_fingerprint;
+    return out;
 }
 
 }  // namespace
@@ -1224,6 +1534,86 @@ MR_API int mr_task_rollout_clear_policy(MRTaskRolloutHandle* handle) {
         drop_graphs(*handle);
         handle->policy.reset();
         handle->have_policy_outputs = false;
+    });
+}
+
+MR_API int mr_task_rollout_set_task(MRTaskRolloutHandle* handle, const MRTaskProgramC* program) {
+    return guarded([&] {
+        if (!handle) throw std::invalid_argument("handle is null");
+        if (!program) throw std::invalid_argument("task program is null");
+        MRTaskRolloutHandle& h = *handle;
+        if (h.scene) throw std::invalid_argument("pile and stack worlds take no actions; a task cannot drive them");
+        std::unique_ptr<InstalledTask> compiled = compile_task(h, *program);
+        if (h.policy) {
+            const int in = h.policy->params.actor[0].in;
+            if (in != compiled->prog.nobs)
+                throw std::invalid_argument("the installed policy takes " + std::to_string(in) + " observations; the task's actor frame has " +
+                                            std::to_string(compiled->prog.nobs) + " (clear the policy first)");
+        }
+        drop_graphs(h);
+        const numi::TaskProgramDevice& P = compiled->prog;
+        h.d_task_state.resize(h.envs);
+        h.d_task_history.resize(static_cast<size_t>(h.envs) * P.history * P.na);
+        h.d_task_previous.resize(static_cast<size_t>(h.envs) * 2 * P.na);
+        h.d_task_frame.resize(static_cast<size_t>(h.envs) * P.nobs);
+        h.d_task_targets.resize(static_cast<size_t>(h.envs) * P.na);
+        check(cudaMemsetAsync(h.d_task_history.ptr, 0, h.d_task_history.count * sizeof(float), h.stream), "clear task history");
+        check(cudaMemsetAsync(h.d_task_previous.ptr, 0, h.d_task_previous.count * sizeof(float), h.stream), "clear task history");
+        h.task = std::move(compiled);
+        h.clear_task_state();
+        h.stats_layout.actor_observation_count = static_cast<std::uint32_t>(P.nobs);
+        h.stats_layout.critic_observation_count = static_cast<std::uint32_t>(P.nobs);
+        h.stats_layout.maximum_episode_steps = static_cast<std::uint32_t>(P.max_episode_steps);
+        h.stats_layout.task_fingerprint = h.task->fingerprint;
+        h.last_steps = 0;
+        h.have_final_q = false;
+    });
+}
+
+MR_API int mr_task_rollout_clear_task(MRTaskRolloutHandle* handle) {
+    return guarded([&] {
+        if (!handle) throw std::invalid_argument("handle is null");
+        MRTaskRolloutHandle& h = *handle;
+        if (!h.task) return;
+        if (h.policy && h.policy->params.actor[0].in != static_cast<int>(h.model.world.nq + h.model.world.nv))
+            throw std::invalid_argument("the installed policy reads the task's actor frame; clear the policy first");
+        drop_graphs(h);
+        h.task.reset();
+        h.transition_steps = 0;
+        h.have_host_transitions = false;
+        // The sampled reset states come back (the task wrote its own).
+        check(cudaMemcpyAsync(h.d_reset_q.ptr, h.reset_q.data(), h.reset_q.size() * sizeof(float), cudaMemcpyHostToDevice, h.stream),
+              "upload reset q");
+        check(cudaMemcpyAsync(h.d_reset_v.ptr, h.reset_v.data(), h.reset_v.size() * sizeof(float), cudaMemcpyHostToDevice, h.stream),
+              "upload reset v");
+        check(cudaStreamSynchronize(h.stream), "clear task");
+        h.stats_layout.actor_observation_count = h.model.world.nq + h.model.world.nv;
+        h.stats_layout.critic_observation_count = h.model.world.nq + h.model.world.nv;
+        h.stats_layout.maximum_episode_steps = 0;
+        h.stats_layout.task_fingerprint = 0;
+        h.last_steps = 0;
+        h.have_final_q = false;
+    });
+}
+
+MR_API const MRTaskTransitionC* mr_task_rollout_transitions(const MRTaskRolloutHandle* handle) {
+    return handle && handle->have_host_transitions ? handle->h_transitions.ptr : nullptr;
+}
+
+MR_API uint64_t mr_task_rollout_device_transitions(const MRTaskRolloutHandle* handle) {
+    return handle && handle->task && handle->transition_steps ? reinterpret_cast<uint64_t>(handle->d_transitions.ptr) : 0u;
+}
+
+MR_API int mr_task_rollout_copy_transitions(const MRTaskRolloutHandle* handle, MRTaskTransitionC* output, size_t count) {
+    return guarded([&] {
+        if (!handle) throw std::invalid_argument("handle is null");
+        const MRTaskRolloutHandle& h = *handle;
+        if (!h.task || h.transition_steps == 0) throw std::invalid_argument("no transitions: install a task and advance first");
+        if (count > static_cast<size_t>(h.transition_steps) * h.envs)
+            throw std::invalid_argument("count exceeds the last advance's steps x environments");
+        if (count != 0 && !output) throw std::invalid_argument("output is null");
+        check(cudaStreamSynchronize(h.stream), "transitions");
+        if (count) check(cudaMemcpy(output, h.d_transitions.ptr, count * sizeof(MRTaskTransitionC), cudaMemcpyDeviceToHost), "transitions D2H");
     });
 }
 
@@ -1309,7 +1699,8 @@ MR_API int mr_task_rollout_advance(MRTaskRolloutHandle* handle, const float* nor
         h.d_actions.resize(expected);
         const bool masks = reset_mask_count != 0;
         if (masks) h.d_masks.resize(mask_expected);
-        const size_t nobs = h.model.world.nq + h.model.world.nv;
+        const size_t nobs = h.observation_count();
+        h.prepare_task(control_step_count);
         h.d_status.resize(mask_expected);
         h.d_contacts.resize(mask_expected);
         h.h_status.resize(mask_expected);
@@ -1331,6 +1722,11 @@ MR_API int mr_task_rollout_advance(MRTaskRolloutHandle* handle, const float* nor
         check(cudaMemcpyAsync(h.h_contacts.ptr, h.d_contacts.ptr, mask_expected * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "contacts D2H");
         check(cudaMemcpyAsync(h.h_stats.ptr, h.d_stats.ptr, numi::kStatCount * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "stats D2H");
         h.read_policy_outputs(control_step_count, s);
+        if (h.task) {
+            h.h_transitions.resize(mask_expected);
+            check(cudaMemcpyAsync(h.h_transitions.ptr, h.d_transitions.ptr, mask_expected * sizeof(MRTaskTransitionC),
+                                  cudaMemcpyDeviceToHost, s), "transitions D2H");
+        }
         if (h.readback) {
             check(cudaMemcpyAsync(h.h_final_q.ptr, h.d_q.ptr, static_cast<size_t>(h.envs) * h.model.world.nq * sizeof(float),
                                   cudaMemcpyDeviceToHost, s), "final q D2H");
@@ -1342,6 +1738,7 @@ MR_API int mr_task_rollout_advance(MRTaskRolloutHandle* handle, const float* nor
         const double wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count();
         h.last_steps = control_step_count;
         h.have_final_q = h.readback;
+        h.have_host_transitions = h.task != nullptr;
         h.fill_advance(control_step_count, h.h_status.ptr, h.h_stats.ptr, advance, gpu_ms, wall_ms);
         // The reference reports failed environments in the counters and also
         // as an error return (src/c_api.cpp:3983-3988).
@@ -1375,6 +1772,7 @@ MR_API int mr_task_rollout_advance_device(MRTaskRolloutHandle* handle, const flo
         check(cudaEventRecord(h.ev_in, caller), "event");
         check(cudaStreamWaitEvent(s, h.ev_in, 0), "stream wait");
         const size_t cells = static_cast<size_t>(control_step_count) * h.envs;
+        h.prepare_task(control_step_count);
         std::uint32_t* status = device_status_codes;
         if (!status) {
             h.d_status.resize(cells);
@@ -1967,6 +2365,7 @@ MR_API MRBatchHandle* mr_create_batch(MRTaskRolloutHandle* const* rollouts, size
             if (h->precision != MR_PRECISION_FP32) throw std::invalid_argument("batched rollouts run in FP32 precision only");
             if (h->quality) throw std::invalid_argument("batched rollouts run the temporalCone solver only");
             if (h->policy) throw std::invalid_argument("batched rollouts take their actions from the caller (no native policy)");
+            if (h->task) throw std::invalid_argument("batched rollouts step raw drive targets (no task program)");
             if (h->scene && h->smodel.support_mapped) b->convex = true;
             if (h->envs > numi::kMixEnvMask) throw std::invalid_argument("a batched rollout holds at most 2^24 - 1 environments");
             for (size_t j = 0; j < i; ++j)

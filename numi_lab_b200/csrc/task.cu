@@ -1,0 +1,611 @@
+// The task layer's three kernels around each control step, one warp per
+// environment for observe and complete, one thread per (environment,
+// action) for apply.  They restate, for the operator subset of
+// include/numi_b200.h, src/metal/LocomotionTask.metal:
+//   observe   :2184-3440  reset draw (:2330-3120), actor frame (:1190-1330)
+//   apply     :3442-3674  delay line, first-order response, target clamp
+//   complete  :3904-6745  reward operators (:4700-6060), terminations
+//                         (:6064-6160), command schedule (:6388-6420),
+//                         next actor frame and joint history (:6478-6630)
+// All arithmetic is FP32 like the reference's shaders; draws use the
+// reference's keyed SplitMix64 counter hash (randomUnit, :121-152).
+#include "task.h"
+
+#include <cmath>
+
+namespace numi {
+namespace {
+
+constexpr float kTwoPi = 6.28318530717958647692f;
+constexpr int kTaskWarps = 4;  // environments per CTA
+constexpr int kApplyThreads = 256;
+
+// SplitMix64's finaliser over a key built from the draw's coordinates.
+__device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
+    x += 0x9e3779b97f4a7c15ull;
+    x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+    x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+    return x ^ (x >> 31);
+}
+
+__device__ __forceinline__ float unit_draw(unsigned long long seed, unsigned env, unsigned episode, unsigned step, unsigned channel) {
+    unsigned long long key = seed;
+    key ^= static_cast<unsigned long long>(env + 1u) * 0xd2b74407b1ce6e93ull;
+    key ^= static_cast<unsigned long long>(episode + 1u) * 0xca5a826395121157ull;
+    key ^= static_cast<unsigned long long>(step + 1u) * 0x9e3779b185ebca87ull;
+    key ^= static_cast<unsigned long long>(channel + 1u) * 0x94d049bb133111ebull;
+    return static_cast<float>(static_cast<unsigned>(mix64(key) >> 40)) * (1.0f / 16777216.0f);
+}
+
+__device__ __forceinline__ float signed_draw(unsigned long long seed, unsigned env, unsigned episode, unsigned step, unsigned channel) {
+    return 2.0f * unit_draw(seed, env, episode, step, channel) - 1.0f;
+}
+
+__device__ __forceinline__ float range_draw(unsigned long long seed, unsigned env, unsigned episode, unsigned step, unsigned channel,
+                                            float lower, float upper) {
+    return lower + (upper - lower) * unit_draw(seed, env, episode, step, channel);
+}
+
+__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 operator*(float s, float3 a) { return make_float3(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 cross3(float3 a, float3 b) {
+    return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float lane3(float3 a, unsigned i) { return i == 0u ? a.x : (i == 1u ? a.y : a.z); }
+
+__device__ __forceinline__ float3 rotate(float4 q, float3 v) {
+    const float3 u = make_float3(q.x, q.y, q.z);
+    const float3 t = 2.0f * cross3(u, v);
+    return v + q.w * t + cross3(u, t);
+}
+
+__device__ __forceinline__ float3 rotate_inverse(float4 q, float3 v) {
+    const float3 u = make_float3(q.x, q.y, q.z);
+    const float3 t = 2.0f * cross3(u, v);
+    return v - q.w * t + cross3(u, t);
+}
+
+__device__ __forceinline__ float4 quat_product(float4 a, float4 b) {
+    return make_float4(a.w * b.x + a.x * b.w + a.y * b.z - a.z * b.y, a.w * b.y - a.x * b.z + a.y * b.w + a.z * b.x,
+                       a.w * b.z + a.x * b.y - a.y * b.x + a.z * b.w, a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z);
+}
+
+__device__ __forceinline__ float3 normalized_or(float3 v, float3 fallback) {
+    const float l2 = dot3(v, v);
+    return l2 > 1.0e-12f && isfinite(l2) ? rsqrtf(l2) * v : fallback;
+}
+
+__device__ __forceinline__ float mixf(float x, float y, float a) { return x + (y - x) * a; }
+
+__device__ __forceinline__ float warp_sum(float x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+// Root link frame of the selected articulation (LocomotionTask.metal:396-478).
+struct Root {
+    float4 orientation;
+    float3 position;
+    float3 linear;   // world linear velocity of the link origin
+    float3 angular;  // world angular velocity
+};
+
+__device__ __forceinline__ Root root_frame(const TaskProgramDevice& P, const float* q, const float* v) {
+    Root r;
+    if (P.fixed_root) {
+        r.orientation = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+        r.position = r.linear = r.angular = make_float3(0.0f, 0.0f, 0.0f);
+        return r;
+    }
+    r.orientation = make_float4(q[3], q[4], q[5], q[6]);
+    const float3 offset = rotate(r.orientation, make_float3(P.root_reference[0], P.root_reference[1], P.root_reference[2]));
+    r.position = make_float3(q[0], q[1], q[2]) + offset;
+    r.angular = make_float3(v[3], v[4], v[5]);
+    r.linear = make_float3(v[0], v[1], v[2]) + cross3(r.angular, offset);
+    return r;
+}
+
+__device__ __forceinline__ float3 projected_gravity(const Root& r) {
+    const float3 down = make_float3(0.0f, 0.0f, -1.0f);
+    return normalized_or(rotate_inverse(r.orientation, down), down);
+}
+
+// One operator's clean value (cleanObservation, :594-1188, the subset):
+// transform applied, no noise.  `raw` points at the delay line's newest raw
+// slot; `previous_q` at the joint positions of the last step's end.
+__device__ float clean_observation(const TaskProgramDevice& P, const MRTaskObservationOperatorC& op, const Root& r, const float* q,
+                                   const float* v, const TaskEnvState& st, const float* raw, const float* previous_q) {
+    float value = 0.0f;
+    const unsigned c = op.component;
+    switch (op.opcode) {
+    case MR_TASK_OBSERVE_ROOT_ANGULAR_VELOCITY_LOCAL:
+        value = lane3(rotate_inverse(r.orientation, r.angular), c);
+        break;
+    case MR_TASK_OBSERVE_PROJECTED_GRAVITY:
+        value = lane3(projected_gravity(r), c);
+        break;
+    case MR_TASK_OBSERVE_COMMAND:
+        value = c < 3u ? st.command[c] : 0.0f;  // the command extension lanes stay zero
+        break;
+    case MR_TASK_OBSERVE_JOINT_POSITION_ERROR: {
+        const int qi = static_cast<int>(P.actions[op.source].q_index);
+        value = q[qi] - P.default_q[qi];
+        break;
+    }
+    case MR_TASK_OBSERVE_JOINT_VELOCITY:
+        value = v[P.actions[op.source].v_index];
+        break;
+    case MR_TASK_OBSERVE_JOINT_FINITE_DIFFERENCE_VELOCITY:
+        value = (q[P.actions[op.source].q_index] - previous_q[op.source]) / P.dt;
+        break;
+    case MR_TASK_OBSERVE_PREVIOUS_ACTION:
+        value = raw[op.source];
+        break;
+    case MR_TASK_OBSERVE_DELAYED_ACTION:
+        value = raw[static_cast<int>(op.source) - static_cast<int>(op.component) * P.na];
+        break;
+    case MR_TASK_OBSERVE_ROOT_LINEAR_VELOCITY_LOCAL:
+        value = lane3(rotate_inverse(r.orientation, r.linear), c);
+        break;
+    case MR_TASK_OBSERVE_ROOT_HEIGHT:
+        value = r.position.z;
+        break;
+    case MR_TASK_OBSERVE_GAIT_PHASE: {
+        const float magnitude = sqrtf(st.command[0] * st.command[0] + st.command[1] * st.command[1] + st.command[2] * st.command[2]);
+        if (magnitude >= 0.1f) value = c == 0u ? sinf(st.phase) : cosf(st.phase);
+        break;
+    }
+    default:
+        break;
+    }
+    return op.transform_scale * value + op.transform_offset;
+}
+
+// The actor frame (writeFrame, :1190-1330): lanes over operators.  The
+// gravity operators flagged NORMALIZE_VECTOR3 publish the unit vector of
+// their noisy components.
+__device__ void write_frame(const TaskProgramDevice& P, const float* q, const float* v, const TaskEnvState& st, const float* raw,
+                            const float* previous_q, unsigned env, unsigned episode, unsigned step, float* frame, int lane) {
+    const Root r = root_frame(P, q, v);
+    float3 g = make_float3(0.0f, 0.0f, -1.0f);
+    bool have = false;
+    for (int i = 0; i < P.nobs; ++i) {
+        const MRTaskObservationOperatorC op = P.actor[i];
+        if (op.opcode != MR_TASK_OBSERVE_PROJECTED_GRAVITY || (op.flags & MR_TASK_OBSERVATION_NORMALIZE_VECTOR3) == 0u) continue;
+        const float value = clean_observation(P, op, r, q, v, st, raw, previous_q) +
+                            op.noise_amplitude * signed_draw(P.seed, env, episode, step, op.noise_channel);
+        if (op.component == 0u) g.x = value;
+        else if (op.component == 1u) g.y = value;
+        else g.z = value;
+        have = true;
+    }
+    if (have) g = normalized_or(g, make_float3(0.0f, 0.0f, -1.0f));
+    for (int i = lane; i < P.nobs; i += 32) {
+        const MRTaskObservationOperatorC op = P.actor[i];
+        if (op.opcode == MR_TASK_OBSERVE_PROJECTED_GRAVITY && (op.flags & MR_TASK_OBSERVATION_NORMALIZE_VECTOR3) != 0u) {
+            frame[i] = lane3(g, op.component);
+            continue;
+        }
+        frame[i] = clean_observation(P, op, r, q, v, st, raw, previous_q) +
+                   op.noise_amplitude * signed_draw(P.seed, env, episode, step, op.noise_channel);
+    }
+}
+
+// durationSteps (:1484-1508).
+__device__ __forceinline__ unsigned duration_steps(const TaskProgramDevice& P, unsigned env, unsigned episode, unsigned step,
+                                                   unsigned channel) {
+    const float seconds = range_draw(P.seed, env, episode, step, channel, P.duration_min, P.duration_max);
+    const float steps = floorf(seconds / P.dt);
+    return steps >= 1.0f ? static_cast<unsigned>(steps) : 1u;
+}
+
+// sampledCommand (:1570-1615) at difficulty band 0.
+__device__ __forceinline__ void sample_command(const TaskProgramDevice& P, unsigned env, unsigned episode, unsigned step, float* out) {
+    for (unsigned k = 0; k < 3u; ++k)
+        out[k] = range_draw(P.seed, env, episode, step, 16u + k, P.command_lower[k], P.command_upper[k]);
+    if (unit_draw(P.seed, env, episode, step, 19u) < P.standing_probability) out[0] = out[1] = out[2] = 0.0f;
+}
+
+__global__ void __launch_bounds__(32 * kTaskWarps) task_observe_kernel(TaskParams p) {
+    const int lane = threadIdx.x & 31;
+    const int local = blockIdx.x * kTaskWarps + (threadIdx.x >> 5);
+    if (local >= p.env_count) return;
+    const TaskProgramDevice& P = p.prog;
+    const unsigned env = static_cast<unsigned>(p.env_base + local);
+    TaskEnvState st = p.state[local];
+    const bool reset = st.initialized == 0u || st.pending_reset != 0u || (p.masks_in != nullptr && p.masks_in[local] != 0u);
+    float* frame = p.frame + static_cast<size_t>(local) * P.nobs;
+    if (reset) {
+        const unsigned episode = st.episode + 1u;
+        float* rq = p.reset_q + static_cast<size_t>(local) * P.nq;
+        float* rv = p.reset_v + static_cast<size_t>(local) * P.nv;
+        for (int i = lane; i < P.nq; i += 32) rq[i] = P.default_q[i];
+        for (int i = lane; i < P.nv; i += 32) rv[i] = 0.0f;
+        __syncwarp();
+        // Randomization operators in order (:2452-2770), channel 2048 + index.
+        for (int k = 0; k < P.nrandom; ++k) {
+            const MRTaskRandomizationOperatorC op = P.randomization[k];
+            const unsigned channel = 2048u + static_cast<unsigned>(k);
+            switch (op.opcode) {
+            case MR_TASK_RANDOMIZE_ROOT_POSITION:
+                if (lane < 3) rq[lane] += op.parameters[lane] * signed_draw(P.seed, env, episode, 0u, channel + lane);
+                break;
+            case MR_TASK_RANDOMIZE_ROOT_YAW:
+                if (lane == 0) {
+                    const float yaw = range_draw(P.seed, env, episode, 0u, channel, op.parameters[0], op.parameters[1]);
+                    const float half = 0.5f * yaw;
+                    const float4 authored = make_float4(P.default_q[3], P.default_q[4], P.default_q[5], P.default_q[6]);
+                    const float4 out = quat_product(make_float4(0.0f, 0.0f, sinf(half), cosf(half)), authored);
+                    rq[3] = out.x;
+                    rq[4] = out.y;
+                    rq[5] = out.z;
+                    rq[6] = out.w;
+                }
+                break;
+            case MR_TASK_RANDOMIZE_ROOT_HEIGHT:
+                if (lane == 0) rq[2] = range_draw(P.seed, env, episode, 0u, channel, op.parameters[0], op.parameters[1]);
+                break;
+            case MR_TASK_RANDOMIZE_JOINT_POSITION:
+                if (lane == 0) rq[op.target] = range_draw(P.seed, env, episode, 0u, channel, op.parameters[0], op.parameters[1]);
+                break;
+            case MR_TASK_RANDOMIZE_ACTION_POSITION:
+                for (int a = lane; a < P.na; a += 32) {
+                    const MRTaskActionBindingC b = P.actions[a];
+                    const float x = P.default_q[b.q_index] +
+                                    range_draw(P.seed, env, episode, 0u, channel + a, op.parameters[0], op.parameters[1]);
+                    rq[b.q_index] = fminf(fmaxf(x, b.lower_target), b.upper_target);
+                }
+                break;
+            case MR_TASK_RANDOMIZE_VELOCITY:
+                for (int i = lane; i < P.nv; i += 32)
+                    rv[i] = range_draw(P.seed, env, episode, 0u, channel + i, op.parameters[0], op.parameters[1]);
+                break;
+            case MR_TASK_RANDOMIZE_ACTION_VELOCITY:
+                for (int a = lane; a < P.na; a += 32)
+                    rv[P.actions[a].v_index] = range_draw(P.seed, env, episode, 0u, channel + a, op.parameters[0], op.parameters[1]);
+                break;
+            default:
+                break;
+            }
+            __syncwarp();
+        }
+        float* hist = p.action_history + static_cast<size_t>(local) * P.history * P.na;
+        float* prev = p.previous_joint + static_cast<size_t>(local) * 2 * P.na;
+        for (int i = lane; i < P.history * P.na; i += 32) hist[i] = 0.0f;
+        for (int a = lane; a < P.na; a += 32) {
+            prev[a] = 0.0f;
+            prev[P.na + a] = rq[P.actions[a].q_index];
+        }
+        // A new episode (:2947-3010).
+        st.episode_step = 0u;
+        st.episode = episode;
+        st.command_steps = duration_steps(P, env, episode, 0u, 32u);
+        st.initialized = 1u;
+        st.pending_reset = 0u;
+        st.last_reason = MR_TASK_TERMINATION_CONTINUING;
+        sample_command(P, env, episode, 0u, st.command);
+        st.phase = 0.0f;
+        st.previous_height = root_frame(P, rq, rv).position.z;
+        st.episode_return = 0.0f;
+        st.episode_tracking = 0.0f;
+        __syncwarp();
+        // Every delay-line slot is zero here; the newest raw slot stands for
+        // all of them.
+        write_frame(P, rq, rv, st, hist + (P.history - 2) * P.na, prev + P.na, env, episode, 0u, frame, lane);
+        if (lane == 0) p.state[local] = st;
+    }
+    if (lane == 0) p.masks_out[local] = reset ? 1u : 0u;
+    __syncwarp();
+    if (p.observations) {
+        float* out = p.observations + static_cast<size_t>(local) * P.nobs;
+        for (int i = lane; i < P.nobs; i += 32) out[i] = frame[i];
+    }
+}
+
+// One thread per (environment, action) (:3520-3668).
+__global__ void __launch_bounds__(kApplyThreads) task_apply_kernel(TaskParams p) {
+    const TaskProgramDevice& P = p.prog;
+    const long long idx = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= static_cast<long long>(p.env_count) * P.na) return;
+    const int local = static_cast<int>(idx / P.na), a = static_cast<int>(idx - static_cast<long long>(local) * P.na);
+    float* hist = p.action_history + static_cast<size_t>(local) * P.history * P.na;
+    const int filter = P.history - 1, raw_last = filter - 1;
+    for (int d = 0; d < raw_last; ++d) hist[d * P.na + a] = hist[(d + 1) * P.na + a];
+    const float requested = p.actions[static_cast<size_t>(local) * P.na + a];
+    const float previous = hist[filter * P.na + a];
+    const MRTaskActionBindingC b = P.actions[a];
+    const float response = b.response_time_seconds > 0.0f
+                               ? fminf(fmaxf(1.0f - expf(-P.dt / b.response_time_seconds), 0.0f), 1.0f)
+                               : 1.0f;
+    hist[raw_last * P.na + a] = requested;
+    const int selected = raw_last - min(P.delay, raw_last);
+    const float filtered = mixf(previous, hist[selected * P.na + a], response);
+    hist[filter * P.na + a] = filtered;
+    const float target = P.default_q[b.q_index] + b.scale * filtered;
+    p.targets[static_cast<size_t>(local) * P.na + a] = fminf(fmaxf(target, b.lower_target), b.upper_target);
+}
+
+__global__ void __launch_bounds__(32 * kTaskWarps) task_complete_kernel(TaskParams p) {
+    const int lane = threadIdx.x & 31;
+    const int local = blockIdx.x * kTaskWarps + (threadIdx.x >> 5);
+    if (local >= p.env_count) return;
+    const TaskProgramDevice& P = p.prog;
+    const unsigned env = static_cast<unsigned>(p.env_base + local);
+    TaskEnvState st = p.state[local];
+    const float* q = p.q + static_cast<size_t>(local) * P.nq;
+    const float* v = p.v + static_cast<size_t>(local) * P.nv;
+    float* hist = p.action_history + static_cast<size_t>(local) * P.history * P.na;
+    float* prev = p.previous_joint + static_cast<size_t>(local) * 2 * P.na;
+    const bool physics_error = p.status[local] != MR_STEP_SUCCESS;
+
+    // Reward inputs (:4376-4500).
+    const Root r = root_frame(P, q, v);
+    const float3 base_linear = rotate_inverse(r.orientation, r.linear);
+    const float3 base_angular = rotate_inverse(r.orientation, r.angular);
+    const float3 gravity = projected_gravity(r);
+    const float height = r.position.z;
+    const float tilt = atan2f(sqrtf(gravity.x * gravity.x + gravity.y * gravity.y), fmaxf(-gravity.z, 1.0e-6f));
+    const float4 o = r.orientation;
+    float yx = 1.0f - 2.0f * (o.y * o.y + o.z * o.z), yy = 2.0f * (o.w * o.z + o.x * o.y);
+    const float ys = rsqrtf(fmaxf(yx * yx + yy * yy, 1.0e-12f));
+    yx *= ys;
+    yy *= ys;
+    const float fx = yx * r.linear.x + yy * r.linear.y, fy = -yy * r.linear.x + yx * r.linear.y;
+    const float tdx = fx - st.command[0], tdy = fy - st.command[1];
+    const float tracking_error = tdx * tdx + tdy * tdy;
+    const float yaw_delta = base_angular.z - st.command[2];
+    const float yaw_error = yaw_delta * yaw_delta;
+
+    const int raw_last = P.history - 2, raw_previous = raw_last - 1;
+    float vel2 = 0.0f, acc2 = 0.0f, rate2 = 0.0f, lim2 = 0.0f;
+    for (int a = lane; a < P.na; a += 32) {
+        const MRTaskActionBindingC b = P.actions[a];
+        const float delta = hist[raw_last * P.na + a] - hist[raw_previous * P.na + a];
+        rate2 += delta * delta;
+        const float position = q[b.q_index], velocity = v[b.v_index];
+        const float acceleration = (velocity - prev[a]) / P.dt;
+        const float lower = fmaxf(P.limit_lower[a] - position, 0.0f), upper = fmaxf(position - P.limit_upper[a], 0.0f);
+        vel2 += velocity * velocity;
+        acc2 += acceleration * acceleration;
+        lim2 += lower * lower + upper * upper;
+    }
+    vel2 = warp_sum(vel2);
+    acc2 = warp_sum(acc2);
+    rate2 = warp_sum(rate2);
+    lim2 = warp_sum(lim2);
+
+    const float phase = fmodf(st.phase + kTwoPi * P.dt / P.gait_period, kTwoPi);
+
+    float reward = 0.0f;
+    float b0[4] = {0.0f, 0.0f, 0.0f, 0.0f}, b1[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    for (int k = 0; k < P.nrewards; ++k) {
+        const MRTaskRewardOperatorC op = P.rewards[k];
+        float value = 0.0f;
+        switch (op.opcode) {
+        case MR_TASK_REWARD_LINEAR_VELOCITY_TRACKING:
+            value = expf(-tracking_error / fmaxf(op.parameters[0], 1.0e-8f));
+            break;
+        case MR_TASK_REWARD_YAW_VELOCITY_TRACKING:
+            value = expf(-yaw_error / fmaxf(op.parameters[0], 1.0e-8f));
+            break;
+        case MR_TASK_REWARD_CONSTANT:
+            value = 1.0f;
+            break;
+        case MR_TASK_REWARD_ROOT_VERTICAL_VELOCITY_SQUARED:
+            value = base_linear.z * base_linear.z;
+            break;
+        case MR_TASK_REWARD_ROOT_ROLL_PITCH_VELOCITY_SQUARED:
+            value = base_angular.x * base_angular.x + base_angular.y * base_angular.y;
+            break;
+        case MR_TASK_REWARD_TILT_SQUARED:
+            value = tilt * tilt;
+            break;
+        case MR_TASK_REWARD_PROJECTED_GRAVITY_HORIZONTAL_SQUARED:
+            value = gravity.x * gravity.x + gravity.y * gravity.y;
+            break;
+        case MR_TASK_REWARD_ROOT_HEIGHT_ERROR_SQUARED: {
+            const float e = height - P.base_height;
+            value = e * e;
+            break;
+        }
+        case MR_TASK_REWARD_ROOT_HEIGHT_NORMALIZED:
+            value = fminf(fmaxf(height / fmaxf(P.base_height, 1.0e-6f), 0.0f), 1.0f);
+            break;
+        case MR_TASK_REWARD_ROOT_HEIGHT_PROGRESS:
+            value = fminf(fmaxf((height - st.previous_height) / P.dt, -2.0f), 2.0f);
+            break;
+        case MR_TASK_REWARD_UPRIGHTNESS: {
+            const float up = fminf(fmaxf(-gravity.z, 0.0f), 1.0f);
+            value = up * up;
+            break;
+        }
+        case MR_TASK_REWARD_JOINT_VELOCITY_SQUARED:
+            value = vel2;
+            break;
+        case MR_TASK_REWARD_JOINT_ACCELERATION_SQUARED:
+            value = acc2;
+            break;
+        case MR_TASK_REWARD_ACTION_RATE_SQUARED:
+            value = rate2;
+            break;
+        case MR_TASK_REWARD_JOINT_LIMIT_VIOLATION_SQUARED:
+            value = lim2;
+            break;
+        case MR_TASK_REWARD_JOINT_LIMIT_VIOLATION_ABSOLUTE: {
+            const float soft = fminf(fmaxf(op.parameters[0], 1.0e-6f), 1.0f);
+            float sum = 0.0f;
+            for (int a = lane; a < P.na; a += 32) {
+                const float center = 0.5f * (P.limit_lower[a] + P.limit_upper[a]);
+                const float half = 0.5f * (P.limit_upper[a] - P.limit_lower[a]) * soft;
+                const float position = q[P.actions[a].q_index];
+                sum += fmaxf(center - half - position, 0.0f) + fmaxf(position - center - half, 0.0f);
+            }
+            value = warp_sum(sum);
+            break;
+        }
+        case MR_TASK_REWARD_JOINT_GROUP_POSTURE_SQUARED:
+        case MR_TASK_REWARD_JOINT_GROUP_POSTURE_ABSOLUTE: {
+            const MRTaskIndexGroupC g = P.groups[op.group];
+            float sum = 0.0f;
+            for (unsigned m = static_cast<unsigned>(lane); m < g.count; m += 32u) {
+                const int qi = static_cast<int>(P.actions[P.members[g.first + m]].q_index);
+                const float e = q[qi] - P.default_q[qi];
+                sum += op.opcode == MR_TASK_REWARD_JOINT_GROUP_POSTURE_SQUARED ? e * e : fabsf(e);
+            }
+            sum = warp_sum(sum);
+            value = op.opcode == MR_TASK_REWARD_JOINT_GROUP_POSTURE_SQUARED ? sum / fmaxf(static_cast<float>(g.count), 1.0f) : sum;
+            break;
+        }
+        default:
+            break;
+        }
+        const float contribution = op.weight * value;
+        reward += contribution;
+        // Reward breakdown lanes (:5985-6046).
+        switch (op.opcode) {
+        case MR_TASK_REWARD_LINEAR_VELOCITY_TRACKING:
+        case MR_TASK_REWARD_YAW_VELOCITY_TRACKING:
+        case MR_TASK_REWARD_CONSTANT:
+            b0[0] += contribution;
+            break;
+        case MR_TASK_REWARD_JOINT_VELOCITY_SQUARED:
+            b0[2] += contribution;
+            break;
+        case MR_TASK_REWARD_JOINT_ACCELERATION_SQUARED:
+            b0[3] += contribution;
+            break;
+        case MR_TASK_REWARD_ACTION_RATE_SQUARED:
+            b1[0] += contribution;
+            break;
+        case MR_TASK_REWARD_JOINT_LIMIT_VIOLATION_SQUARED:
+        case MR_TASK_REWARD_JOINT_LIMIT_VIOLATION_ABSOLUTE:
+        case MR_TASK_REWARD_JOINT_GROUP_POSTURE_SQUARED:
+        case MR_TASK_REWARD_JOINT_GROUP_POSTURE_ABSOLUTE:
+            b1[1] += contribution;
+            break;
+        default:  // the base-state operators
+            b0[1] += contribution;
+            break;
+        }
+    }
+
+    // Terminations (:6064-6160): the highest priority among the triggered.
+    const unsigned episode_steps = st.episode_step + 1u;
+    const bool timeout = episode_steps >= static_cast<unsigned>(P.max_episode_steps);
+    bool done = false;
+    unsigned reason = MR_TASK_TERMINATION_CONTINUING, priority = 0u;
+    float penalty = 0.0f;
+    for (int k = 0; k < P.nterminations; ++k) {
+        const MRTaskTerminationOperatorC op = P.terminations[k];
+        const bool triggered = op.opcode == MR_TASK_TERMINATE_MINIMUM_ROOT_HEIGHT ? height < op.threshold
+                               : op.opcode == MR_TASK_TERMINATE_MAXIMUM_TILT        ? tilt > op.threshold
+                                                                                    : false;
+        if (triggered && (!done || op.priority >= priority)) {
+            done = true;
+            reason = op.reason;
+            priority = op.priority;
+            penalty = op.failure_penalty;
+        }
+    }
+    if (timeout) {
+        done = true;
+        reason = MR_TASK_TERMINATION_TIMEOUT;
+    }
+    if (physics_error) {
+        done = true;
+        reason = MR_TASK_TERMINATION_PHYSICS_ERROR;
+    }
+    if (done && reason != MR_TASK_TERMINATION_TIMEOUT && reason != MR_TASK_TERMINATION_PHYSICS_ERROR) {
+        reward += penalty;
+        b0[1] += penalty;
+    }
+    reward *= P.dt;
+    for (int i = 0; i < 4; ++i) {
+        b0[i] *= P.dt;
+        b1[i] *= P.dt;
+    }
+    const float tracking = expf(-tracking_error / 0.25f);
+    const float yaw_tracking = expf(-yaw_error / 0.25f);
+    const float episode_tracking = st.episode_tracking + tracking;
+    const float episode_score = episode_tracking / fmaxf(static_cast<float>(episode_steps), 1.0f);
+    const float episode_return = st.episode_return + reward;
+
+    // Command schedule and state (:6388-6440).
+    if (!done && st.command_steps <= 1u) {
+        sample_command(P, env, st.episode, episode_steps, st.command);
+        st.command_steps = duration_steps(P, env, st.episode, episode_steps, 64u);
+    } else if (!done) {
+        --st.command_steps;
+    }
+    st.episode_step = episode_steps;
+    st.pending_reset = done ? 1u : 0u;
+    st.last_reason = reason;
+    st.phase = phase;
+    st.previous_height = height;
+    st.episode_return = done ? 0.0f : episode_return;
+    st.episode_tracking = done ? 0.0f : episode_tracking;
+
+    // The next decision's frame, then this step's joint history (:6478-6630).
+    if (!done || (timeout && !physics_error)) {
+        float* frame = p.frame + static_cast<size_t>(local) * P.nobs;
+        write_frame(P, q, v, st, hist + raw_last * P.na, prev + P.na, env, st.episode, episode_steps, frame, lane);
+        __syncwarp();
+        for (int a = lane; a < P.na; a += 32) {
+            const MRTaskActionBindingC b = P.actions[a];
+            prev[a] = v[b.v_index];
+            prev[P.na + a] = q[b.q_index];
+        }
+    }
+    if (lane == 0) {
+        p.state[local] = st;
+        MRTaskTransitionC t{};
+        t.reward = reward;
+        t.tracking_score = 0.5f * (tracking + yaw_tracking);
+        t.root_height = height;
+        t.tilt = tilt;
+        t.done = done ? 1u : 0u;
+        t.timeout = timeout ? 1u : 0u;
+        t.physics_error = physics_error ? 1u : 0u;
+        t.termination_reason = reason;
+        t.task_reward = b0[0];
+        t.base_reward = b0[1];
+        t.joint_velocity_reward = b0[2];
+        t.joint_acceleration_reward = b0[3];
+        t.control_reward = b1[0];
+        t.posture_reward = b1[1];
+        t.energy_reward = b1[2];
+        t.contact_reward = b1[3];
+        t.policy_revision = p.policy_revision;
+        t.episode_tracking_score = done && !physics_error ? episode_score : 0.0f;
+        p.transitions[local] = t;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_task_observe(const TaskParams& p, cudaStream_t stream) {
+    if (p.env_count <= 0) return cudaSuccess;
+    const int blocks = (p.env_count + kTaskWarps - 1) / kTaskWarps;
+    task_observe_kernel<<<blocks, 32 * kTaskWarps, 0, stream>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_task_apply(const TaskParams& p, cudaStream_t stream) {
+    const long long n = static_cast<long long>(p.env_count) * p.prog.na;
+    if (n <= 0) return cudaSuccess;
+    const int blocks = static_cast<int>((n + kApplyThreads - 1) / kApplyThreads);
+    task_apply_kernel<<<blocks, kApplyThreads, 0, stream>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_task_complete(const TaskParams& p, cudaStream_t stream) {
+    if (p.env_count <= 0) return cudaSuccess;
+    const int blocks = (p.env_count + kTaskWarps - 1) / kTaskWarps;
+    task_complete_kernel<<<blocks, 32 * kTaskWarps, 0, stream>>>(p);
+    return cudaGetLastError();
+}
+
+}  // namespace numi

@@ -28,6 +28,7 @@ MR_RUN_SOURCE_SYNTHETIC_CYLINDER_PILE: Final = 104
 MR_RUN_SOURCE_SYNTHETIC_PILE_GJK: Final = 105
 MR_RUN_SOURCE_SYNTHETIC_HULL_PILE: Final = 106
 MR_SHAPE_CONVEX: Final = 5
+MR_DOF_FLAG_ACTUATED: Final = 1 << 1
 MANIFOLD_POINTS: Final = 4
 MR_PRECISION_FP32: Final = 0
 MR_PRECISION_FP64_ARTICULATED_INERTIA: Final = 1
@@ -321,6 +322,125 @@ class TaskRolloutAdvanceC(ct.Structure):
     ]
 
 
+class TaskActionBindingC(ct.Structure):
+    _fields_ = [
+        ("dof_index", ct.c_uint32),
+        ("q_index", ct.c_uint32),
+        ("v_index", ct.c_uint32),
+        ("reserved", ct.c_uint32),
+        ("scale", ct.c_float),
+        ("lower_target", ct.c_float),
+        ("upper_target", ct.c_float),
+        ("response_time_seconds", ct.c_float),
+    ]
+
+
+class TaskObservationOperatorC(ct.Structure):
+    _fields_ = [
+        ("opcode", ct.c_uint32),
+        ("source", ct.c_uint32),
+        ("component", ct.c_uint32),
+        ("flags", ct.c_uint32),
+        ("transform_scale", ct.c_float),
+        ("transform_offset", ct.c_float),
+        ("noise_amplitude", ct.c_float),
+        ("noise_channel", ct.c_uint32),
+    ]
+
+
+class TaskRewardOperatorC(ct.Structure):
+    _fields_ = [
+        ("opcode", ct.c_uint32),
+        ("group", ct.c_uint32),
+        ("weight", ct.c_float),
+        ("parameters", ct.c_float * 3),
+    ]
+
+
+class TaskTerminationOperatorC(ct.Structure):
+    _fields_ = [
+        ("opcode", ct.c_uint32),
+        ("reason", ct.c_uint32),
+        ("priority", ct.c_uint32),
+        ("reserved", ct.c_uint32),
+        ("threshold", ct.c_float),
+        ("failure_penalty", ct.c_float),
+    ]
+
+
+class TaskRandomizationOperatorC(ct.Structure):
+    _fields_ = [
+        ("opcode", ct.c_uint32),
+        ("target", ct.c_uint32),
+        ("parameters", ct.c_float * 4),
+    ]
+
+
+class TaskIndexGroupC(ct.Structure):
+    _fields_ = [("first", ct.c_uint32), ("count", ct.c_uint32)]
+
+
+class TaskProgramC(ct.Structure):
+    _fields_ = [
+        ("actions", ct.POINTER(TaskActionBindingC)),
+        ("action_count", ct.c_uint32),
+        ("actor", ct.POINTER(TaskObservationOperatorC)),
+        ("actor_count", ct.c_uint32),
+        ("rewards", ct.POINTER(TaskRewardOperatorC)),
+        ("reward_count", ct.c_uint32),
+        ("terminations", ct.POINTER(TaskTerminationOperatorC)),
+        ("termination_count", ct.c_uint32),
+        ("randomization", ct.POINTER(TaskRandomizationOperatorC)),
+        ("randomization_count", ct.c_uint32),
+        ("joint_groups", ct.POINTER(TaskIndexGroupC)),
+        ("joint_group_count", ct.c_uint32),
+        ("joint_members", ct.POINTER(ct.c_uint32)),
+        ("joint_member_count", ct.c_uint32),
+        ("default_q", ct.POINTER(ct.c_float)),
+        ("default_q_count", ct.c_uint32),
+        ("maximum_episode_steps", ct.c_uint32),
+        ("action_history", ct.c_uint32),
+        ("action_delay_steps", ct.c_uint32),
+        ("base_height_target", ct.c_float),
+        ("gait_period_seconds", ct.c_float),
+        ("root_reference", ct.c_float * 3),
+        ("command_lower", ct.c_float * 3),
+        ("command_upper", ct.c_float * 3),
+        ("standing_probability", ct.c_float),
+        ("command_duration_seconds", ct.c_float * 2),
+        ("task_fingerprint", ct.c_uint64),
+    ]
+
+
+class TaskTransitionC(ct.Structure):
+    _fields_ = [
+        ("reward", ct.c_float),
+        ("tracking_score", ct.c_float),
+        ("root_height", ct.c_float),
+        ("tilt", ct.c_float),
+        ("done", ct.c_uint32),
+        ("timeout", ct.c_uint32),
+        ("physics_error", ct.c_uint32),
+        ("termination_reason", ct.c_uint32),
+        ("task_reward", ct.c_float),
+        ("base_reward", ct.c_float),
+        ("joint_velocity_reward", ct.c_float),
+        ("joint_acceleration_reward", ct.c_float),
+        ("control_reward", ct.c_float),
+        ("posture_reward", ct.c_float),
+        ("energy_reward", ct.c_float),
+        ("contact_reward", ct.c_float),
+        ("task_outcome_channels", ct.c_float * 8),
+        ("policy_revision", ct.c_uint64),
+        ("timeout_bootstrap_value", ct.c_float),
+        ("episode_tracking_score", ct.c_float),
+        ("difficulty_band", ct.c_uint32),
+        ("terrain_level", ct.c_uint32),
+        ("impact_sequence_index", ct.c_uint32),
+        ("impact_event_flags", ct.c_uint32),
+    ]
+
+
 class ModelWorldC(ct.Structure):
     _fields_ = [
         ("body_count", ct.c_uint32),
@@ -548,6 +668,11 @@ EXPORTED_SYMBOLS: Final = (
     "mr_task_rollout_environment_chains",
     "mr_task_rollout_policy_revision",
     "mr_task_rollout_clear_policy",
+    "mr_task_rollout_set_task",
+    "mr_task_rollout_clear_task",
+    "mr_task_rollout_transitions",
+    "mr_task_rollout_device_transitions",
+    "mr_task_rollout_copy_transitions",
     "mr_task_rollout_policy_latents",
     "mr_task_rollout_policy_log_probabilities",
     "mr_task_rollout_policy_values",
@@ -729,6 +854,16 @@ class Bindings:
         L.mr_task_rollout_load_policy_pack.restype = ct.c_int
         L.mr_policy_pack_inspect.argtypes = [ct.c_char_p, P(PolicyPackInfoC), P(ct.c_float), ct.c_size_t]
         L.mr_policy_pack_inspect.restype = ct.c_int
+        L.mr_task_rollout_set_task.argtypes = [ct.c_void_p, P(TaskProgramC)]
+        L.mr_task_rollout_set_task.restype = ct.c_int
+        L.mr_task_rollout_clear_task.argtypes = [ct.c_void_p]
+        L.mr_task_rollout_clear_task.restype = ct.c_int
+        L.mr_task_rollout_transitions.argtypes = [ct.c_void_p]
+        L.mr_task_rollout_transitions.restype = P(TaskTransitionC)
+        L.mr_task_rollout_device_transitions.argtypes = [ct.c_void_p]
+        L.mr_task_rollout_device_transitions.restype = ct.c_uint64
+        L.mr_task_rollout_copy_transitions.argtypes = [ct.c_void_p, P(TaskTransitionC), ct.c_size_t]
+        L.mr_task_rollout_copy_transitions.restype = ct.c_int
 
     def last_error(self) -> str:
         value = self.lib.mr_last_error()

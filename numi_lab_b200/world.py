@@ -278,6 +278,17 @@ def quality_solve(mass: np.ndarray, jacobian: np.ndarray, free_velocity: np.ndar
     return imp, vel, results
 
 
+# MRTaskTransitionC as a numpy record.
+_TRANSITION_DTYPE = np.dtype([
+    ("reward", "<f4"), ("tracking_score", "<f4"), ("root_height", "<f4"), ("tilt", "<f4"), ("done", "<u4"), ("timeout", "<u4"),
+    ("physics_error", "<u4"), ("termination_reason", "<u4"), ("task_reward", "<f4"), ("base_reward", "<f4"),
+    ("joint_velocity_reward", "<f4"), ("joint_acceleration_reward", "<f4"), ("control_reward", "<f4"), ("posture_reward", "<f4"),
+    ("energy_reward", "<f4"), ("contact_reward", "<f4"), ("task_outcome_channels", "<f4", (8,)), ("policy_revision", "<u8"),
+    ("timeout_bootstrap_value", "<f4"), ("episode_tracking_score", "<f4"), ("difficulty_band", "<u4"), ("terrain_level", "<u4"),
+    ("impact_sequence_index", "<u4"), ("impact_event_flags", "<u4"),
+])
+
+
 class World:
     """A batch of environments of one synthetic world on the current CUDA device."""
 
@@ -325,6 +336,7 @@ class World:
         self.scene_bodies = int(layout.scene_body_count)
         self.scene = self.scene_bodies > 0
         self.solver = "temporal_cone"
+        self.task = None
         self.set_precision(precision)
 
     def set_precision(self, precision: str) -> None:
@@ -647,6 +659,41 @@ class World:
             "values": np.ctypeslib.as_array(L.mr_task_rollout_policy_values(self._handle), shape=(cells,)).reshape(steps, self.envs).copy(),
             "bootstrap_values": np.ctypeslib.as_array(L.mr_task_rollout_bootstrap_policy_values(self._handle), shape=(self.envs,)).copy(),
         }
+
+    # -- task layer ----------------------------------------------------------
+    def set_task(self, program) -> None:
+        """Installs a task program (``numi_lab_b200.task.TaskProgram``,
+        mr_task_rollout_set_task): observations become its actor frames,
+        actions its normalised policy actions; every environment starts a
+        new episode at the next step."""
+
+        from .task import task_program_c
+
+        record, keep = task_program_c(program)
+        self._lib.check(self._lib.lib.mr_task_rollout_set_task(self._handle, ct.byref(record)), "mr_task_rollout_set_task")
+        del keep
+        self.observation_count = int(self.layout().actor_observation_count)
+        self.task = program
+
+    def clear_task(self) -> None:
+        self._lib.check(self._lib.lib.mr_task_rollout_clear_task(self._handle), "mr_task_rollout_clear_task")
+        self.observation_count = self.nq + self.nv
+        self.task = None
+
+    TRANSITION_FIELDS = ("reward", "tracking_score", "root_height", "tilt", "done", "timeout", "physics_error",
+                         "termination_reason", "task_reward", "base_reward", "joint_velocity_reward", "joint_acceleration_reward",
+                         "control_reward", "posture_reward", "energy_reward", "contact_reward", "episode_tracking_score",
+                         "policy_revision")
+
+    def transitions(self, steps: int) -> dict[str, np.ndarray]:
+        """The last advance's transitions ([step][env] per field; the advance
+        must have covered `steps` control steps), copied once its work has
+        finished."""
+
+        raw = (native.TaskTransitionC * (steps * self.envs))()
+        self._lib.check(self._lib.lib.mr_task_rollout_copy_transitions(self._handle, raw, len(raw)), "mr_task_rollout_copy_transitions")
+        arr = np.frombuffer(bytes(raw), dtype=_TRANSITION_DTYPE).reshape(steps, self.envs)
+        return {name: arr[name].copy() for name in self.TRANSITION_FIELDS}
 
     def set_state_readback(self, enabled: bool) -> None:
         self._lib.check(self._lib.lib.mr_task_rollout_set_state_readback(self._handle, 1 if enabled else 0), "set_state_readback")

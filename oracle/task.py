@@ -1,0 +1,420 @@
+"""Oracle for the task layer -- test infrastructure only (tests/ and the
+smoke check import it; the product never does).
+
+An FP64 restatement, one environment at a time, of the reference's task
+kernels for the operator subset the device evaluates
+(src/metal/LocomotionTask.metal):
+
+* ``observe``  -- mr_locomotion_task_observe (:2184-3440): the reset test
+  (:2329-2333), reset pose from default_q plus the randomization operators
+  (:2337-2770), the new episode's state (:2947-3010) and its actor frame
+  (writeFrame :1190-1330 on the reset state, :3070-3098);
+* ``apply``    -- mr_locomotion_task_apply_actions (:3442-3674);
+* ``complete`` -- mr_locomotion_task_complete (:3904-6745): reward inputs
+  (:4376-4500), reward operators (:4700-5960), breakdown lanes (:5985-6046),
+  terminations (:6064-6160), command schedule and state (:6388-6440), next
+  actor frame and joint history (:6478-6630), transition (:6697-6742).
+
+Draws use the reference's keyed counter hash (randomUnit :121-152): a key of
+seed, environment, episode, control step and channel through SplitMix64's
+finaliser, the top 24 bits scaled to [0, 1).
+
+Parity unpinned against the reference itself: the reference evaluates its
+task program only in Metal shaders (there is no CPU path to run here).  The
+restatement is checked against closed forms in tests/test_task_oracle.py and
+the device against it in tests/test_task_gpu.py.
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+M64 = (1 << 64) - 1
+M32 = (1 << 32) - 1
+TWO_PI = 2.0 * math.pi
+
+OBS_ROOT_ANGULAR, OBS_GRAVITY, OBS_COMMAND, OBS_JOINT_ERROR, OBS_JOINT_VELOCITY, OBS_PREVIOUS_ACTION = 0, 1, 2, 3, 4, 5
+OBS_ROOT_LINEAR, OBS_ROOT_HEIGHT, OBS_GAIT_PHASE, OBS_DELAYED_ACTION, OBS_JOINT_FD_VELOCITY = 6, 7, 14, 26, 27
+NORMALIZE = 1
+R_LINEAR, R_YAW, R_CONSTANT, R_VERTICAL, R_ROLL_PITCH, R_TILT, R_HEIGHT_ERROR = 0, 1, 2, 3, 4, 5, 6
+R_JOINT_VELOCITY, R_JOINT_ACCELERATION, R_ACTION_RATE, R_LIMIT_SQUARED = 7, 8, 9, 10
+R_POSTURE_SQUARED, R_POSTURE_ABSOLUTE, R_GRAVITY_HORIZONTAL, R_LIMIT_ABSOLUTE = 12, 17, 18, 20
+R_HEIGHT_NORMALIZED, R_HEIGHT_PROGRESS, R_UPRIGHTNESS = 21, 22, 23
+T_MIN_HEIGHT, T_MAX_TILT = 0, 1
+REASON_CONTINUING, REASON_TIMEOUT, REASON_PHYSICS_ERROR = 0, 4, 5
+RND_ROOT_POSITION, RND_ROOT_YAW, RND_ACTION_POSITION, RND_VELOCITY = 0, 1, 2, 3
+RND_ACTION_VELOCITY, RND_ROOT_HEIGHT, RND_JOINT_POSITION = 9, 10, 12
+
+
+def mix64(x: int) -> int:
+    """SplitMix64's finaliser (LocomotionTask.metal:121-130)."""
+
+    x = (x + 0x9E3779B97F4A7C15) & M64
+    x = ((x ^ (x >> 30)) * 0xBF58476D1CE4E5B9) & M64
+    x = ((x ^ (x >> 27)) * 0x94D049BB133111EB) & M64
+    return x ^ (x >> 31)
+
+
+def unit_draw(seed: int, env: int, episode: int, step: int, channel: int) -> float:
+    """randomUnit (:132-152): the counters are 32-bit before widening."""
+
+    key = seed & M64
+    key ^= (((env + 1) & M32) * 0xD2B74407B1CE6E93) & M64
+    key ^= (((episode + 1) & M32) * 0xCA5A826395121157) & M64
+    key ^= (((step + 1) & M32) * 0x9E3779B185EBCA87) & M64
+    key ^= (((channel + 1) & M32) * 0x94D049BB133111EB) & M64
+    return float((mix64(key) >> 40) & 0xFFFFFF) / 16777216.0
+
+
+def signed_draw(*args) -> float:
+    return 2.0 * unit_draw(*args) - 1.0
+
+
+def range_draw(seed, env, episode, step, channel, lower, upper) -> float:
+    return lower + (upper - lower) * unit_draw(seed, env, episode, step, channel)
+
+
+def rotate(q, v):
+    u = np.asarray(q[:3], np.float64)
+    t = 2.0 * np.cross(u, v)
+    return np.asarray(v, np.float64) + q[3] * t + np.cross(u, t)
+
+
+def rotate_inverse(q, v):
+    u = np.asarray(q[:3], np.float64)
+    t = 2.0 * np.cross(u, v)
+    return np.asarray(v, np.float64) - q[3] * t + np.cross(u, t)
+
+
+def quat_product(a, b):
+    return np.array([a[3] * b[0] + a[0] * b[3] + a[1] * b[2] - a[2] * b[1],
+                     a[3] * b[1] - a[0] * b[2] + a[1] * b[3] + a[2] * b[0],
+                     a[3] * b[2] + a[0] * b[1] - a[1] * b[0] + a[2] * b[3],
+                     a[3] * b[3] - a[0] * b[0] - a[1] * b[1] - a[2] * b[2]])
+
+
+def normalized_or(v, fallback):
+    l2 = float(np.dot(v, v))
+    return np.asarray(v, np.float64) / math.sqrt(l2) if l2 > 1.0e-12 and math.isfinite(l2) else np.asarray(fallback, np.float64)
+
+
+@dataclass
+class EnvState:
+    """One environment's task record (MRTaskStateGPU's used lanes) plus its
+    delay line [history][na], joint history [2][na] and next actor frame."""
+
+    history: np.ndarray
+    previous_joint: np.ndarray
+    frame: np.ndarray
+    episode_step: int = 0
+    episode: int = 0
+    command_steps: int = 0
+    initialized: bool = False
+    pending_reset: bool = False
+    last_reason: int = 0
+    command: np.ndarray = field(default_factory=lambda: np.zeros(3))
+    phase: float = 0.0
+    previous_height: float = 0.0
+    episode_return: float = 0.0
+    episode_tracking: float = 0.0
+
+
+class TaskOracle:
+    """The task layer over one rollout: `program` a numi_lab_b200.task.TaskProgram."""
+
+    def __init__(self, program, *, nq: int, nv: int, dt: float, seed: int, fixed_root: bool, limit_lower, limit_upper,
+                 terminations: bool = True) -> None:
+        self.p = program
+        self.nq, self.nv, self.dt, self.seed, self.fixed_root = nq, nv, float(dt), int(seed), fixed_root
+        self.na = len(program.actions)
+        self.nobs = len(program.actor)
+        self.L = int(program.action_history)
+        self.delay = min(int(program.action_delay_steps), self.L - 2)
+        self.lo = np.asarray(limit_lower, np.float64)
+        self.hi = np.asarray(limit_upper, np.float64)
+        self.default_q = np.asarray(program.default_q, np.float64)
+        self.terminations = program.terminations if terminations else []
+
+    def new_state(self) -> EnvState:
+        return EnvState(np.zeros((self.L, self.na)), np.zeros((2, self.na)), np.zeros(self.nobs))
+
+    # -- root frame (:396-478) ------------------------------------------------
+    def root(self, q, v):
+        if self.fixed_root:
+            z = np.zeros(3)
+            return np.array([0.0, 0.0, 0.0, 1.0]), z, z, z
+        o = np.asarray(q[3:7], np.float64)
+        off = rotate(o, np.asarray(self.p.root_reference, np.float64))
+        ang = np.asarray(v[3:6], np.float64)
+        return o, np.asarray(q[:3], np.float64) + off, np.asarray(v[:3], np.float64) + np.cross(ang, off), ang
+
+    @staticmethod
+    def gravity(o):
+        down = np.array([0.0, 0.0, -1.0])
+        return normalized_or(rotate_inverse(o, down), down)
+
+    def clean(self, op, q, v, st: EnvState, raw_slot: int, previous_q) -> float:
+        o, pos, lin, ang = self.root(q, v)
+        c = op.component
+        b = self.p.actions[op.source] if op.opcode in (OBS_JOINT_ERROR, OBS_JOINT_VELOCITY, OBS_JOINT_FD_VELOCITY) else None
+        if op.opcode == OBS_ROOT_ANGULAR:
+            value = rotate_inverse(o, ang)[c]
+        elif op.opcode == OBS_GRAVITY:
+            value = self.gravity(o)[c]
+        elif op.opcode == OBS_COMMAND:
+            value = st.command[c] if c < 3 else 0.0
+        elif op.opcode == OBS_JOINT_ERROR:
+            value = q[b.q_index] - self.default_q[b.q_index]
+        elif op.opcode == OBS_JOINT_VELOCITY:
+            value = v[b.v_index]
+        elif op.opcode == OBS_JOINT_FD_VELOCITY:
+            value = (q[b.q_index] - previous_q[op.source]) / self.dt
+        elif op.opcode == OBS_PREVIOUS_ACTION:
+            value = st.history[raw_slot, op.source]
+        elif op.opcode == OBS_DELAYED_ACTION:
+            value = st.history[raw_slot - c, op.source]
+        elif op.opcode == OBS_ROOT_LINEAR:
+            value = rotate_inverse(o, lin)[c]
+        elif op.opcode == OBS_ROOT_HEIGHT:
+            value = pos[2]
+        elif op.opcode == OBS_GAIT_PHASE:
+            value = (math.sin(st.phase) if c == 0 else math.cos(st.phase)) if np.linalg.norm(st.command) >= 0.1 else 0.0
+        else:
+            raise ValueError(f"opcode {op.opcode} is outside the subset")
+        return op.scale * float(value) + op.offset
+
+    def frame(self, env, q, v, st: EnvState, raw_slot: int, previous_q, episode: int, step: int) -> np.ndarray:
+        """writeFrame (:1190-1330)."""
+
+        g = np.array([0.0, 0.0, -1.0])
+        have = False
+        for op in self.p.actor:
+            if op.opcode == OBS_GRAVITY and op.flags & NORMALIZE:
+                g[op.component] = self.clean(op, q, v, st, raw_slot, previous_q) + op.noise_amplitude * signed_draw(
+                    self.seed, env, episode, step, op.noise_channel)
+                have = True
+        if have:
+            g = normalized_or(g, [0.0, 0.0, -1.0])
+        out = np.zeros(self.nobs)
+        for i, op in enumerate(self.p.actor):
+            if op.opcode == OBS_GRAVITY and op.flags & NORMALIZE:
+                out[i] = g[op.component]
+            else:
+                out[i] = self.clean(op, q, v, st, raw_slot, previous_q) + op.noise_amplitude * signed_draw(
+                    self.seed, env, episode, step, op.noise_channel)
+        return out
+
+    def duration_steps(self, env, episode, step, channel) -> int:
+        lo, hi = self.p.command_duration_seconds
+        return max(1, int(math.floor(range_draw(self.seed, env, episode, step, channel, lo, hi) / self.dt)))
+
+    def sample_command(self, env, episode, step) -> np.ndarray:
+        cmd = np.array([range_draw(self.seed, env, episode, step, 16 + k, self.p.command_lower[k], self.p.command_upper[k])
+                        for k in range(3)])
+        if unit_draw(self.seed, env, episode, step, 19) < self.p.standing_probability:
+            cmd[:] = 0.0
+        return cmd
+
+    # -- the three stages --------------------------------------------------------
+    def observe(self, env: int, st: EnvState, q, v, mask: bool):
+        """Returns (reset, reset_q, reset_v, observation)."""
+
+        reset = (not st.initialized) or st.pending_reset or bool(mask)
+        if not reset:
+            return False, None, None, st.frame.copy()
+        episode = st.episode + 1
+        rq = self.default_q.copy()
+        rv = np.zeros(self.nv)
+        for k, op in enumerate(self.p.randomization):
+            ch = 2048 + k
+            a, b = op.parameters[0], op.parameters[1]
+            if op.opcode == RND_ROOT_POSITION:
+                for c in range(3):
+                    rq[c] += op.parameters[c] * signed_draw(self.seed, env, episode, 0, ch + c)
+            elif op.opcode == RND_ROOT_YAW:
+                half = 0.5 * range_draw(self.seed, env, episode, 0, ch, a, b)
+                rq[3:7] = quat_product([0.0, 0.0, math.sin(half), math.cos(half)], self.default_q[3:7])
+            elif op.opcode == RND_ROOT_HEIGHT:
+                rq[2] = range_draw(self.seed, env, episode, 0, ch, a, b)
+            elif op.opcode == RND_JOINT_POSITION:
+                rq[op.target] = range_draw(self.seed, env, episode, 0, ch, a, b)
+            elif op.opcode == RND_ACTION_POSITION:
+                for i, bd in enumerate(self.p.actions):
+                    x = self.default_q[bd.q_index] + range_draw(self.seed, env, episode, 0, ch + i, a, b)
+                    rq[bd.q_index] = min(max(x, bd.lower_target), bd.upper_target)
+            elif op.opcode == RND_VELOCITY:
+                for i in range(self.nv):
+                    rv[i] = range_draw(self.seed, env, episode, 0, ch + i, a, b)
+            elif op.opcode == RND_ACTION_VELOCITY:
+                for i, bd in enumerate(self.p.actions):
+                    rv[bd.v_index] = range_draw(self.seed, env, episode, 0, ch + i, a, b)
+            else:
+                raise ValueError(f"randomization opcode {op.opcode} is outside the subset")
+        st.history[:] = 0.0
+        st.previous_joint[0] = 0.0
+        st.previous_joint[1] = [rq[bd.q_index] for bd in self.p.actions]
+        st.episode_step, st.episode = 0, episode
+        st.command_steps = self.duration_steps(env, episode, 0, 32)
+        st.initialized, st.pending_reset, st.last_reason = True, False, REASON_CONTINUING
+        st.command = self.sample_command(env, episode, 0)
+        st.phase = 0.0
+        st.previous_height = self.root(rq, rv)[1][2]
+        st.episode_return = st.episode_tracking = 0.0
+        st.frame = self.frame(env, rq, rv, st, self.L - 2, st.previous_joint[1], episode, 0)
+        return True, rq, rv, st.frame.copy()
+
+    def apply(self, st: EnvState, actions) -> np.ndarray:
+        """Drive targets [na] for the physics step (:3520-3668)."""
+
+        filt, raw_last = self.L - 1, self.L - 2
+        targets = np.zeros(self.na)
+        for a, b in enumerate(self.p.actions):
+            for d in range(raw_last):
+                st.history[d, a] = st.history[d + 1, a]
+            previous = st.history[filt, a]
+            resp = min(max(1.0 - math.exp(-self.dt / b.response_time_seconds), 0.0), 1.0) if b.response_time_seconds > 0.0 else 1.0
+            st.history[raw_last, a] = float(actions[a])
+            delayed = st.history[raw_last - min(self.delay, raw_last), a]
+            st.history[filt, a] = previous + (delayed - previous) * resp
+            targets[a] = min(max(self.default_q[b.q_index] + b.scale * st.history[filt, a], b.lower_target), b.upper_target)
+        return targets
+
+    def complete(self, env: int, st: EnvState, q, v, status: int) -> dict:
+        """Reward, termination, schedule and the next actor frame of one
+        finished physics step; returns the transition's fields."""
+
+        p, dt = self.p, self.dt
+        physics_error = status != 0
+        o, pos, lin, ang = self.root(q, v)
+        base_linear = rotate_inverse(o, lin)
+        base_angular = rotate_inverse(o, ang)
+        g = self.gravity(o)
+        height = pos[2]
+        tilt = math.atan2(math.hypot(g[0], g[1]), max(-g[2], 1.0e-6))
+        yx, yy = 1.0 - 2.0 * (o[1] * o[1] + o[2] * o[2]), 2.0 * (o[3] * o[2] + o[0] * o[1])
+        ys = 1.0 / math.sqrt(max(yx * yx + yy * yy, 1.0e-12))
+        yx, yy = yx * ys, yy * ys
+        fx, fy = yx * lin[0] + yy * lin[1], -yy * lin[0] + yx * lin[1]
+        tracking_error = (fx - st.command[0]) ** 2 + (fy - st.command[1]) ** 2
+        yaw_error = (base_angular[2] - st.command[2]) ** 2
+        raw_last, raw_prev = self.L - 2, self.L - 3
+        vel2 = acc2 = rate2 = lim2 = 0.0
+        for a, b in enumerate(p.actions):
+            rate2 += (st.history[raw_last, a] - st.history[raw_prev, a]) ** 2
+            x, xd = q[b.q_index], v[b.v_index]
+            acc = (xd - st.previous_joint[0, a]) / dt
+            lower, upper = max(self.lo[a] - x, 0.0), max(x - self.hi[a], 0.0)
+            vel2 += xd * xd
+            acc2 += acc * acc
+            lim2 += lower * lower + upper * upper
+        phase = math.fmod(st.phase + TWO_PI * dt / p.gait_period_seconds, TWO_PI)
+        reward = 0.0
+        b0, b1 = np.zeros(4), np.zeros(4)
+        for r in p.rewards:
+            op, w = r.opcode, r.weight
+            if op == R_LINEAR:
+                value = math.exp(-tracking_error / max(r.parameters[0], 1.0e-8))
+            elif op == R_YAW:
+                value = math.exp(-yaw_error / max(r.parameters[0], 1.0e-8))
+            elif op == R_CONSTANT:
+                value = 1.0
+            elif op == R_VERTICAL:
+                value = base_linear[2] ** 2
+            elif op == R_ROLL_PITCH:
+                value = base_angular[0] ** 2 + base_angular[1] ** 2
+            elif op == R_TILT:
+                value = tilt * tilt
+            elif op == R_GRAVITY_HORIZONTAL:
+                value = g[0] ** 2 + g[1] ** 2
+            elif op == R_HEIGHT_ERROR:
+                value = (height - p.base_height_target) ** 2
+            elif op == R_HEIGHT_NORMALIZED:
+                value = min(max(height / max(p.base_height_target, 1.0e-6), 0.0), 1.0)
+            elif op == R_HEIGHT_PROGRESS:
+                value = min(max((height - st.previous_height) / dt, -2.0), 2.0)
+            elif op == R_UPRIGHTNESS:
+                value = min(max(-g[2], 0.0), 1.0) ** 2
+            elif op == R_JOINT_VELOCITY:
+                value = vel2
+            elif op == R_JOINT_ACCELERATION:
+                value = acc2
+            elif op == R_ACTION_RATE:
+                value = rate2
+            elif op == R_LIMIT_SQUARED:
+                value = lim2
+            elif op == R_LIMIT_ABSOLUTE:
+                soft = min(max(r.parameters[0], 1.0e-6), 1.0)
+                value = 0.0
+                for a, b in enumerate(p.actions):
+                    center, half = 0.5 * (self.lo[a] + self.hi[a]), 0.5 * (self.hi[a] - self.lo[a]) * soft
+                    x = q[b.q_index]
+                    value += max(center - half - x, 0.0) + max(x - center - half, 0.0)
+            elif op in (R_POSTURE_SQUARED, R_POSTURE_ABSOLUTE):
+                members = p.joint_groups[r.group]
+                errs = [q[p.actions[m].q_index] - self.default_q[p.actions[m].q_index] for m in members]
+                value = (sum(e * e for e in errs) / max(len(errs), 1)) if op == R_POSTURE_SQUARED else sum(abs(e) for e in errs)
+            else:
+                raise ValueError(f"reward opcode {op} is outside the subset")
+            c = w * value
+            reward += c
+            if op in (R_LINEAR, R_YAW, R_CONSTANT):
+                b0[0] += c
+            elif op == R_JOINT_VELOCITY:
+                b0[2] += c
+            elif op == R_JOINT_ACCELERATION:
+                b0[3] += c
+            elif op == R_ACTION_RATE:
+                b1[0] += c
+            elif op in (R_LIMIT_SQUARED, R_LIMIT_ABSOLUTE, R_POSTURE_SQUARED, R_POSTURE_ABSOLUTE):
+                b1[1] += c
+            else:
+                b0[1] += c
+        steps = st.episode_step + 1
+        timeout = steps >= p.maximum_episode_steps
+        done, reason, priority, penalty = False, REASON_CONTINUING, 0, 0.0
+        for t in self.terminations:
+            trig = height < t.threshold if t.opcode == T_MIN_HEIGHT else (tilt > t.threshold if t.opcode == T_MAX_TILT else False)
+            if trig and (not done or t.priority >= priority):
+                done, reason, priority, penalty = True, t.reason, t.priority, t.failure_penalty
+        if timeout:
+            done, reason = True, REASON_TIMEOUT
+        if physics_error:
+            done, reason = True, REASON_PHYSICS_ERROR
+        if done and reason not in (REASON_TIMEOUT, REASON_PHYSICS_ERROR):
+            reward += penalty
+            b0[1] += penalty
+        reward *= dt
+        b0 *= dt
+        b1 *= dt
+        tracking = math.exp(-tracking_error / 0.25)
+        yaw_tracking = math.exp(-yaw_error / 0.25)
+        episode_tracking = st.episode_tracking + tracking
+        episode_score = episode_tracking / max(steps, 1)
+        episode_return = st.episode_return + reward
+        if not done and st.command_steps <= 1:
+            st.command = self.sample_command(env, st.episode, steps)
+            st.command_steps = self.duration_steps(env, st.episode, steps, 64)
+        elif not done:
+            st.command_steps -= 1
+        st.episode_step = steps
+        st.pending_reset = done
+        st.last_reason = reason
+        st.phase = phase
+        st.previous_height = height
+        st.episode_return = 0.0 if done else episode_return
+        st.episode_tracking = 0.0 if done else episode_tracking
+        if not done or (timeout and not physics_error):
+            st.frame = self.frame(env, q, v, st, raw_last, st.previous_joint[1], st.episode, steps)
+            for a, b in enumerate(p.actions):
+                st.previous_joint[0, a] = v[b.v_index]
+                st.previous_joint[1, a] = q[b.q_index]
+        return {
+            "reward": reward, "tracking_score": 0.5 * (tracking + yaw_tracking), "root_height": height, "tilt": tilt,
+            "done": int(done), "timeout": int(timeout), "physics_error": int(physics_error), "termination_reason": reason,
+            "task_reward": b0[0], "base_reward": b0[1], "joint_velocity_reward": b0[2], "joint_acceleration_reward": b0[3],
+            "control_reward": b1[0], "posture_reward": b1[1], "energy_reward": b1[2], "contact_reward": b1[3],
+            "episode_tracking_score": episode_score if done and not physics_error else 0.0,
+        }

@@ -67,6 +67,14 @@ def test_struct_sizes_match_header_layout(tmp_path):
         "MRQualityDiagnosticsC": native.QualityDiagnosticsC,
         "MRQualityResultC": native.QualityResultC,
         "MRBatchLaunchShapeC": native.BatchLaunchShapeC,
+        "MRTaskActionBindingC": native.TaskActionBindingC,
+        "MRTaskObservationOperatorC": native.TaskObservationOperatorC,
+        "MRTaskRewardOperatorC": native.TaskRewardOperatorC,
+        "MRTaskTerminationOperatorC": native.TaskTerminationOperatorC,
+        "MRTaskRandomizationOperatorC": native.TaskRandomizationOperatorC,
+        "MRTaskIndexGroupC": native.TaskIndexGroupC,
+        "MRTaskProgramC": native.TaskProgramC,
+        "MRTaskTransitionC": native.TaskTransitionC,
     }
     src = tmp_path / "sizes.c"
     body = "".join(f'printf("%zu\\n", sizeof({name}));' for name in records)

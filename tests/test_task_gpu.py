@@ -1,0 +1,194 @@
+"""The task layer on the device (mr_task_rollout_set_task) against its
+oracle (oracle/task.py), through the C ABI, on the 29-DoF contact world:
+
+* step by step in lockstep: each step's actor frames, and its transitions
+  (rewards and their breakdown, terminations, timeouts) computed by the
+  oracle from the device's post-step state, over short episodes with
+  observation noise, an action delay and a first-order response;
+* the drive targets: a twin rollout without a task, put in the same state
+  and given the oracle's targets, ends each step where the tasked one does;
+* a native policy reads the actor frames;
+* the installer refuses programs outside the evaluated subset, and
+  clearing the task restores [q, v] observations.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import numi_lab_b200 as nb
+from numi_lab_b200 import task as T
+from numi_lab_b200.native import MetalRoboError
+from oracle.task import TaskOracle
+
+pytestmark = pytest.mark.gpu
+
+SEED = 5
+DT = 0.02
+OBS_TOL = 2e-5     # FP32 device vs FP64 oracle, same inputs, per value (absolute, scaled by max(1, |x|))
+REWARD_TOL = 2e-5
+
+
+def _default_q(world) -> np.ndarray:
+    q, _, _ = nb.sample_reset("tree29", SEED, SEED, 0, 1)
+    dq = np.zeros(world.nq, np.float32)
+    dq[2], dq[6] = q[0, 2], 1.0
+    return dq
+
+
+def _program(world, **kw):
+    return T.locomotion_task(world.model(), _default_q(world), **kw)
+
+
+def _oracle(world, prog) -> TaskOracle:
+    rec = world.model()
+    lo = [float(np.float32(rec.dofs[b.dof].limits[0])) for b in prog.actions]
+    hi = [float(np.float32(rec.dofs[b.dof].limits[1])) for b in prog.actions]
+    return TaskOracle(prog, nq=world.nq, nv=world.nv, dt=DT, seed=world.seed, fixed_root=False, limit_lower=lo, limit_upper=hi)
+
+
+def _close(a, b, tol) -> float:
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.max(np.abs(a - b) / np.maximum(1.0, np.abs(b)))) if a.size else 0.0
+
+
+def test_task_layer_matches_oracle_step_by_step(cuda_device):
+    import torch
+
+    envs, steps = 16, 40
+    with nb.World("tree29", envs, substeps=4, velocity_iterations=8, control_dt=DT, seed=SEED) as w:
+        # Tight height and tilt limits: episodes end by timeout, height and
+        # tilt within the run.
+        prog = _program(w, maximum_episode_steps=12, noise=0.05, response_time_seconds=0.04, action_history=4,
+                        action_delay_steps=1, min_height_fraction=0.995, max_tilt=0.04)
+        w.set_task(prog)
+        assert w.observation_count == len(prog.actor)
+        o = _oracle(w, prog)
+        states = [o.new_state() for _ in range(envs)]
+        gen = torch.Generator(device="cuda").manual_seed(3)
+        seen = {"reset": 0, "timeout": 0, "height": 0, "tilt": 0}
+        worst_obs = worst_reward = 0.0
+        for k in range(steps):
+            acts = 0.6 * torch.randn((1, envs, w.action_count), device="cuda", generator=gen)
+            obs, status, _ = w.step(acts, wait=True)
+            obs = obs.cpu().numpy()[0]
+            status = status.cpu().numpy()[0]
+            q, v, _ = w.state()
+            tr = w.transitions(1)
+            a_np = acts.cpu().numpy()[0]
+            for e in range(envs):
+                reset, _, _, want = o.observe(e, states[e], None, None, False)
+                seen["reset"] += reset
+                worst_obs = max(worst_obs, _close(obs[e], want, OBS_TOL))
+                assert _close(obs[e], want, OBS_TOL) <= OBS_TOL, (k, e, int(np.argmax(np.abs(obs[e] - want))))
+                o.apply(states[e], a_np[e])
+                t = o.complete(e, states[e], q[e].astype(np.float64), v[e].astype(np.float64), int(status[e]))
+                for f in ("done", "timeout", "physics_error", "termination_reason"):
+                    assert int(tr[f][0, e]) == t[f], (k, e, f)
+                for f in ("reward", "tracking_score", "root_height", "tilt", "task_reward", "base_reward", "joint_velocity_reward",
+                          "joint_acceleration_reward", "control_reward", "posture_reward", "episode_tracking_score"):
+                    err = _close(tr[f][0, e], t[f], REWARD_TOL)
+                    worst_reward = max(worst_reward, err)
+                    assert err <= REWARD_TOL, (k, e, f, float(tr[f][0, e]), t[f])
+                seen["timeout"] += t["timeout"]
+                seen["height"] += t["termination_reason"] == 1
+                seen["tilt"] += t["termination_reason"] == 2
+        print(f"worst observation error {worst_obs:.2e}, worst transition error {worst_reward:.2e}; {seen}")
+        # The run crossed episode boundaries of each kind it can.
+        assert seen["reset"] > envs and seen["timeout"] > 0 and seen["height"] + seen["tilt"] > 0
+
+
+def test_drive_targets_match_the_oracle(cuda_device):
+    """A twin rollout without a task, set to the tasked rollout's state and
+    given the oracle's drive targets, lands where the tasked one does."""
+
+    import torch
+
+    envs, steps = 8, 10
+    with nb.World("tree29", envs, substeps=4, velocity_iterations=8, control_dt=DT, seed=SEED) as a, \
+            nb.World("tree29", envs, substeps=4, velocity_iterations=8, control_dt=DT, seed=SEED) as b:
+        prog = _program(a, response_time_seconds=0.03, action_history=4, action_delay_steps=1)
+        a.set_task(prog)
+        o = _oracle(a, prog)
+        states = [o.new_state() for _ in range(envs)]
+        gen = torch.Generator(device="cuda").manual_seed(9)
+        compared = 0
+        for k in range(steps):
+            qa, va, ma = a.state()
+            acts = 0.8 * torch.randn((1, envs, a.action_count), device="cuda", generator=gen)
+            _, status, _ = a.step(acts, wait=True)
+            a_np = acts.cpu().numpy()[0]
+            targets = np.zeros((envs, a.action_count), np.float32)
+            fresh = []
+            for e in range(envs):
+                reset, _, _, _ = o.observe(e, states[e], None, None, False)
+                fresh.append(reset)
+                targets[e] = o.apply(states[e], a_np[e])
+            qa1, va1, _ = a.state()
+            for e in range(envs):
+                o.complete(e, states[e], qa1[e].astype(np.float64), va1[e].astype(np.float64), int(status[0, e]))
+            b.set_state(qa, va, ma)
+            b.step(torch.tensor(targets[None], device="cuda"), wait=True)
+            qb1, vb1, _ = b.state()
+            for e in range(envs):
+                if fresh[e]:
+                    continue  # the tasked rollout started this step from its task's reset state
+                assert _close(qb1[e], qa1[e], 1e-5) <= 1e-5, (k, e)
+                assert _close(vb1[e], va1[e], 1e-4) <= 1e-4, (k, e)
+                compared += 1
+        assert compared >= envs * (steps - 2)
+
+
+def test_policy_reads_the_actor_frames(cuda_device):
+    from oracle import policy as ref
+
+    rng = np.random.default_rng(4)
+    envs, steps = 32, 4
+    with nb.World("tree29", envs, substeps=4, velocity_iterations=8, control_dt=DT, seed=SEED) as w:
+        prog = _program(w, noise=0.02)
+        w.set_task(prog)
+        nobs, na = w.observation_count, w.action_count
+        layers = []
+        for (n_in, n_out), act in zip(zip([nobs, 128, 64], [128, 64, na]), ["elu", "tanh", "identity"]):
+            layers.append((rng.normal(0.0, 1.0 / np.sqrt(n_in), (n_out, n_in)).astype(np.float32),
+                           rng.normal(0.0, 0.1, n_out).astype(np.float32), act))
+        w.set_policy(layers=layers, revision=3, action_clip=1.0)
+        obs, status = w.step_policy(steps)
+        out = w.policy_outputs()
+        tr = w.transitions(steps)
+        frames = obs.cpu().numpy().astype(np.float64)
+        for k in range(steps):
+            want = ref.forward(frames[k], layers)
+            assert float(np.max(np.abs(out["latents"][k] - want))) <= 1e-4
+        assert np.all(tr["policy_revision"] == 3)
+
+
+def test_installer_refuses_programs_outside_the_subset(cuda_device):
+    with nb.World("tree29", 4, seed=SEED) as w:
+        base = _program(w)
+        bad = [
+            dict(actions=base.actions[:-1]),
+            dict(actor=base.actor + [T.Observation(16)]),
+            dict(actor=base.actor + [T.Observation(T.OBSERVE["joint_velocity"], source=99)]),
+            dict(actor=base.actor + [T.Observation(T.OBSERVE["delayed_action"], source=0, component=5)]),
+            dict(rewards=base.rewards + [T.Reward(11, -1.0)]),
+            dict(rewards=base.rewards + [T.Reward(T.REWARD["joint_group_posture_squared"], -1.0, group=7)]),
+            dict(terminations=[T.Termination(2, 3, 1, 0.5)]),
+            dict(randomization=[T.Randomization(4)]),
+            dict(action_history=2),
+            dict(default_q=base.default_q[:-1]),
+        ]
+        for change in bad:
+            prog = T.TaskProgram(**{**base.__dict__, **change})
+            with pytest.raises(MetalRoboError, match="task program"):
+                w.set_task(prog)
+        w.set_task(base)
+        assert w.observation_count == len(base.actor)
+        w.clear_task()
+        assert w.observation_count == w.nq + w.nv
+        import torch
+
+        obs, status, _ = w.step(torch.zeros((1, 4, w.action_count), device="cuda"), wait=True)
+        q, v, _ = w.state()
+        np.testing.assert_array_equal(obs.cpu().numpy()[0], np.concatenate([q, v], axis=1))
