@@ -619,6 +619,91 @@ MR_API int mr_task_rollout_copy_final_scene_states(
     const MRTaskRolloutHandle* handle, float* output, size_t output_count);
 
 /* ---------------------------------------------------------------------- */
+/* PolicyRolloutPack files (reference: c_api.h:374-394, 750-755;           */
+/* include/metalrobo/LearningPacks.hpp:54-105, src/core/LearningPacks.cpp) */
+/* ---------------------------------------------------------------------- */
+
+typedef struct MRTaskTransitionC MRTaskTransitionC;
+
+/* reference: c_api.h:374-394 (same shape).  Tables [control step][env]
+ * (x features); teacher actions and motion features may be empty. */
+typedef struct MRPolicyRolloutBatchC {
+    uint32_t control_step_count;
+    const float* actor_observations;
+    size_t actor_observation_count;
+    const float* critic_observations;
+    size_t critic_observation_count;
+    const float* motion_features;
+    size_t motion_feature_count;
+    const float* teacher_actions;
+    size_t teacher_action_count;
+    const float* latents;
+    size_t latent_count;
+    const float* log_probabilities;
+    size_t log_probability_count;
+    const float* values;
+    size_t value_count;
+    const float* bootstrap_values;
+    size_t bootstrap_value_count;
+    const MRTaskTransitionC* transitions;
+    size_t transition_count;
+} MRPolicyRolloutBatchC;
+
+/* No counterpart in the reference's C ABI (its PolicyRolloutPackView,
+ * LearningPacks.hpp:83-105, without the outcome schema): a rollout pack
+ * written without a rollout. */
+typedef struct MRPolicyRolloutPackC {
+    const char* id;
+    uint64_t task_fingerprint;
+    uint64_t policy_fingerprint;
+    uint64_t policy_revision;
+    uint32_t environment_count;
+    uint32_t actor_observation_count;
+    uint32_t critic_observation_count;
+    uint32_t action_count;
+    uint32_t motion_feature_count;
+    uint32_t reserved;
+    const MRPolicyRolloutBatchC* batch;
+} MRPolicyRolloutPackC;
+
+typedef struct MRPolicyRolloutPackInfoC {
+    uint64_t task_fingerprint;
+    uint64_t policy_fingerprint;
+    uint64_t policy_revision;
+    uint64_t content_hash;
+    uint32_t environment_count;
+    uint32_t control_step_count;
+    uint32_t actor_observation_count;
+    uint32_t critic_observation_count;
+    uint32_t action_count;
+    uint32_t motion_feature_count;
+    uint32_t outcome_count;
+    uint32_t has_teacher_actions;
+    uint64_t transition_count;
+    double reward_sum;              /* over every transition */
+    uint64_t done_count;
+    char id[64];                    /* truncated, NUL-terminated */
+} MRPolicyRolloutPackInfoC;
+
+/* reference: c_api.h:750-755.  Publishes a batch collected from this
+ * rollout: fingerprints, revision and dimensions come from the installed
+ * task and policy (a policy is required; the task's actor frame is both
+ * the actor and the critic observation; no outcome schema).  Task
+ * transitions become learner transitions (reward and timeout bootstrap,
+ * termination, context, revision) as c_api.cpp:4410-4445 does. */
+MR_API int mr_task_rollout_write_policy_rollout_pack(const MRTaskRolloutHandle* handle, const MRPolicyRolloutBatchC* batch,
+                                                     const char* batch_id, const char* output_path);
+/* No counterpart in the reference: the same file from explicit identity,
+ * fingerprints and dimensions; the artifact rules of the reference's
+ * writer (LearningPacks.cpp:726-918) apply. */
+MR_API int mr_write_policy_rollout_pack(const MRPolicyRolloutPackC* pack, const char* output_path);
+/* No counterpart in the reference: reads and checks a PolicyRolloutPack;
+ * `parameters` (optional, `capacity` floats) receives the actor
+ * observations, latents, log-probabilities, values and bootstrap values in
+ * that order. */
+MR_API int mr_policy_rollout_pack_inspect(const char* path, MRPolicyRolloutPackInfoC* info, float* parameters, size_t capacity);
+
+/* ---------------------------------------------------------------------- */
 /* Task layer (reference: include/metalrobo/task_program_types.h,         */
 /* src/metal/LocomotionTask.metal observe / apply_actions / complete)      */
 /* ---------------------------------------------------------------------- */
@@ -627,7 +712,10 @@ MR_API int mr_task_rollout_copy_final_scene_states(
  * MRTaskRewardOpcode, MRTaskTerminationOpcode, MRTaskTerminationReason and
  * MRTaskRandomizationOpcode (task_program_types.h:68-300), same values.
  * The task layer evaluates the subset listed here; mr_task_rollout_set_task
- * refuses any other code. */
+ * refuses any other code.  A translation unit that already included the
+ * reference's task_program_types.h (which defines
+ * MR_TASK_PROGRAM_ABI_VERSION) keeps its identical definitions. */
+#ifndef MR_TASK_PROGRAM_ABI_VERSION
 enum {
     MR_TASK_OBSERVE_ROOT_ANGULAR_VELOCITY_LOCAL = 0u,
     MR_TASK_OBSERVE_PROJECTED_GRAVITY = 1u,
@@ -683,6 +771,7 @@ enum {
     MR_TASK_RANDOMIZE_ROOT_HEIGHT = 10u,
     MR_TASK_RANDOMIZE_JOINT_POSITION = 12u
 };
+#endif /* MR_TASK_PROGRAM_ABI_VERSION */
 
 /* reference: MRTaskActionBindingGPU (task_program_types.h:443-458), the
  * joint-position actuator.  Action `index` of the policy sets the drive
@@ -786,7 +875,7 @@ typedef struct MRTaskProgramC {
 } MRTaskProgramC;
 
 /* reference: include/metalrobo/c_api.h:261-295 (same layout, 128 bytes). */
-typedef struct MRTaskTransitionC {
+struct MRTaskTransitionC {
     float reward;
     float tracking_score;
     float root_height;
@@ -818,7 +907,7 @@ typedef struct MRTaskTransitionC {
     uint32_t terrain_level;
     uint32_t impact_sequence_index;
     uint32_t impact_event_flags;
-} MRTaskTransitionC;
+};
 
 /* No counterpart in the reference's C ABI, which compiles its task from the
  * run manifest's TaskPack; this installs a compiled task program on an

@@ -61,4 +61,12 @@ cudaError_t launch_mix_horizon(int family, const MixWorld* worlds, int world_cou
                                int item_count, unsigned* next_item, int warps_per_block, int smem_floats_per_warp, int grid,
                                cudaStream_t stream);
 
+// The free-body family kernels (scene_step.cu); `convex`: the instance with
+// the support-mapped narrowphase.
+cudaError_t configure_mix_scene_kernel(bool convex, size_t max_dynamic_smem);
+cudaError_t mix_scene_occupancy(bool convex, int warps_per_block, size_t smem_per_block, int* blocks_per_sm);
+cudaError_t launch_mix_scene(bool convex, const MixWorld* worlds, int world_count, int steps, const std::uint32_t* items,
+                             int item_count, unsigned* next_item, int warps_per_block, int smem_floats_per_warp, int grid,
+                             cudaStream_t stream);
+
 }  // namespace numi

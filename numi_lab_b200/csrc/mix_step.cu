@@ -62,13 +62,13 @@ __global__ void __launch_bounds__(128, 3) mix_step_kernel(const MixWorld* __rest
 
 // Per-family variants: the same env-major claim loop over one family's
 // items only, each compiled to its own register budget -- the articulated
-// one like the articulated kernel (3 CTAs of 4 warps), the free-body one
-// like the scene kernel (16 resident warps, at most 128 registers) -- so a
-// batch can run each family at its own kernel's occupancy.
-template <bool kScene, bool kConvex>
-__device__ __forceinline__ void family_loop(const MixWorld* __restrict__ worlds, int world_count, int steps,
-                                            const std::uint32_t* __restrict__ items, int item_count, unsigned* next_item,
-                                            int smem_floats_per_warp) {
+// one like the articulated kernel (3 CTAs of 4 warps) here, the free-body
+// one like the scene kernel (16 resident warps, at most 128 registers) in
+// scene_step.cu, beside the per-world scene kernel -- so a batch can run
+// each family at its own kernel's occupancy.
+__global__ void __launch_bounds__(128, 3) mix_articulated_kernel(const MixWorld* __restrict__ worlds, int world_count, int steps,
+                                                                 const std::uint32_t* __restrict__ items, int item_count,
+                                                                 unsigned* next_item, int smem_floats_per_warp) {
     extern __shared__ float4 smem4[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -81,50 +81,29 @@ __device__ __forceinline__ void family_loop(const MixWorld* __restrict__ worlds,
         const std::uint32_t code = items[claimed];
         const int world = static_cast<int>(code >> kMixWorldShift);
         const int env = static_cast<int>(code & kMixEnvMask);
-        if (kScene) {
-            for (int k = 0; k < steps; ++k) {
-                scene_step_item<false, kConvex>(worlds[static_cast<size_t>(k) * world_count + world].scene, base, env, env);
-                __syncwarp();
-            }
-        } else {
-            WarpLayout* L = reinterpret_cast<WarpLayout*>(base);
-            if (lane < static_cast<int>(sizeof(WarpLayout) / 4))
-                reinterpret_cast<int*>(L)[lane] = reinterpret_cast<const int*>(&worlds[world].layout)[lane];
+        WarpLayout* L = reinterpret_cast<WarpLayout*>(base);
+        if (lane < static_cast<int>(sizeof(WarpLayout) / 4))
+            reinterpret_cast<int*>(L)[lane] = reinterpret_cast<const int*>(&worlds[world].layout)[lane];
+        __syncwarp();
+        const bool contact = worlds[world].kind == kMixContact;
+        for (int k = 0; k < steps; ++k) {
+            const MixWorld& W = worlds[static_cast<size_t>(k) * world_count + world];
+            if (contact)
+                control_step_item<true, float, false>(W.step, *L, &W.step.model->tables, base + kLayoutFloats, env, env);
+            else
+                control_step_item<false, float, false>(W.step, *L, &W.step.model->tables, base + kLayoutFloats, env, env);
             __syncwarp();
-            const bool contact = worlds[world].kind == kMixContact;
-            for (int k = 0; k < steps; ++k) {
-                const MixWorld& W = worlds[static_cast<size_t>(k) * world_count + world];
-                if (contact)
-                    control_step_item<true, float, false>(W.step, *L, &W.step.model->tables, base + kLayoutFloats, env, env);
-                else
-                    control_step_item<false, float, false>(W.step, *L, &W.step.model->tables, base + kLayoutFloats, env, env);
-                __syncwarp();
-            }
         }
     }
-}
-
-__global__ void __launch_bounds__(128, 3) mix_articulated_kernel(const MixWorld* __restrict__ worlds, int world_count, int steps,
-                                                                 const std::uint32_t* __restrict__ items, int item_count,
-                                                                 unsigned* next_item, int smem_floats_per_warp) {
-    family_loop<false, false>(worlds, world_count, steps, items, item_count, next_item, smem_floats_per_warp);
-}
-
-// kConvex: some free-body world has support-mapped (GJK / EPA) pairs.
-template <bool kConvex>
-__global__ void __launch_bounds__(32, 16) mix_scene_kernel(const MixWorld* __restrict__ worlds, int world_count, int steps,
-                                                           const std::uint32_t* __restrict__ items, int item_count,
-                                                           unsigned* next_item, int smem_floats_per_warp) {
-    family_loop<true, kConvex>(worlds, world_count, steps, items, item_count, next_item, smem_floats_per_warp);
 }
 
 template <typename F>
 cudaError_t for_mix_kernel(int family, F&& f) {
     if (family == kMixFamilyArticulated) return f(mix_articulated_kernel);
-    if (family == kMixFamilyScene) return f(mix_scene_kernel<false>);
-    if (family == kMixFamilySceneConvex) return f(mix_scene_kernel<true>);
     return f(mix_step_kernel);
 }
+
+bool scene_family(int family) { return family == kMixFamilyScene || family == kMixFamilySceneConvex; }
 
 }  // namespace
 
@@ -132,12 +111,14 @@ int mix_articulated_warp_floats(const WarpLayout& layout) { return kLayoutFloats
 int mix_scene_warp_floats() { return static_cast<int>(scene_step_smem_bytes(false) / sizeof(float)); }
 
 cudaError_t configure_mix_kernel(int family, size_t max_dynamic_smem) {
+    if (scene_family(family)) return configure_mix_scene_kernel(family == kMixFamilySceneConvex, max_dynamic_smem);
     return for_mix_kernel(family, [&](auto kernel) {
         return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(max_dynamic_smem));
     });
 }
 
 cudaError_t mix_occupancy(int family, int warps_per_block, size_t smem_per_block, int* blocks_per_sm) {
+    if (scene_family(family)) return mix_scene_occupancy(family == kMixFamilySceneConvex, warps_per_block, smem_per_block, blocks_per_sm);
     return for_mix_kernel(family, [&](auto kernel) {
         return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, 32 * warps_per_block, smem_per_block);
     });
@@ -150,6 +131,9 @@ cudaError_t launch_mix_horizon(int family, const MixWorld* worlds, int world_cou
     if (warps_per_block < 1 || warps_per_block > max_warps || grid < 1 || steps < 1 || world_count < 1 ||
         smem_floats_per_warp < kLayoutFloats || (smem_floats_per_warp & 3) != 0)
         return cudaErrorInvalidValue;
+    if (scene_family(family))
+        return launch_mix_scene(family == kMixFamilySceneConvex, worlds, world_count, steps, items, item_count, next_item,
+                                warps_per_block, smem_floats_per_warp, grid, stream);
     const size_t smem = static_cast<size_t>(smem_floats_per_warp) * sizeof(float) * warps_per_block;
     return for_mix_kernel(family, [&](auto kernel) {
         kernel<<<grid, 32 * warps_per_block, smem, stream>>>(worlds, world_count, steps, items, item_count, next_item,

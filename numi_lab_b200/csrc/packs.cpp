@@ -1,7 +1,11 @@
-// PolicyPack reading and writing (packs.h) and the C-ABI entry points that
-// need no rollout: mr_write_policy_pack, mr_learning_pack_content_hash and
-// mr_policy_pack_inspect.  mr_task_rollout_load_policy_pack (rollout.cu)
-// reads through read_policy_pack and installs like mr_task_rollout_set_policy.
+// PolicyPack and PolicyRolloutPack reading and writing (packs.h) and the
+// C-ABI entry points that need no rollout: mr_write_policy_pack,
+// mr_learning_pack_content_hash, mr_policy_pack_inspect,
+// mr_write_policy_rollout_pack and mr_policy_rollout_pack_inspect.
+// mr_task_rollout_load_policy_pack (rollout.cu) reads through
+// read_policy_pack and installs like mr_task_rollout_set_policy;
+// mr_task_rollout_write_policy_rollout_pack (rollout.cu) writes through
+// write_policy_rollout_pack.
 #include "packs.h"
 
 #include <cerrno>
@@ -264,20 +268,20 @@ void validate_policy_pack(const PolicyPackData& d) {
         throw std::invalid_argument("PolicyPack normalisation and action tables must be finite");
 }
 
-void write_policy_pack(const PolicyPackData& d, const std::string& path) {
-    if (path.empty()) throw std::invalid_argument("PolicyPack output path is empty");
-    validate_policy_pack(d);
-    const std::vector<std::uint8_t> payload = encode(d);
-    if (payload.size() > kMaxPayload) throw std::invalid_argument("PolicyPack payload exceeds 4 GiB");
+namespace {
+
+// Atomically publishes header + payload: a sibling temporary, flushed, renamed.
+void publish_pack(const std::vector<std::uint8_t>& payload, std::uint32_t kind, std::uint32_t version, const std::string& path,
+                  const char* what) {
+    if (path.empty()) throw std::invalid_argument(std::string(what) + " output path is empty");
+    if (payload.size() > kMaxPayload) throw std::invalid_argument(std::string(what) + " payload exceeds 4 GiB");
     std::uint8_t header[kHeaderBytes];
-    const std::uint32_t version = kPolicyPackVersion, kind = kPolicyPackKind;
     const std::uint64_t bytes = payload.size(), hash = learning_pack_hash(payload.data(), payload.size());
     std::memcpy(header, kMagic, 8);
     std::memcpy(header + 8, &version, 4);
     std::memcpy(header + 12, &kind, 4);
     std::memcpy(header + 16, &bytes, 8);
     std::memcpy(header + 24, &hash, 8);
-    // Publish atomically: write a sibling temporary, flush it, rename it.
     std::string tmpl = path + ".tmp.XXXXXX";
     std::vector<char> name(tmpl.begin(), tmpl.end());
     name.push_back('\0');
@@ -305,42 +309,258 @@ void write_policy_pack(const PolicyPackData& d, const std::string& path) {
     }
 }
 
-PolicyPackData read_policy_pack(const std::string& path) {
+struct LoadedPack {
+    std::vector<std::uint8_t> payload;
+    std::uint32_t version = 0;
+    std::uint64_t hash = 0;
+};
+
+// Reads a pack of `kind` and version in [oldest, newest], checking the
+// length and the payload hash.
+LoadedPack load_pack(const std::string& path, std::uint32_t kind, std::uint32_t oldest, std::uint32_t newest, const char* what) {
     std::ifstream in(path, std::ios::binary | std::ios::ate);
-    if (!in) throw std::invalid_argument("cannot open PolicyPack " + path);
+    if (!in) throw std::invalid_argument(std::string("cannot open ") + what + " " + path);
     const std::streamoff size = in.tellg();
     if (size < static_cast<std::streamoff>(kHeaderBytes) || static_cast<std::uint64_t>(size) > kHeaderBytes + kMaxPayload)
-        throw std::invalid_argument("PolicyPack " + path + " has an invalid length");
+        throw std::invalid_argument(std::string(what) + " " + path + " has an invalid length");
     in.seekg(0);
     std::uint8_t header[kHeaderBytes];
-    if (!in.read(reinterpret_cast<char*>(header), kHeaderBytes)) throw std::invalid_argument("cannot read the PolicyPack header");
-    std::uint32_t version = 0, kind = 0;
-    std::uint64_t bytes = 0, hash = 0;
-    std::memcpy(&version, header + 8, 4);
-    std::memcpy(&kind, header + 12, 4);
+    if (!in.read(reinterpret_cast<char*>(header), kHeaderBytes)) throw std::invalid_argument(std::string("cannot read the ") + what + " header");
+    LoadedPack out;
+    std::uint32_t file_kind = 0;
+    std::uint64_t bytes = 0;
+    std::memcpy(&out.version, header + 8, 4);
+    std::memcpy(&file_kind, header + 12, 4);
     std::memcpy(&bytes, header + 16, 8);
-    std::memcpy(&hash, header + 24, 8);
-    if (std::memcmp(header, kMagic, 8) != 0 || kind != kPolicyPackKind)
-        throw std::invalid_argument("not a PolicyPack (learning-pack magic or artifact kind differs)");
-    if (version < kPolicyPackOldestVersion || version > kPolicyPackVersion)
-        throw std::invalid_argument("PolicyPack format version " + std::to_string(version) + " is not supported (3-4)");
+    std::memcpy(&out.hash, header + 24, 8);
+    if (std::memcmp(header, kMagic, 8) != 0 || file_kind != kind)
+        throw std::invalid_argument(std::string("not a ") + what + " (learning-pack magic or artifact kind differs)");
+    if (out.version < oldest || out.version > newest)
+        throw std::invalid_argument(std::string(what) + " format version " + std::to_string(out.version) + " is not supported (" +
+                                    std::to_string(oldest) + (oldest == newest ? "" : "-" + std::to_string(newest)) + ")");
     if (bytes != static_cast<std::uint64_t>(size) - kHeaderBytes)
-        throw std::invalid_argument("PolicyPack payload length does not match the file");
-    std::vector<std::uint8_t> payload(static_cast<std::size_t>(bytes));
-    if (bytes && !in.read(reinterpret_cast<char*>(payload.data()), static_cast<std::streamsize>(bytes)))
-        throw std::invalid_argument("cannot read the PolicyPack payload");
-    if (learning_pack_hash(payload.data(), payload.size()) != hash)
-        throw std::invalid_argument("PolicyPack payload hash does not match its header (corrupt file)");
+        throw std::invalid_argument(std::string(what) + " payload length does not match the file");
+    out.payload.resize(static_cast<std::size_t>(bytes));
+    if (bytes && !in.read(reinterpret_cast<char*>(out.payload.data()), static_cast<std::streamsize>(bytes)))
+        throw std::invalid_argument(std::string("cannot read the ") + what + " payload");
+    if (learning_pack_hash(out.payload.data(), out.payload.size()) != out.hash)
+        throw std::invalid_argument(std::string(what) + " payload hash does not match its header (corrupt file)");
+    return out;
+}
+
+std::vector<std::uint8_t> encode_rollout(const PolicyRolloutPackData& d) {
+    Sink s;
+    s.text(d.id);
+    s.u64(d.task_fingerprint);
+    s.u64(d.policy_fingerprint);
+    s.u64(d.policy_revision);
+    s.u32(d.environment_count);
+    s.u32(d.control_step_count);
+    s.u32(d.actor_observation_count);
+    s.u32(d.critic_observation_count);
+    s.u32(d.action_count);
+    s.u32(d.motion_feature_count);
+    for (const std::vector<float>* v : {&d.actor_observations, &d.critic_observations, &d.motion_features, &d.teacher_actions,
+                                        &d.latents, &d.log_probabilities, &d.values, &d.bootstrap_values})
+        s.floats(*v);
+    s.u64(d.outcomes.size());
+    for (const PolicyOutcome& o : d.outcomes) {
+        s.text(o.id);
+        s.text(o.unit);
+        s.u32(o.direction);
+    }
+    s.floats(d.outcome_values);
+    s.u64(d.transitions.size());
+    if (!d.transitions.empty()) s.raw(d.transitions.data(), d.transitions.size() * sizeof(LearningTransition));
+    return s.bytes;
+}
+
+bool decode_rollout(const std::uint8_t* bytes, std::size_t count, PolicyRolloutPackData& d) {
+    Source s{bytes, count};
+    if (!(s.text(d.id) && s.u64(d.task_fingerprint) && s.u64(d.policy_fingerprint) && s.u64(d.policy_revision) &&
+          s.u32(d.environment_count) && s.u32(d.control_step_count) && s.u32(d.actor_observation_count) &&
+          s.u32(d.critic_observation_count) && s.u32(d.action_count) && s.u32(d.motion_feature_count)))
+        return false;
+    for (std::vector<float>* v : {&d.actor_observations, &d.critic_observations, &d.motion_features, &d.teacher_actions, &d.latents,
+                                  &d.log_probabilities, &d.values, &d.bootstrap_values})
+        if (!s.floats(*v)) return false;
+    std::uint64_t outcomes = 0;
+    // Each outcome takes at least 20 bytes: a corrupt count fails here.
+    if (!s.u64(outcomes) || outcomes > (s.n - s.at) / 20) return false;
+    d.outcomes.resize(static_cast<std::size_t>(outcomes));
+    for (PolicyOutcome& o : d.outcomes)
+        if (!s.text(o.id) || !s.text(o.unit) || !s.u32(o.direction)) return false;
+    std::uint64_t transitions = 0;
+    if (!s.floats(d.outcome_values) || !s.u64(transitions) || transitions > (s.n - s.at) / sizeof(LearningTransition)) return false;
+    d.transitions.resize(static_cast<std::size_t>(transitions));
+    return (transitions == 0 || s.raw(d.transitions.data(), d.transitions.size() * sizeof(LearningTransition))) && s.done();
+}
+
+}  // namespace
+
+void write_policy_pack(const PolicyPackData& d, const std::string& path) {
+    if (path.empty()) throw std::invalid_argument("PolicyPack output path is empty");
+    validate_policy_pack(d);
+    publish_pack(encode(d), kPolicyPackKind, kPolicyPackVersion, path, "PolicyPack");
+}
+
+PolicyPackData read_policy_pack(const std::string& path) {
+    LoadedPack f = load_pack(path, kPolicyPackKind, kPolicyPackOldestVersion, kPolicyPackVersion, "PolicyPack");
     PolicyPackData d;
-    if (!decode(payload.data(), payload.size(), version, d)) throw std::invalid_argument("PolicyPack payload is malformed");
-    d.format_version = version;
-    d.content_hash = hash;
+    if (!decode(f.payload.data(), f.payload.size(), f.version, d)) throw std::invalid_argument("PolicyPack payload is malformed");
+    d.format_version = f.version;
+    d.content_hash = f.hash;
+    return d;
+}
+
+std::uint64_t policy_pack_payload_hash(const PolicyPackData& d) {
+    const std::vector<std::uint8_t> payload = encode(d);
+    return learning_pack_hash(payload.data(), payload.size());
+}
+
+LearningTransition learning_transition(const MRTaskTransitionC& t) {
+    LearningTransition l{};
+    l.reward = t.reward;
+    l.timeout_bootstrap_value = t.timeout_bootstrap_value;
+    l.done = t.done;
+    l.timeout = t.timeout;
+    l.physics_error = t.physics_error;
+    l.termination_reason = t.termination_reason;
+    l.difficulty_band = t.difficulty_band;
+    l.terrain_level = t.terrain_level;
+    l.impact_sequence_index = t.impact_sequence_index;
+    l.impact_event_flags = t.impact_event_flags;
+    l.policy_revision = t.policy_revision;
+    return l;
+}
+
+PolicyRolloutPackData policy_rollout_pack_from_c(const MRPolicyRolloutPackC& c) {
+    if (!c.batch) throw std::invalid_argument("policy rollout batch is null");
+    const MRPolicyRolloutBatchC& b = *c.batch;
+    PolicyRolloutPackData d;
+    d.id = c.id ? c.id : "";
+    d.task_fingerprint = c.task_fingerprint;
+    d.policy_fingerprint = c.policy_fingerprint;
+    d.policy_revision = c.policy_revision;
+    d.environment_count = c.environment_count;
+    d.control_step_count = b.control_step_count;
+    d.actor_observation_count = c.actor_observation_count;
+    d.critic_observation_count = c.critic_observation_count;
+    d.action_count = c.action_count;
+    d.motion_feature_count = c.motion_feature_count;
+    copy_floats(d.actor_observations, b.actor_observations, b.actor_observation_count, "rollout actor observations");
+    copy_floats(d.critic_observations, b.critic_observations, b.critic_observation_count, "rollout critic observations");
+    copy_floats(d.motion_features, b.motion_features, b.motion_feature_count, "rollout motion features");
+    copy_floats(d.teacher_actions, b.teacher_actions, b.teacher_action_count, "rollout teacher actions");
+    copy_floats(d.latents, b.latents, b.latent_count, "rollout latents");
+    copy_floats(d.log_probabilities, b.log_probabilities, b.log_probability_count, "rollout log probabilities");
+    copy_floats(d.values, b.values, b.value_count, "rollout values");
+    copy_floats(d.bootstrap_values, b.bootstrap_values, b.bootstrap_value_count, "rollout bootstrap values");
+    if (b.transition_count != 0 && !b.transitions) throw std::invalid_argument("rollout transition pointer is null");
+    d.transitions.reserve(b.transition_count);
+    for (size_t i = 0; i < b.transition_count; ++i) d.transitions.push_back(learning_transition(b.transitions[i]));
+    return d;
+}
+
+void validate_policy_rollout_pack(const PolicyRolloutPackData& d) {
+    auto need = [](bool ok, const char* what) {
+        if (!ok) throw std::invalid_argument(what);
+    };
+    need(!d.id.empty() && d.id.size() <= kMaxPayload && d.task_fingerprint != 0 && d.policy_fingerprint != 0 &&
+             d.policy_revision != 0 && d.environment_count != 0 && d.control_step_count != 0 && d.actor_observation_count != 0 &&
+             d.critic_observation_count != 0 && d.action_count != 0,
+         "PolicyRolloutPack identity, fingerprints, or dimensions are invalid");
+    const std::uint64_t samples = static_cast<std::uint64_t>(d.environment_count) * d.control_step_count;
+    auto elements = [&](std::uint32_t per) { return samples * per; };  // counts are 32-bit: no overflow in 64 bits
+    bool outcomes_ok = true;
+    for (const PolicyOutcome& o : d.outcomes) outcomes_ok = outcomes_ok && !o.id.empty() && o.direction <= 2u;
+    need(d.actor_observations.size() == elements(d.actor_observation_count) &&
+             d.critic_observations.size() == elements(d.critic_observation_count) &&
+             d.motion_features.size() == elements(d.motion_feature_count) &&
+             (d.teacher_actions.empty() || d.teacher_actions.size() == elements(d.action_count)) &&
+             d.latents.size() == elements(d.action_count) && d.log_probabilities.size() == samples && d.values.size() == samples &&
+             d.bootstrap_values.size() == d.environment_count && d.transitions.size() == samples &&
+             d.outcome_values.size() == samples * d.outcomes.size() && outcomes_ok,
+         "PolicyRolloutPack tensors do not match its declared dimensions");
+    bool ok = finite(d.actor_observations) && finite(d.critic_observations) && finite(d.motion_features) && finite(d.teacher_actions) &&
+              finite(d.latents) && finite(d.log_probabilities) && finite(d.values) && finite(d.bootstrap_values) &&
+              finite(d.outcome_values);
+    for (const LearningTransition& t : d.transitions)
+        ok = ok && t.policy_revision == d.policy_revision && std::isfinite(t.reward) && std::isfinite(t.timeout_bootstrap_value) &&
+             t.done <= 1u && t.timeout <= 1u && t.physics_error <= 1u;
+    need(ok, "PolicyRolloutPack contains non-finite or inconsistent samples");
+}
+
+void write_policy_rollout_pack(const PolicyRolloutPackData& d, const std::string& path) {
+    if (path.empty()) throw std::invalid_argument("PolicyRolloutPack output path is empty");
+    validate_policy_rollout_pack(d);
+    publish_pack(encode_rollout(d), kPolicyRolloutPackKind, kPolicyRolloutPackVersion, path, "PolicyRolloutPack");
+}
+
+PolicyRolloutPackData read_policy_rollout_pack(const std::string& path) {
+    LoadedPack f = load_pack(path, kPolicyRolloutPackKind, kPolicyRolloutPackVersion, kPolicyRolloutPackVersion, "PolicyRolloutPack");
+    PolicyRolloutPackData d;
+    if (!decode_rollout(f.payload.data(), f.payload.size(), d)) throw std::invalid_argument("PolicyRolloutPack payload is malformed");
+    validate_policy_rollout_pack(d);
+    d.content_hash = f.hash;
     return d;
 }
 
 }  // namespace numi
 
 extern "C" {
+
+MR_API int mr_write_policy_rollout_pack(const MRPolicyRolloutPackC* pack, const char* output_path) {
+    try {
+        if (!pack) throw std::invalid_argument("policy rollout pack is null");
+        if (!output_path || !output_path[0]) throw std::invalid_argument("PolicyRolloutPack output path is empty");
+        numi::write_policy_rollout_pack(numi::policy_rollout_pack_from_c(*pack), output_path);
+        return 0;
+    } catch (const std::exception& e) {
+        numi::rt::set_last_error(e.what());
+        return -1;
+    }
+}
+
+MR_API int mr_policy_rollout_pack_inspect(const char* path, MRPolicyRolloutPackInfoC* info, float* parameters, size_t capacity) {
+    try {
+        if (!path || !path[0]) throw std::invalid_argument("PolicyRolloutPack path is empty");
+        if (!info) throw std::invalid_argument("info is null");
+        const numi::PolicyRolloutPackData d = numi::read_policy_rollout_pack(path);
+        MRPolicyRolloutPackInfoC o{};
+        o.task_fingerprint = d.task_fingerprint;
+        o.policy_fingerprint = d.policy_fingerprint;
+        o.policy_revision = d.policy_revision;
+        o.content_hash = d.content_hash;
+        o.environment_count = d.environment_count;
+        o.control_step_count = d.control_step_count;
+        o.actor_observation_count = d.actor_observation_count;
+        o.critic_observation_count = d.critic_observation_count;
+        o.action_count = d.action_count;
+        o.motion_feature_count = d.motion_feature_count;
+        o.outcome_count = static_cast<uint32_t>(d.outcomes.size());
+        o.has_teacher_actions = d.teacher_actions.empty() ? 0u : 1u;
+        o.transition_count = d.transitions.size();
+        for (const numi::LearningTransition& t : d.transitions) {
+            o.reward_sum += t.reward;
+            o.done_count += t.done;
+        }
+        std::snprintf(o.id, sizeof(o.id), "%s", d.id.c_str());
+        if (parameters) {
+            size_t at = 0;
+            for (const std::vector<float>* v : {&d.actor_observations, &d.latents, &d.log_probabilities, &d.values, &d.bootstrap_values}) {
+                if (v->size() > capacity - at) throw std::invalid_argument("parameters capacity is too small");
+                std::memcpy(parameters + at, v->data(), v->size() * sizeof(float));
+                at += v->size();
+            }
+        }
+        *info = o;
+        return 0;
+    } catch (const std::exception& e) {
+        numi::rt::set_last_error(e.what());
+        return -1;
+    }
+}
 
 MR_API int mr_write_policy_pack(const MRPolicyPackC* policy, const char* policy_pack_path) {
     try {

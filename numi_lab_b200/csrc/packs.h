@@ -67,5 +67,56 @@ void validate_policy_pack(const PolicyPackData& d);
 void write_policy_pack(const PolicyPackData& d, const std::string& path);
 // Reads and checks a version 3 or 4 pack; throws with a message.
 PolicyPackData read_policy_pack(const std::string& path);
+// FNV-1a 64 of a pack's payload as this library encodes it (version 4):
+// the installed policy's fingerprint.
+std::uint64_t policy_pack_payload_hash(const PolicyPackData& d);
+
+// PolicyRolloutPack files (reference: include/metalrobo/LearningPacks.hpp:54-105,
+// src/core/LearningPacks.cpp:726-918 rules, :1818-1867 payload): the same
+// container with artifact kind 3, format version 7, and a payload of the id,
+// task and policy fingerprints and revision (u64), environment, control-step,
+// actor-observation, critic-observation, action and motion-feature counts
+// (u32), eight counted FP32 tables (actor and critic observations, motion
+// features, teacher actions, latents, log-probabilities, values, bootstrap
+// values), the outcome schema (u64 count; id, unit, direction u32 each), the
+// outcome values and the learning transitions (u64 count + 64-byte records).
+constexpr std::uint32_t kPolicyRolloutPackKind = 3u;
+constexpr std::uint32_t kPolicyRolloutPackVersion = 7u;
+
+// MRLearningTransitionGPU (task_program_types.h:633-643).
+struct LearningTransition {
+    float reward, timeout_bootstrap_value, reserved0, reserved1;
+    std::uint32_t done, timeout, physics_error, termination_reason;
+    std::uint32_t difficulty_band, terrain_level, impact_sequence_index, impact_event_flags;
+    std::uint64_t policy_revision, reserved;
+};
+static_assert(sizeof(LearningTransition) == 64, "learning transition layout");
+
+struct PolicyOutcome {
+    std::string id, unit;
+    std::uint32_t direction = 0;
+};
+
+struct PolicyRolloutPackData {
+    std::string id;
+    std::uint64_t task_fingerprint = 0, policy_fingerprint = 0, policy_revision = 0;
+    std::uint32_t environment_count = 0, control_step_count = 0, actor_observation_count = 0, critic_observation_count = 0,
+                  action_count = 0, motion_feature_count = 0;
+    std::vector<float> actor_observations, critic_observations, motion_features, teacher_actions, latents, log_probabilities, values,
+        bootstrap_values;
+    std::vector<PolicyOutcome> outcomes;
+    std::vector<float> outcome_values;  // [sample][outcome]
+    std::vector<LearningTransition> transitions;
+    std::uint64_t content_hash = 0;
+};
+
+// A task transition as the learner's record (c_api.cpp's publication).
+LearningTransition learning_transition(const MRTaskTransitionC& t);
+// The C record -> the owned record (spans copied, transitions converted).
+PolicyRolloutPackData policy_rollout_pack_from_c(const MRPolicyRolloutPackC& c);
+// Throws std::invalid_argument on a pack the reference's writer refuses.
+void validate_policy_rollout_pack(const PolicyRolloutPackData& d);
+void write_policy_rollout_pack(const PolicyRolloutPackData& d, const std::string& path);
+PolicyRolloutPackData read_policy_rollout_pack(const std::string& path);
 
 }  // namespace numi

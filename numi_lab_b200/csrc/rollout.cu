@@ -385,6 +385,7 @@ numi::SceneModel numi::rt::pack_scene(const numi::CompiledModel& m, float h) {
 // copied into one device arena, the launch parameters pointing into it.
 struct InstalledPolicy {
     std::uint64_t revision = 0;
+    std::uint64_t fingerprint = 0;  // FNV-1a 64 of the policy's PolicyPack payload (version 4 encoding)
     std::string id;
     DeviceBuffer<float> arena;
     numi::PolicyParams params{};  // arena pointers; state and output pointers are set per launch
@@ -1503,6 +1504,7 @@ MR_API int mr_task_rollout_load_policy_pack(MRTaskRolloutHandle* handle, const c
         const MRPolicyPackC view = numi::policy_pack_view(pack, layers);
         check(numi::configure_policy_kernel(), "policy kernel attributes");
         std::unique_ptr<InstalledPolicy> compiled = compile_policy(*handle, view);
+        compiled->fingerprint = numi::policy_pack_payload_hash(pack);
         // A failed load returns above and leaves the installed policy in place.
         drop_graphs(*handle);
         handle->policy = std::move(compiled);
@@ -1517,6 +1519,7 @@ MR_API int mr_task_rollout_set_policy(MRTaskRolloutHandle* handle, const MRPolic
         if (handle->scene) throw std::invalid_argument("pile and stack worlds take no actions; a policy cannot drive them");
         check(numi::configure_policy_kernel(), "policy kernel attributes");
         std::unique_ptr<InstalledPolicy> compiled = compile_policy(*handle, *policy);
+        compiled->fingerprint = numi::policy_pack_payload_hash(numi::policy_pack_from_c(*policy));
         // Captured graphs hold the previous policy's arena: drop them.
         drop_graphs(*handle);
         handle->policy = std::move(compiled);
@@ -1602,6 +1605,30 @@ MR_API const MRTaskTransitionC* mr_task_rollout_transitions(const MRTaskRolloutH
 
 MR_API uint64_t mr_task_rollout_device_transitions(const MRTaskRolloutHandle* handle) {
     return handle && handle->task && handle->transition_steps ? reinterpret_cast<uint64_t>(handle->d_transitions.ptr) : 0u;
+}
+
+MR_API int mr_task_rollout_write_policy_rollout_pack(const MRTaskRolloutHandle* handle, const MRPolicyRolloutBatchC* batch,
+                                                     const char* batch_id, const char* output_path) {
+    return guarded([&] {
+        if (!handle) throw std::invalid_argument("handle is null");
+        if (!batch || !batch_id || !batch_id[0] || !output_path || !output_path[0])
+            throw std::invalid_argument("policy rollout batch, identity, and output path are required.");
+        const MRTaskRolloutHandle& h = *handle;
+        if (!h.policy) throw std::invalid_argument("a compiled policy must be installed before publishing a rollout pack");
+        MRPolicyRolloutPackC c{};
+        c.id = batch_id;
+        // Without a task program the world's fingerprint names what was rolled out.
+        c.task_fingerprint = h.task && h.task->fingerprint ? h.task->fingerprint : h.stats_layout.world_fingerprint;
+        c.policy_fingerprint = h.policy->fingerprint;
+        c.policy_revision = h.policy->revision;
+        c.environment_count = h.envs;
+        c.actor_observation_count = h.observation_count();
+        c.critic_observation_count = h.observation_count();
+        c.action_count = h.model.world.action_count;
+        c.motion_feature_count = 0;
+        c.batch = batch;
+        numi::write_policy_rollout_pack(numi::policy_rollout_pack_from_c(c), output_path);
+    });
 }
 
 MR_API int mr_task_rollout_copy_transitions(const MRTaskRolloutHandle* handle, MRTaskTransitionC* output, size_t count) {

@@ -1,5 +1,7 @@
-// Per-world free-body control-step kernel and its host launchers; the
-// device code lives in scene_step.cuh.
+// Per-world free-body control-step kernel, the heterogeneous batch's
+// free-body family kernels, and their host launchers; the device code lives
+// in scene_step.cuh.
+#include "mix.h"
 #include "scene_step.cuh"
 
 #include <cstdlib>
@@ -16,6 +18,42 @@ __global__ void __launch_bounds__(32, 16) scene_step_kernel(SceneParams p) {
     if (item >= p.env_count) return;
     const int env = p.env_index != nullptr ? p.env_index[item] : item;
     scene_step_item<kComp, kConvex>(p, reinterpret_cast<float*>(smem4), item, env);
+}
+
+// The batch's free-body family (mix_step.cu): the per-family claim loop over
+// free-body items.  It sits in this translation unit so that it and the
+// per-world kernel run one compiled copy of the out-of-line narrowphase
+// (support_mapped_contacts): a batch reproduces each world alone bit for
+// bit.  A world without support-mapped pairs runs the instance its own
+// kernel runs.
+template <bool kConvex>
+__global__ void __launch_bounds__(32, 16) mix_scene_kernel(const MixWorld* __restrict__ worlds, int world_count, int steps,
+                                                           const std::uint32_t* __restrict__ items, int item_count,
+                                                           unsigned* next_item, int smem_floats_per_warp) {
+    extern __shared__ float4 smem4[];
+    const int lane = threadIdx.x & 31;
+    float* base = reinterpret_cast<float*>(smem4) + static_cast<size_t>(threadIdx.x >> 5) * smem_floats_per_warp;
+    for (;;) {
+        unsigned claimed = 0u;
+        if (lane == 0) claimed = atomicAdd(next_item, 1u);
+        claimed = __shfl_sync(0xffffffffu, claimed, 0);
+        if (claimed >= static_cast<unsigned>(item_count)) break;
+        const std::uint32_t code = items[claimed];
+        const int world = static_cast<int>(code >> kMixWorldShift);
+        const int env = static_cast<int>(code & kMixEnvMask);
+        for (int k = 0; k < steps; ++k) {
+            const SceneParams& sp = worlds[static_cast<size_t>(k) * world_count + world].scene;
+            if constexpr (kConvex) {
+                if (sp.support_mapped)
+                    scene_step_item<false, true>(sp, base, env, env);
+                else
+                    scene_step_item<false, false>(sp, base, env, env);
+            } else {
+                scene_step_item<false, false>(sp, base, env, env);
+            }
+            __syncwarp();
+        }
+    }
 }
 
 // The FP64 audit of the bodies each environment committed in the launch with
@@ -88,6 +126,32 @@ cudaError_t configure_scene_step_kernel() {
                                                 static_cast<int>(scene_launch_smem(compensated)));
                 });
     return e;
+}
+
+cudaError_t configure_mix_scene_kernel(bool convex, size_t max_dynamic_smem) {
+    const int bytes = static_cast<int>(max_dynamic_smem);
+    return convex ? cudaFuncSetAttribute(mix_scene_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)
+                  : cudaFuncSetAttribute(mix_scene_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+cudaError_t mix_scene_occupancy(bool convex, int warps_per_block, size_t smem_per_block, int* blocks_per_sm) {
+    return convex ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, mix_scene_kernel<true>, 32 * warps_per_block,
+                                                                  smem_per_block)
+                  : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, mix_scene_kernel<false>, 32 * warps_per_block,
+                                                                  smem_per_block);
+}
+
+cudaError_t launch_mix_scene(bool convex, const MixWorld* worlds, int world_count, int steps, const std::uint32_t* items,
+                             int item_count, unsigned* next_item, int warps_per_block, int smem_floats_per_warp, int grid,
+                             cudaStream_t stream) {
+    const size_t smem = static_cast<size_t>(smem_floats_per_warp) * sizeof(float) * warps_per_block;
+    if (convex)
+        mix_scene_kernel<true><<<grid, 32 * warps_per_block, smem, stream>>>(worlds, world_count, steps, items, item_count, next_item,
+                                                                             smem_floats_per_warp);
+    else
+        mix_scene_kernel<false><<<grid, 32 * warps_per_block, smem, stream>>>(worlds, world_count, steps, items, item_count, next_item,
+                                                                              smem_floats_per_warp);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_scene_audit(const SceneParams& p, cudaStream_t stream) {

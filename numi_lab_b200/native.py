@@ -441,6 +441,67 @@ class TaskTransitionC(ct.Structure):
     ]
 
 
+class PolicyRolloutBatchC(ct.Structure):
+    _fields_ = [
+        ("control_step_count", ct.c_uint32),
+        ("actor_observations", ct.POINTER(ct.c_float)),
+        ("actor_observation_count", ct.c_size_t),
+        ("critic_observations", ct.POINTER(ct.c_float)),
+        ("critic_observation_count", ct.c_size_t),
+        ("motion_features", ct.POINTER(ct.c_float)),
+        ("motion_feature_count", ct.c_size_t),
+        ("teacher_actions", ct.POINTER(ct.c_float)),
+        ("teacher_action_count", ct.c_size_t),
+        ("latents", ct.POINTER(ct.c_float)),
+        ("latent_count", ct.c_size_t),
+        ("log_probabilities", ct.POINTER(ct.c_float)),
+        ("log_probability_count", ct.c_size_t),
+        ("values", ct.POINTER(ct.c_float)),
+        ("value_count", ct.c_size_t),
+        ("bootstrap_values", ct.POINTER(ct.c_float)),
+        ("bootstrap_value_count", ct.c_size_t),
+        ("transitions", ct.POINTER(TaskTransitionC)),
+        ("transition_count", ct.c_size_t),
+    ]
+
+
+class PolicyRolloutPackC(ct.Structure):
+    _fields_ = [
+        ("id", ct.c_char_p),
+        ("task_fingerprint", ct.c_uint64),
+        ("policy_fingerprint", ct.c_uint64),
+        ("policy_revision", ct.c_uint64),
+        ("environment_count", ct.c_uint32),
+        ("actor_observation_count", ct.c_uint32),
+        ("critic_observation_count", ct.c_uint32),
+        ("action_count", ct.c_uint32),
+        ("motion_feature_count", ct.c_uint32),
+        ("reserved", ct.c_uint32),
+        ("batch", ct.POINTER(PolicyRolloutBatchC)),
+    ]
+
+
+class PolicyRolloutPackInfoC(ct.Structure):
+    _fields_ = [
+        ("task_fingerprint", ct.c_uint64),
+        ("policy_fingerprint", ct.c_uint64),
+        ("policy_revision", ct.c_uint64),
+        ("content_hash", ct.c_uint64),
+        ("environment_count", ct.c_uint32),
+        ("control_step_count", ct.c_uint32),
+        ("actor_observation_count", ct.c_uint32),
+        ("critic_observation_count", ct.c_uint32),
+        ("action_count", ct.c_uint32),
+        ("motion_feature_count", ct.c_uint32),
+        ("outcome_count", ct.c_uint32),
+        ("has_teacher_actions", ct.c_uint32),
+        ("transition_count", ct.c_uint64),
+        ("reward_sum", ct.c_double),
+        ("done_count", ct.c_uint64),
+        ("id", ct.c_char * 64),
+    ]
+
+
 class ModelWorldC(ct.Structure):
     _fields_ = [
         ("body_count", ct.c_uint32),
@@ -673,6 +734,9 @@ EXPORTED_SYMBOLS: Final = (
     "mr_task_rollout_transitions",
     "mr_task_rollout_device_transitions",
     "mr_task_rollout_copy_transitions",
+    "mr_task_rollout_write_policy_rollout_pack",
+    "mr_write_policy_rollout_pack",
+    "mr_policy_rollout_pack_inspect",
     "mr_task_rollout_policy_latents",
     "mr_task_rollout_policy_log_probabilities",
     "mr_task_rollout_policy_values",
@@ -864,6 +928,12 @@ class Bindings:
         L.mr_task_rollout_device_transitions.restype = ct.c_uint64
         L.mr_task_rollout_copy_transitions.argtypes = [ct.c_void_p, P(TaskTransitionC), ct.c_size_t]
         L.mr_task_rollout_copy_transitions.restype = ct.c_int
+        L.mr_task_rollout_write_policy_rollout_pack.argtypes = [ct.c_void_p, P(PolicyRolloutBatchC), ct.c_char_p, ct.c_char_p]
+        L.mr_task_rollout_write_policy_rollout_pack.restype = ct.c_int
+        L.mr_write_policy_rollout_pack.argtypes = [P(PolicyRolloutPackC), ct.c_char_p]
+        L.mr_write_policy_rollout_pack.restype = ct.c_int
+        L.mr_policy_rollout_pack_inspect.argtypes = [ct.c_char_p, P(PolicyRolloutPackInfoC), P(ct.c_float), ct.c_size_t]
+        L.mr_policy_rollout_pack_inspect.restype = ct.c_int
 
     def last_error(self) -> str:
         value = self.lib.mr_last_error()

@@ -241,6 +241,82 @@ def inspect_policy_pack(path: str | os.PathLike[str], *, library: native.Binding
     return fields, params
 
 
+def policy_rollout_pack_c(*, id: str, task_fingerprint: int, policy_fingerprint: int, policy_revision: int, environment_count: int,
+                          control_step_count: int, actor_observations, latents, log_probabilities, values, bootstrap_values,
+                          transitions, critic_observations=None, teacher_actions=None, motion_features=None,
+                          actor_observation_count: int | None = None, critic_observation_count: int | None = None,
+                          action_count: int | None = None, motion_feature_count: int = 0):
+    """(MRPolicyRolloutPackC, keepalive) from arrays: observations
+    [step][env][features], latents [step][env][actions], log-probabilities
+    and values [step][env], bootstrap values [env], transitions a ctypes
+    MRTaskTransitionC array [step * env]."""
+
+    keep: list[Any] = []
+
+    def arr(a, width=None):
+        if a is None:
+            return None, 0
+        x = np.ascontiguousarray(a, np.float32).reshape(-1)
+        keep.append(x)
+        return x.ctypes.data_as(ct.POINTER(ct.c_float)), x.size
+
+    obs = np.asarray(actor_observations, np.float32)
+    lat = np.asarray(latents, np.float32)
+    b = native.PolicyRolloutBatchC()
+    b.control_step_count = control_step_count
+    b.actor_observations, b.actor_observation_count = arr(obs)
+    b.critic_observations, b.critic_observation_count = arr(obs if critic_observations is None else critic_observations)
+    b.motion_features, b.motion_feature_count = arr(motion_features)
+    b.teacher_actions, b.teacher_action_count = arr(teacher_actions)
+    b.latents, b.latent_count = arr(lat)
+    b.log_probabilities, b.log_probability_count = arr(log_probabilities)
+    b.values, b.value_count = arr(values)
+    b.bootstrap_values, b.bootstrap_value_count = arr(bootstrap_values)
+    keep.append(transitions)
+    b.transitions = ct.cast(transitions, ct.POINTER(native.TaskTransitionC))
+    b.transition_count = len(transitions)
+    keep.append(b)
+    c = native.PolicyRolloutPackC()
+    ident = id.encode()
+    keep.append(ident)
+    c.id = ident
+    c.task_fingerprint, c.policy_fingerprint, c.policy_revision = task_fingerprint, policy_fingerprint, policy_revision
+    c.environment_count = environment_count
+    c.actor_observation_count = obs.shape[-1] if actor_observation_count is None else actor_observation_count
+    crit = obs if critic_observations is None else np.asarray(critic_observations)
+    c.critic_observation_count = crit.shape[-1] if critic_observation_count is None else critic_observation_count
+    c.action_count = lat.shape[-1] if action_count is None else action_count
+    c.motion_feature_count = motion_feature_count
+    c.batch = ct.pointer(b)
+    return c, keep
+
+
+def write_policy_rollout_pack(path: str | os.PathLike[str], *, library: native.Bindings | None = None, **fields) -> None:
+    """Writes a PolicyRolloutPack (mr_write_policy_rollout_pack)."""
+
+    lib = library or native.bindings()
+    c, keep = policy_rollout_pack_c(**fields)
+    lib.check(lib.lib.mr_write_policy_rollout_pack(ct.byref(c), os.fsencode(path)), "mr_write_policy_rollout_pack")
+    del keep
+
+
+def inspect_policy_rollout_pack(path: str | os.PathLike[str], *, library: native.Bindings | None = None) -> tuple[dict, np.ndarray]:
+    """(fields, actor observations + latents + log-probabilities + values +
+    bootstrap values concatenated) of a PolicyRolloutPack file."""
+
+    lib = library or native.bindings()
+    info = native.PolicyRolloutPackInfoC()
+    lib.check(lib.lib.mr_policy_rollout_pack_inspect(os.fsencode(path), ct.byref(info), None, 0), "mr_policy_rollout_pack_inspect")
+    samples = int(info.environment_count) * int(info.control_step_count)
+    count = samples * (int(info.actor_observation_count) + int(info.action_count) + 2) + int(info.environment_count)
+    params = np.zeros(count, np.float32)
+    lib.check(lib.lib.mr_policy_rollout_pack_inspect(os.fsencode(path), ct.byref(info), params.ctypes.data_as(ct.POINTER(ct.c_float)),
+                                                     params.size), "mr_policy_rollout_pack_inspect")
+    fields = {name: getattr(info, name) for name, _ in native.PolicyRolloutPackInfoC._fields_}
+    fields["id"] = info.id.decode()
+    return fields, params
+
+
 def quality_solve(mass: np.ndarray, jacobian: np.ndarray, free_velocity: np.ndarray, target: np.ndarray,
                   regularization: np.ndarray, friction: np.ndarray, *, counts: np.ndarray | None = None,
                   warm: np.ndarray | None = None, max_newton: int = 0, tolerance: float = 0.0,
@@ -694,6 +770,27 @@ class World:
         self._lib.check(self._lib.lib.mr_task_rollout_copy_transitions(self._handle, raw, len(raw)), "mr_task_rollout_copy_transitions")
         arr = np.frombuffer(bytes(raw), dtype=_TRANSITION_DTYPE).reshape(steps, self.envs)
         return {name: arr[name].copy() for name in self.TRANSITION_FIELDS}
+
+    def write_policy_rollout_pack(self, path: str | os.PathLike[str], batch_id: str, observations) -> None:
+        """Publishes the last policy-driven advance as a PolicyRolloutPack
+        (mr_task_rollout_write_policy_rollout_pack): `observations` are the
+        actor frames it returned; latents, log-probabilities, values,
+        bootstrap values and transitions are the rollout's own."""
+
+        out = self.policy_outputs()
+        if out is None:
+            raise MetalRoboError("no policy-driven advance to publish")
+        steps = out["latents"].shape[0]
+        raw = (native.TaskTransitionC * (steps * self.envs))()
+        self._lib.check(self._lib.lib.mr_task_rollout_copy_transitions(self._handle, raw, len(raw)), "mr_task_rollout_copy_transitions")
+        frames = observations.cpu().numpy() if hasattr(observations, "cpu") else np.asarray(observations)
+        c, keep = policy_rollout_pack_c(id=batch_id, task_fingerprint=0, policy_fingerprint=0, policy_revision=0,
+                                        environment_count=self.envs, control_step_count=steps, actor_observations=frames,
+                                        latents=out["latents"], log_probabilities=out["log_probabilities"], values=out["values"],
+                                        bootstrap_values=out["bootstrap_values"], transitions=raw)
+        self._lib.check(self._lib.lib.mr_task_rollout_write_policy_rollout_pack(self._handle, c.batch, batch_id.encode(), os.fsencode(path)),
+                        "mr_task_rollout_write_policy_rollout_pack")
+        del keep
 
     def set_state_readback(self, enabled: bool) -> None:
         self._lib.check(self._lib.lib.mr_task_rollout_set_state_readback(self._handle, 1 if enabled else 0), "set_state_readback")

@@ -216,6 +216,43 @@ def reference_write_policy_pack(pack, path) -> None:
         raise ValueError(f"reference writePolicyPack failed ({st}): {err.value.decode()}")
 
 
+def reference_write_policy_rollout_pack(pack, path) -> None:
+    """The reference's writePolicyRolloutPack on a pack given as an
+    MRPolicyRolloutPackC (numi_lab_b200.native.PolicyRolloutPackC)."""
+
+    lib = _ref_lib()
+    lib.ref_write_policy_rollout_pack.restype = ct.c_int
+    lib.ref_write_policy_rollout_pack.argtypes = [ct.c_void_p, ct.c_char_p, ct.c_char_p, ct.c_size_t]
+    err = ct.create_string_buffer(512)
+    st = lib.ref_write_policy_rollout_pack(ct.addressof(pack), os.fsencode(path), err, len(err))
+    if st != 0:
+        raise ValueError(f"reference writePolicyRolloutPack failed ({st}): {err.value.decode()}")
+
+
+def reference_inspect_policy_rollout_pack(path, parameter_count: int = 0):
+    """The reference's readPolicyRolloutPack in the layout of
+    mr_policy_rollout_pack_inspect: (fields, actor observations, latents,
+    log-probabilities, values and bootstrap values concatenated)."""
+
+    from numi_lab_b200 import native
+
+    lib = _ref_lib()
+    lib.ref_policy_rollout_pack_inspect.restype = ct.c_int
+    lib.ref_policy_rollout_pack_inspect.argtypes = [ct.c_char_p, ct.c_void_p, ct.POINTER(ct.c_float), ct.c_size_t, ct.c_char_p,
+                                                    ct.c_size_t]
+    info = native.PolicyRolloutPackInfoC()
+    err = ct.create_string_buffer(512)
+    params = np.zeros(parameter_count, np.float32)
+    st = lib.ref_policy_rollout_pack_inspect(os.fsencode(path), ct.addressof(info),
+                                             params.ctypes.data_as(ct.POINTER(ct.c_float)) if parameter_count else None,
+                                             params.size, err, len(err))
+    if st != 0:
+        raise ValueError(f"reference readPolicyRolloutPack failed ({st}): {err.value.decode()}")
+    fields = {name: getattr(info, name) for name, _ in native.PolicyRolloutPackInfoC._fields_}
+    fields["id"] = info.id.decode()
+    return fields, params
+
+
 def reference_inspect_policy_pack(path):
     """The reference's readPolicyPack: (fields, FP32 tables in file order)
     in the layout of mr_policy_pack_inspect."""

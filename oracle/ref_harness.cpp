@@ -867,6 +867,94 @@ __attribute__((visibility("default"))) int ref_write_policy_pack(const MRPolicyP
     return r.succeeded() ? 0 : static_cast<int>(r.status);
 }
 
+// The reference's PolicyRolloutPack writer (writePolicyRolloutPack) over the
+// same record this library's mr_write_policy_rollout_pack takes; task
+// transitions become learner transitions the way c_api.cpp:4410-4445 does.
+__attribute__((visibility("default"))) int ref_write_policy_rollout_pack(const MRPolicyRolloutPackC* c, const char* path, char* err,
+                                                                         size_t err_len) {
+    const MRPolicyRolloutBatchC& b = *c->batch;
+    std::vector<MRLearningTransitionGPU> transitions(b.transition_count);
+    for (size_t i = 0; i < b.transition_count; ++i) {
+        const MRTaskTransitionC& t = b.transitions[i];
+        MRLearningTransitionGPU& d = transitions[i];
+        d = MRLearningTransitionGPU{};
+        d.rewardAndBootstrap = {t.reward, t.timeout_bootstrap_value, 0.0f, 0.0f};
+        d.termination = {t.done, t.timeout, t.physics_error, t.termination_reason};
+        d.context = {t.difficulty_band, t.terrain_level, t.impact_sequence_index, t.impact_event_flags};
+        d.policyRevision = t.policy_revision;
+    }
+    auto span = [](const float* v, size_t n) { return std::span<const float>(v, n); };
+    const PolicyRolloutPackView view{
+        .id = c->id,
+        .taskFingerprint = c->task_fingerprint,
+        .policyFingerprint = c->policy_fingerprint,
+        .policyRevision = c->policy_revision,
+        .environmentCount = c->environment_count,
+        .controlStepCount = b.control_step_count,
+        .actorObservationCount = c->actor_observation_count,
+        .criticObservationCount = c->critic_observation_count,
+        .actionCount = c->action_count,
+        .motionFeatureCount = c->motion_feature_count,
+        .actorObservations = span(b.actor_observations, b.actor_observation_count),
+        .criticObservations = span(b.critic_observations, b.critic_observation_count),
+        .motionFeatures = span(b.motion_features, b.motion_feature_count),
+        .teacherActions = span(b.teacher_actions, b.teacher_action_count),
+        .latents = span(b.latents, b.latent_count),
+        .logProbabilities = span(b.log_probabilities, b.log_probability_count),
+        .values = span(b.values, b.value_count),
+        .bootstrapValues = span(b.bootstrap_values, b.bootstrap_value_count),
+        .outcomes = {},
+        .outcomeValues = {},
+        .transitions = transitions,
+    };
+    const LearningPackResult r = writePolicyRolloutPack(view, path);
+    if (!r.succeeded() && err && err_len) std::snprintf(err, err_len, "%s", r.message.c_str());
+    return r.succeeded() ? 0 : static_cast<int>(r.status);
+}
+
+// The reference's reader (readPolicyRolloutPack) into this library's info record.
+__attribute__((visibility("default"))) int ref_policy_rollout_pack_inspect(const char* path, MRPolicyRolloutPackInfoC* info,
+                                                                           float* params, size_t cap, char* err, size_t err_len) {
+    PolicyRolloutPack p;
+    const LearningPackResult r = readPolicyRolloutPack(path, p);
+    if (!r.succeeded()) {
+        if (err && err_len) std::snprintf(err, err_len, "%s", r.message.c_str());
+        return static_cast<int>(r.status);
+    }
+    MRPolicyRolloutPackInfoC o{};
+    o.task_fingerprint = p.taskFingerprint;
+    o.policy_fingerprint = p.policyFingerprint;
+    o.policy_revision = p.policyRevision;
+    o.content_hash = r.contentHash;
+    o.environment_count = p.environmentCount;
+    o.control_step_count = p.controlStepCount;
+    o.actor_observation_count = p.actorObservationCount;
+    o.critic_observation_count = p.criticObservationCount;
+    o.action_count = p.actionCount;
+    o.motion_feature_count = p.motionFeatureCount;
+    o.outcome_count = static_cast<uint32_t>(p.outcomes.size());
+    o.has_teacher_actions = p.teacherActions.empty() ? 0u : 1u;
+    o.transition_count = p.transitions.size();
+    for (const MRLearningTransitionGPU& t : p.transitions) {
+        o.reward_sum += t.rewardAndBootstrap.x;
+        o.done_count += t.termination.x;
+    }
+    std::snprintf(o.id, sizeof(o.id), "%s", p.id.c_str());
+    if (params) {
+        size_t at = 0;
+        for (const std::vector<float>* v : {&p.actorObservations, &p.latents, &p.logProbabilities, &p.values, &p.bootstrapValues}) {
+            if (v->size() > cap - at) {
+                if (err && err_len) std::snprintf(err, err_len, "parameters capacity is too small");
+                return -1;
+            }
+            std::memcpy(params + at, v->data(), v->size() * sizeof(float));
+            at += v->size();
+        }
+    }
+    *info = o;
+    return 0;
+}
+
 __attribute__((visibility("default"))) int ref_policy_pack_inspect(const char* path, MRPolicyPackInfoC* info, float* params, size_t cap,
                                                                    char* err, size_t err_len) {
     PolicyPack p;

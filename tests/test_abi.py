@@ -75,6 +75,9 @@ def test_struct_sizes_match_header_layout(tmp_path):
         "MRTaskIndexGroupC": native.TaskIndexGroupC,
         "MRTaskProgramC": native.TaskProgramC,
         "MRTaskTransitionC": native.TaskTransitionC,
+        "MRPolicyRolloutBatchC": native.PolicyRolloutBatchC,
+        "MRPolicyRolloutPackC": native.PolicyRolloutPackC,
+        "MRPolicyRolloutPackInfoC": native.PolicyRolloutPackInfoC,
     }
     src = tmp_path / "sizes.c"
     body = "".join(f'printf("%zu\\n", sizeof({name}));' for name in records)

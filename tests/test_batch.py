@@ -44,8 +44,8 @@ def _state(w):
 
 
 def _assert_same(a, b):
-    for x, y in zip(_state(a), _state(b)):
-        np.testing.assert_array_equal(x, y)
+    for name, x, y in zip(("q", "v", "manifolds"), _state(a), _state(b)):
+        np.testing.assert_array_equal(x, y, err_msg=f"{a.source} ({a.envs} envs, seed {a.seed}): {name}")
 
 
 @pytest.mark.parametrize("gjk", [False, True])

@@ -162,6 +162,29 @@ def test_policy_reads_the_actor_frames(cuda_device):
             want = ref.forward(frames[k], layers)
             assert float(np.max(np.abs(out["latents"][k] - want))) <= 1e-4
         assert np.all(tr["policy_revision"] == 3)
+        # The advance published as a PolicyRolloutPack, read back by both readers.
+        import tempfile
+        from pathlib import Path
+
+        with tempfile.TemporaryDirectory() as tmp:
+            path = Path(tmp) / "batch.mrrollout"
+            w.write_policy_rollout_pack(path, "task-batch", obs)
+            info, params = nb.inspect_policy_rollout_pack(path)
+            assert (info["environment_count"], info["control_step_count"], info["actor_observation_count"],
+                    info["action_count"], info["policy_revision"], info["id"]) == (envs, steps, nobs, na, 3, "task-batch")
+            assert info["task_fingerprint"] == prog.task_fingerprint and info["policy_fingerprint"] != 0
+            want = np.concatenate([frames.astype(np.float32).reshape(-1), out["latents"].reshape(-1), out["log_probabilities"].reshape(-1),
+                                   out["values"].reshape(-1), out["bootstrap_values"].reshape(-1)])
+            np.testing.assert_array_equal(params, want)
+            assert info["reward_sum"] == pytest.approx(float(tr["reward"].astype(np.float64).sum()), rel=1e-6)
+            try:
+                from oracle import reference_inspect_policy_rollout_pack
+                ref_info, ref_params = reference_inspect_policy_rollout_pack(path, params.size)
+            except FileNotFoundError:
+                ref_info = None  # the reference build is absent where this runs
+            if ref_info is not None:
+                np.testing.assert_array_equal(ref_params, params)
+                assert ref_info["transition_count"] == envs * steps
 
 
 def test_installer_refuses_programs_outside_the_subset(cuda_device):
