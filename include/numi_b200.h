@@ -725,11 +725,14 @@ enum {
     MR_TASK_OBSERVE_PREVIOUS_ACTION = 5u,
     MR_TASK_OBSERVE_ROOT_LINEAR_VELOCITY_LOCAL = 6u,
     MR_TASK_OBSERVE_ROOT_HEIGHT = 7u,
+    MR_TASK_OBSERVE_CONTACT_METRIC = 8u,
+    MR_TASK_OBSERVE_CONTACT_WRENCH_LOCAL = 13u,
     MR_TASK_OBSERVE_GAIT_PHASE = 14u,
     MR_TASK_OBSERVE_DELAYED_ACTION = 26u,
     MR_TASK_OBSERVE_JOINT_FINITE_DIFFERENCE_VELOCITY = 27u
 };
 enum { MR_TASK_OBSERVATION_NORMALIZE_VECTOR3 = 1u };
+enum { MR_TASK_CONTACT_SUPPORT = 1u, MR_TASK_CONTACT_FORBIDDEN = 2u };
 enum {
     MR_TASK_REWARD_LINEAR_VELOCITY_TRACKING = 0u,
     MR_TASK_REWARD_YAW_VELOCITY_TRACKING = 1u,
@@ -743,8 +746,13 @@ enum {
     MR_TASK_REWARD_ACTION_RATE_SQUARED = 9u,
     MR_TASK_REWARD_JOINT_LIMIT_VIOLATION_SQUARED = 10u,
     MR_TASK_REWARD_JOINT_GROUP_POSTURE_SQUARED = 12u,
+    MR_TASK_REWARD_GAIT_CONTACT_MATCH = 13u,
+    MR_TASK_REWARD_SWING_CLEARANCE = 14u,
+    MR_TASK_REWARD_SUPPORT_SLIP = 15u,
+    MR_TASK_REWARD_FORBIDDEN_CONTACT = 16u,
     MR_TASK_REWARD_JOINT_GROUP_POSTURE_ABSOLUTE = 17u,
     MR_TASK_REWARD_PROJECTED_GRAVITY_HORIZONTAL_SQUARED = 18u,
+    MR_TASK_REWARD_FOOT_CLEARANCE = 19u,
     MR_TASK_REWARD_JOINT_LIMIT_VIOLATION_ABSOLUTE = 20u,
     MR_TASK_REWARD_ROOT_HEIGHT_NORMALIZED = 21u,
     MR_TASK_REWARD_ROOT_HEIGHT_PROGRESS = 22u,
@@ -752,7 +760,8 @@ enum {
 };
 enum {
     MR_TASK_TERMINATE_MINIMUM_ROOT_HEIGHT = 0u,
-    MR_TASK_TERMINATE_MAXIMUM_TILT = 1u
+    MR_TASK_TERMINATE_MAXIMUM_TILT = 1u,
+    MR_TASK_TERMINATE_CONTACT_GROUP = 2u
 };
 enum {
     MR_TASK_TERMINATION_CONTINUING = 0u,
@@ -810,7 +819,8 @@ typedef struct MRTaskObservationOperatorC {
  * control_dt x sum(weight x value). */
 typedef struct MRTaskRewardOperatorC {
     uint32_t opcode;
-    uint32_t group;      /* joint group of the posture rewards */
+    uint32_t group;      /* joint group of the posture rewards; contact group of
+                            the contact rewards (MR_INVALID_INDEX: every group) */
     float weight;
     float parameters[3]; /* the reference's parameters.yzw */
 } MRTaskRewardOperatorC;
@@ -820,7 +830,7 @@ typedef struct MRTaskTerminationOperatorC {
     uint32_t opcode;
     uint32_t reason;
     uint32_t priority;
-    uint32_t reserved;
+    uint32_t group;      /* contact group of CONTACT_GROUP */
     float threshold;
     float failure_penalty;
 } MRTaskTerminationOperatorC;
@@ -840,10 +850,33 @@ typedef struct MRTaskIndexGroupC {
     uint32_t count;
 } MRTaskIndexGroupC;
 
+/* reference: MRTaskContactGroupGPU (:469-489), without support patches.
+ * Bodies contact_members[first, first + count) (articulated body indices).
+ * Per step the group publishes, from the final microstep's contacts of its
+ * bodies with the ground: support groups the normal force (sum of normal
+ * impulses / physics dt), the slip (planar speed of the kinematic
+ * reference point while in contact), the air time, the clearance of the
+ * reference point above the ground less its radius and the centre of
+ * pressure in the reference body's frame; forbidden groups 1 when a contact
+ * pushes harder than the support force threshold; every group the contact
+ * wrench (force and torque about the reference point) in the reference
+ * body's frame. */
+typedef struct MRTaskContactGroupC {
+    uint32_t first;
+    uint32_t count;
+    uint32_t flags;                 /* MR_TASK_CONTACT_SUPPORT / _FORBIDDEN */
+    uint32_t reference_body;
+    float local_reference[4];       /* point from the reference body's COM, its axes; w clearance radius */
+    float kinematic_reference[4];   /* link-frame origin from the COM, its axes */
+    float gait_phase_offset;        /* radians */
+    float stance_fraction;
+    float reserved[2];
+} MRTaskContactGroupC;
+
 /* A compiled task program: the tables and constants of the reference's
  * MRTaskProgramHeaderGPU (:358-441) that the evaluated subset reads.  One
- * actor history frame, one difficulty band, no terrain, pushes, contact
- * groups or sensor biases. */
+ * actor history frame, one difficulty band, a flat ground; no terrain,
+ * pushes, support patches or sensor biases. */
 typedef struct MRTaskProgramC {
     const MRTaskActionBindingC* actions;
     uint32_t action_count;          /* equals the world's action count */
@@ -859,6 +892,12 @@ typedef struct MRTaskProgramC {
     uint32_t joint_group_count;
     const uint32_t* joint_members;
     uint32_t joint_member_count;
+    const MRTaskContactGroupC* contact_groups;  /* at most 8 */
+    uint32_t contact_group_count;
+    const uint32_t* contact_members;
+    uint32_t contact_member_count;
+    float support_force_threshold;  /* program.dynamics.y, newtons */
+    float clearance_target;         /* program.locomotion.z, metres */
     const float* default_q;         /* [nq]: the reset pose and posture reference */
     uint32_t default_q_count;
     uint32_t maximum_episode_steps; /* timeout */

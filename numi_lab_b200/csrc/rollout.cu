@@ -474,7 +474,7 @@ struct MRTaskRolloutHandle {
     // transitions ([step][env]) of the last advance.
     std::unique_ptr<InstalledTask> task;
     DeviceBuffer<numi::TaskEnvState> d_task_state;
-    DeviceBuffer<float> d_task_history, d_task_previous, d_task_frame, d_task_targets;
+    DeviceBuffer<float> d_task_history, d_task_previous, d_task_frame, d_task_targets, d_task_air;
     DeviceBuffer<std::uint32_t> d_task_masks;
     DeviceBuffer<MRTaskTransitionC> d_transitions;
     PinnedBuffer<MRTaskTransitionC> h_transitions;
@@ -799,6 +799,8 @@ struct MRTaskRolloutHandle {
         t.actions = actions ? actions + item0 * P.na : nullptr;
         t.targets = d_task_targets.ptr + static_cast<size_t>(o) * P.na;
         t.status = status + item0;
+        t.manifolds = d_manifolds.ptr + static_cast<size_t>(o) * manifold_words();
+        t.air_time = d_task_air.ptr + static_cast<size_t>(o) * numi::kTaskMaxGroups;
         t.transitions = d_transitions.ptr + item0;
         t.policy_revision = policy ? policy->revision : 0u;
         t.env_count = static_cast<int>(n);
@@ -1337,6 +1339,10 @@ std::unique_ptr<InstalledTask> compile_task(const MRTaskRolloutHandle& h, const 
             break;
         case MR_TASK_OBSERVE_ROOT_HEIGHT:
             break;
+        case MR_TASK_OBSERVE_CONTACT_METRIC:
+        case MR_TASK_OBSERVE_CONTACT_WRENCH_LOCAL:
+            need(o.source < t.contact_group_count && o.component < 6u, where + ": source must be a contact group and component 0-5");
+            break;
         case MR_TASK_OBSERVE_JOINT_POSITION_ERROR:
         case MR_TASK_OBSERVE_JOINT_VELOCITY:
         case MR_TASK_OBSERVE_PREVIOUS_ACTION:
@@ -1358,6 +1364,23 @@ std::unique_ptr<InstalledTask> compile_task(const MRTaskRolloutHandle& h, const 
         need(static_cast<std::uint64_t>(G.first) + G.count <= t.joint_member_count, "joint group " + to_string(g) + " overruns joint_members");
     }
     for (std::uint32_t m = 0; m < t.joint_member_count; ++m) need(t.joint_members[m] < na, "joint members must be action indices");
+    need(t.contact_group_count <= static_cast<std::uint32_t>(numi::kTaskMaxGroups), "at most 8 contact groups");
+    need(t.contact_group_count == 0 || t.contact_groups != nullptr, "contact_groups is null");
+    need(t.contact_member_count == 0 || t.contact_members != nullptr, "contact_members is null");
+    need(finite_value(t.support_force_threshold) && t.support_force_threshold >= 0.0f && finite_value(t.clearance_target),
+         "support_force_threshold and clearance_target must be finite");
+    for (std::uint32_t g = 0; g < t.contact_group_count; ++g) {
+        const MRTaskContactGroupC& G = t.contact_groups[g];
+        const std::string where = "contact group " + to_string(g);
+        need(static_cast<std::uint64_t>(G.first) + G.count <= t.contact_member_count, where + " overruns contact_members");
+        need(G.reference_body < static_cast<std::uint32_t>(M.nb), where + ": reference_body must be an articulated body");
+        need((G.flags & ~3u) == 0u, where + ": flags are SUPPORT and FORBIDDEN");
+        bool finite_all = finite_value(G.gait_phase_offset) && finite_value(G.stance_fraction);
+        for (int k = 0; k < 4; ++k) finite_all = finite_all && finite_value(G.local_reference[k]) && finite_value(G.kinematic_reference[k]);
+        need(finite_all, where + ": references and gait must be finite");
+    }
+    for (std::uint32_t m = 0; m < t.contact_member_count; ++m)
+        need(t.contact_members[m] < static_cast<std::uint32_t>(M.nb), "contact members must be articulated bodies");
     need(t.reward_count == 0 || t.rewards != nullptr, "rewards is null");
     for (std::uint32_t i = 0; i < t.reward_count; ++i) {
         const MRTaskRewardOperatorC& r = t.rewards[i];
@@ -1368,6 +1391,14 @@ std::unique_ptr<InstalledTask> compile_task(const MRTaskRolloutHandle& h, const 
         case MR_TASK_REWARD_JOINT_GROUP_POSTURE_SQUARED:
         case MR_TASK_REWARD_JOINT_GROUP_POSTURE_ABSOLUTE:
             need(r.group < t.joint_group_count, where + ": group must be a joint group index");
+            break;
+        case MR_TASK_REWARD_GAIT_CONTACT_MATCH:
+        case MR_TASK_REWARD_SWING_CLEARANCE:
+        case MR_TASK_REWARD_FOOT_CLEARANCE:
+        case MR_TASK_REWARD_SUPPORT_SLIP:
+        case MR_TASK_REWARD_FORBIDDEN_CONTACT:
+            need(r.group == MR_INVALID_INDEX || r.group < t.contact_group_count,
+                 where + ": group must be a contact group index or MR_INVALID_INDEX");
             break;
         case MR_TASK_REWARD_LINEAR_VELOCITY_TRACKING:
         case MR_TASK_REWARD_YAW_VELOCITY_TRACKING:
@@ -1394,8 +1425,11 @@ std::unique_ptr<InstalledTask> compile_task(const MRTaskRolloutHandle& h, const 
     need(t.termination_count == 0 || t.terminations != nullptr, "terminations is null");
     for (std::uint32_t i = 0; i < t.termination_count; ++i) {
         const MRTaskTerminationOperatorC& o = t.terminations[i];
-        need(o.opcode == MR_TASK_TERMINATE_MINIMUM_ROOT_HEIGHT || o.opcode == MR_TASK_TERMINATE_MAXIMUM_TILT,
+        need(o.opcode == MR_TASK_TERMINATE_MINIMUM_ROOT_HEIGHT || o.opcode == MR_TASK_TERMINATE_MAXIMUM_TILT ||
+                 o.opcode == MR_TASK_TERMINATE_CONTACT_GROUP,
              "termination operator " + to_string(i) + ": opcode " + to_string(o.opcode) + " is outside the evaluated subset");
+        need(o.opcode != MR_TASK_TERMINATE_CONTACT_GROUP || o.group < t.contact_group_count,
+             "termination operator " + to_string(i) + ": group must be a contact group index");
         need(finite_value(o.threshold) && finite_value(o.failure_penalty), "termination operator " + to_string(i) + " must be finite");
     }
     need(t.randomization_count == 0 || t.randomization != nullptr, "randomization is null");
@@ -1442,6 +1476,8 @@ std::unique_ptr<InstalledTask> compile_task(const MRTaskRolloutHandle& h, const 
     const size_t at_random = put(t.randomization, t.randomization_count * sizeof(MRTaskRandomizationOperatorC));
     const size_t at_groups = put(t.joint_groups, t.joint_group_count * sizeof(MRTaskIndexGroupC));
     const size_t at_members = put(t.joint_members, t.joint_member_count * sizeof(std::uint32_t));
+    const size_t at_cgroups = put(t.contact_groups, t.contact_group_count * sizeof(MRTaskContactGroupC));
+    const size_t at_cmembers = put(t.contact_members, t.contact_member_count * sizeof(std::uint32_t));
     const size_t at_default = put(t.default_q, nq * sizeof(float));
     const size_t at_lower = put(lower.data(), na * sizeof(float));
     const size_t at_upper = put(upper.data(), na * sizeof(float));
@@ -1457,6 +1493,19 @@ std::unique_ptr<InstalledTask> compile_task(const MRTaskRolloutHandle& h, const 
     P.randomization = reinterpret_cast<const MRTaskRandomizationOperatorC*>(base + at_random);
     P.groups = reinterpret_cast<const MRTaskIndexGroupC*>(base + at_groups);
     P.members = reinterpret_cast<const std::uint32_t*>(base + at_members);
+    P.contact_groups = reinterpret_cast<const MRTaskContactGroupC*>(base + at_cgroups);
+    P.contact_members = reinterpret_cast<const std::uint32_t*>(base + at_cmembers);
+    P.ncontact_groups = static_cast<int>(t.contact_group_count);
+    P.model = h.d_model.ptr;
+    P.support_force_threshold = t.support_force_threshold;
+    P.clearance_target = t.clearance_target;
+    P.physics_dt = h.config.control_timestep_seconds / static_cast<float>(std::max<std::uint32_t>(h.config.physics_substeps, 1u));
+    P.ground_height = 0.0f;  // the world's static plane (normal +z): its height
+    for (int sh = 0; sh < M.ns; ++sh)
+        if (M.shape_body[sh] < 0 && M.shape_type[sh] == MR_SHAPE_PLANE) {
+            P.ground_height = M.shape_position[sh].z;  // a static shape's position is in world coordinates
+            break;
+        }
     P.default_q = reinterpret_cast<const float*>(base + at_default);
     P.limit_lower = reinterpret_cast<const float*>(base + at_lower);
     P.limit_upper = reinterpret_cast<const float*>(base + at_upper);
@@ -1560,6 +1609,7 @@ MR_API int mr_task_rollout_set_task(MRTaskRolloutHandle* handle, const MRTaskPro
         h.d_task_previous.resize(static_cast<size_t>(h.envs) * 2 * P.na);
         h.d_task_frame.resize(static_cast<size_t>(h.envs) * P.nobs);
         h.d_task_targets.resize(static_cast<size_t>(h.envs) * P.na);
+        h.d_task_air.resize(static_cast<size_t>(h.envs) * numi::kTaskMaxGroups);
         check(cudaMemsetAsync(h.d_task_history.ptr, 0, h.d_task_history.count * sizeof(float), h.stream), "clear task history");
         check(cudaMemsetAsync(h.d_task_previous.ptr, 0, h.d_task_previous.count * sizeof(float), h.stream), "clear task history");
         h.task = std::move(compiled);

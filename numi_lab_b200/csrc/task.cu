@@ -117,7 +117,8 @@ __device__ __forceinline__ float3 projected_gravity(const Root& r) {
 // transform applied, no noise.  `raw` points at the delay line's newest raw
 // slot; `previous_q` at the joint positions of the last step's end.
 __device__ float clean_observation(const TaskProgramDevice& P, const MRTaskObservationOperatorC& op, const Root& r, const float* q,
-                                   const float* v, const TaskEnvState& st, const float* raw, const float* previous_q) {
+                                   const float* v, const TaskEnvState& st, const float* raw, const float* previous_q,
+                                   const float* metrics) {
     float value = 0.0f;
     const unsigned c = op.component;
     switch (op.opcode) {
@@ -153,6 +154,12 @@ __device__ float clean_observation(const TaskProgramDevice& P, const MRTaskObser
     case MR_TASK_OBSERVE_ROOT_HEIGHT:
         value = r.position.z;
         break;
+    case MR_TASK_OBSERVE_CONTACT_METRIC:  // the group's compact metrics (zero on a reset frame)
+        value = metrics ? metrics[op.source * kTaskGroupMetrics + c] : 0.0f;
+        break;
+    case MR_TASK_OBSERVE_CONTACT_WRENCH_LOCAL:
+        value = metrics ? metrics[op.source * kTaskGroupMetrics + 6 + c] : 0.0f;
+        break;
     case MR_TASK_OBSERVE_GAIT_PHASE: {
         const float magnitude = sqrtf(st.command[0] * st.command[0] + st.command[1] * st.command[1] + st.command[2] * st.command[2]);
         if (magnitude >= 0.1f) value = c == 0u ? sinf(st.phase) : cosf(st.phase);
@@ -168,14 +175,15 @@ __device__ float clean_observation(const TaskProgramDevice& P, const MRTaskObser
 // gravity operators flagged NORMALIZE_VECTOR3 publish the unit vector of
 // their noisy components.
 __device__ void write_frame(const TaskProgramDevice& P, const float* q, const float* v, const TaskEnvState& st, const float* raw,
-                            const float* previous_q, unsigned env, unsigned episode, unsigned step, float* frame, int lane) {
+                            const float* previous_q, const float* metrics, unsigned env, unsigned episode, unsigned step, float* frame,
+                            int lane) {
     const Root r = root_frame(P, q, v);
     float3 g = make_float3(0.0f, 0.0f, -1.0f);
     bool have = false;
     for (int i = 0; i < P.nobs; ++i) {
         const MRTaskObservationOperatorC op = P.actor[i];
         if (op.opcode != MR_TASK_OBSERVE_PROJECTED_GRAVITY || (op.flags & MR_TASK_OBSERVATION_NORMALIZE_VECTOR3) == 0u) continue;
-        const float value = clean_observation(P, op, r, q, v, st, raw, previous_q) +
+        const float value = clean_observation(P, op, r, q, v, st, raw, previous_q, metrics) +
                             op.noise_amplitude * signed_draw(P.seed, env, episode, step, op.noise_channel);
         if (op.component == 0u) g.x = value;
         else if (op.component == 1u) g.y = value;
@@ -189,7 +197,7 @@ __device__ void write_frame(const TaskProgramDevice& P, const float* q, const fl
             frame[i] = lane3(g, op.component);
             continue;
         }
-        frame[i] = clean_observation(P, op, r, q, v, st, raw, previous_q) +
+        frame[i] = clean_observation(P, op, r, q, v, st, raw, previous_q, metrics) +
                    op.noise_amplitude * signed_draw(P.seed, env, episode, step, op.noise_channel);
     }
 }
@@ -207,6 +215,192 @@ __device__ __forceinline__ void sample_command(const TaskProgramDevice& P, unsig
     for (unsigned k = 0; k < 3u; ++k)
         out[k] = range_draw(P.seed, env, episode, step, 16u + k, P.command_lower[k], P.command_upper[k]);
     if (unit_draw(P.seed, env, episode, step, 19u) < P.standing_probability) out[0] = out[1] = out[2] = 0.0f;
+}
+
+__device__ __forceinline__ float3 shfl3(float3 a, int src) {
+    return make_float3(__shfl_sync(0xffffffffu, a.x, src), __shfl_sync(0xffffffffu, a.y, src), __shfl_sync(0xffffffffu, a.z, src));
+}
+__device__ __forceinline__ float4 shfl4(float4 a, int src) {
+    return make_float4(__shfl_sync(0xffffffffu, a.x, src), __shfl_sync(0xffffffffu, a.y, src), __shfl_sync(0xffffffffu, a.z, src),
+                       __shfl_sync(0xffffffffu, a.w, src));
+}
+__device__ __forceinline__ float4 normalized4(float4 a) {
+    const float s = rsqrtf(fmaxf(a.x * a.x + a.y * a.y + a.z * a.z + a.w * a.w, 1.0e-30f));
+    return make_float4(a.x * s, a.y * s, a.z * s, a.w * s);
+}
+__device__ __forceinline__ float3 xyz3(float4 a) { return make_float3(a.x, a.y, a.z); }
+
+// World COM position, orientation and twist of body `lane` (the tree's
+// forward kinematics, the articulated step's formulas: revolute joints turn
+// about their axis, prismatic ones slide along it).
+struct BodyFrame {
+    float3 c, v, w;
+    float4 r;
+};
+
+__device__ BodyFrame body_frames(const DeviceModel& M, const float* q, const float* v, int lane) {
+    BodyFrame f;
+    f.c = f.v = f.w = make_float3(0.0f, 0.0f, 0.0f);
+    f.r = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+    const bool mine = lane < M.nb;
+    if (lane == 0 && M.floating) {
+        f.c = make_float3(q[0], q[1], q[2]);
+        f.r = normalized4(make_float4(q[3], q[4], q[5], q[6]));
+        f.v = make_float3(v[0], v[1], v[2]);
+        f.w = make_float3(v[3], v[4], v[5]);
+    }
+    const int depth = mine ? static_cast<int>(M.tables.depth[lane]) : -1;
+    const int par = mine && lane > 0 ? M.parent[lane] : lane;
+    for (int l = 1; l <= M.n_levels; ++l) {
+        const float3 cp = shfl3(f.c, par), wp = shfl3(f.w, par), vp = shfl3(f.v, par);
+        const float4 qp = shfl4(f.r, par);
+        if (depth == l) {
+            const int dof = M.body_dof[lane];
+            const bool has = dof >= 0, prismatic = M.joint_type[lane] == MR_JOINT_PRISMATIC;
+            const float3 axis = xyz3(M.axis[lane]);
+            const float4 pj = quat_product(qp, M.parent_rotation[lane]);
+            float4 motion = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+            float qj = 0.0f, qdj = 0.0f;
+            if (has) {
+                qj = q[M.dof_q[dof]];
+                qdj = v[dof];
+                if (!prismatic) {
+                    float sh, ch;
+                    sincosf(0.5f * qj, &sh, &ch);
+                    motion = make_float4(axis.x * sh, axis.y * sh, axis.z * sh, ch);
+                }
+            }
+            const float4 rb = normalized4(quat_product(quat_product(pj, motion), M.child_rotation_conj[lane]));
+            const float3 ja = rotate(pj, axis);
+            float3 jp = cp + rotate(qp, xyz3(M.parent_anchor[lane]));
+            if (prismatic) jp = jp + qj * ja;
+            const float3 ca = rotate(rb, xyz3(M.child_anchor[lane]));
+            const float3 wb = wp + ((has && !prismatic) ? qdj * ja : make_float3(0.0f, 0.0f, 0.0f));
+            f.v = vp + cross3(wp, jp - cp) + (prismatic ? qdj * ja : make_float3(0.0f, 0.0f, 0.0f)) - cross3(wb, ca);
+            f.c = jp - ca;
+            f.r = rb;
+            f.w = wb;
+        }
+    }
+    return f;
+}
+
+// The contact groups' compact metrics of this step (the reduction of
+// LocomotionTask.metal:4104-4370 over the committed final-microstep
+// contacts): out[g][0..5] force (forbidden groups: the hard-contact flag),
+// slip, air time, clearance, CoP x, y; out[g][6..11] wrench in the
+// reference body's frame.  `air` holds and receives each group's air time.
+__device__ void contact_metrics(const TaskProgramDevice& P, const float* q, const float* v, const float* manifolds, float* air,
+                                float* out, int lane) {
+    const DeviceModel& M = *P.model;
+    const BodyFrame f = body_frames(M, q, v, lane);
+    float imp[kTaskMaxGroups], hard[kTaskMaxGroups], F[kTaskMaxGroups][3], Mo[kTaskMaxGroups][3], Pw[kTaskMaxGroups][3];
+#pragma unroll
+    for (int g = 0; g < kTaskMaxGroups; ++g) {
+        imp[g] = hard[g] = 0.0f;
+        F[g][0] = F[g][1] = F[g][2] = Mo[g][0] = Mo[g][1] = Mo[g][2] = Pw[g][0] = Pw[g][1] = Pw[g][2] = 0.0f;
+    }
+    for (int p0 = 0; p0 < M.np; p0 += 32) {
+        const int pair = p0 + lane;
+        const bool live = pair < M.np;
+        const int sa = live ? M.pair_a[pair] : 0, sb = live ? M.pair_b[pair] : 0;
+        const int body = live ? M.shape_body[sa] : -1;
+        const float4 ra = shfl4(f.r, body >= 0 ? body : 0);
+        const float3 ca = shfl3(f.c, body >= 0 ? body : 0);
+        if (!live || body < 0 || M.shape_body[sb] >= 0) continue;
+        const float* m = manifolds + static_cast<size_t>(pair) * kManifoldWords;
+        const int count = __float_as_int(m[7]);
+        if (count <= 0) continue;
+        float3 n = rotate(ra, make_float3(m[0], m[1], m[2]));
+        n = rsqrtf(fmaxf(dot3(n, n), 1.0e-30f)) * n;
+        float3 t = rotate(ra, make_float3(m[4], m[5], m[6]));
+        t = t - dot3(t, n) * n;
+        if (dot3(t, t) > 1.0e-12f) {
+            t = rsqrtf(dot3(t, t)) * t;
+        } else {  // the solver's stable tangent of the normal
+            const float3 an = make_float3(fabsf(n.x), fabsf(n.y), fabsf(n.z));
+            const float3 ref = an.x <= an.y && an.x <= an.z ? make_float3(1.0f, 0.0f, 0.0f)
+                               : an.y <= an.z              ? make_float3(0.0f, 1.0f, 0.0f)
+                                                           : make_float3(0.0f, 0.0f, 1.0f);
+            t = cross3(ref, n);
+            t = rsqrtf(fmaxf(dot3(t, t), 1.0e-30f)) * t;
+        }
+        const float3 b = cross3(n, t);
+        const float3 pb0 = xyz3(M.static_body_position[sb]);
+        const float4 rb0 = M.static_body_rotation[sb];
+        for (int i = 0; i < count && i < kManifoldPoints; ++i) {
+            const float* pt = m + 8 + i * 12;
+            const float3 pa = ca + rotate(ra, make_float3(pt[0], pt[1], pt[2]));
+            const float3 pw = 0.5f * (pa + pb0 + rotate(rb0, make_float3(pt[3], pt[4], pt[5])));
+            const float ln = pt[9], lt = pt[10], lb = pt[11];
+            // Impulse on the robot (shape A): -(n ln + t lt + b lb).
+            const float3 fo = make_float3(-(n.x * ln + t.x * lt + b.x * lb), -(n.y * ln + t.y * lt + b.y * lb),
+                                          -(n.z * ln + t.z * lt + b.z * lb));
+            const float3 mo = cross3(pw, fo);
+            const float a = fabsf(ln);
+            for (int g = 0; g < P.ncontact_groups; ++g) {
+                const MRTaskContactGroupC G = P.contact_groups[g];
+                bool member = false;
+                for (unsigned k = 0; k < G.count; ++k) member = member || P.contact_members[G.first + k] == static_cast<unsigned>(body);
+                if (!member) continue;
+                imp[g] += a;
+                hard[g] = fmaxf(hard[g], a);
+                F[g][0] += fo.x; F[g][1] += fo.y; F[g][2] += fo.z;
+                Mo[g][0] += mo.x; Mo[g][1] += mo.y; Mo[g][2] += mo.z;
+                Pw[g][0] += a * pw.x; Pw[g][1] += a * pw.y; Pw[g][2] += a * pw.z;
+            }
+        }
+    }
+    const float inv_h = 1.0f / P.physics_dt;
+    for (int g = 0; g < P.ncontact_groups; ++g) {
+        const MRTaskContactGroupC G = P.contact_groups[g];
+        const float si = warp_sum(imp[g]);
+        float hg = hard[g];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) hg = fmaxf(hg, __shfl_xor_sync(0xffffffffu, hg, o));
+        const float3 Fw = inv_h * make_float3(warp_sum(F[g][0]), warp_sum(F[g][1]), warp_sum(F[g][2]));
+        const float3 Mw = inv_h * make_float3(warp_sum(Mo[g][0]), warp_sum(Mo[g][1]), warp_sum(Mo[g][2]));
+        const float3 Pa = make_float3(warp_sum(Pw[g][0]), warp_sum(Pw[g][1]), warp_sum(Pw[g][2]));
+        const int rbody = static_cast<int>(G.reference_body);
+        const float3 cr = shfl3(f.c, rbody), vr = shfl3(f.v, rbody), wr = shfl3(f.w, rbody);
+        const float4 rr = shfl4(f.r, rbody);
+        const float3 ref = cr + rotate(rr, xyz3(make_float4(G.local_reference[0], G.local_reference[1], G.local_reference[2], 0.0f)));
+        float* o = out + g * kTaskGroupMetrics;
+        const float3 fl = rotate_inverse(rr, Fw);
+        const float3 tl = rotate_inverse(rr, Mw - cross3(ref, Fw));
+        o[6] = fl.x; o[7] = fl.y; o[8] = fl.z;
+        o[9] = tl.x; o[10] = tl.y; o[11] = tl.z;
+        o[1] = o[2] = o[3] = o[4] = o[5] = 0.0f;
+        if (G.flags & MR_TASK_CONTACT_SUPPORT) {
+            const float force = si * inv_h;
+            const bool touching = force > P.support_force_threshold;
+            const float3 koff = rotate(rr, make_float3(G.kinematic_reference[0], G.kinematic_reference[1], G.kinematic_reference[2]));
+            const float3 kv = vr + cross3(wr, koff);
+            const float air_prev = air[g];
+            o[0] = force;
+            o[1] = touching ? sqrtf(kv.x * kv.x + kv.y * kv.y) : 0.0f;
+            o[2] = touching ? 0.0f : air_prev + P.dt;
+            o[3] = ref.z - G.local_reference[3] - P.ground_height;
+            if (si > 1.0e-6f) {
+                const float3 cl = rotate_inverse(rr, Pa - si * ref);
+                o[4] = cl.x / si;
+                o[5] = cl.y / si;
+            }
+        } else if (G.flags & MR_TASK_CONTACT_FORBIDDEN) {
+            o[0] = hg * inv_h > P.support_force_threshold ? 1.0f : 0.0f;
+        } else {
+            o[0] = 0.0f;
+        }
+    }
+    __syncwarp();
+    if (lane < P.ncontact_groups) air[lane] = out[lane * kTaskGroupMetrics + 2];
+}
+
+// desiredSupportContact (:1617-1630).
+__device__ __forceinline__ bool desired_support(const MRTaskContactGroupC& G, float phase) {
+    float x = fmodf(phase + G.gait_phase_offset, kTwoPi);
+    if (x < 0.0f) x += kTwoPi;
+    return x / kTwoPi < G.stance_fraction;
 }
 
 __global__ void __launch_bounds__(32 * kTaskWarps) task_observe_kernel(TaskParams p) {
@@ -275,6 +469,7 @@ __global__ void __launch_bounds__(32 * kTaskWarps) task_observe_kernel(TaskParam
         float* hist = p.action_history + static_cast<size_t>(local) * P.history * P.na;
         float* prev = p.previous_joint + static_cast<size_t>(local) * 2 * P.na;
         for (int i = lane; i < P.history * P.na; i += 32) hist[i] = 0.0f;
+        if (lane < kTaskMaxGroups) p.air_time[static_cast<size_t>(local) * kTaskMaxGroups + lane] = 0.0f;
         for (int a = lane; a < P.na; a += 32) {
             prev[a] = 0.0f;
             prev[P.na + a] = rq[P.actions[a].q_index];
@@ -294,7 +489,7 @@ __global__ void __launch_bounds__(32 * kTaskWarps) task_observe_kernel(TaskParam
         __syncwarp();
         // Every delay-line slot is zero here; the newest raw slot stands for
         // all of them.
-        write_frame(P, rq, rv, st, hist + (P.history - 2) * P.na, prev + P.na, env, episode, 0u, frame, lane);
+        write_frame(P, rq, rv, st, hist + (P.history - 2) * P.na, prev + P.na, nullptr, env, episode, 0u, frame, lane);
         if (lane == 0) p.state[local] = st;
     }
     if (lane == 0) p.masks_out[local] = reset ? 1u : 0u;
@@ -378,6 +573,11 @@ __global__ void __launch_bounds__(32 * kTaskWarps) task_complete_kernel(TaskPara
     lim2 = warp_sum(lim2);
 
     const float phase = fmodf(st.phase + kTwoPi * P.dt / P.gait_period, kTwoPi);
+    const bool moving = sqrtf(st.command[0] * st.command[0] + st.command[1] * st.command[1] + st.command[2] * st.command[2]) > 0.1f;
+    float gm[kTaskMaxGroups * kTaskGroupMetrics];
+    if (P.ncontact_groups > 0)
+        contact_metrics(P, q, v, p.manifolds + static_cast<size_t>(local) * P.model->np * kManifoldWords,
+                        p.air_time + static_cast<size_t>(local) * kTaskMaxGroups, gm, lane);
 
     float reward = 0.0f;
     float b0[4] = {0.0f, 0.0f, 0.0f, 0.0f}, b1[4] = {0.0f, 0.0f, 0.0f, 0.0f};
@@ -459,6 +659,47 @@ __global__ void __launch_bounds__(32 * kTaskWarps) task_complete_kernel(TaskPara
             value = op.opcode == MR_TASK_REWARD_JOINT_GROUP_POSTURE_SQUARED ? sum / fmaxf(static_cast<float>(g.count), 1.0f) : sum;
             break;
         }
+        case MR_TASK_REWARD_GAIT_CONTACT_MATCH:
+        case MR_TASK_REWARD_SWING_CLEARANCE:
+        case MR_TASK_REWARD_FOOT_CLEARANCE:
+        case MR_TASK_REWARD_SUPPORT_SLIP:
+        case MR_TASK_REWARD_FORBIDDEN_CONTACT: {
+            // The contact-group operators (:5405-5553); `group` selects one
+            // group, MR_INVALID_INDEX every group.
+            float acc = 0.0f, count = 0.0f;
+            for (int g = 0; g < P.ncontact_groups; ++g) {
+                if (op.group != MR_INVALID_INDEX && op.group != static_cast<unsigned>(g)) continue;
+                const MRTaskContactGroupC G = P.contact_groups[g];
+                const float* m = gm + g * kTaskGroupMetrics;
+                const bool support = (G.flags & MR_TASK_CONTACT_SUPPORT) != 0u;
+                if (op.opcode == MR_TASK_REWARD_GAIT_CONTACT_MATCH && support) {
+                    acc += desired_support(G, phase) == (m[0] > P.support_force_threshold) ? 1.0f : 0.0f;
+                } else if (op.opcode == MR_TASK_REWARD_SWING_CLEARANCE && support && !desired_support(G, phase)) {
+                    const float e = m[3] - P.clearance_target;
+                    acc += expf(-(e * e) / fmaxf(op.parameters[0], 1.0e-8f));
+                    count += 1.0f;
+                } else if (op.opcode == MR_TASK_REWARD_SUPPORT_SLIP && support) {
+                    acc += m[1];
+                } else if (op.opcode == MR_TASK_REWARD_FORBIDDEN_CONTACT && (G.flags & MR_TASK_CONTACT_FORBIDDEN)) {
+                    acc = fmaxf(acc, m[0]);
+                } else if (op.opcode == MR_TASK_REWARD_FOOT_CLEARANCE && support) {
+                    // Height of the kinematic reference point, weighted by its planar speed.
+                    const int rb = static_cast<int>(G.reference_body);
+                    const BodyFrame fr = body_frames(*P.model, q, v, lane);
+                    const float3 c = shfl3(fr.c, rb), vb = shfl3(fr.v, rb), wb = shfl3(fr.w, rb);
+                    const float4 r = shfl4(fr.r, rb);
+                    const float3 off = rotate(r, make_float3(G.kinematic_reference[0], G.kinematic_reference[1], G.kinematic_reference[2]));
+                    const float3 vel = vb + cross3(wb, off);
+                    const float e = c.z + off.z - P.clearance_target;
+                    acc += e * e * tanhf(op.parameters[1] * sqrtf(vel.x * vel.x + vel.y * vel.y));
+                }
+            }
+            if (op.opcode == MR_TASK_REWARD_FOOT_CLEARANCE) value = expf(-acc / fmaxf(op.parameters[0], 1.0e-8f));
+            else if (op.opcode == MR_TASK_REWARD_SWING_CLEARANCE) value = moving ? acc / fmaxf(count, 1.0f) : 0.0f;
+            else if (op.opcode == MR_TASK_REWARD_GAIT_CONTACT_MATCH) value = moving ? acc : 0.0f;
+            else value = acc;
+            break;
+        }
         default:
             break;
         }
@@ -469,7 +710,14 @@ __global__ void __launch_bounds__(32 * kTaskWarps) task_complete_kernel(TaskPara
         case MR_TASK_REWARD_LINEAR_VELOCITY_TRACKING:
         case MR_TASK_REWARD_YAW_VELOCITY_TRACKING:
         case MR_TASK_REWARD_CONSTANT:
+        case MR_TASK_REWARD_GAIT_CONTACT_MATCH:
+        case MR_TASK_REWARD_SWING_CLEARANCE:
+        case MR_TASK_REWARD_FOOT_CLEARANCE:
             b0[0] += contribution;
+            break;
+        case MR_TASK_REWARD_SUPPORT_SLIP:
+        case MR_TASK_REWARD_FORBIDDEN_CONTACT:
+            b1[3] += contribution;
             break;
         case MR_TASK_REWARD_JOINT_VELOCITY_SQUARED:
             b0[2] += contribution;
@@ -502,7 +750,9 @@ __global__ void __launch_bounds__(32 * kTaskWarps) task_complete_kernel(TaskPara
         const MRTaskTerminationOperatorC op = P.terminations[k];
         const bool triggered = op.opcode == MR_TASK_TERMINATE_MINIMUM_ROOT_HEIGHT ? height < op.threshold
                                : op.opcode == MR_TASK_TERMINATE_MAXIMUM_TILT        ? tilt > op.threshold
-                                                                                    : false;
+                               : op.opcode == MR_TASK_TERMINATE_CONTACT_GROUP
+                                   ? gm[op.group * kTaskGroupMetrics] > op.threshold
+                                   : false;
         if (triggered && (!done || op.priority >= priority)) {
             done = true;
             reason = op.reason;
@@ -551,7 +801,7 @@ __global__ void __launch_bounds__(32 * kTaskWarps) task_complete_kernel(TaskPara
     // The next decision's frame, then this step's joint history (:6478-6630).
     if (!done || (timeout && !physics_error)) {
         float* frame = p.frame + static_cast<size_t>(local) * P.nobs;
-        write_frame(P, q, v, st, hist + raw_last * P.na, prev + P.na, env, st.episode, episode_steps, frame, lane);
+        write_frame(P, q, v, st, hist + raw_last * P.na, prev + P.na, gm, env, st.episode, episode_steps, frame, lane);
         __syncwarp();
         for (int a = lane; a < P.na; a += 32) {
             const MRTaskActionBindingC b = P.actions[a];

@@ -9,11 +9,14 @@
 
 #include <cuda_runtime.h>
 
+#include "device_model.h"
 #include "numi_b200.h"
 
 namespace numi {
 
 constexpr int kTaskMaxActions = 64;
+constexpr int kTaskMaxGroups = 8;          // contact groups
+constexpr int kTaskGroupMetrics = 12;      // per group: force, slip, air time, clearance, CoP x, y; wrench force xyz, torque xyz
 constexpr int kTaskMaxObservations = 256;  // the policy's widest input
 constexpr int kTaskMaxHistory = 8;
 
@@ -48,6 +51,11 @@ struct TaskProgramDevice {
     const float* default_q;    // [nq]
     const float* limit_lower;  // [na]: position limits of each action's DoF
     const float* limit_upper;
+    const MRTaskContactGroupC* contact_groups;
+    const std::uint32_t* contact_members;
+    const DeviceModel* model;  // the world (body tree, shapes, pairs) for the contact groups' kinematics
+    std::int32_t ncontact_groups;
+    float support_force_threshold, clearance_target, physics_dt, ground_height;
     std::int32_t na, nobs, nrewards, nterminations, nrandom, ngroups;
     std::int32_t history, delay, max_episode_steps, nq, nv;
     std::int32_t fixed_root;   // the root is welded to the world: root sources read zero
@@ -76,6 +84,8 @@ struct TaskParams {
     const float* actions;          // [env][na] of this step
     float* targets;                // [env][na]: drive targets for the control step
     const std::uint32_t* status;   // [env] of this step
+    const float* manifolds;        // [env][pair][56]: the step's committed contacts (contact groups)
+    float* air_time;               // [env][kTaskMaxGroups]
     MRTaskTransitionC* transitions;// [env] of this step
     unsigned long long policy_revision;
     std::int32_t env_count, env_base;

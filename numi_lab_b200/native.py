@@ -362,7 +362,7 @@ class TaskTerminationOperatorC(ct.Structure):
         ("opcode", ct.c_uint32),
         ("reason", ct.c_uint32),
         ("priority", ct.c_uint32),
-        ("reserved", ct.c_uint32),
+        ("group", ct.c_uint32),
         ("threshold", ct.c_float),
         ("failure_penalty", ct.c_float),
     ]
@@ -378,6 +378,20 @@ class TaskRandomizationOperatorC(ct.Structure):
 
 class TaskIndexGroupC(ct.Structure):
     _fields_ = [("first", ct.c_uint32), ("count", ct.c_uint32)]
+
+
+class TaskContactGroupC(ct.Structure):
+    _fields_ = [
+        ("first", ct.c_uint32),
+        ("count", ct.c_uint32),
+        ("flags", ct.c_uint32),
+        ("reference_body", ct.c_uint32),
+        ("local_reference", ct.c_float * 4),
+        ("kinematic_reference", ct.c_float * 4),
+        ("gait_phase_offset", ct.c_float),
+        ("stance_fraction", ct.c_float),
+        ("reserved", ct.c_float * 2),
+    ]
 
 
 class TaskProgramC(ct.Structure):
@@ -396,6 +410,12 @@ class TaskProgramC(ct.Structure):
         ("joint_group_count", ct.c_uint32),
         ("joint_members", ct.POINTER(ct.c_uint32)),
         ("joint_member_count", ct.c_uint32),
+        ("contact_groups", ct.POINTER(TaskContactGroupC)),
+        ("contact_group_count", ct.c_uint32),
+        ("contact_members", ct.POINTER(ct.c_uint32)),
+        ("contact_member_count", ct.c_uint32),
+        ("support_force_threshold", ct.c_float),
+        ("clearance_target", ct.c_float),
         ("default_q", ct.POINTER(ct.c_float)),
         ("default_q_count", ct.c_uint32),
         ("maximum_episode_steps", ct.c_uint32),

@@ -27,18 +27,21 @@ from . import native
 # MRTaskTerminationReason / MRTaskRandomizationOpcode (the evaluated subset).
 OBSERVE = {
     "root_angular_velocity_local": 0, "projected_gravity": 1, "command": 2, "joint_position_error": 3, "joint_velocity": 4,
-    "previous_action": 5, "root_linear_velocity_local": 6, "root_height": 7, "gait_phase": 14, "delayed_action": 26,
-    "joint_finite_difference_velocity": 27,
+    "previous_action": 5, "root_linear_velocity_local": 6, "root_height": 7, "contact_metric": 8, "contact_wrench_local": 13,
+    "gait_phase": 14, "delayed_action": 26, "joint_finite_difference_velocity": 27,
 }
 NORMALIZE_VECTOR3 = 1
 REWARD = {
     "linear_velocity_tracking": 0, "yaw_velocity_tracking": 1, "constant": 2, "root_vertical_velocity_squared": 3,
     "root_roll_pitch_velocity_squared": 4, "tilt_squared": 5, "root_height_error_squared": 6, "joint_velocity_squared": 7,
     "joint_acceleration_squared": 8, "action_rate_squared": 9, "joint_limit_violation_squared": 10,
-    "joint_group_posture_squared": 12, "joint_group_posture_absolute": 17, "projected_gravity_horizontal_squared": 18,
+    "joint_group_posture_squared": 12, "gait_contact_match": 13, "swing_clearance": 14, "support_slip": 15, "forbidden_contact": 16,
+    "joint_group_posture_absolute": 17, "projected_gravity_horizontal_squared": 18, "foot_clearance": 19,
     "joint_limit_violation_absolute": 20, "root_height_normalized": 21, "root_height_progress": 22, "uprightness": 23,
 }
-TERMINATE = {"minimum_root_height": 0, "maximum_tilt": 1}
+TERMINATE = {"minimum_root_height": 0, "maximum_tilt": 1, "contact_group": 2}
+CONTACT_SUPPORT, CONTACT_FORBIDDEN = 1, 2
+ALL_GROUPS = 0xFFFFFFFF
 REASON = {"continuing": 0, "height": 1, "tilt": 2, "contact": 3, "timeout": 4, "physics_error": 5}
 RANDOMIZE = {
     "root_position": 0, "root_yaw": 1, "action_position": 2, "velocity": 3, "action_velocity": 9, "root_height": 10,
@@ -84,6 +87,18 @@ class Termination:
     priority: int
     threshold: float
     failure_penalty: float = 0.0
+    group: int = 0
+
+
+@dataclass
+class ContactGroup:
+    bodies: list[int]
+    flags: int
+    reference_body: int
+    local_reference: tuple[float, float, float, float] = (0.0, 0.0, 0.0, 0.0)
+    kinematic_reference: tuple[float, float, float] = (0.0, 0.0, 0.0)
+    gait_phase_offset: float = 0.0
+    stance_fraction: float = 0.5
 
 
 @dataclass
@@ -102,6 +117,9 @@ class TaskProgram:
     terminations: list[Termination] = field(default_factory=list)
     randomization: list[Randomization] = field(default_factory=list)
     joint_groups: list[list[int]] = field(default_factory=list)  # action indices
+    contact_groups: list[ContactGroup] = field(default_factory=list)
+    support_force_threshold: float = 1.0
+    clearance_target: float = 0.08
     maximum_episode_steps: int = 500
     action_history: int = 3
     action_delay_steps: int = 0
@@ -141,6 +159,7 @@ def task_program_c(program: TaskProgram) -> tuple[native.TaskProgramC, list[Any]
 
     def fill_term(c, t: Termination):
         c.opcode, c.reason, c.priority, c.threshold, c.failure_penalty = t.opcode, t.reason, t.priority, t.threshold, t.failure_penalty
+        c.group = t.group
 
     def fill_random(c, r: Randomization):
         c.opcode, c.target = r.opcode, r.target
@@ -165,6 +184,25 @@ def task_program_c(program: TaskProgram) -> tuple[native.TaskProgramC, list[Any]
     m = np.ascontiguousarray(members if members else [0], np.uint32)
     keep.append(m)
     p.joint_members, p.joint_member_count = m.ctypes.data_as(ct.POINTER(ct.c_uint32)), len(members)
+    bodies: list[int] = []
+    cgroups = []
+    for g in program.contact_groups:
+        cgroups.append((len(bodies), g))
+        bodies.extend(int(b) for b in g.bodies)
+
+    def fill_cgroup(c, item):
+        first, g = item
+        c.first, c.count, c.flags, c.reference_body = first, len(g.bodies), g.flags, g.reference_body
+        c.local_reference[:] = list(g.local_reference)
+        c.kinematic_reference[:] = list(g.kinematic_reference) + [0.0]
+        c.gait_phase_offset, c.stance_fraction = g.gait_phase_offset, g.stance_fraction
+
+    p.contact_groups, p.contact_group_count = table(native.TaskContactGroupC, cgroups, fill_cgroup)
+    cm = np.ascontiguousarray(bodies if bodies else [0], np.uint32)
+    keep.append(cm)
+    p.contact_members, p.contact_member_count = cm.ctypes.data_as(ct.POINTER(ct.c_uint32)), len(bodies)
+    p.support_force_threshold = program.support_force_threshold
+    p.clearance_target = program.clearance_target
     dq = np.ascontiguousarray(program.default_q, np.float32)
     keep.append(dq)
     p.default_q, p.default_q_count = dq.ctypes.data_as(ct.POINTER(ct.c_float)), dq.size
@@ -201,16 +239,40 @@ def action_bindings(records, *, scale: float = 0.25, response_time_seconds: floa
     return out
 
 
+def foot_contact_groups(records, *, forbidden_bodies: Sequence[int] = (0,), stance_fraction: float = 0.6) -> list[ContactGroup]:
+    """Support groups for the bodies that carry box collision shapes (the
+    feet of the synthetic humanoid tree), each referenced at its box's sole
+    centre, alternating gait phase; then one forbidden group over
+    `forbidden_bodies` (the torso by default), referenced at the first."""
+
+    groups = []
+    for i in range(int(records.world.shape_count)):
+        sh = records.shapes[i]
+        if int(sh.shape_type) != 2 or int(sh.body) >= int(records.world.body_count) - 1:
+            continue
+        body = int(sh.body)
+        sole = (float(sh.local_position[0]), float(sh.local_position[1]), float(sh.local_position[2]) - float(sh.dimensions[2]), 0.0)
+        groups.append(ContactGroup([body], CONTACT_SUPPORT, body, sole, (0.0, 0.0, 0.0), np.pi * (len(groups) % 2), stance_fraction))
+    if forbidden_bodies:
+        groups.append(ContactGroup(list(forbidden_bodies), CONTACT_FORBIDDEN, int(forbidden_bodies[0])))
+    return groups
+
+
 def locomotion_task(records, default_q: np.ndarray, *, base_height: float | None = None, maximum_episode_steps: int = 500,
                     action_scale: float = 0.25, response_time_seconds: float = 0.0, action_history: int = 3,
                     action_delay_steps: int = 0, noise: float = 0.0, min_height_fraction: float = 0.6,
-                    max_tilt: float = 1.22173048, groups: Sequence[Sequence[int]] | None = None) -> TaskProgram:
+                    max_tilt: float = 1.22173048, groups: Sequence[Sequence[int]] | None = None,
+                    contact_groups: Sequence[ContactGroup] | None = None, support_force_threshold: float = 1.0,
+                    clearance_target: float = 0.08) -> TaskProgram:
     """Velocity-tracking locomotion over every actuated joint of an
     articulated world with a floating root.  Actor frame (per the reference's
     G1 legs frame): raw action one step back, command xyz + extension lane,
     joint position errors, finite-difference joint velocities, normalised
     projected gravity, gait phase sin/cos, root angular velocity in the root
-    frame."""
+    frame; with `contact_groups`, each support group's normal force and air
+    time, and the gait-contact, foot-clearance, swing-clearance, support-slip
+    and forbidden-contact rewards of the reference's G1 tasks, and a
+    forbidden group's contact ending the episode."""
 
     actions = action_bindings(records, scale=action_scale, response_time_seconds=response_time_seconds)
     na = len(actions)
@@ -252,13 +314,30 @@ def locomotion_task(records, default_q: np.ndarray, *, base_height: float | None
         Termination(TERMINATE["minimum_root_height"], REASON["height"], 1, min_height_fraction * height, -2.0),
         Termination(TERMINATE["maximum_tilt"], REASON["tilt"], 2, max_tilt, -2.0),
     ]
+    cgroups = list(contact_groups or [])
+    for g, cg in enumerate(cgroups):
+        if cg.flags & CONTACT_SUPPORT:
+            actor.append(obs("contact_metric", g, 0, scale=0.002))
+            actor.append(obs("contact_metric", g, 2, noise=0.0))
+    if cgroups:
+        rewards += [
+            Reward(REWARD["gait_contact_match"], 0.5, group=ALL_GROUPS),
+            Reward(REWARD["foot_clearance"], 1.0, (0.05, 2.0, 0.0), group=ALL_GROUPS),
+            Reward(REWARD["swing_clearance"], 0.25, (0.01, 0.0, 0.0), group=ALL_GROUPS),
+            Reward(REWARD["support_slip"], -0.2, group=ALL_GROUPS),
+            Reward(REWARD["forbidden_contact"], -1.0, group=ALL_GROUPS),
+        ]
+        for g, cg in enumerate(cgroups):
+            if cg.flags & CONTACT_FORBIDDEN:
+                terminations.append(Termination(TERMINATE["contact_group"], REASON["contact"], 3, 0.5, -2.0, group=g))
     randomization = [
         Randomization(RANDOMIZE["root_yaw"], (-np.pi, np.pi, 0.0, 0.0)),
         Randomization(RANDOMIZE["action_position"], (-0.1, 0.1, 0.0, 0.0)),
         Randomization(RANDOMIZE["action_velocity"], (-0.2, 0.2, 0.0, 0.0)),
     ]
     return TaskProgram(actions=actions, actor=actor, default_q=dq, rewards=rewards, terminations=terminations,
-                       randomization=randomization, joint_groups=[list(g) for g in groups],
+                       randomization=randomization, joint_groups=[list(g) for g in groups], contact_groups=cgroups,
+                       support_force_threshold=support_force_threshold, clearance_target=clearance_target,
                        maximum_episode_steps=maximum_episode_steps, action_history=action_history,
                        action_delay_steps=action_delay_steps, base_height_target=height, gait_period_seconds=0.8,
                        command_lower=(-0.5, -0.3, -0.5), command_upper=(1.0, 0.3, 0.5), standing_probability=0.1,

@@ -293,6 +293,8 @@ class Oracle:
         lib.oracle_aba.argtypes = [ct.c_void_p, _DP, _DP, _DP, _DP]
         lib.oracle_mass_matrix.restype = ct.c_uint32
         lib.oracle_mass_matrix.argtypes = [ct.c_void_p, _DP, _DP]
+        lib.oracle_body_states.restype = ct.c_uint32
+        lib.oracle_body_states.argtypes = [ct.c_void_p, _DP, _DP, _DP]
         lib.oracle_point_jacobian.restype = ct.c_uint32
         lib.oracle_point_jacobian.argtypes = [ct.c_void_p, _DP, ct.c_uint32, _DP, _DP, _DP]
         lib.oracle_drive_efforts.argtypes = [ct.c_void_p, _DP, _DP, _DP, _DP]
@@ -373,6 +375,16 @@ class Oracle:
         st = self.lib.oracle_aba(self.handle, _dp(np.ascontiguousarray(q, np.float64)), _dp(np.ascontiguousarray(v, np.float64)),
                                  _dp(np.ascontiguousarray(tau, np.float64)), _dp(out))
         return int(st), out
+
+    def body_states(self, q: np.ndarray, v: np.ndarray) -> np.ndarray:
+        """[nb][13]: world COM position, orientation xyzw, linear and angular velocity."""
+
+        out = np.zeros((int(self.records.world.body_count), 13))
+        st = self.lib.oracle_body_states(self.handle, _dp(np.ascontiguousarray(q, np.float64)), _dp(np.ascontiguousarray(v, np.float64)),
+                                         _dp(out))
+        if st != 0:
+            raise ValueError(f"oracle_body_states failed ({st})")
+        return out
 
     def mass_matrix(self, q) -> np.ndarray:
         out = np.zeros((self.nv, self.nv))

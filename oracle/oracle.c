@@ -562,6 +562,25 @@ static void mass_matrix_k(const OracleWorld* o, const Kin* k, double* Mm) {
     }
 }
 
+/* World COM position, orientation (xyzw) and linear / angular velocity of
+ * every articulated body ([nb][13]) from the kinematics pass: the task
+ * layer's body states (LocomotionTask.metal reads bodyStates). */
+uint32_t oracle_body_states(const OracleWorld* o, const double* q, const double* v, double* out) {
+    Kin* k = (Kin*)malloc(sizeof(Kin));
+    if (!k) return MR_STEP_UNSUPPORTED;
+    const uint32_t st = kinematics(o, q, v, k);
+    if (st == MR_STEP_SUCCESS)
+        for (uint32_t b = 0; b < o->nb; ++b) {
+            double* r = out + 13 * b;
+            r[0] = k->pos[b].x; r[1] = k->pos[b].y; r[2] = k->pos[b].z;
+            r[3] = k->rot[b].x; r[4] = k->rot[b].y; r[5] = k->rot[b].z; r[6] = k->rot[b].w;
+            r[7] = k->v[b].x; r[8] = k->v[b].y; r[9] = k->v[b].z;
+            r[10] = k->w[b].x; r[11] = k->w[b].y; r[12] = k->w[b].z;
+        }
+    free(k);
+    return st;
+}
+
 uint32_t oracle_mass_matrix(const OracleWorld* o, const double* q, double* mass) {
     double v0[MAXV] = {0};
     Kin k;

@@ -13,7 +13,9 @@ kernels for the operator subset the device evaluates
 * ``complete`` -- mr_locomotion_task_complete (:3904-6745): reward inputs
   (:4376-4500), reward operators (:4700-5960), breakdown lanes (:5985-6046),
   terminations (:6064-6160), command schedule and state (:6388-6440), next
-  actor frame and joint history (:6478-6630), transition (:6697-6742).
+  actor frame and joint history (:6478-6630), transition (:6697-6742);
+  the contact groups' metrics (:4104-4370) from the committed contacts and
+  the contact-group rewards (:5405-5553).
 
 Draws use the reference's keyed counter hash (randomUnit :121-152): a key of
 seed, environment, episode, control step and channel through SplitMix64's
@@ -43,7 +45,12 @@ R_LINEAR, R_YAW, R_CONSTANT, R_VERTICAL, R_ROLL_PITCH, R_TILT, R_HEIGHT_ERROR = 
 R_JOINT_VELOCITY, R_JOINT_ACCELERATION, R_ACTION_RATE, R_LIMIT_SQUARED = 7, 8, 9, 10
 R_POSTURE_SQUARED, R_POSTURE_ABSOLUTE, R_GRAVITY_HORIZONTAL, R_LIMIT_ABSOLUTE = 12, 17, 18, 20
 R_HEIGHT_NORMALIZED, R_HEIGHT_PROGRESS, R_UPRIGHTNESS = 21, 22, 23
-T_MIN_HEIGHT, T_MAX_TILT = 0, 1
+R_GAIT_MATCH, R_SWING_CLEARANCE, R_SUPPORT_SLIP, R_FORBIDDEN, R_FOOT_CLEARANCE = 13, 14, 15, 16, 19
+OBS_CONTACT_METRIC, OBS_CONTACT_WRENCH = 8, 13
+T_MIN_HEIGHT, T_MAX_TILT, T_CONTACT_GROUP = 0, 1, 2
+SUPPORT, FORBIDDEN = 1, 2
+ALL_GROUPS = 0xFFFFFFFF
+MANIFOLD_POINTS = 4
 REASON_CONTINUING, REASON_TIMEOUT, REASON_PHYSICS_ERROR = 0, 4, 5
 RND_ROOT_POSITION, RND_ROOT_YAW, RND_ACTION_POSITION, RND_VELOCITY = 0, 1, 2, 3
 RND_ACTION_VELOCITY, RND_ROOT_HEIGHT, RND_JOINT_POSITION = 9, 10, 12
@@ -101,6 +108,14 @@ def normalized_or(v, fallback):
     return np.asarray(v, np.float64) / math.sqrt(l2) if l2 > 1.0e-12 and math.isfinite(l2) else np.asarray(fallback, np.float64)
 
 
+def stable_tangent(n):
+    a = np.abs(n)
+    ref = np.array([1.0, 0.0, 0.0]) if a[0] <= a[1] and a[0] <= a[2] else (np.array([0.0, 1.0, 0.0]) if a[1] <= a[2] else
+                                                                           np.array([0.0, 0.0, 1.0]))
+    t = np.cross(ref, n)
+    return t / np.linalg.norm(t)
+
+
 @dataclass
 class EnvState:
     """One environment's task record (MRTaskStateGPU's used lanes) plus its
@@ -120,13 +135,18 @@ class EnvState:
     previous_height: float = 0.0
     episode_return: float = 0.0
     episode_tracking: float = 0.0
+    air: np.ndarray = field(default_factory=lambda: np.zeros(8))
 
 
 class TaskOracle:
     """The task layer over one rollout: `program` a numi_lab_b200.task.TaskProgram."""
 
     def __init__(self, program, *, nq: int, nv: int, dt: float, seed: int, fixed_root: bool, limit_lower, limit_upper,
-                 terminations: bool = True) -> None:
+                 terminations: bool = True, records=None, world=None, physics_dt: float = 0.0) -> None:
+        """`records` (compiled world) and `world` (an oracle.Oracle of it,
+        for body states) serve the contact groups; `physics_dt` is the
+        microstep."""
+
         self.p = program
         self.nq, self.nv, self.dt, self.seed, self.fixed_root = nq, nv, float(dt), int(seed), fixed_root
         self.na = len(program.actions)
@@ -137,6 +157,95 @@ class TaskOracle:
         self.hi = np.asarray(limit_upper, np.float64)
         self.default_q = np.asarray(program.default_q, np.float64)
         self.terminations = program.terminations if terminations else []
+        self.records, self.world, self.physics_dt = records, world, float(physics_dt)
+        self.groups = list(getattr(program, "contact_groups", []))
+        self.metrics = np.zeros((len(self.groups), 12))
+        if records is not None:
+            self.ground = 0.0
+            for i in range(int(records.world.shape_count)):
+                sh = records.shapes[i]
+                if int(sh.shape_type) == 3:
+                    pose = np.array(records.bodies[int(sh.body)].static_pose, np.float64)
+                    self.ground = float(pose[2] + rotate(pose[4:8] / np.linalg.norm(pose[4:8]), np.array(sh.local_position[:3], np.float64))[2])
+                    self.plane_pose = (pose[:3], pose[4:8] / np.linalg.norm(pose[4:8]))
+                    break
+
+    # -- contact groups (LocomotionTask.metal:4104-4370) -------------------------
+    def contact_metrics(self, st: EnvState, q, v, manifolds) -> np.ndarray:
+        """[group][12] metrics of one finished step from its committed
+        manifolds (MRManifoldC, one per compiled pair): force (forbidden
+        groups: the hard-contact flag), slip, air time, clearance, CoP x, y,
+        then the wrench in the reference body's frame.  Updates st.air."""
+
+        rec = self.records
+        bs = self.world.body_states(np.asarray(q, np.float64), np.asarray(v, np.float64))
+        ng = len(self.groups)
+        imp, hard = np.zeros(ng), np.zeros(ng)
+        F, Mo, Pw = np.zeros((ng, 3)), np.zeros((ng, 3)), np.zeros((ng, 3))
+        for pidx in range(int(rec.world.pair_count)):
+            pr = rec.pairs[pidx]
+            sa, sb = rec.shapes[int(pr.shape_a)], rec.shapes[int(pr.shape_b)]
+            body = int(sa.body)
+            if int(rec.bodies[int(sb.body)].articulated) or not int(rec.bodies[body].articulated):
+                continue
+            m = manifolds[pidx]
+            count = int(m.count)
+            if count <= 0:
+                continue
+            ra, ca = bs[body, 3:7], bs[body, :3]
+            n = rotate(ra, np.array(m.normal_local, np.float64))
+            n = n / np.linalg.norm(n)
+            t = rotate(ra, np.array(m.tangent_local, np.float64))
+            t = t - np.dot(t, n) * n
+            t = t / np.linalg.norm(t) if np.dot(t, t) > 1e-12 else stable_tangent(n)
+            b = np.cross(n, t)
+            for i in range(min(count, MANIFOLD_POINTS)):
+                pt = m.points[i]
+                pa = ca + rotate(ra, np.array(pt.anchor_a, np.float64))
+                pb = self.plane_pose[0] + rotate(self.plane_pose[1], np.array(pt.anchor_b, np.float64))
+                pw = 0.5 * (pa + pb)
+                ln, lt, lb = (float(x) for x in pt.impulses)
+                fo = -(n * ln + t * lt + b * lb)
+                a = abs(ln)
+                for g, G in enumerate(self.groups):
+                    if body not in G.bodies:
+                        continue
+                    imp[g] += a
+                    hard[g] = max(hard[g], a)
+                    F[g] += fo
+                    Mo[g] += np.cross(pw, fo)
+                    Pw[g] += a * pw
+        out = np.zeros((ng, 12))
+        for g, G in enumerate(self.groups):
+            rb = G.reference_body
+            cr, rr, vr, wr = bs[rb, :3], bs[rb, 3:7], bs[rb, 7:10], bs[rb, 10:13]
+            ref = cr + rotate(rr, np.array(G.local_reference[:3], np.float64))
+            Fw, Mw = F[g] / self.physics_dt, Mo[g] / self.physics_dt
+            out[g, 6:9] = rotate_inverse(rr, Fw)
+            out[g, 9:12] = rotate_inverse(rr, Mw - np.cross(ref, Fw))
+            if G.flags & SUPPORT:
+                force = imp[g] / self.physics_dt
+                touching = force > self.p.support_force_threshold
+                koff = rotate(rr, np.array(G.kinematic_reference[:3], np.float64))
+                kv = vr + np.cross(wr, koff)
+                out[g, 0] = force
+                out[g, 1] = math.hypot(kv[0], kv[1]) if touching else 0.0
+                out[g, 2] = 0.0 if touching else st.air[g] + self.dt
+                out[g, 3] = ref[2] - G.local_reference[3] - self.ground
+                if imp[g] > 1e-6:
+                    cl = rotate_inverse(rr, Pw[g] - imp[g] * ref)
+                    out[g, 4:6] = cl[:2] / imp[g]
+            elif G.flags & FORBIDDEN:
+                out[g, 0] = 1.0 if hard[g] / self.physics_dt > self.p.support_force_threshold else 0.0
+        st.air[:ng] = out[:, 2]
+        return out
+
+    @staticmethod
+    def desired_support(G, phase: float) -> bool:
+        x = math.fmod(phase + G.gait_phase_offset, TWO_PI)
+        if x < 0.0:
+            x += TWO_PI
+        return x / TWO_PI < G.stance_fraction
 
     def new_state(self) -> EnvState:
         return EnvState(np.zeros((self.L, self.na)), np.zeros((2, self.na)), np.zeros(self.nobs))
@@ -156,7 +265,7 @@ class TaskOracle:
         down = np.array([0.0, 0.0, -1.0])
         return normalized_or(rotate_inverse(o, down), down)
 
-    def clean(self, op, q, v, st: EnvState, raw_slot: int, previous_q) -> float:
+    def clean(self, op, q, v, st: EnvState, raw_slot: int, previous_q, metrics=None) -> float:
         o, pos, lin, ang = self.root(q, v)
         c = op.component
         b = self.p.actions[op.source] if op.opcode in (OBS_JOINT_ERROR, OBS_JOINT_VELOCITY, OBS_JOINT_FD_VELOCITY) else None
@@ -180,20 +289,24 @@ class TaskOracle:
             value = rotate_inverse(o, lin)[c]
         elif op.opcode == OBS_ROOT_HEIGHT:
             value = pos[2]
+        elif op.opcode == OBS_CONTACT_METRIC:
+            value = metrics[op.source, c] if metrics is not None else 0.0
+        elif op.opcode == OBS_CONTACT_WRENCH:
+            value = metrics[op.source, 6 + c] if metrics is not None else 0.0
         elif op.opcode == OBS_GAIT_PHASE:
             value = (math.sin(st.phase) if c == 0 else math.cos(st.phase)) if np.linalg.norm(st.command) >= 0.1 else 0.0
         else:
             raise ValueError(f"opcode {op.opcode} is outside the subset")
         return op.scale * float(value) + op.offset
 
-    def frame(self, env, q, v, st: EnvState, raw_slot: int, previous_q, episode: int, step: int) -> np.ndarray:
+    def frame(self, env, q, v, st: EnvState, raw_slot: int, previous_q, episode: int, step: int, metrics=None) -> np.ndarray:
         """writeFrame (:1190-1330)."""
 
         g = np.array([0.0, 0.0, -1.0])
         have = False
         for op in self.p.actor:
             if op.opcode == OBS_GRAVITY and op.flags & NORMALIZE:
-                g[op.component] = self.clean(op, q, v, st, raw_slot, previous_q) + op.noise_amplitude * signed_draw(
+                g[op.component] = self.clean(op, q, v, st, raw_slot, previous_q, metrics) + op.noise_amplitude * signed_draw(
                     self.seed, env, episode, step, op.noise_channel)
                 have = True
         if have:
@@ -203,7 +316,7 @@ class TaskOracle:
             if op.opcode == OBS_GRAVITY and op.flags & NORMALIZE:
                 out[i] = g[op.component]
             else:
-                out[i] = self.clean(op, q, v, st, raw_slot, previous_q) + op.noise_amplitude * signed_draw(
+                out[i] = self.clean(op, q, v, st, raw_slot, previous_q, metrics) + op.noise_amplitude * signed_draw(
                     self.seed, env, episode, step, op.noise_channel)
         return out
 
@@ -254,6 +367,7 @@ class TaskOracle:
             else:
                 raise ValueError(f"randomization opcode {op.opcode} is outside the subset")
         st.history[:] = 0.0
+        st.air[:] = 0.0
         st.previous_joint[0] = 0.0
         st.previous_joint[1] = [rq[bd.q_index] for bd in self.p.actions]
         st.episode_step, st.episode = 0, episode
@@ -282,7 +396,7 @@ class TaskOracle:
             targets[a] = min(max(self.default_q[b.q_index] + b.scale * st.history[filt, a], b.lower_target), b.upper_target)
         return targets
 
-    def complete(self, env: int, st: EnvState, q, v, status: int) -> dict:
+    def complete(self, env: int, st: EnvState, q, v, status: int, manifolds=None) -> dict:
         """Reward, termination, schedule and the next actor frame of one
         finished physics step; returns the transition's fields."""
 
@@ -311,6 +425,8 @@ class TaskOracle:
             acc2 += acc * acc
             lim2 += lower * lower + upper * upper
         phase = math.fmod(st.phase + TWO_PI * dt / p.gait_period_seconds, TWO_PI)
+        moving = float(np.linalg.norm(st.command)) > 0.1
+        gm = self.contact_metrics(st, q, v, manifolds) if self.groups else None
         reward = 0.0
         b0, b1 = np.zeros(4), np.zeros(4)
         for r in p.rewards:
@@ -352,6 +468,37 @@ class TaskOracle:
                     center, half = 0.5 * (self.lo[a] + self.hi[a]), 0.5 * (self.hi[a] - self.lo[a]) * soft
                     x = q[b.q_index]
                     value += max(center - half - x, 0.0) + max(x - center - half, 0.0)
+            elif op in (R_GAIT_MATCH, R_SWING_CLEARANCE, R_SUPPORT_SLIP, R_FORBIDDEN, R_FOOT_CLEARANCE):
+                acc, count = 0.0, 0.0
+                for g, G in enumerate(self.groups):
+                    if r.group != ALL_GROUPS and r.group != g:
+                        continue
+                    m = gm[g]
+                    support = bool(G.flags & SUPPORT)
+                    if op == R_GAIT_MATCH and support:
+                        acc += 1.0 if self.desired_support(G, phase) == (m[0] > p.support_force_threshold) else 0.0
+                    elif op == R_SWING_CLEARANCE and support and not self.desired_support(G, phase):
+                        acc += math.exp(-((m[3] - p.clearance_target) ** 2) / max(r.parameters[0], 1e-8))
+                        count += 1.0
+                    elif op == R_SUPPORT_SLIP and support:
+                        acc += m[1]
+                    elif op == R_FORBIDDEN and G.flags & FORBIDDEN:
+                        acc = max(acc, m[0])
+                    elif op == R_FOOT_CLEARANCE and support:
+                        bs = self.world.body_states(np.asarray(q, np.float64), np.asarray(v, np.float64))
+                        rb = G.reference_body
+                        off = rotate(bs[rb, 3:7], np.array(G.kinematic_reference[:3], np.float64))
+                        vel = bs[rb, 7:10] + np.cross(bs[rb, 10:13], off)
+                        e = bs[rb, 2] + off[2] - p.clearance_target
+                        acc += e * e * math.tanh(r.parameters[1] * math.hypot(vel[0], vel[1]))
+                if op == R_FOOT_CLEARANCE:
+                    value = math.exp(-acc / max(r.parameters[0], 1e-8))
+                elif op == R_SWING_CLEARANCE:
+                    value = acc / max(count, 1.0) if moving else 0.0
+                elif op == R_GAIT_MATCH:
+                    value = acc if moving else 0.0
+                else:
+                    value = acc
             elif op in (R_POSTURE_SQUARED, R_POSTURE_ABSOLUTE):
                 members = p.joint_groups[r.group]
                 errs = [q[p.actions[m].q_index] - self.default_q[p.actions[m].q_index] for m in members]
@@ -360,8 +507,10 @@ class TaskOracle:
                 raise ValueError(f"reward opcode {op} is outside the subset")
             c = w * value
             reward += c
-            if op in (R_LINEAR, R_YAW, R_CONSTANT):
+            if op in (R_LINEAR, R_YAW, R_CONSTANT, R_GAIT_MATCH, R_SWING_CLEARANCE, R_FOOT_CLEARANCE):
                 b0[0] += c
+            elif op in (R_SUPPORT_SLIP, R_FORBIDDEN):
+                b1[3] += c
             elif op == R_JOINT_VELOCITY:
                 b0[2] += c
             elif op == R_JOINT_ACCELERATION:
@@ -376,7 +525,8 @@ class TaskOracle:
         timeout = steps >= p.maximum_episode_steps
         done, reason, priority, penalty = False, REASON_CONTINUING, 0, 0.0
         for t in self.terminations:
-            trig = height < t.threshold if t.opcode == T_MIN_HEIGHT else (tilt > t.threshold if t.opcode == T_MAX_TILT else False)
+            trig = (height < t.threshold if t.opcode == T_MIN_HEIGHT else tilt > t.threshold if t.opcode == T_MAX_TILT
+                    else gm[t.group, 0] > t.threshold if t.opcode == T_CONTACT_GROUP else False)
             if trig and (not done or t.priority >= priority):
                 done, reason, priority, penalty = True, t.reason, t.priority, t.failure_penalty
         if timeout:
@@ -407,7 +557,7 @@ class TaskOracle:
         st.episode_return = 0.0 if done else episode_return
         st.episode_tracking = 0.0 if done else episode_tracking
         if not done or (timeout and not physics_error):
-            st.frame = self.frame(env, q, v, st, raw_last, st.previous_joint[1], st.episode, steps)
+            st.frame = self.frame(env, q, v, st, raw_last, st.previous_joint[1], st.episode, steps, gm)
             for a, b in enumerate(p.actions):
                 st.previous_joint[0, a] = v[b.v_index]
                 st.previous_joint[1, a] = q[b.q_index]
@@ -417,4 +567,5 @@ class TaskOracle:
             "task_reward": b0[0], "base_reward": b0[1], "joint_velocity_reward": b0[2], "joint_acceleration_reward": b0[3],
             "control_reward": b1[0], "posture_reward": b1[1], "energy_reward": b1[2], "contact_reward": b1[3],
             "episode_tracking_score": episode_score if done and not physics_error else 0.0,
+            "contact_metrics": gm,
         }

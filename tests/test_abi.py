@@ -74,6 +74,7 @@ def test_struct_sizes_match_header_layout(tmp_path):
         "MRTaskRandomizationOperatorC": native.TaskRandomizationOperatorC,
         "MRTaskIndexGroupC": native.TaskIndexGroupC,
         "MRTaskProgramC": native.TaskProgramC,
+        "MRTaskContactGroupC": native.TaskContactGroupC,
         "MRTaskTransitionC": native.TaskTransitionC,
         "MRPolicyRolloutBatchC": native.PolicyRolloutBatchC,
         "MRPolicyRolloutPackC": native.PolicyRolloutPackC,

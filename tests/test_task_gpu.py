@@ -53,18 +53,30 @@ def _close(a, b, tol) -> float:
     return float(np.max(np.abs(a - b) / np.maximum(1.0, np.abs(b)))) if a.size else 0.0
 
 
-def test_task_layer_matches_oracle_step_by_step(cuda_device):
+@pytest.mark.parametrize("contacts", [False, True])
+def test_task_layer_matches_oracle_step_by_step(cuda_device, contacts):
+    """With `contacts` the program also has the feet's support groups and a
+    forbidden torso group: their metrics in the frames, the contact rewards
+    and the contact termination, computed from the committed manifolds."""
+
     import torch
+
+    from oracle import Oracle
 
     envs, steps = 16, 40
     with nb.World("tree29", envs, substeps=4, velocity_iterations=8, control_dt=DT, seed=SEED) as w:
         # Tight height and tilt limits: episodes end by timeout, height and
         # tilt within the run.
+        groups = T.foot_contact_groups(w.model()) if contacts else None
         prog = _program(w, maximum_episode_steps=12, noise=0.05, response_time_seconds=0.04, action_history=4,
-                        action_delay_steps=1, min_height_fraction=0.995, max_tilt=0.04)
+                        action_delay_steps=1, min_height_fraction=0.995, max_tilt=0.04, contact_groups=groups)
         w.set_task(prog)
         assert w.observation_count == len(prog.actor)
         o = _oracle(w, prog)
+        if contacts:
+            o = TaskOracle(prog, nq=w.nq, nv=w.nv, dt=DT, seed=w.seed, fixed_root=False, limit_lower=o.lo, limit_upper=o.hi,
+                           records=w.model(), world=Oracle(w.model(), DT / 4, 4, 8, 0), physics_dt=DT / 4)
+        touched = 0
         states = [o.new_state() for _ in range(envs)]
         gen = torch.Generator(device="cuda").manual_seed(3)
         seen = {"reset": 0, "timeout": 0, "height": 0, "tilt": 0}
@@ -74,7 +86,7 @@ def test_task_layer_matches_oracle_step_by_step(cuda_device):
             obs, status, _ = w.step(acts, wait=True)
             obs = obs.cpu().numpy()[0]
             status = status.cpu().numpy()[0]
-            q, v, _ = w.state()
+            q, v, mans = w.state()
             tr = w.transitions(1)
             a_np = acts.cpu().numpy()[0]
             for e in range(envs):
@@ -83,11 +95,14 @@ def test_task_layer_matches_oracle_step_by_step(cuda_device):
                 worst_obs = max(worst_obs, _close(obs[e], want, OBS_TOL))
                 assert _close(obs[e], want, OBS_TOL) <= OBS_TOL, (k, e, int(np.argmax(np.abs(obs[e] - want))))
                 o.apply(states[e], a_np[e])
-                t = o.complete(e, states[e], q[e].astype(np.float64), v[e].astype(np.float64), int(status[e]))
+                env_mans = mans[e * w.pair_count:(e + 1) * w.pair_count] if contacts else None
+                t = o.complete(e, states[e], q[e].astype(np.float64), v[e].astype(np.float64), int(status[e]), env_mans)
+                if contacts:
+                    touched += int(np.sum(t["contact_metrics"][:2, 0] > prog.support_force_threshold))
                 for f in ("done", "timeout", "physics_error", "termination_reason"):
                     assert int(tr[f][0, e]) == t[f], (k, e, f)
                 for f in ("reward", "tracking_score", "root_height", "tilt", "task_reward", "base_reward", "joint_velocity_reward",
-                          "joint_acceleration_reward", "control_reward", "posture_reward", "episode_tracking_score"):
+                          "joint_acceleration_reward", "control_reward", "posture_reward", "contact_reward", "episode_tracking_score"):
                     err = _close(tr[f][0, e], t[f], REWARD_TOL)
                     worst_reward = max(worst_reward, err)
                     assert err <= REWARD_TOL, (k, e, f, float(tr[f][0, e]), t[f])
@@ -97,6 +112,8 @@ def test_task_layer_matches_oracle_step_by_step(cuda_device):
         print(f"worst observation error {worst_obs:.2e}, worst transition error {worst_reward:.2e}; {seen}")
         # The run crossed episode boundaries of each kind it can.
         assert seen["reset"] > envs and seen["timeout"] > 0 and seen["height"] + seen["tilt"] > 0
+        if contacts:
+            assert touched > 0  # the feet carried load on some steps
 
 
 def test_drive_targets_match_the_oracle(cuda_device):
@@ -200,6 +217,9 @@ def test_installer_refuses_programs_outside_the_subset(cuda_device):
             dict(terminations=[T.Termination(2, 3, 1, 0.5)]),
             dict(randomization=[T.Randomization(4)]),
             dict(action_history=2),
+            dict(rewards=base.rewards + [T.Reward(T.REWARD["support_slip"], -1.0, group=0)]),  # no contact groups
+            dict(contact_groups=[T.ContactGroup([99], T.CONTACT_SUPPORT, 0)]),
+            dict(terminations=[T.Termination(T.TERMINATE["contact_group"], 3, 1, 0.5, group=0)]),
             dict(default_q=base.default_q[:-1]),
         ]
         for change in bad:

@@ -197,3 +197,65 @@ def test_command_schedule_and_reset_draws(tree):
         st_again = o.new_state()
         _, rq2, _, obs2 = o.observe(env, st_again, q, v, False)
         assert np.array_equal(rq, rq2) and np.array_equal(obs, obs2)
+
+
+def test_contact_group_metrics_of_a_hand_made_foot_contact(tree):
+    """A foot pressed flat on the ground by four equal normal impulses at its
+    sole corners: force = 4 lambda / h, the centre of pressure at the corners'
+    centre in the foot frame, the wrench's force straight up in that frame,
+    no slip for a still foot, clearance from the sole point."""
+
+    from oracle import Oracle
+    from numi_lab_b200 import native
+
+    rec, prog0, lo, hi = tree
+    groups = T.foot_contact_groups(rec)
+    prog = T.locomotion_task(rec, prog0.default_q, contact_groups=groups, support_force_threshold=1.0)
+    h = DT / 4
+    world = Oracle(rec, h, 4, 8, 0)
+    o = TaskOracle(prog, nq=int(rec.world.nq), nv=int(rec.world.nv), dt=DT, seed=1, fixed_root=False, limit_lower=lo,
+                   limit_upper=hi, records=rec, world=world, physics_dt=h)
+    st = o.new_state()
+    q = prog.default_q.astype(float).copy()
+    v = np.zeros(int(rec.world.nv))
+    bs = world.body_states(q, v)
+    foot = groups[0].reference_body
+    pair = next(i for i in range(int(rec.world.pair_count)) if int(rec.shapes[int(rec.pairs[i].shape_a)].body) == foot)
+    mans = (native.ManifoldC * int(rec.world.pair_count))()
+    m = mans[pair]
+    rot = bs[foot, 3:7]
+    m.normal_local[:] = list(rotate_inverse_np(rot, np.array([0.0, 0.0, -1.0])))
+    m.tangent_local[:] = list(rotate_inverse_np(rot, np.array([1.0, 0.0, 0.0])))
+    m.count = 4
+    sole = np.array(groups[0].local_reference[:3])
+    corners = [sole + np.array([sx * 0.05, sy * 0.02, 0.0]) + np.array([0.01, 0.0, 0.0]) for sx in (-1, 1) for sy in (-1, 1)]
+    lam = 0.3
+    for i, c in enumerate(corners):
+        m.points[i].anchor_a[:] = list(c)
+        m.points[i].anchor_b[:] = list(bs[foot, :3] + rotate_np(rot, c))
+        m.points[i].impulses[:] = [lam, 0.0, 0.0]
+    gm = o.contact_metrics(st, q, v, mans)
+    assert gm[0, 0] == pytest.approx(4 * lam / h)
+    assert gm[0, 1] == 0.0 and gm[0, 2] == 0.0  # still foot, in contact
+    # (anchors are stored as FP32)
+    assert gm[0, 4] == pytest.approx(0.01, abs=1e-7) and gm[0, 5] == pytest.approx(0.0, abs=1e-7)
+    np.testing.assert_allclose(gm[0, 6:9], rotate_inverse_np(rot, np.array([0.0, 0.0, 4 * lam / h])), rtol=1e-6, atol=1e-5)
+    sole_world = bs[foot, :3] + rotate_np(rot, sole)
+    assert gm[0, 3] == pytest.approx(sole_world[2] - o.ground)
+    # The other foot is in the air: its air time grows by the control step.
+    assert gm[1, 0] == 0.0 and gm[1, 2] == pytest.approx(DT)
+    gm2 = o.contact_metrics(st, q, v, (native.ManifoldC * int(rec.world.pair_count))())
+    assert gm2[0, 2] == pytest.approx(DT) and gm2[1, 2] == pytest.approx(2 * DT)
+    assert gm[2, 0] == 0.0  # the forbidden group (torso) does not touch
+
+
+def rotate_np(qv, v):
+    from oracle.task import rotate
+
+    return rotate(np.asarray(qv, float), np.asarray(v, float))
+
+
+def rotate_inverse_np(qv, v):
+    from oracle.task import rotate_inverse
+
+    return rotate_inverse(np.asarray(qv, float), np.asarray(v, float))
