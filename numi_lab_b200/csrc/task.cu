@@ -290,10 +290,9 @@ __device__ BodyFrame body_frames(const DeviceModel& M, const float* q, const flo
 // contacts): out[g][0..5] force (forbidden groups: the hard-contact flag),
 // slip, air time, clearance, CoP x, y; out[g][6..11] wrench in the
 // reference body's frame.  `air` holds and receives each group's air time.
-__device__ void contact_metrics(const TaskProgramDevice& P, const float* q, const float* v, const float* manifolds, float* air,
-                                float* out, int lane) {
+__device__ void contact_metrics(const TaskProgramDevice& P, const BodyFrame& f, const float* manifolds, float* air, float* out,
+                                int lane) {
     const DeviceModel& M = *P.model;
-    const BodyFrame f = body_frames(M, q, v, lane);
     float imp[kTaskMaxGroups], hard[kTaskMaxGroups], F[kTaskMaxGroups][3], Mo[kTaskMaxGroups][3], Pw[kTaskMaxGroups][3];
 #pragma unroll
     for (int g = 0; g < kTaskMaxGroups; ++g) {
@@ -575,9 +574,12 @@ __global__ void __launch_bounds__(32 * kTaskWarps) task_complete_kernel(TaskPara
     const float phase = fmodf(st.phase + kTwoPi * P.dt / P.gait_period, kTwoPi);
     const bool moving = sqrtf(st.command[0] * st.command[0] + st.command[1] * st.command[1] + st.command[2] * st.command[2]) > 0.1f;
     float gm[kTaskMaxGroups * kTaskGroupMetrics];
-    if (P.ncontact_groups > 0)
-        contact_metrics(P, q, v, p.manifolds + static_cast<size_t>(local) * P.model->np * kManifoldWords,
+    BodyFrame frames;  // body `lane`'s world frame (contact groups only)
+    if (P.ncontact_groups > 0) {
+        frames = body_frames(*P.model, q, v, lane);
+        contact_metrics(P, frames, p.manifolds + static_cast<size_t>(local) * P.model->np * kManifoldWords,
                         p.air_time + static_cast<size_t>(local) * kTaskMaxGroups, gm, lane);
+    }
 
     float reward = 0.0f;
     float b0[4] = {0.0f, 0.0f, 0.0f, 0.0f}, b1[4] = {0.0f, 0.0f, 0.0f, 0.0f};
@@ -685,9 +687,8 @@ __global__ void __launch_bounds__(32 * kTaskWarps) task_complete_kernel(TaskPara
                 } else if (op.opcode == MR_TASK_REWARD_FOOT_CLEARANCE && support) {
                     // Height of the kinematic reference point, weighted by its planar speed.
                     const int rb = static_cast<int>(G.reference_body);
-                    const BodyFrame fr = body_frames(*P.model, q, v, lane);
-                    const float3 c = shfl3(fr.c, rb), vb = shfl3(fr.v, rb), wb = shfl3(fr.w, rb);
-                    const float4 r = shfl4(fr.r, rb);
+                    const float3 c = shfl3(frames.c, rb), vb = shfl3(frames.v, rb), wb = shfl3(frames.w, rb);
+                    const float4 r = shfl4(frames.r, rb);
                     const float3 off = rotate(r, make_float3(G.kinematic_reference[0], G.kinematic_reference[1], G.kinematic_reference[2]));
                     const float3 vel = vb + cross3(wb, off);
                     const float e = c.z + off.z - P.clearance_target;
