@@ -9,6 +9,14 @@
 namespace numi {
 namespace {
 
+// The FP32 control step of a world with support-mapped pairs, compiled once
+// out of line: the per-world kernel and the batch's free-body family both
+// call this body, so the two produce the same bits (inlined into two
+// kernels, the compiler's floating-point contractions may differ).
+__device__ __noinline__ void scene_step_convex(const SceneParams& p, float* smem, int item, int env) {
+    scene_step_item<false, true>(p, smem, item, env);
+}
+
 // At most 128 registers: 16 resident warps per SM.  More warps (96
 // registers) ran slower: their narrowphase scratch no longer fits the L1.
 template <bool kComp, bool kConvex>
@@ -17,7 +25,10 @@ __global__ void __launch_bounds__(32, 16) scene_step_kernel(SceneParams p) {
     const int item = blockIdx.x;
     if (item >= p.env_count) return;
     const int env = p.env_index != nullptr ? p.env_index[item] : item;
-    scene_step_item<kComp, kConvex>(p, reinterpret_cast<float*>(smem4), item, env);
+    if constexpr (!kComp && kConvex)
+        scene_step_convex(p, reinterpret_cast<float*>(smem4), item, env);
+    else
+        scene_step_item<kComp, kConvex>(p, reinterpret_cast<float*>(smem4), item, env);
 }
 
 // The batch's free-body family (mix_step.cu): the per-family claim loop over
@@ -45,7 +56,7 @@ __global__ void __launch_bounds__(32, 16) mix_scene_kernel(const MixWorld* __res
             const SceneParams& sp = worlds[static_cast<size_t>(k) * world_count + world].scene;
             if constexpr (kConvex) {
                 if (sp.support_mapped)
-                    scene_step_item<false, true>(sp, base, env, env);
+                    scene_step_convex(sp, base, env, env);
                 else
                     scene_step_item<false, false>(sp, base, env, env);
             } else {

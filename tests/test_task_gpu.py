@@ -235,3 +235,28 @@ def test_installer_refuses_programs_outside_the_subset(cuda_device):
         obs, status, _ = w.step(torch.zeros((1, 4, w.action_count), device="cuda"), wait=True)
         q, v, _ = w.state()
         np.testing.assert_array_equal(obs.cpu().numpy()[0], np.concatenate([q, v], axis=1))
+
+
+def test_reseed_starts_new_episodes_under_the_new_draws(cuda_device):
+    """mr_task_rollout_reset with a new seed: every environment starts a new
+    episode at the next step, its reset draws and commands keyed on the new
+    seed (the first frame equals a fresh oracle's under that seed)."""
+
+    import torch
+
+    envs = 8
+    with nb.World("tree29", envs, substeps=4, velocity_iterations=8, control_dt=DT, seed=SEED) as w:
+        prog = _program(w, noise=0.03)
+        w.set_task(prog)
+        zeros = torch.zeros((1, envs, w.action_count), device="cuda")
+        for _ in range(3):
+            w.step(zeros, wait=True)
+        w.reset(seed=11)
+        obs, _, _ = w.step(zeros, wait=True)
+        o = _oracle(w, prog)
+        assert o.seed == 11
+        for e in range(envs):
+            st = o.new_state()
+            reset, _, _, want = o.observe(e, st, None, None, False)
+            assert reset
+            assert _close(obs.cpu().numpy()[0, e], want, OBS_TOL) <= OBS_TOL, e
