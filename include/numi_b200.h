@@ -728,6 +728,7 @@ enum {
     MR_TASK_OBSERVE_CONTACT_METRIC = 8u,
     MR_TASK_OBSERVE_CONTACT_WRENCH_LOCAL = 13u,
     MR_TASK_OBSERVE_GAIT_PHASE = 14u,
+    MR_TASK_OBSERVE_SUPPORT_SENSE = 18u,
     MR_TASK_OBSERVE_DELAYED_ACTION = 26u,
     MR_TASK_OBSERVE_JOINT_FINITE_DIFFERENCE_VELOCITY = 27u
 };

@@ -1337,6 +1337,9 @@ std::unique_ptr<InstalledTask> compile_task(const MRTaskRolloutHandle& h, const 
         case MR_TASK_OBSERVE_GAIT_PHASE:
             need(o.component < 2u, where + ": component must be 0-1");
             break;
+        case MR_TASK_OBSERVE_SUPPORT_SENSE:
+            need(o.component < 3u, where + ": component must be 0-2");
+            break;
         case MR_TASK_OBSERVE_ROOT_HEIGHT:
             break;
         case MR_TASK_OBSERVE_CONTACT_METRIC:

@@ -160,6 +160,19 @@ __device__ float clean_observation(const TaskProgramDevice& P, const MRTaskObser
     case MR_TASK_OBSERVE_CONTACT_WRENCH_LOCAL:
         value = metrics ? metrics[op.source * kTaskGroupMetrics + 6 + c] : 0.0f;
         break;
+    case MR_TASK_OBSERVE_SUPPORT_SENSE: {  // total support load, phase-signed balance, largest slip (:1082-1116)
+        float total = 0.0f, signed_load = 0.0f, slip = 0.0f;
+        for (int g = 0; metrics && g < P.ncontact_groups; ++g) {
+            const MRTaskContactGroupC G = P.contact_groups[g];
+            if ((G.flags & MR_TASK_CONTACT_SUPPORT) == 0u) continue;
+            const float load = fmaxf(metrics[g * kTaskGroupMetrics], 0.0f);
+            total += load;
+            signed_load += load * cosf(G.gait_phase_offset);
+            slip = fmaxf(slip, fmaxf(metrics[g * kTaskGroupMetrics + 1], 0.0f));
+        }
+        value = c == 0u ? total : (c == 1u ? (total > 1.0e-6f ? signed_load / total : 0.0f) : slip);
+        break;
+    }
     case MR_TASK_OBSERVE_GAIT_PHASE: {
         const float magnitude = sqrtf(st.command[0] * st.command[0] + st.command[1] * st.command[1] + st.command[2] * st.command[2]);
         if (magnitude >= 0.1f) value = c == 0u ? sinf(st.phase) : cosf(st.phase);

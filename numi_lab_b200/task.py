@@ -28,7 +28,7 @@ from . import native
 OBSERVE = {
     "root_angular_velocity_local": 0, "projected_gravity": 1, "command": 2, "joint_position_error": 3, "joint_velocity": 4,
     "previous_action": 5, "root_linear_velocity_local": 6, "root_height": 7, "contact_metric": 8, "contact_wrench_local": 13,
-    "gait_phase": 14, "delayed_action": 26, "joint_finite_difference_velocity": 27,
+    "gait_phase": 14, "support_sense": 18, "delayed_action": 26, "joint_finite_difference_velocity": 27,
 }
 NORMALIZE_VECTOR3 = 1
 REWARD = {
@@ -319,6 +319,8 @@ def locomotion_task(records, default_q: np.ndarray, *, base_height: float | None
         if cg.flags & CONTACT_SUPPORT:
             actor.append(obs("contact_metric", g, 0, scale=0.002))
             actor.append(obs("contact_metric", g, 2, noise=0.0))
+    if cgroups:
+        actor += [obs("support_sense", 0, c, scale=0.002 if c == 0 else 1.0, noise=0.0) for c in range(3)]
     if cgroups:
         rewards += [
             Reward(REWARD["gait_contact_match"], 0.5, group=ALL_GROUPS),

@@ -46,7 +46,7 @@ R_JOINT_VELOCITY, R_JOINT_ACCELERATION, R_ACTION_RATE, R_LIMIT_SQUARED = 7, 8, 9
 R_POSTURE_SQUARED, R_POSTURE_ABSOLUTE, R_GRAVITY_HORIZONTAL, R_LIMIT_ABSOLUTE = 12, 17, 18, 20
 R_HEIGHT_NORMALIZED, R_HEIGHT_PROGRESS, R_UPRIGHTNESS = 21, 22, 23
 R_GAIT_MATCH, R_SWING_CLEARANCE, R_SUPPORT_SLIP, R_FORBIDDEN, R_FOOT_CLEARANCE = 13, 14, 15, 16, 19
-OBS_CONTACT_METRIC, OBS_CONTACT_WRENCH = 8, 13
+OBS_CONTACT_METRIC, OBS_CONTACT_WRENCH, OBS_SUPPORT_SENSE = 8, 13, 18
 T_MIN_HEIGHT, T_MAX_TILT, T_CONTACT_GROUP = 0, 1, 2
 SUPPORT, FORBIDDEN = 1, 2
 ALL_GROUPS = 0xFFFFFFFF
@@ -293,6 +293,16 @@ class TaskOracle:
             value = metrics[op.source, c] if metrics is not None else 0.0
         elif op.opcode == OBS_CONTACT_WRENCH:
             value = metrics[op.source, 6 + c] if metrics is not None else 0.0
+        elif op.opcode == OBS_SUPPORT_SENSE:
+            total = signed = slip = 0.0
+            for g, G in enumerate(self.groups):
+                if metrics is None or not G.flags & SUPPORT:
+                    continue
+                load = max(metrics[g, 0], 0.0)
+                total += load
+                signed += load * math.cos(G.gait_phase_offset)
+                slip = max(slip, max(metrics[g, 1], 0.0))
+            value = total if c == 0 else ((signed / total if total > 1e-6 else 0.0) if c == 1 else slip)
         elif op.opcode == OBS_GAIT_PHASE:
             value = (math.sin(st.phase) if c == 0 else math.cos(st.phase)) if np.linalg.norm(st.command) >= 0.1 else 0.0
         else:
