@@ -27,7 +27,10 @@ Lines printed (rank 0, one JSON line):
     server (p50 / p99 latency);
   * quality_newton: the same world with the converged FP64 contact solve,
     the solver class of the reference's CPU world step (cpu_baseline), and
-    its ratio to cpu_baseline.
+    its ratio to cpu_baseline;
+  * task_closed_loop: the same world driven by a native policy through the
+    locomotion task layer (observe, policy, apply, physics, complete per
+    control step).
 
 ``--impl reference`` times only that CPU reference (rank 0; other ranks exit).
 Multi-GPU (torchrun): one process per GPU; the job is world_size x 4096
@@ -562,6 +565,10 @@ def run_pile(args, source: str = "pile") -> None:
 
 
 def run_policy(args, task: bool = False) -> None:
+    print(json.dumps(measure_closed_loop(args, task)))
+
+
+def measure_closed_loop(args, task: bool = False) -> dict:
     """Closed loop: 4096 tree29 environments driven by a native policy on
     the device (mr_task_rollout_set_policy) -- a seeded random actor
     obs-256-128-29 (elu, silu, tanh) with observation normalisation and
@@ -646,7 +653,7 @@ def run_policy(args, task: bool = False) -> None:
     }
     if task:
         line["last_step_transitions"] = episodes
-    print(json.dumps(line))
+    return line
 
 
 def run_task(args) -> None:
@@ -1182,13 +1189,16 @@ def run_headline(args, rank: int, local_rank: int, world_size: int) -> None:
     plain = plain_aba_chain7(device) if rank == 0 else None
     # The heterogeneous mix (batched vs plain per-config kernels) and the
     # serving stream, on rank 0 (bounded: a few horizons, one arrival rate).
-    mix = serving = quality = None
+    mix = serving = quality = task_loop = None
     if rank == 0 and not args.headline_only:
         mix_args = argparse.Namespace(steps=min(args.steps, 5), warmup=3, envs=0)
         mix = measure_mix(mix_args, device)
         mix["steps"] = mix_args.steps
         serving = measure_serving(SERVE_RATES[:1] + SERVE_RATES[2:3])
         quality = measure_quality(device)
+        loop = measure_closed_loop(argparse.Namespace(steps=min(args.steps, 5), warmup=3, envs=0), task=True)
+        task_loop = {k: loop[k] for k in ("value", "unit", "ms_per_step", "steps", "gpu_launches", "clocks", "last_step_transitions")}
+        task_loop["config"] = loop["config"]["workload"]
 
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
@@ -1248,6 +1258,7 @@ def run_headline(args, rank: int, local_rank: int, world_size: int) -> None:
             "heterogeneous_mix": mix,
             "serving": serving,
             "quality_newton": quality,
+            "task_closed_loop": task_loop,
         }
         if quality and cpu and cpu.get("value"):
             # The reference CPU arm runs the same (converged) solver class.
