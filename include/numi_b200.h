@@ -704,6 +704,39 @@ MR_API int mr_write_policy_rollout_pack(const MRPolicyRolloutPackC* pack, const 
 MR_API int mr_policy_rollout_pack_inspect(const char* path, MRPolicyRolloutPackInfoC* info, float* parameters, size_t capacity);
 
 /* ---------------------------------------------------------------------- */
+/* TaskPack files (reference: include/metalrobo/TaskProgram.hpp:442-500,   */
+/* src/core/LearningPacks.cpp:81-258, 1127-1412, 2300-2345)                */
+/* ---------------------------------------------------------------------- */
+
+/* No counterpart in the reference's C ABI: the authored task's tables and
+ * the episode constants of a TaskPack file. */
+typedef struct MRTaskPackInfoC {
+    uint64_t content_hash;
+    uint32_t action_count;
+    uint32_t outcome_count;
+    uint32_t contact_group_count;
+    uint32_t joint_group_count;
+    uint32_t reward_count;
+    uint32_t termination_count;
+    uint32_t maximum_episode_steps;
+    uint32_t difficulty_band_count;
+    uint32_t terrain_sample_count;
+    uint32_t motion_tracked_body_count;
+    float base_height_target;
+    float gait_period_seconds;
+    float clearance_target;
+    float support_force_threshold;
+    char id[64];                    /* truncated, NUL-terminated */
+} MRTaskPackInfoC;
+
+/* No counterpart in the reference: reads a TaskPack (kind 1, version 17). */
+MR_API int mr_task_pack_inspect(const char* path, MRTaskPackInfoC* info);
+/* No counterpart in the reference: reads a TaskPack, checks the artifact
+ * rules of the reference's writer and writes it to output_path (atomic:
+ * temporary, fsync, rename); the bytes equal the reference writer's. */
+MR_API int mr_task_pack_rewrite(const char* input_path, const char* output_path);
+
+/* ---------------------------------------------------------------------- */
 /* Task layer (reference: include/metalrobo/task_program_types.h,         */
 /* src/metal/LocomotionTask.metal observe / apply_actions / complete)      */
 /* ---------------------------------------------------------------------- */

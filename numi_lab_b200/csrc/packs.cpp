@@ -1,7 +1,8 @@
-// PolicyPack and PolicyRolloutPack reading and writing (packs.h) and the
-// C-ABI entry points that need no rollout: mr_write_policy_pack,
+// PolicyPack, PolicyRolloutPack and TaskPack reading and writing (packs.h)
+// and the C-ABI entry points that need no rollout: mr_write_policy_pack,
 // mr_learning_pack_content_hash, mr_policy_pack_inspect,
-// mr_write_policy_rollout_pack and mr_policy_rollout_pack_inspect.
+// mr_write_policy_rollout_pack, mr_policy_rollout_pack_inspect,
+// mr_task_pack_inspect and mr_task_pack_rewrite.
 // mr_task_rollout_load_policy_pack (rollout.cu) reads through
 // read_policy_pack and installs like mr_task_rollout_set_policy;
 // mr_task_rollout_write_policy_rollout_pack (rollout.cu) writes through
@@ -396,7 +397,211 @@ bool decode_rollout(const std::uint8_t* bytes, std::size_t count, PolicyRolloutP
     return (transitions == 0 || s.raw(d.transitions.data(), d.transitions.size() * sizeof(LearningTransition))) && s.done();
 }
 
+// TaskPack payload (LearningPacks.cpp:1127-1262).
+void put_strings(Sink& s, const std::vector<std::string>& v) {
+    s.u64(v.size());
+    for (const std::string& x : v) s.text(x);
+}
+void put_f4(Sink& s, const float* f) { s.raw(f, 16); }
+void put_f4_list(Sink& s, const std::vector<float>& v) {  // counted four-float records
+    s.u64(v.size() / 4);
+    if (!v.empty()) s.raw(v.data(), v.size() * sizeof(float));
+}
+
+std::vector<std::uint8_t> encode_task(const TaskPackData& d) {
+    Sink s;
+    s.text(d.id);
+    s.raw(d.capacities, sizeof(d.capacities));
+    put_strings(s, d.actions);
+    s.u64(d.outcomes.size());
+    for (const TaskPackOutcome& o : d.outcomes) {
+        s.text(o.id);
+        s.text(o.unit);
+        s.u32(o.source);
+        s.u32(o.direction);
+        s.u32(o.reward_operation);
+    }
+    s.u64(d.contact_groups.size());
+    for (const TaskPackContactGroup& g : d.contact_groups) {
+        s.text(g.id);
+        put_strings(s, g.bodies);
+        s.raw(&g.support, 1);
+        s.raw(&g.forbidden, 1);
+        s.text(g.reference_body);
+        put_f4(s, g.local_reference);
+        s.f32(g.gait_phase_offset);
+        s.f32(g.stance_fraction);
+        put_f4(s, g.support_patch_bounds);
+        s.u32(g.support_patch_width);
+        s.u32(g.support_patch_height);
+    }
+    s.u64(d.joint_groups.size());
+    for (const TaskPackJointGroup& g : d.joint_groups) {
+        s.text(g.id);
+        put_strings(s, g.joints);
+    }
+    s.u64(d.rewards.size());
+    for (const TaskPackReward& r : d.rewards) {
+        s.u32(r.operation);
+        s.text(r.source_group);
+        s.text(r.target);
+        s.f32(r.weight);
+        put_f4(s, r.parameters);
+    }
+    s.u64(d.terminations.size());
+    for (const TaskPackTermination& t : d.terminations) {
+        s.u32(t.operation);
+        s.text(t.source_group);
+        s.u32(t.reason);
+        s.u32(t.priority);
+        s.f32(t.threshold);
+        s.f32(t.failure_penalty);
+        s.u32(t.minimum_band);
+        s.u32(t.maximum_band);
+    }
+    for (const float* c : d.commands) put_f4(s, c);
+    s.f32(d.standing_probability);
+    s.f32(d.difficulty_sampling_exponent);
+    s.f32(d.command_duration[0]);
+    s.f32(d.command_duration[1]);
+    for (float x : d.pushes) s.f32(x);
+    s.text(d.terrain_body);
+    put_f4_list(s, d.terrain_sample_offsets);
+    put_f4_list(s, d.terrain_reset_translations);
+    s.text(d.threat_protected_group);
+    for (float x : d.threat) s.f32(x);
+    s.text(d.motion_anchor);
+    put_strings(s, d.motion_tracked);
+    s.u32(d.maximum_episode_steps);
+    s.u32(d.difficulty_band_count);
+    s.f32(d.interaction_student_authority);
+    s.f32(d.interaction_reset_phase_fraction);
+    s.floats(d.initial_action_positions);
+    s.raw(&d.interaction_control_reference, 1);
+    s.raw(&d.interaction_initialize_from_reference, 1);
+    s.raw(&d.interaction_align_reference_yaw, 1);
+    s.f32(d.base_height_target);
+    s.f32(d.gait_period);
+    s.f32(d.clearance_target);
+    s.f32(d.success_tracking_threshold);
+    s.f32(d.support_force_threshold);
+    return s.bytes;
+}
+
+bool get_strings(Source& s, std::vector<std::string>& v) {
+    std::uint64_t k = 0;
+    if (!s.u64(k) || k > (s.n - s.at) / 8) return false;  // each string takes at least its 8-byte count
+    v.resize(static_cast<std::size_t>(k));
+    for (std::string& x : v)
+        if (!s.text(x)) return false;
+    return true;
+}
+bool get_f4(Source& s, float* f) { return s.raw(f, 16); }
+bool get_f4_list(Source& s, std::vector<float>& v) {
+    std::uint64_t k = 0;
+    if (!s.u64(k) || k > (s.n - s.at) / 16) return false;
+    v.resize(static_cast<std::size_t>(k) * 4);
+    return k == 0 || s.raw(v.data(), v.size() * sizeof(float));
+}
+template <typename T, typename F>
+bool get_records(Source& s, std::vector<T>& v, std::size_t least, F&& f) {
+    std::uint64_t k = 0;
+    if (!s.u64(k) || k > (s.n - s.at) / least) return false;
+    v.resize(static_cast<std::size_t>(k));
+    for (T& x : v)
+        if (!f(x)) return false;
+    return true;
+}
+
+bool decode_task(const std::uint8_t* bytes, std::size_t count, TaskPackData& d) {
+    Source s{bytes, count};
+    if (!s.text(d.id) || !s.raw(d.capacities, sizeof(d.capacities)) || !get_strings(s, d.actions)) return false;
+    if (!get_records(s, d.outcomes, 28, [&](TaskPackOutcome& o) {
+            return s.text(o.id) && s.text(o.unit) && s.u32(o.source) && s.u32(o.direction) && s.u32(o.reward_operation);
+        }))
+        return false;
+    if (!get_records(s, d.contact_groups, 74, [&](TaskPackContactGroup& g) {
+            return s.text(g.id) && get_strings(s, g.bodies) && s.raw(&g.support, 1) && s.raw(&g.forbidden, 1) &&
+                   s.text(g.reference_body) && get_f4(s, g.local_reference) && s.f32(g.gait_phase_offset) &&
+                   s.f32(g.stance_fraction) && get_f4(s, g.support_patch_bounds) && s.u32(g.support_patch_width) &&
+                   s.u32(g.support_patch_height);
+        }))
+        return false;
+    if (!get_records(s, d.joint_groups, 16, [&](TaskPackJointGroup& g) { return s.text(g.id) && get_strings(s, g.joints); }))
+        return false;
+    if (!get_records(s, d.rewards, 40, [&](TaskPackReward& r) {
+            return s.u32(r.operation) && s.text(r.source_group) && s.text(r.target) && s.f32(r.weight) && get_f4(s, r.parameters);
+        }))
+        return false;
+    if (!get_records(s, d.terminations, 36, [&](TaskPackTermination& t) {
+            return s.u32(t.operation) && s.text(t.source_group) && s.u32(t.reason) && s.u32(t.priority) && s.f32(t.threshold) &&
+                   s.f32(t.failure_penalty) && s.u32(t.minimum_band) && s.u32(t.maximum_band);
+        }))
+        return false;
+    for (float* c : d.commands)
+        if (!get_f4(s, c)) return false;
+    if (!s.f32(d.standing_probability) || !s.f32(d.difficulty_sampling_exponent) || !s.f32(d.command_duration[0]) ||
+        !s.f32(d.command_duration[1]))
+        return false;
+    for (float& x : d.pushes)
+        if (!s.f32(x)) return false;
+    if (!s.text(d.terrain_body) || !get_f4_list(s, d.terrain_sample_offsets) || !get_f4_list(s, d.terrain_reset_translations) ||
+        !s.text(d.threat_protected_group))
+        return false;
+    for (float& x : d.threat)
+        if (!s.f32(x)) return false;
+    return s.text(d.motion_anchor) && get_strings(s, d.motion_tracked) && s.u32(d.maximum_episode_steps) &&
+           s.u32(d.difficulty_band_count) && s.f32(d.interaction_student_authority) &&
+           s.f32(d.interaction_reset_phase_fraction) && s.floats(d.initial_action_positions) &&
+           s.raw(&d.interaction_control_reference, 1) && s.raw(&d.interaction_initialize_from_reference, 1) &&
+           s.raw(&d.interaction_align_reference_yaw, 1) && s.f32(d.base_height_target) && s.f32(d.gait_period) &&
+           s.f32(d.clearance_target) && s.f32(d.success_tracking_threshold) && s.f32(d.support_force_threshold) && s.done();
+}
+
 }  // namespace
+
+void validate_task_pack(const TaskPackData& d) {
+    auto need = [](bool ok, const char* what) {
+        if (!ok) throw std::invalid_argument(what);
+    };
+    auto fits = [](const std::string& x) { return x.size() <= kMaxPayload; };
+    need(!d.id.empty() && fits(d.id) && !d.actions.empty() && d.maximum_episode_steps != 0 && d.difficulty_band_count != 0,
+         "TaskPack identity, dimensions, or episode limits are invalid");
+    auto probability = [](float x) { return std::isfinite(x) && x >= 0.0f && x <= 1.0f; };
+    need(probability(d.interaction_student_authority) && probability(d.interaction_reset_phase_fraction),
+         "TaskPack interaction configuration is invalid");
+    const float* t = d.threat;
+    need(d.threat_protected_group.empty() || (t[0] > 0.0f && t[1] > 0.0f && t[2] >= 0.0f && t[3] > 0.0f && t[4] > 0.0f &&
+                                                t[5] > t[4] && t[6] > t[5] && t[7] > 0.0f && t[8] > 0.0f && t[9] > 0.0f),
+         "TaskPack threat program is invalid");
+    const float* p = d.pushes;  // [4] radius, [5] speed lower, [6] speed upper, [7] height lower, [8] height upper
+    const bool ballistics = p[6] > 0.0f;
+    need(std::isfinite(p[4]) && p[4] >= 0.0f && std::isfinite(p[5]) && std::isfinite(p[6]) && std::isfinite(p[7]) &&
+             std::isfinite(p[8]) && p[5] >= 0.0f && p[6] >= p[5] && (!ballistics || p[5] > 0.0f) && p[8] >= p[7],
+         "TaskPack projectile ballistics are invalid");
+    for (const TaskPackContactGroup& g : d.contact_groups) {
+        const bool patch = g.support_patch_width != 0u || g.support_patch_height != 0u;
+        const float* b = g.support_patch_bounds;
+        need(!patch || (g.support && g.support_patch_width != 0u && g.support_patch_height != 0u &&
+                        static_cast<std::uint64_t>(g.support_patch_width) * g.support_patch_height <= 64u && std::isfinite(b[0]) &&
+                        std::isfinite(b[1]) && std::isfinite(b[2]) && std::isfinite(b[3]) && b[2] > b[0] && b[3] > b[1]),
+             "TaskPack support patch is invalid");
+    }
+}
+
+void write_task_pack(const TaskPackData& d, const std::string& path) {
+    if (path.empty()) throw std::invalid_argument("TaskPack output path is empty");
+    validate_task_pack(d);
+    publish_pack(encode_task(d), kTaskPackKind, kTaskPackVersion, path, "TaskPack");
+}
+
+TaskPackData read_task_pack(const std::string& path) {
+    LoadedPack f = load_pack(path, kTaskPackKind, kTaskPackVersion, kTaskPackVersion, "TaskPack");
+    TaskPackData d;
+    if (!decode_task(f.payload.data(), f.payload.size(), d)) throw std::invalid_argument("TaskPack payload is malformed");
+    d.content_hash = f.hash;
+    return d;
+}
 
 void write_policy_pack(const PolicyPackData& d, const std::string& path) {
     if (path.empty()) throw std::invalid_argument("PolicyPack output path is empty");
@@ -509,6 +714,47 @@ PolicyRolloutPackData read_policy_rollout_pack(const std::string& path) {
 }  // namespace numi
 
 extern "C" {
+
+MR_API int mr_task_pack_inspect(const char* path, MRTaskPackInfoC* info) {
+    try {
+        if (!path || !path[0]) throw std::invalid_argument("TaskPack path is empty");
+        if (!info) throw std::invalid_argument("info is null");
+        const numi::TaskPackData d = numi::read_task_pack(path);
+        MRTaskPackInfoC o{};
+        o.content_hash = d.content_hash;
+        o.action_count = static_cast<uint32_t>(d.actions.size());
+        o.outcome_count = static_cast<uint32_t>(d.outcomes.size());
+        o.contact_group_count = static_cast<uint32_t>(d.contact_groups.size());
+        o.joint_group_count = static_cast<uint32_t>(d.joint_groups.size());
+        o.reward_count = static_cast<uint32_t>(d.rewards.size());
+        o.termination_count = static_cast<uint32_t>(d.terminations.size());
+        o.maximum_episode_steps = d.maximum_episode_steps;
+        o.difficulty_band_count = d.difficulty_band_count;
+        o.terrain_sample_count = static_cast<uint32_t>(d.terrain_sample_offsets.size() / 4);
+        o.motion_tracked_body_count = static_cast<uint32_t>(d.motion_tracked.size());
+        o.base_height_target = d.base_height_target;
+        o.gait_period_seconds = d.gait_period;
+        o.clearance_target = d.clearance_target;
+        o.support_force_threshold = d.support_force_threshold;
+        std::snprintf(o.id, sizeof(o.id), "%s", d.id.c_str());
+        *info = o;
+        return 0;
+    } catch (const std::exception& e) {
+        numi::rt::set_last_error(e.what());
+        return -1;
+    }
+}
+
+MR_API int mr_task_pack_rewrite(const char* input_path, const char* output_path) {
+    try {
+        if (!input_path || !input_path[0] || !output_path || !output_path[0]) throw std::invalid_argument("TaskPack paths are required");
+        numi::write_task_pack(numi::read_task_pack(input_path), output_path);
+        return 0;
+    } catch (const std::exception& e) {
+        numi::rt::set_last_error(e.what());
+        return -1;
+    }
+}
 
 MR_API int mr_write_policy_rollout_pack(const MRPolicyRolloutPackC* pack, const char* output_path) {
     try {

@@ -110,6 +110,87 @@ struct PolicyRolloutPackData {
     std::uint64_t content_hash = 0;
 };
 
+// TaskPack files (reference: include/metalrobo/TaskProgram.hpp:211-500,
+// src/core/LearningPacks.cpp:81-258 rules, :1127-1262 payload): the same
+// container with artifact kind 1, format version 17.  The authored task is
+// name-based (actuators, bodies, joints are strings resolved against a robot
+// when compiled); the payload keeps the reference's field order and
+// encodings: strings and string lists as u64 counts + bytes, enums as u32,
+// booleans as u8, four-float records as 16 bytes, the capacity profile as
+// its 27 u32 fields.
+constexpr std::uint32_t kTaskPackKind = 1u;
+constexpr std::uint32_t kTaskPackVersion = 17u;
+constexpr std::size_t kCapacityProfileWords = 27;
+
+struct TaskPackOutcome {
+    std::string id, unit;
+    std::uint32_t source = 2u, direction = 0u, reward_operation = 2u;
+};
+struct TaskPackContactGroup {
+    std::string id;
+    std::vector<std::string> bodies;
+    std::uint8_t support = 0, forbidden = 0;
+    std::string reference_body;
+    float local_reference[4] = {};
+    float gait_phase_offset = 0.0f, stance_fraction = 0.5f;
+    float support_patch_bounds[4] = {};
+    std::uint32_t support_patch_width = 0, support_patch_height = 0;
+};
+struct TaskPackJointGroup {
+    std::string id;
+    std::vector<std::string> joints;
+};
+struct TaskPackReward {
+    std::uint32_t operation = 2u;
+    std::string source_group, target;
+    float weight = 0.0f;
+    float parameters[4] = {};
+};
+struct TaskPackTermination {
+    std::uint32_t operation = 0u;
+    std::string source_group;
+    std::uint32_t reason = 1u, priority = 0u;
+    float threshold = 0.0f, failure_penalty = 0.0f;
+    std::uint32_t minimum_band = 0u, maximum_band = 0xffffffffu;
+};
+
+struct TaskPackData {
+    std::string id;
+    std::uint32_t capacities[kCapacityProfileWords] = {};
+    std::vector<std::string> actions;
+    std::vector<TaskPackOutcome> outcomes;
+    std::vector<TaskPackContactGroup> contact_groups;
+    std::vector<TaskPackJointGroup> joint_groups;
+    std::vector<TaskPackReward> rewards;
+    std::vector<TaskPackTermination> terminations;
+    // Commands: lower, upper, limit lower, limit upper, difficulty step (xyzw each).
+    float commands[5][4] = {};
+    float standing_probability = 0.0f, difficulty_sampling_exponent = 2.0f, command_duration[2] = {5.0f, 10.0f};
+    // Pushes: maximum velocity, interval minimum / maximum, projectile standing
+    // probability, target radius, horizontal speed lower / upper, target height lower / upper.
+    float pushes[9] = {0.0f, 2.0f, 5.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    std::string terrain_body;
+    std::vector<float> terrain_sample_offsets, terrain_reset_translations;  // xyzw each
+    std::string threat_protected_group;
+    // Activation speed, horizon, safety margin, CBF alpha, step-over / sidestep /
+    // lean maximum heights, urgency, desired-velocity horizon, projection epsilon.
+    float threat[10] = {0.5f, 2.0f, 0.05f, 2.0f, 0.35f, 0.75f, 1.10f, 0.35f, 0.20f, 1.0e-5f};
+    std::string motion_anchor;
+    std::vector<std::string> motion_tracked;
+    std::uint32_t maximum_episode_steps = 1000u, difficulty_band_count = 1u;
+    float interaction_student_authority = 0.1f, interaction_reset_phase_fraction = 0.0f;
+    std::vector<float> initial_action_positions;
+    std::uint8_t interaction_control_reference = 1, interaction_initialize_from_reference = 1, interaction_align_reference_yaw = 0;
+    float base_height_target = 0.0f, gait_period = 0.8f, clearance_target = 0.1f, success_tracking_threshold = 0.8f,
+          support_force_threshold = 1.0f;
+    std::uint64_t content_hash = 0;
+};
+
+// Throws std::invalid_argument on a pack the reference's writer refuses.
+void validate_task_pack(const TaskPackData& d);
+void write_task_pack(const TaskPackData& d, const std::string& path);
+TaskPackData read_task_pack(const std::string& path);
+
 // A task transition as the learner's record (c_api.cpp's publication).
 LearningTransition learning_transition(const MRTaskTransitionC& t);
 // The C record -> the owned record (spans copied, transitions converted).

@@ -522,6 +522,27 @@ class PolicyRolloutPackInfoC(ct.Structure):
     ]
 
 
+class TaskPackInfoC(ct.Structure):
+    _fields_ = [
+        ("content_hash", ct.c_uint64),
+        ("action_count", ct.c_uint32),
+        ("outcome_count", ct.c_uint32),
+        ("contact_group_count", ct.c_uint32),
+        ("joint_group_count", ct.c_uint32),
+        ("reward_count", ct.c_uint32),
+        ("termination_count", ct.c_uint32),
+        ("maximum_episode_steps", ct.c_uint32),
+        ("difficulty_band_count", ct.c_uint32),
+        ("terrain_sample_count", ct.c_uint32),
+        ("motion_tracked_body_count", ct.c_uint32),
+        ("base_height_target", ct.c_float),
+        ("gait_period_seconds", ct.c_float),
+        ("clearance_target", ct.c_float),
+        ("support_force_threshold", ct.c_float),
+        ("id", ct.c_char * 64),
+    ]
+
+
 class ModelWorldC(ct.Structure):
     _fields_ = [
         ("body_count", ct.c_uint32),
@@ -757,6 +778,8 @@ EXPORTED_SYMBOLS: Final = (
     "mr_task_rollout_write_policy_rollout_pack",
     "mr_write_policy_rollout_pack",
     "mr_policy_rollout_pack_inspect",
+    "mr_task_pack_inspect",
+    "mr_task_pack_rewrite",
     "mr_task_rollout_policy_latents",
     "mr_task_rollout_policy_log_probabilities",
     "mr_task_rollout_policy_values",
@@ -954,6 +977,10 @@ class Bindings:
         L.mr_write_policy_rollout_pack.restype = ct.c_int
         L.mr_policy_rollout_pack_inspect.argtypes = [ct.c_char_p, P(PolicyRolloutPackInfoC), P(ct.c_float), ct.c_size_t]
         L.mr_policy_rollout_pack_inspect.restype = ct.c_int
+        L.mr_task_pack_inspect.argtypes = [ct.c_char_p, P(TaskPackInfoC)]
+        L.mr_task_pack_inspect.restype = ct.c_int
+        L.mr_task_pack_rewrite.argtypes = [ct.c_char_p, ct.c_char_p]
+        L.mr_task_pack_rewrite.restype = ct.c_int
 
     def last_error(self) -> str:
         value = self.lib.mr_last_error()

@@ -317,6 +317,25 @@ def inspect_policy_rollout_pack(path: str | os.PathLike[str], *, library: native
     return fields, params
 
 
+def inspect_task_pack(path: str | os.PathLike[str], *, library: native.Bindings | None = None) -> dict:
+    """Table counts and episode constants of a TaskPack file (mr_task_pack_inspect)."""
+
+    lib = library or native.bindings()
+    info = native.TaskPackInfoC()
+    lib.check(lib.lib.mr_task_pack_inspect(os.fsencode(path), ct.byref(info)), "mr_task_pack_inspect")
+    fields = {name: getattr(info, name) for name, _ in native.TaskPackInfoC._fields_}
+    fields["id"] = info.id.decode()
+    return fields
+
+
+def rewrite_task_pack(source: str | os.PathLike[str], destination: str | os.PathLike[str], *,
+                      library: native.Bindings | None = None) -> None:
+    """Reads a TaskPack, checks the writer's artifact rules, writes it again (mr_task_pack_rewrite)."""
+
+    lib = library or native.bindings()
+    lib.check(lib.lib.mr_task_pack_rewrite(os.fsencode(source), os.fsencode(destination)), "mr_task_pack_rewrite")
+
+
 def quality_solve(mass: np.ndarray, jacobian: np.ndarray, free_velocity: np.ndarray, target: np.ndarray,
                   regularization: np.ndarray, friction: np.ndarray, *, counts: np.ndarray | None = None,
                   warm: np.ndarray | None = None, max_newton: int = 0, tolerance: float = 0.0,

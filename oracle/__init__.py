@@ -253,6 +253,56 @@ def reference_inspect_policy_rollout_pack(path, parameter_count: int = 0):
     return fields, params
 
 
+def reference_write_task_pack(variant: int, path) -> None:
+    """A TaskPack filled field by field in the harness (0: every table and
+    program used; 1: the smallest valid pack), written by the reference's
+    writeTaskPack."""
+
+    lib = _ref_lib()
+    lib.ref_write_task_pack.restype = ct.c_int
+    lib.ref_write_task_pack.argtypes = [ct.c_int, ct.c_char_p, ct.c_char_p, ct.c_size_t]
+    err = ct.create_string_buffer(512)
+    st = lib.ref_write_task_pack(variant, os.fsencode(path), err, len(err))
+    if st != 0:
+        raise ValueError(f"reference writeTaskPack failed ({st}): {err.value.decode()}")
+
+
+def reference_inspect_task_pack(path) -> dict:
+    """The reference's readTaskPack in the layout of mr_task_pack_inspect."""
+
+    from numi_lab_b200 import native
+
+    lib = _ref_lib()
+    lib.ref_task_pack_inspect.restype = ct.c_int
+    lib.ref_task_pack_inspect.argtypes = [ct.c_char_p, ct.c_void_p, ct.c_char_p, ct.c_size_t]
+    info = native.TaskPackInfoC()
+    err = ct.create_string_buffer(512)
+    st = lib.ref_task_pack_inspect(os.fsencode(path), ct.addressof(info), err, len(err))
+    if st != 0:
+        raise ValueError(f"reference readTaskPack failed ({st}): {err.value.decode()}")
+    fields = {name: getattr(info, name) for name, _ in native.TaskPackInfoC._fields_}
+    fields["id"] = info.id.decode()
+    return fields
+
+
+def reference_rewrite_task_pack(source, destination) -> None:
+    """The reference's readTaskPack then writeTaskPack."""
+
+    lib = _ref_lib()
+    lib.ref_task_pack_rewrite.restype = ct.c_int
+    lib.ref_task_pack_rewrite.argtypes = [ct.c_char_p, ct.c_char_p, ct.c_char_p, ct.c_size_t]
+    err = ct.create_string_buffer(512)
+    st = lib.ref_task_pack_rewrite(os.fsencode(source), os.fsencode(destination), err, len(err))
+    if st != 0:
+        raise ValueError(f"reference TaskPack rewrite failed ({st}): {err.value.decode()}")
+
+
+def reference_capacity_profile_bytes() -> int:
+    lib = _ref_lib()
+    lib.ref_capacity_profile_bytes.restype = ct.c_size_t
+    return int(lib.ref_capacity_profile_bytes())
+
+
 def reference_inspect_policy_pack(path):
     """The reference's readPolicyPack: (fields, FP32 tables in file order)
     in the layout of mr_policy_pack_inspect."""

@@ -24,6 +24,8 @@
 #include "metalrobo/RigidBodyWorld.hpp"
 #include "metalrobo/EngineModel.hpp"
 #include "metalrobo/LearningPacks.hpp"
+#include "metalrobo/MetalWorldCapacity.hpp"
+#include "metalrobo/TaskProgram.hpp"
 #include "metalrobo/PolicyProgram.hpp"
 #include "metalrobo/QualityContactSolver.hpp"
 #include "metalrobo/ReferenceConicSolver.hpp"
@@ -866,6 +868,148 @@ __attribute__((visibility("default"))) int ref_write_policy_pack(const MRPolicyP
     if (!r.succeeded() && err && err_len) std::snprintf(err, err_len, "%s", r.message.c_str());
     return r.succeeded() ? 0 : static_cast<int>(r.status);
 }
+
+// A TaskPack filled field by field (variant 0: every table and program used,
+// a support patch, projectile ballistics, a threat program, terrain samples;
+// variant 1: the smallest valid pack), written by the reference's writer
+// (writeTaskPack).  The reference's own task builders live beside its world
+// compiler, which needs sources absent here.
+__attribute__((visibility("default"))) int ref_write_task_pack(int variant, const char* path, char* err, size_t err_len) {
+    TaskPack p;
+    p.id = variant == 0 ? "full_task_pack" : "minimal";
+    p.actions = {{"hip_pitch"}};
+    if (variant == 0) {
+        p.capacities.candidatePairs = 96u;
+        p.capacities.rawContacts = 384u;
+        p.capacities.manifolds = 48u;
+        p.actions = {{"left_hip"}, {"right_hip"}, {"left_knee"}, {"right_knee"}, {"waist"}};
+        p.outcomes = {{"tracking", "score", TaskOutcomeSource::trackingScore, TaskOutcomeDirection::higherIsBetter,
+                       TaskRewardOperator::constant},
+                      {"slip", "m/s", TaskOutcomeSource::rewardContribution, TaskOutcomeDirection::lowerIsBetter,
+                       TaskRewardOperator::supportSlip}};
+        TaskContactGroup foot;
+        foot.id = "left_foot";
+        foot.bodies = {"left_ankle", "left_toe"};
+        foot.support = true;
+        foot.referenceBody = "left_ankle";
+        foot.localReference = {0.02f, 0.0f, -0.03f, 0.01f};
+        foot.gaitPhaseOffsetRadians = 3.14159f;
+        foot.stanceFraction = 0.6f;
+        foot.supportPatchBounds = {-0.1f, -0.04f, 0.1f, 0.04f};
+        foot.supportPatchWidth = 4u;
+        foot.supportPatchHeight = 2u;
+        TaskContactGroup torso;
+        torso.id = "undesired";
+        torso.bodies = {"pelvis", "torso", "head"};
+        torso.forbidden = true;
+        torso.referenceBody = "torso";
+        p.contactGroups = {foot, torso};
+        p.jointGroups = {{"legs", {"left_hip", "right_hip", "left_knee", "right_knee"}}, {"waist", {"waist"}}};
+        TaskRewardOperatorSpec r0;
+        r0.operation = TaskRewardOperator::linearVelocityTracking;
+        r0.weight = 1.0f;
+        r0.parameters = {0.25f, 0.0f, 0.0f, 0.0f};
+        TaskRewardOperatorSpec r1;
+        r1.operation = TaskRewardOperator::jointGroupPostureAbsolute;
+        r1.sourceGroup = "waist";
+        r1.weight = -1.0f;
+        TaskRewardOperatorSpec r2;
+        r2.operation = TaskRewardOperator::objectLift;
+        r2.target = "box";
+        r2.weight = 2.0f;
+        r2.parameters = {0.1f, 0.4f, 0.0f, 0.0f};
+        p.rewards = {r0, r1, r2};
+        TaskTerminationOperatorSpec t0;
+        t0.operation = TaskTerminationOperator::minimumRootHeight;
+        t0.reason = MR_TASK_TERMINATION_HEIGHT;
+        t0.priority = 1u;
+        t0.threshold = 0.3f;
+        t0.failurePenalty = -2.0f;
+        TaskTerminationOperatorSpec t1;
+        t1.operation = TaskTerminationOperator::contactGroup;
+        t1.sourceGroup = "undesired";
+        t1.reason = MR_TASK_TERMINATION_CONTACT;
+        t1.priority = 3u;
+        t1.threshold = 0.5f;
+        t1.minimumDifficultyBand = 1u;
+        t1.maximumDifficultyBand = 4u;
+        p.terminations = {t0, t1};
+        p.commands.lower = {-0.5f, -0.3f, -0.5f, 0.0f};
+        p.commands.upper = {1.0f, 0.3f, 0.5f, 0.0f};
+        p.commands.limitLower = {-1.0f, -0.6f, -1.0f, 0.0f};
+        p.commands.limitUpper = {2.0f, 0.6f, 1.0f, 0.0f};
+        p.commands.difficultyStep = {0.1f, 0.05f, 0.1f, 0.0f};
+        p.commands.standingProbability = 0.1f;
+        p.commands.minimumDurationSeconds = 2.0f;
+        p.commands.maximumDurationSeconds = 4.0f;
+        p.pushes.maximumVelocity = 1.5f;
+        p.pushes.projectileTargetHorizontalRadius = 0.2f;
+        p.pushes.projectileHorizontalSpeedLower = 2.0f;
+        p.pushes.projectileHorizontalSpeedUpper = 4.0f;
+        p.pushes.projectileTargetHeightLower = 0.3f;
+        p.pushes.projectileTargetHeightUpper = 1.2f;
+        p.terrain.body = "terrain";
+        p.terrain.sampleOffsets = {{0.1f, 0.0f, 0.0f, 0.0f}, {-0.1f, 0.0f, 0.0f, 0.0f}, {0.0f, 0.1f, 0.0f, 0.0f}};
+        p.terrain.resetTranslations = {{0.0f, 0.0f, 0.05f, 0.0f}};
+        p.threat.protectedGroup = "undesired";
+        p.motion.anchorBody = "pelvis";
+        p.motion.trackedBodies = {"left_ankle", "torso"};
+        p.maximumEpisodeSteps = 750u;
+        p.difficultyBandCount = 5u;
+        p.interactionStudentAuthority = 0.25f;
+        p.interactionResetPhaseFraction = 0.1f;
+        p.initialActionPositions = {0.1f, -0.1f, 0.3f, 0.3f, 0.0f};
+        p.interactionAlignReferenceYaw = true;
+        p.baseHeightTarget = 0.74f;
+        p.gaitPeriodSeconds = 0.7f;
+        p.clearanceTarget = 0.08f;
+        p.successTrackingThreshold = 0.75f;
+        p.supportForceThreshold = 2.0f;
+    }
+    const LearningPackResult r = writeTaskPack(p, path);
+    if (!r.succeeded() && err && err_len) std::snprintf(err, err_len, "%s", r.message.c_str());
+    return r.succeeded() ? 0 : static_cast<int>(r.status);
+}
+
+// The reference's reader (readTaskPack) into this library's info record.
+__attribute__((visibility("default"))) int ref_task_pack_inspect(const char* path, MRTaskPackInfoC* info, char* err, size_t err_len) {
+    TaskPack p;
+    const LearningPackResult r = readTaskPack(path, p);
+    if (!r.succeeded()) {
+        if (err && err_len) std::snprintf(err, err_len, "%s", r.message.c_str());
+        return static_cast<int>(r.status);
+    }
+    MRTaskPackInfoC o{};
+    o.content_hash = r.contentHash;
+    o.action_count = static_cast<uint32_t>(p.actions.size());
+    o.outcome_count = static_cast<uint32_t>(p.outcomes.size());
+    o.contact_group_count = static_cast<uint32_t>(p.contactGroups.size());
+    o.joint_group_count = static_cast<uint32_t>(p.jointGroups.size());
+    o.reward_count = static_cast<uint32_t>(p.rewards.size());
+    o.termination_count = static_cast<uint32_t>(p.terminations.size());
+    o.maximum_episode_steps = p.maximumEpisodeSteps;
+    o.difficulty_band_count = p.difficultyBandCount;
+    o.terrain_sample_count = static_cast<uint32_t>(p.terrain.sampleOffsets.size());
+    o.motion_tracked_body_count = static_cast<uint32_t>(p.motion.trackedBodies.size());
+    o.base_height_target = p.baseHeightTarget;
+    o.gait_period_seconds = p.gaitPeriodSeconds;
+    o.clearance_target = p.clearanceTarget;
+    o.support_force_threshold = p.supportForceThreshold;
+    std::snprintf(o.id, sizeof(o.id), "%s", p.id.c_str());
+    *info = o;
+    return 0;
+}
+
+// readTaskPack then writeTaskPack (the reference's artifact rules apply).
+__attribute__((visibility("default"))) int ref_task_pack_rewrite(const char* in, const char* out, char* err, size_t err_len) {
+    TaskPack p;
+    LearningPackResult r = readTaskPack(in, p);
+    if (r.succeeded()) r = writeTaskPack(p, out);
+    if (!r.succeeded() && err && err_len) std::snprintf(err, err_len, "%s", r.message.c_str());
+    return r.succeeded() ? 0 : static_cast<int>(r.status);
+}
+
+__attribute__((visibility("default"))) size_t ref_capacity_profile_bytes() { return sizeof(MetalWorldCapacityProfile); }
 
 // The reference's PolicyRolloutPack writer (writePolicyRolloutPack) over the
 // same record this library's mr_write_policy_rollout_pack takes; task

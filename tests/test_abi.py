@@ -79,6 +79,7 @@ def test_struct_sizes_match_header_layout(tmp_path):
         "MRPolicyRolloutBatchC": native.PolicyRolloutBatchC,
         "MRPolicyRolloutPackC": native.PolicyRolloutPackC,
         "MRPolicyRolloutPackInfoC": native.PolicyRolloutPackInfoC,
+        "MRTaskPackInfoC": native.TaskPackInfoC,
     }
     src = tmp_path / "sizes.c"
     body = "".join(f'printf("%zu\\n", sizeof({name}));' for name in records)
