@@ -908,9 +908,9 @@ typedef struct MRTaskContactGroupC {
 } MRTaskContactGroupC;
 
 /* A compiled task program: the tables and constants of the reference's
- * MRTaskProgramHeaderGPU (:358-441) that the evaluated subset reads.  One
- * actor history frame, one difficulty band, a flat ground; no terrain,
- * pushes, support patches or sensor biases. */
+ * MRTaskProgramHeaderGPU (:358-441) that the evaluated subset reads.  A
+ * stacked actor history without observation delay, one difficulty band, a
+ * flat ground; no terrain, pushes, support patches or sensor biases. */
 typedef struct MRTaskProgramC {
     const MRTaskActionBindingC* actions;
     uint32_t action_count;          /* equals the world's action count */
@@ -937,6 +937,7 @@ typedef struct MRTaskProgramC {
     uint32_t maximum_episode_steps; /* timeout */
     uint32_t action_history;        /* delay-line slots including the filter slot, 3..8 */
     uint32_t action_delay_steps;    /* raw actions of delay; at most action_history - 2 take effect */
+    uint32_t observation_history;   /* actor frames stacked, oldest first (program.layout.y), 1..8 */
     float base_height_target;       /* program.locomotion.x */
     float gait_period_seconds;      /* program.locomotion.y */
     float root_reference[3];        /* root link origin from the root's q position, root axes */
@@ -992,7 +993,8 @@ struct MRTaskTransitionC {
  * the bindings to drive targets); the physics step; complete (rewards,
  * terminations, timeout, the next command and the next actor frame).
  * Observations become the actor frames the step's actions were taken on
- * (actor_count values), actions the policy's normalised outputs.  Every
+ * (observation_history x actor_count values, the oldest frame first),
+ * actions the policy's normalised outputs.  Every
  * environment starts a new episode at the next advance.  Refused: an
  * operator outside the subset above, an index out of range, a pile or
  * stack world. */

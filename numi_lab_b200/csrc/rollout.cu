@@ -775,7 +775,7 @@ struct MRTaskRolloutHandle {
     // Values per environment in an observation row: the task's actor frame,
     // else [q, v].
     std::uint32_t observation_count() const {
-        return task ? static_cast<std::uint32_t>(task->prog.nobs) : model.world.nq + model.world.nv;
+        return task ? static_cast<std::uint32_t>(task->prog.frames * task->prog.nobs) : model.world.nq + model.world.nv;
     }
 
     // Task-layer launch over environments [o, o + n) of control step k.
@@ -788,14 +788,14 @@ struct MRTaskRolloutHandle {
         t.state = d_task_state.ptr + o;
         t.action_history = d_task_history.ptr + static_cast<size_t>(o) * P.history * P.na;
         t.previous_joint = d_task_previous.ptr + static_cast<size_t>(o) * 2 * P.na;
-        t.frame = d_task_frame.ptr + static_cast<size_t>(o) * P.nobs;
+        t.frame = d_task_frame.ptr + static_cast<size_t>(o) * P.frames * P.nobs;
         t.reset_q = d_reset_q.ptr + static_cast<size_t>(o) * P.nq;
         t.reset_v = d_reset_v.ptr + static_cast<size_t>(o) * P.nv;
         t.q = d_q.ptr + static_cast<size_t>(o) * P.nq;
         t.v = d_v.ptr + static_cast<size_t>(o) * P.nv;
         t.masks_in = masks ? masks + item0 : nullptr;
         t.masks_out = d_task_masks.ptr + item0;
-        t.observations = obs ? obs + item0 * P.nobs : nullptr;
+        t.observations = obs ? obs + item0 * P.frames * P.nobs : nullptr;
         t.actions = actions ? actions + item0 * P.na : nullptr;
         t.targets = d_task_targets.ptr + static_cast<size_t>(o) * P.na;
         t.status = status + item0;
@@ -843,8 +843,8 @@ struct MRTaskRolloutHandle {
         pp.nv = static_cast<int>(model.world.nv);
         pp.q = d_q.ptr + static_cast<size_t>(o) * pp.nq;
         pp.v = d_v.ptr + static_cast<size_t>(o) * pp.nv;
-        pp.frame = task ? d_task_frame.ptr + static_cast<size_t>(o) * task->prog.nobs : nullptr;
-        pp.frame_count = task ? task->prog.nobs : 0;
+        pp.frame = task ? d_task_frame.ptr + static_cast<size_t>(o) * task->prog.frames * task->prog.nobs : nullptr;
+        pp.frame_count = task ? task->prog.frames * task->prog.nobs : 0;
         pp.envs = static_cast<int>(n);
         pp.env_base = static_cast<int>(o);
         pp.na = static_cast<int>(model.world.action_count);
@@ -1294,6 +1294,9 @@ std::unique_ptr<InstalledTask> compile_task(const MRTaskRolloutHandle& h, const 
     need(t.default_q != nullptr && t.default_q_count == nq, "default_q must hold nq = " + to_string(nq) + " values");
     for (std::uint32_t i = 0; i < nq; ++i) need(finite_value(t.default_q[i]), "default_q must be finite");
     need(t.action_history >= 3 && t.action_history <= static_cast<std::uint32_t>(numi::kTaskMaxHistory), "action_history must be 3-8");
+    need(t.observation_history >= 1 && t.observation_history <= 8u, "observation_history must be 1-8");
+    need(static_cast<std::uint64_t>(t.observation_history) * t.actor_count <= static_cast<std::uint64_t>(numi::kTaskMaxObservations),
+         "observation_history x actor_count must be at most 256 (the policy's widest input)");
     need(t.maximum_episode_steps >= 1, "maximum_episode_steps must be positive");
     need(finite_value(t.gait_period_seconds) && t.gait_period_seconds > 0.0f, "gait_period_seconds must be positive");
     need(finite_value(t.command_duration_seconds[0]) && finite_value(t.command_duration_seconds[1]) &&
@@ -1519,6 +1522,7 @@ std::unique_ptr<InstalledTask> compile_task(const MRTaskRolloutHandle& h, const 
     P.nrandom = static_cast<int>(t.randomization_count);
     P.ngroups = static_cast<int>(t.joint_group_count);
     P.history = static_cast<int>(t.action_history);
+    P.frames = static_cast<int>(t.observation_history);
     P.delay = static_cast<int>(std::min<std::uint32_t>(t.action_delay_steps, t.action_history - 2));
     P.max_episode_steps = static_cast<int>(t.maximum_episode_steps);
     P.nq = static_cast<int>(nq);
@@ -1601,24 +1605,24 @@ MR_API int mr_task_rollout_set_task(MRTaskRolloutHandle* handle, const MRTaskPro
         std::unique_ptr<InstalledTask> compiled = compile_task(h, *program);
         if (h.policy) {
             const int in = h.policy->params.actor[0].in;
-            if (in != compiled->prog.nobs)
-                throw std::invalid_argument("the installed policy takes " + std::to_string(in) + " observations; the task's actor frame has " +
-                                            std::to_string(compiled->prog.nobs) + " (clear the policy first)");
+            if (in != compiled->prog.frames * compiled->prog.nobs)
+                throw std::invalid_argument("the installed policy takes " + std::to_string(in) + " observations; the task's actor history has " +
+                                            std::to_string(compiled->prog.frames * compiled->prog.nobs) + " (clear the policy first)");
         }
         drop_graphs(h);
         const numi::TaskProgramDevice& P = compiled->prog;
         h.d_task_state.resize(h.envs);
         h.d_task_history.resize(static_cast<size_t>(h.envs) * P.history * P.na);
         h.d_task_previous.resize(static_cast<size_t>(h.envs) * 2 * P.na);
-        h.d_task_frame.resize(static_cast<size_t>(h.envs) * P.nobs);
+        h.d_task_frame.resize(static_cast<size_t>(h.envs) * P.frames * P.nobs);
         h.d_task_targets.resize(static_cast<size_t>(h.envs) * P.na);
         h.d_task_air.resize(static_cast<size_t>(h.envs) * numi::kTaskMaxGroups);
         check(cudaMemsetAsync(h.d_task_history.ptr, 0, h.d_task_history.count * sizeof(float), h.stream), "clear task history");
         check(cudaMemsetAsync(h.d_task_previous.ptr, 0, h.d_task_previous.count * sizeof(float), h.stream), "clear task history");
         h.task = std::move(compiled);
         h.clear_task_state();
-        h.stats_layout.actor_observation_count = static_cast<std::uint32_t>(P.nobs);
-        h.stats_layout.critic_observation_count = static_cast<std::uint32_t>(P.nobs);
+        h.stats_layout.actor_observation_count = static_cast<std::uint32_t>(P.frames * P.nobs);
+        h.stats_layout.critic_observation_count = static_cast<std::uint32_t>(P.frames * P.nobs);
         h.stats_layout.maximum_episode_steps = static_cast<std::uint32_t>(P.max_episode_steps);
         h.stats_layout.task_fingerprint = h.task->fingerprint;
         h.last_steps = 0;

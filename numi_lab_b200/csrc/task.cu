@@ -423,7 +423,7 @@ __global__ void __launch_bounds__(32 * kTaskWarps) task_observe_kernel(TaskParam
     const unsigned env = static_cast<unsigned>(p.env_base + local);
     TaskEnvState st = p.state[local];
     const bool reset = st.initialized == 0u || st.pending_reset != 0u || (p.masks_in != nullptr && p.masks_in[local] != 0u);
-    float* frame = p.frame + static_cast<size_t>(local) * P.nobs;
+    float* frame = p.frame + static_cast<size_t>(local) * P.frames * P.nobs;  // the env's history, oldest first
     if (reset) {
         const unsigned episode = st.episode + 1u;
         float* rq = p.reset_q + static_cast<size_t>(local) * P.nq;
@@ -502,13 +502,15 @@ __global__ void __launch_bounds__(32 * kTaskWarps) task_observe_kernel(TaskParam
         // Every delay-line slot is zero here; the newest raw slot stands for
         // all of them.
         write_frame(P, rq, rv, st, hist + (P.history - 2) * P.na, prev + P.na, nullptr, env, episode, 0u, frame, lane);
+        __syncwarp();
+        for (int i = lane; i < (P.frames - 1) * P.nobs; i += 32) frame[P.nobs + i] = frame[i % P.nobs];  // every slot the reset frame
         if (lane == 0) p.state[local] = st;
     }
     if (lane == 0) p.masks_out[local] = reset ? 1u : 0u;
     __syncwarp();
     if (p.observations) {
-        float* out = p.observations + static_cast<size_t>(local) * P.nobs;
-        for (int i = lane; i < P.nobs; i += 32) out[i] = frame[i];
+        float* out = p.observations + static_cast<size_t>(local) * P.frames * P.nobs;
+        for (int i = lane; i < P.frames * P.nobs; i += 32) out[i] = frame[i];
     }
 }
 
@@ -814,8 +816,14 @@ __global__ void __launch_bounds__(32 * kTaskWarps) task_complete_kernel(TaskPara
 
     // The next decision's frame, then this step's joint history (:6478-6630).
     if (!done || (timeout && !physics_error)) {
-        float* frame = p.frame + static_cast<size_t>(local) * P.nobs;
-        write_frame(P, q, v, st, hist + raw_last * P.na, prev + P.na, gm, env, st.episode, episode_steps, frame, lane);
+        float* frame = p.frame + static_cast<size_t>(local) * P.frames * P.nobs;
+        // Shift the history one frame older, then write the newest (:6478-6517).
+        for (int h = 0; h + 1 < P.frames; ++h) {
+            for (int i = lane; i < P.nobs; i += 32) frame[h * P.nobs + i] = frame[(h + 1) * P.nobs + i];
+            __syncwarp();
+        }
+        write_frame(P, q, v, st, hist + raw_last * P.na, prev + P.na, gm, env, st.episode, episode_steps,
+                    frame + (P.frames - 1) * P.nobs, lane);
         __syncwarp();
         for (int a = lane; a < P.na; a += 32) {
             const MRTaskActionBindingC b = P.actions[a];

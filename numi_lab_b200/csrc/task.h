@@ -58,6 +58,7 @@ struct TaskProgramDevice {
     float support_force_threshold, clearance_target, physics_dt, ground_height;
     std::int32_t na, nobs, nrewards, nterminations, nrandom, ngroups;
     std::int32_t history, delay, max_episode_steps, nq, nv;
+    std::int32_t frames;       // actor frames stacked in an observation (oldest first)
     std::int32_t fixed_root;   // the root is welded to the world: root sources read zero
     float dt;                  // control step, seconds
     float base_height, gait_period, standing_probability, duration_min, duration_max;
@@ -73,14 +74,14 @@ struct TaskParams {
     TaskEnvState* state;           // [env]
     float* action_history;         // [env][history][na]: raw slots 0..history-2, filter slot history-1
     float* previous_joint;         // [env][2][na]: joint velocity, joint position at the last step's end
-    float* frame;                  // [env][nobs]: the actor frame of the next decision
+    float* frame;                  // [env][frames][nobs]: the actor history of the next decision, oldest first
     float* reset_q;                // [env][nq]
     float* reset_v;                // [env][nv]
     const float* q;                // [env][nq]
     const float* v;                // [env][nv]
     const std::uint32_t* masks_in; // caller's reset masks of this step [env], or null
     std::uint32_t* masks_out;      // [env]: the step's resets
-    float* observations;           // [env][nobs] of this step, or null
+    float* observations;           // [env][frames * nobs] of this step, or null
     const float* actions;          // [env][na] of this step
     float* targets;                // [env][na]: drive targets for the control step
     const std::uint32_t* status;   // [env] of this step

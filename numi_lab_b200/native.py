@@ -421,6 +421,7 @@ class TaskProgramC(ct.Structure):
         ("maximum_episode_steps", ct.c_uint32),
         ("action_history", ct.c_uint32),
         ("action_delay_steps", ct.c_uint32),
+        ("observation_history", ct.c_uint32),
         ("base_height_target", ct.c_float),
         ("gait_period_seconds", ct.c_float),
         ("root_reference", ct.c_float * 3),

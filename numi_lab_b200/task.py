@@ -123,6 +123,7 @@ class TaskProgram:
     maximum_episode_steps: int = 500
     action_history: int = 3
     action_delay_steps: int = 0
+    observation_history: int = 1  # actor frames stacked per observation, oldest first
     base_height_target: float = 0.0
     gait_period_seconds: float = 0.8
     root_reference: tuple[float, float, float] = (0.0, 0.0, 0.0)
@@ -209,6 +210,7 @@ def task_program_c(program: TaskProgram) -> tuple[native.TaskProgramC, list[Any]
     p.maximum_episode_steps = program.maximum_episode_steps
     p.action_history = program.action_history
     p.action_delay_steps = program.action_delay_steps
+    p.observation_history = program.observation_history
     p.base_height_target = program.base_height_target
     p.gait_period_seconds = program.gait_period_seconds
     p.root_reference[:] = list(program.root_reference)
@@ -263,7 +265,7 @@ def locomotion_task(records, default_q: np.ndarray, *, base_height: float | None
                     action_delay_steps: int = 0, noise: float = 0.0, min_height_fraction: float = 0.6,
                     max_tilt: float = 1.22173048, groups: Sequence[Sequence[int]] | None = None,
                     contact_groups: Sequence[ContactGroup] | None = None, support_force_threshold: float = 1.0,
-                    clearance_target: float = 0.08) -> TaskProgram:
+                    clearance_target: float = 0.08, observation_history: int = 1) -> TaskProgram:
     """Velocity-tracking locomotion over every actuated joint of an
     articulated world with a floating root.  Actor frame (per the reference's
     G1 legs frame): raw action one step back, command xyz + extension lane,
@@ -341,6 +343,7 @@ def locomotion_task(records, default_q: np.ndarray, *, base_height: float | None
                        randomization=randomization, joint_groups=[list(g) for g in groups], contact_groups=cgroups,
                        support_force_threshold=support_force_threshold, clearance_target=clearance_target,
                        maximum_episode_steps=maximum_episode_steps, action_history=action_history,
-                       action_delay_steps=action_delay_steps, base_height_target=height, gait_period_seconds=0.8,
+                       action_delay_steps=action_delay_steps, observation_history=observation_history,
+                       base_height_target=height, gait_period_seconds=0.8,
                        command_lower=(-0.5, -0.3, -0.5), command_upper=(1.0, 0.3, 0.5), standing_probability=0.1,
                        command_duration_seconds=(2.0, 5.0), task_fingerprint=0x7A5C0001)

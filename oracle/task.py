@@ -152,6 +152,7 @@ class TaskOracle:
         self.na = len(program.actions)
         self.nobs = len(program.actor)
         self.L = int(program.action_history)
+        self.H = int(getattr(program, "observation_history", 1))  # stacked actor frames, oldest first
         self.delay = min(int(program.action_delay_steps), self.L - 2)
         self.lo = np.asarray(limit_lower, np.float64)
         self.hi = np.asarray(limit_upper, np.float64)
@@ -248,7 +249,7 @@ class TaskOracle:
         return x / TWO_PI < G.stance_fraction
 
     def new_state(self) -> EnvState:
-        return EnvState(np.zeros((self.L, self.na)), np.zeros((2, self.na)), np.zeros(self.nobs))
+        return EnvState(np.zeros((self.L, self.na)), np.zeros((2, self.na)), np.zeros((self.H, self.nobs)))
 
     # -- root frame (:396-478) ------------------------------------------------
     def root(self, q, v):
@@ -347,7 +348,7 @@ class TaskOracle:
 
         reset = (not st.initialized) or st.pending_reset or bool(mask)
         if not reset:
-            return False, None, None, st.frame.copy()
+            return False, None, None, st.frame.reshape(-1).copy()
         episode = st.episode + 1
         rq = self.default_q.copy()
         rv = np.zeros(self.nv)
@@ -387,8 +388,9 @@ class TaskOracle:
         st.phase = 0.0
         st.previous_height = self.root(rq, rv)[1][2]
         st.episode_return = st.episode_tracking = 0.0
-        st.frame = self.frame(env, rq, rv, st, self.L - 2, st.previous_joint[1], episode, 0)
-        return True, rq, rv, st.frame.copy()
+        first = self.frame(env, rq, rv, st, self.L - 2, st.previous_joint[1], episode, 0)
+        st.frame = np.tile(first, (self.H, 1))  # every history slot the reset frame (:3072-3098)
+        return True, rq, rv, st.frame.reshape(-1).copy()
 
     def apply(self, st: EnvState, actions) -> np.ndarray:
         """Drive targets [na] for the physics step (:3520-3668)."""
@@ -567,7 +569,7 @@ class TaskOracle:
         st.episode_return = 0.0 if done else episode_return
         st.episode_tracking = 0.0 if done else episode_tracking
         if not done or (timeout and not physics_error):
-            st.frame = self.frame(env, q, v, st, raw_last, st.previous_joint[1], st.episode, steps, gm)
+            st.frame = np.vstack([st.frame[1:], self.frame(env, q, v, st, raw_last, st.previous_joint[1], st.episode, steps, gm)[None]])
             for a, b in enumerate(p.actions):
                 st.previous_joint[0, a] = v[b.v_index]
                 st.previous_joint[1, a] = q[b.q_index]

@@ -68,10 +68,12 @@ def test_task_layer_matches_oracle_step_by_step(cuda_device, contacts):
         # Tight height and tilt limits: episodes end by timeout, height and
         # tilt within the run.
         groups = T.foot_contact_groups(w.model()) if contacts else None
+        # The contact variant also stacks three actor frames.
         prog = _program(w, maximum_episode_steps=12, noise=0.05, response_time_seconds=0.04, action_history=4,
-                        action_delay_steps=1, min_height_fraction=0.995, max_tilt=0.04, contact_groups=groups)
+                        action_delay_steps=1, min_height_fraction=0.995, max_tilt=0.04, contact_groups=groups,
+                        observation_history=3 if contacts else 1)
         w.set_task(prog)
-        assert w.observation_count == len(prog.actor)
+        assert w.observation_count == len(prog.actor) * prog.observation_history
         o = _oracle(w, prog)
         if contacts:
             o = TaskOracle(prog, nq=w.nq, nv=w.nv, dt=DT, seed=w.seed, fixed_root=False, limit_lower=o.lo, limit_upper=o.hi,
