@@ -916,6 +916,9 @@ typedef struct MRTaskProgramC {
     uint32_t action_count;          /* equals the world's action count */
     const MRTaskObservationOperatorC* actor;
     uint32_t actor_count;
+    const MRTaskObservationOperatorC* critic;  /* the critic's frame (program.counts0.z): clean values, no
+                                                  noise; 0 operators: the critic reads the actor history */
+    uint32_t critic_count;
     const MRTaskRewardOperatorC* rewards;
     uint32_t reward_count;
     const MRTaskTerminationOperatorC* terminations;

@@ -56,15 +56,16 @@ __device__ __forceinline__ float normal_draw(unsigned long long key, int action)
 
 // Observation feature i of the tile's environment e into x (normalised).
 __device__ __forceinline__ void load_observation(const PolicyParams& p, const float* mean, const float* inv_std, int env0,
-                                                 float* x) {
-    const int nobs = p.frame ? p.frame_count : p.nq + p.nv;
+                                                 float* x, bool critic = false) {
+    const float* frame = critic && p.critic_frame ? p.critic_frame : p.frame;
+    const int nobs = critic && p.critic_frame ? p.critic_frame_count : (p.frame ? p.frame_count : p.nq + p.nv);
     for (int idx = threadIdx.x; idx < kPolicyTile * nobs; idx += blockDim.x) {
         const int e = idx / nobs, i = idx - e * nobs;
         const int env = env0 + e;
         float value = 0.0f;
         if (env < p.envs) {
-            if (p.frame)
-                value = p.frame[static_cast<size_t>(env) * nobs + i];
+            if (frame)
+                value = frame[static_cast<size_t>(env) * nobs + i];
             else
                 value = i < p.nq ? p.q[static_cast<size_t>(env) * p.nq + i] : p.v[static_cast<size_t>(env) * p.nv + (i - p.nq)];
             if (mean) value = fminf(fmaxf((value - mean[i]) * inv_std[i], -p.obs_clip), p.obs_clip);
@@ -159,7 +160,7 @@ __global__ void __launch_bounds__(kThreads) policy_kernel(PolicyParams p) {
         return;
     }
     __syncthreads();
-    load_observation(p, p.critic_mean, p.critic_inv_std, env0, a);
+    load_observation(p, p.critic_mean, p.critic_inv_std, env0, a, true);
     const float* value = forward(p.critic, p.critic_layers, a, b);
     if (e < kPolicyTile && env0 + e < p.envs) p.values[env0 + e] = value[e * kPolicyMaxWidth];
 }

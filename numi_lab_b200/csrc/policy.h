@@ -37,6 +37,8 @@ struct PolicyParams {
     const float* v;
     const float* frame;
     std::int32_t frame_count;
+    const float* critic_frame;  // the critic's own frames ([env][critic_frame_count]), or null: it reads `frame`
+    std::int32_t critic_frame_count;
     std::int32_t nq, nv, envs, na;
     // Outputs of this control step (per env), any of them null to skip.
     float* actions;    // [env][na]: fed to the control step

@@ -474,7 +474,7 @@ struct MRTaskRolloutHandle {
     // transitions ([step][env]) of the last advance.
     std::unique_ptr<InstalledTask> task;
     DeviceBuffer<numi::TaskEnvState> d_task_state;
-    DeviceBuffer<float> d_task_history, d_task_previous, d_task_frame, d_task_targets, d_task_air;
+    DeviceBuffer<float> d_task_history, d_task_previous, d_task_frame, d_task_critic, d_task_targets, d_task_air;
     DeviceBuffer<std::uint32_t> d_task_masks;
     DeviceBuffer<MRTaskTransitionC> d_transitions;
     PinnedBuffer<MRTaskTransitionC> h_transitions;
@@ -789,6 +789,7 @@ struct MRTaskRolloutHandle {
         t.action_history = d_task_history.ptr + static_cast<size_t>(o) * P.history * P.na;
         t.previous_joint = d_task_previous.ptr + static_cast<size_t>(o) * 2 * P.na;
         t.frame = d_task_frame.ptr + static_cast<size_t>(o) * P.frames * P.nobs;
+        t.critic_frame = P.ncritic ? d_task_critic.ptr + static_cast<size_t>(o) * P.ncritic : nullptr;
         t.reset_q = d_reset_q.ptr + static_cast<size_t>(o) * P.nq;
         t.reset_v = d_reset_v.ptr + static_cast<size_t>(o) * P.nv;
         t.q = d_q.ptr + static_cast<size_t>(o) * P.nq;
@@ -845,6 +846,8 @@ struct MRTaskRolloutHandle {
         pp.v = d_v.ptr + static_cast<size_t>(o) * pp.nv;
         pp.frame = task ? d_task_frame.ptr + static_cast<size_t>(o) * task->prog.frames * task->prog.nobs : nullptr;
         pp.frame_count = task ? task->prog.frames * task->prog.nobs : 0;
+        pp.critic_frame = task && task->prog.ncritic ? d_task_critic.ptr + static_cast<size_t>(o) * task->prog.ncritic : nullptr;
+        pp.critic_frame_count = task ? task->prog.ncritic : 0;
         pp.envs = static_cast<int>(n);
         pp.env_base = static_cast<int>(o);
         pp.na = static_cast<int>(model.world.action_count);
@@ -1179,8 +1182,10 @@ std::unique_ptr<InstalledPolicy> compile_policy(const MRTaskRolloutHandle& h, co
     if (optional(pk.observation_inverse_standard_deviation, pk.observation_inverse_standard_deviation_count, nobs,
                  "observation_inverse_standard_deviation") != norm)
         throw std::invalid_argument("observation mean and inverse standard deviation go together");
-    const bool cnorm = optional(pk.critic_observation_mean, pk.critic_observation_mean_count, nobs, "critic_observation_mean");
-    if (optional(pk.critic_observation_inverse_standard_deviation, pk.critic_observation_inverse_standard_deviation_count, nobs,
+    // The critic reads the task's critic frame when the task has critic operators.
+    const std::uint32_t ncrit = h.task && h.task->prog.ncritic ? static_cast<std::uint32_t>(h.task->prog.ncritic) : nobs;
+    const bool cnorm = optional(pk.critic_observation_mean, pk.critic_observation_mean_count, ncrit, "critic_observation_mean");
+    if (optional(pk.critic_observation_inverse_standard_deviation, pk.critic_observation_inverse_standard_deviation_count, ncrit,
                  "critic_observation_inverse_standard_deviation") != cnorm)
         throw std::invalid_argument("critic observation mean and inverse standard deviation go together");
     if ((norm || cnorm) && !(pk.observation_clip > 0.0f)) throw std::invalid_argument("observation_clip must be positive");
@@ -1188,8 +1193,8 @@ std::unique_ptr<InstalledPolicy> compile_policy(const MRTaskRolloutHandle& h, co
                                      "action_log_standard_deviation");
     const bool has_bias = optional(pk.action_bias, pk.action_bias_count, na, "action_bias");
     const bool has_scale = optional(pk.action_scale, pk.action_scale_count, na, "action_scale");
-    auto check_chain = [&](const MRPolicyDenseLayerC* L, size_t n, std::uint32_t out, const char* net) {
-        std::uint32_t in = nobs;
+    auto check_chain = [&](const MRPolicyDenseLayerC* L, size_t n, std::uint32_t out, const char* net, std::uint32_t inputs) {
+        std::uint32_t in = inputs;
         for (size_t l = 0; l < n; ++l) {
             const MRPolicyDenseLayerC& d = L[l];
             const std::string where = std::string(net) + " layer " + std::to_string(l);
@@ -1205,8 +1210,8 @@ std::unique_ptr<InstalledPolicy> compile_policy(const MRTaskRolloutHandle& h, co
         }
         if (in != out) throw std::invalid_argument(std::string(net) + " must end in " + std::to_string(out) + " outputs");
     };
-    check_chain(pk.layers, pk.layer_count, na, "actor");
-    if (pk.critic_layer_count) check_chain(pk.critic_layers, pk.critic_layer_count, 1u, "critic");
+    check_chain(pk.layers, pk.layer_count, na, "actor", nobs);
+    if (pk.critic_layer_count) check_chain(pk.critic_layers, pk.critic_layer_count, 1u, "critic", ncrit);
 
     // Arena: per layer [in][out] weights then bias; then the vectors.
     std::vector<float> arena;
@@ -1230,8 +1235,8 @@ std::unique_ptr<InstalledPolicy> compile_policy(const MRTaskRolloutHandle& h, co
     put_layers(pk.layers, pk.layer_count, w_at, b_at);
     put_layers(pk.critic_layers, pk.critic_layer_count, cw_at, cb_at);
     const size_t mean_at = norm ? put(pk.observation_mean, nobs, 0.0f) : 0, inv_at = norm ? put(pk.observation_inverse_standard_deviation, nobs, 0.0f) : 0;
-    const size_t cmean_at = cnorm ? put(pk.critic_observation_mean, nobs, 0.0f) : 0,
-                 cinv_at = cnorm ? put(pk.critic_observation_inverse_standard_deviation, nobs, 0.0f) : 0;
+    const size_t cmean_at = cnorm ? put(pk.critic_observation_mean, ncrit, 0.0f) : 0,
+                 cinv_at = cnorm ? put(pk.critic_observation_inverse_standard_deviation, ncrit, 0.0f) : 0;
     const size_t ls_at = stochastic ? put(pk.action_log_standard_deviation, na, 0.0f) : 0;
     const size_t ab_at = put(has_bias ? pk.action_bias : nullptr, na, 0.0f);
     const size_t as_at = put(has_scale ? pk.action_scale : nullptr, na, 1.0f);
@@ -1321,9 +1326,12 @@ std::unique_ptr<InstalledTask> compile_task(const MRTaskRolloutHandle& h, const 
              where + ": scale and target bounds must be finite with lower <= upper");
         need(finite_value(b.response_time_seconds) && b.response_time_seconds >= 0.0f, where + ": response time must be >= 0");
     }
-    for (std::uint32_t i = 0; i < t.actor_count; ++i) {
-        const MRTaskObservationOperatorC& o = t.actor[i];
-        const std::string where = "actor operator " + to_string(i);
+    need(t.critic_count == 0 || t.critic != nullptr, "critic is null");
+    need(t.critic_count <= static_cast<std::uint32_t>(numi::kTaskMaxObservations), "at most 256 critic operators");
+    for (std::uint32_t i = 0; i < t.actor_count + t.critic_count; ++i) {
+        const bool actor_op = i < t.actor_count;
+        const MRTaskObservationOperatorC& o = actor_op ? t.actor[i] : t.critic[i - t.actor_count];
+        const std::string where = (actor_op ? "actor operator " : "critic operator ") + to_string(actor_op ? i : i - t.actor_count);
         need(finite_value(o.transform_scale) && finite_value(o.transform_offset) && finite_value(o.noise_amplitude) &&
                  o.noise_amplitude >= 0.0f, where + ": transform and noise must be finite");
         need((o.flags & ~static_cast<std::uint32_t>(MR_TASK_OBSERVATION_NORMALIZE_VECTOR3)) == 0u &&
@@ -1477,6 +1485,7 @@ std::unique_ptr<InstalledTask> compile_task(const MRTaskRolloutHandle& h, const 
     const std::uint32_t nterm = terminations ? t.termination_count : 0u;
     const size_t at_actions = put(t.actions, na * sizeof(MRTaskActionBindingC));
     const size_t at_actor = put(t.actor, t.actor_count * sizeof(MRTaskObservationOperatorC));
+    const size_t at_critic = put(t.critic, t.critic_count * sizeof(MRTaskObservationOperatorC));
     const size_t at_rewards = put(t.rewards, t.reward_count * sizeof(MRTaskRewardOperatorC));
     const size_t at_terms = put(t.terminations, nterm * sizeof(MRTaskTerminationOperatorC));
     const size_t at_random = put(t.randomization, t.randomization_count * sizeof(MRTaskRandomizationOperatorC));
@@ -1494,6 +1503,8 @@ std::unique_ptr<InstalledTask> compile_task(const MRTaskRolloutHandle& h, const 
     numi::TaskProgramDevice& P = out->prog;
     P.actions = reinterpret_cast<const MRTaskActionBindingC*>(base + at_actions);
     P.actor = reinterpret_cast<const MRTaskObservationOperatorC*>(base + at_actor);
+    P.critic = reinterpret_cast<const MRTaskObservationOperatorC*>(base + at_critic);
+    P.ncritic = static_cast<int>(t.critic_count);
     P.rewards = reinterpret_cast<const MRTaskRewardOperatorC*>(base + at_rewards);
     P.terminations = reinterpret_cast<const MRTaskTerminationOperatorC*>(base + at_terms);
     P.randomization = reinterpret_cast<const MRTaskRandomizationOperatorC*>(base + at_random);
@@ -1605,6 +1616,11 @@ MR_API int mr_task_rollout_set_task(MRTaskRolloutHandle* handle, const MRTaskPro
         std::unique_ptr<InstalledTask> compiled = compile_task(h, *program);
         if (h.policy) {
             const int in = h.policy->params.actor[0].in;
+            const int cin = h.policy->params.critic_layers ? h.policy->params.critic[0].in : 0;
+            const int cwant = compiled->prog.ncritic ? compiled->prog.ncritic : compiled->prog.frames * compiled->prog.nobs;
+            if (cin != 0 && cin != cwant)
+                throw std::invalid_argument("the installed policy's critic takes " + std::to_string(cin) + " observations; the task's critic frame has " +
+                                            std::to_string(cwant) + " (clear the policy first)");
             if (in != compiled->prog.frames * compiled->prog.nobs)
                 throw std::invalid_argument("the installed policy takes " + std::to_string(in) + " observations; the task's actor history has " +
                                             std::to_string(compiled->prog.frames * compiled->prog.nobs) + " (clear the policy first)");
@@ -1615,6 +1631,7 @@ MR_API int mr_task_rollout_set_task(MRTaskRolloutHandle* handle, const MRTaskPro
         h.d_task_history.resize(static_cast<size_t>(h.envs) * P.history * P.na);
         h.d_task_previous.resize(static_cast<size_t>(h.envs) * 2 * P.na);
         h.d_task_frame.resize(static_cast<size_t>(h.envs) * P.frames * P.nobs);
+        if (P.ncritic) h.d_task_critic.resize(static_cast<size_t>(h.envs) * P.ncritic);
         h.d_task_targets.resize(static_cast<size_t>(h.envs) * P.na);
         h.d_task_air.resize(static_cast<size_t>(h.envs) * numi::kTaskMaxGroups);
         check(cudaMemsetAsync(h.d_task_history.ptr, 0, h.d_task_history.count * sizeof(float), h.stream), "clear task history");
@@ -1622,7 +1639,7 @@ MR_API int mr_task_rollout_set_task(MRTaskRolloutHandle* handle, const MRTaskPro
         h.task = std::move(compiled);
         h.clear_task_state();
         h.stats_layout.actor_observation_count = static_cast<std::uint32_t>(P.frames * P.nobs);
-        h.stats_layout.critic_observation_count = static_cast<std::uint32_t>(P.frames * P.nobs);
+        h.stats_layout.critic_observation_count = static_cast<std::uint32_t>(P.ncritic ? P.ncritic : P.frames * P.nobs);
         h.stats_layout.maximum_episode_steps = static_cast<std::uint32_t>(P.max_episode_steps);
         h.stats_layout.task_fingerprint = h.task->fingerprint;
         h.last_steps = 0;

@@ -215,6 +215,14 @@ __device__ void write_frame(const TaskProgramDevice& P, const float* q, const fl
     }
 }
 
+// The critic's frame (writeCriticFrame, :1403-1456): clean values, lanes
+// over operators.
+__device__ void write_critic(const TaskProgramDevice& P, const float* q, const float* v, const TaskEnvState& st, const float* raw,
+                             const float* previous_q, const float* metrics, float* out, int lane) {
+    const Root r = root_frame(P, q, v);
+    for (int i = lane; i < P.ncritic; i += 32) out[i] = clean_observation(P, P.critic[i], r, q, v, st, raw, previous_q, metrics);
+}
+
 // durationSteps (:1484-1508).
 __device__ __forceinline__ unsigned duration_steps(const TaskProgramDevice& P, unsigned env, unsigned episode, unsigned step,
                                                    unsigned channel) {
@@ -502,6 +510,9 @@ __global__ void __launch_bounds__(32 * kTaskWarps) task_observe_kernel(TaskParam
         // Every delay-line slot is zero here; the newest raw slot stands for
         // all of them.
         write_frame(P, rq, rv, st, hist + (P.history - 2) * P.na, prev + P.na, nullptr, env, episode, 0u, frame, lane);
+        if (P.ncritic > 0)
+            write_critic(P, rq, rv, st, hist + (P.history - 2) * P.na, prev + P.na, nullptr,
+                         p.critic_frame + static_cast<size_t>(local) * P.ncritic, lane);
         __syncwarp();
         for (int i = lane; i < (P.frames - 1) * P.nobs; i += 32) frame[P.nobs + i] = frame[i % P.nobs];  // every slot the reset frame
         if (lane == 0) p.state[local] = st;
@@ -824,6 +835,9 @@ __global__ void __launch_bounds__(32 * kTaskWarps) task_complete_kernel(TaskPara
         }
         write_frame(P, q, v, st, hist + raw_last * P.na, prev + P.na, gm, env, st.episode, episode_steps,
                     frame + (P.frames - 1) * P.nobs, lane);
+        if (P.ncritic > 0)
+            write_critic(P, q, v, st, hist + raw_last * P.na, prev + P.na, gm, p.critic_frame + static_cast<size_t>(local) * P.ncritic,
+                         lane);
         __syncwarp();
         for (int a = lane; a < P.na; a += 32) {
             const MRTaskActionBindingC b = P.actions[a];

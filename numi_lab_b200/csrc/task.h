@@ -43,6 +43,7 @@ static_assert(sizeof(TaskEnvState) == 64, "task state layout");
 struct TaskProgramDevice {
     const MRTaskActionBindingC* actions;
     const MRTaskObservationOperatorC* actor;
+    const MRTaskObservationOperatorC* critic;
     const MRTaskRewardOperatorC* rewards;
     const MRTaskTerminationOperatorC* terminations;
     const MRTaskRandomizationOperatorC* randomization;
@@ -59,6 +60,7 @@ struct TaskProgramDevice {
     std::int32_t na, nobs, nrewards, nterminations, nrandom, ngroups;
     std::int32_t history, delay, max_episode_steps, nq, nv;
     std::int32_t frames;       // actor frames stacked in an observation (oldest first)
+    std::int32_t ncritic;      // critic operators (0: the critic reads the actor history)
     std::int32_t fixed_root;   // the root is welded to the world: root sources read zero
     float dt;                  // control step, seconds
     float base_height, gait_period, standing_probability, duration_min, duration_max;
@@ -75,6 +77,7 @@ struct TaskParams {
     float* action_history;         // [env][history][na]: raw slots 0..history-2, filter slot history-1
     float* previous_joint;         // [env][2][na]: joint velocity, joint position at the last step's end
     float* frame;                  // [env][frames][nobs]: the actor history of the next decision, oldest first
+    float* critic_frame;           // [env][ncritic]: the critic's frame of the next decision
     float* reset_q;                // [env][nq]
     float* reset_v;                // [env][nv]
     const float* q;                // [env][nq]

@@ -400,6 +400,8 @@ class TaskProgramC(ct.Structure):
         ("action_count", ct.c_uint32),
         ("actor", ct.POINTER(TaskObservationOperatorC)),
         ("actor_count", ct.c_uint32),
+        ("critic", ct.POINTER(TaskObservationOperatorC)),
+        ("critic_count", ct.c_uint32),
         ("rewards", ct.POINTER(TaskRewardOperatorC)),
         ("reward_count", ct.c_uint32),
         ("terminations", ct.POINTER(TaskTerminationOperatorC)),

@@ -113,6 +113,7 @@ class TaskProgram:
     actions: list[ActionBinding]
     actor: list[Observation]
     default_q: np.ndarray
+    critic: list[Observation] = field(default_factory=list)  # the critic's own clean frame (empty: the actor history)
     rewards: list[Reward] = field(default_factory=list)
     terminations: list[Termination] = field(default_factory=list)
     randomization: list[Randomization] = field(default_factory=list)
@@ -169,6 +170,7 @@ def task_program_c(program: TaskProgram) -> tuple[native.TaskProgramC, list[Any]
     p = native.TaskProgramC()
     p.actions, p.action_count = table(native.TaskActionBindingC, program.actions, fill_action)
     p.actor, p.actor_count = table(native.TaskObservationOperatorC, program.actor, fill_obs)
+    p.critic, p.critic_count = table(native.TaskObservationOperatorC, program.critic, fill_obs)
     p.rewards, p.reward_count = table(native.TaskRewardOperatorC, program.rewards, fill_reward)
     p.terminations, p.termination_count = table(native.TaskTerminationOperatorC, program.terminations, fill_term)
     p.randomization, p.randomization_count = table(native.TaskRandomizationOperatorC, program.randomization, fill_random)

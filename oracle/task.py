@@ -136,6 +136,7 @@ class EnvState:
     episode_return: float = 0.0
     episode_tracking: float = 0.0
     air: np.ndarray = field(default_factory=lambda: np.zeros(8))
+    critic: np.ndarray = field(default_factory=lambda: np.zeros(0))
 
 
 class TaskOracle:
@@ -331,6 +332,11 @@ class TaskOracle:
                     self.seed, env, episode, step, op.noise_channel)
         return out
 
+    def critic_frame(self, q, v, st: EnvState, raw_slot: int, previous_q, metrics=None) -> np.ndarray:
+        """writeCriticFrame (:1403-1456): the critic operators' clean values."""
+
+        return np.array([self.clean(op, q, v, st, raw_slot, previous_q, metrics) for op in getattr(self.p, "critic", [])])
+
     def duration_steps(self, env, episode, step, channel) -> int:
         lo, hi = self.p.command_duration_seconds
         return max(1, int(math.floor(range_draw(self.seed, env, episode, step, channel, lo, hi) / self.dt)))
@@ -389,6 +395,7 @@ class TaskOracle:
         st.previous_height = self.root(rq, rv)[1][2]
         st.episode_return = st.episode_tracking = 0.0
         first = self.frame(env, rq, rv, st, self.L - 2, st.previous_joint[1], episode, 0)
+        st.critic = self.critic_frame(rq, rv, st, self.L - 2, st.previous_joint[1])
         st.frame = np.tile(first, (self.H, 1))  # every history slot the reset frame (:3072-3098)
         return True, rq, rv, st.frame.reshape(-1).copy()
 
@@ -570,6 +577,7 @@ class TaskOracle:
         st.episode_tracking = 0.0 if done else episode_tracking
         if not done or (timeout and not physics_error):
             st.frame = np.vstack([st.frame[1:], self.frame(env, q, v, st, raw_last, st.previous_joint[1], st.episode, steps, gm)[None]])
+            st.critic = self.critic_frame(q, v, st, raw_last, st.previous_joint[1], gm)
             for a, b in enumerate(p.actions):
                 st.previous_joint[0, a] = v[b.v_index]
                 st.previous_joint[1, a] = q[b.q_index]

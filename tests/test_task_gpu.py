@@ -68,10 +68,10 @@ def test_task_layer_matches_oracle_step_by_step(cuda_device, contacts):
         # Tight height and tilt limits: episodes end by timeout, height and
         # tilt within the run.
         groups = T.foot_contact_groups(w.model()) if contacts else None
-        # The contact variant also stacks three actor frames.
+        # The contact variant also stacks two actor frames.
         prog = _program(w, maximum_episode_steps=12, noise=0.05, response_time_seconds=0.04, action_history=4,
                         action_delay_steps=1, min_height_fraction=0.995, max_tilt=0.04, contact_groups=groups,
-                        observation_history=3 if contacts else 1)
+                        observation_history=2 if contacts else 1)
         w.set_task(prog)
         assert w.observation_count == len(prog.actor) * prog.observation_history
         o = _oracle(w, prog)
@@ -204,6 +204,46 @@ def test_policy_reads_the_actor_frames(cuda_device):
             if ref_info is not None:
                 np.testing.assert_array_equal(ref_params, params)
                 assert ref_info["transition_count"] == envs * steps
+
+
+def test_critic_reads_its_own_frame(cuda_device):
+    """A task with critic operators (privileged, noise-free: root height,
+    linear velocity, joint velocities, command): the policy's critic values
+    equal the critic network on the oracle's critic frames."""
+
+    import torch
+
+    from oracle import policy as ref
+
+    rng = np.random.default_rng(6)
+    envs, steps = 16, 3
+    with nb.World("tree29", envs, substeps=4, velocity_iterations=8, control_dt=DT, seed=SEED) as w:
+        prog = _program(w, noise=0.02)
+        prog.critic = ([T.Observation(T.OBSERVE["root_height"])] +
+                       [T.Observation(T.OBSERVE["root_linear_velocity_local"], 0, c) for c in range(3)] +
+                       [T.Observation(T.OBSERVE["joint_velocity"], a) for a in range(w.action_count)] +
+                       [T.Observation(T.OBSERVE["command"], 0, c) for c in range(3)])
+        w.set_task(prog)
+        nobs, ncrit, na = w.observation_count, len(prog.critic), w.action_count
+        assert int(w.layout().critic_observation_count) == ncrit
+        dense = lambda sizes, acts: [(rng.normal(0.0, 1.0 / np.sqrt(a), (b, a)).astype(np.float32),  # noqa: E731
+                                      rng.normal(0.0, 0.1, b).astype(np.float32), f) for (a, b), f in zip(zip(sizes[:-1], sizes[1:]), acts)]
+        critic = dense([ncrit, 32, 1], ["tanh", "identity"])
+        w.set_policy(layers=dense([nobs, 64, na], ["elu", "identity"]), critic_layers=critic, revision=5, action_clip=1.0)
+        o = _oracle(w, prog)
+        states = [o.new_state() for _ in range(envs)]
+        for k in range(steps):
+            obs, status = w.step_policy(1)
+            out = w.policy_outputs()
+            q, v, _ = w.state()
+            tr = w.transitions(1)
+            for e in range(envs):
+                o.observe(e, states[e], None, None, False)
+                want = ref.forward(states[e].critic[None], critic)[0, 0]
+                assert abs(float(out["values"][0, e]) - want) <= 1e-4, (k, e)
+                o.apply(states[e], out["latents"][0, e].clip(-1.0, 1.0))
+                o.complete(e, states[e], q[e].astype(np.float64), v[e].astype(np.float64), int(status[0, e]))
+        del tr
 
 
 def test_installer_refuses_programs_outside_the_subset(cuda_device):
