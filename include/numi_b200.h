@@ -810,6 +810,8 @@ enum {
     MR_TASK_RANDOMIZE_ROOT_YAW = 1u,
     MR_TASK_RANDOMIZE_ACTION_POSITION = 2u,
     MR_TASK_RANDOMIZE_VELOCITY = 3u,
+    MR_TASK_RANDOMIZE_ACTION_DELAY = 7u,
+    MR_TASK_RANDOMIZE_OBSERVATION_DELAY = 8u,
     MR_TASK_RANDOMIZE_ACTION_VELOCITY = 9u,
     MR_TASK_RANDOMIZE_ROOT_HEIGHT = 10u,
     MR_TASK_RANDOMIZE_JOINT_POSITION = 12u
@@ -939,8 +941,10 @@ typedef struct MRTaskProgramC {
     uint32_t default_q_count;
     uint32_t maximum_episode_steps; /* timeout */
     uint32_t action_history;        /* delay-line slots including the filter slot, 3..8 */
-    uint32_t action_delay_steps;    /* raw actions of delay; at most action_history - 2 take effect */
+    uint32_t action_delay_steps;    /* an episode's action delay without an ACTION_DELAY operator;
+                                       at most action_history - 2 take effect */
     uint32_t observation_history;   /* actor frames stacked, oldest first (program.layout.y), 1..8 */
+    uint32_t maximum_observation_delay; /* program.schedule.y: the OBSERVATION_DELAY draw's ceiling */
     float base_height_target;       /* program.locomotion.x */
     float gait_period_seconds;      /* program.locomotion.y */
     float root_reference[3];        /* root link origin from the root's q position, root axes */

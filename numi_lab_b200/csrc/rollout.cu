@@ -1463,6 +1463,8 @@ std::unique_ptr<InstalledTask> compile_task(const MRTaskRolloutHandle& h, const 
         case MR_TASK_RANDOMIZE_ACTION_POSITION:
         case MR_TASK_RANDOMIZE_VELOCITY:
         case MR_TASK_RANDOMIZE_ACTION_VELOCITY:
+        case MR_TASK_RANDOMIZE_ACTION_DELAY:
+        case MR_TASK_RANDOMIZE_OBSERVATION_DELAY:
             break;
         default:
             need(false, where + ": opcode " + to_string(o.opcode) + " is outside the evaluated subset");
@@ -1534,6 +1536,7 @@ std::unique_ptr<InstalledTask> compile_task(const MRTaskRolloutHandle& h, const 
     P.ngroups = static_cast<int>(t.joint_group_count);
     P.history = static_cast<int>(t.action_history);
     P.frames = static_cast<int>(t.observation_history);
+    P.max_observation_delay = static_cast<int>(std::min<std::uint32_t>(t.maximum_observation_delay, 8u));
     P.delay = static_cast<int>(std::min<std::uint32_t>(t.action_delay_steps, t.action_history - 2));
     P.max_episode_steps = static_cast<int>(t.maximum_episode_steps);
     P.nq = static_cast<int>(nq);

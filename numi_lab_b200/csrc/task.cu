@@ -439,6 +439,8 @@ __global__ void __launch_bounds__(32 * kTaskWarps) task_observe_kernel(TaskParam
         for (int i = lane; i < P.nq; i += 32) rq[i] = P.default_q[i];
         for (int i = lane; i < P.nv; i += 32) rv[i] = 0.0f;
         __syncwarp();
+        st.action_delay = static_cast<unsigned>(P.delay);
+        st.observation_delay = 0u;
         // Randomization operators in order (:2452-2770), channel 2048 + index.
         for (int k = 0; k < P.nrandom; ++k) {
             const MRTaskRandomizationOperatorC op = P.randomization[k];
@@ -477,6 +479,19 @@ __global__ void __launch_bounds__(32 * kTaskWarps) task_observe_kernel(TaskParam
                 for (int i = lane; i < P.nv; i += 32)
                     rv[i] = range_draw(P.seed, env, episode, 0u, channel + i, op.parameters[0], op.parameters[1]);
                 break;
+            case MR_TASK_RANDOMIZE_ACTION_DELAY:
+            case MR_TASK_RANDOMIZE_OBSERVATION_DELAY: {
+                // An integer in [lower, upper] (:2738-2783), capped.
+                const unsigned lo = static_cast<unsigned>(fmaxf(op.parameters[0], 0.0f));
+                const unsigned hi = static_cast<unsigned>(fmaxf(op.parameters[1], op.parameters[0]));
+                const unsigned d = lo + static_cast<unsigned>(floorf(static_cast<float>(hi - lo + 1u) *
+                                                                     unit_draw(P.seed, env, episode, 0u, channel)));
+                if (op.opcode == MR_TASK_RANDOMIZE_ACTION_DELAY)
+                    st.action_delay = min(d, static_cast<unsigned>(P.history - 1));
+                else
+                    st.observation_delay = min(d, static_cast<unsigned>(P.max_observation_delay));
+                break;
+            }
             case MR_TASK_RANDOMIZE_ACTION_VELOCITY:
                 for (int a = lane; a < P.na; a += 32)
                     rv[P.actions[a].v_index] = range_draw(P.seed, env, episode, 0u, channel + a, op.parameters[0], op.parameters[1]);
@@ -541,7 +556,7 @@ __global__ void __launch_bounds__(kApplyThreads) task_apply_kernel(TaskParams p)
                                ? fminf(fmaxf(1.0f - expf(-P.dt / b.response_time_seconds), 0.0f), 1.0f)
                                : 1.0f;
     hist[raw_last * P.na + a] = requested;
-    const int selected = raw_last - min(P.delay, raw_last);
+    const int selected = raw_last - min(static_cast<int>(p.state[local].action_delay), raw_last);
     const float filtered = mixf(previous, hist[selected * P.na + a], response);
     hist[filter * P.na + a] = filtered;
     const float target = P.default_q[b.q_index] + b.scale * filtered;
@@ -835,6 +850,11 @@ __global__ void __launch_bounds__(32 * kTaskWarps) task_complete_kernel(TaskPara
         }
         write_frame(P, q, v, st, hist + raw_last * P.na, prev + P.na, gm, env, st.episode, episode_steps,
                     frame + (P.frames - 1) * P.nobs, lane);
+        if (st.observation_delay != 0u && P.frames > 1) {  // the newest slot shows an older frame (:6549-6565)
+            __syncwarp();
+            const int src = P.frames - 1 - min(static_cast<int>(st.observation_delay), P.frames - 1);
+            for (int i = lane; i < P.nobs; i += 32) frame[(P.frames - 1) * P.nobs + i] = frame[src * P.nobs + i];
+        }
         if (P.ncritic > 0)
             write_critic(P, q, v, st, hist + raw_last * P.na, prev + P.na, gm, p.critic_frame + static_cast<size_t>(local) * P.ncritic,
                          lane);

@@ -29,7 +29,8 @@ struct alignas(16) TaskEnvState {
     std::uint32_t initialized;
     std::uint32_t pending_reset; // the last step ended the episode
     std::uint32_t last_reason;
-    std::uint32_t reserved[2];
+    std::uint32_t action_delay;       // raw actions of delay this episode
+    std::uint32_t observation_delay;  // frames of delay this episode
     float command[3];            // x, y velocity and yaw rate
     float phase;                 // gait phase in [0, 2 pi)
     float previous_height;       // root height at the last step's end
@@ -60,6 +61,7 @@ struct TaskProgramDevice {
     std::int32_t na, nobs, nrewards, nterminations, nrandom, ngroups;
     std::int32_t history, delay, max_episode_steps, nq, nv;
     std::int32_t frames;       // actor frames stacked in an observation (oldest first)
+    std::int32_t max_observation_delay;
     std::int32_t ncritic;      // critic operators (0: the critic reads the actor history)
     std::int32_t fixed_root;   // the root is welded to the world: root sources read zero
     float dt;                  // control step, seconds

@@ -424,6 +424,7 @@ class TaskProgramC(ct.Structure):
         ("action_history", ct.c_uint32),
         ("action_delay_steps", ct.c_uint32),
         ("observation_history", ct.c_uint32),
+        ("maximum_observation_delay", ct.c_uint32),
         ("base_height_target", ct.c_float),
         ("gait_period_seconds", ct.c_float),
         ("root_reference", ct.c_float * 3),

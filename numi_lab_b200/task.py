@@ -44,8 +44,8 @@ CONTACT_SUPPORT, CONTACT_FORBIDDEN = 1, 2
 ALL_GROUPS = 0xFFFFFFFF
 REASON = {"continuing": 0, "height": 1, "tilt": 2, "contact": 3, "timeout": 4, "physics_error": 5}
 RANDOMIZE = {
-    "root_position": 0, "root_yaw": 1, "action_position": 2, "velocity": 3, "action_velocity": 9, "root_height": 10,
-    "joint_position": 12,
+    "root_position": 0, "root_yaw": 1, "action_position": 2, "velocity": 3, "action_delay": 7, "observation_delay": 8,
+    "action_velocity": 9, "root_height": 10, "joint_position": 12,
 }
 
 
@@ -125,6 +125,7 @@ class TaskProgram:
     action_history: int = 3
     action_delay_steps: int = 0
     observation_history: int = 1  # actor frames stacked per observation, oldest first
+    maximum_observation_delay: int = 0
     base_height_target: float = 0.0
     gait_period_seconds: float = 0.8
     root_reference: tuple[float, float, float] = (0.0, 0.0, 0.0)
@@ -213,6 +214,7 @@ def task_program_c(program: TaskProgram) -> tuple[native.TaskProgramC, list[Any]
     p.action_history = program.action_history
     p.action_delay_steps = program.action_delay_steps
     p.observation_history = program.observation_history
+    p.maximum_observation_delay = program.maximum_observation_delay
     p.base_height_target = program.base_height_target
     p.gait_period_seconds = program.gait_period_seconds
     p.root_reference[:] = list(program.root_reference)

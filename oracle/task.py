@@ -54,6 +54,7 @@ MANIFOLD_POINTS = 4
 REASON_CONTINUING, REASON_TIMEOUT, REASON_PHYSICS_ERROR = 0, 4, 5
 RND_ROOT_POSITION, RND_ROOT_YAW, RND_ACTION_POSITION, RND_VELOCITY = 0, 1, 2, 3
 RND_ACTION_VELOCITY, RND_ROOT_HEIGHT, RND_JOINT_POSITION = 9, 10, 12
+RND_ACTION_DELAY, RND_OBSERVATION_DELAY = 7, 8
 
 
 def mix64(x: int) -> int:
@@ -137,6 +138,8 @@ class EnvState:
     episode_tracking: float = 0.0
     air: np.ndarray = field(default_factory=lambda: np.zeros(8))
     critic: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    action_delay: int = 0
+    observation_delay: int = 0
 
 
 class TaskOracle:
@@ -357,6 +360,7 @@ class TaskOracle:
             return False, None, None, st.frame.reshape(-1).copy()
         episode = st.episode + 1
         rq = self.default_q.copy()
+        st.action_delay, st.observation_delay = self.delay, 0
         rv = np.zeros(self.nv)
         for k, op in enumerate(self.p.randomization):
             ch = 2048 + k
@@ -378,6 +382,14 @@ class TaskOracle:
             elif op.opcode == RND_VELOCITY:
                 for i in range(self.nv):
                     rv[i] = range_draw(self.seed, env, episode, 0, ch + i, a, b)
+            elif op.opcode in (RND_ACTION_DELAY, RND_OBSERVATION_DELAY):
+                lo_d = int(max(op.parameters[0], 0.0))
+                hi_d = int(max(op.parameters[1], op.parameters[0]))
+                d = lo_d + int(math.floor((hi_d - lo_d + 1) * unit_draw(self.seed, env, episode, 0, ch)))
+                if op.opcode == RND_ACTION_DELAY:
+                    st.action_delay = min(d, self.L - 1)
+                else:
+                    st.observation_delay = min(d, int(getattr(self.p, "maximum_observation_delay", 0)), 8)
             elif op.opcode == RND_ACTION_VELOCITY:
                 for i, bd in enumerate(self.p.actions):
                     rv[bd.v_index] = range_draw(self.seed, env, episode, 0, ch + i, a, b)
@@ -410,7 +422,7 @@ class TaskOracle:
             previous = st.history[filt, a]
             resp = min(max(1.0 - math.exp(-self.dt / b.response_time_seconds), 0.0), 1.0) if b.response_time_seconds > 0.0 else 1.0
             st.history[raw_last, a] = float(actions[a])
-            delayed = st.history[raw_last - min(self.delay, raw_last), a]
+            delayed = st.history[raw_last - min(st.action_delay, raw_last), a]
             st.history[filt, a] = previous + (delayed - previous) * resp
             targets[a] = min(max(self.default_q[b.q_index] + b.scale * st.history[filt, a], b.lower_target), b.upper_target)
         return targets
@@ -577,6 +589,8 @@ class TaskOracle:
         st.episode_tracking = 0.0 if done else episode_tracking
         if not done or (timeout and not physics_error):
             st.frame = np.vstack([st.frame[1:], self.frame(env, q, v, st, raw_last, st.previous_joint[1], st.episode, steps, gm)[None]])
+            if st.observation_delay and self.H > 1:
+                st.frame[-1] = st.frame[self.H - 1 - min(st.observation_delay, self.H - 1)]
             st.critic = self.critic_frame(q, v, st, raw_last, st.previous_joint[1], gm)
             for a, b in enumerate(p.actions):
                 st.previous_joint[0, a] = v[b.v_index]

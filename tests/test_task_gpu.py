@@ -72,6 +72,10 @@ def test_task_layer_matches_oracle_step_by_step(cuda_device, contacts):
         prog = _program(w, maximum_episode_steps=12, noise=0.05, response_time_seconds=0.04, action_history=4,
                         action_delay_steps=1, min_height_fraction=0.995, max_tilt=0.04, contact_groups=groups,
                         observation_history=2 if contacts else 1)
+        if contacts:  # per-episode action and observation delays too
+            prog.randomization += [T.Randomization(T.RANDOMIZE["action_delay"], (0.0, 2.0, 0.0, 0.0)),
+                                   T.Randomization(T.RANDOMIZE["observation_delay"], (0.0, 1.0, 0.0, 0.0))]
+            prog.maximum_observation_delay = 1
         w.set_task(prog)
         assert w.observation_count == len(prog.actor) * prog.observation_history
         o = _oracle(w, prog)

@@ -155,6 +155,7 @@ def test_delay_line_and_first_order_response(tree):
     prog = T.locomotion_task(rec, dq, response_time_seconds=tau, action_history=5, action_delay_steps=2)
     o = _oracle(prog, rec, lo, hi)
     st = o.new_state()
+    st.action_delay = o.delay  # a reset sets it (no ACTION_DELAY operator here)
     alpha = 1.0 - math.exp(-DT / tau)
     seq = [0.4, -0.2, 0.9, 0.1, 0.0]
     filt = 0.0
