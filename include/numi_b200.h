@@ -869,6 +869,8 @@ typedef struct MRTaskTerminationOperatorC {
     uint32_t group;      /* contact group of CONTACT_GROUP */
     float threshold;
     float failure_penalty;
+    uint32_t minimum_band;   /* active in episodes of bands [minimum_band, maximum_band] */
+    uint32_t maximum_band;   /* MR_INVALID_INDEX: the last band */
 } MRTaskTerminationOperatorC;
 
 /* reference: MRTaskRandomizationOperatorGPU (:515-520); `target` is the q
@@ -876,6 +878,8 @@ typedef struct MRTaskTerminationOperatorC {
 typedef struct MRTaskRandomizationOperatorC {
     uint32_t opcode;
     uint32_t target;
+    uint32_t minimum_band;   /* inactive in episodes of a lower difficulty band */
+    uint32_t reserved;
     float parameters[4];
 } MRTaskRandomizationOperatorC;
 
@@ -948,10 +952,15 @@ typedef struct MRTaskProgramC {
     float base_height_target;       /* program.locomotion.x */
     float gait_period_seconds;      /* program.locomotion.y */
     float root_reference[3];        /* root link origin from the root's q position, root axes */
-    float command_lower[3];         /* x, y velocity and yaw rate */
+    float command_lower[3];         /* x, y velocity and yaw rate, band 0 */
     float command_upper[3];
     float standing_probability;     /* a drawn command is zeroed with it */
     float command_duration_seconds[2];
+    uint32_t difficulty_band_count; /* program.schedule.z; an episode draws its band (0 for one band) */
+    float band_sampling_exponent;   /* band = floor(u^exponent x bands) over the configuration's band range */
+    float command_limit_lower[3];   /* each band widens the command range by command_band_step, within these limits */
+    float command_limit_upper[3];
+    float command_band_step[3];
     uint64_t task_fingerprint;
 } MRTaskProgramC;
 

@@ -1310,11 +1310,23 @@ std::unique_ptr<InstalledTask> compile_task(const MRTaskRolloutHandle& h, const 
     need(finite_value(t.standing_probability) && t.standing_probability >= 0.0f && t.standing_probability <= 1.0f,
          "standing_probability must lie in [0, 1]");
     need(finite_value(t.base_height_target), "base_height_target must be finite");
+    // One band at least, as the reference's pack validation asks
+    // (TaskProgram.cpp:855); the band range widens each command bound by
+    // its step per band, within limits that contain the band-0 range.
+    need(t.difficulty_band_count >= 1 && t.difficulty_band_count <= 1024u, "difficulty_band_count must be 1-1024");
+    need(finite_value(t.band_sampling_exponent) && t.band_sampling_exponent > 0.0f, "band_sampling_exponent must be positive");
     for (int k = 0; k < 3; ++k) {
         need(finite_value(t.command_lower[k]) && finite_value(t.command_upper[k]) && t.command_lower[k] <= t.command_upper[k],
              "command bounds must be finite with lower <= upper");
+        need(finite_value(t.command_limit_lower[k]) && finite_value(t.command_limit_upper[k]) &&
+                 t.command_limit_lower[k] <= t.command_lower[k] && t.command_upper[k] <= t.command_limit_upper[k],
+             "command limits must be finite and contain the command bounds");
+        need(finite_value(t.command_band_step[k]) && t.command_band_step[k] >= 0.0f, "command_band_step must be finite and >= 0");
         need(finite_value(t.root_reference[k]), "root_reference must be finite");
     }
+    if (h.config.override_difficulty_band_range != 0u)
+        need(h.config.minimum_difficulty_band <= h.config.maximum_difficulty_band,
+             "minimum_difficulty_band must not exceed maximum_difficulty_band");
     for (std::uint32_t a = 0; a < na; ++a) {
         const MRTaskActionBindingC& b = t.actions[a];
         const std::string where = "action " + to_string(a);
@@ -1445,6 +1457,8 @@ std::unique_ptr<InstalledTask> compile_task(const MRTaskRolloutHandle& h, const 
         need(o.opcode != MR_TASK_TERMINATE_CONTACT_GROUP || o.group < t.contact_group_count,
              "termination operator " + to_string(i) + ": group must be a contact group index");
         need(finite_value(o.threshold) && finite_value(o.failure_penalty), "termination operator " + to_string(i) + " must be finite");
+        need(o.maximum_band == MR_INVALID_INDEX || o.minimum_band <= o.maximum_band,
+             "termination operator " + to_string(i) + ": minimum_band must not exceed maximum_band");
     }
     need(t.randomization_count == 0 || t.randomization != nullptr, "randomization is null");
     for (std::uint32_t i = 0; i < t.randomization_count; ++i) {
@@ -1552,7 +1566,18 @@ std::unique_ptr<InstalledTask> compile_task(const MRTaskRolloutHandle& h, const 
         P.root_reference[k] = t.root_reference[k];
         P.command_lower[k] = t.command_lower[k];
         P.command_upper[k] = t.command_upper[k];
+        P.command_limit_lower[k] = t.command_limit_lower[k];
+        P.command_limit_upper[k] = t.command_limit_upper[k];
+        P.command_step[k] = t.command_band_step[k];
     }
+    // The sampled band range: the configuration's override, else every band
+    // (the dispatch's sampling lanes).
+    P.bands = static_cast<int>(t.difficulty_band_count);
+    P.band_exponent = t.band_sampling_exponent;
+    P.band_min = h.config.override_difficulty_band_range ? static_cast<int>(std::min<std::uint32_t>(h.config.minimum_difficulty_band, 1023u)) : 0;
+    P.band_max = h.config.override_difficulty_band_range && h.config.maximum_difficulty_band != MR_INVALID_INDEX
+                     ? static_cast<int>(std::min<std::uint32_t>(h.config.maximum_difficulty_band, 1023u))
+                     : -1;
     P.seed = h.seed;
     out->fingerprint = t.task_fingerprint;
     return out;

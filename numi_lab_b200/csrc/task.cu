@@ -231,10 +231,28 @@ __device__ __forceinline__ unsigned duration_steps(const TaskProgramDevice& P, u
     return steps >= 1.0f ? static_cast<unsigned>(steps) : 1u;
 }
 
-// sampledCommand (:1570-1615) at difficulty band 0.
-__device__ __forceinline__ void sample_command(const TaskProgramDevice& P, unsigned env, unsigned episode, unsigned step, float* out) {
-    for (unsigned k = 0; k < 3u; ++k)
-        out[k] = range_draw(P.seed, env, episode, step, 16u + k, P.command_lower[k], P.command_upper[k]);
+// sampledDifficultyBand (:1537-1568).
+__device__ __forceinline__ unsigned sample_band(const TaskProgramDevice& P, unsigned env, unsigned episode) {
+    const unsigned count = static_cast<unsigned>(max(P.bands, 1));
+    const unsigned lo = min(static_cast<unsigned>(P.band_min), count - 1u);
+    const unsigned req = P.band_max < 0 ? count - 1u : static_cast<unsigned>(P.band_max);
+    const unsigned hi = max(lo, min(req, count - 1u));
+    const unsigned n = hi - lo + 1u;
+    if (n == 1u) return lo;
+    const float u = powf(unit_draw(P.seed, env, episode, 0u, 15u), fmaxf(P.band_exponent, 0.01f));
+    return lo + min(static_cast<unsigned>(floorf(u * static_cast<float>(n))), n - 1u);
+}
+
+// sampledCommand (:1570-1615): each band widens the range by the step,
+// within the limits.
+__device__ __forceinline__ void sample_command(const TaskProgramDevice& P, unsigned env, unsigned episode, unsigned step, unsigned band,
+                                               float* out) {
+    const float b = static_cast<float>(band);
+    for (unsigned k = 0; k < 3u; ++k) {
+        const float lower = fmaxf(P.command_lower[k] - b * P.command_step[k], P.command_limit_lower[k]);
+        const float upper = fminf(P.command_upper[k] + b * P.command_step[k], P.command_limit_upper[k]);
+        out[k] = range_draw(P.seed, env, episode, step, 16u + k, lower, upper);
+    }
     if (unit_draw(P.seed, env, episode, step, 19u) < P.standing_probability) out[0] = out[1] = out[2] = 0.0f;
 }
 
@@ -441,10 +459,12 @@ __global__ void __launch_bounds__(32 * kTaskWarps) task_observe_kernel(TaskParam
         __syncwarp();
         st.action_delay = static_cast<unsigned>(P.delay);
         st.observation_delay = 0u;
+        st.band = sample_band(P, env, episode);
         // Randomization operators in order (:2452-2770), channel 2048 + index.
         for (int k = 0; k < P.nrandom; ++k) {
             const MRTaskRandomizationOperatorC op = P.randomization[k];
             const unsigned channel = 2048u + static_cast<unsigned>(k);
+            if (st.band < op.minimum_band) continue;
             switch (op.opcode) {
             case MR_TASK_RANDOMIZE_ROOT_POSITION:
                 if (lane < 3) rq[lane] += op.parameters[lane] * signed_draw(P.seed, env, episode, 0u, channel + lane);
@@ -516,7 +536,7 @@ __global__ void __launch_bounds__(32 * kTaskWarps) task_observe_kernel(TaskParam
         st.initialized = 1u;
         st.pending_reset = 0u;
         st.last_reason = MR_TASK_TERMINATION_CONTINUING;
-        sample_command(P, env, episode, 0u, st.command);
+        sample_command(P, env, episode, 0u, st.band, st.command);
         st.phase = 0.0f;
         st.previous_height = root_frame(P, rq, rv).position.z;
         st.episode_return = 0.0f;
@@ -790,6 +810,8 @@ __global__ void __launch_bounds__(32 * kTaskWarps) task_complete_kernel(TaskPara
     float penalty = 0.0f;
     for (int k = 0; k < P.nterminations; ++k) {
         const MRTaskTerminationOperatorC op = P.terminations[k];
+        const unsigned top = op.maximum_band == MR_INVALID_INDEX ? static_cast<unsigned>(max(P.bands, 1) - 1) : op.maximum_band;
+        if (st.band < op.minimum_band || st.band > top) continue;
         const bool triggered = op.opcode == MR_TASK_TERMINATE_MINIMUM_ROOT_HEIGHT ? height < op.threshold
                                : op.opcode == MR_TASK_TERMINATE_MAXIMUM_TILT        ? tilt > op.threshold
                                : op.opcode == MR_TASK_TERMINATE_CONTACT_GROUP
@@ -827,7 +849,7 @@ __global__ void __launch_bounds__(32 * kTaskWarps) task_complete_kernel(TaskPara
 
     // Command schedule and state (:6388-6440).
     if (!done && st.command_steps <= 1u) {
-        sample_command(P, env, st.episode, episode_steps, st.command);
+        sample_command(P, env, st.episode, episode_steps, st.band, st.command);
         st.command_steps = duration_steps(P, env, st.episode, episode_steps, 64u);
     } else if (!done) {
         --st.command_steps;
@@ -886,6 +908,7 @@ __global__ void __launch_bounds__(32 * kTaskWarps) task_complete_kernel(TaskPara
         t.contact_reward = b1[3];
         t.policy_revision = p.policy_revision;
         t.episode_tracking_score = done && !physics_error ? episode_score : 0.0f;
+        t.difficulty_band = st.band;
         p.transitions[local] = t;
     }
 }

@@ -37,8 +37,10 @@ struct alignas(16) TaskEnvState {
     float episode_return;
     float episode_tracking;      // sum of the linear tracking scores
     float reserved2;
+    std::uint32_t band;          // the episode's difficulty band
+    std::uint32_t reserved3[3];
 };
-static_assert(sizeof(TaskEnvState) == 64, "task state layout");
+static_assert(sizeof(TaskEnvState) == 80, "task state layout");
 
 // The installed program: tables in one device arena plus its constants.
 struct TaskProgramDevice {
@@ -68,6 +70,9 @@ struct TaskProgramDevice {
     float base_height, gait_period, standing_probability, duration_min, duration_max;
     float root_reference[3];
     float command_lower[3], command_upper[3];
+    float command_limit_lower[3], command_limit_upper[3], command_step[3];
+    std::int32_t bands, band_min, band_max;  // band count; the rollout's sampled band range
+    float band_exponent;
     unsigned long long seed;
 };
 

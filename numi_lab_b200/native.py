@@ -365,6 +365,8 @@ class TaskTerminationOperatorC(ct.Structure):
         ("group", ct.c_uint32),
         ("threshold", ct.c_float),
         ("failure_penalty", ct.c_float),
+        ("minimum_band", ct.c_uint32),
+        ("maximum_band", ct.c_uint32),
     ]
 
 
@@ -372,6 +374,8 @@ class TaskRandomizationOperatorC(ct.Structure):
     _fields_ = [
         ("opcode", ct.c_uint32),
         ("target", ct.c_uint32),
+        ("minimum_band", ct.c_uint32),
+        ("reserved", ct.c_uint32),
         ("parameters", ct.c_float * 4),
     ]
 
@@ -432,6 +436,11 @@ class TaskProgramC(ct.Structure):
         ("command_upper", ct.c_float * 3),
         ("standing_probability", ct.c_float),
         ("command_duration_seconds", ct.c_float * 2),
+        ("difficulty_band_count", ct.c_uint32),
+        ("band_sampling_exponent", ct.c_float),
+        ("command_limit_lower", ct.c_float * 3),
+        ("command_limit_upper", ct.c_float * 3),
+        ("command_band_step", ct.c_float * 3),
         ("task_fingerprint", ct.c_uint64),
     ]
 

@@ -88,6 +88,8 @@ class Termination:
     threshold: float
     failure_penalty: float = 0.0
     group: int = 0
+    minimum_band: int = 0
+    maximum_band: int = 0xFFFFFFFF  # every band from minimum_band up
 
 
 @dataclass
@@ -106,6 +108,7 @@ class Randomization:
     opcode: int
     parameters: tuple[float, float, float, float] = (0.0, 0.0, 0.0, 0.0)
     target: int = 0
+    minimum_band: int = 0  # skipped in episodes of a lower difficulty band
 
 
 @dataclass
@@ -133,6 +136,11 @@ class TaskProgram:
     command_upper: tuple[float, float, float] = (0.0, 0.0, 0.0)
     standing_probability: float = 0.0
     command_duration_seconds: tuple[float, float] = (1.0, 1.0)
+    difficulty_band_count: int = 1
+    band_sampling_exponent: float = 1.0
+    command_limit_lower: tuple[float, float, float] | None = None  # None: command_lower
+    command_limit_upper: tuple[float, float, float] | None = None  # None: command_upper
+    command_band_step: tuple[float, float, float] = (0.0, 0.0, 0.0)
     task_fingerprint: int = 0
 
 
@@ -162,10 +170,10 @@ def task_program_c(program: TaskProgram) -> tuple[native.TaskProgramC, list[Any]
 
     def fill_term(c, t: Termination):
         c.opcode, c.reason, c.priority, c.threshold, c.failure_penalty = t.opcode, t.reason, t.priority, t.threshold, t.failure_penalty
-        c.group = t.group
+        c.group, c.minimum_band, c.maximum_band = t.group, t.minimum_band, t.maximum_band
 
     def fill_random(c, r: Randomization):
-        c.opcode, c.target = r.opcode, r.target
+        c.opcode, c.target, c.minimum_band = r.opcode, r.target, r.minimum_band
         c.parameters[:] = list(r.parameters)
 
     p = native.TaskProgramC()
@@ -222,6 +230,11 @@ def task_program_c(program: TaskProgram) -> tuple[native.TaskProgramC, list[Any]
     p.command_upper[:] = list(program.command_upper)
     p.standing_probability = program.standing_probability
     p.command_duration_seconds[:] = list(program.command_duration_seconds)
+    p.difficulty_band_count = program.difficulty_band_count
+    p.band_sampling_exponent = program.band_sampling_exponent
+    p.command_limit_lower[:] = list(program.command_limit_lower or program.command_lower)
+    p.command_limit_upper[:] = list(program.command_limit_upper or program.command_upper)
+    p.command_band_step[:] = list(program.command_band_step)
     p.task_fingerprint = program.task_fingerprint
     return p, keep
 

@@ -398,6 +398,7 @@ class World:
         control_dt: float = 0.02,
         seed: int = 0,
         precision: str = "fp32",
+        difficulty_bands: tuple[int, int] | None = None,
         library: native.Bindings | None = None,
     ) -> None:
         self._lib = library or native.bindings()
@@ -413,6 +414,9 @@ class World:
             control_timestep_seconds=control_dt,
             seed=seed,
         )
+        if difficulty_bands is not None:  # the sampled band range of a task's episodes
+            manifest.profile.override_difficulty_band_range = 1
+            manifest.profile.minimum_difficulty_band, manifest.profile.maximum_difficulty_band = difficulty_bands
         handle = self._lib.lib.mr_create_task_rollout(ct.byref(manifest))
         if not handle:
             raise MetalRoboError(f"mr_create_task_rollout: {self._lib.last_error()}")
@@ -778,7 +782,7 @@ class World:
     TRANSITION_FIELDS = ("reward", "tracking_score", "root_height", "tilt", "done", "timeout", "physics_error",
                          "termination_reason", "task_reward", "base_reward", "joint_velocity_reward", "joint_acceleration_reward",
                          "control_reward", "posture_reward", "energy_reward", "contact_reward", "episode_tracking_score",
-                         "policy_revision")
+                         "policy_revision", "difficulty_band")
 
     def transitions(self, steps: int) -> dict[str, np.ndarray]:
         """The last advance's transitions ([step][env] per field; the advance

@@ -140,16 +140,19 @@ class EnvState:
     critic: np.ndarray = field(default_factory=lambda: np.zeros(0))
     action_delay: int = 0
     observation_delay: int = 0
+    band: int = 0
 
 
 class TaskOracle:
     """The task layer over one rollout: `program` a numi_lab_b200.task.TaskProgram."""
 
     def __init__(self, program, *, nq: int, nv: int, dt: float, seed: int, fixed_root: bool, limit_lower, limit_upper,
-                 terminations: bool = True, records=None, world=None, physics_dt: float = 0.0) -> None:
+                 terminations: bool = True, records=None, world=None, physics_dt: float = 0.0,
+                 band_range: tuple[int, int] | None = None) -> None:
         """`records` (compiled world) and `world` (an oracle.Oracle of it,
         for body states) serve the contact groups; `physics_dt` is the
-        microstep."""
+        microstep; `band_range` the rollout's sampled difficulty bands
+        (None: every band)."""
 
         self.p = program
         self.nq, self.nv, self.dt, self.seed, self.fixed_root = nq, nv, float(dt), int(seed), fixed_root
@@ -162,6 +165,8 @@ class TaskOracle:
         self.hi = np.asarray(limit_upper, np.float64)
         self.default_q = np.asarray(program.default_q, np.float64)
         self.terminations = program.terminations if terminations else []
+        self.bands = max(int(getattr(program, "difficulty_band_count", 1)), 1)
+        self.band_range = band_range
         self.records, self.world, self.physics_dt = records, world, float(physics_dt)
         self.groups = list(getattr(program, "contact_groups", []))
         self.metrics = np.zeros((len(self.groups), 12))
@@ -344,9 +349,29 @@ class TaskOracle:
         lo, hi = self.p.command_duration_seconds
         return max(1, int(math.floor(range_draw(self.seed, env, episode, step, channel, lo, hi) / self.dt)))
 
-    def sample_command(self, env, episode, step) -> np.ndarray:
-        cmd = np.array([range_draw(self.seed, env, episode, step, 16 + k, self.p.command_lower[k], self.p.command_upper[k])
-                        for k in range(3)])
+    def sample_band(self, env, episode) -> int:
+        """sampledDifficultyBand (LocomotionTask.metal:1537-1568)."""
+
+        lo, hi = (0, 0xFFFFFFFF) if self.band_range is None else self.band_range
+        lo = min(lo, self.bands - 1)
+        hi = max(lo, min(self.bands - 1 if hi == 0xFFFFFFFF else hi, self.bands - 1))
+        n = hi - lo + 1
+        if n == 1:
+            return lo
+        u = unit_draw(self.seed, env, episode, 0, 15) ** max(float(getattr(self.p, "band_sampling_exponent", 1.0)), 0.01)
+        return lo + min(int(math.floor(u * n)), n - 1)
+
+    def sample_command(self, env, episode, step, band: int = 0) -> np.ndarray:
+        """sampledCommand (:1570-1615): each band widens the range by the
+        step, within the limits."""
+
+        p = self.p
+        step_k = getattr(p, "command_band_step", (0.0, 0.0, 0.0))
+        lim_lo = getattr(p, "command_limit_lower", None) or p.command_lower
+        lim_hi = getattr(p, "command_limit_upper", None) or p.command_upper
+        lower = [max(p.command_lower[k] - band * step_k[k], lim_lo[k]) for k in range(3)]
+        upper = [min(p.command_upper[k] + band * step_k[k], lim_hi[k]) for k in range(3)]
+        cmd = np.array([range_draw(self.seed, env, episode, step, 16 + k, lower[k], upper[k]) for k in range(3)])
         if unit_draw(self.seed, env, episode, step, 19) < self.p.standing_probability:
             cmd[:] = 0.0
         return cmd
@@ -361,9 +386,12 @@ class TaskOracle:
         episode = st.episode + 1
         rq = self.default_q.copy()
         st.action_delay, st.observation_delay = self.delay, 0
+        st.band = self.sample_band(env, episode)
         rv = np.zeros(self.nv)
         for k, op in enumerate(self.p.randomization):
             ch = 2048 + k
+            if st.band < getattr(op, "minimum_band", 0):
+                continue
             a, b = op.parameters[0], op.parameters[1]
             if op.opcode == RND_ROOT_POSITION:
                 for c in range(3):
@@ -402,7 +430,7 @@ class TaskOracle:
         st.episode_step, st.episode = 0, episode
         st.command_steps = self.duration_steps(env, episode, 0, 32)
         st.initialized, st.pending_reset, st.last_reason = True, False, REASON_CONTINUING
-        st.command = self.sample_command(env, episode, 0)
+        st.command = self.sample_command(env, episode, 0, st.band)
         st.phase = 0.0
         st.previous_height = self.root(rq, rv)[1][2]
         st.episode_return = st.episode_tracking = 0.0
@@ -556,6 +584,9 @@ class TaskOracle:
         timeout = steps >= p.maximum_episode_steps
         done, reason, priority, penalty = False, REASON_CONTINUING, 0, 0.0
         for t in self.terminations:
+            top = self.bands - 1 if getattr(t, "maximum_band", 0xFFFFFFFF) == 0xFFFFFFFF else t.maximum_band
+            if st.band < getattr(t, "minimum_band", 0) or st.band > top:
+                continue
             trig = (height < t.threshold if t.opcode == T_MIN_HEIGHT else tilt > t.threshold if t.opcode == T_MAX_TILT
                     else gm[t.group, 0] > t.threshold if t.opcode == T_CONTACT_GROUP else False)
             if trig and (not done or t.priority >= priority):
@@ -576,7 +607,7 @@ class TaskOracle:
         episode_score = episode_tracking / max(steps, 1)
         episode_return = st.episode_return + reward
         if not done and st.command_steps <= 1:
-            st.command = self.sample_command(env, st.episode, steps)
+            st.command = self.sample_command(env, st.episode, steps, st.band)
             st.command_steps = self.duration_steps(env, st.episode, steps, 64)
         elif not done:
             st.command_steps -= 1
@@ -597,7 +628,7 @@ class TaskOracle:
                 st.previous_joint[1, a] = q[b.q_index]
         return {
             "reward": reward, "tracking_score": 0.5 * (tracking + yaw_tracking), "root_height": height, "tilt": tilt,
-            "done": int(done), "timeout": int(timeout), "physics_error": int(physics_error), "termination_reason": reason,
+            "difficulty_band": st.band, "done": int(done), "timeout": int(timeout), "physics_error": int(physics_error), "termination_reason": reason,
             "task_reward": b0[0], "base_reward": b0[1], "joint_velocity_reward": b0[2], "joint_acceleration_reward": b0[3],
             "control_reward": b1[0], "posture_reward": b1[1], "energy_reward": b1[2], "contact_reward": b1[3],
             "episode_tracking_score": episode_score if done and not physics_error else 0.0,

@@ -64,7 +64,8 @@ def test_task_layer_matches_oracle_step_by_step(cuda_device, contacts):
     from oracle import Oracle
 
     envs, steps = 16, 40
-    with nb.World("tree29", envs, substeps=4, velocity_iterations=8, control_dt=DT, seed=SEED) as w:
+    bands = (1, 3) if contacts else None
+    with nb.World("tree29", envs, substeps=4, velocity_iterations=8, control_dt=DT, seed=SEED, difficulty_bands=bands) as w:
         # Tight height and tilt limits: episodes end by timeout, height and
         # tilt within the run.
         groups = T.foot_contact_groups(w.model()) if contacts else None
@@ -76,12 +77,21 @@ def test_task_layer_matches_oracle_step_by_step(cuda_device, contacts):
             prog.randomization += [T.Randomization(T.RANDOMIZE["action_delay"], (0.0, 2.0, 0.0, 0.0)),
                                    T.Randomization(T.RANDOMIZE["observation_delay"], (0.0, 1.0, 0.0, 0.0))]
             prog.maximum_observation_delay = 1
+            # Difficulty bands: episodes draw bands 1-3 (of 4), each band
+            # widens the command range; the velocity kick starts at band 2
+            # and the tilt termination stops after band 2.
+            prog.difficulty_band_count, prog.band_sampling_exponent = 4, 0.8
+            prog.command_band_step = (0.2, 0.1, 0.2)
+            prog.command_limit_lower, prog.command_limit_upper = (-1.0, -0.6, -1.0), (1.6, 0.6, 1.0)
+            prog.randomization.append(T.Randomization(T.RANDOMIZE["velocity"], (-0.2, 0.2, 0.0, 0.0), minimum_band=2))
+            prog.terminations[1].maximum_band = 2
         w.set_task(prog)
         assert w.observation_count == len(prog.actor) * prog.observation_history
         o = _oracle(w, prog)
         if contacts:
             o = TaskOracle(prog, nq=w.nq, nv=w.nv, dt=DT, seed=w.seed, fixed_root=False, limit_lower=o.lo, limit_upper=o.hi,
-                           records=w.model(), world=Oracle(w.model(), DT / 4, 4, 8, 0), physics_dt=DT / 4)
+                           records=w.model(), world=Oracle(w.model(), DT / 4, 4, 8, 0), physics_dt=DT / 4, band_range=bands)
+        band_seen = set()
         touched = 0
         states = [o.new_state() for _ in range(envs)]
         gen = torch.Generator(device="cuda").manual_seed(3)
@@ -105,8 +115,10 @@ def test_task_layer_matches_oracle_step_by_step(cuda_device, contacts):
                 t = o.complete(e, states[e], q[e].astype(np.float64), v[e].astype(np.float64), int(status[e]), env_mans)
                 if contacts:
                     touched += int(np.sum(t["contact_metrics"][:2, 0] > prog.support_force_threshold))
-                for f in ("done", "timeout", "physics_error", "termination_reason"):
+                for f in ("done", "timeout", "physics_error", "termination_reason", "difficulty_band"):
                     assert int(tr[f][0, e]) == t[f], (k, e, f)
+                if contacts:
+                    band_seen.add(t["difficulty_band"])
                 for f in ("reward", "tracking_score", "root_height", "tilt", "task_reward", "base_reward", "joint_velocity_reward",
                           "joint_acceleration_reward", "control_reward", "posture_reward", "contact_reward", "episode_tracking_score"):
                     err = _close(tr[f][0, e], t[f], REWARD_TOL)
@@ -120,6 +132,7 @@ def test_task_layer_matches_oracle_step_by_step(cuda_device, contacts):
         assert seen["reset"] > envs and seen["timeout"] > 0 and seen["height"] + seen["tilt"] > 0
         if contacts:
             assert touched > 0  # the feet carried load on some steps
+            assert band_seen == {1, 2, 3}, band_seen
 
 
 def test_drive_targets_match_the_oracle(cuda_device):

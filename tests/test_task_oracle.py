@@ -260,3 +260,44 @@ def rotate_inverse_np(qv, v):
     from oracle.task import rotate_inverse
 
     return rotate_inverse(np.asarray(qv, float), np.asarray(v, float))
+
+
+def test_difficulty_bands_widen_commands_and_filter_operators(tree):
+    """sampledDifficultyBand and sampledCommand: bands stay in the sampled
+    range, the exponent skews them towards the low end, each band widens
+    the command range by its step within the limits, and band-filtered
+    randomization and termination operators apply only inside their bands."""
+
+    import dataclasses
+
+    rec, prog, lo, hi = tree
+    prog = dataclasses.replace(prog, difficulty_band_count=6, band_sampling_exponent=3.0, command_band_step=(0.25, 0.1, 0.0),
+                               command_limit_lower=(-1.0, -0.4, -0.5), command_limit_upper=(1.5, 0.4, 0.5), standing_probability=0.0,
+                               randomization=[T.Randomization(T.RANDOMIZE["root_height"], (0.9, 0.95, 0.0, 0.0), minimum_band=3)],
+                               terminations=[T.Termination(T.TERMINATE["minimum_root_height"], T.REASON["height"], 1, 1e9,
+                                                           minimum_band=1, maximum_band=2)])
+    q = prog.default_q.astype(float).copy()
+    v = np.zeros(int(rec.world.nv))
+    for band_range, allowed in ((None, range(6)), ((2, 4), range(2, 5)), ((4, 0xFFFFFFFF), range(4, 6)), ((9, 9), [5])):
+        o = TaskOracle(prog, nq=int(rec.world.nq), nv=int(rec.world.nv), dt=DT, seed=3, fixed_root=False, limit_lower=lo,
+                       limit_upper=hi, band_range=band_range)
+        counts = np.zeros(6, int)
+        for env in range(400):
+            st = o.new_state()
+            _, rq, rv, _ = o.observe(env, st, q, v, False)
+            assert st.band in allowed, (band_range, st.band)
+            counts[st.band] += 1
+            b = st.band
+            for k in range(3):
+                lower = max(prog.command_lower[k] - b * prog.command_band_step[k], prog.command_limit_lower[k])
+                upper = min(prog.command_upper[k] + b * prog.command_band_step[k], prog.command_limit_upper[k])
+                assert lower - 1e-12 <= st.command[k] <= upper + 1e-12
+            # The root height draw applies from band 3 on.
+            assert (0.9 <= rq[2] <= 0.95) if b >= 3 else rq[2] == q[2]
+            # The always-true height termination fires only in bands 1-2.
+            t = o.complete(env, st, rq, rv, 0)
+            assert t["difficulty_band"] == b
+            assert (t["termination_reason"] == T.REASON["height"]) == (1 <= b <= 2)
+        if band_range is None:
+            # u^3 puts 1/6^(1/3) = 55 % of the episodes in band 0.
+            assert counts[0] > 180 and counts[5] < counts[0] / 3
