@@ -8,6 +8,9 @@
 namespace numi {
 
 // Words of one solver contact record in shared memory.
+// Most environments (warps) one CTA of the FP32 temporalCone control-step
+// kernel may carry; the other instances carry at most 4.
+constexpr int kMaxStepWarpsPerBlock = 13;
 constexpr int kContactWords = 45;  // 44 used; odd stride keeps lane-per-contact access conflict free
 enum ContactWord : int {
     kCwPoint = 0,      // world contact point (3)

@@ -289,7 +289,12 @@ void numi::rt::make_plan(const numi::CompiledModel& m, float h, KernelPlan& plan
         for (std::uint32_t prec = 0; prec < static_cast<std::uint32_t>(numi::rt::kPrecisionModes); ++prec) {
             const size_t per_warp = static_cast<size_t>(plan.layout_for(prec, quality != 0).total) * sizeof(float);
             int best = 1, best_warps = 0;
-            for (int wpb = 1; wpb <= 4; ++wpb) {
+            // NUMI_B200_STEP_WARPS_PER_BLOCK fixes the CTA size (clamped to
+            // what the instance is built for) instead of the search.
+            const int max_wpb = numi::control_step_max_warps_per_block(prec, quality != 0);
+            int lo = 1, hi = max_wpb;
+            if (const char* env = std::getenv("NUMI_B200_STEP_WARPS_PER_BLOCK")) lo = hi = std::max(1, std::min(max_wpb, std::atoi(env)));
+            for (int wpb = lo; wpb <= hi; ++wpb) {
                 const size_t smem = tables + wpb * per_warp;
                 if (smem > limit) break;
                 int blocks = 0;

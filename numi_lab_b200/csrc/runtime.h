@@ -32,6 +32,8 @@ cudaError_t configure_control_step_kernels(size_t max_dynamic_smem);
 cudaError_t launch_audit_step(const StepParams& p, const WarpLayout& layout, bool fp64_inertia, int warps_per_block,
                               cudaStream_t stream);
 size_t control_step_table_bytes();
+// Largest CTA (in warps) the control-step instance for (precision, quality) is built for.
+int control_step_max_warps_per_block(std::uint32_t precision, bool quality);
 
 namespace rt {
 

@@ -2,11 +2,21 @@
 // device code lives in world_step.cuh.
 #include "world_step.cuh"
 
+#include <type_traits>
+
 namespace numi {
 namespace {
 
+// The FP32 temporalCone instance may run up to kMaxStepWarpsPerBlock
+// environments per CTA (one copy of the topology tables for all of them);
+// the FP64 and quality instances keep CTAs of at most 4 warps and their
+// larger register budgets.
+template <typename R, bool kQuality>
+constexpr bool kWideStepBlock = std::is_same<R, float>::value && !kQuality;
+
 template <bool kContact, typename R, bool kComp, bool kQuality>
-__global__ void __launch_bounds__(128, 3) control_step_kernel(StepParams p, WarpLayout layout, int warps_per_block) {
+__global__ void __launch_bounds__(kWideStepBlock<R, kQuality> ? 32 * kMaxStepWarpsPerBlock : 128, kWideStepBlock<R, kQuality> ? 1 : 3)
+    control_step_kernel(StepParams p, WarpLayout layout, int warps_per_block) {
     extern __shared__ float4 smem4[];
     // Topology tables: one copy per CTA.
     {
@@ -29,7 +39,7 @@ __global__ void __launch_bounds__(128, 3) control_step_kernel(StepParams p, Warp
 // The FP64 audit of the state each environment committed in the launch
 // with the same parameters (one warp per environment, like that launch).
 template <typename R>
-__global__ void __launch_bounds__(128) audit_step_kernel(StepParams p, WarpLayout layout, int warps_per_block) {
+__global__ void __launch_bounds__(32 * kMaxStepWarpsPerBlock) audit_step_kernel(StepParams p, WarpLayout layout, int warps_per_block) {
     extern __shared__ float4 smem4[];
     {
         const uint4* src = reinterpret_cast<const uint4*>(&p.model->tables);
@@ -75,6 +85,10 @@ cudaError_t launch_audit_step(const StepParams& p, const WarpLayout& layout, boo
 }
 
 size_t control_step_table_bytes() { return sizeof(DeviceTables); }
+
+int control_step_max_warps_per_block(std::uint32_t precision, bool quality) {
+    return precision == MR_PRECISION_FP32 && !quality ? kMaxStepWarpsPerBlock : 4;
+}
 
 namespace {
 
